@@ -1,0 +1,303 @@
+"""Benchmark of the B200 flow-solver hot path: multigrid cycles per second.
+
+One step is one multigrid cycle (oneCycle, SolverSource/mgnsg3d_mg_par.F90:
+907-1196) of the growing V-cycle over every level, on the bump-channel mesh
+264x88x88 hexes split into tets (2,099,065 nodes, 14,473,976 edges, 4
+agglomerated levels), seeded synthetic initial state.  The mesh and state
+far exceed the 126 MB L2, so no flush is needed between timed cycles.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (one process per GPU under torchrun) every rank runs an
+independent replica of the solve: the path does not shard (one mesh per GPU,
+no collectives on the data path); value = cycles of all ranks / max time.
+--impl reference times the CPU restatement of the reference solver (the
+Fortran reference cannot be compiled here) on the host cores instead.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+MESH = dict(nx=264, ny=88, nz=88, bump=0.05, levels=4)
+METRIC = "MG cycles/s"
+CONTROLS = dict(ReynoldsNumber=0.0, MachNumber=0.5, alpha=0.0, CFLNumber=2.0, fluxType=1,
+                multigridScheme=3, numberOfGridsToUse=4)
+WORKLOAD = ("bump channel 264x88x88 hex -> 6 tets (2,099,065 nodes, 14,473,976 edges), "
+            "4 agglomerated MG levels, growing V-cycle, 3-stage RK, CFL 2, M 0.5; "
+            "inviscid Euler central flux + JST (viscous terms not yet in this build)")
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 5 + k and s[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_case():
+    import flite3d_b200 as F
+    t0 = time.time()
+    mesh = F.Mesh.bump_channel(MESH["nx"], MESH["ny"], MESH["nz"], MESH["bump"], MESH["levels"])
+    c = F.default_controls(**CONTROLS)
+    u0 = F.initial_state(c, mesh, perturb_seed=20261203, amplitude=0.01)
+    return F, mesh, c, u0, time.time() - t0
+
+
+def edge_kernel_bytes(mesh):
+    """Algorithmic bytes of one edge-flux launch on level 1: per edge the two
+    node indices (8 B), the edge coefficients (24 B) and the flux written to
+    the edge buffer (40 B); per node the state and pressure read once (48 B)."""
+    d = mesh.level(1)
+    return d.n_sides * (8 + 24 + 40) + d.n_nodes * 48
+
+
+def gather_kernel_bytes(mesh):
+    """Algorithmic bytes of one node residual gather (RESID mode) on level 1:
+    per edge two incidence records (16 B) and two flux reads (80 B), per
+    boundary edge two records and two reads (8 + 80 B), per node the CSR
+    offsets (8 B) and the residual written (40 B)."""
+    d = mesh.level(1)
+    return d.n_sides * (16 + 80) + d.n_bsides * (8 + 80) + d.n_nodes * (8 + 40)
+
+
+def run_ours(args):
+    ws, rank, local = _dist()
+    import torch
+    import torch.distributed as dist
+    if not torch.cuda.is_available():
+        raise SystemExit("no CUDA device: the product path has no CPU fallback")
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    F, mesh, c, u0, t_mesh = build_case()
+    solver = F.Solver(c, mesh)
+    solver.set_state(u0)
+    solver.start()
+    # warm-up (also captures the cycle graph)
+    for i in range(1, args.warmup + 1):
+        solver.cycle(i)
+    res, _, _ = solver.residuals()
+    launches_per_cycle = solver.cycle_launches()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms = solver.time_cycles(args.steps, cycle_no=args.warmup + 1)
+    torch.cuda.synchronize()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = ws * args.steps / (ms_max / 1e3)
+
+    # kernel-level timing of the dominant edge kernels on level 1
+    edge_ms, gather_ms = solver.profile_level(1, reps=20)
+    hbm, peak_kind = _peaks()
+    eb = edge_kernel_bytes(mesh)
+    achieved = eb / (edge_ms / 1e3) / 1e9
+
+    # end to end through the public API with host buffers: per cycle the
+    # level-1 state goes host->device from pinned memory, the cycle runs, and
+    # the residual norms, forces and state come back to the host
+    n = mesh.level(1).n_nodes
+    pin = torch.empty((5, n), dtype=torch.float64, pin_memory=True)
+    host_u = pin.numpy()
+    host_u[:] = solver.get_state(1)
+    cyc = args.warmup + args.steps + 1
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        solver.set_state(host_u)
+        solver.cycle(cyc + k)
+        r, _, _ = solver.residuals()
+        fc = solver.forces()
+        host_u[:] = solver.get_state(1)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = ws * args.steps / float(te.item())
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(mesh, c, u0, cycles=args.cpu_cycles)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "cycles/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (generated bump-channel mesh, seeded +-1% density perturbation)",
+        "config": {"workload": WORKLOAD, "mesh_nodes": mesh.level(1).n_nodes,
+                   "mesh_edges": mesh.level(1).n_sides, "levels": mesh.nlevels,
+                   "parallelism": f"replicas{ws}" if ws > 1 else "single",
+                   "l2": "inputs larger than L2 (state+mesh+edge buffer > 1 GB)",
+                   "mesh_build_s": round(t_mesh, 2)},
+        "e2e": {"value": e2e_value, "unit": "cycles/s", "h2d_bytes_per_step": 5 * n * 8 + 4,
+                "d2h_bytes_per_step": 5 * n * 8 + 15 * 8 + 6 * 8},
+        "gpu_launches": int(launches_per_cycle * args.steps),
+        "roofline": {"kernel": "k_edge_flux (level 1)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "algorithmic_bytes": eb, "launch_ms": edge_ms,
+                     "traffic": None,
+                     "gather_kernel": {"launch_ms": gather_ms,
+                                       "achieved": gather_kernel_bytes(mesh) / (gather_ms / 1e3) / 1e9}},
+        "clocks": clk.summary(),
+        "residual_after_warmup": float(res[0]),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(mesh, c, u0, cycles=2):
+    """The CPU restatement (oracle/) timed on the host: a bounded sample of the
+    same workload (a few cycles of the same mesh and controls)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import flite3d_b200.build as b
+    from flite3d_b200.solver import Backend, Solver
+    b.build_oracle()
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
+    o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
+    o.set_state(u0)
+    o.start()
+    o.cycle(1)  # warm the caches
+    t0 = time.perf_counter()
+    for i in range(cycles):
+        o.cycle(2 + i)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": cycles / dt, "unit": "cycles/s", "cores": 1, "kind": "port",
+            "sample": f"{cycles} cycles of the same 2.1M-node workload after one warm-up cycle, "
+                      "single thread, FP64 C++ restatement in reference edge order"}
+
+
+def run_reference(args):
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    F, mesh, c, u0, _ = build_case()
+    import flite3d_b200.build as b
+    from flite3d_b200.solver import Backend, Solver
+    b.build_oracle()
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
+    o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
+    o.set_state(u0)
+    o.start()
+    for i in range(1, min(args.warmup, 1) + 1):
+        o.cycle(i)
+    steps = max(1, min(args.steps, args.cpu_cycles))
+    t0 = time.perf_counter()
+    for i in range(steps):
+        o.cycle(2 + i)
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "cycles/s", "n_gpus": 0,
+        "steps": steps, "warmup": 1, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": v, "unit": "cycles/s", "cores": 1, "kind": "port",
+                         "sample": f"{steps} cycles after 1 warm-up cycle; the Fortran reference "
+                                   "cannot be compiled here (no Fortran compiler), so the CPU "
+                                   "restatement of it runs"},
+        "e2e": {"value": v, "unit": "cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-cycles", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

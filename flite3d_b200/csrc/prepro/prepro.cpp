@@ -1,0 +1,1117 @@
+// Host-side preprocessor: synthetic tetrahedral meshes, a restatement of
+// gen3d's tetrahedral path, greedy agglomeration, and the reference's
+// Fortran-record file formats.  C ABI in include/flite_prepro.h.
+//
+// What follows the reference step by step (file:line in PreProSource/):
+//   * median-dual edge coefficients and nodal volumes of a tetrahedron:
+//     makeCalcDataForTet gen3d_grid.f90:2092-2332 with registerSideGCL
+//     :786-855 (static mesh: the GCL terms vanish and are written as 0);
+//   * edge registration with i1<i2 orientation and coefficient summation:
+//     registerSideData gen3d_struct.f90:366-464;
+//   * boundary-edge coefficients of a triangle: makeCalcDataForBoundary
+//     gen3d_boundary.f90:511-620 with registerBoundarySideGCL :289-372;
+//   * node-indicator priority (inviscid < symmetry < wall < far field <
+//     engine): setBoundIndForViscousMesh gen3d_boundary.f90:1587-1640;
+//   * the indicator register and the node list written per indicator:
+//     writeParallelComputationFiles gen3d_grid.f90:4548-4580;
+//   * coarse edges as sums of fine edges between different parents:
+//     createSides gen3d_grid.f90:3558-3611; coarse boundary edges including
+//     self-edges of one coarse node: agglomerateBoundary gen3d_boundary.f90:
+//     922-1023; coarse node indicators by the same priority :1101-1121;
+//   * coarse volumes as sums of fine volumes (mergeNodes gen3d_grid.f90:
+//     2822-2829) and restriction weights V_f/V_c.
+// The seed selection of the agglomeration is this project's own greedy
+// scheme (largest available connectivity first, boundary nodes before
+// interior nodes, all free neighbours merged, single-node aggregates merged
+// into their strongest neighbour); gen3d's mergeNodes (:2358-2902) follows
+// the same priority idea with a different list-update order.
+#include <algorithm>
+#include <chrono>
+#include <cctype>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "flite_prepro.h"
+#include "fortran_io.hpp"
+
+namespace {
+
+struct LevelData {
+    int32_t N = 0, E = 0, B = 0, Nb = 0;
+    std::vector<int32_t> side;   // [2][E] column-major, 1-based
+    std::vector<double> sw;      // [3][E]
+    std::vector<double> slen;    // [E]
+    std::vector<int32_t> bside;  // [3][B] (i1, i2, indicator)
+    std::vector<double> bw;      // [3][B]
+    int32_t reg[21] = {0};       // nodeIndicatorRegister(-20:0)
+    std::vector<int32_t> node_ind;
+    std::vector<double> bnormal;  // [3][n_normals]
+    std::vector<int32_t> bnd_indicator;  // [Nb] indicator per boundary node
+    std::vector<double> vol, wdist;
+    std::vector<int32_t> wnode;
+    std::vector<double> xyz;      // [3][N] (level 1 only)
+    std::vector<int32_t> seed;    // [N] (coarse levels)
+    std::vector<int32_t> parent;  // [N_finer] (coarse levels)
+    std::vector<double> rweight;  // [N_finer]
+};
+
+}  // namespace
+
+struct fp_mesh {
+    std::vector<LevelData> lv;
+    std::vector<int32_t> perm;    // new -> old, 1-based
+    std::vector<int32_t> tets;    // [4][ntet] new numbering
+    std::vector<int32_t> tris;    // [3][ntri]
+    std::vector<int32_t> tri_ind;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+// optional section timing on stderr (FP_TIMING=1)
+struct SectionTimer {
+    const char *name;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    explicit SectionTimer(const char *n) : name(n) {}
+    ~SectionTimer() {
+        static const bool on = std::getenv("FP_TIMING") != nullptr;
+        if (on)
+            std::fprintf(stderr, "[prepro] %s %.3f s\n", name,
+                         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
+
+// ---- open-addressing map from an ordered node pair to a slot -------------
+class PairMap {
+  public:
+    explicit PairMap(size_t expect) {
+        size_t cap = 16;
+        while (cap < expect * 2 + 16) cap <<= 1;
+        keys_.assign(cap, ~0ull);
+        vals_.assign(cap, -1);
+        mask_ = cap - 1;
+    }
+    // returns existing value or inserts `val` and returns -1
+    int64_t find_or_insert(uint64_t key, int64_t val) {
+        size_t h = hash(key) & mask_;
+        while (true) {
+            if (keys_[h] == key) return vals_[h];
+            if (keys_[h] == ~0ull) {
+                keys_[h] = key; vals_[h] = val;
+                if (++count_ * 2 > keys_.size()) grow();
+                return -1;
+            }
+            h = (h + 1) & mask_;
+        }
+    }
+    int64_t find(uint64_t key) const {
+        size_t h = hash(key) & mask_;
+        while (true) {
+            if (keys_[h] == key) return vals_[h];
+            if (keys_[h] == ~0ull) return -1;
+            h = (h + 1) & mask_;
+        }
+    }
+
+  private:
+    static size_t hash(uint64_t k) {
+        k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33;
+        k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+        return (size_t)k;
+    }
+    void grow() {
+        std::vector<uint64_t> ok; std::vector<int64_t> ov;
+        ok.swap(keys_); ov.swap(vals_);
+        keys_.assign(ok.size() * 2, ~0ull); vals_.assign(ok.size() * 2, -1);
+        mask_ = keys_.size() - 1; count_ = 0;
+        for (size_t i = 0; i < ok.size(); ++i)
+            if (ok[i] != ~0ull) find_or_insert(ok[i], ov[i]);
+    }
+    std::vector<uint64_t> keys_;
+    std::vector<int64_t> vals_;
+    size_t mask_ = 0, count_ = 0;
+};
+
+inline uint64_t pkey(int64_t a, int64_t b) { return ((uint64_t)a << 32) | (uint64_t)(uint32_t)b; }
+
+struct V3 { double x, y, z; };
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 scl(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline V3 div3(V3 a) { return {a.x / 3., a.y / 3., a.z / 3.}; }
+
+// Cxx(1,:) = 0.5*(r1(2)*r2(3)-r1(3)*r2(2)) ... (gen3d_grid.f90:799-804)
+inline V3 halfcross(V3 r1, V3 r2) {
+    return {0.5 * (r1.y * r2.z - r1.z * r2.y), 0.5 * (r1.z * r2.x - r1.x * r2.z),
+            0.5 * (r1.x * r2.y - r1.y * r2.x)};
+}
+
+// Indicator priority of setBoundIndForViscousMesh (gen3d_boundary.f90:
+// 1607-1620) and agglomerateBoundary (:1101-1121).
+inline int merge_indicator(int cur, int nw) {
+    if (nw == cur) return cur;
+    if (cur > 0) {
+        if (cur == 9) return nw;
+        if (cur == 2 && nw != 9) return nw;
+        if (cur == 1 && nw > 2) return nw;
+        if (cur <= 4 && nw > 4) return nw;
+        return cur;
+    }
+    return nw;
+}
+
+// Register and node list from per-boundary-node indicators (gen3d_grid.f90:
+// 4548-4580): counts at -21+2k, then running (start, end) pairs.
+void build_register(LevelData &L) {
+    int32_t r[21] = {0};
+    auto R = [&](int i) -> int32_t & { return r[i + 20]; };
+    for (int j = 0; j < L.Nb; ++j) {
+        int ind = L.bnd_indicator[j];
+        if (ind > 0) R(-21 + ind * 2) += 1;
+    }
+    R(-20) = 1;
+    for (int j = -18; j <= -2; j += 2) {
+        R(j + 1) = R(j + 1) + R(j - 1);
+        R(j) = R(j - 1) + 1;
+    }
+    std::memcpy(L.reg, r, sizeof r);
+    L.node_ind.clear();
+    std::vector<double> nrm;
+    for (int k = 1; k <= 9; ++k)
+        for (int j = 0; j < L.Nb; ++j)
+            if (L.bnd_indicator[j] == k) L.node_ind.push_back(j + 1);
+    // normals written beside each node (not read by the solver): -sum w_b
+    std::vector<double> acc(3 * (size_t)L.Nb, 0.0);
+    for (int b = 0; b < L.B; ++b) {
+        for (int s = 0; s < 2; ++s) {
+            int n = L.bside[(size_t)s * L.B + b] - 1;
+            for (int k = 0; k < 3; ++k) acc[3 * (size_t)n + k] -= L.bw[(size_t)k * L.B + b];
+        }
+    }
+    size_t nn = L.node_ind.size();
+    L.bnormal.assign(3 * nn, 0.0);
+    for (size_t i = 0; i < nn; ++i) {
+        int n = L.node_ind[i] - 1;
+        double a = acc[3 * n], b = acc[3 * n + 1], c = acc[3 * n + 2];
+        double s = std::sqrt(a * a + b * b + c * c);
+        if (s > 1e-20) { a /= s; b /= s; c /= s; } else { a = b = c = 0; }
+        L.bnormal[0 * nn + i] = a; L.bnormal[1 * nn + i] = b; L.bnormal[2 * nn + i] = c;
+    }
+}
+
+
+// k-d tree over a point subset for nearest-point queries
+class KdTree {
+  public:
+    template <class Get>
+    KdTree(const std::vector<int32_t> &ids, Get get) : id_(ids) {
+        pt_.resize(id_.size());
+        for (size_t i = 0; i < id_.size(); ++i) pt_[i] = get(id_[i]);
+        build(0, id_.size(), 0);
+    }
+    int32_t nearest(V3 q, double *d2) const {
+        best_ = 1e300; bid_ = 0;
+        search(0, id_.size(), 0, q);
+        *d2 = best_;
+        return bid_;
+    }
+
+  private:
+    static double comp(V3 p, int a) { return a == 0 ? p.x : (a == 1 ? p.y : p.z); }
+    void build(size_t lo, size_t hi, int depth) {
+        if (hi - lo <= 8) return;
+        size_t mid = (lo + hi) / 2;
+        int a = depth % 3;
+        std::vector<size_t> idx(hi - lo);
+        for (size_t i = 0; i < idx.size(); ++i) idx[i] = lo + i;
+        std::nth_element(idx.begin(), idx.begin() + (mid - lo), idx.end(),
+                         [&](size_t x, size_t y) { return comp(pt_[x], a) < comp(pt_[y], a); });
+        std::vector<V3> p2(idx.size()); std::vector<int32_t> i2(idx.size());
+        for (size_t i = 0; i < idx.size(); ++i) { p2[i] = pt_[idx[i]]; i2[i] = id_[idx[i]]; }
+        for (size_t i = 0; i < idx.size(); ++i) { pt_[lo + i] = p2[i]; id_[lo + i] = i2[i]; }
+        build(lo, mid, depth + 1);
+        build(mid + 1, hi, depth + 1);
+    }
+    void visit(size_t i, V3 q) const {
+        V3 d = pt_[i] - q;
+        double dd = d.x * d.x + d.y * d.y + d.z * d.z;
+        if (dd < best_ || (dd == best_ && id_[i] < bid_)) { best_ = dd; bid_ = id_[i]; }
+    }
+    void search(size_t lo, size_t hi, int depth, V3 q) const {
+        if (hi - lo <= 8) { for (size_t i = lo; i < hi; ++i) visit(i, q); return; }
+        size_t mid = (lo + hi) / 2;
+        int a = depth % 3;
+        visit(mid, q);
+        double diff = comp(q, a) - comp(pt_[mid], a);
+        if (diff < 0) {
+            search(lo, mid, depth + 1, q);
+            if (diff * diff <= best_) search(mid + 1, hi, depth + 1, q);
+        } else {
+            search(mid + 1, hi, depth + 1, q);
+            if (diff * diff <= best_) search(lo, mid, depth + 1, q);
+        }
+    }
+    std::vector<int32_t> id_;
+    std::vector<V3> pt_;
+    mutable double best_ = 0;
+    mutable int32_t bid_ = 0;
+};
+
+// ---- level 1 from tetrahedra --------------------------------------------
+void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
+                std::vector<int32_t> tets_old, std::vector<int32_t> tris_old,
+                const std::vector<int32_t> &tri_ind) {
+    const int32_t NT = (int32_t)(tets_old.size() / 4);
+    const int32_t NF = (int32_t)(tris_old.size() / 3);
+    // boundary-first numbering (gen3d_grid.f90:127-383): boundary nodes keep
+    // their relative order and take 1..Nb, interior nodes follow
+    std::vector<char> isb(N, 0);
+    for (int32_t f = 0; f < NF; ++f)
+        for (int k = 0; k < 3; ++k) isb[tris_old[(size_t)k * NF + f] - 1] = 1;
+    std::vector<int32_t> o2n(N), n2o(N);
+    int32_t nb = 0;
+    for (int32_t i = 0; i < N; ++i) if (isb[i]) { o2n[i] = nb; n2o[nb] = i; ++nb; }
+    int32_t ni = nb;
+    for (int32_t i = 0; i < N; ++i) if (!isb[i]) { o2n[i] = ni; n2o[ni] = i; ++ni; }
+    M.perm.resize(N);
+    for (int32_t i = 0; i < N; ++i) M.perm[i] = n2o[i] + 1;
+
+    LevelData L;
+    L.N = N; L.Nb = nb;
+    L.xyz.resize(3 * (size_t)N);
+    for (int32_t i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) L.xyz[(size_t)k * N + i] = xyz_old[(size_t)k * N + n2o[i]];
+    auto X = [&](int32_t p) -> V3 {  // 1-based new index
+        return {L.xyz[p - 1], L.xyz[(size_t)N + p - 1], L.xyz[2 * (size_t)N + p - 1]};
+    };
+    for (auto &t : tets_old) t = o2n[t - 1] + 1;
+    for (auto &t : tris_old) t = o2n[t - 1] + 1;
+
+    // edges of every tetrahedron (makeCalcDataForTet, gen3d_grid.f90:2092-2332)
+    auto *tm_edges = new SectionTimer("tet edges");
+    // side lookup: a few slots per first node (edges are keyed by their
+    // smaller node, and tets arrive roughly in node order, so this stays in
+    // cache); nodes with more sides spill into a hash map
+    constexpr int kSlots = 12;
+    std::vector<int32_t> slot_i2((size_t)N * kSlots, 0), slot_id((size_t)N * kSlots, -1);
+    PairMap smap(1024);
+    std::vector<int32_t> s1, s2;
+    std::vector<V3> sc;
+    std::vector<double> sl;
+    s1.reserve(NT * 7 / 6 + 16); s2.reserve(NT * 7 / 6 + 16);
+    sc.reserve(NT * 7 / 6 + 16); sl.reserve(NT * 7 / 6 + 16);
+    L.vol.assign(N, 0.0);
+    int64_t nneg = 0;
+    auto register_side = [&](int32_t p1, int32_t p2, V3 r1, V3 r2, V3 r3, V3 r4, V3 rv) -> double {
+        V3 c1 = halfcross(r1, r2), c2 = halfcross(r3, r4);
+        V3 cxx = c1 + c2;
+        double nv = (rv.x * cxx.x + rv.y * cxx.y + rv.z * cxx.z) / 3.;
+        L.vol[p1 - 1] += nv;
+        L.vol[p2 - 1] += nv;
+        V3 coef = scl(0.5, cxx);  // store half the side coefficient
+        V3 d = X(p2) - X(p1);
+        double len = std::sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+        int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
+        if (i1 != p1) coef = scl(-1.0, coef);
+        int64_t slot = -1;
+        {
+            const size_t base = (size_t)(i1 - 1) * kSlots;
+            int q = 0;
+            for (; q < kSlots; ++q) {
+                if (slot_id[base + q] < 0) break;
+                if (slot_i2[base + q] == i2) { slot = slot_id[base + q]; break; }
+            }
+            if (slot < 0) {
+                if (q < kSlots) {
+                    slot_i2[base + q] = i2; slot_id[base + q] = (int32_t)s1.size();
+                } else {
+                    slot = smap.find_or_insert(pkey(i1, i2), (int64_t)s1.size());
+                }
+            }
+        }
+        if (slot < 0) {
+            s1.push_back(i1); s2.push_back(i2); sc.push_back(coef); sl.push_back(len);
+        } else {
+            sc[slot] = sc[slot] + coef;
+        }
+        return nv;
+    };
+    for (int32_t t = 0; t < NT; ++t) {
+        int32_t p[4] = {tets_old[t], tets_old[(size_t)NT + t], tets_old[2 * (size_t)NT + t],
+                        tets_old[3 * (size_t)NT + t]};
+        // orientation: the element volume of gen3d must be positive; a tet
+        // given with the opposite orientation is flipped (swap nodes 3, 4)
+        {
+            V3 a = X(p[1]) - X(p[0]), b = X(p[2]) - X(p[0]), c = X(p[3]) - X(p[0]);
+            double det = a.x * (b.y * c.z - b.z * c.y) - a.y * (b.x * c.z - b.z * c.x) +
+                         a.z * (b.x * c.y - b.y * c.x);
+            if (det < 0) std::swap(p[2], p[3]);
+        }
+        tets_old[t] = p[0]; tets_old[(size_t)NT + t] = p[1];
+        tets_old[2 * (size_t)NT + t] = p[2]; tets_old[3 * (size_t)NT + t] = p[3];
+        V3 x1 = X(p[0]), x2 = X(p[1]), x3 = X(p[2]), x4 = X(p[3]);
+        V3 xmm = scl(0.25, x1 + x2 + x3 + x4);
+        double ev = 0;
+        {   // node 1
+            V3 xm1 = scl(0.5, x1 + x2), xm2 = scl(0.5, x1 + x3), xm3 = scl(0.5, x1 + x4);
+            V3 xb1 = div3(x1 + x2 + x3), xb2 = div3(x1 + x2 + x4), xb3 = div3(x1 + x3 + x4);
+            ev += 2. * register_side(p[0], p[1], xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x1);
+            ev += 2. * register_side(p[0], p[2], xmm - xm2, xb1 - xm2, xb3 - xm2, xmm - xm2, xm2 - x1);
+            ev += 2. * register_side(p[0], p[3], xmm - xm3, xb3 - xm3, xb2 - xm3, xmm - xm3, xm3 - x1);
+        }
+        {   // node 2
+            V3 xm1 = scl(0.5, x2 + x3), xm2 = scl(0.5, x2 + x4);
+            V3 xb1 = div3(x1 + x2 + x3), xb2 = div3(x2 + x3 + x4), xb3 = div3(x1 + x2 + x4);
+            ev += 2. * register_side(p[1], p[2], xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x2);
+            ev += 2. * register_side(p[1], p[3], xmm - xm2, xb3 - xm2, xb2 - xm2, xmm - xm2, xm2 - x2);
+        }
+        {   // node 3
+            V3 xm1 = scl(0.5, x3 + x4);
+            V3 xb1 = div3(x1 + x3 + x4), xb2 = div3(x2 + x3 + x4);
+            ev += 2. * register_side(p[2], p[3], xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x3);
+        }
+        if (ev <= 0) ++nneg;
+    }
+    delete tm_edges;
+    { std::vector<int32_t>().swap(slot_i2); std::vector<int32_t>().swap(slot_id); }
+    if (nneg) throw std::runtime_error("negative element volumes: " + std::to_string(nneg));
+    L.E = (int32_t)s1.size();
+    L.side.resize(2 * (size_t)L.E); L.sw.resize(3 * (size_t)L.E); L.slen = sl;
+    for (int32_t e = 0; e < L.E; ++e) {
+        L.side[e] = s1[e]; L.side[(size_t)L.E + e] = s2[e];
+        L.sw[e] = sc[e].x; L.sw[(size_t)L.E + e] = sc[e].y; L.sw[2 * (size_t)L.E + e] = sc[e].z;
+    }
+    { std::vector<V3>().swap(sc); }
+
+    // boundary triangles: orient each so that its right-hand normal points
+    // into the domain (towards the tet that owns it), which makes the
+    // boundary coefficients outward like the edge coefficients
+    SectionTimer tm_faces("boundary faces");
+    PairMap fmap((size_t)NF + 16);
+    auto fkey = [&](int32_t a, int32_t b, int32_t c) {
+        int32_t s[3] = {a, b, c};
+        std::sort(s, s + 3);
+        // 21 bits per index would overflow for big meshes; combine two keys
+        return std::make_pair(pkey(s[0], s[1]), (uint64_t)s[2]);
+    };
+    // face -> opposite vertex: store in a map keyed by (min,mid) with a
+    // per-face list; faces sharing (min,mid) are few, resolved linearly
+    std::vector<int32_t> fopp(NF, 0);
+    {
+        std::vector<std::vector<std::pair<int32_t, int32_t>>> buckets;  // (max, face)
+        buckets.reserve(NF);
+        for (int32_t f = 0; f < NF; ++f) {
+            auto k = fkey(tris_old[f], tris_old[(size_t)NF + f], tris_old[2 * (size_t)NF + f]);
+            int64_t slot = fmap.find_or_insert(k.first, (int64_t)buckets.size());
+            if (slot < 0) { buckets.emplace_back(); slot = (int64_t)buckets.size() - 1; }
+            buckets[slot].push_back({(int32_t)k.second, f});
+        }
+        for (int32_t t = 0; t < NT; ++t) {
+            int32_t p[4] = {tets_old[t], tets_old[(size_t)NT + t], tets_old[2 * (size_t)NT + t],
+                            tets_old[3 * (size_t)NT + t]};
+            int nbn = (p[0] <= nb) + (p[1] <= nb) + (p[2] <= nb) + (p[3] <= nb);
+            if (nbn < 3) continue;  // a boundary face has three boundary nodes
+            for (int o = 0; o < 4; ++o) {
+                int32_t a = p[(o + 1) % 4], b = p[(o + 2) % 4], c = p[(o + 3) % 4];
+                auto k = fkey(a, b, c);
+                int64_t slot = fmap.find(k.first);
+                if (slot < 0) continue;
+                for (auto &pr : buckets[slot])
+                    if (pr.first == (int32_t)k.second) fopp[pr.second] = p[o];
+            }
+        }
+    }
+    PairMap bmap((size_t)NF * 2 + 16);
+    std::vector<int32_t> b1, b2, bi;
+    std::vector<V3> bc;
+    auto register_bside = [&](int32_t p1, int32_t p2, V3 r1, V3 r2, int ind) {
+        V3 cxx = halfcross(r1, r2);
+        int32_t i1 = std::min(p1, p2), i2 = std::max(p1, p2);
+        int64_t slot = bmap.find_or_insert(pkey(i1, i2), (int64_t)b1.size());
+        if (slot >= 0) {
+            bc[slot] = bc[slot] + scl(0.25, cxx);
+        } else {
+            b1.push_back(i1); b2.push_back(i2); bi.push_back(ind); bc.push_back(scl(0.25, cxx));
+        }
+    };
+    std::vector<int32_t> tris_new(3 * (size_t)NF);
+    for (int32_t f = 0; f < NF; ++f) {
+        int32_t p1 = tris_old[f], p2 = tris_old[(size_t)NF + f], p3 = tris_old[2 * (size_t)NF + f];
+        if (fopp[f] == 0) throw std::runtime_error("boundary triangle without a tetrahedron");
+        V3 a = X(p2) - X(p1), b = X(p3) - X(p1), d = X(fopp[f]) - X(p1);
+        V3 n = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+        if (n.x * d.x + n.y * d.y + n.z * d.z < 0) std::swap(p2, p3);
+        tris_new[f] = p1; tris_new[(size_t)NF + f] = p2; tris_new[2 * (size_t)NF + f] = p3;
+        int ind = tri_ind[f];
+        V3 x1 = X(p1), x2 = X(p2), x3 = X(p3);
+        V3 xm = div3(x1 + x2 + x3);
+        V3 xb1 = scl(0.5, x1 + x2), xb2 = scl(0.5, x2 + x3), xb3 = scl(0.5, x3 + x1);
+        register_bside(p1, p2, xm - x1, xb1 - x1, ind);
+        register_bside(p1, p3, xb3 - x1, xm - x1, ind);
+        register_bside(p2, p3, xm - x2, xb2 - x2, ind);
+    }
+    L.B = (int32_t)b1.size();
+    L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B);
+    for (int32_t b = 0; b < L.B; ++b) {
+        L.bside[b] = b1[b]; L.bside[(size_t)L.B + b] = b2[b]; L.bside[2 * (size_t)L.B + b] = bi[b];
+        L.bw[b] = bc[b].x; L.bw[(size_t)L.B + b] = bc[b].y; L.bw[2 * (size_t)L.B + b] = bc[b].z;
+    }
+    // node indicators by priority over the faces in order
+    L.bnd_indicator.assign(nb, 0);
+    for (int32_t f = 0; f < NF; ++f)
+        for (int k = 0; k < 3; ++k) {
+            int32_t n = tris_new[(size_t)k * NF + f] - 1;
+            L.bnd_indicator[n] = merge_indicator(L.bnd_indicator[n], tri_ind[f]);
+        }
+    build_register(L);
+
+    // wall distance: Euclidean distance to the nearest wall (indicator 1)
+    // node and that node's number, by a k-d tree over the wall nodes
+    L.wdist.assign(N, 1.0e6);
+    L.wnode.assign(N, 0);
+    std::vector<int32_t> wall;
+    for (int32_t j = 0; j < nb; ++j) if (L.bnd_indicator[j] == 1) wall.push_back(j + 1);
+    SectionTimer tm_wall("wall distance");
+    if (!wall.empty()) {
+        KdTree kd(wall, [&](int32_t p) { return X(p); });
+        unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                KdTree local = kd;  // queries keep per-tree scratch state
+                for (int32_t i = (int32_t)t; i < N; i += (int32_t)nt) {
+                    double d2; int32_t w = local.nearest(X(i + 1), &d2);
+                    L.wdist[i] = std::sqrt(d2);
+                    L.wnode[i] = w;
+                }
+            });
+        for (auto &x : th) x.join();
+    }
+    M.tets = std::move(tets_old);
+    M.tris = std::move(tris_new);
+    M.tri_ind = tri_ind;
+    M.lv.clear();
+    M.lv.push_back(std::move(L));
+}
+
+// ---- agglomeration --------------------------------------------------------
+void agglomerate(const LevelData &F, LevelData &C) {
+    const int32_t N = F.N, E = F.E;
+    // node -> incident edges in edge order
+    std::vector<int32_t> rp(N + 1, 0), adj(2 * (size_t)E);
+    for (int32_t e = 0; e < E; ++e) { rp[F.side[e]]++; rp[F.side[(size_t)E + e]]++; }
+    for (int32_t i = 0; i < N; ++i) rp[i + 1] += rp[i];
+    {
+        std::vector<int32_t> fill(rp.begin(), rp.end() - 1);
+        for (int32_t e = 0; e < E; ++e) {
+            adj[fill[F.side[e] - 1]++] = e;
+            adj[fill[F.side[(size_t)E + e] - 1]++] = e;
+        }
+    }
+    auto other = [&](int32_t e, int32_t i) {  // 0-based node
+        int32_t a = F.side[e] - 1, b = F.side[(size_t)E + e] - 1;
+        return a == i ? b : a;
+    };
+    auto wnorm = [&](int32_t e) {
+        double x = F.sw[e], y = F.sw[(size_t)E + e], z = F.sw[2 * (size_t)E + e];
+        return std::sqrt(x * x + y * y + z * z);
+    };
+    std::vector<int32_t> avail(N), agg(N, -1);
+    int32_t maxdeg = 0;
+    for (int32_t i = 0; i < N; ++i) { avail[i] = rp[i + 1] - rp[i]; maxdeg = std::max(maxdeg, avail[i]); }
+    std::vector<int32_t> seed_of;  // aggregate -> fine seed (0-based)
+    for (int grp = 0; grp < 2; ++grp) {
+        int32_t lo = grp == 0 ? 0 : F.Nb, hi = grp == 0 ? F.Nb : N;
+        std::vector<std::deque<int32_t>> bucket(maxdeg + 1);
+        for (int32_t i = lo; i < hi; ++i) bucket[avail[i]].push_back(i);
+        int cur = maxdeg;
+        while (true) {
+            while (cur >= 0 && bucket[cur].empty()) --cur;
+            if (cur < 0) break;
+            int32_t s = bucket[cur].front(); bucket[cur].pop_front();
+            if (agg[s] >= 0 || avail[s] != cur) continue;  // stale entry
+            int32_t a = (int32_t)seed_of.size();
+            seed_of.push_back(s);
+            agg[s] = a; avail[s] = 0;
+            std::vector<int32_t> merged;
+            for (int32_t k = rp[s]; k < rp[s + 1]; ++k) {
+                int32_t n = other(adj[k], s);
+                if (agg[n] < 0) { agg[n] = a; avail[n] = 0; merged.push_back(n); }
+            }
+            for (int32_t n : merged)
+                for (int32_t k = rp[n]; k < rp[n + 1]; ++k) {
+                    int32_t m = other(adj[k], n);
+                    if (agg[m] < 0) {
+                        avail[m] -= 1;
+                        if (m >= lo && m < hi) bucket[avail[m]].push_back(m);
+                    }
+                }
+        }
+    }
+    // single-node aggregates join the neighbour aggregate of the strongest edge
+    int32_t na = (int32_t)seed_of.size();
+    std::vector<int32_t> size(na, 0);
+    for (int32_t i = 0; i < N; ++i) size[agg[i]]++;
+    std::vector<int32_t> remap(na);
+    for (int32_t a = 0; a < na; ++a) remap[a] = a;
+    for (int32_t a = 0; a < na; ++a) {
+        if (size[a] != 1) continue;
+        int32_t s = seed_of[a];
+        double best = -1; int32_t to = -1;
+        for (int32_t k = rp[s]; k < rp[s + 1]; ++k) {
+            int32_t n = other(adj[k], s);
+            int32_t an = remap[agg[n]];
+            if (an == a) continue;
+            double w = wnorm(adj[k]);
+            if (w > best) { best = w; to = an; }
+        }
+        if (to >= 0) { remap[a] = to; size[to] += 1; size[a] = 0; }
+    }
+    for (int32_t i = 0; i < N; ++i) agg[i] = remap[agg[i]];
+    // number boundary aggregates first (those holding a fine boundary node)
+    std::vector<char> live(na, 0), bnd(na, 0);
+    for (int32_t i = 0; i < N; ++i) { live[agg[i]] = 1; if (i < F.Nb) bnd[agg[i]] = 1; }
+    std::vector<int32_t> newid(na, -1);
+    int32_t nc = 0;
+    for (int32_t a = 0; a < na; ++a) if (live[a] && bnd[a]) newid[a] = nc++;
+    int32_t ncb = nc;
+    for (int32_t a = 0; a < na; ++a) if (live[a] && !bnd[a]) newid[a] = nc++;
+
+    C = LevelData();
+    C.N = nc; C.Nb = ncb;
+    C.parent.resize(N);
+    for (int32_t i = 0; i < N; ++i) C.parent[i] = newid[agg[i]] + 1;
+    C.vol.assign(nc, 0.0);
+    for (int32_t i = 0; i < N; ++i) C.vol[C.parent[i] - 1] += F.vol[i];
+    C.rweight.resize(N);
+    for (int32_t i = 0; i < N; ++i) C.rweight[i] = F.vol[i] / C.vol[C.parent[i] - 1];
+    C.seed.assign(nc, 0); C.wdist.assign(nc, 0.0); C.wnode.assign(nc, 0);
+    for (int32_t a = 0; a < na; ++a) {
+        if (!live[a] || seed_of[a] < 0) continue;
+        int32_t c = newid[a], s = seed_of[a];
+        int32_t lvl1 = F.seed.empty() ? s + 1 : F.seed[s];
+        C.seed[c] = lvl1; C.wdist[c] = F.wdist[s]; C.wnode[c] = F.wnode[s];
+    }
+    // a merged single-node aggregate has no own coarse node: nothing to fix
+    // coarse edges (createSides)
+    PairMap smap((size_t)E / 4 + 16);
+    std::vector<int32_t> s1, s2; std::vector<V3> sc; std::vector<double> sl;
+    for (int32_t e = 0; e < E; ++e) {
+        int32_t c1 = C.parent[F.side[e] - 1], c2 = C.parent[F.side[(size_t)E + e] - 1];
+        if (c1 == c2) continue;
+        V3 w = {F.sw[e], F.sw[(size_t)E + e], F.sw[2 * (size_t)E + e]};
+        int32_t i1 = std::min(c1, c2), i2 = c1 + c2 - i1;
+        if (i1 != c1) w = scl(-1.0, w);
+        int64_t slot = smap.find_or_insert(pkey(i1, i2), (int64_t)s1.size());
+        if (slot < 0) { s1.push_back(i1); s2.push_back(i2); sc.push_back(w); sl.push_back(F.slen[e]); }
+        else sc[slot] = sc[slot] + w;
+    }
+    C.E = (int32_t)s1.size();
+    C.side.resize(2 * (size_t)C.E); C.sw.resize(3 * (size_t)C.E); C.slen = sl;
+    for (int32_t e = 0; e < C.E; ++e) {
+        C.side[e] = s1[e]; C.side[(size_t)C.E + e] = s2[e];
+        C.sw[e] = sc[e].x; C.sw[(size_t)C.E + e] = sc[e].y; C.sw[2 * (size_t)C.E + e] = sc[e].z;
+    }
+    // coarse boundary edges (agglomerateBoundary): self-edges are kept
+    PairMap bmap((size_t)F.B + 16);
+    std::vector<int32_t> b1, b2, bi; std::vector<V3> bc;
+    for (int32_t b = 0; b < F.B; ++b) {
+        int32_t c1 = C.parent[F.bside[b] - 1], c2 = C.parent[F.bside[(size_t)F.B + b] - 1];
+        int32_t i1 = std::min(c1, c2), i2 = std::max(c1, c2);
+        V3 w = {F.bw[b], F.bw[(size_t)F.B + b], F.bw[2 * (size_t)F.B + b]};
+        int64_t slot = bmap.find_or_insert(pkey(i1, i2), (int64_t)b1.size());
+        if (slot < 0) { b1.push_back(i1); b2.push_back(i2); bi.push_back(F.bside[2 * (size_t)F.B + b]); bc.push_back(w); }
+        else bc[slot] = bc[slot] + w;
+    }
+    C.B = (int32_t)b1.size();
+    C.bside.resize(3 * (size_t)C.B); C.bw.resize(3 * (size_t)C.B);
+    for (int32_t b = 0; b < C.B; ++b) {
+        C.bside[b] = b1[b]; C.bside[(size_t)C.B + b] = b2[b]; C.bside[2 * (size_t)C.B + b] = bi[b];
+        C.bw[b] = bc[b].x; C.bw[(size_t)C.B + b] = bc[b].y; C.bw[2 * (size_t)C.B + b] = bc[b].z;
+    }
+    C.bnd_indicator.assign(ncb, 0);
+    for (int32_t i = 0; i < F.Nb; ++i) {
+        int32_t c = C.parent[i] - 1;
+        C.bnd_indicator[c] = merge_indicator(C.bnd_indicator[c], F.bnd_indicator[i]);
+    }
+    build_register(C);
+}
+
+void build_levels(fp_mesh &M, int nlevels) {
+    for (int l = 1; l < nlevels; ++l) {
+        LevelData C;
+        SectionTimer tm("agglomeration");
+        agglomerate(M.lv.back(), C);
+        if (C.N >= M.lv.back().N || C.N < 2) break;
+        M.lv.push_back(std::move(C));
+    }
+}
+
+template <class F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const fio::io_error &e) {
+        g_err = e.what();
+        return FLITE_EIO;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return FLITE_EINVAL;
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int fp_from_tets(int32_t nnodes, const double *xyz, int32_t ntet, const int32_t *tets,
+                 int32_t ntri, const int32_t *tris, const int32_t *tri_ind, int nlevels,
+                 fp_mesh **out) {
+    return guarded([&] {
+        if (!out || nnodes <= 0 || ntet <= 0 || ntri <= 0 || nlevels < 1) return FLITE_EINVAL;
+        auto M = std::make_unique<fp_mesh>();
+        std::vector<double> x(xyz, xyz + 3 * (size_t)nnodes);
+        std::vector<int32_t> t(tets, tets + 4 * (size_t)ntet), f(tris, tris + 3 * (size_t)ntri),
+            fi(tri_ind, tri_ind + ntri);
+        for (auto v : t) if (v < 1 || v > nnodes) throw std::runtime_error("tet index out of range");
+        for (auto v : f) if (v < 1 || v > nnodes) throw std::runtime_error("face index out of range");
+        for (auto v : fi) if (v < 1 || v > 9) throw std::runtime_error("boundary indicator out of range");
+        build_fine(*M, nnodes, x, std::move(t), std::move(f), fi);
+        build_levels(*M, nlevels);
+        *out = M.release();
+        return FLITE_OK;
+    });
+}
+
+int fp_bump_channel(int nx, int ny, int nz, double bump_h, int nlevels, fp_mesh **out) {
+    return guarded([&] {
+        if (nx < 1 || ny < 1 || nz < 1) return FLITE_EINVAL;
+        const int32_t NX = nx + 1, NY = ny + 1, NZ = nz + 1;
+        const int64_t N = (int64_t)NX * NY * NZ;
+        if (N > 2000000000LL) return FLITE_EINVAL;
+        auto id = [&](int i, int j, int k) { return (int32_t)(i + NX * (j + (int64_t)NY * k)) + 1; };
+        std::vector<double> xyz(3 * (size_t)N);
+        const double PI = 4.0 * std::atan(1.0);
+        for (int k = 0; k < NZ; ++k)
+            for (int j = 0; j < NY; ++j)
+                for (int i = 0; i < NX; ++i) {
+                    double x = 3.0 * i / nx, y = (double)j / ny, s = (double)k / nz;
+                    double hb = 0.0;
+                    if (x >= 1.0 && x <= 2.0) { double sn = std::sin(PI * (x - 1.0)); hb = bump_h * sn * sn; }
+                    double z = hb * (1.0 - s) + s;
+                    size_t n = (size_t)id(i, j, k) - 1;
+                    xyz[n] = x; xyz[(size_t)N + n] = y; xyz[2 * (size_t)N + n] = z;
+                }
+        // Kuhn split: 6 tets per hex along the main diagonal
+        const int64_t NT = 6LL * nx * ny * nz;
+        std::vector<int32_t> tets(4 * (size_t)NT);
+        static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+        size_t t = 0;
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                    for (int p = 0; p < 6; ++p) {
+                        int c[3] = {i, j, k};
+                        int32_t v[4];
+                        v[0] = id(c[0], c[1], c[2]);
+                        for (int s = 0; s < 3; ++s) { c[perm[p][s]] += 1; v[s + 1] = id(c[0], c[1], c[2]); }
+                        for (int q = 0; q < 4; ++q) tets[(size_t)q * NT + t] = v[q];
+                        ++t;
+                    }
+        // boundary triangles on the six faces, split along the diagonal of
+        // the Kuhn tets that touch them
+        std::vector<int32_t> tri, ind;
+        auto quad = [&](int a, int lo, int i, int j, int k, int indicator) {
+            // face normal to axis a at the low (lo=1) or high side of hex (i,j,k)
+            int b = (a + 1) % 3, c = (a + 2) % 3;
+            int base[3] = {i, j, k};
+            if (!lo) base[a] += 1;
+            int p0[3] = {base[0], base[1], base[2]};
+            int pb[3] = {base[0], base[1], base[2]}; pb[b] += 1;
+            int pc[3] = {base[0], base[1], base[2]}; pc[c] += 1;
+            int pbc[3] = {base[0], base[1], base[2]}; pbc[b] += 1; pbc[c] += 1;
+            int32_t v0 = id(p0[0], p0[1], p0[2]), vb = id(pb[0], pb[1], pb[2]);
+            int32_t vc = id(pc[0], pc[1], pc[2]), vbc = id(pbc[0], pbc[1], pbc[2]);
+            tri.push_back(v0); tri.push_back(vb); tri.push_back(vbc); ind.push_back(indicator);
+            tri.push_back(v0); tri.push_back(vc); tri.push_back(vbc); ind.push_back(indicator);
+        };
+        for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) {
+            quad(0, 1, 0, j, k, 3); quad(0, 0, nx - 1, j, k, 3);
+        }
+        for (int k = 0; k < nz; ++k) for (int i = 0; i < nx; ++i) {
+            quad(1, 1, i, 0, k, 2); quad(1, 0, i, ny - 1, k, 2);
+        }
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+            quad(2, 1, i, j, 0, 1); quad(2, 0, i, j, nz - 1, 2);
+        }
+        const size_t NF = ind.size();
+        std::vector<int32_t> tris(3 * NF);
+        for (size_t f = 0; f < NF; ++f)
+            for (int q = 0; q < 3; ++q) tris[q * NF + f] = tri[3 * f + q];
+        auto M = std::make_unique<fp_mesh>();
+        build_fine(*M, (int32_t)N, xyz, std::move(tets), std::move(tris), ind);
+        build_levels(*M, nlevels);
+        *out = M.release();
+        return FLITE_OK;
+    });
+}
+
+int fp_free(fp_mesh *m) { delete m; return FLITE_OK; }
+
+int fp_num_levels(const fp_mesh *m) { return m ? (int)m->lv.size() : 0; }
+
+int fp_level_desc(const fp_mesh *m, int level, flite_level_desc *o) {
+    if (!m || !o || level < 1 || level > (int)m->lv.size()) return FLITE_EINVAL;
+    const LevelData &L = m->lv[level - 1];
+    std::memset(o, 0, sizeof *o);
+    o->n_nodes = L.N; o->n_sides = L.E; o->n_bsides = L.B; o->n_bnodes = L.Nb;
+    o->n_normals = (int32_t)L.node_ind.size();
+    o->side_idx = L.side.data(); o->side_w = L.sw.data(); o->side_len = L.slen.data();
+    o->bnd_idx = L.bside.data(); o->bnd_w = L.bw.data();
+    o->node_reg = L.reg; o->node_ind = L.node_ind.data();
+    o->volume = L.vol.data(); o->wall_dist = L.wdist.data();
+    o->coords = L.xyz.empty() ? nullptr : L.xyz.data();
+    o->coord_move = nullptr;
+    o->parent = L.parent.empty() ? nullptr : L.parent.data();
+    o->rweight = L.rweight.empty() ? nullptr : L.rweight.data();
+    return FLITE_OK;
+}
+
+int fp_node_perm(const fp_mesh *m, int32_t *perm) {
+    if (!m || !perm || m->perm.empty()) return FLITE_EINVAL;
+    std::memcpy(perm, m->perm.data(), m->perm.size() * 4);
+    return FLITE_OK;
+}
+
+int fp_check(const fp_mesh *m, int level, double *closure, double *volume) {
+    if (!m || level < 1 || level > (int)m->lv.size()) return FLITE_EINVAL;
+    const LevelData &L = m->lv[level - 1];
+    // closure of def_par:14430-14568: sum_j +-w + 2 sum_b w_b per node
+    std::vector<double> chk(3 * (size_t)L.N, 0.0);
+    double wmax = 0;
+    for (int32_t e = 0; e < L.E; ++e) {
+        int32_t a = L.side[e] - 1, b = L.side[(size_t)L.E + e] - 1;
+        for (int k = 0; k < 3; ++k) {
+            double w = L.sw[(size_t)k * L.E + e];
+            chk[3 * (size_t)a + k] += w; chk[3 * (size_t)b + k] -= w;
+            wmax = std::max(wmax, std::fabs(w));
+        }
+    }
+    for (int32_t e = 0; e < L.B; ++e) {
+        int32_t a = L.bside[e] - 1, b = L.bside[(size_t)L.B + e] - 1;
+        for (int k = 0; k < 3; ++k) {
+            double w = L.bw[(size_t)k * L.B + e];
+            chk[3 * (size_t)a + k] += 2 * w; chk[3 * (size_t)b + k] += 2 * w;
+        }
+    }
+    double mx = 0;
+    for (double v : chk) mx = std::max(mx, std::fabs(v));
+    if (closure) *closure = wmax > 0 ? mx / wmax : mx;
+    double vs = 0;
+    for (double v : L.vol) vs += v;
+    if (volume) *volume = vs;
+    return FLITE_OK;
+}
+
+// ---- .sol: the record sequence read by readComputationData (mg_par:
+// 1210-1266) and readGridComputationData (def_par:13837-14074) ------------
+int fp_write_sol(const fp_mesh *m, const char *path) {
+    if (!m || !path) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Writer w(path);
+        w.i4((int32_t)m->lv.size()).end();
+        w.i4(1).i4(1).end();  // domain, numberOfGridDomains
+        for (size_t l = 0; l < m->lv.size(); ++l) {
+            const LevelData &L = m->lv[l];
+            const bool fine = l == 0;
+            // readBoundarySolverData (def_par:803-864)
+            w.i4(L.B).end();
+            for (int32_t b = 0; b < L.B; ++b) {
+                w.i4(L.bside[b]).i4(L.bside[(size_t)L.B + b]).i4(L.bside[2 * (size_t)L.B + b]);
+                w.r8(L.bw[b]).r8(L.bw[(size_t)L.B + b]).r8(L.bw[2 * (size_t)L.B + b]);
+                w.r8(0).r8(0).r8(0).r8(0).end();  // GCL(2), GCLprev(2): static mesh
+            }
+            const int32_t nn = (int32_t)L.node_ind.size();
+            w.i4(L.Nb).i4(nn).end();
+            for (int j = 0; j < 21; ++j) w.i4(L.reg[j]).end();
+            for (int32_t i = 0; i < nn; ++i)
+                w.i4(L.node_ind[i]).r8(L.bnormal[i]).r8(L.bnormal[(size_t)nn + i])
+                    .r8(L.bnormal[2 * (size_t)nn + i]).end();
+            w.i4(0).end();  // engine inlet sides
+            // sides
+            w.i4(L.E).end();
+            for (int32_t e = 0; e < L.E; ++e) {
+                w.i4(L.side[e]).i4(L.side[(size_t)L.E + e]);
+                w.r8(L.sw[e]).r8(L.sw[(size_t)L.E + e]).r8(L.sw[2 * (size_t)L.E + e]);
+                w.r8(0).r8(0).r8(L.slen[e]).end();
+            }
+            // nodes
+            w.i4(L.N).end();
+            if (fine) {
+                for (int32_t i = 0; i < L.N; ++i) {
+                    double x = L.xyz[i], y = L.xyz[(size_t)L.N + i], z = L.xyz[2 * (size_t)L.N + i];
+                    w.i4(i + 1).r8(L.vol[i]).r8(L.vol[i]).r8(L.vol[i]).r8(L.wdist[i]).i4(L.wnode[i]);
+                    w.r8(x).r8(y).r8(z).r8(x).r8(y).r8(z).r8(x).r8(y).r8(z).end();
+                }
+                w.i4(0).end();  // trip nodes
+                w.i4(0).end();  // trip field nodes
+            } else {
+                for (int32_t i = 0; i < L.N; ++i)
+                    w.i4(i + 1).r8(L.vol[i]).r8(L.wdist[i]).i4(L.wnode[i]).i4(L.seed[i]).end();
+            }
+            // parallel data, one process (def_par:667-683)
+            w.i4(0).i4(0).end();
+            w.i4(0).end();
+            w.i4(0).end();
+            if (!fine) {
+                const int32_t nf = (int32_t)L.parent.size();
+                // prolongation (def_par:455-482)
+                w.i4(nf).end();
+                w.i4(L.N).end();
+                for (int32_t i = 0; i < nf; ++i) w.i4(i + 1).i4(L.parent[i]).end();
+                w.i4(0).end();
+                // restriction (def_par:517-540)
+                w.i4(nf).end();
+                w.i4(L.N).end();
+                for (int32_t i = 0; i < nf; ++i) w.i4(i + 1).r8(L.rweight[i]).end();
+                w.i4(0).end();
+                // com-parallel (def_par:703-737)
+                w.i4(0).end();
+                w.i4(0).end();
+                w.i4(0).end();
+                w.i4(0).end();
+            }
+        }
+        w.close();
+        return FLITE_OK;
+    });
+}
+
+int fp_read_sol(const char *path, fp_mesh **out) {
+    if (!path || !out) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Reader r(path);
+        auto M = std::make_unique<fp_mesh>();
+        r.next(); int32_t ng = r.i4();
+        r.next(); int32_t dom = r.i4(), ndom = r.i4();
+        (void)dom;
+        if (ndom != 1) throw std::runtime_error("multi-domain .sol is not supported (one GPU, one domain)");
+        if (ng < 1 || ng > 32) throw fio::io_error("bad number of grids");
+        for (int32_t l = 0; l < ng; ++l) {
+            LevelData L;
+            const bool fine = l == 0;
+            r.next(); L.B = r.i4();
+            if (L.B < 0) throw fio::io_error("negative count");
+            L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B);
+            for (int32_t b = 0; b < L.B; ++b) {
+                r.next();
+                for (int k = 0; k < 3; ++k) L.bside[(size_t)k * L.B + b] = r.i4();
+                for (int k = 0; k < 3; ++k) L.bw[(size_t)k * L.B + b] = r.r8();
+            }
+            r.next(); L.Nb = r.i4(); int32_t nn = r.i4();
+            for (int j = 0; j < 21; ++j) { r.next(); L.reg[j] = r.i4(); }
+            L.node_ind.resize(nn); L.bnormal.assign(3 * (size_t)nn, 0.0);
+            for (int32_t i = 0; i < nn; ++i) {
+                r.next(); L.node_ind[i] = r.i4();
+                if (r.remaining() >= 24)
+                    for (int k = 0; k < 3; ++k) L.bnormal[(size_t)k * nn + i] = r.r8();
+            }
+            r.next(); int32_t neis = r.i4();
+            if (neis != 0) throw std::runtime_error("engine inlet sides are not supported");
+            r.next(); L.E = r.i4();
+            L.side.resize(2 * (size_t)L.E); L.sw.resize(3 * (size_t)L.E); L.slen.resize(L.E);
+            for (int32_t e = 0; e < L.E; ++e) {
+                r.next();
+                L.side[e] = r.i4(); L.side[(size_t)L.E + e] = r.i4();
+                for (int k = 0; k < 3; ++k) L.sw[(size_t)k * L.E + e] = r.r8();
+                double g = r.r8(), gp = r.r8();
+                if (g != 0.0 || gp != 0.0) throw std::runtime_error("moving-mesh GCL weights are not supported");
+                L.slen[e] = r.r8();
+            }
+            r.next(); L.N = r.i4();
+            L.vol.resize(L.N); L.wdist.resize(L.N); L.wnode.resize(L.N);
+            if (fine) {
+                L.xyz.resize(3 * (size_t)L.N);
+                for (int32_t i = 0; i < L.N; ++i) {
+                    r.next();
+                    int32_t id = r.i4();
+                    if (id < 1 || id > L.N) throw fio::io_error("node id out of range");
+                    --id;
+                    L.vol[id] = r.r8(); r.r8(); r.r8();
+                    L.wdist[id] = r.r8(); L.wnode[id] = r.i4();
+                    for (int k = 0; k < 3; ++k) L.xyz[(size_t)k * L.N + id] = r.r8();
+                }
+                r.next(); int32_t ntrip = r.i4();
+                for (int32_t i = 0; i < ntrip; ++i) r.next();
+                r.next(); int32_t ntf = r.i4();
+                for (int32_t i = 0; i < ntf; ++i) r.next();
+            } else {
+                L.seed.resize(L.N);
+                for (int32_t i = 0; i < L.N; ++i) {
+                    r.next();
+                    int32_t id = r.i4();
+                    if (id < 1 || id > L.N) throw fio::io_error("node id out of range");
+                    --id;
+                    L.vol[id] = r.r8(); L.wdist[id] = r.r8(); L.wnode[id] = r.i4();
+                    L.seed[i] = r.i4();
+                }
+            }
+            r.next(); r.i4(); r.i4();
+            r.next(); r.i4();
+            r.next(); r.i4();
+            if (!fine) {
+                const int32_t nfine = M->lv.back().N;
+                L.parent.assign(nfine, 0); L.rweight.assign(nfine, 0.0);
+                r.next(); int32_t nif = r.i4();
+                r.next(); r.i4();
+                for (int32_t i = 0; i < nif; ++i) {
+                    r.next(); int32_t f = r.i4(); int32_t p = r.i4();
+                    if (f < 1 || f > nfine || p < 1 || p > L.N) throw fio::io_error("bad prolongation record");
+                    L.parent[f - 1] = p;
+                }
+                r.next(); int32_t ncom = r.i4();
+                for (int32_t i = 0; i < ncom; ++i) r.next();
+                r.next(); nif = r.i4();
+                r.next(); r.i4();
+                for (int32_t i = 0; i < nif; ++i) {
+                    r.next(); int32_t f = r.i4(); double wv = r.r8();
+                    if (f < 1 || f > nfine) throw fio::io_error("bad restriction record");
+                    L.rweight[f - 1] = wv;
+                }
+                r.next(); ncom = r.i4();
+                for (int32_t i = 0; i < ncom; ++i) r.next();
+                for (int s = 0; s < 2; ++s) {
+                    r.next(); r.i4();  // numberOfComS/RNodes
+                    r.next(); int32_t cnt = r.i4();
+                    for (int32_t i = 0; i < cnt; ++i) r.next();
+                }
+            }
+            // indicators per boundary node from the register
+            L.bnd_indicator.assign(L.Nb, 0);
+            for (int k = 1; k <= 9; ++k) {
+                int32_t st = L.reg[(-20 + 2 * (k - 1)) + 20], en = L.reg[(-19 + 2 * (k - 1)) + 20];
+                for (int32_t ib = st; ib <= en; ++ib)
+                    if (ib >= 1 && ib <= nn) {
+                        int32_t n = L.node_ind[ib - 1];
+                        if (n >= 1 && n <= L.Nb) L.bnd_indicator[n - 1] = k;
+                    }
+            }
+            M->lv.push_back(std::move(L));
+        }
+        M->perm.resize(M->lv[0].N);
+        for (int32_t i = 0; i < M->lv[0].N; ++i) M->perm[i] = i + 1;
+        *out = M.release();
+        return FLITE_OK;
+    });
+}
+
+int fp_write_rst(const char *path, int32_t n, int nvar, const double *prim) {
+    if (!path || n <= 0 || nvar < 5 || !prim) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Writer w(path);
+        w.i4(n).end();
+        w.r8s(prim, (size_t)n * nvar).end();
+        w.close();
+        return FLITE_OK;
+    });
+}
+
+int fp_read_rst(const char *path, int32_t n, int nvar, double *prim) {
+    if (!path || n <= 0 || nvar < 5 || !prim) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Reader r(path);
+        r.next();
+        int32_t num = r.i4();
+        if (num != n) throw fio::io_error("Startup file is not compatible");  // def_par:3748
+        r.next();
+        if (r.remaining() < (size_t)n * nvar * 8) throw fio::io_error("restart record too short");
+        r.r8s(prim, (size_t)n * nvar);
+        return FLITE_OK;
+    });
+}
+
+int fp_write_res(const char *path, int32_t n, int nvar, const double *u) {
+    if (!path || n <= 0 || nvar < 5 || !u) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Writer w(path);
+        w.i4(n).end();
+        std::vector<double> col((size_t)n * nvar);
+        for (int32_t i = 0; i < n; ++i) col[i] = u[i];
+        for (int j = 1; j < nvar; ++j)
+            for (int32_t i = 0; i < n; ++i) col[(size_t)j * n + i] = u[(size_t)j * n + i] / u[i];
+        w.r8s(col.data(), col.size()).end();
+        w.close();
+        return FLITE_OK;
+    });
+}
+
+int fp_write_unk(const char *path, int32_t n, int nvar, const double *u) {
+    if (!path || n <= 0 || nvar < 1 || !u) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Writer w(path);
+        w.i4(n).end();
+        w.r8s(u, (size_t)n * nvar).end();
+        w.close();
+        return FLITE_OK;
+    });
+}
+
+int fp_read_unk(const char *path, int32_t n, int nvar, double *u) {
+    if (!path || n <= 0 || nvar < 1 || !u) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Reader r(path);
+        r.next();
+        if (r.i4() != n) throw fio::io_error("node count differs");
+        r.next();
+        if (r.remaining() < (size_t)n * nvar * 8) throw fio::io_error("unk record too short");
+        r.r8s(u, (size_t)n * nvar);
+        return FLITE_OK;
+    });
+}
+
+int fp_write_plotreg(const fp_mesh *m, const char *path) {
+    if (!m || !path) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Writer w(path);
+        const int32_t N = m->lv[0].N;
+        w.i4(N).i4(1).end();
+        w.i4(N).end();
+        for (int32_t i = 0; i < N; ++i) w.i4(i + 1).i4(m->perm[i]).end();
+        w.close();
+        return FLITE_OK;
+    });
+}
+
+int fp_write_plt(const fp_mesh *m, const char *path) {
+    if (!m || !path || m->tets.empty()) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Writer w(path);
+        const LevelData &L = m->lv[0];
+        const int32_t NT = (int32_t)(m->tets.size() / 4), NF = (int32_t)m->tri_ind.size();
+        w.i4(NT).i4(L.N).i4(NF).end();
+        w.i4s(m->tets.data(), m->tets.size()).end();
+        w.r8s(L.xyz.data(), L.xyz.size()).end();
+        std::vector<int32_t> f(5 * (size_t)NF);
+        for (int32_t i = 0; i < NF; ++i) {
+            for (int k = 0; k < 3; ++k) f[(size_t)k * NF + i] = m->tris[(size_t)k * NF + i];
+            f[3 * (size_t)NF + i] = 0;
+            f[4 * (size_t)NF + i] = m->tri_ind[i];
+        }
+        w.i4s(f.data(), f.size()).end();
+        w.close();
+        return FLITE_OK;
+    });
+}
+
+}  // extern "C"

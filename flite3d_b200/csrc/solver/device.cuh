@@ -1,0 +1,161 @@
+// Device-side views of one grid level and the per-edge / per-node physics
+// shared by the kernels.  Every function restates the reference expression
+// it cites in the same operation order (the FP64 kernels are compiled with
+// --fmad=false), so that the GPU result equals the CPU restatement bit for
+// bit.
+#pragma once
+#include <cstdint>
+
+namespace flite {
+
+// Node boundary classes, from the indicator ranges of nodeIndicatorRegister
+// (def_par:4033-4042): 1 wall, 2 symmetry, 3/4 far field, 9 inviscid wall.
+enum : unsigned char { BC_NONE = 0, BC_WALL = 1, BC_SYM = 2, BC_FAR3 = 3, BC_FAR4 = 4, BC_IWALL = 9 };
+
+struct Params {
+    double gamma, gm1, CFL, maxInc, minRho, Re, am, k2, k4, cgdf, pts, Tinf, mach;
+    double mgBCRelax, prolRelax, clip;
+    double inf[12];
+    double RK[3];
+    int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
+};
+
+// A level's mesh and state on the device.  Node-indexed arrays are SoA
+// ([component][node]), like the reference's column-major u(N,nvar).
+struct LevelView {
+    int N, E, B, Nb, grid;
+    const int2 *edge;            // [E] (i1, i2), 0-based
+    const double *wx, *wy, *wz;  // [E] edge coefficients
+    const double *slen;          // [E]
+    const int2 *bedge;           // [B]
+    const int *bind;             // [B] face indicator
+    const double *bwx, *bwy, *bwz;
+    // node -> incident edges in edge order: (signed edge, other node); a
+    // negative entry ~e marks the node as the second node of edge e
+    const int *inc_ptr;
+    const int2 *inc;
+    // node -> incident boundary edges in boundary-edge order: 2*b + side
+    const int *binc_ptr;
+    const int *binc;
+    const double *V, *conn, *nx, *ny, *nz, *wallArea;
+    const double *cx, *cy, *cz;      // level 1; zero on coarse levels
+    const double *cmx, *cmy, *cmz;   // coordinateMovement (level 1)
+    const unsigned char *bc;         // [N] boundary class
+    // coarse levels: fine -> coarse parent map and the inverse (children in
+    // increasing fine order)
+    const int *parent;               // [N_fine]
+    const double *rweight;           // [N_fine]
+    const int *child_ptr;            // [N+1]
+    const int *child;                // [N_fine]
+    // state
+    double *u, *uprev, *rhs, *src, *diss;  // [5][N]
+    double *p, *dt, *mu;                   // [N]
+    double *lap;                           // [5][N] undivided Laplacian
+    double *sens;                          // [N]  pressure sensor
+    double *hvis;                          // [N]  viscous time-step term
+    double *grad;                          // [15][N] (level 1, HLLC order 2)
+    double *bnd;                           // [10][N]
+    double *flux;                          // [E][5] edge flux buffer
+    double *bflux;                         // [B][10] boundary-edge contributions
+    int *cyc;                              // cycle number of this level
+};
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+
+// makePressureField (def_par:13624-13627)
+__device__ __forceinline__ double pressure(const Params &P, double r, double m1, double m2, double m3, double E) {
+    double pp = P.gm1 * (E - 0.5 * ((m1 * m1 + m2 * m2) + m3 * m3) / r);
+    return dmax(pp, 0.1);
+}
+
+// tangential projection used by every slip condition (def_par:4448-4451,
+// 4480-4484, 4494-4499 and the increment forms :5028-5031, 5061-5066)
+__device__ __forceinline__ void remove_normal(double *x, double n0, double n1, double n2, double scale) {
+    double nv = (x[1] * n0 + x[2] * n1) + x[3] * n2;
+    double s = scale * nv;
+    x[1] = x[1] - s * n0;
+    x[2] = x[2] - s * n1;
+    x[3] = x[3] - s * n2;
+}
+
+// setBCsOnIncrementField (def_par:4978-5140)
+__device__ __forceinline__ void bc_increment(const Params &P, unsigned char cls, double n0, double n1, double n2,
+                                             double *r) {
+    if (cls == BC_WALL) {
+        if (P.viscous) {
+            r[1] = 0.0; r[2] = 0.0; r[3] = 0.0;
+            if (!P.isentropic) r[4] = 0.0;
+        } else {
+            remove_normal(r, n0, n1, n2, 1.0);
+        }
+    } else if (cls == BC_IWALL || cls == BC_SYM) {
+        remove_normal(r, n0, n1, n2, 1.0);
+    }
+}
+
+// setBCsOnSolutionField for static walls (def_par:4364-4500)
+__device__ __forceinline__ void bc_solution(const Params &P, unsigned char cls, double n0, double n1, double n2,
+                                            double cm0, double cm1, double cm2, double relax, double *u) {
+    if (cls == BC_WALL) {
+        if (P.viscous) {
+            u[1] = u[0] * cm0 / P.pts;
+            u[2] = u[0] * cm1 / P.pts;
+            u[3] = u[0] * cm2 / P.pts;
+            if (!P.isentropic) u[4] = u[0] * P.Tinf / P.gamma;
+        } else {
+            remove_normal(u, n0, n1, n2, 1.0);
+        }
+    } else if (cls == BC_IWALL) {
+        remove_normal(u, n0, n1, n2, relax);
+        if (!P.isentropic) {
+            double ke = (u[1] * u[1] + u[2] * u[2]) + u[3] * u[3];
+            u[4] = u[0] * P.Tinf / P.gamma + 0.5 * ke / u[0];
+        }
+    } else if (cls == BC_SYM) {
+        remove_normal(u, n0, n1, n2, 1.0);
+    }
+}
+
+// setOuterBoundaryConditions (def_par:4018-4251)
+__device__ __forceinline__ void bc_outer(const Params &P, unsigned char cls, double n0, double n1, double n2,
+                                         double p, double *u) {
+    if (cls != BC_FAR3 && cls != BC_FAR4) return;
+    const double *inf = &P.inf[cls == BC_FAR3 ? 0 : 6];
+    double iR = inf[0], iU1 = inf[1], iU2 = inf[2], iU3 = inf[3], iE = inf[4], iP = inf[5];
+    double rho = u[0], U1 = u[1], U2 = u[2], U3 = u[3];
+    double nvel = (iU1 * n0 + iU2 * n1) + iU3 * n2;
+    if (nvel > 0.00) {
+        u[0] = iR; u[1] = iU1 * iR; u[2] = iU2 * iR; u[3] = iU3 * iR;
+        if (P.mach > 1.0) u[4] = iE * iR;
+        else u[4] = p / P.gm1 + 0.5 * ((iU1 * iU1 + iU2 * iU2) + iU3 * iU3) * iR;
+    } else {
+        if (P.mach < 1.0) u[4] = iP / P.gm1 + 0.5 * ((U1 * U1 + U2 * U2) + U3 * U3) / rho;
+    }
+}
+
+// relaxation parameter of the slip conditions (def_par:4389-4394)
+__device__ __forceinline__ double relax_param(const Params &P, int cycle) {
+    if (P.ncfl > 0) {
+        double r = (double)(cycle - 1) / (double)P.ncfl;
+        return dmin(r, 1.0);
+    }
+    return 1.0;
+}
+
+// density update with the increment clip (def_par:1343-1366)
+__device__ __forceinline__ void clipped_update(const Params &P, const double *up, const double *d, double *u) {
+    double inc = d[0];
+    if (fabs(inc / up[0]) < P.maxInc) {
+        u[0] = up[0] - inc;
+    } else {
+        double sign = inc / fabs(inc);
+        u[0] = up[0] - sign * P.maxInc * up[0];
+    }
+    u[1] = up[1] - d[1];
+    u[2] = up[2] - d[2];
+    u[3] = up[3] - d[3];
+    u[4] = up[4] - d[4];
+}
+
+}  // namespace flite

@@ -1,0 +1,816 @@
+// Host side of the C ABI (include/flite_gpu.h): context, device layout and
+// the orchestration of the reference's solver calls as kernel sequences.
+//
+// The call structure mirrors SolverSource/mgnsg3d_def_par.F90 and
+// mgnsg3d_mg_par.F90 routine for routine (cited at each function); only the
+// inner loops moved into the kernels of kernels.cu.  One oneCycle is a fixed
+// kernel sequence for given controls, so it is captured once into a CUDA
+// graph and replayed; the cycle number reaches the kernels through device
+// memory so the same graph serves every cycle.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "flite_gpu.h"
+#include "kernels.h"
+
+using namespace flite;
+
+namespace {
+
+struct cuda_error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            throw cuda_error(std::string(#call) + ": " + cudaGetErrorString(_e));             \
+    } while (0)
+
+constexpr int kBlock = 256;
+constexpr int kResidBlocks = 296;  // 2 x 148 SMs
+
+struct DevLevel {
+    int N = 0, E = 0, B = 0, Nb = 0;
+    LevelView v{};
+    std::vector<int> wall;  // level-1 wall nodes in register order (forces)
+    int *d_wall = nullptr;
+};
+
+}  // namespace
+
+struct flite_ctx {
+    flite_controls c{};
+    Params P{};
+    std::vector<DevLevel> lv;
+    std::vector<void *> allocs;
+    cudaStream_t s = nullptr;
+    int *d_cycle = nullptr;
+    int *d_cyc = nullptr;  // per-level cycle numbers
+    double *d_part = nullptr, *d_out = nullptr;
+    int *h_cycle = nullptr;  // pinned
+    cudaGraphExec_t graph = nullptr;
+    int64_t launches = 0;
+    bool counting = false;
+    std::string err;
+
+    template <class T>
+    T *alloc(size_t n) {
+        void *p = nullptr;
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        if (e != cudaSuccess) throw cuda_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(p);
+        return (T *)p;
+    }
+    template <class T>
+    T *upload(const std::vector<T> &h) {
+        T *d = alloc<T>(h.size());
+        if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return d;
+    }
+    ~flite_ctx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void *p : allocs) cudaFree(p);
+        if (h_cycle) cudaFreeHost(h_cycle);
+        if (s) cudaStreamDestroy(s);
+    }
+
+    static unsigned blocks(size_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+    void counted() {
+        if (counting) ++launches;
+    }
+
+    // ---- single-grid building blocks ------------------------------------
+    LevelView &V(int l) { return lv[l].v; }
+
+    void pressure(int l) {
+        counted();
+        k_pressure<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
+    }
+    void timesteps(int l) {
+        counted();
+        k_timestep<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
+    }
+    void zero_diss(int l) {
+        counted();
+        k_fill<<<blocks(5 * (size_t)V(l).N), kBlock, 0, s>>>(V(l).diss, 5 * (size_t)V(l).N, 0.0);
+    }
+    // makeArtificialDissipation2 (def_par:11484-11993), scalar form
+    void jst(int l) {
+        const LevelView &L = V(l);
+        if ((c.fluxType == 4 && L.grid == 1) ||
+            (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0)) {
+            zero_diss(l);
+            return;
+        }
+        counted();
+        k_jst_lap<<<blocks(L.N), kBlock, 0, s>>>(P, L);
+        counted();
+        k_jst_flux<<<blocks(L.N), kBlock, 0, s>>>(P, L);
+    }
+    void first_order_diss(int l) {
+        counted();
+        k_first_order_diss<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
+    }
+    // dissipation choice of singleIteration (def_par:1030-1036)
+    void dissipation(int l) {
+        if (c.dissipationScheme == 3) first_order_diss(l);
+        else jst(l);
+    }
+    // makeRHS up to the node gather (def_par:1587-1607 and the edge loops)
+    void rhs_terms(int l) {
+        const LevelView &L = V(l);
+        if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
+            counted();
+            k_gradient<<<blocks(L.N), kBlock, 0, s>>>(P, L);
+            if (c.Automaticlipping == 1) {
+                counted();
+                k_minmax<<<blocks(L.N), kBlock, 0, s>>>(P, L);
+            }
+        }
+        if (L.E > 0) {
+            counted();
+            k_edge_flux<<<blocks(L.E), kBlock, 0, s>>>(P, L);
+        }
+        if (L.B > 0) {
+            counted();
+            k_bnd_flux<<<blocks(L.B), kBlock, 0, s>>>(P, L);
+        }
+    }
+    void node_update(int l, int mode, int stage) {
+        counted();
+        k_node_update<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l), mode, stage);
+    }
+
+    // ---- singleIteration (def_par:1002-1181) -----------------------------
+    void singleIteration(int l, bool calcDiss) {
+        if (calcDiss) {
+            pressure(l);  // p = |p| is the identity after the 0.1 floor
+            timesteps(l);
+            dissipation(l);
+        }
+        for (int st = 1; st <= 3; ++st) {
+            pressure(l);
+            rhs_terms(l);
+            node_update(l, MODE_STAGE, st);
+        }
+    }
+    // ---- doTimeIterations (def_par:966-1000) -----------------------------
+    void doTimeIterations(int l, int nsteps, bool calcDiss) {
+        counted();
+        k_set_int<<<1, 1, 0, s>>>(V(l).cyc, d_cycle);
+        for (int i = 0; i < nsteps; ++i) {
+            counted();
+            k_copy<<<blocks(5 * (size_t)V(l).N), kBlock, 0, s>>>(V(l).u, V(l).uprev, 5 * (size_t)V(l).N);
+            singleIteration(l, calcDiss);
+        }
+    }
+    // ---- restrictGrid (def_par:12141-12430) ------------------------------
+    void restrictGrid(int fl) {
+        const int cl = fl + 1;
+        counted();
+        k_restrict_state<<<blocks(V(cl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
+        timesteps(cl);
+        if (c.coarseGridDissipationScheme == 2) jst(cl);
+        else if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
+        rhs_terms(cl);
+        node_update(cl, MODE_RCOARSE, 0);
+        pressure(fl);
+        jst(fl);  // the fine part always uses scheme 2 (def_par:12266-12270)
+        rhs_terms(fl);
+        node_update(fl, MODE_RFINE, 0);
+        counted();
+        k_restrict_incr<<<blocks(V(cl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
+    }
+    // ---- prolongateGrid (def_par:12432-12570) ----------------------------
+    void prolongateGrid(int cl) {
+        const int fl = cl - 1;
+        counted();
+        k_prolong_coarse<<<blocks(V(cl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
+        counted();
+        k_prolong_fine<<<blocks(V(fl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
+    }
+    void mapFineToCoarse(int fl) {
+        counted();
+        k_restrict_u<<<blocks(V(fl + 1).N), kBlock, 0, s>>>(V(fl + 1), V(fl));
+    }
+    // ---- oneCycle (mg_par:907-1196) --------------------------------------
+    void oneCycle() {
+        const int G = (int)lv.size();
+        const int nr = c.numberOfRelaxationSteps;
+        auto relax = [&](int j1, int steps, bool calc) { doTimeIterations(j1 - 1, steps, calc); };
+        const int sch = c.multigridScheme;
+        if (sch <= 0) {
+            for (int i = 1; i <= G - 1; ++i) {
+                counted();
+                k_copy<<<blocks(5 * (size_t)V(i - 1).N), kBlock, 0, s>>>(V(i - 1).u, V(i - 1).uprev,
+                                                                        5 * (size_t)V(i - 1).N);
+                mapFineToCoarse(i - 1);
+            }
+            counted();
+            k_fill<<<blocks(5 * (size_t)V(G - 1).N), kBlock, 0, s>>>(V(G - 1).src, 5 * (size_t)V(G - 1).N, 0.0);
+            relax(G, nr, true);
+            for (int i = G; i >= 2; --i) {
+                counted();
+                k_inject_u<<<blocks(V(i - 2).N), kBlock, 0, s>>>(V(i - 1), V(i - 2));
+            }
+        } else if (sch == 1) {
+            for (int i = 1; i <= G - 1; ++i) {
+                relax(i, nr, i == 1);
+                restrictGrid(i - 1);
+                mapFineToCoarse(i - 1);
+            }
+            relax(G, nr, G == 1);
+            for (int i = G; i >= 2; --i) {
+                prolongateGrid(i - 1);
+                relax(i - 1, nr, (i - 1) == 1);
+            }
+        } else if (sch == 2 || sch == 5) {
+            int nsw = G <= 2 ? 1 : 2 * G - 4;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, sch == 5 ? j : nr, j == fsl);
+                    restrictGrid(j - 1);
+                }
+                relax(G, sch == 5 ? G : nr, G == 1);
+                if (fsl == 1) fsl = G > 2 ? G - 1 : G;
+                else if (i <= nsw / 2) fsl = fsl - 1;
+                else fsl = fsl + 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prolongateGrid(j - 1);
+                    relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+            for (int j = G; j >= 2; --j) {
+                prolongateGrid(j - 1);
+                relax(j - 1, nr, (j - 1) == 1);
+            }
+        } else if (sch == 3 || sch == 7) {
+            int nsw = G == 1 ? 1 : G - 1;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, nr, j == fsl);
+                    restrictGrid(j - 1);
+                }
+                relax(G, nr, G == 1);
+                if (fsl == 1) fsl = G >= 2 ? G - 1 : G;
+                else fsl = fsl - 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prolongateGrid(j - 1);
+                    if (sch == 7) relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+        } else if (sch == 4) {
+            int nsw = G == 1 ? 1 : G - 1;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, nr, j == fsl);
+                    restrictGrid(j - 1);
+                }
+                relax(G, nr, G == 1);
+                fsl = fsl + 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prolongateGrid(j - 1);
+                    relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+            for (int j = G; j >= 2; --j) {
+                prolongateGrid(j - 1);
+                relax(j - 1, nr, (j - 1) == 1);
+            }
+        }
+    }
+
+    void set_cycle(int cyc) {
+        *h_cycle = cyc;
+        CK(cudaMemcpyAsync(d_cycle, h_cycle, sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+
+    void ensure_graph() {
+        if (graph) return;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        launches = 0;
+        counting = true;
+        try {
+            oneCycle();
+        } catch (...) {
+            counting = false;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        counting = false;
+        CK(cudaStreamEndCapture(s, &g));
+        cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+};
+
+namespace {
+
+int fail(flite_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+template <class F>
+int guarded(flite_ctx *ctx, F &&f) {
+    if (!ctx) return FLITE_EINVAL;
+    try {
+        return f();
+    } catch (const cuda_error &e) {
+        return fail(ctx, FLITE_ECUDA, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, FLITE_ENOMEM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(ctx, FLITE_EINVAL, e.what());
+    }
+}
+
+const char *unsupported_reason(const flite_controls &c) {
+    if (c.flowType != 0) return "flowType != 0 (unsteady) is not supported";
+    if (c.explicit_) return "explicit time stepping is not supported";
+    if (c.SAS || c.GUSTMODEL || c.movingwall || c.patchInitialization || c.nspan != 0)
+        return "SAS, gust, moving-wall, patch initialisation and spanwise loads are not supported";
+    if (c.residualSmoothingFactor > 0 || c.prolongationSmoothingFactor > 0)
+        return "residual and prolongation smoothing are not supported";
+    if (c.turbulenceModel != 0) return "turbulenceModel != 0 is not supported yet";
+    if (c.ReynoldsNumber > 0) return "viscous flow (ReynoldsNumber > 0) is not supported yet";
+    if (c.fluxType < 1 || c.fluxType > 4) return "fluxType must be 1..4";
+    if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1)
+        return "least-squares gradients are not supported (GradientMethod must be 1)";
+    if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1)
+        return "dissipation scheme 1 is not supported";
+    if (c.useMatrixDissipation) return "matrix dissipation is not supported";
+    if (c.prolongationMappingScheme != 1) return "prolongationMappingScheme must be 1";
+    if (c.precision != FLITE_FP64) return "only FLITE_FP64 is available in this build";
+    int s = c.multigridScheme;
+    if (!(s <= 0 || (s >= 1 && s <= 5) || s == 7)) return "multigridScheme not implemented";
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int flite_last_error(const flite_ctx *ctx, char *buf, size_t len) {
+    if (!ctx || !buf || !len) return FLITE_EINVAL;
+    std::snprintf(buf, len, "%s", ctx->err.c_str());
+    return FLITE_OK;
+}
+
+int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *levels, flite_ctx **out) {
+    if (!c || !levels || !out || nlevels < 1) return FLITE_EINVAL;
+    *out = nullptr;
+    if (unsupported_reason(*c)) return FLITE_EUNSUPPORTED;
+    auto ctx = std::make_unique<flite_ctx>();
+    int rc = guarded(ctx.get(), [&]() -> int {
+        flite_ctx &X = *ctx;
+        X.c = *c;
+        Params &P = X.P;
+        P.gamma = c->gamma; P.gm1 = c->gamma - 1.0; P.CFL = c->CFLNumber; P.maxInc = c->maxIncrementFactor;
+        P.minRho = c->minimumDensity; P.Re = c->ReynoldsNumber; P.am = c->ReynoldsNumber > 0 ? 1.0 / c->ReynoldsNumber : 0.0;
+        P.k2 = c->secondOrderDissipationFactor; P.k4 = c->fourthOrderDissipationFactor;
+        P.cgdf = c->coarseGridDissipationFactor; P.pts = c->physicalTimeStep; P.Tinf = c->inflowTemperature;
+        P.mach = c->MachNumber; P.mgBCRelax = c->multigridBCRelaxation; P.prolRelax = c->prolongationRelaxation;
+        P.clip = c->HLLCClipping;
+        for (int i = 0; i < 12; ++i) P.inf[i] = c->inflowField[i];
+        P.RK[0] = 0.6; P.RK[1] = 0.6; P.RK[2] = 1.0;  // def_par:14240-14244
+        P.fluxType = c->fluxType; P.hllcOrder = c->HLLCFluxOrder; P.autoClip = c->Automaticlipping;
+        P.nsig = c->ReynoldsNumber < 1 ? 4 : 2;       // def_par:1592-1596
+        P.isentropic = c->wallsAreIsentropic; P.viscous = c->ReynoldsNumber > 0.0;
+        P.boundaryTerm = c->boundaryTerm; P.useDissW = c->useDissipationWeighting; P.ncfl = c->numberOfCFLIncrements;
+
+        int G = nlevels;
+        if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);  // mg_par:1212-1214
+        CK(cudaStreamCreateWithFlags(&X.s, cudaStreamNonBlocking));
+        CK(cudaMallocHost(&X.h_cycle, sizeof(int)));
+        X.d_cycle = X.alloc<int>(1);
+        X.d_cyc = X.alloc<int>(G);
+        {
+            std::vector<int> cyc0(G, 0);
+            cyc0[0] = 1;  // setUpInitialField2 sets grid 1 (def_par:3992)
+            CK(cudaMemcpy(X.d_cyc, cyc0.data(), G * sizeof(int), cudaMemcpyHostToDevice));
+        }
+        X.d_part = X.alloc<double>(kResidBlocks * 15);
+        X.d_out = X.alloc<double>(32);
+        X.lv.resize(G);
+        for (int l = 0; l < G; ++l) {
+            const flite_level_desc &d = levels[l];
+            DevLevel &D = X.lv[l];
+            const int N = d.n_nodes, E = d.n_sides, B = d.n_bsides, Nb = d.n_bnodes;
+            if (N <= 0 || E < 0 || B < 0 || Nb < 0 || Nb > N || d.n_normals < 0)
+                throw std::runtime_error("bad level sizes");
+            if (!d.side_idx || !d.side_w || !d.bnd_idx || !d.bnd_w || !d.node_reg || !d.volume ||
+                (d.n_normals > 0 && !d.node_ind))
+                throw std::runtime_error("missing level array");
+            D.N = N; D.E = E; D.B = B; D.Nb = Nb;
+            LevelView &L = D.v;
+            L.N = N; L.E = E; L.B = B; L.Nb = Nb; L.grid = l + 1;
+            // edges
+            std::vector<int2> edge(E);
+            std::vector<double> wx(E), wy(E), wz(E), slen(E, 0.0);
+            for (int e = 0; e < E; ++e) {
+                int a = d.side_idx[e] - 1, b = d.side_idx[(size_t)E + e] - 1;
+                if (a < 0 || a >= N || b < 0 || b >= N || a == b) throw std::runtime_error("edge index out of range");
+                edge[e] = make_int2(a, b);
+                wx[e] = d.side_w[e]; wy[e] = d.side_w[(size_t)E + e]; wz[e] = d.side_w[2 * (size_t)E + e];
+                if (d.side_len) slen[e] = d.side_len[e];
+            }
+            std::vector<int2> bedge(B);
+            std::vector<int> bind(B);
+            std::vector<double> bwx(B), bwy(B), bwz(B);
+            for (int b = 0; b < B; ++b) {
+                int a = d.bnd_idx[b] - 1, q = d.bnd_idx[(size_t)B + b] - 1;
+                if (a < 0 || a >= N || q < 0 || q >= N) throw std::runtime_error("boundary edge index out of range");
+                bedge[b] = make_int2(a, q);
+                bind[b] = d.bnd_idx[2 * (size_t)B + b];
+                if (bind[b] >= 5 && bind[b] <= 8) return FLITE_EUNSUPPORTED;  // engine faces
+                bwx[b] = d.bnd_w[b]; bwy[b] = d.bnd_w[(size_t)B + b]; bwz[b] = d.bnd_w[2 * (size_t)B + b];
+            }
+            // node -> incident edges in edge order
+            std::vector<int> ip(N + 1, 0);
+            for (int e = 0; e < E; ++e) { ip[edge[e].x + 1]++; ip[edge[e].y + 1]++; }
+            for (int i = 0; i < N; ++i) ip[i + 1] += ip[i];
+            std::vector<int2> inc(2 * (size_t)E);
+            {
+                std::vector<int> fill(ip.begin(), ip.end() - 1);
+                for (int e = 0; e < E; ++e) {
+                    inc[fill[edge[e].x]++] = make_int2(e, edge[e].y);
+                    inc[fill[edge[e].y]++] = make_int2(~e, edge[e].x);
+                }
+            }
+            std::vector<int> bp(N + 1, 0);
+            for (int b = 0; b < B; ++b) { bp[bedge[b].x + 1]++; bp[bedge[b].y + 1]++; }
+            for (int i = 0; i < N; ++i) bp[i + 1] += bp[i];
+            std::vector<int> binc(2 * (size_t)B);
+            {
+                std::vector<int> fill(bp.begin(), bp.end() - 1);
+                for (int b = 0; b < B; ++b) {
+                    binc[fill[bedge[b].x]++] = 2 * b;
+                    binc[fill[bedge[b].y]++] = 2 * b + 1;
+                }
+            }
+            // geometry of readGridComputationData: normals (def_par:15394-
+            // 15521), wall area (:15523-15634, level 1), connectivity
+            std::vector<double> nx(N, 0.0), ny(N, 0.0), nz(N, 0.0), wa(N, 0.0), conn(N, 0.0);
+            for (int b = 0; b < B; ++b) {
+                int a = bedge[b].x, q = bedge[b].y;
+                nx[a] = nx[a] - bwx[b]; ny[a] = ny[a] - bwy[b]; nz[a] = nz[a] - bwz[b];
+                nx[q] = nx[q] - bwx[b]; ny[q] = ny[q] - bwy[b]; nz[q] = nz[q] - bwz[b];
+            }
+            for (int i = 0; i < Nb; ++i) {
+                double nrm = std::sqrt((nx[i] * nx[i] + ny[i] * ny[i]) + nz[i] * nz[i]);
+                if (nrm > 1.0e-10) { nx[i] = nx[i] / nrm; ny[i] = ny[i] / nrm; nz[i] = nz[i] / nrm; }
+                else { nx[i] = 0.0; ny[i] = 0.0; nz[i] = 0.0; }
+            }
+            if (l == 0)
+                for (int b = 0; b < B; ++b) {
+                    double ai = std::sqrt((bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b]);
+                    wa[bedge[b].x] = wa[bedge[b].x] + 4.0 * ai;
+                    wa[bedge[b].y] = wa[bedge[b].y] + 4.0 * ai;
+                }
+            for (int e = 0; e < E; ++e) { conn[edge[e].x] += 1.0; conn[edge[e].y] += 1.0; }
+            // boundary classes from the indicator register
+            std::vector<unsigned char> bc(N, BC_NONE);
+            auto R = [&](int i) { return d.node_reg[i + 20]; };
+            const int cls_of[10] = {0, BC_WALL, BC_SYM, BC_FAR3, BC_FAR4, 5, 6, 7, 8, BC_IWALL};
+            for (int k = 1; k <= 9; ++k) {
+                int st = R(-20 + 2 * (k - 1)), en = R(-19 + 2 * (k - 1));
+                for (int ib = st; ib <= en; ++ib) {
+                    if (ib < 1 || ib > d.n_normals) throw std::runtime_error("indicator register out of range");
+                    int n = d.node_ind[ib - 1] - 1;
+                    if (n < 0 || n >= N) throw std::runtime_error("indicator node out of range");
+                    if (k >= 5 && k <= 8) return FLITE_EUNSUPPORTED;  // engine nodes
+                    bc[n] = (unsigned char)cls_of[k];
+                    if (l == 0 && k == 1) D.wall.push_back(n);
+                }
+            }
+            std::vector<double> coords(3 * (size_t)N, 0.0), cm(3 * (size_t)N, 0.0);
+            if (l == 0 && d.coords) std::memcpy(coords.data(), d.coords, 3 * (size_t)N * sizeof(double));
+            if (l == 0 && d.coord_move) std::memcpy(cm.data(), d.coord_move, 3 * (size_t)N * sizeof(double));
+            // upload
+            L.edge = X.upload(edge);
+            L.wx = X.upload(wx); L.wy = X.upload(wy); L.wz = X.upload(wz); L.slen = X.upload(slen);
+            L.bedge = X.upload(bedge); L.bind = X.upload(bind);
+            L.bwx = X.upload(bwx); L.bwy = X.upload(bwy); L.bwz = X.upload(bwz);
+            L.inc_ptr = X.upload(ip); L.inc = X.upload(inc);
+            L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
+            L.V = X.upload(std::vector<double>(d.volume, d.volume + N));
+            L.conn = X.upload(conn);
+            L.nx = X.upload(nx); L.ny = X.upload(ny); L.nz = X.upload(nz); L.wallArea = X.upload(wa);
+            double *dc = X.upload(coords);
+            L.cx = dc; L.cy = dc + N; L.cz = dc + 2 * (size_t)N;
+            double *dm = X.upload(cm);
+            L.cmx = dm; L.cmy = dm + N; L.cmz = dm + 2 * (size_t)N;
+            L.bc = X.upload(bc);
+            if (l > 0) {
+                const int nf = X.lv[l - 1].N;
+                if (!d.parent || !d.rweight) throw std::runtime_error("coarse level without transfer operators");
+                std::vector<int> par(nf);
+                std::vector<double> rw(d.rweight, d.rweight + nf);
+                std::vector<int> cp(N + 1, 0);
+                for (int f = 0; f < nf; ++f) {
+                    par[f] = d.parent[f] - 1;
+                    if (par[f] >= N) throw std::runtime_error("parent out of range");
+                    if (par[f] >= 0) cp[par[f] + 1]++;
+                }
+                for (int i = 0; i < N; ++i) cp[i + 1] += cp[i];
+                std::vector<int> ch(std::max(cp[N], 1));
+                std::vector<int> fill(cp.begin(), cp.end() - 1);
+                for (int f = 0; f < nf; ++f)
+                    if (par[f] >= 0) ch[fill[par[f]]++] = f;
+                L.parent = X.upload(par); L.rweight = X.upload(rw);
+                L.child_ptr = X.upload(cp); L.child = X.upload(ch);
+            }
+            // state
+            L.u = X.alloc<double>(5 * (size_t)N); L.uprev = X.alloc<double>(5 * (size_t)N);
+            L.rhs = X.alloc<double>(5 * (size_t)N); L.src = X.alloc<double>(5 * (size_t)N);
+            L.diss = X.alloc<double>(5 * (size_t)N); L.lap = X.alloc<double>(5 * (size_t)N);
+            L.p = X.alloc<double>(N); L.dt = X.alloc<double>(N); L.mu = X.alloc<double>(N);
+            L.sens = X.alloc<double>(N); L.hvis = X.alloc<double>(N);
+            for (double *a : {L.u, L.uprev, L.rhs, L.src, L.diss, L.lap})
+                CK(cudaMemset(a, 0, 5 * (size_t)N * sizeof(double)));
+            for (double *a : {L.p, L.dt, L.mu, L.sens, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
+            const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
+            L.grad = hllc2 ? X.alloc<double>(15 * (size_t)N) : nullptr;
+            L.bnd = hllc2 ? X.alloc<double>(10 * (size_t)N) : nullptr;
+            L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
+            L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
+            L.cyc = X.d_cyc + l;
+            if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
+        }
+        CK(cudaDeviceSynchronize());
+        return FLITE_OK;
+    });
+    if (rc != FLITE_OK) return rc;
+    *out = ctx.release();
+    return FLITE_OK;
+}
+
+int flite_destroy(flite_ctx *ctx) {
+    if (!ctx) return FLITE_EINVAL;
+    cudaStreamSynchronize(ctx->s);
+    delete ctx;
+    return FLITE_OK;
+}
+
+static bool bad_level(flite_ctx *ctx, int level) { return !ctx || level < 1 || level > (int)ctx->lv.size(); }
+
+int flite_set_state(flite_ctx *ctx, int level, const double *u) {
+    if (bad_level(ctx, level) || !u) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        LevelView &L = ctx->V(level - 1);
+        CK(cudaMemcpyAsync(L.u, u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_get_state(flite_ctx *ctx, int level, double *u) {
+    if (bad_level(ctx, level) || !u) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        LevelView &L = ctx->V(level - 1);
+        CK(cudaMemcpyAsync(u, L.u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_get_pressure(flite_ctx *ctx, int level, double *p) {
+    if (bad_level(ctx, level) || !p) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        LevelView &L = ctx->V(level - 1);
+        CK(cudaMemcpyAsync(p, L.p, (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_init_freestream(flite_ctx *ctx) {
+    if (!ctx) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        LevelView &L = ctx->V(0);
+        for (int k = 0; k < 5; ++k)
+            k_fill<<<flite_ctx::blocks(L.N), kBlock, 0, ctx->s>>>(L.u + (size_t)k * L.N, L.N, ctx->c.inflowField[k]);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_start(flite_ctx *ctx) {
+    if (!ctx) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        // makePressureField + setBCsOnSolutionField on level 1 with
+        // cycleNumber = 1 (def_par:3990-3994)
+        X.pressure(0);
+        X.set_cycle(1);
+        k_set_int<<<1, 1, 0, X.s>>>(X.V(0).cyc, X.d_cycle);
+        k_bc_solution<<<flite_ctx::blocks(X.V(0).N), kBlock, 0, X.s>>>(X.P, X.V(0));
+        // laminar viscosity and the restriction of u to every coarse level
+        // (mg_par:586-602)
+        const double mu = X.c.ReynoldsNumber > 0.0 ? 1. / X.c.ReynoldsNumber : 0.0;
+        for (size_t l = 0; l < X.lv.size(); ++l) {
+            k_fill<<<flite_ctx::blocks(X.V(l).N), kBlock, 0, X.s>>>(X.V(l).mu, X.V(l).N, mu);
+            if (l > 0) X.mapFineToCoarse((int)l - 1);
+        }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(X.s));
+        return FLITE_OK;
+    });
+}
+
+int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps, int calc_diss, int calc_turb, int cycle_no) {
+    (void)calc_turb;
+    if (bad_level(ctx, level) || nsteps < 0) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->set_cycle(cycle_no);
+        ctx->doTimeIterations(level - 1, nsteps, calc_diss != 0);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_restrict(flite_ctx *ctx, int fine_level, int calc_turb) {
+    (void)calc_turb;
+    if (bad_level(ctx, fine_level) || bad_level(ctx, fine_level + 1)) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->restrictGrid(fine_level - 1);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_prolong(flite_ctx *ctx, int coarse_level) {
+    if (bad_level(ctx, coarse_level) || coarse_level < 2) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->prolongateGrid(coarse_level - 1);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_map_fine_to_coarse(flite_ctx *ctx, int fine_level) {
+    if (bad_level(ctx, fine_level) || bad_level(ctx, fine_level + 1)) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->mapFineToCoarse(fine_level - 1);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_cycle(flite_ctx *ctx, int cycle_no) {
+    if (!ctx) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->ensure_graph();
+        ctx->set_cycle(cycle_no);
+        CK(cudaGraphLaunch(ctx->graph, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_residuals(flite_ctx *ctx, double res[7], double maxres[7], int32_t maxind[7]) {
+    if (!ctx || !res || !maxres || !maxind) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        const LevelView &L = X.c.multigridScheme > 0 ? X.V(0) : X.V((int)X.lv.size() - 1);
+        k_resid_partial<<<kResidBlocks, 256, 0, X.s>>>(L, X.d_part, kResidBlocks);
+        k_resid_final<<<1, 1, 0, X.s>>>(X.d_part, kResidBlocks, X.d_out);
+        double h[15];
+        CK(cudaMemcpyAsync(h, X.d_out, sizeof h, cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+        for (int k = 0; k < 7; ++k) { res[k] = 0.0; maxres[k] = 0.0; maxind[k] = 1; }
+        bool finite = true;
+        for (int k = 0; k < 5; ++k) {
+            res[k] = h[k];
+            maxres[k] = h[5 + k];
+            maxind[k] = (int32_t)h[10 + k] + 1;
+            if (!std::isfinite(res[k])) finite = false;
+        }
+        if (!finite) return fail(ctx, FLITE_ENAN, "NaN in residual");
+        return FLITE_OK;
+    });
+}
+
+int flite_forces(flite_ctx *ctx, double out[6]) {
+    if (!ctx || !out) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        DevLevel &D = X.lv[0];
+        const double PI = 4.0 * std::atan(1.0);
+        if (D.wall.empty()) {
+            for (int k = 0; k < 6; ++k) out[k] = 0.0;
+            return FLITE_OK;
+        }
+        k_forces<<<1, 256, 0, X.s>>>(X.P, D.v, D.d_wall, (int)D.wall.size(), X.c.alpha * PI / 180.,
+                                    X.c.beta * PI / 180., X.c.groundplane, X.c.datum[0], X.c.datum[1],
+                                    X.c.datum[2], X.d_out);
+        double h[6];
+        CK(cudaMemcpyAsync(h, X.d_out, sizeof h, cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+        for (int k = 0; k < 6; ++k) out[k] = k < 4 ? h[k] / X.c.referenceArea : h[k];
+        return FLITE_OK;
+    });
+}
+
+int flite_residual_fwd(flite_ctx *ctx, int level, const double *u, double *r) {
+    if (bad_level(ctx, level) || !u || !r) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        const int l = level - 1;
+        LevelView &L = X.V(l);
+        CK(cudaMemcpyAsync(L.u, u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        X.pressure(l);
+        X.rhs_terms(l);
+        X.node_update(l, MODE_RESID, 0);
+        CK(cudaMemcpyAsync(r, L.rhs, 5 * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+        return FLITE_OK;
+    });
+}
+
+int flite_time_cycles(flite_ctx *ctx, int cycle_no, int ncycles, double *ms) {
+    if (!ctx || ncycles < 1 || !ms) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        X.ensure_graph();
+        X.set_cycle(cycle_no);
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        CK(cudaEventRecord(a, X.s));
+        for (int i = 0; i < ncycles; ++i) CK(cudaGraphLaunch(X.graph, X.s));
+        CK(cudaEventRecord(b, X.s));
+        CK(cudaEventSynchronize(b));
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        *ms = t;
+        return FLITE_OK;
+    });
+}
+
+int flite_cycle_launches(flite_ctx *ctx, int64_t *n) {
+    if (!ctx || !n) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->ensure_graph();
+        *n = ctx->launches;
+        return FLITE_OK;
+    });
+}
+
+int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, double *node_ms) {
+    if (bad_level(ctx, level) || reps < 1 || !edge_ms || !node_ms) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        const int l = level - 1;
+        LevelView &L = X.V(l);
+        cudaEvent_t ev[4];
+        for (auto &e : ev) CK(cudaEventCreate(&e));
+        double te = 0, tn = 0;
+        for (int r = 0; r < reps; ++r) {
+            X.pressure(l);
+            CK(cudaEventRecord(ev[0], X.s));
+            k_edge_flux<<<flite_ctx::blocks(L.E), kBlock, 0, X.s>>>(X.P, L);
+            CK(cudaEventRecord(ev[1], X.s));
+            if (L.B > 0) k_bnd_flux<<<flite_ctx::blocks(L.B), kBlock, 0, X.s>>>(X.P, L);
+            CK(cudaEventRecord(ev[2], X.s));
+            k_node_update<<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            CK(cudaEventRecord(ev[3], X.s));
+            CK(cudaEventSynchronize(ev[3]));
+            float a = 0, b = 0;
+            CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+            CK(cudaEventElapsedTime(&b, ev[2], ev[3]));
+            te += a; tn += b;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        *edge_ms = te / reps;
+        *node_ms = tn / reps;
+        return FLITE_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,345 @@
+// Edge and boundary-edge fluxes of makeRHS (def_par:1525-2512).
+#pragma once
+#include "device.cuh"
+
+namespace flite {
+
+struct NodeState {
+    double r, ru, rv, rw, E, p;
+};
+
+__device__ __forceinline__ NodeState load_state(const LevelView &L, int i) {
+    NodeState s;
+    s.r = L.u[i];
+    s.ru = L.u[L.N + i];
+    s.rv = L.u[2 * L.N + i];
+    s.rw = L.u[3 * L.N + i];
+    s.E = L.u[4 * L.N + i];
+    s.p = L.p[i];
+    return s;
+}
+
+// LED limiter of the HLLC reconstruction (def_par:1856-1867); the root
+// (1+t^nsig)^(1/nsig) is sqrt(sqrt(.)) for nsig=4 and sqrt(.) for nsig=2
+__device__ __forceinline__ double led(double a, double bmin, double bmax, int nsig) {
+    double cc = a;
+    double a1 = 2.0 * a;
+    if (a1 > 0.0) {
+        double invmax = 0.0;
+        if (bmax > 0.0) invmax = 1.0 / bmax;
+        double t = a1 * invmax;
+        double tn = nsig == 4 ? (t * t) * (t * t) : t * t;
+        double root = nsig == 4 ? sqrt(sqrt(1. + tn)) : sqrt(1. + tn);
+        cc = 0.5 * bmax * t / root;
+    } else if (a1 < 0.0) {
+        double invmin = 0.0;
+        if (bmin < 0.0) invmin = 1.0 / bmin;
+        double t = a1 * invmin;
+        double tn = nsig == 4 ? (t * t) * (t * t) : t * t;
+        double root = nsig == 4 ? sqrt(sqrt(1. + tn)) : sqrt(1. + tn);
+        cc = 0.5 * bmin * t / root;
+    }
+    return cc;
+}
+
+// Interior edge flux f of edge e (i1 -> i2), added to rhs(i1) and
+// subtracted from rhs(i2).
+__device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, int e, int i1, int i2, double *f) {
+    const NodeState a = load_state(L, i1), b = load_state(L, i2);
+    const double gam = P.gamma, gam1 = P.gm1;
+    double pr1 = a.p, r1 = a.r, rinv1 = 1. / a.r;
+    double ru1 = a.ru, rv1 = a.rv, rw1 = a.rw;
+    double u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1;
+    double E1 = a.E, rh1 = a.E + pr1;
+    double pr2 = b.p, r2 = b.r, rinv2 = 1. / b.r;
+    double ru2 = b.ru, rv2 = b.rv, rw2 = b.rw;
+    double u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2;
+    double E2 = b.E, rh2 = b.E + pr2;
+    const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
+    f[0] = f[1] = f[2] = f[3] = f[4] = 0.0;
+    if (P.fluxType == 1 || P.fluxType == 4) {
+        // central flux (def_par:1664-1669); HLLC starts from it too (:1798)
+        f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
+        f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
+        f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
+        f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+        f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+        if (P.fluxType == 1) return;
+    }
+    if (P.fluxType == 2) {  // local Lax-Friedrichs (def_par:1670-1724)
+        double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
+        if (rnorm > 1.0e-10) {
+            double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+            double c1 = sqrt(gam * pr1 * rinv1);
+            double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+            double c2 = sqrt(gam * pr2 * rinv2);
+            double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+            double l11 = fabs(nv1 + c1), l12 = fabs(nv2 + c2);
+            double l1 = l11; if (l1 < l12) l1 = l12;
+            double l21 = fabs(nv1 - c1), l22 = fabs(nv2 - c2);
+            double l2 = l21; if (l2 < l22) l2 = l22;
+            double lam = l1; if (lam < l2) lam = l2;
+            f[0] = rnorm * ((r1 * nv1 + r2 * nv2) - lam * (r1 - r2));
+            f[1] = rnorm * (((pr1 * rnx + ru1 * nv1) + (pr2 * rnx + ru2 * nv2)) - lam * (ru1 - ru2));
+            f[2] = rnorm * (((pr1 * rny + rv1 * nv1) + (pr2 * rny + rv2 * nv2)) - lam * (rv1 - rv2));
+            f[3] = rnorm * (((pr1 * rnz + rw1 * nv1) + (pr2 * rnz + rw2 * nv2)) - lam * (rw1 - rw2));
+            f[4] = rnorm * ((rh1 * nv1 + rh2 * nv2) - lam * (E1 - E2));
+        }
+        return;
+    }
+    if (P.fluxType == 3) {  // Roe (def_par:1725-1792)
+        double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
+        if (rnorm > 1.0e-10) {
+            double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+            u1 = ru1 * rinv1; v1 = rv1 * rinv1; w1 = rw1 * rinv1;
+            double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+            double f11 = r1 * nv1, f21 = pr1 * rnx + ru1 * nv1, f31 = pr1 * rny + rv1 * nv1;
+            double f41 = pr1 * rnz + rw1 * nv1, f51 = rh1 * nv1;
+            double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+            double f12 = r2 * nv2, f22 = pr2 * rnx + ru2 * nv2, f32 = pr2 * rny + rv2 * nv2;
+            double f42 = pr2 * rnz + rw2 * nv2, f52 = rh2 * nv2;
+            double h1 = rh1 * rinv1, h2 = rh2 * rinv2;
+            double di = sqrt(r1 / r2), d1 = 1.0 / (di + 1.0);
+            double ui = (di * u1 + u2) * d1, vi = (di * v1 + v2) * d1, wi = (di * w1 + w2) * d1;
+            double hi = (di * h1 + h2) * d1;
+            double ci2 = gam1 * (hi - 0.5 * ((ui * ui + vi * vi) + wi * wi));
+            ci2 = dmax(ci2, 1.0e-5);
+            double ci = sqrt(ci2);
+            double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+            double ucp = (ui * rnx + vi * rny) + wi * rnz;
+            double du1 = r1 - r2, du2 = ru1 - ru2, du3 = rv1 - rv2, du4 = rw1 - rw2, du5 = E1 - E2;
+            double l1 = fabs(ucp + ci), l2 = fabs(ucp - ci), l3 = fabs(ucp);
+            double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+            double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+            double al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+            double cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+            double cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+            f[0] = rnorm * ((f11 + f12) - (l3 * du1 + cc1));
+            f[1] = rnorm * ((f21 + f22) - ((l3 * du2 + cc1 * ui) + cc2 * rnx));
+            f[2] = rnorm * ((f31 + f32) - ((l3 * du3 + cc1 * vi) + cc2 * rny));
+            f[3] = rnorm * ((f41 + f42) - ((l3 * du4 + cc1 * wi) + cc2 * rnz));
+            f[4] = rnorm * ((f51 + f52) - ((l3 * du5 + cc1 * hi) + cc2 * ucp));
+        }
+        return;
+    }
+    // HLLC (def_par:1794-2085)
+    double roe1 = a.r, roe2 = b.r, re1 = a.E, re2 = b.E;
+    double wx2 = 2.0 * wx, wy2 = 2.0 * wy, wz2 = 2.0 * wz;
+    double rnorm = sqrt((wx2 * wx2 + wy2 * wy2) + wz2 * wz2);
+    double rnorm1 = rnorm;
+    if (rnorm > 0.0) rnorm = 1.0 / rnorm;
+    double rnx = wx2 * rnorm, rny = wy2 * rnorm, rnz = wz2 * rnorm;
+    if (P.hllcOrder > 1) {
+        double dpvl[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (L.grid == 1) {
+            // coarse levels have zero coordinates: dx = 0 gives dpvl = 0
+            double dx = L.cx[i2] - L.cx[i1], dy = L.cy[i2] - L.cy[i1], dz = L.cz[i2] - L.cz[i1];
+            double hlength = 0.5 * P.clip * sqrt((dx * dx + dy * dy) + dz * dz);
+            const int N = L.N;
+            for (int j = 0; j < 5; ++j) {
+                double dpv1 = 0.5 * ((L.grad[j * N + i1] * dx + L.grad[(j + 5) * N + i1] * dy) + L.grad[(j + 10) * N + i1] * dz);
+                double dpv11 = 0.5 * ((L.grad[j * N + i2] * dx + L.grad[(j + 5) * N + i2] * dy) + L.grad[(j + 10) * N + i2] * dz);
+                if (P.autoClip == 1) {
+                    dpv1 = led(dpv1, L.bnd[j * N + i1], L.bnd[(j + 5) * N + i1], P.nsig);
+                    dpv11 = -led(-dpv11, L.bnd[j * N + i2], L.bnd[(j + 5) * N + i2], P.nsig);
+                }
+                double aa = dpv1, bb = dpv11, cc;
+                if (aa * bb <= 0.0) {
+                    cc = 0.0;
+                } else {
+                    cc = fabs(aa) <= fabs(bb) ? aa : bb;
+                    if (fabs(cc) > hlength && hlength > 0.0) cc = hlength * cc / fabs(cc);
+                }
+                dpvl[j] = cc;
+            }
+        }
+        if ((roe1 + dpvl[0]) > 0.1) roe1 = roe1 + dpvl[0];
+        u1 = u1 + dpvl[1]; v1 = v1 + dpvl[2]; w1 = w1 + dpvl[3];
+        if ((re1 + dpvl[4]) > 0.0001) re1 = re1 + dpvl[4];
+        pr1 = gam1 * (re1 - 0.5 * ((u1 * u1 + v1 * v1) + w1 * w1) * roe1);
+        pr1 = dmax(pr1, 0.1);
+        rh1 = re1 + pr1; rinv1 = 1 / roe1;
+        ru1 = roe1 * u1; rv1 = roe1 * v1; rw1 = roe1 * w1;
+        if ((roe2 - dpvl[0]) > 0.1) roe2 = roe2 - dpvl[0];
+        u2 = u2 - dpvl[1]; v2 = v2 - dpvl[2]; w2 = w2 - dpvl[3];
+        if ((re2 - dpvl[4]) > 0.0001) re2 = re2 - dpvl[4];
+        pr2 = gam1 * (re2 - 0.5 * ((u2 * u2 + v2 * v2) + w2 * w2) * roe2);
+        pr2 = dmax(pr2, 0.1);
+        rh2 = re2 + pr2; rinv2 = 1 / roe2;
+        ru2 = roe2 * u2; rv2 = roe2 * v2; rw2 = roe2 * w2;
+    }
+    double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+    double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+    double beta0 = sqrt(gam1 / (2 * gam));
+    double rroe = sqrt(roe2 / roe1);
+    double ut = (u1 + u2 * rroe) / (1 + rroe), vt = (v1 + v2 * rroe) / (1 + rroe);
+    double wt = (w1 + w2 * rroe) / (1 + rroe);
+    double qt = (ut * rnx + vt * rny) + wt * rnz;
+    double ht = (rh1 * rinv1 + rh2 * rinv2 * rroe) / (1 + rroe);
+    double ct = gam1 * (ht - 0.5 * ((ut * ut + vt * vt) + wt * wt));
+    ct = sqrt(fabs(ct));
+    double c1 = sqrt(gam1 * fabs(rh1 * rinv1 - 0.5 * ((u1 * u1 + v1 * v1) + w1 * w1)));
+    double c2 = sqrt(gam1 * fabs(rh2 * rinv2 - 0.5 * ((u2 * u2 + v2 * v2) + w2 * w2)));
+    double sl = dmin(nv1 - beta0 * c1, qt - ct);
+    double sr = dmax(nv2 + beta0 * c2, qt + ct);
+    sl = dmin(sl, nv2 - beta0 * c2);
+    sr = dmax(sr, nv1 + beta0 * c1);
+    double sm = roe2 * nv2 * (sr - nv2) - roe1 * nv1 * (sl - nv1);
+    sm = (sm + pr1) - pr2;
+    double fact = roe2 * (sr - nv2) - roe1 * (sl - nv1);
+    if (fact != 0.0) fact = 1.0 / fact;
+    sm = fact * sm;
+    if (sl > 0.0) {
+        f[0] = ((rnx * ru1 + rny * rv1) + rnz * rw1) * rnorm1;
+        f[1] = ((rnx * (ru1 * u1 + pr1) + rny * (ru1 * v1)) + rnz * (ru1 * w1)) * rnorm1;
+        f[2] = ((rnx * (rv1 * u1) + rny * (rv1 * v1 + pr1)) + rnz * (rv1 * w1)) * rnorm1;
+        f[3] = ((rnx * (rw1 * u1) + rny * (rw1 * v1)) + rnz * (rw1 * w1 + pr1)) * rnorm1;
+        f[4] = ((rnx * (rh1 * u1) + rny * (rh1 * v1)) + rnz * (rh1 * w1)) * rnorm1;
+    } else if (sl <= 0.0 && sm > 0.0) {
+        double fl0 = (rnx * ru1 + rny * rv1) + rnz * rw1;
+        double fl1 = (rnx * (ru1 * u1 + pr1) + rny * (ru1 * v1)) + rnz * (ru1 * w1);
+        double fl2 = (rnx * (rv1 * u1) + rny * (rv1 * v1 + pr1)) + rnz * (rv1 * w1);
+        double fl3 = (rnx * (rw1 * u1) + rny * (rw1 * v1)) + rnz * (rw1 * w1 + pr1);
+        double fl4 = (rnx * (rh1 * u1) + rny * (rh1 * v1)) + rnz * (rh1 * w1);
+        double pls = roe1 * (nv1 - sl) * (nv1 - sm) + pr1;
+        double ls0, ls1, ls2, ls3, ls4;
+        double factl = sl - sm;
+        if (factl != 0.0) {
+            factl = 1.0 / factl;
+            ls0 = roe1 * (sl - nv1) * factl;
+            ls1 = ((sl - nv1) * roe1 * u1 + (pls - pr1) * rnx) * factl;
+            ls2 = ((sl - nv1) * roe1 * v1 + (pls - pr1) * rny) * factl;
+            ls3 = ((sl - nv1) * roe1 * w1 + (pls - pr1) * rnz) * factl;
+            ls4 = (((sl - nv1) * re1 - pr1 * nv1) + pls * sm) * factl;
+        } else {
+            ls0 = roe1; ls1 = ru1; ls2 = rv1; ls3 = rw1; ls4 = re1;
+        }
+        f[0] = (fl0 + sl * (ls0 - roe1)) * rnorm1;
+        f[1] = (fl1 + sl * (ls1 - ru1)) * rnorm1;
+        f[2] = (fl2 + sl * (ls2 - rv1)) * rnorm1;
+        f[3] = (fl3 + sl * (ls3 - rw1)) * rnorm1;
+        f[4] = (fl4 + sl * (ls4 - re1)) * rnorm1;
+    } else if (sm <= 0.0 && sr >= 0.0) {
+        double fr0 = (rnx * ru2 + rny * rv2) + rnz * rw2;
+        double fr1 = (rnx * (ru2 * u2 + pr2) + rny * (ru2 * v2)) + rnz * (ru2 * w2);
+        double fr2 = (rnx * (rv2 * u2) + rny * (rv2 * v2 + pr2)) + rnz * (rv2 * w2);
+        double fr3 = (rnx * (rw2 * u2) + rny * (rw2 * v2)) + rnz * (rw2 * w2 + pr2);
+        double fr4 = (rnx * (rh2 * u2) + rny * (rh2 * v2)) + rnz * (rh2 * w2);
+        double prs = roe2 * (nv2 - sr) * (nv2 - sm) + pr2;
+        double rs0, rs1, rs2, rs3, rs4;
+        double factr = sr - sm;
+        if (factr != 0.0) {
+            factr = 1.0 / factr;
+            rs0 = roe2 * (sr - nv2) * factr;
+            rs1 = ((sr - nv2) * roe2 * u2 + (prs - pr2) * rnx) * factr;
+            rs2 = ((sr - nv2) * roe2 * v2 + (prs - pr2) * rny) * factr;
+            rs3 = ((sr - nv2) * roe2 * w2 + (prs - pr2) * rnz) * factr;
+            rs4 = (((sr - nv2) * re2 - pr2 * nv2) + prs * sm) * factr;
+        } else {
+            rs0 = roe2; rs1 = ru2; rs2 = rv2; rs3 = rw2; rs4 = re2;
+        }
+        f[0] = (fr0 + sr * (rs0 - roe2)) * rnorm1;
+        f[1] = (fr1 + sr * (rs1 - ru2)) * rnorm1;
+        f[2] = (fr2 + sr * (rs2 - rv2)) * rnorm1;
+        f[3] = (fr3 + sr * (rs3 - rw2)) * rnorm1;
+        f[4] = (fr4 + sr * (rs4 - re2)) * rnorm1;
+    } else if (sr < 0.0) {
+        f[0] = ((rnx * ru2 + rny * rv2) + rnz * rw2) * rnorm1;
+        f[1] = ((rnx * (ru2 * u2 + pr2) + rny * (ru2 * v2)) + rnz * (ru2 * w2)) * rnorm1;
+        f[2] = ((rnx * (rv2 * u2) + rny * (rv2 * v2 + pr2)) + rnz * (rv2 * w2)) * rnorm1;
+        f[3] = ((rnx * (rw2 * u2) + rny * (rw2 * v2)) + rnz * (rw2 * w2 + pr2)) * rnorm1;
+        f[4] = ((rnx * (rh2 * u2) + rny * (rh2 * v2)) + rnz * (rh2 * w2)) * rnorm1;
+    }
+}
+
+// wall/symmetry own-state flux (def_par:2194-2230)
+__device__ __forceinline__ void wall_flux(const NodeState &s, double rnx, double rny, double rnz, double *F) {
+    double pr = s.p, rho = s.r, rinv = 1. / rho;
+    double rh = s.E + pr;
+    double uu = s.ru * rinv, vv = s.rv * rinv, ww = s.rw * rinv;
+    double nv = (uu * rnx + vv * rny) + ww * rnz;
+    F[0] = rho * nv;
+    F[1] = pr * rnx + rho * uu * nv;
+    F[2] = pr * rny + rho * vv * nv;
+    F[3] = pr * rnz + rho * ww * nv;
+    F[4] = rh * nv;
+}
+
+// Roe flux between a node state and the freestream (def_par:2268-2346)
+__device__ __forceinline__ void farfield_flux(const Params &P, const NodeState &s, double rnx, double rny, double rnz,
+                                              const double *inf, double *F) {
+    const double gam1 = P.gm1;
+    double ro = inf[0], ro1 = 1. / ro, uo = inf[1], vo = inf[2], wo = inf[3], eo = inf[4], po = inf[5];
+    double prl = s.p, rhol = s.r, rinvl = 1. / rhol;
+    double rhl = s.E + prl;
+    double ul = s.ru * rinvl, vl = s.rv * rinvl, wl = s.rw * rinvl;
+    double epsl = s.E, hl = rhl * rinvl;
+    double nvl = (ul * rnx + vl * rny) + wl * rnz;
+    double fl1 = rhol * nvl, fl2 = prl * rnx + rhol * ul * nvl, fl3 = prl * rny + rhol * vl * nvl;
+    double fl4 = prl * rnz + rhol * wl * nvl, fl5 = rhl * nvl;
+    double rhor = ro, uxr = uo, vyr = vo, wzr = wo, epsr = eo * ro, presr = po, hr = eo + po * ro1;
+    double unr = (uxr * rnx + vyr * rny) + wzr * rnz;
+    double fr1 = rhor * unr, fr2 = rnx * presr + rhor * uxr * unr, fr3 = rny * presr + rhor * vyr * unr;
+    double fr4 = rnz * presr + rhor * wzr * unr, fr5 = (epsr + presr) * unr;
+    double di = sqrt(rhor / rhol), d1 = 1.0 / (di + 1.0);
+    double ui = (di * uxr + ul) * d1, vi = (di * vyr + vl) * d1, wi = (di * wzr + wl) * d1;
+    double hi = (di * hr + hl) * d1;
+    double ci2 = gam1 * (hi - 0.5 * ((ui * ui + vi * vi) + wi * wi));
+    ci2 = dmax(ci2, 1.0e-5);
+    double ci = sqrt(ci2);
+    double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+    double ucp = (ui * rnx + vi * rny) + wi * rnz;
+    double du1 = rhor - rhol, du2 = rhor * uxr - rhol * ul, du3 = rhor * vyr - rhol * vl;
+    double du4 = rhor * wzr - rhol * wl, du5 = epsr - epsl;
+    double l1 = fabs(ucp + ci), l2 = fabs(ucp - ci), l3 = fabs(ucp);
+    double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+    double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+    double al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+    double cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+    double cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+    F[0] = 0.5 * (fr1 + fl1) - 0.5 * (l3 * du1 + cc1);
+    F[1] = 0.5 * (fr2 + fl2) - 0.5 * ((l3 * du2 + cc1 * ui) + cc2 * rnx);
+    F[2] = 0.5 * (fr3 + fl3) - 0.5 * ((l3 * du3 + cc1 * vi) + cc2 * rny);
+    F[3] = 0.5 * (fr4 + fl4) - 0.5 * ((l3 * du4 + cc1 * wi) + cc2 * rnz);
+    F[4] = 0.5 * (fr5 + fl5) - 0.5 * ((l3 * du5 + cc1 * hi) + cc2 * ucp);
+}
+
+// Contributions g1 (to node 1) and g2 (to node 2) of boundary edge b
+// (def_par:2182-2511, static mesh)
+__device__ __forceinline__ void boundary_flux(const Params &P, const LevelView &L, int b, double *g1, double *g2) {
+    const int2 nd = L.bedge[b];
+    const int ind = L.bind[b];
+    const double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
+    for (int k = 0; k < 5; ++k) { g1[k] = 0.0; g2[k] = 0.0; }
+    const NodeState s1 = load_state(L, nd.x), s2 = load_state(L, nd.y);
+    const bool fe = P.boundaryTerm == 1;
+    double F1[5], F2[5];
+    if (ind <= 2 || ind == 9) {
+        double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
+        if (!(rnorm > 1.0e-10)) return;
+        double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+        wall_flux(s1, rnx, rny, rnz, F1);
+        wall_flux(s2, rnx, rny, rnz, F2);
+    } else if (ind <= 4) {
+        double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
+        if (!(rnorm > 1.0e-10)) return;
+        double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+        const double *inf = &P.inf[(ind - 3) * 6];
+        farfield_flux(P, s1, rnx, rny, rnz, inf, F1);
+        farfield_flux(P, s2, rnx, rny, rnz, inf, F2);
+    } else {
+        return;  // engine faces are rejected at context creation
+    }
+    const double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
+    for (int k = 0; k < 5; ++k) {
+        if (fe) {
+            g1[k] = rnorm * (3. * F1[k] + F2[k]);
+            g2[k] = rnorm * (F1[k] + 3. * F2[k]);
+        } else {
+            g1[k] = rnorm * 4. * F1[k];
+            g2[k] = rnorm * 4. * F2[k];
+        }
+    }
+}
+
+}  // namespace flite

@@ -1,0 +1,609 @@
+// CUDA kernels of the flow-solver hot path (sm_100a, FP64).
+//
+// Layout and scheduling (the reasoning is in DESIGN.md):
+//  * node state is SoA [component][node] so node kernels read and write each
+//    component coalesced;
+//  * the interior-edge flux is computed once per edge into an edge buffer
+//    [E][5]; a node kernel then sums it through a CSR list of incident
+//    edges kept in edge order.  Summing in edge order reproduces the
+//    reference's scatter loop (rhs(i1)+=f, rhs(i2)-=f in edge order) bit for
+//    bit, with no atomics;
+//  * cheap edge terms (time step, JST Laplacian and sensor, JST flux,
+//    gradients, min/max) are recomputed by both endpoints inside a node
+//    gather, which replaces an edge buffer round trip by reads of the
+//    neighbour's state;
+//  * everything the reference does per node after the residual (add the
+//    dissipation, multiply by dt/V, boundary conditions on the increment,
+//    the clipped update, boundary conditions on the solution, the FAS
+//    source, the density floor, the far-field conditions) is fused into the
+//    node kernel that gathers the residual.
+#include <cuda_runtime.h>
+
+#include "flux.cuh"
+#include "kernels.h"
+
+namespace flite {
+
+static __device__ __forceinline__ int tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+// ---- makePressureField (def_par:13612-13630) ------------------------------
+__global__ void k_pressure(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    L.p[i] = pressure(P, L.u[i], L.u[N + i], L.u[2 * N + i], L.u[3 * N + i], L.u[4 * N + i]);
+}
+
+// ---- makeTimeSteps (def_par:13335-13610) as a node gather -----------------
+__global__ void k_timestep(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double c1 = P.gamma;
+    const double ri = L.u[i], ro = 1. / ri;
+    const double m1 = L.u[N + i], m2 = L.u[2 * N + i], m3 = L.u[3 * N + i];
+    const double cc = dmax(c1 * L.p[i] * ro, 0.001);
+    double acc = 0.0, h = 0.0;
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int e = t.x >= 0 ? t.x : ~t.x;
+        double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
+        double al = (wx * wx + wy * wy) + wz * wz;
+        double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
+        acc = (acc + fabs(vn)) + sqrt(cc * al);
+        if (P.viscous) {
+            // the other node's viscous term (def_par:13432-13433)
+            int j = t.y;
+            double vis = dmax(P.am, L.mu[j]);
+            double dv = 2.0 * vis * al / L.u[j];
+            h = h + dv;
+        }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        int2 nd = L.bedge[b];
+        double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
+        double al = (wx * wx + wy * wy) + wz * wz;
+        int j1 = nd.x, j2 = nd.y;
+        double ro1 = 1. / L.u[j1], ro2 = 1. / L.u[j2];
+        double cc1 = dmax(c1 * L.p[j1] * ro1, 0.001);
+        double cc2 = dmax(c1 * L.p[j2] * ro2, 0.001);
+        double vn1 = ((wx * L.u[N + j1] + wy * L.u[2 * N + j1]) + wz * L.u[3 * N + j1]) * ro1;
+        double vn2 = ((wx * L.u[N + j2] + wy * L.u[2 * N + j2]) + wz * L.u[3 * N + j2]) * ro2;
+        vn1 = fabs(vn1); vn2 = fabs(vn2);
+        double vnm = vn1 + vn2;
+        cc1 = sqrt(cc1 * al); cc2 = sqrt(cc2 * al);
+        double ccm = cc1 + cc2;
+        if (side == 0) acc = (((acc + vn1) + vnm) + cc1) + ccm;
+        else acc = (((acc + vn2) + vnm) + cc2) + ccm;
+        if (P.viscous) {
+            double vis1 = dmax(P.am, L.mu[j1]), vis2 = dmax(P.am, L.mu[j2]);
+            double dv1 = 2.0 * vis1 * al / L.u[j1];
+            double dv2 = 2.0 * vis2 * al / L.u[j2];
+            double dvm = dv1 + dv2;
+            h = side == 0 ? (h + dv1) + dvm : (h + dv2) + dvm;
+        }
+    }
+    const double V = L.V[i];
+    L.dt[i] = 0.5 / (acc / V + h / (V * V));
+}
+
+// ---- makeArtificialDissipation2, passes 1-2 and the node finish -----------
+// (def_par:11513-11780): undivided Laplacian with dE+dp, pressure sensor
+__global__ void k_jst_lap(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, s7 = 0, s8 = 0;
+    const double ui0 = L.u[i], ui1 = L.u[N + i], ui2 = L.u[2 * N + i], ui3 = L.u[3 * N + i], ui4 = L.u[4 * N + i];
+    const double pi = L.p[i];
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int j = t.y;
+        double df = 1.0;
+        if (P.useDissW) df = 1. / L.slen[t.x >= 0 ? t.x : ~t.x];
+        double uj0 = L.u[j], uj1 = L.u[N + j], uj2 = L.u[2 * N + j], uj3 = L.u[3 * N + j], uj4 = L.u[4 * N + j];
+        double pj = L.p[j];
+        if (t.x >= 0) {  // this node is i1: d = u(i) - u(j)
+            double d0 = ui0 - uj0, d1 = ui1 - uj1, d2 = ui2 - uj2, d3 = ui3 - uj3;
+            double d4 = ((ui4 - uj4) + pi) - pj;
+            l0 = l0 - d0 * df; l1 = l1 - d1 * df; l2 = l2 - d2 * df; l3 = l3 - d3 * df; l4 = l4 - d4 * df;
+            double dp = pi - pj, sp = pi + pj;
+            s7 = s7 - dp; s8 = s8 + sp;
+        } else {          // i2: d = u(j) - u(i)
+            double d0 = uj0 - ui0, d1 = uj1 - ui1, d2 = uj2 - ui2, d3 = uj3 - ui3;
+            double d4 = ((uj4 - ui4) + pj) - pi;
+            l0 = l0 + d0 * df; l1 = l1 + d1 * df; l2 = l2 + d2 * df; l3 = l3 + d3 * df; l4 = l4 + d4 * df;
+            double dp = pj - pi, sp = pj + pi;
+            s7 = s7 + dp; s8 = s8 + sp;
+        }
+    }
+    double fact = 1. / L.conn[i];
+    L.sens[i] = 12. * fabs(s7 / s8);
+    L.lap[i] = fact * l0;
+    L.lap[N + i] = fact * l1;
+    L.lap[2 * N + i] = fact * l2;
+    L.lap[3 * N + i] = fact * l3;
+    L.lap[4 * N + i] = fact * l4;
+}
+
+// ---- makeArtificialDissipation2, pass 3 (def_par:11770-11906), scalar -----
+__global__ void k_jst_flux(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double k4 = L.grid == 1 ? P.k4 : P.cgdf;
+    double acc[5] = {0, 0, 0, 0, 0};
+    double Li[5], Ui[5];
+    for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
+    const double vdi = L.V[i] / L.dt[i], coni = L.conn[i], si = L.sens[i];
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int j = t.y;
+        double vdj = L.V[j] / L.dt[j];
+        const bool first = t.x >= 0;
+        double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
+        d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
+        double sj = L.sens[j];
+        double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
+        double d4 = d0 * k4;
+        d4 = d4 > d2 ? d4 - d2 : 0.0;
+        for (int c = 0; c < 5; ++c) {
+            double Lj = L.lap[c * N + j], Uj = L.u[c * N + j];
+            if (first) {
+                double d4v = Li[c] - Lj, d2v = Ui[c] - Uj;
+                acc[c] = (acc[c] - d4v * d4) + d2v * d2;
+            } else {
+                double d4v = Lj - Li[c], d2v = Uj - Ui[c];
+                acc[c] = (acc[c] + d4v * d4) - d2v * d2;
+            }
+        }
+    }
+    for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
+}
+
+// ---- makeArtificialDissipation3 (def_par:11995-12139) ---------------------
+__global__ void k_first_order_diss(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double acc[5] = {0, 0, 0, 0, 0};
+    const double vdi = L.V[i] / L.dt[i], coni = L.conn[i];
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int j = t.y;
+        double vdj = L.V[j] / L.dt[j];
+        const bool first = t.x >= 0;
+        double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
+        d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
+        double d2 = d0 * P.cgdf;
+        for (int c = 0; c < 5; ++c) {
+            double dk = first ? L.u[c * N + i] - L.u[c * N + j] : L.u[c * N + j] - L.u[c * N + i];
+            acc[c] = first ? acc[c] + dk * d2 : acc[c] - dk * d2;
+        }
+    }
+    for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
+}
+
+__global__ void k_fill(double *a, size_t n, double v) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+// ---- computeGradient, Galerkin (def_par:2923-3245) ------------------------
+__global__ void k_gradient(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double g[15];
+    for (int c = 0; c < 15; ++c) g[c] = 0.0;
+    const double ri = L.u[i];
+    const double qi[5] = {ri, L.u[N + i] / ri, L.u[2 * N + i] / ri, L.u[3 * N + i] / ri, L.u[4 * N + i]};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int e = t.x >= 0 ? t.x : ~t.x, j = t.y;
+        const double rj = L.u[j];
+        const double qj[5] = {rj, L.u[N + j] / rj, L.u[2 * N + j] / rj, L.u[3 * N + j] / rj, L.u[4 * N + j]};
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 5; ++c) {
+                double s = t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c];
+                double dq = s * w[a];
+                g[a * 5 + c] = t.x >= 0 ? g[a * 5 + c] + dq : g[a * 5 + c] - dq;
+            }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        int2 nd = L.bedge[b];
+        const double r1 = L.u[nd.x], r2 = L.u[nd.y];
+        const double q1[5] = {r1, L.u[N + nd.x] / r1, L.u[2 * N + nd.x] / r1, L.u[3 * N + nd.x] / r1, L.u[4 * N + nd.x]};
+        const double q2[5] = {r2, L.u[N + nd.y] / r2, L.u[2 * N + nd.y] / r2, L.u[3 * N + nd.y] / r2, L.u[4 * N + nd.y]};
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 5; ++c) {
+                double s = q1[c] + q2[c];
+                double own = side == 0 ? q1[c] : q2[c];
+                g[a * 5 + c] = g[a * 5 + c] + (2. * own + s) * w[a];
+            }
+    }
+    const double vt = 1. / L.V[i];
+    for (int c = 0; c < 15; ++c) L.grad[c * N + i] = g[c] * vt;
+}
+
+// ---- LocalMinMax (def_par:3248-3459) ---------------------------------------
+__global__ void k_minmax(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double mn[5], mx[5];
+    for (int c = 0; c < 5; ++c) { mn[c] = 1.0e15; mx[c] = 1.0e15; }
+    const double ri = L.u[i];
+    const double qi[5] = {ri, L.u[N + i] / ri, L.u[2 * N + i] / ri, L.u[3 * N + i] / ri, L.u[4 * N + i]};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int j = t.y;
+        const double rj = L.u[j];
+        const double qj[5] = {rj, L.u[N + j] / rj, L.u[2 * N + j] / rj, L.u[3 * N + j] / rj, L.u[4 * N + j]};
+        // amin1(q(i1), q(i2)) with the edge's own node order
+        for (int c = 0; c < 5; ++c) {
+            double a = t.x >= 0 ? qi[c] : qj[c], b = t.x >= 0 ? qj[c] : qi[c];
+            mn[c] = dmin(mn[c], dmin(a, b));
+            mx[c] = dmin(mx[c], dmin(-a, -b));
+        }
+    }
+    for (int c = 0; c < 5; ++c) {
+        L.bnd[c * N + i] = mn[c] - qi[c];
+        L.bnd[(c + 5) * N + i] = -mx[c] - qi[c];
+    }
+}
+
+// ---- interior edge flux into the edge buffer ------------------------------
+__global__ void k_edge_flux(Params P, LevelView L) {
+    int e = tid();
+    if (e >= L.E) return;
+    int2 nd = L.edge[e];
+    double f[5];
+    edge_flux(P, L, e, nd.x, nd.y, f);
+    double *o = L.flux + (size_t)e * 5;
+    o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = f[3]; o[4] = f[4];
+}
+
+// ---- boundary-edge contributions ------------------------------------------
+__global__ void k_bnd_flux(Params P, LevelView L) {
+    int b = tid();
+    if (b >= L.B) return;
+    double g1[5], g2[5];
+    boundary_flux(P, L, b, g1, g2);
+    double *o = L.bflux + (size_t)b * 10;
+    for (int k = 0; k < 5; ++k) { o[k] = g1[k]; o[5 + k] = g2[k]; }
+}
+
+// residual of node i: interior edges in edge order, then boundary edges
+__device__ __forceinline__ void gather_rhs(const LevelView &L, int i, double *r) {
+    r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int s = L.inc[k].x;
+        if (s >= 0) {
+            const double *f = L.flux + (size_t)s * 5;
+            r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
+        } else {
+            const double *f = L.flux + (size_t)(~s) * 5;
+            r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
+        }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int v = L.binc[k];
+        const double *g = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
+        r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
+    }
+}
+
+// ---- the node part of one RK stage (def_par:1069-1178), fused -------------
+// mode STAGE:   u <- update of stage `stage`
+// mode RCOARSE: restrictGrid coarse one-step (def_par:12244-12263): src
+// mode RFINE:   restrictGrid fine increment (def_par:12356-12383): rhs
+// mode RESID:   rhs <- makeRHS only
+__global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double r[5];
+    gather_rhs(L, i, r);
+    if (mode == MODE_RESID) {
+        for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
+        return;
+    }
+    for (int c = 0; c < 5; ++c) r[c] = r[c] + L.diss[c * N + i];
+    const double dt = L.dt[i], V = L.V[i];
+    for (int c = 0; c < 5; ++c) r[c] = dt * r[c] / V;  // solveSystem
+    const unsigned char cls = L.bc[i];
+    double n0 = 0, n1 = 0, n2 = 0;
+    if (cls != BC_NONE) { n0 = L.nx[i]; n1 = L.ny[i]; n2 = L.nz[i]; }
+    bc_increment(P, cls, n0, n1, n2, r);
+    const double dtJ = stage > 0 ? P.CFL * P.RK[stage - 1] : P.CFL;
+    double d[5], up[5], un[5];
+    for (int c = 0; c < 5; ++c) { d[c] = dtJ * r[c]; up[c] = L.uprev[c * N + i]; }
+    clipped_update(P, up, d, un);
+    if (mode == MODE_RFINE) {
+        // the density floor of updateSolutionVector acts on grp%u, which is
+        // not the array being updated in this call (def_par:1398-1403)
+        if (L.u[i] < P.minRho) L.u[i] = P.minRho;
+    } else {
+        if (un[0] < P.minRho) un[0] = P.minRho;
+    }
+    double cm0 = 0, cm1 = 0, cm2 = 0;
+    if (cls == BC_WALL && P.viscous) { cm0 = L.cmx[i]; cm1 = L.cmy[i]; cm2 = L.cmz[i]; }
+    bc_solution(P, cls, n0, n1, n2, cm0, cm1, cm2, relax_param(P, *L.cyc), un);
+    if (mode == MODE_STAGE) {
+        if (L.grid > 1) {
+            const double a = P.RK[stage - 1];
+            for (int c = 0; c < 5; ++c) un[c] = un[c] - a * L.src[c * N + i];
+        }
+        un[0] = dmax(un[0], P.minRho);  // limitDensity
+        bc_outer(P, cls, n0, n1, n2, L.p[i], un);
+        for (int c = 0; c < 5; ++c) L.u[c * N + i] = un[c];
+    } else if (mode == MODE_RCOARSE) {
+        bc_outer(P, cls, n0, n1, n2, L.p[i], un);
+        for (int c = 0; c < 5; ++c) L.src[c * N + i] = un[c] - up[c];
+    } else {  // MODE_RFINE
+        if (L.grid > 1)
+            for (int c = 0; c < 5; ++c) un[c] = un[c] - L.src[c * N + i];
+        bc_outer(P, cls, n0, n1, n2, L.p[i], un);
+        for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = un[c] - up[c];
+    }
+}
+
+// ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
+__global__ void k_copy(const double *a, double *b, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+// mapFineToCoarse (def_par:12572-12596) as a gather over each coarse node's
+// children in increasing fine order: the same additions in the same order as
+// the reference's scatter over fine nodes
+__device__ __forceinline__ void restrict_gather(const LevelView &C, const double *fine, int nf, int c, int ncomp,
+                                                double *out) {
+    for (int k = 0; k < ncomp; ++k) out[k] = 0.0;
+    for (int q = C.child_ptr[c]; q < C.child_ptr[c + 1]; ++q) {
+        int f = C.child[q];
+        double w = C.rweight[f];
+        for (int k = 0; k < ncomp; ++k) out[k] = out[k] + w * fine[(size_t)k * nf + f];
+    }
+}
+
+// C.u = R(F.u) (plain mapFineToCoarse of the solution)
+__global__ void k_restrict_u(LevelView C, LevelView F) {
+    int c = tid();
+    if (c >= C.N) return;
+    double v[5];
+    restrict_gather(C, F.u, F.N, c, 5, v);
+    for (int k = 0; k < 5; ++k) C.u[k * C.N + c] = v[k];
+}
+
+// restrictGrid head (def_par:12159-12185): C.u = R(F.u), C.mu = R(F.mu),
+// pressure, boundary conditions, uprev = u, pressure again
+__global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
+    int c = tid();
+    if (c >= C.N) return;
+    const int N = C.N;
+    double v[5], m;
+    restrict_gather(C, F.u, F.N, c, 5, v);
+    restrict_gather(C, F.mu, F.N, c, 1, &m);
+    C.mu[c] = m;
+    double p0 = pressure(P, v[0], v[1], v[2], v[3], v[4]);
+    const unsigned char cls = C.bc[c];
+    double n0 = 0, n1 = 0, n2 = 0;
+    if (cls != BC_NONE) { n0 = C.nx[c]; n1 = C.ny[c]; n2 = C.nz[c]; }
+    bc_solution(P, cls, n0, n1, n2, 0.0, 0.0, 0.0, relax_param(P, *C.cyc), v);
+    bc_outer(P, cls, n0, n1, n2, p0, v);
+    for (int k = 0; k < 5; ++k) { C.u[k * N + c] = v[k]; C.uprev[k * N + c] = v[k]; }
+    C.p[c] = fabs(pressure(P, v[0], v[1], v[2], v[3], v[4]));
+}
+
+// restrictGrid tail (def_par:12385-12427): C.rhs = R(F.rhs), increment
+// conditions, src -= rhs, u += rhs
+__global__ void k_restrict_incr(Params P, LevelView C, LevelView F) {
+    int c = tid();
+    if (c >= C.N) return;
+    const int N = C.N;
+    double r[5];
+    restrict_gather(C, F.rhs, F.N, c, 5, r);
+    const unsigned char cls = C.bc[c];
+    double n0 = 0, n1 = 0, n2 = 0;
+    if (cls != BC_NONE) { n0 = C.nx[c]; n1 = C.ny[c]; n2 = C.nz[c]; }
+    bc_increment(P, cls, n0, n1, n2, r);
+    for (int k = 0; k < 5; ++k) {
+        C.rhs[k * N + c] = r[k];
+        C.src[k * N + c] = C.src[k * N + c] - r[k];
+        C.u[k * N + c] = C.u[k * N + c] + r[k];
+    }
+}
+
+// prolongateGrid coarse part (def_par:12445-12468): uprev = R(F.u) with the
+// solution conditions, rhs = u - uprev with the increment conditions
+__global__ void k_prolong_coarse(Params P, LevelView C, LevelView F) {
+    int c = tid();
+    if (c >= C.N) return;
+    const int N = C.N;
+    double v[5];
+    restrict_gather(C, F.u, F.N, c, 5, v);
+    const unsigned char cls = C.bc[c];
+    double n0 = 0, n1 = 0, n2 = 0;
+    if (cls != BC_NONE) { n0 = C.nx[c]; n1 = C.ny[c]; n2 = C.nz[c]; }
+    bc_solution(P, cls, n0, n1, n2, 0.0, 0.0, 0.0, relax_param(P, *C.cyc), v);
+    bc_outer(P, cls, n0, n1, n2, C.p[c], v);
+    double r[5];
+    for (int k = 0; k < 5; ++k) {
+        C.uprev[k * N + c] = v[k];
+        r[k] = C.u[k * N + c] - v[k];
+    }
+    bc_increment(P, cls, n0, n1, n2, r);
+    for (int k = 0; k < 5; ++k) C.rhs[k * N + c] = r[k];
+}
+
+// prolongateGrid fine part (def_par:12470-12567): injection, relaxation,
+// u += correction, boundary conditions, floors
+__global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
+    int i = tid();
+    if (i >= F.N) return;
+    const int N = F.N;
+    int pc = C.parent[i];
+    double un[5];
+    for (int k = 0; k < 5; ++k) un[k] = F.u[k * N + i];
+    if (pc >= 0) {
+        for (int k = 0; k < 5; ++k) {
+            double r = C.rhs[k * C.N + pc];
+            r = P.prolRelax * r;
+            if (i < F.Nb) r = P.mgBCRelax * r;
+            F.rhs[k * N + i] = r;
+            un[k] = un[k] + r;
+        }
+    } else {
+        for (int k = 0; k < 5; ++k) {
+            double r = F.rhs[k * N + i];
+            r = P.prolRelax * r;
+            if (i < F.Nb) r = P.mgBCRelax * r;
+            F.rhs[k * N + i] = r;
+            un[k] = un[k] + r;
+        }
+    }
+    const unsigned char cls = F.bc[i];
+    double n0 = 0, n1 = 0, n2 = 0;
+    if (cls != BC_NONE) { n0 = F.nx[i]; n1 = F.ny[i]; n2 = F.nz[i]; }
+    double cm0 = 0, cm1 = 0, cm2 = 0;
+    if (cls == BC_WALL && P.viscous && F.grid == 1) { cm0 = F.cmx[i]; cm1 = F.cmy[i]; cm2 = F.cmz[i]; }
+    bc_solution(P, cls, n0, n1, n2, cm0, cm1, cm2, relax_param(P, *F.cyc), un);
+    bc_outer(P, cls, n0, n1, n2, F.p[i], un);
+    un[0] = dmax(un[0], P.minRho);
+    for (int k = 0; k < 5; ++k) F.u[k * N + i] = un[k];
+}
+
+// mapCoarseToFine of the solution (injection, def_par:12694-12700)
+__global__ void k_inject_u(LevelView C, LevelView F) {
+    int i = tid();
+    if (i >= F.N) return;
+    int pc = C.parent[i];
+    if (pc < 0) return;
+    for (int k = 0; k < 5; ++k) F.u[k * F.N + i] = C.u[k * C.N + pc];
+}
+
+// setBCsOnSolutionField on a level's solution (start-up, def_par:3994)
+__global__ void k_bc_solution(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const unsigned char cls = L.bc[i];
+    if (cls == BC_NONE) return;
+    const int N = L.N;
+    double un[5];
+    for (int k = 0; k < 5; ++k) un[k] = L.u[k * N + i];
+    double cm0 = 0, cm1 = 0, cm2 = 0;
+    if (cls == BC_WALL && P.viscous) { cm0 = L.cmx[i]; cm1 = L.cmy[i]; cm2 = L.cmz[i]; }
+    bc_solution(P, cls, L.nx[i], L.ny[i], L.nz[i], cm0, cm1, cm2, relax_param(P, *L.cyc), un);
+    for (int k = 0; k < 5; ++k) L.u[k * N + i] = un[k];
+}
+
+__global__ void k_set_int(int *dst, const int *src) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *src;
+}
+
+// ---- residual norms (writeResiduals mg_par:1299-1443) ---------------------
+// per block: sum (u-uprev)^2 and max |u-uprev| with its first index
+__global__ void k_resid_partial(LevelView L, double *part, int nblk) {
+    __shared__ double ss[5][256];
+    __shared__ double sm[5][256];
+    __shared__ int si[5][256];
+    const int N = L.N;
+    double s[5] = {0, 0, 0, 0, 0}, m[5] = {0, 0, 0, 0, 0};
+    int mi[5] = {0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        for (int k = 0; k < 5; ++k) {
+            double d = L.u[k * N + i] - L.uprev[k * N + i];
+            s[k] = s[k] + d * d;
+            double a = fabs(d);
+            if (a > m[k]) { m[k] = a; mi[k] = i; }
+        }
+    }
+    for (int k = 0; k < 5; ++k) { ss[k][threadIdx.x] = s[k]; sm[k][threadIdx.x] = m[k]; si[k][threadIdx.x] = mi[k]; }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            for (int k = 0; k < 5; ++k) {
+                ss[k][threadIdx.x] += ss[k][threadIdx.x + w];
+                double a = sm[k][threadIdx.x], b = sm[k][threadIdx.x + w];
+                int ia = si[k][threadIdx.x], ib = si[k][threadIdx.x + w];
+                if (b > a || (b == a && ib < ia)) { sm[k][threadIdx.x] = b; si[k][threadIdx.x] = ib; }
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 5; ++k) {
+            part[blockIdx.x * 15 + k] = ss[k][0];
+            part[blockIdx.x * 15 + 5 + k] = sm[k][0];
+            part[blockIdx.x * 15 + 10 + k] = (double)si[k][0];
+        }
+    }
+}
+
+__global__ void k_resid_final(const double *part, int nblk, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int k = 0; k < 5; ++k) {
+        double s = 0, m = 0;
+        int mi = 0x7fffffff;
+        for (int b = 0; b < nblk; ++b) {
+            s += part[b * 15 + k];
+            double v = part[b * 15 + 5 + k];
+            int iv = (int)part[b * 15 + 10 + k];
+            if (v > m || (v == m && iv < mi)) { m = v; mi = iv; }
+        }
+        out[k] = sqrt(s);
+        out[5 + k] = m;
+        out[10 + k] = (double)(mi == 0x7fffffff ? 0 : mi);
+    }
+}
+
+// ---- forces (calculateLiftAndDrag def_par:14710-14805), one block ---------
+__global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
+                         double ground, double d0, double d1, double d2, double *out) {
+    __shared__ double red[6][256];
+    double ft[3] = {cos(alphaR) * cos(betaR), sin(betaR), sin(alphaR)};
+    double fn1[3] = {-ft[2], 0.0, ft[0]}, fn2[3] = {-ft[1], ft[0], 0.0};
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const double pinf = 1. / (P.gamma * P.mach * P.mach);
+    const int N = L.N;
+    for (int q = threadIdx.x; q < nwall; q += blockDim.x) {
+        int ip = wall[q];
+        double h = L.cz[ip];
+        if (!(h > (ground + 0.01))) continue;
+        double xd = L.cx[ip] - d0, yd = L.cy[ip] - d1, zd = L.cz[ip] - d2;
+        double n[3] = {L.nx[ip], L.ny[ip], L.nz[ip]};
+        double A = L.wallArea[ip], dp = L.p[ip] - pinf;
+        double dn1 = (n[0] * fn1[0] + n[1] * fn1[1]) + n[2] * fn1[2];
+        double dn2 = (n[0] * fn2[0] + n[1] * fn2[1]) + n[2] * fn2[2];
+        double dt = (n[0] * ft[0] + n[1] * ft[1]) + n[2] * ft[2];
+        acc[0] -= A * dp * dn1;
+        acc[1] -= A * dp * dt;
+        acc[2] -= A * dp * dn2;
+        acc[4] += xd * A * dp * dn2 - yd * A * dp * dt;
+        acc[5] += xd * A * dp * dn1 - zd * A * dp * dt;
+        (void)N;
+    }
+    for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 6; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = 2.0 * red[0][0];
+        out[1] = 2.0 * red[1][0];
+        out[2] = 2.0 * red[2][0];
+        out[3] = 0.0;
+        out[4] = red[4][0];
+        out[5] = red[5][0];
+    }
+}
+
+}  // namespace flite

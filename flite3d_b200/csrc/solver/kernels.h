@@ -1,0 +1,34 @@
+// Kernel declarations shared by the host orchestration.
+#pragma once
+#include "device.cuh"
+
+namespace flite {
+
+enum { MODE_STAGE = 0, MODE_RCOARSE = 1, MODE_RFINE = 2, MODE_RESID = 3 };
+
+__global__ void k_pressure(Params P, LevelView L);
+__global__ void k_timestep(Params P, LevelView L);
+__global__ void k_jst_lap(Params P, LevelView L);
+__global__ void k_jst_flux(Params P, LevelView L);
+__global__ void k_first_order_diss(Params P, LevelView L);
+__global__ void k_fill(double *a, size_t n, double v);
+__global__ void k_gradient(Params P, LevelView L);
+__global__ void k_minmax(Params P, LevelView L);
+__global__ void k_edge_flux(Params P, LevelView L);
+__global__ void k_bnd_flux(Params P, LevelView L);
+__global__ void k_node_update(Params P, LevelView L, int mode, int stage);
+__global__ void k_copy(const double *a, double *b, size_t n);
+__global__ void k_restrict_u(LevelView C, LevelView F);
+__global__ void k_restrict_state(Params P, LevelView C, LevelView F);
+__global__ void k_restrict_incr(Params P, LevelView C, LevelView F);
+__global__ void k_prolong_coarse(Params P, LevelView C, LevelView F);
+__global__ void k_prolong_fine(Params P, LevelView C, LevelView F);
+__global__ void k_inject_u(LevelView C, LevelView F);
+__global__ void k_bc_solution(Params P, LevelView L);
+__global__ void k_set_int(int *dst, const int *src);
+__global__ void k_resid_partial(LevelView L, double *part, int nblk);
+__global__ void k_resid_final(const double *part, int nblk, double *out);
+__global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
+                         double ground, double d0, double d1, double d2, double *out);
+
+}  // namespace flite

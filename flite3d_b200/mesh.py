@@ -1,0 +1,186 @@
+"""Meshes and reference file formats (wraps libflite_prepro.so).
+
+A :class:`Mesh` holds the multi-level solver input that gen3d writes to a
+``.sol`` file (PreProSource/gen3d_grid.f90:4082-5231) and hands the
+solver one :class:`~flite3d_b200._abi.LevelDesc` per level, exactly the
+arrays readGridComputationData reads (SolverSource/mgnsg3d_def_par.F90:
+13812-14074).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+_c_double = ctypes.c_double
+
+
+def _lib():
+    return _abi.prepro_lib()
+
+
+class Mesh:
+    """Multi-level mesh owned by the preprocessor library."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle) if not isinstance(handle, ctypes.c_void_p) else handle
+        self.nlevels = _lib().fp_num_levels(self._h)
+        self._descs = (_abi.LevelDesc * self.nlevels)()
+        for level in range(self.nlevels):
+            _abi.check(_lib().fp_level_desc(self._h, level + 1, ctypes.byref(self._descs[level])),
+                       "fp_level_desc")
+
+    # ---- construction -------------------------------------------------
+    @classmethod
+    def bump_channel(cls, nx, ny, nz, bump_height=0.05, nlevels=3):
+        """Bump channel [0,3]x[0,1]x[0,1], nx*ny*nz hexes split into 6 tets."""
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_bump_channel(int(nx), int(ny), int(nz), _c_double(bump_height),
+                                          int(nlevels), ctypes.byref(h)), "fp_bump_channel")
+        return cls(h)
+
+    @classmethod
+    def from_tets(cls, xyz, tets, tris, tri_indicator, nlevels=3):
+        """xyz (N,3), tets (T,4), tris (F,3) 1-based, indicators (F,) in 1..9."""
+        xyz = np.asfortranarray(np.asarray(xyz, dtype=np.float64))
+        tets = np.asfortranarray(np.asarray(tets, dtype=np.int32))
+        tris = np.asfortranarray(np.asarray(tris, dtype=np.int32))
+        ind = np.ascontiguousarray(np.asarray(tri_indicator, dtype=np.int32))
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_from_tets(
+            xyz.shape[0], xyz.ctypes.data_as(ctypes.c_void_p), tets.shape[0],
+            tets.ctypes.data_as(ctypes.c_void_p), tris.shape[0],
+            tris.ctypes.data_as(ctypes.c_void_p), ind.ctypes.data_as(ctypes.c_void_p),
+            int(nlevels), ctypes.byref(h)), "fp_from_tets")
+        return cls(h)
+
+    @classmethod
+    def read_sol(cls, path):
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_read_sol(str(path).encode(), ctypes.byref(h)), "fp_read_sol")
+        return cls(h)
+
+    def write_sol(self, path):
+        _abi.check(_lib().fp_write_sol(self._h, str(path).encode()), "fp_write_sol")
+
+    def write_plt(self, path):
+        _abi.check(_lib().fp_write_plt(self._h, str(path).encode()), "fp_write_plt")
+
+    def write_plotreg(self, path):
+        _abi.check(_lib().fp_write_plotreg(self._h, str(path).encode()), "fp_write_plotreg")
+
+    def close(self):
+        if self._h:
+            _lib().fp_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- access --------------------------------------------------------
+    @property
+    def descs(self):
+        return self._descs
+
+    def level(self, level):
+        return self._descs[level - 1]
+
+    def sizes(self, level=1):
+        d = self.level(level)
+        return dict(nodes=d.n_nodes, sides=d.n_sides, bsides=d.n_bsides, bnodes=d.n_bnodes)
+
+    def check(self, level=1):
+        closure, vol = _c_double(), _c_double()
+        _abi.check(_lib().fp_check(self._h, level, ctypes.byref(closure), ctypes.byref(vol)),
+                   "fp_check")
+        return closure.value, vol.value
+
+    def array(self, level, name):
+        """Copy of one level array as numpy (column-major fields as (k, n))."""
+        d = self.level(level)
+        n, e, b = d.n_nodes, d.n_sides, d.n_bsides
+        spec = {
+            "side_idx": (d.side_idx, np.int32, (2, e)), "side_w": (d.side_w, np.float64, (3, e)),
+            "side_len": (d.side_len, np.float64, (e,)), "bnd_idx": (d.bnd_idx, np.int32, (3, b)),
+            "bnd_w": (d.bnd_w, np.float64, (3, b)), "node_reg": (d.node_reg, np.int32, (21,)),
+            "node_ind": (d.node_ind, np.int32, (d.n_normals,)),
+            "volume": (d.volume, np.float64, (n,)), "wall_dist": (d.wall_dist, np.float64, (n,)),
+            "coords": (d.coords, np.float64, (3, n)),
+        }
+        if level > 1:
+            nf = self.level(level - 1).n_nodes
+            spec["parent"] = (d.parent, np.int32, (nf,))
+            spec["rweight"] = (d.rweight, np.float64, (nf,))
+        ptr, dt, shape = spec[name]
+        if not ptr:
+            return None
+        count = int(np.prod(shape))
+        ctype = ctypes.c_int32 if dt == np.int32 else ctypes.c_double
+        buf = (ctype * count).from_address(ptr)
+        return np.frombuffer(buf, dtype=dt, count=count).reshape(shape).copy()
+
+
+# ---- restart / result files ---------------------------------------------
+
+def write_rst(path, prim):
+    """prim: (nvar, N) primitive rho, u, v, w, E/rho [, nu] (def_par:3740-3873)."""
+    prim = np.ascontiguousarray(prim, dtype=np.float64)
+    nvar, n = prim.shape
+    _abi.check(_lib().fp_write_rst(str(path).encode(), n, nvar, prim.ctypes.data_as(ctypes.c_void_p)),
+               "fp_write_rst")
+
+
+def read_rst(path, n, nvar=5):
+    out = np.zeros((nvar, n))
+    _abi.check(_lib().fp_read_rst(str(path).encode(), n, nvar, out.ctypes.data_as(ctypes.c_void_p)),
+               "fp_read_rst")
+    return out
+
+
+def write_res(path, u):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    nvar, n = u.shape
+    _abi.check(_lib().fp_write_res(str(path).encode(), n, nvar, u.ctypes.data_as(ctypes.c_void_p)),
+               "fp_write_res")
+
+
+def write_unk(path, u):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    nvar, n = u.shape
+    _abi.check(_lib().fp_write_unk(str(path).encode(), n, nvar, u.ctypes.data_as(ctypes.c_void_p)),
+               "fp_write_unk")
+
+
+def read_unk(path, n, nvar=5):
+    out = np.zeros((nvar, n))
+    _abi.check(_lib().fp_read_unk(str(path).encode(), n, nvar, out.ctypes.data_as(ctypes.c_void_p)),
+               "fp_read_unk")
+    return out
+
+
+def primitive_to_conserved(prim):
+    """The restart conversion u(2:5) = rho*u(2:5) (def_par:3850-3856)."""
+    prim = np.asarray(prim, dtype=np.float64)
+    u = prim.copy()
+    u[1:5] = prim[0] * prim[1:5]
+    return u
+
+
+def splitmix64(seed, n):
+    """First n outputs of the SplitMix64 generator (public-domain method by
+    S. Vigna): state_i = seed + i*0x9E3779B97F4A7C15, then the mix."""
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) + np.arange(1, n + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+        z = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def density_perturbation(n, seed=20261203, amplitude=0.01):
+    """delta_i uniform on [-amplitude, amplitude] from SplitMix64 in file order."""
+    bits = splitmix64(seed, n) >> np.uint64(11)
+    u01 = bits.astype(np.float64) / float(1 << 53)
+    return amplitude * (2.0 * u01 - 1.0)

@@ -1,0 +1,217 @@
+"""Solver host mirror over the C ABI (include/flite_gpu.h).
+
+:class:`Solver` holds one device context.  Its methods are the reference's
+module calls from the multigrid driver into the grid solver
+(SolverSource/mgnsg3d_mg_par.F90 into mgnsg3d_def_par.F90), one for one.
+:func:`run_steady` restates the steady convergence loop of multiGridCycles
+(mg_par:459-905): cycles until log10(res1/res1_first) <= -orders or
+maximumnumberofcycles.
+
+The product path is the CUDA library: constructing a Solver raises when
+libflite_gpu.so is missing or no CUDA device is present; there is no CPU
+fallback.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _abi
+from .mesh import Mesh
+
+_vp = ctypes.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_vp)
+
+
+def default_controls(**overrides):
+    """Reference defaults (def_par:217-378) with keyword overrides applied,
+    then the post-read derivation (def_par:387-415)."""
+    lib = _abi.gpu_lib()
+    c = _abi.Controls()
+    _abi.check(lib.flite_controls_default(ctypes.byref(c)), "flite_controls_default")
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise KeyError(f"unknown control {k}")
+        setattr(c, k, v)
+    _abi.check(lib.flite_controls_derive(ctypes.byref(c)), "flite_controls_derive")
+    return c
+
+
+def controls_from_inp(path_or_text, **overrides):
+    """Defaults, then the &InputVariables deck, then overrides, then derive."""
+    lib = _abi.gpu_lib()
+    pre = _abi.prepro_lib()
+    c = _abi.Controls()
+    _abi.check(lib.flite_controls_default(ctypes.byref(c)), "flite_controls_default")
+    unk = ctypes.create_string_buffer(4096)
+    text = str(path_or_text)
+    if "&" in text:
+        rc = pre.fp_parse_inp_text(text.encode(), ctypes.byref(c), unk, len(unk))
+    else:
+        rc = pre.fp_read_inp(text.encode(), ctypes.byref(c), unk, len(unk))
+    _abi.check(rc, "namelist read")
+    for k, v in overrides.items():
+        setattr(c, k, v)
+    _abi.check(lib.flite_controls_derive(ctypes.byref(c)), "flite_controls_derive")
+    return c, [u for u in unk.value.decode().split(",") if u]
+
+
+class Backend:
+    """A set of entry points with the flite_* signatures (the GPU library) or
+    the same signatures under another prefix (the CPU checker)."""
+
+    def __init__(self, lib, prefix):
+        self.lib, self.prefix = lib, prefix
+
+    def __getattr__(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+
+class Solver:
+    def __init__(self, controls, mesh: Mesh, backend=None):
+        self.c = controls
+        self.mesh = mesh
+        self.be = backend or Backend(_abi.gpu_lib(), "flite_")
+        self._h = _vp()
+        rc = self.be.create(ctypes.byref(controls), mesh.nlevels, mesh.descs, ctypes.byref(self._h))
+        if rc != _abi.FLITE_OK:
+            raise RuntimeError(f"create failed with status {rc}")
+        ng = mesh.nlevels
+        if controls.numberOfGridsToUse > 0:
+            ng = min(ng, controls.numberOfGridsToUse)
+        self.nlevels = ng
+        self.nodes = [mesh.level(l + 1).n_nodes for l in range(ng)]
+
+    def _err(self):
+        if not hasattr(self.be.lib, self.be.prefix + "last_error"):
+            return None
+        buf = ctypes.create_string_buffer(1024)
+        self.be.last_error(self._h, buf, len(buf))
+        return buf.value.decode()
+
+    def _ck(self, rc, what):
+        if rc != _abi.FLITE_OK:
+            raise RuntimeError(f"{what} failed with status {rc}: {self._err()}")
+
+    def close(self):
+        if self._h:
+            self.be.destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state -------------------------------------------------------------
+    def set_state(self, u, level=1):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.shape == (5, self.nodes[level - 1])
+        self._ck(self.be.set_state(self._h, level, _ptr(u)), "set_state")
+
+    def get_state(self, level=1):
+        u = np.zeros((5, self.nodes[level - 1]))
+        self._ck(self.be.get_state(self._h, level, _ptr(u)), "get_state")
+        return u
+
+    def get_pressure(self, level=1):
+        p = np.zeros(self.nodes[level - 1])
+        self._ck(self.be.get_pressure(self._h, level, _ptr(p)), "get_pressure")
+        return p
+
+    def init_freestream(self):
+        self._ck(self.be.init_freestream(self._h), "init_freestream")
+
+    def start(self):
+        self._ck(self.be.start(self._h), "start")
+
+    # ---- solver calls ------------------------------------------------------
+    def do_time_iterations(self, level, nsteps=1, calc_diss=True, cycle=1):
+        self._ck(self.be.do_time_iterations(self._h, level, nsteps, int(calc_diss), 0, cycle),
+                 "do_time_iterations")
+
+    def restrict(self, fine_level):
+        self._ck(self.be.restrict(self._h, fine_level, 0), "restrict")
+
+    def prolong(self, coarse_level):
+        self._ck(self.be.prolong(self._h, coarse_level), "prolong")
+
+    def cycle(self, cycle_no):
+        self._ck(self.be.cycle(self._h, cycle_no), "cycle")
+
+    def residuals(self):
+        res = (ctypes.c_double * 7)()
+        mres = (ctypes.c_double * 7)()
+        mind = (ctypes.c_int32 * 7)()
+        rc = self.be.residuals(self._h, res, mres, mind)
+        if rc == _abi.FLITE_ENAN:
+            raise FloatingPointError("NaN in residual")
+        self._ck(rc, "residuals")
+        return np.array(res[:5]), np.array(mres[:5]), np.array(mind[:5])
+
+    def forces(self):
+        out = (ctypes.c_double * 6)()
+        self._ck(self.be.forces(self._h, out), "forces")
+        return np.array(out[:])
+
+    def residual_fwd(self, u, level=1):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        r = np.zeros_like(u)
+        self._ck(self.be.residual_fwd(self._h, level, _ptr(u), _ptr(r)), "residual_fwd")
+        return r
+
+    def time_cycles(self, ncycles, cycle_no=1):
+        ms = ctypes.c_double()
+        self._ck(self.be.time_cycles(self._h, cycle_no, ncycles, ctypes.byref(ms)), "time_cycles")
+        return ms.value
+
+    def cycle_launches(self):
+        n = ctypes.c_int64()
+        self._ck(self.be.cycle_launches(self._h, ctypes.byref(n)), "cycle_launches")
+        return n.value
+
+    def profile_level(self, level=1, reps=10):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.be.profile_level(self._h, level, reps, ctypes.byref(a), ctypes.byref(b)),
+                 "profile_level")
+        return a.value, b.value
+
+
+def initial_state(controls, mesh, perturb_seed=None, amplitude=0.01):
+    """Freestream state of level 1 as conserved variables; with a seed the
+    density gets the seeded +-amplitude perturbation in primitive form (the
+    velocity and E/rho stay at freestream), as a restart file would carry."""
+    from .mesh import density_perturbation, primitive_to_conserved
+    n = mesh.level(1).n_nodes
+    inf = list(controls.inflowField)
+    prim = np.empty((5, n))
+    for k in range(5):
+        prim[k] = inf[k]
+    prim[0] = inf[0]
+    if perturb_seed is not None:
+        prim[0] = inf[0] * (1.0 + density_perturbation(n, perturb_seed, amplitude))
+    return primitive_to_conserved(prim)
+
+
+def run_steady(solver, orders=8.0, max_cycles=1000, callback=None):
+    """Convergence loop of multiGridCycles (mg_par:789-816): cycles until
+    log(res0)-log(res) >= orders*log(10) or max_cycles.  Returns the history
+    of (cycle, res1, lift, drag)."""
+    hist = []
+    res0 = None
+    for it in range(1, max_cycles + 1):
+        solver.cycle(it)
+        res, _, _ = solver.residuals()
+        f = solver.forces()
+        if res0 is None:
+            res0 = res[0]
+        hist.append((it, res[0], f[0], f[1]))
+        if callback:
+            callback(it, res, f)
+        if not (math.log(res0) - math.log(res[0]) < math.log(10.0) * orders):
+            break
+    return hist

@@ -1,0 +1,194 @@
+/*
+ * flite_gpu.h -- C ABI of the B200 (sm_100a) flow-solver hot path.
+ *
+ * The Fortran solver host (SolverSource/mgnsg3d_mg_par.F90) drives the grid
+ * solver module GridSolver (SolverSource/mgnsg3d_def_par.F90) through a small
+ * set of module calls.  Each entry point below replaces one of those calls one
+ * for one; the reference routine it replaces is cited beside it.  All arrays
+ * cross the boundary as plain host pointers in the reference's own layout
+ * (Fortran column-major, 1-based node indices), so a Fortran host can bind them
+ * with ISO_C_BINDING without copies or reshapes.
+ *
+ * Every function returns an int status (FLITE_OK on success).  The reference
+ * STOPs on errors; this library returns a code and keeps a message that
+ * flite_last_error() retrieves.
+ */
+#ifndef FLITE_GPU_H
+#define FLITE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define FLITE_OK            0
+#define FLITE_EINVAL        1   /* bad argument, inconsistent mesh arrays   */
+#define FLITE_EUNSUPPORTED  2   /* control value outside the supported path */
+#define FLITE_ENAN          3   /* non-finite residual (mg_par:1464-1470)   */
+#define FLITE_ETIMEOUT      4   /* a bounded device wait expired            */
+#define FLITE_ECUDA         5   /* CUDA runtime error                       */
+#define FLITE_ENOMEM        6   /* device allocation failed                 */
+#define FLITE_EIO           7   /* file format / record error               */
+
+/* ---- precision modes --------------------------------------------------- */
+#define FLITE_FP64   0   /* every kernel in double precision                  */
+#define FLITE_MIXED  1   /* FP32 fluxes/gradients/stages, FP64 accumulation   */
+
+/*
+ * Controls: a POD mirror of the InputVariablesData fields the hot path reads
+ * (SolverSource/mgnsg3d_def_par.F90:64-196).  flite_controls_default() sets the
+ * reference defaults (def_par:217-378); flite_controls_derive() applies the
+ * post-read overrides and the freestream state (def_par:387-415).  Logical
+ * fields are ints (0 = .false.).
+ */
+typedef struct flite_controls {
+    /* freestream and physics */
+    double MachNumber, alpha, beta, ReynoldsNumber, PrandtlNumber, gamma;
+    double inflowTemperature, wallTemperature;
+    int    wallsAreIsentropic;
+    int    fluxType;            /* 1 central, 2 LLF, 3 Roe, 4 HLLC            */
+    int    HLLCFluxOrder;
+    double HLLCClipping;
+    int    Automaticlipping;
+    int    GradientMethod;      /* 1 Galerkin, else least squares            */
+    int    dissipationScheme, coarseGridDissipationScheme;
+    double secondOrderDissipationFactor, fourthOrderDissipationFactor;
+    double coarseGridDissipationFactor;
+    int    useMatrixDissipation;
+    double HartensCorrectionFactor;
+    int    useDissipationWeighting;
+    int    viscosityScheme;
+    int    boundaryTerm;
+    /* time stepping and multigrid */
+    double CFLNumber, turbulentCFLNumber, turbK, maxIncrementFactor, minimumDensity;
+    int    multigridScheme, numberOfRelaxationSteps, numberOfGridsToUse;
+    double multigridBCRelaxation, prolongationRelaxation, turbProlongationRelaxation;
+    int    prolongationMappingScheme;
+    int    numberOfMGIterations, maximumnumberofcycles, writeToFileInterval;
+    double initialResidual;
+    int    numberOfCFLIncrements;
+    /* turbulence and bookkeeping */
+    int    turbulenceModel, numberOfTurbulenceGrids, numberOfTurbulenceSteps;
+    double tripFactor, triggerRadius, turbulenceTriggerValue;
+    int    numberOfTriggerSteps;
+    double maxTurbulenceValue, turbulentPrandtlNumber;
+    double referenceArea, datum[3], groundplane;
+    int    forceCalcType, restartNumber, numberOfProcesses;
+    /* controls the path rejects unless they hold their steady default */
+    int    flowType, explicit_, SAS, GUSTMODEL, movingwall, patchInitialization, nspan;
+    int    timeScheme, numberOfRSSteps, numberOfPSSteps;
+    double residualSmoothingFactor, prolongationSmoothingFactor, physicalTimeStep;
+    double engineBCRelaxation;
+    /* derived: inflowField(1:6, 1:2) stored column-major as in def_par:88 */
+    double inflowField[12];
+    /* extension controls (no reference counterpart) */
+    int    precision;           /* FLITE_FP64 | FLITE_MIXED                   */
+} flite_controls;
+
+/*
+ * One grid level as read from a gen3d .sol file (readGridComputationData,
+ * def_par:13812-14074).  Pointers are host memory owned by the caller; the
+ * library copies what it needs.  Index arrays are 1-based as in the file.
+ */
+typedef struct flite_level_desc {
+    int32_t n_nodes;            /* N                                          */
+    int32_t n_sides;            /* E interior edges                           */
+    int32_t n_bsides;           /* B boundary edges                           */
+    int32_t n_bnodes;           /* boundary nodes (numbered 1..n_bnodes)      */
+    int32_t n_normals;          /* length of node_ind                         */
+    const int32_t *side_idx;    /* [2][E] sideIndexArray(E,2)                 */
+    const double  *side_w;      /* [3][E] sideWeightsArray(E,3)               */
+    const double  *side_len;    /* [E]    sideLengthArray                     */
+    const int32_t *bnd_idx;     /* [3][B] brp%sideIndexArray(B,3)             */
+    const double  *bnd_w;       /* [3][B] brp%sideWeightsArray(B,3)           */
+    const int32_t *node_reg;    /* [21]   nodeIndicatorRegister(-20:0)        */
+    const int32_t *node_ind;    /* [n_normals] nodeIndicatorArray             */
+    const double  *volume;      /* [N]    nodeVolume                          */
+    const double  *wall_dist;   /* [N]    wallDistance (may be NULL)          */
+    const double  *coords;      /* [3][N] coordinates (level 1; NULL coarse)  */
+    const double  *coord_move;  /* [3][N] coordinateMovement (NULL = zero)    */
+    const int32_t *parent;      /* [N_finer] prolongationArray (levels >= 2)  */
+    const double  *rweight;     /* [N_finer] restrictionArray  (levels >= 2)  */
+} flite_level_desc;
+
+typedef struct flite_ctx flite_ctx;
+
+/* ---- controls --------------------------------------------------------- */
+/* defaults of readInputVariables (def_par:217-378)                        */
+int flite_controls_default(flite_controls *c);
+/* post-read overrides + freestream (def_par:387-415)                      */
+int flite_controls_derive(flite_controls *c);
+
+/* ---- lifecycle -------------------------------------------------------- */
+/* Replaces readComputationData (mg_par:1198-1268) + the allocations of
+ * readGridComputationData and the geometry set-up it performs
+ * (makeBoundaryNormals def_par:15394, makeSurfaceArea :15523, connectivity
+ * count :14262-14275).  Copies every level to the current CUDA device.    */
+int flite_create(const flite_controls *c, int nlevels,
+                 const flite_level_desc *levels, flite_ctx **out);
+int flite_destroy(flite_ctx *ctx);
+int flite_last_error(const flite_ctx *ctx, char *buf, size_t len);
+
+/* ---- state ------------------------------------------------------------ */
+/* u is [nvar][N] column-major conserved variables (grp%u(N,nvar)),        */
+/* nvar = 5 (+1 with Spalart-Allmaras).                                    */
+int flite_set_state(flite_ctx *ctx, int level, const double *u);
+int flite_get_state(flite_ctx *ctx, int level, double *u);
+int flite_get_pressure(flite_ctx *ctx, int level, double *p);
+/* Freestream start-up: setUpInitialField2 freestream branch (def_par:
+ * 3878-3996) on level 1.  The restart branch (:3740-3873) is the host
+ * reading .rst, converting to conserved and calling flite_set_state, then
+ * flite_start.                                                             */
+int flite_init_freestream(flite_ctx *ctx);
+/* The start-up tail shared by both branches: makePressureField +
+ * setBCsOnSolutionField on level 1 (def_par:3992-3994), laminar viscosity
+ * and restriction of u to every coarse level (mg_par:586-602).             */
+int flite_start(flite_ctx *ctx);
+
+/* ---- solver steps (one per replaced Fortran call) --------------------- */
+/* doTimeIterations (def_par:966-1000)                                     */
+int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps,
+                             int calc_diss, int calc_turb, int cycle_no);
+/* restrictGrid (def_par:12141-12430)                                      */
+int flite_restrict(flite_ctx *ctx, int fine_level, int calc_turb);
+/* prolongateGrid (def_par:12432-12570)                                    */
+int flite_prolong(flite_ctx *ctx, int coarse_level);
+/* mapFineToCoarse of the solution (def_par:12572-12679)                   */
+int flite_map_fine_to_coarse(flite_ctx *ctx, int fine_level);
+/* oneCycle (mg_par:907-1196), every kernel on the device                  */
+int flite_cycle(flite_ctx *ctx, int cycle_no);
+/* residual norms of writeResiduals (mg_par:1271-1516): res_k = sqrt(sum
+ * (u-uprev)^2) on level 1, max |u-uprev| and its 1-based node.  Returns
+ * FLITE_ENAN when any res_k is not finite (the reference STOPs).          */
+int flite_residuals(flite_ctx *ctx, double res[7], double maxres[7],
+                    int32_t maxind[7]);
+/* calculateLiftAndDrag (def_par:14710-14870): out = {lift, drag, latF,
+ * frictionDrag, latM, longM} as coefficients.                              */
+int flite_forces(flite_ctx *ctx, double out[6]);
+
+/* ---- one residual evaluation (adjoint primal / parity probe) ----------- */
+/* rhs = makeRHS(u) on a level (def_par:1525-2590) with the level's current
+ * pressure recomputed from u; r is [5][N].                                 */
+int flite_residual_fwd(flite_ctx *ctx, int level, const double *u, double *r);
+
+/* ---- timing ----------------------------------------------------------- */
+/* Capture one oneCycle as a CUDA graph and replay it `ncycles` times;
+ * returns the device time (ms) measured with CUDA events on the context's
+ * stream.  cycle numbers only affect numberOfCFLIncrements ramps and are
+ * frozen at cycle_no inside the graph.                                     */
+int flite_time_cycles(flite_ctx *ctx, int cycle_no, int ncycles, double *ms);
+/* Number of kernel launches one oneCycle issues (for launch accounting).  */
+int flite_cycle_launches(flite_ctx *ctx, int64_t *n);
+/* Kernel-level timing of the dominant kernel (edge flux + gather) over one
+ * relaxation of level 1: average ms per launch of the edge-flux kernel and
+ * of the node gather/update kernel.                                        */
+int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms,
+                        double *node_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLITE_GPU_H */

@@ -1,0 +1,78 @@
+/*
+ * flite_prepro.h -- C ABI of the host-side preprocessor and file formats.
+ *
+ * The reference builds its solver input with the separate gen3d executable
+ * (PreProSource/*.f90) and reads/writes Fortran sequential-unformatted files.
+ * This library restates gen3d's tetrahedral path (median-dual edge and
+ * boundary coefficients, boundary-first numbering, node indicators, greedy
+ * agglomeration) for synthetic meshes and reads/writes the reference's
+ * formats: .sol (multi-level solver input), .rst (restart), .res (result),
+ * .unk (merged result), plotreg.reg and .plt.  It also parses the NAMELIST
+ * subset of the run deck (&InputVariables ivd%... = ...).
+ */
+#ifndef FLITE_PREPRO_H
+#define FLITE_PREPRO_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "flite_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fp_mesh fp_mesh;
+
+/* Bump channel [0,3]x[0,1]x[0,1]: nx*ny*nz hexes, each split into 6 tets
+ * (Kuhn split), lower wall lifted by bump_h*sin^2(pi(x-1)) on x in [1,2].
+ * Surfaces: z=0 wall (indicator 1), z=1/y=0/y=1 symmetry (2), x=0/x=3 far
+ * field (3).  nlevels agglomerated levels are built.                       */
+int fp_bump_channel(int nx, int ny, int nz, double bump_h, int nlevels,
+                    fp_mesh **out);
+/* General tetrahedral input (the .plt content): coordinates [3][n] column
+ * major, tets [4][ntet] 1-based, boundary triangles [3][ntri] 1-based and a
+ * per-triangle boundary indicator (1..9).                                  */
+int fp_from_tets(int32_t nnodes, const double *xyz, int32_t ntet,
+                 const int32_t *tets, int32_t ntri, const int32_t *tris,
+                 const int32_t *tri_ind, int nlevels, fp_mesh **out);
+int fp_free(fp_mesh *m);
+
+int fp_num_levels(const fp_mesh *m);
+/* Fill a level descriptor whose pointers stay valid while m lives.        */
+int fp_level_desc(const fp_mesh *m, int level, flite_level_desc *out);
+/* Coordinates of level 1 in original (generator) numbering are permuted to
+ * boundary-first numbering; perm[new-1] = old (1-based), length N.         */
+int fp_node_perm(const fp_mesh *m, int32_t *perm);
+/* Max closure error |sum_j +-w_ij + 2 sum_b w_b| over nodes, relative to
+ * max |w| (def_par:14430-14568), and total volume.                         */
+int fp_check(const fp_mesh *m, int level, double *closure, double *volume);
+
+/* ---- files (Fortran sequential unformatted, 4-byte record markers) ---- */
+int fp_write_sol(const fp_mesh *m, const char *path);
+int fp_read_sol(const char *path, fp_mesh **out);
+/* .rst: N; then rho, u, v, w, E/rho [, nu] column-major (def_par:3740-3873) */
+int fp_write_rst(const char *path, int32_t n, int nvar, const double *prim);
+int fp_read_rst(const char *path, int32_t n, int nvar, double *prim);
+/* .res: N; rho, (u_j/rho) j=2..nvar from conserved u (def_par:15315-15346) */
+int fp_write_res(const char *path, int32_t n, int nvar, const double *u);
+/* .unk: N_global; u(N,nvar) as stored (mg_par:1698-1700)                   */
+int fp_write_unk(const char *path, int32_t n, int nvar, const double *u);
+int fp_read_unk(const char *path, int32_t n, int nvar, double *u);
+/* plotreg.reg for one domain: (N,1); N; N x (local, global)              */
+int fp_write_plotreg(const fp_mesh *m, const char *path);
+/* .plt (tet form, gen3d_generator.f90:377-389): (nEl,N,nBF); iel(4,nEl);
+ * x(3,N); iface(5,nBF) with column 5 the surface (indicator) number.       */
+int fp_write_plt(const fp_mesh *m, const char *path);
+
+/* ---- controls deck -------------------------------------------------- */
+/* Parse "&InputVariables ivd%key = value, ... /" onto c (which should hold
+ * defaults).  Unknown keys are listed (comma separated) in unknown.         */
+int fp_read_inp(const char *path, flite_controls *c, char *unknown,
+                size_t unknown_len);
+int fp_parse_inp_text(const char *text, flite_controls *c, char *unknown,
+                      size_t unknown_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

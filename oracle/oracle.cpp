@@ -1,0 +1,1257 @@
+// CPU restatement of the reference flow solver -- test infrastructure only.
+//
+// Every routine below restates the Fortran routine cited beside it, in the
+// same operation order: the same edge-order scatter, left-to-right
+// evaluation of every expression, and no fused multiply-add (this file is
+// compiled with -ffp-contract=off).  The shared nodeHelpArray of the
+// reference (one array for all levels, def_par:14231) is kept shared here
+// too, so any state that would leak between levels in the reference leaks
+// the same way here.
+//
+// Pinned choices where the reference reads undefined values (each is also
+// listed in DESIGN.md):
+//  * Roe and LLF read rho1/rho2/h1/h2 that the interior loop never sets
+//    (def_par:1682,1693,1738,1748,1760): rho = r and h = (E+p)/rho.
+//  * LLF/Roe leave f unchanged when |w| <= 1e-10 (def_par:1672,1727),
+//    i.e. the previous edge's flux is added again: pinned to f = 0.
+//  * nullifyOuterBoundary declares its own uninitialised ivd (def_par:4259):
+//    a no-op for turbulenceModel 0, components 1..6 zeroed for SA.
+//  * numberOfIONodes is never set (makeIORegister is commented out,
+//    mg_par:1248,1262): pinned to 0.
+//  * coarse-level coordinates are allocated but never filled
+//    (def_par:14002-14011,14071): pinned to 0.
+//  * the cycle number of a coarse level before its first relaxation is 0.
+//  * the LED limiter's (1+t^nsig)^(1/nsig) (def_par:1861) is evaluated as
+//    sqrt(sqrt(1+(t*t)*(t*t))) for nsig=4 and sqrt(1+t*t) for nsig=2.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+using vec = std::vector<double>;
+
+struct Level {
+    int N = 0, E = 0, B = 0, Nb = 0, nnorm = 0, grid = 1;
+    std::vector<int> s1, s2;  // 0-based
+    vec wx, wy, wz, slen;
+    std::vector<int> b1, b2, bind;
+    vec bwx, bwy, bwz;
+    int reg[21];
+    std::vector<int> node_ind;  // 0-based node numbers
+    vec V, wdist, cx, cy, cz, cmx, cmy, cmz;
+    std::vector<int> parent;  // [N_finer], 0-based coarse node or -1
+    vec rweight;
+    // state
+    vec u[6], uprev[6], rhs[6], src[6], diss[5];
+    vec p, dt, mu, conn, wallArea, nx, ny, nz, wallStress[3];
+    int cycleNumber = 0;
+    int R(int i) const { return reg[i + 20]; }  // nodeIndicatorRegister(i)
+};
+
+struct Oracle {
+    flite_controls c;
+    std::vector<Level> lv;
+    int nvar = 5;
+    std::vector<vec> nh;  // nodeHelpArray(:,1:25), sized for level 1
+    double RK[3] = {0.6, 0.6, 1.0};  // def_par:14240-14244
+
+    // ---- makePressureField (def_par:13612-13630) --------------------------
+    void makePressureField(Level &g, vec *u) {
+        const double gm1 = c.gamma - 1.0;
+        for (int i = 0; i < g.N; ++i) {
+            double pp = gm1 * (u[4][i] - 0.5 * ((u[1][i] * u[1][i] + u[2][i] * u[2][i]) + u[3][i] * u[3][i]) / u[0][i]);
+            g.p[i] = std::max(pp, 0.1);
+        }
+    }
+
+    // ---- makeTimeSteps (def_par:13335-13610) ------------------------------
+    void makeTimeSteps(Level &g) {
+        const double c1 = c.gamma;
+        vec &h1 = nh[0];
+        for (int i = 0; i < g.N; ++i) { g.dt[i] = 0.0; }
+        std::fill(h1.begin(), h1.end(), 0.0);
+        const bool visc = c.ReynoldsNumber > 0.0;
+        const double am = 1.0 / c.ReynoldsNumber;
+        auto visc_of = [&](int i) {
+            if (c.turbulenceModel == 1) return g.mu[i] + g.u[5][i] / c.ReynoldsNumber;
+            return g.mu[i];
+        };
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+            double al = (wx * wx + wy * wy) + wz * wz;
+            double ro1 = 1. / g.u[0][i1], ro2 = 1. / g.u[0][i2];
+            double cc1 = std::max(c1 * g.p[i1] * ro1, 0.001);
+            double cc2 = std::max(c1 * g.p[i2] * ro2, 0.001);
+            double vn1 = ((wx * g.u[1][i1] + wy * g.u[2][i1]) + wz * g.u[3][i1]) * ro1;
+            double vn2 = ((wx * g.u[1][i2] + wy * g.u[2][i2]) + wz * g.u[3][i2]) * ro2;
+            g.dt[i1] = (g.dt[i1] + std::fabs(vn1)) + std::sqrt(cc1 * al);
+            g.dt[i2] = (g.dt[i2] + std::fabs(vn2)) + std::sqrt(cc2 * al);
+            if (visc) {
+                double vis1 = std::max(am, visc_of(i1)), vis2 = std::max(am, visc_of(i2));
+                double dv1 = 2.0 * vis1 * al / g.u[0][i1];
+                double dv2 = 2.0 * vis2 * al / g.u[0][i2];
+                h1[i1] = h1[i1] + dv2;
+                h1[i2] = h1[i2] + dv1;
+            }
+        }
+        for (int b = 0; b < g.B; ++b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double wx = g.bwx[b], wy = g.bwy[b], wz = g.bwz[b];
+            double al = (wx * wx + wy * wy) + wz * wz;
+            double ro1 = 1. / g.u[0][i1], ro2 = 1. / g.u[0][i2];
+            double cc1 = std::max(c1 * g.p[i1] * ro1, 0.001);
+            double cc2 = std::max(c1 * g.p[i2] * ro2, 0.001);
+            double vn1 = ((wx * g.u[1][i1] + wy * g.u[2][i1]) + wz * g.u[3][i1]) * ro1;
+            double vn2 = ((wx * g.u[1][i2] + wy * g.u[2][i2]) + wz * g.u[3][i2]) * ro2;
+            vn1 = std::fabs(vn1); vn2 = std::fabs(vn2);
+            double vnm = vn1 + vn2;
+            cc1 = std::sqrt(cc1 * al); cc2 = std::sqrt(cc2 * al);
+            double ccm = cc1 + cc2;
+            g.dt[i1] = (((g.dt[i1] + vn1) + vnm) + cc1) + ccm;
+            g.dt[i2] = (((g.dt[i2] + vn2) + vnm) + cc2) + ccm;
+            if (visc) {
+                double vis1 = std::max(am, visc_of(i1)), vis2 = std::max(am, visc_of(i2));
+                double dv1 = 2.0 * vis1 * al / g.u[0][i1];
+                double dv2 = 2.0 * vis2 * al / g.u[0][i2];
+                double dvm = dv1 + dv2;
+                h1[i1] = (h1[i1] + dv1) + dvm;
+                h1[i2] = (h1[i2] + dv2) + dvm;
+            }
+        }
+        for (int i = 0; i < g.N; ++i)
+            g.dt[i] = 0.5 / (g.dt[i] / g.V[i] + h1[i] / (g.V[i] * g.V[i]));
+    }
+
+    // ---- makeArtificialDissipation2, scalar form (def_par:11484-11993) ----
+    void makeArtificialDissipation2(Level &g) {
+        for (int k = 0; k < 5; ++k) std::fill(g.diss[k].begin(), g.diss[k].end(), 0.0);
+        for (auto &col : nh) std::fill(col.begin(), col.end(), 0.0);
+        if (c.fluxType == 4 && g.grid == 1) return;
+        if (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0) return;
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double d[5];
+            for (int k = 0; k < 4; ++k) d[k] = g.u[k][i1] - g.u[k][i2];
+            d[4] = ((g.u[4][i1] - g.u[4][i2]) + g.p[i1]) - g.p[i2];
+            double df = 1.0;
+            if (c.useDissipationWeighting) df = 1. / g.slen[e];
+            for (int k = 0; k < 5; ++k) {
+                nh[k][i1] = nh[k][i1] - d[k] * df;
+                nh[k][i2] = nh[k][i2] + d[k] * df;
+            }
+            nh[5][i1] = nh[5][i1] + df;
+            nh[5][i2] = nh[5][i2] + df;
+        }
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double dp = g.p[i1] - g.p[i2], sp = g.p[i1] + g.p[i2];
+            nh[6][i1] = nh[6][i1] - dp;
+            nh[7][i1] = nh[7][i1] + sp;
+            nh[6][i2] = nh[6][i2] + dp;
+            nh[7][i2] = nh[7][i2] + sp;
+        }
+        for (int i = 0; i < g.N; ++i) {
+            double fact = 1. / g.conn[i];
+            nh[8][i] = 12. * std::fabs(nh[6][i] / nh[7][i]);
+            for (int k = 0; k < 5; ++k) nh[k][i] = fact * nh[k][i];
+        }
+        const double k2 = c.secondOrderDissipationFactor;
+        const double k4 = g.grid == 1 ? c.fourthOrderDissipationFactor : c.coarseGridDissipationFactor;
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double d4v[5], d2v[5];
+            for (int k = 0; k < 5; ++k) d4v[k] = nh[k][i1] - nh[k][i2];
+            for (int k = 0; k < 5; ++k) d2v[k] = g.u[k][i1] - g.u[k][i2];
+            double d0 = std::min(g.V[i1] / g.dt[i1], g.V[i2] / g.dt[i2]) / (g.conn[i1] + g.conn[i2]);
+            double d2 = d0 * k2 * std::max(nh[8][i1], nh[8][i2]);
+            double d4 = d0 * k4;
+            d4 = d4 > d2 ? d4 - d2 : 0.0;  // dim(d4,d2)
+            for (int k = 0; k < 5; ++k) {
+                g.diss[k][i1] = (g.diss[k][i1] - d4v[k] * d4) + d2v[k] * d2;
+                g.diss[k][i2] = (g.diss[k][i2] + d4v[k] * d4) - d2v[k] * d2;
+            }
+        }
+    }
+
+    // ---- makeArtificialDissipation3 (def_par:11995-12139) -----------------
+    void makeArtificialDissipation3(Level &g) {
+        for (int k = 0; k < 5; ++k) std::fill(g.diss[k].begin(), g.diss[k].end(), 0.0);
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double d0 = std::min(g.V[i1] / g.dt[i1], g.V[i2] / g.dt[i2]) / (g.conn[i1] + g.conn[i2]);
+            double d2 = d0 * c.coarseGridDissipationFactor;
+            for (int k = 0; k < 5; ++k) {
+                double dk = g.u[k][i1] - g.u[k][i2];
+                g.diss[k][i1] = g.diss[k][i1] + dk * d2;
+                g.diss[k][i2] = g.diss[k][i2] - dk * d2;
+            }
+        }
+    }
+
+    // ---- computeGradient, Galerkin (def_par:2923-3245) --------------------
+    void computeGradient(Level &g, vec *u) {
+        for (int k = 0; k < 15; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double w[3] = {g.wx[e], g.wy[e], g.wz[e]};
+            double r1 = u[0][i1], q1[5] = {r1, u[1][i1] / r1, u[2][i1] / r1, u[3][i1] / r1, u[4][i1]};
+            double r2 = u[0][i2], q2[5] = {r2, u[1][i2] / r2, u[2][i2] / r2, u[3][i2] / r2, u[4][i2]};
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 5; ++k) {
+                    double dq = (q1[k] + q2[k]) * w[a];
+                    nh[a * 5 + k][i1] = nh[a * 5 + k][i1] + dq;
+                    nh[a * 5 + k][i2] = nh[a * 5 + k][i2] - dq;
+                }
+        }
+        for (int b = 0; b < g.B; ++b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
+            double r1 = u[0][i1], q1[5] = {r1, u[1][i1] / r1, u[2][i1] / r1, u[3][i1] / r1, u[4][i1]};
+            double r2 = u[0][i2], q2[5] = {r2, u[1][i2] / r2, u[2][i2] / r2, u[3][i2] / r2, u[4][i2]};
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 5; ++k) {
+                    double s = q1[k] + q2[k];
+                    nh[a * 5 + k][i1] = nh[a * 5 + k][i1] + (2. * q1[k] + s) * w[a];
+                }
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 5; ++k) {
+                    double s = q1[k] + q2[k];
+                    nh[a * 5 + k][i2] = nh[a * 5 + k][i2] + (2. * q2[k] + s) * w[a];
+                }
+        }
+        for (int i = 0; i < g.N; ++i) {
+            double vt = 1. / g.V[i];
+            for (int k = 0; k < 15; ++k) nh[k][i] = nh[k][i] * vt;
+        }
+    }
+
+    // ---- LocalMinMax (def_par:3248-3459) ----------------------------------
+    void LocalMinMax(Level &g) {
+        for (int k = 15; k < 25; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 1.0e15);
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double r1 = g.u[0][i1], q1[5] = {r1, g.u[1][i1] / r1, g.u[2][i1] / r1, g.u[3][i1] / r1, g.u[4][i1]};
+            double r2 = g.u[0][i2], q2[5] = {r2, g.u[1][i2] / r2, g.u[2][i2] / r2, g.u[3][i2] / r2, g.u[4][i2]};
+            double mn[5], mx[5];
+            for (int k = 0; k < 5; ++k) { mn[k] = std::min(q1[k], q2[k]); mx[k] = std::min(-q1[k], -q2[k]); }
+            for (int k = 0; k < 5; ++k) nh[15 + k][i1] = std::min(nh[15 + k][i1], mn[k]);
+            for (int k = 0; k < 5; ++k) nh[15 + k][i2] = std::min(nh[15 + k][i2], mn[k]);
+            for (int k = 0; k < 5; ++k) nh[20 + k][i1] = std::min(nh[20 + k][i1], mx[k]);
+            for (int k = 0; k < 5; ++k) nh[20 + k][i2] = std::min(nh[20 + k][i2], mx[k]);
+        }
+        for (int i = 0; i < g.N; ++i) {
+            double r = g.u[0][i];
+            double q[5] = {r, g.u[1][i] / r, g.u[2][i] / r, g.u[3][i] / r, g.u[4][i]};
+            for (int k = 0; k < 5; ++k) nh[15 + k][i] = nh[15 + k][i] - q[k];
+            for (int k = 0; k < 5; ++k) nh[20 + k][i] = -nh[20 + k][i] - q[k];
+        }
+    }
+
+    // LED limiter branch of the HLLC reconstruction (def_par:1856-1867)
+    static double led(double a, double bmin, double bmax, int nsig) {
+        double cc = a;
+        double a1 = 2.0 * a;
+        if (a1 > 0.0) {
+            double invmax = 0.0;
+            if (bmax > 0.0) invmax = 1.0 / bmax;
+            double t = a1 * invmax;
+            double tn = nsig == 4 ? (t * t) * (t * t) : t * t;
+            double root = nsig == 4 ? std::sqrt(std::sqrt(1. + tn)) : std::sqrt(1. + tn);
+            cc = 0.5 * bmax * t / root;
+        } else if (a1 < 0.0) {
+            double invmin = 0.0;
+            if (bmin < 0.0) invmin = 1.0 / bmin;
+            double t = a1 * invmin;
+            double tn = nsig == 4 ? (t * t) * (t * t) : t * t;
+            double root = nsig == 4 ? std::sqrt(std::sqrt(1. + tn)) : std::sqrt(1. + tn);
+            cc = 0.5 * bmin * t / root;
+        }
+        return cc;
+    }
+
+    // ---- makeRHS (def_par:1525-2590) --------------------------------------
+    void makeRHS(Level &g) {
+        const double gam = c.gamma, gam1 = c.gamma - 1.0;
+        int hllcflux = 1, autoClip = 0, nsig = 4;
+        double clip = 0;
+        if (c.fluxType == 4) {
+            hllcflux = c.HLLCFluxOrder;
+            clip = c.HLLCClipping;
+            autoClip = c.Automaticlipping;
+            nsig = c.ReynoldsNumber < 1 ? 4 : 2;
+            if (hllcflux > 1) {
+                computeGradient(g, g.u);
+                if (autoClip == 1) LocalMinMax(g);
+            }
+        }
+        for (int e = 0; e < g.E; ++e) {
+            const int i1 = g.s1[e], i2 = g.s2[e];
+            double pr1 = g.p[i1], r1 = g.u[0][i1], rinv1 = 1. / g.u[0][i1];
+            double ru1 = g.u[1][i1], rv1 = g.u[2][i1], rw1 = g.u[3][i1];
+            double u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1;
+            double E1 = g.u[4][i1], rh1 = g.u[4][i1] + pr1;
+            double pr2 = g.p[i2], r2 = g.u[0][i2], rinv2 = 1. / g.u[0][i2];
+            double ru2 = g.u[1][i2], rv2 = g.u[2][i2], rw2 = g.u[3][i2];
+            double u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2;
+            double E2 = g.u[4][i2], rh2 = g.u[4][i2] + pr2;
+            double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+            double f[5] = {0, 0, 0, 0, 0};
+            if (c.fluxType == 1) {
+                f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
+                f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
+                f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
+                f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+                f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+            } else if (c.fluxType == 2) {  // LLF (def_par:1670-1724)
+                double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
+                if (rnorm > 1.0e-10) {
+                    double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+                    double c1 = std::sqrt(gam * pr1 * rinv1);
+                    double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+                    double f11 = r1 * nv1, f21 = pr1 * rnx + ru1 * nv1, f31 = pr1 * rny + rv1 * nv1;
+                    double f41 = pr1 * rnz + rw1 * nv1, f51 = rh1 * nv1;
+                    double c2 = std::sqrt(gam * pr2 * rinv2);
+                    double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+                    double f12 = r2 * nv2, f22 = pr2 * rnx + ru2 * nv2, f32 = pr2 * rny + rv2 * nv2;
+                    double f42 = pr2 * rnz + rw2 * nv2, f52 = rh2 * nv2;
+                    double du[5] = {r1 - r2, ru1 - ru2, rv1 - rv2, rw1 - rw2, E1 - E2};
+                    double l11 = std::fabs(nv1 + c1), l12 = std::fabs(nv2 + c2);
+                    double l1 = l11; if (l1 < l12) l1 = l12;
+                    double l21 = std::fabs(nv1 - c1), l22 = std::fabs(nv2 - c2);
+                    double l2 = l21; if (l2 < l22) l2 = l22;
+                    double lam = l1; if (lam < l2) lam = l2;
+                    f[0] = rnorm * ((f11 + f12) - lam * du[0]);
+                    f[1] = rnorm * ((f21 + f22) - lam * du[1]);
+                    f[2] = rnorm * ((f31 + f32) - lam * du[2]);
+                    f[3] = rnorm * ((f41 + f42) - lam * du[3]);
+                    f[4] = rnorm * ((f51 + f52) - lam * du[4]);
+                }
+            } else if (c.fluxType == 3) {  // Roe (def_par:1725-1792)
+                double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
+                if (rnorm > 1.0e-10) {
+                    double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+                    u1 = ru1 * rinv1; v1 = rv1 * rinv1; w1 = rw1 * rinv1;
+                    double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+                    double f11 = r1 * nv1, f21 = pr1 * rnx + ru1 * nv1, f31 = pr1 * rny + rv1 * nv1;
+                    double f41 = pr1 * rnz + rw1 * nv1, f51 = rh1 * nv1;
+                    double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+                    double f12 = r2 * nv2, f22 = pr2 * rnx + ru2 * nv2, f32 = pr2 * rny + rv2 * nv2;
+                    double f42 = pr2 * rnz + rw2 * nv2, f52 = rh2 * nv2;
+                    double h1 = rh1 * rinv1, h2 = rh2 * rinv2;
+                    double di = std::sqrt(r1 / r2), d1 = 1.0 / (di + 1.0);
+                    double ui = (di * u1 + u2) * d1, vi = (di * v1 + v2) * d1, wi = (di * w1 + w2) * d1;
+                    double hi = (di * h1 + h2) * d1;
+                    double ci2 = gam1 * (hi - 0.5 * ((ui * ui + vi * vi) + wi * wi));
+                    ci2 = std::max(ci2, 1.0e-5);
+                    double ci = std::sqrt(ci2);
+                    double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+                    double ucp = (ui * rnx + vi * rny) + wi * rnz;
+                    double du1 = r1 - r2, du2 = ru1 - ru2, du3 = rv1 - rv2, du4 = rw1 - rw2, du5 = E1 - E2;
+                    double l1 = std::fabs(ucp + ci), l2 = std::fabs(ucp - ci), l3 = std::fabs(ucp);
+                    double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+                    double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+                    double al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+                    double cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+                    double cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+                    f[0] = rnorm * ((f11 + f12) - (l3 * du1 + cc1));
+                    f[1] = rnorm * ((f21 + f22) - ((l3 * du2 + cc1 * ui) + cc2 * rnx));
+                    f[2] = rnorm * ((f31 + f32) - ((l3 * du3 + cc1 * vi) + cc2 * rny));
+                    f[3] = rnorm * ((f41 + f42) - ((l3 * du4 + cc1 * wi) + cc2 * rnz));
+                    f[4] = rnorm * ((f51 + f52) - ((l3 * du5 + cc1 * hi) + cc2 * ucp));
+                }
+            } else {  // HLLC (def_par:1794-2085)
+                // central flux of the unreconstructed states (def_par:1798-
+                // 1802); it stays only if no wave-speed branch applies
+                f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
+                f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
+                f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
+                f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+                f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+                double roe1 = g.u[0][i1], roe2 = g.u[0][i2], re1 = g.u[4][i1], re2 = g.u[4][i2];
+                double wx2 = 2.0 * wx, wy2 = 2.0 * wy, wz2 = 2.0 * wz;
+                double rnorm = std::sqrt((wx2 * wx2 + wy2 * wy2) + wz2 * wz2);
+                double rnorm1 = rnorm;
+                if (rnorm > 0.0) rnorm = 1.0 / rnorm;
+                double rnx = wx2 * rnorm, rny = wy2 * rnorm, rnz = wz2 * rnorm;
+                if (hllcflux > 1) {
+                    double dx = g.cx[i2] - g.cx[i1], dy = g.cy[i2] - g.cy[i1], dz = g.cz[i2] - g.cz[i1];
+                    double hlength = 0.5 * clip * std::sqrt((dx * dx + dy * dy) + dz * dz);
+                    double dpvl[5];
+                    for (int j = 0; j < 5; ++j) {
+                        double dpv1 = 0.5 * ((nh[j][i1] * dx + nh[j + 5][i1] * dy) + nh[j + 10][i1] * dz);
+                        double dpv11 = 0.5 * ((nh[j][i2] * dx + nh[j + 5][i2] * dy) + nh[j + 10][i2] * dz);
+                        if (autoClip == 1) {
+                            dpv1 = led(dpv1, nh[j + 15][i1], nh[j + 20][i1], nsig);
+                            dpv11 = -led(-dpv11, nh[j + 15][i2], nh[j + 20][i2], nsig);
+                        }
+                        double a = dpv1, b = dpv11, cc;
+                        if (a * b <= 0.0) {
+                            cc = 0.0;
+                        } else {
+                            cc = std::fabs(a) <= std::fabs(b) ? a : b;
+                            if (std::fabs(cc) > hlength && hlength > 0.0) cc = hlength * cc / std::fabs(cc);
+                        }
+                        dpvl[j] = cc;
+                    }
+                    if ((roe1 + dpvl[0]) > 0.1) roe1 = roe1 + dpvl[0];
+                    u1 = u1 + dpvl[1]; v1 = v1 + dpvl[2]; w1 = w1 + dpvl[3];
+                    if ((re1 + dpvl[4]) > 0.0001) re1 = re1 + dpvl[4];
+                    pr1 = gam1 * (re1 - 0.5 * ((u1 * u1 + v1 * v1) + w1 * w1) * roe1);
+                    pr1 = std::max(pr1, 0.1);
+                    rh1 = re1 + pr1; rinv1 = 1 / roe1;
+                    ru1 = roe1 * u1; rv1 = roe1 * v1; rw1 = roe1 * w1;
+                    if ((roe2 - dpvl[0]) > 0.1) roe2 = roe2 - dpvl[0];
+                    u2 = u2 - dpvl[1]; v2 = v2 - dpvl[2]; w2 = w2 - dpvl[3];
+                    if ((re2 - dpvl[4]) > 0.0001) re2 = re2 - dpvl[4];
+                    pr2 = gam1 * (re2 - 0.5 * ((u2 * u2 + v2 * v2) + w2 * w2) * roe2);
+                    pr2 = std::max(pr2, 0.1);
+                    rh2 = re2 + pr2; rinv2 = 1 / roe2;
+                    ru2 = roe2 * u2; rv2 = roe2 * v2; rw2 = roe2 * w2;
+                }
+                double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+                double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+                double beta0 = std::sqrt(gam1 / (2 * gam));
+                double rroe = std::sqrt(roe2 / roe1);
+                double ut = (u1 + u2 * rroe) / (1 + rroe), vt = (v1 + v2 * rroe) / (1 + rroe);
+                double wt = (w1 + w2 * rroe) / (1 + rroe);
+                double qt = (ut * rnx + vt * rny) + wt * rnz;
+                double ht = (rh1 * rinv1 + rh2 * rinv2 * rroe) / (1 + rroe);
+                double ct = gam1 * (ht - 0.5 * ((ut * ut + vt * vt) + wt * wt));
+                ct = std::sqrt(std::fabs(ct));
+                double c1 = std::sqrt(gam1 * std::fabs(rh1 * rinv1 - 0.5 * ((u1 * u1 + v1 * v1) + w1 * w1)));
+                double c2 = std::sqrt(gam1 * std::fabs(rh2 * rinv2 - 0.5 * ((u2 * u2 + v2 * v2) + w2 * w2)));
+                double sl = std::min(nv1 - beta0 * c1, qt - ct);
+                double sr = std::max(nv2 + beta0 * c2, qt + ct);
+                sl = std::min(sl, nv2 - beta0 * c2);
+                sr = std::max(sr, nv1 + beta0 * c1);
+                double sm = roe2 * nv2 * (sr - nv2) - roe1 * nv1 * (sl - nv1);
+                sm = (sm + pr1) - pr2;
+                double fact = roe2 * (sr - nv2) - roe1 * (sl - nv1);
+                if (fact != 0.0) fact = 1.0 / fact;
+                sm = fact * sm;
+                double fl[5] = {(rnx * ru1 + rny * rv1) + rnz * rw1,
+                                (rnx * (ru1 * u1 + pr1) + rny * (ru1 * v1)) + rnz * (ru1 * w1),
+                                (rnx * (rv1 * u1) + rny * (rv1 * v1 + pr1)) + rnz * (rv1 * w1),
+                                (rnx * (rw1 * u1) + rny * (rw1 * v1)) + rnz * (rw1 * w1 + pr1),
+                                (rnx * (rh1 * u1) + rny * (rh1 * v1)) + rnz * (rh1 * w1)};
+                double fr[5] = {(rnx * ru2 + rny * rv2) + rnz * rw2,
+                                (rnx * (ru2 * u2 + pr2) + rny * (ru2 * v2)) + rnz * (ru2 * w2),
+                                (rnx * (rv2 * u2) + rny * (rv2 * v2 + pr2)) + rnz * (rv2 * w2),
+                                (rnx * (rw2 * u2) + rny * (rw2 * v2)) + rnz * (rw2 * w2 + pr2),
+                                (rnx * (rh2 * u2) + rny * (rh2 * v2)) + rnz * (rh2 * w2)};
+                double pls = roe1 * (nv1 - sl) * (nv1 - sm) + pr1;
+                double prs = roe2 * (nv2 - sr) * (nv2 - sm) + pr2;
+                double ls[5], rs[5];
+                double factl = sl - sm;
+                if (factl != 0.0) {
+                    factl = 1.0 / factl;
+                    ls[0] = roe1 * (sl - nv1) * factl;
+                    ls[1] = ((sl - nv1) * roe1 * u1 + (pls - pr1) * rnx) * factl;
+                    ls[2] = ((sl - nv1) * roe1 * v1 + (pls - pr1) * rny) * factl;
+                    ls[3] = ((sl - nv1) * roe1 * w1 + (pls - pr1) * rnz) * factl;
+                    ls[4] = (((sl - nv1) * re1 - pr1 * nv1) + pls * sm) * factl;
+                } else {
+                    ls[0] = roe1; ls[1] = ru1; ls[2] = rv1; ls[3] = rw1; ls[4] = re1;
+                }
+                double factr = sr - sm;
+                if (factr != 0.0) {
+                    factr = 1.0 / factr;
+                    rs[0] = roe2 * (sr - nv2) * factr;
+                    rs[1] = ((sr - nv2) * roe2 * u2 + (prs - pr2) * rnx) * factr;
+                    rs[2] = ((sr - nv2) * roe2 * v2 + (prs - pr2) * rny) * factr;
+                    rs[3] = ((sr - nv2) * roe2 * w2 + (prs - pr2) * rnz) * factr;
+                    rs[4] = (((sr - nv2) * re2 - pr2 * nv2) + prs * sm) * factr;
+                } else {
+                    rs[0] = roe2; rs[1] = ru2; rs[2] = rv2; rs[3] = rw2; rs[4] = re2;
+                }
+                double L0[5] = {roe1, ru1, rv1, rw1, re1}, R0[5] = {roe2, ru2, rv2, rw2, re2};
+                if (sl > 0.0) {
+                    for (int k = 0; k < 5; ++k) f[k] = fl[k] * rnorm1;
+                } else if (sl <= 0.0 && sm > 0.0) {
+                    for (int k = 0; k < 5; ++k) f[k] = (fl[k] + sl * (ls[k] - L0[k])) * rnorm1;
+                } else if (sm <= 0.0 && sr >= 0.0) {
+                    for (int k = 0; k < 5; ++k) f[k] = (fr[k] + sr * (rs[k] - R0[k])) * rnorm1;
+                } else if (sr < 0.0) {
+                    for (int k = 0; k < 5; ++k) f[k] = fr[k] * rnorm1;
+                }
+            }
+            for (int k = 0; k < 5; ++k) {
+                g.rhs[k][i1] = g.rhs[k][i1] + f[k];
+                g.rhs[k][i2] = g.rhs[k][i2] - f[k];
+            }
+        }
+        // boundary faces (def_par:2116-2512); the GCL terms vanish for the
+        // static meshes this path accepts
+        for (int b = 0; b < g.B; ++b) {
+            const int i1 = g.b1[b], i2 = g.b2[b], ind = g.bind[b];
+            double g1[5], g2[5];
+            boundary_flux(g, i1, i2, ind, g.bwx[b], g.bwy[b], g.bwz[b], g1, g2);
+            for (int k = 0; k < 5; ++k) g.rhs[k][i1] = g.rhs[k][i1] + g1[k];
+            for (int k = 0; k < 5; ++k) g.rhs[k][i2] = g.rhs[k][i2] + g2[k];
+        }
+    }
+
+    // contributions of one boundary edge to its two nodes
+    void boundary_flux(Level &g, int i1, int i2, int ind, double wx, double wy, double wz,
+                       double *g1, double *g2) {
+        const double gam1 = c.gamma - 1.0;
+        for (int k = 0; k < 5; ++k) { g1[k] = 0.0; g2[k] = 0.0; }
+        const bool fe = c.boundaryTerm == 1;
+        if (ind <= 2 || ind == 9) {  // wall or symmetry (def_par:2182-2257)
+            double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
+            if (rnorm > 1.0e-10) {
+                double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+                double F1[5], F2[5];
+                wall_flux(g, i1, rnx, rny, rnz, F1);
+                wall_flux(g, i2, rnx, rny, rnz, F2);
+                for (int k = 0; k < 5; ++k) {
+                    if (fe) { g1[k] = rnorm * (3. * F1[k] + F2[k]); g2[k] = rnorm * (F1[k] + 3. * F2[k]); }
+                    else { g1[k] = rnorm * 4. * F1[k]; g2[k] = rnorm * 4. * F2[k]; }
+                }
+            }
+        } else if (ind <= 4) {  // far field: Roe flux against freestream
+            double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
+            if (rnorm > 1.0e-10) {
+                double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+                const double *inf = &c.inflowField[(ind - 3) * 6];
+                double F1[5], F2[5];
+                farfield_flux(g, i1, rnx, rny, rnz, inf, gam1, F1);
+                farfield_flux(g, i2, rnx, rny, rnz, inf, gam1, F2);
+                for (int k = 0; k < 5; ++k) {
+                    if (fe) { g1[k] = rnorm * (3. * F1[k] + F2[k]); g2[k] = rnorm * (F1[k] + 3. * F2[k]); }
+                    else { g1[k] = rnorm * 4. * F1[k]; g2[k] = rnorm * 4. * F2[k]; }
+                }
+            }
+        } else {  // engine faces: average flux (def_par:2447-2511)
+            double q1[5], q2[5];
+            engine_flux(g, i1, wx, wy, wz, q1);
+            engine_flux(g, i2, wx, wy, wz, q2);
+            for (int k = 0; k < 5; ++k) {
+                double fs = q1[k] + q2[k];
+                g1[k] = fs + 2.0 * q1[k];
+                g2[k] = fs + 2.0 * q2[k];
+            }
+        }
+    }
+
+    void wall_flux(Level &g, int i, double rnx, double rny, double rnz, double *F) {
+        double pr = g.p[i], rho = g.u[0][i], rinv = 1. / rho;
+        double ru = g.u[1][i], rv = g.u[2][i], rw = g.u[3][i], rh = g.u[4][i] + pr;
+        double uu = ru * rinv, vv = rv * rinv, ww = rw * rinv;
+        double nv = (uu * rnx + vv * rny) + ww * rnz;
+        F[0] = rho * nv;
+        F[1] = pr * rnx + rho * uu * nv;
+        F[2] = pr * rny + rho * vv * nv;
+        F[3] = pr * rnz + rho * ww * nv;
+        F[4] = rh * nv;
+    }
+
+    // Roe flux between a node state and the freestream (def_par:2258-2419)
+    void farfield_flux(Level &g, int i, double rnx, double rny, double rnz, const double *inf,
+                       double gam1, double *F) {
+        double ro = inf[0], ro1 = 1. / ro, uo = inf[1], vo = inf[2], wo = inf[3], eo = inf[4], po = inf[5];
+        double prl = g.p[i], rhol = g.u[0][i], rinvl = 1. / rhol;
+        double rul = g.u[1][i], rvl = g.u[2][i], rwl = g.u[3][i], rhl = g.u[4][i] + prl;
+        double ul = rul * rinvl, vl = rvl * rinvl, wl = rwl * rinvl;
+        double epsl = g.u[4][i], hl = rhl * rinvl;
+        double nvl = (ul * rnx + vl * rny) + wl * rnz;
+        double fl1 = rhol * nvl, fl2 = prl * rnx + rhol * ul * nvl, fl3 = prl * rny + rhol * vl * nvl;
+        double fl4 = prl * rnz + rhol * wl * nvl, fl5 = rhl * nvl;
+        double rhor = ro, uxr = uo, vyr = vo, wzr = wo, epsr = eo * ro, presr = po, hr = eo + po * ro1;
+        double unr = (uxr * rnx + vyr * rny) + wzr * rnz;
+        double fr1 = rhor * unr, fr2 = rnx * presr + rhor * uxr * unr, fr3 = rny * presr + rhor * vyr * unr;
+        double fr4 = rnz * presr + rhor * wzr * unr, fr5 = (epsr + presr) * unr;
+        double di = std::sqrt(rhor / rhol), d1 = 1.0 / (di + 1.0);
+        double ui = (di * uxr + ul) * d1, vi = (di * vyr + vl) * d1, wi = (di * wzr + wl) * d1;
+        double hi = (di * hr + hl) * d1;
+        double ci2 = gam1 * (hi - 0.5 * ((ui * ui + vi * vi) + wi * wi));
+        ci2 = std::max(ci2, 1.0e-5);
+        double ci = std::sqrt(ci2);
+        double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+        double ucp = (ui * rnx + vi * rny) + wi * rnz;
+        double du1 = rhor - rhol, du2 = rhor * uxr - rhol * ul, du3 = rhor * vyr - rhol * vl;
+        double du4 = rhor * wzr - rhol * wl, du5 = epsr - epsl;
+        double l1 = std::fabs(ucp + ci), l2 = std::fabs(ucp - ci), l3 = std::fabs(ucp);
+        double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+        double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+        double al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+        double cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+        double cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+        F[0] = 0.5 * (fr1 + fl1) - 0.5 * (l3 * du1 + cc1);
+        F[1] = 0.5 * (fr2 + fl2) - 0.5 * ((l3 * du2 + cc1 * ui) + cc2 * rnx);
+        F[2] = 0.5 * (fr3 + fl3) - 0.5 * ((l3 * du3 + cc1 * vi) + cc2 * rny);
+        F[3] = 0.5 * (fr4 + fl4) - 0.5 * ((l3 * du4 + cc1 * wi) + cc2 * rnz);
+        F[4] = 0.5 * (fr5 + fl5) - 0.5 * ((l3 * du5 + cc1 * hi) + cc2 * ucp);
+    }
+
+    void engine_flux(Level &g, int i, double wx, double wy, double wz, double *F) {
+        double pr = g.p[i], r = g.u[0][i], rinv = 1. / g.u[0][i];
+        double ru = g.u[1][i], rv = g.u[2][i], rw = g.u[3][i];
+        double uu = rinv * ru, vv = rinv * rv, ww = rinv * rw, E = g.u[4][i];
+        double pu = pr * rinv * ru, pv = pr * rinv * rv, pw = pr * rinv * rw;
+        F[0] = (wx * r * uu + wy * r * vv) + wz * r * ww;
+        F[1] = (wx * (ru * uu + pr) + wy * ru * vv) + wz * ru * ww;
+        F[2] = (wx * rv * uu + wy * (rv * vv + pr)) + wz * rv * ww;
+        F[3] = (wx * rw * uu + wy * rw * vv) + wz * (rw * ww + pr);
+        F[4] = (wx * (E * uu + pu) + wy * (E * vv + pv)) + wz * (E * ww + pw);
+    }
+
+    // ---- solveSystem (def_par:1407-1479) ----------------------------------
+    void solveSystem(Level &g, vec *rhs) {
+        for (int i = 0; i < g.N; ++i) {
+            double dt = g.dt[i];
+            for (int k = 0; k < 5; ++k) rhs[k][i] = dt * rhs[k][i] / g.V[i];
+        }
+    }
+
+    double relaxation_param(const Level &g) const {
+        if (c.numberOfCFLIncrements > 0) {
+            double r = (double)(g.cycleNumber - 1) / (double)c.numberOfCFLIncrements;
+            return std::min(r, 1.0);
+        }
+        return 1.0;
+    }
+
+    template <class Fn>
+    void for_range(const Level &g, int a, int b, Fn fn) {
+        for (int ib = g.R(a); ib <= g.R(b); ++ib) fn(g.node_ind[ib - 1]);
+    }
+
+    void remove_normal(Level &g, vec *x, int ip, double scale) {
+        double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+        double nv = (x[1][ip] * n[0] + x[2][ip] * n[1]) + x[3][ip] * n[2];
+        for (int k = 0; k < 3; ++k) x[1 + k][ip] = x[1 + k][ip] - scale * nv * n[k];
+    }
+
+    // ---- setBCsOnIncrementField (def_par:4978-5140) -----------------------
+    void setBCsOnIncrementField(Level &g, vec *rhs) {
+        if (c.ReynoldsNumber > 0) {
+            for_range(g, -20, -19, [&](int ip) {
+                rhs[1][ip] = 0.0; rhs[2][ip] = 0.0; rhs[3][ip] = 0.0;
+                if (!c.wallsAreIsentropic) rhs[4][ip] = 0.0;
+            });
+        } else {
+            for_range(g, -20, -19, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
+        }
+        for_range(g, -4, -3, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
+        for_range(g, -18, -17, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
+    }
+
+    // ---- updateSolutionVector (def_par:1292-1405); u may alias delu -------
+    void updateSolutionVector(Level &g, vec *u, vec *uprev, vec *delu, int rk) {
+        double dtJ = rk > 0 ? c.CFLNumber * RK[rk - 1] : c.CFLNumber;
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < g.N; ++i) delu[k][i] = dtJ * delu[k][i];
+        for (int i = 0; i < g.N; ++i) {
+            double inc = delu[0][i];
+            if (std::fabs(inc / uprev[0][i]) < c.maxIncrementFactor) {
+                u[0][i] = uprev[0][i] - inc;
+            } else {
+                double sign = inc / std::fabs(inc);
+                u[0][i] = uprev[0][i] - sign * c.maxIncrementFactor * uprev[0][i];
+            }
+            for (int k = 1; k < 5; ++k) u[k][i] = uprev[k][i] - delu[k][i];
+        }
+        for (int i = 0; i < g.N; ++i)
+            if (g.u[0][i] < c.minimumDensity) g.u[0][i] = c.minimumDensity;
+    }
+
+    // ---- setBCsOnSolutionField (def_par:4364-4976), static walls ----------
+    void setBCsOnSolutionField(Level &g, vec *u) {
+        const double relax = relaxation_param(g);
+        if (c.ReynoldsNumber > 0) {
+            for_range(g, -20, -19, [&](int ip) {
+                double cm[3] = {g.cmx[ip], g.cmy[ip], g.cmz[ip]};
+                for (int k = 0; k < 3; ++k) u[1 + k][ip] = u[0][ip] * cm[k] / c.physicalTimeStep;
+                if (!c.wallsAreIsentropic) u[4][ip] = u[0][ip] * c.inflowTemperature / c.gamma;
+            });
+        } else {
+            // the wall velocity term adds grp%u(ip,1)*0*normal for a steady
+            // run (def_par:4445-4456): the tangential projection only
+            for_range(g, -20, -19, [&](int ip) { remove_normal(g, u, ip, 1.0); });
+        }
+        for_range(g, -4, -3, [&](int ip) {
+            remove_normal(g, u, ip, relax);
+            if (!c.wallsAreIsentropic) {
+                double ke = (u[1][ip] * u[1][ip] + u[2][ip] * u[2][ip]) + u[3][ip] * u[3][ip];
+                u[4][ip] = u[0][ip] * c.inflowTemperature / c.gamma + 0.5 * ke / u[0][ip];
+            }
+        });
+        for_range(g, -18, -17, [&](int ip) { remove_normal(g, u, ip, 1.0); });
+    }
+
+    // ---- setOuterBoundaryConditions (def_par:4018-4251) -------------------
+    void setOuterBoundaryConditions(Level &g, vec *u, const vec &p) {
+        const double gm1 = c.gamma - 1.0;
+        for (int side = 0; side < 2; ++side) {
+            const double *inf = &c.inflowField[side * 6];
+            double iR = inf[0], iU1 = inf[1], iU2 = inf[2], iU3 = inf[3], iE = inf[4], iP = inf[5];
+            for_range(g, side == 0 ? -16 : -14, side == 0 ? -15 : -13, [&](int ip) {
+                double rho = u[0][ip], U1 = u[1][ip], U2 = u[2][ip], U3 = u[3][ip];
+                double nvel = (iU1 * g.nx[ip] + iU2 * g.ny[ip]) + iU3 * g.nz[ip];
+                if (nvel > 0.00) {
+                    if (c.MachNumber > 1.0) {
+                        u[0][ip] = iR; u[1][ip] = iU1 * iR; u[2][ip] = iU2 * iR; u[3][ip] = iU3 * iR;
+                        u[4][ip] = iE * iR;
+                    } else {
+                        u[0][ip] = iR; u[1][ip] = iU1 * iR; u[2][ip] = iU2 * iR; u[3][ip] = iU3 * iR;
+                        u[4][ip] = p[ip] / gm1 + 0.5 * ((iU1 * iU1 + iU2 * iU2) + iU3 * iU3) * iR;
+                    }
+                } else {
+                    if (c.MachNumber < 1.0) u[4][ip] = iP / gm1 + 0.5 * ((U1 * U1 + U2 * U2) + U3 * U3) / rho;
+                }
+            });
+        }
+    }
+
+    void limitDensity(Level &g) {
+        for (int i = 0; i < g.N; ++i) g.u[0][i] = std::max(g.u[0][i], c.minimumDensity);
+    }
+
+    void dissipation_for(Level &g, bool in_restrict_fine) {
+        if (in_restrict_fine) { makeArtificialDissipation2(g); return; }
+        if (c.dissipationScheme == 3) makeArtificialDissipation3(g);
+        else makeArtificialDissipation2(g);
+    }
+
+    // ---- singleIteration (def_par:1002-1181) ------------------------------
+    void singleIteration(Level &g, bool calcDiss) {
+        if (calcDiss) {
+            makePressureField(g, g.u);
+            for (int i = 0; i < g.N; ++i) g.p[i] = std::fabs(g.p[i]);
+            makeTimeSteps(g);
+            dissipation_for(g, false);
+        }
+        for (int st = 1; st <= 3; ++st) {
+            makePressureField(g, g.u);
+            for (int k = 0; k < 5; ++k) std::fill(g.rhs[k].begin(), g.rhs[k].end(), 0.0);
+            makeRHS(g);
+            for (int k = 0; k < 5; ++k)
+                for (int i = 0; i < g.N; ++i) g.rhs[k][i] = g.rhs[k][i] + g.diss[k][i];
+            solveSystem(g, g.rhs);
+            setBCsOnIncrementField(g, g.rhs);
+            // nullifyOuterBoundary: no-op for turbulenceModel 0
+            updateSolutionVector(g, g.u, g.uprev, g.rhs, st);
+            setBCsOnSolutionField(g, g.u);
+            if (g.grid > 1)
+                for (int k = 0; k < 5; ++k)
+                    for (int i = 0; i < g.N; ++i) g.u[k][i] = g.u[k][i] - RK[st - 1] * g.src[k][i];
+            limitDensity(g);
+            setOuterBoundaryConditions(g, g.u, g.p);
+        }
+    }
+
+    void doTimeIterations(int l, int nsteps, bool calcDiss, int cycle) {
+        Level &g = lv[l];
+        g.cycleNumber = cycle;
+        for (int s = 0; s < nsteps; ++s) {
+            for (int k = 0; k < nvar; ++k) g.uprev[k] = g.u[k];
+            singleIteration(g, calcDiss);
+        }
+    }
+
+    // ---- mapFineToCoarse (def_par:12572-12679) ----------------------------
+    void mapFineToCoarse(const Level &f, const Level &cg, vec *fu, vec *cu, int ncomp) {
+        for (int k = 0; k < ncomp; ++k) {
+            std::fill(cu[k].begin(), cu[k].end(), 0.0);
+            for (int i = 0; i < f.N; ++i) {
+                int pp = cg.parent[i];
+                if (pp >= 0) cu[k][pp] = cu[k][pp] + cg.rweight[i] * fu[k][i];
+            }
+        }
+    }
+    // ---- mapCoarseToFine, injection (def_par:12681-12783) -----------------
+    void mapCoarseToFine(const Level &cg, const Level &f, vec *cu, vec *fu, int ncomp) {
+        for (int i = 0; i < f.N; ++i) {
+            int pp = cg.parent[i];
+            if (pp >= 0)
+                for (int k = 0; k < ncomp; ++k) fu[k][i] = cu[k][pp];
+        }
+    }
+
+    // ---- restrictGrid (def_par:12141-12430) -------------------------------
+    void restrictGrid(int fl) {
+        Level &F = lv[fl], &C = lv[fl + 1];
+        mapFineToCoarse(F, C, F.u, C.u, 5);
+        {   // mapScalarFineToCoarse of the laminar viscosity
+            vec m(C.N, 0.0);
+            for (int i = 0; i < F.N; ++i) {
+                int pp = C.parent[i];
+                if (pp >= 0) m[pp] = m[pp] + C.rweight[i] * F.mu[i];
+            }
+            C.mu = m;
+        }
+        makePressureField(C, C.u);
+        setBCsOnSolutionField(C, C.u);
+        setOuterBoundaryConditions(C, C.u, C.p);
+        for (int k = 0; k < 5; ++k) C.uprev[k] = C.u[k];
+        makePressureField(C, C.u);
+        for (int i = 0; i < C.N; ++i) C.p[i] = std::fabs(C.p[i]);
+        makeTimeSteps(C);
+        if (c.coarseGridDissipationScheme == 2) makeArtificialDissipation2(C);
+        else if (c.coarseGridDissipationScheme == 3) makeArtificialDissipation3(C);
+        for (int k = 0; k < 5; ++k) std::fill(C.rhs[k].begin(), C.rhs[k].end(), 0.0);
+        makeRHS(C);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < C.N; ++i) C.rhs[k][i] = C.rhs[k][i] + C.diss[k][i];
+        solveSystem(C, C.rhs);
+        setBCsOnIncrementField(C, C.rhs);
+        updateSolutionVector(C, C.u, C.uprev, C.rhs, 0);
+        setBCsOnSolutionField(C, C.u);
+        setOuterBoundaryConditions(C, C.u, C.p);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < C.N; ++i) C.src[k][i] = C.u[k][i] - C.uprev[k][i];
+        for (int k = 0; k < 5; ++k) C.u[k] = C.uprev[k];
+        // fine-grid one-step increment at the current fine state
+        makePressureField(F, F.u);
+        for (int i = 0; i < F.N; ++i) F.p[i] = std::fabs(F.p[i]);
+        dissipation_for(F, true);
+        for (int k = 0; k < 5; ++k) std::fill(F.rhs[k].begin(), F.rhs[k].end(), 0.0);
+        makeRHS(F);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < F.N; ++i) F.rhs[k][i] = F.rhs[k][i] + F.diss[k][i];
+        solveSystem(F, F.rhs);
+        setBCsOnIncrementField(F, F.rhs);
+        updateSolutionVector(F, F.rhs, F.uprev, F.rhs, 0);
+        setBCsOnSolutionField(F, F.rhs);
+        if (F.grid > 1)
+            for (int k = 0; k < 5; ++k)
+                for (int i = 0; i < F.N; ++i) F.rhs[k][i] = F.rhs[k][i] - F.src[k][i];
+        setOuterBoundaryConditions(F, F.rhs, F.p);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < F.N; ++i) F.rhs[k][i] = F.rhs[k][i] - F.uprev[k][i];
+        mapFineToCoarse(F, C, F.rhs, C.rhs, 5);
+        setBCsOnIncrementField(C, C.rhs);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < C.N; ++i) C.src[k][i] = C.src[k][i] - C.rhs[k][i];
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < C.N; ++i) C.u[k][i] = C.u[k][i] + C.rhs[k][i];
+    }
+
+    // ---- prolongateGrid (def_par:12432-12570) -----------------------------
+    void prolongateGrid(int cl) {
+        Level &C = lv[cl], &F = lv[cl - 1];
+        mapFineToCoarse(F, C, F.u, C.uprev, 5);
+        setBCsOnSolutionField(C, C.uprev);
+        setOuterBoundaryConditions(C, C.uprev, C.p);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < C.N; ++i) C.rhs[k][i] = C.u[k][i] - C.uprev[k][i];
+        setBCsOnIncrementField(C, C.rhs);
+        mapCoarseToFine(C, F, C.rhs, F.rhs, 5);
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < F.N; ++i) F.rhs[k][i] = c.prolongationRelaxation * F.rhs[k][i];
+        for (int k = 0; k < 5; ++k)
+            for (int i = 0; i < F.Nb; ++i) F.rhs[k][i] = c.multigridBCRelaxation * F.rhs[k][i];
+        for (int i = 0; i < F.N; ++i)
+            for (int k = 0; k < 5; ++k) F.u[k][i] = F.u[k][i] + F.rhs[k][i];
+        setBCsOnSolutionField(F, F.u);
+        setOuterBoundaryConditions(F, F.u, F.p);
+        for (int i = 0; i < F.N; ++i) F.u[0][i] = std::max(F.u[0][i], c.minimumDensity);
+    }
+
+    // ---- oneCycle (mg_par:907-1196) ---------------------------------------
+    void oneCycle(int cyc) {
+        const int G = (int)lv.size();
+        const int nr = c.numberOfRelaxationSteps;
+        auto relax = [&](int j1, int steps, bool calc) { doTimeIterations(j1 - 1, steps, calc, cyc); };
+        auto restr = [&](int j1) { restrictGrid(j1 - 1); };
+        auto prol = [&](int j1) { prolongateGrid(j1 - 1); };
+        const int s = c.multigridScheme;
+        if (s <= 0) {
+            for (int i = 1; i <= G - 1; ++i) {
+                for (int k = 0; k < 5; ++k) lv[i - 1].uprev[k] = lv[i - 1].u[k];
+                mapFineToCoarse(lv[i - 1], lv[i], lv[i - 1].u, lv[i].u, 5);
+            }
+            for (int k = 0; k < 5; ++k) std::fill(lv[G - 1].src[k].begin(), lv[G - 1].src[k].end(), 0.0);
+            relax(G, nr, true);
+            for (int i = G; i >= 2; --i) mapCoarseToFine(lv[i - 1], lv[i - 2], lv[i - 1].u, lv[i - 2].u, 5);
+        } else if (s == 1) {
+            for (int i = 1; i <= G - 1; ++i) {
+                relax(i, nr, i == 1);
+                restr(i);
+                mapFineToCoarse(lv[i - 1], lv[i], lv[i - 1].u, lv[i].u, 5);
+            }
+            relax(G, nr, G == 1);
+            for (int i = G; i >= 2; --i) { prol(i); relax(i - 1, nr, (i - 1) == 1); }
+        } else if (s == 2 || s == 5) {
+            int nsw = G <= 2 ? 1 : 2 * G - 4;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, s == 5 ? j : nr, j == fsl);
+                    restr(j);
+                }
+                relax(G, s == 5 ? G : nr, G == 1);
+                if (fsl == 1) fsl = G > 2 ? G - 1 : G;
+                else if (i <= nsw / 2) fsl = fsl - 1;
+                else fsl = fsl + 1;
+                for (int j = G; j >= fsl + 1; --j) { prol(j); relax(j - 1, nr, (j - 1) == 1); }
+            }
+            for (int j = G; j >= 2; --j) { prol(j); relax(j - 1, nr, (j - 1) == 1); }
+        } else if (s == 3 || s == 7) {
+            int nsw = G == 1 ? 1 : G - 1;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) { relax(j, nr, j == fsl); restr(j); }
+                relax(G, nr, G == 1);
+                if (fsl == 1) fsl = G >= 2 ? G - 1 : G;
+                else fsl = fsl - 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prol(j);
+                    if (s == 7) relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+        } else if (s == 4) {
+            int nsw = G == 1 ? 1 : G - 1;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) { relax(j, nr, j == fsl); restr(j); }
+                relax(G, nr, G == 1);
+                fsl = fsl + 1;
+                for (int j = G; j >= fsl + 1; --j) { prol(j); relax(j - 1, nr, (j - 1) == 1); }
+            }
+            for (int j = G; j >= 2; --j) { prol(j); relax(j - 1, nr, (j - 1) == 1); }
+        } else {
+            throw std::runtime_error("Specified multigrid scheme not implemented");
+        }
+    }
+
+    // ---- geometry set-up of readGridComputationData -----------------------
+    void setup_level(Level &g) {
+        // makeBoundaryNormals (def_par:15394-15521)
+        g.nx.assign(g.N, 0.0); g.ny.assign(g.N, 0.0); g.nz.assign(g.N, 0.0);
+        for (int b = 0; b < g.B; ++b) {
+            int a = g.b1[b], d = g.b2[b];
+            g.nx[a] = g.nx[a] - g.bwx[b]; g.ny[a] = g.ny[a] - g.bwy[b]; g.nz[a] = g.nz[a] - g.bwz[b];
+            g.nx[d] = g.nx[d] - g.bwx[b]; g.ny[d] = g.ny[d] - g.bwy[b]; g.nz[d] = g.nz[d] - g.bwz[b];
+        }
+        for (int i = 0; i < g.Nb; ++i) {
+            double nrm = std::sqrt((g.nx[i] * g.nx[i] + g.ny[i] * g.ny[i]) + g.nz[i] * g.nz[i]);
+            if (nrm > 1.0e-10) { g.nx[i] = g.nx[i] / nrm; g.ny[i] = g.ny[i] / nrm; g.nz[i] = g.nz[i] / nrm; }
+            else { g.nx[i] = 0.0; g.ny[i] = 0.0; g.nz[i] = 0.0; }
+        }
+        // makeSurfaceArea (def_par:15523-15634), level 1 only
+        g.wallArea.assign(g.N, 0.0);
+        if (g.grid == 1)
+            for (int b = 0; b < g.B; ++b) {
+                double ai = std::sqrt((g.bwx[b] * g.bwx[b] + g.bwy[b] * g.bwy[b]) + g.bwz[b] * g.bwz[b]);
+                g.wallArea[g.b1[b]] = g.wallArea[g.b1[b]] + 4.0 * ai;
+                g.wallArea[g.b2[b]] = g.wallArea[g.b2[b]] + 4.0 * ai;
+            }
+        // nodeConnectivityArray (def_par:14262-14275)
+        g.conn.assign(g.N, 0.0);
+        for (int e = 0; e < g.E; ++e) { g.conn[g.s1[e]] += 1.0; g.conn[g.s2[e]] += 1.0; }
+    }
+
+    // ---- calculateLiftAndDrag (def_par:14710-14870) -----------------------
+    void forces(double *out) {
+        Level &g = lv[0];
+        const double PI = 4.0 * std::atan(1.0);
+        double aR = c.alpha * PI / 180., bR = c.beta * PI / 180.;
+        double ft[3] = {std::cos(aR) * std::cos(bR), std::sin(bR), std::sin(aR)};
+        double fn1[3] = {-ft[2], 0.0, ft[0]}, fn2[3] = {-ft[1], ft[0], 0.0};
+        double lift = 0, drag = 0, latF = 0, fric = 0, latM = 0, longM = 0;
+        const double pinf = 1. / (c.gamma * c.MachNumber * c.MachNumber);
+        for_range(g, -20, -19, [&](int ip) {
+            double h = g.cz[ip];
+            double xd = g.cx[ip] - c.datum[0], yd = g.cy[ip] - c.datum[1], zd = g.cz[ip] - c.datum[2];
+            if (!(h > (c.groundplane + 0.01))) return;
+            double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+            auto dot = [&](const double *a) { return (n[0] * a[0] + n[1] * a[1]) + n[2] * a[2]; };
+            double A = g.wallArea[ip], dp = g.p[ip] - pinf;
+            lift = lift - A * dp * dot(fn1);
+            latF = latF - A * dp * dot(fn2);
+            drag = drag - A * dp * dot(ft);
+            latM = latM + xd * A * dp * dot(fn2);
+            latM = latM - yd * A * dp * dot(ft);
+            longM = longM + xd * A * dp * dot(fn1);
+            longM = longM - zd * A * dp * dot(ft);
+            if (c.ReynoldsNumber > 0.0) {
+                double s[3] = {g.wallStress[0][ip], g.wallStress[1][ip], g.wallStress[2][ip]};
+                auto sd = [&](const double *a) { return (s[0] * a[0] + s[1] * a[1]) + s[2] * a[2]; };
+                lift = lift + A * sd(fn1);
+                latF = latF + A * sd(fn2);
+                drag = drag + A * sd(ft);
+                fric = fric + A * sd(ft);
+                latM = latM - xd * A * sd(fn2);
+                latM = latM + yd * A * sd(ft);
+                longM = longM - xd * A * sd(fn1);
+                longM = longM + zd * A * sd(ft);
+            }
+        });
+        out[0] = 2.0 * lift / c.referenceArea;
+        out[1] = 2.0 * drag / c.referenceArea;
+        out[2] = 2.0 * latF / c.referenceArea;
+        out[3] = 2.0 * fric / c.referenceArea;
+        out[4] = latM;
+        out[5] = longM;
+    }
+};
+
+int check_controls(const flite_controls &c) {
+    if (c.flowType != 0 || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
+        c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
+        c.prolongationSmoothingFactor > 0)
+        return FLITE_EUNSUPPORTED;
+    if (c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
+    if (c.ReynoldsNumber > 0) return FLITE_EUNSUPPORTED;
+    if (c.fluxType < 1 || c.fluxType > 4) return FLITE_EUNSUPPORTED;
+    if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1) return FLITE_EUNSUPPORTED;
+    if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
+    if (c.useMatrixDissipation) return FLITE_EUNSUPPORTED;
+    if (c.prolongationMappingScheme != 1) return FLITE_EUNSUPPORTED;
+    return FLITE_OK;
+}
+
+}  // namespace
+
+struct oracle_ctx {
+    Oracle o;
+};
+
+extern "C" {
+
+int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *lv, oracle_ctx **out) {
+    if (!c || !lv || !out || nlevels < 1) return FLITE_EINVAL;
+    int st = check_controls(*c);
+    if (st) return st;
+    auto ctx = std::make_unique<oracle_ctx>();
+    Oracle &o = ctx->o;
+    o.c = *c;
+    int G = nlevels;
+    if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);
+    o.lv.resize(G);
+    for (int l = 0; l < G; ++l) {
+        const flite_level_desc &d = lv[l];
+        Level &g = o.lv[l];
+        g.grid = l + 1;
+        g.N = d.n_nodes; g.E = d.n_sides; g.B = d.n_bsides; g.Nb = d.n_bnodes; g.nnorm = d.n_normals;
+        g.s1.resize(g.E); g.s2.resize(g.E);
+        g.wx.resize(g.E); g.wy.resize(g.E); g.wz.resize(g.E); g.slen.assign(g.E, 0.0);
+        for (int e = 0; e < g.E; ++e) {
+            g.s1[e] = d.side_idx[e] - 1; g.s2[e] = d.side_idx[(size_t)g.E + e] - 1;
+            g.wx[e] = d.side_w[e]; g.wy[e] = d.side_w[(size_t)g.E + e]; g.wz[e] = d.side_w[2 * (size_t)g.E + e];
+            if (d.side_len) g.slen[e] = d.side_len[e];
+        }
+        g.b1.resize(g.B); g.b2.resize(g.B); g.bind.resize(g.B);
+        g.bwx.resize(g.B); g.bwy.resize(g.B); g.bwz.resize(g.B);
+        for (int b = 0; b < g.B; ++b) {
+            g.b1[b] = d.bnd_idx[b] - 1; g.b2[b] = d.bnd_idx[(size_t)g.B + b] - 1;
+            g.bind[b] = d.bnd_idx[2 * (size_t)g.B + b];
+            if (g.bind[b] >= 5 && g.bind[b] <= 8) return FLITE_EUNSUPPORTED;
+            g.bwx[b] = d.bnd_w[b]; g.bwy[b] = d.bnd_w[(size_t)g.B + b]; g.bwz[b] = d.bnd_w[2 * (size_t)g.B + b];
+        }
+        std::memcpy(g.reg, d.node_reg, sizeof g.reg);
+        for (int r = -12; r <= -5; r += 2)
+            if (g.R(r + 1) >= g.R(r)) return FLITE_EUNSUPPORTED;  // engine nodes
+        g.node_ind.resize(g.nnorm);
+        for (int i = 0; i < g.nnorm; ++i) g.node_ind[i] = d.node_ind[i] - 1;
+        g.V.assign(d.volume, d.volume + g.N);
+        g.wdist.assign(g.N, 0.0);
+        if (d.wall_dist) g.wdist.assign(d.wall_dist, d.wall_dist + g.N);
+        g.cx.assign(g.N, 0.0); g.cy.assign(g.N, 0.0); g.cz.assign(g.N, 0.0);
+        if (l == 0 && d.coords) {
+            for (int i = 0; i < g.N; ++i) {
+                g.cx[i] = d.coords[i]; g.cy[i] = d.coords[(size_t)g.N + i]; g.cz[i] = d.coords[2 * (size_t)g.N + i];
+            }
+        }
+        g.cmx.assign(g.N, 0.0); g.cmy.assign(g.N, 0.0); g.cmz.assign(g.N, 0.0);
+        if (l == 0 && d.coord_move)
+            for (int i = 0; i < g.N; ++i) {
+                g.cmx[i] = d.coord_move[i]; g.cmy[i] = d.coord_move[(size_t)g.N + i];
+                g.cmz[i] = d.coord_move[2 * (size_t)g.N + i];
+            }
+        if (l > 0) {
+            int nf = o.lv[l - 1].N;
+            if (!d.parent || !d.rweight) return FLITE_EINVAL;
+            g.parent.resize(nf); g.rweight.assign(d.rweight, d.rweight + nf);
+            for (int i = 0; i < nf; ++i) g.parent[i] = d.parent[i] - 1;
+        }
+        for (int k = 0; k < 6; ++k) {
+            g.u[k].assign(g.N, 0.0); g.uprev[k].assign(g.N, 0.0); g.rhs[k].assign(g.N, 0.0);
+            g.src[k].assign(g.N, 0.0);
+        }
+        for (int k = 0; k < 5; ++k) g.diss[k].assign(g.N, 0.0);
+        g.p.assign(g.N, 0.0); g.dt.assign(g.N, 0.0); g.mu.assign(g.N, 0.0);
+        for (int k = 0; k < 3; ++k) g.wallStress[k].assign(g.N, 0.0);
+        g.cycleNumber = l == 0 ? 1 : 0;
+        o.setup_level(g);
+    }
+    o.nh.assign(25, vec(o.lv[0].N, 0.0));
+    *out = ctx.release();
+    return FLITE_OK;
+}
+
+int oracle_destroy(oracle_ctx *o) { delete o; return FLITE_OK; }
+
+static Level *lvl(oracle_ctx *o, int level) {
+    if (!o || level < 1 || level > (int)o->o.lv.size()) return nullptr;
+    return &o->o.lv[level - 1];
+}
+
+int oracle_set_state(oracle_ctx *o, int level, const double *u) {
+    Level *g = lvl(o, level);
+    if (!g || !u) return FLITE_EINVAL;
+    for (int k = 0; k < o->o.nvar; ++k) std::memcpy(g->u[k].data(), u + (size_t)k * g->N, 8 * (size_t)g->N);
+    return FLITE_OK;
+}
+
+int oracle_get_state(oracle_ctx *o, int level, double *u) {
+    Level *g = lvl(o, level);
+    if (!g || !u) return FLITE_EINVAL;
+    for (int k = 0; k < o->o.nvar; ++k) std::memcpy(u + (size_t)k * g->N, g->u[k].data(), 8 * (size_t)g->N);
+    return FLITE_OK;
+}
+
+int oracle_get_pressure(oracle_ctx *o, int level, double *p) {
+    Level *g = lvl(o, level);
+    if (!g || !p) return FLITE_EINVAL;
+    std::memcpy(p, g->p.data(), 8 * (size_t)g->N);
+    return FLITE_OK;
+}
+
+int oracle_get_array(oracle_ctx *o, int level, const char *name, double *out) {
+    Level *g = lvl(o, level);
+    if (!g || !name || !out) return FLITE_EINVAL;
+    const size_t N = g->N;
+    std::string n(name);
+    auto cols = [&](const vec *a, int nc) { for (int k = 0; k < nc; ++k) std::memcpy(out + k * N, a[k].data(), 8 * N); };
+    if (n == "dt") std::memcpy(out, g->dt.data(), 8 * N);
+    else if (n == "diss") cols(g->diss, 5);
+    else if (n == "rhs") cols(g->rhs, 5);
+    else if (n == "uprev") cols(g->uprev, 5);
+    else if (n == "src") cols(g->src, 5);
+    else if (n == "mu") std::memcpy(out, g->mu.data(), 8 * N);
+    else if (n == "conn") std::memcpy(out, g->conn.data(), 8 * N);
+    else if (n == "wallArea") std::memcpy(out, g->wallArea.data(), 8 * N);
+    else if (n == "normal") {
+        std::memcpy(out, g->nx.data(), 8 * N); std::memcpy(out + N, g->ny.data(), 8 * N);
+        std::memcpy(out + 2 * N, g->nz.data(), 8 * N);
+    } else if (n == "grad") {
+        for (int k = 0; k < 15; ++k) std::memcpy(out + k * N, o->o.nh[k].data(), 8 * N);
+    } else return FLITE_EINVAL;
+    return FLITE_OK;
+}
+
+int oracle_init_freestream(oracle_ctx *o) {
+    if (!o) return FLITE_EINVAL;
+    Level &g = o->o.lv[0];
+    for (int i = 0; i < g.N; ++i)
+        for (int k = 0; k < 5; ++k) g.u[k][i] = o->o.c.inflowField[k];
+    return FLITE_OK;
+}
+
+int oracle_start(oracle_ctx *o) {
+    if (!o) return FLITE_EINVAL;
+    Oracle &O = o->o;
+    Level &g = O.lv[0];
+    O.makePressureField(g, g.u);
+    g.cycleNumber = 1;
+    O.setBCsOnSolutionField(g, g.u);
+    const double mu = O.c.ReynoldsNumber > 0.0 ? 1. / O.c.ReynoldsNumber : 0.0;
+    for (size_t l = 0; l < O.lv.size(); ++l) {
+        std::fill(O.lv[l].mu.begin(), O.lv[l].mu.end(), mu);
+        if (l > 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].u, O.lv[l].u, 5);
+    }
+    return FLITE_OK;
+}
+
+int oracle_do_time_iterations(oracle_ctx *o, int level, int nsteps, int calc_diss, int calc_turb,
+                              int cycle_no) {
+    (void)calc_turb;
+    if (!lvl(o, level)) return FLITE_EINVAL;
+    o->o.doTimeIterations(level - 1, nsteps, calc_diss != 0, cycle_no);
+    return FLITE_OK;
+}
+
+int oracle_restrict(oracle_ctx *o, int fine_level, int calc_turb) {
+    (void)calc_turb;
+    if (!lvl(o, fine_level) || !lvl(o, fine_level + 1)) return FLITE_EINVAL;
+    o->o.restrictGrid(fine_level - 1);
+    return FLITE_OK;
+}
+
+int oracle_prolong(oracle_ctx *o, int coarse_level) {
+    if (coarse_level < 2 || !lvl(o, coarse_level)) return FLITE_EINVAL;
+    o->o.prolongateGrid(coarse_level - 1);
+    return FLITE_OK;
+}
+
+int oracle_map_fine_to_coarse(oracle_ctx *o, int fine_level) {
+    if (!lvl(o, fine_level) || !lvl(o, fine_level + 1)) return FLITE_EINVAL;
+    Oracle &O = o->o;
+    O.mapFineToCoarse(O.lv[fine_level - 1], O.lv[fine_level], O.lv[fine_level - 1].u, O.lv[fine_level].u, 5);
+    return FLITE_OK;
+}
+
+int oracle_cycle(oracle_ctx *o, int cycle_no) {
+    if (!o) return FLITE_EINVAL;
+    try {
+        o->o.oneCycle(cycle_no);
+    } catch (const std::exception &) {
+        return FLITE_EUNSUPPORTED;
+    }
+    return FLITE_OK;
+}
+
+int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[7]) {
+    if (!o) return FLITE_EINVAL;
+    Oracle &O = o->o;
+    Level &g = O.c.multigridScheme > 0 ? O.lv[0] : O.lv.back();
+    const int nres = 5;
+    for (int k = 0; k < 7; ++k) { res[k] = 0.0; maxres[k] = 0.0; maxind[k] = 1; }
+    for (int k = 0; k < nres; ++k) {
+        double s = 0.0;
+        for (int i = 0; i < g.N; ++i) {
+            double d = g.u[k][i] - g.uprev[k][i];
+            s = s + d * d;
+        }
+        res[k] = std::sqrt(s);
+    }
+    for (int i = 0; i < g.N; ++i)
+        for (int k = 0; k < nres; ++k) {
+            double cr = std::fabs(g.u[k][i] - g.uprev[k][i]);
+            if (cr > maxres[k]) { maxres[k] = cr; maxind[k] = i + 1; }
+        }
+    for (int k = 0; k < nres; ++k)
+        if (!std::isfinite(res[k])) return FLITE_ENAN;
+    return FLITE_OK;
+}
+
+int oracle_forces(oracle_ctx *o, double out[6]) {
+    if (!o || !out) return FLITE_EINVAL;
+    o->o.forces(out);
+    return FLITE_OK;
+}
+
+int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r) {
+    Level *g = lvl(o, level);
+    if (!g || !u || !r) return FLITE_EINVAL;
+    for (int k = 0; k < 5; ++k) std::memcpy(g->u[k].data(), u + (size_t)k * g->N, 8 * (size_t)g->N);
+    o->o.makePressureField(*g, g->u);
+    for (int k = 0; k < 5; ++k) std::fill(g->rhs[k].begin(), g->rhs[k].end(), 0.0);
+    o->o.makeRHS(*g);
+    for (int k = 0; k < 5; ++k) std::memcpy(r + (size_t)k * g->N, g->rhs[k].data(), 8 * (size_t)g->N);
+    return FLITE_OK;
+}
+
+int oracle_eval_dissipation(oracle_ctx *o, int level) {
+    Level *g = lvl(o, level);
+    if (!g) return FLITE_EINVAL;
+    o->o.makePressureField(*g, g->u);
+    for (int i = 0; i < g->N; ++i) g->p[i] = std::fabs(g->p[i]);
+    o->o.makeTimeSteps(*g);
+    o->o.dissipation_for(*g, false);
+    return FLITE_OK;
+}
+
+}  // extern "C"

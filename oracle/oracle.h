@@ -1,0 +1,47 @@
+/*
+ * oracle.h -- CPU restatement of the reference flow solver (test
+ * infrastructure only).
+ *
+ * This is the checker the GPU library is compared against.  It is a plain
+ * FP64 C++ restatement of the Fortran routines of SolverSource/
+ * mgnsg3d_def_par.F90 and mgnsg3d_mg_par.F90 on the hot path, in the
+ * reference's own operation order (edge-order scatter, left-to-right
+ * evaluation, no FMA contraction).  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg load it.  Parity is pinned by the reference's
+ * own invariants and analytic known answers (the reference ships no tests,
+ * fixtures or outputs and cannot be compiled here: there is no Fortran
+ * compiler), see tests/golden/.
+ */
+#ifndef FLITE_ORACLE_H
+#define FLITE_ORACLE_H
+#include "flite_gpu.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+typedef struct oracle_ctx oracle_ctx;
+int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *lv,
+                  oracle_ctx **out);
+int oracle_destroy(oracle_ctx *o);
+int oracle_set_state(oracle_ctx *o, int level, const double *u);
+int oracle_get_state(oracle_ctx *o, int level, double *u);
+int oracle_get_pressure(oracle_ctx *o, int level, double *p);
+/* named per-level arrays: "dt", "diss", "rhs", "uprev", "src", "normal",
+ * "wallArea", "conn", "mu", "grad" (15 columns of nodeHelpArray)          */
+int oracle_get_array(oracle_ctx *o, int level, const char *name, double *out);
+int oracle_init_freestream(oracle_ctx *o);
+int oracle_start(oracle_ctx *o);
+int oracle_do_time_iterations(oracle_ctx *o, int level, int nsteps, int calc_diss,
+                              int calc_turb, int cycle_no);
+int oracle_restrict(oracle_ctx *o, int fine_level, int calc_turb);
+int oracle_prolong(oracle_ctx *o, int coarse_level);
+int oracle_map_fine_to_coarse(oracle_ctx *o, int fine_level);
+int oracle_cycle(oracle_ctx *o, int cycle_no);
+int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[7]);
+int oracle_forces(oracle_ctx *o, double out[6]);
+int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);
+/* one makeTimeSteps + dissipation evaluation at the level's current state */
+int oracle_eval_dissipation(oracle_ctx *o, int level);
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,45 @@
+"""The C-ABI libraries load and export every symbol their headers declare."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+from flite3d_b200 import _abi
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\bint\s+(f(?:lite|p)_\w+)\s*\(", text)))
+
+
+def test_gpu_library_exports_header():
+    lib = _abi.gpu_lib()
+    names = _declared("flite_gpu.h")
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_abi.GPU_SYMBOLS) | (set(names) - set(_abi.GPU_SYMBOLS))
+
+
+def test_prepro_library_exports_header():
+    lib = _abi.prepro_lib()
+    for n in _declared("flite_prepro.h"):
+        assert hasattr(lib, n), n
+
+
+def test_struct_sizes_match_c():
+    # sizeof(flite_controls) and sizeof(flite_level_desc) as compiled
+    assert ctypes.sizeof(_abi.LevelDesc) == 5 * 4 + 4 + 13 * 8
+
+
+def test_create_rejects_unsupported_controls():
+    from flite3d_b200 import Mesh, default_controls
+    m = Mesh.bump_channel(4, 2, 2, 0.05, nlevels=1)
+    lib = _abi.gpu_lib()
+    h = ctypes.c_void_p()
+    for bad in (dict(flowType=1), dict(turbulenceModel=2), dict(movingwall=1),
+                dict(ReynoldsNumber=0.0, multigridScheme=6)):
+        c = default_controls(**bad)
+        rc = lib.flite_create(ctypes.byref(c), m.nlevels, m.descs, ctypes.byref(h))
+        assert rc == _abi.FLITE_EUNSUPPORTED, bad

@@ -1,0 +1,144 @@
+"""GPU (CUDA sm_100a, FP64) against the CPU restatement of the reference.
+
+The FP64 kernels evaluate every reference expression in the reference's
+order without FMA contraction, and sum per-node contributions in the
+reference's edge order, so states are compared bit for bit
+(np.array_equal).  Only the reductions (residual L2 norms, forces) use a
+different summation order on the GPU; they are compared to 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_backend
+from flite3d_b200 import Mesh, Solver, default_controls, initial_state
+
+pytestmark = pytest.mark.gpu
+
+RTOL_REDUCTION = 1e-12
+
+BASE = dict(ReynoldsNumber=0.0, MachNumber=0.5, CFLNumber=2.0, numberOfGridsToUse=3,
+            multigridScheme=3)
+
+CASES = {
+    "central_jst": dict(fluxType=1),
+    "hllc2_autoclip": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1),
+    "hllc2_noclip": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=0, HLLCClipping=0.5),
+    "hllc1": dict(fluxType=4, HLLCFluxOrder=1),
+    "first_order_diss": dict(fluxType=1, dissipationScheme=3, coarseGridDissipationScheme=3),
+    "fv_boundary_term": dict(fluxType=1, boundaryTerm=2),
+    "alpha_beta": dict(fluxType=1, alpha=3.0, beta=2.0),
+    "supersonic_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1, MachNumber=1.3,
+                             CFLNumber=1.0),
+    "dissipation_weighting": dict(fluxType=1, useDissipationWeighting=1),
+    "relax_steps2": dict(fluxType=1, numberOfRelaxationSteps=2, prolongationRelaxation=0.8,
+                         multigridBCRelaxation=0.5, maxIncrementFactor=0.05),
+}
+SCHEMES = [0, 1, 2, 4, 5, 7]
+
+
+def make_pair(mesh, **ctl):
+    c = default_controls(**{**BASE, **ctl})
+    g = Solver(c, mesh)
+    o = Solver(c, mesh, backend=oracle_backend())
+    u0 = initial_state(c, mesh, perturb_seed=20261203, amplitude=0.01)
+    for s in (g, o):
+        s.set_state(u0)
+        s.start()
+    return c, g, o
+
+
+def assert_same_state(g, o, what=""):
+    for level in range(1, g.nlevels + 1):
+        a, b = g.get_state(level), o.get_state(level)
+        if not np.array_equal(a, b):
+            d = np.abs(a - b)
+            k, i = np.unravel_index(np.argmax(d), d.shape)
+            raise AssertionError(f"{what} level {level}: max |diff| {d.max():.3e} at comp {k} "
+                                 f"node {i} ({a[k, i]!r} vs {b[k, i]!r})")
+
+
+@pytest.fixture(scope="module")
+def mesh():
+    return Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+
+
+@pytest.mark.parametrize("flux", [1, 2, 3, 4])
+def test_residual_bitwise(mesh, flux):
+    extra = dict(HLLCFluxOrder=2, Automaticlipping=1) if flux == 4 else {}
+    c, g, o = make_pair(mesh, fluxType=flux, **extra)
+    u = initial_state(c, mesh, perturb_seed=7, amplitude=0.05)
+    u[1] *= 1.0 + 0.02 * np.sin(np.arange(u.shape[1]))
+    rg, ro = g.residual_fwd(u), o.residual_fwd(u)
+    assert np.array_equal(rg, ro)
+    # coarse levels run the same edge kernels
+    for level in (2, 3):
+        uc = g.get_state(level)
+        assert np.array_equal(g.residual_fwd(uc, level), o.residual_fwd(uc, level))
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_calls_and_cycles_bitwise(mesh, case):
+    c, g, o = make_pair(mesh, **CASES[case])
+    assert_same_state(g, o, "start")
+    for s in (g, o):
+        s.do_time_iterations(1, 1, True, 1)
+    assert_same_state(g, o, "doTimeIterations")
+    for s in (g, o):
+        s.restrict(1)
+    assert_same_state(g, o, "restrictGrid")
+    for s in (g, o):
+        s.do_time_iterations(2, 1, False, 1)
+        s.prolong(2)
+    assert_same_state(g, o, "prolongateGrid")
+    for cyc in range(1, 4):
+        for s in (g, o):
+            s.cycle(cyc)
+        assert_same_state(g, o, f"cycle {cyc}")
+        rg, mg, ig = g.residuals()
+        ro, mo, io = o.residuals()
+        np.testing.assert_allclose(rg, ro, rtol=RTOL_REDUCTION)
+        assert np.array_equal(mg, mo) and np.array_equal(ig, io)
+        np.testing.assert_allclose(g.forces(), o.forces(), rtol=RTOL_REDUCTION, atol=1e-15)
+    assert np.array_equal(g.get_pressure(1), o.get_pressure(1))
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_multigrid_schemes_bitwise(mesh, scheme):
+    c, g, o = make_pair(mesh, fluxType=1, multigridScheme=scheme)
+    for cyc in range(1, 3):
+        for s in (g, o):
+            s.cycle(cyc)
+        assert_same_state(g, o, f"scheme {scheme} cycle {cyc}")
+
+
+def test_cycle_graph_replay_matches_eager(mesh):
+    # flite_cycle replays a captured graph; do the same cycle call by call
+    # through the individual entry points and compare
+    c, g, o = make_pair(mesh, fluxType=1)
+    c2, g2, _ = make_pair(mesh, fluxType=1)
+    g.cycle(1)
+    # growing V for 3 grids, spelled out (mg_par:1017-1058)
+    g2.do_time_iterations(1, 1, True, 1)
+    g2.restrict(1)
+    g2.do_time_iterations(2, 1, False, 1)
+    g2.restrict(2)
+    g2.do_time_iterations(3, 1, False, 1)
+    g2.prolong(3)
+    g2.do_time_iterations(2, 1, True, 1)
+    g2.restrict(2)
+    g2.do_time_iterations(3, 1, False, 1)
+    g2.prolong(3)
+    g2.prolong(2)
+    assert_same_state(g, g2, "graph vs eager")
+
+
+def test_convergence_history_matches(mesh):
+    # residual history of 30 cycles on a coarser mesh: the states stay
+    # bitwise equal, the norms agree to the reduction tolerance
+    m = Mesh.bump_channel(12, 4, 4, 0.05, nlevels=3)
+    c, g, o = make_pair(m, fluxType=1)
+    for cyc in range(1, 31):
+        g.cycle(cyc)
+        o.cycle(cyc)
+    assert_same_state(g, o, "30 cycles")
+    np.testing.assert_allclose(g.residuals()[0], o.residuals()[0], rtol=RTOL_REDUCTION)
