@@ -32,11 +32,11 @@ import numpy as np  # noqa: E402
 
 MESH = dict(nx=264, ny=88, nz=88, bump=0.05, levels=4)
 METRIC = "MG cycles/s"
-CONTROLS = dict(ReynoldsNumber=0.0, MachNumber=0.5, alpha=0.0, CFLNumber=2.0, fluxType=1,
-                multigridScheme=3, numberOfGridsToUse=4)
-WORKLOAD = ("bump channel 264x88x88 hex -> 6 tets (2,099,065 nodes, 14,473,976 edges), "
-            "4 agglomerated MG levels, growing V-cycle, 3-stage RK, CFL 2, M 0.5; "
-            "inviscid Euler central flux + JST (viscous terms not yet in this build)")
+CONTROLS = dict(ReynoldsNumber=5000.0, MachNumber=0.5, alpha=0.0, CFLNumber=2.0, fluxType=1,
+                multigridScheme=3, numberOfGridsToUse=4, wallsAreIsentropic=1, viscosityScheme=1)
+WORKLOAD = ("laminar Navier-Stokes, Re 5e3, M 0.5, adiabatic walls, on the bump channel "
+            "264x88x88 hex -> 6 tets (2,099,065 nodes, 14,473,976 edges), 4 agglomerated MG "
+            "levels, growing V-cycle, 3-stage RK, CFL 2, central flux + JST, FP64")
 
 
 def _dist():
@@ -172,7 +172,7 @@ def run_ours(args):
     n = mesh.level(1).n_nodes
     pin = torch.empty((5, n), dtype=torch.float64, pin_memory=True)
     host_u = pin.numpy()
-    host_u[:] = solver.get_state(1)
+    solver.get_state(1, out=host_u)
     cyc = args.warmup + args.steps + 1
     if ws > 1:
         dist.barrier()
@@ -183,9 +183,19 @@ def run_ours(args):
         solver.cycle(cyc + k)
         r, _, _ = solver.residuals()
         fc = solver.forces()
-        host_u[:] = solver.get_state(1)
+        solver.get_state(1, out=host_u)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
+    # the resident variant: per cycle only the cycle number goes in and the
+    # residual norms and forces come out (the state stays on the device, as
+    # when the whole multigrid loop is driven through the library)
+    t1 = time.perf_counter()
+    for k in range(args.steps):
+        solver.cycle(cyc + args.steps + k)
+        r, _, _ = solver.residuals()
+        fc = solver.forces()
+    torch.cuda.synchronize()
+    resident_s = time.perf_counter() - t1
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if ws > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
@@ -210,7 +220,11 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (state+mesh+edge buffer > 1 GB)",
                    "mesh_build_s": round(t_mesh, 2)},
         "e2e": {"value": e2e_value, "unit": "cycles/s", "h2d_bytes_per_step": 5 * n * 8 + 4,
-                "d2h_bytes_per_step": 5 * n * 8 + 15 * 8 + 6 * 8},
+                "d2h_bytes_per_step": 5 * n * 8 + 15 * 8 + 6 * 8,
+                "what": "per cycle: level-1 state host->device from pinned memory, flite_cycle, "
+                        "residual norms and forces read back, level-1 state device->host",
+                "resident": {"value": args.steps / resident_s, "h2d_bytes_per_step": 4,
+                             "d2h_bytes_per_step": 15 * 8 + 6 * 8}},
         "gpu_launches": int(launches_per_cycle * args.steps),
         "roofline": {"kernel": "k_edge_flux (level 1)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -285,14 +299,17 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-cycles", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mesh", default=None, help="NX,NY,NZ hexes (default 264,88,88)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.mesh:
+        MESH["nx"], MESH["ny"], MESH["nz"] = [int(v) for v in args.mesh.split(",")]
     if args.impl == "reference":
         run_reference(args)
     else:

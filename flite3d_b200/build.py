@@ -78,7 +78,7 @@ def build_gpu(force=False, verbose=False):
     objs = []
     for s in cu + cpp:
         o = os.path.join(objdir, os.path.basename(s) + ".o")
-        cmd = [_nvcc(), "-c", s, "-o", o, "-std=c++17", "-O3", *ARCH, "-lineinfo",
+        cmd = [_nvcc(), "-c", s, "-o", o, "-std=c++17", "-O3", *ARCH, "-lineinfo", "--fmad=false",
                "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", f"-I{INC}",
                f"-I{sdir}", "--expt-relaxed-constexpr"]
         objs.append(o)

@@ -14,7 +14,7 @@ enum : unsigned char { BC_NONE = 0, BC_WALL = 1, BC_SYM = 2, BC_FAR3 = 3, BC_FAR
 
 struct Params {
     double gamma, gm1, CFL, maxInc, minRho, Re, am, k2, k4, cgdf, pts, Tinf, mach;
-    double mgBCRelax, prolRelax, clip;
+    double mgBCRelax, prolRelax, clip, Pr;
     double inf[12];
     double RK[3];
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
@@ -53,6 +53,8 @@ struct LevelView {
     double *lap;                           // [5][N] undivided Laplacian
     double *sens;                          // [N]  pressure sensor
     double *hvis;                          // [N]  viscous time-step term
+    double *tau;                           // [9][N] stress tensor + heat flux
+    double *wstress;                       // [3][N] wall stress (level 1)
     double *grad;                          // [15][N] (level 1, HLLC order 2)
     double *bnd;                           // [10][N]
     double *flux;                          // [E][5] edge flux buffer

@@ -127,6 +127,14 @@ struct flite_ctx {
         if (c.dissipationScheme == 3) first_order_diss(l);
         else jst(l);
     }
+    // makeViscosityTerm (def_par:5198-5893), subtracted from the dissipation
+    void viscous(int l) {
+        if (!(c.ReynoldsNumber > 0.0)) return;
+        counted();
+        k_visc_grad<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
+        counted();
+        k_visc_flux<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
+    }
     // makeRHS up to the node gather (def_par:1587-1607 and the edge loops)
     void rhs_terms(int l) {
         const LevelView &L = V(l);
@@ -140,11 +148,24 @@ struct flite_ctx {
         }
         if (L.E > 0) {
             counted();
-            k_edge_flux<<<blocks(L.E), kBlock, 0, s>>>(P, L);
+            edge_flux_launch(L);
         }
         if (L.B > 0) {
             counted();
             k_bnd_flux<<<blocks(L.B), kBlock, 0, s>>>(P, L);
+        }
+    }
+    // the flux kernel instance of this run's fluxType (and HLLC order; the
+    // reconstruction only acts on level 1, where coordinates exist)
+    void edge_flux_launch(const LevelView &L) {
+        const unsigned nb = blocks(L.E);
+        switch (c.fluxType) {
+            case 1: k_edge_flux<1, false><<<nb, kBlock, 0, s>>>(P, L); break;
+            case 2: k_edge_flux<2, false><<<nb, kBlock, 0, s>>>(P, L); break;
+            case 3: k_edge_flux<3, false><<<nb, kBlock, 0, s>>>(P, L); break;
+            default:
+                if (c.HLLCFluxOrder > 1) k_edge_flux<4, true><<<nb, kBlock, 0, s>>>(P, L);
+                else k_edge_flux<4, false><<<nb, kBlock, 0, s>>>(P, L);
         }
     }
     void node_update(int l, int mode, int stage) {
@@ -158,6 +179,7 @@ struct flite_ctx {
             pressure(l);  // p = |p| is the identity after the 0.1 floor
             timesteps(l);
             dissipation(l);
+            viscous(l);
         }
         for (int st = 1; st <= 3; ++st) {
             pressure(l);
@@ -183,10 +205,12 @@ struct flite_ctx {
         timesteps(cl);
         if (c.coarseGridDissipationScheme == 2) jst(cl);
         else if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
+        viscous(cl);
         rhs_terms(cl);
         node_update(cl, MODE_RCOARSE, 0);
         pressure(fl);
         jst(fl);  // the fine part always uses scheme 2 (def_par:12266-12270)
+        viscous(fl);
         rhs_terms(fl);
         node_update(fl, MODE_RFINE, 0);
         counted();
@@ -350,7 +374,7 @@ const char *unsupported_reason(const flite_controls &c) {
     if (c.residualSmoothingFactor > 0 || c.prolongationSmoothingFactor > 0)
         return "residual and prolongation smoothing are not supported";
     if (c.turbulenceModel != 0) return "turbulenceModel != 0 is not supported yet";
-    if (c.ReynoldsNumber > 0) return "viscous flow (ReynoldsNumber > 0) is not supported yet";
+    if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return "viscosityScheme 2 is not supported";
     if (c.fluxType < 1 || c.fluxType > 4) return "fluxType must be 1..4";
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1)
         return "least-squares gradients are not supported (GradientMethod must be 1)";
@@ -388,7 +412,7 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
         P.k2 = c->secondOrderDissipationFactor; P.k4 = c->fourthOrderDissipationFactor;
         P.cgdf = c->coarseGridDissipationFactor; P.pts = c->physicalTimeStep; P.Tinf = c->inflowTemperature;
         P.mach = c->MachNumber; P.mgBCRelax = c->multigridBCRelaxation; P.prolRelax = c->prolongationRelaxation;
-        P.clip = c->HLLCClipping;
+        P.clip = c->HLLCClipping; P.Pr = c->PrandtlNumber;
         for (int i = 0; i < 12; ++i) P.inf[i] = c->inflowField[i];
         P.RK[0] = 0.6; P.RK[1] = 0.6; P.RK[2] = 1.0;  // def_par:14240-14244
         P.fluxType = c->fluxType; P.hllcOrder = c->HLLCFluxOrder; P.autoClip = c->Automaticlipping;
@@ -548,6 +572,10 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
                 CK(cudaMemset(a, 0, 5 * (size_t)N * sizeof(double)));
             for (double *a : {L.p, L.dt, L.mu, L.sens, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
             const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
+            const bool visc = c->ReynoldsNumber > 0.0;
+            L.tau = visc ? X.alloc<double>(9 * (size_t)N) : nullptr;
+            L.wstress = X.alloc<double>(3 * (size_t)N);
+            CK(cudaMemset(L.wstress, 0, 3 * (size_t)N * sizeof(double)));
             L.grad = hllc2 ? X.alloc<double>(15 * (size_t)N) : nullptr;
             L.bnd = hllc2 ? X.alloc<double>(10 * (size_t)N) : nullptr;
             L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
@@ -794,7 +822,7 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, do
         for (int r = 0; r < reps; ++r) {
             X.pressure(l);
             CK(cudaEventRecord(ev[0], X.s));
-            k_edge_flux<<<flite_ctx::blocks(L.E), kBlock, 0, X.s>>>(X.P, L);
+            X.edge_flux_launch(L);
             CK(cudaEventRecord(ev[1], X.s));
             if (L.B > 0) k_bnd_flux<<<flite_ctx::blocks(L.B), kBlock, 0, X.s>>>(X.P, L);
             CK(cudaEventRecord(ev[2], X.s));

@@ -43,7 +43,10 @@ __device__ __forceinline__ double led(double a, double bmin, double bmax, int ns
 }
 
 // Interior edge flux f of edge e (i1 -> i2), added to rhs(i1) and
-// subtracted from rhs(i2).
+// subtracted from rhs(i2).  FT is the fluxType and O2 selects the HLLC
+// reconstruction; both are compile-time so that each kernel instance only
+// holds the registers of its own flux.
+template <int FT, bool O2>
 __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, int e, int i1, int i2, double *f) {
     const NodeState a = load_state(L, i1), b = load_state(L, i2);
     const double gam = P.gamma, gam1 = P.gm1;
@@ -57,16 +60,16 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
     double E2 = b.E, rh2 = b.E + pr2;
     const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
     f[0] = f[1] = f[2] = f[3] = f[4] = 0.0;
-    if (P.fluxType == 1 || P.fluxType == 4) {
+    if constexpr (FT == 1 || FT == 4) {
         // central flux (def_par:1664-1669); HLLC starts from it too (:1798)
         f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
         f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
         f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
         f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
         f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
-        if (P.fluxType == 1) return;
+        if constexpr (FT == 1) return;
     }
-    if (P.fluxType == 2) {  // local Lax-Friedrichs (def_par:1670-1724)
+    if constexpr (FT == 2) {  // local Lax-Friedrichs (def_par:1670-1724)
         double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
         if (rnorm > 1.0e-10) {
             double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
@@ -87,7 +90,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         }
         return;
     }
-    if (P.fluxType == 3) {  // Roe (def_par:1725-1792)
+    if constexpr (FT == 3) {  // Roe (def_par:1725-1792)
         double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
         if (rnorm > 1.0e-10) {
             double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
@@ -122,6 +125,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         }
         return;
     }
+    if constexpr (FT == 4) {
     // HLLC (def_par:1794-2085)
     double roe1 = a.r, roe2 = b.r, re1 = a.E, re2 = b.E;
     double wx2 = 2.0 * wx, wy2 = 2.0 * wy, wz2 = 2.0 * wz;
@@ -129,7 +133,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
     double rnorm1 = rnorm;
     if (rnorm > 0.0) rnorm = 1.0 / rnorm;
     double rnx = wx2 * rnorm, rny = wy2 * rnorm, rnz = wz2 * rnorm;
-    if (P.hllcOrder > 1) {
+    if constexpr (O2) {
         double dpvl[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         if (L.grid == 1) {
             // coarse levels have zero coordinates: dx = 0 gives dpvl = 0
@@ -249,6 +253,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         f[2] = ((rnx * (rv2 * u2) + rny * (rv2 * v2 + pr2)) + rnz * (rv2 * w2)) * rnorm1;
         f[3] = ((rnx * (rw2 * u2) + rny * (rw2 * v2)) + rnz * (rw2 * w2 + pr2)) * rnorm1;
         f[4] = ((rnx * (rh2 * u2) + rny * (rh2 * v2)) + rnz * (rh2 * w2)) * rnorm1;
+    }
     }
 }
 

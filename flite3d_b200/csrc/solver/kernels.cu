@@ -185,6 +185,152 @@ __global__ void k_first_order_diss(Params P, LevelView L) {
     for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
 }
 
+// ---- makeViscosityTerm, wide stencil (def_par:5198-5893) ------------------
+// pass 1: Galerkin gradients of (u, v, w, T), then per node the Sutherland
+// viscosity (T^1.5 evaluated as T*sqrt(T)), the stress tensor and heat
+// flux, the adiabatic-wall projection and the wall stress (level 1)
+__global__ void k_visc_grad(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double gOg = P.gamma / (P.gamma - 1.0);
+    double g[12];
+    for (int c = 0; c < 12; ++c) g[c] = 0.0;
+    auto prim = [&](int j, double *q) {
+        double r = L.u[j];
+        q[0] = L.u[N + j] / r; q[1] = L.u[2 * N + j] / r; q[2] = L.u[3 * N + j] / r;
+        q[3] = gOg * L.p[j] / r;
+    };
+    double qi[4];
+    prim(i, qi);
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int e = t.x >= 0 ? t.x : ~t.x;
+        double qj[4];
+        prim(t.y, qj);
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 4; ++c) {
+                double d = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
+                g[a * 4 + c] = t.x >= 0 ? g[a * 4 + c] + d : g[a * 4 + c] - d;
+            }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        int2 nd = L.bedge[b];
+        double q1[4], q2[4];
+        prim(nd.x, q1); prim(nd.y, q2);
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 4; ++c) {
+                double s = q1[c] + q2[c];
+                double own = side == 0 ? q1[c] : q2[c];
+                g[a * 4 + c] = g[a * 4 + c] + (2. * own + s) * w[a];
+            }
+    }
+    const double vt = 1. / L.V[i];
+    double dudx = g[0] * vt, dvdx = g[1] * vt, dwdx = g[2] * vt, dTdx = g[3] * vt;
+    double dudy = g[4] * vt, dvdy = g[5] * vt, dwdy = g[6] * vt, dTdy = g[7] * vt;
+    double dudz = g[8] * vt, dvdz = g[9] * vt, dwdz = g[10] * vt, dTdz = g[11] * vt;
+    const double tempConv = (P.gamma - 1.0) * P.mach * P.mach;
+    double T = gOg * L.p[i] / L.u[i];
+    if (T <= 0.001) T = 0.001;
+    double a = tempConv * T;
+    double mu = (1. / P.Re) * ((a * sqrt(a)) * ((P.Tinf + 198.6) / (tempConv * P.Tinf * T + 198.6)));
+    double kc = (1. / P.Pr) * mu;
+    L.mu[i] = mu;
+    const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+    double tau[9];
+    tau[0] = mu * (fourThirds * dudx - twoThirds * (dvdy + dwdz));
+    tau[1] = mu * (dudy + dvdx);
+    tau[2] = mu * (dudz + dwdx);
+    tau[3] = mu * (fourThirds * dvdy - twoThirds * (dudx + dwdz));
+    tau[4] = mu * (dvdz + dwdy);
+    tau[5] = mu * (fourThirds * dwdz - twoThirds * (dudx + dvdy));
+    tau[6] = kc * dTdx;
+    tau[7] = kc * dTdy;
+    tau[8] = kc * dTdz;
+    const unsigned char cls = L.bc[i];
+    if (L.grid == 1 && cls != BC_NONE) {
+        double n0 = L.nx[i], n1 = L.ny[i], n2 = L.nz[i];
+        if (cls == BC_WALL) {  // setTemperatureForAdiabaticWall (def_par:5170-5196)
+            double nt = (tau[6] * n0 + tau[7] * n1) + tau[8] * n2;
+            tau[6] = tau[6] - nt * n0;
+            tau[7] = tau[7] - nt * n1;
+            tau[8] = tau[8] - nt * n2;
+        }
+        L.wstress[i] = (tau[0] * n0 + tau[1] * n1) + tau[2] * n2;
+        L.wstress[N + i] = (tau[1] * n0 + tau[3] * n1) + tau[4] * n2;
+        L.wstress[2 * N + i] = (tau[2] * n0 + tau[4] * n1) + tau[5] * n2;
+    }
+    for (int c = 0; c < 9; ++c) L.tau[c * N + i] = tau[c];
+}
+
+// pass 2: viscous edge fluxes gathered per node and subtracted from the
+// dissipation vector (def_par:5662-5892)
+__global__ void k_visc_flux(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double ti[9], ui[3];
+    for (int c = 0; c < 9; ++c) ti[c] = L.tau[c * N + i];
+    ui[0] = L.u[N + i] / L.u[i]; ui[1] = L.u[2 * N + i] / L.u[i]; ui[2] = L.u[3 * N + i] / L.u[i];
+    double acc[4] = {0, 0, 0, 0};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int e = t.x >= 0 ? t.x : ~t.x, j = t.y;
+        double tj[9], uj[3];
+        for (int c = 0; c < 9; ++c) tj[c] = L.tau[c * N + j];
+        uj[0] = L.u[N + j] / L.u[j]; uj[1] = L.u[2 * N + j] / L.u[j]; uj[2] = L.u[3 * N + j] / L.u[j];
+        const bool first = t.x >= 0;
+        const double *a = first ? ti : tj, *b = first ? tj : ti;
+        const double *ua = first ? ui : uj, *ub = first ? uj : ui;
+        const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
+        double dt[9];
+        for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
+        double dut1 = ((((ua[0] * a[0] + ub[0] * b[0]) + ua[1] * a[1]) + ub[1] * b[1]) + ua[2] * a[2]) + ub[2] * b[2];
+        double dut2 = ((((ua[0] * a[1] + ub[0] * b[1]) + ua[1] * a[3]) + ub[1] * b[3]) + ua[2] * a[4]) + ub[2] * b[4];
+        double dut3 = ((((ua[0] * a[2] + ub[0] * b[2]) + ua[1] * a[4]) + ub[1] * b[4]) + ua[2] * a[5]) + ub[2] * b[5];
+        double f[4];
+        f[0] = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+        f[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+        f[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+        f[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+        for (int c = 0; c < 4; ++c) acc[c] = first ? acc[c] + f[c] : acc[c] - f[c];
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int bb = L.binc[k] >> 1, side = L.binc[k] & 1;
+        int ind = L.bind[bb];
+        if (ind == 2 || ind == 9) continue;
+        int2 nd = L.bedge[bb];
+        double a[9], b[9], ua[3], ub[3];
+        for (int c = 0; c < 9; ++c) { a[c] = L.tau[c * N + nd.x]; b[c] = L.tau[c * N + nd.y]; }
+        ua[0] = L.u[N + nd.x] / L.u[nd.x]; ua[1] = L.u[2 * N + nd.x] / L.u[nd.x]; ua[2] = L.u[3 * N + nd.x] / L.u[nd.x];
+        ub[0] = L.u[N + nd.y] / L.u[nd.y]; ub[1] = L.u[2 * N + nd.y] / L.u[nd.y]; ub[2] = L.u[3 * N + nd.y] / L.u[nd.y];
+        const double wx = L.bwx[bb], wy = L.bwy[bb], wz = L.bwz[bb];
+        double dt[9];
+        for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
+        double d11 = (ua[0] * a[0] + ua[1] * a[1]) + ua[2] * a[2];
+        double d12 = (ub[0] * b[0] + ub[1] * b[1]) + ub[2] * b[2];
+        double d21 = (ua[0] * a[1] + ua[1] * a[3]) + ua[2] * a[4];
+        double d22 = (ub[0] * b[1] + ub[1] * b[3]) + ub[2] * b[4];
+        double d31 = (ua[0] * a[2] + ua[1] * a[4]) + ua[2] * a[5];
+        double d32 = (ub[0] * b[2] + ub[1] * b[4]) + ub[2] * b[5];
+        double dut1 = d11 + d12, dut2 = d21 + d22, dut3 = d31 + d32;
+        double f2 = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+        double f3 = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+        double f4 = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+        double f5 = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+        const double *o = side == 0 ? a : b;
+        double do1 = side == 0 ? d11 : d12, do2 = side == 0 ? d21 : d22, do3 = side == 0 ? d31 : d32;
+        acc[0] = (acc[0] + f2) + 2.0 * ((wx * o[0] + wy * o[1]) + wz * o[2]);
+        acc[1] = (acc[1] + f3) + 2.0 * ((wx * o[1] + wy * o[3]) + wz * o[4]);
+        acc[2] = (acc[2] + f4) + 2.0 * ((wx * o[2] + wy * o[4]) + wz * o[5]);
+        acc[3] = (acc[3] + f5) + 2.0 * ((wx * (o[6] + do1) + wy * (o[7] + do2)) + wz * (o[8] + do3));
+    }
+    for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
+}
+
 __global__ void k_fill(double *a, size_t n, double v) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = v;
@@ -258,15 +404,21 @@ __global__ void k_minmax(Params P, LevelView L) {
 }
 
 // ---- interior edge flux into the edge buffer ------------------------------
-__global__ void k_edge_flux(Params P, LevelView L) {
+template <int FT, bool O2>
+__global__ void __launch_bounds__(256) k_edge_flux(Params P, LevelView L) {
     int e = tid();
     if (e >= L.E) return;
     int2 nd = L.edge[e];
     double f[5];
-    edge_flux(P, L, e, nd.x, nd.y, f);
+    edge_flux<FT, O2>(P, L, e, nd.x, nd.y, f);
     double *o = L.flux + (size_t)e * 5;
     o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = f[3]; o[4] = f[4];
 }
+template __global__ void k_edge_flux<1, false>(Params, LevelView);
+template __global__ void k_edge_flux<2, false>(Params, LevelView);
+template __global__ void k_edge_flux<3, false>(Params, LevelView);
+template __global__ void k_edge_flux<4, false>(Params, LevelView);
+template __global__ void k_edge_flux<4, true>(Params, LevelView);
 
 // ---- boundary-edge contributions ------------------------------------------
 __global__ void k_bnd_flux(Params P, LevelView L) {
@@ -587,7 +739,18 @@ __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, doub
         acc[2] -= A * dp * dn2;
         acc[4] += xd * A * dp * dn2 - yd * A * dp * dt;
         acc[5] += xd * A * dp * dn1 - zd * A * dp * dt;
-        (void)N;
+        if (P.viscous) {
+            double s0 = L.wstress[ip], s1 = L.wstress[N + ip], s2 = L.wstress[2 * N + ip];
+            double sn1 = (s0 * fn1[0] + s1 * fn1[1]) + s2 * fn1[2];
+            double sn2 = (s0 * fn2[0] + s1 * fn2[1]) + s2 * fn2[2];
+            double st = (s0 * ft[0] + s1 * ft[1]) + s2 * ft[2];
+            acc[0] += A * sn1;
+            acc[2] += A * sn2;
+            acc[1] += A * st;
+            acc[3] += A * st;
+            acc[4] += -xd * A * sn2 + yd * A * st;
+            acc[5] += -xd * A * sn1 + zd * A * st;
+        }
     }
     for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = acc[k];
     __syncthreads();
@@ -600,7 +763,7 @@ __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, doub
         out[0] = 2.0 * red[0][0];
         out[1] = 2.0 * red[1][0];
         out[2] = 2.0 * red[2][0];
-        out[3] = 0.0;
+        out[3] = 2.0 * red[3][0];
         out[4] = red[4][0];
         out[5] = red[5][0];
     }

@@ -11,9 +11,12 @@ __global__ void k_timestep(Params P, LevelView L);
 __global__ void k_jst_lap(Params P, LevelView L);
 __global__ void k_jst_flux(Params P, LevelView L);
 __global__ void k_first_order_diss(Params P, LevelView L);
+__global__ void k_visc_grad(Params P, LevelView L);
+__global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
 __global__ void k_minmax(Params P, LevelView L);
+template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 __global__ void k_bnd_flux(Params P, LevelView L);
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);

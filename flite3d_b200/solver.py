@@ -113,8 +113,10 @@ class Solver:
         assert u.shape == (5, self.nodes[level - 1])
         self._ck(self.be.set_state(self._h, level, _ptr(u)), "set_state")
 
-    def get_state(self, level=1):
-        u = np.zeros((5, self.nodes[level - 1]))
+    def get_state(self, level=1, out=None):
+        u = np.zeros((5, self.nodes[level - 1])) if out is None else out
+        assert u.shape == (5, self.nodes[level - 1]) and u.dtype == np.float64
+        assert u.flags["C_CONTIGUOUS"]
         self._ck(self.be.get_state(self._h, level, _ptr(u)), "get_state")
         return u
 

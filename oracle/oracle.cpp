@@ -197,6 +197,144 @@ struct Oracle {
         }
     }
 
+    // ---- makeViscosityTerm, wide stencil (def_par:5198-5893) --------------
+    // Sutherland's (T)^1.5 is evaluated as T*sqrt(T).
+    void makeViscosityTerm(Level &g) {
+        const double gOg = c.gamma / (c.gamma - 1.0);
+        const double tempConv = (c.gamma - 1.0) * c.MachNumber * c.MachNumber;
+        const double Tin = c.inflowTemperature;
+        for (int k = 0; k < 12; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        auto prim = [&](int i, double *q) {
+            double r = g.u[0][i];
+            q[0] = g.u[1][i] / r; q[1] = g.u[2][i] / r; q[2] = g.u[3][i] / r;
+            q[3] = gOg * g.p[i] / r;
+        };
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double w[3] = {g.wx[e], g.wy[e], g.wz[e]};
+            double q1[4], q2[4];
+            prim(i1, q1); prim(i2, q2);
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    double d = (q1[k] + q2[k]) * w[a];
+                    nh[a * 4 + k][i1] = nh[a * 4 + k][i1] + d;
+                    nh[a * 4 + k][i2] = nh[a * 4 + k][i2] - d;
+                }
+        }
+        for (int b = 0; b < g.B; ++b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
+            double q1[4], q2[4];
+            prim(i1, q1); prim(i2, q2);
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    double s = q1[k] + q2[k];
+                    nh[a * 4 + k][i1] = nh[a * 4 + k][i1] + (2. * q1[k] + s) * w[a];
+                }
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    double s = q1[k] + q2[k];
+                    nh[a * 4 + k][i2] = nh[a * 4 + k][i2] + (2. * q2[k] + s) * w[a];
+                }
+        }
+        const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+        const double oRe = 1. / c.ReynoldsNumber, oPr = 1. / c.PrandtlNumber;
+        for (int i = 0; i < g.N; ++i) {
+            double vt = 1. / g.V[i];
+            double dudx = nh[0][i] * vt, dvdx = nh[1][i] * vt, dwdx = nh[2][i] * vt, dTdx = nh[3][i] * vt;
+            double dudy = nh[4][i] * vt, dvdy = nh[5][i] * vt, dwdy = nh[6][i] * vt, dTdy = nh[7][i] * vt;
+            double dudz = nh[8][i] * vt, dvdz = nh[9][i] * vt, dwdz = nh[10][i] * vt, dTdz = nh[11][i] * vt;
+            double T = gOg * g.p[i] / g.u[0][i];
+            if (T <= 0.001) T = 0.001;
+            double a = tempConv * T;
+            double mu = oRe * ((a * std::sqrt(a)) * ((Tin + 198.6) / (tempConv * Tin * T + 198.6)));
+            double k = oPr * mu;
+            g.mu[i] = mu;
+            nh[0][i] = mu * (fourThirds * dudx - twoThirds * (dvdy + dwdz));
+            nh[1][i] = mu * (dudy + dvdx);
+            nh[2][i] = mu * (dudz + dwdx);
+            nh[3][i] = mu * (fourThirds * dvdy - twoThirds * (dudx + dwdz));
+            nh[4][i] = mu * (dvdz + dwdy);
+            nh[5][i] = mu * (fourThirds * dwdz - twoThirds * (dudx + dvdy));
+            nh[6][i] = k * dTdx;
+            nh[7][i] = k * dTdy;
+            nh[8][i] = k * dTdz;
+        }
+        if (g.grid == 1) {
+            // setTemperatureForAdiabaticWall (def_par:5170-5196)
+            for_range(g, -20, -19, [&](int ip) {
+                double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+                double dT[3] = {nh[6][ip], nh[7][ip], nh[8][ip]};
+                double nt = (dT[0] * n[0] + dT[1] * n[1]) + dT[2] * n[2];
+                for (int k = 0; k < 3; ++k) nh[6 + k][ip] = dT[k] - nt * n[k];
+            });
+            // wall stress of the boundary nodes (def_par:5620-5635)
+            for (int ib = 0; ib < std::min(g.Nb, g.nnorm); ++ib) {
+                int ip = g.node_ind[ib];
+                double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+                g.wallStress[0][ip] = (nh[0][ip] * n[0] + nh[1][ip] * n[1]) + nh[2][ip] * n[2];
+                g.wallStress[1][ip] = (nh[1][ip] * n[0] + nh[3][ip] * n[1]) + nh[4][ip] * n[2];
+                g.wallStress[2][ip] = (nh[2][ip] * n[0] + nh[4][ip] * n[1]) + nh[5][ip] * n[2];
+            }
+        }
+        for (int k = 9; k < 13; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        auto loadt = [&](int i, double *t, double *uu) {
+            for (int k = 0; k < 9; ++k) t[k] = nh[k][i];
+            uu[0] = g.u[1][i] / g.u[0][i]; uu[1] = g.u[2][i] / g.u[0][i]; uu[2] = g.u[3][i] / g.u[0][i];
+        };
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+            double a[9], b[9], ua[3], ub[3];
+            loadt(i1, a, ua); loadt(i2, b, ub);
+            double dt[9];
+            for (int k = 0; k < 9; ++k) dt[k] = a[k] + b[k];
+            double dut1 = ((((ua[0] * a[0] + ub[0] * b[0]) + ua[1] * a[1]) + ub[1] * b[1]) + ua[2] * a[2]) + ub[2] * b[2];
+            double dut2 = ((((ua[0] * a[1] + ub[0] * b[1]) + ua[1] * a[3]) + ub[1] * b[3]) + ua[2] * a[4]) + ub[2] * b[4];
+            double dut3 = ((((ua[0] * a[2] + ub[0] * b[2]) + ua[1] * a[4]) + ub[1] * b[4]) + ua[2] * a[5]) + ub[2] * b[5];
+            double f2 = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+            double f3 = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+            double f4 = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+            double f5 = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+            double f[4] = {f2, f3, f4, f5};
+            for (int k = 0; k < 4; ++k) {
+                nh[9 + k][i1] = nh[9 + k][i1] + f[k];
+                nh[9 + k][i2] = nh[9 + k][i2] - f[k];
+            }
+        }
+        for (int bb = 0; bb < g.B; ++bb) {
+            int ind = g.bind[bb];
+            if (ind == 2 || ind == 9) continue;
+            int i1 = g.b1[bb], i2 = g.b2[bb];
+            double wx = g.bwx[bb], wy = g.bwy[bb], wz = g.bwz[bb];
+            double a[9], b[9], ua[3], ub[3];
+            loadt(i1, a, ua); loadt(i2, b, ub);
+            double dt[9];
+            for (int k = 0; k < 9; ++k) dt[k] = a[k] + b[k];
+            double d11 = (ua[0] * a[0] + ua[1] * a[1]) + ua[2] * a[2];
+            double d12 = (ub[0] * b[0] + ub[1] * b[1]) + ub[2] * b[2];
+            double d21 = (ua[0] * a[1] + ua[1] * a[3]) + ua[2] * a[4];
+            double d22 = (ub[0] * b[1] + ub[1] * b[3]) + ub[2] * b[4];
+            double d31 = (ua[0] * a[2] + ua[1] * a[4]) + ua[2] * a[5];
+            double d32 = (ub[0] * b[2] + ub[1] * b[4]) + ub[2] * b[5];
+            double dut1 = d11 + d12, dut2 = d21 + d22, dut3 = d31 + d32;
+            double f2 = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+            double f3 = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+            double f4 = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+            double f5 = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+            nh[9][i1] = (nh[9][i1] + f2) + 2.0 * ((wx * a[0] + wy * a[1]) + wz * a[2]);
+            nh[10][i1] = (nh[10][i1] + f3) + 2.0 * ((wx * a[1] + wy * a[3]) + wz * a[4]);
+            nh[11][i1] = (nh[11][i1] + f4) + 2.0 * ((wx * a[2] + wy * a[4]) + wz * a[5]);
+            nh[12][i1] = (nh[12][i1] + f5) + 2.0 * ((wx * (a[6] + d11) + wy * (a[7] + d21)) + wz * (a[8] + d31));
+            nh[9][i2] = (nh[9][i2] + f2) + 2.0 * ((wx * b[0] + wy * b[1]) + wz * b[2]);
+            nh[10][i2] = (nh[10][i2] + f3) + 2.0 * ((wx * b[1] + wy * b[3]) + wz * b[4]);
+            nh[11][i2] = (nh[11][i2] + f4) + 2.0 * ((wx * b[2] + wy * b[4]) + wz * b[5]);
+            nh[12][i2] = (nh[12][i2] + f5) + 2.0 * ((wx * (b[6] + d12) + wy * (b[7] + d22)) + wz * (b[8] + d32));
+        }
+        for (int i = 0; i < g.N; ++i)
+            for (int k = 0; k < 4; ++k) g.diss[1 + k][i] = g.diss[1 + k][i] - nh[9 + k][i];
+    }
+
     // ---- computeGradient, Galerkin (def_par:2923-3245) --------------------
     void computeGradient(Level &g, vec *u) {
         for (int k = 0; k < 15; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
@@ -730,6 +868,7 @@ struct Oracle {
             for (int i = 0; i < g.N; ++i) g.p[i] = std::fabs(g.p[i]);
             makeTimeSteps(g);
             dissipation_for(g, false);
+            if (c.ReynoldsNumber > 0.0) makeViscosityTerm(g);
         }
         for (int st = 1; st <= 3; ++st) {
             makePressureField(g, g.u);
@@ -799,6 +938,7 @@ struct Oracle {
         makeTimeSteps(C);
         if (c.coarseGridDissipationScheme == 2) makeArtificialDissipation2(C);
         else if (c.coarseGridDissipationScheme == 3) makeArtificialDissipation3(C);
+        if (c.ReynoldsNumber > 0.0) makeViscosityTerm(C);
         for (int k = 0; k < 5; ++k) std::fill(C.rhs[k].begin(), C.rhs[k].end(), 0.0);
         makeRHS(C);
         for (int k = 0; k < 5; ++k)
@@ -815,6 +955,7 @@ struct Oracle {
         makePressureField(F, F.u);
         for (int i = 0; i < F.N; ++i) F.p[i] = std::fabs(F.p[i]);
         dissipation_for(F, true);
+        if (c.ReynoldsNumber > 0.0) makeViscosityTerm(F);
         for (int k = 0; k < 5; ++k) std::fill(F.rhs[k].begin(), F.rhs[k].end(), 0.0);
         makeRHS(F);
         for (int k = 0; k < 5; ++k)
@@ -1003,7 +1144,7 @@ int check_controls(const flite_controls &c) {
         c.prolongationSmoothingFactor > 0)
         return FLITE_EUNSUPPORTED;
     if (c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
-    if (c.ReynoldsNumber > 0) return FLITE_EUNSUPPORTED;
+    if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return FLITE_EUNSUPPORTED;
     if (c.fluxType < 1 || c.fluxType > 4) return FLITE_EUNSUPPORTED;
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1) return FLITE_EUNSUPPORTED;
     if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
@@ -1133,6 +1274,7 @@ int oracle_get_array(oracle_ctx *o, int level, const char *name, double *out) {
     else if (n == "mu") std::memcpy(out, g->mu.data(), 8 * N);
     else if (n == "conn") std::memcpy(out, g->conn.data(), 8 * N);
     else if (n == "wallArea") std::memcpy(out, g->wallArea.data(), 8 * N);
+    else if (n == "wallStress") cols(g->wallStress, 3);
     else if (n == "normal") {
         std::memcpy(out, g->nx.data(), 8 * N); std::memcpy(out + N, g->ny.data(), 8 * N);
         std::memcpy(out + 2 * N, g->nz.data(), 8 * N);
@@ -1251,6 +1393,7 @@ int oracle_eval_dissipation(oracle_ctx *o, int level) {
     for (int i = 0; i < g->N; ++i) g->p[i] = std::fabs(g->p[i]);
     o->o.makeTimeSteps(*g);
     o->o.dissipation_for(*g, false);
+    if (o->o.c.ReynoldsNumber > 0.0) o->o.makeViscosityTerm(*g);
     return FLITE_OK;
 }
 

@@ -29,9 +29,15 @@ CASES = {
     "alpha_beta": dict(fluxType=1, alpha=3.0, beta=2.0),
     "supersonic_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1, MachNumber=1.3,
                              CFLNumber=1.0),
-    "dissipation_weighting": dict(fluxType=1, useDissipationWeighting=1),
+    "dissipation_weighting": dict(fluxType=1, useDissipationWeighting=1, CFLNumber=0.5,
+                                  fourthOrderDissipationFactor=0.05),
     "relax_steps2": dict(fluxType=1, numberOfRelaxationSteps=2, prolongationRelaxation=0.8,
                          multigridBCRelaxation=0.5, maxIncrementFactor=0.05),
+    "laminar_adiabatic": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=1),
+    "laminar_isothermal": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=0,
+                               CFLNumber=0.5),
+    "laminar_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1,
+                          ReynoldsNumber=5000.0, wallsAreIsentropic=1),
 }
 SCHEMES = [0, 1, 2, 4, 5, 7]
 
