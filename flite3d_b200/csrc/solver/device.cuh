@@ -58,6 +58,11 @@ struct LevelView {
     double *grad;                          // [15][N] (level 1, HLLC order 2)
     double *bnd;                           // [10][N]
     double *flux;                          // [E][5] edge flux buffer
+    // mixed precision (FLITE_MIXED): FP32 shadows of the state and edge
+    // coefficients, and the FP32 edge buffer
+    float *u32, *p32;                      // [5][N], [N]
+    const float *wx32, *wy32, *wz32;       // [E]
+    float *flux32;                         // [E][5]
     double *bflux;                         // [B][10] boundary-edge contributions
     int *cyc;                              // cycle number of this level
 };

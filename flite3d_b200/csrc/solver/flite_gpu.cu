@@ -140,7 +140,8 @@ struct flite_ctx {
         const LevelView &L = V(l);
         if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
             counted();
-            k_gradient<<<blocks(L.N), kBlock, 0, s>>>(P, L);
+            if (c.GradientMethod == 1) k_gradient<<<blocks(L.N), kBlock, 0, s>>>(P, L);
+            else k_ls_gradient<<<blocks(L.N), kBlock, 0, s>>>(P, L);
             if (c.Automaticlipping == 1) {
                 counted();
                 k_minmax<<<blocks(L.N), kBlock, 0, s>>>(P, L);
@@ -155,10 +156,18 @@ struct flite_ctx {
             k_bnd_flux<<<blocks(L.B), kBlock, 0, s>>>(P, L);
         }
     }
+    bool mixed() const { return c.precision == FLITE_MIXED; }
     // the flux kernel instance of this run's fluxType (and HLLC order; the
     // reconstruction only acts on level 1, where coordinates exist)
     void edge_flux_launch(const LevelView &L) {
         const unsigned nb = blocks(L.E);
+        if (mixed()) {
+            // FP32 fluxes from FP32 shadows of the state (central flux)
+            k_shadow<<<blocks(L.N), kBlock, 0, s>>>(L);
+            counted();
+            k_edge_flux_f32_central<<<nb, kBlock, 0, s>>>(L);
+            return;
+        }
         switch (c.fluxType) {
             case 1: k_edge_flux<1, false><<<nb, kBlock, 0, s>>>(P, L); break;
             case 2: k_edge_flux<2, false><<<nb, kBlock, 0, s>>>(P, L); break;
@@ -170,7 +179,8 @@ struct flite_ctx {
     }
     void node_update(int l, int mode, int stage) {
         counted();
-        k_node_update<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l), mode, stage);
+        if (mixed()) k_node_update<true><<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l), mode, stage);
+        else k_node_update<false><<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l), mode, stage);
     }
 
     // ---- singleIteration (def_par:1002-1181) -----------------------------
@@ -376,13 +386,15 @@ const char *unsupported_reason(const flite_controls &c) {
     if (c.turbulenceModel != 0) return "turbulenceModel != 0 is not supported yet";
     if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return "viscosityScheme 2 is not supported";
     if (c.fluxType < 1 || c.fluxType > 4) return "fluxType must be 1..4";
-    if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1)
-        return "least-squares gradients are not supported (GradientMethod must be 1)";
+    if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
+        return "least-squares gradients need numberOfGridsToUse = 1: the reference's LS gradient divides "
+               "by |dx|^2 of coarse-level coordinates it never fills";
     if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1)
         return "dissipation scheme 1 is not supported";
     if (c.useMatrixDissipation) return "matrix dissipation is not supported";
     if (c.prolongationMappingScheme != 1) return "prolongationMappingScheme must be 1";
-    if (c.precision != FLITE_FP64) return "only FLITE_FP64 is available in this build";
+    if (c.precision != FLITE_FP64 && c.precision != FLITE_MIXED) return "precision must be FLITE_FP64 or FLITE_MIXED";
+    if (c.precision == FLITE_MIXED && c.fluxType != 1) return "FLITE_MIXED supports the central flux (fluxType 1)";
     int s = c.multigridScheme;
     if (!(s <= 0 || (s >= 1 && s <= 5) || s == 7)) return "multigridScheme not implemented";
     return nullptr;
@@ -578,7 +590,20 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
             CK(cudaMemset(L.wstress, 0, 3 * (size_t)N * sizeof(double)));
             L.grad = hllc2 ? X.alloc<double>(15 * (size_t)N) : nullptr;
             L.bnd = hllc2 ? X.alloc<double>(10 * (size_t)N) : nullptr;
-            L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
+            if (c->precision == FLITE_MIXED) {
+                L.u32 = X.alloc<float>(5 * (size_t)N);
+                L.p32 = X.alloc<float>(N);
+                std::vector<float> w32(3 * (size_t)std::max(E, 1));
+                for (int e = 0; e < E; ++e) {
+                    w32[e] = (float)wx[e]; w32[(size_t)E + e] = (float)wy[e]; w32[2 * (size_t)E + e] = (float)wz[e];
+                }
+                float *dw = X.upload(w32);
+                L.wx32 = dw; L.wy32 = dw + E; L.wz32 = dw + 2 * (size_t)E;
+                L.flux32 = X.alloc<float>(5 * (size_t)std::max(E, 1));
+                L.flux = X.alloc<double>(5);  // unused in this mode
+            } else {
+                L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
+            }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
             L.cyc = X.d_cyc + l;
             if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
@@ -826,7 +851,8 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, do
             CK(cudaEventRecord(ev[1], X.s));
             if (L.B > 0) k_bnd_flux<<<flite_ctx::blocks(L.B), kBlock, 0, X.s>>>(X.P, L);
             CK(cudaEventRecord(ev[2], X.s));
-            k_node_update<<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            if (X.mixed()) k_node_update<true><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            else k_node_update<false><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
             CK(cudaEventRecord(ev[3], X.s));
             CK(cudaEventSynchronize(ev[3]));
             float a = 0, b = 0;

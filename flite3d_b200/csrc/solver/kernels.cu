@@ -376,6 +376,51 @@ __global__ void k_gradient(Params P, LevelView L) {
     for (int c = 0; c < 15; ++c) L.grad[c * N + i] = g[c] * vt;
 }
 
+// ---- LSComputeGradient + computegradhat (def_par:2593-2920) ---------------
+// the moment matrix is the same for the five scalars and is built once; the
+// right-hand sides of the five scalars are gathered in the same edge order
+__global__ void k_ls_gradient(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double m[6] = {0, 0, 0, 0, 0, 0}, b[5][3];
+    for (int sc = 0; sc < 5; ++sc) b[sc][0] = b[sc][1] = b[sc][2] = 0.0;
+    const double ri = L.u[i];
+    const double qi[5] = {ri, L.u[N + i] / ri, L.u[2 * N + i] / ri, L.u[3 * N + i] / ri, L.u[4 * N + i]};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int2 t = L.inc[k];
+        int j = t.y;
+        const bool first = t.x >= 0;
+        const int i1 = first ? i : j, i2 = first ? j : i;
+        double dx = L.cx[i2] - L.cx[i1], dy = L.cy[i2] - L.cy[i1], dz = L.cz[i2] - L.cz[i1];
+        double dist1 = 1. / ((dx * dx + dy * dy) + dz * dz);
+        m[0] = m[0] + dx * dx * dist1; m[1] = m[1] + dx * dy * dist1; m[2] = m[2] + dx * dz * dist1;
+        m[3] = m[3] + dy * dy * dist1; m[4] = m[4] + dy * dz * dist1; m[5] = m[5] + dz * dz * dist1;
+        const double rj = L.u[j];
+        const double qj[5] = {rj, L.u[N + j] / rj, L.u[2 * N + j] / rj, L.u[3 * N + j] / rj, L.u[4 * N + j]};
+        for (int sc = 0; sc < 5; ++sc) {
+            double dr2 = first ? qj[sc] - qi[sc] : qi[sc] - qj[sc];  // q(i2) - q(i1)
+            b[sc][0] = b[sc][0] + dr2 * dx * dist1;
+            b[sc][1] = b[sc][1] + dr2 * dy * dist1;
+            b[sc][2] = b[sc][2] + dr2 * dz * dist1;
+        }
+    }
+    double a11 = m[0], a12 = m[1], a13 = m[2], a21 = m[1], a22 = m[3], a23 = m[4], a31 = m[2], a32 = m[4], a33 = m[5];
+    double c11 = a22 * a33 - a23 * a32, c21 = a23 * a31 - a21 * a33, c31 = a21 * a32 - a22 * a31;
+    double det = (a11 * c11 + a12 * c21) + a13 * c31;
+    if (fabs(det) > 0.0) det = 1.0 / det;
+    c11 = det * c11; c21 = det * c21; c31 = det * c31;
+    double c12 = det * (a13 * a32 - a12 * a33), c22 = det * (a11 * a33 - a13 * a31);
+    double c32 = det * (a12 * a31 - a11 * a32), c13 = det * (a12 * a23 - a13 * a22);
+    double c23 = det * (a13 * a21 - a23 * a11), c33 = det * (a11 * a22 - a12 * a21);
+    for (int sc = 0; sc < 5; ++sc) {
+        double b1 = b[sc][0], b2 = b[sc][1], b3 = b[sc][2];
+        L.grad[sc * N + i] = (c11 * b1 + c12 * b2) + c13 * b3;
+        L.grad[(5 + sc) * N + i] = (c21 * b1 + c22 * b2) + c23 * b3;
+        L.grad[(10 + sc) * N + i] = (c31 * b1 + c32 * b2) + c33 * b3;
+    }
+}
+
 // ---- LocalMinMax (def_par:3248-3459) ---------------------------------------
 __global__ void k_minmax(Params P, LevelView L) {
     int i = tid();
@@ -430,6 +475,69 @@ __global__ void k_bnd_flux(Params P, LevelView L) {
     for (int k = 0; k < 5; ++k) { o[k] = g1[k]; o[5 + k] = g2[k]; }
 }
 
+// ---- mixed precision ------------------------------------------------------
+// FP32 shadows of the conserved state and pressure for the FP32 edge fluxes
+__global__ void k_shadow(LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    for (int c = 0; c < 5; ++c) L.u32[c * N + i] = (float)L.u[c * N + i];
+    L.p32[i] = (float)L.p[i];
+}
+
+// central flux (def_par:1664-1669) in FP32 into the FP32 edge buffer
+__global__ void __launch_bounds__(256) k_edge_flux_f32_central(LevelView L) {
+    int e = tid();
+    if (e >= L.E) return;
+    const int N = L.N;
+    const int2 nd = L.edge[e];
+    const int i1 = nd.x, i2 = nd.y;
+    const float r1 = L.u32[i1], ru1 = L.u32[N + i1], rv1 = L.u32[2 * N + i1], rw1 = L.u32[3 * N + i1];
+    const float E1 = L.u32[4 * N + i1], pr1 = L.p32[i1];
+    const float r2 = L.u32[i2], ru2 = L.u32[N + i2], rv2 = L.u32[2 * N + i2], rw2 = L.u32[3 * N + i2];
+    const float E2 = L.u32[4 * N + i2], pr2 = L.p32[i2];
+    const float rinv1 = 1.f / r1, rinv2 = 1.f / r2;
+    const float u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1, rh1 = E1 + pr1;
+    const float u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2, rh2 = E2 + pr2;
+    const float wx = L.wx32[e], wy = L.wy32[e], wz = L.wz32[e];
+    float *o = L.flux32 + (size_t)e * 5;
+    o[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
+    o[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
+    o[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
+    o[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+    o[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+    (void)E1; (void)E2;
+}
+
+// error-free sum s + x = hi + lo (Knuth's TwoSum; additions only)
+__device__ __forceinline__ void two_sum(float a, float b, float &hi, float &lo) {
+    float s = a + b;
+    float bp = s - a;
+    lo = (a - (s - bp)) + (b - bp);
+    hi = s;
+}
+
+// residual of node i from the FP32 edge buffer: compensated FP32 sums in
+// edge order, then the FP64 boundary-edge contributions
+__device__ __forceinline__ void gather_rhs_mixed(const LevelView &L, int i, double *r) {
+    float hi[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, lo[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int s = L.inc[k].x;
+        const float *f = L.flux32 + (size_t)(s >= 0 ? s : ~s) * 5;
+        for (int c = 0; c < 5; ++c) {
+            float e;
+            two_sum(hi[c], s >= 0 ? f[c] : -f[c], hi[c], e);
+            lo[c] += e;
+        }
+    }
+    for (int c = 0; c < 5; ++c) r[c] = (double)hi[c] + (double)lo[c];
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int v = L.binc[k];
+        const double *g = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
+        r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
+    }
+}
+
 // residual of node i: interior edges in edge order, then boundary edges
 __device__ __forceinline__ void gather_rhs(const LevelView &L, int i, double *r) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
@@ -455,12 +563,14 @@ __device__ __forceinline__ void gather_rhs(const LevelView &L, int i, double *r)
 // mode RCOARSE: restrictGrid coarse one-step (def_par:12244-12263): src
 // mode RFINE:   restrictGrid fine increment (def_par:12356-12383): rhs
 // mode RESID:   rhs <- makeRHS only
+template <bool MIXED>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
     double r[5];
-    gather_rhs(L, i, r);
+    if constexpr (MIXED) gather_rhs_mixed(L, i, r);
+    else gather_rhs(L, i, r);
     if (mode == MODE_RESID) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
@@ -504,6 +614,8 @@ __global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = un[c] - up[c];
     }
 }
+template __global__ void k_node_update<false>(Params, LevelView, int, int);
+template __global__ void k_node_update<true>(Params, LevelView, int, int);
 
 // ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
 __global__ void k_copy(const double *a, double *b, size_t n) {

@@ -15,11 +15,15 @@ __global__ void k_visc_grad(Params P, LevelView L);
 __global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
+__global__ void k_ls_gradient(Params P, LevelView L);
 __global__ void k_minmax(Params P, LevelView L);
 template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 __global__ void k_bnd_flux(Params P, LevelView L);
+template <bool MIXED>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
+__global__ void k_shadow(LevelView L);
+__global__ void k_edge_flux_f32_central(LevelView L);
 __global__ void k_copy(const double *a, double *b, size_t n);
 __global__ void k_restrict_u(LevelView C, LevelView F);
 __global__ void k_restrict_state(Params P, LevelView C, LevelView F);

@@ -372,6 +372,60 @@ struct Oracle {
         }
     }
 
+    // ---- LSComputeGradient + computegradhat (def_par:2593-2920) -----------
+    // five scalar passes (rho, u, v, w, E) of the least-squares gradient with
+    // 1/|dx|^2 weights and the adjugate inverse of the 3x3 moment matrix
+    void LSComputeGradient(Level &g, vec *u) {
+        vec grad[15];
+        for (auto &a : grad) a.assign(g.N, 0.0);
+        for (int k = 0; k < 15; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        vec v(g.N);
+        for (int sc = 0; sc < 5; ++sc) {
+            for (int i = 0; i < g.N; ++i) v[i] = (sc == 0 || sc == 4) ? u[sc][i] : u[sc][i] / u[0][i];
+            computegradhat(g, v);
+            for (int i = 0; i < g.N; ++i) {
+                grad[sc][i] = nh[9][i];
+                grad[5 + sc][i] = nh[10][i];
+                grad[10 + sc][i] = nh[11][i];
+            }
+        }
+        for (int k = 0; k < 15; ++k) nh[k] = grad[k].size() == nh[k].size() ? grad[k] : nh[k];
+        for (int k = 0; k < 15; ++k)
+            for (int i = 0; i < g.N; ++i) nh[k][i] = grad[k][i];
+    }
+    void computegradhat(Level &g, const vec &q) {
+        for (int k = 0; k < 9; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        for (int e = 0; e < g.E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double dx = g.cx[i2] - g.cx[i1], dy = g.cy[i2] - g.cy[i1], dz = g.cz[i2] - g.cz[i1];
+            double dist1 = 1. / ((dx * dx + dy * dy) + dz * dz);
+            double dr2 = q[i2] - q[i1];
+            double m[6] = {dx * dx * dist1, dx * dy * dist1, dx * dz * dist1,
+                           dy * dy * dist1, dy * dz * dist1, dz * dz * dist1};
+            for (int k = 0; k < 6; ++k) nh[k][i1] = nh[k][i1] + m[k];
+            for (int k = 0; k < 6; ++k) nh[k][i2] = nh[k][i2] + m[k];
+            double b[3] = {dr2 * dx * dist1, dr2 * dy * dist1, dr2 * dz * dist1};
+            for (int k = 0; k < 3; ++k) nh[6 + k][i1] = nh[6 + k][i1] + b[k];
+            for (int k = 0; k < 3; ++k) nh[6 + k][i2] = nh[6 + k][i2] + b[k];
+        }
+        for (int i = 0; i < g.N; ++i) {
+            double a11 = nh[0][i], a12 = nh[1][i], a13 = nh[2][i];
+            double a21 = nh[1][i], a22 = nh[3][i], a23 = nh[4][i];
+            double a31 = nh[2][i], a32 = nh[4][i], a33 = nh[5][i];
+            double c11 = a22 * a33 - a23 * a32, c21 = a23 * a31 - a21 * a33, c31 = a21 * a32 - a22 * a31;
+            double det = (a11 * c11 + a12 * c21) + a13 * c31;
+            if (std::fabs(det) > 0.0) det = 1.0 / det;
+            c11 = det * c11; c21 = det * c21; c31 = det * c31;
+            double c12 = det * (a13 * a32 - a12 * a33), c22 = det * (a11 * a33 - a13 * a31);
+            double c32 = det * (a12 * a31 - a11 * a32), c13 = det * (a12 * a23 - a13 * a22);
+            double c23 = det * (a13 * a21 - a23 * a11), c33 = det * (a11 * a22 - a12 * a21);
+            double b1 = nh[6][i], b2 = nh[7][i], b3 = nh[8][i];
+            nh[9][i] = (c11 * b1 + c12 * b2) + c13 * b3;
+            nh[10][i] = (c21 * b1 + c22 * b2) + c23 * b3;
+            nh[11][i] = (c31 * b1 + c32 * b2) + c33 * b3;
+        }
+    }
+
     // ---- LocalMinMax (def_par:3248-3459) ----------------------------------
     void LocalMinMax(Level &g) {
         for (int k = 15; k < 25; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 1.0e15);
@@ -427,7 +481,8 @@ struct Oracle {
             autoClip = c.Automaticlipping;
             nsig = c.ReynoldsNumber < 1 ? 4 : 2;
             if (hllcflux > 1) {
-                computeGradient(g, g.u);
+                if (c.GradientMethod == 1) computeGradient(g, g.u);
+                else LSComputeGradient(g, g.u);
                 if (autoClip == 1) LocalMinMax(g);
             }
         }
@@ -1146,7 +1201,10 @@ int check_controls(const flite_controls &c) {
     if (c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
     if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return FLITE_EUNSUPPORTED;
     if (c.fluxType < 1 || c.fluxType > 4) return FLITE_EUNSUPPORTED;
-    if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1) return FLITE_EUNSUPPORTED;
+    // least-squares gradients divide by |dx|^2 of coarse-level coordinates
+    // the reference never fills (0*inf = NaN): single-grid runs only
+    if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
+        return FLITE_EUNSUPPORTED;
     if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
     if (c.useMatrixDissipation) return FLITE_EUNSUPPORTED;
     if (c.prolongationMappingScheme != 1) return FLITE_EUNSUPPORTED;

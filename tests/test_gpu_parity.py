@@ -108,6 +108,15 @@ def test_calls_and_cycles_bitwise(mesh, case):
     assert np.array_equal(g.get_pressure(1), o.get_pressure(1))
 
 
+def test_least_squares_gradients_single_grid(mesh):
+    c, g, o = make_pair(mesh, fluxType=4, HLLCFluxOrder=2, Automaticlipping=1, GradientMethod=2,
+                        numberOfGridsToUse=1)
+    for cyc in range(1, 4):
+        for s in (g, o):
+            s.cycle(cyc)
+        assert_same_state(g, o, f"LS gradients cycle {cyc}")
+
+
 @pytest.mark.parametrize("scheme", SCHEMES)
 def test_multigrid_schemes_bitwise(mesh, scheme):
     c, g, o = make_pair(mesh, fluxType=1, multigridScheme=scheme)
