@@ -139,6 +139,7 @@ def run_ours(args):
     if ws > 1:
         dist.init_process_group("nccl", init_method="env://",
                                 timeout=__import__("datetime").timedelta(seconds=600))
+    from flite3d_b200 import replicas
     F, mesh, c, u0, t_mesh = build_case()
     solver = F.Solver(c, mesh)
     solver.set_state(u0)
@@ -154,14 +155,13 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms = solver.time_cycles(args.steps, cycle_no=args.warmup + 1)
     torch.cuda.synchronize()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = ws * args.steps / (ms_max / 1e3)
+    value, ms_max = replicas.replica_rate(ms, args.steps)
 
     # kernel-level timing of the dominant edge kernels on level 1
     edge_ms, gather_ms = solver.profile_level(1, reps=20)
+    # adjoint cost ratio: one adjoint product against one forward residual
+    # evaluation on level 1 (same level, FP64)
+    fwd_ms, vjp_ms = solver.profile_adjoint(1, reps=20)
     hbm, peak_kind = _peaks()
     eb = edge_kernel_bytes(mesh)
     achieved = eb / (edge_ms / 1e3) / 1e9
@@ -196,10 +196,25 @@ def run_ours(args):
         fc = solver.forces()
     torch.cuda.synchronize()
     resident_s = time.perf_counter() - t1
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = ws * args.steps / float(te.item())
+    e2e_value = ws * args.steps / replicas.max_over_ranks(e2e_s)
+
+    # the same workload with FLITE_MIXED (FP32 flux increments over an FP64
+    # anchor): cycles per second
+    mixed = None
+    if not args.no_mixed:
+        solver_m = F.Solver(F.default_controls(**CONTROLS, precision=1), mesh)
+        solver_m.set_state(u0)
+        solver_m.start()
+        for i in range(1, args.warmup + 1):
+            solver_m.cycle(i)
+        torch.cuda.synchronize()
+        ms_m = solver_m.time_cycles(args.steps, cycle_no=args.warmup + 1)
+        solver_m.close()
+        v_m, ms_m = replicas.replica_rate(ms_m, args.steps)
+        mixed = {"value": v_m, "unit": "cycles/s", "ms_per_step": ms_m / args.steps}
+    ttc = None
+    if args.converge:
+        ttc = time_to_converge(F, mesh, c, u0, args.converge_max)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -235,10 +250,49 @@ def run_ours(args):
                                        "achieved": gather_kernel_bytes(mesh) / (gather_ms / 1e3) / 1e9}},
         "clocks": clk.summary(),
         "residual_after_warmup": float(res[0]),
+        "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,
+                    "what": "flite_residual_vjp vs flite_residual_fwd kernels on level 1, FP64"},
     }
+    if mixed is not None:
+        line["mixed"] = mixed
+    if ttc is not None:
+        line["time_to_1e-8"] = ttc
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
+
+
+def time_to_converge(F, mesh, c, u0, max_cycles):
+    """Wall time from the first cycle until res1 <= 1e-8 res1(cycle 1), for
+    FP64 and FLITE_MIXED on the same workload, with lift and drag there."""
+    import torch
+    out = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        cc = F.default_controls(**CONTROLS, precision=prec)
+        s = F.Solver(cc, mesh)
+        s.set_state(u0)
+        s.start()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r0 = None
+        cyc = 0
+        for cyc in range(1, max_cycles + 1):
+            s.cycle(cyc)
+            r = s.residuals()[0][0]
+            r0 = r0 or r
+            if r <= 1e-8 * r0:
+                break
+        secs = time.perf_counter() - t0
+        f = s.forces()
+        out[name] = {"seconds": secs, "cycles": cyc, "reached": bool(r <= 1e-8 * r0),
+                     "log10_reduction": float(math.log10(r / r0)), "CL": float(f[0]), "CD": float(f[1])}
+        s.close()
+    a, b = out["fp64"], out["mixed"]
+    if a["reached"] and b["reached"]:
+        out["speedup_mixed"] = a["seconds"] / b["seconds"]
+        out["CL_rel_diff"] = abs(b["CL"] - a["CL"]) / max(abs(a["CL"]), 1e-300)
+        out["CD_rel_diff"] = abs(b["CD"] - a["CD"]) / max(abs(a["CD"]), 1e-300)
+    return out
 
 
 def cpu_baseline(mesh, c, u0, cycles=2):
@@ -249,6 +303,8 @@ def cpu_baseline(mesh, c, u0, cycles=2):
     from flite3d_b200.solver import Backend, Solver
     b.build_oracle()
     lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
+    threads = host_threads()
+    lib.oracle_set_threads(threads)
     o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
     o.set_state(u0)
     o.start()
@@ -258,9 +314,17 @@ def cpu_baseline(mesh, c, u0, cycles=2):
         o.cycle(2 + i)
     dt = time.perf_counter() - t0
     o.close()
-    return {"value": cycles / dt, "unit": "cycles/s", "cores": 1, "kind": "port",
+    return {"value": cycles / dt, "unit": "cycles/s", "cores": threads, "kind": "port",
             "sample": f"{cycles} cycles of the same 2.1M-node workload after one warm-up cycle, "
-                      "single thread, FP64 C++ restatement in reference edge order"}
+                      f"FP64 C++ restatement on {threads} threads (edge loops over coloured "
+                      "blocks of edges)"}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def run_reference(args):
@@ -272,6 +336,8 @@ def run_reference(args):
     from flite3d_b200.solver import Backend, Solver
     b.build_oracle()
     lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
+    threads = host_threads()
+    lib.oracle_set_threads(threads)
     o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
     o.set_state(u0)
     o.start()
@@ -288,10 +354,10 @@ def run_reference(args):
         "steps": steps, "warmup": 1, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD},
-        "cpu_baseline": {"value": v, "unit": "cycles/s", "cores": 1, "kind": "port",
-                         "sample": f"{steps} cycles after 1 warm-up cycle; the Fortran reference "
-                                   "cannot be compiled here (no Fortran compiler), so the CPU "
-                                   "restatement of it runs"},
+        "cpu_baseline": {"value": v, "unit": "cycles/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} cycles after 1 warm-up cycle on {threads} threads; the "
+                                   "Fortran reference cannot be compiled here (no Fortran "
+                                   "compiler), so the CPU restatement of it runs"},
         "e2e": {"value": v, "unit": "cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -302,9 +368,13 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-cycles", type=int, default=2)
+    ap.add_argument("--cpu-cycles", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mesh", default=None, help="NX,NY,NZ hexes (default 264,88,88)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FLITE_MIXED cycle rate")
+    ap.add_argument("--converge", action="store_true",
+                    help="also measure time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
+    ap.add_argument("--converge-max", type=int, default=3000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -84,7 +84,9 @@ GPU_SYMBOLS = [
     "flite_init_freestream", "flite_start", "flite_do_time_iterations", "flite_restrict",
     "flite_prolong", "flite_map_fine_to_coarse", "flite_cycle", "flite_residuals",
     "flite_forces", "flite_residual_fwd", "flite_time_cycles", "flite_cycle_launches",
-    "flite_profile_level",
+    "flite_profile_level", "flite_batch_create", "flite_batch_destroy", "flite_batch_context",
+    "flite_batch_cycle", "flite_batch_run", "flite_batch_time_cycles", "flite_batch_autotune", "flite_batch_set_blocks",
+    "flite_residual_vjp", "flite_profile_adjoint",
 ]
 
 PREPRO_SYMBOLS = [

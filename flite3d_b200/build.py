@@ -95,7 +95,7 @@ def build_oracle(force=False, verbose=False):
     os.makedirs(outdir, exist_ok=True)
     out = os.path.join(outdir, "liboracle.so")
     if force or _stale(out, deps):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
               "-fno-fast-math", f"-I{INC}", f"-I{odir}", *src, "-o", out], verbose)
     return out
 

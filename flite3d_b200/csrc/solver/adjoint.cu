@@ -1,0 +1,301 @@
+// Discrete adjoint of the edge residual: the transpose Jacobian-vector
+// product ubar = (dR/du)^T rbar of makeRHS (def_par:1525-2512) for the
+// central interior flux and the wall/symmetry/far-field boundary fluxes.
+//
+// The central flux of an edge and the wall flux of a boundary edge are sums of
+// one-sided fluxes G(u; w) = F(u).w, linear in the coefficients w:
+//   interior  f = G(u1; w) + G(u2; w), rhs(i1) += f, rhs(i2) -= f
+//   wall      g1 = 3G(u1; w) + G(u2; w), g2 = G(u1; w) + 3G(u2; w)
+// so for node i,  ubar_i = sum_d A_d(u_i)^T b_d  with  b_d = sum over its
+// edges of w_d times the adjoint weights (rbar(i1)-rbar(i2) for interior
+// edges, 3 rbar_own + rbar_other for wall edges); A_d = dF_d/du with the
+// pressure p(u) (zero derivative where the 0.1 floor holds).  One node
+// gather builds b_d and one 3x(5x5) transpose product per node finishes it:
+// no edge buffer, and nothing stored beyond the state.
+// The far-field Roe flux against the freestream (def_par:2258-2446) is
+// nonlinear in the normal; its 5x5 Jacobians are formed with forward-mode
+// dual numbers per far-field edge.
+#include <cuda_runtime.h>
+
+#include "context.h"
+#include "flux.cuh"
+
+namespace flite {
+
+struct Dual {
+    double v, d;
+    __device__ Dual() : v(0), d(0) {}
+    __device__ Dual(double a) : v(a), d(0) {}
+    __device__ Dual(double a, double b) : v(a), d(b) {}
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+__device__ __forceinline__ Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    double q = a.v / b.v;
+    return Dual(q, (a.d - q * b.d) / b.v);
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+    double s = sqrt(a.v);
+    return Dual(s, s > 0 ? 0.5 * a.d / s : 0.0);
+}
+__device__ __forceinline__ Dual dfabs(Dual a) { return a.v < 0 ? -a : a; }
+__device__ __forceinline__ Dual dmaxc(Dual a, double c) { return (a.v < c) ? Dual(c) : a; }
+
+// far-field Roe flux of def_par:2268-2346 on the left (node) state
+__device__ void farfield_dual(const Params &P, const Dual *q, Dual pr, double rnx, double rny, double rnz,
+                              const double *inf, Dual *F) {
+    const double gam1 = P.gm1;
+    double ro = inf[0], ro1 = 1. / ro, uo = inf[1], vo = inf[2], wo = inf[3], eo = inf[4], po = inf[5];
+    Dual rhol = q[0], rinvl = Dual(1.0) / rhol;
+    Dual rhl = q[4] + pr;
+    Dual ul = q[1] * rinvl, vl = q[2] * rinvl, wl = q[3] * rinvl;
+    Dual epsl = q[4], hl = rhl * rinvl;
+    Dual nvl = (ul * rnx + vl * rny) + wl * rnz;
+    Dual fl1 = rhol * nvl, fl2 = pr * rnx + rhol * ul * nvl, fl3 = pr * rny + rhol * vl * nvl;
+    Dual fl4 = pr * rnz + rhol * wl * nvl, fl5 = rhl * nvl;
+    double rhor = ro, uxr = uo, vyr = vo, wzr = wo, epsr = eo * ro, presr = po, hr = eo + po * ro1;
+    double unr = (uxr * rnx + vyr * rny) + wzr * rnz;
+    double fr1 = rhor * unr, fr2 = rnx * presr + rhor * uxr * unr, fr3 = rny * presr + rhor * vyr * unr;
+    double fr4 = rnz * presr + rhor * wzr * unr, fr5 = (epsr + presr) * unr;
+    Dual di = dsqrt(Dual(rhor) / rhol), d1 = Dual(1.0) / (di + Dual(1.0));
+    Dual ui = (di * uxr + ul) * d1, vi = (di * vyr + vl) * d1, wi = (di * wzr + wl) * d1;
+    Dual hi = (di * hr + hl) * d1;
+    Dual ci2 = Dual(gam1) * (hi - Dual(0.5) * ((ui * ui + vi * vi) + wi * wi));
+    ci2 = dmaxc(ci2, 1.0e-5);
+    Dual ci = dsqrt(ci2);
+    Dual af = Dual(0.5) * ((ui * ui + vi * vi) + wi * wi);
+    Dual ucp = (ui * rnx + vi * rny) + wi * rnz;
+    Dual du1 = Dual(rhor) - rhol, du2 = Dual(rhor * uxr) - rhol * ul, du3 = Dual(rhor * vyr) - rhol * vl;
+    Dual du4 = Dual(rhor * wzr) - rhol * wl, du5 = Dual(epsr) - epsl;
+    Dual l1 = dfabs(ucp + ci), l2 = dfabs(ucp - ci), l3 = dfabs(ucp);
+    Dual s1 = Dual(0.5) * (l1 + l2), s2 = Dual(0.5) * (l1 - l2);
+    Dual al1x = Dual(gam1) * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+    Dual al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+    Dual cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+    Dual cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+    F[0] = Dual(0.5) * (Dual(fr1) + fl1) - Dual(0.5) * (l3 * du1 + cc1);
+    F[1] = Dual(0.5) * (Dual(fr2) + fl2) - Dual(0.5) * ((l3 * du2 + cc1 * ui) + cc2 * rnx);
+    F[2] = Dual(0.5) * (Dual(fr3) + fl3) - Dual(0.5) * ((l3 * du3 + cc1 * vi) + cc2 * rny);
+    F[3] = Dual(0.5) * (Dual(fr4) + fl4) - Dual(0.5) * ((l3 * du4 + cc1 * wi) + cc2 * rnz);
+    F[4] = Dual(0.5) * (Dual(fr5) + fl5) - Dual(0.5) * ((l3 * du5 + cc1 * hi) + cc2 * ucp);
+}
+
+// pressure and its gradient wrt the conserved state (0 under the floor)
+__device__ __forceinline__ void pressure_grad(const Params &P, const double *u, double *p, double *dp) {
+    double r = u[0], m1 = u[1], m2 = u[2], m3 = u[3], E = u[4];
+    double q = (m1 * m1 + m2 * m2) + m3 * m3;
+    double pp = P.gm1 * (E - 0.5 * q / r);
+    if (pp < 0.1) {
+        *p = 0.1;
+        for (int k = 0; k < 5; ++k) dp[k] = 0.0;
+        return;
+    }
+    *p = pp;
+    dp[0] = P.gm1 * 0.5 * q / (r * r);
+    dp[1] = -P.gm1 * m1 / r;
+    dp[2] = -P.gm1 * m2 / r;
+    dp[3] = -P.gm1 * m3 / r;
+    dp[4] = P.gm1;
+}
+
+// far-field contributions per boundary edge: J(u_b1)^T |w|(3 rbar1 + rbar2)
+// and J(u_b2)^T |w|(rbar1 + 3 rbar2) (FV weighting: 4 rbar_own)
+__global__ void k_vjp_farfield(Params P, LevelView L, const double *rbar, double *bvjp) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= L.B) return;
+    double *o = bvjp + (size_t)b * 10;
+    for (int k = 0; k < 10; ++k) o[k] = 0.0;
+    const int ind = L.bind[b];
+    if (ind != 3 && ind != 4) return;
+    const double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
+    const double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
+    if (!(rnorm > 1.0e-10)) return;
+    const double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
+    const double *inf = &P.inf[(ind - 3) * 6];
+    const int2 nd = L.bedge[b];
+    const int N = L.N;
+    const bool fe = P.boundaryTerm == 1;
+    for (int side = 0; side < 2; ++side) {
+        const int n = side == 0 ? nd.x : nd.y;
+        double a[5];
+        for (int k = 0; k < 5; ++k) {
+            double r1 = rbar[(size_t)k * N + nd.x], r2 = rbar[(size_t)k * N + nd.y];
+            a[k] = fe ? rnorm * (side == 0 ? 3. * r1 + r2 : r1 + 3. * r2) : rnorm * 4. * (side == 0 ? r1 : r2);
+        }
+        double u[5], p, dp[5];
+        for (int k = 0; k < 5; ++k) u[k] = L.u[(size_t)k * N + n];
+        pressure_grad(P, u, &p, dp);
+        for (int j = 0; j < 5; ++j) {  // column j of the Jacobian
+            Dual q[5];
+            for (int k = 0; k < 5; ++k) q[k] = Dual(u[k], k == j ? 1.0 : 0.0);
+            Dual F[5];
+            farfield_dual(P, q, Dual(p, dp[j]), rnx, rny, rnz, inf, F);
+            double s = 0.0;
+            for (int k = 0; k < 5; ++k) s += F[k].d * a[k];
+            o[side * 5 + j] = s;
+        }
+    }
+}
+
+// A_d(u)^T b accumulated into ubar for the three directions d
+__device__ __forceinline__ void apply_flux_jacobian_t(const Params &P, const double *u, const double b[3][5],
+                                                      double *ub) {
+    double p, dp[5];
+    pressure_grad(P, u, &p, dp);
+    const double r = u[0], E = u[4];
+    const double m[3] = {u[1], u[2], u[3]};
+    for (int k = 0; k < 5; ++k) ub[k] = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const double *a = b[d];
+        const double md = m[d];
+        // F_0 = m_d; F_{1+c} = m_c m_d / r + p [c==d]; F_4 = (E+p) m_d / r
+        double pbar = a[1 + d] + a[4] * md / r;
+        double rbar = 0.0, mbar[3] = {0, 0, 0}, Ebar = a[4] * md / r;
+        double s = a[0] + a[4] * (E + p) / r;  // d/dm_d of the parts linear in m_d
+        for (int c = 0; c < 3; ++c) {
+            rbar -= a[1 + c] * m[c] * md / (r * r);
+            mbar[c] += a[1 + c] * md / r;
+            s += a[1 + c] * m[c] / r;
+        }
+        rbar -= a[4] * (E + p) * md / (r * r);
+        mbar[d] += s;
+        ub[0] += rbar + pbar * dp[0];
+        ub[1] += mbar[0] + pbar * dp[1];
+        ub[2] += mbar[1] + pbar * dp[2];
+        ub[3] += mbar[2] + pbar * dp[3];
+        ub[4] += Ebar + pbar * dp[4];
+    }
+}
+
+__global__ void k_vjp_node(Params P, LevelView L, const double *rbar, const double *bvjp, double *ubar) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.N) return;
+    const int N = L.N;
+    double b[3][5];
+    for (int d = 0; d < 3; ++d)
+        for (int k = 0; k < 5; ++k) b[d][k] = 0.0;
+    double ri[5];
+    for (int k = 0; k < 5; ++k) ri[k] = rbar[(size_t)k * N + i];
+    for (int q = L.inc_ptr[i]; q < L.inc_ptr[i + 1]; ++q) {
+        int2 t = L.inc[q];
+        int e = t.x >= 0 ? t.x : ~t.x, j = t.y;
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        double a[5];
+        for (int k = 0; k < 5; ++k) {
+            double rj = rbar[(size_t)k * N + j];
+            a[k] = t.x >= 0 ? ri[k] - rj : rj - ri[k];  // rbar(i1) - rbar(i2)
+        }
+        for (int d = 0; d < 3; ++d)
+            for (int k = 0; k < 5; ++k) b[d][k] += w[d] * a[k];
+    }
+    double extra[5] = {0, 0, 0, 0, 0};
+    const bool fe = P.boundaryTerm == 1;
+    for (int q = L.binc_ptr[i]; q < L.binc_ptr[i + 1]; ++q) {
+        int bb = L.binc[q] >> 1, side = L.binc[q] & 1;
+        int ind = L.bind[bb];
+        if (ind == 3 || ind == 4) {
+            for (int k = 0; k < 5; ++k) extra[k] += bvjp[(size_t)bb * 10 + side * 5 + k];
+            continue;
+        }
+        if (!(ind <= 2 || ind == 9)) continue;
+        const double w[3] = {L.bwx[bb], L.bwy[bb], L.bwz[bb]};
+        if (!(sqrt((w[0] * w[0] + w[1] * w[1]) + w[2] * w[2]) > 1.0e-10)) continue;
+        const int2 nd = L.bedge[bb];
+        double a[5];
+        for (int k = 0; k < 5; ++k) {
+            double r1 = rbar[(size_t)k * N + nd.x], r2 = rbar[(size_t)k * N + nd.y];
+            a[k] = fe ? (side == 0 ? 3. * r1 + r2 : r1 + 3. * r2) : 4. * (side == 0 ? r1 : r2);
+        }
+        for (int d = 0; d < 3; ++d)
+            for (int k = 0; k < 5; ++k) b[d][k] += w[d] * a[k];
+    }
+    double u[5], ub[5];
+    for (int k = 0; k < 5; ++k) u[k] = L.u[(size_t)k * N + i];
+    apply_flux_jacobian_t(P, u, b, ub);
+    for (int k = 0; k < 5; ++k) ubar[(size_t)k * N + i] = ub[k] + extra[k];
+}
+
+}  // namespace flite
+
+extern "C" int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, const double *rbar, double *ubar) {
+    if (!ctx || level < 1 || level > (int)ctx->lv.size() || !u || !rbar || !ubar) return FLITE_EINVAL;
+    if (ctx->c.fluxType != 1 || ctx->c.precision != FLITE_FP64) return FLITE_EUNSUPPORTED;
+    try {
+        flite_ctx &X = *ctx;
+        LevelView &L = X.V(level - 1);
+        const size_t n5 = 5 * (size_t)L.N;
+        // the adjoint input and output reuse the level's residual and
+        // dissipation-sized state buffers are not touched: dedicated buffers
+        if (!X.adj_rbar || X.adj_n < n5) {
+            if (X.adj_rbar) { cudaFree(X.adj_rbar); cudaFree(X.adj_ubar); cudaFree(X.adj_b); }
+            CK(cudaMalloc(&X.adj_rbar, n5 * sizeof(double)));
+            CK(cudaMalloc(&X.adj_ubar, n5 * sizeof(double)));
+            size_t maxB = 1;
+            for (auto &D : X.lv) maxB = std::max(maxB, (size_t)D.B);
+            CK(cudaMalloc(&X.adj_b, 10 * maxB * sizeof(double)));
+            X.adj_n = n5;
+        }
+        CK(cudaMemcpyAsync(L.u, u, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        CK(cudaMemcpyAsync(X.adj_rbar, rbar, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        X.vjp_kernels(level - 1);
+        CK(cudaMemcpyAsync(ubar, X.adj_ubar, n5 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+        return FLITE_OK;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return FLITE_ECUDA;
+    }
+}
+
+void flite_ctx::vjp_kernels(int l) {
+    LevelView &L = V(l);
+    if (L.B > 0) k_vjp_farfield<<<eblk(L.B), eb, 0, s>>>(P, L, adj_rbar, adj_b);
+    k_vjp_node<<<nblk(L.N), nb, 0, s>>>(P, L, adj_rbar, adj_b, adj_ubar);
+}
+
+extern "C" int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double *fwd_ms, double *vjp_ms) {
+    if (!ctx || level < 1 || level > (int)ctx->lv.size() || reps < 1 || !fwd_ms || !vjp_ms) return FLITE_EINVAL;
+    if (ctx->c.fluxType != 1 || ctx->c.precision != FLITE_FP64) return FLITE_EUNSUPPORTED;
+    try {
+        flite_ctx &X = *ctx;
+        const int l = level - 1;
+        LevelView &L = X.V(l);
+        const size_t n5 = 5 * (size_t)L.N;
+        if (!X.adj_rbar || X.adj_n < n5) {
+            std::vector<double> zero(n5, 1.0);
+            std::vector<double> u(n5);
+            CK(cudaMemcpy(u.data(), L.u, n5 * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<double> out(n5);
+            int rc = flite_residual_vjp(ctx, level, u.data(), zero.data(), out.data());
+            if (rc != FLITE_OK) return rc;
+        }
+        cudaEvent_t e[4];
+        for (auto &x : e) CK(cudaEventCreate(&x));
+        double tf = 0, tv = 0;
+        for (int r = 0; r < reps; ++r) {
+            // forward residual: pressure, edge fluxes, boundary fluxes, gather
+            CK(cudaEventRecord(e[0], X.s));
+            X.pressure(l);
+            X.rhs_terms(l);
+            k_node_update<GATHER_FP64><<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            CK(cudaEventRecord(e[1], X.s));
+            CK(cudaEventRecord(e[2], X.s));
+            X.vjp_kernels(l);
+            CK(cudaEventRecord(e[3], X.s));
+            CK(cudaEventSynchronize(e[3]));
+            float a = 0, b = 0;
+            CK(cudaEventElapsedTime(&a, e[0], e[1]));
+            CK(cudaEventElapsedTime(&b, e[2], e[3]));
+            tf += a; tv += b;
+        }
+        for (auto &x : e) cudaEventDestroy(x);
+        *fwd_ms = tf / reps;
+        *vjp_ms = tv / reps;
+        return FLITE_OK;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return FLITE_ECUDA;
+    }
+}

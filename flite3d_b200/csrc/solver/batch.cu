@@ -1,0 +1,300 @@
+// Batched solves: many flow conditions on several meshes advanced together.
+//
+// A batch holds one context per case (mesh x flow condition).  Cases on the
+// same mesh share that mesh's device copy (edges, coefficients, incidence
+// lists, transfer operators, geometry); each case has its own solution state
+// and controls.  One batch cycle is ONE launch of a CUDA graph whose
+// independent branches are the cases' own cycle graphs, so small meshes and
+// coarse levels of different cases run concurrently instead of one launch
+// after another.  All cases read the cycle number from one device word.
+//
+// The autotuner times batch cycles for a set of edge-kernel and node-kernel
+// block sizes and keeps the fastest pair (the caller stores the choice).
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "context.h"
+
+struct flite_batch {
+    std::vector<flite_ctx *> cases;
+    std::vector<int> donor;  // index of the case owning the mesh copy
+    std::vector<char> active;  // cases the batch graph advances
+    double *h_res = nullptr;   // pinned: res1 of every case
+    cudaStream_t s = nullptr;
+    int *d_cycle = nullptr;
+    int *h_cycle = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int64_t launches = 0;
+    std::string err;
+
+    ~flite_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        // cases that borrow a mesh go first, mesh owners last
+        for (size_t i = cases.size(); i-- > 0;)
+            if (donor[i] != (int)i && cases[i]) { flite_destroy(cases[i]); cases[i] = nullptr; }
+        for (size_t i = cases.size(); i-- > 0;)
+            if (cases[i]) { flite_destroy(cases[i]); cases[i] = nullptr; }
+        if (d_cycle) cudaFree(d_cycle);
+        if (h_cycle) cudaFreeHost(h_cycle);
+        if (h_res) cudaFreeHost(h_res);
+        if (s) cudaStreamDestroy(s);
+    }
+
+    void build_graph() {
+        if (graph) return;
+        cudaGraph_t parent = nullptr;
+        CK(cudaGraphCreate(&parent, 0));
+        launches = 0;
+        try {
+            for (size_t i = 0; i < cases.size(); ++i) {
+                if (!active[i]) continue;
+                flite_ctx *c = cases[i];
+                cudaGraph_t g = nullptr;
+                c->capture_cycle(&g);
+                launches += c->launches;
+                cudaGraphNode_t node;
+                cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, g);
+                cudaGraphDestroy(g);
+                CK(e);
+            }
+            CK(cudaGraphInstantiate(&graph, parent, 0));
+        } catch (...) {
+            cudaGraphDestroy(parent);
+            throw;
+        }
+        cudaGraphDestroy(parent);
+    }
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        for (flite_ctx *c : cases) c->drop_graph();
+    }
+    void set_cycle(int cyc) {
+        *h_cycle = cyc;
+        CK(cudaMemcpyAsync(d_cycle, h_cycle, sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+    // res1 of every active case (writeResiduals' density norm), one
+    // synchronisation for all of them
+    void residuals() {
+        for (size_t i = 0; i < cases.size(); ++i) {
+            if (!active[i]) continue;
+            flite_ctx *c = cases[i];
+            const LevelView &L = c->c.multigridScheme > 0 ? c->V(0) : c->V((int)c->lv.size() - 1);
+            k_resid_partial<<<kResidBlocks, 256, 0, s>>>(L, c->d_part, kResidBlocks);
+            k_resid_final<<<1, 1, 0, s>>>(c->d_part, kResidBlocks, c->d_out);
+            CK(cudaMemcpyAsync(h_res + i, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaStreamSynchronize(s));
+    }
+    // the cases' own graphs launched one after another on the batch stream
+    void launch_sequential() {
+        for (flite_ctx *c : cases) {
+            c->ensure_graph();
+            CK(cudaGraphLaunch(c->graph, s));
+        }
+    }
+};
+
+namespace {
+template <class F>
+int bguard(flite_batch *b, F &&f) {
+    if (!b) return FLITE_EINVAL;
+    try {
+        return f();
+    } catch (const std::exception &e) {
+        b->err = e.what();
+        return FLITE_ECUDA;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int flite_batch_create(int ncases, const flite_controls *controls, const int32_t *mesh_of_case, int nmeshes,
+                       const int32_t *nlevels, const flite_level_desc *const *levels, flite_batch **out) {
+    if (ncases < 1 || !controls || !mesh_of_case || nmeshes < 1 || !nlevels || !levels || !out)
+        return FLITE_EINVAL;
+    *out = nullptr;
+    auto B = std::make_unique<flite_batch>();
+    B->cases.assign(ncases, nullptr);
+    B->donor.assign(ncases, -1);
+    B->active.assign(ncases, 1);
+    std::vector<int> owner(nmeshes, -1);
+    for (int i = 0; i < ncases; ++i) {
+        const int m = mesh_of_case[i];
+        if (m < 0 || m >= nmeshes || !levels[m] || nlevels[m] < 1) return FLITE_EINVAL;
+        const flite_ctx *donor = owner[m] >= 0 ? B->cases[owner[m]] : nullptr;
+        int rc = flite::create_context(&controls[i], nlevels[m], levels[m], donor, &B->cases[i]);
+        if (rc != FLITE_OK) return rc;
+        if (owner[m] < 0) owner[m] = i;
+        B->donor[i] = owner[m];
+    }
+    int rc = bguard(B.get(), [&] {
+        CK(cudaStreamCreateWithFlags(&B->s, cudaStreamNonBlocking));
+        CK(cudaMalloc(&B->d_cycle, sizeof(int)));
+        CK(cudaMallocHost(&B->h_cycle, sizeof(int)));
+        CK(cudaMallocHost(&B->h_res, (size_t)ncases * sizeof(double)));
+        // every case reads the batch's cycle number
+        for (flite_ctx *c : B->cases) c->d_cycle = B->d_cycle;
+        return FLITE_OK;
+    });
+    if (rc != FLITE_OK) return rc;
+    *out = B.release();
+    return FLITE_OK;
+}
+
+int flite_batch_destroy(flite_batch *b) {
+    if (!b) return FLITE_EINVAL;
+    if (b->s) cudaStreamSynchronize(b->s);
+    delete b;
+    return FLITE_OK;
+}
+
+int flite_batch_context(flite_batch *b, int case_index, flite_ctx **ctx) {
+    if (!b || !ctx || case_index < 0 || case_index >= (int)b->cases.size()) return FLITE_EINVAL;
+    *ctx = b->cases[case_index];
+    return FLITE_OK;
+}
+
+int flite_batch_cycle(flite_batch *b, int cycle_no) {
+    return bguard(b, [&] {
+        b->build_graph();
+        b->set_cycle(cycle_no);
+        CK(cudaGraphLaunch(b->graph, b->s));
+        CK(cudaStreamSynchronize(b->s));
+        return FLITE_OK;
+    });
+}
+
+int flite_batch_run(flite_batch *b, int first_cycle, int max_cycles, double orders, int check_every,
+                    int32_t *cycles, double *log10_reduction) {
+    if (!b || max_cycles < 1 || check_every < 1 || !cycles || !log10_reduction || !(orders > 0))
+        return FLITE_EINVAL;
+    return bguard(b, [&] {
+        const size_t n = b->cases.size();
+        std::vector<double> r0(n, 0.0), last(n, 0.0);
+        for (size_t i = 0; i < n; ++i) { cycles[i] = 0; log10_reduction[i] = 0.0; }
+        b->drop_graph();
+        std::fill(b->active.begin(), b->active.end(), 1);
+        const double target = std::pow(10.0, -orders);
+        size_t left = n;
+        for (int k = 0; k < max_cycles && left > 0; ++k) {
+            b->build_graph();
+            b->set_cycle(first_cycle + k);
+            CK(cudaGraphLaunch(b->graph, b->s));
+            for (size_t i = 0; i < n; ++i)
+                if (b->active[i]) cycles[i] = k + 1;
+            if (k > 0 && (k + 1) % check_every != 0 && k + 1 != max_cycles) continue;
+            b->residuals();
+            bool changed = false;
+            for (size_t i = 0; i < n; ++i) {
+                if (!b->active[i]) continue;
+                const double r = b->h_res[i];
+                if (!std::isfinite(r)) {
+                    b->err = "NaN in the residual of case " + std::to_string(i);
+                    return FLITE_ENAN;
+                }
+                if (k == 0) r0[i] = r;
+                last[i] = r;
+                if (r0[i] > 0 && r <= target * r0[i]) {
+                    b->active[i] = 0;
+                    --left;
+                    changed = true;
+                }
+            }
+            if (changed) {
+                // converged cases leave the batch graph
+                if (b->graph) cudaGraphExecDestroy(b->graph);
+                b->graph = nullptr;
+            }
+        }
+        for (size_t i = 0; i < n; ++i)
+            log10_reduction[i] = (r0[i] > 0 && last[i] > 0) ? std::log10(last[i] / r0[i]) : 0.0;
+        std::fill(b->active.begin(), b->active.end(), 1);
+        b->drop_graph();
+        return FLITE_OK;
+    });
+}
+
+int flite_batch_time_cycles(flite_batch *b, int cycle_no, int ncycles, int sequential, double *ms,
+                            int64_t *launches_per_cycle) {
+    if (ncycles < 1 || !ms) return FLITE_EINVAL;
+    return bguard(b, [&] {
+        if (sequential) {
+            for (flite_ctx *c : b->cases) c->ensure_graph();
+        } else {
+            b->build_graph();
+        }
+        b->set_cycle(cycle_no);
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, b->s));
+        for (int k = 0; k < ncycles; ++k) {
+            if (sequential) b->launch_sequential();
+            else CK(cudaGraphLaunch(b->graph, b->s));
+        }
+        CK(cudaEventRecord(e1, b->s));
+        CK(cudaEventSynchronize(e1));
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = t;
+        if (launches_per_cycle) {
+            int64_t n = 0;
+            for (flite_ctx *c : b->cases) n += c->launches;
+            *launches_per_cycle = n;
+        }
+        return FLITE_OK;
+    });
+}
+
+int flite_batch_autotune(flite_batch *b, int cycle_no, int reps, int32_t *edge_block, int32_t *node_block,
+                         double *best_ms) {
+    if (!edge_block || !node_block || reps < 1) return FLITE_EINVAL;
+    return bguard(b, [&] {
+        static const int cand[3] = {64, 128, 256};
+        double best = 1e300;
+        int be = 256, bn = 256;
+        for (int e : cand)
+            for (int n : cand) {
+                b->drop_graph();
+                for (flite_ctx *c : b->cases) { c->eb = e; c->nb = n; }
+                b->build_graph();
+                b->set_cycle(cycle_no);
+                CK(cudaGraphLaunch(b->graph, b->s));  // warm
+                cudaEvent_t e0, e1;
+                CK(cudaEventCreate(&e0));
+                CK(cudaEventCreate(&e1));
+                CK(cudaEventRecord(e0, b->s));
+                for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(b->graph, b->s));
+                CK(cudaEventRecord(e1, b->s));
+                CK(cudaEventSynchronize(e1));
+                float t = 0;
+                CK(cudaEventElapsedTime(&t, e0, e1));
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (t / reps < best) { best = t / reps; be = e; bn = n; }
+            }
+        b->drop_graph();
+        for (flite_ctx *c : b->cases) { c->eb = be; c->nb = bn; }
+        *edge_block = be;
+        *node_block = bn;
+        if (best_ms) *best_ms = best;
+        return FLITE_OK;
+    });
+}
+
+int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_block) {
+    if (!b || edge_block < 32 || edge_block > 256 || node_block < 32 || node_block > 256 ||
+        edge_block % 32 || node_block % 32)
+        return FLITE_EINVAL;
+    b->drop_graph();
+    for (flite_ctx *c : b->cases) { c->eb = edge_block; c->nb = node_block; }
+    return FLITE_OK;
+}
+
+}  // extern "C"

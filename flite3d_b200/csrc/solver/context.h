@@ -1,0 +1,399 @@
+// Device context of one solve: the per-level device layout and the host
+// orchestration that mirrors the reference's solver routines.  Shared by the
+// single-solve ABI (flite_gpu.cu) and the batched one (batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "flite_gpu.h"
+#include "kernels.h"
+
+using namespace flite;
+
+namespace flite_detail {
+
+struct cuda_error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            throw cuda_error(std::string(#call) + ": " + cudaGetErrorString(_e));             \
+    } while (0)
+
+constexpr int kBlock = 256;
+constexpr int kResidBlocks = 296;  // 2 x 148 SMs
+
+struct DevLevel {
+    int N = 0, E = 0, B = 0, Nb = 0;
+    LevelView v{};
+    std::vector<int> wall;  // level-1 wall nodes in register order (forces)
+    int *d_wall = nullptr;
+};
+
+}  // namespace flite_detail
+
+using namespace flite_detail;
+
+struct flite_ctx {
+    flite_controls c{};
+    Params P{};
+    std::vector<DevLevel> lv;
+    std::vector<void *> allocs;
+    cudaStream_t s = nullptr;
+    int *d_cycle = nullptr;
+    int *d_cyc = nullptr;  // per-level cycle numbers
+    double *d_part = nullptr, *d_out = nullptr;
+    int *h_cycle = nullptr;  // pinned
+    cudaGraphExec_t graph = nullptr;
+    int64_t launches = 0;
+    bool counting = false;
+    // threads per block of the edge kernels and of the node kernels (the
+    // batch autotuner may change them; kernels with launch bounds take <= 256)
+    int eb = kBlock, nb = kBlock;
+    // adjoint buffers (allocated on the first flite_residual_vjp)
+    double *adj_rbar = nullptr, *adj_ubar = nullptr, *adj_b = nullptr;
+    size_t adj_n = 0;
+    void vjp_kernels(int l);
+    std::string err;
+
+    template <class T>
+    T *alloc(size_t n) {
+        void *p = nullptr;
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        if (e != cudaSuccess) throw cuda_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(p);
+        return (T *)p;
+    }
+    template <class T>
+    T *upload(const std::vector<T> &h) {
+        T *d = alloc<T>(h.size());
+        if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return d;
+    }
+    ~flite_ctx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (adj_rbar) { cudaFree(adj_rbar); cudaFree(adj_ubar); cudaFree(adj_b); }
+        for (void *p : allocs) cudaFree(p);
+        if (h_cycle) cudaFreeHost(h_cycle);
+        if (s) cudaStreamDestroy(s);
+    }
+
+    static unsigned blocks(size_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+    unsigned nblk(size_t n) const { return (unsigned)((n + nb - 1) / nb); }
+    unsigned eblk(size_t n) const { return (unsigned)((n + eb - 1) / eb); }
+    void counted() {
+        if (counting) ++launches;
+    }
+
+    // ---- single-grid building blocks ------------------------------------
+    LevelView &V(int l) { return lv[l].v; }
+
+    void pressure(int l) {
+        counted();
+        k_pressure<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+    }
+    void timesteps(int l) {
+        counted();
+        k_timestep<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+    }
+    void zero_diss(int l) {
+        counted();
+        k_fill<<<nblk(5 * (size_t)V(l).N), nb, 0, s>>>(V(l).diss, 5 * (size_t)V(l).N, 0.0);
+    }
+    // makeArtificialDissipation2 (def_par:11484-11993), scalar form
+    void jst(int l) {
+        const LevelView &L = V(l);
+        if ((c.fluxType == 4 && L.grid == 1) ||
+            (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0)) {
+            zero_diss(l);
+            return;
+        }
+        counted();
+        k_jst_lap<<<nblk(L.N), nb, 0, s>>>(P, L);
+        counted();
+        k_jst_flux<<<nblk(L.N), nb, 0, s>>>(P, L);
+    }
+    void first_order_diss(int l) {
+        counted();
+        k_first_order_diss<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+    }
+    // dissipation choice of singleIteration (def_par:1030-1036)
+    void dissipation(int l) {
+        if (c.dissipationScheme == 3) first_order_diss(l);
+        else jst(l);
+    }
+    // makeViscosityTerm (def_par:5198-5893), subtracted from the dissipation
+    void viscous(int l) {
+        if (!(c.ReynoldsNumber > 0.0)) return;
+        counted();
+        k_visc_prim<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        counted();
+        k_visc_grad<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        counted();
+        k_visc_flux<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+    }
+    // makeRHS up to the node gather (def_par:1587-1607 and the edge loops);
+    // with FLITE_MIXED, `anchor` selects the FP64 evaluation that refreshes
+    // the anchor state, otherwise the FP32 increments over it
+    void rhs_terms(int l, bool anchor = true) {
+        const LevelView &L = V(l);
+        if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
+            counted();
+            if (c.GradientMethod == 1) k_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
+            else k_ls_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
+            if (c.Automaticlipping == 1) {
+                counted();
+                k_minmax<<<nblk(L.N), nb, 0, s>>>(P, L);
+            }
+        }
+        if (L.E > 0) {
+            counted();
+            edge_flux_launch(L, anchor);
+        }
+        if (L.B > 0) {
+            counted();
+            k_bnd_flux<<<eblk(L.B), eb, 0, s>>>(P, L);
+        }
+    }
+    bool mixed() const { return c.precision == FLITE_MIXED; }
+    // the flux kernel instance of this run's fluxType (and HLLC order; the
+    // reconstruction only acts on level 1, where coordinates exist)
+    void edge_flux_launch(const LevelView &L, bool anchor = true) {
+        const unsigned ng = eblk(L.E);
+        if (mixed() && !anchor) {
+            // FP32 flux increments over the anchor (central flux)
+            k_delta_state<<<nblk(L.N), nb, 0, s>>>(L);
+            counted();
+            k_edge_flux_f32_delta<<<ng, eb, 0, s>>>(L);
+            return;
+        }
+        switch (c.fluxType) {
+            case 1: k_edge_flux<1, false><<<ng, eb, 0, s>>>(P, L); break;
+            case 2: k_edge_flux<2, false><<<ng, eb, 0, s>>>(P, L); break;
+            case 3: k_edge_flux<3, false><<<ng, eb, 0, s>>>(P, L); break;
+            default:
+                if (c.HLLCFluxOrder > 1) k_edge_flux<4, true><<<ng, eb, 0, s>>>(P, L);
+                else k_edge_flux<4, false><<<ng, eb, 0, s>>>(P, L);
+        }
+    }
+    void node_update(int l, int mode, int stage, bool anchor = true) {
+        counted();
+        const unsigned g = nblk(V(l).N);
+        if (!mixed()) k_node_update<GATHER_FP64><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+        else if (anchor) k_node_update<GATHER_ANCHOR><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+        else k_node_update<GATHER_DELTA><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+    }
+
+    // ---- singleIteration (def_par:1002-1181) -----------------------------
+    void singleIteration(int l, bool calcDiss) {
+        if (calcDiss) {
+            pressure(l);  // p = |p| is the identity after the 0.1 floor
+            timesteps(l);
+            dissipation(l);
+            viscous(l);
+        }
+        for (int st = 1; st <= 3; ++st) {
+            // u == uprev at stage 1: the FP64 evaluation there is the anchor
+            // of the mixed-precision increments of stages 2 and 3
+            pressure(l);
+            rhs_terms(l, st == 1);
+            node_update(l, MODE_STAGE, st, st == 1);
+        }
+    }
+    // ---- doTimeIterations (def_par:966-1000) -----------------------------
+    void doTimeIterations(int l, int nsteps, bool calcDiss) {
+        counted();
+        k_set_int<<<1, 1, 0, s>>>(V(l).cyc, d_cycle);
+        for (int i = 0; i < nsteps; ++i) {
+            counted();
+            k_copy<<<nblk(5 * (size_t)V(l).N), nb, 0, s>>>(V(l).u, V(l).uprev, 5 * (size_t)V(l).N);
+            singleIteration(l, calcDiss);
+        }
+    }
+    // ---- restrictGrid (def_par:12141-12430) ------------------------------
+    void restrictGrid(int fl) {
+        const int cl = fl + 1;
+        counted();
+        k_restrict_state<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        timesteps(cl);
+        if (c.coarseGridDissipationScheme == 2) jst(cl);
+        else if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
+        viscous(cl);
+        rhs_terms(cl);
+        node_update(cl, MODE_RCOARSE, 0);
+        pressure(fl);
+        jst(fl);  // the fine part always uses scheme 2 (def_par:12266-12270)
+        viscous(fl);
+        rhs_terms(fl, false);
+        node_update(fl, MODE_RFINE, 0, false);
+        counted();
+        k_restrict_incr<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
+    }
+    // ---- prolongateGrid (def_par:12432-12570) ----------------------------
+    void prolongateGrid(int cl) {
+        const int fl = cl - 1;
+        counted();
+        k_prolong_coarse<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        counted();
+        k_prolong_fine<<<nblk(V(fl).N), nb, 0, s>>>(P, V(cl), V(fl));
+    }
+    void mapFineToCoarse(int fl) {
+        counted();
+        k_restrict_u<<<nblk(V(fl + 1).N), nb, 0, s>>>(V(fl + 1), V(fl));
+    }
+    // ---- oneCycle (mg_par:907-1196) --------------------------------------
+    void oneCycle() {
+        const int G = (int)lv.size();
+        const int nr = c.numberOfRelaxationSteps;
+        auto relax = [&](int j1, int steps, bool calc) { doTimeIterations(j1 - 1, steps, calc); };
+        const int sch = c.multigridScheme;
+        if (sch <= 0) {
+            for (int i = 1; i <= G - 1; ++i) {
+                counted();
+                k_copy<<<nblk(5 * (size_t)V(i - 1).N), nb, 0, s>>>(V(i - 1).u, V(i - 1).uprev,
+                                                                        5 * (size_t)V(i - 1).N);
+                mapFineToCoarse(i - 1);
+            }
+            counted();
+            k_fill<<<nblk(5 * (size_t)V(G - 1).N), nb, 0, s>>>(V(G - 1).src, 5 * (size_t)V(G - 1).N, 0.0);
+            relax(G, nr, true);
+            for (int i = G; i >= 2; --i) {
+                counted();
+                k_inject_u<<<nblk(V(i - 2).N), nb, 0, s>>>(V(i - 1), V(i - 2));
+            }
+        } else if (sch == 1) {
+            for (int i = 1; i <= G - 1; ++i) {
+                relax(i, nr, i == 1);
+                restrictGrid(i - 1);
+                mapFineToCoarse(i - 1);
+            }
+            relax(G, nr, G == 1);
+            for (int i = G; i >= 2; --i) {
+                prolongateGrid(i - 1);
+                relax(i - 1, nr, (i - 1) == 1);
+            }
+        } else if (sch == 2 || sch == 5) {
+            int nsw = G <= 2 ? 1 : 2 * G - 4;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, sch == 5 ? j : nr, j == fsl);
+                    restrictGrid(j - 1);
+                }
+                relax(G, sch == 5 ? G : nr, G == 1);
+                if (fsl == 1) fsl = G > 2 ? G - 1 : G;
+                else if (i <= nsw / 2) fsl = fsl - 1;
+                else fsl = fsl + 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prolongateGrid(j - 1);
+                    relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+            for (int j = G; j >= 2; --j) {
+                prolongateGrid(j - 1);
+                relax(j - 1, nr, (j - 1) == 1);
+            }
+        } else if (sch == 3 || sch == 7) {
+            int nsw = G == 1 ? 1 : G - 1;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, nr, j == fsl);
+                    restrictGrid(j - 1);
+                }
+                relax(G, nr, G == 1);
+                if (fsl == 1) fsl = G >= 2 ? G - 1 : G;
+                else fsl = fsl - 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prolongateGrid(j - 1);
+                    if (sch == 7) relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+        } else if (sch == 4) {
+            int nsw = G == 1 ? 1 : G - 1;
+            int fsl = 1;
+            for (int i = 1; i <= nsw; ++i) {
+                for (int j = fsl; j <= G - 1; ++j) {
+                    relax(j, nr, j == fsl);
+                    restrictGrid(j - 1);
+                }
+                relax(G, nr, G == 1);
+                fsl = fsl + 1;
+                for (int j = G; j >= fsl + 1; --j) {
+                    prolongateGrid(j - 1);
+                    relax(j - 1, nr, (j - 1) == 1);
+                }
+            }
+            for (int j = G; j >= 2; --j) {
+                prolongateGrid(j - 1);
+                relax(j - 1, nr, (j - 1) == 1);
+            }
+        }
+    }
+
+    void set_cycle(int cyc) {
+        *h_cycle = cyc;
+        CK(cudaMemcpyAsync(d_cycle, h_cycle, sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+
+    // capture one oneCycle into a graph (not instantiated)
+    void capture_cycle(cudaGraph_t *g) {
+        *g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        launches = 0;
+        counting = true;
+        try {
+            oneCycle();
+        } catch (...) {
+            counting = false;
+            cudaStreamEndCapture(s, g);
+            if (*g) cudaGraphDestroy(*g);
+            *g = nullptr;
+            throw;
+        }
+        counting = false;
+        CK(cudaStreamEndCapture(s, g));
+    }
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+
+    void ensure_graph() {
+        if (graph) return;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        launches = 0;
+        counting = true;
+        try {
+            oneCycle();
+        } catch (...) {
+            counting = false;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        counting = false;
+        CK(cudaStreamEndCapture(s, &g));
+        cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+};
+
+namespace flite {
+int create_context(const flite_controls *c, int nlevels, const flite_level_desc *levels, const flite_ctx *donor,
+                   flite_ctx **out);
+}  // namespace flite

@@ -54,15 +54,19 @@ struct LevelView {
     double *sens;                          // [N]  pressure sensor
     double *hvis;                          // [N]  viscous time-step term
     double *tau;                           // [9][N] stress tensor + heat flux
+    double *prim;                          // [4][N] u, v, w, T of the viscous term
+    double *vdt;                           // [N]  V/dt of the dissipation
     double *wstress;                       // [3][N] wall stress (level 1)
     double *grad;                          // [15][N] (level 1, HLLC order 2)
     double *bnd;                           // [10][N]
     double *flux;                          // [E][5] edge flux buffer
-    // mixed precision (FLITE_MIXED): FP32 shadows of the state and edge
-    // coefficients, and the FP32 edge buffer
-    float *u32, *p32;                      // [5][N], [N]
+    // mixed precision (FLITE_MIXED): interior central fluxes as FP32
+    // increments over an FP64 anchor state
+    double *ua, *ra, *pa;                  // anchor u [5][N], its interior-edge residual [5][N], p [N]
+    float *a32;                            // [5][N] anchor rho, u, v, w, E+p
+    float *d32;                            // [6][N] u - ua (5) and p - pa
     const float *wx32, *wy32, *wz32;       // [E]
-    float *flux32;                         // [E][5]
+    float *flux32;                         // [E][5] flux increments
     double *bflux;                         // [B][10] boundary-edge contributions
     int *cyc;                              // cycle number of this level
 };

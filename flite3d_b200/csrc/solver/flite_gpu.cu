@@ -18,342 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "flite_gpu.h"
-#include "kernels.h"
-
-using namespace flite;
-
-namespace {
-
-struct cuda_error : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-
-#define CK(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t _e = (call);                                                              \
-        if (_e != cudaSuccess)                                                                \
-            throw cuda_error(std::string(#call) + ": " + cudaGetErrorString(_e));             \
-    } while (0)
-
-constexpr int kBlock = 256;
-constexpr int kResidBlocks = 296;  // 2 x 148 SMs
-
-struct DevLevel {
-    int N = 0, E = 0, B = 0, Nb = 0;
-    LevelView v{};
-    std::vector<int> wall;  // level-1 wall nodes in register order (forces)
-    int *d_wall = nullptr;
-};
-
-}  // namespace
-
-struct flite_ctx {
-    flite_controls c{};
-    Params P{};
-    std::vector<DevLevel> lv;
-    std::vector<void *> allocs;
-    cudaStream_t s = nullptr;
-    int *d_cycle = nullptr;
-    int *d_cyc = nullptr;  // per-level cycle numbers
-    double *d_part = nullptr, *d_out = nullptr;
-    int *h_cycle = nullptr;  // pinned
-    cudaGraphExec_t graph = nullptr;
-    int64_t launches = 0;
-    bool counting = false;
-    std::string err;
-
-    template <class T>
-    T *alloc(size_t n) {
-        void *p = nullptr;
-        if (n == 0) n = 1;
-        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-        if (e != cudaSuccess) throw cuda_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        allocs.push_back(p);
-        return (T *)p;
-    }
-    template <class T>
-    T *upload(const std::vector<T> &h) {
-        T *d = alloc<T>(h.size());
-        if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-        return d;
-    }
-    ~flite_ctx() {
-        if (graph) cudaGraphExecDestroy(graph);
-        for (void *p : allocs) cudaFree(p);
-        if (h_cycle) cudaFreeHost(h_cycle);
-        if (s) cudaStreamDestroy(s);
-    }
-
-    static unsigned blocks(size_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
-    void counted() {
-        if (counting) ++launches;
-    }
-
-    // ---- single-grid building blocks ------------------------------------
-    LevelView &V(int l) { return lv[l].v; }
-
-    void pressure(int l) {
-        counted();
-        k_pressure<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
-    }
-    void timesteps(int l) {
-        counted();
-        k_timestep<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
-    }
-    void zero_diss(int l) {
-        counted();
-        k_fill<<<blocks(5 * (size_t)V(l).N), kBlock, 0, s>>>(V(l).diss, 5 * (size_t)V(l).N, 0.0);
-    }
-    // makeArtificialDissipation2 (def_par:11484-11993), scalar form
-    void jst(int l) {
-        const LevelView &L = V(l);
-        if ((c.fluxType == 4 && L.grid == 1) ||
-            (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0)) {
-            zero_diss(l);
-            return;
-        }
-        counted();
-        k_jst_lap<<<blocks(L.N), kBlock, 0, s>>>(P, L);
-        counted();
-        k_jst_flux<<<blocks(L.N), kBlock, 0, s>>>(P, L);
-    }
-    void first_order_diss(int l) {
-        counted();
-        k_first_order_diss<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
-    }
-    // dissipation choice of singleIteration (def_par:1030-1036)
-    void dissipation(int l) {
-        if (c.dissipationScheme == 3) first_order_diss(l);
-        else jst(l);
-    }
-    // makeViscosityTerm (def_par:5198-5893), subtracted from the dissipation
-    void viscous(int l) {
-        if (!(c.ReynoldsNumber > 0.0)) return;
-        counted();
-        k_visc_grad<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
-        counted();
-        k_visc_flux<<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l));
-    }
-    // makeRHS up to the node gather (def_par:1587-1607 and the edge loops)
-    void rhs_terms(int l) {
-        const LevelView &L = V(l);
-        if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
-            counted();
-            if (c.GradientMethod == 1) k_gradient<<<blocks(L.N), kBlock, 0, s>>>(P, L);
-            else k_ls_gradient<<<blocks(L.N), kBlock, 0, s>>>(P, L);
-            if (c.Automaticlipping == 1) {
-                counted();
-                k_minmax<<<blocks(L.N), kBlock, 0, s>>>(P, L);
-            }
-        }
-        if (L.E > 0) {
-            counted();
-            edge_flux_launch(L);
-        }
-        if (L.B > 0) {
-            counted();
-            k_bnd_flux<<<blocks(L.B), kBlock, 0, s>>>(P, L);
-        }
-    }
-    bool mixed() const { return c.precision == FLITE_MIXED; }
-    // the flux kernel instance of this run's fluxType (and HLLC order; the
-    // reconstruction only acts on level 1, where coordinates exist)
-    void edge_flux_launch(const LevelView &L) {
-        const unsigned nb = blocks(L.E);
-        if (mixed()) {
-            // FP32 fluxes from FP32 shadows of the state (central flux)
-            k_shadow<<<blocks(L.N), kBlock, 0, s>>>(L);
-            counted();
-            k_edge_flux_f32_central<<<nb, kBlock, 0, s>>>(L);
-            return;
-        }
-        switch (c.fluxType) {
-            case 1: k_edge_flux<1, false><<<nb, kBlock, 0, s>>>(P, L); break;
-            case 2: k_edge_flux<2, false><<<nb, kBlock, 0, s>>>(P, L); break;
-            case 3: k_edge_flux<3, false><<<nb, kBlock, 0, s>>>(P, L); break;
-            default:
-                if (c.HLLCFluxOrder > 1) k_edge_flux<4, true><<<nb, kBlock, 0, s>>>(P, L);
-                else k_edge_flux<4, false><<<nb, kBlock, 0, s>>>(P, L);
-        }
-    }
-    void node_update(int l, int mode, int stage) {
-        counted();
-        if (mixed()) k_node_update<true><<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l), mode, stage);
-        else k_node_update<false><<<blocks(V(l).N), kBlock, 0, s>>>(P, V(l), mode, stage);
-    }
-
-    // ---- singleIteration (def_par:1002-1181) -----------------------------
-    void singleIteration(int l, bool calcDiss) {
-        if (calcDiss) {
-            pressure(l);  // p = |p| is the identity after the 0.1 floor
-            timesteps(l);
-            dissipation(l);
-            viscous(l);
-        }
-        for (int st = 1; st <= 3; ++st) {
-            pressure(l);
-            rhs_terms(l);
-            node_update(l, MODE_STAGE, st);
-        }
-    }
-    // ---- doTimeIterations (def_par:966-1000) -----------------------------
-    void doTimeIterations(int l, int nsteps, bool calcDiss) {
-        counted();
-        k_set_int<<<1, 1, 0, s>>>(V(l).cyc, d_cycle);
-        for (int i = 0; i < nsteps; ++i) {
-            counted();
-            k_copy<<<blocks(5 * (size_t)V(l).N), kBlock, 0, s>>>(V(l).u, V(l).uprev, 5 * (size_t)V(l).N);
-            singleIteration(l, calcDiss);
-        }
-    }
-    // ---- restrictGrid (def_par:12141-12430) ------------------------------
-    void restrictGrid(int fl) {
-        const int cl = fl + 1;
-        counted();
-        k_restrict_state<<<blocks(V(cl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
-        timesteps(cl);
-        if (c.coarseGridDissipationScheme == 2) jst(cl);
-        else if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
-        viscous(cl);
-        rhs_terms(cl);
-        node_update(cl, MODE_RCOARSE, 0);
-        pressure(fl);
-        jst(fl);  // the fine part always uses scheme 2 (def_par:12266-12270)
-        viscous(fl);
-        rhs_terms(fl);
-        node_update(fl, MODE_RFINE, 0);
-        counted();
-        k_restrict_incr<<<blocks(V(cl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
-    }
-    // ---- prolongateGrid (def_par:12432-12570) ----------------------------
-    void prolongateGrid(int cl) {
-        const int fl = cl - 1;
-        counted();
-        k_prolong_coarse<<<blocks(V(cl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
-        counted();
-        k_prolong_fine<<<blocks(V(fl).N), kBlock, 0, s>>>(P, V(cl), V(fl));
-    }
-    void mapFineToCoarse(int fl) {
-        counted();
-        k_restrict_u<<<blocks(V(fl + 1).N), kBlock, 0, s>>>(V(fl + 1), V(fl));
-    }
-    // ---- oneCycle (mg_par:907-1196) --------------------------------------
-    void oneCycle() {
-        const int G = (int)lv.size();
-        const int nr = c.numberOfRelaxationSteps;
-        auto relax = [&](int j1, int steps, bool calc) { doTimeIterations(j1 - 1, steps, calc); };
-        const int sch = c.multigridScheme;
-        if (sch <= 0) {
-            for (int i = 1; i <= G - 1; ++i) {
-                counted();
-                k_copy<<<blocks(5 * (size_t)V(i - 1).N), kBlock, 0, s>>>(V(i - 1).u, V(i - 1).uprev,
-                                                                        5 * (size_t)V(i - 1).N);
-                mapFineToCoarse(i - 1);
-            }
-            counted();
-            k_fill<<<blocks(5 * (size_t)V(G - 1).N), kBlock, 0, s>>>(V(G - 1).src, 5 * (size_t)V(G - 1).N, 0.0);
-            relax(G, nr, true);
-            for (int i = G; i >= 2; --i) {
-                counted();
-                k_inject_u<<<blocks(V(i - 2).N), kBlock, 0, s>>>(V(i - 1), V(i - 2));
-            }
-        } else if (sch == 1) {
-            for (int i = 1; i <= G - 1; ++i) {
-                relax(i, nr, i == 1);
-                restrictGrid(i - 1);
-                mapFineToCoarse(i - 1);
-            }
-            relax(G, nr, G == 1);
-            for (int i = G; i >= 2; --i) {
-                prolongateGrid(i - 1);
-                relax(i - 1, nr, (i - 1) == 1);
-            }
-        } else if (sch == 2 || sch == 5) {
-            int nsw = G <= 2 ? 1 : 2 * G - 4;
-            int fsl = 1;
-            for (int i = 1; i <= nsw; ++i) {
-                for (int j = fsl; j <= G - 1; ++j) {
-                    relax(j, sch == 5 ? j : nr, j == fsl);
-                    restrictGrid(j - 1);
-                }
-                relax(G, sch == 5 ? G : nr, G == 1);
-                if (fsl == 1) fsl = G > 2 ? G - 1 : G;
-                else if (i <= nsw / 2) fsl = fsl - 1;
-                else fsl = fsl + 1;
-                for (int j = G; j >= fsl + 1; --j) {
-                    prolongateGrid(j - 1);
-                    relax(j - 1, nr, (j - 1) == 1);
-                }
-            }
-            for (int j = G; j >= 2; --j) {
-                prolongateGrid(j - 1);
-                relax(j - 1, nr, (j - 1) == 1);
-            }
-        } else if (sch == 3 || sch == 7) {
-            int nsw = G == 1 ? 1 : G - 1;
-            int fsl = 1;
-            for (int i = 1; i <= nsw; ++i) {
-                for (int j = fsl; j <= G - 1; ++j) {
-                    relax(j, nr, j == fsl);
-                    restrictGrid(j - 1);
-                }
-                relax(G, nr, G == 1);
-                if (fsl == 1) fsl = G >= 2 ? G - 1 : G;
-                else fsl = fsl - 1;
-                for (int j = G; j >= fsl + 1; --j) {
-                    prolongateGrid(j - 1);
-                    if (sch == 7) relax(j - 1, nr, (j - 1) == 1);
-                }
-            }
-        } else if (sch == 4) {
-            int nsw = G == 1 ? 1 : G - 1;
-            int fsl = 1;
-            for (int i = 1; i <= nsw; ++i) {
-                for (int j = fsl; j <= G - 1; ++j) {
-                    relax(j, nr, j == fsl);
-                    restrictGrid(j - 1);
-                }
-                relax(G, nr, G == 1);
-                fsl = fsl + 1;
-                for (int j = G; j >= fsl + 1; --j) {
-                    prolongateGrid(j - 1);
-                    relax(j - 1, nr, (j - 1) == 1);
-                }
-            }
-            for (int j = G; j >= 2; --j) {
-                prolongateGrid(j - 1);
-                relax(j - 1, nr, (j - 1) == 1);
-            }
-        }
-    }
-
-    void set_cycle(int cyc) {
-        *h_cycle = cyc;
-        CK(cudaMemcpyAsync(d_cycle, h_cycle, sizeof(int), cudaMemcpyHostToDevice, s));
-    }
-
-    void ensure_graph() {
-        if (graph) return;
-        cudaGraph_t g = nullptr;
-        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        launches = 0;
-        counting = true;
-        try {
-            oneCycle();
-        } catch (...) {
-            counting = false;
-            cudaStreamEndCapture(s, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-        }
-        counting = false;
-        CK(cudaStreamEndCapture(s, &g));
-        cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        CK(e);
-    }
-};
+#include "context.h"
 
 namespace {
 
@@ -410,7 +75,13 @@ int flite_last_error(const flite_ctx *ctx, char *buf, size_t len) {
     return FLITE_OK;
 }
 
-int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *levels, flite_ctx **out) {
+}  // extern "C"
+
+// Create one solve's context.  With a donor context on the same mesh, the
+// device copy of the mesh (edges, coefficients, incidence lists, transfer
+// operators, geometry) is shared and only the solution state is allocated.
+int flite::create_context(const flite_controls *c, int nlevels, const flite_level_desc *levels,
+                          const flite_ctx *donor, flite_ctx **out) {
     if (!c || !levels || !out || nlevels < 1) return FLITE_EINVAL;
     *out = nullptr;
     if (unsupported_reason(*c)) return FLITE_EUNSUPPORTED;
@@ -458,6 +129,13 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
             D.N = N; D.E = E; D.B = B; D.Nb = Nb;
             LevelView &L = D.v;
             L.N = N; L.E = E; L.B = B; L.Nb = Nb; L.grid = l + 1;
+            if (donor) {
+                if ((int)donor->lv.size() <= l || donor->lv[l].N != N || donor->lv[l].E != E || donor->lv[l].B != B)
+                    throw std::runtime_error("mesh donor differs from the levels given");
+                L = donor->lv[l].v;  // mesh arrays shared; state set below
+                D.wall = donor->lv[l].wall;
+                D.d_wall = donor->lv[l].d_wall;
+            } else {
             // edges
             std::vector<int2> edge(E);
             std::vector<double> wx(E), wy(E), wz(E), slen(E, 0.0);
@@ -574,6 +252,8 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
                 L.parent = X.upload(par); L.rweight = X.upload(rw);
                 L.child_ptr = X.upload(cp); L.child = X.upload(ch);
             }
+            if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
+            }  // mesh upload
             // state
             L.u = X.alloc<double>(5 * (size_t)N); L.uprev = X.alloc<double>(5 * (size_t)N);
             L.rhs = X.alloc<double>(5 * (size_t)N); L.src = X.alloc<double>(5 * (size_t)N);
@@ -586,27 +266,38 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
             const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
             const bool visc = c->ReynoldsNumber > 0.0;
             L.tau = visc ? X.alloc<double>(9 * (size_t)N) : nullptr;
+            L.prim = visc ? X.alloc<double>(4 * (size_t)N) : nullptr;
+            L.vdt = X.alloc<double>(N);
             L.wstress = X.alloc<double>(3 * (size_t)N);
             CK(cudaMemset(L.wstress, 0, 3 * (size_t)N * sizeof(double)));
             L.grad = hllc2 ? X.alloc<double>(15 * (size_t)N) : nullptr;
             L.bnd = hllc2 ? X.alloc<double>(10 * (size_t)N) : nullptr;
+            L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
             if (c->precision == FLITE_MIXED) {
-                L.u32 = X.alloc<float>(5 * (size_t)N);
-                L.p32 = X.alloc<float>(N);
-                std::vector<float> w32(3 * (size_t)std::max(E, 1));
-                for (int e = 0; e < E; ++e) {
-                    w32[e] = (float)wx[e]; w32[(size_t)E + e] = (float)wy[e]; w32[2 * (size_t)E + e] = (float)wz[e];
+                L.ua = X.alloc<double>(5 * (size_t)N);
+                L.ra = X.alloc<double>(5 * (size_t)N);
+                L.pa = X.alloc<double>(N);
+                L.a32 = X.alloc<float>(5 * (size_t)N);
+                L.d32 = X.alloc<float>(6 * (size_t)N);
+                // a zero anchor makes the increments the full FP32 fluxes
+                // until the first FP64 evaluation
+                for (double *a : {L.ua, L.ra}) CK(cudaMemset(a, 0, 5 * (size_t)N * sizeof(double)));
+                CK(cudaMemset(L.pa, 0, (size_t)N * sizeof(double)));
+                CK(cudaMemset(L.a32, 0, 5 * (size_t)N * sizeof(float)));
+                if (!(donor && L.wx32)) {
+                    std::vector<float> w32(3 * (size_t)std::max(E, 1));
+                    for (size_t k = 0; k < 3 * (size_t)E; ++k) w32[k] = (float)d.side_w[k];
+                    float *dw = X.upload(w32);
+                    L.wx32 = dw; L.wy32 = dw + E; L.wz32 = dw + 2 * (size_t)E;
                 }
-                float *dw = X.upload(w32);
-                L.wx32 = dw; L.wy32 = dw + E; L.wz32 = dw + 2 * (size_t)E;
                 L.flux32 = X.alloc<float>(5 * (size_t)std::max(E, 1));
-                L.flux = X.alloc<double>(5);  // unused in this mode
             } else {
-                L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
+                L.ua = L.ra = L.pa = nullptr;
+                L.a32 = L.d32 = nullptr;
+                L.flux32 = nullptr;
             }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
             L.cyc = X.d_cyc + l;
-            if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
         }
         CK(cudaDeviceSynchronize());
         return FLITE_OK;
@@ -614,6 +305,12 @@ int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *l
     if (rc != FLITE_OK) return rc;
     *out = ctx.release();
     return FLITE_OK;
+}
+
+extern "C" {
+
+int flite_create(const flite_controls *c, int nlevels, const flite_level_desc *levels, flite_ctx **out) {
+    return flite::create_context(c, nlevels, levels, nullptr, out);
 }
 
 int flite_destroy(flite_ctx *ctx) {
@@ -794,10 +491,16 @@ int flite_residual_fwd(flite_ctx *ctx, int level, const double *u, double *r) {
         flite_ctx &X = *ctx;
         const int l = level - 1;
         LevelView &L = X.V(l);
+        if (X.mixed()) {
+            // anchor at the level's current state, then the increments to u
+            X.pressure(l);
+            X.rhs_terms(l, true);
+            X.node_update(l, MODE_RESID, 0, true);
+        }
         CK(cudaMemcpyAsync(L.u, u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, X.s));
         X.pressure(l);
-        X.rhs_terms(l);
-        X.node_update(l, MODE_RESID, 0);
+        X.rhs_terms(l, false);
+        X.node_update(l, MODE_RESID, 0, false);
         CK(cudaMemcpyAsync(r, L.rhs, 5 * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
         return FLITE_OK;
@@ -847,12 +550,14 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, do
         for (int r = 0; r < reps; ++r) {
             X.pressure(l);
             CK(cudaEventRecord(ev[0], X.s));
-            X.edge_flux_launch(L);
+            X.edge_flux_launch(L, false);
             CK(cudaEventRecord(ev[1], X.s));
             if (L.B > 0) k_bnd_flux<<<flite_ctx::blocks(L.B), kBlock, 0, X.s>>>(X.P, L);
             CK(cudaEventRecord(ev[2], X.s));
-            if (X.mixed()) k_node_update<true><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
-            else k_node_update<false><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            if (X.mixed())
+                k_node_update<GATHER_DELTA><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            else
+                k_node_update<GATHER_FP64><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
             CK(cudaEventRecord(ev[3], X.s));
             CK(cudaEventSynchronize(ev[3]));
             float a = 0, b = 0;

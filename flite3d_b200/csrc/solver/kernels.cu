@@ -85,7 +85,9 @@ __global__ void k_timestep(Params P, LevelView L) {
         }
     }
     const double V = L.V[i];
-    L.dt[i] = 0.5 / (acc / V + h / (V * V));
+    const double dt = 0.5 / (acc / V + h / (V * V));
+    L.dt[i] = dt;
+    L.vdt[i] = V / dt;  // V/dt of the dissipation coefficient d0
 }
 
 // ---- makeArtificialDissipation2, passes 1-2 and the node finish -----------
@@ -128,7 +130,7 @@ __global__ void k_jst_lap(Params P, LevelView L) {
 }
 
 // ---- makeArtificialDissipation2, pass 3 (def_par:11770-11906), scalar -----
-__global__ void k_jst_flux(Params P, LevelView L) {
+__global__ void __launch_bounds__(256, 3) k_jst_flux(Params P, LevelView L) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -136,11 +138,11 @@ __global__ void k_jst_flux(Params P, LevelView L) {
     double acc[5] = {0, 0, 0, 0, 0};
     double Li[5], Ui[5];
     for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
-    const double vdi = L.V[i] / L.dt[i], coni = L.conn[i], si = L.sens[i];
+    const double vdi = L.vdt[i], coni = L.conn[i], si = L.sens[i];
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
         int j = t.y;
-        double vdj = L.V[j] / L.dt[j];
+        double vdj = L.vdt[j];
         const bool first = t.x >= 0;
         double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
         d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
@@ -168,11 +170,11 @@ __global__ void k_first_order_diss(Params P, LevelView L) {
     if (i >= L.N) return;
     const int N = L.N;
     double acc[5] = {0, 0, 0, 0, 0};
-    const double vdi = L.V[i] / L.dt[i], coni = L.conn[i];
+    const double vdi = L.vdt[i], coni = L.conn[i];
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
         int j = t.y;
-        double vdj = L.V[j] / L.dt[j];
+        double vdj = L.vdt[j];
         const bool first = t.x >= 0;
         double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
         d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
@@ -189,7 +191,21 @@ __global__ void k_first_order_diss(Params P, LevelView L) {
 // pass 1: Galerkin gradients of (u, v, w, T), then per node the Sutherland
 // viscosity (T^1.5 evaluated as T*sqrt(T)), the stress tensor and heat
 // flux, the adiabatic-wall projection and the wall stress (level 1)
-__global__ void k_visc_grad(Params P, LevelView L) {
+// per node (u, v, w, T) of the viscous routine (def_par:5260-5270): each
+// edge of the reference divides again; the quotients are the same numbers
+__global__ void k_visc_prim(Params P, LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double gOg = P.gamma / (P.gamma - 1.0);
+    const double r = L.u[i];
+    L.prim[i] = L.u[N + i] / r;
+    L.prim[N + i] = L.u[2 * N + i] / r;
+    L.prim[2 * N + i] = L.u[3 * N + i] / r;
+    L.prim[3 * N + i] = gOg * L.p[i] / r;
+}
+
+__global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -197,9 +213,7 @@ __global__ void k_visc_grad(Params P, LevelView L) {
     double g[12];
     for (int c = 0; c < 12; ++c) g[c] = 0.0;
     auto prim = [&](int j, double *q) {
-        double r = L.u[j];
-        q[0] = L.u[N + j] / r; q[1] = L.u[2 * N + j] / r; q[2] = L.u[3 * N + j] / r;
-        q[3] = gOg * L.p[j] / r;
+        q[0] = L.prim[j]; q[1] = L.prim[N + j]; q[2] = L.prim[2 * N + j]; q[3] = L.prim[3 * N + j];
     };
     double qi[4];
     prim(i, qi);
@@ -268,20 +282,20 @@ __global__ void k_visc_grad(Params P, LevelView L) {
 
 // pass 2: viscous edge fluxes gathered per node and subtracted from the
 // dissipation vector (def_par:5662-5892)
-__global__ void k_visc_flux(Params P, LevelView L) {
+__global__ void __launch_bounds__(256, 3) k_visc_flux(Params P, LevelView L) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
     double ti[9], ui[3];
     for (int c = 0; c < 9; ++c) ti[c] = L.tau[c * N + i];
-    ui[0] = L.u[N + i] / L.u[i]; ui[1] = L.u[2 * N + i] / L.u[i]; ui[2] = L.u[3 * N + i] / L.u[i];
+    ui[0] = L.prim[i]; ui[1] = L.prim[N + i]; ui[2] = L.prim[2 * N + i];
     double acc[4] = {0, 0, 0, 0};
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
         int e = t.x >= 0 ? t.x : ~t.x, j = t.y;
         double tj[9], uj[3];
         for (int c = 0; c < 9; ++c) tj[c] = L.tau[c * N + j];
-        uj[0] = L.u[N + j] / L.u[j]; uj[1] = L.u[2 * N + j] / L.u[j]; uj[2] = L.u[3 * N + j] / L.u[j];
+        uj[0] = L.prim[j]; uj[1] = L.prim[N + j]; uj[2] = L.prim[2 * N + j];
         const bool first = t.x >= 0;
         const double *a = first ? ti : tj, *b = first ? tj : ti;
         const double *ua = first ? ui : uj, *ub = first ? uj : ui;
@@ -305,8 +319,8 @@ __global__ void k_visc_flux(Params P, LevelView L) {
         int2 nd = L.bedge[bb];
         double a[9], b[9], ua[3], ub[3];
         for (int c = 0; c < 9; ++c) { a[c] = L.tau[c * N + nd.x]; b[c] = L.tau[c * N + nd.y]; }
-        ua[0] = L.u[N + nd.x] / L.u[nd.x]; ua[1] = L.u[2 * N + nd.x] / L.u[nd.x]; ua[2] = L.u[3 * N + nd.x] / L.u[nd.x];
-        ub[0] = L.u[N + nd.y] / L.u[nd.y]; ub[1] = L.u[2 * N + nd.y] / L.u[nd.y]; ub[2] = L.u[3 * N + nd.y] / L.u[nd.y];
+        ua[0] = L.prim[nd.x]; ua[1] = L.prim[N + nd.x]; ua[2] = L.prim[2 * N + nd.x];
+        ub[0] = L.prim[nd.y]; ub[1] = L.prim[N + nd.y]; ub[2] = L.prim[2 * N + nd.y];
         const double wx = L.bwx[bb], wy = L.bwy[bb], wz = L.bwz[bb];
         double dt[9];
         for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
@@ -476,70 +490,63 @@ __global__ void k_bnd_flux(Params P, LevelView L) {
 }
 
 // ---- mixed precision ------------------------------------------------------
-// FP32 shadows of the conserved state and pressure for the FP32 edge fluxes
-__global__ void k_shadow(LevelView L) {
+// The interior central flux of an edge is G(u1; w) + G(u2; w) with the
+// one-sided flux G(u; w) = F(u).w.  FLITE_MIXED evaluates it as
+//   G(u; w) = G(ua; w) + dG,
+// where ua is an FP64 anchor state whose interior-edge residual was summed in
+// FP64, and dG is computed in FP32 from the increments du = u - ua and
+// dp = p - pa in a form whose every term carries an increment:
+//   dv   = (dm - va drho) / rho
+//   dG_0 = dm.w
+//   dG_k = dm_k (v.w) + ma_k (dv.w) + dp w_k          k = 1..3
+//   dG_4 = (dE + dp)(v.w) + (Ea + pa)(dv.w)
+// so its rounding error is relative to the increment, not to the flux: the
+// iteration converges to the FP64 fixed point.  The anchor is refreshed by an
+// FP64 evaluation at the first stage of every relaxation step (and at the
+// coarse-level evaluation of restrictGrid).
+
+// increments over the anchor: du (FP64 difference, rounded once) and dp
+__global__ void k_delta_state(LevelView L) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
-    for (int c = 0; c < 5; ++c) L.u32[c * N + i] = (float)L.u[c * N + i];
-    L.p32[i] = (float)L.p[i];
+    for (int c = 0; c < 5; ++c) L.d32[c * N + i] = (float)(L.u[c * N + i] - L.ua[c * N + i]);
+    L.d32[5 * N + i] = (float)(L.p[i] - L.pa[i]);
 }
 
-// central flux (def_par:1664-1669) in FP32 into the FP32 edge buffer
-__global__ void __launch_bounds__(256) k_edge_flux_f32_central(LevelView L) {
+// increment of the one-sided flux G(u; w) of one node
+__device__ __forceinline__ void delta_flux(const LevelView &L, int i, float wx, float wy, float wz, float *g) {
+    const int N = L.N;
+    const float ra = L.a32[i], vax = L.a32[N + i], vay = L.a32[2 * N + i], vaz = L.a32[3 * N + i];
+    const float ha = L.a32[4 * N + i];
+    const float dr = L.d32[i], dmx = L.d32[N + i], dmy = L.d32[2 * N + i], dmz = L.d32[3 * N + i];
+    const float dE = L.d32[4 * N + i], dp = L.d32[5 * N + i];
+    const float rinv = 1.f / (ra + dr);
+    const float dvx = (dmx - vax * dr) * rinv, dvy = (dmy - vay * dr) * rinv, dvz = (dmz - vaz * dr) * rinv;
+    const float vw = ((vax + dvx) * wx + (vay + dvy) * wy) + (vaz + dvz) * wz;
+    const float dvw = (dvx * wx + dvy * wy) + dvz * wz;
+    g[0] = (dmx * wx + dmy * wy) + dmz * wz;
+    g[1] = (dmx * vw + (ra * vax) * dvw) + dp * wx;
+    g[2] = (dmy * vw + (ra * vay) * dvw) + dp * wy;
+    g[3] = (dmz * vw + (ra * vaz) * dvw) + dp * wz;
+    g[4] = (dE + dp) * vw + ha * dvw;
+}
+
+// interior central-flux increments in FP32 into the FP32 edge buffer
+__global__ void __launch_bounds__(256) k_edge_flux_f32_delta(LevelView L) {
     int e = tid();
     if (e >= L.E) return;
-    const int N = L.N;
     const int2 nd = L.edge[e];
-    const int i1 = nd.x, i2 = nd.y;
-    const float r1 = L.u32[i1], ru1 = L.u32[N + i1], rv1 = L.u32[2 * N + i1], rw1 = L.u32[3 * N + i1];
-    const float E1 = L.u32[4 * N + i1], pr1 = L.p32[i1];
-    const float r2 = L.u32[i2], ru2 = L.u32[N + i2], rv2 = L.u32[2 * N + i2], rw2 = L.u32[3 * N + i2];
-    const float E2 = L.u32[4 * N + i2], pr2 = L.p32[i2];
-    const float rinv1 = 1.f / r1, rinv2 = 1.f / r2;
-    const float u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1, rh1 = E1 + pr1;
-    const float u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2, rh2 = E2 + pr2;
     const float wx = L.wx32[e], wy = L.wy32[e], wz = L.wz32[e];
+    float g1[5], g2[5];
+    delta_flux(L, nd.x, wx, wy, wz, g1);
+    delta_flux(L, nd.y, wx, wy, wz, g2);
     float *o = L.flux32 + (size_t)e * 5;
-    o[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
-    o[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
-    o[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
-    o[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
-    o[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
-    (void)E1; (void)E2;
+    for (int c = 0; c < 5; ++c) o[c] = g1[c] + g2[c];
 }
 
-// error-free sum s + x = hi + lo (Knuth's TwoSum; additions only)
-__device__ __forceinline__ void two_sum(float a, float b, float &hi, float &lo) {
-    float s = a + b;
-    float bp = s - a;
-    lo = (a - (s - bp)) + (b - bp);
-    hi = s;
-}
-
-// residual of node i from the FP32 edge buffer: compensated FP32 sums in
-// edge order, then the FP64 boundary-edge contributions
-__device__ __forceinline__ void gather_rhs_mixed(const LevelView &L, int i, double *r) {
-    float hi[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, lo[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-        int s = L.inc[k].x;
-        const float *f = L.flux32 + (size_t)(s >= 0 ? s : ~s) * 5;
-        for (int c = 0; c < 5; ++c) {
-            float e;
-            two_sum(hi[c], s >= 0 ? f[c] : -f[c], hi[c], e);
-            lo[c] += e;
-        }
-    }
-    for (int c = 0; c < 5; ++c) r[c] = (double)hi[c] + (double)lo[c];
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-        int v = L.binc[k];
-        const double *g = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
-        r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
-    }
-}
-
-// residual of node i: interior edges in edge order, then boundary edges
-__device__ __forceinline__ void gather_rhs(const LevelView &L, int i, double *r) {
+// interior edges of node i from the FP64 edge buffer, in edge order
+__device__ __forceinline__ void gather_interior(const LevelView &L, int i, double *r) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int s = L.inc[k].x;
@@ -551,6 +558,10 @@ __device__ __forceinline__ void gather_rhs(const LevelView &L, int i, double *r)
             r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
         }
     }
+}
+
+// boundary edges of node i (FP64)
+__device__ __forceinline__ void gather_boundary(const LevelView &L, int i, double *r) {
     for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
         int v = L.binc[k];
         const double *g = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
@@ -558,19 +569,63 @@ __device__ __forceinline__ void gather_rhs(const LevelView &L, int i, double *r)
     }
 }
 
+// interior residual of node i as the anchor's FP64 sum plus the FP32 sum of
+// the flux increments of its edges
+__device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i, double *r) {
+    float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        int s = L.inc[k].x;
+        const float *f = L.flux32 + (size_t)(s >= 0 ? s : ~s) * 5;
+        if (s >= 0) {
+            for (int c = 0; c < 5; ++c) acc[c] += f[c];
+        } else {
+            for (int c = 0; c < 5; ++c) acc[c] -= f[c];
+        }
+    }
+    const int N = L.N;
+    for (int c = 0; c < 5; ++c) r[c] = L.ra[c * N + i] + (double)acc[c];
+}
+
+// the FP64 evaluation becomes the new anchor of node i
+__device__ __forceinline__ void store_anchor(const LevelView &L, int i, const double *rint) {
+    const int N = L.N;
+    double u[5];
+    for (int c = 0; c < 5; ++c) {
+        u[c] = L.u[c * N + i];
+        L.ua[c * N + i] = u[c];
+        L.ra[c * N + i] = rint[c];
+    }
+    const double p = L.p[i];
+    L.pa[i] = p;
+    const double rinv = 1.0 / u[0];
+    L.a32[i] = (float)u[0];
+    L.a32[N + i] = (float)(u[1] * rinv);
+    L.a32[2 * N + i] = (float)(u[2] * rinv);
+    L.a32[3 * N + i] = (float)(u[3] * rinv);
+    L.a32[4 * N + i] = (float)(u[4] + p);
+}
+
 // ---- the node part of one RK stage (def_par:1069-1178), fused -------------
 // mode STAGE:   u <- update of stage `stage`
 // mode RCOARSE: restrictGrid coarse one-step (def_par:12244-12263): src
 // mode RFINE:   restrictGrid fine increment (def_par:12356-12383): rhs
 // mode RESID:   rhs <- makeRHS only
-template <bool MIXED>
+// PREC: GATHER_FP64 (FP64 edge buffer), GATHER_ANCHOR (FP64 edge buffer,
+// stored as the new mixed-precision anchor), GATHER_DELTA (anchor + FP32
+// increments)
+template <int PREC>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
     double r[5];
-    if constexpr (MIXED) gather_rhs_mixed(L, i, r);
-    else gather_rhs(L, i, r);
+    if constexpr (PREC == GATHER_DELTA) {
+        gather_interior_delta(L, i, r);
+    } else {
+        gather_interior(L, i, r);
+        if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, r);
+    }
+    gather_boundary(L, i, r);
     if (mode == MODE_RESID) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
@@ -614,8 +669,9 @@ __global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = un[c] - up[c];
     }
 }
-template __global__ void k_node_update<false>(Params, LevelView, int, int);
-template __global__ void k_node_update<true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_FP64>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA>(Params, LevelView, int, int);
 
 // ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
 __global__ void k_copy(const double *a, double *b, size_t n) {

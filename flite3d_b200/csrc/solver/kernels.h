@@ -11,6 +11,7 @@ __global__ void k_timestep(Params P, LevelView L);
 __global__ void k_jst_lap(Params P, LevelView L);
 __global__ void k_jst_flux(Params P, LevelView L);
 __global__ void k_first_order_diss(Params P, LevelView L);
+__global__ void k_visc_prim(Params P, LevelView L);
 __global__ void k_visc_grad(Params P, LevelView L);
 __global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
@@ -20,10 +21,11 @@ __global__ void k_minmax(Params P, LevelView L);
 template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 __global__ void k_bnd_flux(Params P, LevelView L);
-template <bool MIXED>
+enum { GATHER_FP64 = 0, GATHER_ANCHOR = 1, GATHER_DELTA = 2 };
+template <int PREC>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
-__global__ void k_shadow(LevelView L);
-__global__ void k_edge_flux_f32_central(LevelView L);
+__global__ void k_delta_state(LevelView L);
+__global__ void k_edge_flux_f32_delta(LevelView L);
 __global__ void k_copy(const double *a, double *b, size_t n);
 __global__ void k_restrict_u(LevelView C, LevelView F);
 __global__ void k_restrict_state(Params P, LevelView C, LevelView F);

@@ -166,6 +166,29 @@ class Solver:
         self._ck(self.be.residual_fwd(self._h, level, _ptr(u), _ptr(r)), "residual_fwd")
         return r
 
+    def residual_vjp(self, u, rbar, level=1):
+        """ubar = (dR/du)^T rbar of residual_fwd (GPU library only)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        rbar = np.ascontiguousarray(rbar, dtype=np.float64)
+        ub = np.zeros_like(u)
+        self._ck(self.be.residual_vjp(self._h, level, _ptr(u), _ptr(rbar), _ptr(ub)), "residual_vjp")
+        return ub
+
+    def residual_jvp(self, u, du, level=1):
+        """jv = (dR/du) du of residual_fwd (the oracle's tangent)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        jv = np.zeros_like(u)
+        self._ck(self.be.residual_jvp(self._h, level, _ptr(u), _ptr(du), _ptr(jv)), "residual_jvp")
+        return jv
+
+    def profile_adjoint(self, level=1, reps=10):
+        """(forward ms, adjoint ms) per residual evaluation on a level."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.be.profile_adjoint(self._h, level, reps, ctypes.byref(a), ctypes.byref(b)),
+                 "profile_adjoint")
+        return a.value, b.value
+
     def time_cycles(self, ncycles, cycle_no=1):
         ms = ctypes.c_double()
         self._ck(self.be.time_cycles(self._h, cycle_no, ncycles, ctypes.byref(ms)), "time_cycles")
@@ -217,3 +240,86 @@ def run_steady(solver, orders=8.0, max_cycles=1000, callback=None):
         if not (math.log(res0) - math.log(res[0]) < math.log(10.0) * orders):
             break
     return hist
+
+
+class Batch:
+    """Many solves (mesh x flow condition) advanced together: one CUDA-graph
+    launch per batch cycle; cases on one mesh share the mesh's device copy."""
+
+    def __init__(self, cases):
+        """cases: list of (controls, mesh) pairs."""
+        lib = _abi.gpu_lib()
+        self._lib = lib
+        meshes, mesh_of = [], []
+        for _, m in cases:
+            for k, mm in enumerate(meshes):
+                if mm is m:
+                    mesh_of.append(k)
+                    break
+            else:
+                meshes.append(m)
+                mesh_of.append(len(meshes) - 1)
+        self.meshes = meshes
+        n = len(cases)
+        ctl = (_abi.Controls * n)(*[c for c, _ in cases])
+        mof = (ctypes.c_int32 * n)(*mesh_of)
+        nlev = (ctypes.c_int32 * len(meshes))(*[m.nlevels for m in meshes])
+        lv = (ctypes.c_void_p * len(meshes))(*[ctypes.addressof(m.descs) for m in meshes])
+        self._h = _vp()
+        rc = lib.flite_batch_create(n, ctl, mof, len(meshes), nlev, lv, ctypes.byref(self._h))
+        if rc != _abi.FLITE_OK:
+            raise RuntimeError(f"flite_batch_create failed with status {rc}")
+        self.cases = []
+        for i, (c, m) in enumerate(cases):
+            h = _vp()
+            _abi.check(lib.flite_batch_context(self._h, i, ctypes.byref(h)), "flite_batch_context")
+            s = Solver.__new__(Solver)
+            s.c, s.mesh, s.be, s._h = c, m, Backend(lib, "flite_"), h
+            ng = m.nlevels if c.numberOfGridsToUse <= 0 else min(m.nlevels, c.numberOfGridsToUse)
+            s.nlevels = ng
+            s.nodes = [m.level(l + 1).n_nodes for l in range(ng)]
+            s.close = lambda: None  # owned by the batch
+            self.cases.append(s)
+
+    def cycle(self, cycle_no):
+        _abi.check(self._lib.flite_batch_cycle(self._h, cycle_no), "flite_batch_cycle")
+
+    def run(self, orders=8.0, max_cycles=1000, first_cycle=1, check_every=1):
+        """Cycle every case until its res1 falls by 10^-orders (or max_cycles);
+        returns (cycles run per case, log10 residual reduction per case)."""
+        n = len(self.cases)
+        cyc = (ctypes.c_int32 * n)()
+        red = (ctypes.c_double * n)()
+        _abi.check(self._lib.flite_batch_run(self._h, first_cycle, max_cycles, ctypes.c_double(orders),
+                                             check_every, cyc, red), "flite_batch_run")
+        return np.array(cyc[:]), np.array(red[:])
+
+    def time_cycles(self, ncycles, cycle_no=1, sequential=False):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        _abi.check(self._lib.flite_batch_time_cycles(self._h, cycle_no, ncycles, int(sequential),
+                                                     ctypes.byref(ms), ctypes.byref(n)),
+                   "flite_batch_time_cycles")
+        return ms.value, n.value
+
+    def autotune(self, reps=3, cycle_no=1):
+        e, n, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        _abi.check(self._lib.flite_batch_autotune(self._h, cycle_no, reps, ctypes.byref(e),
+                                                  ctypes.byref(n), ctypes.byref(ms)),
+                   "flite_batch_autotune")
+        return e.value, n.value, ms.value
+
+    def set_blocks(self, edge_block, node_block):
+        _abi.check(self._lib.flite_batch_set_blocks(self._h, edge_block, node_block),
+                   "flite_batch_set_blocks")
+
+    def close(self):
+        if self._h:
+            self._lib.flite_batch_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

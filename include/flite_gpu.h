@@ -174,6 +174,51 @@ int flite_forces(flite_ctx *ctx, double out[6]);
  * pressure recomputed from u; r is [5][N].                                 */
 int flite_residual_fwd(flite_ctx *ctx, int level, const double *u, double *r);
 
+/* ---- discrete adjoint of the edge residual ------------------------------
+ * ubar = (dR/du)^T rbar for R = flite_residual_fwd on a level (central flux,
+ * fluxType 1, FP64; wall, symmetry and far-field boundary fluxes), the
+ * backward half of the forward/backward pair.  u, rbar, ubar are [5][N].
+ * Like flite_residual_fwd it replaces the level's state by u.  No reference
+ * counterpart: the reference has no adjoint.                               */
+int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, const double *rbar,
+                       double *ubar);
+/* average device ms of one forward residual evaluation and of one adjoint
+ * product on a level (the adjoint cost ratio is vjp/fwd)                  */
+int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double *fwd_ms, double *vjp_ms);
+
+/* ---- batched solves (no reference counterpart: the reference runs one
+ * condition per job) --------------------------------------------------------
+ * ncases solves, case i on mesh mesh_of_case[i] (levels[m] points to the
+ * nlevels[m] level descriptors of mesh m) with its own controls[i].  Cases on
+ * one mesh share its device copy.  flite_batch_cycle advances every case by
+ * one oneCycle with a single CUDA-graph launch; flite_batch_context returns
+ * a case's context for flite_set_state/flite_start/flite_residuals/...      */
+typedef struct flite_batch flite_batch;
+int flite_batch_create(int ncases, const flite_controls *controls, const int32_t *mesh_of_case,
+                       int nmeshes, const int32_t *nlevels, const flite_level_desc *const *levels,
+                       flite_batch **out);
+int flite_batch_destroy(flite_batch *b);
+int flite_batch_context(flite_batch *b, int case_index, flite_ctx **ctx);
+int flite_batch_cycle(flite_batch *b, int cycle_no);
+/* multiGridCycles over the batch: batch cycles first_cycle, first_cycle+1, ...
+ * until every case has res1 <= 10^-orders times its res1 after the first
+ * cycle (checked after the first cycle and then every check_every cycles),
+ * or max_cycles.  A converged case leaves the batch graph.  cycles[i] is the
+ * number of cycles case i ran, log10_reduction[i] its log10(res1/res1(1));
+ * FLITE_ENAN when a residual is not finite.                                */
+int flite_batch_run(flite_batch *b, int first_cycle, int max_cycles, double orders, int check_every,
+                    int32_t *cycles, double *log10_reduction);
+/* device time of ncycles batch cycles, as one graph launch each
+ * (sequential = 0) or as the cases' own graphs launched one after another
+ * (sequential = 1); also the kernel launches one batch cycle holds          */
+int flite_batch_time_cycles(flite_batch *b, int cycle_no, int ncycles, int sequential, double *ms,
+                            int64_t *launches_per_cycle);
+/* time reps batch cycles for each edge/node block size in {64,128,256} and
+ * keep the fastest pair (advances every case by 9*(reps+1) cycles)       */
+int flite_batch_autotune(flite_batch *b, int cycle_no, int reps, int32_t *edge_block,
+                         int32_t *node_block, double *best_ms);
+int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_block);
+
 /* ---- timing ----------------------------------------------------------- */
 /* Capture one oneCycle as a CUDA graph and replay it `ncycles` times;
  * returns the device time (ms) measured with CUDA events on the context's

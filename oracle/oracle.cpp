@@ -54,7 +54,97 @@ struct Level {
     vec p, dt, mu, conn, wallArea, nx, ny, nz, wallStress[3];
     int cycleNumber = 0;
     int R(int i) const { return reg[i + 20]; }  // nodeIndicatorRegister(i)
+    // colouring of edge blocks for the threaded timing mode (built on first
+    // use): blocks of colour k are cord[cptr[k] .. cptr[k+1])
+    std::vector<int> cptr, cord, bcptr, bcord;
 };
+
+// Threads of the timing mode.  1 (the default) runs every loop in the
+// reference's order; more threads run each edge loop colour by colour in
+// parallel, which changes the order of the sums at a node (results then
+// differ in the last bits) but not the algorithm.  Used only to time the
+// CPU baseline on all host cores.
+int g_threads = 1;
+
+// Edges are grouped in blocks of consecutive edges (kept in the
+// reference's order inside a block, for locality), and the blocks coloured
+// greedily so that no two blocks of a colour share a node.
+constexpr int kEdgeBlock = 2048;
+
+void colour_blocks(int n, const int *a, const int *b, int nnodes, std::vector<int> &cptr,
+                   std::vector<int> &cord) {
+    const int nb = (n + kEdgeBlock - 1) / kEdgeBlock;
+    std::vector<uint64_t> mask(nnodes, 0);
+    std::vector<int> col(nb, 0);
+    int ncol = 0;
+    for (int q = 0; q < nb; ++q) {
+        const int e0 = q * kEdgeBlock, e1 = std::min(n, e0 + kEdgeBlock);
+        uint64_t m = 0;
+        for (int e = e0; e < e1; ++e) m |= mask[a[e]] | mask[b[e]];
+        int k = 0;
+        while (k < 64 && (m >> k & 1)) ++k;
+        if (k == 64) {  // too many colours: one block per colour from here
+            k = ncol;
+        } else {
+            for (int e = e0; e < e1; ++e) {
+                mask[a[e]] |= uint64_t(1) << k;
+                mask[b[e]] |= uint64_t(1) << k;
+            }
+        }
+        col[q] = k;
+        ncol = std::max(ncol, k + 1);
+    }
+    cptr.assign(ncol + 1, 0);
+    for (int q = 0; q < nb; ++q) ++cptr[col[q] + 1];
+    for (int k = 0; k < ncol; ++k) cptr[k + 1] += cptr[k];
+    cord.resize(nb);
+    std::vector<int> at(cptr.begin(), cptr.end() - 1);
+    for (int q = 0; q < nb; ++q) cord[at[col[q]]++] = q;
+}
+
+template <class F>
+void for_blocks(int n, const std::vector<int> &cptr, const std::vector<int> &cord, F &&f) {
+    const int ncol = (int)cptr.size() - 1;
+    for (int k = 0; k < ncol; ++k) {
+        const int a = cptr[k], b = cptr[k + 1];
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads)
+        for (int q = a; q < b; ++q) {
+            const int e0 = cord[q] * kEdgeBlock, e1 = std::min(n, e0 + kEdgeBlock);
+            for (int e = e0; e < e1; ++e) f(e);
+        }
+    }
+}
+
+template <class F>
+void for_edges(Level &g, F &&f) {
+    if (g_threads <= 1) {
+        for (int e = 0; e < g.E; ++e) f(e);
+        return;
+    }
+    if (g.cptr.empty()) colour_blocks(g.E, g.s1.data(), g.s2.data(), g.N, g.cptr, g.cord);
+    for_blocks(g.E, g.cptr, g.cord, f);
+}
+
+// boundary edges, likewise
+template <class F>
+void for_bedges(Level &g, F &&f) {
+    if (g_threads <= 1) {
+        for (int b = 0; b < g.B; ++b) f(b);
+        return;
+    }
+    if (g.bcptr.empty()) colour_blocks(g.B, g.b1.data(), g.b2.data(), g.N, g.bcptr, g.bcord);
+    for_blocks(g.B, g.bcptr, g.bcord, f);
+}
+
+template <class F>
+void for_nodes(int n, F &&f) {
+    if (g_threads <= 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int i = 0; i < n; ++i) f(i);
+}
 
 struct Oracle {
     flite_controls c;
@@ -66,10 +156,10 @@ struct Oracle {
     // ---- makePressureField (def_par:13612-13630) --------------------------
     void makePressureField(Level &g, vec *u) {
         const double gm1 = c.gamma - 1.0;
-        for (int i = 0; i < g.N; ++i) {
+        for_nodes(g.N, [&](int i) {
             double pp = gm1 * (u[4][i] - 0.5 * ((u[1][i] * u[1][i] + u[2][i] * u[2][i]) + u[3][i] * u[3][i]) / u[0][i]);
             g.p[i] = std::max(pp, 0.1);
-        }
+        });
     }
 
     // ---- makeTimeSteps (def_par:13335-13610) ------------------------------
@@ -84,7 +174,7 @@ struct Oracle {
             if (c.turbulenceModel == 1) return g.mu[i] + g.u[5][i] / c.ReynoldsNumber;
             return g.mu[i];
         };
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
             double al = (wx * wx + wy * wy) + wz * wz;
@@ -102,8 +192,8 @@ struct Oracle {
                 h1[i1] = h1[i1] + dv2;
                 h1[i2] = h1[i2] + dv1;
             }
-        }
-        for (int b = 0; b < g.B; ++b) {
+        });
+        for_bedges(g, [&](int b) {
             int i1 = g.b1[b], i2 = g.b2[b];
             double wx = g.bwx[b], wy = g.bwy[b], wz = g.bwz[b];
             double al = (wx * wx + wy * wy) + wz * wz;
@@ -126,9 +216,8 @@ struct Oracle {
                 h1[i1] = (h1[i1] + dv1) + dvm;
                 h1[i2] = (h1[i2] + dv2) + dvm;
             }
-        }
-        for (int i = 0; i < g.N; ++i)
-            g.dt[i] = 0.5 / (g.dt[i] / g.V[i] + h1[i] / (g.V[i] * g.V[i]));
+        });
+        for_nodes(g.N, [&](int i) { g.dt[i] = 0.5 / (g.dt[i] / g.V[i] + h1[i] / (g.V[i] * g.V[i])); });
     }
 
     // ---- makeArtificialDissipation2, scalar form (def_par:11484-11993) ----
@@ -137,7 +226,7 @@ struct Oracle {
         for (auto &col : nh) std::fill(col.begin(), col.end(), 0.0);
         if (c.fluxType == 4 && g.grid == 1) return;
         if (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0) return;
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double d[5];
             for (int k = 0; k < 4; ++k) d[k] = g.u[k][i1] - g.u[k][i2];
@@ -150,23 +239,23 @@ struct Oracle {
             }
             nh[5][i1] = nh[5][i1] + df;
             nh[5][i2] = nh[5][i2] + df;
-        }
-        for (int e = 0; e < g.E; ++e) {
+        });
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double dp = g.p[i1] - g.p[i2], sp = g.p[i1] + g.p[i2];
             nh[6][i1] = nh[6][i1] - dp;
             nh[7][i1] = nh[7][i1] + sp;
             nh[6][i2] = nh[6][i2] + dp;
             nh[7][i2] = nh[7][i2] + sp;
-        }
-        for (int i = 0; i < g.N; ++i) {
+        });
+        for_nodes(g.N, [&](int i) {
             double fact = 1. / g.conn[i];
             nh[8][i] = 12. * std::fabs(nh[6][i] / nh[7][i]);
             for (int k = 0; k < 5; ++k) nh[k][i] = fact * nh[k][i];
-        }
+        });
         const double k2 = c.secondOrderDissipationFactor;
         const double k4 = g.grid == 1 ? c.fourthOrderDissipationFactor : c.coarseGridDissipationFactor;
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double d4v[5], d2v[5];
             for (int k = 0; k < 5; ++k) d4v[k] = nh[k][i1] - nh[k][i2];
@@ -179,13 +268,13 @@ struct Oracle {
                 g.diss[k][i1] = (g.diss[k][i1] - d4v[k] * d4) + d2v[k] * d2;
                 g.diss[k][i2] = (g.diss[k][i2] + d4v[k] * d4) - d2v[k] * d2;
             }
-        }
+        });
     }
 
     // ---- makeArtificialDissipation3 (def_par:11995-12139) -----------------
     void makeArtificialDissipation3(Level &g) {
         for (int k = 0; k < 5; ++k) std::fill(g.diss[k].begin(), g.diss[k].end(), 0.0);
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double d0 = std::min(g.V[i1] / g.dt[i1], g.V[i2] / g.dt[i2]) / (g.conn[i1] + g.conn[i2]);
             double d2 = d0 * c.coarseGridDissipationFactor;
@@ -194,7 +283,7 @@ struct Oracle {
                 g.diss[k][i1] = g.diss[k][i1] + dk * d2;
                 g.diss[k][i2] = g.diss[k][i2] - dk * d2;
             }
-        }
+        });
     }
 
     // ---- makeViscosityTerm, wide stencil (def_par:5198-5893) --------------
@@ -209,7 +298,7 @@ struct Oracle {
             q[0] = g.u[1][i] / r; q[1] = g.u[2][i] / r; q[2] = g.u[3][i] / r;
             q[3] = gOg * g.p[i] / r;
         };
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double w[3] = {g.wx[e], g.wy[e], g.wz[e]};
             double q1[4], q2[4];
@@ -220,8 +309,8 @@ struct Oracle {
                     nh[a * 4 + k][i1] = nh[a * 4 + k][i1] + d;
                     nh[a * 4 + k][i2] = nh[a * 4 + k][i2] - d;
                 }
-        }
-        for (int b = 0; b < g.B; ++b) {
+        });
+        for_bedges(g, [&](int b) {
             int i1 = g.b1[b], i2 = g.b2[b];
             double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
             double q1[4], q2[4];
@@ -236,10 +325,10 @@ struct Oracle {
                     double s = q1[k] + q2[k];
                     nh[a * 4 + k][i2] = nh[a * 4 + k][i2] + (2. * q2[k] + s) * w[a];
                 }
-        }
+        });
         const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
         const double oRe = 1. / c.ReynoldsNumber, oPr = 1. / c.PrandtlNumber;
-        for (int i = 0; i < g.N; ++i) {
+        for_nodes(g.N, [&](int i) {
             double vt = 1. / g.V[i];
             double dudx = nh[0][i] * vt, dvdx = nh[1][i] * vt, dwdx = nh[2][i] * vt, dTdx = nh[3][i] * vt;
             double dudy = nh[4][i] * vt, dvdy = nh[5][i] * vt, dwdy = nh[6][i] * vt, dTdy = nh[7][i] * vt;
@@ -259,7 +348,7 @@ struct Oracle {
             nh[6][i] = k * dTdx;
             nh[7][i] = k * dTdy;
             nh[8][i] = k * dTdz;
-        }
+        });
         if (g.grid == 1) {
             // setTemperatureForAdiabaticWall (def_par:5170-5196)
             for_range(g, -20, -19, [&](int ip) {
@@ -282,7 +371,7 @@ struct Oracle {
             for (int k = 0; k < 9; ++k) t[k] = nh[k][i];
             uu[0] = g.u[1][i] / g.u[0][i]; uu[1] = g.u[2][i] / g.u[0][i]; uu[2] = g.u[3][i] / g.u[0][i];
         };
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
             double a[9], b[9], ua[3], ub[3];
@@ -301,7 +390,7 @@ struct Oracle {
                 nh[9 + k][i1] = nh[9 + k][i1] + f[k];
                 nh[9 + k][i2] = nh[9 + k][i2] - f[k];
             }
-        }
+        });
         for (int bb = 0; bb < g.B; ++bb) {
             int ind = g.bind[bb];
             if (ind == 2 || ind == 9) continue;
@@ -331,14 +420,13 @@ struct Oracle {
             nh[11][i2] = (nh[11][i2] + f4) + 2.0 * ((wx * b[2] + wy * b[4]) + wz * b[5]);
             nh[12][i2] = (nh[12][i2] + f5) + 2.0 * ((wx * (b[6] + d12) + wy * (b[7] + d22)) + wz * (b[8] + d32));
         }
-        for (int i = 0; i < g.N; ++i)
-            for (int k = 0; k < 4; ++k) g.diss[1 + k][i] = g.diss[1 + k][i] - nh[9 + k][i];
+        for_nodes(g.N, [&](int i) { for (int k = 0; k < 4; ++k) g.diss[1 + k][i] = g.diss[1 + k][i] - nh[9 + k][i]; });
     }
 
     // ---- computeGradient, Galerkin (def_par:2923-3245) --------------------
     void computeGradient(Level &g, vec *u) {
         for (int k = 0; k < 15; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double w[3] = {g.wx[e], g.wy[e], g.wz[e]};
             double r1 = u[0][i1], q1[5] = {r1, u[1][i1] / r1, u[2][i1] / r1, u[3][i1] / r1, u[4][i1]};
@@ -349,8 +437,8 @@ struct Oracle {
                     nh[a * 5 + k][i1] = nh[a * 5 + k][i1] + dq;
                     nh[a * 5 + k][i2] = nh[a * 5 + k][i2] - dq;
                 }
-        }
-        for (int b = 0; b < g.B; ++b) {
+        });
+        for_bedges(g, [&](int b) {
             int i1 = g.b1[b], i2 = g.b2[b];
             double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
             double r1 = u[0][i1], q1[5] = {r1, u[1][i1] / r1, u[2][i1] / r1, u[3][i1] / r1, u[4][i1]};
@@ -365,7 +453,7 @@ struct Oracle {
                     double s = q1[k] + q2[k];
                     nh[a * 5 + k][i2] = nh[a * 5 + k][i2] + (2. * q2[k] + s) * w[a];
                 }
-        }
+        });
         for (int i = 0; i < g.N; ++i) {
             double vt = 1. / g.V[i];
             for (int k = 0; k < 15; ++k) nh[k][i] = nh[k][i] * vt;
@@ -395,7 +483,7 @@ struct Oracle {
     }
     void computegradhat(Level &g, const vec &q) {
         for (int k = 0; k < 9; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double dx = g.cx[i2] - g.cx[i1], dy = g.cy[i2] - g.cy[i1], dz = g.cz[i2] - g.cz[i1];
             double dist1 = 1. / ((dx * dx + dy * dy) + dz * dz);
@@ -407,8 +495,8 @@ struct Oracle {
             double b[3] = {dr2 * dx * dist1, dr2 * dy * dist1, dr2 * dz * dist1};
             for (int k = 0; k < 3; ++k) nh[6 + k][i1] = nh[6 + k][i1] + b[k];
             for (int k = 0; k < 3; ++k) nh[6 + k][i2] = nh[6 + k][i2] + b[k];
-        }
-        for (int i = 0; i < g.N; ++i) {
+        });
+        for_nodes(g.N, [&](int i) {
             double a11 = nh[0][i], a12 = nh[1][i], a13 = nh[2][i];
             double a21 = nh[1][i], a22 = nh[3][i], a23 = nh[4][i];
             double a31 = nh[2][i], a32 = nh[4][i], a33 = nh[5][i];
@@ -423,13 +511,13 @@ struct Oracle {
             nh[9][i] = (c11 * b1 + c12 * b2) + c13 * b3;
             nh[10][i] = (c21 * b1 + c22 * b2) + c23 * b3;
             nh[11][i] = (c31 * b1 + c32 * b2) + c33 * b3;
-        }
+        });
     }
 
     // ---- LocalMinMax (def_par:3248-3459) ----------------------------------
     void LocalMinMax(Level &g) {
         for (int k = 15; k < 25; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 1.0e15);
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double r1 = g.u[0][i1], q1[5] = {r1, g.u[1][i1] / r1, g.u[2][i1] / r1, g.u[3][i1] / r1, g.u[4][i1]};
             double r2 = g.u[0][i2], q2[5] = {r2, g.u[1][i2] / r2, g.u[2][i2] / r2, g.u[3][i2] / r2, g.u[4][i2]};
@@ -439,13 +527,13 @@ struct Oracle {
             for (int k = 0; k < 5; ++k) nh[15 + k][i2] = std::min(nh[15 + k][i2], mn[k]);
             for (int k = 0; k < 5; ++k) nh[20 + k][i1] = std::min(nh[20 + k][i1], mx[k]);
             for (int k = 0; k < 5; ++k) nh[20 + k][i2] = std::min(nh[20 + k][i2], mx[k]);
-        }
-        for (int i = 0; i < g.N; ++i) {
+        });
+        for_nodes(g.N, [&](int i) {
             double r = g.u[0][i];
             double q[5] = {r, g.u[1][i] / r, g.u[2][i] / r, g.u[3][i] / r, g.u[4][i]};
             for (int k = 0; k < 5; ++k) nh[15 + k][i] = nh[15 + k][i] - q[k];
             for (int k = 0; k < 5; ++k) nh[20 + k][i] = -nh[20 + k][i] - q[k];
-        }
+        });
     }
 
     // LED limiter branch of the HLLC reconstruction (def_par:1856-1867)
@@ -486,7 +574,7 @@ struct Oracle {
                 if (autoClip == 1) LocalMinMax(g);
             }
         }
-        for (int e = 0; e < g.E; ++e) {
+        for_edges(g, [&](int e) {
             const int i1 = g.s1[e], i2 = g.s2[e];
             double pr1 = g.p[i1], r1 = g.u[0][i1], rinv1 = 1. / g.u[0][i1];
             double ru1 = g.u[1][i1], rv1 = g.u[2][i1], rw1 = g.u[3][i1];
@@ -681,16 +769,16 @@ struct Oracle {
                 g.rhs[k][i1] = g.rhs[k][i1] + f[k];
                 g.rhs[k][i2] = g.rhs[k][i2] - f[k];
             }
-        }
+        });
         // boundary faces (def_par:2116-2512); the GCL terms vanish for the
         // static meshes this path accepts
-        for (int b = 0; b < g.B; ++b) {
+        for_bedges(g, [&](int b) {
             const int i1 = g.b1[b], i2 = g.b2[b], ind = g.bind[b];
             double g1[5], g2[5];
             boundary_flux(g, i1, i2, ind, g.bwx[b], g.bwy[b], g.bwz[b], g1, g2);
             for (int k = 0; k < 5; ++k) g.rhs[k][i1] = g.rhs[k][i1] + g1[k];
             for (int k = 0; k < 5; ++k) g.rhs[k][i2] = g.rhs[k][i2] + g2[k];
-        }
+        });
     }
 
     // contributions of one boundary edge to its two nodes
@@ -800,10 +888,10 @@ struct Oracle {
 
     // ---- solveSystem (def_par:1407-1479) ----------------------------------
     void solveSystem(Level &g, vec *rhs) {
-        for (int i = 0; i < g.N; ++i) {
+        for_nodes(g.N, [&](int i) {
             double dt = g.dt[i];
             for (int k = 0; k < 5; ++k) rhs[k][i] = dt * rhs[k][i] / g.V[i];
-        }
+        });
     }
 
     double relaxation_param(const Level &g) const {
@@ -843,8 +931,8 @@ struct Oracle {
     void updateSolutionVector(Level &g, vec *u, vec *uprev, vec *delu, int rk) {
         double dtJ = rk > 0 ? c.CFLNumber * RK[rk - 1] : c.CFLNumber;
         for (int k = 0; k < 5; ++k)
-            for (int i = 0; i < g.N; ++i) delu[k][i] = dtJ * delu[k][i];
-        for (int i = 0; i < g.N; ++i) {
+            for_nodes(g.N, [&](int i) { delu[k][i] = dtJ * delu[k][i]; });
+        for_nodes(g.N, [&](int i) {
             double inc = delu[0][i];
             if (std::fabs(inc / uprev[0][i]) < c.maxIncrementFactor) {
                 u[0][i] = uprev[0][i] - inc;
@@ -853,9 +941,8 @@ struct Oracle {
                 u[0][i] = uprev[0][i] - sign * c.maxIncrementFactor * uprev[0][i];
             }
             for (int k = 1; k < 5; ++k) u[k][i] = uprev[k][i] - delu[k][i];
-        }
-        for (int i = 0; i < g.N; ++i)
-            if (g.u[0][i] < c.minimumDensity) g.u[0][i] = c.minimumDensity;
+        });
+        for_nodes(g.N, [&](int i) { if (g.u[0][i] < c.minimumDensity) g.u[0][i] = c.minimumDensity; });
     }
 
     // ---- setBCsOnSolutionField (def_par:4364-4976), static walls ----------
@@ -907,7 +994,7 @@ struct Oracle {
     }
 
     void limitDensity(Level &g) {
-        for (int i = 0; i < g.N; ++i) g.u[0][i] = std::max(g.u[0][i], c.minimumDensity);
+        for_nodes(g.N, [&](int i) { g.u[0][i] = std::max(g.u[0][i], c.minimumDensity); });
     }
 
     void dissipation_for(Level &g, bool in_restrict_fine) {
@@ -920,7 +1007,7 @@ struct Oracle {
     void singleIteration(Level &g, bool calcDiss) {
         if (calcDiss) {
             makePressureField(g, g.u);
-            for (int i = 0; i < g.N; ++i) g.p[i] = std::fabs(g.p[i]);
+            for_nodes(g.N, [&](int i) { g.p[i] = std::fabs(g.p[i]); });
             makeTimeSteps(g);
             dissipation_for(g, false);
             if (c.ReynoldsNumber > 0.0) makeViscosityTerm(g);
@@ -930,7 +1017,7 @@ struct Oracle {
             for (int k = 0; k < 5; ++k) std::fill(g.rhs[k].begin(), g.rhs[k].end(), 0.0);
             makeRHS(g);
             for (int k = 0; k < 5; ++k)
-                for (int i = 0; i < g.N; ++i) g.rhs[k][i] = g.rhs[k][i] + g.diss[k][i];
+                for_nodes(g.N, [&](int i) { g.rhs[k][i] = g.rhs[k][i] + g.diss[k][i]; });
             solveSystem(g, g.rhs);
             setBCsOnIncrementField(g, g.rhs);
             // nullifyOuterBoundary: no-op for turbulenceModel 0
@@ -938,7 +1025,7 @@ struct Oracle {
             setBCsOnSolutionField(g, g.u);
             if (g.grid > 1)
                 for (int k = 0; k < 5; ++k)
-                    for (int i = 0; i < g.N; ++i) g.u[k][i] = g.u[k][i] - RK[st - 1] * g.src[k][i];
+                    for_nodes(g.N, [&](int i) { g.u[k][i] = g.u[k][i] - RK[st - 1] * g.src[k][i]; });
             limitDensity(g);
             setOuterBoundaryConditions(g, g.u, g.p);
         }
@@ -1211,6 +1298,60 @@ int check_controls(const flite_controls &c) {
     return FLITE_OK;
 }
 
+
+// ---- tangent of the edge residual (central flux + boundary fluxes) -------
+// forward-mode dual numbers; the CPU reference for the GPU adjoint product
+struct Dl {
+    double v, d;
+    Dl(double a = 0, double b = 0) : v(a), d(b) {}
+};
+inline Dl operator+(Dl a, Dl b) { return {a.v + b.v, a.d + b.d}; }
+inline Dl operator-(Dl a, Dl b) { return {a.v - b.v, a.d - b.d}; }
+inline Dl operator-(Dl a) { return {-a.v, -a.d}; }
+inline Dl operator*(Dl a, Dl b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dl operator/(Dl a, Dl b) { double q = a.v / b.v; return {q, (a.d - q * b.d) / b.v}; }
+inline Dl dsqrt(Dl a) { double s = std::sqrt(a.v); return {s, s > 0 ? 0.5 * a.d / s : 0.0}; }
+inline Dl dabs(Dl a) { return a.v < 0 ? -a : a; }
+
+Dl tan_pressure(const flite_controls &c, const Dl *u) {
+    Dl p = Dl(c.gamma - 1.0) * (u[4] - Dl(0.5) * ((u[1] * u[1] + u[2] * u[2]) + u[3] * u[3]) / u[0]);
+    return p.v < 0.1 ? Dl(0.1) : p;
+}
+// one-sided flux G(u; w) = F(u).w
+void tan_G(const Dl *u, Dl p, const double *w, Dl *G) {
+    Dl mw = (u[1] * w[0] + u[2] * w[1]) + u[3] * w[2];
+    G[0] = mw;
+    for (int c = 0; c < 3; ++c) G[1 + c] = u[1 + c] * mw / u[0] + p * w[c];
+    G[4] = (u[4] + p) * mw / u[0];
+}
+void tan_farfield(const flite_controls &c, const Dl *q, Dl pr, const double *n, const double *inf, Dl *F) {
+    const double gam1 = c.gamma - 1.0;
+    double ro = inf[0], ro1 = 1. / ro, uo = inf[1], vo = inf[2], wo = inf[3], eo = inf[4], po = inf[5];
+    Dl rhol = q[0], rinvl = Dl(1.0) / rhol, rhl = q[4] + pr;
+    Dl ul = q[1] * rinvl, vl = q[2] * rinvl, wl = q[3] * rinvl, epsl = q[4], hl = rhl * rinvl;
+    Dl nvl = (ul * n[0] + vl * n[1]) + wl * n[2];
+    Dl fl[5] = {rhol * nvl, pr * n[0] + rhol * ul * nvl, pr * n[1] + rhol * vl * nvl,
+                pr * n[2] + rhol * wl * nvl, rhl * nvl};
+    double rhor = ro, epsr = eo * ro, hr = eo + po * ro1;
+    double unr = (uo * n[0] + vo * n[1]) + wo * n[2];
+    double fr[5] = {rhor * unr, n[0] * po + rhor * uo * unr, n[1] * po + rhor * vo * unr,
+                    n[2] * po + rhor * wo * unr, (epsr + po) * unr};
+    Dl di = dsqrt(Dl(rhor) / rhol), d1 = Dl(1.0) / (di + Dl(1.0));
+    Dl ui = (di * uo + ul) * d1, vi = (di * vo + vl) * d1, wi = (di * wo + wl) * d1, hi = (di * hr + hl) * d1;
+    Dl ci2 = Dl(gam1) * (hi - Dl(0.5) * ((ui * ui + vi * vi) + wi * wi));
+    if (ci2.v < 1.0e-5) ci2 = Dl(1.0e-5);
+    Dl ci = dsqrt(ci2), af = Dl(0.5) * ((ui * ui + vi * vi) + wi * wi);
+    Dl ucp = (ui * n[0] + vi * n[1]) + wi * n[2];
+    Dl du[5] = {Dl(rhor) - rhol, Dl(rhor * uo) - rhol * ul, Dl(rhor * vo) - rhol * vl, Dl(rhor * wo) - rhol * wl,
+                Dl(epsr) - epsl};
+    Dl l1 = dabs(ucp + ci), l2 = dabs(ucp - ci), l3 = dabs(ucp);
+    Dl s1 = Dl(0.5) * (l1 + l2), s2 = Dl(0.5) * (l1 - l2);
+    Dl al1x = Dl(gam1) * ((((af * du[0] - ui * du[1]) - vi * du[2]) - wi * du[3]) + du[4]);
+    Dl al2x = ((-ucp * du[0] + du[1] * n[0]) + du[2] * n[1]) + du[3] * n[2];
+    Dl cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci), cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+    Dl ex[5] = {cc1, cc1 * ui + cc2 * n[0], cc1 * vi + cc2 * n[1], cc1 * wi + cc2 * n[2], cc1 * hi + cc2 * ucp};
+    for (int k = 0; k < 5; ++k) F[k] = Dl(0.5) * (Dl(fr[k]) + fl[k]) - Dl(0.5) * (l3 * du[k] + ex[k]);
+}
 }  // namespace
 
 struct oracle_ctx {
@@ -1433,6 +1574,12 @@ int oracle_forces(oracle_ctx *o, double out[6]) {
     return FLITE_OK;
 }
 
+int oracle_set_threads(int n) {
+    if (n < 1) return FLITE_EINVAL;
+    g_threads = n;
+    return FLITE_OK;
+}
+
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r) {
     Level *g = lvl(o, level);
     if (!g || !u || !r) return FLITE_EINVAL;
@@ -1452,6 +1599,61 @@ int oracle_eval_dissipation(oracle_ctx *o, int level) {
     o->o.makeTimeSteps(*g);
     o->o.dissipation_for(*g, false);
     if (o->o.c.ReynoldsNumber > 0.0) o->o.makeViscosityTerm(*g);
+    return FLITE_OK;
+}
+
+
+// tangent J du of the residual of oracle_residual_fwd (central flux, wall,
+// symmetry and far-field boundary fluxes)
+int oracle_residual_jvp(oracle_ctx *o, int level, const double *u, const double *du, double *jv) {
+    Level *g = lvl(o, level);
+    if (!g || !u || !du || !jv) return FLITE_EINVAL;
+    const flite_controls &c = o->o.c;
+    if (c.fluxType != 1) return FLITE_EUNSUPPORTED;
+    const size_t N = g->N;
+    std::vector<Dl> acc(5 * N);
+    auto state = [&](int i, Dl *q) { for (int k = 0; k < 5; ++k) q[k] = Dl(u[k * N + i], du[k * N + i]); };
+    for (int e = 0; e < g->E; ++e) {
+        int i1 = g->s1[e], i2 = g->s2[e];
+        double w[3] = {g->wx[e], g->wy[e], g->wz[e]};
+        Dl q1[5], q2[5], G1[5], G2[5];
+        state(i1, q1); state(i2, q2);
+        tan_G(q1, tan_pressure(c, q1), w, G1);
+        tan_G(q2, tan_pressure(c, q2), w, G2);
+        for (int k = 0; k < 5; ++k) {
+            Dl f = G1[k] + G2[k];
+            acc[k * N + i1] = acc[k * N + i1] + f;
+            acc[k * N + i2] = acc[k * N + i2] - f;
+        }
+    }
+    const bool fe = c.boundaryTerm == 1;
+    for (int b = 0; b < g->B; ++b) {
+        int i1 = g->b1[b], i2 = g->b2[b], ind = g->bind[b];
+        double w[3] = {g->bwx[b], g->bwy[b], g->bwz[b]};
+        double rn = std::sqrt((w[0] * w[0] + w[1] * w[1]) + w[2] * w[2]);
+        if (!(rn > 1.0e-10)) continue;
+        Dl q1[5], q2[5], F1[5], F2[5];
+        state(i1, q1); state(i2, q2);
+        if (ind <= 2 || ind == 9) {
+            tan_G(q1, tan_pressure(c, q1), w, F1);
+            tan_G(q2, tan_pressure(c, q2), w, F2);
+            for (int k = 0; k < 5; ++k) { F1[k] = F1[k] / Dl(rn); F2[k] = F2[k] / Dl(rn); }
+        } else if (ind <= 4) {
+            double n[3] = {w[0] / rn, w[1] / rn, w[2] / rn};
+            const double *inf = &c.inflowField[(ind - 3) * 6];
+            tan_farfield(c, q1, tan_pressure(c, q1), n, inf, F1);
+            tan_farfield(c, q2, tan_pressure(c, q2), n, inf, F2);
+        } else {
+            continue;
+        }
+        for (int k = 0; k < 5; ++k) {
+            Dl g1 = fe ? Dl(rn) * (Dl(3.) * F1[k] + F2[k]) : Dl(rn) * Dl(4.) * F1[k];
+            Dl g2 = fe ? Dl(rn) * (F1[k] + Dl(3.) * F2[k]) : Dl(rn) * Dl(4.) * F2[k];
+            acc[k * N + i1] = acc[k * N + i1] + g1;
+            acc[k * N + i2] = acc[k * N + i2] + g2;
+        }
+    }
+    for (size_t k = 0; k < 5 * N; ++k) jv[k] = acc[k].d;
     return FLITE_OK;
 }
 

@@ -41,6 +41,10 @@ int oracle_forces(oracle_ctx *o, double out[6]);
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);
 /* one makeTimeSteps + dissipation evaluation at the level's current state */
 int oracle_eval_dissipation(oracle_ctx *o, int level);
+/* threads of the timing mode (default 1 = the reference's loop order)  */
+int oracle_set_threads(int n);
+/* tangent (forward-mode) of the residual: jv = (dR/du) du               */
+int oracle_residual_jvp(oracle_ctx *o, int level, const double *u, const double *du, double *jv);
 #ifdef __cplusplus
 }
 #endif

@@ -1,15 +1,20 @@
 """Mixed precision (FLITE_MIXED) against the FP64 CPU restatement.
 
-FLITE_MIXED computes the interior edge fluxes in FP32 from FP32 shadows of
-the state into an FP32 edge buffer, sums them per node with compensated
-(TwoSum) FP32 accumulation, and keeps FP64 for the conserved-variable update,
-the boundary-edge (wall and far-field characteristic) fluxes, the dissipation,
-the time steps and the residual norms.  Stated error bounds against FP64:
+FLITE_MIXED evaluates the interior central fluxes in FP32 as increments over
+an FP64 anchor state (the state at the first stage of each relaxation step,
+whose interior-edge residual is summed in FP64), and keeps FP64 for the
+conserved-variable update, the boundary-edge (wall and far-field
+characteristic) fluxes, the dissipation, the time steps and the residual
+norms.  Its rounding error is relative to the increment, not to the flux, so
+the iteration converges to the FP64 fixed point.  Stated error bounds:
 
-* one residual evaluation: |r_mixed - r_fp64| <= 2e-5 * max|r| per component;
+* one residual evaluation at u1 anchored at u0: |r_mixed - r_fp64| <=
+  1e-5 * max|r_fp64(u1) - r_fp64(u0)| per component, for a 5 % and for a
+  1e-7 increment;
 * state after 5 cycles: relative difference <= 1e-6;
-* converged (res1 reduced 1e-8) lift and drag: within 1e-6 relative (or 1e-9
-  absolute for a coefficient near zero) of the FP64 result.
+* res1 reduced by 1e-8 within 1.2x the FP64 cycle count; lift and drag there
+  within 1e-6 relative (or 1e-9 absolute for a coefficient near zero) of the
+  FP64 result.
 """
 import numpy as np
 import pytest
@@ -28,13 +33,18 @@ def pair(mesh, **ctl):
     return c64, Solver(c32, mesh), Solver(c64, mesh, backend=oracle_backend())
 
 
-def test_mixed_residual_error_bound():
+@pytest.mark.parametrize("size", [0.05, 1e-7])
+def test_mixed_residual_error_is_relative_to_the_increment(size):
     mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
     c, m, o = pair(mesh)
-    u = initial_state(c, mesh, perturb_seed=9, amplitude=0.05)
-    rm, ro = m.residual_fwd(u), o.residual_fwd(u)
-    scale = np.abs(ro).max(axis=1, keepdims=True)
-    assert np.all(np.abs(rm - ro) <= 2e-5 * scale)
+    u0 = initial_state(c, mesh, perturb_seed=9, amplitude=0.05)
+    rng = np.random.default_rng(4)
+    u1 = u0 * (1.0 + size * rng.uniform(-1.0, 1.0, u0.shape))
+    m.set_state(u0)
+    rm = m.residual_fwd(u1)
+    ro1, ro0 = o.residual_fwd(u1), o.residual_fwd(u0)
+    scale = np.abs(ro1 - ro0).max(axis=1, keepdims=True)
+    assert np.all(np.abs(rm - ro1) <= 1e-5 * scale)
 
 
 @pytest.mark.parametrize("ctl", [dict(), dict(ReynoldsNumber=5000.0, wallsAreIsentropic=1)])
@@ -71,5 +81,6 @@ def test_mixed_converged_forces_within_1e6():
         assert r < 1e-8 * r0, f"precision {c.precision} did not converge: {r / r0:.3e}"
         out.append((cyc, s.forces()))
     (n64, f64), (n32, f32) = out
+    assert n32 <= 1.2 * n64, (n32, n64)
     for k in (0, 1):
         assert abs(f32[k] - f64[k]) <= max(1e-6 * abs(f64[k]), 1e-9), (k, f32[k], f64[k])
