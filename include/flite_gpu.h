@@ -219,6 +219,25 @@ int flite_batch_autotune(flite_batch *b, int cycle_no, int reps, int32_t *edge_b
                          int32_t *node_block, double *best_ms);
 int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_block);
 
+/* ---- residual evaluation that allocates nothing ------------------------
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc (device memory owned by another allocator or by the host
+ * program, or code where allocation is not allowed).  Computes the residual
+ * of flite_residual_fwd for the central flux (fluxType 1) with its boundary
+ * faces, from caller-owned DEVICE arrays in the reference layout: side_idx
+ * [2][E] and bnd_idx [3][B] 1-based, side_w [3][E], bnd_w [3][B], u [5][N];
+ * writes rhs [5][N].  Scratch lives in one static device array of the
+ * library (24,380,160 bytes on every GPU that loads it); limits N <= 65536,
+ * E <= 262144, B <= 65536, larger sizes return FLITE_EINVAL, as does an
+ * index outside 1..N.  The first call on a device looks the scratch up for
+ * that device and should come before any stream capture.  Calls share the
+ * scratch: calls that overlap on the GPU race.  The call runs on `stream`
+ * (a cudaStream_t, NULL for the default stream) and synchronises it.      */
+int flite_residual_noalloc(const flite_controls *c, int32_t n_nodes, int32_t n_sides,
+                           int32_t n_bsides, const int32_t *d_side_idx, const double *d_side_w,
+                           const int32_t *d_bnd_idx, const double *d_bnd_w, const double *d_u,
+                           double *d_rhs, void *stream);
+
 /* ---- timing ----------------------------------------------------------- */
 /* Capture one oneCycle as a CUDA graph and replay it `ncycles` times;
  * returns the device time (ms) measured with CUDA events on the context's
