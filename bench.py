@@ -112,21 +112,28 @@ def build_case():
     return F, mesh, c, u0, time.time() - t0
 
 
-def edge_kernel_bytes(mesh):
-    """Algorithmic bytes of one edge-flux launch on level 1: per edge the two
-    node indices (8 B), the edge coefficients (24 B) and the flux written to
-    the edge buffer (40 B); per node the state and pressure read once (48 B)."""
+def node_kernel_bytes(mesh):
+    """Algorithmic bytes of one launch of the dominant kernel on level 1: the
+    node kernel that computes the central fluxes of every incident edge and
+    applies the RK stage update (measured in restrictGrid's fine-increment
+    mode, which has the stage's read set).  Per node: the 64-byte state
+    record (own and neighbours' reads of one array, counted once), uprev
+    (40 B), dissipation (40 B), dt and volume (16 B), u(rho) (8 B), boundary
+    class (1 B), two CSR offsets (8 B) and the result (40 B); per interior
+    edge its two 8-byte incidence entries and its 32-byte coefficient record;
+    per boundary edge two incidence entries and two 40-byte contributions; per
+    boundary node its normal (24 B)."""
     d = mesh.level(1)
-    return d.n_sides * (8 + 24 + 40) + d.n_nodes * 48
+    return d.n_nodes * (64 + 40 + 40 + 16 + 8 + 1 + 8 + 40) + d.n_sides * 48 + d.n_bsides * 88 \
+        + d.n_bnodes * 24
 
 
-def gather_kernel_bytes(mesh):
-    """Algorithmic bytes of one node residual gather (RESID mode) on level 1:
-    per edge two incidence records (16 B) and two flux reads (80 B), per
-    boundary edge two records and two reads (8 + 80 B), per node the CSR
-    offsets (8 B) and the residual written (40 B)."""
-    d = mesh.level(1)
-    return d.n_sides * (16 + 80) + d.n_bsides * (8 + 80) + d.n_nodes * (8 + 40)
+# DRAM traffic of the dominant kernel per algorithmic byte, from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
+# 192x64x64 bump channel (469.5 MB measured against 461.8 MB algorithmic);
+# the bench mesh is too large to capture with --set full, and the traffic
+# scales with the nodes and edges processed
+NCU_TRAFFIC_PER_ALGORITHMIC_BYTE = 469.521408 / 461.847625
 
 
 def run_ours(args):
@@ -157,14 +164,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     value, ms_max = replicas.replica_rate(ms, args.steps)
 
-    # kernel-level timing of the dominant edge kernels on level 1
-    edge_ms, gather_ms = solver.profile_level(1, reps=20)
+    # kernel-level timing of the dominant kernel on level 1
+    _, node_ms = solver.profile_level(1, reps=20)
     # adjoint cost ratio: one adjoint product against one forward residual
     # evaluation on level 1 (same level, FP64)
     fwd_ms, vjp_ms = solver.profile_adjoint(1, reps=20)
     hbm, peak_kind = _peaks()
-    eb = edge_kernel_bytes(mesh)
-    achieved = eb / (edge_ms / 1e3) / 1e9
+    nbytes = node_kernel_bytes(mesh)
+    achieved = nbytes / (node_ms / 1e3) / 1e9
 
     # end to end through the public API with host buffers: per cycle the
     # level-1 state goes host->device from pinned memory, the cycle runs, and
@@ -209,9 +216,11 @@ def run_ours(args):
             solver_m.cycle(i)
         torch.cuda.synchronize()
         ms_m = solver_m.time_cycles(args.steps, cycle_no=args.warmup + 1)
+        delta_ms, node_m_ms = solver_m.profile_level(1, reps=20)
         solver_m.close()
         v_m, ms_m = replicas.replica_rate(ms_m, args.steps)
-        mixed = {"value": v_m, "unit": "cycles/s", "ms_per_step": ms_m / args.steps}
+        mixed = {"value": v_m, "unit": "cycles/s", "ms_per_step": ms_m / args.steps,
+                 "node_kernel_ms": node_m_ms, "increment_records_ms": delta_ms}
     ttc = None
     if args.converge:
         ttc = time_to_converge(F, mesh, c, u0, args.converge_max)
@@ -241,13 +250,15 @@ def run_ours(args):
                 "resident": {"value": args.steps / resident_s, "h2d_bytes_per_step": 4,
                              "d2h_bytes_per_step": 15 * 8 + 6 * 8}},
         "gpu_launches": int(launches_per_cycle * args.steps),
-        "roofline": {"kernel": "k_edge_flux (level 1)", "bound": "hbm",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+        "roofline": {"kernel": "k_node_update<GATHER_CENTRAL> (level 1: central fluxes of the "
+                               "incident edges computed in the node gather, fused with the RK "
+                               "stage update)",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
-                     "algorithmic_bytes": eb, "launch_ms": edge_ms,
-                     "traffic": None,
-                     "gather_kernel": {"launch_ms": gather_ms,
-                                       "achieved": gather_kernel_bytes(mesh) / (gather_ms / 1e3) / 1e9}},
+                     "algorithmic_bytes": nbytes, "launch_ms": node_ms,
+                     "traffic": nbytes * NCU_TRAFFIC_PER_ALGORITHMIC_BYTE,
+                     "traffic_source": "ncu capture of one launch on the 192x64x64 mesh, "
+                                       "scaled by the units processed"},
         "clocks": clk.summary(),
         "residual_after_warmup": float(res[0]),
         "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,

@@ -90,13 +90,14 @@ def build_gpu(force=False, verbose=False):
 def build_oracle(force=False, verbose=False):
     odir = os.path.join(ROOT, "oracle")
     src = [os.path.join(odir, "oracle.cpp")]
-    deps = src + [os.path.join(odir, "oracle.h")] + _sources(INC, {".h"})
+    sdir = os.path.join(ROOT, "flite3d_b200", "csrc", "solver")
+    deps = src + [os.path.join(odir, "oracle.h"), os.path.join(sdir, "pinned_math.h")] + _sources(INC, {".h"})
     outdir = os.path.join(odir, "_build")
     os.makedirs(outdir, exist_ok=True)
     out = os.path.join(outdir, "liboracle.so")
     if force or _stale(out, deps):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
-              "-fno-fast-math", f"-I{INC}", f"-I{odir}", *src, "-o", out], verbose)
+              "-fno-fast-math", f"-I{INC}", f"-I{odir}", f"-I{sdir}", *src, "-o", out], verbose)
     return out
 
 

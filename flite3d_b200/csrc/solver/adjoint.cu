@@ -279,7 +279,7 @@ extern "C" int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double
             CK(cudaEventRecord(e[0], X.s));
             X.pressure(l);
             X.rhs_terms(l);
-            k_node_update<GATHER_FP64><<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            X.launch_node_update(l, MODE_RESID, 0, true);
             CK(cudaEventRecord(e[1], X.s));
             CK(cudaEventRecord(e[2], X.s));
             X.vjp_kernels(l);

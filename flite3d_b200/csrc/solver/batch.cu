@@ -83,7 +83,7 @@ struct flite_batch {
             flite_ctx *c = cases[i];
             const LevelView &L = c->c.multigridScheme > 0 ? c->V(0) : c->V((int)c->lv.size() - 1);
             k_resid_partial<<<kResidBlocks, 256, 0, s>>>(L, c->d_part, kResidBlocks);
-            k_resid_final<<<1, 1, 0, s>>>(c->d_part, kResidBlocks, c->d_out);
+            k_resid_final<<<1, 160, 0, s>>>(c->d_part, kResidBlocks, c->d_out);
             CK(cudaMemcpyAsync(h_res + i, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, s));
         }
         CK(cudaStreamSynchronize(s));

@@ -159,8 +159,14 @@ struct flite_ctx {
             }
         }
         if (L.E > 0) {
-            counted();
-            edge_flux_launch(L, anchor);
+            if (mixed() && !anchor) {
+                // FP32 records of the increments over the anchor
+                counted();
+                k_delta_state<<<nblk(L.N), nb, 0, s>>>(L);
+            } else if (!fused()) {
+                counted();
+                edge_flux_launch(L);
+            }
         }
         if (L.B > 0) {
             counted();
@@ -168,32 +174,37 @@ struct flite_ctx {
         }
     }
     bool mixed() const { return c.precision == FLITE_MIXED; }
+    // the central flux (and FLITE_MIXED, which only takes it) is computed
+    // inside the node gather; the upwind fluxes go through the edge buffer
+    bool fused() const { return c.fluxType == 1; }
     // the flux kernel instance of this run's fluxType (and HLLC order; the
     // reconstruction only acts on level 1, where coordinates exist)
-    void edge_flux_launch(const LevelView &L, bool anchor = true) {
+    void edge_flux_launch(const LevelView &L) {
         const unsigned ng = eblk(L.E);
-        if (mixed() && !anchor) {
-            // FP32 flux increments over the anchor (central flux)
-            k_delta_state<<<nblk(L.N), nb, 0, s>>>(L);
-            counted();
-            k_edge_flux_f32_delta<<<ng, eb, 0, s>>>(L);
-            return;
-        }
         switch (c.fluxType) {
-            case 1: k_edge_flux<1, false><<<ng, eb, 0, s>>>(P, L); break;
             case 2: k_edge_flux<2, false><<<ng, eb, 0, s>>>(P, L); break;
             case 3: k_edge_flux<3, false><<<ng, eb, 0, s>>>(P, L); break;
-            default:
+            case 4:
                 if (c.HLLCFluxOrder > 1) k_edge_flux<4, true><<<ng, eb, 0, s>>>(P, L);
                 else k_edge_flux<4, false><<<ng, eb, 0, s>>>(P, L);
+                break;
+            default: k_edge_flux<1, false><<<ng, eb, 0, s>>>(P, L);
         }
     }
     void node_update(int l, int mode, int stage, bool anchor = true) {
         counted();
+        launch_node_update(l, mode, stage, anchor);
+    }
+    void launch_node_update(int l, int mode, int stage, bool anchor) {
         const unsigned g = nblk(V(l).N);
-        if (!mixed()) k_node_update<GATHER_FP64><<<g, nb, 0, s>>>(P, V(l), mode, stage);
-        else if (anchor) k_node_update<GATHER_ANCHOR><<<g, nb, 0, s>>>(P, V(l), mode, stage);
-        else k_node_update<GATHER_DELTA><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+        if (mixed()) {
+            if (anchor) k_node_update<GATHER_ANCHOR><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            else k_node_update<GATHER_DELTA><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+        } else if (fused()) {
+            k_node_update<GATHER_CENTRAL><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+        } else {
+            k_node_update<GATHER_BUFFER><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+        }
     }
 
     // ---- singleIteration (def_par:1002-1181) -----------------------------

@@ -20,6 +20,25 @@ struct Params {
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
 };
 
+// Records gathered by node kernels from a node's incident edges and from its
+// neighbours.  Each is a multiple of 16 bytes and read with 16-byte loads,
+// so that a neighbour costs one or two 32-byte sectors instead of one sector
+// per component of an SoA array.
+struct __align__(16) EdgeW {  // coefficients of an edge (32 B)
+    double wx, wy, wz, pad;
+};
+struct __align__(16) IncRec32 {  // the same in FP32 (16 B); j is ~j when this
+    float wx, wy, wz;            // node is the edge's second node
+    int j;
+};
+struct __align__(16) NodeRec {  // conserved state, pressure, viscosity (64 B)
+    double r, ru, rv, rw, E, p, mu, pad;
+};
+struct __align__(16) DeltaRec {  // FP32 anchor primitives and increments (48 B)
+    float ra, vax, vay, vaz, ha;  // anchor rho, velocity, E + p
+    float dr, dmx, dmy, dmz, dE, dp, pad;  // u - ua and p - pa
+};
+
 // A level's mesh and state on the device.  Node-indexed arrays are SoA
 // ([component][node]), like the reference's column-major u(N,nvar).
 struct LevelView {
@@ -34,6 +53,7 @@ struct LevelView {
     // negative entry ~e marks the node as the second node of edge e
     const int *inc_ptr;
     const int2 *inc;
+    const EdgeW *ew;             // [E] the edge coefficients as one record
     // node -> incident boundary edges in boundary-edge order: 2*b + side
     const int *binc_ptr;
     const int *binc;
@@ -50,11 +70,12 @@ struct LevelView {
     // state
     double *u, *uprev, *rhs, *src, *diss;  // [5][N]
     double *p, *dt, *mu;                   // [N]
+    double *hvis;                          // [N]  viscous time-step term
     double *lap;                           // [5][N] undivided Laplacian
     double *sens;                          // [N]  pressure sensor
-    double *hvis;                          // [N]  viscous time-step term
     double *tau;                           // [9][N] stress tensor + heat flux
     double *prim;                          // [4][N] u, v, w, T of the viscous term
+    NodeRec *q;                            // [N] written with p by k_pressure
     double *vdt;                           // [N]  V/dt of the dissipation
     double *wstress;                       // [3][N] wall stress (level 1)
     double *grad;                          // [15][N] (level 1, HLLC order 2)
@@ -64,12 +85,52 @@ struct LevelView {
     // increments over an FP64 anchor state
     double *ua, *ra, *pa;                  // anchor u [5][N], its interior-edge residual [5][N], p [N]
     float *a32;                            // [5][N] anchor rho, u, v, w, E+p
-    float *d32;                            // [6][N] u - ua (5) and p - pa
-    const float *wx32, *wy32, *wz32;       // [E]
-    float *flux32;                         // [E][5] flux increments
+    DeltaRec *dq;                          // [N] anchor primitives and increments
+    const IncRec32 *inc32;                 // [2E] incidences in FP32
     double *bflux;                         // [B][10] boundary-edge contributions
     int *cyc;                              // cycle number of this level
 };
+
+__device__ __forceinline__ EdgeW load_edgew(const EdgeW *w, int e) {
+    const double2 *p = reinterpret_cast<const double2 *>(w + e);
+    const double2 a = __ldg(p), b = __ldg(p + 1);
+    EdgeW o;
+    o.wx = a.x; o.wy = a.y; o.wz = b.x; o.pad = b.y;
+    return o;
+}
+__device__ __forceinline__ IncRec32 load_inc32(const IncRec32 *r, int k) {
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(r + k));
+    IncRec32 o;
+    o.wx = a.x; o.wy = a.y; o.wz = a.z; o.j = __float_as_int(a.w);
+    return o;
+}
+
+// 16-byte loads (read-only path) and stores of the node records
+template <class R, int K>
+__device__ __forceinline__ R load_rec(const R *base, int j) {
+    static_assert(sizeof(R) == 16 * K, "record size");
+    const double2 *p = reinterpret_cast<const double2 *>(base + j);
+    R o;
+    double2 *d = reinterpret_cast<double2 *>(&o);
+#pragma unroll
+    for (int k = 0; k < K; ++k) d[k] = __ldg(p + k);
+    return o;
+}
+template <class R, int K>
+__device__ __forceinline__ void store_rec(R *base, int j, const R &o) {
+    static_assert(sizeof(R) == 16 * K, "record size");
+    double2 *p = reinterpret_cast<double2 *>(base + j);
+    const double2 *d = reinterpret_cast<const double2 *>(&o);
+#pragma unroll
+    for (int k = 0; k < K; ++k) p[k] = d[k];
+}
+__device__ __forceinline__ NodeRec load_node(const NodeRec *q, int j) { return load_rec<NodeRec, 4>(q, j); }
+__device__ __forceinline__ void store_node(NodeRec *q, int j, double r, double ru, double rv, double rw, double E,
+                                           double p, double mu) {
+    NodeRec o;
+    o.r = r; o.ru = ru; o.rv = rv; o.rw = rw; o.E = E; o.p = p; o.mu = mu; o.pad = 0.0;
+    store_rec<NodeRec, 4>(q, j, o);
+}
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }

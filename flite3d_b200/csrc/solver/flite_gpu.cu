@@ -224,6 +224,12 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             L.bedge = X.upload(bedge); L.bind = X.upload(bind);
             L.bwx = X.upload(bwx); L.bwy = X.upload(bwy); L.bwz = X.upload(bwz);
             L.inc_ptr = X.upload(ip); L.inc = X.upload(inc);
+            {
+                std::vector<EdgeW> ew(std::max(E, 1));
+                for (int e = 0; e < E; ++e) ew[e] = EdgeW{wx[e], wy[e], wz[e], 0.0};
+                L.ew = X.upload(ew);
+            }
+            L.inc32 = nullptr;
             L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
             L.V = X.upload(std::vector<double>(d.volume, d.volume + N));
             L.conn = X.upload(conn);
@@ -257,44 +263,49 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             // state
             L.u = X.alloc<double>(5 * (size_t)N); L.uprev = X.alloc<double>(5 * (size_t)N);
             L.rhs = X.alloc<double>(5 * (size_t)N); L.src = X.alloc<double>(5 * (size_t)N);
-            L.diss = X.alloc<double>(5 * (size_t)N); L.lap = X.alloc<double>(5 * (size_t)N);
+            L.diss = X.alloc<double>(5 * (size_t)N);
             L.p = X.alloc<double>(N); L.dt = X.alloc<double>(N); L.mu = X.alloc<double>(N);
-            L.sens = X.alloc<double>(N); L.hvis = X.alloc<double>(N);
-            for (double *a : {L.u, L.uprev, L.rhs, L.src, L.diss, L.lap})
+            L.hvis = X.alloc<double>(N);
+            for (double *a : {L.u, L.uprev, L.rhs, L.src, L.diss})
                 CK(cudaMemset(a, 0, 5 * (size_t)N * sizeof(double)));
-            for (double *a : {L.p, L.dt, L.mu, L.sens, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
+            for (double *a : {L.p, L.dt, L.mu, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
             const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
             const bool visc = c->ReynoldsNumber > 0.0;
+            L.q = X.alloc<NodeRec>(N);
+            CK(cudaMemset(L.q, 0, (size_t)N * sizeof(NodeRec)));
             L.tau = visc ? X.alloc<double>(9 * (size_t)N) : nullptr;
             L.prim = visc ? X.alloc<double>(4 * (size_t)N) : nullptr;
+            L.lap = X.alloc<double>(5 * (size_t)N);
+            L.sens = X.alloc<double>(N);
             L.vdt = X.alloc<double>(N);
             L.wstress = X.alloc<double>(3 * (size_t)N);
             CK(cudaMemset(L.wstress, 0, 3 * (size_t)N * sizeof(double)));
             L.grad = hllc2 ? X.alloc<double>(15 * (size_t)N) : nullptr;
             L.bnd = hllc2 ? X.alloc<double>(10 * (size_t)N) : nullptr;
-            L.flux = X.alloc<double>(5 * (size_t)std::max(E, 1));
+            // the edge buffer carries the upwind fluxes; the central flux is
+            // computed inside the node gather
+            L.flux = c->fluxType != 1 ? X.alloc<double>(5 * (size_t)std::max(E, 1)) : nullptr;
             if (c->precision == FLITE_MIXED) {
                 L.ua = X.alloc<double>(5 * (size_t)N);
                 L.ra = X.alloc<double>(5 * (size_t)N);
                 L.pa = X.alloc<double>(N);
                 L.a32 = X.alloc<float>(5 * (size_t)N);
-                L.d32 = X.alloc<float>(6 * (size_t)N);
+                L.dq = X.alloc<DeltaRec>(N);
                 // a zero anchor makes the increments the full FP32 fluxes
                 // until the first FP64 evaluation
                 for (double *a : {L.ua, L.ra}) CK(cudaMemset(a, 0, 5 * (size_t)N * sizeof(double)));
                 CK(cudaMemset(L.pa, 0, (size_t)N * sizeof(double)));
                 CK(cudaMemset(L.a32, 0, 5 * (size_t)N * sizeof(float)));
-                if (!(donor && L.wx32)) {
-                    std::vector<float> w32(3 * (size_t)std::max(E, 1));
-                    for (size_t k = 0; k < 3 * (size_t)E; ++k) w32[k] = (float)d.side_w[k];
-                    float *dw = X.upload(w32);
-                    L.wx32 = dw; L.wy32 = dw + E; L.wz32 = dw + 2 * (size_t)E;
+                if (!L.inc32) {
+                    IncRec32 *d32 = X.alloc<IncRec32>(2 * (size_t)std::max(E, 1));
+                    if (E > 0) k_make_inc32<<<(unsigned)((2 * (size_t)E + 255) / 256), 256>>>(L.inc, L.ew, 2 * E, d32);
+                    CK(cudaGetLastError());
+                    L.inc32 = d32;
                 }
-                L.flux32 = X.alloc<float>(5 * (size_t)std::max(E, 1));
             } else {
                 L.ua = L.ra = L.pa = nullptr;
-                L.a32 = L.d32 = nullptr;
-                L.flux32 = nullptr;
+                L.a32 = nullptr;
+                L.dq = nullptr;
             }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
             L.cyc = X.d_cyc + l;
@@ -447,7 +458,7 @@ int flite_residuals(flite_ctx *ctx, double res[7], double maxres[7], int32_t max
         flite_ctx &X = *ctx;
         const LevelView &L = X.c.multigridScheme > 0 ? X.V(0) : X.V((int)X.lv.size() - 1);
         k_resid_partial<<<kResidBlocks, 256, 0, X.s>>>(L, X.d_part, kResidBlocks);
-        k_resid_final<<<1, 1, 0, X.s>>>(X.d_part, kResidBlocks, X.d_out);
+        k_resid_final<<<1, 160, 0, X.s>>>(X.d_part, kResidBlocks, X.d_out);
         double h[15];
         CK(cudaMemcpyAsync(h, X.d_out, sizeof h, cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
@@ -474,9 +485,10 @@ int flite_forces(flite_ctx *ctx, double out[6]) {
             for (int k = 0; k < 6; ++k) out[k] = 0.0;
             return FLITE_OK;
         }
-        k_forces<<<1, 256, 0, X.s>>>(X.P, D.v, D.d_wall, (int)D.wall.size(), X.c.alpha * PI / 180.,
-                                    X.c.beta * PI / 180., X.c.groundplane, X.c.datum[0], X.c.datum[1],
-                                    X.c.datum[2], X.d_out);
+        k_forces<<<kForceBlocks, 256, 0, X.s>>>(X.P, D.v, D.d_wall, (int)D.wall.size(), X.c.alpha * PI / 180.,
+                                               X.c.beta * PI / 180., X.c.groundplane, X.c.datum[0],
+                                               X.c.datum[1], X.c.datum[2], X.d_part);
+        k_forces_final<<<1, 32, 0, X.s>>>(X.d_part, kForceBlocks, X.d_out);
         double h[6];
         CK(cudaMemcpyAsync(h, X.d_out, sizeof h, cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
@@ -550,14 +562,17 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, do
         for (int r = 0; r < reps; ++r) {
             X.pressure(l);
             CK(cudaEventRecord(ev[0], X.s));
-            X.edge_flux_launch(L, false);
+            // the edge pass before the gather: the upwind-flux edge kernel,
+            // the increment records of FLITE_MIXED, or nothing for the FP64
+            // central flux (computed in the gather)
+            if (X.mixed()) k_delta_state<<<X.nblk(L.N), X.nb, 0, X.s>>>(L);
+            else if (!X.fused()) X.edge_flux_launch(L);
             CK(cudaEventRecord(ev[1], X.s));
-            if (L.B > 0) k_bnd_flux<<<flite_ctx::blocks(L.B), kBlock, 0, X.s>>>(X.P, L);
+            if (L.B > 0) k_bnd_flux<<<X.eblk(L.B), X.eb, 0, X.s>>>(X.P, L);
             CK(cudaEventRecord(ev[2], X.s));
-            if (X.mixed())
-                k_node_update<GATHER_DELTA><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
-            else
-                k_node_update<GATHER_FP64><<<flite_ctx::blocks(L.N), kBlock, 0, X.s>>>(X.P, L, MODE_RESID, 0);
+            // the node kernel with the whole read set of an RK stage
+            // (restrictGrid's fine increment: the result goes to rhs)
+            X.launch_node_update(l, MODE_RFINE, 0, false);
             CK(cudaEventRecord(ev[3], X.s));
             CK(cudaEventSynchronize(ev[3]));
             float a = 0, b = 0;

@@ -42,6 +42,24 @@ __device__ __forceinline__ double led(double a, double bmin, double bmax, int ns
     return cc;
 }
 
+// central flux of an edge from its two node states (def_par:1664-1669)
+__device__ __forceinline__ void central_flux(const NodeState &a, const NodeState &b, double wx, double wy,
+                                             double wz, double *f) {
+    double pr1 = a.p, rinv1 = 1. / a.r;
+    double ru1 = a.ru, rv1 = a.rv, rw1 = a.rw;
+    double u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1;
+    double rh1 = a.E + pr1;
+    double pr2 = b.p, rinv2 = 1. / b.r;
+    double ru2 = b.ru, rv2 = b.rv, rw2 = b.rw;
+    double u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2;
+    double rh2 = b.E + pr2;
+    f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
+    f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
+    f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
+    f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+    f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+}
+
 // Interior edge flux f of edge e (i1 -> i2), added to rhs(i1) and
 // subtracted from rhs(i2).  FT is the fluxType and O2 selects the HLLC
 // reconstruction; both are compile-time so that each kernel instance only
@@ -61,12 +79,8 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
     const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
     f[0] = f[1] = f[2] = f[3] = f[4] = 0.0;
     if constexpr (FT == 1 || FT == 4) {
-        // central flux (def_par:1664-1669); HLLC starts from it too (:1798)
-        f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
-        f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
-        f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
-        f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
-        f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+        // central flux; HLLC starts from it too (def_par:1798)
+        central_flux(a, b, wx, wy, wz, f);
         if constexpr (FT == 1) return;
     }
     if constexpr (FT == 2) {  // local Lax-Friedrichs (def_par:1670-1724)

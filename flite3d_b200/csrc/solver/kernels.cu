@@ -31,7 +31,10 @@ __global__ void k_pressure(Params P, LevelView L) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
-    L.p[i] = pressure(P, L.u[i], L.u[N + i], L.u[2 * N + i], L.u[3 * N + i], L.u[4 * N + i]);
+    const double r = L.u[i], ru = L.u[N + i], rv = L.u[2 * N + i], rw = L.u[3 * N + i], E = L.u[4 * N + i];
+    const double p = pressure(P, r, ru, rv, rw, E);
+    L.p[i] = p;
+    store_node(L.q, i, r, ru, rv, rw, E, p, L.mu[i]);
 }
 
 // ---- makeTimeSteps (def_par:13335-13610) as a node gather -----------------
@@ -505,44 +508,103 @@ __global__ void k_bnd_flux(Params P, LevelView L) {
 // FP64 evaluation at the first stage of every relaxation step (and at the
 // coarse-level evaluation of restrictGrid).
 
-// increments over the anchor: du (FP64 difference, rounded once) and dp
+// the node's record for the increments: anchor primitives and u - ua (FP64
+// difference, rounded once), p - pa
 __global__ void k_delta_state(LevelView L) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
-    for (int c = 0; c < 5; ++c) L.d32[c * N + i] = (float)(L.u[c * N + i] - L.ua[c * N + i]);
-    L.d32[5 * N + i] = (float)(L.p[i] - L.pa[i]);
+    DeltaRec o;
+    o.ra = L.a32[i]; o.vax = L.a32[N + i]; o.vay = L.a32[2 * N + i]; o.vaz = L.a32[3 * N + i];
+    o.ha = L.a32[4 * N + i];
+    o.dr = (float)(L.u[i] - L.ua[i]);
+    o.dmx = (float)(L.u[N + i] - L.ua[N + i]);
+    o.dmy = (float)(L.u[2 * N + i] - L.ua[2 * N + i]);
+    o.dmz = (float)(L.u[3 * N + i] - L.ua[3 * N + i]);
+    o.dE = (float)(L.u[4 * N + i] - L.ua[4 * N + i]);
+    o.dp = (float)(L.p[i] - L.pa[i]);
+    o.pad = 0.f;
+    float4 *p = reinterpret_cast<float4 *>(L.dq + i);
+    const float4 *d = reinterpret_cast<const float4 *>(&o);
+    p[0] = d[0]; p[1] = d[1]; p[2] = d[2];
+}
+
+// FP32 incidences of the increments (w rounded once; j is ~j when the node
+// is the edge's second node)
+__global__ void k_make_inc32(const int2 *inc, const EdgeW *ew, int n, IncRec32 *o) {
+    int k = tid();
+    if (k >= n) return;
+    const int2 t = inc[k];
+    const EdgeW w = ew[t.x >= 0 ? t.x : ~t.x];
+    o[k] = IncRec32{(float)w.wx, (float)w.wy, (float)w.wz, t.x >= 0 ? t.y : ~t.y};
+}
+
+__device__ __forceinline__ DeltaRec load_delta(const DeltaRec *q, int j) {
+    const float4 *p = reinterpret_cast<const float4 *>(q + j);
+    DeltaRec o;
+    float4 *d = reinterpret_cast<float4 *>(&o);
+    d[0] = __ldg(p); d[1] = __ldg(p + 1); d[2] = __ldg(p + 2);
+    return o;
 }
 
 // increment of the one-sided flux G(u; w) of one node
-__device__ __forceinline__ void delta_flux(const LevelView &L, int i, float wx, float wy, float wz, float *g) {
-    const int N = L.N;
-    const float ra = L.a32[i], vax = L.a32[N + i], vay = L.a32[2 * N + i], vaz = L.a32[3 * N + i];
-    const float ha = L.a32[4 * N + i];
-    const float dr = L.d32[i], dmx = L.d32[N + i], dmy = L.d32[2 * N + i], dmz = L.d32[3 * N + i];
-    const float dE = L.d32[4 * N + i], dp = L.d32[5 * N + i];
-    const float rinv = 1.f / (ra + dr);
-    const float dvx = (dmx - vax * dr) * rinv, dvy = (dmy - vay * dr) * rinv, dvz = (dmz - vaz * dr) * rinv;
-    const float vw = ((vax + dvx) * wx + (vay + dvy) * wy) + (vaz + dvz) * wz;
+__device__ __forceinline__ void delta_flux(const DeltaRec &n, float wx, float wy, float wz, float *g) {
+    const float rinv = 1.f / (n.ra + n.dr);
+    const float dvx = (n.dmx - n.vax * n.dr) * rinv, dvy = (n.dmy - n.vay * n.dr) * rinv;
+    const float dvz = (n.dmz - n.vaz * n.dr) * rinv;
+    const float vw = ((n.vax + dvx) * wx + (n.vay + dvy) * wy) + (n.vaz + dvz) * wz;
     const float dvw = (dvx * wx + dvy * wy) + dvz * wz;
-    g[0] = (dmx * wx + dmy * wy) + dmz * wz;
-    g[1] = (dmx * vw + (ra * vax) * dvw) + dp * wx;
-    g[2] = (dmy * vw + (ra * vay) * dvw) + dp * wy;
-    g[3] = (dmz * vw + (ra * vaz) * dvw) + dp * wz;
-    g[4] = (dE + dp) * vw + ha * dvw;
+    g[0] = (n.dmx * wx + n.dmy * wy) + n.dmz * wz;
+    g[1] = (n.dmx * vw + (n.ra * n.vax) * dvw) + n.dp * wx;
+    g[2] = (n.dmy * vw + (n.ra * n.vay) * dvw) + n.dp * wy;
+    g[3] = (n.dmz * vw + (n.ra * n.vaz) * dvw) + n.dp * wz;
+    g[4] = (n.dE + n.dp) * vw + n.ha * dvw;
 }
 
-// interior central-flux increments in FP32 into the FP32 edge buffer
-__global__ void __launch_bounds__(256) k_edge_flux_f32_delta(LevelView L) {
-    int e = tid();
-    if (e >= L.E) return;
-    const int2 nd = L.edge[e];
-    const float wx = L.wx32[e], wy = L.wy32[e], wz = L.wz32[e];
-    float g1[5], g2[5];
-    delta_flux(L, nd.x, wx, wy, wz, g1);
-    delta_flux(L, nd.y, wx, wy, wz, g2);
-    float *o = L.flux32 + (size_t)e * 5;
-    for (int c = 0; c < 5; ++c) o[c] = g1[c] + g2[c];
+// interior residual of node i as the anchor's FP64 sum plus the FP32 sum of
+// the flux increments of its edges
+__device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i, double *r) {
+    float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    const DeltaRec me = load_delta(L.dq, i);
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const IncRec32 t = load_inc32(L.inc32, k);
+        const bool first = t.j >= 0;
+        const DeltaRec nb = load_delta(L.dq, first ? t.j : ~t.j);
+        float g1[5], g2[5];
+        delta_flux(first ? me : nb, t.wx, t.wy, t.wz, g1);
+        delta_flux(first ? nb : me, t.wx, t.wy, t.wz, g2);
+        if (first) {
+            for (int c = 0; c < 5; ++c) acc[c] += g1[c] + g2[c];
+        } else {
+            for (int c = 0; c < 5; ++c) acc[c] -= g1[c] + g2[c];
+        }
+    }
+    const int N = L.N;
+    for (int c = 0; c < 5; ++c) r[c] = L.ra[c * N + i] + (double)acc[c];
+}
+
+// interior central fluxes of node i computed from the two node records of
+// each incident edge, summed in edge order: the same numbers, in the same
+// order, as the edge kernel followed by the buffer gather
+__device__ __forceinline__ void gather_interior_central(const LevelView &L, int i, double *r) {
+    r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
+    const NodeRec m = load_node(L.q, i);
+    const NodeState si{m.r, m.ru, m.rv, m.rw, m.E, m.p};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const int e = t.x >= 0 ? t.x : ~t.x;
+        const EdgeW w = load_edgew(L.ew, e);
+        const NodeRec n = load_node(L.q, t.y);
+        const NodeState sj{n.r, n.ru, n.rv, n.rw, n.E, n.p};
+        double f[5];
+        if (t.x >= 0) {
+            central_flux(si, sj, w.wx, w.wy, w.wz, f);
+            r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
+        } else {
+            central_flux(sj, si, w.wx, w.wy, w.wz, f);
+            r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
+        }
+    }
 }
 
 // interior edges of node i from the FP64 edge buffer, in edge order
@@ -569,23 +631,6 @@ __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, doubl
     }
 }
 
-// interior residual of node i as the anchor's FP64 sum plus the FP32 sum of
-// the flux increments of its edges
-__device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i, double *r) {
-    float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-        int s = L.inc[k].x;
-        const float *f = L.flux32 + (size_t)(s >= 0 ? s : ~s) * 5;
-        if (s >= 0) {
-            for (int c = 0; c < 5; ++c) acc[c] += f[c];
-        } else {
-            for (int c = 0; c < 5; ++c) acc[c] -= f[c];
-        }
-    }
-    const int N = L.N;
-    for (int c = 0; c < 5; ++c) r[c] = L.ra[c * N + i] + (double)acc[c];
-}
-
 // the FP64 evaluation becomes the new anchor of node i
 __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const double *rint) {
     const int N = L.N;
@@ -610,19 +655,22 @@ __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const do
 // mode RCOARSE: restrictGrid coarse one-step (def_par:12244-12263): src
 // mode RFINE:   restrictGrid fine increment (def_par:12356-12383): rhs
 // mode RESID:   rhs <- makeRHS only
-// PREC: GATHER_FP64 (FP64 edge buffer), GATHER_ANCHOR (FP64 edge buffer,
-// stored as the new mixed-precision anchor), GATHER_DELTA (anchor + FP32
-// increments)
+// PREC: GATHER_BUFFER (FP64 edge buffer of the upwind fluxes),
+// GATHER_CENTRAL (central fluxes computed in the gather), GATHER_ANCHOR (the
+// same, stored as the new mixed-precision anchor), GATHER_DELTA (anchor +
+// FP32 increments)
 template <int PREC>
-__global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
+__global__ void __launch_bounds__(256, 3) k_node_update(Params P, LevelView L, int mode, int stage) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
     double r[5];
     if constexpr (PREC == GATHER_DELTA) {
         gather_interior_delta(L, i, r);
-    } else {
+    } else if constexpr (PREC == GATHER_BUFFER) {
         gather_interior(L, i, r);
+    } else {
+        gather_interior_central(L, i, r);
         if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, r);
     }
     gather_boundary(L, i, r);
@@ -669,7 +717,8 @@ __global__ void k_node_update(Params P, LevelView L, int mode, int stage) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = un[c] - up[c];
     }
 }
-template __global__ void k_node_update<GATHER_FP64>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_DELTA>(Params, LevelView, int, int);
 
@@ -719,6 +768,7 @@ __global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
     bc_outer(P, cls, n0, n1, n2, p0, v);
     for (int k = 0; k < 5; ++k) { C.u[k * N + c] = v[k]; C.uprev[k * N + c] = v[k]; }
     C.p[c] = fabs(pressure(P, v[0], v[1], v[2], v[3], v[4]));
+    store_node(C.q, c, v[0], v[1], v[2], v[3], v[4], C.p[c], m);
 }
 
 // restrictGrid tail (def_par:12385-12427): C.rhs = R(F.rhs), increment
@@ -866,33 +916,44 @@ __global__ void k_resid_partial(LevelView L, double *part, int nblk) {
     }
 }
 
+// one warp per component (blockDim.x = 160); each lane folds the block
+// partials b = lane, lane+32, ... and the warp combines the lanes in a fixed
+// tree, so the result does not depend on timing
 __global__ void k_resid_final(const double *part, int nblk, double *out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    for (int k = 0; k < 5; ++k) {
-        double s = 0, m = 0;
-        int mi = 0x7fffffff;
-        for (int b = 0; b < nblk; ++b) {
-            s += part[b * 15 + k];
-            double v = part[b * 15 + 5 + k];
-            int iv = (int)part[b * 15 + 10 + k];
-            if (v > m || (v == m && iv < mi)) { m = v; mi = iv; }
-        }
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k >= 5) return;
+    double s = 0, m = 0;
+    int mi = 0x7fffffff;
+    for (int b = lane; b < nblk; b += 32) {
+        s += part[b * 15 + k];
+        double v = part[b * 15 + 5 + k];
+        int iv = (int)part[b * 15 + 10 + k];
+        if (v > m || (v == m && iv < mi)) { m = v; mi = iv; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, off);
+        double v = __shfl_down_sync(0xffffffffu, m, off);
+        int iv = __shfl_down_sync(0xffffffffu, mi, off);
+        if (v > m || (v == m && iv < mi)) { m = v; mi = iv; }
+    }
+    if (lane == 0) {
         out[k] = sqrt(s);
         out[5 + k] = m;
         out[10 + k] = (double)(mi == 0x7fffffff ? 0 : mi);
     }
 }
 
-// ---- forces (calculateLiftAndDrag def_par:14710-14805), one block ---------
+// ---- forces (calculateLiftAndDrag def_par:14710-14805): block partials ---
+// part[6*block + k]; k_forces_final sums the partials in block order
 __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
-                         double ground, double d0, double d1, double d2, double *out) {
+                         double ground, double d0, double d1, double d2, double *part) {
     __shared__ double red[6][256];
     double ft[3] = {cos(alphaR) * cos(betaR), sin(betaR), sin(alphaR)};
     double fn1[3] = {-ft[2], 0.0, ft[0]}, fn2[3] = {-ft[1], ft[0], 0.0};
     double acc[6] = {0, 0, 0, 0, 0, 0};
     const double pinf = 1. / (P.gamma * P.mach * P.mach);
     const int N = L.N;
-    for (int q = threadIdx.x; q < nwall; q += blockDim.x) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nwall; q += gridDim.x * blockDim.x) {
         int ip = wall[q];
         double h = L.cz[ip];
         if (!(h > (ground + 0.01))) continue;
@@ -927,14 +988,15 @@ __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, doub
             for (int k = 0; k < 6; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[0] = 2.0 * red[0][0];
-        out[1] = 2.0 * red[1][0];
-        out[2] = 2.0 * red[2][0];
-        out[3] = 2.0 * red[3][0];
-        out[4] = red[4][0];
-        out[5] = red[5][0];
-    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 6; ++k) part[6 * blockIdx.x + k] = red[k][0];
 }
 
+__global__ void k_forces_final(const double *part, int nblk, double *out) {
+    if (threadIdx.x >= 6) return;
+    const int k = threadIdx.x;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += part[6 * b + k];
+    out[k] = k < 4 ? 2.0 * s : s;
+}
 }  // namespace flite

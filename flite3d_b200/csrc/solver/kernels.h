@@ -21,11 +21,11 @@ __global__ void k_minmax(Params P, LevelView L);
 template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 __global__ void k_bnd_flux(Params P, LevelView L);
-enum { GATHER_FP64 = 0, GATHER_ANCHOR = 1, GATHER_DELTA = 2 };
+enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3 };
 template <int PREC>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
 __global__ void k_delta_state(LevelView L);
-__global__ void k_edge_flux_f32_delta(LevelView L);
+__global__ void k_make_inc32(const int2 *inc, const EdgeW *ew, int n, IncRec32 *o);
 __global__ void k_copy(const double *a, double *b, size_t n);
 __global__ void k_restrict_u(LevelView C, LevelView F);
 __global__ void k_restrict_state(Params P, LevelView C, LevelView F);
@@ -38,6 +38,8 @@ __global__ void k_set_int(int *dst, const int *src);
 __global__ void k_resid_partial(LevelView L, double *part, int nblk);
 __global__ void k_resid_final(const double *part, int nblk, double *out);
 __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
-                         double ground, double d0, double d1, double d2, double *out);
+                         double ground, double d0, double d1, double d2, double *part);
+__global__ void k_forces_final(const double *part, int nblk, double *out);
+constexpr int kForceBlocks = 64;
 
 }  // namespace flite

@@ -84,6 +84,8 @@ class Solver:
             ng = min(ng, controls.numberOfGridsToUse)
         self.nlevels = ng
         self.nodes = [mesh.level(l + 1).n_nodes for l in range(ng)]
+        # conserved variables, plus nu~ with the Spalart-Allmaras model
+        self.nvar = 6 if controls.turbulenceModel == 1 else 5
 
     def _err(self):
         if not hasattr(self.be.lib, self.be.prefix + "last_error"):
@@ -110,12 +112,12 @@ class Solver:
     # ---- state -------------------------------------------------------------
     def set_state(self, u, level=1):
         u = np.ascontiguousarray(u, dtype=np.float64)
-        assert u.shape == (5, self.nodes[level - 1])
+        assert u.shape == (self.nvar, self.nodes[level - 1])
         self._ck(self.be.set_state(self._h, level, _ptr(u)), "set_state")
 
     def get_state(self, level=1, out=None):
-        u = np.zeros((5, self.nodes[level - 1])) if out is None else out
-        assert u.shape == (5, self.nodes[level - 1]) and u.dtype == np.float64
+        u = np.zeros((self.nvar, self.nodes[level - 1])) if out is None else out
+        assert u.shape == (self.nvar, self.nodes[level - 1]) and u.dtype == np.float64
         assert u.flags["C_CONTIGUOUS"]
         self._ck(self.be.get_state(self._h, level, _ptr(u)), "get_state")
         return u
@@ -132,12 +134,12 @@ class Solver:
         self._ck(self.be.start(self._h), "start")
 
     # ---- solver calls ------------------------------------------------------
-    def do_time_iterations(self, level, nsteps=1, calc_diss=True, cycle=1):
-        self._ck(self.be.do_time_iterations(self._h, level, nsteps, int(calc_diss), 0, cycle),
+    def do_time_iterations(self, level, nsteps=1, calc_diss=True, cycle=1, calc_turb=True):
+        self._ck(self.be.do_time_iterations(self._h, level, nsteps, int(calc_diss), int(calc_turb), cycle),
                  "do_time_iterations")
 
-    def restrict(self, fine_level):
-        self._ck(self.be.restrict(self._h, fine_level, 0), "restrict")
+    def restrict(self, fine_level, calc_turb=True):
+        self._ck(self.be.restrict(self._h, fine_level, int(calc_turb)), "restrict")
 
     def prolong(self, coarse_level):
         self._ck(self.be.prolong(self._h, coarse_level), "prolong")
@@ -153,7 +155,8 @@ class Solver:
         if rc == _abi.FLITE_ENAN:
             raise FloatingPointError("NaN in residual")
         self._ck(rc, "residuals")
-        return np.array(res[:5]), np.array(mres[:5]), np.array(mind[:5])
+        n = self.nvar
+        return np.array(res[:n]), np.array(mres[:n]), np.array(mind[:n])
 
     def forces(self):
         out = (ctypes.c_double * 6)()
@@ -161,8 +164,9 @@ class Solver:
         return np.array(out[:])
 
     def residual_fwd(self, u, level=1):
+        """makeRHS of the mean flow (5 components) at the state u of a level."""
         u = np.ascontiguousarray(u, dtype=np.float64)
-        r = np.zeros_like(u)
+        r = np.zeros((5, u.shape[1]))
         self._ck(self.be.residual_fwd(self._h, level, _ptr(u), _ptr(r)), "residual_fwd")
         return r
 
@@ -219,7 +223,11 @@ def initial_state(controls, mesh, perturb_seed=None, amplitude=0.01):
     prim[0] = inf[0]
     if perturb_seed is not None:
         prim[0] = inf[0] * (1.0 + density_perturbation(n, perturb_seed, amplitude))
-    return primitive_to_conserved(prim)
+    u = primitive_to_conserved(prim)
+    if controls.turbulenceModel == 1:
+        # nu~ of the freestream initialisation (def_par:3961-3963)
+        u = np.vstack([u, np.full((1, n), 0.1)])
+    return u
 
 
 def run_steady(solver, orders=8.0, max_cycles=1000, callback=None):

@@ -24,6 +24,7 @@
 //  * the LED limiter's (1+t^nsig)^(1/nsig) (def_par:1861) is evaluated as
 //    sqrt(sqrt(1+(t*t)*(t*t))) for nsig=4 and sqrt(1+t*t) for nsig=2.
 #include "oracle.h"
+#include "pinned_math.h"
 
 #include <algorithm>
 #include <cmath>
@@ -52,6 +53,9 @@ struct Level {
     // state
     vec u[6], uprev[6], rhs[6], src[6], diss[5];
     vec p, dt, mu, conn, wallArea, nx, ny, nz, wallStress[3];
+    // Spalart-Allmaras: turbulenceDiffusionTerm, localTurbulentTimeSteps,
+    // vorticity and divergence of the viscous routine
+    vec turbDiff, dtT, vort, divg;
     int cycleNumber = 0;
     int R(int i) const { return reg[i + 20]; }  // nodeIndicatorRegister(i)
     // colouring of edge blocks for the threaded timing mode (built on first
@@ -339,6 +343,18 @@ struct Oracle {
             double mu = oRe * ((a * std::sqrt(a)) * ((Tin + 198.6) / (tempConv * Tin * T + 198.6)));
             double k = oPr * mu;
             g.mu[i] = mu;
+            {
+                const double a1 = dudy - dvdx, a2 = dvdz - dwdy, a3 = dwdx - dudz;
+                g.vort[i] = std::sqrt((a1 * a1 + a2 * a2) + a3 * a3);
+                g.divg[i] = (dudx + dvdy) + dwdz;
+            }
+            if (sa()) {  // def_par:5556-5566
+                double tvc = oRe * g.u[0][i] * g.u[5][i];
+                const double ksi3 = flite_pm::pm_cube(tvc / mu);
+                tvc = tvc * ksi3 / (ksi3 + 357.9);
+                mu = mu + tvc;
+                k = k + tvc * (1. / c.turbulentPrandtlNumber);
+            }
             nh[0][i] = mu * (fourThirds * dudx - twoThirds * (dvdy + dwdz));
             nh[1][i] = mu * (dudy + dvdx);
             nh[2][i] = mu * (dudz + dwdx);
@@ -886,12 +902,219 @@ struct Oracle {
         F[4] = (wx * (E * uu + pu) + wy * (E * vv + pv)) + wz * (E * ww + pw);
     }
 
-    // ---- solveSystem (def_par:1407-1479) ----------------------------------
+    bool sa() const { return c.turbulenceModel == 1; }
+
+    // ---- makeTurbulentTimeSteps (def_par:12878-13100) ---------------------
+    void makeTurbulentTimeSteps(Level &g) {
+        const double oneOverSigma = 3.0 / 2.0, oneOverKappaSquared = 1.0 / (0.41 * 0.41);
+        const double cb1 = 0.1355, cb2 = 0.622, ct3 = 1.1;
+        const double cw1 = cb1 * oneOverKappaSquared + (1.0 + cb2) * oneOverSigma;
+        const double oRe = 1.0 / c.ReynoldsNumber;
+        vec &h = nh[0];
+        std::fill(g.dtT.begin(), g.dtT.end(), 0.0);
+        std::fill(h.begin(), h.end(), 0.0);
+        for_edges(g, [&](int e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+            double al = (wx * wx + wy * wy) + wz * wz;
+            double ro1 = 1. / g.u[0][i1], ro2 = 1. / g.u[0][i2];
+            double vn1 = ((wx * g.u[1][i1] + wy * g.u[2][i1]) + wz * g.u[3][i1]) * ro1;
+            double vn2 = ((wx * g.u[1][i2] + wy * g.u[2][i2]) + wz * g.u[3][i2]) * ro2;
+            vn1 = c.turbK * std::sqrt(al) + std::fabs(vn1);
+            vn2 = c.turbK * std::sqrt(al) + std::fabs(vn2);
+            g.dtT[i1] = g.dtT[i1] + vn1;
+            g.dtT[i2] = g.dtT[i2] + vn2;
+            double vis1 = oneOverSigma * (g.mu[i1] + 3.0 * cb2 * g.u[5][i1] * oRe);
+            double vis2 = oneOverSigma * (g.mu[i2] + 3.0 * cb2 * g.u[5][i2] * oRe);
+            double dv1 = 2.0 * vis1 * al, dv2 = 2.0 * vis2 * al;
+            h[i1] = h[i1] + dv2;
+            h[i2] = h[i2] + dv1;
+        });
+        for_bedges(g, [&](int b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double wx = g.bwx[b], wy = g.bwy[b], wz = g.bwz[b];
+            double al = (wx * wx + wy * wy) + wz * wz;
+            double ro1 = 1. / g.u[0][i1], ro2 = 1. / g.u[0][i2];
+            double vn1 = ((wx * g.u[1][i1] + wy * g.u[2][i1]) + wz * g.u[3][i1]) * ro1;
+            double vn2 = ((wx * g.u[1][i2] + wy * g.u[2][i2]) + wz * g.u[3][i2]) * ro2;
+            vn1 = c.turbK * std::sqrt(al) + std::fabs(vn1);
+            vn2 = c.turbK * std::sqrt(al) + std::fabs(vn2);
+            double vnm = vn1 + vn2;
+            g.dtT[i1] = (g.dtT[i1] + vn1) + vnm;
+            g.dtT[i2] = (g.dtT[i2] + vn2) + vnm;
+            double vis1 = oneOverSigma * (g.mu[i1] + 3.0 * cb2 * g.u[5][i1] * oRe);
+            double vis2 = oneOverSigma * (g.mu[i2] + 3.0 * cb2 * g.u[5][i2] * oRe);
+            double dv1 = 2.0 * vis1 * al, dv2 = 2.0 * vis2 * al;
+            double dvm = dv1 + dv2;
+            h[i1] = (h[i1] + dv1) + dvm;
+            h[i2] = (h[i2] + dv2) + dvm;
+        });
+        for_nodes(g.N, [&](int i) {
+            double V = g.V[i];
+            g.dtT[i] = 0.5 / (g.dtT[i] / V + h[i] / (V * V));
+            double dt = g.dtT[i];
+            double dInvSquared = g.wdist[i] > 1.0e-10 ? 1.0 / g.wdist[i] : 1.0e10;
+            dInvSquared = dInvSquared * dInvSquared;
+            double S = (std::fabs(g.divg[i]) +
+                        cb1 * (g.vort[i] + (1.0 + ct3) * g.u[5][i] * oneOverKappaSquared * dInvSquared * oRe)) +
+                       cw1 * g.u[5][i] * dInvSquared * oRe;
+            g.dtT[i] = dt / (1.0 + 0.5 * S * dt);
+        });
+    }
+
+    // ---- makeSADiffusion (def_par:7436-7809) ------------------------------
+    void makeSADiffusion(Level &g) {
+        const double sigma = 2. / 3., cb2 = 0.622, oRe = 1. / c.ReynoldsNumber;
+        std::fill(g.turbDiff.begin(), g.turbDiff.end(), 0.0);
+        for (int k = 8; k < 14; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        for_edges(g, [&](int e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double t1 = g.u[5][i1], t2 = g.u[5][i2];
+            double f1 = g.wx[e] * (t1 + t2), f2 = g.wy[e] * (t1 + t2), f3 = g.wz[e] * (t1 + t2);
+            nh[8][i1] = nh[8][i1] + f1; nh[8][i2] = nh[8][i2] - f1;
+            nh[9][i1] = nh[9][i1] + f2; nh[9][i2] = nh[9][i2] - f2;
+            nh[10][i1] = nh[10][i1] + f3; nh[10][i2] = nh[10][i2] - f3;
+        });
+        for_bedges(g, [&](int b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double wx = g.bwx[b], wy = g.bwy[b], wz = g.bwz[b];
+            double t1 = g.u[5][i1], t2 = g.u[5][i2];
+            if (c.boundaryTerm == 1) {
+                nh[8][i1] = nh[8][i1] + (3. * t1 + t2) * wx; nh[8][i2] = nh[8][i2] + (t1 + 3. * t2) * wx;
+                nh[9][i1] = nh[9][i1] + (3. * t1 + t2) * wy; nh[9][i2] = nh[9][i2] + (t1 + 3. * t2) * wy;
+                nh[10][i1] = nh[10][i1] + (3. * t1 + t2) * wz; nh[10][i2] = nh[10][i2] + (t1 + 3. * t2) * wz;
+            } else {
+                nh[8][i1] = nh[8][i1] + 4. * t1 * wx; nh[8][i2] = nh[8][i2] + 4. * t2 * wx;
+                nh[9][i1] = nh[9][i1] + 4. * t1 * wy; nh[9][i2] = nh[9][i2] + 4. * t2 * wy;
+                nh[10][i1] = nh[10][i1] + 4. * t1 * wz; nh[10][i2] = nh[10][i2] + 4. * t2 * wz;
+            }
+        });
+        std::fill(nh[0].begin(), nh[0].end(), 0.0);
+        double fact = oRe * cb2 / sigma;
+        for_nodes(g.N, [&](int i) {
+            double vt = 1. / g.V[i];
+            double dx = nh[8][i] * vt, dy = nh[9][i] * vt, dz = nh[10][i] * vt;
+            nh[11][i] = dx; nh[12][i] = dy; nh[13][i] = dz;
+            double vp = (nh[8][i] * dx + nh[9][i] * dy) + nh[10][i] * dz;
+            nh[0][i] = nh[0][i] - fact * vp;
+        });
+        fact = oRe / sigma;
+        auto visc = [&](int i) { return c.ReynoldsNumber * g.mu[i] / g.u[0][i] + g.u[5][i]; };
+        for_edges(g, [&](int e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+            double fd1 = visc(i1) * ((wx * nh[11][i1] + wy * nh[12][i1]) + wz * nh[13][i1]);
+            double fd2 = visc(i2) * ((wx * nh[11][i2] + wy * nh[12][i2]) + wz * nh[13][i2]);
+            g.turbDiff[i1] = g.turbDiff[i1] - fact * (fd1 + fd2);
+            g.turbDiff[i2] = g.turbDiff[i2] + fact * (fd1 + fd2);
+        });
+        for_bedges(g, [&](int b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double wx = g.bwx[b], wy = g.bwy[b], wz = g.bwz[b];
+            double fd1 = visc(i1) * ((wx * nh[11][i1] + wy * nh[12][i1]) + wz * nh[13][i1]);
+            double fd2 = visc(i2) * ((wx * nh[11][i2] + wy * nh[12][i2]) + wz * nh[13][i2]);
+            if (c.boundaryTerm == 1) {
+                g.turbDiff[i1] = g.turbDiff[i1] - fact * (3. * fd1 + fd2);
+                g.turbDiff[i2] = g.turbDiff[i2] - fact * (fd1 + 3. * fd2);
+            } else {
+                g.turbDiff[i1] = g.turbDiff[i1] - fact * 4. * fd1;
+                g.turbDiff[i2] = g.turbDiff[i2] - fact * 4. * fd2;
+            }
+        });
+        for_nodes(g.N, [&](int i) { g.turbDiff[i] = g.turbDiff[i] + nh[0][i]; });
+    }
+
+    // ---- makeSARHS (def_par:6809-6950): upwinded convection of nu~ ---------
+    void makeSARHS(Level &g) {
+        for_edges(g, [&](int e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double rinv1 = 1. / g.u[0][i1], t1 = g.u[5][i1];
+            double u1 = rinv1 * g.u[1][i1], v1 = rinv1 * g.u[2][i1], w1 = rinv1 * g.u[3][i1];
+            double rinv2 = 1. / g.u[0][i2], t2 = g.u[5][i2];
+            double u2 = rinv2 * g.u[1][i2], v2 = rinv2 * g.u[2][i2], w2 = rinv2 * g.u[3][i2];
+            double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+            double fconv = (wx * (u1 * t1 + u2 * t2) + wy * (v1 * t1 + v2 * t2)) + wz * (w1 * t1 + w2 * t2);
+            if (std::fabs(t1 - t2) > 1.0e-20) {
+                double ax = (u2 * t2 - u1 * t1) / (t1 - t2);
+                double ay = (v2 * t2 - v1 * t1) / (t1 - t2);
+                double az = (w2 * t2 - w1 * t1) / (t1 - t2);
+                fconv = fconv + std::fabs((wx * ax + wy * ay) + wz * az) * (t1 - t2);
+            }
+            g.rhs[5][i1] = g.rhs[5][i1] + fconv;
+            g.rhs[5][i2] = g.rhs[5][i2] - fconv;
+        });
+    }
+
+    // ---- makeSASourceTerm (def_par:9285-9371) -----------------------------
+    // The laminar viscosity floor writes 0.1*Re (not 0.1/Re) into the array,
+    // as the reference does (def_par:9321-9323).
+    void makeSASourceTerm(Level &g) {
+        using namespace flite_pm;
+        const double oRe = 1. / c.ReynoldsNumber;
+        const double cb1 = 0.1355, cb2 = 0.622, kappa = 0.41, kappaSquared = kappa * kappa, sigma = 2. / 3.;
+        const double cw1 = cb1 / kappaSquared + (1.0 + cb2) / sigma;
+        const double cw2 = 0.3, cw3 = 2.0, cv1 = 7.1, ct3 = 1.1, ct4 = 2.0;
+        const double cv1Tripled = pm_cube(cv1), cw3InSixth = pm_pow6(cw3), oneOverSix = 1. / 6.;
+        const double cFact = pm_exp(oneOverSix * pm_log(1.0 + cw3InSixth));
+        for_nodes(g.N, [&](int i) {
+            double vt = g.V[i];
+            double mucurl = std::max(g.u[5][i], 0.0);
+            if (g.mu[i] < 0.1 / c.ReynoldsNumber) g.mu[i] = 0.1 * c.ReynoldsNumber;
+            double Ksi = g.u[0][i] * oRe * mucurl / g.mu[i];
+            Ksi = std::max(Ksi, 0.001);
+            double ft2 = ct3 * pm_exp(-ct4 * Ksi * Ksi);
+            double K3 = pm_cube(Ksi);
+            double d = std::max(g.wdist[i], 1.0e-10);
+            double muOverd = mucurl / d, dSquared = d * d;
+            double fv1 = K3 / (K3 + cv1Tripled);
+            double fv2 = 1.0 - (Ksi / (1.0 + Ksi * fv1));
+            double fv3 = 1.0;
+            double Scurl = fv3 * g.vort[i] + oRe * mucurl * fv2 / (kappaSquared * dSquared);
+            double r;
+            if (std::fabs(Scurl) > 1.0e-10) {
+                r = oRe * mucurl / (Scurl * kappaSquared * dSquared);
+                if (r < 0.0) r = 0.0;
+                if (r > 100.0) r = 100.0;
+            } else {
+                r = 100.0;
+            }
+            double gg = r + cw2 * (pm_pow6(r) - r);
+            double radicand = (1.0 + cw3InSixth) / (pm_pow6(gg) + cw3InSixth);
+            double fw = radicand > 1.0e-10 ? gg * pm_exp(oneOverSix * pm_log(radicand)) : cFact;
+            g.rhs[5][i] = g.rhs[5][i] - vt * cb1 * (1.0 - ft2) * Scurl * mucurl;
+            g.rhs[5][i] = g.rhs[5][i] + oRe * vt * (cw1 * fw - cb1 * ft2 / kappaSquared) * muOverd * muOverd;
+            g.rhs[5][i] = g.rhs[5][i] - vt * mucurl * g.divg[i];
+        });
+    }
+
+    // ---- limitTurbulence (def_par:1259-1290): a is floored at zero; the
+    // state's nu~ (not a) is capped at maxTurbulenceValue
+    void limitTurbulence(Level &g, vec &a) {
+        for (int i = 0; i < g.N; ++i) {
+            a[i] = std::max(a[i], 0.0);
+            if (g.u[5][i] > c.maxTurbulenceValue) g.u[5][i] = c.maxTurbulenceValue;
+        }
+    }
+
+    // ---- nullifyOuterBoundary (def_par:4254-4362), SA: components 1..6 of
+    // the far-field (indicator 3) and engine nodes
+    void nullifyOuterBoundary(Level &g, vec *u) {
+        if (!sa()) return;
+        const int ranges[5][2] = {{-16, -15}, {-12, -11}, {-10, -9}, {-8, -7}, {-6, -5}};
+        for (auto &rg : ranges)
+            for_range(g, rg[0], rg[1], [&](int ip) {
+                for (int k = 0; k < 6; ++k) u[k][ip] = 0.0;
+            });
+    }
+
+    // ---- solveSystem (def_par:1407-1479) + solveTurbulenceSystem
+    // (def_par:1481-1522) -------------------------------------------------
     void solveSystem(Level &g, vec *rhs) {
         for_nodes(g.N, [&](int i) {
             double dt = g.dt[i];
             for (int k = 0; k < 5; ++k) rhs[k][i] = dt * rhs[k][i] / g.V[i];
         });
+        if (sa()) for_nodes(g.N, [&](int i) { rhs[5][i] = g.dtT[i] * rhs[5][i] / g.V[i]; });
     }
 
     double relaxation_param(const Level &g) const {
@@ -915,15 +1138,23 @@ struct Oracle {
 
     // ---- setBCsOnIncrementField (def_par:4978-5140) -----------------------
     void setBCsOnIncrementField(Level &g, vec *rhs) {
+        const bool t = sa();
         if (c.ReynoldsNumber > 0) {
             for_range(g, -20, -19, [&](int ip) {
                 rhs[1][ip] = 0.0; rhs[2][ip] = 0.0; rhs[3][ip] = 0.0;
                 if (!c.wallsAreIsentropic) rhs[4][ip] = 0.0;
+                if (t) rhs[5][ip] = 0.0;
             });
         } else {
-            for_range(g, -20, -19, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
+            for_range(g, -20, -19, [&](int ip) {
+                remove_normal(g, rhs, ip, 1.0);
+                if (t) rhs[5][ip] = 0.0;
+            });
         }
-        for_range(g, -4, -3, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
+        for_range(g, -4, -3, [&](int ip) {
+            remove_normal(g, rhs, ip, 1.0);
+            if (t) rhs[5][ip] = 0.0;
+        });
         for_range(g, -18, -17, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
     }
 
@@ -942,6 +1173,14 @@ struct Oracle {
             }
             for (int k = 1; k < 5; ++k) u[k][i] = uprev[k][i] - delu[k][i];
         });
+        if (sa()) {
+            const double dtT = rk > 0 ? c.turbulentCFLNumber * RK[rk - 1] : c.turbulentCFLNumber;
+            for_nodes(g.N, [&](int i) {
+                delu[5][i] = dtT * delu[5][i];
+                u[5][i] = uprev[5][i] - delu[5][i];
+                u[5][i] = std::max(u[5][i], 0.0);
+            });
+        }
         for_nodes(g.N, [&](int i) { if (g.u[0][i] < c.minimumDensity) g.u[0][i] = c.minimumDensity; });
     }
 
@@ -953,11 +1192,15 @@ struct Oracle {
                 double cm[3] = {g.cmx[ip], g.cmy[ip], g.cmz[ip]};
                 for (int k = 0; k < 3; ++k) u[1 + k][ip] = u[0][ip] * cm[k] / c.physicalTimeStep;
                 if (!c.wallsAreIsentropic) u[4][ip] = u[0][ip] * c.inflowTemperature / c.gamma;
+                if (sa()) u[5][ip] = 0.0;
             });
         } else {
             // the wall velocity term adds grp%u(ip,1)*0*normal for a steady
             // run (def_par:4445-4456): the tangential projection only
-            for_range(g, -20, -19, [&](int ip) { remove_normal(g, u, ip, 1.0); });
+            for_range(g, -20, -19, [&](int ip) {
+                remove_normal(g, u, ip, 1.0);
+                if (sa()) u[5][ip] = 0.0;
+            });
         }
         for_range(g, -4, -3, [&](int ip) {
             remove_normal(g, u, ip, relax);
@@ -965,6 +1208,7 @@ struct Oracle {
                 double ke = (u[1][ip] * u[1][ip] + u[2][ip] * u[2][ip]) + u[3][ip] * u[3][ip];
                 u[4][ip] = u[0][ip] * c.inflowTemperature / c.gamma + 0.5 * ke / u[0][ip];
             }
+            if (sa()) u[5][ip] = 0.0;
         });
         for_range(g, -18, -17, [&](int ip) { remove_normal(g, u, ip, 1.0); });
     }
@@ -989,6 +1233,7 @@ struct Oracle {
                 } else {
                     if (c.MachNumber < 1.0) u[4][ip] = iP / gm1 + 0.5 * ((U1 * U1 + U2 * U2) + U3 * U3) / rho;
                 }
+                if (sa()) u[5][ip] = 0.1;  // every branch (def_par:4076-4140)
             });
         }
     }
@@ -1004,39 +1249,58 @@ struct Oracle {
     }
 
     // ---- singleIteration (def_par:1002-1181) ------------------------------
-    void singleIteration(Level &g, bool calcDiss) {
+    void singleIteration(Level &g, bool calcDiss, bool calcTurb) {
+        const bool turb = sa() && calcTurb;
         if (calcDiss) {
             makePressureField(g, g.u);
             for_nodes(g.N, [&](int i) { g.p[i] = std::fabs(g.p[i]); });
             makeTimeSteps(g);
             dissipation_for(g, false);
-            if (c.ReynoldsNumber > 0.0) makeViscosityTerm(g);
+            if (c.ReynoldsNumber > 0.0) {
+                makeViscosityTerm(g);
+                if (turb) {
+                    makeTurbulentTimeSteps(g);
+                    makeSADiffusion(g);
+                }
+            }
         }
         for (int st = 1; st <= 3; ++st) {
             makePressureField(g, g.u);
-            for (int k = 0; k < 5; ++k) std::fill(g.rhs[k].begin(), g.rhs[k].end(), 0.0);
+            for (int k = 0; k < nvar; ++k) std::fill(g.rhs[k].begin(), g.rhs[k].end(), 0.0);
             makeRHS(g);
+            if (turb) {
+                // triggerTurbulenceField and makeSATripTerm act on the trip
+                // field nodes of a .wid file; none are read (no trip lines)
+                makeSARHS(g);
+                makeSASourceTerm(g);
+            }
             for (int k = 0; k < 5; ++k)
                 for_nodes(g.N, [&](int i) { g.rhs[k][i] = g.rhs[k][i] + g.diss[k][i]; });
+            if (turb) for_nodes(g.N, [&](int i) { g.rhs[5][i] = g.rhs[5][i] + g.turbDiff[i]; });
             solveSystem(g, g.rhs);
             setBCsOnIncrementField(g, g.rhs);
-            // nullifyOuterBoundary: no-op for turbulenceModel 0
+            if (g.grid > 1) nullifyOuterBoundary(g, g.rhs);
             updateSolutionVector(g, g.u, g.uprev, g.rhs, st);
             setBCsOnSolutionField(g, g.u);
-            if (g.grid > 1)
+            if (g.grid > 1) {
                 for (int k = 0; k < 5; ++k)
                     for_nodes(g.N, [&](int i) { g.u[k][i] = g.u[k][i] - RK[st - 1] * g.src[k][i]; });
+                if (turb) for_nodes(g.N, [&](int i) { g.u[5][i] = g.u[5][i] - RK[st - 1] * g.src[5][i]; });
+            }
             limitDensity(g);
+            if (turb) limitTurbulence(g, g.u[5]);
             setOuterBoundaryConditions(g, g.u, g.p);
         }
     }
+
+    bool calcTurbOfCycle = true;  // cycleNo <= numberOfTurbulenceSteps (mg_par:922-926)
 
     void doTimeIterations(int l, int nsteps, bool calcDiss, int cycle) {
         Level &g = lv[l];
         g.cycleNumber = cycle;
         for (int s = 0; s < nsteps; ++s) {
             for (int k = 0; k < nvar; ++k) g.uprev[k] = g.u[k];
-            singleIteration(g, calcDiss);
+            singleIteration(g, calcDiss, calcTurbOfCycle);
         }
     }
 
@@ -1060,9 +1324,11 @@ struct Oracle {
     }
 
     // ---- restrictGrid (def_par:12141-12430) -------------------------------
-    void restrictGrid(int fl) {
+    void restrictGrid(int fl, bool calcTurb) {
         Level &F = lv[fl], &C = lv[fl + 1];
-        mapFineToCoarse(F, C, F.u, C.u, 5);
+        const bool turb = sa() && calcTurb;
+        const int nv = nvar;
+        mapFineToCoarse(F, C, F.u, C.u, nv);
         {   // mapScalarFineToCoarse of the laminar viscosity
             vec m(C.N, 0.0);
             for (int i = 0; i < F.N; ++i) {
@@ -1074,94 +1340,124 @@ struct Oracle {
         makePressureField(C, C.u);
         setBCsOnSolutionField(C, C.u);
         setOuterBoundaryConditions(C, C.u, C.p);
-        for (int k = 0; k < 5; ++k) C.uprev[k] = C.u[k];
+        for (int k = 0; k < nv; ++k) C.uprev[k] = C.u[k];
         makePressureField(C, C.u);
         for (int i = 0; i < C.N; ++i) C.p[i] = std::fabs(C.p[i]);
         makeTimeSteps(C);
         if (c.coarseGridDissipationScheme == 2) makeArtificialDissipation2(C);
         else if (c.coarseGridDissipationScheme == 3) makeArtificialDissipation3(C);
         if (c.ReynoldsNumber > 0.0) makeViscosityTerm(C);
-        for (int k = 0; k < 5; ++k) std::fill(C.rhs[k].begin(), C.rhs[k].end(), 0.0);
+        for (int k = 0; k < nv; ++k) std::fill(C.rhs[k].begin(), C.rhs[k].end(), 0.0);
         makeRHS(C);
+        if (turb) {
+            makeTurbulentTimeSteps(C);
+            makeSADiffusion(C);
+            makeSARHS(C);
+            makeSASourceTerm(C);
+        }
         for (int k = 0; k < 5; ++k)
             for (int i = 0; i < C.N; ++i) C.rhs[k][i] = C.rhs[k][i] + C.diss[k][i];
+        // the turbulent diffusion is added with or without calculateTurbulence
+        // (def_par:12238-12240): the last computed one
+        if (sa()) for (int i = 0; i < C.N; ++i) C.rhs[5][i] = C.rhs[5][i] + C.turbDiff[i];
         solveSystem(C, C.rhs);
         setBCsOnIncrementField(C, C.rhs);
+        nullifyOuterBoundary(C, C.rhs);
         updateSolutionVector(C, C.u, C.uprev, C.rhs, 0);
         setBCsOnSolutionField(C, C.u);
         setOuterBoundaryConditions(C, C.u, C.p);
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < nv; ++k)
             for (int i = 0; i < C.N; ++i) C.src[k][i] = C.u[k][i] - C.uprev[k][i];
-        for (int k = 0; k < 5; ++k) C.u[k] = C.uprev[k];
+        for (int k = 0; k < nv; ++k) C.u[k] = C.uprev[k];
         // fine-grid one-step increment at the current fine state
         makePressureField(F, F.u);
         for (int i = 0; i < F.N; ++i) F.p[i] = std::fabs(F.p[i]);
         dissipation_for(F, true);
         if (c.ReynoldsNumber > 0.0) makeViscosityTerm(F);
-        for (int k = 0; k < 5; ++k) std::fill(F.rhs[k].begin(), F.rhs[k].end(), 0.0);
+        for (int k = 0; k < nv; ++k) std::fill(F.rhs[k].begin(), F.rhs[k].end(), 0.0);
         makeRHS(F);
+        if (turb) {
+            makeSADiffusion(F);
+            makeSARHS(F);
+            makeSASourceTerm(F);
+        }
         for (int k = 0; k < 5; ++k)
             for (int i = 0; i < F.N; ++i) F.rhs[k][i] = F.rhs[k][i] + F.diss[k][i];
+        if (sa()) for (int i = 0; i < F.N; ++i) F.rhs[5][i] = F.rhs[5][i] + F.turbDiff[i];
         solveSystem(F, F.rhs);
         setBCsOnIncrementField(F, F.rhs);
+        if (F.grid > 1) nullifyOuterBoundary(F, F.rhs);  // FAS source term allocated
         updateSolutionVector(F, F.rhs, F.uprev, F.rhs, 0);
         setBCsOnSolutionField(F, F.rhs);
         if (F.grid > 1)
-            for (int k = 0; k < 5; ++k)
+            for (int k = 0; k < nv; ++k)
                 for (int i = 0; i < F.N; ++i) F.rhs[k][i] = F.rhs[k][i] - F.src[k][i];
+        if (sa()) limitTurbulence(F, F.rhs[5]);
         setOuterBoundaryConditions(F, F.rhs, F.p);
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < nv; ++k)
             for (int i = 0; i < F.N; ++i) F.rhs[k][i] = F.rhs[k][i] - F.uprev[k][i];
-        mapFineToCoarse(F, C, F.rhs, C.rhs, 5);
+        mapFineToCoarse(F, C, F.rhs, C.rhs, nv);
         setBCsOnIncrementField(C, C.rhs);
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < nv; ++k)
             for (int i = 0; i < C.N; ++i) C.src[k][i] = C.src[k][i] - C.rhs[k][i];
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < nv; ++k)
             for (int i = 0; i < C.N; ++i) C.u[k][i] = C.u[k][i] + C.rhs[k][i];
     }
 
     // ---- prolongateGrid (def_par:12432-12570) -----------------------------
     void prolongateGrid(int cl) {
         Level &C = lv[cl], &F = lv[cl - 1];
-        mapFineToCoarse(F, C, F.u, C.uprev, 5);
+        const int nv = nvar;
+        mapFineToCoarse(F, C, F.u, C.uprev, nv);
         setBCsOnSolutionField(C, C.uprev);
         setOuterBoundaryConditions(C, C.uprev, C.p);
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < nv; ++k)
             for (int i = 0; i < C.N; ++i) C.rhs[k][i] = C.u[k][i] - C.uprev[k][i];
+        nullifyOuterBoundary(C, C.rhs);
         setBCsOnIncrementField(C, C.rhs);
-        mapCoarseToFine(C, F, C.rhs, F.rhs, 5);
+        mapCoarseToFine(C, F, C.rhs, F.rhs, nv);
+        nullifyOuterBoundary(F, F.rhs);
         for (int k = 0; k < 5; ++k)
             for (int i = 0; i < F.N; ++i) F.rhs[k][i] = c.prolongationRelaxation * F.rhs[k][i];
+        if (sa())
+            for (int i = 0; i < F.N; ++i) F.rhs[5][i] = c.turbProlongationRelaxation * F.rhs[5][i];
         for (int k = 0; k < 5; ++k)
             for (int i = 0; i < F.Nb; ++i) F.rhs[k][i] = c.multigridBCRelaxation * F.rhs[k][i];
+        // the nu~ correction reaches levels finer than numberOfTurbulenceGrids
+        const int ncomp = (sa() && F.grid < c.numberOfTurbulenceGrids) ? 6 : 5;
         for (int i = 0; i < F.N; ++i)
-            for (int k = 0; k < 5; ++k) F.u[k][i] = F.u[k][i] + F.rhs[k][i];
+            for (int k = 0; k < ncomp; ++k) F.u[k][i] = F.u[k][i] + F.rhs[k][i];
         setBCsOnSolutionField(F, F.u);
         setOuterBoundaryConditions(F, F.u, F.p);
-        for (int i = 0; i < F.N; ++i) F.u[0][i] = std::max(F.u[0][i], c.minimumDensity);
+        for (int i = 0; i < F.N; ++i) {
+            if (sa()) F.u[5][i] = std::max(F.u[5][i], 0.0);
+            F.u[0][i] = std::max(F.u[0][i], c.minimumDensity);
+        }
     }
 
     // ---- oneCycle (mg_par:907-1196) ---------------------------------------
     void oneCycle(int cyc) {
         const int G = (int)lv.size();
+        calcTurbOfCycle = cyc <= c.numberOfTurbulenceSteps;
+        const bool ct = calcTurbOfCycle;
         const int nr = c.numberOfRelaxationSteps;
         auto relax = [&](int j1, int steps, bool calc) { doTimeIterations(j1 - 1, steps, calc, cyc); };
-        auto restr = [&](int j1) { restrictGrid(j1 - 1); };
+        auto restr = [&](int j1) { restrictGrid(j1 - 1, ct); };
         auto prol = [&](int j1) { prolongateGrid(j1 - 1); };
         const int s = c.multigridScheme;
         if (s <= 0) {
             for (int i = 1; i <= G - 1; ++i) {
-                for (int k = 0; k < 5; ++k) lv[i - 1].uprev[k] = lv[i - 1].u[k];
-                mapFineToCoarse(lv[i - 1], lv[i], lv[i - 1].u, lv[i].u, 5);
+                for (int k = 0; k < nvar; ++k) lv[i - 1].uprev[k] = lv[i - 1].u[k];
+                mapFineToCoarse(lv[i - 1], lv[i], lv[i - 1].u, lv[i].u, nvar);
             }
-            for (int k = 0; k < 5; ++k) std::fill(lv[G - 1].src[k].begin(), lv[G - 1].src[k].end(), 0.0);
+            for (int k = 0; k < nvar; ++k) std::fill(lv[G - 1].src[k].begin(), lv[G - 1].src[k].end(), 0.0);
             relax(G, nr, true);
-            for (int i = G; i >= 2; --i) mapCoarseToFine(lv[i - 1], lv[i - 2], lv[i - 1].u, lv[i - 2].u, 5);
+            for (int i = G; i >= 2; --i) mapCoarseToFine(lv[i - 1], lv[i - 2], lv[i - 1].u, lv[i - 2].u, nvar);
         } else if (s == 1) {
             for (int i = 1; i <= G - 1; ++i) {
                 relax(i, nr, i == 1);
                 restr(i);
-                mapFineToCoarse(lv[i - 1], lv[i], lv[i - 1].u, lv[i].u, 5);
+                mapFineToCoarse(lv[i - 1], lv[i], lv[i - 1].u, lv[i].u, nvar);
             }
             relax(G, nr, G == 1);
             for (int i = G; i >= 2; --i) { prol(i); relax(i - 1, nr, (i - 1) == 1); }
@@ -1285,7 +1581,10 @@ int check_controls(const flite_controls &c) {
         c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
         c.prolongationSmoothingFactor > 0)
         return FLITE_EUNSUPPORTED;
-    if (c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
+    // Spalart-Allmaras (1) is on the path and needs a viscous run; k-omega
+    // and SST (2, 3) are not
+    if (c.turbulenceModel != 0 && c.turbulenceModel != 1) return FLITE_EUNSUPPORTED;
+    if (c.turbulenceModel == 1 && !(c.ReynoldsNumber > 0)) return FLITE_EUNSUPPORTED;
     if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return FLITE_EUNSUPPORTED;
     if (c.fluxType < 1 || c.fluxType > 4) return FLITE_EUNSUPPORTED;
     // least-squares gradients divide by |dx|^2 of coarse-level coordinates
@@ -1367,6 +1666,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
     auto ctx = std::make_unique<oracle_ctx>();
     Oracle &o = ctx->o;
     o.c = *c;
+    o.nvar = c->turbulenceModel == 1 ? 6 : 5;
     int G = nlevels;
     if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);
     o.lv.resize(G);
@@ -1422,6 +1722,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
         }
         for (int k = 0; k < 5; ++k) g.diss[k].assign(g.N, 0.0);
         g.p.assign(g.N, 0.0); g.dt.assign(g.N, 0.0); g.mu.assign(g.N, 0.0);
+        g.turbDiff.assign(g.N, 0.0); g.dtT.assign(g.N, 0.0); g.vort.assign(g.N, 0.0); g.divg.assign(g.N, 0.0);
         for (int k = 0; k < 3; ++k) g.wallStress[k].assign(g.N, 0.0);
         g.cycleNumber = l == 0 ? 1 : 0;
         o.setup_level(g);
@@ -1472,6 +1773,10 @@ int oracle_get_array(oracle_ctx *o, int level, const char *name, double *out) {
     else if (n == "src") cols(g->src, 5);
     else if (n == "mu") std::memcpy(out, g->mu.data(), 8 * N);
     else if (n == "conn") std::memcpy(out, g->conn.data(), 8 * N);
+    else if (n == "turbDiff") std::memcpy(out, g->turbDiff.data(), 8 * N);
+    else if (n == "dtT") std::memcpy(out, g->dtT.data(), 8 * N);
+    else if (n == "vort") std::memcpy(out, g->vort.data(), 8 * N);
+    else if (n == "div") std::memcpy(out, g->divg.data(), 8 * N);
     else if (n == "wallArea") std::memcpy(out, g->wallArea.data(), 8 * N);
     else if (n == "wallStress") cols(g->wallStress, 3);
     else if (n == "normal") {
@@ -1488,6 +1793,9 @@ int oracle_init_freestream(oracle_ctx *o) {
     Level &g = o->o.lv[0];
     for (int i = 0; i < g.N; ++i)
         for (int k = 0; k < 5; ++k) g.u[k][i] = o->o.c.inflowField[k];
+    // setUpInitialField2's freestream branch (def_par:3953-3963)
+    if (o->o.c.ReynoldsNumber > 0.0) std::fill(g.mu.begin(), g.mu.end(), 1. / o->o.c.ReynoldsNumber);
+    if (o->o.sa()) std::fill(g.u[5].begin(), g.u[5].end(), 0.1);
     return FLITE_OK;
 }
 
@@ -1508,16 +1816,15 @@ int oracle_start(oracle_ctx *o) {
 
 int oracle_do_time_iterations(oracle_ctx *o, int level, int nsteps, int calc_diss, int calc_turb,
                               int cycle_no) {
-    (void)calc_turb;
     if (!lvl(o, level)) return FLITE_EINVAL;
+    o->o.calcTurbOfCycle = calc_turb != 0;
     o->o.doTimeIterations(level - 1, nsteps, calc_diss != 0, cycle_no);
     return FLITE_OK;
 }
 
 int oracle_restrict(oracle_ctx *o, int fine_level, int calc_turb) {
-    (void)calc_turb;
     if (!lvl(o, fine_level) || !lvl(o, fine_level + 1)) return FLITE_EINVAL;
-    o->o.restrictGrid(fine_level - 1);
+    o->o.restrictGrid(fine_level - 1, calc_turb != 0);
     return FLITE_OK;
 }
 
@@ -1548,7 +1855,7 @@ int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[
     if (!o) return FLITE_EINVAL;
     Oracle &O = o->o;
     Level &g = O.c.multigridScheme > 0 ? O.lv[0] : O.lv.back();
-    const int nres = 5;
+    const int nres = O.nvar;  // writeResiduals: 6 with SA (mg_par:1292-1293)
     for (int k = 0; k < 7; ++k) { res[k] = 0.0; maxres[k] = 0.0; maxind[k] = 1; }
     for (int k = 0; k < nres; ++k) {
         double s = 0.0;
