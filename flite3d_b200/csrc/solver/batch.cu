@@ -21,6 +21,7 @@ struct flite_batch {
     std::vector<flite_ctx *> cases;
     std::vector<int> donor;  // index of the case owning the mesh copy
     std::vector<char> active;  // cases the batch graph advances
+    std::vector<char> turb;    // calculateTurbulence each case's part of the graph was captured with
     double *h_res = nullptr;   // pinned: res1 of every case
     cudaStream_t s = nullptr;
     int *d_cycle = nullptr;
@@ -42,8 +43,18 @@ struct flite_batch {
         if (s) cudaStreamDestroy(s);
     }
 
+    // calculateTurbulence of every case for cycle `cyc` (SA cases); a change
+    // drops the batch graph
+    void select_cycle(int cyc) {
+        for (size_t i = 0; i < cases.size(); ++i) {
+            cases[i]->select_cycle(cyc);
+            if (graph && turb[i] != (char)cases[i]->calcTurb) drop_graph();
+        }
+    }
     void build_graph() {
         if (graph) return;
+        turb.resize(cases.size());
+        for (size_t i = 0; i < cases.size(); ++i) turb[i] = (char)cases[i]->calcTurb;
         cudaGraph_t parent = nullptr;
         CK(cudaGraphCreate(&parent, 0));
         launches = 0;
@@ -83,7 +94,7 @@ struct flite_batch {
             flite_ctx *c = cases[i];
             const LevelView &L = c->c.multigridScheme > 0 ? c->V(0) : c->V((int)c->lv.size() - 1);
             k_resid_partial<<<kResidBlocks, 256, 0, s>>>(L, c->d_part, kResidBlocks);
-            k_resid_final<<<1, 160, 0, s>>>(c->d_part, kResidBlocks, c->d_out);
+            k_resid_final<<<1, 192, 0, s>>>(c->d_part, kResidBlocks, c->d_out);
             CK(cudaMemcpyAsync(h_res + i, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, s));
         }
         CK(cudaStreamSynchronize(s));
@@ -160,6 +171,7 @@ int flite_batch_context(flite_batch *b, int case_index, flite_ctx **ctx) {
 
 int flite_batch_cycle(flite_batch *b, int cycle_no) {
     return bguard(b, [&] {
+        b->select_cycle(cycle_no);
         b->build_graph();
         b->set_cycle(cycle_no);
         CK(cudaGraphLaunch(b->graph, b->s));
@@ -181,6 +193,7 @@ int flite_batch_run(flite_batch *b, int first_cycle, int max_cycles, double orde
         const double target = std::pow(10.0, -orders);
         size_t left = n;
         for (int k = 0; k < max_cycles && left > 0; ++k) {
+            b->select_cycle(first_cycle + k);
             b->build_graph();
             b->set_cycle(first_cycle + k);
             CK(cudaGraphLaunch(b->graph, b->s));
@@ -222,6 +235,7 @@ int flite_batch_time_cycles(flite_batch *b, int cycle_no, int ncycles, int seque
                             int64_t *launches_per_cycle) {
     if (ncycles < 1 || !ms) return FLITE_EINVAL;
     return bguard(b, [&] {
+        b->select_cycle(cycle_no);
         if (sequential) {
             for (flite_ctx *c : b->cases) c->ensure_graph();
         } else {

@@ -61,6 +61,19 @@ struct flite_ctx {
     // threads per block of the edge kernels and of the node kernels (the
     // batch autotuner may change them; kernels with launch bounds take <= 256)
     int eb = kBlock, nb = kBlock;
+    // calculateTurbulence of the cycle being run or captured (Spalart-
+    // Allmaras: cycleNo <= numberOfTurbulenceSteps, mg_par:922-926), and the
+    // value the instantiated graph was captured with
+    bool calcTurb = true, graphTurb = true;
+    int nvar() const { return c.turbulenceModel == 1 ? 6 : 5; }
+    bool sa() const { return c.turbulenceModel == 1; }
+    bool turb() const { return sa() && calcTurb; }
+    // set calcTurb for cycle `cyc`, dropping a graph captured with the other value
+    void select_cycle(int cyc) {
+        const bool t = !sa() || cyc <= c.numberOfTurbulenceSteps;
+        if (graph && graphTurb != t) drop_graph();
+        calcTurb = t;
+    }
     // adjoint buffers (allocated on the first flite_residual_vjp)
     double *adj_rbar = nullptr, *adj_ubar = nullptr, *adj_b = nullptr;
     size_t adj_n = 0;
@@ -144,6 +157,28 @@ struct flite_ctx {
         counted();
         k_visc_flux<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
+    // ---- Spalart-Allmaras ----------------------------------------------
+    void sa_timesteps(int l) {
+        counted();
+        k_sa_timestep<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+    }
+    void sa_diffusion(int l) {
+        counted();
+        k_sa_grad<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        counted();
+        k_sa_diff<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+    }
+    // the nu~ part of a stage or one-step update; before the mean-flow node
+    // update, which overwrites the density the source term reads
+    void sa_stage(int l, int mode, int stage) {
+        if (!sa()) return;
+        if (turb()) {
+            counted();
+            k_sa_conv<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        }
+        counted();
+        k_sa_stage<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), mode, stage, turb() ? 1 : 0);
+    }
     // makeRHS up to the node gather (def_par:1587-1607 and the edge loops);
     // with FLITE_MIXED, `anchor` selects the FP64 evaluation that refreshes
     // the anchor state, otherwise the FP32 increments over it
@@ -214,12 +249,17 @@ struct flite_ctx {
             timesteps(l);
             dissipation(l);
             viscous(l);
+            if (turb()) {
+                sa_timesteps(l);
+                sa_diffusion(l);
+            }
         }
         for (int st = 1; st <= 3; ++st) {
             // u == uprev at stage 1: the FP64 evaluation there is the anchor
             // of the mixed-precision increments of stages 2 and 3
             pressure(l);
             rhs_terms(l, st == 1);
+            sa_stage(l, MODE_STAGE, st);
             node_update(l, MODE_STAGE, st, st == 1);
         }
     }
@@ -229,7 +269,7 @@ struct flite_ctx {
         k_set_int<<<1, 1, 0, s>>>(V(l).cyc, d_cycle);
         for (int i = 0; i < nsteps; ++i) {
             counted();
-            k_copy<<<nblk(5 * (size_t)V(l).N), nb, 0, s>>>(V(l).u, V(l).uprev, 5 * (size_t)V(l).N);
+            k_copy<<<nblk(nvar() * (size_t)V(l).N), nb, 0, s>>>(V(l).u, V(l).uprev, nvar() * (size_t)V(l).N);
             singleIteration(l, calcDiss);
         }
     }
@@ -243,11 +283,18 @@ struct flite_ctx {
         else if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
         viscous(cl);
         rhs_terms(cl);
+        if (turb()) {
+            sa_timesteps(cl);
+            sa_diffusion(cl);
+        }
+        sa_stage(cl, MODE_RCOARSE, 0);
         node_update(cl, MODE_RCOARSE, 0);
         pressure(fl);
         jst(fl);  // the fine part always uses scheme 2 (def_par:12266-12270)
         viscous(fl);
         rhs_terms(fl, false);
+        if (turb()) sa_diffusion(fl);  // the fine level keeps its turbulent time steps
+        sa_stage(fl, MODE_RFINE, 0);
         node_update(fl, MODE_RFINE, 0, false);
         counted();
         k_restrict_incr<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
@@ -273,12 +320,12 @@ struct flite_ctx {
         if (sch <= 0) {
             for (int i = 1; i <= G - 1; ++i) {
                 counted();
-                k_copy<<<nblk(5 * (size_t)V(i - 1).N), nb, 0, s>>>(V(i - 1).u, V(i - 1).uprev,
-                                                                        5 * (size_t)V(i - 1).N);
+                k_copy<<<nblk(nvar() * (size_t)V(i - 1).N), nb, 0, s>>>(V(i - 1).u, V(i - 1).uprev,
+                                                                            nvar() * (size_t)V(i - 1).N);
                 mapFineToCoarse(i - 1);
             }
             counted();
-            k_fill<<<nblk(5 * (size_t)V(G - 1).N), nb, 0, s>>>(V(G - 1).src, 5 * (size_t)V(G - 1).N, 0.0);
+            k_fill<<<nblk(nvar() * (size_t)V(G - 1).N), nb, 0, s>>>(V(G - 1).src, nvar() * (size_t)V(G - 1).N, 0.0);
             relax(G, nr, true);
             for (int i = G; i >= 2; --i) {
                 counted();
@@ -398,6 +445,7 @@ struct flite_ctx {
         }
         counting = false;
         CK(cudaStreamEndCapture(s, &g));
+        graphTurb = calcTurb;
         cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
         cudaGraphDestroy(g);
         CK(e);

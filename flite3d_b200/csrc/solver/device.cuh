@@ -18,6 +18,9 @@ struct Params {
     double inf[12];
     double RK[3];
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
+    // Spalart-Allmaras (turbulenceModel 1)
+    int sa, nTurbGrids;
+    double turbCFL, turbK, maxTurb, turbProlRelax, oPrt;
 };
 
 // Records gathered by node kernels from a node's incident edges and from its
@@ -43,6 +46,7 @@ struct __align__(16) DeltaRec {  // FP32 anchor primitives and increments (48 B)
 // ([component][node]), like the reference's column-major u(N,nvar).
 struct LevelView {
     int N, E, B, Nb, grid;
+    int nvar;                    // 5, or 6 with the Spalart-Allmaras nu~
     const int2 *edge;            // [E] (i1, i2), 0-based
     const double *wx, *wy, *wz;  // [E] edge coefficients
     const double *slen;          // [E]
@@ -58,6 +62,7 @@ struct LevelView {
     const int *binc_ptr;
     const int *binc;
     const double *V, *conn, *nx, *ny, *nz, *wallArea;
+    const double *wdist;             // wall distance (zero where the mesh has none)
     const double *cx, *cy, *cz;      // level 1; zero on coarse levels
     const double *cmx, *cmy, *cmz;   // coordinateMovement (level 1)
     const unsigned char *bc;         // [N] boundary class
@@ -76,6 +81,10 @@ struct LevelView {
     double *tau;                           // [9][N] stress tensor + heat flux
     double *prim;                          // [4][N] u, v, w, T of the viscous term
     NodeRec *q;                            // [N] written with p by k_pressure
+    // Spalart-Allmaras: nu~ is component 6 of u, uprev, rhs, src ([6][N])
+    double *turbDiff, *dtT, *vort, *divg;  // [N] diffusion, turbulent dt, |curl u|, div u
+    double *sag;                           // [3][N] Galerkin gradient of nu~
+    double *sanh;                          // [N] the cb2 term of the diffusion
     double *vdt;                           // [N]  V/dt of the dissipation
     double *wstress;                       // [3][N] wall stress (level 1)
     double *grad;                          // [15][N] (level 1, HLLC order 2)

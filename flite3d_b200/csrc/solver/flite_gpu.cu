@@ -48,7 +48,10 @@ const char *unsupported_reason(const flite_controls &c) {
         return "SAS, gust, moving-wall, patch initialisation and spanwise loads are not supported";
     if (c.residualSmoothingFactor > 0 || c.prolongationSmoothingFactor > 0)
         return "residual and prolongation smoothing are not supported";
-    if (c.turbulenceModel != 0) return "turbulenceModel != 0 is not supported yet";
+    if (c.turbulenceModel != 0 && c.turbulenceModel != 1)
+        return "turbulenceModel 2 and 3 (k-omega, SST) are not supported";
+    if (c.turbulenceModel == 1 && !(c.ReynoldsNumber > 0)) return "the Spalart-Allmaras model needs ReynoldsNumber > 0";
+    if (c.turbulenceModel == 1 && c.precision != FLITE_FP64) return "the Spalart-Allmaras model runs in FP64";
     if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return "viscosityScheme 2 is not supported";
     if (c.fluxType < 1 || c.fluxType > 4) return "fluxType must be 1..4";
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
@@ -102,6 +105,10 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         P.nsig = c->ReynoldsNumber < 1 ? 4 : 2;       // def_par:1592-1596
         P.isentropic = c->wallsAreIsentropic; P.viscous = c->ReynoldsNumber > 0.0;
         P.boundaryTerm = c->boundaryTerm; P.useDissW = c->useDissipationWeighting; P.ncfl = c->numberOfCFLIncrements;
+        P.sa = c->turbulenceModel == 1; P.nTurbGrids = c->numberOfTurbulenceGrids;
+        P.turbCFL = c->turbulentCFLNumber; P.turbK = c->turbK; P.maxTurb = c->maxTurbulenceValue;
+        P.turbProlRelax = c->turbProlongationRelaxation;
+        P.oPrt = c->turbulentPrandtlNumber > 0 ? 1. / c->turbulentPrandtlNumber : 0.0;
 
         int G = nlevels;
         if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);  // mg_par:1212-1214
@@ -114,7 +121,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             cyc0[0] = 1;  // setUpInitialField2 sets grid 1 (def_par:3992)
             CK(cudaMemcpy(X.d_cyc, cyc0.data(), G * sizeof(int), cudaMemcpyHostToDevice));
         }
-        X.d_part = X.alloc<double>(kResidBlocks * 15);
+        X.d_part = X.alloc<double>(kResidBlocks * 18);
         X.d_out = X.alloc<double>(32);
         X.lv.resize(G);
         for (int l = 0; l < G; ++l) {
@@ -232,6 +239,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             L.inc32 = nullptr;
             L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
             L.V = X.upload(std::vector<double>(d.volume, d.volume + N));
+            L.wdist = d.wall_dist ? X.upload(std::vector<double>(d.wall_dist, d.wall_dist + N))
+                                  : X.upload(std::vector<double>(N, 0.0));
             L.conn = X.upload(conn);
             L.nx = X.upload(nx); L.ny = X.upload(ny); L.nz = X.upload(nz); L.wallArea = X.upload(wa);
             double *dc = X.upload(coords);
@@ -261,13 +270,24 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
             }  // mesh upload
             // state
-            L.u = X.alloc<double>(5 * (size_t)N); L.uprev = X.alloc<double>(5 * (size_t)N);
-            L.rhs = X.alloc<double>(5 * (size_t)N); L.src = X.alloc<double>(5 * (size_t)N);
+            const size_t nv = (size_t)X.nvar();
+            L.u = X.alloc<double>(nv * N); L.uprev = X.alloc<double>(nv * N);
+            L.rhs = X.alloc<double>(nv * N); L.src = X.alloc<double>(nv * N);
             L.diss = X.alloc<double>(5 * (size_t)N);
             L.p = X.alloc<double>(N); L.dt = X.alloc<double>(N); L.mu = X.alloc<double>(N);
             L.hvis = X.alloc<double>(N);
-            for (double *a : {L.u, L.uprev, L.rhs, L.src, L.diss})
-                CK(cudaMemset(a, 0, 5 * (size_t)N * sizeof(double)));
+            for (double *a : {L.u, L.uprev, L.rhs, L.src})
+                CK(cudaMemset(a, 0, nv * N * sizeof(double)));
+            CK(cudaMemset(L.diss, 0, 5 * (size_t)N * sizeof(double)));
+            if (c->turbulenceModel == 1) {
+                L.turbDiff = X.alloc<double>(N); L.dtT = X.alloc<double>(N);
+                L.vort = X.alloc<double>(N); L.divg = X.alloc<double>(N);
+                L.sag = X.alloc<double>(3 * (size_t)N); L.sanh = X.alloc<double>(N);
+                for (double *a : {L.turbDiff, L.dtT, L.vort, L.divg, L.sanh})
+                    CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
+            } else {
+                L.turbDiff = L.dtT = L.vort = L.divg = L.sag = L.sanh = nullptr;
+            }
             for (double *a : {L.p, L.dt, L.mu, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
             const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
             const bool visc = c->ReynoldsNumber > 0.0;
@@ -309,6 +329,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
             L.cyc = X.d_cyc + l;
+            L.nvar = X.nvar();
         }
         CK(cudaDeviceSynchronize());
         return FLITE_OK;
@@ -337,7 +358,7 @@ int flite_set_state(flite_ctx *ctx, int level, const double *u) {
     if (bad_level(ctx, level) || !u) return FLITE_EINVAL;
     return guarded(ctx, [&] {
         LevelView &L = ctx->V(level - 1);
-        CK(cudaMemcpyAsync(L.u, u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, ctx->s));
+        CK(cudaMemcpyAsync(L.u, u, ctx->nvar() * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
         return FLITE_OK;
     });
@@ -347,7 +368,7 @@ int flite_get_state(flite_ctx *ctx, int level, double *u) {
     if (bad_level(ctx, level) || !u) return FLITE_EINVAL;
     return guarded(ctx, [&] {
         LevelView &L = ctx->V(level - 1);
-        CK(cudaMemcpyAsync(u, L.u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(u, L.u, ctx->nvar() * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
         return FLITE_OK;
     });
@@ -369,6 +390,10 @@ int flite_init_freestream(flite_ctx *ctx) {
         LevelView &L = ctx->V(0);
         for (int k = 0; k < 5; ++k)
             k_fill<<<flite_ctx::blocks(L.N), kBlock, 0, ctx->s>>>(L.u + (size_t)k * L.N, L.N, ctx->c.inflowField[k]);
+        // setUpInitialField2's freestream branch (def_par:3953-3963)
+        if (ctx->c.ReynoldsNumber > 0.0)
+            k_fill<<<flite_ctx::blocks(L.N), kBlock, 0, ctx->s>>>(L.mu, L.N, 1. / ctx->c.ReynoldsNumber);
+        if (ctx->P.sa) k_fill<<<flite_ctx::blocks(L.N), kBlock, 0, ctx->s>>>(L.u + 5 * (size_t)L.N, L.N, 0.1);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->s));
         return FLITE_OK;
@@ -399,9 +424,9 @@ int flite_start(flite_ctx *ctx) {
 }
 
 int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps, int calc_diss, int calc_turb, int cycle_no) {
-    (void)calc_turb;
     if (bad_level(ctx, level) || nsteps < 0) return FLITE_EINVAL;
     return guarded(ctx, [&] {
+        ctx->calcTurb = calc_turb != 0;
         ctx->set_cycle(cycle_no);
         ctx->doTimeIterations(level - 1, nsteps, calc_diss != 0);
         CK(cudaGetLastError());
@@ -411,9 +436,9 @@ int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps, int calc_dis
 }
 
 int flite_restrict(flite_ctx *ctx, int fine_level, int calc_turb) {
-    (void)calc_turb;
     if (bad_level(ctx, fine_level) || bad_level(ctx, fine_level + 1)) return FLITE_EINVAL;
     return guarded(ctx, [&] {
+        ctx->calcTurb = calc_turb != 0;
         ctx->restrictGrid(fine_level - 1);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->s));
@@ -444,6 +469,7 @@ int flite_map_fine_to_coarse(flite_ctx *ctx, int fine_level) {
 int flite_cycle(flite_ctx *ctx, int cycle_no) {
     if (!ctx) return FLITE_EINVAL;
     return guarded(ctx, [&] {
+        ctx->select_cycle(cycle_no);
         ctx->ensure_graph();
         ctx->set_cycle(cycle_no);
         CK(cudaGraphLaunch(ctx->graph, ctx->s));
@@ -458,16 +484,16 @@ int flite_residuals(flite_ctx *ctx, double res[7], double maxres[7], int32_t max
         flite_ctx &X = *ctx;
         const LevelView &L = X.c.multigridScheme > 0 ? X.V(0) : X.V((int)X.lv.size() - 1);
         k_resid_partial<<<kResidBlocks, 256, 0, X.s>>>(L, X.d_part, kResidBlocks);
-        k_resid_final<<<1, 160, 0, X.s>>>(X.d_part, kResidBlocks, X.d_out);
-        double h[15];
+        k_resid_final<<<1, 192, 0, X.s>>>(X.d_part, kResidBlocks, X.d_out);
+        double h[18];
         CK(cudaMemcpyAsync(h, X.d_out, sizeof h, cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
         for (int k = 0; k < 7; ++k) { res[k] = 0.0; maxres[k] = 0.0; maxind[k] = 1; }
         bool finite = true;
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < X.nvar(); ++k) {  // nres = 6 with SA (mg_par:1292-1293)
             res[k] = h[k];
-            maxres[k] = h[5 + k];
-            maxind[k] = (int32_t)h[10 + k] + 1;
+            maxres[k] = h[6 + k];
+            maxind[k] = (int32_t)h[12 + k] + 1;
             if (!std::isfinite(res[k])) finite = false;
         }
         if (!finite) return fail(ctx, FLITE_ENAN, "NaN in residual");
@@ -523,6 +549,7 @@ int flite_time_cycles(flite_ctx *ctx, int cycle_no, int ncycles, double *ms) {
     if (!ctx || ncycles < 1 || !ms) return FLITE_EINVAL;
     return guarded(ctx, [&] {
         flite_ctx &X = *ctx;
+        X.select_cycle(cycle_no);
         X.ensure_graph();
         X.set_cycle(cycle_no);
         cudaEvent_t a, b;

@@ -21,6 +21,7 @@
 
 #include "flux.cuh"
 #include "kernels.h"
+#include "pinned_math.h"
 
 namespace flite {
 
@@ -55,9 +56,10 @@ __global__ void k_timestep(Params P, LevelView L) {
         double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
         acc = (acc + fabs(vn)) + sqrt(cc * al);
         if (P.viscous) {
-            // the other node's viscous term (def_par:13432-13433)
+            // the other node's viscous term (def_par:13432-13433); with SA
+            // the viscosity is mu + nu~/Re
             int j = t.y;
-            double vis = dmax(P.am, L.mu[j]);
+            double vis = dmax(P.am, P.sa ? L.mu[j] + L.u[5 * N + j] / P.Re : L.mu[j]);
             double dv = 2.0 * vis * al / L.u[j];
             h = h + dv;
         }
@@ -80,7 +82,8 @@ __global__ void k_timestep(Params P, LevelView L) {
         if (side == 0) acc = (((acc + vn1) + vnm) + cc1) + ccm;
         else acc = (((acc + vn2) + vnm) + cc2) + ccm;
         if (P.viscous) {
-            double vis1 = dmax(P.am, L.mu[j1]), vis2 = dmax(P.am, L.mu[j2]);
+            double vis1 = dmax(P.am, P.sa ? L.mu[j1] + L.u[5 * N + j1] / P.Re : L.mu[j1]);
+            double vis2 = dmax(P.am, P.sa ? L.mu[j2] + L.u[5 * N + j2] / P.Re : L.mu[j2]);
             double dv1 = 2.0 * vis1 * al / L.u[j1];
             double dv2 = 2.0 * vis2 * al / L.u[j2];
             double dvm = dv1 + dv2;
@@ -256,6 +259,17 @@ __global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
     double mu = (1. / P.Re) * ((a * sqrt(a)) * ((P.Tinf + 198.6) / (tempConv * P.Tinf * T + 198.6)));
     double kc = (1. / P.Pr) * mu;
     L.mu[i] = mu;
+    if (P.sa) {
+        const double a1 = dudy - dvdx, a2 = dvdz - dwdy, a3 = dwdx - dudz;
+        L.vort[i] = sqrt((a1 * a1 + a2 * a2) + a3 * a3);
+        L.divg[i] = (dudx + dvdy) + dwdz;
+        // turbulent viscosity of the SA model (def_par:5556-5566)
+        double tvc = (1. / P.Re) * L.u[i] * L.u[5 * N + i];
+        const double ksi3 = flite_pm::pm_cube(tvc / mu);
+        tvc = tvc * ksi3 / (ksi3 + 357.9);
+        mu = mu + tvc;
+        kc = kc + tvc * P.oPrt;
+    }
     const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
     double tau[9];
     tau[0] = mu * (fourThirds * dudx - twoThirds * (dvdy + dwdz));
@@ -685,6 +699,9 @@ __global__ void __launch_bounds__(256, 3) k_node_update(Params P, LevelView L, i
     double n0 = 0, n1 = 0, n2 = 0;
     if (cls != BC_NONE) { n0 = L.nx[i]; n1 = L.ny[i]; n2 = L.nz[i]; }
     bc_increment(P, cls, n0, n1, n2, r);
+    // nullifyOuterBoundary (coarse levels): zeroes the far-field (indicator
+    // 3) increments for the SA model and is a no-op otherwise
+    if (P.sa && L.grid > 1 && cls == BC_FAR3) r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     const double dtJ = stage > 0 ? P.CFL * P.RK[stage - 1] : P.CFL;
     double d[5], up[5], un[5];
     for (int c = 0; c < 5; ++c) { d[c] = dtJ * r[c]; up[c] = L.uprev[c * N + i]; }
@@ -745,9 +762,17 @@ __device__ __forceinline__ void restrict_gather(const LevelView &C, const double
 __global__ void k_restrict_u(LevelView C, LevelView F) {
     int c = tid();
     if (c >= C.N) return;
-    double v[5];
-    restrict_gather(C, F.u, F.N, c, 5, v);
-    for (int k = 0; k < 5; ++k) C.u[k * C.N + c] = v[k];
+    double v[6];
+    restrict_gather(C, F.u, F.N, c, C.nvar, v);
+    for (int k = 0; k < C.nvar; ++k) C.u[k * C.N + c] = v[k];
+}
+
+// the nu~ solution conditions: zero on walls (def_par:4416-4418, 4446-4448,
+// 4469-4471), 0.1 on the far field (def_par:4076-4140)
+__device__ __forceinline__ double sa_bc_solution(unsigned char cls, double v) {
+    if (cls == BC_WALL || cls == BC_IWALL) return 0.0;
+    if (cls == BC_FAR3 || cls == BC_FAR4) return 0.1;
+    return v;
 }
 
 // restrictGrid head (def_par:12159-12185): C.u = R(F.u), C.mu = R(F.mu),
@@ -767,6 +792,13 @@ __global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
     bc_solution(P, cls, n0, n1, n2, 0.0, 0.0, 0.0, relax_param(P, *C.cyc), v);
     bc_outer(P, cls, n0, n1, n2, p0, v);
     for (int k = 0; k < 5; ++k) { C.u[k * N + c] = v[k]; C.uprev[k * N + c] = v[k]; }
+    if (P.sa) {
+        double t;
+        restrict_gather(C, F.u + 5 * (size_t)F.N, F.N, c, 1, &t);
+        t = sa_bc_solution(cls, t);
+        C.u[5 * N + c] = t;
+        C.uprev[5 * N + c] = t;
+    }
     C.p[c] = fabs(pressure(P, v[0], v[1], v[2], v[3], v[4]));
     store_node(C.q, c, v[0], v[1], v[2], v[3], v[4], C.p[c], m);
 }
@@ -788,6 +820,14 @@ __global__ void k_restrict_incr(Params P, LevelView C, LevelView F) {
         C.src[k * N + c] = C.src[k * N + c] - r[k];
         C.u[k * N + c] = C.u[k * N + c] + r[k];
     }
+    if (P.sa) {
+        double t;
+        restrict_gather(C, F.rhs + 5 * (size_t)F.N, F.N, c, 1, &t);
+        if (cls == BC_WALL || cls == BC_IWALL) t = 0.0;
+        C.rhs[5 * N + c] = t;
+        C.src[5 * N + c] = C.src[5 * N + c] - t;
+        C.u[5 * N + c] = C.u[5 * N + c] + t;
+    }
 }
 
 // prolongateGrid coarse part (def_par:12445-12468): uprev = R(F.u) with the
@@ -808,8 +848,20 @@ __global__ void k_prolong_coarse(Params P, LevelView C, LevelView F) {
         C.uprev[k * N + c] = v[k];
         r[k] = C.u[k * N + c] - v[k];
     }
+    double r6 = 0.0;
+    if (P.sa) {
+        double t;
+        restrict_gather(C, F.u + 5 * (size_t)F.N, F.N, c, 1, &t);
+        t = sa_bc_solution(cls, t);
+        C.uprev[5 * N + c] = t;
+        r6 = C.u[5 * N + c] - t;
+        // nullifyOuterBoundary, then the increment conditions
+        if (cls == BC_FAR3) { r[0] = r[1] = r[2] = r[3] = r[4] = 0.0; r6 = 0.0; }
+        if (cls == BC_WALL || cls == BC_IWALL) r6 = 0.0;
+    }
     bc_increment(P, cls, n0, n1, n2, r);
     for (int k = 0; k < 5; ++k) C.rhs[k * N + c] = r[k];
+    if (P.sa) C.rhs[5 * N + c] = r6;
 }
 
 // prolongateGrid fine part (def_par:12470-12567): injection, relaxation,
@@ -819,26 +871,33 @@ __global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
     if (i >= F.N) return;
     const int N = F.N;
     int pc = C.parent[i];
+    const unsigned char cls = F.bc[i];
+    // nullifyOuterBoundary of the injected correction (SA runs only)
+    const bool nul = P.sa && cls == BC_FAR3;
     double un[5];
     for (int k = 0; k < 5; ++k) un[k] = F.u[k * N + i];
-    if (pc >= 0) {
-        for (int k = 0; k < 5; ++k) {
-            double r = C.rhs[k * C.N + pc];
-            r = P.prolRelax * r;
-            if (i < F.Nb) r = P.mgBCRelax * r;
-            F.rhs[k * N + i] = r;
-            un[k] = un[k] + r;
-        }
-    } else {
-        for (int k = 0; k < 5; ++k) {
-            double r = F.rhs[k * N + i];
-            r = P.prolRelax * r;
-            if (i < F.Nb) r = P.mgBCRelax * r;
-            F.rhs[k * N + i] = r;
-            un[k] = un[k] + r;
-        }
+    for (int k = 0; k < 5; ++k) {
+        double r = pc >= 0 ? C.rhs[k * C.N + pc] : F.rhs[k * N + i];
+        if (nul) r = 0.0;
+        r = P.prolRelax * r;
+        if (i < F.Nb) r = P.mgBCRelax * r;
+        F.rhs[k * N + i] = r;
+        un[k] = un[k] + r;
     }
-    const unsigned char cls = F.bc[i];
+    double un6 = 0.0;
+    if (P.sa) {
+        double r = pc >= 0 ? C.rhs[5 * C.N + pc] : F.rhs[5 * N + i];
+        if (nul) r = 0.0;
+        r = P.turbProlRelax * r;
+        F.rhs[5 * N + i] = r;
+        un6 = F.u[5 * N + i];
+        // the nu~ correction reaches the levels finer than
+        // numberOfTurbulenceGrids (def_par:12540-12552)
+        if (F.grid < P.nTurbGrids) un6 = un6 + r;
+        un6 = sa_bc_solution(cls, un6);
+        un6 = dmax(un6, 0.0);
+        F.u[5 * N + i] = un6;
+    }
     double n0 = 0, n1 = 0, n2 = 0;
     if (cls != BC_NONE) { n0 = F.nx[i]; n1 = F.ny[i]; n2 = F.nz[i]; }
     double cm0 = 0, cm1 = 0, cm2 = 0;
@@ -855,7 +914,7 @@ __global__ void k_inject_u(LevelView C, LevelView F) {
     if (i >= F.N) return;
     int pc = C.parent[i];
     if (pc < 0) return;
-    for (int k = 0; k < 5; ++k) F.u[k * F.N + i] = C.u[k * C.N + pc];
+    for (int k = 0; k < F.nvar; ++k) F.u[k * F.N + i] = C.u[k * C.N + pc];
 }
 
 // setBCsOnSolutionField on a level's solution (start-up, def_par:3994)
@@ -871,6 +930,7 @@ __global__ void k_bc_solution(Params P, LevelView L) {
     if (cls == BC_WALL && P.viscous) { cm0 = L.cmx[i]; cm1 = L.cmy[i]; cm2 = L.cmz[i]; }
     bc_solution(P, cls, L.nx[i], L.ny[i], L.nz[i], cm0, cm1, cm2, relax_param(P, *L.cyc), un);
     for (int k = 0; k < 5; ++k) L.u[k * N + i] = un[k];
+    if (P.sa && (cls == BC_WALL || cls == BC_IWALL)) L.u[5 * N + i] = 0.0;
 }
 
 __global__ void k_set_int(int *dst, const int *src) {
@@ -880,25 +940,25 @@ __global__ void k_set_int(int *dst, const int *src) {
 // ---- residual norms (writeResiduals mg_par:1299-1443) ---------------------
 // per block: sum (u-uprev)^2 and max |u-uprev| with its first index
 __global__ void k_resid_partial(LevelView L, double *part, int nblk) {
-    __shared__ double ss[5][256];
-    __shared__ double sm[5][256];
-    __shared__ int si[5][256];
-    const int N = L.N;
-    double s[5] = {0, 0, 0, 0, 0}, m[5] = {0, 0, 0, 0, 0};
-    int mi[5] = {0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff};
+    __shared__ double ss[6][256];
+    __shared__ double sm[6][256];
+    __shared__ int si[6][256];
+    const int N = L.N, nv = L.nvar;
+    double s[6] = {0, 0, 0, 0, 0, 0}, m[6] = {0, 0, 0, 0, 0, 0};
+    int mi[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < nv; ++k) {
             double d = L.u[k * N + i] - L.uprev[k * N + i];
             s[k] = s[k] + d * d;
             double a = fabs(d);
             if (a > m[k]) { m[k] = a; mi[k] = i; }
         }
     }
-    for (int k = 0; k < 5; ++k) { ss[k][threadIdx.x] = s[k]; sm[k][threadIdx.x] = m[k]; si[k][threadIdx.x] = mi[k]; }
+    for (int k = 0; k < 6; ++k) { ss[k][threadIdx.x] = s[k]; sm[k][threadIdx.x] = m[k]; si[k][threadIdx.x] = mi[k]; }
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) {
-            for (int k = 0; k < 5; ++k) {
+            for (int k = 0; k < 6; ++k) {
                 ss[k][threadIdx.x] += ss[k][threadIdx.x + w];
                 double a = sm[k][threadIdx.x], b = sm[k][threadIdx.x + w];
                 int ia = si[k][threadIdx.x], ib = si[k][threadIdx.x + w];
@@ -908,26 +968,26 @@ __global__ void k_resid_partial(LevelView L, double *part, int nblk) {
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        for (int k = 0; k < 5; ++k) {
-            part[blockIdx.x * 15 + k] = ss[k][0];
-            part[blockIdx.x * 15 + 5 + k] = sm[k][0];
-            part[blockIdx.x * 15 + 10 + k] = (double)si[k][0];
+        for (int k = 0; k < 6; ++k) {
+            part[blockIdx.x * 18 + k] = ss[k][0];
+            part[blockIdx.x * 18 + 6 + k] = sm[k][0];
+            part[blockIdx.x * 18 + 12 + k] = (double)si[k][0];
         }
     }
 }
 
-// one warp per component (blockDim.x = 160); each lane folds the block
+// one warp per component (blockDim.x = 192); each lane folds the block
 // partials b = lane, lane+32, ... and the warp combines the lanes in a fixed
 // tree, so the result does not depend on timing
 __global__ void k_resid_final(const double *part, int nblk, double *out) {
     const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (k >= 5) return;
+    if (k >= 6) return;
     double s = 0, m = 0;
     int mi = 0x7fffffff;
     for (int b = lane; b < nblk; b += 32) {
-        s += part[b * 15 + k];
-        double v = part[b * 15 + 5 + k];
-        int iv = (int)part[b * 15 + 10 + k];
+        s += part[b * 18 + k];
+        double v = part[b * 18 + 6 + k];
+        int iv = (int)part[b * 18 + 12 + k];
         if (v > m || (v == m && iv < mi)) { m = v; mi = iv; }
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -938,8 +998,8 @@ __global__ void k_resid_final(const double *part, int nblk, double *out) {
     }
     if (lane == 0) {
         out[k] = sqrt(s);
-        out[5 + k] = m;
-        out[10 + k] = (double)(mi == 0x7fffffff ? 0 : mi);
+        out[6 + k] = m;
+        out[12 + k] = (double)(mi == 0x7fffffff ? 0 : mi);
     }
 }
 

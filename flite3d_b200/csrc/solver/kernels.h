@@ -25,6 +25,11 @@ enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 
 template <int PREC>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
 __global__ void k_delta_state(LevelView L);
+__global__ void k_sa_timestep(Params P, LevelView L);
+__global__ void k_sa_grad(Params P, LevelView L);
+__global__ void k_sa_diff(Params P, LevelView L);
+__global__ void k_sa_conv(Params P, LevelView L);
+__global__ void k_sa_stage(Params P, LevelView L, int mode, int stage, int turb);
 __global__ void k_make_inc32(const int2 *inc, const EdgeW *ew, int n, IncRec32 *o);
 __global__ void k_copy(const double *a, double *b, size_t n);
 __global__ void k_restrict_u(LevelView C, LevelView F);

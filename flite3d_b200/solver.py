@@ -286,6 +286,7 @@ class Batch:
             ng = m.nlevels if c.numberOfGridsToUse <= 0 else min(m.nlevels, c.numberOfGridsToUse)
             s.nlevels = ng
             s.nodes = [m.level(l + 1).n_nodes for l in range(ng)]
+            s.nvar = 6 if c.turbulenceModel == 1 else 5
             s.close = lambda: None  # owned by the batch
             self.cases.append(s)
 

@@ -1809,7 +1809,7 @@ int oracle_start(oracle_ctx *o) {
     const double mu = O.c.ReynoldsNumber > 0.0 ? 1. / O.c.ReynoldsNumber : 0.0;
     for (size_t l = 0; l < O.lv.size(); ++l) {
         std::fill(O.lv[l].mu.begin(), O.lv[l].mu.end(), mu);
-        if (l > 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].u, O.lv[l].u, 5);
+        if (l > 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].u, O.lv[l].u, O.nvar);
     }
     return FLITE_OK;
 }
@@ -1878,6 +1878,14 @@ int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[
 int oracle_forces(oracle_ctx *o, double out[6]) {
     if (!o || !out) return FLITE_EINVAL;
     o->o.forces(out);
+    return FLITE_OK;
+}
+
+// the pinned exp (which = 0) and log (which = 1) of the SA source term,
+// exported for their accuracy test
+int oracle_pinned_math(int which, const double *x, double *y, int n) {
+    if (!x || !y || n < 0) return FLITE_EINVAL;
+    for (int i = 0; i < n; ++i) y[i] = which == 0 ? flite_pm::pm_exp(x[i]) : flite_pm::pm_log(x[i]);
     return FLITE_OK;
 }
 

@@ -41,6 +41,8 @@ int oracle_forces(oracle_ctx *o, double out[6]);
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);
 /* one makeTimeSteps + dissipation evaluation at the level's current state */
 int oracle_eval_dissipation(oracle_ctx *o, int level);
+/* pinned exp (which 0) / log (which 1) of the SA source term            */
+int oracle_pinned_math(int which, const double *x, double *y, int n);
 /* threads of the timing mode (default 1 = the reference's loop order)  */
 int oracle_set_threads(int n);
 /* tangent (forward-mode) of the residual: jv = (dR/du) du               */
