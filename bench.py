@@ -116,7 +116,7 @@ def node_kernel_bytes(mesh):
     """Algorithmic bytes of one launch of the dominant kernel on level 1: the
     node kernel that computes the central fluxes of every incident edge and
     applies the RK stage update (measured in restrictGrid's fine-increment
-    mode, which has the stage's read set).  Per node: the 64-byte state
+    mode, which has the stage's read set).  Per node: the 48-byte state
     record (own and neighbours' reads of one array, counted once), uprev
     (40 B), dissipation (40 B), dt and volume (16 B), u(rho) (8 B), boundary
     class (1 B), two CSR offsets (8 B) and the result (40 B); per interior
@@ -124,7 +124,7 @@ def node_kernel_bytes(mesh):
     per boundary edge two incidence entries and two 40-byte contributions; per
     boundary node its normal (24 B)."""
     d = mesh.level(1)
-    return d.n_nodes * (64 + 40 + 40 + 16 + 8 + 1 + 8 + 40) + d.n_sides * 48 + d.n_bsides * 88 \
+    return d.n_nodes * (48 + 40 + 40 + 16 + 8 + 1 + 8 + 40) + d.n_sides * 48 + d.n_bsides * 88 \
         + d.n_bnodes * 24
 
 
@@ -151,6 +151,16 @@ def run_ours(args):
     solver = F.Solver(c, mesh)
     solver.set_state(u0)
     solver.start()
+    # pick the node-kernel launch options on this GPU (no effect on results)
+    tuning = {}
+    for nb in (128, 256):
+        for unroll in (1, 2):
+            solver.set_kernel_options(256, nb, unroll)
+            tuning[(nb, unroll)] = solver.profile_level(1, reps=5)[1]
+    best = min(tuning, key=tuning.get)
+    solver.set_kernel_options(256, best[0], best[1])
+    solver.set_state(u0)
+    solver.start()
     # warm-up (also captures the cycle graph)
     for i in range(1, args.warmup + 1):
         solver.cycle(i)
@@ -169,6 +179,9 @@ def run_ours(args):
     # adjoint cost ratio: one adjoint product against one forward residual
     # evaluation on level 1 (same level, FP64)
     fwd_ms, vjp_ms = solver.profile_adjoint(1, reps=20)
+    # device ms of the kernel groups of one level-1 relaxation step
+    kernels_l1 = solver.profile_kernels(1, reps=10)
+    kernels_coarse = {f"level{l}": solver.profile_kernels(l, reps=10) for l in range(2, solver.nlevels + 1)}
     hbm, peak_kind = _peaks()
     nbytes = node_kernel_bytes(mesh)
     achieved = nbytes / (node_ms / 1e3) / 1e9
@@ -261,6 +274,10 @@ def run_ours(args):
                                        "scaled by the units processed"},
         "clocks": clk.summary(),
         "residual_after_warmup": float(res[0]),
+        "level1_kernel_ms": kernels_l1,
+        "coarse_kernel_ms": kernels_coarse,
+        "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1]},
+                                "ms": {f"nb{k[0]}_unroll{k[1]}": v for k, v in tuning.items()}},
         "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,
                     "what": "flite_residual_vjp vs flite_residual_fwd kernels on level 1, FP64"},
     }
@@ -373,6 +390,55 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_batch(args):
+    """Batched solves: the bump channel at 120x40x40, 192x64x64 and
+    264x88x88 hexes x 16 flow conditions each (angle of attack uniform in
+    [-4, 8] degrees, Mach uniform in [0.3, 0.8], SplitMix64 seed 5), inviscid,
+    FLITE_MIXED.  One JSON line: case-cycles per second of one graph launch
+    per batch cycle against the cases' graphs launched one after another."""
+    import torch
+    import flite3d_b200 as F
+    from flite3d_b200.mesh import splitmix64
+    from flite3d_b200.solver import Batch
+    if not torch.cuda.is_available():
+        raise SystemExit("no CUDA device: the product path has no CPU fallback")
+    sizes = [(120, 40, 40), (192, 64, 64), (264, 88, 88)][:args.batch_meshes]
+    meshes = [F.Mesh.bump_channel(nx, ny, nz, 0.05, 4) for nx, ny, nz in sizes]
+    bits = splitmix64(5, 2 * args.batch_conditions) >> np.uint64(11)
+    uni = bits.astype(np.float64) / float(1 << 53)
+    cases = []
+    for m in meshes:
+        for k in range(args.batch_conditions):
+            alpha = -4.0 + 12.0 * uni[2 * k]
+            mach = 0.3 + 0.5 * uni[2 * k + 1]
+            c = F.default_controls(ReynoldsNumber=0.0, MachNumber=mach, alpha=alpha, CFLNumber=2.0,
+                                   fluxType=1, multigridScheme=3, numberOfGridsToUse=4, precision=1)
+            cases.append((c, m))
+    batch = Batch(cases)
+    for (c, m), s in zip(cases, batch.cases):
+        s.set_state(F.initial_state(c, m))
+        s.start()
+    e, nb, best = batch.autotune(reps=2)
+    for (c, m), s in zip(cases, batch.cases):
+        s.set_state(F.initial_state(c, m))
+        s.start()
+    batch.time_cycles(args.warmup)
+    ms_g, launches = batch.time_cycles(args.steps, cycle_no=args.warmup + 1, sequential=False)
+    ms_s, _ = batch.time_cycles(args.steps, cycle_no=args.warmup + args.steps + 1, sequential=True)
+    n = len(cases)
+    print(json.dumps({
+        "metric": "batched MG case-cycles/s", "value": n * args.steps / (ms_g / 1e3), "unit": "case-cycles/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_g / args.steps,
+        "higher_is_better": True, "dtype": "f32 flux increments / f64", "data": "synthetic",
+        "config": {"workload": f"{len(meshes)} bump-channel meshes {sizes} x {args.batch_conditions} "
+                               "conditions (alpha U[-4,8] deg, M U[0.3,0.8]), inviscid, FLITE_MIXED",
+                   "cases": n, "mesh_nodes": [m.level(1).n_nodes for m in meshes]},
+        "sequential": {"value": n * args.steps / (ms_s / 1e3), "ms_per_step": ms_s / args.steps},
+        "graph_vs_sequential": ms_s / ms_g, "kernel_launches_per_batch_cycle": launches,
+        "autotune": {"edge_block": e, "node_block": nb, "best_ms": best},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,6 +452,9 @@ def main():
     ap.add_argument("--converge", action="store_true",
                     help="also measure time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
     ap.add_argument("--converge-max", type=int, default=3000)
+    ap.add_argument("--batch", action="store_true", help="the batched multi-condition workload instead")
+    ap.add_argument("--batch-meshes", type=int, default=3)
+    ap.add_argument("--batch-conditions", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -393,6 +462,8 @@ def main():
         MESH["nx"], MESH["ny"], MESH["nz"] = [int(v) for v in args.mesh.split(",")]
     if args.impl == "reference":
         run_reference(args)
+    elif args.batch:
+        run_batch(args)
     else:
         run_ours(args)
 

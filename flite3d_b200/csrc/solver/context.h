@@ -61,6 +61,8 @@ struct flite_ctx {
     // threads per block of the edge kernels and of the node kernels (the
     // batch autotuner may change them; kernels with launch bounds take <= 256)
     int eb = kBlock, nb = kBlock;
+    // incidences per load batch of the fused central gather (1 or 2)
+    int unroll = 1;
     // calculateTurbulence of the cycle being run or captured (Spalart-
     // Allmaras: cycleNo <= numberOfTurbulenceSteps, mg_par:922-926), and the
     // value the instantiated graph was captured with
@@ -236,7 +238,8 @@ struct flite_ctx {
             if (anchor) k_node_update<GATHER_ANCHOR><<<g, nb, 0, s>>>(P, V(l), mode, stage);
             else k_node_update<GATHER_DELTA><<<g, nb, 0, s>>>(P, V(l), mode, stage);
         } else if (fused()) {
-            k_node_update<GATHER_CENTRAL><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            if (unroll == 2) k_node_update<GATHER_CENTRAL2><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            else k_node_update<GATHER_CENTRAL><<<g, nb, 0, s>>>(P, V(l), mode, stage);
         } else {
             k_node_update<GATHER_BUFFER><<<g, nb, 0, s>>>(P, V(l), mode, stage);
         }

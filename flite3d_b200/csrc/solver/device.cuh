@@ -34,8 +34,8 @@ struct __align__(16) IncRec32 {  // the same in FP32 (16 B); j is ~j when this
     float wx, wy, wz;            // node is the edge's second node
     int j;
 };
-struct __align__(16) NodeRec {  // conserved state, pressure, viscosity (64 B)
-    double r, ru, rv, rw, E, p, mu, pad;
+struct __align__(16) NodeRec {  // conserved state and pressure (48 B)
+    double r, ru, rv, rw, E, p;
 };
 struct __align__(16) DeltaRec {  // FP32 anchor primitives and increments (48 B)
     float ra, vax, vay, vaz, ha;  // anchor rho, velocity, E + p
@@ -80,7 +80,8 @@ struct LevelView {
     double *sens;                          // [N]  pressure sensor
     double *tau;                           // [9][N] stress tensor + heat flux
     double *prim;                          // [4][N] u, v, w, T of the viscous term
-    NodeRec *q;                            // [N] written with p by k_pressure
+    NodeRec *q;                            // [N] written with p by k_pressure (48 B: the level-1
+                                           // records of the bench mesh fit the 126 MB L2)
     // Spalart-Allmaras: nu~ is component 6 of u, uprev, rhs, src ([6][N])
     double *turbDiff, *dtT, *vort, *divg;  // [N] diffusion, turbulent dt, |curl u|, div u
     double *sag;                           // [3][N] Galerkin gradient of nu~
@@ -133,12 +134,12 @@ __device__ __forceinline__ void store_rec(R *base, int j, const R &o) {
 #pragma unroll
     for (int k = 0; k < K; ++k) p[k] = d[k];
 }
-__device__ __forceinline__ NodeRec load_node(const NodeRec *q, int j) { return load_rec<NodeRec, 4>(q, j); }
+__device__ __forceinline__ NodeRec load_node(const NodeRec *q, int j) { return load_rec<NodeRec, 3>(q, j); }
 __device__ __forceinline__ void store_node(NodeRec *q, int j, double r, double ru, double rv, double rw, double E,
-                                           double p, double mu) {
+                                           double p) {
     NodeRec o;
-    o.r = r; o.ru = ru; o.rv = rv; o.rw = rw; o.E = E; o.p = p; o.mu = mu; o.pad = 0.0;
-    store_rec<NodeRec, 4>(q, j, o);
+    o.r = r; o.ru = ru; o.rv = rv; o.rw = rw; o.E = E; o.p = p;
+    store_rec<NodeRec, 3>(q, j, o);
 }
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }

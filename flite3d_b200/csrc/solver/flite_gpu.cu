@@ -9,6 +9,8 @@
 // memory so the same graph serves every cycle.
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -610,6 +612,57 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, do
         for (auto &e : ev) cudaEventDestroy(e);
         *edge_ms = te / reps;
         *node_ms = tn / reps;
+        return FLITE_OK;
+    });
+}
+
+int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll) {
+    if (!ctx || edge_block < 32 || edge_block > 256 || node_block < 32 || node_block > 256 || edge_block % 32 ||
+        node_block % 32 || (gather_unroll != 1 && gather_unroll != 2))
+        return FLITE_EINVAL;
+    ctx->drop_graph();
+    ctx->eb = edge_block;
+    ctx->nb = node_block;
+    ctx->unroll = gather_unroll;
+    return FLITE_OK;
+}
+
+int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32_t nmax, int32_t *n) {
+    if (bad_level(ctx, level) || reps < 1 || !ms || !n || nmax < 1) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        const int l = level - 1;
+        LevelView &L = X.V(l);
+        // the kernels of one relaxation step of this level, in cycle order
+        std::vector<std::function<void()>> k;
+        k.push_back([&] { X.pressure(l); });
+        k.push_back([&] { X.timesteps(l); });
+        k.push_back([&] { X.dissipation(l); });
+        k.push_back([&] { if (X.c.ReynoldsNumber > 0) k_visc_prim<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
+        k.push_back([&] { if (X.c.ReynoldsNumber > 0) k_visc_grad<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
+        k.push_back([&] { if (X.c.ReynoldsNumber > 0) k_visc_flux<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
+        k.push_back([&] { X.rhs_terms(l, true); });
+        k.push_back([&] { X.launch_node_update(l, MODE_RFINE, 0, true); });
+        const int m = std::min<int>((int)k.size(), nmax);
+        std::vector<cudaEvent_t> ev(m + 1);
+        for (auto &e : ev) CK(cudaEventCreate(&e));
+        std::vector<double> acc(m, 0.0);
+        for (int r = 0; r < reps; ++r) {
+            CK(cudaEventRecord(ev[0], X.s));
+            for (int q = 0; q < m; ++q) {
+                k[q]();
+                CK(cudaEventRecord(ev[q + 1], X.s));
+            }
+            CK(cudaEventSynchronize(ev[m]));
+            for (int q = 0; q < m; ++q) {
+                float t = 0;
+                CK(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+                acc[q] += t;
+            }
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        for (int q = 0; q < m; ++q) ms[q] = acc[q] / reps;
+        *n = m;
         return FLITE_OK;
     });
 }

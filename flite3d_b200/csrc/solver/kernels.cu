@@ -35,7 +35,7 @@ __global__ void k_pressure(Params P, LevelView L) {
     const double r = L.u[i], ru = L.u[N + i], rv = L.u[2 * N + i], rw = L.u[3 * N + i], E = L.u[4 * N + i];
     const double p = pressure(P, r, ru, rv, rw, E);
     L.p[i] = p;
-    store_node(L.q, i, r, ru, rv, rw, E, p, L.mu[i]);
+    store_node(L.q, i, r, ru, rv, rw, E, p);
 }
 
 // ---- makeTimeSteps (def_par:13335-13610) as a node gather -----------------
@@ -597,6 +597,40 @@ __device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i,
     for (int c = 0; c < 5; ++c) r[c] = L.ra[c * N + i] + (double)acc[c];
 }
 
+// the same sum with the loads of two incidences issued before either flux
+// is computed (more loads in flight per thread); the additions stay in edge
+// order, so the result is the same bit for bit
+__device__ __forceinline__ void gather_interior_central2(const LevelView &L, int i, double *r) {
+    r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
+    const NodeRec m = load_node(L.q, i);
+    const NodeState si{m.r, m.ru, m.rv, m.rw, m.E, m.p};
+    const int end = L.inc_ptr[i + 1];
+    int k = L.inc_ptr[i];
+    auto add = [&](const int2 t, const EdgeW &w, const NodeRec &n) {
+        const NodeState sj{n.r, n.ru, n.rv, n.rw, n.E, n.p};
+        double f[5];
+        if (t.x >= 0) {
+            central_flux(si, sj, w.wx, w.wy, w.wz, f);
+            r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
+        } else {
+            central_flux(sj, si, w.wx, w.wy, w.wz, f);
+            r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
+        }
+    };
+    for (; k + 1 < end; k += 2) {
+        const int2 t0 = L.inc[k], t1 = L.inc[k + 1];
+        const EdgeW w0 = load_edgew(L.ew, t0.x >= 0 ? t0.x : ~t0.x);
+        const EdgeW w1 = load_edgew(L.ew, t1.x >= 0 ? t1.x : ~t1.x);
+        const NodeRec n0 = load_node(L.q, t0.y), n1 = load_node(L.q, t1.y);
+        add(t0, w0, n0);
+        add(t1, w1, n1);
+    }
+    if (k < end) {
+        const int2 t0 = L.inc[k];
+        add(t0, load_edgew(L.ew, t0.x >= 0 ? t0.x : ~t0.x), load_node(L.q, t0.y));
+    }
+}
+
 // interior central fluxes of node i computed from the two node records of
 // each incident edge, summed in edge order: the same numbers, in the same
 // order, as the edge kernel followed by the buffer gather
@@ -674,7 +708,8 @@ __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const do
 // same, stored as the new mixed-precision anchor), GATHER_DELTA (anchor +
 // FP32 increments)
 template <int PREC>
-__global__ void __launch_bounds__(256, 3) k_node_update(Params P, LevelView L, int mode, int stage) {
+__global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : 3)
+    k_node_update(Params P, LevelView L, int mode, int stage) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -683,6 +718,8 @@ __global__ void __launch_bounds__(256, 3) k_node_update(Params P, LevelView L, i
         gather_interior_delta(L, i, r);
     } else if constexpr (PREC == GATHER_BUFFER) {
         gather_interior(L, i, r);
+    } else if constexpr (PREC == GATHER_CENTRAL2) {
+        gather_interior_central2(L, i, r);
     } else {
         gather_interior_central(L, i, r);
         if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, r);
@@ -736,6 +773,7 @@ __global__ void __launch_bounds__(256, 3) k_node_update(Params P, LevelView L, i
 }
 template __global__ void k_node_update<GATHER_BUFFER>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_DELTA>(Params, LevelView, int, int);
 
@@ -800,7 +838,7 @@ __global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
         C.uprev[5 * N + c] = t;
     }
     C.p[c] = fabs(pressure(P, v[0], v[1], v[2], v[3], v[4]));
-    store_node(C.q, c, v[0], v[1], v[2], v[3], v[4], C.p[c], m);
+    store_node(C.q, c, v[0], v[1], v[2], v[3], v[4], C.p[c]);
 }
 
 // restrictGrid tail (def_par:12385-12427): C.rhs = R(F.rhs), increment

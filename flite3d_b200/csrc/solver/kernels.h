@@ -21,7 +21,7 @@ __global__ void k_minmax(Params P, LevelView L);
 template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 __global__ void k_bnd_flux(Params P, LevelView L);
-enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3 };
+enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3, GATHER_CENTRAL2 = 4 };
 template <int PREC>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
 __global__ void k_delta_state(LevelView L);

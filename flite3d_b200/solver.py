@@ -186,6 +186,20 @@ class Solver:
         self._ck(self.be.residual_jvp(self._h, level, _ptr(u), _ptr(du), _ptr(jv)), "residual_jvp")
         return jv
 
+    def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1):
+        self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll),
+                 "set_kernel_options")
+
+    KERNEL_GROUPS = ("pressure", "timestep", "dissipation", "visc_prim", "visc_grad", "visc_flux",
+                     "flux_terms", "node_update")
+
+    def profile_kernels(self, level=1, reps=10):
+        """{kernel group: average device ms} over one relaxation step of a level."""
+        ms = (ctypes.c_double * 16)()
+        n = ctypes.c_int32()
+        self._ck(self.be.profile_kernels(self._h, level, reps, ms, 16, ctypes.byref(n)), "profile_kernels")
+        return {k: ms[i] for i, k in enumerate(self.KERNEL_GROUPS[:n.value])}
+
     def profile_adjoint(self, level=1, reps=10):
         """(forward ms, adjoint ms) per residual evaluation on a level."""
         a, b = ctypes.c_double(), ctypes.c_double()

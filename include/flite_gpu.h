@@ -251,6 +251,18 @@ int flite_cycle_launches(flite_ctx *ctx, int64_t *n);
  * of the node gather/update kernel.                                        */
 int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms,
                         double *node_ms);
+/* Launch options of a context (no effect on any result): threads per block
+ * of the edge kernels and of the node kernels (32..256, multiples of 32) and
+ * the incidences whose loads the fused central gather issues together (1 or
+ * 2).  Drops the captured cycle graph.                                     */
+int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll);
+/* Average device ms of the kernel groups of one relaxation step of a level,
+ * in order: pressure, time steps, dissipation, viscous primitives, viscous
+ * gradients, viscous fluxes, flux terms (edge or boundary kernels), node
+ * update (restrictGrid's fine-increment mode: the stage's read set); *n is
+ * the number written (at most nmax).  The level's rhs and dissipation are
+ * overwritten.                                                              */
+int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32_t nmax, int32_t *n);
 
 #ifdef __cplusplus
 }

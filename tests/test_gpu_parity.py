@@ -157,3 +157,14 @@ def test_convergence_history_matches(mesh):
         o.cycle(cyc)
     assert_same_state(g, o, "30 cycles")
     np.testing.assert_allclose(g.residuals()[0], o.residuals()[0], rtol=RTOL_REDUCTION)
+
+
+@pytest.mark.parametrize("opts", [(128, 128, 2), (64, 256, 1), (256, 64, 2)])
+def test_launch_options_do_not_change_results(opts):
+    mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+    c, g, o = make_pair(mesh, fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=1)
+    g.set_kernel_options(*opts)
+    for cyc in range(1, 4):
+        g.cycle(cyc)
+        o.cycle(cyc)
+    assert_same_state(g, o, f"options {opts}")
