@@ -27,6 +27,8 @@ CASES = {
                   CFLNumber=2.0, numberOfGridsToUse=3, multigridScheme=3),
     "laminar": dict(ReynoldsNumber=5000.0, fluxType=1, CFLNumber=2.0, numberOfGridsToUse=3,
                     multigridScheme=3, wallsAreIsentropic=1),
+    "sa": dict(ReynoldsNumber=1.0e5, fluxType=1, CFLNumber=1.0, numberOfGridsToUse=3,
+               multigridScheme=3, wallsAreIsentropic=1, turbulenceModel=1),
 }
 MESH = (12, 4, 4)
 
@@ -37,7 +39,10 @@ def main():
     b.build_oracle()
     lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
     mesh = Mesh.bump_channel(*MESH, 0.05, nlevels=3)
+    only = sys.argv[1:] or list(CASES)
     for name, ctl in CASES.items():
+        if name not in only:
+            continue
         c = default_controls(**ctl)
         o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
         o.set_state(initial_state(c, mesh, perturb_seed=20261203))
