@@ -34,8 +34,8 @@ struct __align__(16) IncRec32 {  // the same in FP32 (16 B); j is ~j when this
     float wx, wy, wz;            // node is the edge's second node
     int j;
 };
-struct __align__(16) NodeRec {  // conserved state and pressure (48 B)
-    double r, ru, rv, rw, E, p;
+struct __align__(16) NodeRec {  // what the central flux reads of a node (48 B)
+    double ru, rv, rw, rinv, p, rh;  // momentum, 1/rho, pressure, E + p
 };
 struct __align__(16) DeltaRec {  // FP32 anchor primitives and increments (48 B)
     float ra, vax, vay, vaz, ha;  // anchor rho, velocity, E + p
@@ -135,10 +135,12 @@ __device__ __forceinline__ void store_rec(R *base, int j, const R &o) {
     for (int k = 0; k < K; ++k) p[k] = d[k];
 }
 __device__ __forceinline__ NodeRec load_node(const NodeRec *q, int j) { return load_rec<NodeRec, 3>(q, j); }
+// 1/rho and E + p are the operations the central flux performs per edge
+// end, done once per node
 __device__ __forceinline__ void store_node(NodeRec *q, int j, double r, double ru, double rv, double rw, double E,
                                            double p) {
     NodeRec o;
-    o.r = r; o.ru = ru; o.rv = rv; o.rw = rw; o.E = E; o.p = p;
+    o.ru = ru; o.rv = rv; o.rw = rw; o.rinv = 1. / r; o.p = p; o.rh = E + p;
     store_rec<NodeRec, 3>(q, j, o);
 }
 

@@ -60,6 +60,21 @@ __device__ __forceinline__ void central_flux(const NodeState &a, const NodeState
     f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
 }
 
+// the same central flux from two node records (1/rho and E + p formed once
+// per node by k_pressure with the same operations)
+__device__ __forceinline__ void central_flux_rec(const NodeRec &a, const NodeRec &b, double wx, double wy,
+                                                 double wz, double *f) {
+    const double pr1 = a.p, rinv1 = a.rinv, ru1 = a.ru, rv1 = a.rv, rw1 = a.rw, rh1 = a.rh;
+    const double u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1;
+    const double pr2 = b.p, rinv2 = b.rinv, ru2 = b.ru, rv2 = b.rv, rw2 = b.rw, rh2 = b.rh;
+    const double u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2;
+    f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
+    f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
+    f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
+    f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+    f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+}
+
 // Interior edge flux f of edge e (i1 -> i2), added to rhs(i1) and
 // subtracted from rhs(i2).  FT is the fluxType and O2 selects the HLLC
 // reconstruction; both are compile-time so that each kernel instance only

@@ -602,18 +602,17 @@ __device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i,
 // order, so the result is the same bit for bit
 __device__ __forceinline__ void gather_interior_central2(const LevelView &L, int i, double *r) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
-    const NodeRec m = load_node(L.q, i);
-    const NodeState si{m.r, m.ru, m.rv, m.rw, m.E, m.p};
+    const NodeRec si = load_node(L.q, i);
     const int end = L.inc_ptr[i + 1];
     int k = L.inc_ptr[i];
     auto add = [&](const int2 t, const EdgeW &w, const NodeRec &n) {
-        const NodeState sj{n.r, n.ru, n.rv, n.rw, n.E, n.p};
+        const NodeRec &sj = n;
         double f[5];
         if (t.x >= 0) {
-            central_flux(si, sj, w.wx, w.wy, w.wz, f);
+            central_flux_rec(si, sj, w.wx, w.wy, w.wz, f);
             r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
         } else {
-            central_flux(sj, si, w.wx, w.wy, w.wz, f);
+            central_flux_rec(sj, si, w.wx, w.wy, w.wz, f);
             r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
         }
     };
@@ -636,20 +635,19 @@ __device__ __forceinline__ void gather_interior_central2(const LevelView &L, int
 // order, as the edge kernel followed by the buffer gather
 __device__ __forceinline__ void gather_interior_central(const LevelView &L, int i, double *r) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
-    const NodeRec m = load_node(L.q, i);
-    const NodeState si{m.r, m.ru, m.rv, m.rw, m.E, m.p};
+    const NodeRec si = load_node(L.q, i);
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         const int2 t = L.inc[k];
         const int e = t.x >= 0 ? t.x : ~t.x;
         const EdgeW w = load_edgew(L.ew, e);
         const NodeRec n = load_node(L.q, t.y);
-        const NodeState sj{n.r, n.ru, n.rv, n.rw, n.E, n.p};
+        const NodeRec &sj = n;
         double f[5];
         if (t.x >= 0) {
-            central_flux(si, sj, w.wx, w.wy, w.wz, f);
+            central_flux_rec(si, sj, w.wx, w.wy, w.wz, f);
             r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
         } else {
-            central_flux(sj, si, w.wx, w.wy, w.wz, f);
+            central_flux_rec(sj, si, w.wx, w.wy, w.wz, f);
             r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
         }
     }
