@@ -151,14 +151,24 @@ def run_ours(args):
     solver = F.Solver(c, mesh)
     solver.set_state(u0)
     solver.start()
-    # pick the node-kernel launch options on this GPU (no effect on results)
+    # pick the launch options on this GPU (none changes a result): node-kernel
+    # block size and gather unroll by the level-1 node kernel, then the level
+    # size below which gathers use a warp per node by the time of whole cycles
     tuning = {}
     for nb in (128, 256):
         for unroll in (1, 2):
             solver.set_kernel_options(256, nb, unroll)
             tuning[(nb, unroll)] = solver.profile_level(1, reps=5)[1]
     best = min(tuning, key=tuning.get)
-    solver.set_kernel_options(256, best[0], best[1])
+    warp_tune = {}
+    for below in sorted({0, 8192} | {mesh.level(l).n_nodes + 1 for l in range(2, mesh.nlevels + 1)}):
+        solver.set_kernel_options(256, best[0], best[1], below)
+        solver.set_state(u0)
+        solver.start()
+        solver.time_cycles(2)
+        warp_tune[below] = solver.time_cycles(10, cycle_no=3) / 10
+    warp_below = min(warp_tune, key=warp_tune.get)
+    solver.set_kernel_options(256, best[0], best[1], warp_below)
     solver.set_state(u0)
     solver.start()
     # warm-up (also captures the cycle graph)
@@ -276,7 +286,9 @@ def run_ours(args):
         "residual_after_warmup": float(res[0]),
         "level1_kernel_ms": kernels_l1,
         "coarse_kernel_ms": kernels_coarse,
-        "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1]},
+        "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1],
+                                           "warp_gather_below": warp_below},
+                                "cycle_ms_by_warp_threshold": {str(k): v for k, v in warp_tune.items()},
                                 "ms": {f"nb{k[0]}_unroll{k[1]}": v for k, v in tuning.items()}},
         "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,
                     "what": "flite_residual_vjp vs flite_residual_fwd kernels on level 1, FP64"},

@@ -114,6 +114,13 @@ struct flite_ctx {
 
     // ---- single-grid building blocks ------------------------------------
     LevelView &V(int l) { return lv[l].v; }
+    // small levels gather with a warp per node (the lanes load and evaluate
+    // the incidences in parallel, the sums keep their order): there a
+    // thread per node leaves most SMs idle and each thread waits on a long
+    // chain of dependent loads
+    int small_nodes = kSmallLevelNodes;
+    bool small(int l) const { return lv[l].v.N < small_nodes; }
+    unsigned wblk(int l) const { return (unsigned)((32 * (size_t)lv[l].v.N + nb - 1) / nb); }
 
     void pressure(int l) {
         counted();
@@ -121,7 +128,8 @@ struct flite_ctx {
     }
     void timesteps(int l) {
         counted();
-        k_timestep<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        if (small(l)) k_timestep<32><<<wblk(l), nb, 0, s>>>(P, V(l));
+        else k_timestep<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
     void zero_diss(int l) {
         counted();
@@ -136,13 +144,15 @@ struct flite_ctx {
             return;
         }
         counted();
-        k_jst_lap<<<nblk(L.N), nb, 0, s>>>(P, L);
+        if (small(l)) k_jst_lap<32><<<wblk(l), nb, 0, s>>>(P, L);
+        else k_jst_lap<1><<<nblk(L.N), nb, 0, s>>>(P, L);
         counted();
-        k_jst_flux<<<nblk(L.N), nb, 0, s>>>(P, L);
+        if (small(l)) k_jst_flux<32><<<wblk(l), nb, 0, s>>>(P, L);
+        else k_jst_flux<1><<<nblk(L.N), nb, 0, s>>>(P, L);
     }
     void first_order_diss(int l) {
         counted();
-        k_first_order_diss<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        k_first_order_diss<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
     // dissipation choice of singleIteration (def_par:1030-1036)
     void dissipation(int l) {
@@ -155,9 +165,11 @@ struct flite_ctx {
         counted();
         k_visc_prim<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
         counted();
-        k_visc_grad<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        if (small(l)) k_visc_grad<32><<<wblk(l), nb, 0, s>>>(P, V(l));
+        else k_visc_grad<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
         counted();
-        k_visc_flux<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        if (small(l)) k_visc_flux<32><<<wblk(l), nb, 0, s>>>(P, V(l));
+        else k_visc_flux<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
     // ---- Spalart-Allmaras ----------------------------------------------
     void sa_timesteps(int l) {
@@ -233,15 +245,20 @@ struct flite_ctx {
         launch_node_update(l, mode, stage, anchor);
     }
     void launch_node_update(int l, int mode, int stage, bool anchor) {
-        const unsigned g = nblk(V(l).N);
+        if (small(l)) launch_node_update_u<32>(l, mode, stage, anchor);
+        else launch_node_update_u<1>(l, mode, stage, anchor);
+    }
+    template <int U>
+    void launch_node_update_u(int l, int mode, int stage, bool anchor) {
+        const unsigned g = U == 32 ? wblk(l) : nblk(V(l).N);
         if (mixed()) {
-            if (anchor) k_node_update<GATHER_ANCHOR><<<g, nb, 0, s>>>(P, V(l), mode, stage);
-            else k_node_update<GATHER_DELTA><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            if (anchor) k_node_update<GATHER_ANCHOR, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            else k_node_update<GATHER_DELTA, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
         } else if (fused()) {
-            if (unroll == 2) k_node_update<GATHER_CENTRAL2><<<g, nb, 0, s>>>(P, V(l), mode, stage);
-            else k_node_update<GATHER_CENTRAL><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            if (unroll == 2 && U == 1) k_node_update<GATHER_CENTRAL2, 1><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            else k_node_update<GATHER_CENTRAL, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
         } else {
-            k_node_update<GATHER_BUFFER><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            k_node_update<GATHER_BUFFER, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
         }
     }
 

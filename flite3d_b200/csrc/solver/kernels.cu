@@ -27,6 +27,20 @@ namespace flite {
 
 static __device__ __forceinline__ int tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
+// Warp-per-node gathers (small levels): lane l computes the terms of
+// incidence k0 + l; the warp then applies them to the node's accumulators in
+// incidence order, every lane doing the same additions on the broadcast
+// terms, so the sums are those of the serial loop bit for bit.
+template <int K, class Fn>
+__device__ __forceinline__ void warp_ordered(const double (&v)[K], int n, Fn &&fn) {
+    for (int q = 0; q < n; ++q) {
+        double x[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) x[c] = __shfl_sync(0xffffffffu, v[c], q);
+        fn(x);
+    }
+}
+
 // ---- makePressureField (def_par:13612-13630) ------------------------------
 __global__ void k_pressure(Params P, LevelView L) {
     int i = tid();
@@ -39,8 +53,10 @@ __global__ void k_pressure(Params P, LevelView L) {
 }
 
 // ---- makeTimeSteps (def_par:13335-13610) as a node gather -----------------
+template <int U>
 __global__ void k_timestep(Params P, LevelView L) {
-    int i = tid();
+    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
+    const int i = U == 32 ? tid() >> 5 : tid();
     if (i >= L.N) return;
     const int N = L.N;
     const double c1 = P.gamma;
@@ -48,6 +64,31 @@ __global__ void k_timestep(Params P, LevelView L) {
     const double m1 = L.u[N + i], m2 = L.u[2 * N + i], m3 = L.u[3 * N + i];
     const double cc = dmax(c1 * L.p[i] * ro, 0.001);
     double acc = 0.0, h = 0.0;
+    if constexpr (U == 32) {
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            const int k = k0 + lane;
+            double v[3] = {0.0, 0.0, 0.0};
+            if (k < end) {
+                const int2 t = L.inc[k];
+                const int e = t.x >= 0 ? t.x : ~t.x;
+                const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
+                const double al = (wx * wx + wy * wy) + wz * wz;
+                const double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
+                v[0] = fabs(vn);
+                v[1] = sqrt(cc * al);
+                if (P.viscous) {
+                    const int j = t.y;
+                    const double vis = dmax(P.am, P.sa ? L.mu[j] + L.u[5 * N + j] / P.Re : L.mu[j]);
+                    v[2] = 2.0 * vis * al / L.u[j];
+                }
+            }
+            warp_ordered<3>(v, min(32, end - k0), [&](const double *x) {
+                acc = (acc + x[0]) + x[1];
+                if (P.viscous) h = h + x[2];
+            });
+        }
+    } else
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
         int e = t.x >= 0 ? t.x : ~t.x;
@@ -64,7 +105,7 @@ __global__ void k_timestep(Params P, LevelView L) {
             h = h + dv;
         }
     }
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+    auto bterms = [&](int k, double *v) {
         int b = L.binc[k] >> 1, side = L.binc[k] & 1;
         int2 nd = L.bedge[b];
         double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
@@ -76,19 +117,39 @@ __global__ void k_timestep(Params P, LevelView L) {
         double vn1 = ((wx * L.u[N + j1] + wy * L.u[2 * N + j1]) + wz * L.u[3 * N + j1]) * ro1;
         double vn2 = ((wx * L.u[N + j2] + wy * L.u[2 * N + j2]) + wz * L.u[3 * N + j2]) * ro2;
         vn1 = fabs(vn1); vn2 = fabs(vn2);
-        double vnm = vn1 + vn2;
         cc1 = sqrt(cc1 * al); cc2 = sqrt(cc2 * al);
-        double ccm = cc1 + cc2;
-        if (side == 0) acc = (((acc + vn1) + vnm) + cc1) + ccm;
-        else acc = (((acc + vn2) + vnm) + cc2) + ccm;
+        v[0] = side == 0 ? vn1 : vn2;
+        v[1] = vn1 + vn2;
+        v[2] = side == 0 ? cc1 : cc2;
+        v[3] = cc1 + cc2;
         if (P.viscous) {
             double vis1 = dmax(P.am, P.sa ? L.mu[j1] + L.u[5 * N + j1] / P.Re : L.mu[j1]);
             double vis2 = dmax(P.am, P.sa ? L.mu[j2] + L.u[5 * N + j2] / P.Re : L.mu[j2]);
             double dv1 = 2.0 * vis1 * al / L.u[j1];
             double dv2 = 2.0 * vis2 * al / L.u[j2];
-            double dvm = dv1 + dv2;
-            h = side == 0 ? (h + dv1) + dvm : (h + dv2) + dvm;
+            v[4] = side == 0 ? dv1 : dv2;
+            v[5] = dv1 + dv2;
+        } else {
+            v[4] = v[5] = 0.0;
         }
+    };
+    auto badd = [&](const double *x) {
+        acc = (((acc + x[0]) + x[1]) + x[2]) + x[3];
+        if (P.viscous) h = (h + x[4]) + x[5];
+    };
+    if constexpr (U == 32) {
+        const int beg = L.binc_ptr[i], end = L.binc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            double v[6] = {0, 0, 0, 0, 0, 0};
+            if (k0 + lane < end) bterms(k0 + lane, v);
+            warp_ordered<6>(v, min(32, end - k0), badd);
+        }
+        if (lane) return;
+    } else
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        double v[6];
+        bterms(k, v);
+        badd(v);
     }
     const double V = L.V[i];
     const double dt = 0.5 / (acc / V + h / (V * V));
@@ -98,13 +159,46 @@ __global__ void k_timestep(Params P, LevelView L) {
 
 // ---- makeArtificialDissipation2, passes 1-2 and the node finish -----------
 // (def_par:11513-11780): undivided Laplacian with dE+dp, pressure sensor
+template <int U>
 __global__ void k_jst_lap(Params P, LevelView L) {
-    int i = tid();
+    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
+    const int i = U == 32 ? tid() >> 5 : tid();
     if (i >= L.N) return;
     const int N = L.N;
     double l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, s7 = 0, s8 = 0;
     const double ui0 = L.u[i], ui1 = L.u[N + i], ui2 = L.u[2 * N + i], ui3 = L.u[3 * N + i], ui4 = L.u[4 * N + i];
     const double pi = L.p[i];
+    if constexpr (U == 32) {
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            const int k = k0 + lane;
+            double v[7] = {0, 0, 0, 0, 0, 0, 0};
+            if (k < end) {
+                const int2 t = L.inc[k];
+                const int j = t.y;
+                double df = 1.0;
+                if (P.useDissW) df = 1. / L.slen[t.x >= 0 ? t.x : ~t.x];
+                const double uj0 = L.u[j], uj1 = L.u[N + j], uj2 = L.u[2 * N + j], uj3 = L.u[3 * N + j];
+                const double uj4 = L.u[4 * N + j], pj = L.p[j];
+                // x - y is x + (-y): the subtractions of the serial loop become
+                // additions of negated terms
+                if (t.x >= 0) {
+                    v[0] = -((ui0 - uj0) * df); v[1] = -((ui1 - uj1) * df); v[2] = -((ui2 - uj2) * df);
+                    v[3] = -((ui3 - uj3) * df); v[4] = -((((ui4 - uj4) + pi) - pj) * df);
+                    v[5] = -(pi - pj); v[6] = pi + pj;
+                } else {
+                    v[0] = (uj0 - ui0) * df; v[1] = (uj1 - ui1) * df; v[2] = (uj2 - ui2) * df;
+                    v[3] = (uj3 - ui3) * df; v[4] = (((uj4 - ui4) + pj) - pi) * df;
+                    v[5] = pj - pi; v[6] = pj + pi;
+                }
+            }
+            warp_ordered<7>(v, min(32, end - k0), [&](const double *x) {
+                l0 = l0 + x[0]; l1 = l1 + x[1]; l2 = l2 + x[2]; l3 = l3 + x[3]; l4 = l4 + x[4];
+                s7 = s7 + x[5]; s8 = s8 + x[6];
+            });
+        }
+        if (lane) return;
+    } else
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
         int j = t.y;
@@ -136,8 +230,10 @@ __global__ void k_jst_lap(Params P, LevelView L) {
 }
 
 // ---- makeArtificialDissipation2, pass 3 (def_par:11770-11906), scalar -----
-__global__ void __launch_bounds__(256, 3) k_jst_flux(Params P, LevelView L) {
-    int i = tid();
+template <int U>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_jst_flux(Params P, LevelView L) {
+    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
+    const int i = U == 32 ? tid() >> 5 : tid();
     if (i >= L.N) return;
     const int N = L.N;
     const double k4 = L.grid == 1 ? P.k4 : P.cgdf;
@@ -145,6 +241,39 @@ __global__ void __launch_bounds__(256, 3) k_jst_flux(Params P, LevelView L) {
     double Li[5], Ui[5];
     for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
     const double vdi = L.vdt[i], coni = L.conn[i], si = L.sens[i];
+    if constexpr (U == 32) {
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            const int k = k0 + lane;
+            double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (k < end) {
+                const int2 t = L.inc[k];
+                const int j = t.y;
+                const double vdj = L.vdt[j];
+                const bool first = t.x >= 0;
+                double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
+                d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
+                const double sj = L.sens[j];
+                const double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
+                double d4 = d0 * k4;
+                d4 = d4 > d2 ? d4 - d2 : 0.0;
+                for (int c = 0; c < 5; ++c) {
+                    const double Lj = L.lap[c * N + j], Uj = L.u[c * N + j];
+                    if (first) {
+                        v[2 * c] = -((Li[c] - Lj) * d4);
+                        v[2 * c + 1] = (Ui[c] - Uj) * d2;
+                    } else {
+                        v[2 * c] = (Lj - Li[c]) * d4;
+                        v[2 * c + 1] = -((Uj - Ui[c]) * d2);
+                    }
+                }
+            }
+            warp_ordered<10>(v, min(32, end - k0), [&](const double *x) {
+                for (int c = 0; c < 5; ++c) acc[c] = (acc[c] + x[2 * c]) + x[2 * c + 1];
+            });
+        }
+        if (lane) return;
+    } else
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
         int j = t.y;
@@ -171,6 +300,7 @@ __global__ void __launch_bounds__(256, 3) k_jst_flux(Params P, LevelView L) {
 }
 
 // ---- makeArtificialDissipation3 (def_par:11995-12139) ---------------------
+template <int U>
 __global__ void k_first_order_diss(Params P, LevelView L) {
     int i = tid();
     if (i >= L.N) return;
@@ -211,8 +341,10 @@ __global__ void k_visc_prim(Params P, LevelView L) {
     L.prim[3 * N + i] = gOg * L.p[i] / r;
 }
 
-__global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
-    int i = tid();
+template <int U>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, LevelView L) {
+    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
+    const int i = U == 32 ? tid() >> 5 : tid();
     if (i >= L.N) return;
     const int N = L.N;
     const double gOg = P.gamma / (P.gamma - 1.0);
@@ -223,7 +355,7 @@ __global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
     };
     double qi[4];
     prim(i, qi);
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+    auto iterms = [&](int k, double *d) {
         int2 t = L.inc[k];
         int e = t.x >= 0 ? t.x : ~t.x;
         double qj[4];
@@ -231,11 +363,11 @@ __global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
         const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
         for (int a = 0; a < 3; ++a)
             for (int c = 0; c < 4; ++c) {
-                double d = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
-                g[a * 4 + c] = t.x >= 0 ? g[a * 4 + c] + d : g[a * 4 + c] - d;
+                double x = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
+                d[a * 4 + c] = t.x >= 0 ? x : -x;  // g - x is g + (-x)
             }
-    }
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+    };
+    auto bterms = [&](int k, double *d) {
         int b = L.binc[k] >> 1, side = L.binc[k] & 1;
         int2 nd = L.bedge[b];
         double q1[4], q2[4];
@@ -243,10 +375,39 @@ __global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
         const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
         for (int a = 0; a < 3; ++a)
             for (int c = 0; c < 4; ++c) {
-                double s = q1[c] + q2[c];
+                double sm = q1[c] + q2[c];
                 double own = side == 0 ? q1[c] : q2[c];
-                g[a * 4 + c] = g[a * 4 + c] + (2. * own + s) * w[a];
+                d[a * 4 + c] = (2. * own + sm) * w[a];
             }
+    };
+    auto add = [&](const double *d) {
+        for (int c = 0; c < 12; ++c) g[c] = g[c] + d[c];
+    };
+    if constexpr (U == 32) {
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (k0 + lane < end) iterms(k0 + lane, v);
+            warp_ordered<12>(v, min(32, end - k0), add);
+        }
+        const int bbeg = L.binc_ptr[i], bend = L.binc_ptr[i + 1];
+        for (int k0 = bbeg; k0 < bend; k0 += 32) {
+            double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (k0 + lane < bend) bterms(k0 + lane, v);
+            warp_ordered<12>(v, min(32, bend - k0), add);
+        }
+        if (lane) return;
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[12];
+            iterms(k, v);
+            add(v);
+        }
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[12];
+            bterms(k, v);
+            add(v);
+        }
     }
     const double vt = 1. / L.V[i];
     double dudx = g[0] * vt, dvdx = g[1] * vt, dwdx = g[2] * vt, dTdx = g[3] * vt;
@@ -299,15 +460,18 @@ __global__ void __launch_bounds__(256, 3) k_visc_grad(Params P, LevelView L) {
 
 // pass 2: viscous edge fluxes gathered per node and subtracted from the
 // dissipation vector (def_par:5662-5892)
-__global__ void __launch_bounds__(256, 3) k_visc_flux(Params P, LevelView L) {
-    int i = tid();
+template <int U>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, LevelView L) {
+    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
+    const int i = U == 32 ? tid() >> 5 : tid();
     if (i >= L.N) return;
     const int N = L.N;
     double ti[9], ui[3];
     for (int c = 0; c < 9; ++c) ti[c] = L.tau[c * N + i];
     ui[0] = L.prim[i]; ui[1] = L.prim[N + i]; ui[2] = L.prim[2 * N + i];
     double acc[4] = {0, 0, 0, 0};
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+    // interior edge: the edge flux with the sign of this node (x - y is x + (-y))
+    auto iterms = [&](int k, double *g) {
         int2 t = L.inc[k];
         int e = t.x >= 0 ? t.x : ~t.x, j = t.y;
         double tj[9], uj[3];
@@ -327,12 +491,17 @@ __global__ void __launch_bounds__(256, 3) k_visc_flux(Params P, LevelView L) {
         f[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
         f[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
         f[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
-        for (int c = 0; c < 4; ++c) acc[c] = first ? acc[c] + f[c] : acc[c] - f[c];
-    }
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        for (int c = 0; c < 4; ++c) g[c] = first ? f[c] : -f[c];
+    };
+    auto iadd = [&](const double *g) {
+        for (int c = 0; c < 4; ++c) acc[c] = acc[c] + g[c];
+    };
+    // boundary edge: the two terms of each component, g[8] = 1 if it counts
+    auto bterms = [&](int k, double *g) {
         int bb = L.binc[k] >> 1, side = L.binc[k] & 1;
         int ind = L.bind[bb];
-        if (ind == 2 || ind == 9) continue;
+        g[8] = (ind == 2 || ind == 9) ? 0.0 : 1.0;
+        if (g[8] == 0.0) return;
         int2 nd = L.bedge[bb];
         double a[9], b[9], ua[3], ub[3];
         for (int c = 0; c < 9; ++c) { a[c] = L.tau[c * N + nd.x]; b[c] = L.tau[c * N + nd.y]; }
@@ -348,16 +517,46 @@ __global__ void __launch_bounds__(256, 3) k_visc_flux(Params P, LevelView L) {
         double d31 = (ua[0] * a[2] + ua[1] * a[4]) + ua[2] * a[5];
         double d32 = (ub[0] * b[2] + ub[1] * b[4]) + ub[2] * b[5];
         double dut1 = d11 + d12, dut2 = d21 + d22, dut3 = d31 + d32;
-        double f2 = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
-        double f3 = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
-        double f4 = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
-        double f5 = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+        g[0] = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+        g[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+        g[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+        g[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
         const double *o = side == 0 ? a : b;
         double do1 = side == 0 ? d11 : d12, do2 = side == 0 ? d21 : d22, do3 = side == 0 ? d31 : d32;
-        acc[0] = (acc[0] + f2) + 2.0 * ((wx * o[0] + wy * o[1]) + wz * o[2]);
-        acc[1] = (acc[1] + f3) + 2.0 * ((wx * o[1] + wy * o[3]) + wz * o[4]);
-        acc[2] = (acc[2] + f4) + 2.0 * ((wx * o[2] + wy * o[4]) + wz * o[5]);
-        acc[3] = (acc[3] + f5) + 2.0 * ((wx * (o[6] + do1) + wy * (o[7] + do2)) + wz * (o[8] + do3));
+        g[4] = 2.0 * ((wx * o[0] + wy * o[1]) + wz * o[2]);
+        g[5] = 2.0 * ((wx * o[1] + wy * o[3]) + wz * o[4]);
+        g[6] = 2.0 * ((wx * o[2] + wy * o[4]) + wz * o[5]);
+        g[7] = 2.0 * ((wx * (o[6] + do1) + wy * (o[7] + do2)) + wz * (o[8] + do3));
+    };
+    auto badd = [&](const double *g) {
+        if (g[8] == 0.0) return;
+        for (int c = 0; c < 4; ++c) acc[c] = (acc[c] + g[c]) + g[4 + c];
+    };
+    if constexpr (U == 32) {
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            double v[4] = {0, 0, 0, 0};
+            if (k0 + lane < end) iterms(k0 + lane, v);
+            warp_ordered<4>(v, min(32, end - k0), iadd);
+        }
+        const int bbeg = L.binc_ptr[i], bend = L.binc_ptr[i + 1];
+        for (int k0 = bbeg; k0 < bend; k0 += 32) {
+            double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (k0 + lane < bend) bterms(k0 + lane, v);
+            warp_ordered<9>(v, min(32, bend - k0), badd);
+        }
+        if (lane) return;
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[4];
+            iterms(k, v);
+            iadd(v);
+        }
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[9];
+            bterms(k, v);
+            badd(v);
+        }
     }
     for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
 }
@@ -577,20 +776,46 @@ __device__ __forceinline__ void delta_flux(const DeltaRec &n, float wx, float wy
 
 // interior residual of node i as the anchor's FP64 sum plus the FP32 sum of
 // the flux increments of its edges
+template <int U>
 __device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i, double *r) {
     float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     const DeltaRec me = load_delta(L.dq, i);
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+    auto terms = [&](int k, float *s5, bool &first) {
         const IncRec32 t = load_inc32(L.inc32, k);
-        const bool first = t.j >= 0;
+        first = t.j >= 0;
         const DeltaRec nb = load_delta(L.dq, first ? t.j : ~t.j);
         float g1[5], g2[5];
         delta_flux(first ? me : nb, t.wx, t.wy, t.wz, g1);
         delta_flux(first ? nb : me, t.wx, t.wy, t.wz, g2);
-        if (first) {
-            for (int c = 0; c < 5; ++c) acc[c] += g1[c] + g2[c];
-        } else {
-            for (int c = 0; c < 5; ++c) acc[c] -= g1[c] + g2[c];
+        for (int c = 0; c < 5; ++c) s5[c] = g1[c] + g2[c];
+    };
+    if constexpr (U == 32) {
+        const int lane = threadIdx.x & 31;
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            float v[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+            bool first = true;
+            if (k0 + lane < end) terms(k0 + lane, v, first);
+            const float sg = first ? 1.f : 0.f;
+            const int n = min(32, end - k0);
+            for (int q = 0; q < n; ++q) {
+                const bool f = __shfl_sync(0xffffffffu, sg, q) != 0.f;
+                for (int c = 0; c < 5; ++c) {
+                    const float x = __shfl_sync(0xffffffffu, v[c], q);
+                    acc[c] = f ? acc[c] + x : acc[c] - x;
+                }
+            }
+        }
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            float v[5];
+            bool first;
+            terms(k, v, first);
+            if (first) {
+                for (int c = 0; c < 5; ++c) acc[c] += v[c];
+            } else {
+                for (int c = 0; c < 5; ++c) acc[c] -= v[c];
+            }
         }
     }
     const int N = L.N;
@@ -633,47 +858,99 @@ __device__ __forceinline__ void gather_interior_central2(const LevelView &L, int
 // interior central fluxes of node i computed from the two node records of
 // each incident edge, summed in edge order: the same numbers, in the same
 // order, as the edge kernel followed by the buffer gather
+template <int U>
 __device__ __forceinline__ void gather_interior_central(const LevelView &L, int i, double *r) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     const NodeRec si = load_node(L.q, i);
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+    // the flux of incidence k with this node's sign (x - y is x + (-y))
+    auto terms = [&](int k, double *g) {
         const int2 t = L.inc[k];
         const int e = t.x >= 0 ? t.x : ~t.x;
         const EdgeW w = load_edgew(L.ew, e);
         const NodeRec n = load_node(L.q, t.y);
-        const NodeRec &sj = n;
         double f[5];
         if (t.x >= 0) {
-            central_flux_rec(si, sj, w.wx, w.wy, w.wz, f);
-            r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
+            central_flux_rec(si, n, w.wx, w.wy, w.wz, f);
+            for (int c = 0; c < 5; ++c) g[c] = f[c];
         } else {
-            central_flux_rec(sj, si, w.wx, w.wy, w.wz, f);
-            r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
+            central_flux_rec(n, si, w.wx, w.wy, w.wz, f);
+            for (int c = 0; c < 5; ++c) g[c] = -f[c];
+        }
+    };
+    auto add = [&](const double *g) {
+        r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
+    };
+    if constexpr (U == 32) {
+        const int lane = threadIdx.x & 31;
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            double v[5] = {0, 0, 0, 0, 0};
+            if (k0 + lane < end) terms(k0 + lane, v);
+            warp_ordered<5>(v, min(32, end - k0), add);
+        }
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[5];
+            terms(k, v);
+            add(v);
         }
     }
 }
 
 // interior edges of node i from the FP64 edge buffer, in edge order
+template <int U>
 __device__ __forceinline__ void gather_interior(const LevelView &L, int i, double *r) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-        int s = L.inc[k].x;
-        if (s >= 0) {
-            const double *f = L.flux + (size_t)s * 5;
-            r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
-        } else {
-            const double *f = L.flux + (size_t)(~s) * 5;
-            r[0] = r[0] - f[0]; r[1] = r[1] - f[1]; r[2] = r[2] - f[2]; r[3] = r[3] - f[3]; r[4] = r[4] - f[4];
+    auto terms = [&](int k, double *g) {
+        const int s = L.inc[k].x;
+        const double *f = L.flux + (size_t)(s >= 0 ? s : ~s) * 5;
+        for (int c = 0; c < 5; ++c) g[c] = s >= 0 ? f[c] : -f[c];  // x - y is x + (-y)
+    };
+    auto add = [&](const double *g) {
+        r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
+    };
+    if constexpr (U == 32) {
+        const int lane = threadIdx.x & 31;
+        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            double v[5] = {0, 0, 0, 0, 0};
+            if (k0 + lane < end) terms(k0 + lane, v);
+            warp_ordered<5>(v, min(32, end - k0), add);
+        }
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[5];
+            terms(k, v);
+            add(v);
         }
     }
 }
 
 // boundary edges of node i (FP64)
+template <int U>
 __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, double *r) {
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-        int v = L.binc[k];
-        const double *g = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
+    auto terms = [&](int k, double *g) {
+        const int v = L.binc[k];
+        const double *b = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
+        for (int c = 0; c < 5; ++c) g[c] = b[c];
+    };
+    auto add = [&](const double *g) {
         r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
+    };
+    if constexpr (U == 32) {
+        const int lane = threadIdx.x & 31;
+        const int beg = L.binc_ptr[i], end = L.binc_ptr[i + 1];
+        for (int k0 = beg; k0 < end; k0 += 32) {
+            double v[5] = {0, 0, 0, 0, 0};
+            if (k0 + lane < end) terms(k0 + lane, v);
+            warp_ordered<5>(v, min(32, end - k0), add);
+        }
+    } else {
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[5];
+            terms(k, v);
+            add(v);
+        }
     }
 }
 
@@ -705,24 +982,30 @@ __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const do
 // GATHER_CENTRAL (central fluxes computed in the gather), GATHER_ANCHOR (the
 // same, stored as the new mixed-precision anchor), GATHER_DELTA (anchor +
 // FP32 increments)
-template <int PREC>
-__global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : 3)
+template <int PREC, int U>
+__global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3 : 1))
     k_node_update(Params P, LevelView L, int mode, int stage) {
-    int i = tid();
+    const int i = U == 32 ? tid() >> 5 : tid();
     if (i >= L.N) return;
     const int N = L.N;
     double r[5];
     if constexpr (PREC == GATHER_DELTA) {
-        gather_interior_delta(L, i, r);
+        gather_interior_delta<U>(L, i, r);
     } else if constexpr (PREC == GATHER_BUFFER) {
-        gather_interior(L, i, r);
+        gather_interior<U>(L, i, r);
     } else if constexpr (PREC == GATHER_CENTRAL2) {
         gather_interior_central2(L, i, r);
     } else {
-        gather_interior_central(L, i, r);
-        if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, r);
+        gather_interior_central<U>(L, i, r);
     }
-    gather_boundary(L, i, r);
+    double rint[5];
+    if constexpr (PREC == GATHER_ANCHOR)
+        for (int c = 0; c < 5; ++c) rint[c] = r[c];
+    gather_boundary<U>(L, i, r);
+    // with a warp per node every lane holds the same sums; one lane goes on
+    if constexpr (U == 32)
+        if (threadIdx.x & 31) return;
+    if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, rint);
     if (mode == MODE_RESID) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
@@ -769,11 +1052,27 @@ __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : 3)
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = un[c] - up[c];
     }
 }
-template __global__ void k_node_update<GATHER_BUFFER>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL2>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 32>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 32>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2, 32>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 32>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 32>(Params, LevelView, int, int);
+template __global__ void k_timestep<1>(Params, LevelView);
+template __global__ void k_timestep<32>(Params, LevelView);
+template __global__ void k_jst_lap<1>(Params, LevelView);
+template __global__ void k_jst_lap<32>(Params, LevelView);
+template __global__ void k_jst_flux<1>(Params, LevelView);
+template __global__ void k_jst_flux<32>(Params, LevelView);
+template __global__ void k_first_order_diss<1>(Params, LevelView);
+template __global__ void k_visc_grad<1>(Params, LevelView);
+template __global__ void k_visc_grad<32>(Params, LevelView);
+template __global__ void k_visc_flux<1>(Params, LevelView);
+template __global__ void k_visc_flux<32>(Params, LevelView);
 
 // ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
 __global__ void k_copy(const double *a, double *b, size_t n) {

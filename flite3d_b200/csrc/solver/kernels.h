@@ -7,12 +7,18 @@ namespace flite {
 enum { MODE_STAGE = 0, MODE_RCOARSE = 1, MODE_RFINE = 2, MODE_RESID = 3 };
 
 __global__ void k_pressure(Params P, LevelView L);
+template <int U>
 __global__ void k_timestep(Params P, LevelView L);
+template <int U>
 __global__ void k_jst_lap(Params P, LevelView L);
+template <int U>
 __global__ void k_jst_flux(Params P, LevelView L);
+template <int U>
 __global__ void k_first_order_diss(Params P, LevelView L);
 __global__ void k_visc_prim(Params P, LevelView L);
+template <int U>
 __global__ void k_visc_grad(Params P, LevelView L);
+template <int U>
 __global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
@@ -22,8 +28,11 @@ template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 __global__ void k_bnd_flux(Params P, LevelView L);
 enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3, GATHER_CENTRAL2 = 4 };
-template <int PREC>
+template <int PREC, int U>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
+// levels below this many nodes gather with a warp per node (U = 32) instead
+// of a thread per node (U = 1)
+constexpr int kSmallLevelNodes = 8192;
 __global__ void k_delta_state(LevelView L);
 __global__ void k_sa_timestep(Params P, LevelView L);
 __global__ void k_sa_grad(Params P, LevelView L);

@@ -186,8 +186,8 @@ class Solver:
         self._ck(self.be.residual_jvp(self._h, level, _ptr(u), _ptr(du), _ptr(jv)), "residual_jvp")
         return jv
 
-    def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1):
-        self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll),
+    def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1, warp_gather_below=8192):
+        self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll, warp_gather_below),
                  "set_kernel_options")
 
     KERNEL_GROUPS = ("pressure", "timestep", "dissipation", "visc_prim", "visc_grad", "visc_flux",
