@@ -160,15 +160,17 @@ def run_ours(args):
             solver.set_kernel_options(256, nb, unroll)
             tuning[(nb, unroll)] = solver.profile_level(1, reps=5)[1]
     best = min(tuning, key=tuning.get)
-    warp_tune = {}
-    for below in sorted({0, 8192} | {mesh.level(l).n_nodes + 1 for l in range(2, mesh.nlevels + 1)}):
-        solver.set_kernel_options(256, best[0], best[1], below)
-        solver.set_state(u0)
-        solver.start()
-        solver.time_cycles(2)
-        warp_tune[below] = solver.time_cycles(10, cycle_no=3) / 10
-    warp_below = min(warp_tune, key=warp_tune.get)
-    solver.set_kernel_options(256, best[0], best[1], warp_below)
+    solver.set_kernel_options(256, best[0], best[1])
+    # lanes per node of each level's gathers, by the device time of that
+    # level's kernels over one relaxation step
+    lanes = {}
+    for lvl in range(1, solver.nlevels + 1):
+        t = {}
+        for g in ((1, 4, 8) if lvl == 1 else (1, 4, 8, 16, 32)):
+            solver.set_gather_lanes(lvl, g)
+            t[g] = sum(solver.profile_kernels(lvl, reps=5).values())
+        lanes[lvl] = min(t, key=t.get)
+        solver.set_gather_lanes(lvl, lanes[lvl])
     solver.set_state(u0)
     solver.start()
     # warm-up (also captures the cycle graph)
@@ -287,8 +289,7 @@ def run_ours(args):
         "level1_kernel_ms": kernels_l1,
         "coarse_kernel_ms": kernels_coarse,
         "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1],
-                                           "warp_gather_below": warp_below},
-                                "cycle_ms_by_warp_threshold": {str(k): v for k, v in warp_tune.items()},
+                                           "gather_lanes_per_level": lanes},
                                 "ms": {f"nb{k[0]}_unroll{k[1]}": v for k, v in tuning.items()}},
         "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,
                     "what": "flite_residual_vjp vs flite_residual_fwd kernels on level 1, FP64"},

@@ -45,6 +45,18 @@ struct DevLevel {
 
 using namespace flite_detail;
 
+// a gather kernel template launched with the lanes per node of level l
+#define FLITE_GATHER(kern, l, ...)                                                  \
+    do {                                                                            \
+        switch (lanes_of(l)) {                                                      \
+            case 4: kern<4><<<gblk(l, 4), nb, 0, s>>>(__VA_ARGS__); break;          \
+            case 8: kern<8><<<gblk(l, 8), nb, 0, s>>>(__VA_ARGS__); break;          \
+            case 16: kern<16><<<gblk(l, 16), nb, 0, s>>>(__VA_ARGS__); break;       \
+            case 32: kern<32><<<gblk(l, 32), nb, 0, s>>>(__VA_ARGS__); break;       \
+            default: kern<1><<<gblk(l, 1), nb, 0, s>>>(__VA_ARGS__);                \
+        }                                                                           \
+    } while (0)
+
 struct flite_ctx {
     flite_controls c{};
     Params P{};
@@ -118,9 +130,13 @@ struct flite_ctx {
     // the incidences in parallel, the sums keep their order): there a
     // thread per node leaves most SMs idle and each thread waits on a long
     // chain of dependent loads
-    int small_nodes = kSmallLevelNodes;
-    bool small(int l) const { return lv[l].v.N < small_nodes; }
-    unsigned wblk(int l) const { return (unsigned)((32 * (size_t)lv[l].v.N + nb - 1) / nb); }
+    // lanes per node of each level's gathers (1, 4, 8, 16 or 32)
+    int lanes[kMaxLevels] = {0};
+    int lanes_of(int l) const {
+        if (l < kMaxLevels && lanes[l] > 0) return lanes[l];
+        return lv[l].v.N < kSmallLevelNodes ? 32 : 1;
+    }
+    unsigned gblk(int l, int g) const { return (unsigned)((g * (size_t)lv[l].v.N + nb - 1) / nb); }
 
     void pressure(int l) {
         counted();
@@ -128,8 +144,7 @@ struct flite_ctx {
     }
     void timesteps(int l) {
         counted();
-        if (small(l)) k_timestep<32><<<wblk(l), nb, 0, s>>>(P, V(l));
-        else k_timestep<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        FLITE_GATHER(k_timestep, l, P, V(l));
     }
     void zero_diss(int l) {
         counted();
@@ -144,11 +159,9 @@ struct flite_ctx {
             return;
         }
         counted();
-        if (small(l)) k_jst_lap<32><<<wblk(l), nb, 0, s>>>(P, L);
-        else k_jst_lap<1><<<nblk(L.N), nb, 0, s>>>(P, L);
+        FLITE_GATHER(k_jst_lap, l, P, L);
         counted();
-        if (small(l)) k_jst_flux<32><<<wblk(l), nb, 0, s>>>(P, L);
-        else k_jst_flux<1><<<nblk(L.N), nb, 0, s>>>(P, L);
+        FLITE_GATHER(k_jst_flux, l, P, L);
     }
     void first_order_diss(int l) {
         counted();
@@ -165,11 +178,13 @@ struct flite_ctx {
         counted();
         k_visc_prim<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
         counted();
-        if (small(l)) k_visc_grad<32><<<wblk(l), nb, 0, s>>>(P, V(l));
-        else k_visc_grad<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        visc_grad(l);
         counted();
-        if (small(l)) k_visc_flux<32><<<wblk(l), nb, 0, s>>>(P, V(l));
-        else k_visc_flux<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        visc_flux(l);
+    }
+    void visc_grad(int l) { FLITE_GATHER(k_visc_grad, l, P, V(l)); }
+    void visc_flux(int l) {
+        FLITE_GATHER(k_visc_flux, l, P, V(l));
     }
     // ---- Spalart-Allmaras ----------------------------------------------
     void sa_timesteps(int l) {
@@ -245,12 +260,17 @@ struct flite_ctx {
         launch_node_update(l, mode, stage, anchor);
     }
     void launch_node_update(int l, int mode, int stage, bool anchor) {
-        if (small(l)) launch_node_update_u<32>(l, mode, stage, anchor);
-        else launch_node_update_u<1>(l, mode, stage, anchor);
+        switch (lanes_of(l)) {
+            case 4: launch_node_update_u<4>(l, mode, stage, anchor); break;
+            case 8: launch_node_update_u<8>(l, mode, stage, anchor); break;
+            case 16: launch_node_update_u<16>(l, mode, stage, anchor); break;
+            case 32: launch_node_update_u<32>(l, mode, stage, anchor); break;
+            default: launch_node_update_u<1>(l, mode, stage, anchor);
+        }
     }
     template <int U>
     void launch_node_update_u(int l, int mode, int stage, bool anchor) {
-        const unsigned g = U == 32 ? wblk(l) : nblk(V(l).N);
+        const unsigned g = gblk(l, U);
         if (mixed()) {
             if (anchor) k_node_update<GATHER_ANCHOR, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
             else k_node_update<GATHER_DELTA, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);

@@ -616,16 +616,22 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms, do
     });
 }
 
-int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll,
-                             int32_t warp_gather_below) {
+int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll) {
     if (!ctx || edge_block < 32 || edge_block > 256 || node_block < 32 || node_block > 256 || edge_block % 32 ||
-        node_block % 32 || (gather_unroll != 1 && gather_unroll != 2) || warp_gather_below < 0)
+        node_block % 32 || (gather_unroll != 1 && gather_unroll != 2))
         return FLITE_EINVAL;
     ctx->drop_graph();
     ctx->eb = edge_block;
     ctx->nb = node_block;
     ctx->unroll = gather_unroll;
-    ctx->small_nodes = warp_gather_below;
+    return FLITE_OK;
+}
+
+int flite_set_gather_lanes(flite_ctx *ctx, int32_t level, int32_t lanes) {
+    if (bad_level(ctx, level) || level > kMaxLevels) return FLITE_EINVAL;
+    if (!(lanes == 0 || lanes == 1 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32)) return FLITE_EINVAL;
+    ctx->drop_graph();
+    ctx->lanes[level - 1] = lanes;
     return FLITE_OK;
 }
 
@@ -641,18 +647,8 @@ int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32
         k.push_back([&] { X.timesteps(l); });
         k.push_back([&] { X.dissipation(l); });
         k.push_back([&] { if (X.c.ReynoldsNumber > 0) k_visc_prim<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
-        k.push_back([&] {
-            if (X.c.ReynoldsNumber > 0) {
-                if (X.small(l)) k_visc_grad<32><<<X.wblk(l), X.nb, 0, X.s>>>(X.P, L);
-                else k_visc_grad<1><<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L);
-            }
-        });
-        k.push_back([&] {
-            if (X.c.ReynoldsNumber > 0) {
-                if (X.small(l)) k_visc_flux<32><<<X.wblk(l), X.nb, 0, X.s>>>(X.P, L);
-                else k_visc_flux<1><<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L);
-            }
-        });
+        k.push_back([&] { if (X.c.ReynoldsNumber > 0) X.visc_grad(l); });
+        k.push_back([&] { if (X.c.ReynoldsNumber > 0) X.visc_flux(l); });
         k.push_back([&] { X.rhs_terms(l, true); });
         k.push_back([&] { X.launch_node_update(l, MODE_RFINE, 0, true); });
         const int m = std::min<int>((int)k.size(), nmax);

@@ -27,17 +27,30 @@ namespace flite {
 
 static __device__ __forceinline__ int tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
-// Warp-per-node gathers (small levels): lane l computes the terms of
-// incidence k0 + l; the warp then applies them to the node's accumulators in
-// incidence order, every lane doing the same additions on the broadcast
-// terms, so the sums are those of the serial loop bit for bit.
-template <int K, class Fn>
-__device__ __forceinline__ void warp_ordered(const double (&v)[K], int n, Fn &&fn) {
-    for (int q = 0; q < n; ++q) {
-        double x[K];
+// Group-per-node gathers (small levels): U lanes (a power of two up to 32)
+// serve one node.  Lane l of a group evaluates the terms of incidence k0 + l;
+// the group then applies them to the node's accumulators in incidence order,
+// every lane doing the same additions on broadcast terms, so the sums are
+// those of the serial loop bit for bit.  Groups past the last node stay in
+// the loop (the shuffles need every lane) but apply nothing.
+template <int U, int K, class T, class Terms, class Add>
+__device__ __forceinline__ void group_gather(int beg, int end, bool active, int gl, Terms &&terms, Add &&add) {
+    const int span = active ? end - beg : 0;
+    const unsigned trips = (unsigned)((span + U - 1) / U);
+    const unsigned maxtrips = __reduce_max_sync(0xffffffffu, trips);
+    for (unsigned t = 0; t < maxtrips; ++t) {
+        const int k0 = beg + (int)t * U;
+        T v[K];
 #pragma unroll
-        for (int c = 0; c < K; ++c) x[c] = __shfl_sync(0xffffffffu, v[c], q);
-        fn(x);
+        for (int c = 0; c < K; ++c) v[c] = T(0);
+        if (active && k0 + gl < end) terms(k0 + gl, v);
+        const int n = active ? min(U, end - k0) : 0;
+        for (int q = 0; q < U; ++q) {
+            T x[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) x[c] = __shfl_sync(0xffffffffu, v[c], q, U);
+            if (q < n) add(x);
+        }
     }
 }
 
@@ -55,39 +68,39 @@ __global__ void k_pressure(Params P, LevelView L) {
 // ---- makeTimeSteps (def_par:13335-13610) as a node gather -----------------
 template <int U>
 __global__ void k_timestep(Params P, LevelView L) {
-    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
-    const int i = U == 32 ? tid() >> 5 : tid();
-    if (i >= L.N) return;
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
     const int N = L.N;
     const double c1 = P.gamma;
     const double ri = L.u[i], ro = 1. / ri;
     const double m1 = L.u[N + i], m2 = L.u[2 * N + i], m3 = L.u[3 * N + i];
     const double cc = dmax(c1 * L.p[i] * ro, 0.001);
     double acc = 0.0, h = 0.0;
-    if constexpr (U == 32) {
+    if constexpr (U > 1) {
         const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            const int k = k0 + lane;
-            double v[3] = {0.0, 0.0, 0.0};
-            if (k < end) {
-                const int2 t = L.inc[k];
-                const int e = t.x >= 0 ? t.x : ~t.x;
-                const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
-                const double al = (wx * wx + wy * wy) + wz * wz;
-                const double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
-                v[0] = fabs(vn);
-                v[1] = sqrt(cc * al);
-                if (P.viscous) {
-                    const int j = t.y;
-                    const double vis = dmax(P.am, P.sa ? L.mu[j] + L.u[5 * N + j] / P.Re : L.mu[j]);
-                    v[2] = 2.0 * vis * al / L.u[j];
-                }
+        group_gather<U, 3, double>(
+            beg, end, active, gl,
+            [&](int k, double *v) {
+            const int2 t = L.inc[k];
+            const int e = t.x >= 0 ? t.x : ~t.x;
+            const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
+            const double al = (wx * wx + wy * wy) + wz * wz;
+            const double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
+            v[0] = fabs(vn);
+            v[1] = sqrt(cc * al);
+            if (P.viscous) {
+                const int j = t.y;
+                const double vis = dmax(P.am, P.sa ? L.mu[j] + L.u[5 * N + j] / P.Re : L.mu[j]);
+                v[2] = 2.0 * vis * al / L.u[j];
             }
-            warp_ordered<3>(v, min(32, end - k0), [&](const double *x) {
-                acc = (acc + x[0]) + x[1];
-                if (P.viscous) h = h + x[2];
+            },
+            [&](const double *x) {
+            acc = (acc + x[0]) + x[1];
+            if (P.viscous) h = h + x[2];
             });
-        }
     } else
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
@@ -137,14 +150,9 @@ __global__ void k_timestep(Params P, LevelView L) {
         acc = (((acc + x[0]) + x[1]) + x[2]) + x[3];
         if (P.viscous) h = (h + x[4]) + x[5];
     };
-    if constexpr (U == 32) {
-        const int beg = L.binc_ptr[i], end = L.binc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            double v[6] = {0, 0, 0, 0, 0, 0};
-            if (k0 + lane < end) bterms(k0 + lane, v);
-            warp_ordered<6>(v, min(32, end - k0), badd);
-        }
-        if (lane) return;
+    if constexpr (U > 1) {
+        group_gather<U, 6, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, badd);
+        if (!active || gl) return;
     } else
     for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
         double v[6];
@@ -161,43 +169,43 @@ __global__ void k_timestep(Params P, LevelView L) {
 // (def_par:11513-11780): undivided Laplacian with dE+dp, pressure sensor
 template <int U>
 __global__ void k_jst_lap(Params P, LevelView L) {
-    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
-    const int i = U == 32 ? tid() >> 5 : tid();
-    if (i >= L.N) return;
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
     const int N = L.N;
     double l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, s7 = 0, s8 = 0;
     const double ui0 = L.u[i], ui1 = L.u[N + i], ui2 = L.u[2 * N + i], ui3 = L.u[3 * N + i], ui4 = L.u[4 * N + i];
     const double pi = L.p[i];
-    if constexpr (U == 32) {
+    if constexpr (U > 1) {
         const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            const int k = k0 + lane;
-            double v[7] = {0, 0, 0, 0, 0, 0, 0};
-            if (k < end) {
-                const int2 t = L.inc[k];
-                const int j = t.y;
-                double df = 1.0;
-                if (P.useDissW) df = 1. / L.slen[t.x >= 0 ? t.x : ~t.x];
-                const double uj0 = L.u[j], uj1 = L.u[N + j], uj2 = L.u[2 * N + j], uj3 = L.u[3 * N + j];
-                const double uj4 = L.u[4 * N + j], pj = L.p[j];
-                // x - y is x + (-y): the subtractions of the serial loop become
-                // additions of negated terms
-                if (t.x >= 0) {
-                    v[0] = -((ui0 - uj0) * df); v[1] = -((ui1 - uj1) * df); v[2] = -((ui2 - uj2) * df);
-                    v[3] = -((ui3 - uj3) * df); v[4] = -((((ui4 - uj4) + pi) - pj) * df);
-                    v[5] = -(pi - pj); v[6] = pi + pj;
-                } else {
-                    v[0] = (uj0 - ui0) * df; v[1] = (uj1 - ui1) * df; v[2] = (uj2 - ui2) * df;
-                    v[3] = (uj3 - ui3) * df; v[4] = (((uj4 - ui4) + pj) - pi) * df;
-                    v[5] = pj - pi; v[6] = pj + pi;
-                }
+        group_gather<U, 7, double>(
+            beg, end, active, gl,
+            [&](int k, double *v) {
+            const int2 t = L.inc[k];
+            const int j = t.y;
+            double df = 1.0;
+            if (P.useDissW) df = 1. / L.slen[t.x >= 0 ? t.x : ~t.x];
+            const double uj0 = L.u[j], uj1 = L.u[N + j], uj2 = L.u[2 * N + j], uj3 = L.u[3 * N + j];
+            const double uj4 = L.u[4 * N + j], pj = L.p[j];
+            // x - y is x + (-y): the subtractions of the serial loop become
+            // additions of negated terms
+            if (t.x >= 0) {
+                v[0] = -((ui0 - uj0) * df); v[1] = -((ui1 - uj1) * df); v[2] = -((ui2 - uj2) * df);
+                v[3] = -((ui3 - uj3) * df); v[4] = -((((ui4 - uj4) + pi) - pj) * df);
+                v[5] = -(pi - pj); v[6] = pi + pj;
+            } else {
+                v[0] = (uj0 - ui0) * df; v[1] = (uj1 - ui1) * df; v[2] = (uj2 - ui2) * df;
+                v[3] = (uj3 - ui3) * df; v[4] = (((uj4 - ui4) + pj) - pi) * df;
+                v[5] = pj - pi; v[6] = pj + pi;
             }
-            warp_ordered<7>(v, min(32, end - k0), [&](const double *x) {
-                l0 = l0 + x[0]; l1 = l1 + x[1]; l2 = l2 + x[2]; l3 = l3 + x[3]; l4 = l4 + x[4];
-                s7 = s7 + x[5]; s8 = s8 + x[6];
+            },
+            [&](const double *x) {
+            l0 = l0 + x[0]; l1 = l1 + x[1]; l2 = l2 + x[2]; l3 = l3 + x[3]; l4 = l4 + x[4];
+            s7 = s7 + x[5]; s8 = s8 + x[6];
             });
-        }
-        if (lane) return;
+        if (!active || gl) return;
     } else
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
@@ -232,47 +240,47 @@ __global__ void k_jst_lap(Params P, LevelView L) {
 // ---- makeArtificialDissipation2, pass 3 (def_par:11770-11906), scalar -----
 template <int U>
 __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_jst_flux(Params P, LevelView L) {
-    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
-    const int i = U == 32 ? tid() >> 5 : tid();
-    if (i >= L.N) return;
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
     const int N = L.N;
     const double k4 = L.grid == 1 ? P.k4 : P.cgdf;
     double acc[5] = {0, 0, 0, 0, 0};
     double Li[5], Ui[5];
     for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
     const double vdi = L.vdt[i], coni = L.conn[i], si = L.sens[i];
-    if constexpr (U == 32) {
+    if constexpr (U > 1) {
         const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            const int k = k0 + lane;
-            double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (k < end) {
-                const int2 t = L.inc[k];
-                const int j = t.y;
-                const double vdj = L.vdt[j];
-                const bool first = t.x >= 0;
-                double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
-                d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
-                const double sj = L.sens[j];
-                const double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
-                double d4 = d0 * k4;
-                d4 = d4 > d2 ? d4 - d2 : 0.0;
-                for (int c = 0; c < 5; ++c) {
-                    const double Lj = L.lap[c * N + j], Uj = L.u[c * N + j];
-                    if (first) {
-                        v[2 * c] = -((Li[c] - Lj) * d4);
-                        v[2 * c + 1] = (Ui[c] - Uj) * d2;
-                    } else {
-                        v[2 * c] = (Lj - Li[c]) * d4;
-                        v[2 * c + 1] = -((Uj - Ui[c]) * d2);
-                    }
+        group_gather<U, 10, double>(
+            beg, end, active, gl,
+            [&](int k, double *v) {
+            const int2 t = L.inc[k];
+            const int j = t.y;
+            const double vdj = L.vdt[j];
+            const bool first = t.x >= 0;
+            double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
+            d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
+            const double sj = L.sens[j];
+            const double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
+            double d4 = d0 * k4;
+            d4 = d4 > d2 ? d4 - d2 : 0.0;
+            for (int c = 0; c < 5; ++c) {
+                const double Lj = L.lap[c * N + j], Uj = L.u[c * N + j];
+                if (first) {
+                    v[2 * c] = -((Li[c] - Lj) * d4);
+                    v[2 * c + 1] = (Ui[c] - Uj) * d2;
+                } else {
+                    v[2 * c] = (Lj - Li[c]) * d4;
+                    v[2 * c + 1] = -((Uj - Ui[c]) * d2);
                 }
             }
-            warp_ordered<10>(v, min(32, end - k0), [&](const double *x) {
-                for (int c = 0; c < 5; ++c) acc[c] = (acc[c] + x[2 * c]) + x[2 * c + 1];
+            },
+            [&](const double *x) {
+            for (int c = 0; c < 5; ++c) acc[c] = (acc[c] + x[2 * c]) + x[2 * c + 1];
             });
-        }
-        if (lane) return;
+        if (!active || gl) return;
     } else
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         int2 t = L.inc[k];
@@ -343,9 +351,11 @@ __global__ void k_visc_prim(Params P, LevelView L) {
 
 template <int U>
 __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, LevelView L) {
-    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
-    const int i = U == 32 ? tid() >> 5 : tid();
-    if (i >= L.N) return;
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
     const int N = L.N;
     const double gOg = P.gamma / (P.gamma - 1.0);
     double g[12];
@@ -383,20 +393,10 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, Lev
     auto add = [&](const double *d) {
         for (int c = 0; c < 12; ++c) g[c] = g[c] + d[c];
     };
-    if constexpr (U == 32) {
-        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (k0 + lane < end) iterms(k0 + lane, v);
-            warp_ordered<12>(v, min(32, end - k0), add);
-        }
-        const int bbeg = L.binc_ptr[i], bend = L.binc_ptr[i + 1];
-        for (int k0 = bbeg; k0 < bend; k0 += 32) {
-            double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (k0 + lane < bend) bterms(k0 + lane, v);
-            warp_ordered<12>(v, min(32, bend - k0), add);
-        }
-        if (lane) return;
+    if constexpr (U > 1) {
+        group_gather<U, 12, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, iterms, add);
+        group_gather<U, 12, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, add);
+        if (!active || gl) return;
     } else {
         for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
             double v[12];
@@ -462,9 +462,11 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, Lev
 // dissipation vector (def_par:5662-5892)
 template <int U>
 __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, LevelView L) {
-    const int lane = U == 32 ? (int)(threadIdx.x & 31) : 0;
-    const int i = U == 32 ? tid() >> 5 : tid();
-    if (i >= L.N) return;
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
     const int N = L.N;
     double ti[9], ui[3];
     for (int c = 0; c < 9; ++c) ti[c] = L.tau[c * N + i];
@@ -532,20 +534,10 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, Lev
         if (g[8] == 0.0) return;
         for (int c = 0; c < 4; ++c) acc[c] = (acc[c] + g[c]) + g[4 + c];
     };
-    if constexpr (U == 32) {
-        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            double v[4] = {0, 0, 0, 0};
-            if (k0 + lane < end) iterms(k0 + lane, v);
-            warp_ordered<4>(v, min(32, end - k0), iadd);
-        }
-        const int bbeg = L.binc_ptr[i], bend = L.binc_ptr[i + 1];
-        for (int k0 = bbeg; k0 < bend; k0 += 32) {
-            double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (k0 + lane < bend) bterms(k0 + lane, v);
-            warp_ordered<9>(v, min(32, bend - k0), badd);
-        }
-        if (lane) return;
+    if constexpr (U > 1) {
+        group_gather<U, 4, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, iterms, iadd);
+        group_gather<U, 9, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, badd);
+        if (!active || gl) return;
     } else {
         for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
             double v[4];
@@ -777,7 +769,8 @@ __device__ __forceinline__ void delta_flux(const DeltaRec &n, float wx, float wy
 // interior residual of node i as the anchor's FP64 sum plus the FP32 sum of
 // the flux increments of its edges
 template <int U>
-__device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i, double *r) {
+__device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i, double *r, bool active = true,
+                                         int gl = 0) {
     float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     const DeltaRec me = load_delta(L.dq, i);
     auto terms = [&](int k, float *s5, bool &first) {
@@ -789,23 +782,19 @@ __device__ __forceinline__ void gather_interior_delta(const LevelView &L, int i,
         delta_flux(first ? nb : me, t.wx, t.wy, t.wz, g2);
         for (int c = 0; c < 5; ++c) s5[c] = g1[c] + g2[c];
     };
-    if constexpr (U == 32) {
-        const int lane = threadIdx.x & 31;
-        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            float v[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-            bool first = true;
-            if (k0 + lane < end) terms(k0 + lane, v, first);
-            const float sg = first ? 1.f : 0.f;
-            const int n = min(32, end - k0);
-            for (int q = 0; q < n; ++q) {
-                const bool f = __shfl_sync(0xffffffffu, sg, q) != 0.f;
-                for (int c = 0; c < 5; ++c) {
-                    const float x = __shfl_sync(0xffffffffu, v[c], q);
-                    acc[c] = f ? acc[c] + x : acc[c] - x;
-                }
-            }
-        }
+    if constexpr (U > 1) {
+        // the terms carry the node's sign of the edge as a sixth value
+        group_gather<U, 6, float>(
+            L.inc_ptr[i], L.inc_ptr[i + 1], active, gl,
+            [&](int k, float *v) {
+                bool first;
+                terms(k, v, first);
+                v[5] = first ? 1.f : 0.f;
+            },
+            [&](const float *x) {
+                const bool f = x[5] != 0.f;
+                for (int c = 0; c < 5; ++c) acc[c] = f ? acc[c] + x[c] : acc[c] - x[c];
+            });
     } else {
         for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
             float v[5];
@@ -859,7 +848,8 @@ __device__ __forceinline__ void gather_interior_central2(const LevelView &L, int
 // each incident edge, summed in edge order: the same numbers, in the same
 // order, as the edge kernel followed by the buffer gather
 template <int U>
-__device__ __forceinline__ void gather_interior_central(const LevelView &L, int i, double *r) {
+__device__ __forceinline__ void gather_interior_central(const LevelView &L, int i, double *r, bool active = true,
+                                         int gl = 0) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     const NodeRec si = load_node(L.q, i);
     // the flux of incidence k with this node's sign (x - y is x + (-y))
@@ -880,14 +870,8 @@ __device__ __forceinline__ void gather_interior_central(const LevelView &L, int 
     auto add = [&](const double *g) {
         r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
     };
-    if constexpr (U == 32) {
-        const int lane = threadIdx.x & 31;
-        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            double v[5] = {0, 0, 0, 0, 0};
-            if (k0 + lane < end) terms(k0 + lane, v);
-            warp_ordered<5>(v, min(32, end - k0), add);
-        }
+    if constexpr (U > 1) {
+        group_gather<U, 5, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, terms, add);
     } else {
         for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
             double v[5];
@@ -899,7 +883,8 @@ __device__ __forceinline__ void gather_interior_central(const LevelView &L, int 
 
 // interior edges of node i from the FP64 edge buffer, in edge order
 template <int U>
-__device__ __forceinline__ void gather_interior(const LevelView &L, int i, double *r) {
+__device__ __forceinline__ void gather_interior(const LevelView &L, int i, double *r, bool active = true,
+                                         int gl = 0) {
     r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     auto terms = [&](int k, double *g) {
         const int s = L.inc[k].x;
@@ -909,14 +894,8 @@ __device__ __forceinline__ void gather_interior(const LevelView &L, int i, doubl
     auto add = [&](const double *g) {
         r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
     };
-    if constexpr (U == 32) {
-        const int lane = threadIdx.x & 31;
-        const int beg = L.inc_ptr[i], end = L.inc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            double v[5] = {0, 0, 0, 0, 0};
-            if (k0 + lane < end) terms(k0 + lane, v);
-            warp_ordered<5>(v, min(32, end - k0), add);
-        }
+    if constexpr (U > 1) {
+        group_gather<U, 5, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, terms, add);
     } else {
         for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
             double v[5];
@@ -928,7 +907,8 @@ __device__ __forceinline__ void gather_interior(const LevelView &L, int i, doubl
 
 // boundary edges of node i (FP64)
 template <int U>
-__device__ __forceinline__ void gather_boundary(const LevelView &L, int i, double *r) {
+__device__ __forceinline__ void gather_boundary(const LevelView &L, int i, double *r, bool active = true,
+                                         int gl = 0) {
     auto terms = [&](int k, double *g) {
         const int v = L.binc[k];
         const double *b = L.bflux + (size_t)(v >> 1) * 10 + (v & 1) * 5;
@@ -937,14 +917,8 @@ __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, doubl
     auto add = [&](const double *g) {
         r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
     };
-    if constexpr (U == 32) {
-        const int lane = threadIdx.x & 31;
-        const int beg = L.binc_ptr[i], end = L.binc_ptr[i + 1];
-        for (int k0 = beg; k0 < end; k0 += 32) {
-            double v[5] = {0, 0, 0, 0, 0};
-            if (k0 + lane < end) terms(k0 + lane, v);
-            warp_ordered<5>(v, min(32, end - k0), add);
-        }
+    if constexpr (U > 1) {
+        group_gather<U, 5, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms, add);
     } else {
         for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
             double v[5];
@@ -985,26 +959,29 @@ __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const do
 template <int PREC, int U>
 __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3 : 1))
     k_node_update(Params P, LevelView L, int mode, int stage) {
-    const int i = U == 32 ? tid() >> 5 : tid();
-    if (i >= L.N) return;
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
     const int N = L.N;
     double r[5];
     if constexpr (PREC == GATHER_DELTA) {
-        gather_interior_delta<U>(L, i, r);
+        gather_interior_delta<U>(L, i, r, active, gl);
     } else if constexpr (PREC == GATHER_BUFFER) {
-        gather_interior<U>(L, i, r);
+        gather_interior<U>(L, i, r, active, gl);
     } else if constexpr (PREC == GATHER_CENTRAL2) {
         gather_interior_central2(L, i, r);
     } else {
-        gather_interior_central<U>(L, i, r);
+        gather_interior_central<U>(L, i, r, active, gl);
     }
     double rint[5];
     if constexpr (PREC == GATHER_ANCHOR)
         for (int c = 0; c < 5; ++c) rint[c] = r[c];
-    gather_boundary<U>(L, i, r);
-    // with a warp per node every lane holds the same sums; one lane goes on
-    if constexpr (U == 32)
-        if (threadIdx.x & 31) return;
+    gather_boundary<U>(L, i, r, active, gl);
+    // with a group per node every lane holds the same sums; one lane goes on
+    if constexpr (U > 1)
+        if (!active || gl) return;
     if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, rint);
     if (mode == MODE_RESID) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
@@ -1053,26 +1030,52 @@ __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3
     }
 }
 template __global__ void k_node_update<GATHER_BUFFER, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 4>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 8>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 16>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 32>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 4>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 8>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 16>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 32>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL2, 1>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL2, 32>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 4>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 8>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 16>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 32>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 1>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 4>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 8>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 16>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 32>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2, 1>(Params, LevelView, int, int);
 template __global__ void k_timestep<1>(Params, LevelView);
+template __global__ void k_timestep<4>(Params, LevelView);
+template __global__ void k_timestep<8>(Params, LevelView);
+template __global__ void k_timestep<16>(Params, LevelView);
 template __global__ void k_timestep<32>(Params, LevelView);
 template __global__ void k_jst_lap<1>(Params, LevelView);
+template __global__ void k_jst_lap<4>(Params, LevelView);
+template __global__ void k_jst_lap<8>(Params, LevelView);
+template __global__ void k_jst_lap<16>(Params, LevelView);
 template __global__ void k_jst_lap<32>(Params, LevelView);
 template __global__ void k_jst_flux<1>(Params, LevelView);
+template __global__ void k_jst_flux<4>(Params, LevelView);
+template __global__ void k_jst_flux<8>(Params, LevelView);
+template __global__ void k_jst_flux<16>(Params, LevelView);
 template __global__ void k_jst_flux<32>(Params, LevelView);
-template __global__ void k_first_order_diss<1>(Params, LevelView);
 template __global__ void k_visc_grad<1>(Params, LevelView);
+template __global__ void k_visc_grad<4>(Params, LevelView);
+template __global__ void k_visc_grad<8>(Params, LevelView);
+template __global__ void k_visc_grad<16>(Params, LevelView);
 template __global__ void k_visc_grad<32>(Params, LevelView);
 template __global__ void k_visc_flux<1>(Params, LevelView);
+template __global__ void k_visc_flux<4>(Params, LevelView);
+template __global__ void k_visc_flux<8>(Params, LevelView);
+template __global__ void k_visc_flux<16>(Params, LevelView);
 template __global__ void k_visc_flux<32>(Params, LevelView);
+template __global__ void k_first_order_diss<1>(Params, LevelView);
 
 // ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
 __global__ void k_copy(const double *a, double *b, size_t n) {

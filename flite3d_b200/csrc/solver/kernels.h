@@ -30,9 +30,10 @@ __global__ void k_bnd_flux(Params P, LevelView L);
 enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3, GATHER_CENTRAL2 = 4 };
 template <int PREC, int U>
 __global__ void k_node_update(Params P, LevelView L, int mode, int stage);
-// levels below this many nodes gather with a warp per node (U = 32) instead
-// of a thread per node (U = 1)
+// gathers: U lanes per node (1 = a thread per node); by default levels
+// below kSmallLevelNodes nodes use a warp per node
 constexpr int kSmallLevelNodes = 8192;
+constexpr int kMaxLevels = 16;
 __global__ void k_delta_state(LevelView L);
 __global__ void k_sa_timestep(Params P, LevelView L);
 __global__ void k_sa_grad(Params P, LevelView L);

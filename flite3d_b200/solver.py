@@ -186,9 +186,12 @@ class Solver:
         self._ck(self.be.residual_jvp(self._h, level, _ptr(u), _ptr(du), _ptr(jv)), "residual_jvp")
         return jv
 
-    def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1, warp_gather_below=8192):
-        self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll, warp_gather_below),
-                 "set_kernel_options")
+    def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1):
+        self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll), "set_kernel_options")
+
+    def set_gather_lanes(self, level, lanes):
+        """Lanes per node of a level's gathers: 1, 4, 8, 16, 32 (0: default)."""
+        self._ck(self.be.set_gather_lanes(self._h, level, lanes), "set_gather_lanes")
 
     KERNEL_GROUPS = ("pressure", "timestep", "dissipation", "visc_prim", "visc_grad", "visc_flux",
                      "flux_terms", "node_update")

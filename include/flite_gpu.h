@@ -252,13 +252,14 @@ int flite_cycle_launches(flite_ctx *ctx, int64_t *n);
 int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms,
                         double *node_ms);
 /* Launch options of a context (no effect on any result): threads per block
- * of the edge kernels and of the node kernels (32..256, multiples of 32),
+ * of the edge kernels and of the node kernels (32..256, multiples of 32) and
  * the incidences whose loads the fused central gather issues together (1 or
- * 2), and the level size below which the node gathers use a warp per node
- * (default 8192; 0 = a thread per node everywhere).  Drops the captured
- * cycle graph.                                                             */
-int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll,
-                             int32_t warp_gather_below);
+ * 2).  Drops the captured cycle graph.                                     */
+int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll);
+/* Lanes per node of the node gathers of a level (no effect on any result):
+ * 1 (a thread per node), 4, 8, 16 or 32, or 0 for the default (32 below 8192
+ * nodes, else 1).  Drops the captured cycle graph.                         */
+int flite_set_gather_lanes(flite_ctx *ctx, int32_t level, int32_t lanes);
 /* Average device ms of the kernel groups of one relaxation step of a level,
  * in order: pressure, time steps, dissipation, viscous primitives, viscous
  * gradients, viscous fluxes, flux terms (edge or boundary kernels), node
