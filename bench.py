@@ -235,6 +235,9 @@ def run_ours(args):
     mixed = None
     if not args.no_mixed:
         solver_m = F.Solver(F.default_controls(**CONTROLS, precision=1), mesh)
+        solver_m.set_kernel_options(256, best[0], 1)
+        for lvl, g in lanes.items():
+            solver_m.set_gather_lanes(lvl, g)
         solver_m.set_state(u0)
         solver_m.start()
         for i in range(1, args.warmup + 1):
@@ -248,7 +251,7 @@ def run_ours(args):
                  "node_kernel_ms": node_m_ms, "increment_records_ms": delta_ms}
     ttc = None
     if args.converge:
-        ttc = time_to_converge(F, mesh, c, u0, args.converge_max)
+        ttc = time_to_converge(F, mesh, c, u0, args.converge_max, (best[0], lanes))
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -303,7 +306,7 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
-def time_to_converge(F, mesh, c, u0, max_cycles):
+def time_to_converge(F, mesh, c, u0, max_cycles, options=None):
     """Wall time from the first cycle until res1 <= 1e-8 res1(cycle 1), for
     FP64 and FLITE_MIXED on the same workload, with lift and drag there."""
     import torch
@@ -311,6 +314,10 @@ def time_to_converge(F, mesh, c, u0, max_cycles):
     for name, prec in (("fp64", 0), ("mixed", 1)):
         cc = F.default_controls(**CONTROLS, precision=prec)
         s = F.Solver(cc, mesh)
+        if options:
+            s.set_kernel_options(256, options[0], 1)
+            for lvl, g in options[1].items():
+                s.set_gather_lanes(lvl, g)
         s.set_state(u0)
         s.start()
         torch.cuda.synchronize()

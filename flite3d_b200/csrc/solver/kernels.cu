@@ -239,7 +239,7 @@ __global__ void k_jst_lap(Params P, LevelView L) {
 
 // ---- makeArtificialDissipation2, pass 3 (def_par:11770-11906), scalar -----
 template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_jst_flux(Params P, LevelView L) {
+__global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P, LevelView L) {
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
