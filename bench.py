@@ -410,6 +410,45 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_rans(args):
+    """The RANS configuration: Spalart-Allmaras on the extruded
+    NACA0012 O-grid (200 x 120 x 240 cells: 40 wall layers from 1e-5 chord
+    growing by 1.15, far field at 20 chords, one chord of span), Re 6e6,
+    M 0.8, alpha 1.25, HLLC order 2 with Galerkin gradients, 5 levels, FP64.
+    One JSON line: MG cycles/s (device time of graph-replayed cycles)."""
+    import torch
+    import flite3d_b200 as F
+    if not torch.cuda.is_available():
+        raise SystemExit("no CUDA device: the product path has no CPU fallback")
+    t0 = time.time()
+    mesh = F.Mesh.naca0012(args.rans_ni, args.rans_nj, args.rans_nk, first_cell=1.0e-5, growth=1.15, nlayer=40,
+                           farfield=20.0, span=1.0, nlevels=5)
+    t_mesh = time.time() - t0
+    c = F.default_controls(ReynoldsNumber=6.0e6, MachNumber=0.8, alpha=1.25, CFLNumber=1.0, fluxType=4,
+                           HLLCFluxOrder=2, Automaticlipping=1, GradientMethod=1, multigridScheme=3,
+                           numberOfGridsToUse=5, turbulenceModel=1, wallsAreIsentropic=1)
+    s = F.Solver(c, mesh)
+    s.init_freestream()
+    s.start()
+    for i in range(1, args.warmup + 1):
+        s.cycle(i)
+    torch.cuda.synchronize()
+    ms = s.time_cycles(args.steps, cycle_no=args.warmup + 1)
+    res = s.residuals()[0]
+    d = mesh.level(1)
+    print(json.dumps({
+        "metric": METRIC, "value": args.steps / (ms / 1e3), "unit": "cycles/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated NACA0012 O-grid, freestream start)",
+        "config": {"workload": "RANS Spalart-Allmaras, Re 6e6, M 0.8, alpha 1.25, HLLC order 2, on the extruded "
+                               f"NACA0012 O-grid {args.rans_ni}x{args.rans_nj}x{args.rans_nk} hex -> 6 tets, "
+                               "5 agglomerated MG levels, growing V-cycle",
+                   "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides, "levels": mesh.nlevels,
+                   "mesh_build_s": round(t_mesh, 2)},
+        "residuals_after": [float(x) for x in res], "gpu_launches": s.cycle_launches() * args.steps,
+    }), flush=True)
+
+
 def run_batch(args):
     """Batched solves: the bump channel at 120x40x40, 192x64x64 and
     264x88x88 hexes x 16 flow conditions each (angle of attack uniform in
@@ -473,6 +512,10 @@ def main():
                     help="also measure time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
     ap.add_argument("--converge-max", type=int, default=3000)
     ap.add_argument("--batch", action="store_true", help="the batched multi-condition workload instead")
+    ap.add_argument("--rans", action="store_true", help="the RANS (Spalart-Allmaras, NACA0012) workload instead")
+    ap.add_argument("--rans-ni", type=int, default=200)
+    ap.add_argument("--rans-nj", type=int, default=120)
+    ap.add_argument("--rans-nk", type=int, default=240)
     ap.add_argument("--batch-meshes", type=int, default=3)
     ap.add_argument("--batch-conditions", type=int, default=16)
     args = ap.parse_args()
@@ -484,6 +527,8 @@ def main():
         run_reference(args)
     elif args.batch:
         run_batch(args)
+    elif args.rans:
+        run_rans(args)
     else:
         run_ours(args)
 

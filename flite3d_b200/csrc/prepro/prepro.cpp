@@ -767,6 +767,119 @@ int fp_bump_channel(int nx, int ny, int nz, double bump_h, int nlevels, fp_mesh 
     });
 }
 
+// Extruded NACA0012 O-grid (the RANS configuration's geometry): ni points
+// around the section (cosine-clustered at the leading and trailing edges, the
+// standard 4-digit thickness law with its open trailing edge), nj cells from
+// the wall to a circular far field of radius `farfield` chords about x = 0.5
+// (nlayer layers from first_cell with ratio `growth`, then a geometric
+// stretching whose ratio makes the lines end on the circle), nk cells over
+// the span.  Hexes are split into 6 tets as in the bump channel (periodic
+// around the section).  Indicators: wall 1, span ends 2 (symmetry), far
+// field 3.
+int fp_naca0012(int ni, int nj, int nk, double first_cell, double growth, int nlayer, double farfield, double span,
+                int nlevels, fp_mesh **out) {
+    return guarded([&] {
+        if (ni < 8 || nj < 2 || nk < 1 || !(first_cell > 0) || !(growth >= 1) || nlayer < 0 || nlayer >= nj ||
+            !(farfield > 1) || !(span > 0))
+            return FLITE_EINVAL;
+        const int32_t NJ = nj + 1, NK = nk + 1;
+        const int64_t N = (int64_t)ni * NJ * NK;
+        if (N > 2000000000LL) return FLITE_EINVAL;
+        auto id = [&](int i, int j, int k) { return (int32_t)((i % ni) + ni * (j + (int64_t)NJ * k)) + 1; };
+        const double PI = 4.0 * std::atan(1.0);
+        // radial distances along each line, as a fraction of its length:
+        // fixed cells near the wall, then a ratio q found by bisection
+        auto yt = [](double x) {
+            return 0.6 * ((((0.2969 * std::sqrt(x) - 0.1260 * x) - 0.3516 * x * x) + 0.2843 * x * x * x) -
+                          0.1015 * x * x * x * x);
+        };
+        std::vector<double> sx(ni), sy(ni), cx(ni), cy(ni), len(ni);
+        for (int i = 0; i < ni; ++i) {
+            const double th = 2.0 * PI * i / ni;
+            const double x = 0.5 * (1.0 + std::cos(th));
+            sx[i] = x;
+            sy[i] = (th <= PI ? 1.0 : -1.0) * yt(x);
+            cx[i] = 0.5 + farfield * std::cos(th);
+            cy[i] = farfield * std::sin(th);
+            len[i] = std::hypot(cx[i] - sx[i], cy[i] - sy[i]);
+        }
+        double Lmin = len[0];
+        for (double v : len) Lmin = std::min(Lmin, v);
+        std::vector<double> d(NJ, 0.0);  // distances for the shortest line
+        for (int j = 1; j <= nlayer; ++j) d[j] = d[j - 1] + first_cell * std::pow(growth, j - 1);
+        const double rest = Lmin - d[nlayer];
+        const double h0 = first_cell * std::pow(growth, nlayer);
+        const int m = nj - nlayer;
+        if (!(rest > h0 * m * 0.5)) throw std::runtime_error("far field too close for the wall layers");
+        double lo = 1.0, hi = 2.0;
+        auto total = [&](double q) { return q == 1.0 ? h0 * m : h0 * (std::pow(q, m) - 1.0) / (q - 1.0); };
+        while (total(hi) < rest) hi *= 2.0;
+        for (int it = 0; it < 200; ++it) {
+            const double q = 0.5 * (lo + hi);
+            (total(q) < rest ? lo : hi) = q;
+        }
+        const double q = 0.5 * (lo + hi);
+        for (int j = nlayer + 1; j <= nj; ++j) d[j] = d[j - 1] + h0 * std::pow(q, j - nlayer - 1);
+        std::vector<double> xyz(3 * (size_t)N);
+        for (int k = 0; k < NK; ++k)
+            for (int j = 0; j < NJ; ++j)
+                for (int i = 0; i < ni; ++i) {
+                    const double f = d[j] / d[nj];  // the same fraction on every line
+                    const size_t n = (size_t)id(i, j, k) - 1;
+                    xyz[n] = sx[i] + f * (cx[i] - sx[i]);
+                    xyz[(size_t)N + n] = sy[i] + f * (cy[i] - sy[i]);
+                    xyz[2 * (size_t)N + n] = span * k / nk;
+                }
+        const int64_t NT = 6LL * ni * nj * nk;
+        std::vector<int32_t> tets(4 * (size_t)NT);
+        static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+        size_t t = 0;
+        for (int k = 0; k < nk; ++k)
+            for (int j = 0; j < nj; ++j)
+                for (int i = 0; i < ni; ++i)
+                    for (int p = 0; p < 6; ++p) {
+                        int c[3] = {i, j, k};
+                        int32_t v[4];
+                        v[0] = id(c[0], c[1], c[2]);
+                        for (int r = 0; r < 3; ++r) { c[perm[p][r]] += 1; v[r + 1] = id(c[0], c[1], c[2]); }
+                        for (int qq = 0; qq < 4; ++qq) tets[(size_t)qq * NT + t] = v[qq];
+                        ++t;
+                    }
+        std::vector<int32_t> tri, ind;
+        auto quad = [&](int a, int lo_side, int i, int j, int k, int indicator) {
+            int b = (a + 1) % 3, c = (a + 2) % 3;
+            int base[3] = {i, j, k};
+            if (!lo_side) base[a] += 1;
+            int pb[3] = {base[0], base[1], base[2]}; pb[b] += 1;
+            int pc[3] = {base[0], base[1], base[2]}; pc[c] += 1;
+            int pbc[3] = {base[0], base[1], base[2]}; pbc[b] += 1; pbc[c] += 1;
+            int32_t v0 = id(base[0], base[1], base[2]), vb = id(pb[0], pb[1], pb[2]);
+            int32_t vc = id(pc[0], pc[1], pc[2]), vbc = id(pbc[0], pbc[1], pbc[2]);
+            tri.push_back(v0); tri.push_back(vb); tri.push_back(vbc); ind.push_back(indicator);
+            tri.push_back(v0); tri.push_back(vc); tri.push_back(vbc); ind.push_back(indicator);
+        };
+        for (int k = 0; k < nk; ++k)
+            for (int i = 0; i < ni; ++i) {
+                quad(1, 1, i, 0, k, 1);       // wall
+                quad(1, 0, i, nj - 1, k, 3);  // far field
+            }
+        for (int j = 0; j < nj; ++j)
+            for (int i = 0; i < ni; ++i) {
+                quad(2, 1, i, j, 0, 2);
+                quad(2, 0, i, j, nk - 1, 2);
+            }
+        const size_t NF = ind.size();
+        std::vector<int32_t> tris(3 * NF);
+        for (size_t f = 0; f < NF; ++f)
+            for (int qq = 0; qq < 3; ++qq) tris[qq * NF + f] = tri[3 * f + qq];
+        auto M = std::make_unique<fp_mesh>();
+        build_fine(*M, (int32_t)N, xyz, std::move(tets), std::move(tris), ind);
+        build_levels(*M, nlevels);
+        *out = M.release();
+        return FLITE_OK;
+    });
+}
+
 int fp_free(fp_mesh *m) { delete m; return FLITE_OK; }
 
 int fp_num_levels(const fp_mesh *m) { return m ? (int)m->lv.size() : 0; }

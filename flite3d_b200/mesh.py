@@ -40,6 +40,16 @@ class Mesh:
         return cls(h)
 
     @classmethod
+    def naca0012(cls, ni, nj, nk, first_cell=1.0e-5, growth=1.15, nlayer=40, farfield=20.0, span=1.0,
+                 nlevels=3):
+        """Extruded NACA0012 O-grid (wall 1, span ends 2, far field 3)."""
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_naca0012(int(ni), int(nj), int(nk), ctypes.c_double(first_cell),
+                                      ctypes.c_double(growth), int(nlayer), ctypes.c_double(farfield),
+                                      ctypes.c_double(span), int(nlevels), ctypes.byref(h)), "fp_naca0012")
+        return cls(h)
+
+    @classmethod
     def from_tets(cls, xyz, tets, tris, tri_indicator, nlevels=3):
         """xyz (N,3), tets (T,4), tris (F,3) 1-based, indicators (F,) in 1..9."""
         xyz = np.asfortranarray(np.asarray(xyz, dtype=np.float64))

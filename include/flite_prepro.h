@@ -35,6 +35,12 @@ int fp_bump_channel(int nx, int ny, int nz, double bump_h, int nlevels,
 int fp_from_tets(int32_t nnodes, const double *xyz, int32_t ntet,
                  const int32_t *tets, int32_t ntri, const int32_t *tris,
                  const int32_t *tri_ind, int nlevels, fp_mesh **out);
+/* Extruded NACA0012 O-grid: ni points around the section, nj cells from the
+ * wall (nlayer cells from first_cell growing by `growth`, then stretched to a
+ * circular far field of radius `farfield` chords), nk cells over `span`.
+ * Wall 1, span ends 2 (symmetry), far field 3.                              */
+int fp_naca0012(int ni, int nj, int nk, double first_cell, double growth, int nlayer, double farfield,
+                double span, int nlevels, fp_mesh **out);
 int fp_free(fp_mesh *m);
 
 int fp_num_levels(const fp_mesh *m);

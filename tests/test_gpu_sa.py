@@ -78,3 +78,24 @@ def test_sa_rejected_without_viscosity():
     c = default_controls(**{**BASE, "ReynoldsNumber": 0.0, "numberOfGridsToUse": 1})
     with pytest.raises(RuntimeError):
         Solver(c, mesh)
+
+
+@pytest.mark.parametrize("flux", [1, 4])
+def test_sa_naca0012_rans_bitwise(flux):
+    # the RANS configuration's geometry (extruded NACA0012, M 0.8, alpha 1.25,
+    # Re 6e6) at a coarse resolution: far field, airfoil wall and span
+    # symmetry planes with the SA model
+    mesh = Mesh.naca0012(64, 24, 4, first_cell=1e-3, growth=1.2, nlayer=10, farfield=10.0, span=0.5,
+                         nlevels=3)
+    c = default_controls(ReynoldsNumber=6.0e6, MachNumber=0.8, alpha=1.25, CFLNumber=1.0, fluxType=flux,
+                         HLLCFluxOrder=2, Automaticlipping=1, multigridScheme=3, numberOfGridsToUse=3,
+                         turbulenceModel=1, wallsAreIsentropic=1)
+    g, o = Solver(c, mesh), Solver(c, mesh, backend=oracle_backend())
+    for s in (g, o):
+        s.init_freestream()
+        s.start()
+    for cyc in range(1, 4):
+        g.cycle(cyc)
+        o.cycle(cyc)
+        assert_same(g, o, f"naca flux {flux} cycle {cyc}")
+    np.testing.assert_allclose(g.forces(), o.forces(), rtol=1e-12, atol=1e-15)

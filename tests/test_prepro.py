@@ -135,3 +135,19 @@ def test_plt_and_plotreg(tmp_path):
     raw = (tmp_path / "base.plt").read_bytes()
     head = np.frombuffer(raw[4:16], dtype=np.int32)
     assert head.tolist() == [6 * 6 * 2 * 2, 7 * 3 * 3, 2 * (2 * 6 * 2 + 2 * 6 * 2 + 2 * 2 * 2)]
+
+
+def test_naca0012_generator():
+    from flite3d_b200 import Mesh
+    m = Mesh.naca0012(64, 24, 4, first_cell=1e-3, growth=1.2, nlayer=10, farfield=10.0, span=0.5, nlevels=3)
+    d = m.level(1)
+    assert d.n_nodes == 64 * 25 * 5
+    closure, volume = m.check(1)
+    assert closure < 1e-13
+    # the O-grid's polygonal far field of 64 sides, less the section, over the span
+    poly = 0.5 * 64 * 10.0 ** 2 * np.sin(2 * np.pi / 64) * 0.5
+    assert abs(volume - poly) < 0.01 * poly
+    ind = set(int(v) for v in m.array(1, "bnd_idx").reshape(3, -1)[2])
+    assert ind == {1, 2, 3}
+    wd = m.array(1, "wall_dist")
+    assert wd.min() >= 0.0 and wd.max() <= 10.5
