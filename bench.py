@@ -130,10 +130,10 @@ def node_kernel_bytes(mesh):
 
 # DRAM traffic of the dominant kernel per algorithmic byte, from an ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
-# 192x64x64 bump channel (469.5 MB measured against 461.8 MB algorithmic);
+# 192x64x64 bump channel (462.0 MB measured against 448.8 MB algorithmic);
 # the bench mesh is too large to capture with --set full, and the traffic
 # scales with the nodes and edges processed
-NCU_TRAFFIC_PER_ALGORITHMIC_BYTE = 469.521408 / 461.847625
+NCU_TRAFFIC_PER_ALGORITHMIC_BYTE = 461.967872 / 448.800825
 
 
 def run_ours(args):
@@ -361,8 +361,15 @@ def cpu_baseline(mesh, c, u0, cycles=2):
     for i in range(cycles):
         o.cycle(2 + i)
     dt = time.perf_counter() - t0
+    # the same restatement on one thread (the reference's loop order)
+    lib.oracle_set_threads(1)
+    t1 = time.perf_counter()
+    o.cycle(2 + cycles)
+    dt1 = time.perf_counter() - t1
+    lib.oracle_set_threads(threads)
     o.close()
     return {"value": cycles / dt, "unit": "cycles/s", "cores": threads, "kind": "port",
+            "single_thread": {"value": 1.0 / dt1, "cycles": 1},
             "sample": f"{cycles} cycles of the same 2.1M-node workload after one warm-up cycle, "
                       f"FP64 C++ restatement on {threads} threads (edge loops over coloured "
                       "blocks of edges)"}
