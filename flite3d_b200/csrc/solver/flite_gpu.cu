@@ -24,6 +24,10 @@
 
 namespace {
 
+// Message of the calling thread's last failed flite_create/flite_batch_create,
+// which leave no context to hold it; flite_last_error(NULL, ...) returns it.
+thread_local std::string t_create_err;
+
 int fail(flite_ctx *ctx, int code, const std::string &msg) {
     if (ctx) ctx->err = msg;
     return code;
@@ -75,8 +79,8 @@ const char *unsupported_reason(const flite_controls &c) {
 extern "C" {
 
 int flite_last_error(const flite_ctx *ctx, char *buf, size_t len) {
-    if (!ctx || !buf || !len) return FLITE_EINVAL;
-    std::snprintf(buf, len, "%s", ctx->err.c_str());
+    if (!buf || !len) return FLITE_EINVAL;
+    std::snprintf(buf, len, "%s", ctx ? ctx->err.c_str() : t_create_err.c_str());
     return FLITE_OK;
 }
 
@@ -87,9 +91,16 @@ int flite_last_error(const flite_ctx *ctx, char *buf, size_t len) {
 // operators, geometry) is shared and only the solution state is allocated.
 int flite::create_context(const flite_controls *c, int nlevels, const flite_level_desc *levels,
                           const flite_ctx *donor, flite_ctx **out) {
-    if (!c || !levels || !out || nlevels < 1) return FLITE_EINVAL;
+    t_create_err.clear();
+    if (!c || !levels || !out || nlevels < 1) {
+        t_create_err = "null argument or nlevels < 1";
+        return FLITE_EINVAL;
+    }
     *out = nullptr;
-    if (unsupported_reason(*c)) return FLITE_EUNSUPPORTED;
+    if (const char *why = unsupported_reason(*c)) {
+        t_create_err = why;
+        return FLITE_EUNSUPPORTED;
+    }
     auto ctx = std::make_unique<flite_ctx>();
     int rc = guarded(ctx.get(), [&]() -> int {
         flite_ctx &X = *ctx;
@@ -336,7 +347,10 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         CK(cudaDeviceSynchronize());
         return FLITE_OK;
     });
-    if (rc != FLITE_OK) return rc;
+    if (rc != FLITE_OK) {
+        t_create_err = ctx->err;
+        return rc;
+    }
     *out = ctx.release();
     return FLITE_OK;
 }

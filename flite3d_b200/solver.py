@@ -78,7 +78,8 @@ class Solver:
         self._h = _vp()
         rc = self.be.create(ctypes.byref(controls), mesh.nlevels, mesh.descs, ctypes.byref(self._h))
         if rc != _abi.FLITE_OK:
-            raise RuntimeError(f"create failed with status {rc}")
+            why = self._err()
+            raise RuntimeError(f"create failed with status {rc}" + (f": {why}" if why else ""))
         ng = mesh.nlevels
         if controls.numberOfGridsToUse > 0:
             ng = min(ng, controls.numberOfGridsToUse)

@@ -11,7 +11,8 @@
  *
  * Every function returns an int status (FLITE_OK on success).  The reference
  * STOPs on errors; this library returns a code and keeps a message that
- * flite_last_error() retrieves.
+ * flite_last_error() retrieves; with a NULL context it returns the message of
+ * the calling thread's last failed flite_create or flite_batch_create.
  */
 #ifndef FLITE_GPU_H
 #define FLITE_GPU_H

@@ -43,3 +43,8 @@ def test_create_rejects_unsupported_controls():
         c = default_controls(**bad)
         rc = lib.flite_create(ctypes.byref(c), m.nlevels, m.descs, ctypes.byref(h))
         assert rc == _abi.FLITE_EUNSUPPORTED, bad
+        # the reason is kept for the calling thread, retrieved with a NULL context
+        buf = ctypes.create_string_buffer(256)
+        assert lib.flite_last_error(None, buf, len(buf)) == _abi.FLITE_OK
+        assert buf.value, bad
+    assert b"multigridScheme" in buf.value
