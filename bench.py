@@ -155,21 +155,29 @@ def run_ours(args):
     # block size and gather unroll by the level-1 node kernel, then the level
     # size below which gathers use a warp per node by the time of whole cycles
     tuning = {}
-    for nb in (128, 256):
-        for unroll in (1, 2):
-            solver.set_kernel_options(256, nb, unroll)
-            tuning[(nb, unroll)] = solver.profile_level(1, reps=5)[1]
-    best = min(tuning, key=tuning.get)
+    if args.kernel_options:
+        # fixed options (profiling runs: no tuning launches before the cycles)
+        v = [int(x) for x in args.kernel_options.split(",")]
+        best = (v[0], v[1])
+        lanes = {lvl: v[1 + lvl] for lvl in range(1, solver.nlevels + 1)}
+    else:
+        for nb in (128, 256):
+            for unroll in (1, 2):
+                solver.set_kernel_options(256, nb, unroll)
+                tuning[(nb, unroll)] = solver.profile_level(1, reps=5)[1]
+        best = min(tuning, key=tuning.get)
     solver.set_kernel_options(256, best[0], best[1])
     # lanes per node of each level's gathers, by the device time of that
     # level's kernels over one relaxation step
-    lanes = {}
+    if not args.kernel_options:
+        lanes = {}
+        for lvl in range(1, solver.nlevels + 1):
+            t = {}
+            for g in ((1, 4, 8) if lvl == 1 else (1, 4, 8, 16, 32)):
+                solver.set_gather_lanes(lvl, g)
+                t[g] = sum(solver.profile_kernels(lvl, reps=5).values())
+            lanes[lvl] = min(t, key=t.get)
     for lvl in range(1, solver.nlevels + 1):
-        t = {}
-        for g in ((1, 4, 8) if lvl == 1 else (1, 4, 8, 16, 32)):
-            solver.set_gather_lanes(lvl, g)
-            t[g] = sum(solver.profile_kernels(lvl, reps=5).values())
-        lanes[lvl] = min(t, key=t.get)
         solver.set_gather_lanes(lvl, lanes[lvl])
     solver.set_state(u0)
     solver.start()
@@ -515,6 +523,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mesh", default=None, help="NX,NY,NZ hexes (default 264,88,88)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the FLITE_MIXED cycle rate")
+    ap.add_argument("--kernel-options", default=None,
+                    help="NODE_BLOCK,UNROLL,LANES_L1,...: fixed launch options instead of tuning them")
     ap.add_argument("--converge", action="store_true",
                     help="also measure time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
     ap.add_argument("--converge-max", type=int, default=3000)
