@@ -144,16 +144,109 @@ class PairMap {
 
 inline uint64_t pkey(int64_t a, int64_t b) { return ((uint64_t)a << 32) | (uint64_t)(uint32_t)b; }
 
-struct V3 { double x, y, z; };
-inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-inline V3 scl(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
-inline V3 div3(V3 a) { return {a.x / 3., a.y / 3., a.z / 3.}; }
+// 3-vectors of a scalar type S: double, or the forward-mode numbers of the
+// geometry derivative below
+template <class S>
+struct V3T { S x, y, z; };
+using V3 = V3T<double>;
+template <class S> inline V3T<S> operator+(V3T<S> a, V3T<S> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class S> inline V3T<S> operator-(V3T<S> a, V3T<S> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class S> inline V3T<S> scl(double s, V3T<S> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class S> inline V3T<S> div3(V3T<S> a) { return {a.x / 3., a.y / 3., a.z / 3.}; }
 
 // Cxx(1,:) = 0.5*(r1(2)*r2(3)-r1(3)*r2(2)) ... (gen3d_grid.f90:799-804)
-inline V3 halfcross(V3 r1, V3 r2) {
+template <class S>
+inline V3T<S> halfcross(V3T<S> r1, V3T<S> r2) {
     return {0.5 * (r1.y * r2.z - r1.z * r2.y), 0.5 * (r1.z * r2.x - r1.x * r2.z),
             0.5 * (r1.x * r2.y - r1.y * r2.x)};
+}
+
+// Forward-mode number with K derivative slots (the geometry derivative with
+// respect to the K vertex coordinates of one element)
+template <int K>
+struct DN {
+    double v = 0, d[K] = {};
+};
+template <int K> inline DN<K> operator+(const DN<K> &a, const DN<K> &b) {
+    DN<K> o; o.v = a.v + b.v;
+    for (int k = 0; k < K; ++k) o.d[k] = a.d[k] + b.d[k];
+    return o;
+}
+template <int K> inline DN<K> operator-(const DN<K> &a, const DN<K> &b) {
+    DN<K> o; o.v = a.v - b.v;
+    for (int k = 0; k < K; ++k) o.d[k] = a.d[k] - b.d[k];
+    return o;
+}
+template <int K> inline DN<K> operator*(const DN<K> &a, const DN<K> &b) {
+    DN<K> o; o.v = a.v * b.v;
+    for (int k = 0; k < K; ++k) o.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return o;
+}
+template <int K> inline DN<K> operator*(double s, const DN<K> &a) {
+    DN<K> o; o.v = s * a.v;
+    for (int k = 0; k < K; ++k) o.d[k] = s * a.d[k];
+    return o;
+}
+template <int K> inline DN<K> operator/(const DN<K> &a, double s) {
+    DN<K> o; o.v = a.v / s;
+    for (int k = 0; k < K; ++k) o.d[k] = a.d[k] / s;
+    return o;
+}
+
+// The six sides of a tetrahedron with positively oriented vertices x[0..3],
+// in the order of makeCalcDataForTet (gen3d_grid.f90:2092-2332): the local
+// vertex pair, half the side coefficient Cxx of its two dual-face triangles
+// (registerSideGCL :786-855) and the nodal-volume share rv.Cxx/3 that both
+// vertices receive.
+template <class S>
+struct TetSide { int a, b; V3T<S> coef; S nv; };
+template <class S>
+void tet_sides(const V3T<S> *x, TetSide<S> *out) {
+    int n = 0;
+    auto side = [&](int a, int b, V3T<S> r1, V3T<S> r2, V3T<S> r3, V3T<S> r4, V3T<S> rv) {
+        V3T<S> c1 = halfcross(r1, r2), c2 = halfcross(r3, r4);
+        V3T<S> cxx = c1 + c2;
+        out[n].a = a; out[n].b = b;
+        out[n].nv = (rv.x * cxx.x + rv.y * cxx.y + rv.z * cxx.z) / 3.;
+        out[n].coef = scl(0.5, cxx);
+        ++n;
+    };
+    const V3T<S> x1 = x[0], x2 = x[1], x3 = x[2], x4 = x[3];
+    V3T<S> xmm = scl(0.25, x1 + x2 + x3 + x4);
+    {   // node 1
+        V3T<S> xm1 = scl(0.5, x1 + x2), xm2 = scl(0.5, x1 + x3), xm3 = scl(0.5, x1 + x4);
+        V3T<S> xb1 = div3(x1 + x2 + x3), xb2 = div3(x1 + x2 + x4), xb3 = div3(x1 + x3 + x4);
+        side(0, 1, xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x1);
+        side(0, 2, xmm - xm2, xb1 - xm2, xb3 - xm2, xmm - xm2, xm2 - x1);
+        side(0, 3, xmm - xm3, xb3 - xm3, xb2 - xm3, xmm - xm3, xm3 - x1);
+    }
+    {   // node 2
+        V3T<S> xm1 = scl(0.5, x2 + x3), xm2 = scl(0.5, x2 + x4);
+        V3T<S> xb1 = div3(x1 + x2 + x3), xb2 = div3(x2 + x3 + x4), xb3 = div3(x1 + x2 + x4);
+        side(1, 2, xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x2);
+        side(1, 3, xmm - xm2, xb3 - xm2, xb2 - xm2, xmm - xm2, xm2 - x2);
+    }
+    {   // node 3
+        V3T<S> xm1 = scl(0.5, x3 + x4);
+        V3T<S> xb1 = div3(x1 + x3 + x4), xb2 = div3(x2 + x3 + x4);
+        side(2, 3, xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x3);
+    }
+}
+
+// The three sides of a boundary triangle oriented into the domain, in the
+// order of makeCalcDataForBoundary (gen3d_boundary.f90:511-620): the local
+// vertex pair and the quarter of Cxx that registerBoundarySideGCL (:289-372)
+// adds to the boundary side.
+template <class S>
+struct TriSide { int a, b; V3T<S> coef; };
+template <class S>
+void tri_sides(const V3T<S> *x, TriSide<S> *out) {
+    const V3T<S> x1 = x[0], x2 = x[1], x3 = x[2];
+    V3T<S> xm = div3(x1 + x2 + x3);
+    V3T<S> xb1 = scl(0.5, x1 + x2), xb2 = scl(0.5, x2 + x3), xb3 = scl(0.5, x3 + x1);
+    out[0] = {0, 1, scl(0.25, halfcross(xm - x1, xb1 - x1))};
+    out[1] = {0, 2, scl(0.25, halfcross(xb3 - x1, xm - x1))};
+    out[2] = {1, 2, scl(0.25, halfcross(xm - x2, xb2 - x2))};
 }
 
 // Indicator priority of setBoundIndForViscousMesh (gen3d_boundary.f90:
@@ -312,13 +405,11 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
     sc.reserve(NT * 7 / 6 + 16); sl.reserve(NT * 7 / 6 + 16);
     L.vol.assign(N, 0.0);
     int64_t nneg = 0;
-    auto register_side = [&](int32_t p1, int32_t p2, V3 r1, V3 r2, V3 r3, V3 r4, V3 rv) -> double {
-        V3 c1 = halfcross(r1, r2), c2 = halfcross(r3, r4);
-        V3 cxx = c1 + c2;
-        double nv = (rv.x * cxx.x + rv.y * cxx.y + rv.z * cxx.z) / 3.;
+    auto register_side = [&](int32_t p1, int32_t p2, const TetSide<double> &ts) -> double {
+        const double nv = ts.nv;
         L.vol[p1 - 1] += nv;
         L.vol[p2 - 1] += nv;
-        V3 coef = scl(0.5, cxx);  // store half the side coefficient
+        V3 coef = ts.coef;  // half the side coefficient
         V3 d = X(p2) - X(p1);
         double len = std::sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
         int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
@@ -359,27 +450,11 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         }
         tets_old[t] = p[0]; tets_old[(size_t)NT + t] = p[1];
         tets_old[2 * (size_t)NT + t] = p[2]; tets_old[3 * (size_t)NT + t] = p[3];
-        V3 x1 = X(p[0]), x2 = X(p[1]), x3 = X(p[2]), x4 = X(p[3]);
-        V3 xmm = scl(0.25, x1 + x2 + x3 + x4);
+        const V3 xv[4] = {X(p[0]), X(p[1]), X(p[2]), X(p[3])};
+        TetSide<double> ts[6];
+        tet_sides(xv, ts);
         double ev = 0;
-        {   // node 1
-            V3 xm1 = scl(0.5, x1 + x2), xm2 = scl(0.5, x1 + x3), xm3 = scl(0.5, x1 + x4);
-            V3 xb1 = div3(x1 + x2 + x3), xb2 = div3(x1 + x2 + x4), xb3 = div3(x1 + x3 + x4);
-            ev += 2. * register_side(p[0], p[1], xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x1);
-            ev += 2. * register_side(p[0], p[2], xmm - xm2, xb1 - xm2, xb3 - xm2, xmm - xm2, xm2 - x1);
-            ev += 2. * register_side(p[0], p[3], xmm - xm3, xb3 - xm3, xb2 - xm3, xmm - xm3, xm3 - x1);
-        }
-        {   // node 2
-            V3 xm1 = scl(0.5, x2 + x3), xm2 = scl(0.5, x2 + x4);
-            V3 xb1 = div3(x1 + x2 + x3), xb2 = div3(x2 + x3 + x4), xb3 = div3(x1 + x2 + x4);
-            ev += 2. * register_side(p[1], p[2], xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x2);
-            ev += 2. * register_side(p[1], p[3], xmm - xm2, xb3 - xm2, xb2 - xm2, xmm - xm2, xm2 - x2);
-        }
-        {   // node 3
-            V3 xm1 = scl(0.5, x3 + x4);
-            V3 xb1 = div3(x1 + x3 + x4), xb2 = div3(x2 + x3 + x4);
-            ev += 2. * register_side(p[2], p[3], xmm - xm1, xb2 - xm1, xb1 - xm1, xmm - xm1, xm1 - x3);
-        }
+        for (int k = 0; k < 6; ++k) ev += 2. * register_side(p[ts[k].a], p[ts[k].b], ts[k]);
         if (ev <= 0) ++nneg;
     }
     delete tm_edges;
@@ -434,14 +509,13 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
     PairMap bmap((size_t)NF * 2 + 16);
     std::vector<int32_t> b1, b2, bi;
     std::vector<V3> bc;
-    auto register_bside = [&](int32_t p1, int32_t p2, V3 r1, V3 r2, int ind) {
-        V3 cxx = halfcross(r1, r2);
+    auto register_bside = [&](int32_t p1, int32_t p2, V3 coef, int ind) {
         int32_t i1 = std::min(p1, p2), i2 = std::max(p1, p2);
         int64_t slot = bmap.find_or_insert(pkey(i1, i2), (int64_t)b1.size());
         if (slot >= 0) {
-            bc[slot] = bc[slot] + scl(0.25, cxx);
+            bc[slot] = bc[slot] + coef;
         } else {
-            b1.push_back(i1); b2.push_back(i2); bi.push_back(ind); bc.push_back(scl(0.25, cxx));
+            b1.push_back(i1); b2.push_back(i2); bi.push_back(ind); bc.push_back(coef);
         }
     };
     std::vector<int32_t> tris_new(3 * (size_t)NF);
@@ -453,12 +527,11 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         if (n.x * d.x + n.y * d.y + n.z * d.z < 0) std::swap(p2, p3);
         tris_new[f] = p1; tris_new[(size_t)NF + f] = p2; tris_new[2 * (size_t)NF + f] = p3;
         int ind = tri_ind[f];
-        V3 x1 = X(p1), x2 = X(p2), x3 = X(p3);
-        V3 xm = div3(x1 + x2 + x3);
-        V3 xb1 = scl(0.5, x1 + x2), xb2 = scl(0.5, x2 + x3), xb3 = scl(0.5, x3 + x1);
-        register_bside(p1, p2, xm - x1, xb1 - x1, ind);
-        register_bside(p1, p3, xb3 - x1, xm - x1, ind);
-        register_bside(p2, p3, xm - x2, xb2 - x2, ind);
+        const int32_t pv[3] = {p1, p2, p3};
+        const V3 xv[3] = {X(p1), X(p2), X(p3)};
+        TriSide<double> ts[3];
+        tri_sides(xv, ts);
+        for (int k = 0; k < 3; ++k) register_bside(pv[ts[k].a], pv[ts[k].b], ts[k].coef, ind);
     }
     L.B = (int32_t)b1.size();
     L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B);
@@ -656,6 +729,139 @@ void build_levels(fp_mesh &M, int nlevels) {
         M.lv.push_back(std::move(C));
     }
 }
+
+// level-1 side numbers by node pair: for the smaller (1-based) node of a
+// pair, the larger nodes of its sides and the sides' 0-based numbers
+struct PairIndex {
+    std::vector<int32_t> ptr, other, id;
+    PairIndex(int32_t N, int32_t n, const int32_t *first, const int32_t *second) : ptr(N + 2, 0) {
+        for (int32_t e = 0; e < n; ++e) ++ptr[std::min(first[e], second[e]) + 1];
+        for (int32_t i = 0; i <= N; ++i) ptr[i + 1] += ptr[i];
+        other.resize(n); id.resize(n);
+        std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1);
+        for (int32_t e = 0; e < n; ++e) {
+            int32_t a = std::min(first[e], second[e]), b = std::max(first[e], second[e]);
+            other[pos[a]] = b; id[pos[a]++] = e;
+        }
+    }
+    int32_t find(int32_t a, int32_t b) const {
+        for (int32_t q = ptr[a]; q < ptr[a + 1]; ++q)
+            if (other[q] == b) return id[q];
+        throw std::runtime_error("element side not in the mesh's side list");
+    }
+};
+
+// The level-1 geometry of the mesh's own (oriented) tetrahedra and boundary
+// triangles at the coordinates xyz, accumulated in the element order of
+// build_fine so that the mesh's own coordinates give its arrays back bit for
+// bit; with DN numbers, the derivative with respect to each element's vertex
+// coordinates.
+struct Geometry {
+    const fp_mesh &M;
+    const LevelData &L;
+    PairIndex sides, bsides;
+    int32_t NT, NF;
+    explicit Geometry(const fp_mesh &m)
+        : M(m), L(m.lv.at(0)),
+          sides(L.N, L.E, L.side.data(), L.side.data() + L.E),
+          bsides(L.N, L.B, L.bside.data(), L.bside.data() + L.B),
+          NT((int32_t)(m.tets.size() / 4)), NF((int32_t)(m.tris.size() / 3)) {}
+    V3 X(const double *xyz, int32_t p) const {
+        return {xyz[p - 1], xyz[(size_t)L.N + p - 1], xyz[2 * (size_t)L.N + p - 1]};
+    }
+    void tet(int32_t t, int32_t *p) const {
+        for (int k = 0; k < 4; ++k) p[k] = M.tets[(size_t)k * NT + t];
+    }
+    void tri(int32_t f, int32_t *p) const {
+        for (int k = 0; k < 3; ++k) p[k] = M.tris[(size_t)k * NF + f];
+    }
+    void eval(const double *xyz, double *sw, double *bw, double *vol) const {
+        const size_t E = L.E, B = L.B;
+        std::fill(sw, sw + 3 * E, 0.0);
+        std::fill(bw, bw + 3 * B, 0.0);
+        std::fill(vol, vol + L.N, 0.0);
+        for (int32_t t = 0; t < NT; ++t) {
+            int32_t p[4];
+            tet(t, p);
+            const V3 xv[4] = {X(xyz, p[0]), X(xyz, p[1]), X(xyz, p[2]), X(xyz, p[3])};
+            TetSide<double> ts[6];
+            tet_sides(xv, ts);
+            for (int k = 0; k < 6; ++k) {
+                int32_t p1 = p[ts[k].a], p2 = p[ts[k].b];
+                vol[p1 - 1] += ts[k].nv;
+                vol[p2 - 1] += ts[k].nv;
+                V3 coef = ts[k].coef;
+                int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
+                if (i1 != p1) coef = scl(-1.0, coef);
+                const int32_t e = sides.find(i1, i2);
+                sw[e] = sw[e] + coef.x; sw[E + e] = sw[E + e] + coef.y; sw[2 * E + e] = sw[2 * E + e] + coef.z;
+            }
+        }
+        for (int32_t f = 0; f < NF; ++f) {
+            int32_t p[3];
+            tri(f, p);
+            const V3 xv[3] = {X(xyz, p[0]), X(xyz, p[1]), X(xyz, p[2])};
+            TriSide<double> ts[3];
+            tri_sides(xv, ts);
+            for (int k = 0; k < 3; ++k) {
+                const int32_t b = bsides.find(std::min(p[ts[k].a], p[ts[k].b]), std::max(p[ts[k].a], p[ts[k].b]));
+                const V3 c = ts[k].coef;
+                bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
+            }
+        }
+    }
+    // xyz_bar = (d(sw, bw, vol)/d xyz)^T (sw_bar, bw_bar, vol_bar)
+    void vjp(const double *xyz, const double *swb, const double *bwb, const double *volb, double *xb) const {
+        const size_t E = L.E, B = L.B, N = L.N;
+        std::fill(xb, xb + 3 * N, 0.0);
+        for (int32_t t = 0; t < NT; ++t) {
+            int32_t p[4];
+            tet(t, p);
+            V3T<DN<12>> xv[4];
+            for (int k = 0; k < 4; ++k) {
+                const V3 x = X(xyz, p[k]);
+                xv[k].x.v = x.x; xv[k].y.v = x.y; xv[k].z.v = x.z;
+                xv[k].x.d[3 * k] = 1.0; xv[k].y.d[3 * k + 1] = 1.0; xv[k].z.d[3 * k + 2] = 1.0;
+            }
+            TetSide<DN<12>> ts[6];
+            tet_sides(xv, ts);
+            double g[12] = {};
+            for (int k = 0; k < 6; ++k) {
+                int32_t p1 = p[ts[k].a], p2 = p[ts[k].b];
+                int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
+                const double sg = i1 != p1 ? -1.0 : 1.0;
+                const int32_t e = sides.find(i1, i2);
+                const double cb[3] = {sg * swb[e], sg * swb[E + e], sg * swb[2 * E + e]};
+                const double vb = volb[p1 - 1] + volb[p2 - 1];
+                for (int j = 0; j < 12; ++j)
+                    g[j] += ((cb[0] * ts[k].coef.x.d[j] + cb[1] * ts[k].coef.y.d[j]) + cb[2] * ts[k].coef.z.d[j]) +
+                            vb * ts[k].nv.d[j];
+            }
+            for (int k = 0; k < 4; ++k)
+                for (int c = 0; c < 3; ++c) xb[(size_t)c * N + p[k] - 1] += g[3 * k + c];
+        }
+        for (int32_t f = 0; f < NF; ++f) {
+            int32_t p[3];
+            tri(f, p);
+            V3T<DN<9>> xv[3];
+            for (int k = 0; k < 3; ++k) {
+                const V3 x = X(xyz, p[k]);
+                xv[k].x.v = x.x; xv[k].y.v = x.y; xv[k].z.v = x.z;
+                xv[k].x.d[3 * k] = 1.0; xv[k].y.d[3 * k + 1] = 1.0; xv[k].z.d[3 * k + 2] = 1.0;
+            }
+            TriSide<DN<9>> ts[3];
+            tri_sides(xv, ts);
+            double g[9] = {};
+            for (int k = 0; k < 3; ++k) {
+                const int32_t b = bsides.find(std::min(p[ts[k].a], p[ts[k].b]), std::max(p[ts[k].a], p[ts[k].b]));
+                for (int j = 0; j < 9; ++j)
+                    g[j] += (bwb[b] * ts[k].coef.x.d[j] + bwb[B + b] * ts[k].coef.y.d[j]) + bwb[2 * B + b] * ts[k].coef.z.d[j];
+            }
+            for (int k = 0; k < 3; ++k)
+                for (int c = 0; c < 3; ++c) xb[(size_t)c * N + p[k] - 1] += g[3 * k + c];
+        }
+    }
+};
 
 template <class F>
 int guarded(F &&f) {
@@ -905,6 +1111,26 @@ int fp_node_perm(const fp_mesh *m, int32_t *perm) {
     if (!m || !perm || m->perm.empty()) return FLITE_EINVAL;
     std::memcpy(perm, m->perm.data(), m->perm.size() * 4);
     return FLITE_OK;
+}
+
+int fp_geometry(const fp_mesh *m, const double *xyz, double *side_w, double *bnd_w, double *volume) {
+    if (!m || m->lv.empty() || m->tets.empty() || !side_w || !bnd_w || !volume) return FLITE_EINVAL;
+    return guarded([&] {
+        Geometry G(*m);
+        G.eval(xyz ? xyz : m->lv[0].xyz.data(), side_w, bnd_w, volume);
+        return FLITE_OK;
+    });
+}
+
+int fp_geometry_vjp(const fp_mesh *m, const double *xyz, const double *side_w_bar, const double *bnd_w_bar,
+                    const double *volume_bar, double *xyz_bar) {
+    if (!m || m->lv.empty() || m->tets.empty() || !side_w_bar || !bnd_w_bar || !volume_bar || !xyz_bar)
+        return FLITE_EINVAL;
+    return guarded([&] {
+        Geometry G(*m);
+        G.vjp(xyz ? xyz : m->lv[0].xyz.data(), side_w_bar, bnd_w_bar, volume_bar, xyz_bar);
+        return FLITE_OK;
+    });
 }
 
 int fp_check(const fp_mesh *m, int level, double *closure, double *volume) {

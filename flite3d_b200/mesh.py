@@ -108,6 +108,36 @@ class Mesh:
                    "fp_check")
         return closure.value, vol.value
 
+    def geometry(self, xyz=None):
+        """Level-1 side_w (3, E), bnd_w (3, B) and volume (N) of the mesh's
+        own elements at the node coordinates xyz (3, N) (None: the mesh's)."""
+        d = self.level(1)
+        sw = np.zeros((3, d.n_sides)); bw = np.zeros((3, d.n_bsides)); vol = np.zeros(d.n_nodes)
+        x = None if xyz is None else np.ascontiguousarray(xyz, dtype=np.float64)
+        _abi.check(_lib().fp_geometry(self._h, None if x is None else x.ctypes.data_as(ctypes.c_void_p),
+                                      sw.ctypes.data_as(ctypes.c_void_p), bw.ctypes.data_as(ctypes.c_void_p),
+                                      vol.ctypes.data_as(ctypes.c_void_p)), "fp_geometry")
+        return sw, bw, vol
+
+    def geometry_vjp(self, side_w_bar, bnd_w_bar, volume_bar, xyz=None):
+        """(d geometry / d xyz)^T applied to the three geometry adjoints:
+        the sensitivity (3, N) of a function of the level-1 geometry to the
+        node coordinates."""
+        d = self.level(1)
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (side_w_bar, bnd_w_bar, volume_bar)]
+        xb = np.zeros((3, d.n_nodes))
+        x = None if xyz is None else np.ascontiguousarray(xyz, dtype=np.float64)
+        _abi.check(_lib().fp_geometry_vjp(self._h, None if x is None else x.ctypes.data_as(ctypes.c_void_p),
+                                          *[v.ctypes.data_as(ctypes.c_void_p) for v in a],
+                                          xb.ctypes.data_as(ctypes.c_void_p)), "fp_geometry_vjp")
+        return xb
+
+    def with_level1_geometry(self, side_w, bnd_w, volume):
+        """Level descriptors of this mesh with level 1's side_w, bnd_w and
+        volume replaced (the arrays are kept alive by the returned object,
+        which has the nlevels / descs / level() of a Mesh for Solver)."""
+        return _GeometryView(self, side_w, bnd_w, volume)
+
     def array(self, level, name):
         """Copy of one level array as numpy (column-major fields as (k, n))."""
         d = self.level(level)
@@ -131,6 +161,25 @@ class Mesh:
         ctype = ctypes.c_int32 if dt == np.int32 else ctypes.c_double
         buf = (ctype * count).from_address(ptr)
         return np.frombuffer(buf, dtype=dt, count=count).reshape(shape).copy()
+
+
+class _GeometryView:
+    """A mesh whose level-1 geometry arrays are replaced (perturbed meshes of
+    finite-difference checks, moved surfaces)."""
+
+    def __init__(self, mesh, side_w, bnd_w, volume):
+        self.mesh = mesh
+        self._keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (side_w, bnd_w, volume)]
+        self.nlevels = mesh.nlevels
+        self.descs = (_abi.LevelDesc * mesh.nlevels)(*[mesh.level(l + 1) for l in range(mesh.nlevels)])
+        d = self.descs[0]
+        d.side_w, d.bnd_w, d.volume = [a.ctypes.data_as(ctypes.c_void_p) for a in self._keep]
+
+    def level(self, level):
+        return self.descs[level - 1]
+
+    def array(self, level, name):
+        return self.mesh.array(level, name)
 
 
 # ---- restart / result files ---------------------------------------------

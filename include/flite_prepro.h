@@ -52,6 +52,18 @@ int fp_node_perm(const fp_mesh *m, int32_t *perm);
 /* Max closure error |sum_j +-w_ij + 2 sum_b w_b| over nodes, relative to
  * max |w| (def_par:14430-14568), and total volume.                         */
 int fp_check(const fp_mesh *m, int level, double *closure, double *volume);
+/* Level-1 geometry of the mesh's own tetrahedra and boundary triangles at
+ * node coordinates xyz [3][N] (boundary-first numbering; NULL = the mesh's
+ * own): side_w [3][E], bnd_w [3][B] and volume [N] in the mesh's side and
+ * boundary-side order (makeCalcDataForTet gen3d_grid.f90:2092-2332,
+ * makeCalcDataForBoundary gen3d_boundary.f90:511-620).  The mesh's own
+ * coordinates give its level-1 arrays back.  Meshes read from a .sol hold
+ * no elements: FLITE_EINVAL.                                                */
+int fp_geometry(const fp_mesh *m, const double *xyz, double *side_w, double *bnd_w, double *volume);
+/* Transpose of the derivative of fp_geometry at xyz: xyz_bar [3][N] =
+ * (d(side_w, bnd_w, volume)/d xyz)^T (side_w_bar, bnd_w_bar, volume_bar).   */
+int fp_geometry_vjp(const fp_mesh *m, const double *xyz, const double *side_w_bar, const double *bnd_w_bar,
+                    const double *volume_bar, double *xyz_bar);
 
 /* ---- files (Fortran sequential unformatted, 4-byte record markers) ---- */
 int fp_write_sol(const fp_mesh *m, const char *path);

@@ -1651,6 +1651,335 @@ void tan_farfield(const flite_controls &c, const Dl *q, Dl pr, const double *n, 
     Dl ex[5] = {cc1, cc1 * ui + cc2 * n[0], cc1 * vi + cc2 * n[1], cc1 * wi + cc2 * n[2], cc1 * hi + cc2 * ucp};
     for (int k = 0; k < 5; ++k) F[k] = Dl(0.5) * (Dl(fr[k]) + fl[k]) - Dl(0.5) * (l3 * du[k] + ex[k]);
 }
+
+// ---- tangent of one smoother iteration on level 1 ------------------------
+// singleIteration with calcDiss (def_par:1002-1181) for the central flux
+// (fluxType 1), scalar JST dissipation (def_par:11484-11993) and an inviscid
+// run, restated with dual numbers whose derivative part carries one
+// direction in the state u and in the level-1 geometry (side_w, bnd_w,
+// volume; the node normals and wall areas follow from bnd_w as in
+// makeBoundaryNormals def_par:15394-15521 and makeSurfaceArea :15523-15634).
+// The value parts repeat the double routines' operations in their order, so
+// they equal one doTimeIterations step of this restatement bit for bit.
+inline Dl dmaxl(Dl a, Dl b) { return a.v < b.v ? b : a; }        // std::max
+inline Dl dminl(Dl a, Dl b) { return b.v < a.v ? b : a; }        // std::min
+inline Dl dmaxc(Dl a, double c) { return a.v < c ? Dl(c) : a; }  // std::max(a, c)
+
+// far-field Roe flux (def_par:2258-2419) with the normal as a dual number
+void tan_farfield_n(const flite_controls &c, const Dl *q, Dl prl, const Dl *n, const double *inf, Dl *F) {
+    const double gam1 = c.gamma - 1.0;
+    double ro = inf[0], ro1 = 1. / ro, uo = inf[1], vo = inf[2], wo = inf[3], eo = inf[4], po = inf[5];
+    Dl rhol = q[0], rinvl = Dl(1.) / rhol;
+    Dl rul = q[1], rvl = q[2], rwl = q[3], rhl = q[4] + prl;
+    Dl ul = rul * rinvl, vl = rvl * rinvl, wl = rwl * rinvl;
+    Dl epsl = q[4], hl = rhl * rinvl;
+    Dl nvl = (ul * n[0] + vl * n[1]) + wl * n[2];
+    Dl fl1 = rhol * nvl, fl2 = prl * n[0] + rhol * ul * nvl, fl3 = prl * n[1] + rhol * vl * nvl;
+    Dl fl4 = prl * n[2] + rhol * wl * nvl, fl5 = rhl * nvl;
+    double rhor = ro, uxr = uo, vyr = vo, wzr = wo, epsr = eo * ro, presr = po, hr = eo + po * ro1;
+    Dl unr = (Dl(uxr) * n[0] + Dl(vyr) * n[1]) + Dl(wzr) * n[2];
+    Dl fr1 = Dl(rhor) * unr, fr2 = n[0] * presr + Dl(rhor * uxr) * unr, fr3 = n[1] * presr + Dl(rhor * vyr) * unr;
+    Dl fr4 = n[2] * presr + Dl(rhor * wzr) * unr, fr5 = Dl(epsr + presr) * unr;
+    Dl di = dsqrt(Dl(rhor) / rhol), d1 = Dl(1.0) / (di + Dl(1.0));
+    Dl ui = (di * uxr + ul) * d1, vi = (di * vyr + vl) * d1, wi = (di * wzr + wl) * d1;
+    Dl hi = (di * hr + hl) * d1;
+    Dl ci2 = Dl(gam1) * (hi - Dl(0.5) * ((ui * ui + vi * vi) + wi * wi));
+    ci2 = dmaxc(ci2, 1.0e-5);
+    Dl ci = dsqrt(ci2);
+    Dl af = Dl(0.5) * ((ui * ui + vi * vi) + wi * wi);
+    Dl ucp = (ui * n[0] + vi * n[1]) + wi * n[2];
+    Dl du1 = Dl(rhor) - rhol, du2 = Dl(rhor * uxr) - rhol * ul, du3 = Dl(rhor * vyr) - rhol * vl;
+    Dl du4 = Dl(rhor * wzr) - rhol * wl, du5 = Dl(epsr) - epsl;
+    Dl l1 = dabs(ucp + ci), l2 = dabs(ucp - ci), l3 = dabs(ucp);
+    Dl s1 = Dl(0.5) * (l1 + l2), s2 = Dl(0.5) * (l1 - l2);
+    Dl al1x = Dl(gam1) * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+    Dl al2x = ((-ucp * du1 + du2 * n[0]) + du3 * n[1]) + du4 * n[2];
+    Dl cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+    Dl cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+    F[0] = Dl(0.5) * (fr1 + fl1) - Dl(0.5) * (l3 * du1 + cc1);
+    F[1] = Dl(0.5) * (fr2 + fl2) - Dl(0.5) * ((l3 * du2 + cc1 * ui) + cc2 * n[0]);
+    F[2] = Dl(0.5) * (fr3 + fl3) - Dl(0.5) * ((l3 * du3 + cc1 * vi) + cc2 * n[1]);
+    F[3] = Dl(0.5) * (fr4 + fl4) - Dl(0.5) * ((l3 * du4 + cc1 * wi) + cc2 * n[2]);
+    F[4] = Dl(0.5) * (fr5 + fl5) - Dl(0.5) * ((l3 * du5 + cc1 * hi) + cc2 * ucp);
+}
+
+struct TanIteration {
+    const Oracle &o;
+    const Level &g;
+    const flite_controls &c;
+    int N, E, B;
+    std::vector<Dl> wx, wy, wz, bwx, bwy, bwz, V, nx, ny, nz, area;
+
+    TanIteration(const Oracle &o_, const double *dsw, const double *dbw, const double *dvol)
+        : o(o_), g(o_.lv[0]), c(o_.c), N(g.N), E(g.E), B(g.B) {
+        wx.resize(E); wy.resize(E); wz.resize(E);
+        for (int e = 0; e < E; ++e) {
+            wx[e] = Dl(g.wx[e], dsw ? dsw[e] : 0.0);
+            wy[e] = Dl(g.wy[e], dsw ? dsw[(size_t)E + e] : 0.0);
+            wz[e] = Dl(g.wz[e], dsw ? dsw[2 * (size_t)E + e] : 0.0);
+        }
+        bwx.resize(B); bwy.resize(B); bwz.resize(B);
+        for (int b = 0; b < B; ++b) {
+            bwx[b] = Dl(g.bwx[b], dbw ? dbw[b] : 0.0);
+            bwy[b] = Dl(g.bwy[b], dbw ? dbw[(size_t)B + b] : 0.0);
+            bwz[b] = Dl(g.bwz[b], dbw ? dbw[2 * (size_t)B + b] : 0.0);
+        }
+        V.resize(N);
+        for (int i = 0; i < N; ++i) V[i] = Dl(g.V[i], dvol ? dvol[i] : 0.0);
+        // makeBoundaryNormals and makeSurfaceArea (the setup_level forms)
+        nx.assign(N, Dl()); ny.assign(N, Dl()); nz.assign(N, Dl()); area.assign(N, Dl());
+        for (int b = 0; b < B; ++b) {
+            int a = g.b1[b], d = g.b2[b];
+            nx[a] = nx[a] - bwx[b]; ny[a] = ny[a] - bwy[b]; nz[a] = nz[a] - bwz[b];
+            nx[d] = nx[d] - bwx[b]; ny[d] = ny[d] - bwy[b]; nz[d] = nz[d] - bwz[b];
+        }
+        for (int i = 0; i < g.Nb; ++i) {
+            Dl nrm = dsqrt((nx[i] * nx[i] + ny[i] * ny[i]) + nz[i] * nz[i]);
+            if (nrm.v > 1.0e-10) { nx[i] = nx[i] / nrm; ny[i] = ny[i] / nrm; nz[i] = nz[i] / nrm; }
+            else { nx[i] = Dl(); ny[i] = Dl(); nz[i] = Dl(); }
+        }
+        for (int b = 0; b < B; ++b) {
+            Dl ai = dsqrt((bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b]);
+            area[g.b1[b]] = area[g.b1[b]] + Dl(4.0) * ai;
+            area[g.b2[b]] = area[g.b2[b]] + Dl(4.0) * ai;
+        }
+    }
+
+    template <class Fn>
+    void for_range(int a, int b, Fn fn) const {
+        for (int ib = g.R(a); ib <= g.R(b); ++ib) fn(g.node_ind[ib - 1]);
+    }
+    Dl pressure(const std::vector<Dl> *u, int i) const {
+        Dl pp = Dl(c.gamma - 1.0) * (u[4][i] - Dl(0.5) * ((u[1][i] * u[1][i] + u[2][i] * u[2][i]) + u[3][i] * u[3][i]) / u[0][i]);
+        return dmaxc(pp, 0.1);
+    }
+    void remove_normal(std::vector<Dl> *x, int ip, double scale) const {
+        Dl n[3] = {nx[ip], ny[ip], nz[ip]};
+        Dl nv = (x[1][ip] * n[0] + x[2][ip] * n[1]) + x[3][ip] * n[2];
+        for (int k = 0; k < 3; ++k) x[1 + k][ip] = x[1 + k][ip] - Dl(scale) * nv * n[k];
+    }
+    // makeTimeSteps, inviscid (def_par:13335-13610)
+    void timesteps(const std::vector<Dl> *u, const std::vector<Dl> &p, std::vector<Dl> &dt) const {
+        const double c1 = c.gamma;
+        dt.assign(N, Dl());
+        for (int e = 0; e < E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            Dl al = (wx[e] * wx[e] + wy[e] * wy[e]) + wz[e] * wz[e];
+            Dl ro1 = Dl(1.) / u[0][i1], ro2 = Dl(1.) / u[0][i2];
+            Dl cc1 = dmaxc(Dl(c1) * p[i1] * ro1, 0.001), cc2 = dmaxc(Dl(c1) * p[i2] * ro2, 0.001);
+            Dl vn1 = ((wx[e] * u[1][i1] + wy[e] * u[2][i1]) + wz[e] * u[3][i1]) * ro1;
+            Dl vn2 = ((wx[e] * u[1][i2] + wy[e] * u[2][i2]) + wz[e] * u[3][i2]) * ro2;
+            dt[i1] = (dt[i1] + dabs(vn1)) + dsqrt(cc1 * al);
+            dt[i2] = (dt[i2] + dabs(vn2)) + dsqrt(cc2 * al);
+        }
+        for (int b = 0; b < B; ++b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            Dl al = (bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b];
+            Dl ro1 = Dl(1.) / u[0][i1], ro2 = Dl(1.) / u[0][i2];
+            Dl cc1 = dmaxc(Dl(c1) * p[i1] * ro1, 0.001), cc2 = dmaxc(Dl(c1) * p[i2] * ro2, 0.001);
+            Dl vn1 = ((bwx[b] * u[1][i1] + bwy[b] * u[2][i1]) + bwz[b] * u[3][i1]) * ro1;
+            Dl vn2 = ((bwx[b] * u[1][i2] + bwy[b] * u[2][i2]) + bwz[b] * u[3][i2]) * ro2;
+            vn1 = dabs(vn1); vn2 = dabs(vn2);
+            Dl vnm = vn1 + vn2;
+            cc1 = dsqrt(cc1 * al); cc2 = dsqrt(cc2 * al);
+            Dl ccm = cc1 + cc2;
+            dt[i1] = (((dt[i1] + vn1) + vnm) + cc1) + ccm;
+            dt[i2] = (((dt[i2] + vn2) + vnm) + cc2) + ccm;
+        }
+        for (int i = 0; i < N; ++i) dt[i] = Dl(0.5) / (dt[i] / V[i] + Dl(0.0) / (V[i] * V[i]));
+    }
+    // makeArtificialDissipation2 on level 1, unweighted (def_par:11484-11993)
+    void jst(const std::vector<Dl> *u, const std::vector<Dl> &p, const std::vector<Dl> &dt,
+             std::vector<Dl> *diss) const {
+        for (int k = 0; k < 5; ++k) diss[k].assign(N, Dl());
+        if (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0) return;
+        std::vector<Dl> nh[9];
+        for (auto &v : nh) v.assign(N, Dl());
+        for (int e = 0; e < E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            Dl d[5];
+            for (int k = 0; k < 4; ++k) d[k] = u[k][i1] - u[k][i2];
+            d[4] = ((u[4][i1] - u[4][i2]) + p[i1]) - p[i2];
+            for (int k = 0; k < 5; ++k) {
+                nh[k][i1] = nh[k][i1] - d[k] * Dl(1.0);
+                nh[k][i2] = nh[k][i2] + d[k] * Dl(1.0);
+            }
+        }
+        for (int e = 0; e < E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            Dl dp = p[i1] - p[i2], sp = p[i1] + p[i2];
+            nh[6][i1] = nh[6][i1] - dp;
+            nh[7][i1] = nh[7][i1] + sp;
+            nh[6][i2] = nh[6][i2] + dp;
+            nh[7][i2] = nh[7][i2] + sp;
+        }
+        for (int i = 0; i < N; ++i) {
+            double fact = 1. / g.conn[i];
+            nh[8][i] = Dl(12.) * dabs(nh[6][i] / nh[7][i]);
+            for (int k = 0; k < 5; ++k) nh[k][i] = Dl(fact) * nh[k][i];
+        }
+        const double k2 = c.secondOrderDissipationFactor, k4 = c.fourthOrderDissipationFactor;
+        for (int e = 0; e < E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            Dl d4v[5], d2v[5];
+            for (int k = 0; k < 5; ++k) d4v[k] = nh[k][i1] - nh[k][i2];
+            for (int k = 0; k < 5; ++k) d2v[k] = u[k][i1] - u[k][i2];
+            Dl d0 = dminl(V[i1] / dt[i1], V[i2] / dt[i2]) / Dl(g.conn[i1] + g.conn[i2]);
+            Dl d2 = d0 * Dl(k2) * dmaxl(nh[8][i1], nh[8][i2]);
+            Dl d4 = d0 * Dl(k4);
+            d4 = d4.v > d2.v ? d4 - d2 : Dl(0.0);
+            for (int k = 0; k < 5; ++k) {
+                diss[k][i1] = (diss[k][i1] - d4v[k] * d4) + d2v[k] * d2;
+                diss[k][i2] = (diss[k][i2] + d4v[k] * d4) - d2v[k] * d2;
+            }
+        }
+    }
+    void wall_flux(const std::vector<Dl> *u, const std::vector<Dl> &p, int i, const Dl *rn, Dl *F) const {
+        Dl pr = p[i], rho = u[0][i], rinv = Dl(1.) / rho;
+        Dl ru = u[1][i], rv = u[2][i], rw = u[3][i], rh = u[4][i] + pr;
+        Dl uu = ru * rinv, vv = rv * rinv, ww = rw * rinv;
+        Dl nv = (uu * rn[0] + vv * rn[1]) + ww * rn[2];
+        F[0] = rho * nv;
+        F[1] = pr * rn[0] + rho * uu * nv;
+        F[2] = pr * rn[1] + rho * vv * nv;
+        F[3] = pr * rn[2] + rho * ww * nv;
+        F[4] = rh * nv;
+    }
+    // makeRHS for the central flux with the boundary faces (def_par:1525-2512)
+    void rhs(const std::vector<Dl> *u, const std::vector<Dl> &p, std::vector<Dl> *r) const {
+        for (int k = 0; k < 5; ++k) r[k].assign(N, Dl());
+        for (int e = 0; e < E; ++e) {
+            const int i1 = g.s1[e], i2 = g.s2[e];
+            Dl pr1 = p[i1], rinv1 = Dl(1.) / u[0][i1];
+            Dl ru1 = u[1][i1], rv1 = u[2][i1], rw1 = u[3][i1];
+            Dl u1 = rinv1 * ru1, v1 = rinv1 * rv1, w1 = rinv1 * rw1;
+            Dl rh1 = u[4][i1] + pr1;
+            Dl pr2 = p[i2], rinv2 = Dl(1.) / u[0][i2];
+            Dl ru2 = u[1][i2], rv2 = u[2][i2], rw2 = u[3][i2];
+            Dl u2 = rinv2 * ru2, v2 = rinv2 * rv2, w2 = rinv2 * rw2;
+            Dl rh2 = u[4][i2] + pr2;
+            const Dl wx_ = wx[e], wy_ = wy[e], wz_ = wz[e];
+            Dl f[5];
+            f[0] = (wx_ * (ru1 + ru2) + wy_ * (rv1 + rv2)) + wz_ * (rw1 + rw2);
+            f[1] = (wx_ * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy_ * (ru1 * v1 + ru2 * v2)) + wz_ * (ru1 * w1 + ru2 * w2);
+            f[2] = (wx_ * (rv1 * u1 + rv2 * u2) + wy_ * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz_ * (rv1 * w1 + rv2 * w2);
+            f[3] = (wx_ * (rw1 * u1 + rw2 * u2) + wy_ * (rw1 * v1 + rw2 * v2)) + wz_ * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
+            f[4] = (wx_ * (rh1 * u1 + rh2 * u2) + wy_ * (rh1 * v1 + rh2 * v2)) + wz_ * (rh1 * w1 + rh2 * w2);
+            for (int k = 0; k < 5; ++k) {
+                r[k][i1] = r[k][i1] + f[k];
+                r[k][i2] = r[k][i2] - f[k];
+            }
+        }
+        const bool fe = c.boundaryTerm == 1;
+        for (int b = 0; b < B; ++b) {
+            const int i1 = g.b1[b], i2 = g.b2[b], ind = g.bind[b];
+            Dl g1[5], g2[5];
+            Dl rnorm = dsqrt((bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b]);
+            if ((ind <= 4 || ind == 9) && rnorm.v > 1.0e-10) {
+                Dl rn[3] = {bwx[b] / rnorm, bwy[b] / rnorm, bwz[b] / rnorm};
+                Dl F1[5], F2[5];
+                if (ind <= 2 || ind == 9) {
+                    wall_flux(u, p, i1, rn, F1);
+                    wall_flux(u, p, i2, rn, F2);
+                } else {
+                    const double *inf = &c.inflowField[(ind - 3) * 6];
+                    Dl q1[5], q2[5];
+                    for (int k = 0; k < 5; ++k) { q1[k] = u[k][i1]; q2[k] = u[k][i2]; }
+                    tan_farfield_n(c, q1, p[i1], rn, inf, F1);
+                    tan_farfield_n(c, q2, p[i2], rn, inf, F2);
+                }
+                for (int k = 0; k < 5; ++k) {
+                    if (fe) { g1[k] = rnorm * (Dl(3.) * F1[k] + F2[k]); g2[k] = rnorm * (F1[k] + Dl(3.) * F2[k]); }
+                    else { g1[k] = rnorm * Dl(4.) * F1[k]; g2[k] = rnorm * Dl(4.) * F2[k]; }
+                }
+            } else {
+                for (int k = 0; k < 5; ++k) { g1[k] = Dl(); g2[k] = Dl(); }
+            }
+            for (int k = 0; k < 5; ++k) r[k][i1] = r[k][i1] + g1[k];
+            for (int k = 0; k < 5; ++k) r[k][i2] = r[k][i2] + g2[k];
+        }
+    }
+    // one doTimeIterations step on level 1: u <- G(u)
+    void iterate(std::vector<Dl> *u) const {
+        std::vector<Dl> up[5], p(N), dt, diss[5], r[5];
+        for (int k = 0; k < 5; ++k) up[k] = u[k];
+        for (int i = 0; i < N; ++i) p[i] = dabs(pressure(u, i));
+        timesteps(u, p, dt);
+        jst(u, p, dt, diss);
+        const double relax = o.relaxation_param(g);
+        for (int st = 1; st <= 3; ++st) {
+            for (int i = 0; i < N; ++i) p[i] = pressure(u, i);
+            rhs(u, p, r);
+            for (int k = 0; k < 5; ++k)
+                for (int i = 0; i < N; ++i) r[k][i] = r[k][i] + diss[k][i];
+            for (int i = 0; i < N; ++i)
+                for (int k = 0; k < 5; ++k) r[k][i] = dt[i] * r[k][i] / V[i];
+            for_range(-20, -19, [&](int ip) { remove_normal(r, ip, 1.0); });
+            for_range(-4, -3, [&](int ip) { remove_normal(r, ip, 1.0); });
+            for_range(-18, -17, [&](int ip) { remove_normal(r, ip, 1.0); });
+            const double dtJ = c.CFLNumber * o.RK[st - 1];
+            for (int k = 0; k < 5; ++k)
+                for (int i = 0; i < N; ++i) r[k][i] = Dl(dtJ) * r[k][i];
+            for (int i = 0; i < N; ++i) {
+                Dl inc = r[0][i];
+                if (std::fabs(inc.v / up[0][i].v) < c.maxIncrementFactor) {
+                    u[0][i] = up[0][i] - inc;
+                } else {
+                    double sign = inc.v / std::fabs(inc.v);
+                    u[0][i] = up[0][i] - Dl(sign * c.maxIncrementFactor) * up[0][i];
+                }
+                for (int k = 1; k < 5; ++k) u[k][i] = up[k][i] - r[k][i];
+                if (u[0][i].v < c.minimumDensity) u[0][i] = Dl(c.minimumDensity);
+            }
+            for_range(-20, -19, [&](int ip) { remove_normal(u, ip, 1.0); });
+            for_range(-4, -3, [&](int ip) {
+                remove_normal(u, ip, relax);
+                if (!c.wallsAreIsentropic) {
+                    Dl ke = (u[1][ip] * u[1][ip] + u[2][ip] * u[2][ip]) + u[3][ip] * u[3][ip];
+                    u[4][ip] = u[0][ip] * Dl(c.inflowTemperature) / Dl(c.gamma) + Dl(0.5) * ke / u[0][ip];
+                }
+            });
+            for_range(-18, -17, [&](int ip) { remove_normal(u, ip, 1.0); });
+            for (int i = 0; i < N; ++i) u[0][i] = dmaxc(u[0][i], c.minimumDensity);
+            const double gm1 = c.gamma - 1.0;
+            for (int side = 0; side < 2; ++side) {
+                const double *inf = &c.inflowField[side * 6];
+                double iR = inf[0], iU1 = inf[1], iU2 = inf[2], iU3 = inf[3], iE = inf[4], iP = inf[5];
+                for_range(side == 0 ? -16 : -14, side == 0 ? -15 : -13, [&](int ip) {
+                    Dl rho = u[0][ip], U1 = u[1][ip], U2 = u[2][ip], U3 = u[3][ip];
+                    double nvel = (iU1 * nx[ip].v + iU2 * ny[ip].v) + iU3 * nz[ip].v;
+                    if (nvel > 0.00) {
+                        u[0][ip] = Dl(iR); u[1][ip] = Dl(iU1 * iR); u[2][ip] = Dl(iU2 * iR); u[3][ip] = Dl(iU3 * iR);
+                        if (c.MachNumber > 1.0) u[4][ip] = Dl(iE * iR);
+                        else u[4][ip] = p[ip] / Dl(gm1) + Dl(0.5 * ((iU1 * iU1 + iU2 * iU2) + iU3 * iU3) * iR);
+                    } else {
+                        if (c.MachNumber < 1.0)
+                            u[4][ip] = Dl(iP / gm1) + Dl(0.5) * ((U1 * U1 + U2 * U2) + U3 * U3) / rho;
+                    }
+                });
+            }
+        }
+    }
+    // lift (which 0) or drag (which 1) coefficient of calculateLiftAndDrag
+    // (def_par:14710-14870), inviscid, with the pressure of the state u
+    Dl objective(const std::vector<Dl> *u, int which) const {
+        const double PI = 4.0 * std::atan(1.0);
+        double aR = c.alpha * PI / 180., bR = c.beta * PI / 180.;
+        double ft[3] = {std::cos(aR) * std::cos(bR), std::sin(bR), std::sin(aR)};
+        double fn1[3] = {-ft[2], 0.0, ft[0]};
+        const double *dir = which == 0 ? fn1 : ft;
+        const double pinf = 1. / (c.gamma * c.MachNumber * c.MachNumber);
+        Dl acc;
+        for_range(-20, -19, [&](int ip) {
+            if (!(g.cz[ip] > (c.groundplane + 0.01))) return;
+            Dl dn = (nx[ip] * dir[0] + ny[ip] * dir[1]) + nz[ip] * dir[2];
+            Dl dp = pressure(u, ip) - Dl(pinf);
+            acc = acc - area[ip] * dp * dn;
+        });
+        return Dl(2.0) * acc / Dl(c.referenceArea);
+    }
+};
+
 }  // namespace
 
 struct oracle_ctx {
@@ -1969,6 +2298,49 @@ int oracle_residual_jvp(oracle_ctx *o, int level, const double *u, const double 
         }
     }
     for (size_t k = 0; k < 5 * N; ++k) jv[k] = acc[k].d;
+    return FLITE_OK;
+}
+
+// tangent of one smoother iteration on level 1 (central flux, scalar JST,
+// inviscid): v = G(u), dv = G_u du + G_g dg for the geometry direction dg =
+// (dsw [3][E], dbw [3][B], dvol [N]); any of the geometry directions may be
+// NULL (zero)
+int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const double *dsw, const double *dbw,
+                         const double *dvol, double *v, double *dv) {
+    if (!o || !u || !du || !v || !dv) return FLITE_EINVAL;
+    const flite_controls &c = o->o.c;
+    if (c.fluxType != 1 || c.ReynoldsNumber > 0 || c.turbulenceModel != 0 || c.dissipationScheme == 3 ||
+        c.useDissipationWeighting)
+        return FLITE_EUNSUPPORTED;
+    TanIteration T(o->o, dsw, dbw, dvol);
+    const size_t N = T.N;
+    std::vector<Dl> x[5];
+    for (int k = 0; k < 5; ++k) {
+        x[k].resize(N);
+        for (size_t i = 0; i < N; ++i) x[k][i] = Dl(u[k * N + i], du[k * N + i]);
+    }
+    T.iterate(x);
+    for (int k = 0; k < 5; ++k)
+        for (size_t i = 0; i < N; ++i) { v[k * N + i] = x[k][i].v; dv[k * N + i] = x[k][i].d; }
+    return FLITE_OK;
+}
+
+// lift (which 0) or drag (which 1) coefficient of the level-1 state u with
+// its tangent along (du, dbw); dbw may be NULL
+int oracle_objective_jvp(oracle_ctx *o, int which, const double *u, const double *du, const double *dbw, double *J,
+                         double *dJ) {
+    if (!o || !u || !du || !J || !dJ || which < 0 || which > 1) return FLITE_EINVAL;
+    if (o->o.c.ReynoldsNumber > 0) return FLITE_EUNSUPPORTED;
+    TanIteration T(o->o, nullptr, dbw, nullptr);
+    const size_t N = T.N;
+    std::vector<Dl> x[5];
+    for (int k = 0; k < 5; ++k) {
+        x[k].resize(N);
+        for (size_t i = 0; i < N; ++i) x[k][i] = Dl(u[k * N + i], du[k * N + i]);
+    }
+    Dl j = T.objective(x, which);
+    *J = j.v;
+    *dJ = j.d;
     return FLITE_OK;
 }
 
