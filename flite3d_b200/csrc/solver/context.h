@@ -18,6 +18,12 @@
 
 using namespace flite;
 
+namespace flite {
+// buffers of the steady adjoint (steady_adjoint.cu), made on its first call
+struct SteadyAdjoint;
+void destroy_steady_adjoint(SteadyAdjoint *a);
+}  // namespace flite
+
 namespace flite_detail {
 
 struct cuda_error : std::runtime_error {
@@ -92,6 +98,7 @@ struct flite_ctx {
     double *adj_rbar = nullptr, *adj_ubar = nullptr, *adj_b = nullptr;
     size_t adj_n = 0;
     void vjp_kernels(int l);
+    flite::SteadyAdjoint *sadj = nullptr;
     std::string err;
 
     template <class T>
@@ -112,6 +119,7 @@ struct flite_ctx {
     ~flite_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
         if (adj_rbar) { cudaFree(adj_rbar); cudaFree(adj_ubar); cudaFree(adj_b); }
+        if (sadj) flite::destroy_steady_adjoint(sadj);
         for (void *p : allocs) cudaFree(p);
         if (h_cycle) cudaFreeHost(h_cycle);
         if (s) cudaStreamDestroy(s);

@@ -56,5 +56,9 @@ __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, doub
                          double ground, double d0, double d1, double d2, double *part);
 __global__ void k_forces_final(const double *part, int nblk, double *out);
 constexpr int kForceBlocks = 64;
+// transposed residual Jacobian at the state x (adjoint.cu)
+__global__ void k_vjp_farfield(Params P, LevelView L, const double *x, const double *rbar, double *bvjp);
+__global__ void k_vjp_node(Params P, LevelView L, const double *x, const double *rbar, const double *bvjp,
+                           const double *pbar, double *ubar, int add);
 
 }  // namespace flite

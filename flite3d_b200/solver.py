@@ -187,6 +187,41 @@ class Solver:
         self._ck(self.be.residual_jvp(self._h, level, _ptr(u), _ptr(du), _ptr(jv)), "residual_jvp")
         return jv
 
+    OBJECTIVES = {"CL": 0, "CD": 1}
+
+    def objective(self, name="CL"):
+        """Lift or drag coefficient of the level-1 state with the pressure of
+        the state (the objective of adjoint_solve)."""
+        J = ctypes.c_double()
+        self._ck(self.be.objective(self._h, self.OBJECTIVES[name], ctypes.byref(J)), "objective")
+        return J.value
+
+    def iteration_vjp(self, u, lam, geometry=False):
+        """(dG/du)^T lam of one level-1 smoother iteration G at the state u;
+        with geometry=True also (dG/dg)^T lam for g = side_w, bnd_w, volume."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        ub = np.zeros_like(u)
+        d = self.mesh.level(1)
+        g = [np.zeros((3, d.n_sides)), np.zeros((3, d.n_bsides)), np.zeros(d.n_nodes)] if geometry else None
+        gp = [_ptr(a) for a in g] if geometry else [None, None, None]
+        self._ck(self.be.iteration_vjp(self._h, _ptr(u), _ptr(lam), _ptr(ub), *gp), "iteration_vjp")
+        return (ub, *g) if geometry else ub
+
+    def adjoint_solve(self, name="CL", tol=1e-10, max_iter=100000):
+        """Sensitivity of the lift or drag coefficient of the converged
+        level-1 state to the level-1 geometry: dict with J, side_w_bar (3, E),
+        bnd_w_bar (3, B), volume_bar (N), iterations and residual.  The
+        sensitivity to node coordinates is Mesh.geometry_vjp of the three."""
+        d = self.mesh.level(1)
+        sw, bw, vol = np.zeros((3, d.n_sides)), np.zeros((3, d.n_bsides)), np.zeros(d.n_nodes)
+        J, it, res = ctypes.c_double(), ctypes.c_int32(), ctypes.c_double()
+        self._ck(self.be.adjoint_solve(self._h, self.OBJECTIVES[name], ctypes.c_double(tol), int(max_iter),
+                                       ctypes.byref(J), _ptr(sw), _ptr(bw), _ptr(vol), ctypes.byref(it),
+                                       ctypes.byref(res)), "adjoint_solve")
+        return dict(J=J.value, side_w_bar=sw, bnd_w_bar=bw, volume_bar=vol, iterations=it.value,
+                    residual=res.value)
+
     def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1):
         self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll), "set_kernel_options")
 

@@ -187,6 +187,36 @@ int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, const double 
  * product on a level (the adjoint cost ratio is vjp/fwd)                  */
 int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double *fwd_ms, double *vjp_ms);
 
+/* ---- steady adjoint: force sensitivities to the level-1 geometry ---------
+ * For the central flux with scalar JST dissipation, inviscid, FP64 (other
+ * controls: FLITE_EUNSUPPORTED).  G is one smoother iteration of level 1
+ * (doTimeIterations with calcDiss, def_par:966-1181: time steps, dissipation,
+ * three RK stages with their boundary conditions); the geometry g is the
+ * level-1 side_w [3][E], bnd_w [3][B] and volume [N] of the level descriptor
+ * (the node normals and wall areas follow from bnd_w as in
+ * makeBoundaryNormals def_par:15394 and makeSurfaceArea :15523).
+ * flite_iteration_vjp: ubar = (dG/du)^T lam at the state u [5][N] and, for
+ * the geometry pointers that are not NULL, (dG/dg)^T lam.
+ * flite_adjoint_solve: at the context's level-1 state, which must be a
+ * converged solution u* = G(u*), the objective J (FLITE_OBJ_CL or
+ * FLITE_OBJ_CD of calculateLiftAndDrag def_par:14710-14870 with the pressure
+ * of the state) and dJ/dg = J_g + lam^T (dG/dg), where lam = P((dG/du)^T lam
+ * + (dJ/du)^T) is iterated until |lam_new - lam| <= tol |lam| or max_iter
+ * iterations (P keeps the energy of subsonic inflow nodes, which the
+ * boundary condition never updates, out of the adjoint).  Sensitivities to
+ * node coordinates follow with fp_geometry_vjp of the preprocessor, which
+ * owns the elements.  No reference counterpart: the reference has no
+ * adjoint.                                                                  */
+#define FLITE_OBJ_CL 0
+#define FLITE_OBJ_CD 1
+/* the objective J of flite_adjoint_solve at the context's level-1 state    */
+int flite_objective(flite_ctx *ctx, int objective, double *J);
+int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double *lam, double *ubar,
+                        double *side_w_bar, double *bnd_w_bar, double *volume_bar);
+int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, int max_iter, double *J,
+                        double *side_w_bar, double *bnd_w_bar, double *volume_bar, int *iterations,
+                        double *residual);
+
 /* ---- batched solves (no reference counterpart: the reference runs one
  * condition per job) --------------------------------------------------------
  * ncases solves, case i on mesh mesh_of_case[i] (levels[m] points to the

@@ -1664,6 +1664,14 @@ void tan_farfield(const flite_controls &c, const Dl *q, Dl pr, const double *n, 
 inline Dl dmaxl(Dl a, Dl b) { return a.v < b.v ? b : a; }        // std::max
 inline Dl dminl(Dl a, Dl b) { return b.v < a.v ? b : a; }        // std::min
 inline Dl dmaxc(Dl a, double c) { return a.v < c ? Dl(c) : a; }  // std::max(a, c)
+// |vn| of the time step with the derivative 0 where vn = w.m/rho is rounding
+// noise (|w.m| <= 1e-12 |w||m|: the momentum of a slip-wall or symmetry node
+// projected onto the plane), the mean of the one-sided derivatives there
+inline Dl kink_abs(Dl vn, Dl wm, Dl al, const Dl *m) {
+    double mm = std::sqrt((m[0].v * m[0].v + m[1].v * m[1].v) + m[2].v * m[2].v);
+    if (std::fabs(wm.v) <= 1.0e-12 * std::sqrt(al.v) * mm) return Dl(std::fabs(vn.v), 0.0);
+    return dabs(vn);
+}
 
 // far-field Roe flux (def_par:2258-2419) with the normal as a dual number
 void tan_farfield_n(const flite_controls &c, const Dl *q, Dl prl, const Dl *n, const double *inf, Dl *F) {
@@ -1767,19 +1775,23 @@ struct TanIteration {
             Dl al = (wx[e] * wx[e] + wy[e] * wy[e]) + wz[e] * wz[e];
             Dl ro1 = Dl(1.) / u[0][i1], ro2 = Dl(1.) / u[0][i2];
             Dl cc1 = dmaxc(Dl(c1) * p[i1] * ro1, 0.001), cc2 = dmaxc(Dl(c1) * p[i2] * ro2, 0.001);
-            Dl vn1 = ((wx[e] * u[1][i1] + wy[e] * u[2][i1]) + wz[e] * u[3][i1]) * ro1;
-            Dl vn2 = ((wx[e] * u[1][i2] + wy[e] * u[2][i2]) + wz[e] * u[3][i2]) * ro2;
-            dt[i1] = (dt[i1] + dabs(vn1)) + dsqrt(cc1 * al);
-            dt[i2] = (dt[i2] + dabs(vn2)) + dsqrt(cc2 * al);
+            Dl wm1 = (wx[e] * u[1][i1] + wy[e] * u[2][i1]) + wz[e] * u[3][i1];
+            Dl wm2 = (wx[e] * u[1][i2] + wy[e] * u[2][i2]) + wz[e] * u[3][i2];
+            Dl vn1 = wm1 * ro1, vn2 = wm2 * ro2;
+            const Dl m1[3] = {u[1][i1], u[2][i1], u[3][i1]}, m2[3] = {u[1][i2], u[2][i2], u[3][i2]};
+            dt[i1] = (dt[i1] + kink_abs(vn1, wm1, al, m1)) + dsqrt(cc1 * al);
+            dt[i2] = (dt[i2] + kink_abs(vn2, wm2, al, m2)) + dsqrt(cc2 * al);
         }
         for (int b = 0; b < B; ++b) {
             int i1 = g.b1[b], i2 = g.b2[b];
             Dl al = (bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b];
             Dl ro1 = Dl(1.) / u[0][i1], ro2 = Dl(1.) / u[0][i2];
             Dl cc1 = dmaxc(Dl(c1) * p[i1] * ro1, 0.001), cc2 = dmaxc(Dl(c1) * p[i2] * ro2, 0.001);
-            Dl vn1 = ((bwx[b] * u[1][i1] + bwy[b] * u[2][i1]) + bwz[b] * u[3][i1]) * ro1;
-            Dl vn2 = ((bwx[b] * u[1][i2] + bwy[b] * u[2][i2]) + bwz[b] * u[3][i2]) * ro2;
-            vn1 = dabs(vn1); vn2 = dabs(vn2);
+            Dl wm1 = (bwx[b] * u[1][i1] + bwy[b] * u[2][i1]) + bwz[b] * u[3][i1];
+            Dl wm2 = (bwx[b] * u[1][i2] + bwy[b] * u[2][i2]) + bwz[b] * u[3][i2];
+            Dl vn1 = wm1 * ro1, vn2 = wm2 * ro2;
+            const Dl m1[3] = {u[1][i1], u[2][i1], u[3][i1]}, m2[3] = {u[1][i2], u[2][i2], u[3][i2]};
+            vn1 = kink_abs(vn1, wm1, al, m1); vn2 = kink_abs(vn2, wm2, al, m2);
             Dl vnm = vn1 + vn2;
             cc1 = dsqrt(cc1 * al); cc2 = dsqrt(cc2 * al);
             Dl ccm = cc1 + cc2;
