@@ -464,6 +464,103 @@ def run_rans(args):
     }), flush=True)
 
 
+def run_adjoint(args):
+    """The adjoint configuration for the central flux: dCL/dX and
+    dCD/dX along the normal displacement of wall nodes of the bump channel
+    48x16x16 hex -> tets (the Euler configuration's mesh) with its interior
+    nodes jittered by up to 15% of the spacing (seed 11: no two edges tie in
+    the dissipation's min/max switches), inviscid, M 0.5, central flux + JST,
+    CFL 2, 3 levels, FP64.  The primal is converged to a residual of 1e-15,
+    the adjoint to 1e-12; then central differences of converged solutions on
+    moved meshes at 32 seeded wall nodes (SplitMix64 seed 4), step 1e-7 of
+    the channel height.  One JSON line: the adjoint solve's seconds, beside
+    the primal solve's and the finite-difference agreement."""
+    import torch
+    import flite3d_b200 as F
+    from flite3d_b200.mesh import splitmix64
+    if not torch.cuda.is_available():
+        raise SystemExit("no CUDA device: the product path has no CPU fallback")
+    nx, ny, nz = 48, 16, 16
+    base = F.Mesh.bump_channel(nx, ny, nz, 0.05, nlevels=3)
+    X = base.array(1, "coords")
+    jit = np.random.default_rng(11).uniform(-1, 1, X.shape) * 0.15 / nz
+    jit[:, :base.level(1).n_bnodes] = 0.0
+    X = X + jit
+    at = lambda Y: base.with_level1_geometry(*base.geometry(Y))
+    mesh = at(X)
+    c = F.default_controls(ReynoldsNumber=0.0, fluxType=1, CFLNumber=2.0, multigridScheme=3,
+                           numberOfGridsToUse=3)
+
+    def converge(m, u0=None, tol=1e-15, max_cycles=6000):
+        s = F.Solver(c, m)
+        s.set_state(F.initial_state(c, m) if u0 is None else u0)
+        s.start()
+        res, it = None, 0
+        for it in range(1, max_cycles + 1):
+            s.cycle(it)
+            if it % 50 == 0:
+                res = s.residuals()[0][0]
+                if res < tol:
+                    break
+        return s, res, it
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s, res, ncyc = converge(mesh)
+    torch.cuda.synchronize()
+    t_primal = time.perf_counter() - t0
+    u = s.get_state(1)
+    out = {}
+    for name in ("CL", "CD"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = s.adjoint_solve(name, tol=1e-12, max_iter=400000)
+        torch.cuda.synchronize()
+        out[name] = (r, time.perf_counter() - t0,
+                     base.geometry_vjp(r["side_w_bar"], r["bnd_w_bar"], r["volume_bar"], xyz=X))
+    reg, ind = base.array(1, "node_reg"), base.array(1, "node_ind")
+    wall = ind[reg[0] - 1:reg[1]] - 1
+    bw, bidx = base.array(1, "bnd_w"), base.array(1, "bnd_idx")
+    a = np.zeros_like(X)
+    for k in range(2):
+        np.add.at(a, (slice(None), bidx[k] - 1), -bw)
+    nrm = a / np.linalg.norm(a, axis=0).clip(1e-300)
+    pick = (splitmix64(4, 64) % np.uint64(len(wall))).astype(np.int64)
+    nodes = list(dict.fromkeys(wall[pick].tolist()))[:args.adjoint_nodes]
+    h = 1e-7
+    errs = {"CL": [], "CD": []}
+    t0 = time.perf_counter()
+    for k in nodes:
+        dX = np.zeros_like(X)
+        dX[:, k] = nrm[:, k] * h
+        sp = converge(at(X + dX), u0=u, max_cycles=3000)[0]
+        sm = converge(at(X - dX), u0=u, max_cycles=3000)[0]
+        for name in ("CL", "CD"):
+            fd = (sp.objective(name) - sm.objective(name)) / (2 * h)
+            adj = float((out[name][2][:, k] * nrm[:, k]).sum())
+            errs[name].append(abs(adj - fd) / max(abs(fd), 1e-300))
+    t_fd = time.perf_counter() - t0
+    d = mesh.level(1)
+    rl = out["CL"][0]
+    print(json.dumps({
+        "metric": "adjoint dCL/dX solve time", "value": out["CL"][1], "unit": "s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (generated bump-channel mesh, jittered interior nodes, freestream start)",
+        "config": {"workload": f"steady adjoint of CL and CD, inviscid M 0.5, central flux + JST, on the bump "
+                               f"channel {nx}x{ny}x{nz} hex -> 6 tets with interior nodes jittered by 15% of the "
+                               "spacing, 3 agglomerated MG levels for the primal, FP64",
+                   "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides},
+        "primal": {"seconds": t_primal, "cycles": ncyc, "residual": res},
+        "adjoint": {name: {"J": out[name][0]["J"], "seconds": out[name][1], "iterations": out[name][0]["iterations"],
+                           "residual": out[name][0]["residual"]} for name in out},
+        "adjoint_over_primal_time": out["CL"][1] / t_primal,
+        "fd_check": {"nodes": len(nodes), "step": h, "seconds": t_fd,
+                     "max_rel_err": {n: max(e) for n, e in errs.items()},
+                     "median_rel_err": {n: float(np.median(e)) for n, e in errs.items()}},
+        "gpu_launches": None,
+    }), flush=True)
+
+
 def run_batch(args):
     """Batched solves: the bump channel at 120x40x40, 192x64x64 and
     264x88x88 hexes x 16 flow conditions each (angle of attack uniform in
@@ -533,6 +630,9 @@ def main():
     ap.add_argument("--rans-ni", type=int, default=200)
     ap.add_argument("--rans-nj", type=int, default=120)
     ap.add_argument("--rans-nk", type=int, default=240)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="the steady adjoint (dCL/dX, dCD/dX) workload with its finite-difference check")
+    ap.add_argument("--adjoint-nodes", type=int, default=32)
     ap.add_argument("--batch-meshes", type=int, default=3)
     ap.add_argument("--batch-conditions", type=int, default=16)
     args = ap.parse_args()
@@ -546,6 +646,8 @@ def main():
         run_batch(args)
     elif args.rans:
         run_rans(args)
+    elif args.adjoint:
+        run_adjoint(args)
     else:
         run_ours(args)
 

@@ -880,13 +880,35 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
         const double ref = std::sqrt(h[3]);
         int it = 0;
         double res = ref > 0 ? 1.0 : 0.0;
+        // `check` iterations per launch of one captured graph, then the norms
         const int check = 10;
-        while (ref > 0 && it < max_iter && res > tol) {
-            for (int k = 0; k < check && it < max_iter; ++k, ++it) {
-                reverse(X, A, A.lam, false);
-                k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.ubar, A.Ju, A.lam, A.part);
-            }
+        auto iterate = [&]() {
+            reverse(X, A, A.lam, false);
+            k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.ubar, A.Ju, A.lam, A.part);
+        };
+        cudaGraphExec_t gexec = nullptr;
+        if (max_iter >= check) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(X.s, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < check; ++k) iterate();
             k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
+            CK(cudaStreamEndCapture(X.s, &g));
+            cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+            cudaGraphDestroy(g);
+            CK(e);
+        }
+        struct GraphGuard {
+            cudaGraphExec_t &g;
+            ~GraphGuard() { if (g) cudaGraphExecDestroy(g); }
+        } guard{gexec};
+        while (ref > 0 && it < max_iter && res > tol) {
+            if (gexec && it + check <= max_iter) {
+                CK(cudaGraphLaunch(gexec, X.s));
+                it += check;
+            } else {
+                for (int k = 0; k < check && it < max_iter; ++k, ++it) iterate();
+                k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
+            }
             CK(cudaMemcpyAsync(h + 2, A.out + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
             CK(cudaStreamSynchronize(X.s));
             if (!std::isfinite(h[2])) {

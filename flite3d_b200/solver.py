@@ -208,6 +208,29 @@ class Solver:
         self._ck(self.be.iteration_vjp(self._h, _ptr(u), _ptr(lam), _ptr(ub), *gp), "iteration_vjp")
         return (ub, *g) if geometry else ub
 
+    def iteration_jvp(self, u, du, side_w=None, bnd_w=None, volume=None):
+        """(G(u), dG) with dG = G_u du + G_g dg along the geometry direction
+        dg = (side_w, bnd_w, volume) (None: zero) -- the oracle's tangent."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        g = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (side_w, bnd_w, volume)]
+        v, dv = np.zeros_like(u), np.zeros_like(u)
+        self._ck(self.be.iteration_jvp(self._h, _ptr(u), _ptr(du), *[None if a is None else _ptr(a) for a in g],
+                                       _ptr(v), _ptr(dv)), "iteration_jvp")
+        return v, dv
+
+    def objective_jvp(self, name, u, du, bnd_w=None):
+        """(J, dJ) of the lift or drag coefficient along (du, d bnd_w) -- the
+        oracle's tangent."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        b = None if bnd_w is None else np.ascontiguousarray(bnd_w, dtype=np.float64)
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.be.objective_jvp(self._h, self.OBJECTIVES[name], _ptr(u), _ptr(du),
+                                       None if b is None else _ptr(b), ctypes.byref(J), ctypes.byref(dJ)),
+                 "objective_jvp")
+        return J.value, dJ.value
+
     def adjoint_solve(self, name="CL", tol=1e-10, max_iter=100000):
         """Sensitivity of the lift or drag coefficient of the converged
         level-1 state to the level-1 geometry: dict with J, side_w_bar (3, E),
