@@ -518,6 +518,16 @@ def run_adjoint(args):
         torch.cuda.synchronize()
         out[name] = (r, time.perf_counter() - t0,
                      base.geometry_vjp(r["side_w_bar"], r["bnd_w_bar"], r["volume_bar"], xyz=X))
+    # the same CL adjoint by the plain fixed-point iteration, for comparison
+    s.set_adjoint_method("fixed-point")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rf = s.adjoint_solve("CL", tol=1e-12, max_iter=400000)
+    torch.cuda.synchronize()
+    t_fixed = time.perf_counter() - t0
+    s.set_adjoint_method("gmres")
+    xf = base.geometry_vjp(rf["side_w_bar"], rf["bnd_w_bar"], rf["volume_bar"], xyz=X)
+    agree = float(np.abs(xf - out["CL"][2]).max() / np.abs(out["CL"][2]).max())
     reg, ind = base.array(1, "node_reg"), base.array(1, "node_ind")
     wall = ind[reg[0] - 1:reg[1]] - 1
     bw, bidx = base.array(1, "bnd_w"), base.array(1, "bnd_idx")
@@ -554,6 +564,9 @@ def run_adjoint(args):
         "adjoint": {name: {"J": out[name][0]["J"], "seconds": out[name][1], "iterations": out[name][0]["iterations"],
                            "residual": out[name][0]["residual"]} for name in out},
         "adjoint_over_primal_time": out["CL"][1] / t_primal,
+        "method": "GMRES(50) on (I - P G_u^T) lam = P J_u^T",
+        "fixed_point": {"seconds": t_fixed, "iterations": rf["iterations"], "residual": rf["residual"],
+                        "max_rel_diff_dCL_dX_vs_gmres": agree},
         "fd_check": {"nodes": len(nodes), "step": h, "seconds": t_fd,
                      "max_rel_err": {n: max(e) for n, e in errs.items()},
                      "median_rel_err": {n: float(np.median(e)) for n, e in errs.items()}},

@@ -99,6 +99,7 @@ struct flite_ctx {
     size_t adj_n = 0;
     void vjp_kernels(int l);
     flite::SteadyAdjoint *sadj = nullptr;
+    int adj_method = 1, adj_restart = 50;  // flite_set_adjoint_method (GMRES(50))
     std::string err;
 
     template <class T>

@@ -657,11 +657,74 @@ __global__ void k_adj_zero(double *a, size_t n) {
 }
 
 // ---- host side ----------------------------------------------------------
+// ---- GMRES on (I - A) lam = b, A = P G_u^T, b = P Ju ------------------------
+// Restarted GMRES (Saad and Schultz 1986) with classical Gram-Schmidt applied
+// twice; the Krylov vectors stay on the device, the Hessenberg matrix and
+// its Givens rotations on the host.  Every reduction sums block partials in
+// block order, so a solve is deterministic.
+constexpr int kDotBlocks = 148;
+__global__ void k_gm_dots(const double *V, size_t n, const double *w, double *part) {
+    __shared__ double red[256];
+    const double *v = V + (size_t)blockIdx.y * n;
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s += v[i] * w[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+__global__ void k_gm_dots_final(const double *part, int nblk, int k, double *h) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += part[(size_t)j * nblk + b];
+    h[j] = s;
+}
+// w += sgn sum_j c[j] V_j
+__global__ void k_gm_combine(const double *V, size_t n, int k, const double *c, double sgn, double *w) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < k; ++j) s += c[j] * V[(size_t)j * n + i];
+        w[i] = w[i] + sgn * s;
+    }
+}
+__global__ void k_gm_scale(double *w, size_t n, double a) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        w[i] = a * w[i];
+}
+__device__ __forceinline__ bool inflow_energy_fixed(const Params &P, const LevelView &L, int i) {
+    const unsigned char cls = L.bc[i];
+    if (!((cls == BC_FAR3 || cls == BC_FAR4) && !(P.mach > 1.0))) return false;
+    const double *inf = &P.inf[cls == BC_FAR3 ? 0 : 6];
+    return ((inf[1] * L.nx[i] + inf[2] * L.ny[i]) + inf[3] * L.nz[i]) > 0.00;
+}
+// mode 0: w = v - P ubar; mode 1: w = b - (v - P ubar); mode 2: w = P v
+__global__ void k_gm_apply(Params P, LevelView L, const double *v, const double *ubar, const double *b, double *w,
+                           int mode) {
+    const int N = L.N;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const bool fixE = inflow_energy_fixed(P, L, i);
+        for (int c = 0; c < 5; ++c) {
+            const size_t k = (size_t)c * N + i;
+            double pu = mode == 2 ? v[k] : ubar[k];
+            if (c == 4 && fixE) pu = 0.0;
+            w[k] = mode == 2 ? pu : (mode == 0 ? v[k] - pu : b[k] - (v[k] - pu));
+        }
+    }
+}
+
 struct SteadyAdjoint {
     int N = 0, E = 0, B = 0;
     double *u0, *v1, *v2, *Q[3], *p0, *dt, *D, *lap, *sens, *nh6, *nh7;
     double *lam, *vb[2], *ubar, *Qbar, *Dbar, *dtbar, *pbar, *p0bar, *nhbar, *nh6bar, *nh7bar, *Sbar, *bvjp;
     double *Vbar, *nbar, *swbar, *bwbar, *Abar, *abar, *Ju, *part, *out;
+    // GMRES: Krylov vectors [(m+1)][5N], right-hand side, dot partials
+    double *kry = nullptr, *rhs = nullptr, *gpart = nullptr, *gh = nullptr;
+    int kry_m = 0;
     bool recorded = false;
 };
 
@@ -794,6 +857,147 @@ static void download_geometry(flite_ctx &X, SteadyAdjoint &A, double *swb, doubl
     if (vb) CK(cudaMemcpyAsync(vb, A.Vbar, (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
 }
 
+// lam <- P (G_u^T lam + Ju) from lam = P Ju, `check` iterations per launch of
+// one captured graph, until |dlam| <= tol |P Ju|
+static int fixed_point_solve(flite_ctx &X, SteadyAdjoint &A, double ref, double tol, int max_iter, int *its,
+                             double *res_out) {
+    LevelView &L = X.V(0);
+    const int check = 10;
+    auto iterate = [&]() {
+        reverse(X, A, A.lam, false);
+        k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.ubar, A.Ju, A.lam, A.part);
+    };
+    cudaGraphExec_t gexec = nullptr;
+    if (max_iter >= check) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(X.s, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < check; ++k) iterate();
+        k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
+        CK(cudaStreamEndCapture(X.s, &g));
+        cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+    struct GraphGuard {
+        cudaGraphExec_t &g;
+        ~GraphGuard() { if (g) cudaGraphExecDestroy(g); }
+    } guard{gexec};
+    int it = 0;
+    double res = 1.0, h[2];
+    while (it < max_iter && res > tol) {
+        if (gexec && it + check <= max_iter) {
+            CK(cudaGraphLaunch(gexec, X.s));
+            it += check;
+        } else {
+            for (int k = 0; k < check && it < max_iter; ++k, ++it) iterate();
+            k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
+        }
+        CK(cudaMemcpyAsync(h, A.out + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+        if (!std::isfinite(h[0])) return FLITE_ENAN;
+        res = std::sqrt(h[0]) / ref;
+    }
+    *its = it;
+    *res_out = res;
+    return FLITE_OK;
+}
+
+// GMRES(m) for (I - P G_u^T) lam = P Ju from lam = P Ju; `its` counts
+// products with G_u^T (one per Arnoldi step plus one per restart)
+static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol, int max_iter, int m, int *its,
+                       double *res_out) {
+    LevelView &L = X.V(0);
+    const size_t n = 5 * (size_t)L.N;
+    if (A.kry_m < m) {
+        // the vectors of a smaller restart length stay allocated until the context goes
+        A.kry = X.alloc<double>((size_t)(m + 1) * n);
+        A.gpart = X.alloc<double>((size_t)kDotBlocks * (m + 1));
+        A.gh = X.alloc<double>(m + 1);
+        if (!A.rhs) A.rhs = X.alloc<double>(n);
+        A.kry_m = m;
+    }
+    const unsigned eb = 592;
+    k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.Ju, nullptr, nullptr, A.rhs, 2);  // b = P Ju
+    auto Vj = [&](int j) { return A.kry + (size_t)j * n; };
+    // h[0..k) = V[0..k)^T w, copied to the host
+    auto dots = [&](int k, const double *w, double *h) {
+        k_gm_dots<<<dim3(kDotBlocks, k), 256, 0, X.s>>>(A.kry, n, w, A.gpart);
+        k_gm_dots_final<<<(k + 127) / 128, 128, 0, X.s>>>(A.gpart, kDotBlocks, k, A.gh);
+        CK(cudaMemcpyAsync(h, A.gh, k * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+    };
+    auto norm = [&](const double *w) {
+        k_gm_dots<<<dim3(kDotBlocks, 1), 256, 0, X.s>>>(w, n, w, A.gpart);
+        k_gm_dots_final<<<1, 32, 0, X.s>>>(A.gpart, kDotBlocks, 1, A.gh);
+        double h;
+        CK(cudaMemcpyAsync(&h, A.gh, sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        CK(cudaStreamSynchronize(X.s));
+        return std::sqrt(h);
+    };
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hv(m + 1), y(m);
+    auto Hij = [&](int i, int j) -> double & { return H[(size_t)j * (m + 1) + i]; };
+    int total = 0;
+    double res = 1.0;
+    while (true) {
+        // r = b - (I - A) lam in V_0
+        reverse(X, A, A.lam, false);
+        k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.lam, A.ubar, A.rhs, Vj(0), 1);
+        ++total;
+        const double beta = norm(Vj(0));
+        if (!std::isfinite(beta)) return FLITE_ENAN;
+        res = beta / bnorm;
+        if (res <= tol || total >= max_iter) break;
+        k_gm_scale<<<eb, 256, 0, X.s>>>(Vj(0), n, 1.0 / beta);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;
+        for (; k < m && total < max_iter; ++k) {
+            double *w = Vj(k + 1);
+            reverse(X, A, Vj(k), false);
+            k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, Vj(k), A.ubar, nullptr, w, 0);
+            ++total;
+            for (int i = 0; i <= k; ++i) Hij(i, k) = 0.0;
+            for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+                dots(k + 1, w, hv.data());  // also left in A.gh
+                k_gm_combine<<<eb, 256, 0, X.s>>>(A.kry, n, k + 1, A.gh, -1.0, w);
+                for (int i = 0; i <= k; ++i) Hij(i, k) += hv[i];
+            }
+            const double hn = norm(w);
+            if (!std::isfinite(hn)) return FLITE_ENAN;
+            Hij(k + 1, k) = hn;
+            if (hn > 0) k_gm_scale<<<eb, 256, 0, X.s>>>(w, n, 1.0 / hn);
+            for (int i = 0; i < k; ++i) {  // earlier rotations
+                const double a = Hij(i, k), b = Hij(i + 1, k);
+                Hij(i, k) = cs[i] * a + sn[i] * b;
+                Hij(i + 1, k) = -sn[i] * a + cs[i] * b;
+            }
+            const double a = Hij(k, k), b = Hij(k + 1, k);
+            const double r = std::hypot(a, b);
+            cs[k] = r > 0 ? a / r : 1.0;
+            sn[k] = r > 0 ? b / r : 0.0;
+            Hij(k, k) = r;
+            Hij(k + 1, k) = 0.0;
+            g[k + 1] = -sn[k] * g[k];
+            g[k] = cs[k] * g[k];
+            if (std::fabs(g[k + 1]) / bnorm <= tol || hn == 0) {
+                ++k;
+                break;
+            }
+        }
+        // lam += V y with H y = g (upper triangular, k columns)
+        for (int i = k - 1; i >= 0; --i) {
+            double s = g[i];
+            for (int j = i + 1; j < k; ++j) s -= Hij(i, j) * y[j];
+            y[i] = s / Hij(i, i);
+        }
+        CK(cudaMemcpyAsync(A.gh, y.data(), k * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        k_gm_combine<<<eb, 256, 0, X.s>>>(A.kry, n, k, A.gh, 1.0, A.lam);
+    }
+    *its = total;
+    *res_out = res;
+    return FLITE_OK;
+}
+
 }  // namespace flite
 
 using namespace flite;
@@ -880,42 +1084,16 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
         const double ref = std::sqrt(h[3]);
         int it = 0;
         double res = ref > 0 ? 1.0 : 0.0;
-        // `check` iterations per launch of one captured graph, then the norms
-        const int check = 10;
-        auto iterate = [&]() {
-            reverse(X, A, A.lam, false);
-            k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.ubar, A.Ju, A.lam, A.part);
-        };
-        cudaGraphExec_t gexec = nullptr;
-        if (max_iter >= check) {
-            cudaGraph_t g = nullptr;
-            CK(cudaStreamBeginCapture(X.s, cudaStreamCaptureModeThreadLocal));
-            for (int k = 0; k < check; ++k) iterate();
-            k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
-            CK(cudaStreamEndCapture(X.s, &g));
-            cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
-            cudaGraphDestroy(g);
-            CK(e);
+        int rc = FLITE_OK;
+        if (ref > 0) {
+            rc = X.adj_method == 1 ? gmres_solve(X, A, ref, tol, max_iter, X.adj_restart, &it, &res)
+                                   : fixed_point_solve(X, A, ref, tol, max_iter, &it, &res);
         }
-        struct GraphGuard {
-            cudaGraphExec_t &g;
-            ~GraphGuard() { if (g) cudaGraphExecDestroy(g); }
-        } guard{gexec};
-        while (ref > 0 && it < max_iter && res > tol) {
-            if (gexec && it + check <= max_iter) {
-                CK(cudaGraphLaunch(gexec, X.s));
-                it += check;
-            } else {
-                for (int k = 0; k < check && it < max_iter; ++k, ++it) iterate();
-                k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
-            }
-            CK(cudaMemcpyAsync(h + 2, A.out + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
-            CK(cudaStreamSynchronize(X.s));
-            if (!std::isfinite(h[2])) {
-                ctx->err = "the adjoint iteration diverged";
-                return FLITE_ENAN;
-            }
-            res = std::sqrt(h[2]) / ref;
+        if (rc != FLITE_OK) {
+            copy(X, A.u0, L.u, n5);
+            cudaStreamSynchronize(X.s);
+            ctx->err = "the adjoint iteration diverged";
+            return rc;
         }
         if (iterations) *iterations = it;
         if (residual) *residual = res;
@@ -967,4 +1145,11 @@ extern "C" int flite_objective(flite_ctx *ctx, int objective, double *J) {
         ctx->err = e.what();
         return FLITE_ECUDA;
     }
+}
+
+extern "C" int flite_set_adjoint_method(flite_ctx *ctx, int method, int restart) {
+    if (!ctx || method < 0 || method > 1 || (method == 1 && (restart < 1 || restart > 500))) return FLITE_EINVAL;
+    ctx->adj_method = method;
+    if (method == 1) ctx->adj_restart = restart;
+    return FLITE_OK;
 }

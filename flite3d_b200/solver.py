@@ -231,6 +231,14 @@ class Solver:
                  "objective_jvp")
         return J.value, dJ.value
 
+    ADJOINT_METHODS = {"fixed-point": 0, "gmres": 1}
+
+    def set_adjoint_method(self, method="gmres", restart=50):
+        """How adjoint_solve iterates: "gmres" (restarted, the default) or
+        "fixed-point"."""
+        self._ck(self.be.set_adjoint_method(self._h, self.ADJOINT_METHODS[method], int(restart)),
+                 "set_adjoint_method")
+
     def adjoint_solve(self, name="CL", tol=1e-10, max_iter=100000):
         """Sensitivity of the lift or drag coefficient of the converged
         level-1 state to the level-1 geometry: dict with J, side_w_bar (3, E),

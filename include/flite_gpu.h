@@ -201,14 +201,21 @@ int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double *fwd_ms, d
  * converged solution u* = G(u*), the objective J (FLITE_OBJ_CL or
  * FLITE_OBJ_CD of calculateLiftAndDrag def_par:14710-14870 with the pressure
  * of the state) and dJ/dg = J_g + lam^T (dG/dg), where lam = P((dG/du)^T lam
- * + (dJ/du)^T) is iterated until |lam_new - lam| <= tol |lam| or max_iter
- * iterations (P keeps the energy of subsonic inflow nodes, which the
+ * + (dJ/du)^T) is solved to the relative residual tol or max_iter products
+ * with (dG/du)^T (P keeps the energy of subsonic inflow nodes, which the
  * boundary condition never updates, out of the adjoint).  Sensitivities to
  * node coordinates follow with fp_geometry_vjp of the preprocessor, which
  * owns the elements.  No reference counterpart: the reference has no
  * adjoint.                                                                  */
 #define FLITE_OBJ_CL 0
 #define FLITE_OBJ_CD 1
+/* How flite_adjoint_solve iterates: FLITE_ADJ_FIXED_POINT (lam <- P(G_u^T
+ * lam + J_u^T)) or FLITE_ADJ_GMRES (restarted GMRES with the given restart
+ * length on the same equation; the default, restart 50).  The stopping test
+ * is the same: |P J_u^T - (I - P G_u^T) lam| <= tol |P J_u^T|.               */
+#define FLITE_ADJ_FIXED_POINT 0
+#define FLITE_ADJ_GMRES 1
+int flite_set_adjoint_method(flite_ctx *ctx, int method, int restart);
 /* the objective J of flite_adjoint_solve at the context's level-1 state    */
 int flite_objective(flite_ctx *ctx, int objective, double *J);
 int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double *lam, double *ubar,

@@ -4,7 +4,8 @@
   one level-1 smoother iteration: lam . (G_u du + G_g dg) equals
   ubar . du + gbar . dg for random lam, du and geometry directions dg, at a
   generic state and at a converged one (1e-11 relative to the terms).
-* flite_adjoint_solve: dCL/dX and dCD/dX (through fp_geometry_vjp) along
+* flite_adjoint_solve (GMRES, and the fixed-point iteration, which agree):
+  dCL/dX and dCD/dX (through fp_geometry_vjp) along
   the normal displacement of seeded wall nodes against the oracle's FP64
   tangent solve (the forward sensitivity of the same fixed point, 1e-7) and
   against central differences of converged GPU solutions on moved meshes
@@ -170,6 +171,18 @@ def test_adjoint_matches_central_differences():
         fd = (Jp - Jm) / (2 * h)
         adj = (xb[:, k] * nrm[:, k]).sum()
         assert abs(adj - fd) <= 1e-5 * abs(fd), (k, adj, fd)
+
+
+def test_gmres_and_fixed_point_agree(small_case):
+    j, c, s, res = small_case
+    r1 = s.adjoint_solve("CL", tol=1e-12, max_iter=200000)
+    s.set_adjoint_method("fixed-point")
+    r2 = s.adjoint_solve("CL", tol=1e-12, max_iter=200000)
+    s.set_adjoint_method("gmres")
+    assert r1["residual"] <= 1e-12 and r2["residual"] <= 1e-12
+    assert r1["iterations"] < r2["iterations"]
+    for k in ("side_w_bar", "bnd_w_bar"):
+        assert np.abs(r1[k] - r2[k]).max() <= 1e-9 * np.abs(r2[k]).max()
 
 
 def test_adjoint_leaves_the_solve_unchanged():
