@@ -34,9 +34,13 @@ MESH = dict(nx=264, ny=88, nz=88, bump=0.05, levels=4)
 METRIC = "MG cycles/s"
 CONTROLS = dict(ReynoldsNumber=5000.0, MachNumber=0.5, alpha=0.0, CFLNumber=2.0, fluxType=1,
                 multigridScheme=3, numberOfGridsToUse=4, wallsAreIsentropic=1, viscosityScheme=1)
-WORKLOAD = ("laminar Navier-Stokes, Re 5e3, M 0.5, adiabatic walls, on the bump channel "
-            "264x88x88 hex -> 6 tets (2,099,065 nodes, 14,473,976 edges), 4 agglomerated MG "
-            "levels, growing V-cycle, 3-stage RK, CFL 2, central flux + JST, FP64")
+def workload(nodes=None, edges=None):
+    """The workload's name, with the mesh's size (the default mesh's when not given)."""
+    nodes = 2099065 if nodes is None else nodes
+    edges = 14473976 if edges is None else edges
+    return ("laminar Navier-Stokes, Re 5e3, M 0.5, adiabatic walls, on the bump channel "
+            f"{MESH['nx']}x{MESH['ny']}x{MESH['nz']} hex -> 6 tets ({nodes:,} nodes, {edges:,} edges), "
+            f"{MESH['levels']} agglomerated MG levels, growing V-cycle, 3-stage RK, CFL 2, central flux + JST, FP64")
 
 
 def _dist():
@@ -274,7 +278,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (generated bump-channel mesh, seeded +-1% density perturbation)",
-        "config": {"workload": WORKLOAD, "mesh_nodes": mesh.level(1).n_nodes,
+        "config": {"workload": workload(mesh.level(1).n_nodes, mesh.level(1).n_sides),
+                   "mesh_nodes": mesh.level(1).n_nodes,
                    "mesh_edges": mesh.level(1).n_sides, "levels": mesh.nlevels,
                    "parallelism": f"replicas{ws}" if ws > 1 else "single",
                    "l2": "inputs larger than L2 (state+mesh+edge buffer > 1 GB)",
@@ -416,7 +421,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "cycles/s", "n_gpus": 0,
         "steps": steps, "warmup": 1, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": {"workload": workload(mesh.level(1).n_nodes, mesh.level(1).n_sides)},
         "cpu_baseline": {"value": v, "unit": "cycles/s", "cores": threads, "kind": "port",
                          "sample": f"{steps} cycles after 1 warm-up cycle on {threads} threads; the "
                                    "Fortran reference cannot be compiled here (no Fortran "
@@ -480,8 +485,9 @@ def run_adjoint(args):
     from flite3d_b200.mesh import splitmix64
     if not torch.cuda.is_available():
         raise SystemExit("no CUDA device: the product path has no CPU fallback")
-    nx, ny, nz = 48, 16, 16
-    base = F.Mesh.bump_channel(nx, ny, nz, 0.05, nlevels=3)
+    nx, ny, nz = [int(v) for v in args.adjoint_mesh.split(",")]
+    nlev = 3 if nx * ny * nz <= 48 * 16 * 16 else 4
+    base = F.Mesh.bump_channel(nx, ny, nz, 0.05, nlevels=nlev)
     X = base.array(1, "coords")
     jit = np.random.default_rng(11).uniform(-1, 1, X.shape) * 0.15 / nz
     jit[:, :base.level(1).n_bnodes] = 0.0
@@ -489,9 +495,9 @@ def run_adjoint(args):
     at = lambda Y: base.with_level1_geometry(*base.geometry(Y))
     mesh = at(X)
     c = F.default_controls(ReynoldsNumber=0.0, fluxType=1, CFLNumber=2.0, multigridScheme=3,
-                           numberOfGridsToUse=3)
+                           numberOfGridsToUse=nlev)
 
-    def converge(m, u0=None, tol=1e-15, max_cycles=6000):
+    def converge(m, u0=None, tol=1e-15, max_cycles=args.adjoint_primal_cycles):
         s = F.Solver(c, m)
         s.set_state(F.initial_state(c, m) if u0 is None else u0)
         s.start()
@@ -514,20 +520,25 @@ def run_adjoint(args):
     for name in ("CL", "CD"):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = s.adjoint_solve(name, tol=1e-12, max_iter=400000)
+        r = s.adjoint_solve(name, tol=1e-12, max_iter=args.adjoint_max_iter)
         torch.cuda.synchronize()
         out[name] = (r, time.perf_counter() - t0,
                      base.geometry_vjp(r["side_w_bar"], r["bnd_w_bar"], r["volume_bar"], xyz=X))
     # the same CL adjoint by the plain fixed-point iteration, for comparison
-    s.set_adjoint_method("fixed-point")
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    rf = s.adjoint_solve("CL", tol=1e-12, max_iter=400000)
-    torch.cuda.synchronize()
-    t_fixed = time.perf_counter() - t0
-    s.set_adjoint_method("gmres")
-    xf = base.geometry_vjp(rf["side_w_bar"], rf["bnd_w_bar"], rf["volume_bar"], xyz=X)
-    agree = float(np.abs(xf - out["CL"][2]).max() / np.abs(out["CL"][2]).max())
+    # (on the Euler mesh; on larger ones it takes too long for a bench run)
+    fixed = None
+    if nx * ny * nz <= 48 * 16 * 16:
+        s.set_adjoint_method("fixed-point")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rf = s.adjoint_solve("CL", tol=1e-12, max_iter=400000)
+        torch.cuda.synchronize()
+        t_fixed = time.perf_counter() - t0
+        s.set_adjoint_method("gmres")
+        xf = base.geometry_vjp(rf["side_w_bar"], rf["bnd_w_bar"], rf["volume_bar"], xyz=X)
+        fixed = {"seconds": t_fixed, "iterations": rf["iterations"], "residual": rf["residual"],
+                 "max_rel_diff_dCL_dX_vs_gmres": float(np.abs(xf - out["CL"][2]).max() /
+                                                        np.abs(out["CL"][2]).max())}
     reg, ind = base.array(1, "node_reg"), base.array(1, "node_ind")
     wall = ind[reg[0] - 1:reg[1]] - 1
     bw, bidx = base.array(1, "bnd_w"), base.array(1, "bnd_idx")
@@ -558,18 +569,19 @@ def run_adjoint(args):
         "dtype": "f64", "data": "synthetic (generated bump-channel mesh, jittered interior nodes, freestream start)",
         "config": {"workload": f"steady adjoint of CL and CD, inviscid M 0.5, central flux + JST, on the bump "
                                f"channel {nx}x{ny}x{nz} hex -> 6 tets with interior nodes jittered by 15% of the "
-                               "spacing, 3 agglomerated MG levels for the primal, FP64",
+                               f"spacing, {nlev} agglomerated MG levels for the primal, FP64",
                    "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides},
         "primal": {"seconds": t_primal, "cycles": ncyc, "residual": res},
         "adjoint": {name: {"J": out[name][0]["J"], "seconds": out[name][1], "iterations": out[name][0]["iterations"],
                            "residual": out[name][0]["residual"]} for name in out},
         "adjoint_over_primal_time": out["CL"][1] / t_primal,
+        "ms_per_transpose_product": 1e3 * out["CL"][1] / max(out["CL"][0]["iterations"], 1),
+        "ms_per_primal_cycle": 1e3 * t_primal / ncyc,
         "method": "GMRES(50) on (I - P G_u^T) lam = P J_u^T",
-        "fixed_point": {"seconds": t_fixed, "iterations": rf["iterations"], "residual": rf["residual"],
-                        "max_rel_diff_dCL_dX_vs_gmres": agree},
+        "fixed_point": fixed,
         "fd_check": {"nodes": len(nodes), "step": h, "seconds": t_fd,
                      "max_rel_err": {n: max(e) for n, e in errs.items()},
-                     "median_rel_err": {n: float(np.median(e)) for n, e in errs.items()}},
+                     "median_rel_err": {n: float(np.median(e)) for n, e in errs.items()}} if nodes else None,
         "gpu_launches": None,
     }), flush=True)
 
@@ -645,7 +657,11 @@ def main():
     ap.add_argument("--rans-nk", type=int, default=240)
     ap.add_argument("--adjoint", action="store_true",
                     help="the steady adjoint (dCL/dX, dCD/dX) workload with its finite-difference check")
-    ap.add_argument("--adjoint-nodes", type=int, default=32)
+    ap.add_argument("--adjoint-nodes", type=int, default=32, help="wall nodes of the finite-difference check")
+    ap.add_argument("--adjoint-mesh", default="48,16,16", help="NX,NY,NZ hexes of the adjoint workload")
+    ap.add_argument("--adjoint-primal-cycles", type=int, default=6000)
+    ap.add_argument("--adjoint-max-iter", type=int, default=400000,
+                    help="products with the transposed iteration Jacobian per adjoint solve")
     ap.add_argument("--batch-meshes", type=int, default=3)
     ap.add_argument("--batch-conditions", type=int, default=16)
     args = ap.parse_args()

@@ -563,6 +563,43 @@ __global__ void k_adj_objective(Params P, LevelView L, const int *wall, int nwal
     *J = f * acc;
 }
 
+// the same with a thread per wall-list entry, for a list without repeated
+// nodes: the terms of J summed per block, the blocks in order by
+// k_gm_dots_final
+constexpr int kObjBlocks = 64;
+__global__ void k_adj_objective_par(Params P, LevelView L, const int *wall, int nwall, double ground, double e0,
+                                    double e1, double e2, double aref, const double *u, double *part, double *Ju,
+                                    double *Abar, double *nbar) {
+    __shared__ double red[256];
+    const int N = L.N;
+    const double pinf = 1. / (P.gamma * P.mach * P.mach);
+    const double f = 2.0 / aref;
+    double acc = 0.0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nwall; q += gridDim.x * blockDim.x) {
+        const int ip = wall[q];
+        if (!(L.cz[ip] > (ground + 0.01))) continue;
+        double x[5], p, dp[5];
+        for (int c = 0; c < 5; ++c) x[c] = u[(size_t)c * N + ip];
+        pressure_grad(P, x, &p, dp);
+        const double n[3] = {L.nx[ip], L.ny[ip], L.nz[ip]};
+        const double dn = (n[0] * e0 + n[1] * e1) + n[2] * e2;
+        const double A = L.wallArea[ip], dpi = p - pinf;
+        acc -= A * dpi * dn;
+        for (int c = 0; c < 5; ++c) Ju[(size_t)c * N + ip] += -f * A * dn * dp[c];
+        Abar[ip] += -f * dpi * dn;
+        nbar[ip] += -f * A * dpi * e0;
+        nbar[(size_t)N + ip] += -f * A * dpi * e1;
+        nbar[2 * (size_t)N + ip] += -f * A * dpi * e2;
+    }
+    red[threadIdx.x] = f * acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
 // ---- node normals and wall areas from the boundary coefficients ------------
 // n_i = a_i/|a_i|, a_i = -sum over the node's boundary edges of w_b
 // (makeBoundaryNormals def_par:15394-15521): abar_i = (nbar - (nbar.n) n)/|a|
@@ -762,6 +799,35 @@ static SteadyAdjoint &buffers(flite_ctx &X) {
         a->out = X.alloc<double>(4);
     }
     return *X.sadj;
+}
+
+static void zero(flite_ctx &X, double *p, size_t n);
+
+// J into out[0], and its adjoints dJ/du (Ju), dJ/dA (Abar), dJ/dn (nbar),
+// which the caller has zeroed
+static void objective_terms(flite_ctx &X, SteadyAdjoint &A, int objective, const double *u) {
+    LevelView &L = X.V(0);
+    DevLevel &D = X.lv[0];
+    const double PI = 4.0 * std::atan(1.0);
+    const double aR = X.c.alpha * PI / 180., bR = X.c.beta * PI / 180.;
+    const double ft[3] = {std::cos(aR) * std::cos(bR), std::sin(bR), std::sin(aR)};
+    const double fn1[3] = {-ft[2], 0.0, ft[0]};
+    const double *dir = objective == FLITE_OBJ_CL ? fn1 : ft;
+    const int nw = (int)D.wall.size();
+    if (nw == 0) {
+        zero(X, A.out, 1);
+        return;
+    }
+    std::vector<int> w(D.wall);
+    std::sort(w.begin(), w.end());
+    if (std::adjacent_find(w.begin(), w.end()) == w.end()) {
+        k_adj_objective_par<<<kObjBlocks, 256, 0, X.s>>>(X.P, L, D.d_wall, nw, X.c.groundplane, dir[0], dir[1],
+                                                         dir[2], X.c.referenceArea, u, A.part, A.Ju, A.Abar, A.nbar);
+        k_gm_dots_final<<<1, 32, 0, X.s>>>(A.part, kObjBlocks, 1, A.out);
+    } else {
+        k_adj_objective<<<1, 1, 0, X.s>>>(X.P, L, D.d_wall, nw, X.c.groundplane, dir[0], dir[1], dir[2],
+                                          X.c.referenceArea, u, A.out, A.Ju, A.Abar, A.nbar);
+    }
 }
 
 static void zero(flite_ctx &X, double *p, size_t n) {
@@ -1052,7 +1118,6 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
         flite_ctx &X = *ctx;
         SteadyAdjoint &A = buffers(X);
         LevelView &L = X.V(0);
-        DevLevel &D = X.lv[0];
         const size_t n5 = 5 * (size_t)L.N, N = L.N;
         // linearisation point: the context's level-1 state
         copy(X, L.u, A.u0, n5);
@@ -1060,17 +1125,7 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
         zero(X, A.Abar, N);
         zero(X, A.Vbar, N);
         zero(X, A.nbar, 3 * N);
-        const double PI = 4.0 * std::atan(1.0);
-        const double aR = X.c.alpha * PI / 180., bR = X.c.beta * PI / 180.;
-        const double ft[3] = {std::cos(aR) * std::cos(bR), std::sin(bR), std::sin(aR)};
-        const double fn1[3] = {-ft[2], 0.0, ft[0]};
-        const double *dir = objective == FLITE_OBJ_CL ? fn1 : ft;
-        if (!D.wall.empty())
-            k_adj_objective<<<1, 1, 0, X.s>>>(X.P, L, D.d_wall, (int)D.wall.size(), X.c.groundplane, dir[0],
-                                              dir[1], dir[2], X.c.referenceArea, A.u0, A.out, A.Ju, A.Abar,
-                                              A.nbar);
-        else
-            zero(X, A.out, 1);
+        objective_terms(X, A, objective, A.u0);
         record(X, A);
         // lam_0 = P Ju
         zero(X, A.lam, n5);
@@ -1123,21 +1178,11 @@ extern "C" int flite_objective(flite_ctx *ctx, int objective, double *J) {
         flite_ctx &X = *ctx;
         SteadyAdjoint &A = buffers(X);
         LevelView &L = X.V(0);
-        DevLevel &D = X.lv[0];
         const size_t n5 = 5 * (size_t)L.N, N = L.N;
         zero(X, A.Ju, n5);
         zero(X, A.Abar, N);
         zero(X, A.nbar, 3 * N);
-        zero(X, A.out, 1);
-        const double PI = 4.0 * std::atan(1.0);
-        const double aR = X.c.alpha * PI / 180., bR = X.c.beta * PI / 180.;
-        const double ft[3] = {std::cos(aR) * std::cos(bR), std::sin(bR), std::sin(aR)};
-        const double fn1[3] = {-ft[2], 0.0, ft[0]};
-        const double *dir = objective == FLITE_OBJ_CL ? fn1 : ft;
-        if (!D.wall.empty())
-            k_adj_objective<<<1, 1, 0, X.s>>>(X.P, L, D.d_wall, (int)D.wall.size(), X.c.groundplane, dir[0],
-                                              dir[1], dir[2], X.c.referenceArea, L.u, A.out, A.Ju, A.Abar,
-                                              A.nbar);
+        objective_terms(X, A, objective, L.u);
         CK(cudaMemcpyAsync(J, A.out, sizeof(double), cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
         return FLITE_OK;
