@@ -162,9 +162,16 @@ __global__ void k_adj_stage(Params P, LevelView L, int stage, const double *vbar
     const unsigned char cls = L.bc[i];
     double n0 = 0, n1 = 0, n2 = 0;
     if (cls != BC_NONE) { n0 = L.nx[i]; n1 = L.ny[i]; n2 = L.nz[i]; }
-    const bool inc_proj = cls == BC_WALL || cls == BC_IWALL || cls == BC_SYM;  // inviscid
+    // setBCsOnIncrementField: slip projection, or the no-slip wall of a
+    // viscous run (momentum, and the energy of a non-isentropic wall, zeroed)
+    const bool vwall = cls == BC_WALL && P.viscous;
+    const bool inc_proj = (cls == BC_WALL && !P.viscous) || cls == BC_IWALL || cls == BC_SYM;
     for (int c = 0; c < 5; ++c) sp[c] = s[c];
     if (inc_proj) remove_normal(sp, n0, n1, n2, 1.0);
+    if (vwall) {
+        sp[1] = 0.0; sp[2] = 0.0; sp[3] = 0.0;
+        if (!P.isentropic) sp[4] = 0.0;
+    }
     const double dtJ = P.CFL * P.RK[stage - 1];
     for (int c = 0; c < 5; ++c) d[c] = dtJ * sp[c];
     const bool clip = !(fabs(d[0] / up[0]) < P.maxInc);
@@ -174,7 +181,13 @@ __global__ void k_adj_stage(Params P, LevelView L, int stage, const double *vbar
     const double relax = relax_param(P, *L.cyc);
     for (int c = 0; c < 5; ++c) z2[c] = z[c];
     double m2[3] = {0, 0, 0};
-    if (cls == BC_WALL || cls == BC_SYM) remove_normal(z2, n0, n1, n2, 1.0);
+    if ((cls == BC_WALL && !P.viscous) || cls == BC_SYM) remove_normal(z2, n0, n1, n2, 1.0);
+    if (vwall) {  // momentum rho * coordinateMovement / physicalTimeStep
+        z2[1] = z2[0] * L.cmx[i] / P.pts;
+        z2[2] = z2[0] * L.cmy[i] / P.pts;
+        z2[3] = z2[0] * L.cmz[i] / P.pts;
+        if (!P.isentropic) z2[4] = z2[0] * P.Tinf / P.gamma;
+    }
     if (cls == BC_IWALL) {
         remove_normal(z2, n0, n1, n2, relax);
         m2[0] = z2[1]; m2[1] = z2[2]; m2[2] = z2[3];
@@ -203,7 +216,15 @@ __global__ void k_adj_stage(Params P, LevelView L, int stage, const double *vbar
     }
     if (lim2) zb[0] = 0.0;
     double nb[3] = {0, 0, 0};
-    if (cls == BC_WALL || cls == BC_SYM) remove_normal_rev(z, n0, n1, n2, 1.0, zb, nb);
+    if ((cls == BC_WALL && !P.viscous) || cls == BC_SYM) remove_normal_rev(z, n0, n1, n2, 1.0, zb, nb);
+    if (vwall) {
+        zb[0] += ((zb[1] * L.cmx[i] + zb[2] * L.cmy[i]) + zb[3] * L.cmz[i]) / P.pts;
+        zb[1] = 0.0; zb[2] = 0.0; zb[3] = 0.0;
+        if (!P.isentropic) {
+            zb[0] += zb[4] * P.Tinf / P.gamma;
+            zb[4] = 0.0;
+        }
+    }
     if (cls == BC_IWALL) {
         if (!P.isentropic) {  // E = rho Tinf / gamma + ke / (2 rho) of the projected momentum
             const double r = z2[0], ke = (m2[0] * m2[0] + m2[1] * m2[1]) + m2[2] * m2[2];
@@ -227,6 +248,10 @@ __global__ void k_adj_stage(Params P, LevelView L, int stage, const double *vbar
     double sb[5];
     for (int c = 0; c < 5; ++c) sb[c] = dtJ * db[c];
     if (inc_proj) remove_normal_rev(s, n0, n1, n2, 1.0, sb, nb);
+    if (vwall) {
+        sb[1] = 0.0; sb[2] = 0.0; sb[3] = 0.0;
+        if (!P.isentropic) sb[4] = 0.0;
+    }
     double dtb = 0.0, vbv = 0.0;
     for (int c = 0; c < 5; ++c) {
         const double tb = sb[c] * dti / Vi;
@@ -372,20 +397,44 @@ __device__ __forceinline__ void ts_term_grad(const Params &P, const double *u, d
     }
 }
 
-// Sbar = dJ/dS of dt = 0.5 / (S/V): the interior edges add f of this node's
-// own state, each boundary edge 2 f(own) + f(other); then the pressure of the
-// iteration's start goes back to the state
+// the viscous term of one edge end: dv = 2 max(1/Re, mu) |w|^2 / rho
+__device__ __forceinline__ double visc_ts_term(const Params &P, double mu, double r, double al, double *dvr,
+                                               double *dvmu, double *dval) {
+    const bool m = P.am < mu;
+    const double vis = m ? mu : P.am;
+    const double dv = 2.0 * vis * al / r;
+    *dvr = -dv / r;
+    *dvmu = m ? 2.0 * al / r : 0.0;
+    *dval = 2.0 * vis / r;
+    return dv;
+}
+
+// dt = 0.5 / t with t = S/V + h/V^2: S sums the convective terms (each
+// interior edge f of this node's own state, each boundary edge 2 f(own) +
+// f(other)), h the viscous ones (each interior edge the other end's dv, each
+// boundary edge 2 dv(own) + dv(other)); the adjoints of S and h per node
+// (Sbar, Hbar), this node's own terms in reverse, then the pressure of the
+// iteration's start back to the state.  mu: the viscosity the step read;
+// mubar its adjoint (laminar runs)
 __global__ void k_adj_timestep(Params P, LevelView L, const double *u0, const double *p0, const double *dt,
-                               const double *dtbar, const double *p0bar, double *ubar, double *Sbar, double *Vbar) {
+                               const double *dtbar, const double *p0bar, const double *mu, double *ubar,
+                               double *mubar, double *Sbar, double *Hbar, double *Vbar) {
     const int i = tidx();
     if (i >= L.N) return;
     const int N = L.N;
     const double Vi = L.V[i], dti = dt[i];
-    const double tt = 0.5 / dti;  // S/V
+    const double tt = 0.5 / dti;  // S/V + h/V^2
     const double tb = -0.5 * dtbar[i] / (tt * tt);
-    const double sbi = tb / Vi;
+    const double sbi = tb / Vi, hbi = tb / (Vi * Vi);
     Sbar[i] = sbi;
-    if (Vbar) Vbar[i] += -tb * tt / Vi;
+    Hbar[i] = hbi;
+    auto hbar_of = [&](int j) {
+        const double tj = 0.5 / dt[j];
+        return (-0.5 * dtbar[j] / (tj * tj)) / (L.V[j] * L.V[j]);
+    };
+    double h = 0.0, mb = 0.0, rvb = 0.0;  // viscous sum, and this node's rho / mu adjoints from it
+    const bool visc = P.viscous;
+    const double mui = visc ? mu[i] : 0.0;
     double ui[5];
     for (int c = 0; c < 5; ++c) ui[c] = u0[(size_t)c * N + i];
     const double pi = p0[i];
@@ -397,6 +446,16 @@ __global__ void k_adj_timestep(Params P, LevelView L, const double *u0, const do
         ts_term_grad(P, ui, pi, w, fu, &fp, nullptr);
         for (int c = 0; c < 5; ++c) ub[c] += sbi * fu[c];
         pb += sbi * fp;
+        if (visc) {
+            const int j = L.inc[k].y;
+            const double al = (w[0] * w[0] + w[1] * w[1]) + w[2] * w[2];
+            double dr, dm, da;
+            h += visc_ts_term(P, mu[j], u0[j], al, &dr, &dm, &da);  // the other end's term
+            visc_ts_term(P, mui, ui[0], al, &dr, &dm, &da);         // this end's, in the other's h
+            const double hj = hbar_of(j);
+            rvb += hj * dr;
+            mb += hj * dm;
+        }
     }
     for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
         const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
@@ -411,7 +470,21 @@ __global__ void k_adj_timestep(Params P, LevelView L, const double *u0, const do
         ts_term_grad(P, ui, pi, w, fu, &fp, nullptr);
         for (int c = 0; c < 5; ++c) ub[c] += wgt * fu[c];
         pb += wgt * fp;
+        if (visc) {
+            const double al = (w[0] * w[0] + w[1] * w[1]) + w[2] * w[2];
+            double dr, dm, da;
+            const double own = visc_ts_term(P, mui, ui[0], al, &dr, &dm, &da);
+            double drj, dmj, daj;
+            h += 2.0 * own + visc_ts_term(P, mu[j], u0[j], al, &drj, &dmj, &daj);
+            const double hw = 2.0 * hbi + hbar_of(j);
+            rvb += hw * dr;
+            mb += hw * dm;
+        }
     }
+    ub[0] += rvb;
+    if (visc && mubar) mubar[i] = mb;
+    // V: t = S/V + h/V^2
+    if (Vbar) Vbar[i] += tb * (-tt / Vi - h / (Vi * Vi * Vi));
     pb += p0bar[i];
     double p, dp[5];
     pressure_grad(P, ui, &p, dp);
@@ -420,7 +493,7 @@ __global__ void k_adj_timestep(Params P, LevelView L, const double *u0, const do
 
 // geometry sweep: the coefficient adjoints of the time step, per edge
 __global__ void k_adj_timestep_w(Params P, LevelView L, const double *u0, const double *p0, const double *Sbar,
-                                 double *swbar) {
+                                 const double *Hbar, const double *mu, double *swbar) {
     const int e = tidx();
     if (e >= L.E) return;
     const int N = L.N, E = L.E;
@@ -433,12 +506,19 @@ __global__ void k_adj_timestep_w(Params P, LevelView L, const double *u0, const 
         for (int c = 0; c < 5; ++c) u[c] = u0[(size_t)c * N + n];
         ts_term_grad(P, u, p0[n], w, fu, &fp, fw);
         for (int c = 0; c < 3; ++c) acc[c] += Sbar[n] * fw[c];
+        if (P.viscous) {  // this end's dv goes to the other end's h
+            const double al = (w[0] * w[0] + w[1] * w[1]) + w[2] * w[2];
+            double dr, dm, da;
+            visc_ts_term(P, mu[n], u[0], al, &dr, &dm, &da);
+            const double hw = Hbar[side == 0 ? nd.y : nd.x];
+            for (int c = 0; c < 3; ++c) acc[c] += hw * da * 2.0 * w[c];
+        }
     }
     for (int c = 0; c < 3; ++c) swbar[(size_t)c * E + e] += acc[c];
 }
 
 __global__ void k_adj_timestep_bw(Params P, LevelView L, const double *u0, const double *p0, const double *Sbar,
-                                  double *bwbar) {
+                                  const double *Hbar, const double *mu, double *bwbar) {
     const int b = tidx();
     if (b >= L.B) return;
     const int N = L.N, B = L.B;
@@ -452,6 +532,13 @@ __global__ void k_adj_timestep_bw(Params P, LevelView L, const double *u0, const
         ts_term_grad(P, u, p0[n], w, fu, &fp, fw);
         const double wgt = 2.0 * Sbar[n] + Sbar[o];
         for (int c = 0; c < 3; ++c) acc[c] += wgt * fw[c];
+        if (P.viscous) {
+            const double al = (w[0] * w[0] + w[1] * w[1]) + w[2] * w[2];
+            double dr, dm, da;
+            visc_ts_term(P, mu[n], u[0], al, &dr, &dm, &da);
+            const double hw = 2.0 * Hbar[n] + Hbar[o];
+            for (int c = 0; c < 3; ++c) acc[c] += hw * da * 2.0 * w[c];
+        }
     }
     for (int c = 0; c < 3; ++c) bwbar[(size_t)c * B + b] += acc[c];
 }
@@ -531,14 +618,366 @@ __global__ void k_adj_flux_bw(Params P, LevelView L, const double *x, const doub
     for (int d = 0; d < 3; ++d) bwbar[(size_t)d * B + b] += acc[d];
 }
 
+// ---- makeViscosityTerm (def_par:5198-5893), laminar, reverse ---------------
+// Layout: G [12][N] Galerkin sums of the primitives (u, v, w, T = gamma/(gamma-1)
+// p/rho) per direction (index 4a + k), tau [9][N] (stress xx, xy, xz, yy, yz,
+// zz, then the heat flux, projected at adiabatic walls), prim [4][N].
+
+// forward helper of the record: the sums G of def_par:5380-5480 at the
+// iteration's start (the primal keeps them in registers)
+__global__ void k_adj_visc_sums(LevelView L, const double *prim, double *G) {
+    const int i = tidx();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double g[12];
+    for (int c = 0; c < 12; ++c) g[c] = 0.0;
+    double qi[4];
+    for (int c = 0; c < 4; ++c) qi[c] = prim[(size_t)c * N + i];
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const int e = t.x >= 0 ? t.x : ~t.x;
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        for (int c = 0; c < 4; ++c) {
+            const double sq = qi[c] + prim[(size_t)c * N + t.y];
+            for (int a = 0; a < 3; ++a) g[a * 4 + c] += (t.x >= 0 ? sq : -sq) * w[a];
+        }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        const int2 nd = L.bedge[b];
+        const int j = side == 0 ? nd.y : nd.x;
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        for (int c = 0; c < 4; ++c) {
+            const double q = 3. * qi[c] + prim[(size_t)c * N + j];
+            for (int a = 0; a < 3; ++a) g[a * 4 + c] += q * w[a];
+        }
+    }
+    for (int c = 0; c < 12; ++c) G[(size_t)c * N + i] = g[c];
+}
+
+// adjoint of one viscous edge flux (f2..f5 of def_par:5700-5760) to one end:
+// W = the adjoints of f2..f5, w the coefficients, t (9) and v (3) that end's
+// tensor and velocity; adds to tb (9) and vb (3)
+__device__ __forceinline__ void visc_flux_end_rev(const double *W, const double *w, const double *t,
+                                                  const double *v, double *tb, double *vb) {
+    const double wx = w[0], wy = w[1], wz = w[2];
+    tb[0] += wx * W[0];
+    tb[1] += wy * W[0] + wx * W[1];
+    tb[2] += wz * W[0] + wx * W[2];
+    tb[3] += wy * W[1];
+    tb[4] += wz * W[1] + wy * W[2];
+    tb[5] += wz * W[2];
+    tb[6] += wx * W[3];
+    tb[7] += wy * W[3];
+    tb[8] += wz * W[3];
+    const double D0 = wx * W[3], D1 = wy * W[3], D2 = wz * W[3];  // adjoints of dut1..dut3
+    tb[0] += v[0] * D0;
+    tb[1] += v[1] * D0 + v[0] * D1;
+    tb[2] += v[2] * D0 + v[0] * D2;
+    tb[3] += v[1] * D1;
+    tb[4] += v[2] * D1 + v[1] * D2;
+    tb[5] += v[2] * D2;
+    vb[0] += (t[0] * D0 + t[1] * D1) + t[2] * D2;
+    vb[1] += (t[1] * D0 + t[3] * D1) + t[4] * D2;
+    vb[2] += (t[2] * D0 + t[4] * D1) + t[5] * D2;
+}
+// d f2..f5 / d w of the same terms (dt = the summed tensors, dut the summed
+// velocity products)
+__device__ __forceinline__ void visc_flux_w_rev(const double *W, const double *dt, const double *dut, double *wb) {
+    wb[0] += ((W[0] * dt[0] + W[1] * dt[1]) + W[2] * dt[2]) + W[3] * (dt[6] + dut[0]);
+    wb[1] += ((W[0] * dt[1] + W[1] * dt[3]) + W[2] * dt[4]) + W[3] * (dt[7] + dut[1]);
+    wb[2] += ((W[0] * dt[2] + W[1] * dt[4]) + W[2] * dt[5]) + W[3] * (dt[8] + dut[2]);
+}
+__device__ __forceinline__ void visc_dut(const double *t, const double *v, double *dut) {
+    dut[0] = (v[0] * t[0] + v[1] * t[1]) + v[2] * t[2];
+    dut[1] = (v[0] * t[1] + v[1] * t[3]) + v[2] * t[4];
+    dut[2] = (v[0] * t[2] + v[1] * t[4]) + v[2] * t[5];
+}
+
+// pass 2 in reverse, gathered per node: the adjoints of this node's tensor and
+// velocity from the adjoints of the viscous fluxes (diss(:,2:5) -= flux)
+__global__ void k_adj_visc_flux(LevelView L, const double *Dbar, const double *tau, const double *prim,
+                                double *tbar, double *velbar) {
+    const int i = tidx();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double ti[9], vi[3], Wi[4], tb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, vb[3] = {0, 0, 0};
+    for (int c = 0; c < 9; ++c) ti[c] = tau[(size_t)c * N + i];
+    for (int c = 0; c < 3; ++c) vi[c] = prim[(size_t)c * N + i];
+    for (int c = 0; c < 4; ++c) Wi[c] = -Dbar[(size_t)(1 + c) * N + i];
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const int e = t.x >= 0 ? t.x : ~t.x;
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        double W[4];
+        for (int c = 0; c < 4; ++c) {
+            const double Wj = -Dbar[(size_t)(1 + c) * N + t.y];
+            W[c] = t.x >= 0 ? Wi[c] - Wj : Wj - Wi[c];  // +f to node 1, -f to node 2
+        }
+        visc_flux_end_rev(W, w, ti, vi, tb, vb);
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        const int ind = L.bind[b];
+        if (ind == 2 || ind == 9) continue;
+        const int2 nd = L.bedge[b];
+        const int j = side == 0 ? nd.y : nd.x;
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        double W[4];
+        // +f to both ends and 2 g(own) to each: f's weight W_i + W_j, g's 2 W_i
+        for (int c = 0; c < 4; ++c) W[c] = 3. * Wi[c] - Dbar[(size_t)(1 + c) * N + j];
+        visc_flux_end_rev(W, w, ti, vi, tb, vb);
+    }
+    for (int c = 0; c < 9; ++c) tbar[(size_t)c * N + i] = tb[c];
+    for (int c = 0; c < 3; ++c) velbar[(size_t)c * N + i] = vb[c];
+}
+
+// the node part in reverse (def_par:5500-5635): tensor and heat flux from the
+// gradients, Sutherland's viscosity of T (and the viscosity's own adjoint
+// mubar_out, when given), the adiabatic-wall projection; out: the adjoint of
+// the sums G, and the parts of ubar (rho) and p0bar; geometry: V and normals
+__global__ void k_adj_visc_node(Params P, LevelView L, const double *u0, const double *p0, const double *G,
+                                const double *tbar, const double *lam_mu, double *Gbar, double *ubar, double *p0bar,
+                                double *Vbar, double *nbar) {
+    const int i = tidx();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double gOg = P.gamma / (P.gamma - 1.0);
+    const double tc = (P.gamma - 1.0) * P.mach * P.mach;
+    const double Vi = L.V[i], vt = 1. / Vi;
+    double gr[12];
+    for (int c = 0; c < 12; ++c) gr[c] = G[(size_t)c * N + i] * vt;
+    const double ux = gr[0], vx = gr[1], wx = gr[2], Tx = gr[3];
+    const double uy = gr[4], vy = gr[5], wy = gr[6], Ty = gr[7];
+    const double uz = gr[8], vz = gr[9], wz = gr[10], Tz = gr[11];
+    const double r = u0[i];
+    double T = gOg * p0[i] / r;
+    const bool tfloor = T <= 0.001;
+    if (tfloor) T = 0.001;
+    const double a = tc * T, sa = sqrt(a);
+    const double C = P.Tinf + 198.6, Dn = tc * P.Tinf * T + 198.6;
+    const double oRe = 1. / P.Re, oPr = 1. / P.Pr;
+    const double mu = oRe * ((a * sa) * (C / Dn));
+    const double kc = oPr * mu;
+    double tb[9];
+    for (int c = 0; c < 9; ++c) tb[c] = tbar[(size_t)c * N + i];
+    const double f43 = 4. / 3., f23 = 2. / 3.;
+    const double lin[6] = {f43 * ux - f23 * (vy + wz), uy + vx, uz + wx, f43 * vy - f23 * (ux + wz), vz + wy,
+                           f43 * wz - f23 * (ux + vy)};
+    double mub = lam_mu ? lam_mu[i] : 0.0;
+    for (int c = 0; c < 6; ++c) mub += tb[c] * lin[c];
+    // heat flux h = kc grad T, projected at adiabatic walls of level 1
+    double h[3] = {kc * Tx, kc * Ty, kc * Tz}, hb[3] = {tb[6], tb[7], tb[8]};
+    if (L.grid == 1 && L.bc[i] == BC_WALL) {
+        const double n[3] = {L.nx[i], L.ny[i], L.nz[i]};
+        const double hn = (h[0] * n[0] + h[1] * n[1]) + h[2] * n[2];
+        const double bn = (hb[0] * n[0] + hb[1] * n[1]) + hb[2] * n[2];
+        if (nbar)
+            for (int c = 0; c < 3; ++c) nbar[(size_t)c * N + i] -= bn * h[c] + hn * hb[c];
+        for (int c = 0; c < 3; ++c) hb[c] -= bn * n[c];
+    }
+    mub += oPr * ((hb[0] * Tx + hb[1] * Ty) + hb[2] * Tz);
+    double gb[12];
+    gb[0] = mu * (f43 * tb[0] - f23 * tb[3] - f23 * tb[5]);  // u_x
+    gb[5] = mu * (-f23 * tb[0] + f43 * tb[3] - f23 * tb[5]);  // v_y
+    gb[10] = mu * (-f23 * tb[0] - f23 * tb[3] + f43 * tb[5]);  // w_z
+    gb[4] = mu * tb[1];  // u_y
+    gb[1] = mu * tb[1];  // v_x
+    gb[8] = mu * tb[2];  // u_z
+    gb[2] = mu * tb[2];  // w_x
+    gb[9] = mu * tb[4];  // v_z
+    gb[6] = mu * tb[4];  // w_y
+    gb[3] = kc * hb[0];
+    gb[7] = kc * hb[1];
+    gb[11] = kc * hb[2];
+    double vb = 0.0;
+    for (int c = 0; c < 12; ++c) {
+        Gbar[(size_t)c * N + i] = gb[c] * vt;
+        vb -= gb[c] * gr[c] * vt;
+    }
+    if (Vbar) Vbar[i] += vb;
+    // mu(T) = oRe (tc T)^1.5 C / (tc Tin T + 198.6)
+    const double dmu = tfloor ? 0.0 : oRe * C * (1.5 * tc * sa / Dn - (a * sa) * tc * P.Tinf / (Dn * Dn));
+    const double Tb = mub * dmu;
+    p0bar[i] += Tb * gOg / r;
+    ubar[i] += -Tb * (gOg * p0[i] / r) / r;
+}
+
+// pass 1 in reverse, gathered per node: the primitives' adjoints from the
+// sums' adjoints (interior edges: G(1) += (q1+q2) w, G(2) -= (q1+q2) w;
+// boundary edges: G(own) += (3 q_own + q_other) w), plus the velocities'
+// adjoints of the flux pass, to the state and the pressure
+__global__ void k_adj_visc_prim(Params P, LevelView L, const double *u0, const double *p0, const double *Gbar,
+                                const double *velbar, double *ubar, double *p0bar) {
+    const int i = tidx();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double gi[12], qb[4] = {0, 0, 0, 0};
+    for (int c = 0; c < 12; ++c) gi[c] = Gbar[(size_t)c * N + i];
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const int e = t.x >= 0 ? t.x : ~t.x;
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        for (int c = 0; c < 4; ++c)
+            for (int a = 0; a < 3; ++a) {
+                const double gj = Gbar[(size_t)(a * 4 + c) * N + t.y];
+                qb[c] += w[a] * (t.x >= 0 ? gi[a * 4 + c] - gj : gj - gi[a * 4 + c]);
+            }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        const int2 nd = L.bedge[b];
+        const int j = side == 0 ? nd.y : nd.x;
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        for (int c = 0; c < 4; ++c)
+            for (int a = 0; a < 3; ++a)
+                qb[c] += w[a] * (3. * gi[a * 4 + c] + Gbar[(size_t)(a * 4 + c) * N + j]);
+    }
+    for (int c = 0; c < 3; ++c) qb[c] += velbar[(size_t)c * N + i];
+    const double gOg = P.gamma / (P.gamma - 1.0);
+    const double r = u0[i];
+    double rb = 0.0;
+    for (int c = 0; c < 3; ++c) {
+        const double m = u0[(size_t)(1 + c) * N + i];
+        ubar[(size_t)(1 + c) * N + i] += qb[c] / r;
+        rb -= qb[c] * (m / r) / r;
+    }
+    const double q3 = gOg * p0[i] / r;
+    p0bar[i] += qb[3] * gOg / r;
+    rb -= qb[3] * q3 / r;
+    ubar[i] += rb;
+}
+
+// geometry sweep: coefficient adjoints of both viscous passes, per edge
+__global__ void k_adj_visc_w(LevelView L, const double *Dbar, const double *tau, const double *prim,
+                             const double *Gbar, double *swbar) {
+    const int e = tidx();
+    if (e >= L.E) return;
+    const int N = L.N, E = L.E;
+    const int2 nd = L.edge[e];
+    double a[9], b[9], va[3], vb[3], dt[9], da[3], db[3], dut[3], W[4], wb[3] = {0, 0, 0};
+    for (int c = 0; c < 9; ++c) {
+        a[c] = tau[(size_t)c * N + nd.x];
+        b[c] = tau[(size_t)c * N + nd.y];
+        dt[c] = a[c] + b[c];
+    }
+    for (int c = 0; c < 3; ++c) { va[c] = prim[(size_t)c * N + nd.x]; vb[c] = prim[(size_t)c * N + nd.y]; }
+    visc_dut(a, va, da);
+    visc_dut(b, vb, db);
+    for (int c = 0; c < 3; ++c) dut[c] = da[c] + db[c];
+    for (int c = 0; c < 4; ++c) W[c] = -Dbar[(size_t)(1 + c) * N + nd.x] + Dbar[(size_t)(1 + c) * N + nd.y];
+    visc_flux_w_rev(W, dt, dut, wb);
+    for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < 3; ++k) {
+            const double sq = prim[(size_t)c * N + nd.x] + prim[(size_t)c * N + nd.y];
+            wb[k] += sq * (Gbar[(size_t)(k * 4 + c) * N + nd.x] - Gbar[(size_t)(k * 4 + c) * N + nd.y]);
+        }
+    for (int k = 0; k < 3; ++k) swbar[(size_t)k * E + e] += wb[k];
+}
+
+__global__ void k_adj_visc_bw(LevelView L, const double *Dbar, const double *tau, const double *prim,
+                              const double *Gbar, double *bwbar) {
+    const int b = tidx();
+    if (b >= L.B) return;
+    const int N = L.N, B = L.B;
+    const int2 nd = L.bedge[b];
+    double wb[3] = {0, 0, 0};
+    if (!(L.bind[b] == 2 || L.bind[b] == 9)) {
+        double ta[9], tbb[9], va[3], vb[3], dt[9], da[3], db[3], dut[3], W1[4], W2[4], Wf[4];
+        for (int c = 0; c < 9; ++c) {
+            ta[c] = tau[(size_t)c * N + nd.x];
+            tbb[c] = tau[(size_t)c * N + nd.y];
+            dt[c] = ta[c] + tbb[c];
+        }
+        for (int c = 0; c < 3; ++c) { va[c] = prim[(size_t)c * N + nd.x]; vb[c] = prim[(size_t)c * N + nd.y]; }
+        visc_dut(ta, va, da);
+        visc_dut(tbb, vb, db);
+        for (int c = 0; c < 3; ++c) dut[c] = da[c] + db[c];
+        for (int c = 0; c < 4; ++c) {
+            W1[c] = -Dbar[(size_t)(1 + c) * N + nd.x];
+            W2[c] = -Dbar[(size_t)(1 + c) * N + nd.y];
+            Wf[c] = W1[c] + W2[c];
+        }
+        visc_flux_w_rev(Wf, dt, dut, wb);
+        for (int c = 0; c < 4; ++c) { W1[c] *= 2.; W2[c] *= 2.; }
+        visc_flux_w_rev(W1, ta, da, wb);
+        visc_flux_w_rev(W2, tbb, db, wb);
+    }
+    for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < 3; ++k) {
+            const double q1 = prim[(size_t)c * N + nd.x], q2 = prim[(size_t)c * N + nd.y];
+            wb[k] += (3. * q1 + q2) * Gbar[(size_t)(k * 4 + c) * N + nd.x] +
+                     (3. * q2 + q1) * Gbar[(size_t)(k * 4 + c) * N + nd.y];
+        }
+    for (int k = 0; k < 3; ++k) bwbar[(size_t)k * B + b] += wb[k];
+}
+
+// the objective's wall-stress part: tbar seeds of sum over wall nodes of
+// f A (S n).e (S the stress of tau), with its A and n adjoints
+__global__ void k_adj_objective_stress(Params P, LevelView L, const int *wall, int nwall, double ground, double e0,
+                                       double e1, double e2, double aref, const double *tau, double *tJ,
+                                       double *Abar, double *nbar) {
+    const int N = L.N;
+    const double f = 2.0 / aref;
+    const double e[3] = {e0, e1, e2};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nwall; q += gridDim.x * blockDim.x) {
+        const int ip = wall[q];
+        if (!(L.cz[ip] > (ground + 0.01))) continue;
+        const double n[3] = {L.nx[ip], L.ny[ip], L.nz[ip]};
+        double t[6];
+        for (int c = 0; c < 6; ++c) t[c] = tau[(size_t)c * N + ip];
+        const double S[3][3] = {{t[0], t[1], t[2]}, {t[1], t[3], t[4]}, {t[2], t[4], t[5]}};
+        const double A = L.wallArea[ip];
+        double sd = 0.0;
+        for (int d = 0; d < 3; ++d)
+            for (int c = 0; c < 3; ++c) sd += e[d] * S[d][c] * n[c];
+        Abar[ip] += f * sd;
+        for (int c = 0; c < 3; ++c) {
+            double s = 0.0;
+            for (int d = 0; d < 3; ++d) s += e[d] * S[d][c];
+            nbar[(size_t)c * N + ip] += f * A * s;
+        }
+        const double fA = f * A;
+        tJ[ip] += fA * e[0] * n[0];
+        tJ[(size_t)N + ip] += fA * (e[0] * n[1] + e[1] * n[0]);
+        tJ[2 * (size_t)N + ip] += fA * (e[0] * n[2] + e[2] * n[0]);
+        tJ[3 * (size_t)N + ip] += fA * e[1] * n[1];
+        tJ[4 * (size_t)N + ip] += fA * (e[1] * n[2] + e[2] * n[1]);
+        tJ[5 * (size_t)N + ip] += fA * e[2] * n[2];
+    }
+}
+
+// pbar (of the iteration's starting pressure) onto the state
+__global__ void k_adj_pbar_to_u(Params P, LevelView L, const double *u0, const double *pbar, double *ubar) {
+    const int i = tidx();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double x[5], p, dp[5];
+    for (int c = 0; c < 5; ++c) x[c] = u0[(size_t)c * N + i];
+    pressure_grad(P, x, &p, dp);
+    for (int c = 0; c < 5; ++c) ubar[(size_t)c * N + i] += pbar[i] * dp[c];
+}
+
 // ---- objective -----------------------------------------------------------
 // J = 2/A_ref sum over wall nodes (above the ground plane) of
 // -A_i (p_i - p_inf) (n_i . e) (calculateLiftAndDrag def_par:14710-14870,
 // inviscid part, pressure of the state): J, dJ/du, dJ/dA and dJ/dn.  One
 // thread walks the wall list in order (a node listed twice counts twice).
+// the wall-stress term A (S n).e of a laminar run, S the stress part of tau
+__device__ __forceinline__ double stress_term(const LevelView &L, const double *tau, int ip, double e0, double e1,
+                                              double e2) {
+    const size_t N = L.N;
+    const double t0 = tau[ip], t1 = tau[N + ip], t2 = tau[2 * N + ip], t3 = tau[3 * N + ip];
+    const double t4 = tau[4 * N + ip], t5 = tau[5 * N + ip];
+    const double n0 = L.nx[ip], n1 = L.ny[ip], n2 = L.nz[ip];
+    const double s0 = (t0 * n0 + t1 * n1) + t2 * n2, s1 = (t1 * n0 + t3 * n1) + t4 * n2;
+    const double s2 = (t2 * n0 + t4 * n1) + t5 * n2;
+    return L.wallArea[ip] * ((s0 * e0 + s1 * e1) + s2 * e2);
+}
+
 __global__ void k_adj_objective(Params P, LevelView L, const int *wall, int nwall, double ground, double e0,
-                                double e1, double e2, double aref, const double *u, double *J, double *Ju,
-                                double *Abar, double *nbar) {
+                                double e1, double e2, double aref, const double *u, const double *tau, double *J,
+                                double *Ju, double *Abar, double *nbar) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     const int N = L.N;
     const double pinf = 1. / (P.gamma * P.mach * P.mach);
@@ -554,6 +993,7 @@ __global__ void k_adj_objective(Params P, LevelView L, const int *wall, int nwal
         const double dn = (n[0] * e0 + n[1] * e1) + n[2] * e2;
         const double A = L.wallArea[ip], dpi = p - pinf;
         acc -= A * dpi * dn;
+        if (tau) acc += stress_term(L, tau, ip, e0, e1, e2);
         for (int c = 0; c < 5; ++c) Ju[(size_t)c * N + ip] += -f * A * dn * dp[c];
         Abar[ip] += -f * dpi * dn;
         nbar[ip] += -f * A * dpi * e0;
@@ -568,8 +1008,8 @@ __global__ void k_adj_objective(Params P, LevelView L, const int *wall, int nwal
 // k_gm_dots_final
 constexpr int kObjBlocks = 64;
 __global__ void k_adj_objective_par(Params P, LevelView L, const int *wall, int nwall, double ground, double e0,
-                                    double e1, double e2, double aref, const double *u, double *part, double *Ju,
-                                    double *Abar, double *nbar) {
+                                    double e1, double e2, double aref, const double *u, const double *tau,
+                                    double *part, double *Ju, double *Abar, double *nbar) {
     __shared__ double red[256];
     const int N = L.N;
     const double pinf = 1. / (P.gamma * P.mach * P.mach);
@@ -585,6 +1025,7 @@ __global__ void k_adj_objective_par(Params P, LevelView L, const int *wall, int 
         const double dn = (n[0] * e0 + n[1] * e1) + n[2] * e2;
         const double A = L.wallArea[ip], dpi = p - pinf;
         acc -= A * dpi * dn;
+        if (tau) acc += stress_term(L, tau, ip, e0, e1, e2);
         for (int c = 0; c < 5; ++c) Ju[(size_t)c * N + ip] += -f * A * dn * dp[c];
         Abar[ip] += -f * dpi * dn;
         nbar[ip] += -f * A * dpi * e0;
@@ -643,7 +1084,7 @@ __global__ void k_adj_bedge_geom(LevelView L, const double *abar, const double *
 
 // ---- iteration: lam_new = P (ubar + Ju), with the norms of the change ------
 constexpr int kAdjBlocks = 128;
-__global__ void k_adj_update(Params P, LevelView L, const double *ubar, const double *Ju, double *lam,
+__global__ void k_adj_update(Params P, LevelView L, int ncomp, const double *ubar, const double *Ju, double *lam,
                              double *part) {
     __shared__ double red[2][256];
     const int N = L.N;
@@ -655,7 +1096,7 @@ __global__ void k_adj_update(Params P, LevelView L, const double *ubar, const do
             const double *inf = &P.inf[cls == BC_FAR3 ? 0 : 6];
             fixE = ((inf[1] * L.nx[i] + inf[2] * L.ny[i]) + inf[3] * L.nz[i]) > 0.00;
         }
-        for (int c = 0; c < 5; ++c) {
+        for (int c = 0; c < ncomp; ++c) {
             const size_t k = (size_t)c * N + i;
             double v = ubar[k] + Ju[k];
             if (c == 4 && fixE) v = 0.0;
@@ -686,6 +1127,11 @@ __global__ void k_adj_norms(const double *part, int nblk, double *out) {
     double s = 0.0;
     for (int b = 0; b < nblk; ++b) s += part[2 * b + threadIdx.x];
     out[threadIdx.x] = s;
+}
+
+__global__ void k_adj_add(const double *a, size_t n, double *w) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        w[i] = w[i] + a[i];
 }
 
 __global__ void k_adj_zero(double *a, size_t n) {
@@ -740,12 +1186,12 @@ __device__ __forceinline__ bool inflow_energy_fixed(const Params &P, const Level
     return ((inf[1] * L.nx[i] + inf[2] * L.ny[i]) + inf[3] * L.nz[i]) > 0.00;
 }
 // mode 0: w = v - P ubar; mode 1: w = b - (v - P ubar); mode 2: w = P v
-__global__ void k_gm_apply(Params P, LevelView L, const double *v, const double *ubar, const double *b, double *w,
-                           int mode) {
+__global__ void k_gm_apply(Params P, LevelView L, int ncomp, const double *v, const double *ubar, const double *b,
+                           double *w, int mode) {
     const int N = L.N;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const bool fixE = inflow_energy_fixed(P, L, i);
-        for (int c = 0; c < 5; ++c) {
+        for (int c = 0; c < ncomp; ++c) {
             const size_t k = (size_t)c * N + i;
             double pu = mode == 2 ? v[k] : ubar[k];
             if (c == 4 && fixE) pu = 0.0;
@@ -754,12 +1200,22 @@ __global__ void k_gm_apply(Params P, LevelView L, const double *v, const double 
     }
 }
 
+// The adjoint's unknowns are the level-1 state (5 components) and, in a
+// laminar run, the laminar viscosity that the next iteration's time step reads
+// (makeTimeSteps runs before makeViscosityTerm recomputes it, def_par:
+// 1010-1035): lam, ubar, Ju and the Krylov vectors hold nc = 5 or 6
+// components of N values.
 struct SteadyAdjoint {
-    int N = 0, E = 0, B = 0;
+    int N = 0, E = 0, B = 0, nc = 5;
     double *u0, *v1, *v2, *Q[3], *p0, *dt, *D, *lap, *sens, *nh6, *nh7;
-    double *lam, *vb[2], *ubar, *Qbar, *Dbar, *dtbar, *pbar, *p0bar, *nhbar, *nh6bar, *nh7bar, *Sbar, *bvjp;
+    double *lam, *vb[2], *ubar, *Qbar, *Dbar, *dtbar, *pbar, *p0bar, *nhbar, *nh6bar, *nh7bar, *Sbar, *Hbar, *bvjp;
     double *Vbar, *nbar, *swbar, *bwbar, *Abar, *abar, *Ju, *part, *out;
-    // GMRES: Krylov vectors [(m+1)][5N], right-hand side, dot partials
+    // laminar runs: the viscosity the time step reads, the tensor, primitives
+    // and gradient sums of the iteration's start, their adjoints, the
+    // objective's tensor seeds and the primal's viscosity kept aside
+    double *mu0 = nullptr, *tau = nullptr, *prim = nullptr, *Gv = nullptr, *tbar = nullptr, *velbar = nullptr;
+    double *Gbar = nullptr, *tJ = nullptr, *mu_keep = nullptr, *ws_keep = nullptr;
+    // GMRES: Krylov vectors [(m+1)][nc N], right-hand side, dot partials
     double *kry = nullptr, *rhs = nullptr, *gpart = nullptr, *gh = nullptr;
     int kry_m = 0;
     bool recorded = false;
@@ -771,7 +1227,7 @@ static const char *steady_adjoint_unsupported(const flite_ctx &X) {
     const flite_controls &c = X.c;
     if (c.fluxType != 1) return "the steady adjoint takes the central flux (fluxType 1)";
     if (c.precision != FLITE_FP64) return "the steady adjoint runs in FP64";
-    if (c.ReynoldsNumber > 0) return "the steady adjoint covers inviscid runs (ReynoldsNumber 0)";
+    if (c.turbulenceModel != 0) return "the steady adjoint covers inviscid and laminar runs (no turbulence model)";
     if (c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";
     if (c.useDissipationWeighting) return "the steady adjoint takes unweighted dissipation";
     return nullptr;
@@ -783,13 +1239,27 @@ static SteadyAdjoint &buffers(flite_ctx &X) {
         auto *a = new SteadyAdjoint();
         X.sadj = a;
         a->N = L.N; a->E = L.E; a->B = L.B;
-        const size_t n5 = 5 * (size_t)L.N, N = L.N;
-        for (double **p : {&a->u0, &a->v1, &a->v2, &a->Q[0], &a->Q[1], &a->Q[2], &a->D, &a->lap, &a->lam,
-                           &a->vb[0], &a->vb[1], &a->ubar, &a->Qbar, &a->Dbar, &a->nhbar, &a->Ju})
+        a->nc = X.P.viscous ? 6 : 5;
+        const size_t n5 = 5 * (size_t)L.N, N = L.N, na = (size_t)a->nc * N;
+        for (double **p : {&a->u0, &a->v1, &a->v2, &a->Q[0], &a->Q[1], &a->Q[2], &a->D, &a->lap, &a->vb[0],
+                           &a->vb[1], &a->Qbar, &a->Dbar, &a->nhbar})
             *p = X.alloc<double>(n5);
+        for (double **p : {&a->lam, &a->ubar, &a->Ju}) *p = X.alloc<double>(na);
         for (double **p : {&a->p0, &a->dt, &a->sens, &a->nh6, &a->nh7, &a->dtbar, &a->pbar, &a->p0bar, &a->nh6bar,
-                           &a->nh7bar, &a->Sbar, &a->Vbar, &a->Abar})
+                           &a->nh7bar, &a->Sbar, &a->Hbar, &a->Vbar, &a->Abar})
             *p = X.alloc<double>(N);
+        if (X.P.viscous) {
+            a->mu0 = X.alloc<double>(N);
+            a->mu_keep = X.alloc<double>(N);
+            a->ws_keep = X.alloc<double>(3 * N);
+            a->tau = X.alloc<double>(9 * N);
+            a->tbar = X.alloc<double>(9 * N);
+            a->tJ = X.alloc<double>(9 * N);
+            a->prim = X.alloc<double>(4 * N);
+            a->velbar = X.alloc<double>(3 * N);
+            a->Gv = X.alloc<double>(12 * N);
+            a->Gbar = X.alloc<double>(12 * N);
+        }
         a->nbar = X.alloc<double>(3 * N);
         a->abar = X.alloc<double>(3 * N);
         a->swbar = X.alloc<double>(3 * (size_t)L.E);
@@ -805,7 +1275,8 @@ static void zero(flite_ctx &X, double *p, size_t n);
 
 // J into out[0], and its adjoints dJ/du (Ju), dJ/dA (Abar), dJ/dn (nbar),
 // which the caller has zeroed
-static void objective_terms(flite_ctx &X, SteadyAdjoint &A, int objective, const double *u) {
+static void objective_terms(flite_ctx &X, SteadyAdjoint &A, int objective, const double *u,
+                            const double *tau = nullptr) {
     LevelView &L = X.V(0);
     DevLevel &D = X.lv[0];
     const double PI = 4.0 * std::atan(1.0);
@@ -820,13 +1291,21 @@ static void objective_terms(flite_ctx &X, SteadyAdjoint &A, int objective, const
     }
     std::vector<int> w(D.wall);
     std::sort(w.begin(), w.end());
-    if (std::adjacent_find(w.begin(), w.end()) == w.end()) {
+    const bool unique = std::adjacent_find(w.begin(), w.end()) == w.end();
+    if (unique) {
         k_adj_objective_par<<<kObjBlocks, 256, 0, X.s>>>(X.P, L, D.d_wall, nw, X.c.groundplane, dir[0], dir[1],
-                                                         dir[2], X.c.referenceArea, u, A.part, A.Ju, A.Abar, A.nbar);
+                                                         dir[2], X.c.referenceArea, u, tau, A.part, A.Ju, A.Abar,
+                                                         A.nbar);
         k_gm_dots_final<<<1, 32, 0, X.s>>>(A.part, kObjBlocks, 1, A.out);
     } else {
         k_adj_objective<<<1, 1, 0, X.s>>>(X.P, L, D.d_wall, nw, X.c.groundplane, dir[0], dir[1], dir[2],
-                                          X.c.referenceArea, u, A.out, A.Ju, A.Abar, A.nbar);
+                                          X.c.referenceArea, u, tau, A.out, A.Ju, A.Abar, A.nbar);
+    }
+    if (tau && A.tJ) {  // the wall stress: seeds of the tensor's adjoint, kept for the geometry sweep
+        zero(X, A.tJ, 9 * (size_t)L.N);
+        k_adj_objective_stress<<<unique ? kObjBlocks : 1, unique ? 256 : 1, 0, X.s>>>(
+            X.P, L, D.d_wall, nw, X.c.groundplane, dir[0], dir[1], dir[2], X.c.referenceArea, tau, A.tJ, A.Abar,
+            A.nbar);
     }
 }
 
@@ -837,6 +1316,43 @@ static void copy(flite_ctx &X, const double *a, double *b, size_t n) {
     CK(cudaMemcpyAsync(b, a, n * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
 }
 
+// the laminar part of the reverse sweep: the viscous fluxes' adjoints (from
+// Dbar; with tseed added, the objective's tensor seeds), the node part with
+// the viscosity's own adjoint lam_mu, the gradient sums; into ubar and p0bar
+static void viscous_reverse(flite_ctx &X, SteadyAdjoint &A, const double *lam_mu, const double *tseed,
+                            bool from_fluxes, bool geom) {
+    LevelView &L = X.V(0);
+    const size_t N = L.N;
+    const unsigned nbk = X.nblk(N);
+    if (from_fluxes) {
+        k_adj_visc_flux<<<nbk, X.nb, 0, X.s>>>(L, A.Dbar, A.tau, A.prim, A.tbar, A.velbar);
+    } else {
+        zero(X, A.tbar, 9 * N);
+        zero(X, A.velbar, 3 * N);
+    }
+    if (tseed) k_adj_add<<<592, 256, 0, X.s>>>(tseed, 9 * N, A.tbar);
+    k_adj_visc_node<<<nbk, X.nb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.Gv, A.tbar, lam_mu, A.Gbar, A.ubar, A.p0bar,
+                                           geom ? A.Vbar : nullptr, geom ? A.nbar : nullptr);
+    k_adj_visc_prim<<<nbk, X.nb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.Gbar, A.velbar, A.ubar, A.p0bar);
+    if (geom) {
+        k_adj_visc_w<<<X.eblk(L.E), X.eb, 0, X.s>>>(L, A.Dbar, A.tau, A.prim, A.Gbar, A.swbar);
+        if (L.B > 0) k_adj_visc_bw<<<X.eblk(L.B), X.eb, 0, X.s>>>(L, A.Dbar, A.tau, A.prim, A.Gbar, A.bwbar);
+    }
+}
+
+// laminar runs: the objective's wall-stress part of dJ/du, through the
+// gradient chain at the recorded state, added to Ju
+static void objective_stress_u(flite_ctx &X, SteadyAdjoint &A) {
+    LevelView &L = X.V(0);
+    const size_t N = L.N, n5 = 5 * N;
+    zero(X, A.ubar, n5);
+    zero(X, A.p0bar, N);
+    zero(X, A.Dbar, n5);
+    viscous_reverse(X, A, nullptr, A.tJ, false, false);
+    k_adj_pbar_to_u<<<X.nblk(N), X.nb, 0, X.s>>>(X.P, L, A.u0, A.p0bar, A.ubar);
+    k_adj_add<<<592, 256, 0, X.s>>>(A.ubar, n5, A.Ju);
+}
+
 // the primal iteration from A.u0, recording the stage states, their
 // residuals and the iteration's time step and dissipation
 static void record(flite_ctx &X, SteadyAdjoint &A) {
@@ -844,9 +1360,16 @@ static void record(flite_ctx &X, SteadyAdjoint &A) {
     const size_t n5 = 5 * (size_t)L.N, N = L.N;
     copy(X, A.u0, L.u, n5);
     copy(X, A.u0, L.uprev, n5);
+    if (X.P.viscous) copy(X, A.mu0, L.mu, N);
     X.pressure(0);
     X.timesteps(0);
     X.dissipation(0);
+    if (X.P.viscous) {
+        X.viscous(0);
+        copy(X, L.tau, A.tau, 9 * N);
+        copy(X, L.prim, A.prim, 4 * N);
+        k_adj_visc_sums<<<X.nblk(N), X.nb, 0, X.s>>>(L, A.prim, A.Gv);
+    }
     copy(X, L.p, A.p0, N);
     copy(X, L.dt, A.dt, N);
     copy(X, L.diss, A.D, n5);
@@ -865,12 +1388,13 @@ static void record(flite_ctx &X, SteadyAdjoint &A) {
     A.recorded = true;
 }
 
-// ubar = G_u^T lam (geometry sweep: and the geometry adjoints)
-static void reverse(flite_ctx &X, SteadyAdjoint &A, const double *lam, bool geom) {
+// ubar = G_u^T lam (geometry sweep: and the geometry adjoints); lam and ubar
+// hold nc components (the state, and in laminar runs the viscosity)
+static void reverse(flite_ctx &X, SteadyAdjoint &A, const double *lam, bool geom, const double *tseed = nullptr) {
     LevelView &L = X.V(0);
     const size_t n5 = 5 * (size_t)L.N, N = L.N;
     const unsigned nbk = X.nblk(N);
-    zero(X, A.ubar, n5);
+    zero(X, A.ubar, (size_t)A.nc * N);
     zero(X, A.Dbar, n5);
     zero(X, A.dtbar, N);
     zero(X, A.p0bar, N);
@@ -891,26 +1415,29 @@ static void reverse(flite_ctx &X, SteadyAdjoint &A, const double *lam, bool geom
         }
         vin = vout;
     }
+    if (X.P.viscous) viscous_reverse(X, A, lam + n5, geom ? tseed : nullptr, true, geom);
     const bool jst = !(X.c.fourthOrderDissipationFactor == 0 && X.c.secondOrderDissipationFactor == 0);
     if (jst) {
         k_adj_jst_edges<<<nbk, X.nb, 0, X.s>>>(X.P, L, A.u0, A.dt, A.lap, A.sens, A.nh6, A.nh7, A.Dbar, A.ubar,
                                                A.dtbar, A.nhbar, A.nh6bar, A.nh7bar, Vb);
         k_adj_jst_lap<<<nbk, X.nb, 0, X.s>>>(L, A.nhbar, A.nh6bar, A.nh7bar, A.ubar, A.p0bar);
     }
-    k_adj_timestep<<<nbk, X.nb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.dt, A.dtbar, A.p0bar, A.ubar, A.Sbar, Vb);
+    k_adj_timestep<<<nbk, X.nb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.dt, A.dtbar, A.p0bar, A.mu0, A.ubar,
+                                          X.P.viscous ? A.ubar + n5 : nullptr, A.Sbar, A.Hbar, Vb);
     if (geom) {
-        k_adj_timestep_w<<<X.eblk(L.E), X.eb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.Sbar, A.swbar);
-        if (L.B > 0) k_adj_timestep_bw<<<X.eblk(L.B), X.eb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.Sbar, A.bwbar);
+        k_adj_timestep_w<<<X.eblk(L.E), X.eb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.Sbar, A.Hbar, A.mu0, A.swbar);
+        if (L.B > 0)
+            k_adj_timestep_bw<<<X.eblk(L.B), X.eb, 0, X.s>>>(X.P, L, A.u0, A.p0, A.Sbar, A.Hbar, A.mu0, A.bwbar);
     }
 }
 
 // geometry adjoints: zeroed, swept, the normals and wall areas chained to bnd_w
-static void geometry_sweep(flite_ctx &X, SteadyAdjoint &A, const double *lam) {
+static void geometry_sweep(flite_ctx &X, SteadyAdjoint &A, const double *lam, const double *tseed = nullptr) {
     LevelView &L = X.V(0);
     const size_t N = L.N;
     zero(X, A.swbar, 3 * (size_t)L.E);
     zero(X, A.bwbar, 3 * (size_t)std::max(L.B, 1));
-    reverse(X, A, lam, true);
+    reverse(X, A, lam, true, tseed);
     k_adj_normals<<<X.nblk(N), X.nb, 0, X.s>>>(L, A.nbar, A.abar);
     if (L.B > 0) k_adj_bedge_geom<<<X.eblk(L.B), X.eb, 0, X.s>>>(L, A.abar, A.Abar, A.bwbar);
 }
@@ -931,7 +1458,7 @@ static int fixed_point_solve(flite_ctx &X, SteadyAdjoint &A, double ref, double 
     const int check = 10;
     auto iterate = [&]() {
         reverse(X, A, A.lam, false);
-        k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.ubar, A.Ju, A.lam, A.part);
+        k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.nc, A.ubar, A.Ju, A.lam, A.part);
     };
     cudaGraphExec_t gexec = nullptr;
     if (max_iter >= check) {
@@ -973,7 +1500,7 @@ static int fixed_point_solve(flite_ctx &X, SteadyAdjoint &A, double ref, double 
 static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol, int max_iter, int m, int *its,
                        double *res_out) {
     LevelView &L = X.V(0);
-    const size_t n = 5 * (size_t)L.N;
+    const size_t n = (size_t)A.nc * L.N;
     if (A.kry_m < m) {
         // the vectors of a smaller restart length stay allocated until the context goes
         A.kry = X.alloc<double>((size_t)(m + 1) * n);
@@ -983,7 +1510,7 @@ static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol,
         A.kry_m = m;
     }
     const unsigned eb = 592;
-    k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.Ju, nullptr, nullptr, A.rhs, 2);  // b = P Ju
+    k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.nc, A.Ju, nullptr, nullptr, A.rhs, 2);  // b = P Ju
     auto Vj = [&](int j) { return A.kry + (size_t)j * n; };
     // h[0..k) = V[0..k)^T w, copied to the host
     auto dots = [&](int k, const double *w, double *h) {
@@ -1007,7 +1534,7 @@ static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol,
     while (true) {
         // r = b - (I - A) lam in V_0
         reverse(X, A, A.lam, false);
-        k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.lam, A.ubar, A.rhs, Vj(0), 1);
+        k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.nc, A.lam, A.ubar, A.rhs, Vj(0), 1);
         ++total;
         const double beta = norm(Vj(0));
         if (!std::isfinite(beta)) return FLITE_ENAN;
@@ -1020,7 +1547,7 @@ static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol,
         for (; k < m && total < max_iter; ++k) {
             double *w = Vj(k + 1);
             reverse(X, A, Vj(k), false);
-            k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, Vj(k), A.ubar, nullptr, w, 0);
+            k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.nc, Vj(k), A.ubar, nullptr, w, 0);
             ++total;
             for (int i = 0; i <= k; ++i) Hij(i, k) = 0.0;
             for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
@@ -1069,21 +1596,34 @@ static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol,
 using namespace flite;
 
 extern "C" int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double *lam, double *ubar,
-                                   double *side_w_bar, double *bnd_w_bar, double *volume_bar) {
+                                   double *side_w_bar, double *bnd_w_bar, double *volume_bar, const double *mu,
+                                   const double *lam_mu, double *mu_bar) {
     if (!ctx || !u || !lam || !ubar) return FLITE_EINVAL;
     if (const char *why = steady_adjoint_unsupported(*ctx)) {
         ctx->err = why;
         return FLITE_EUNSUPPORTED;
+    }
+    if (ctx->P.viscous && !mu) {
+        ctx->err = "a laminar run's iteration needs the viscosity its time step reads";
+        return FLITE_EINVAL;
     }
     try {
         flite_ctx &X = *ctx;
         SteadyAdjoint &A = buffers(X);
         LevelView &L = X.V(0);
         const size_t n5 = 5 * (size_t)L.N, N = L.N;
+        const bool visc = X.P.viscous;
         // the primal state of level 1 is kept: the record overwrites u, uprev,
-        // p, dt, the dissipation and rhs
+        // p, dt, the dissipation and rhs (and the viscosity and wall stress)
         std::vector<double> keep(n5);
         CK(cudaMemcpyAsync(keep.data(), L.u, n5 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        if (visc) {
+            copy(X, L.mu, A.mu_keep, N);
+            copy(X, L.wstress, A.ws_keep, 3 * N);
+            CK(cudaMemcpyAsync(A.mu0, mu, N * sizeof(double), cudaMemcpyHostToDevice, X.s));
+            if (lam_mu) CK(cudaMemcpyAsync(A.lam + n5, lam_mu, N * sizeof(double), cudaMemcpyHostToDevice, X.s));
+            else zero(X, A.lam + n5, N);
+        }
         CK(cudaMemcpyAsync(A.u0, u, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
         CK(cudaMemcpyAsync(A.lam, lam, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
         record(X, A);
@@ -1094,7 +1634,12 @@ extern "C" int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double
         if (geom) geometry_sweep(X, A, A.lam);
         else reverse(X, A, A.lam, false);
         CK(cudaMemcpyAsync(ubar, A.ubar, n5 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        if (visc && mu_bar) CK(cudaMemcpyAsync(mu_bar, A.ubar + n5, N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
         if (geom) download_geometry(X, A, side_w_bar, bnd_w_bar, volume_bar);
+        if (visc) {
+            copy(X, A.mu_keep, L.mu, N);
+            copy(X, A.ws_keep, L.wstress, 3 * N);
+        }
         CK(cudaStreamSynchronize(X.s));
         CK(cudaMemcpy(L.u, keep.data(), n5 * sizeof(double), cudaMemcpyHostToDevice));
         X.drop_graph();
@@ -1118,19 +1663,27 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
         flite_ctx &X = *ctx;
         SteadyAdjoint &A = buffers(X);
         LevelView &L = X.V(0);
-        const size_t n5 = 5 * (size_t)L.N, N = L.N;
-        // linearisation point: the context's level-1 state
+        const size_t n5 = 5 * (size_t)L.N, N = L.N, na = (size_t)A.nc * N;
+        const bool visc = X.P.viscous;
+        // linearisation point: the context's level-1 state and, in a laminar
+        // run, the viscosity its next time step reads
         copy(X, L.u, A.u0, n5);
-        zero(X, A.Ju, n5);
+        if (visc) {
+            copy(X, L.mu, A.mu0, N);
+            copy(X, L.mu, A.mu_keep, N);
+            copy(X, L.wstress, A.ws_keep, 3 * N);
+        }
+        zero(X, A.Ju, na);
         zero(X, A.Abar, N);
         zero(X, A.Vbar, N);
         zero(X, A.nbar, 3 * N);
-        objective_terms(X, A, objective, A.u0);
         record(X, A);
+        objective_terms(X, A, objective, A.u0, visc ? A.tau : nullptr);
+        if (visc) objective_stress_u(X, A);
         // lam_0 = P Ju
-        zero(X, A.lam, n5);
-        zero(X, A.ubar, n5);
-        k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.ubar, A.Ju, A.lam, A.part);
+        zero(X, A.lam, na);
+        zero(X, A.ubar, na);
+        k_adj_update<<<kAdjBlocks, 256, 0, X.s>>>(X.P, L, A.nc, A.ubar, A.Ju, A.lam, A.part);
         k_adj_norms<<<1, 32, 0, X.s>>>(A.part, kAdjBlocks, A.out + 2);
         double h[4];
         CK(cudaMemcpyAsync(h, A.out, 4 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
@@ -1144,8 +1697,15 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
             rc = X.adj_method == 1 ? gmres_solve(X, A, ref, tol, max_iter, X.adj_restart, &it, &res)
                                    : fixed_point_solve(X, A, ref, tol, max_iter, &it, &res);
         }
-        if (rc != FLITE_OK) {
+        auto restore = [&]() {
             copy(X, A.u0, L.u, n5);
+            if (visc) {
+                copy(X, A.mu_keep, L.mu, N);
+                copy(X, A.ws_keep, L.wstress, 3 * N);
+            }
+        };
+        if (rc != FLITE_OK) {
+            restore();
             cudaStreamSynchronize(X.s);
             ctx->err = "the adjoint iteration diverged";
             return rc;
@@ -1153,12 +1713,11 @@ extern "C" int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, in
         if (iterations) *iterations = it;
         if (residual) *residual = res;
         // dJ/dg = J_g + lam^T G_g (the objective's own A and n adjoints are
-        // already in Abar and nbar)
-        geometry_sweep(X, A, A.lam);
+        // already in Abar and nbar; its wall-stress seeds join the sweep)
+        geometry_sweep(X, A, A.lam, visc ? A.tJ : nullptr);
         download_geometry(X, A, side_w_bar, bnd_w_bar, volume_bar);
-        CK(cudaStreamSynchronize(X.s));
         // the record left the iterate in u: put the solution back
-        copy(X, A.u0, L.u, n5);
+        restore();
         CK(cudaStreamSynchronize(X.s));
         X.drop_graph();
         return FLITE_OK;
@@ -1182,7 +1741,23 @@ extern "C" int flite_objective(flite_ctx *ctx, int objective, double *J) {
         zero(X, A.Ju, n5);
         zero(X, A.Abar, N);
         zero(X, A.nbar, 3 * N);
-        objective_terms(X, A, objective, L.u);
+        zero(X, A.out, 1);
+        const double *tau = nullptr;
+        if (X.P.viscous) {
+            // the tensor of makeViscosityTerm at the state (its viscosity and
+            // wall stress, which the next iteration and flite_forces read,
+            // are put back)
+            copy(X, L.mu, A.mu_keep, N);
+            copy(X, L.wstress, A.ws_keep, 3 * N);
+            X.pressure(0);
+            k_visc_prim<<<X.nblk(N), X.nb, 0, X.s>>>(X.P, L);
+            X.visc_grad(0);
+            copy(X, L.tau, A.tau, 9 * N);
+            copy(X, A.mu_keep, L.mu, N);
+            copy(X, A.ws_keep, L.wstress, 3 * N);
+            tau = A.tau;
+        }
+        objective_terms(X, A, objective, L.u, tau);
         CK(cudaMemcpyAsync(J, A.out, sizeof(double), cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
         return FLITE_OK;

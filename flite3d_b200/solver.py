@@ -196,39 +196,56 @@ class Solver:
         self._ck(self.be.objective(self._h, self.OBJECTIVES[name], ctypes.byref(J)), "objective")
         return J.value
 
-    def iteration_vjp(self, u, lam, geometry=False):
+    def iteration_vjp(self, u, lam, geometry=False, mu=None, lam_mu=None):
         """(dG/du)^T lam of one level-1 smoother iteration G at the state u;
-        with geometry=True also (dG/dg)^T lam for g = side_w, bnd_w, volume."""
+        with geometry=True also (dG/dg)^T lam for g = side_w, bnd_w, volume.
+        In a laminar run mu is the viscosity the time step reads, lam_mu the
+        adjoint of the viscosity the iteration computes, and the result ends
+        with mu_bar."""
         u = np.ascontiguousarray(u, dtype=np.float64)
         lam = np.ascontiguousarray(lam, dtype=np.float64)
         ub = np.zeros_like(u)
         d = self.mesh.level(1)
         g = [np.zeros((3, d.n_sides)), np.zeros((3, d.n_bsides)), np.zeros(d.n_nodes)] if geometry else None
         gp = [_ptr(a) for a in g] if geometry else [None, None, None]
-        self._ck(self.be.iteration_vjp(self._h, _ptr(u), _ptr(lam), _ptr(ub), *gp), "iteration_vjp")
-        return (ub, *g) if geometry else ub
+        m = None if mu is None else np.ascontiguousarray(mu, dtype=np.float64)
+        lm = None if lam_mu is None else np.ascontiguousarray(lam_mu, dtype=np.float64)
+        mb = None if mu is None else np.zeros(d.n_nodes)
+        self._ck(self.be.iteration_vjp(self._h, _ptr(u), _ptr(lam), _ptr(ub), *gp,
+                                       *[None if a is None else _ptr(a) for a in (m, lm, mb)]), "iteration_vjp")
+        out = (ub, *g) if geometry else (ub,)
+        if mu is not None:
+            out = out + (mb,)
+        return out if len(out) > 1 else out[0]
 
-    def iteration_jvp(self, u, du, side_w=None, bnd_w=None, volume=None):
+    def iteration_jvp(self, u, du, side_w=None, bnd_w=None, volume=None, mu=None, dmu=None):
         """(G(u), dG) with dG = G_u du + G_g dg along the geometry direction
-        dg = (side_w, bnd_w, volume) (None: zero) -- the oracle's tangent."""
+        dg = (side_w, bnd_w, volume) (None: zero) -- the oracle's tangent.  In
+        a laminar run mu is the viscosity the time step reads and the result
+        is (G, dG, mu', dmu') with mu' the viscosity of u."""
         u = np.ascontiguousarray(u, dtype=np.float64)
         du = np.ascontiguousarray(du, dtype=np.float64)
         g = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (side_w, bnd_w, volume)]
         v, dv = np.zeros_like(u), np.zeros_like(u)
+        m = None if mu is None else np.ascontiguousarray(mu, dtype=np.float64)
+        dm = None if dmu is None else np.ascontiguousarray(dmu, dtype=np.float64)
+        mo = np.zeros(u.shape[1]) if mu is not None else None
+        dmo = np.zeros(u.shape[1]) if mu is not None else None
         self._ck(self.be.iteration_jvp(self._h, _ptr(u), _ptr(du), *[None if a is None else _ptr(a) for a in g],
-                                       _ptr(v), _ptr(dv)), "iteration_jvp")
-        return v, dv
+                                       _ptr(v), _ptr(dv), *[None if a is None else _ptr(a) for a in (m, dm, mo, dmo)]),
+                 "iteration_jvp")
+        return (v, dv) if mu is None else (v, dv, mo, dmo)
 
-    def objective_jvp(self, name, u, du, bnd_w=None):
-        """(J, dJ) of the lift or drag coefficient along (du, d bnd_w) -- the
-        oracle's tangent."""
+    def objective_jvp(self, name, u, du, side_w=None, bnd_w=None, volume=None):
+        """(J, dJ) of the lift or drag coefficient along (du, d side_w,
+        d bnd_w, d volume) -- the oracle's tangent."""
         u = np.ascontiguousarray(u, dtype=np.float64)
         du = np.ascontiguousarray(du, dtype=np.float64)
-        b = None if bnd_w is None else np.ascontiguousarray(bnd_w, dtype=np.float64)
+        g = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (side_w, bnd_w, volume)]
         J, dJ = ctypes.c_double(), ctypes.c_double()
         self._ck(self.be.objective_jvp(self._h, self.OBJECTIVES[name], _ptr(u), _ptr(du),
-                                       None if b is None else _ptr(b), ctypes.byref(J), ctypes.byref(dJ)),
-                 "objective_jvp")
+                                       *[None if a is None else _ptr(a) for a in g], ctypes.byref(J),
+                                       ctypes.byref(dJ)), "objective_jvp")
         return J.value, dJ.value
 
     ADJOINT_METHODS = {"fixed-point": 0, "gmres": 1}

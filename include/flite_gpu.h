@@ -188,20 +188,27 @@ int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, const double 
 int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double *fwd_ms, double *vjp_ms);
 
 /* ---- steady adjoint: force sensitivities to the level-1 geometry ---------
- * For the central flux with scalar JST dissipation, inviscid, FP64 (other
- * controls: FLITE_EUNSUPPORTED).  G is one smoother iteration of level 1
- * (doTimeIterations with calcDiss, def_par:966-1181: time steps, dissipation,
- * three RK stages with their boundary conditions); the geometry g is the
- * level-1 side_w [3][E], bnd_w [3][B] and volume [N] of the level descriptor
+ * For the central flux with scalar JST dissipation, inviscid or laminar
+ * (no turbulence model), FP64 (other controls: FLITE_EUNSUPPORTED).  G is
+ * one smoother iteration of level 1 (doTimeIterations with calcDiss,
+ * def_par:966-1181: time steps, dissipation, the viscous term, three RK
+ * stages with their boundary conditions); in a laminar run its state is the
+ * conserved variables and the laminar viscosity [N] that the time step reads
+ * (makeTimeSteps runs before makeViscosityTerm recomputes it).  The
+ * geometry g is the level-1 side_w [3][E], bnd_w [3][B] and volume [N] of
+ * the level descriptor
  * (the node normals and wall areas follow from bnd_w as in
  * makeBoundaryNormals def_par:15394 and makeSurfaceArea :15523).
  * flite_iteration_vjp: ubar = (dG/du)^T lam at the state u [5][N] and, for
- * the geometry pointers that are not NULL, (dG/dg)^T lam.
+ * the geometry pointers that are not NULL, (dG/dg)^T lam; laminar runs pass
+ * the viscosity mu [N] the step reads and the adjoint lam_mu [N] of the
+ * viscosity the iteration computes (NULL: zero), and get mu_bar [N].
  * flite_adjoint_solve: at the context's level-1 state, which must be a
  * converged solution u* = G(u*), the objective J (FLITE_OBJ_CL or
- * FLITE_OBJ_CD of calculateLiftAndDrag def_par:14710-14870 with the pressure
- * of the state) and dJ/dg = J_g + lam^T (dG/dg), where lam = P((dG/du)^T lam
- * + (dJ/du)^T) is solved to the relative residual tol or max_iter products
+ * FLITE_OBJ_CD of calculateLiftAndDrag def_par:14710-14870 with the
+ * pressure and, in laminar runs, the wall stress of the state) and dJ/dg =
+ * J_g + lam^T (dG/dg), where lam = P((dG/du)^T lam + (dJ/du)^T) is solved
+ * to the relative residual tol or max_iter products
  * with (dG/du)^T (P keeps the energy of subsonic inflow nodes, which the
  * boundary condition never updates, out of the adjoint).  Sensitivities to
  * node coordinates follow with fp_geometry_vjp of the preprocessor, which
@@ -219,7 +226,8 @@ int flite_set_adjoint_method(flite_ctx *ctx, int method, int restart);
 /* the objective J of flite_adjoint_solve at the context's level-1 state    */
 int flite_objective(flite_ctx *ctx, int objective, double *J);
 int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double *lam, double *ubar,
-                        double *side_w_bar, double *bnd_w_bar, double *volume_bar);
+                        double *side_w_bar, double *bnd_w_bar, double *volume_bar,
+                        const double *mu, const double *lam_mu, double *mu_bar);
 int flite_adjoint_solve(flite_ctx *ctx, int objective, double tol, int max_iter, double *J,
                         double *side_w_bar, double *bnd_w_bar, double *volume_bar, int *iterations,
                         double *residual);

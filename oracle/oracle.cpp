@@ -1767,9 +1767,14 @@ struct TanIteration {
         for (int k = 0; k < 3; ++k) x[1 + k][ip] = x[1 + k][ip] - Dl(scale) * nv * n[k];
     }
     // makeTimeSteps, inviscid (def_par:13335-13610)
-    void timesteps(const std::vector<Dl> *u, const std::vector<Dl> &p, std::vector<Dl> &dt) const {
+    void timesteps(const std::vector<Dl> *u, const std::vector<Dl> &p, const std::vector<Dl> *mu,
+                   std::vector<Dl> &dt) const {
         const double c1 = c.gamma;
         dt.assign(N, Dl());
+        std::vector<Dl> h1(N, Dl());
+        const bool visc = c.ReynoldsNumber > 0.0;
+        const double am = visc ? 1.0 / c.ReynoldsNumber : 0.0;
+        auto vis = [&](int i) { return am < (*mu)[i].v ? (*mu)[i] : Dl(am); };  // std::max(am, mu)
         for (int e = 0; e < E; ++e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             Dl al = (wx[e] * wx[e] + wy[e] * wy[e]) + wz[e] * wz[e];
@@ -1781,6 +1786,11 @@ struct TanIteration {
             const Dl m1[3] = {u[1][i1], u[2][i1], u[3][i1]}, m2[3] = {u[1][i2], u[2][i2], u[3][i2]};
             dt[i1] = (dt[i1] + kink_abs(vn1, wm1, al, m1)) + dsqrt(cc1 * al);
             dt[i2] = (dt[i2] + kink_abs(vn2, wm2, al, m2)) + dsqrt(cc2 * al);
+            if (visc) {
+                Dl dv1 = Dl(2.0) * vis(i1) * al / u[0][i1], dv2 = Dl(2.0) * vis(i2) * al / u[0][i2];
+                h1[i1] = h1[i1] + dv2;
+                h1[i2] = h1[i2] + dv1;
+            }
         }
         for (int b = 0; b < B; ++b) {
             int i1 = g.b1[b], i2 = g.b2[b];
@@ -1797,8 +1807,150 @@ struct TanIteration {
             Dl ccm = cc1 + cc2;
             dt[i1] = (((dt[i1] + vn1) + vnm) + cc1) + ccm;
             dt[i2] = (((dt[i2] + vn2) + vnm) + cc2) + ccm;
+            if (visc) {
+                Dl dv1 = Dl(2.0) * vis(i1) * al / u[0][i1], dv2 = Dl(2.0) * vis(i2) * al / u[0][i2];
+                Dl dvm = dv1 + dv2;
+                h1[i1] = (h1[i1] + dv1) + dvm;
+                h1[i2] = (h1[i2] + dv2) + dvm;
+            }
         }
-        for (int i = 0; i < N; ++i) dt[i] = Dl(0.5) / (dt[i] / V[i] + Dl(0.0) / (V[i] * V[i]));
+        for (int i = 0; i < N; ++i) dt[i] = Dl(0.5) / (dt[i] / V[i] + h1[i] / (V[i] * V[i]));
+    }
+    // makeViscosityTerm, wide stencil (def_par:5198-5893), laminar: subtracts the
+    // viscous fluxes from diss, returns the laminar viscosity mu of each node and,
+    // on level 1, the wall stress of the boundary nodes (ws [3][N], may be null)
+    void viscous(const std::vector<Dl> *u, const std::vector<Dl> &p, std::vector<Dl> *diss, std::vector<Dl> &mu,
+                 std::vector<Dl> *ws) const {
+        const double gOg = c.gamma / (c.gamma - 1.0);
+        const double tempConv = (c.gamma - 1.0) * c.MachNumber * c.MachNumber;
+        const double Tin = c.inflowTemperature;
+        std::vector<Dl> q[4], G[12], t[9], f[4];
+        for (auto &v : q) v.resize(N);
+        for (auto &v : G) v.assign(N, Dl());
+        for (auto &v : t) v.assign(N, Dl());
+        for (auto &v : f) v.assign(N, Dl());
+        for (int i = 0; i < N; ++i) {
+            Dl r = u[0][i];
+            q[0][i] = u[1][i] / r; q[1][i] = u[2][i] / r; q[2][i] = u[3][i] / r;
+            q[3][i] = Dl(gOg) * p[i] / r;
+        }
+        for (int e = 0; e < E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            const Dl w[3] = {wx[e], wy[e], wz[e]};
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    Dl d = (q[k][i1] + q[k][i2]) * w[a];
+                    G[a * 4 + k][i1] = G[a * 4 + k][i1] + d;
+                    G[a * 4 + k][i2] = G[a * 4 + k][i2] - d;
+                }
+        }
+        for (int b = 0; b < B; ++b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            const Dl w[3] = {bwx[b], bwy[b], bwz[b]};
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    Dl sm = q[k][i1] + q[k][i2];
+                    G[a * 4 + k][i1] = G[a * 4 + k][i1] + (Dl(2.) * q[k][i1] + sm) * w[a];
+                }
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    Dl sm = q[k][i1] + q[k][i2];
+                    G[a * 4 + k][i2] = G[a * 4 + k][i2] + (Dl(2.) * q[k][i2] + sm) * w[a];
+                }
+        }
+        const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+        const double oRe = 1. / c.ReynoldsNumber, oPr = 1. / c.PrandtlNumber;
+        mu.assign(N, Dl());
+        for (int i = 0; i < N; ++i) {
+            Dl vt = Dl(1.) / V[i];
+            Dl dudx = G[0][i] * vt, dvdx = G[1][i] * vt, dwdx = G[2][i] * vt, dTdx = G[3][i] * vt;
+            Dl dudy = G[4][i] * vt, dvdy = G[5][i] * vt, dwdy = G[6][i] * vt, dTdy = G[7][i] * vt;
+            Dl dudz = G[8][i] * vt, dvdz = G[9][i] * vt, dwdz = G[10][i] * vt, dTdz = G[11][i] * vt;
+            Dl T = Dl(gOg) * p[i] / u[0][i];
+            if (T.v <= 0.001) T = Dl(0.001);
+            Dl a = Dl(tempConv) * T;
+            Dl m = Dl(oRe) * ((a * dsqrt(a)) * (Dl(Tin + 198.6) / (Dl(tempConv * Tin) * T + Dl(198.6))));
+            Dl k = Dl(oPr) * m;
+            mu[i] = m;
+            t[0][i] = m * (Dl(fourThirds) * dudx - Dl(twoThirds) * (dvdy + dwdz));
+            t[1][i] = m * (dudy + dvdx);
+            t[2][i] = m * (dudz + dwdx);
+            t[3][i] = m * (Dl(fourThirds) * dvdy - Dl(twoThirds) * (dudx + dwdz));
+            t[4][i] = m * (dvdz + dwdy);
+            t[5][i] = m * (Dl(fourThirds) * dwdz - Dl(twoThirds) * (dudx + dvdy));
+            t[6][i] = k * dTdx;
+            t[7][i] = k * dTdy;
+            t[8][i] = k * dTdz;
+        }
+        if (g.grid == 1) {
+            for_range(-20, -19, [&](int ip) {
+                Dl n[3] = {nx[ip], ny[ip], nz[ip]};
+                Dl dT[3] = {t[6][ip], t[7][ip], t[8][ip]};
+                Dl nt = (dT[0] * n[0] + dT[1] * n[1]) + dT[2] * n[2];
+                for (int kk = 0; kk < 3; ++kk) t[6 + kk][ip] = dT[kk] - nt * n[kk];
+            });
+            if (ws)
+                for (int ib = 0; ib < std::min(g.Nb, g.nnorm); ++ib) {
+                    int ip = g.node_ind[ib];
+                    Dl n[3] = {nx[ip], ny[ip], nz[ip]};
+                    ws[0][ip] = (t[0][ip] * n[0] + t[1][ip] * n[1]) + t[2][ip] * n[2];
+                    ws[1][ip] = (t[1][ip] * n[0] + t[3][ip] * n[1]) + t[4][ip] * n[2];
+                    ws[2][ip] = (t[2][ip] * n[0] + t[4][ip] * n[1]) + t[5][ip] * n[2];
+                }
+        }
+        auto loadt = [&](int i, Dl *tt, Dl *uu) {
+            for (int kk = 0; kk < 9; ++kk) tt[kk] = t[kk][i];
+            uu[0] = u[1][i] / u[0][i]; uu[1] = u[2][i] / u[0][i]; uu[2] = u[3][i] / u[0][i];
+        };
+        for (int e = 0; e < E; ++e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            Dl wx_ = wx[e], wy_ = wy[e], wz_ = wz[e];
+            Dl a[9], b[9], ua[3], ub[3];
+            loadt(i1, a, ua); loadt(i2, b, ub);
+            Dl dt[9];
+            for (int kk = 0; kk < 9; ++kk) dt[kk] = a[kk] + b[kk];
+            Dl dut1 = ((((ua[0] * a[0] + ub[0] * b[0]) + ua[1] * a[1]) + ub[1] * b[1]) + ua[2] * a[2]) + ub[2] * b[2];
+            Dl dut2 = ((((ua[0] * a[1] + ub[0] * b[1]) + ua[1] * a[3]) + ub[1] * b[3]) + ua[2] * a[4]) + ub[2] * b[4];
+            Dl dut3 = ((((ua[0] * a[2] + ub[0] * b[2]) + ua[1] * a[4]) + ub[1] * b[4]) + ua[2] * a[5]) + ub[2] * b[5];
+            Dl ff[4] = {(wx_ * dt[0] + wy_ * dt[1]) + wz_ * dt[2], (wx_ * dt[1] + wy_ * dt[3]) + wz_ * dt[4],
+                        (wx_ * dt[2] + wy_ * dt[4]) + wz_ * dt[5],
+                        (wx_ * (dt[6] + dut1) + wy_ * (dt[7] + dut2)) + wz_ * (dt[8] + dut3)};
+            for (int kk = 0; kk < 4; ++kk) {
+                f[kk][i1] = f[kk][i1] + ff[kk];
+                f[kk][i2] = f[kk][i2] - ff[kk];
+            }
+        }
+        for (int bb = 0; bb < B; ++bb) {
+            int ind = g.bind[bb];
+            if (ind == 2 || ind == 9) continue;
+            int i1 = g.b1[bb], i2 = g.b2[bb];
+            Dl wx_ = bwx[bb], wy_ = bwy[bb], wz_ = bwz[bb];
+            Dl a[9], b[9], ua[3], ub[3];
+            loadt(i1, a, ua); loadt(i2, b, ub);
+            Dl dt[9];
+            for (int kk = 0; kk < 9; ++kk) dt[kk] = a[kk] + b[kk];
+            Dl d11 = (ua[0] * a[0] + ua[1] * a[1]) + ua[2] * a[2];
+            Dl d12 = (ub[0] * b[0] + ub[1] * b[1]) + ub[2] * b[2];
+            Dl d21 = (ua[0] * a[1] + ua[1] * a[3]) + ua[2] * a[4];
+            Dl d22 = (ub[0] * b[1] + ub[1] * b[3]) + ub[2] * b[4];
+            Dl d31 = (ua[0] * a[2] + ua[1] * a[4]) + ua[2] * a[5];
+            Dl d32 = (ub[0] * b[2] + ub[1] * b[4]) + ub[2] * b[5];
+            Dl dut1 = d11 + d12, dut2 = d21 + d22, dut3 = d31 + d32;
+            Dl f2 = (wx_ * dt[0] + wy_ * dt[1]) + wz_ * dt[2];
+            Dl f3 = (wx_ * dt[1] + wy_ * dt[3]) + wz_ * dt[4];
+            Dl f4 = (wx_ * dt[2] + wy_ * dt[4]) + wz_ * dt[5];
+            Dl f5 = (wx_ * (dt[6] + dut1) + wy_ * (dt[7] + dut2)) + wz_ * (dt[8] + dut3);
+            f[0][i1] = (f[0][i1] + f2) + Dl(2.0) * ((wx_ * a[0] + wy_ * a[1]) + wz_ * a[2]);
+            f[1][i1] = (f[1][i1] + f3) + Dl(2.0) * ((wx_ * a[1] + wy_ * a[3]) + wz_ * a[4]);
+            f[2][i1] = (f[2][i1] + f4) + Dl(2.0) * ((wx_ * a[2] + wy_ * a[4]) + wz_ * a[5]);
+            f[3][i1] = (f[3][i1] + f5) + Dl(2.0) * ((wx_ * (a[6] + d11) + wy_ * (a[7] + d21)) + wz_ * (a[8] + d31));
+            f[0][i2] = (f[0][i2] + f2) + Dl(2.0) * ((wx_ * b[0] + wy_ * b[1]) + wz_ * b[2]);
+            f[1][i2] = (f[1][i2] + f3) + Dl(2.0) * ((wx_ * b[1] + wy_ * b[3]) + wz_ * b[4]);
+            f[2][i2] = (f[2][i2] + f4) + Dl(2.0) * ((wx_ * b[2] + wy_ * b[4]) + wz_ * b[5]);
+            f[3][i2] = (f[3][i2] + f5) + Dl(2.0) * ((wx_ * (b[6] + d12) + wy_ * (b[7] + d22)) + wz_ * (b[8] + d32));
+        }
+        for (int i = 0; i < N; ++i)
+            for (int kk = 0; kk < 4; ++kk) diss[1 + kk][i] = diss[1 + kk][i] - f[kk][i];
     }
     // makeArtificialDissipation2 on level 1, unweighted (def_par:11484-11993)
     void jst(const std::vector<Dl> *u, const std::vector<Dl> &p, const std::vector<Dl> &dt,
@@ -1912,12 +2064,20 @@ struct TanIteration {
         }
     }
     // one doTimeIterations step on level 1: u <- G(u)
-    void iterate(std::vector<Dl> *u) const {
+    // mu: the laminar viscosity the time step reads (viscous runs), replaced
+    // by the one makeViscosityTerm computes from u
+    void iterate(std::vector<Dl> *u, std::vector<Dl> *mu) const {
         std::vector<Dl> up[5], p(N), dt, diss[5], r[5];
         for (int k = 0; k < 5; ++k) up[k] = u[k];
         for (int i = 0; i < N; ++i) p[i] = dabs(pressure(u, i));
-        timesteps(u, p, dt);
+        const bool visc = c.ReynoldsNumber > 0.0;
+        timesteps(u, p, mu, dt);
         jst(u, p, dt, diss);
+        if (visc) {
+            std::vector<Dl> mu_new;
+            viscous(u, p, diss, mu_new, nullptr);
+            *mu = mu_new;
+        }
         const double relax = o.relaxation_param(g);
         for (int st = 1; st <= 3; ++st) {
             for (int i = 0; i < N; ++i) p[i] = pressure(u, i);
@@ -1926,7 +2086,13 @@ struct TanIteration {
                 for (int i = 0; i < N; ++i) r[k][i] = r[k][i] + diss[k][i];
             for (int i = 0; i < N; ++i)
                 for (int k = 0; k < 5; ++k) r[k][i] = dt[i] * r[k][i] / V[i];
-            for_range(-20, -19, [&](int ip) { remove_normal(r, ip, 1.0); });
+            if (visc)
+                for_range(-20, -19, [&](int ip) {
+                    r[1][ip] = Dl(); r[2][ip] = Dl(); r[3][ip] = Dl();
+                    if (!c.wallsAreIsentropic) r[4][ip] = Dl();
+                });
+            else
+                for_range(-20, -19, [&](int ip) { remove_normal(r, ip, 1.0); });
             for_range(-4, -3, [&](int ip) { remove_normal(r, ip, 1.0); });
             for_range(-18, -17, [&](int ip) { remove_normal(r, ip, 1.0); });
             const double dtJ = c.CFLNumber * o.RK[st - 1];
@@ -1943,7 +2109,14 @@ struct TanIteration {
                 for (int k = 1; k < 5; ++k) u[k][i] = up[k][i] - r[k][i];
                 if (u[0][i].v < c.minimumDensity) u[0][i] = Dl(c.minimumDensity);
             }
-            for_range(-20, -19, [&](int ip) { remove_normal(u, ip, 1.0); });
+            if (visc)
+                for_range(-20, -19, [&](int ip) {
+                    const double cm[3] = {g.cmx[ip], g.cmy[ip], g.cmz[ip]};
+                    for (int k = 0; k < 3; ++k) u[1 + k][ip] = u[0][ip] * Dl(cm[k]) / Dl(c.physicalTimeStep);
+                    if (!c.wallsAreIsentropic) u[4][ip] = u[0][ip] * Dl(c.inflowTemperature) / Dl(c.gamma);
+                });
+            else
+                for_range(-20, -19, [&](int ip) { remove_normal(u, ip, 1.0); });
             for_range(-4, -3, [&](int ip) {
                 remove_normal(u, ip, relax);
                 if (!c.wallsAreIsentropic) {
@@ -1981,12 +2154,25 @@ struct TanIteration {
         double fn1[3] = {-ft[2], 0.0, ft[0]};
         const double *dir = which == 0 ? fn1 : ft;
         const double pinf = 1. / (c.gamma * c.MachNumber * c.MachNumber);
+        const bool visc = c.ReynoldsNumber > 0.0;
+        std::vector<Dl> ws[3];
+        if (visc) {  // the wall stress of makeViscosityTerm at the state u
+            std::vector<Dl> p(N), mu, d[5];
+            for (int i = 0; i < N; ++i) p[i] = dabs(pressure(u, i));
+            for (auto &x : d) x.assign(N, Dl());
+            for (auto &x : ws) x.assign(N, Dl());
+            viscous(u, p, d, mu, ws);
+        }
         Dl acc;
         for_range(-20, -19, [&](int ip) {
             if (!(g.cz[ip] > (c.groundplane + 0.01))) return;
             Dl dn = (nx[ip] * dir[0] + ny[ip] * dir[1]) + nz[ip] * dir[2];
             Dl dp = pressure(u, ip) - Dl(pinf);
             acc = acc - area[ip] * dp * dn;
+            if (visc) {
+                Dl sd = (ws[0][ip] * dir[0] + ws[1][ip] * dir[1]) + ws[2][ip] * dir[2];
+                acc = acc + area[ip] * sd;
+            }
         });
         return Dl(2.0) * acc / Dl(c.referenceArea);
     }
@@ -2318,32 +2504,38 @@ int oracle_residual_jvp(oracle_ctx *o, int level, const double *u, const double 
 // (dsw [3][E], dbw [3][B], dvol [N]); any of the geometry directions may be
 // NULL (zero)
 int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const double *dsw, const double *dbw,
-                         const double *dvol, double *v, double *dv) {
+                         const double *dvol, double *v, double *dv, const double *mu, const double *dmu,
+                         double *mu_out, double *dmu_out) {
     if (!o || !u || !du || !v || !dv) return FLITE_EINVAL;
     const flite_controls &c = o->o.c;
-    if (c.fluxType != 1 || c.ReynoldsNumber > 0 || c.turbulenceModel != 0 || c.dissipationScheme == 3 ||
-        c.useDissipationWeighting)
+    if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 3 || c.useDissipationWeighting)
         return FLITE_EUNSUPPORTED;
+    const bool visc = c.ReynoldsNumber > 0;
+    if (visc && (!mu || !mu_out || !dmu_out)) return FLITE_EINVAL;
     TanIteration T(o->o, dsw, dbw, dvol);
     const size_t N = T.N;
-    std::vector<Dl> x[5];
+    std::vector<Dl> x[5], m(N);
     for (int k = 0; k < 5; ++k) {
         x[k].resize(N);
         for (size_t i = 0; i < N; ++i) x[k][i] = Dl(u[k * N + i], du[k * N + i]);
     }
-    T.iterate(x);
+    if (visc)
+        for (size_t i = 0; i < N; ++i) m[i] = Dl(mu[i], dmu ? dmu[i] : 0.0);
+    T.iterate(x, &m);
     for (int k = 0; k < 5; ++k)
         for (size_t i = 0; i < N; ++i) { v[k * N + i] = x[k][i].v; dv[k * N + i] = x[k][i].d; }
+    if (visc)
+        for (size_t i = 0; i < N; ++i) { mu_out[i] = m[i].v; dmu_out[i] = m[i].d; }
     return FLITE_OK;
 }
 
 // lift (which 0) or drag (which 1) coefficient of the level-1 state u with
-// its tangent along (du, dbw); dbw may be NULL
-int oracle_objective_jvp(oracle_ctx *o, int which, const double *u, const double *du, const double *dbw, double *J,
-                         double *dJ) {
+// its tangent along (du, dsw, dbw, dvol); the geometry directions may be NULL
+int oracle_objective_jvp(oracle_ctx *o, int which, const double *u, const double *du, const double *dsw,
+                         const double *dbw, const double *dvol, double *J, double *dJ) {
     if (!o || !u || !du || !J || !dJ || which < 0 || which > 1) return FLITE_EINVAL;
-    if (o->o.c.ReynoldsNumber > 0) return FLITE_EUNSUPPORTED;
-    TanIteration T(o->o, nullptr, dbw, nullptr);
+    if (o->o.c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
+    TanIteration T(o->o, dsw, dbw, dvol);
     const size_t N = T.N;
     std::vector<Dl> x[5];
     for (int k = 0; k < 5; ++k) {

@@ -48,13 +48,17 @@ int oracle_set_threads(int n);
 /* tangent (forward-mode) of the residual: jv = (dR/du) du               */
 int oracle_residual_jvp(oracle_ctx *o, int level, const double *u, const double *du, double *jv);
 /* tangent of one smoother iteration on level 1 (central flux, scalar JST,
- * inviscid): v = G(u), dv = G_u du + G_g dg with dg = (dsw [3][E], dbw [3][B],
- * dvol [N]) a direction in the level-1 geometry (NULL = zero)            */
+ * inviscid or laminar): v = G(u, mu), dv = G_u du + G_mu dmu + G_g dg with
+ * dg = (dsw [3][E], dbw [3][B], dvol [N]) a direction in the level-1
+ * geometry (NULL = zero); in a laminar run mu [N] is the viscosity the time
+ * step reads, and mu_out = the viscosity of u with its tangent dmu_out      */
 int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const double *dsw,
-                         const double *dbw, const double *dvol, double *v, double *dv);
-/* lift (which 0) or drag (1) coefficient of u and its tangent along (du, dbw) */
+                         const double *dbw, const double *dvol, double *v, double *dv,
+                         const double *mu, const double *dmu, double *mu_out, double *dmu_out);
+/* lift (which 0) or drag (1) coefficient of u (pressure and, in laminar
+ * runs, wall stress) and its tangent along (du, dsw, dbw, dvol)            */
 int oracle_objective_jvp(oracle_ctx *o, int which, const double *u, const double *du,
-                         const double *dbw, double *J, double *dJ);
+                         const double *dsw, const double *dbw, const double *dvol, double *J, double *dJ);
 #ifdef __cplusplus
 }
 #endif

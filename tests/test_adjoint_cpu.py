@@ -73,7 +73,7 @@ def test_objective_tangent(mesh, name):
     du = rng.standard_normal(u.shape)
     bw = mesh.array(1, "bnd_w")
     dbw = rng.standard_normal(bw.shape) * 1e-2
-    J, dJ = o.objective_jvp(name, u, du, dbw)
+    J, dJ = o.objective_jvp(name, u, du, bnd_w=dbw)
     h = 1e-6
 
     def Jt(t):
@@ -116,3 +116,65 @@ def test_geometry_needs_elements(tmp_path):
     r = Mesh.read_sol(tmp_path / "m.sol")
     with pytest.raises(RuntimeError):
         r.geometry()
+
+
+LAMINAR = dict(ReynoldsNumber=500.0, CFLNumber=1.0)
+
+
+@pytest.mark.parametrize("ctl", [dict(wallsAreIsentropic=1), dict(wallsAreIsentropic=0)])
+def test_laminar_iteration_tangent(mesh, ctl):
+    """The state of a laminar iteration is (u, mu): mu the viscosity the
+    time step reads; the iteration also returns the viscosity of u."""
+    c, o = oracle_on(mesh, **LAMINAR, **ctl)
+    u = generic_state(c, mesh)
+    n = u.shape[1]
+    mu_u = o.iteration_jvp(u, np.zeros_like(u), mu=np.zeros(n), dmu=np.zeros(n))[2]
+    # the value part is the oracle's own iteration with that viscosity read
+    s = Solver(c, mesh, backend=oracle_backend())
+    s.set_state(u)
+    s.start()  # the wall condition on u and the viscosity 1/Re of the initial field
+    us = s.get_state(1)
+    v1, _, mu1, _ = o.iteration_jvp(us, np.zeros_like(u), mu=np.full(n, 1.0 / c.ReynoldsNumber), dmu=np.zeros(n))
+    s.do_time_iterations(1, 1, True, 1)
+    assert np.array_equal(v1, s.get_state(1))
+    # the viscosity the iteration returns is that of its input state alone
+    assert np.array_equal(o.iteration_jvp(us, np.zeros_like(u), mu=np.zeros(n), dmu=np.zeros(n))[2], mu1)
+    mu = mu_u * (1 + 0.05 * np.random.default_rng(3).standard_normal(n))
+    d = mesh.level(1)
+    rng = np.random.default_rng(1)
+    du = rng.standard_normal(u.shape)
+    dmu = rng.standard_normal(n) * 1e-4
+    dg = [rng.standard_normal((3, d.n_sides)) * 1e-2, rng.standard_normal((3, d.n_bsides)) * 1e-2,
+          rng.standard_normal(n) * 1e-3]
+    _, dv, _, dmo = o.iteration_jvp(u, du, *dg, mu=mu, dmu=dmu)
+    base = [mesh.array(1, k) for k in ("side_w", "bnd_w", "volume")]
+    h = 1e-6
+
+    def G(t):
+        m = mesh.with_level1_geometry(*[b + t * x for b, x in zip(base, dg)])
+        return Solver(c, m, backend=oracle_backend()).iteration_jvp(u + t * du, np.zeros_like(u), mu=mu + t * dmu,
+                                                                     dmu=np.zeros(n))
+    a, b = G(h), G(-h)
+    assert np.abs((a[0] - b[0]) / (2 * h) - dv).max() <= 1e-8 * np.abs(dv).max()
+    assert np.abs((a[2] - b[2]) / (2 * h) - dmo).max() <= 1e-8 * np.abs(dmo).max()
+
+
+@pytest.mark.parametrize("name", ["CL", "CD"])
+def test_laminar_objective_tangent(mesh, name):
+    c, o = oracle_on(mesh, **LAMINAR)
+    u = generic_state(c, mesh)
+    d = mesh.level(1)
+    rng = np.random.default_rng(2)
+    du = rng.standard_normal(u.shape)
+    dg = [rng.standard_normal((3, d.n_sides)) * 1e-2, rng.standard_normal((3, d.n_bsides)) * 1e-2,
+          rng.standard_normal(d.n_nodes) * 1e-3]
+    J, dJ = o.objective_jvp(name, u, du, *dg)
+    base = [mesh.array(1, k) for k in ("side_w", "bnd_w", "volume")]
+    h = 1e-6
+
+    def Jt(t):
+        m = mesh.with_level1_geometry(*[b + t * x for b, x in zip(base, dg)])
+        return Solver(c, m, backend=oracle_backend()).objective_jvp(name, u + t * du, np.zeros_like(u))[0]
+
+    fd = (Jt(h) - Jt(-h)) / (2 * h)
+    assert abs(fd - dJ) <= 1e-7 * abs(dJ)

@@ -11,6 +11,8 @@
   against central differences of converged GPU solutions on moved meshes
   (step 1e-6 of the channel height, 1e-5).  The meshes have jittered
   interior nodes, so no two edges tie in the dissipation's min/max switches.
+* The same for laminar runs, whose iteration state also holds the viscosity
+  the time step reads.
 * The adjoint leaves the solution as it was, and refuses controls it does
   not cover.
 """
@@ -148,7 +150,7 @@ def test_adjoint_matches_the_cpu_tangent(small_case, name):
             du = dv
             if done:
                 break
-        _, dJ = o.objective_jvp(name, u, du, dg[1])
+        _, dJ = o.objective_jvp(name, u, du, *dg)
         adj = (xb[:, k] * nrm[:, k]).sum()
         assert abs(adj - dJ) <= 1e-7 * abs(dJ), (k, adj, dJ)
 
@@ -197,7 +199,7 @@ def test_adjoint_leaves_the_solve_unchanged():
     assert np.array_equal(a.get_state(1), b.get_state(1))
 
 
-@pytest.mark.parametrize("ctl", [dict(ReynoldsNumber=500.0), dict(fluxType=4), dict(precision=1),
+@pytest.mark.parametrize("ctl", [dict(ReynoldsNumber=5e6, turbulenceModel=1), dict(fluxType=4), dict(precision=1),
                                  dict(dissipationScheme=3)])
 def test_adjoint_refuses_what_it_does_not_cover(ctl):
     mesh = Mesh.bump_channel(6, 2, 2, 0.05, nlevels=1)
@@ -209,3 +211,106 @@ def test_adjoint_refuses_what_it_does_not_cover(ctl):
         s.adjoint_solve("CL")
     with pytest.raises(RuntimeError, match="status 2"):
         s.objective("CL")
+
+
+# ---- laminar runs: the iteration's state is (u, mu), mu the viscosity the
+# time step reads (makeTimeSteps runs before makeViscosityTerm)
+
+LAMINAR = dict(ReynoldsNumber=500.0, CFLNumber=1.0, wallsAreIsentropic=1)
+
+
+def viscosity_of(o, u):
+    """mu of the state u: the viscosity makeViscosityTerm computes (oracle)."""
+    n = u.shape[1]
+    return o.iteration_jvp(u, np.zeros_like(u), mu=np.zeros(n), dmu=np.zeros(n))[2]
+
+
+def laminar_dot_check(g, o, u, mu, seed):
+    d = g.mesh.level(1)
+    rng = np.random.default_rng(seed)
+    du = rng.standard_normal(u.shape)
+    dmu = rng.standard_normal(mu.shape) * 1e-3
+    dg = [rng.standard_normal((3, d.n_sides)) * 1e-2, rng.standard_normal((3, d.n_bsides)) * 1e-2,
+          rng.standard_normal(d.n_nodes) * 1e-3]
+    lam = rng.standard_normal(u.shape)
+    lam_mu = rng.standard_normal(mu.shape) * 1e2
+    _, dv, _, dmo = o.iteration_jvp(u, du, *dg, mu=mu, dmu=dmu)
+    ub, *gb, mub = g.iteration_vjp(u, lam, geometry=True, mu=mu, lam_mu=lam_mu)
+    lhs = (lam * dv).sum() + (lam_mu * dmo).sum()
+    terms = [(ub * du).sum(), (mub * dmu).sum()] + [(a * b).sum() for a, b in zip(gb, dg)]
+    scale = sum(abs(t) for t in terms) + abs(lhs)
+    assert abs(lhs - sum(terms)) <= 1e-11 * scale, (lhs, terms)
+
+
+@pytest.mark.parametrize("ctl", [dict(), dict(wallsAreIsentropic=0), dict(boundaryTerm=0)])
+def test_laminar_iteration_vjp_is_the_transpose_of_the_tangent(ctl):
+    mesh = Mesh.bump_channel(12, 4, 4, 0.05, nlevels=1)
+    c = controls(numberOfGridsToUse=1, **{**LAMINAR, **ctl})
+    g, o = Solver(c, mesh), Solver(c, mesh, backend=oracle_backend())
+    u = initial_state(c, mesh, perturb_seed=3, amplitude=0.02)
+    u = u + np.random.default_rng(7).standard_normal(u.shape) * 0.01
+    for s in (g, o):
+        s.set_state(u)
+        s.start()
+    # viscosities on both sides of the 1/Re floor of the time step
+    mu = viscosity_of(o, u) * (1 + 0.05 * np.random.default_rng(3).standard_normal(u.shape[1]))
+    for seed in (1, 2):
+        laminar_dot_check(g, o, u, mu, seed)
+
+
+@pytest.fixture(scope="module")
+def laminar_case():
+    j = Jittered(16, 6, 6, nlevels=2)
+    c = controls(numberOfGridsToUse=2, **LAMINAR)
+    s, res = converge(c, j.mesh, tol=1e-14, max_cycles=8000)
+    return j, c, s, res
+
+
+@pytest.mark.parametrize("name", ["CL", "CD"])
+def test_laminar_adjoint_matches_the_cpu_tangent(laminar_case, name):
+    j, c, s, res = laminar_case
+    assert res < 1e-13
+    u = s.get_state(1)
+    r = s.adjoint_solve(name, tol=1e-13, max_iter=200000)
+    assert r["residual"] <= 1e-13
+    assert np.array_equal(s.get_state(1), u)
+    assert r["J"] == s.objective(name)
+    xb = j.coords_sensitivity(r)
+    wall, nrm = j.wall_nodes_and_normals()
+    o = Solver(controls(numberOfGridsToUse=1, **LAMINAR), j.mesh, backend=oracle_backend())
+    mu = viscosity_of(o, u)
+    J0, _ = o.objective_jvp(name, u, np.zeros_like(u))
+    assert abs(J0 - r["J"]) <= 1e-12 * abs(J0)
+    for k in np.random.default_rng(21).choice(wall, 2, replace=False):
+        dX = np.zeros_like(j.X)
+        dX[:, k] = nrm[:, k]
+        h = 1e-6
+        gp, gm = j.base.geometry(j.X + h * dX), j.base.geometry(j.X - h * dX)
+        dg = [(a - b) / (2 * h) for a, b in zip(gp, gm)]
+        du, dmu = np.zeros_like(u), np.zeros_like(mu)
+        for _ in range(60000):
+            _, dv, _, dmv = o.iteration_jvp(u, du, *dg, mu=mu, dmu=dmu)
+            done = max(np.abs(dv - du).max(), np.abs(dmv - dmu).max() * 1e3) <= 1e-14 * max(1.0, np.abs(dv).max())
+            du, dmu = dv, dmv
+            if done:
+                break
+        _, dJ = o.objective_jvp(name, u, du, *dg)
+        adj = (xb[:, k] * nrm[:, k]).sum()
+        assert abs(adj - dJ) <= 1e-7 * abs(dJ), (k, adj, dJ)
+
+
+def test_laminar_adjoint_matches_central_differences(laminar_case):
+    j, c, s, res = laminar_case
+    u = s.get_state(1)
+    r = s.adjoint_solve("CD", tol=1e-12, max_iter=200000)
+    xb = j.coords_sensitivity(r)
+    wall, nrm = j.wall_nodes_and_normals()
+    h = 1e-6
+    for k in np.random.default_rng(6).choice(wall, 3, replace=False):
+        dX = np.zeros_like(j.X)
+        dX[:, k] = nrm[:, k] * h
+        Jp = converge(c, j.at(j.X + dX), u0=u, tol=1e-15, max_cycles=3000)[0].objective("CD")
+        Jm = converge(c, j.at(j.X - dX), u0=u, tol=1e-15, max_cycles=3000)[0].objective("CD")
+        fd = (Jp - Jm) / (2 * h)
+        adj = (xb[:, k] * nrm[:, k]).sum()
+        assert abs(adj - fd) <= 1e-5 * abs(fd), (k, adj, fd)
