@@ -474,8 +474,9 @@ def run_adjoint(args):
     dCD/dX along the normal displacement of wall nodes of the bump channel
     48x16x16 hex -> tets (the Euler configuration's mesh) with its interior
     nodes jittered by up to 15% of the spacing (seed 11: no two edges tie in
-    the dissipation's min/max switches), inviscid, M 0.5, central flux + JST,
-    CFL 2, 3 levels, FP64.  The primal is converged to a residual of 1e-15,
+    the dissipation's min/max switches), inviscid (or laminar with
+    --adjoint-re, adiabatic walls), M 0.5, central flux + JST, CFL 2, 3
+    levels, FP64.  The primal is converged to a residual of 1e-15,
     the adjoint to 1e-12; then central differences of converged solutions on
     moved meshes at 32 seeded wall nodes (SplitMix64 seed 4), step 1e-7 of
     the channel height.  One JSON line: the adjoint solve's seconds, beside
@@ -494,8 +495,10 @@ def run_adjoint(args):
     X = X + jit
     at = lambda Y: base.with_level1_geometry(*base.geometry(Y))
     mesh = at(X)
-    c = F.default_controls(ReynoldsNumber=0.0, fluxType=1, CFLNumber=2.0, multigridScheme=3,
-                           numberOfGridsToUse=nlev)
+    re = args.adjoint_re
+    c = F.default_controls(ReynoldsNumber=re, fluxType=1, CFLNumber=2.0, multigridScheme=3,
+                           numberOfGridsToUse=nlev, wallsAreIsentropic=1, viscosityScheme=1)
+    flow = f"laminar Re {re:g}, adiabatic walls" if re > 0 else "inviscid"
 
     def converge(m, u0=None, tol=1e-15, max_cycles=args.adjoint_primal_cycles):
         s = F.Solver(c, m)
@@ -567,7 +570,7 @@ def run_adjoint(args):
         "metric": "adjoint dCL/dX solve time", "value": out["CL"][1], "unit": "s", "n_gpus": 1,
         "steps": 1, "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (generated bump-channel mesh, jittered interior nodes, freestream start)",
-        "config": {"workload": f"steady adjoint of CL and CD, inviscid M 0.5, central flux + JST, on the bump "
+        "config": {"workload": f"steady adjoint of CL and CD, {flow}, M 0.5, central flux + JST, on the bump "
                                f"channel {nx}x{ny}x{nz} hex -> 6 tets with interior nodes jittered by 15% of the "
                                f"spacing, {nlev} agglomerated MG levels for the primal, FP64",
                    "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides},
@@ -659,6 +662,7 @@ def main():
                     help="the steady adjoint (dCL/dX, dCD/dX) workload with its finite-difference check")
     ap.add_argument("--adjoint-nodes", type=int, default=32, help="wall nodes of the finite-difference check")
     ap.add_argument("--adjoint-mesh", default="48,16,16", help="NX,NY,NZ hexes of the adjoint workload")
+    ap.add_argument("--adjoint-re", type=float, default=0.0, help="Reynolds number (0: inviscid)")
     ap.add_argument("--adjoint-primal-cycles", type=int, default=6000)
     ap.add_argument("--adjoint-max-iter", type=int, default=400000,
                     help="products with the transposed iteration Jacobian per adjoint solve")

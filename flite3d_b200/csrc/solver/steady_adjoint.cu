@@ -1530,16 +1530,34 @@ static int gmres_solve(flite_ctx &X, SteadyAdjoint &A, double bnorm, double tol,
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hv(m + 1), y(m);
     auto Hij = [&](int i, int j) -> double & { return H[(size_t)j * (m + 1) + i]; };
     int total = 0;
-    double res = 1.0;
+    double res = 1.0, prev = -1.0;
     while (true) {
         // r = b - (I - A) lam in V_0
         reverse(X, A, A.lam, false);
         k_gm_apply<<<eb, 256, 0, X.s>>>(X.P, L, A.nc, A.lam, A.ubar, A.rhs, Vj(0), 1);
         ++total;
-        const double beta = norm(Vj(0));
+        double beta = norm(Vj(0));
         if (!std::isfinite(beta)) return FLITE_ENAN;
         res = beta / bnorm;
         if (res <= tol || total >= max_iter) break;
+        if (prev > 0 && res > 0.9 * prev) {
+            // Restarted GMRES can stall where G_u^T is far from normal (its
+            // powers grow for a while before they decay): the fixed-point
+            // iteration, which converges at the smoother's rate whatever the
+            // transient, takes over for a stretch, then GMRES again
+            int fit = 0;
+            double fres = res;
+            const int rc = fixed_point_solve(X, A, bnorm, tol, std::min(max_iter - total, 20 * (m + 1)), &fit, &fres);
+            if (rc != FLITE_OK) return rc;
+            total += fit;
+            prev = -1.0;
+            if (fres <= tol || total >= max_iter) {
+                res = fres;
+                break;
+            }
+            continue;
+        }
+        prev = res;
         k_gm_scale<<<eb, 256, 0, X.s>>>(Vj(0), n, 1.0 / beta);
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
