@@ -1226,7 +1226,7 @@ void destroy_steady_adjoint(SteadyAdjoint *a) { delete a; }
 static const char *steady_adjoint_unsupported(const flite_ctx &X) {
     const flite_controls &c = X.c;
     if (c.fluxType != 1) return "the steady adjoint takes the central flux (fluxType 1)";
-    if (c.precision != FLITE_FP64) return "the steady adjoint runs in FP64";
+
     if (c.turbulenceModel != 0) return "the steady adjoint covers inviscid and laminar runs (no turbulence model)";
     if (c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";
     if (c.useDissipationWeighting) return "the steady adjoint takes unweighted dissipation";
@@ -1358,6 +1358,14 @@ static void objective_stress_u(flite_ctx &X, SteadyAdjoint &A) {
 static void record(flite_ctx &X, SteadyAdjoint &A) {
     LevelView &L = X.V(0);
     const size_t n5 = 5 * (size_t)L.N, N = L.N;
+    // a FLITE_MIXED run converges to the FP64 iteration's fixed point: its
+    // adjoint is the FP64 one, recorded with the FP64 kernels
+    struct PrecisionGuard {
+        flite_ctx &X;
+        int keep;
+        ~PrecisionGuard() { X.c.precision = keep; }
+    } guard{X, X.c.precision};
+    X.c.precision = FLITE_FP64;
     copy(X, A.u0, L.u, n5);
     copy(X, A.u0, L.uprev, n5);
     if (X.P.viscous) copy(X, A.mu0, L.mu, N);

@@ -199,7 +199,7 @@ def test_adjoint_leaves_the_solve_unchanged():
     assert np.array_equal(a.get_state(1), b.get_state(1))
 
 
-@pytest.mark.parametrize("ctl", [dict(ReynoldsNumber=5e6, turbulenceModel=1), dict(fluxType=4), dict(precision=1),
+@pytest.mark.parametrize("ctl", [dict(ReynoldsNumber=5e6, turbulenceModel=1), dict(fluxType=4),
                                  dict(dissipationScheme=3)])
 def test_adjoint_refuses_what_it_does_not_cover(ctl):
     mesh = Mesh.bump_channel(6, 2, 2, 0.05, nlevels=1)
@@ -314,3 +314,22 @@ def test_laminar_adjoint_matches_central_differences(laminar_case):
         fd = (Jp - Jm) / (2 * h)
         adj = (xb[:, k] * nrm[:, k]).sum()
         assert abs(adj - fd) <= 1e-5 * abs(fd), (k, adj, fd)
+
+
+@pytest.mark.parametrize("lam", [dict(), LAMINAR])
+def test_mixed_precision_solution_has_the_fp64_sensitivities(lam):
+    """FLITE_MIXED converges to the FP64 iteration's fixed point, so the
+    adjoint of its solution (computed in FP64) equals the FP64 run's."""
+    j = Jittered(12, 4, 4, nlevels=2)
+    out = []
+    for prec in (0, 1):
+        c = controls(numberOfGridsToUse=2, precision=prec, **lam)
+        s, res = converge(c, j.mesh, tol=1e-14, max_cycles=8000)
+        assert res < 1e-13
+        r = s.adjoint_solve("CL", tol=1e-12, max_iter=200000)
+        out.append((s.get_state(1), r))
+    (u0, r0), (u1, r1) = out
+    assert np.abs(u1 - u0).max() <= 1e-11 * np.abs(u0).max()
+    assert abs(r1["J"] - r0["J"]) <= 1e-10 * abs(r0["J"])
+    for k in ("side_w_bar", "bnd_w_bar"):
+        assert np.abs(r1[k] - r0[k]).max() <= 1e-8 * np.abs(r0[k]).max()
