@@ -356,6 +356,20 @@ struct flite_ctx {
         counted();
         k_prolong_fine<<<nblk(V(fl).N), nb, 0, s>>>(P, V(cl), V(fl));
     }
+    // the head of a physical time step (mg_par:586-602): laminar viscosity
+    // 1/Re on every level, u (and in unsteady runs uold) restricted to every
+    // coarse level
+    void physical_step_start() {
+        const double mu = c.ReynoldsNumber > 0.0 ? 1. / c.ReynoldsNumber : 0.0;
+        for (size_t l = 0; l < lv.size(); ++l) {
+            k_fill<<<blocks(V(l).N), kBlock, 0, s>>>(V(l).mu, V(l).N, mu);
+            if (l > 0) {
+                mapFineToCoarse((int)l - 1);
+                if (P.unsteady)
+                    k_restrict_arr<<<nblk(V(l).N), nb, 0, s>>>(V(l), V(l - 1), V(l - 1).uold, V(l).uold, 5);
+            }
+        }
+    }
     void mapFineToCoarse(int fl) {
         counted();
         k_restrict_u<<<nblk(V(fl + 1).N), nb, 0, s>>>(V(fl + 1), V(fl));

@@ -18,6 +18,10 @@ struct Params {
     double inf[12];
     double RK[3];
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
+    // unsteady dual time (flowType 1): the physical time step and the
+    // second-order backward difference on level 1 (timeScheme 2)
+    int unsteady, bdf2;
+    double dtp;
     // Spalart-Allmaras (turbulenceModel 1)
     int sa, nTurbGrids;
     double turbCFL, turbK, maxTurb, turbProlRelax, oPrt;
@@ -98,6 +102,9 @@ struct LevelView {
     DeltaRec *dq;                          // [N] anchor primitives and increments
     const IncRec32 *inc32;                 // [2E] incidences in FP32
     double *bflux;                         // [B][10] boundary-edge contributions
+    // unsteady dual time: the solution of the previous physical time steps
+    // (uold2 on level 1 only)
+    double *uold, *uold2;                  // [5][N]
     int *cyc;                              // cycle number of this level
 };
 

@@ -48,8 +48,12 @@ int guarded(flite_ctx *ctx, F &&f) {
 }
 
 const char *unsupported_reason(const flite_controls &c) {
-    if (c.flowType != 0) return "flowType != 0 (unsteady) is not supported";
+    if (c.flowType == 2) return "flowType 2 (moving meshes, ALE) is not supported";
+    if (c.flowType != 0 && c.flowType != 1) return "flowType must be 0 (steady) or 1 (unsteady, static mesh)";
     if (c.explicit_) return "explicit time stepping is not supported";
+    if (c.flowType == 1 && c.turbulenceModel != 0)
+        return "unsteady runs take no turbulence model";
+    if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return "unsteady runs need physicalTimeStep > 0";
     if (c.SAS || c.GUSTMODEL || c.movingwall || c.patchInitialization || c.nspan != 0)
         return "SAS, gust, moving-wall, patch initialisation and spanwise loads are not supported";
     if (c.residualSmoothingFactor > 0 || c.prolongationSmoothingFactor > 0)
@@ -118,6 +122,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         P.nsig = c->ReynoldsNumber < 1 ? 4 : 2;       // def_par:1592-1596
         P.isentropic = c->wallsAreIsentropic; P.viscous = c->ReynoldsNumber > 0.0;
         P.boundaryTerm = c->boundaryTerm; P.useDissW = c->useDissipationWeighting; P.ncfl = c->numberOfCFLIncrements;
+        P.unsteady = c->flowType != 0; P.bdf2 = c->timeScheme == 2; P.dtp = c->physicalTimeStep;
         P.sa = c->turbulenceModel == 1; P.nTurbGrids = c->numberOfTurbulenceGrids;
         P.turbCFL = c->turbulentCFLNumber; P.turbK = c->turbK; P.maxTurb = c->maxTurbulenceValue;
         P.turbProlRelax = c->turbProlongationRelaxation;
@@ -341,6 +346,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L.dq = nullptr;
             }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
+            L.uold = c->flowType != 0 ? X.alloc<double>(5 * (size_t)N) : nullptr;
+            L.uold2 = c->flowType != 0 && l == 0 ? X.alloc<double>(5 * (size_t)N) : nullptr;
             L.cyc = X.d_cyc + l;
             L.nvar = X.nvar();
         }
@@ -426,13 +433,30 @@ int flite_start(flite_ctx *ctx) {
         X.set_cycle(1);
         k_set_int<<<1, 1, 0, X.s>>>(X.V(0).cyc, X.d_cycle);
         k_bc_solution<<<flite_ctx::blocks(X.V(0).N), kBlock, 0, X.s>>>(X.P, X.V(0));
-        // laminar viscosity and the restriction of u to every coarse level
-        // (mg_par:586-602)
-        const double mu = X.c.ReynoldsNumber > 0.0 ? 1. / X.c.ReynoldsNumber : 0.0;
-        for (size_t l = 0; l < X.lv.size(); ++l) {
-            k_fill<<<flite_ctx::blocks(X.V(l).N), kBlock, 0, X.s>>>(X.V(l).mu, X.V(l).N, mu);
-            if (l > 0) X.mapFineToCoarse((int)l - 1);
+        // an unsteady run starts with uold = uold2 = u (def_par:3594-3596)
+        if (X.P.unsteady) {
+            const size_t n5 = 5 * (size_t)X.V(0).N;
+            CK(cudaMemcpyAsync(X.V(0).uold, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
+            CK(cudaMemcpyAsync(X.V(0).uold2, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
         }
+        X.physical_step_start();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(X.s));
+        return FLITE_OK;
+    });
+}
+
+int flite_next_physical_step(flite_ctx *ctx) {
+    if (!ctx) return FLITE_EINVAL;
+    if (!ctx->P.unsteady) return fail(ctx, FLITE_EINVAL, "not an unsteady run (flowType 0)");
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        // end of the step (mg_par:889-890): uold2 = uold, uold = u on level 1
+        const size_t n5 = 5 * (size_t)X.V(0).N;
+        CK(cudaMemcpyAsync(X.V(0).uold2, X.V(0).uold, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
+        CK(cudaMemcpyAsync(X.V(0).uold, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
+        // head of the next one
+        X.physical_step_start();
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(X.s));
         return FLITE_OK;

@@ -987,8 +987,22 @@ __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
     }
+    if (P.unsteady && mode == MODE_STAGE) {  // addTimeDifferences (def_par:1184-1241)
+        const double Vi = L.V[i], dtp = P.dtp;
+        if (L.grid == 1 && P.bdf2) {
+            for (int c = 0; c < 5; ++c) {
+                const double uc = L.u[c * N + i], u1 = L.uold[c * N + i], u2 = L.uold2[c * N + i];
+                r[c] = r[c] + ((((1.5 * Vi) * uc - (2.0 * Vi) * u1) + (0.5 * Vi) * u2) / dtp);
+            }
+        } else {
+            for (int c = 0; c < 5; ++c)
+                r[c] = r[c] + Vi * (L.u[c * N + i] - L.uold[c * N + i]) / dtp;
+        }
+    }
     for (int c = 0; c < 5; ++c) r[c] = r[c] + L.diss[c * N + i];
-    const double dt = L.dt[i], V = L.V[i];
+    double dt = L.dt[i];
+    const double V = L.V[i];
+    if (P.unsteady) dt = dt / (1.0 + 1.5 * dt / P.dtp);  // solveSystem's dual-time step (def_par:1427-1442)
     for (int c = 0; c < 5; ++c) r[c] = dt * r[c] / V;  // solveSystem
     const unsigned char cls = L.bc[i];
     double n0 = 0, n1 = 0, n2 = 0;
@@ -1103,6 +1117,15 @@ __global__ void k_restrict_u(LevelView C, LevelView F) {
     double v[6];
     restrict_gather(C, F.u, F.N, c, C.nvar, v);
     for (int k = 0; k < C.nvar; ++k) C.u[k * C.N + c] = v[k];
+}
+
+// mapFineToCoarse of another array (def_par:12572-12679)
+__global__ void k_restrict_arr(LevelView C, LevelView F, const double *fsrc, double *cdst, int ncomp) {
+    int c = tid();
+    if (c >= C.N) return;
+    double v[6];
+    restrict_gather(C, fsrc, F.N, c, ncomp, v);
+    for (int k = 0; k < ncomp; ++k) cdst[k * C.N + c] = v[k];
 }
 
 // the nu~ solution conditions: zero on walls (def_par:4416-4418, 4446-4448,

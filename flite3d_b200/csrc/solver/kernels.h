@@ -43,6 +43,7 @@ __global__ void k_sa_stage(Params P, LevelView L, int mode, int stage, int turb)
 __global__ void k_make_inc32(const int2 *inc, const EdgeW *ew, int n, IncRec32 *o);
 __global__ void k_copy(const double *a, double *b, size_t n);
 __global__ void k_restrict_u(LevelView C, LevelView F);
+__global__ void k_restrict_arr(LevelView C, LevelView F, const double *fsrc, double *cdst, int ncomp);
 __global__ void k_restrict_state(Params P, LevelView C, LevelView F);
 __global__ void k_restrict_incr(Params P, LevelView C, LevelView F);
 __global__ void k_prolong_coarse(Params P, LevelView C, LevelView F);

@@ -135,6 +135,11 @@ class Solver:
         self._ck(self.be.start(self._h), "start")
 
     # ---- solver calls ------------------------------------------------------
+    def next_physical_step(self):
+        """Unsteady runs: close the physical time step (uold2 = uold, uold =
+        u) and open the next one (viscosity reset, restrictions)."""
+        self._ck(self.be.next_physical_step(self._h), "next_physical_step")
+
     def do_time_iterations(self, level, nsteps=1, calc_diss=True, cycle=1, calc_turb=True):
         self._ck(self.be.do_time_iterations(self._h, level, nsteps, int(calc_diss), int(calc_turb), cycle),
                  "do_time_iterations")
@@ -348,6 +353,25 @@ def run_steady(solver, orders=8.0, max_cycles=1000, callback=None):
             callback(it, res, f)
         if not (math.log(res0) - math.log(res[0]) < math.log(10.0) * orders):
             break
+    return hist
+
+
+def run_unsteady(solver, steps, cycles_per_step, callback=None):
+    """Dual time stepping of multiGridCycles for flowType 1 (mg_par:483-890):
+    per physical step a fixed number of multigrid cycles (numberOfMGIterations
+    > 0), then the step is closed and the next one opened.  Returns the
+    (step, res1, lift, drag) at the end of each step."""
+    hist = []
+    for step in range(1, steps + 1):
+        for it in range(1, cycles_per_step + 1):
+            solver.cycle(it)
+        res, _, _ = solver.residuals()
+        f = solver.forces()
+        hist.append((step, res[0], f[0], f[1]))
+        if callback:
+            callback(step, res, f)
+        if step < steps:
+            solver.next_physical_step()
     return hist
 
 

@@ -151,6 +151,17 @@ int flite_start(flite_ctx *ctx);
 
 /* ---- solver steps (one per replaced Fortran call) --------------------- */
 /* doTimeIterations (def_par:966-1000)                                     */
+/* Unsteady runs (flowType 1, dual time on a static mesh): between physical
+ * time steps of multiGridCycles (mg_par:483-890), uold2 = uold and uold = u
+ * on level 1, then the head of the next step: laminar viscosity 1/Re on
+ * every level, u and uold restricted to every coarse level (mg_par:586-602).
+ * flite_start sets uold = uold2 = u and performs the first step's head.
+ * Each RK stage adds the time differences of addTimeDifferences
+ * (def_par:1184-1241: second-order backward on level 1 with timeScheme 2,
+ * first order elsewhere) and solveSystem divides the local step by
+ * 1 + 1.5 dt / physicalTimeStep (def_par:1427-1442).  The mesh is static:
+ * the previous volumes are the volumes.                                    */
+int flite_next_physical_step(flite_ctx *ctx);
 int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps,
                              int calc_diss, int calc_turb, int cycle_no);
 /* restrictGrid (def_par:12141-12430)                                      */

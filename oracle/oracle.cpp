@@ -52,6 +52,7 @@ struct Level {
     vec rweight;
     // state
     vec u[6], uprev[6], rhs[6], src[6], diss[5];
+    vec uold[5], uold2[5];  // unsteady runs: previous physical time steps
     vec p, dt, mu, conn, wallArea, nx, ny, nz, wallStress[3];
     // Spalart-Allmaras: turbulenceDiffusionTerm, localTurbulentTimeSteps,
     // vorticity and divergence of the viscous routine
@@ -1110,8 +1111,12 @@ struct Oracle {
     // ---- solveSystem (def_par:1407-1479) + solveTurbulenceSystem
     // (def_par:1481-1522) -------------------------------------------------
     void solveSystem(Level &g, vec *rhs) {
+        // flowType != 0: the dual-time step dt / (1 + 1.5 dt / physicalTimeStep)
+        // (def_par:1427-1442)
+        const bool unsteady = c.flowType != 0;
         for_nodes(g.N, [&](int i) {
             double dt = g.dt[i];
+            if (unsteady) dt = dt / (1.0 + 1.5 * dt / c.physicalTimeStep);
             for (int k = 0; k < 5; ++k) rhs[k][i] = dt * rhs[k][i] / g.V[i];
         });
         if (sa()) for_nodes(g.N, [&](int i) { rhs[5][i] = g.dtT[i] * rhs[5][i] / g.V[i]; });
@@ -1248,6 +1253,23 @@ struct Oracle {
         else makeArtificialDissipation2(g);
     }
 
+    // ---- addTimeDifferences (def_par:1184-1241), static mesh: the previous
+    // volumes are the volumes -------------------------------------------------
+    void addTimeDifferences(Level &g) {
+        if (c.flowType == 0) return;
+        const double dtp = c.physicalTimeStep;
+        if (g.grid == 1 && c.timeScheme == 2) {
+            for (int i = 0; i < g.N; ++i)
+                for (int k = 0; k < 5; ++k)
+                    g.rhs[k][i] = g.rhs[k][i] + (((1.5 * g.V[i]) * g.u[k][i] - (2.0 * g.V[i]) * g.uold[k][i]) +
+                                                 (0.5 * g.V[i]) * g.uold2[k][i]) / dtp;
+        } else {
+            for (int i = 0; i < g.N; ++i)
+                for (int k = 0; k < 5; ++k)
+                    g.rhs[k][i] = g.rhs[k][i] + g.V[i] * (g.u[k][i] - g.uold[k][i]) / dtp;
+        }
+    }
+
     // ---- singleIteration (def_par:1002-1181) ------------------------------
     void singleIteration(Level &g, bool calcDiss, bool calcTurb) {
         const bool turb = sa() && calcTurb;
@@ -1268,6 +1290,7 @@ struct Oracle {
             makePressureField(g, g.u);
             for (int k = 0; k < nvar; ++k) std::fill(g.rhs[k].begin(), g.rhs[k].end(), 0.0);
             makeRHS(g);
+            addTimeDifferences(g);
             if (turb) {
                 // triggerTurbulenceField and makeSATripTerm act on the trip
                 // field nodes of a .wid file; none are read (no trip lines)
@@ -1577,7 +1600,9 @@ struct Oracle {
 };
 
 int check_controls(const flite_controls &c) {
-    if (c.flowType != 0 || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
+    // flowType 1: dual time on a static mesh, without a turbulence model
+    if (c.flowType == 1 && (c.turbulenceModel != 0 || !(c.physicalTimeStep > 0))) return FLITE_EUNSUPPORTED;
+    if ((c.flowType != 0 && c.flowType != 1) || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
         c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
         c.prolongationSmoothingFactor > 0)
         return FLITE_EUNSUPPORTED;
@@ -2248,6 +2273,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
             g.src[k].assign(g.N, 0.0);
         }
         for (int k = 0; k < 5; ++k) g.diss[k].assign(g.N, 0.0);
+        for (int k = 0; k < 5; ++k) { g.uold[k].assign(g.N, 0.0); g.uold2[k].assign(g.N, 0.0); }
         g.p.assign(g.N, 0.0); g.dt.assign(g.N, 0.0); g.mu.assign(g.N, 0.0);
         g.turbDiff.assign(g.N, 0.0); g.dtT.assign(g.N, 0.0); g.vort.assign(g.N, 0.0); g.divg.assign(g.N, 0.0);
         for (int k = 0; k < 3; ++k) g.wallStress[k].assign(g.N, 0.0);
@@ -2326,6 +2352,8 @@ int oracle_init_freestream(oracle_ctx *o) {
     return FLITE_OK;
 }
 
+static void physical_step_head(Oracle &O);
+
 int oracle_start(oracle_ctx *o) {
     if (!o) return FLITE_EINVAL;
     Oracle &O = o->o;
@@ -2333,11 +2361,31 @@ int oracle_start(oracle_ctx *o) {
     O.makePressureField(g, g.u);
     g.cycleNumber = 1;
     O.setBCsOnSolutionField(g, g.u);
+    if (O.c.flowType != 0)  // uold = uold2 = u (def_par:3594-3596)
+        for (int k = 0; k < 5; ++k) { g.uold[k] = g.u[k]; g.uold2[k] = g.u[k]; }
+    physical_step_head(O);
+    return FLITE_OK;
+}
+
+// the head of a physical time step (mg_par:586-602): laminar viscosity on
+// every level, u and (unsteady) uold restricted to every coarse level
+static void physical_step_head(Oracle &O) {
     const double mu = O.c.ReynoldsNumber > 0.0 ? 1. / O.c.ReynoldsNumber : 0.0;
     for (size_t l = 0; l < O.lv.size(); ++l) {
         std::fill(O.lv[l].mu.begin(), O.lv[l].mu.end(), mu);
-        if (l > 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].u, O.lv[l].u, O.nvar);
+        if (l > 0) {
+            O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].u, O.lv[l].u, O.nvar);
+            if (O.c.flowType != 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].uold, O.lv[l].uold, 5);
+        }
     }
+}
+
+int oracle_next_physical_step(oracle_ctx *o) {
+    if (!o || o->o.c.flowType == 0) return FLITE_EINVAL;
+    Oracle &O = o->o;
+    Level &g = O.lv[0];
+    for (int k = 0; k < 5; ++k) { g.uold2[k] = g.uold[k]; g.uold[k] = g.u[k]; }  // mg_par:889-890
+    physical_step_head(O);
     return FLITE_OK;
 }
 
