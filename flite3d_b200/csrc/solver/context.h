@@ -212,7 +212,7 @@ struct flite_ctx {
         if (!sa()) return;
         if (turb()) {
             counted();
-            k_sa_conv<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+            k_sa_conv<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), P.unsteady && mode == MODE_STAGE ? 1 : 0);
         }
         counted();
         k_sa_stage<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), mode, stage, turb() ? 1 : 0);
@@ -366,7 +366,7 @@ struct flite_ctx {
             if (l > 0) {
                 mapFineToCoarse((int)l - 1);
                 if (P.unsteady)
-                    k_restrict_arr<<<nblk(V(l).N), nb, 0, s>>>(V(l), V(l - 1), V(l - 1).uold, V(l).uold, 5);
+                    k_restrict_arr<<<nblk(V(l).N), nb, 0, s>>>(V(l), V(l - 1), V(l - 1).uold, V(l).uold, nvar());
             }
         }
     }

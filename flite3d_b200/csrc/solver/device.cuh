@@ -104,7 +104,7 @@ struct LevelView {
     double *bflux;                         // [B][10] boundary-edge contributions
     // unsteady dual time: the solution of the previous physical time steps
     // (uold2 on level 1 only)
-    double *uold, *uold2;                  // [5][N]
+    double *uold, *uold2;                  // [nvar][N]
     int *cyc;                              // cycle number of this level
 };
 
@@ -158,6 +158,17 @@ __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b 
 __device__ __forceinline__ double pressure(const Params &P, double r, double m1, double m2, double m3, double E) {
     double pp = P.gm1 * (E - 0.5 * ((m1 * m1 + m2 * m2) + m3 * m3) / r);
     return dmax(pp, 0.1);
+}
+
+// addTimeDifferences (def_par:1184-1241) of component c at node i: the
+// second-order backward difference on level 1 with timeScheme 2, first order
+// elsewhere; static mesh (the previous volumes are the volumes)
+__device__ __forceinline__ double time_difference(const Params &P, const LevelView &L, int i, int c) {
+    const size_t k = (size_t)c * L.N + i;
+    const double Vi = L.V[i];
+    if (L.grid == 1 && P.bdf2)
+        return (((1.5 * Vi) * L.u[k] - (2.0 * Vi) * L.uold[k]) + (0.5 * Vi) * L.uold2[k]) / P.dtp;
+    return Vi * (L.u[k] - L.uold[k]) / P.dtp;
 }
 
 // tangential projection used by every slip condition (def_par:4448-4451,

@@ -51,8 +51,6 @@ const char *unsupported_reason(const flite_controls &c) {
     if (c.flowType == 2) return "flowType 2 (moving meshes, ALE) is not supported";
     if (c.flowType != 0 && c.flowType != 1) return "flowType must be 0 (steady) or 1 (unsteady, static mesh)";
     if (c.explicit_) return "explicit time stepping is not supported";
-    if (c.flowType == 1 && c.turbulenceModel != 0)
-        return "unsteady runs take no turbulence model";
     if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return "unsteady runs need physicalTimeStep > 0";
     if (c.SAS || c.GUSTMODEL || c.movingwall || c.patchInitialization || c.nspan != 0)
         return "SAS, gust, moving-wall, patch initialisation and spanwise loads are not supported";
@@ -346,8 +344,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L.dq = nullptr;
             }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
-            L.uold = c->flowType != 0 ? X.alloc<double>(5 * (size_t)N) : nullptr;
-            L.uold2 = c->flowType != 0 && l == 0 ? X.alloc<double>(5 * (size_t)N) : nullptr;
+            L.uold = c->flowType != 0 ? X.alloc<double>(nv * N) : nullptr;
+            L.uold2 = c->flowType != 0 && l == 0 ? X.alloc<double>(nv * N) : nullptr;
             L.cyc = X.d_cyc + l;
             L.nvar = X.nvar();
         }
@@ -435,7 +433,7 @@ int flite_start(flite_ctx *ctx) {
         k_bc_solution<<<flite_ctx::blocks(X.V(0).N), kBlock, 0, X.s>>>(X.P, X.V(0));
         // an unsteady run starts with uold = uold2 = u (def_par:3594-3596)
         if (X.P.unsteady) {
-            const size_t n5 = 5 * (size_t)X.V(0).N;
+            const size_t n5 = X.nvar() * (size_t)X.V(0).N;
             CK(cudaMemcpyAsync(X.V(0).uold, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
             CK(cudaMemcpyAsync(X.V(0).uold2, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
         }
@@ -452,7 +450,7 @@ int flite_next_physical_step(flite_ctx *ctx) {
     return guarded(ctx, [&] {
         flite_ctx &X = *ctx;
         // end of the step (mg_par:889-890): uold2 = uold, uold = u on level 1
-        const size_t n5 = 5 * (size_t)X.V(0).N;
+        const size_t n5 = X.nvar() * (size_t)X.V(0).N;
         CK(cudaMemcpyAsync(X.V(0).uold2, X.V(0).uold, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
         CK(cudaMemcpyAsync(X.V(0).uold, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
         // head of the next one

@@ -987,18 +987,8 @@ __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
     }
-    if (P.unsteady && mode == MODE_STAGE) {  // addTimeDifferences (def_par:1184-1241)
-        const double Vi = L.V[i], dtp = P.dtp;
-        if (L.grid == 1 && P.bdf2) {
-            for (int c = 0; c < 5; ++c) {
-                const double uc = L.u[c * N + i], u1 = L.uold[c * N + i], u2 = L.uold2[c * N + i];
-                r[c] = r[c] + ((((1.5 * Vi) * uc - (2.0 * Vi) * u1) + (0.5 * Vi) * u2) / dtp);
-            }
-        } else {
-            for (int c = 0; c < 5; ++c)
-                r[c] = r[c] + Vi * (L.u[c * N + i] - L.uold[c * N + i]) / dtp;
-        }
-    }
+    if (P.unsteady && mode == MODE_STAGE)  // addTimeDifferences (def_par:1184-1241)
+        for (int c = 0; c < 5; ++c) r[c] = r[c] + time_difference(P, L, i, c);
     for (int c = 0; c < 5; ++c) r[c] = r[c] + L.diss[c * N + i];
     double dt = L.dt[i];
     const double V = L.V[i];

@@ -38,7 +38,7 @@ __global__ void k_delta_state(LevelView L);
 __global__ void k_sa_timestep(Params P, LevelView L);
 __global__ void k_sa_grad(Params P, LevelView L);
 __global__ void k_sa_diff(Params P, LevelView L);
-__global__ void k_sa_conv(Params P, LevelView L);
+__global__ void k_sa_conv(Params P, LevelView L, int td);
 __global__ void k_sa_stage(Params P, LevelView L, int mode, int stage, int turb);
 __global__ void k_make_inc32(const int2 *inc, const EdgeW *ew, int n, IncRec32 *o);
 __global__ void k_copy(const double *a, double *b, size_t n);

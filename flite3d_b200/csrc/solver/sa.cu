@@ -157,7 +157,7 @@ __global__ void k_sa_diff(Params P, LevelView L) {
     L.turbDiff[i] = acc + L.sanh[i];
 }
 
-__global__ void k_sa_conv(Params P, LevelView L) {
+__global__ void k_sa_conv(Params P, LevelView L, int td) {
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -169,7 +169,8 @@ __global__ void k_sa_conv(Params P, LevelView L) {
     };
     double qi[4];
     prim(i, qi);
-    double acc = 0.0;
+    // an unsteady stage's time difference comes first (def_par:1073)
+    double acc = td ? time_difference(P, L, i, 5) : 0.0;
     for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
         const int2 t = L.inc[k];
         const int e = t.x >= 0 ? t.x : ~t.x;
@@ -241,7 +242,9 @@ __global__ void k_sa_stage(Params P, LevelView L, int mode, int stage, int turb)
     if (i >= L.N) return;
     const size_t o6 = 5 * (size_t)L.N + i;
     const unsigned char cls = L.bc[i];
-    double r = turb ? L.rhs[o6] : 0.0;  // convection from k_sa_conv
+    // convection from k_sa_conv (after the time difference of an unsteady
+    // stage, which is all of it when the turbulence is not recomputed)
+    double r = turb ? L.rhs[o6] : (P.unsteady && mode == MODE_STAGE ? time_difference(P, L, i, 5) : 0.0);
     if (turb) r = sa_source(P, L, i, r);
     // restrictGrid adds the (last computed) diffusion term whether or not
     // the turbulence is recomputed (def_par:12238-12240, 12315-12317)

@@ -158,9 +158,10 @@ int flite_start(flite_ctx *ctx);
  * flite_start sets uold = uold2 = u and performs the first step's head.
  * Each RK stage adds the time differences of addTimeDifferences
  * (def_par:1184-1241: second-order backward on level 1 with timeScheme 2,
- * first order elsewhere) and solveSystem divides the local step by
- * 1 + 1.5 dt / physicalTimeStep (def_par:1427-1442).  The mesh is static:
- * the previous volumes are the volumes.                                    */
+ * first order elsewhere; for nu~ before its convection) and solveSystem
+ * divides the local step by 1 + 1.5 dt / physicalTimeStep (def_par:
+ * 1427-1442; solveTurbulenceSystem does not).  The mesh is static: the
+ * previous volumes are the volumes.                                         */
 int flite_next_physical_step(flite_ctx *ctx);
 int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps,
                              int calc_diss, int calc_turb, int cycle_no);

@@ -52,7 +52,7 @@ struct Level {
     vec rweight;
     // state
     vec u[6], uprev[6], rhs[6], src[6], diss[5];
-    vec uold[5], uold2[5];  // unsteady runs: previous physical time steps
+    vec uold[6], uold2[6];  // unsteady runs: previous physical time steps
     vec p, dt, mu, conn, wallArea, nx, ny, nz, wallStress[3];
     // Spalart-Allmaras: turbulenceDiffusionTerm, localTurbulentTimeSteps,
     // vorticity and divergence of the viscous routine
@@ -1260,12 +1260,12 @@ struct Oracle {
         const double dtp = c.physicalTimeStep;
         if (g.grid == 1 && c.timeScheme == 2) {
             for (int i = 0; i < g.N; ++i)
-                for (int k = 0; k < 5; ++k)
+                for (int k = 0; k < nvar; ++k)
                     g.rhs[k][i] = g.rhs[k][i] + (((1.5 * g.V[i]) * g.u[k][i] - (2.0 * g.V[i]) * g.uold[k][i]) +
                                                  (0.5 * g.V[i]) * g.uold2[k][i]) / dtp;
         } else {
             for (int i = 0; i < g.N; ++i)
-                for (int k = 0; k < 5; ++k)
+                for (int k = 0; k < nvar; ++k)
                     g.rhs[k][i] = g.rhs[k][i] + g.V[i] * (g.u[k][i] - g.uold[k][i]) / dtp;
         }
     }
@@ -1601,7 +1601,7 @@ struct Oracle {
 
 int check_controls(const flite_controls &c) {
     // flowType 1: dual time on a static mesh, without a turbulence model
-    if (c.flowType == 1 && (c.turbulenceModel != 0 || !(c.physicalTimeStep > 0))) return FLITE_EUNSUPPORTED;
+    if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return FLITE_EUNSUPPORTED;
     if ((c.flowType != 0 && c.flowType != 1) || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
         c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
         c.prolongationSmoothingFactor > 0)
@@ -2273,7 +2273,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
             g.src[k].assign(g.N, 0.0);
         }
         for (int k = 0; k < 5; ++k) g.diss[k].assign(g.N, 0.0);
-        for (int k = 0; k < 5; ++k) { g.uold[k].assign(g.N, 0.0); g.uold2[k].assign(g.N, 0.0); }
+        for (int k = 0; k < 6; ++k) { g.uold[k].assign(g.N, 0.0); g.uold2[k].assign(g.N, 0.0); }
         g.p.assign(g.N, 0.0); g.dt.assign(g.N, 0.0); g.mu.assign(g.N, 0.0);
         g.turbDiff.assign(g.N, 0.0); g.dtT.assign(g.N, 0.0); g.vort.assign(g.N, 0.0); g.divg.assign(g.N, 0.0);
         for (int k = 0; k < 3; ++k) g.wallStress[k].assign(g.N, 0.0);
@@ -2362,7 +2362,7 @@ int oracle_start(oracle_ctx *o) {
     g.cycleNumber = 1;
     O.setBCsOnSolutionField(g, g.u);
     if (O.c.flowType != 0)  // uold = uold2 = u (def_par:3594-3596)
-        for (int k = 0; k < 5; ++k) { g.uold[k] = g.u[k]; g.uold2[k] = g.u[k]; }
+        for (int k = 0; k < O.nvar; ++k) { g.uold[k] = g.u[k]; g.uold2[k] = g.u[k]; }
     physical_step_head(O);
     return FLITE_OK;
 }
@@ -2375,7 +2375,7 @@ static void physical_step_head(Oracle &O) {
         std::fill(O.lv[l].mu.begin(), O.lv[l].mu.end(), mu);
         if (l > 0) {
             O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].u, O.lv[l].u, O.nvar);
-            if (O.c.flowType != 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].uold, O.lv[l].uold, 5);
+            if (O.c.flowType != 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].uold, O.lv[l].uold, O.nvar);
         }
     }
 }
@@ -2384,7 +2384,7 @@ int oracle_next_physical_step(oracle_ctx *o) {
     if (!o || o->o.c.flowType == 0) return FLITE_EINVAL;
     Oracle &O = o->o;
     Level &g = O.lv[0];
-    for (int k = 0; k < 5; ++k) { g.uold2[k] = g.uold[k]; g.uold[k] = g.u[k]; }  // mg_par:889-890
+    for (int k = 0; k < O.nvar; ++k) { g.uold2[k] = g.uold[k]; g.uold[k] = g.u[k]; }  // mg_par:889-890
     physical_step_head(O);
     return FLITE_OK;
 }

@@ -1,7 +1,8 @@
 """Unsteady dual time stepping (flowType 1 on a static mesh): the GPU library
 against the CPU restatement, bit for bit on every level after each physical
 time step, for the second-order backward difference (timeScheme 2) and the
-first-order one, inviscid and laminar; residual norms and forces to 1e-12.
+first-order one, inviscid, laminar and with the Spalart-Allmaras model;
+residual norms and forces to 1e-12.
 """
 import numpy as np
 import pytest
@@ -36,3 +37,27 @@ def test_unsteady_steps_match(ctl):
         g.next_physical_step()
         o.next_physical_step()
     assert not np.array_equal(g.get_state(1), u0)
+
+
+@pytest.mark.parametrize("ctl", [dict(), dict(numberOfTurbulenceSteps=2), dict(timeScheme=1)])
+def test_unsteady_spalart_allmaras_steps_match(ctl):
+    """Unsteady RANS: the time difference of nu~ comes before its convection,
+    and alone when the turbulence is not recomputed."""
+    mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+    base = dict(ReynoldsNumber=1.0e5, MachNumber=0.5, CFLNumber=1.0, fluxType=1, numberOfGridsToUse=3,
+                multigridScheme=3, turbulenceModel=1, wallsAreIsentropic=1, flowType=1, physicalTimeStep=0.2)
+    c = default_controls(**{**base, **ctl})
+    g, o = Solver(c, mesh), Solver(c, mesh, backend=oracle_backend())
+    u0 = initial_state(c, mesh, perturb_seed=20261203)
+    for s in (g, o):
+        s.set_state(u0)
+        s.start()
+    for step in range(1, 4):
+        for it in range(1, 4):
+            g.cycle(it)
+            o.cycle(it)
+        for level in range(1, 4):
+            a, b = g.get_state(level), o.get_state(level)
+            assert a.shape[0] == 6 and np.array_equal(a, b), (step, level)
+        g.next_physical_step()
+        o.next_physical_step()
