@@ -1432,6 +1432,51 @@ int fp_write_plotreg(const fp_mesh *m, const char *path) {
     });
 }
 
+// makeplot (mg_par:1599-1707): plotreg.reg = (N, nDomains), per domain
+// nLocal and nLocal records (local, global); the result file of domain d is
+// res_prefix followed by d; u(global, :) = unk_d(local, :); the .unk holds N
+// and the merged columns
+int fp_makeplot(const char *plotreg, const char *res_prefix, int nvar, const char *unk) {
+    if (!plotreg || !res_prefix || !unk || nvar < 1 || nvar > 7) return FLITE_EINVAL;
+    return guarded([&] {
+        fio::Reader r(plotreg);
+        r.next();
+        const int32_t N = r.i4(), nd = r.i4();
+        if (N < 1 || nd < 1) throw fio::io_error("bad plotreg header");
+        std::vector<double> u((size_t)N * nvar, 0.0);
+        for (int32_t d = 1; d <= nd; ++d) {
+            r.next();
+            const int32_t nl = r.i4();
+            if (nl < 0) throw fio::io_error("bad plotreg domain size");
+            std::vector<int32_t> loc(nl), glob(nl);
+            for (int32_t j = 0; j < nl; ++j) {
+                r.next();
+                loc[j] = r.i4();
+                glob[j] = r.i4();
+            }
+            const std::string rpath = std::string(res_prefix) + std::to_string(d);
+            fio::Reader rd(rpath.c_str());
+            rd.next();
+            const int32_t nto = rd.i4();
+            rd.next();
+            if (rd.remaining() < (size_t)nto * nvar * 8) throw fio::io_error("result record too short");
+            std::vector<double> x((size_t)nto * nvar);
+            rd.r8s(x.data(), x.size());
+            for (int32_t j = 0; j < nl; ++j) {
+                if (loc[j] < 1 || loc[j] > nto || glob[j] < 1 || glob[j] > N)
+                    throw fio::io_error("plotreg node out of range");
+                for (int k = 0; k < nvar; ++k)
+                    u[(size_t)k * N + glob[j] - 1] = x[(size_t)k * nto + loc[j] - 1];
+            }
+        }
+        fio::Writer w(unk);
+        w.i4(N).end();
+        w.r8s(u.data(), u.size()).end();
+        w.close();
+        return FLITE_OK;
+    });
+}
+
 int fp_write_plt(const fp_mesh *m, const char *path) {
     if (!m || !path || m->tets.empty()) return FLITE_EINVAL;
     return guarded([&] {

@@ -220,6 +220,13 @@ def read_unk(path, n, nvar=5):
     return out
 
 
+def makeplot(plotreg, res_prefix, nvar, unk):
+    """Merge per-domain result files <res_prefix>1.. through plotreg.reg into
+    one .unk, as the reference's makeplot does."""
+    _abi.check(_lib().fp_makeplot(str(plotreg).encode(), str(res_prefix).encode(), int(nvar), str(unk).encode()),
+               "fp_makeplot")
+
+
 def primitive_to_conserved(prim):
     """The restart conversion u(2:5) = rho*u(2:5) (def_par:3850-3856)."""
     prim = np.asarray(prim, dtype=np.float64)

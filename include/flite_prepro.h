@@ -78,6 +78,10 @@ int fp_write_unk(const char *path, int32_t n, int nvar, const double *u);
 int fp_read_unk(const char *path, int32_t n, int nvar, double *u);
 /* plotreg.reg for one domain: (N,1); N; N x (local, global)              */
 int fp_write_plotreg(const fp_mesh *m, const char *path);
+/* makeplot (mg_par:1599-1707): merge the result files <res_prefix>1 ..
+ * <res_prefix>nDomains (N_d, then nvar columns) through plotreg.reg's
+ * (local, global) pairs into one .unk (N, then nvar columns).               */
+int fp_makeplot(const char *plotreg, const char *res_prefix, int nvar, const char *unk);
 /* .plt (tet form, gen3d_generator.f90:377-389): (nEl,N,nBF); iel(4,nEl);
  * x(3,N); iface(5,nBF) with column 5 the surface (indicator) number.       */
 int fp_write_plt(const fp_mesh *m, const char *path);

@@ -151,3 +151,46 @@ def test_naca0012_generator():
     assert ind == {1, 2, 3}
     wd = m.array(1, "wall_dist")
     assert wd.min() >= 0.0 and wd.max() <= 10.5
+
+
+def test_makeplot_merges_domains(tmp_path):
+    """makeplot scatters each domain's result columns to the global nodes of
+    plotreg.reg: one domain through the mesh's own register, and two
+    hand-made domains that share a node."""
+    from flite3d_b200.mesh import makeplot, write_res
+    from flite3d_b200 import _abi
+    import ctypes
+    m = Mesh.bump_channel(6, 2, 2, 0.05, nlevels=1)
+    n = m.level(1).n_nodes
+    rng = np.random.default_rng(0)
+    u = np.abs(rng.standard_normal((5, n))) + 1.0
+    m.write_plotreg(tmp_path / "plotreg.reg")
+    write_res(tmp_path / "case.res_1", u)
+    makeplot(tmp_path / "plotreg.reg", tmp_path / "case.res_", 5, tmp_path / "case.unk")
+    merged = read_unk(tmp_path / "case.unk", n, 5)
+    perm = np.zeros(n, dtype=np.int32)
+    _abi.check(_abi.prepro_lib().fp_node_perm(m._h, perm.ctypes.data_as(ctypes.c_void_p)), "fp_node_perm")
+    res = np.vstack([u[:1], u[1:] / u[0]])  # what the result file holds
+    assert np.array_equal(merged[:, perm - 1], res)
+    # two domains of 3 local nodes over 5 global ones, node 3 in both
+    import struct
+
+    def rec(f, payload):
+        f.write(struct.pack("<i", len(payload)) + payload + struct.pack("<i", len(payload)))
+    with open(tmp_path / "two.reg", "wb") as f:
+        rec(f, struct.pack("<ii", 5, 2))
+        for pairs in (((1, 1), (2, 2), (3, 3)), ((1, 3), (2, 4), (3, 5))):
+            rec(f, struct.pack("<i", 3))
+            for a, b in pairs:
+                rec(f, struct.pack("<ii", a, b))
+    parts = [np.arange(1, 16, dtype=float).reshape(5, 3), 100 + np.arange(1, 16, dtype=float).reshape(5, 3)]
+    for d, x in enumerate(parts, 1):
+        with open(tmp_path / f"two.res_{d}", "wb") as f:
+            rec(f, struct.pack("<i", 3))
+            rec(f, x.tobytes())
+    makeplot(tmp_path / "two.reg", tmp_path / "two.res_", 5, tmp_path / "two.unk")
+    got = read_unk(tmp_path / "two.unk", 5, 5)
+    want = np.zeros((5, 5))
+    want[:, 0:3] = parts[0]
+    want[:, 2:5] = parts[1]  # the later domain writes node 3 last
+    assert np.array_equal(got, want)
