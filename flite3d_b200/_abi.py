@@ -18,6 +18,8 @@ FLITE_ENOMEM = 6
 FLITE_EIO = 7
 FLITE_FP64 = 0
 FLITE_MIXED = 1
+FLITE_RECON_NONE = 0
+FLITE_RECON_VAN_ALBADA = 1
 
 _d, _i = ctypes.c_double, ctypes.c_int
 
@@ -50,7 +52,7 @@ _CONTROL_FIELDS = [
     ("numberOfPSSteps", _i), ("residualSmoothingFactor", _d),
     ("prolongationSmoothingFactor", _d), ("physicalTimeStep", _d), ("engineBCRelaxation", _d),
     ("inflowField", _d * 12),
-    ("precision", _i),
+    ("precision", _i), ("reconstruction", _i), ("rungeKuttaStages", _i),
 ]
 
 

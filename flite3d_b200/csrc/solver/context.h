@@ -222,7 +222,11 @@ struct flite_ctx {
     // the anchor state, otherwise the FP32 increments over it
     void rhs_terms(int l, bool anchor = true) {
         const LevelView &L = V(l);
-        if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
+        if (c.reconstruction == FLITE_RECON_VAN_ALBADA && L.grid == 1) {
+            // the extension reconstructs from the Galerkin gradients
+            counted();
+            k_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
+        } else if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
             counted();
             if (c.GradientMethod == 1) k_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
             else k_ls_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
@@ -256,7 +260,10 @@ struct flite_ctx {
         const unsigned ng = eblk(L.E);
         switch (c.fluxType) {
             case 2: k_edge_flux<2, false><<<ng, eb, 0, s>>>(P, L); break;
-            case 3: k_edge_flux<3, false><<<ng, eb, 0, s>>>(P, L); break;
+            case 3:
+                if (P.recon == FLITE_RECON_VAN_ALBADA) k_edge_flux<3, true><<<ng, eb, 0, s>>>(P, L);
+                else k_edge_flux<3, false><<<ng, eb, 0, s>>>(P, L);
+                break;
             case 4:
                 if (c.HLLCFluxOrder > 1) k_edge_flux<4, true><<<ng, eb, 0, s>>>(P, L);
                 else k_edge_flux<4, false><<<ng, eb, 0, s>>>(P, L);
@@ -303,9 +310,9 @@ struct flite_ctx {
                 sa_diffusion(l);
             }
         }
-        for (int st = 1; st <= 3; ++st) {
+        for (int st = 1; st <= P.nstage; ++st) {
             // u == uprev at stage 1: the FP64 evaluation there is the anchor
-            // of the mixed-precision increments of stages 2 and 3
+            // of the mixed-precision increments of the later stages
             pressure(l);
             rhs_terms(l, st == 1);
             sa_stage(l, MODE_STAGE, st);

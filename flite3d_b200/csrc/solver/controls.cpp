@@ -87,6 +87,8 @@ extern "C" int flite_controls_default(flite_controls *c) {
     c->datum[0] = c->datum[1] = c->datum[2] = 0.0;
     c->numberOfProcesses = 1;
     c->precision = FLITE_FP64;
+    c->reconstruction = FLITE_RECON_NONE;
+    c->rungeKuttaStages = 3;
     return FLITE_OK;
 }
 

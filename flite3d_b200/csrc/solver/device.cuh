@@ -16,7 +16,11 @@ struct Params {
     double gamma, gm1, CFL, maxInc, minRho, Re, am, k2, k4, cgdf, pts, Tinf, mach;
     double mgBCRelax, prolRelax, clip, Pr;
     double inf[12];
-    double RK[3];
+    // stage coefficients: the reference's three (def_par:14240-14244) or the
+    // five of the extension; recon selects the MUSCL reconstruction of the
+    // Roe flux (an extension, level 1 only)
+    double RK[5];
+    int nstage, recon;
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
     // unsteady dual time (flowType 1): the physical time step and the
     // second-order backward difference on level 1 (timeScheme 2)

@@ -71,6 +71,11 @@ const char *unsupported_reason(const flite_controls &c) {
     if (c.prolongationMappingScheme != 1) return "prolongationMappingScheme must be 1";
     if (c.precision != FLITE_FP64 && c.precision != FLITE_MIXED) return "precision must be FLITE_FP64 or FLITE_MIXED";
     if (c.precision == FLITE_MIXED && c.fluxType != 1) return "FLITE_MIXED supports the central flux (fluxType 1)";
+    if (c.rungeKuttaStages != 3 && c.rungeKuttaStages != 5) return "rungeKuttaStages must be 3 or 5";
+    if (c.reconstruction != FLITE_RECON_NONE && c.reconstruction != FLITE_RECON_VAN_ALBADA)
+        return "reconstruction must be FLITE_RECON_NONE or FLITE_RECON_VAN_ALBADA";
+    if (c.reconstruction == FLITE_RECON_VAN_ALBADA && c.fluxType != 3)
+        return "the Van Albada reconstruction acts on the Roe flux (fluxType 3)";
     int s = c.multigridScheme;
     if (!(s <= 0 || (s >= 1 && s <= 5) || s == 7)) return "multigridScheme not implemented";
     return nullptr;
@@ -115,7 +120,14 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         P.mach = c->MachNumber; P.mgBCRelax = c->multigridBCRelaxation; P.prolRelax = c->prolongationRelaxation;
         P.clip = c->HLLCClipping; P.Pr = c->PrandtlNumber;
         for (int i = 0; i < 12; ++i) P.inf[i] = c->inflowField[i];
-        P.RK[0] = 0.6; P.RK[1] = 0.6; P.RK[2] = 1.0;  // def_par:14240-14244
+        if (c->rungeKuttaStages == 5) {  // extension: no reference counterpart
+            P.RK[0] = 0.25; P.RK[1] = 1. / 6.; P.RK[2] = 0.375; P.RK[3] = 0.5; P.RK[4] = 1.0;
+        } else {
+            P.RK[0] = 0.6; P.RK[1] = 0.6; P.RK[2] = 1.0;  // def_par:14240-14244
+            P.RK[3] = P.RK[4] = 0.0;
+        }
+        P.nstage = c->rungeKuttaStages;
+        P.recon = c->reconstruction;
         P.fluxType = c->fluxType; P.hllcOrder = c->HLLCFluxOrder; P.autoClip = c->Automaticlipping;
         P.nsig = c->ReynoldsNumber < 1 ? 4 : 2;       // def_par:1592-1596
         P.isentropic = c->wallsAreIsentropic; P.viscous = c->ReynoldsNumber > 0.0;
@@ -305,7 +317,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L.turbDiff = L.dtT = L.vort = L.divg = L.sag = L.sanh = nullptr;
             }
             for (double *a : {L.p, L.dt, L.mu, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
-            const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
+            const bool hllc2 = ((c->fluxType == 4 && c->HLLCFluxOrder > 1) ||
+                                c->reconstruction == FLITE_RECON_VAN_ALBADA) && l == 0;
             const bool visc = c->ReynoldsNumber > 0.0;
             L.q = X.alloc<NodeRec>(N);
             CK(cudaMemset(L.q, 0, (size_t)N * sizeof(NodeRec)));

@@ -75,9 +75,18 @@ __device__ __forceinline__ void central_flux_rec(const NodeRec &a, const NodeRec
     f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
 }
 
+// The Van Albada limited slope of the upwind-biased difference a and the
+// edge difference b (an extension, no reference counterpart): ab(a+b) /
+// (a^2+b^2) when a and b have the same sign, else 0.
+__device__ __forceinline__ double van_albada(double a, double b) {
+    const double ab = a * b;
+    if (ab <= 0.0) return 0.0;
+    return (ab * (a + b)) / (a * a + b * b);
+}
+
 // Interior edge flux f of edge e (i1 -> i2), added to rhs(i1) and
 // subtracted from rhs(i2).  FT is the fluxType and O2 selects the HLLC
-// reconstruction; both are compile-time so that each kernel instance only
+// reconstruction (or, with the Roe flux, the MUSCL / Van Albada extension); both are compile-time so that each kernel instance only
 // holds the registers of its own flux.
 template <int FT, bool O2>
 __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, int e, int i1, int i2, double *f) {
@@ -120,6 +129,34 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         return;
     }
     if constexpr (FT == 3) {  // Roe (def_par:1725-1792)
+        if constexpr (O2) {
+            // the upwind MUSCL / Van Albada extension (no reference
+            // counterpart): states reconstructed on level 1 only, where
+            // coordinates and gradients exist
+            if (L.grid == 1) {
+                const int N = L.N;
+                const double dx = L.cx[i2] - L.cx[i1], dy = L.cy[i2] - L.cy[i1], dz = L.cz[i2] - L.cz[i1];
+                const double q1[5] = {r1, u1, v1, w1, E1}, q2[5] = {r2, u2, v2, w2, E2};
+                double qa[5], qb[5];
+#pragma unroll
+                for (int j = 0; j < 5; ++j) {
+                    const double dq = q2[j] - q1[j];
+                    const double g1 = (L.grad[j * N + i1] * dx + L.grad[(j + 5) * N + i1] * dy) + L.grad[(j + 10) * N + i1] * dz;
+                    const double g2 = (L.grad[j * N + i2] * dx + L.grad[(j + 5) * N + i2] * dy) + L.grad[(j + 10) * N + i2] * dz;
+                    qa[j] = q1[j] + 0.5 * van_albada(2.0 * g1 - dq, dq);
+                    qb[j] = q2[j] - 0.5 * van_albada(2.0 * g2 - dq, dq);
+                }
+                const double pa = gam1 * (qa[4] - 0.5 * ((qa[1] * qa[1] + qa[2] * qa[2]) + qa[3] * qa[3]) * qa[0]);
+                const double pb = gam1 * (qb[4] - 0.5 * ((qb[1] * qb[1] + qb[2] * qb[2]) + qb[3] * qb[3]) * qb[0]);
+                if (qa[0] > 0.0 && qb[0] > 0.0 && pa > 0.0 && pb > 0.0) {
+                    r1 = qa[0]; rinv1 = 1. / r1; ru1 = r1 * qa[1]; rv1 = r1 * qa[2]; rw1 = r1 * qa[3];
+                    E1 = qa[4]; pr1 = pa; rh1 = E1 + pr1;
+                    r2 = qb[0]; rinv2 = 1. / r2; ru2 = r2 * qb[1]; rv2 = r2 * qb[2]; rw2 = r2 * qb[3];
+                    E2 = qb[4]; pr2 = pb; rh2 = E2 + pr2;
+                    u2 = rinv2 * ru2; v2 = rinv2 * rv2; w2 = rinv2 * rw2;
+                }
+            }
+        }
         double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
         if (rnorm > 1.0e-10) {
             double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
@@ -140,6 +177,11 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
             double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
             double ucp = (ui * rnx + vi * rny) + wi * rnz;
             double du1 = r1 - r2, du2 = ru1 - ru2, du3 = rv1 - rv2, du4 = rw1 - rw2, du5 = E1 - E2;
+            if constexpr (O2) {
+                // the extension adds the Roe dissipation with the upwind
+                // sign; the reference's interior branch subtracts it
+                du1 = r2 - r1; du2 = ru2 - ru1; du3 = rv2 - rv1; du4 = rw2 - rw1; du5 = E2 - E1;
+            }
             double l1 = fabs(ucp + ci), l2 = fabs(ucp - ci), l3 = fabs(ucp);
             double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
             double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);

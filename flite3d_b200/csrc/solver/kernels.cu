@@ -684,6 +684,7 @@ __global__ void __launch_bounds__(256) k_edge_flux(Params P, LevelView L) {
 template __global__ void k_edge_flux<1, false>(Params, LevelView);
 template __global__ void k_edge_flux<2, false>(Params, LevelView);
 template __global__ void k_edge_flux<3, false>(Params, LevelView);
+template __global__ void k_edge_flux<3, true>(Params, LevelView);
 template __global__ void k_edge_flux<4, false>(Params, LevelView);
 template __global__ void k_edge_flux<4, true>(Params, LevelView);
 

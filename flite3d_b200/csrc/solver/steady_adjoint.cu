@@ -1226,7 +1226,8 @@ void destroy_steady_adjoint(SteadyAdjoint *a) { delete a; }
 static const char *steady_adjoint_unsupported(const flite_ctx &X) {
     const flite_controls &c = X.c;
     if (c.fluxType != 1) return "the steady adjoint takes the central flux (fluxType 1)";
-
+    if (c.flowType != 0) return "the steady adjoint takes steady runs (flowType 0)";
+    if (c.rungeKuttaStages != 3) return "the steady adjoint takes the reference's three stages";
     if (c.turbulenceModel != 0) return "the steady adjoint covers inviscid and laminar runs (no turbulence model)";
     if (c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";
     if (c.useDissipationWeighting) return "the steady adjoint takes unweighted dissipation";

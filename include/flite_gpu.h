@@ -87,7 +87,27 @@ typedef struct flite_controls {
     double inflowField[12];
     /* extension controls (no reference counterpart) */
     int    precision;           /* FLITE_FP64 | FLITE_MIXED                   */
+    int    reconstruction;      /* FLITE_RECON_NONE | FLITE_RECON_VAN_ALBADA  */
+    int    rungeKuttaStages;    /* 3 (the reference's 0.6, 0.6, 1) or 5       */
 } flite_controls;
+
+/*
+ * The upwind extension (no reference counterpart).  FLITE_RECON_VAN_ALBADA
+ * makes the Roe flux (fluxType 3) upwind on every level (the reference's
+ * interior branch, def_par:1725-1792, subtracts its dissipation; the
+ * extension adds it) and second order on level 1: the states of an
+ * edge i1 -> i2 are reconstructed in (rho, u, v, w, rho E) from the Galerkin
+ * node gradients (computeGradient, def_par:2923-3245) with the Van Albada
+ * limiter,
+ *     q_L = q1 + va(2 g1.d - dq, dq) / 2,   q_R = q2 - va(2 g2.d - dq, dq) / 2,
+ *     va(a, b) = ab (a + b) / (a^2 + b^2) if ab > 0, else 0,
+ * d = x2 - x1, dq = q2 - q1; an edge whose reconstructed density or pressure
+ * is not positive keeps its first-order states.  Coarse levels stay first
+ * order.  rungeKuttaStages 5 runs the stages with the coefficients
+ * 1/4, 1/6, 3/8, 1/2, 1 in place of the reference's three.
+ */
+#define FLITE_RECON_NONE        0
+#define FLITE_RECON_VAN_ALBADA  1
 
 /*
  * One grid level as read from a gen3d .sol file (readGridComputationData,

@@ -151,12 +151,28 @@ void for_nodes(int n, F &&f) {
     for (int i = 0; i < n; ++i) f(i);
 }
 
+// the Van Albada limited slope of the upwind-biased difference a and the
+// edge difference b (an extension, no reference counterpart)
+static inline double van_albada(double a, double b) {
+    const double ab = a * b;
+    if (ab <= 0.0) return 0.0;
+    return (ab * (a + b)) / (a * a + b * b);
+}
+
 struct Oracle {
     flite_controls c;
     std::vector<Level> lv;
     int nvar = 5;
     std::vector<vec> nh;  // nodeHelpArray(:,1:25), sized for level 1
-    double RK[3] = {0.6, 0.6, 1.0};  // def_par:14240-14244
+    double RK[5] = {0.6, 0.6, 1.0, 0.0, 0.0};  // def_par:14240-14244
+    int nstage = 3;
+    // the five-stage extension (no reference counterpart)
+    void set_stages(int n) {
+        nstage = n;
+        if (n == 5) {
+            RK[0] = 0.25; RK[1] = 1. / 6.; RK[2] = 0.375; RK[3] = 0.5; RK[4] = 1.0;
+        }
+    }
 
     // ---- makePressureField (def_par:13612-13630) --------------------------
     void makePressureField(Level &g, vec *u) {
@@ -591,6 +607,11 @@ struct Oracle {
                 if (autoClip == 1) LocalMinMax(g);
             }
         }
+        // the upwind MUSCL / Van Albada extension of the Roe flux (no
+        // reference counterpart): Galerkin gradients, level 1 only
+        const bool upwind = c.fluxType == 3 && c.reconstruction == FLITE_RECON_VAN_ALBADA;
+        const bool muscl = upwind && g.grid == 1;
+        if (muscl) computeGradient(g, g.u);
         for_edges(g, [&](int e) {
             const int i1 = g.s1[e], i2 = g.s2[e];
             double pr1 = g.p[i1], r1 = g.u[0][i1], rinv1 = 1. / g.u[0][i1];
@@ -634,6 +655,29 @@ struct Oracle {
                     f[4] = rnorm * ((f51 + f52) - lam * du[4]);
                 }
             } else if (c.fluxType == 3) {  // Roe (def_par:1725-1792)
+                if (muscl) {
+                    const double dx = g.cx[i2] - g.cx[i1], dy = g.cy[i2] - g.cy[i1], dz = g.cz[i2] - g.cz[i1];
+                    const double q1[5] = {r1, u1, v1, w1, E1}, q2[5] = {r2, u2, v2, w2, E2};
+                    double qa[5], qb[5];
+                    for (int j = 0; j < 5; ++j) {
+                        const double dq = q2[j] - q1[j];
+                        const double g1 = (nh[j][i1] * dx + nh[j + 5][i1] * dy) + nh[j + 10][i1] * dz;
+                        const double g2 = (nh[j][i2] * dx + nh[j + 5][i2] * dy) + nh[j + 10][i2] * dz;
+                        qa[j] = q1[j] + 0.5 * van_albada(2.0 * g1 - dq, dq);
+                        qb[j] = q2[j] - 0.5 * van_albada(2.0 * g2 - dq, dq);
+                    }
+                    const double pa = gam1 * (qa[4] - 0.5 * ((qa[1] * qa[1] + qa[2] * qa[2]) + qa[3] * qa[3]) * qa[0]);
+                    const double pb = gam1 * (qb[4] - 0.5 * ((qb[1] * qb[1] + qb[2] * qb[2]) + qb[3] * qb[3]) * qb[0]);
+                    // an edge with a non-positive reconstructed density or
+                    // pressure keeps its first-order states
+                    if (qa[0] > 0.0 && qb[0] > 0.0 && pa > 0.0 && pb > 0.0) {
+                        r1 = qa[0]; rinv1 = 1. / r1; ru1 = r1 * qa[1]; rv1 = r1 * qa[2]; rw1 = r1 * qa[3];
+                        E1 = qa[4]; pr1 = pa; rh1 = E1 + pr1;
+                        r2 = qb[0]; rinv2 = 1. / r2; ru2 = r2 * qb[1]; rv2 = r2 * qb[2]; rw2 = r2 * qb[3];
+                        E2 = qb[4]; pr2 = pb; rh2 = E2 + pr2;
+                        u2 = rinv2 * ru2; v2 = rinv2 * rv2; w2 = rinv2 * rw2;
+                    }
+                }
                 double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
                 if (rnorm > 1.0e-10) {
                     double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
@@ -654,6 +698,11 @@ struct Oracle {
                     double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
                     double ucp = (ui * rnx + vi * rny) + wi * rnz;
                     double du1 = r1 - r2, du2 = ru1 - ru2, du3 = rv1 - rv2, du4 = rw1 - rw2, du5 = E1 - E2;
+                    if (upwind) {
+                        // the extension adds the Roe dissipation with the
+                        // upwind sign; the reference's branch subtracts it
+                        du1 = r2 - r1; du2 = ru2 - ru1; du3 = rv2 - rv1; du4 = rw2 - rw1; du5 = E2 - E1;
+                    }
                     double l1 = std::fabs(ucp + ci), l2 = std::fabs(ucp - ci), l3 = std::fabs(ucp);
                     double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
                     double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
@@ -1286,7 +1335,7 @@ struct Oracle {
                 }
             }
         }
-        for (int st = 1; st <= 3; ++st) {
+        for (int st = 1; st <= nstage; ++st) {
             makePressureField(g, g.u);
             for (int k = 0; k < nvar; ++k) std::fill(g.rhs[k].begin(), g.rhs[k].end(), 0.0);
             makeRHS(g);
@@ -1600,7 +1649,7 @@ struct Oracle {
 };
 
 int check_controls(const flite_controls &c) {
-    // flowType 1: dual time on a static mesh, without a turbulence model
+    // flowType 1: dual time on a static mesh
     if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return FLITE_EUNSUPPORTED;
     if ((c.flowType != 0 && c.flowType != 1) || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
         c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
@@ -1619,6 +1668,10 @@ int check_controls(const flite_controls &c) {
     if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
     if (c.useMatrixDissipation) return FLITE_EUNSUPPORTED;
     if (c.prolongationMappingScheme != 1) return FLITE_EUNSUPPORTED;
+    // the upwind extension (no reference counterpart)
+    if (c.rungeKuttaStages != 3 && c.rungeKuttaStages != 5) return FLITE_EUNSUPPORTED;
+    if (c.reconstruction != FLITE_RECON_NONE && c.reconstruction != FLITE_RECON_VAN_ALBADA) return FLITE_EUNSUPPORTED;
+    if (c.reconstruction == FLITE_RECON_VAN_ALBADA && c.fluxType != 3) return FLITE_EUNSUPPORTED;
     return FLITE_OK;
 }
 
@@ -2218,6 +2271,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
     auto ctx = std::make_unique<oracle_ctx>();
     Oracle &o = ctx->o;
     o.c = *c;
+    o.set_stages(c->rungeKuttaStages);
     o.nvar = c->turbulenceModel == 1 ? 6 : 5;
     int G = nlevels;
     if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);
@@ -2556,7 +2610,8 @@ int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const
                          double *mu_out, double *dmu_out) {
     if (!o || !u || !du || !v || !dv) return FLITE_EINVAL;
     const flite_controls &c = o->o.c;
-    if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 3 || c.useDissipationWeighting)
+    if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 3 || c.useDissipationWeighting ||
+        c.flowType != 0 || c.rungeKuttaStages != 3)
         return FLITE_EUNSUPPORTED;
     const bool visc = c.ReynoldsNumber > 0;
     if (visc && (!mu || !mu_out || !dmu_out)) return FLITE_EINVAL;

@@ -38,6 +38,16 @@ CASES = {
                                CFLNumber=0.5),
     "laminar_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1,
                           ReynoldsNumber=5000.0, wallsAreIsentropic=1),
+    # the upwind MUSCL / Van Albada extension and the five-stage scheme (no
+    # reference counterpart): the GPU against the same extension on the CPU
+    "roe_muscl_va_rk5": dict(fluxType=3, reconstruction=1, rungeKuttaStages=5,
+                             secondOrderDissipationFactor=0.0, fourthOrderDissipationFactor=0.0),
+    "roe_muscl_va_jst": dict(fluxType=3, reconstruction=1),
+    "central_rk5": dict(fluxType=1, rungeKuttaStages=5),
+    "laminar_roe_muscl_va_rk5": dict(fluxType=3, reconstruction=1, rungeKuttaStages=5,
+                                     secondOrderDissipationFactor=0.0,
+                                     fourthOrderDissipationFactor=0.0, ReynoldsNumber=5000.0,
+                                     wallsAreIsentropic=1),
 }
 SCHEMES = [0, 1, 2, 4, 5, 7]
 
@@ -68,9 +78,11 @@ def mesh():
     return Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
 
 
-@pytest.mark.parametrize("flux", [1, 2, 3, 4])
-def test_residual_bitwise(mesh, flux):
-    extra = dict(HLLCFluxOrder=2, Automaticlipping=1) if flux == 4 else {}
+@pytest.mark.parametrize("flux,extra", [
+    (1, {}), (2, {}), (3, {}), (4, dict(HLLCFluxOrder=2, Automaticlipping=1)),
+    (3, dict(reconstruction=1)),
+])
+def test_residual_bitwise(mesh, flux, extra):
     c, g, o = make_pair(mesh, fluxType=flux, **extra)
     u = initial_state(c, mesh, perturb_seed=7, amplitude=0.05)
     u[1] *= 1.0 + 0.02 * np.sin(np.arange(u.shape[1]))
@@ -171,7 +183,8 @@ def test_launch_options_do_not_change_results(opts):
 
 
 @pytest.mark.parametrize("lanes", [1, 4, 8, 16, 32])
-@pytest.mark.parametrize("name", ["central_jst", "hllc2_autoclip", "laminar_adiabatic", "first_order_diss"])
+@pytest.mark.parametrize("name", ["central_jst", "hllc2_autoclip", "laminar_adiabatic", "first_order_diss",
+                                  "roe_muscl_va_rk5"])
 def test_gather_lanes_match(name, lanes):
     # every gather shape (a thread, or a group of 4..32 lanes, per node) on
     # every level gives the reference's sums
