@@ -356,7 +356,7 @@ def time_to_converge(F, mesh, c, u0, max_cycles, options=None):
     return out
 
 
-def cpu_baseline(mesh, c, u0, cycles=2):
+def cpu_baseline(mesh, c, u0, cycles=2, sample_of="the same 2.1M-node workload"):
     """The CPU restatement (oracle/) timed on the host: a bounded sample of the
     same workload (a few cycles of the same mesh and controls)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -383,7 +383,7 @@ def cpu_baseline(mesh, c, u0, cycles=2):
     o.close()
     return {"value": cycles / dt, "unit": "cycles/s", "cores": threads, "kind": "port",
             "single_thread": {"value": 1.0 / dt1, "cycles": 1},
-            "sample": f"{cycles} cycles of the same 2.1M-node workload after one warm-up cycle, "
+            "sample": f"{cycles} cycles of {sample_of} after one warm-up cycle, "
                       f"FP64 C++ restatement on {threads} threads (edge loops over coloured "
                       "blocks of edges)"}
 
@@ -466,6 +466,72 @@ def run_rans(args):
                    "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides, "levels": mesh.nlevels,
                    "mesh_build_s": round(t_mesh, 2)},
         "residuals_after": [float(x) for x in res], "gpu_launches": s.cycle_launches() * args.steps,
+    }), flush=True)
+
+
+UPWIND = dict(ReynoldsNumber=0.0, MachNumber=0.5, alpha=0.0, CFLNumber=2.0, fluxType=3, reconstruction=1,
+              rungeKuttaStages=5, secondOrderDissipationFactor=0.0, fourthOrderDissipationFactor=0.0,
+              multigridScheme=3, numberOfGridsToUse=3)
+
+
+def run_upwind(args):
+    """The bump-channel Euler case with the upwind extension (no reference
+    counterpart): Roe flux with MUSCL reconstruction from the Galerkin
+    gradients and the Van Albada limiter on level 1, five stages
+    (1/4, 1/6, 3/8, 1/2, 1), CFL 2, M 0.5, 3 agglomerated levels, seeded
+    +-1% density start.  One JSON line: MG cycles/s (device time of
+    graph-replayed cycles), the wall time to an 8-order residual drop, and
+    the CPU restatement of the same extension timed on the host."""
+    import torch
+    import flite3d_b200 as F
+    if not torch.cuda.is_available():
+        raise SystemExit("no CUDA device: the product path has no CPU fallback")
+    nx, ny, nz = [int(v) for v in args.upwind_mesh.split(",")]
+    mesh = F.Mesh.bump_channel(nx, ny, nz, 0.05, nlevels=3)
+    c = F.default_controls(**UPWIND)
+    u0 = F.initial_state(c, mesh, perturb_seed=20261203, amplitude=0.01)
+    s = F.Solver(c, mesh)
+    s.set_state(u0)
+    s.start()
+    for i in range(1, args.warmup + 1):
+        s.cycle(i)
+    torch.cuda.synchronize()
+    ms = s.time_cycles(args.steps, cycle_no=args.warmup + 1)
+    launches = s.cycle_launches() * args.steps
+    s.close()
+    # time to converge: res1 down 8 orders (numberOfMGIterations = -8)
+    s = F.Solver(c, mesh)
+    s.set_state(u0)
+    s.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r0 = r = None
+    cyc = 0
+    for cyc in range(1, args.converge_max + 1):
+        s.cycle(cyc)
+        r = s.residuals()[0][0]
+        r0 = r0 or r
+        if r <= 1e-8 * r0:
+            break
+    secs = time.perf_counter() - t0
+    f = s.forces()
+    s.close()
+    d = mesh.level(1)
+    name = f"{nx}x{ny}x{nz} hex -> 6 tets ({d.n_nodes:,} nodes, {d.n_sides:,} edges)"
+    cpu = None if args.no_cpu_baseline else cpu_baseline(mesh, c, u0, cycles=args.cpu_cycles,
+                                                          sample_of=f"the same {d.n_nodes:,}-node upwind workload")
+    print(json.dumps({
+        "metric": METRIC, "value": args.steps / (ms / 1e3), "unit": "cycles/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated bump channel, seeded +-1% density)",
+        "config": {"workload": "inviscid Euler, M 0.5, CFL 2, on the bump channel " + name + ", 3 agglomerated "
+                               "MG levels, growing V-cycle; the upwind extension (no reference counterpart): "
+                               "Roe flux, MUSCL from Galerkin gradients with the Van Albada limiter on level 1, "
+                               "5 stages (1/4, 1/6, 3/8, 1/2, 1)",
+                   "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides, "levels": mesh.nlevels},
+        "converge": {"seconds": secs, "cycles": cyc, "reached": bool(r <= 1e-8 * r0),
+                     "log10_reduction": float(math.log10(r / r0)), "CL": float(f[0]), "CD": float(f[1])},
+        "cpu_baseline": cpu, "gpu_launches": launches,
     }), flush=True)
 
 
@@ -666,6 +732,10 @@ def main():
     ap.add_argument("--adjoint-primal-cycles", type=int, default=6000)
     ap.add_argument("--adjoint-max-iter", type=int, default=400000,
                     help="products with the transposed iteration Jacobian per adjoint solve")
+    ap.add_argument("--upwind", action="store_true",
+                    help="the bump-channel Euler case with the upwind Roe / MUSCL / Van Albada, five-stage "
+                         "extension instead")
+    ap.add_argument("--upwind-mesh", default="48,16,16", help="NX,NY,NZ hexes of the upwind workload")
     ap.add_argument("--batch-meshes", type=int, default=3)
     ap.add_argument("--batch-conditions", type=int, default=16)
     args = ap.parse_args()
@@ -681,6 +751,8 @@ def main():
         run_rans(args)
     elif args.adjoint:
         run_adjoint(args)
+    elif args.upwind:
+        run_upwind(args)
     else:
         run_ours(args)
 

@@ -223,9 +223,12 @@ struct flite_ctx {
     void rhs_terms(int l, bool anchor = true) {
         const LevelView &L = V(l);
         if (c.reconstruction == FLITE_RECON_VAN_ALBADA && L.grid == 1) {
-            // the extension reconstructs from the Galerkin gradients
+            // the extension reconstructs from the Galerkin gradients, through
+            // the primitive and gradient records
             counted();
-            k_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
+            k_prim_rec<<<nblk(L.N), nb, 0, s>>>(L);
+            counted();
+            k_gradient_rec<<<nblk(L.N), nb, 0, s>>>(L);
         } else if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
             counted();
             if (c.GradientMethod == 1) k_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
@@ -261,7 +264,10 @@ struct flite_ctx {
         switch (c.fluxType) {
             case 2: k_edge_flux<2, false><<<ng, eb, 0, s>>>(P, L); break;
             case 3:
-                if (P.recon == FLITE_RECON_VAN_ALBADA) k_edge_flux<3, true><<<ng, eb, 0, s>>>(P, L);
+                // the extension: MUSCL on level 1, upwind first order below
+                if (P.recon == FLITE_RECON_VAN_ALBADA && L.grid == 1)  // 256 threads: its store staging
+                    k_edge_flux_muscl<<<(unsigned)((L.E + 255) / 256), 256, 0, s>>>(P, L);
+                else if (P.recon == FLITE_RECON_VAN_ALBADA) k_edge_flux<3, true><<<ng, eb, 0, s>>>(P, L);
                 else k_edge_flux<3, false><<<ng, eb, 0, s>>>(P, L);
                 break;
             case 4:

@@ -50,6 +50,18 @@ struct __align__(16) DeltaRec {  // FP32 anchor primitives and increments (48 B)
     float dr, dmx, dmy, dmz, dE, dp, pad;  // u - ua and p - pa
 };
 
+// Level-1 records of the upwind extension (no reference counterpart): the
+// primitives of the Galerkin gradient with the node's coordinates (64 B, two
+// sectors), and that gradient, component-major (g[3c + a] = d q_c / d x_a,
+// 128 B), so that an edge end costs six sectors instead of twenty-four SoA
+// ones and no divisions.
+struct __align__(16) PrimRec {
+    double r, u, v, w, E, x, y, z;  // rho, (rho u)/rho, ..., rho E, coordinates
+};
+struct __align__(16) GradRec {
+    double g[16];  // 15 used
+};
+
 // A level's mesh and state on the device.  Node-indexed arrays are SoA
 // ([component][node]), like the reference's column-major u(N,nvar).
 struct LevelView {
@@ -97,6 +109,8 @@ struct LevelView {
     double *vdt;                           // [N]  V/dt of the dissipation
     double *wstress;                       // [3][N] wall stress (level 1)
     double *grad;                          // [15][N] (level 1, HLLC order 2)
+    PrimRec *qp;                           // [N] (level 1, upwind extension)
+    GradRec *gq;                           // [N] (level 1, upwind extension)
     double *bnd;                           // [10][N]
     double *flux;                          // [E][5] edge flux buffer
     // mixed precision (FLITE_MIXED): interior central fluxes as FP32
@@ -146,6 +160,7 @@ __device__ __forceinline__ void store_rec(R *base, int j, const R &o) {
     for (int k = 0; k < K; ++k) p[k] = d[k];
 }
 __device__ __forceinline__ NodeRec load_node(const NodeRec *q, int j) { return load_rec<NodeRec, 3>(q, j); }
+__device__ __forceinline__ PrimRec load_prim(const PrimRec *q, int j) { return load_rec<PrimRec, 4>(q, j); }
 // 1/rho and E + p are the operations the central flux performs per edge
 // end, done once per node
 __device__ __forceinline__ void store_node(NodeRec *q, int j, double r, double ru, double rv, double rw, double E,

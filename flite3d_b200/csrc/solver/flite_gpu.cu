@@ -317,8 +317,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L.turbDiff = L.dtT = L.vort = L.divg = L.sag = L.sanh = nullptr;
             }
             for (double *a : {L.p, L.dt, L.mu, L.hvis}) CK(cudaMemset(a, 0, (size_t)N * sizeof(double)));
-            const bool hllc2 = ((c->fluxType == 4 && c->HLLCFluxOrder > 1) ||
-                                c->reconstruction == FLITE_RECON_VAN_ALBADA) && l == 0;
+            const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
+            const bool muscl = c->reconstruction == FLITE_RECON_VAN_ALBADA && l == 0;
             const bool visc = c->ReynoldsNumber > 0.0;
             L.q = X.alloc<NodeRec>(N);
             CK(cudaMemset(L.q, 0, (size_t)N * sizeof(NodeRec)));
@@ -331,6 +331,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             CK(cudaMemset(L.wstress, 0, 3 * (size_t)N * sizeof(double)));
             L.grad = hllc2 ? X.alloc<double>(15 * (size_t)N) : nullptr;
             L.bnd = hllc2 ? X.alloc<double>(10 * (size_t)N) : nullptr;
+            L.qp = muscl ? X.alloc<PrimRec>(N) : nullptr;
+            L.gq = muscl ? X.alloc<GradRec>(N) : nullptr;
             // the edge buffer carries the upwind fluxes; the central flux is
             // computed inside the node gather
             L.flux = c->fluxType != 1 ? X.alloc<double>(5 * (size_t)std::max(E, 1)) : nullptr;

@@ -86,7 +86,7 @@ __device__ __forceinline__ double van_albada(double a, double b) {
 
 // Interior edge flux f of edge e (i1 -> i2), added to rhs(i1) and
 // subtracted from rhs(i2).  FT is the fluxType and O2 selects the HLLC
-// reconstruction (or, with the Roe flux, the MUSCL / Van Albada extension); both are compile-time so that each kernel instance only
+// reconstruction (with the Roe flux: the upwind sign of the extension); both are compile-time so that each kernel instance only
 // holds the registers of its own flux.
 template <int FT, bool O2>
 __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, int e, int i1, int i2, double *f) {
@@ -129,34 +129,6 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         return;
     }
     if constexpr (FT == 3) {  // Roe (def_par:1725-1792)
-        if constexpr (O2) {
-            // the upwind MUSCL / Van Albada extension (no reference
-            // counterpart): states reconstructed on level 1 only, where
-            // coordinates and gradients exist
-            if (L.grid == 1) {
-                const int N = L.N;
-                const double dx = L.cx[i2] - L.cx[i1], dy = L.cy[i2] - L.cy[i1], dz = L.cz[i2] - L.cz[i1];
-                const double q1[5] = {r1, u1, v1, w1, E1}, q2[5] = {r2, u2, v2, w2, E2};
-                double qa[5], qb[5];
-#pragma unroll
-                for (int j = 0; j < 5; ++j) {
-                    const double dq = q2[j] - q1[j];
-                    const double g1 = (L.grad[j * N + i1] * dx + L.grad[(j + 5) * N + i1] * dy) + L.grad[(j + 10) * N + i1] * dz;
-                    const double g2 = (L.grad[j * N + i2] * dx + L.grad[(j + 5) * N + i2] * dy) + L.grad[(j + 10) * N + i2] * dz;
-                    qa[j] = q1[j] + 0.5 * van_albada(2.0 * g1 - dq, dq);
-                    qb[j] = q2[j] - 0.5 * van_albada(2.0 * g2 - dq, dq);
-                }
-                const double pa = gam1 * (qa[4] - 0.5 * ((qa[1] * qa[1] + qa[2] * qa[2]) + qa[3] * qa[3]) * qa[0]);
-                const double pb = gam1 * (qb[4] - 0.5 * ((qb[1] * qb[1] + qb[2] * qb[2]) + qb[3] * qb[3]) * qb[0]);
-                if (qa[0] > 0.0 && qb[0] > 0.0 && pa > 0.0 && pb > 0.0) {
-                    r1 = qa[0]; rinv1 = 1. / r1; ru1 = r1 * qa[1]; rv1 = r1 * qa[2]; rw1 = r1 * qa[3];
-                    E1 = qa[4]; pr1 = pa; rh1 = E1 + pr1;
-                    r2 = qb[0]; rinv2 = 1. / r2; ru2 = r2 * qb[1]; rv2 = r2 * qb[2]; rw2 = r2 * qb[3];
-                    E2 = qb[4]; pr2 = pb; rh2 = E2 + pr2;
-                    u2 = rinv2 * ru2; v2 = rinv2 * rv2; w2 = rinv2 * rw2;
-                }
-            }
-        }
         double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
         if (rnorm > 1.0e-10) {
             double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
@@ -178,8 +150,8 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
             double ucp = (ui * rnx + vi * rny) + wi * rnz;
             double du1 = r1 - r2, du2 = ru1 - ru2, du3 = rv1 - rv2, du4 = rw1 - rw2, du5 = E1 - E2;
             if constexpr (O2) {
-                // the extension adds the Roe dissipation with the upwind
-                // sign; the reference's interior branch subtracts it
+                // the extension (coarse levels) adds the Roe dissipation with
+                // the upwind sign; the reference's interior branch subtracts it
                 du1 = r2 - r1; du2 = ru2 - ru1; du3 = rv2 - rv1; du4 = rw2 - rw1; du5 = E2 - E1;
             }
             double l1 = fabs(ucp + ci), l2 = fabs(ucp - ci), l3 = fabs(ucp);
@@ -416,6 +388,86 @@ __device__ __forceinline__ void boundary_flux(const Params &P, const LevelView &
             g2[k] = rnorm * 4. * F2[k];
         }
     }
+}
+
+
+// ---- the upwind extension on level 1 (no reference counterpart) -----------
+// Roe flux of the MUSCL / Van Albada states of edge e (i1 -> i2), from the
+// primitive and gradient records.  The states are (rho, u, v, w, rho E) with
+// u = (rho u)/rho, reconstructed as
+//     q_L = q1 + va(2 g1.d - dq, dq) / 2,  q_R = q2 - va(2 g2.d - dq, dq) / 2,
+// d = x2 - x1, dq = q2 - q1; an edge whose reconstructed density or pressure
+// is not positive takes the unreconstructed states.  p = (gamma-1)(rho E -
+// rho |u|^2 / 2) of each state; the Roe average and wave strengths are those
+// of the reference's Roe branch (def_par:1725-1792) with the dissipation
+// added with the upwind sign.
+__device__ __forceinline__ double prim_pressure(double gam1, const double *q) {
+    return gam1 * (q[4] - 0.5 * ((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3]) * q[0]);
+}
+__device__ __forceinline__ void edge_flux_muscl(const Params &P, const LevelView &L, int e, int i1, int i2,
+                                                double *f) {
+    const double gam1 = P.gm1;
+    const PrimRec A = load_prim(L.qp, i1), B = load_prim(L.qp, i2);
+    const double dx = B.x - A.x, dy = B.y - A.y, dz = B.z - A.z;
+    const double q1[5] = {A.r, A.u, A.v, A.w, A.E}, q2[5] = {B.r, B.u, B.v, B.w, B.E};
+    // g.d at each end, one gradient record (eight 16-byte loads) at a time
+    double g1[5], g2[5];
+    {
+        const GradRec G = load_rec<GradRec, 8>(L.gq, i1);
+#pragma unroll
+        for (int j = 0; j < 5; ++j) g1[j] = (G.g[3 * j] * dx + G.g[3 * j + 1] * dy) + G.g[3 * j + 2] * dz;
+    }
+    {
+        const GradRec G = load_rec<GradRec, 8>(L.gq, i2);
+#pragma unroll
+        for (int j = 0; j < 5; ++j) g2[j] = (G.g[3 * j] * dx + G.g[3 * j + 1] * dy) + G.g[3 * j + 2] * dz;
+    }
+    double qa[5], qb[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        const double dq = q2[j] - q1[j];
+        qa[j] = q1[j] + 0.5 * van_albada(2.0 * g1[j] - dq, dq);
+        qb[j] = q2[j] - 0.5 * van_albada(2.0 * g2[j] - dq, dq);
+    }
+    double pa = prim_pressure(gam1, qa), pb = prim_pressure(gam1, qb);
+    if (!(qa[0] > 0.0 && qb[0] > 0.0 && pa > 0.0 && pb > 0.0)) {
+#pragma unroll
+        for (int j = 0; j < 5; ++j) { qa[j] = q1[j]; qb[j] = q2[j]; }
+        pa = prim_pressure(gam1, qa);
+        pb = prim_pressure(gam1, qb);
+    }
+    f[0] = f[1] = f[2] = f[3] = f[4] = 0.0;
+    const EdgeW w = load_edgew(L.ew, e);
+    const double rnorm = sqrt((w.wx * w.wx + w.wy * w.wy) + w.wz * w.wz);
+    if (!(rnorm > 1.0e-10)) return;
+    const double rn = 1.0 / rnorm;
+    const double rnx = w.wx * rn, rny = w.wy * rn, rnz = w.wz * rn;
+    const double r1 = qa[0], u1 = qa[1], v1 = qa[2], w1 = qa[3], E1 = qa[4];
+    const double r2 = qb[0], u2 = qb[1], v2 = qb[2], w2 = qb[3], E2 = qb[4];
+    const double ru1 = r1 * u1, rv1 = r1 * v1, rw1 = r1 * w1, rh1 = E1 + pa;
+    const double ru2 = r2 * u2, rv2 = r2 * v2, rw2 = r2 * w2, rh2 = E2 + pb;
+    const double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+    const double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+    const double h1 = rh1 / r1, h2 = rh2 / r2;
+    const double di = sqrt(r1 / r2), d1 = 1.0 / (di + 1.0);
+    const double ui = (di * u1 + u2) * d1, vi = (di * v1 + v2) * d1, wi = (di * w1 + w2) * d1;
+    const double hi = (di * h1 + h2) * d1;
+    const double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+    const double ci2 = dmax(gam1 * (hi - af), 1.0e-5);
+    const double ci = sqrt(ci2), ici = 1.0 / ci, ici2 = 1.0 / ci2;
+    const double ucp = (ui * rnx + vi * rny) + wi * rnz;
+    const double du1 = r2 - r1, du2 = ru2 - ru1, du3 = rv2 - rv1, du4 = rw2 - rw1, du5 = E2 - E1;
+    const double l1 = fabs(ucp + ci), l2 = fabs(ucp - ci), l3 = fabs(ucp);
+    const double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+    const double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+    const double al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+    const double cc1 = (s1 - l3) * al1x * ici2 + s2 * al2x * ici;
+    const double cc2 = s2 * al1x * ici + (s1 - l3) * al2x;
+    f[0] = rnorm * ((r1 * nv1 + r2 * nv2) - (l3 * du1 + cc1));
+    f[1] = rnorm * (((pa * rnx + ru1 * nv1) + (pb * rnx + ru2 * nv2)) - ((l3 * du2 + cc1 * ui) + cc2 * rnx));
+    f[2] = rnorm * (((pa * rny + rv1 * nv1) + (pb * rny + rv2 * nv2)) - ((l3 * du3 + cc1 * vi) + cc2 * rny));
+    f[3] = rnorm * (((pa * rnz + rw1 * nv1) + (pb * rnz + rw2 * nv2)) - ((l3 * du4 + cc1 * wi) + cc2 * rnz));
+    f[4] = rnorm * ((rh1 * nv1 + rh2 * nv2) - ((l3 * du5 + cc1 * hi) + cc2 * ucp));
 }
 
 }  // namespace flite

@@ -598,6 +598,70 @@ __global__ void k_gradient(Params P, LevelView L) {
     for (int c = 0; c < 15; ++c) L.grad[c * N + i] = g[c] * vt;
 }
 
+// ---- the upwind extension's level-1 records (no reference counterpart) ----
+// primitives (rho, (rho u)/rho, ..., rho E) and coordinates of every node
+__global__ void k_prim_rec(LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double r = L.u[i];
+    PrimRec o;
+    o.r = r; o.u = L.u[N + i] / r; o.v = L.u[2 * N + i] / r; o.w = L.u[3 * N + i] / r; o.E = L.u[4 * N + i];
+    o.x = L.cx[i]; o.y = L.cy[i]; o.z = L.cz[i];
+    store_rec<PrimRec, 4>(L.qp, i, o);
+}
+// the Galerkin gradient of k_gradient (computeGradient, def_par:2923-3245),
+// in the same summation order, from the primitive records, stored as
+// component-major records
+__global__ void k_gradient_rec(LevelView L) {
+    int i = tid();
+    if (i >= L.N) return;
+    double g[15];
+#pragma unroll
+    for (int c = 0; c < 15; ++c) g[c] = 0.0;
+    const PrimRec Qi = load_prim(L.qp, i);
+    const double qi[5] = {Qi.r, Qi.u, Qi.v, Qi.w, Qi.E};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const int e = t.x >= 0 ? t.x : ~t.x;
+        const PrimRec Qj = load_prim(L.qp, t.y);
+        const double qj[5] = {Qj.r, Qj.u, Qj.v, Qj.w, Qj.E};
+        const EdgeW ew = load_edgew(L.ew, e);
+        const double w[3] = {ew.wx, ew.wy, ew.wz};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                const double sum = t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c];
+                const double dq = sum * w[a];
+                g[a * 5 + c] = t.x >= 0 ? g[a * 5 + c] + dq : g[a * 5 + c] - dq;
+            }
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        const int2 nd = L.bedge[b];
+        const PrimRec Q1 = load_prim(L.qp, nd.x), Q2 = load_prim(L.qp, nd.y);
+        const double q1[5] = {Q1.r, Q1.u, Q1.v, Q1.w, Q1.E}, q2[5] = {Q2.r, Q2.u, Q2.v, Q2.w, Q2.E};
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                const double sum = q1[c] + q2[c];
+                const double own = side == 0 ? q1[c] : q2[c];
+                g[a * 5 + c] = g[a * 5 + c] + (2. * own + sum) * w[a];
+            }
+    }
+    const double vt = 1. / L.V[i];
+    GradRec o;
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) o.g[3 * c + a] = g[a * 5 + c] * vt;
+    o.g[15] = 0.0;
+    store_rec<GradRec, 8>(L.gq, i, o);
+}
+
 // ---- LSComputeGradient + computegradhat (def_par:2593-2920) ---------------
 // the moment matrix is the same for the five scalars and is built once; the
 // right-hand sides of the five scalars are gathered in the same edge order
@@ -687,6 +751,28 @@ template __global__ void k_edge_flux<3, false>(Params, LevelView);
 template __global__ void k_edge_flux<3, true>(Params, LevelView);
 template __global__ void k_edge_flux<4, false>(Params, LevelView);
 template __global__ void k_edge_flux<4, true>(Params, LevelView);
+
+// the upwind extension's level-1 edge flux into the edge buffer; the block's
+// 256 x 5 fluxes are staged in shared memory and written as one contiguous
+// run of 16-byte stores
+__global__ void __launch_bounds__(256) k_edge_flux_muscl(Params P, LevelView L) {
+    __shared__ __align__(16) double sf[256 * 5];
+    const int e0 = blockIdx.x * 256, e = e0 + threadIdx.x;
+    if (e < L.E) {
+        const int2 nd = L.edge[e];
+        double f[5];
+        edge_flux_muscl(P, L, e, nd.x, nd.y, f);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sf[threadIdx.x * 5 + k] = f[k];
+    }
+    __syncthreads();
+    // e0 * 5 doubles is a multiple of 16 bytes (e0 is a multiple of 256)
+    const int n = 5 * min(256, L.E - e0);
+    double2 *o = reinterpret_cast<double2 *>(L.flux + (size_t)e0 * 5);
+    const double2 *src = reinterpret_cast<const double2 *>(sf);
+    for (int k = threadIdx.x; k < n / 2; k += 256) o[k] = src[k];
+    if ((n & 1) && threadIdx.x == 0) L.flux[(size_t)e0 * 5 + n - 1] = sf[n - 1];
+}
 
 // ---- boundary-edge contributions ------------------------------------------
 __global__ void k_bnd_flux(Params P, LevelView L) {

@@ -22,6 +22,9 @@ template <int U>
 __global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
+__global__ void k_prim_rec(LevelView L);
+__global__ void k_gradient_rec(LevelView L);
+__global__ void k_edge_flux_muscl(Params P, LevelView L);
 __global__ void k_ls_gradient(Params P, LevelView L);
 __global__ void k_minmax(Params P, LevelView L);
 template <int FT, bool O2>

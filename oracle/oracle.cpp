@@ -592,6 +592,69 @@ struct Oracle {
     }
 
     // ---- makeRHS (def_par:1525-2590) --------------------------------------
+    // ---- the upwind extension on level 1 (no reference counterpart) -------
+    // Roe flux of the MUSCL / Van Albada states of edge i1 -> i2: states
+    // (rho, (rho u)/rho, ..., rho E) reconstructed from the Galerkin gradient
+    // nh, q_L = q1 + va(2 g1.d - dq, dq)/2, q_R = q2 - va(2 g2.d - dq, dq)/2;
+    // unreconstructed states where a reconstructed density or pressure is
+    // not positive; p = (gamma-1)(rho E - rho |u|^2/2); the Roe average and
+    // wave strengths of def_par:1725-1792 with the upwind sign
+    static double prim_pressure(double gam1, const double *q) {
+        return gam1 * (q[4] - 0.5 * ((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3]) * q[0]);
+    }
+    void muscl_roe_flux(const Level &g, int i1, int i2, double wx, double wy, double wz, double *f) {
+        const double gam1 = c.gamma - 1.0;
+        const double ra = g.u[0][i1], rb = g.u[0][i2];
+        const double q1[5] = {ra, g.u[1][i1] / ra, g.u[2][i1] / ra, g.u[3][i1] / ra, g.u[4][i1]};
+        const double q2[5] = {rb, g.u[1][i2] / rb, g.u[2][i2] / rb, g.u[3][i2] / rb, g.u[4][i2]};
+        const double dx = g.cx[i2] - g.cx[i1], dy = g.cy[i2] - g.cy[i1], dz = g.cz[i2] - g.cz[i1];
+        double qa[5], qb[5];
+        for (int j = 0; j < 5; ++j) {
+            const double dq = q2[j] - q1[j];
+            const double g1 = (nh[j][i1] * dx + nh[j + 5][i1] * dy) + nh[j + 10][i1] * dz;
+            const double g2 = (nh[j][i2] * dx + nh[j + 5][i2] * dy) + nh[j + 10][i2] * dz;
+            qa[j] = q1[j] + 0.5 * van_albada(2.0 * g1 - dq, dq);
+            qb[j] = q2[j] - 0.5 * van_albada(2.0 * g2 - dq, dq);
+        }
+        double pa = prim_pressure(gam1, qa), pb = prim_pressure(gam1, qb);
+        if (!(qa[0] > 0.0 && qb[0] > 0.0 && pa > 0.0 && pb > 0.0)) {
+            for (int j = 0; j < 5; ++j) { qa[j] = q1[j]; qb[j] = q2[j]; }
+            pa = prim_pressure(gam1, qa);
+            pb = prim_pressure(gam1, qb);
+        }
+        for (int k = 0; k < 5; ++k) f[k] = 0.0;
+        const double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
+        if (!(rnorm > 1.0e-10)) return;
+        const double rn = 1.0 / rnorm;
+        const double rnx = wx * rn, rny = wy * rn, rnz = wz * rn;
+        const double r1 = qa[0], u1 = qa[1], v1 = qa[2], w1 = qa[3], E1 = qa[4];
+        const double r2 = qb[0], u2 = qb[1], v2 = qb[2], w2 = qb[3], E2 = qb[4];
+        const double ru1 = r1 * u1, rv1 = r1 * v1, rw1 = r1 * w1, rh1 = E1 + pa;
+        const double ru2 = r2 * u2, rv2 = r2 * v2, rw2 = r2 * w2, rh2 = E2 + pb;
+        const double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
+        const double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
+        const double h1 = rh1 / r1, h2 = rh2 / r2;
+        const double di = std::sqrt(r1 / r2), d1 = 1.0 / (di + 1.0);
+        const double ui = (di * u1 + u2) * d1, vi = (di * v1 + v2) * d1, wi = (di * w1 + w2) * d1;
+        const double hi = (di * h1 + h2) * d1;
+        const double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+        const double ci2 = std::max(gam1 * (hi - af), 1.0e-5);
+        const double ci = std::sqrt(ci2), ici = 1.0 / ci, ici2 = 1.0 / ci2;
+        const double ucp = (ui * rnx + vi * rny) + wi * rnz;
+        const double du1 = r2 - r1, du2 = ru2 - ru1, du3 = rv2 - rv1, du4 = rw2 - rw1, du5 = E2 - E1;
+        const double l1 = std::fabs(ucp + ci), l2 = std::fabs(ucp - ci), l3 = std::fabs(ucp);
+        const double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+        const double al1x = gam1 * ((((af * du1 - ui * du2) - vi * du3) - wi * du4) + du5);
+        const double al2x = ((-ucp * du1 + du2 * rnx) + du3 * rny) + du4 * rnz;
+        const double cc1 = (s1 - l3) * al1x * ici2 + s2 * al2x * ici;
+        const double cc2 = s2 * al1x * ici + (s1 - l3) * al2x;
+        f[0] = rnorm * ((r1 * nv1 + r2 * nv2) - (l3 * du1 + cc1));
+        f[1] = rnorm * (((pa * rnx + ru1 * nv1) + (pb * rnx + ru2 * nv2)) - ((l3 * du2 + cc1 * ui) + cc2 * rnx));
+        f[2] = rnorm * (((pa * rny + rv1 * nv1) + (pb * rny + rv2 * nv2)) - ((l3 * du3 + cc1 * vi) + cc2 * rny));
+        f[3] = rnorm * (((pa * rnz + rw1 * nv1) + (pb * rnz + rw2 * nv2)) - ((l3 * du4 + cc1 * wi) + cc2 * rnz));
+        f[4] = rnorm * ((rh1 * nv1 + rh2 * nv2) - ((l3 * du5 + cc1 * hi) + cc2 * ucp));
+    }
+
     void makeRHS(Level &g) {
         const double gam = c.gamma, gam1 = c.gamma - 1.0;
         int hllcflux = 1, autoClip = 0, nsig = 4;
@@ -654,30 +717,9 @@ struct Oracle {
                     f[3] = rnorm * ((f41 + f42) - lam * du[3]);
                     f[4] = rnorm * ((f51 + f52) - lam * du[4]);
                 }
+            } else if (c.fluxType == 3 && muscl) {
+                muscl_roe_flux(g, i1, i2, wx, wy, wz, f);
             } else if (c.fluxType == 3) {  // Roe (def_par:1725-1792)
-                if (muscl) {
-                    const double dx = g.cx[i2] - g.cx[i1], dy = g.cy[i2] - g.cy[i1], dz = g.cz[i2] - g.cz[i1];
-                    const double q1[5] = {r1, u1, v1, w1, E1}, q2[5] = {r2, u2, v2, w2, E2};
-                    double qa[5], qb[5];
-                    for (int j = 0; j < 5; ++j) {
-                        const double dq = q2[j] - q1[j];
-                        const double g1 = (nh[j][i1] * dx + nh[j + 5][i1] * dy) + nh[j + 10][i1] * dz;
-                        const double g2 = (nh[j][i2] * dx + nh[j + 5][i2] * dy) + nh[j + 10][i2] * dz;
-                        qa[j] = q1[j] + 0.5 * van_albada(2.0 * g1 - dq, dq);
-                        qb[j] = q2[j] - 0.5 * van_albada(2.0 * g2 - dq, dq);
-                    }
-                    const double pa = gam1 * (qa[4] - 0.5 * ((qa[1] * qa[1] + qa[2] * qa[2]) + qa[3] * qa[3]) * qa[0]);
-                    const double pb = gam1 * (qb[4] - 0.5 * ((qb[1] * qb[1] + qb[2] * qb[2]) + qb[3] * qb[3]) * qb[0]);
-                    // an edge with a non-positive reconstructed density or
-                    // pressure keeps its first-order states
-                    if (qa[0] > 0.0 && qb[0] > 0.0 && pa > 0.0 && pb > 0.0) {
-                        r1 = qa[0]; rinv1 = 1. / r1; ru1 = r1 * qa[1]; rv1 = r1 * qa[2]; rw1 = r1 * qa[3];
-                        E1 = qa[4]; pr1 = pa; rh1 = E1 + pr1;
-                        r2 = qb[0]; rinv2 = 1. / r2; ru2 = r2 * qb[1]; rv2 = r2 * qb[2]; rw2 = r2 * qb[3];
-                        E2 = qb[4]; pr2 = pb; rh2 = E2 + pr2;
-                        u2 = rinv2 * ru2; v2 = rinv2 * rv2; w2 = rinv2 * rw2;
-                    }
-                }
                 double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
                 if (rnorm > 1.0e-10) {
                     double rnx = wx / rnorm, rny = wy / rnorm, rnz = wz / rnorm;
@@ -699,8 +741,9 @@ struct Oracle {
                     double ucp = (ui * rnx + vi * rny) + wi * rnz;
                     double du1 = r1 - r2, du2 = ru1 - ru2, du3 = rv1 - rv2, du4 = rw1 - rw2, du5 = E1 - E2;
                     if (upwind) {
-                        // the extension adds the Roe dissipation with the
-                        // upwind sign; the reference's branch subtracts it
+                        // the extension (coarse levels) adds the Roe
+                        // dissipation with the upwind sign; the reference's
+                        // branch subtracts it
                         du1 = r2 - r1; du2 = ru2 - ru1; du3 = rv2 - rv1; du4 = rw2 - rw1; du5 = E2 - E1;
                     }
                     double l1 = std::fabs(ucp + ci), l2 = std::fabs(ucp - ci), l3 = std::fabs(ucp);
