@@ -170,7 +170,8 @@ struct flite_ctx {
         counted();
         FLITE_GATHER(k_jst_lap, l, P, L);
         counted();
-        FLITE_GATHER(k_jst_flux, l, P, L);
+        if (P.matrixDiss) k_jst_flux_matrix<<<nblk(L.N), nb, 0, s>>>(P, L);
+        else FLITE_GATHER(k_jst_flux, l, P, L);
     }
     void first_order_diss(int l) {
         counted();

@@ -21,6 +21,9 @@ struct Params {
     // Roe flux (an extension, level 1 only)
     double RK[5];
     int nstage, recon;
+    // the matrix variant of the JST dissipation and Harten's correction
+    int matrixDiss;
+    double harten;
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
     // unsteady dual time (flowType 1): the physical time step and the
     // second-order backward difference on level 1 (timeScheme 2)

@@ -67,7 +67,6 @@ const char *unsupported_reason(const flite_controls &c) {
                "by |dx|^2 of coarse-level coordinates it never fills";
     if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1)
         return "dissipation scheme 1 is not supported";
-    if (c.useMatrixDissipation) return "matrix dissipation is not supported";
     if (c.prolongationMappingScheme != 1) return "prolongationMappingScheme must be 1";
     if (c.precision != FLITE_FP64 && c.precision != FLITE_MIXED) return "precision must be FLITE_FP64 or FLITE_MIXED";
     if (c.precision == FLITE_MIXED && c.fluxType != 1) return "FLITE_MIXED supports the central flux (fluxType 1)";
@@ -127,6 +126,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             P.RK[3] = P.RK[4] = 0.0;
         }
         P.nstage = c->rungeKuttaStages;
+        P.matrixDiss = c->useMatrixDissipation != 0;
+        P.harten = c->HartensCorrectionFactor;
         P.recon = c->reconstruction;
         P.fluxType = c->fluxType; P.hllcOrder = c->HLLCFluxOrder; P.autoClip = c->Automaticlipping;
         P.nsig = c->ReynoldsNumber < 1 ? 4 : 2;       // def_par:1592-1596

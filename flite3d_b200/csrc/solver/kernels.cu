@@ -307,6 +307,80 @@ __global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P, Leve
     for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
 }
 
+// ---- makeArtificialDissipation2, pass 3, matrix variant (def_par:11814-
+// 11898): the one-dimensional Roe matrix |A| along edge e (i1 -> i2), with
+// Harten's correction, applied to the Laplacian and state differences
+__device__ __forceinline__ void matrix_diss(const Params &P, const LevelView &L, int e, int i1, int i2,
+                                            double *d4v, double *d2v) {
+    const int N = L.N;
+    const double H = P.harten;
+    const double eps1 = 1. / dmax(H, 1.e-5), gam1 = P.gm1;
+    double rnx = L.wx[e], rny = L.wy[e], rnz = L.wz[e];
+    const double al = sqrt((rnx * rnx + rny * rny) + rnz * rnz);
+    const double vmo1 = 1. / al;
+    rnx = rnx * vmo1; rny = rny * vmo1; rnz = rnz * vmo1;
+    const double rhol = L.u[i1];
+    double rho1 = 1. / rhol;
+    const double uxl = L.u[N + i1] * rho1, vyl = L.u[2 * N + i1] * rho1, wzl = L.u[3 * N + i1] * rho1;
+    const double hl = (L.u[4 * N + i1] + L.p[i1]) * rho1;
+    const double rhor = L.u[i2];
+    rho1 = 1. / rhor;
+    const double uxr = L.u[N + i2] * rho1, vyr = L.u[2 * N + i2] * rho1, wzr = L.u[3 * N + i2] * rho1;
+    const double hr = (L.u[4 * N + i2] + L.p[i2]) * rho1;
+    const double di = sqrt(rhor / rhol), d1 = 1.0 / (di + 1.0);
+    const double ui = (di * uxr + uxl) * d1, vi = (di * vyr + vyl) * d1, wi = (di * wzr + wzl) * d1;
+    const double hi = (di * hr + hl) * d1;
+    const double ci2 = gam1 * (hi - 0.5 * ((ui * ui + vi * vi) + wi * wi));
+    const double ci = sqrt(ci2);
+    const double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+    const double ucp = (ui * rnx + vi * rny) + wi * rnz;
+    double l1 = fabs(ucp + ci), l2 = fabs(ucp - ci), l3 = fabs(ucp);
+    if (l1 < H) l1 = 0.5 * (l1 * l1 * eps1 + H);
+    if (l2 < H) l2 = 0.5 * (l2 * l2 * eps1 + H);
+    if (l3 < H) l3 = 0.5 * (l3 * l3 * eps1 + H);
+    const double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+    auto apply = [&](double *d) {
+        const double al1x = gam1 * ((((af * d[0] - ui * d[1]) - vi * d[2]) - wi * d[3]) + d[4]);
+        const double al2x = ((-ucp * d[0] + d[1] * rnx) + d[2] * rny) + d[3] * rnz;
+        const double cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+        const double cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+        d[0] = al * (l3 * d[0] + cc1);
+        d[1] = al * ((l3 * d[1] + cc1 * ui) + cc2 * rnx);
+        d[2] = al * ((l3 * d[2] + cc1 * vi) + cc2 * rny);
+        d[3] = al * ((l3 * d[3] + cc1 * wi) + cc2 * rnz);
+        d[4] = al * ((l3 * d[4] + cc1 * hi) + cc2 * ucp);
+    };
+    apply(d4v);
+    apply(d2v);
+}
+
+// the matrix variant's pass 3 as a node gather in edge order; each edge's
+// matrix terms are evaluated in the edge's own node order at both ends
+__global__ void k_jst_flux_matrix(Params P, LevelView L) {
+    const int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double k4 = L.grid == 1 ? P.k4 : P.cgdf;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const bool first = t.x >= 0;
+        const int e = first ? t.x : ~t.x;
+        const int i1 = first ? i : t.y, i2 = first ? t.y : i;
+        double d4v[5], d2v[5];
+        for (int c = 0; c < 5; ++c) {
+            d4v[c] = L.lap[c * N + i1] - L.lap[c * N + i2];
+            d2v[c] = L.u[c * N + i1] - L.u[c * N + i2];
+        }
+        matrix_diss(P, L, e, i1, i2, d4v, d2v);
+        const double d2 = P.k2 * dmax(L.sens[i1], L.sens[i2]);
+        const double d4 = k4 > d2 ? k4 - d2 : 0.0;
+        for (int c = 0; c < 5; ++c)
+            acc[c] = first ? (acc[c] - d4v[c] * d4) + d2v[c] * d2 : (acc[c] + d4v[c] * d4) - d2v[c] * d2;
+    }
+    for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
+}
+
 // ---- makeArtificialDissipation3 (def_par:11995-12139) ---------------------
 template <int U>
 __global__ void k_first_order_diss(Params P, LevelView L) {

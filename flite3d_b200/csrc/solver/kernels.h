@@ -22,6 +22,7 @@ template <int U>
 __global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
+__global__ void k_jst_flux_matrix(Params P, LevelView L);
 __global__ void k_prim_rec(LevelView L);
 __global__ void k_gradient_rec(LevelView L);
 __global__ void k_edge_flux_muscl(Params P, LevelView L);

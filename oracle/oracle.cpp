@@ -276,20 +276,74 @@ struct Oracle {
         });
         const double k2 = c.secondOrderDissipationFactor;
         const double k4 = g.grid == 1 ? c.fourthOrderDissipationFactor : c.coarseGridDissipationFactor;
+        const bool matrix = c.useMatrixDissipation != 0;
         for_edges(g, [&](int e) {
             int i1 = g.s1[e], i2 = g.s2[e];
             double d4v[5], d2v[5];
             for (int k = 0; k < 5; ++k) d4v[k] = nh[k][i1] - nh[k][i2];
             for (int k = 0; k < 5; ++k) d2v[k] = g.u[k][i1] - g.u[k][i2];
-            double d0 = std::min(g.V[i1] / g.dt[i1], g.V[i2] / g.dt[i2]) / (g.conn[i1] + g.conn[i2]);
-            double d2 = d0 * k2 * std::max(nh[8][i1], nh[8][i2]);
-            double d4 = d0 * k4;
+            double d2, d4;
+            if (!matrix) {
+                double d0 = std::min(g.V[i1] / g.dt[i1], g.V[i2] / g.dt[i2]) / (g.conn[i1] + g.conn[i2]);
+                d2 = d0 * k2 * std::max(nh[8][i1], nh[8][i2]);
+                d4 = d0 * k4;
+            } else {
+                matrix_dissipation(g, e, i1, i2, d4v, d2v);
+                d2 = k2 * std::max(nh[8][i1], nh[8][i2]);
+                d4 = k4;
+            }
             d4 = d4 > d2 ? d4 - d2 : 0.0;  // dim(d4,d2)
             for (int k = 0; k < 5; ++k) {
                 g.diss[k][i1] = (g.diss[k][i1] - d4v[k] * d4) + d2v[k] * d2;
                 g.diss[k][i2] = (g.diss[k][i2] + d4v[k] * d4) - d2v[k] * d2;
             }
         });
+    }
+
+    // ---- the matrix variant of makeArtificialDissipation2 (def_par:11814-
+    // 11898): the one-dimensional Roe matrix |A| along the edge, with
+    // Harten's correction of small eigenvalues, applied to the Laplacian
+    // differences d4v and the state differences d2v (both i1 - i2)
+    void matrix_dissipation(const Level &g, int e, int i1, int i2, double *d4v, double *d2v) {
+        const double H = c.HartensCorrectionFactor;
+        const double eps1 = 1. / std::max(H, 1.e-5), gam1 = c.gamma - 1.;
+        double rnx = g.wx[e], rny = g.wy[e], rnz = g.wz[e];
+        const double al = std::sqrt((rnx * rnx + rny * rny) + rnz * rnz);
+        const double vmo1 = 1. / al;
+        rnx = rnx * vmo1; rny = rny * vmo1; rnz = rnz * vmo1;
+        const double rhol = g.u[0][i1];
+        double rho1 = 1. / rhol;
+        const double uxl = g.u[1][i1] * rho1, vyl = g.u[2][i1] * rho1, wzl = g.u[3][i1] * rho1;
+        const double hl = (g.u[4][i1] + g.p[i1]) * rho1;
+        const double rhor = g.u[0][i2];
+        rho1 = 1. / rhor;
+        const double uxr = g.u[1][i2] * rho1, vyr = g.u[2][i2] * rho1, wzr = g.u[3][i2] * rho1;
+        const double hr = (g.u[4][i2] + g.p[i2]) * rho1;
+        const double di = std::sqrt(rhor / rhol), d1 = 1.0 / (di + 1.0);
+        const double ui = (di * uxr + uxl) * d1, vi = (di * vyr + vyl) * d1, wi = (di * wzr + wzl) * d1;
+        const double hi = (di * hr + hl) * d1;
+        const double ci2 = gam1 * (hi - 0.5 * ((ui * ui + vi * vi) + wi * wi));
+        const double ci = std::sqrt(ci2);
+        const double af = 0.5 * ((ui * ui + vi * vi) + wi * wi);
+        const double ucp = (ui * rnx + vi * rny) + wi * rnz;
+        double l1 = std::fabs(ucp + ci), l2 = std::fabs(ucp - ci), l3 = std::fabs(ucp);
+        if (l1 < H) l1 = 0.5 * (l1 * l1 * eps1 + H);
+        if (l2 < H) l2 = 0.5 * (l2 * l2 * eps1 + H);
+        if (l3 < H) l3 = 0.5 * (l3 * l3 * eps1 + H);
+        const double s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
+        auto apply = [&](double *d) {
+            const double al1x = gam1 * ((((af * d[0] - ui * d[1]) - vi * d[2]) - wi * d[3]) + d[4]);
+            const double al2x = ((-ucp * d[0] + d[1] * rnx) + d[2] * rny) + d[3] * rnz;
+            const double cc1 = ((s1 - l3) * al1x / ci2) + (s2 * al2x / ci);
+            const double cc2 = (s2 * al1x / ci) + (s1 - l3) * al2x;
+            d[0] = al * (l3 * d[0] + cc1);
+            d[1] = al * ((l3 * d[1] + cc1 * ui) + cc2 * rnx);
+            d[2] = al * ((l3 * d[2] + cc1 * vi) + cc2 * rny);
+            d[3] = al * ((l3 * d[3] + cc1 * wi) + cc2 * rnz);
+            d[4] = al * ((l3 * d[4] + cc1 * hi) + cc2 * ucp);
+        };
+        apply(d4v);
+        apply(d2v);
     }
 
     // ---- makeArtificialDissipation3 (def_par:11995-12139) -----------------
@@ -1709,7 +1763,6 @@ int check_controls(const flite_controls &c) {
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
         return FLITE_EUNSUPPORTED;
     if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
-    if (c.useMatrixDissipation) return FLITE_EUNSUPPORTED;
     if (c.prolongationMappingScheme != 1) return FLITE_EUNSUPPORTED;
     // the upwind extension (no reference counterpart)
     if (c.rungeKuttaStages != 3 && c.rungeKuttaStages != 5) return FLITE_EUNSUPPORTED;
@@ -2654,7 +2707,7 @@ int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const
     if (!o || !u || !du || !v || !dv) return FLITE_EINVAL;
     const flite_controls &c = o->o.c;
     if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 3 || c.useDissipationWeighting ||
-        c.flowType != 0 || c.rungeKuttaStages != 3)
+        c.useMatrixDissipation || c.flowType != 0 || c.rungeKuttaStages != 3)
         return FLITE_EUNSUPPORTED;
     const bool visc = c.ReynoldsNumber > 0;
     if (visc && (!mu || !mu_out || !dmu_out)) return FLITE_EINVAL;

@@ -38,6 +38,11 @@ CASES = {
                                CFLNumber=0.5),
     "laminar_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1,
                           ReynoldsNumber=5000.0, wallsAreIsentropic=1),
+    "matrix_dissipation": dict(fluxType=1, useMatrixDissipation=1),
+    "matrix_dissipation_harten": dict(fluxType=1, useMatrixDissipation=1, HartensCorrectionFactor=0.3,
+                                      secondOrderDissipationFactor=0.6),
+    "laminar_matrix_dissipation": dict(fluxType=1, useMatrixDissipation=1, ReynoldsNumber=5000.0,
+                                       wallsAreIsentropic=1),
     # the upwind MUSCL / Van Albada extension and the five-stage scheme (no
     # reference counterpart): the GPU against the same extension on the CPU
     "roe_muscl_va_rk5": dict(fluxType=3, reconstruction=1, rungeKuttaStages=5,
