@@ -179,8 +179,16 @@ struct flite_ctx {
     }
     // dissipation choice of singleIteration (def_par:1030-1036)
     void dissipation(int l) {
-        if (c.dissipationScheme == 3) first_order_diss(l);
+        if (c.dissipationScheme == 1 && V(l).grid == 1) lp_diss(l);
+        else if (c.dissipationScheme == 3) first_order_diss(l);
         else jst(l);
+    }
+    // makeArtificialDissipation1 (def_par:10706-11482), level 1 only
+    void lp_diss(int l) {
+        counted();
+        k_lp_sums<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        counted();
+        k_lp_flux<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
     // makeViscosityTerm (def_par:5198-5893), subtracted from the dissipation
     void viscous(int l) {
@@ -353,7 +361,10 @@ struct flite_ctx {
         sa_stage(cl, MODE_RCOARSE, 0);
         node_update(cl, MODE_RCOARSE, 0);
         pressure(fl);
-        jst(fl);  // the fine part always uses scheme 2 (def_par:12266-12270)
+        // the fine part uses scheme 1 on level 1 under dissipationScheme 1,
+        // scheme 2 otherwise (def_par:12269-12273)
+        if (c.dissipationScheme == 1 && V(fl).grid == 1) lp_diss(fl);
+        else jst(fl);
         viscous(fl);
         rhs_terms(fl, false);
         if (turb()) sa_diffusion(fl);  // the fine level keeps its turbulent time steps

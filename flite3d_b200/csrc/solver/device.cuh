@@ -101,6 +101,7 @@ struct LevelView {
     double *hvis;                          // [N]  viscous time-step term
     double *lap;                           // [5][N] undivided Laplacian
     double *sens;                          // [N]  pressure sensor
+    double *lpw;                           // [N]  edge-factor sums of dissipation scheme 1 (level 1)
     double *tau;                           // [9][N] stress tensor + heat flux
     double *prim;                          // [4][N] u, v, w, T of the viscous term
     NodeRec *q;                            // [N] written with p by k_pressure (48 B: the level-1

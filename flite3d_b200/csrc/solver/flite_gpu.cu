@@ -65,8 +65,9 @@ const char *unsupported_reason(const flite_controls &c) {
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
         return "least-squares gradients need numberOfGridsToUse = 1: the reference's LS gradient divides "
                "by |dx|^2 of coarse-level coordinates it never fills";
-    if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1)
-        return "dissipation scheme 1 is not supported";
+    if (c.coarseGridDissipationScheme == 1)
+        return "coarseGridDissipationScheme 1 is not supported: the reference's scheme 1 on a coarse level reads "
+               "coordinates through finer-level seed indices beyond the coarse arrays";
     if (c.prolongationMappingScheme != 1) return "prolongationMappingScheme must be 1";
     if (c.precision != FLITE_FP64 && c.precision != FLITE_MIXED) return "precision must be FLITE_FP64 or FLITE_MIXED";
     if (c.precision == FLITE_MIXED && c.fluxType != 1) return "FLITE_MIXED supports the central flux (fluxType 1)";
@@ -327,6 +328,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             L.prim = visc ? X.alloc<double>(4 * (size_t)N) : nullptr;
             L.lap = X.alloc<double>(5 * (size_t)N);
             L.sens = X.alloc<double>(N);
+            L.lpw = c->dissipationScheme == 1 && l == 0 ? X.alloc<double>(N) : nullptr;
             L.vdt = X.alloc<double>(N);
             L.wstress = X.alloc<double>(3 * (size_t)N);
             CK(cudaMemset(L.wstress, 0, 3 * (size_t)N * sizeof(double)));

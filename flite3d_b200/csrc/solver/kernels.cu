@@ -381,6 +381,107 @@ __global__ void k_jst_flux_matrix(Params P, LevelView L) {
     for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
 }
 
+// ---- makeArtificialDissipation1 (def_par:10706-11482), level 1 -----------
+// the linearity-preserving dissipation of Crumpton et al.  Pass 1, per node
+// in edge order: the gradient sums of (rho, rho u, rho v, rho w, rho E), the
+// undivided Laplacian L(U), the sum of the edge factors and L(x); then the
+// boundary faces, the volume scaling, L^(U) = L(U) - (grad U).L(x) (L(x) = 0
+// on boundary nodes) and the pressure sensor.  Writes L^ to lap, the sensor
+// to sens and the factor sum to lpw.
+__global__ void k_lp_sums(Params P, LevelView L) {
+    const int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double g[15], l[5], lx[3] = {0.0, 0.0, 0.0}, s21 = 0.0, pd = 0.0, ps = 0.0;
+    for (int c = 0; c < 15; ++c) g[c] = 0.0;
+    for (int c = 0; c < 5; ++c) l[c] = 0.0;
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const bool first = t.x >= 0;
+        const int e = first ? t.x : ~t.x;
+        const int i1 = first ? i : t.y, i2 = first ? t.y : i;
+        const EdgeW ew = load_edgew(L.ew, e);
+        const double w[3] = {ew.wx, ew.wy, ew.wz};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 5; ++c) {
+                const double sv = (L.u[c * N + i1] + L.u[c * N + i2]) * w[a];
+                g[5 * a + c] = first ? g[5 * a + c] + sv : g[5 * a + c] - sv;
+            }
+        double df = 1.0;
+        if (P.useDissW) df = 1. / L.slen[e];
+        for (int c = 0; c < 5; ++c) {
+            const double d = L.u[c * N + i1] - L.u[c * N + i2];
+            l[c] = first ? l[c] - d * df : l[c] + d * df;
+        }
+        s21 = s21 + df;
+        const double dx[3] = {L.cx[i1] - L.cx[i2], L.cy[i1] - L.cy[i2], L.cz[i1] - L.cz[i2]};
+        for (int a = 0; a < 3; ++a) lx[a] = first ? lx[a] - dx[a] * df : lx[a] + dx[a] * df;
+        const double dp = L.p[i1] - L.p[i2], sp = L.p[i1] + L.p[i2];
+        pd = first ? pd - dp : pd + dp;
+        ps = ps + sp;
+    }
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        const int2 nd = L.bedge[b];
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 5; ++c) {
+                const double q1 = L.u[c * N + nd.x], q2 = L.u[c * N + nd.y];
+                double v;
+                if (P.boundaryTerm == 1) v = side == 0 ? (3. * q1 + q2) * w[a] : (q1 + 3. * q2) * w[a];
+                else v = side == 0 ? 4. * q1 * w[a] : 4. * w[a];  // the reference's second term has no state
+                g[5 * a + c] = g[5 * a + c] + v;
+            }
+    }
+    if (P.useDissW) s21 = 3.0 * s21;
+    const double vt = 1. / L.V[i];
+    for (int c = 0; c < 15; ++c) g[c] = g[c] * vt;
+    if (i < L.Nb) lx[0] = lx[1] = lx[2] = 0.0;
+    for (int c = 0; c < 5; ++c)
+        L.lap[c * N + i] = ((l[c] + g[c] * lx[0]) + g[5 + c] * lx[1]) + g[10 + c] * lx[2];
+    L.sens[i] = 12. * fabs(pd / ps);
+    L.lpw[i] = s21;
+}
+
+// pass 2: the edge terms, as a node gather in edge order; under
+// useMatrixDissipation the scalar coefficient divided by each end's factor
+// sum, otherwise the Roe matrix (the reference's branch order)
+__global__ void k_lp_flux(Params P, LevelView L) {
+    const int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        const bool first = t.x >= 0;
+        const int e = first ? t.x : ~t.x;
+        const int i1 = first ? i : t.y, i2 = first ? t.y : i;
+        double d4v[5], d2v[5];
+        for (int c = 0; c < 5; ++c) {
+            d4v[c] = L.lap[c * N + i1] - L.lap[c * N + i2];
+            d2v[c] = L.u[c * N + i1] - L.u[c * N + i2];
+        }
+        double d2, d4, d41, d42;
+        if (P.matrixDiss) {
+            const double d0 = dmin(L.vdt[i1], L.vdt[i2]) / (L.conn[i1] + L.conn[i2]);
+            d2 = d0 * P.k2 * dmax(L.sens[i1], L.sens[i2]);
+            d4 = d0 * P.k4;
+            d4 = d4 > d2 ? d4 - d2 : 0.0;
+            d41 = d4 / L.lpw[i1];
+            d42 = d4 / L.lpw[i2];
+        } else {
+            matrix_diss(P, L, e, i1, i2, d4v, d2v);
+            d2 = P.k2 * dmax(L.sens[i1], L.sens[i2]);
+            d4 = P.k4;
+            d4 = d4 > d2 ? d4 - d2 : 0.0;
+            d41 = d42 = d4;
+        }
+        for (int c = 0; c < 5; ++c)
+            acc[c] = first ? (acc[c] - d4v[c] * d41) + d2v[c] * d2 : (acc[c] + d4v[c] * d42) - d2v[c] * d2;
+    }
+    for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
+}
+
 // ---- makeArtificialDissipation3 (def_par:11995-12139) ---------------------
 template <int U>
 __global__ void k_first_order_diss(Params P, LevelView L) {

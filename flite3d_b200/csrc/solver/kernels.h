@@ -23,6 +23,8 @@ __global__ void k_visc_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
 __global__ void k_jst_flux_matrix(Params P, LevelView L);
+__global__ void k_lp_sums(Params P, LevelView L);
+__global__ void k_lp_flux(Params P, LevelView L);
 __global__ void k_prim_rec(LevelView L);
 __global__ void k_gradient_rec(LevelView L);
 __global__ void k_edge_flux_muscl(Params P, LevelView L);

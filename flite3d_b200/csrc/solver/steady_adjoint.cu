@@ -1229,7 +1229,7 @@ static const char *steady_adjoint_unsupported(const flite_ctx &X) {
     if (c.flowType != 0) return "the steady adjoint takes steady runs (flowType 0)";
     if (c.rungeKuttaStages != 3) return "the steady adjoint takes the reference's three stages";
     if (c.turbulenceModel != 0) return "the steady adjoint covers inviscid and laminar runs (no turbulence model)";
-    if (c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";
+    if (c.dissipationScheme == 1 || c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";
     if (c.useDissipationWeighting) return "the steady adjoint takes unweighted dissipation";
     if (c.useMatrixDissipation) return "the steady adjoint takes the scalar JST dissipation";
     return nullptr;

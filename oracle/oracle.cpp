@@ -346,6 +346,109 @@ struct Oracle {
         apply(d2v);
     }
 
+    // ---- makeArtificialDissipation1 (def_par:10706-11482): the linearity-
+    // preserving dissipation of Crumpton et al. on level 1.  Help columns
+    // (0-based): 0-14 the gradient sums of (rho, rho u, rho v, rho w, rho E)
+    // in x, y, z; 15-19 L(U), then L^(U); 20 the sum of the edge factors;
+    // 21-23 L(x).  The far-field zeroing of the reference's columns 9-12 (def_par:11120-
+    // 11126) touches columns that are not read again.
+    void makeArtificialDissipation1(Level &g) {
+        for (int k = 0; k < 5; ++k) std::fill(g.diss[k].begin(), g.diss[k].end(), 0.0);
+        for (auto &col : nh) std::fill(col.begin(), col.end(), 0.0);
+        for_edges(g, [&](int e) {
+            const int i1 = g.s1[e], i2 = g.s2[e];
+            const double w[3] = {g.wx[e], g.wy[e], g.wz[e]};
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 5; ++k) {
+                    const double sv = (g.u[k][i1] + g.u[k][i2]) * w[a];
+                    nh[5 * a + k][i1] = nh[5 * a + k][i1] + sv;
+                    nh[5 * a + k][i2] = nh[5 * a + k][i2] - sv;
+                }
+            double df = 1.0;
+            if (c.useDissipationWeighting) df = 1. / g.slen[e];
+            for (int k = 0; k < 5; ++k) {
+                const double d = g.u[k][i1] - g.u[k][i2];
+                nh[15 + k][i1] = nh[15 + k][i1] - d * df;
+                nh[15 + k][i2] = nh[15 + k][i2] + d * df;
+            }
+            nh[20][i1] = nh[20][i1] + df;
+            nh[20][i2] = nh[20][i2] + df;
+            const double dx[3] = {g.cx[i1] - g.cx[i2], g.cy[i1] - g.cy[i2], g.cz[i1] - g.cz[i2]};
+            for (int a = 0; a < 3; ++a) {
+                nh[21 + a][i1] = nh[21 + a][i1] - dx[a] * df;
+                nh[21 + a][i2] = nh[21 + a][i2] + dx[a] * df;
+            }
+        });
+        // boundary faces; with boundaryTerm != 1 the second node's term
+        // carries no state (4 w, def_par:10974-10988), restated as is
+        for_bedges(g, [&](int b) {
+            const int i1 = g.b1[b], i2 = g.b2[b];
+            const double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 5; ++k) {
+                    const double q1 = g.u[k][i1], q2 = g.u[k][i2];
+                    if (c.boundaryTerm == 1) {
+                        nh[5 * a + k][i1] = nh[5 * a + k][i1] + (3. * q1 + q2) * w[a];
+                        nh[5 * a + k][i2] = nh[5 * a + k][i2] + (q1 + 3. * q2) * w[a];
+                    } else {
+                        nh[5 * a + k][i1] = nh[5 * a + k][i1] + 4. * q1 * w[a];
+                        nh[5 * a + k][i2] = nh[5 * a + k][i2] + 4. * w[a];
+                    }
+                }
+        });
+        if (c.useDissipationWeighting)
+            for (int i = 0; i < g.N; ++i) nh[20][i] = 3.0 * nh[20][i];
+        for (int i = 0; i < g.N; ++i) {
+            const double vt = 1. / g.V[i];
+            for (int k = 0; k < 15; ++k) nh[k][i] = nh[k][i] * vt;
+        }
+        for (int i = 0; i < g.Nb; ++i) nh[21][i] = nh[22][i] = nh[23][i] = 0.0;
+        for (int i = 0; i < g.N; ++i)
+            for (int k = 0; k < 5; ++k)
+                nh[15 + k][i] = ((nh[15 + k][i] + nh[k][i] * nh[21][i]) + nh[5 + k][i] * nh[22][i]) +
+                                nh[10 + k][i] * nh[23][i];
+        // pressure switch
+        std::fill(nh[0].begin(), nh[0].end(), 0.0);
+        std::fill(nh[1].begin(), nh[1].end(), 0.0);
+        for_edges(g, [&](int e) {
+            const int i1 = g.s1[e], i2 = g.s2[e];
+            const double dp = g.p[i1] - g.p[i2], sp = g.p[i1] + g.p[i2];
+            nh[0][i1] = nh[0][i1] - dp;
+            nh[1][i1] = nh[1][i1] + sp;
+            nh[0][i2] = nh[0][i2] + dp;
+            nh[1][i2] = nh[1][i2] + sp;
+        });
+        for (int i = 0; i < g.N; ++i) nh[8][i] = 12. * std::fabs(nh[0][i] / nh[1][i]);
+        const double k2 = c.secondOrderDissipationFactor, k4 = c.fourthOrderDissipationFactor;
+        for_edges(g, [&](int e) {
+            const int i1 = g.s1[e], i2 = g.s2[e];
+            double d4v[5], d2v[5];
+            for (int k = 0; k < 5; ++k) d4v[k] = nh[15 + k][i1] - nh[15 + k][i2];
+            for (int k = 0; k < 5; ++k) d2v[k] = g.u[k][i1] - g.u[k][i2];
+            double d2, d4, d41, d42;
+            // the branches as the reference orders them: the scalar
+            // coefficient under useMatrixDissipation, the matrix otherwise
+            if (c.useMatrixDissipation) {
+                const double d0 = std::min(g.V[i1] / g.dt[i1], g.V[i2] / g.dt[i2]) / (g.conn[i1] + g.conn[i2]);
+                d2 = d0 * k2 * std::max(nh[8][i1], nh[8][i2]);
+                d4 = d0 * k4;
+                d4 = d4 > d2 ? d4 - d2 : 0.0;
+                d41 = d4 / nh[20][i1];
+                d42 = d4 / nh[20][i2];
+            } else {
+                matrix_dissipation(g, e, i1, i2, d4v, d2v);
+                d2 = k2 * std::max(nh[8][i1], nh[8][i2]);
+                d4 = k4;
+                d4 = d4 > d2 ? d4 - d2 : 0.0;
+                d41 = d42 = d4;
+            }
+            for (int k = 0; k < 5; ++k) {
+                g.diss[k][i1] = (g.diss[k][i1] - d4v[k] * d41) + d2v[k] * d2;
+                g.diss[k][i2] = (g.diss[k][i2] + d4v[k] * d42) - d2v[k] * d2;
+            }
+        });
+    }
+
     // ---- makeArtificialDissipation3 (def_par:11995-12139) -----------------
     void makeArtificialDissipation3(Level &g) {
         for (int k = 0; k < 5; ++k) std::fill(g.diss[k].begin(), g.diss[k].end(), 0.0);
@@ -1393,7 +1496,10 @@ struct Oracle {
         for_nodes(g.N, [&](int i) { g.u[0][i] = std::max(g.u[0][i], c.minimumDensity); });
     }
 
+    // singleIteration (def_par:1030-1036) and restrictGrid's fine part
+    // (def_par:12269-12273): scheme 1 acts on level 1 only
     void dissipation_for(Level &g, bool in_restrict_fine) {
+        if (c.dissipationScheme == 1 && g.grid == 1) { makeArtificialDissipation1(g); return; }
         if (in_restrict_fine) { makeArtificialDissipation2(g); return; }
         if (c.dissipationScheme == 3) makeArtificialDissipation3(g);
         else makeArtificialDissipation2(g);
@@ -1762,7 +1868,9 @@ int check_controls(const flite_controls &c) {
     // the reference never fills (0*inf = NaN): single-grid runs only
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
         return FLITE_EUNSUPPORTED;
-    if (c.dissipationScheme == 1 || c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
+    // scheme 1 on coarse levels reads coordinates through seed-node indices
+    // of the finer level (def_par:10874-10878) beyond the coarse arrays
+    if (c.coarseGridDissipationScheme == 1) return FLITE_EUNSUPPORTED;
     if (c.prolongationMappingScheme != 1) return FLITE_EUNSUPPORTED;
     // the upwind extension (no reference counterpart)
     if (c.rungeKuttaStages != 3 && c.rungeKuttaStages != 5) return FLITE_EUNSUPPORTED;
@@ -2706,7 +2814,8 @@ int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const
                          double *mu_out, double *dmu_out) {
     if (!o || !u || !du || !v || !dv) return FLITE_EINVAL;
     const flite_controls &c = o->o.c;
-    if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 3 || c.useDissipationWeighting ||
+    if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 1 || c.dissipationScheme == 3 ||
+        c.useDissipationWeighting ||
         c.useMatrixDissipation || c.flowType != 0 || c.rungeKuttaStages != 3)
         return FLITE_EUNSUPPORTED;
     const bool visc = c.ReynoldsNumber > 0;

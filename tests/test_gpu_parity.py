@@ -39,6 +39,16 @@ CASES = {
     "laminar_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1,
                           ReynoldsNumber=5000.0, wallsAreIsentropic=1),
     "matrix_dissipation": dict(fluxType=1, useMatrixDissipation=1),
+    # dissipation scheme 1 (linearity preserving) on level 1: the Roe matrix
+    # by default, the scalar coefficient under useMatrixDissipation
+    "lp_dissipation": dict(fluxType=1, dissipationScheme=1, fourthOrderDissipationFactor=0.05),
+    "lp_dissipation_scalar": dict(fluxType=1, dissipationScheme=1, useMatrixDissipation=1),
+    "lp_dissipation_weighted": dict(fluxType=1, dissipationScheme=1, useDissipationWeighting=1,
+                                    CFLNumber=0.5, fourthOrderDissipationFactor=0.05),
+    "lp_dissipation_fv": dict(fluxType=1, dissipationScheme=1, boundaryTerm=2,
+                              fourthOrderDissipationFactor=0.05),
+    "laminar_lp_dissipation": dict(fluxType=1, dissipationScheme=1, ReynoldsNumber=5000.0,
+                                   wallsAreIsentropic=1, fourthOrderDissipationFactor=0.05),
     "matrix_dissipation_harten": dict(fluxType=1, useMatrixDissipation=1, HartensCorrectionFactor=0.3,
                                       secondOrderDissipationFactor=0.6),
     "laminar_matrix_dissipation": dict(fluxType=1, useMatrixDissipation=1, ReynoldsNumber=5000.0,

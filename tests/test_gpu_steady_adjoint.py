@@ -201,7 +201,8 @@ def test_adjoint_leaves_the_solve_unchanged():
 
 @pytest.mark.parametrize("ctl", [dict(ReynoldsNumber=5e6, turbulenceModel=1), dict(fluxType=4),
                                  dict(dissipationScheme=3), dict(flowType=1, physicalTimeStep=0.1),
-                                 dict(rungeKuttaStages=5), dict(useMatrixDissipation=1)])
+                                 dict(rungeKuttaStages=5), dict(useMatrixDissipation=1),
+                                 dict(dissipationScheme=1)])
 def test_adjoint_refuses_what_it_does_not_cover(ctl):
     mesh = Mesh.bump_channel(6, 2, 2, 0.05, nlevels=1)
     c = controls(numberOfGridsToUse=1, **ctl)
