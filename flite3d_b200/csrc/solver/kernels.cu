@@ -910,15 +910,29 @@ __global__ void k_minmax(Params P, LevelView L) {
 }
 
 // ---- interior edge flux into the edge buffer ------------------------------
+// The block's fluxes (at most 256 x 5) are staged in shared memory and
+// written as one contiguous run of 16-byte stores; the block size is even,
+// so the run starts on a 16-byte boundary.
+__device__ __forceinline__ void store_block_fluxes(double *flux, const double *sf, int e0, int count) {
+    const int n = 5 * count;
+    double2 *o = reinterpret_cast<double2 *>(flux + (size_t)e0 * 5);
+    const double2 *src = reinterpret_cast<const double2 *>(sf);
+    for (int k = threadIdx.x; k < n / 2; k += blockDim.x) o[k] = src[k];
+    if ((n & 1) && threadIdx.x == 0) flux[(size_t)e0 * 5 + n - 1] = sf[n - 1];
+}
 template <int FT, bool O2>
 __global__ void __launch_bounds__(256) k_edge_flux(Params P, LevelView L) {
-    int e = tid();
-    if (e >= L.E) return;
-    int2 nd = L.edge[e];
-    double f[5];
-    edge_flux<FT, O2>(P, L, e, nd.x, nd.y, f);
-    double *o = L.flux + (size_t)e * 5;
-    o[0] = f[0]; o[1] = f[1]; o[2] = f[2]; o[3] = f[3]; o[4] = f[4];
+    __shared__ __align__(16) double sf[256 * 5];
+    const int e0 = blockIdx.x * blockDim.x, e = e0 + threadIdx.x;
+    if (e < L.E) {
+        const int2 nd = L.edge[e];
+        double f[5];
+        edge_flux<FT, O2>(P, L, e, nd.x, nd.y, f);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sf[threadIdx.x * 5 + k] = f[k];
+    }
+    __syncthreads();
+    store_block_fluxes(L.flux, sf, e0, min((int)blockDim.x, L.E - e0));
 }
 template __global__ void k_edge_flux<1, false>(Params, LevelView);
 template __global__ void k_edge_flux<2, false>(Params, LevelView);
@@ -927,12 +941,11 @@ template __global__ void k_edge_flux<3, true>(Params, LevelView);
 template __global__ void k_edge_flux<4, false>(Params, LevelView);
 template __global__ void k_edge_flux<4, true>(Params, LevelView);
 
-// the upwind extension's level-1 edge flux into the edge buffer; the block's
-// 256 x 5 fluxes are staged in shared memory and written as one contiguous
-// run of 16-byte stores
+// the upwind extension's level-1 edge flux into the edge buffer, stored as
+// k_edge_flux stores
 __global__ void __launch_bounds__(256) k_edge_flux_muscl(Params P, LevelView L) {
     __shared__ __align__(16) double sf[256 * 5];
-    const int e0 = blockIdx.x * 256, e = e0 + threadIdx.x;
+    const int e0 = blockIdx.x * blockDim.x, e = e0 + threadIdx.x;
     if (e < L.E) {
         const int2 nd = L.edge[e];
         double f[5];
@@ -941,12 +954,7 @@ __global__ void __launch_bounds__(256) k_edge_flux_muscl(Params P, LevelView L) 
         for (int k = 0; k < 5; ++k) sf[threadIdx.x * 5 + k] = f[k];
     }
     __syncthreads();
-    // e0 * 5 doubles is a multiple of 16 bytes (e0 is a multiple of 256)
-    const int n = 5 * min(256, L.E - e0);
-    double2 *o = reinterpret_cast<double2 *>(L.flux + (size_t)e0 * 5);
-    const double2 *src = reinterpret_cast<const double2 *>(sf);
-    for (int k = threadIdx.x; k < n / 2; k += 256) o[k] = src[k];
-    if ((n & 1) && threadIdx.x == 0) L.flux[(size_t)e0 * 5 + n - 1] = sf[n - 1];
+    store_block_fluxes(L.flux, sf, e0, min((int)blockDim.x, L.E - e0));
 }
 
 // ---- boundary-edge contributions ------------------------------------------
