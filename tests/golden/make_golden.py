@@ -29,6 +29,14 @@ CASES = {
                     multigridScheme=3, wallsAreIsentropic=1),
     "sa": dict(ReynoldsNumber=1.0e5, fluxType=1, CFLNumber=1.0, numberOfGridsToUse=3,
                multigridScheme=3, wallsAreIsentropic=1, turbulenceModel=1),
+    "matrix_dissipation": dict(ReynoldsNumber=0.0, fluxType=1, CFLNumber=2.0, numberOfGridsToUse=3,
+                               multigridScheme=3, useMatrixDissipation=1),
+    "lp_dissipation": dict(ReynoldsNumber=0.0, fluxType=1, CFLNumber=2.0, numberOfGridsToUse=3,
+                           multigridScheme=3, dissipationScheme=1, fourthOrderDissipationFactor=0.05),
+    # the upwind extension (no reference counterpart)
+    "upwind_extension": dict(ReynoldsNumber=0.0, fluxType=3, reconstruction=1, rungeKuttaStages=5,
+                             secondOrderDissipationFactor=0.0, fourthOrderDissipationFactor=0.0,
+                             CFLNumber=2.0, numberOfGridsToUse=3, multigridScheme=3),
 }
 MESH = (12, 4, 4)
 
