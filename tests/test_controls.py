@@ -52,3 +52,17 @@ def test_namelist_deck():
     assert c.inflowField[1] == pytest.approx(math.cos(a), rel=1e-15)
     assert c.inflowField[3] == pytest.approx(math.sin(a), rel=1e-15)
     assert "ivd%dataDirectory" in unknown and "ivd%spanCor" in unknown
+
+
+def test_extension_controls_default_to_the_reference_scheme():
+    # the fields after inflowField have no reference counterpart; their
+    # defaults select the reference's scheme
+    c = default_controls()
+    assert c.precision == 0 and c.reconstruction == 0 and c.rungeKuttaStages == 3
+    assert c.useMatrixDissipation == 0 and c.dissipationScheme == 2 and c.HartensCorrectionFactor == 0.0
+
+
+def test_deck_leaves_the_extension_controls_alone():
+    # a reference deck cannot name them: they keep their defaults
+    c, unknown = controls_from_inp(DECK)
+    assert c.reconstruction == 0 and c.rungeKuttaStages == 3 and c.precision == 0
