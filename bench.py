@@ -434,7 +434,7 @@ def run_reference(args):
 
 
 def run_rans(args):
-    """The RANS configuration (SURVEY c3): Spalart-Allmaras on the extruded
+    """The RANS configuration: Spalart-Allmaras on the extruded
     NACA0012 O-grid (200 x 120 x 240 cells: 40 wall layers from 1e-5 chord
     growing by 1.15, far field at 20 chords, one chord of span), Re 6e6,
     M 0.8, alpha 1.25, HLLC order 2 with Galerkin gradients, 5 levels, FP64.
@@ -539,7 +539,7 @@ def run_upwind(args):
 
 
 def run_adjoint(args):
-    """The adjoint configuration (SURVEY c4) for the central flux: dCL/dX and
+    """The adjoint configuration for the central flux: dCL/dX and
     dCD/dX along the normal displacement of wall nodes of the bump channel
     48x16x16 hex -> tets (the Euler configuration's mesh) with its interior
     nodes jittered by up to 15% of the spacing (seed 11: no two edges tie in
@@ -659,7 +659,7 @@ def run_adjoint(args):
 
 
 def run_batch(args):
-    """Batched solves (SURVEY c5): the bump channel at 120x40x40, 192x64x64 and
+    """Batched solves: the bump channel at 120x40x40, 192x64x64 and
     264x88x88 hexes x 16 flow conditions each (angle of attack uniform in
     [-4, 8] degrees, Mach uniform in [0.3, 0.8], SplitMix64 seed 5), inviscid,
     FLITE_MIXED.  One JSON line: case-cycles per second of one graph launch

@@ -1,6 +1,6 @@
 // CUDA kernels of the flow-solver hot path (sm_100a, FP64).
 //
-// Layout and scheduling (the reasoning is in DESIGN.md):
+// Layout and scheduling:
 //  * node state is SoA [component][node] so node kernels read and write each
 //    component coalesced;
 //  * the interior-edge flux is computed once per edge into an edge buffer

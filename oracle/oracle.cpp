@@ -8,8 +8,7 @@
 // too, so any state that would leak between levels in the reference leaks
 // the same way here.
 //
-// Pinned choices where the reference reads undefined values (each is also
-// listed in DESIGN.md):
+// Pinned choices where the reference reads undefined values:
 //  * Roe and LLF read rho1/rho2/h1/h2 that the interior loop never sets
 //    (def_par:1682,1693,1738,1748,1760): rho = r and h = (E+p)/rho.
 //  * LLF/Roe leave f unchanged when |w| <= 1e-10 (def_par:1672,1727),
