@@ -2738,14 +2738,26 @@ int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r) {
     return FLITE_OK;
 }
 
-int oracle_eval_dissipation(oracle_ctx *o, int level) {
+// one column of the shared help array (nodeHelpArray(:, col + 1)) after the
+// last evaluation, for tests of the dissipation schemes' intermediate sums
+int oracle_help_column(oracle_ctx *o, int col, double *out) {
+    if (!o || !out || col < 0 || col >= (int)o->o.nh.size() || o->o.lv.empty()) return FLITE_EINVAL;
+    std::memcpy(out, o->o.nh[col].data(), 8 * (size_t)o->o.lv[0].N);
+    return FLITE_OK;
+}
+
+// the artificial dissipation of singleIteration (def_par:1022-1036) at the
+// state u of a level: pressure, |p|, local time steps, then the run's
+// dissipation scheme; diss [5][N] out
+int oracle_dissipation(oracle_ctx *o, int level, const double *u, double *diss) {
     Level *g = lvl(o, level);
-    if (!g) return FLITE_EINVAL;
+    if (!g || !u || !diss) return FLITE_EINVAL;
+    for (int k = 0; k < 5; ++k) std::memcpy(g->u[k].data(), u + (size_t)k * g->N, 8 * (size_t)g->N);
     o->o.makePressureField(*g, g->u);
     for (int i = 0; i < g->N; ++i) g->p[i] = std::fabs(g->p[i]);
     o->o.makeTimeSteps(*g);
     o->o.dissipation_for(*g, false);
-    if (o->o.c.ReynoldsNumber > 0.0) o->o.makeViscosityTerm(*g);
+    for (int k = 0; k < 5; ++k) std::memcpy(diss + (size_t)k * g->N, g->diss[k].data(), 8 * (size_t)g->N);
     return FLITE_OK;
 }
 

@@ -41,8 +41,10 @@ int oracle_next_physical_step(oracle_ctx *o);
 int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[7]);
 int oracle_forces(oracle_ctx *o, double out[6]);
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);
-/* one makeTimeSteps + dissipation evaluation at the level's current state */
-int oracle_eval_dissipation(oracle_ctx *o, int level);
+/* the artificial dissipation (time steps, then the run's scheme) at the state u */
+int oracle_dissipation(oracle_ctx *o, int level, const double *u, double *diss);
+/* nodeHelpArray(:, col + 1) of level 1 after the last evaluation */
+int oracle_help_column(oracle_ctx *o, int col, double *out);
 /* pinned exp (which 0) / log (which 1) of the SA source term            */
 int oracle_pinned_math(int which, const double *x, double *y, int n);
 /* threads of the timing mode (default 1 = the reference's loop order)  */
