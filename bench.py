@@ -107,11 +107,14 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def build_case():
+def build_case(host_only=False):
+    """The mesh, controls and seeded initial state of the workload.  With
+    host_only the controls come from the host preprocessor library, so the
+    CUDA library is never loaded (the CPU reference arm)."""
     import flite3d_b200 as F
     t0 = time.time()
     mesh = F.Mesh.bump_channel(MESH["nx"], MESH["ny"], MESH["nz"], MESH["bump"], MESH["levels"])
-    c = F.default_controls(**CONTROLS)
+    c = F.host_controls(**CONTROLS) if host_only else F.default_controls(**CONTROLS)
     u0 = F.initial_state(c, mesh, perturb_seed=20261203, amplitude=0.01)
     return F, mesh, c, u0, time.time() - t0
 
@@ -262,12 +265,15 @@ def run_ours(args):
         mixed = {"value": v_m, "unit": "cycles/s", "ms_per_step": ms_m / args.steps,
                  "node_kernel_ms": node_m_ms, "increment_records_ms": delta_ms}
     ttc = None
-    if args.converge:
+    if not args.no_converge:
         ttc = time_to_converge(F, mesh, c, u0, args.converge_max, (best[0], lanes))
 
     cpu = None
+    parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mesh, c, u0, cycles=args.cpu_cycles)
+    if rank == 0 and ws == 1 and args.parity_cycles > 0:
+        parity = parity_check(F, mesh, c, u0, args.parity_cycles, (best[0], lanes))
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -285,11 +291,11 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (state+mesh+edge buffer > 1 GB)",
                    "mesh_build_s": round(t_mesh, 2)},
         "e2e": {"value": e2e_value, "unit": "cycles/s", "h2d_bytes_per_step": 5 * n * 8 + 4,
-                "d2h_bytes_per_step": 5 * n * 8 + 15 * 8 + 6 * 8,
+                "d2h_bytes_per_step": 5 * n * 8 + 15 * 8 + 9 * 8,
                 "what": "per cycle: level-1 state host->device from pinned memory, flite_cycle, "
                         "residual norms and forces read back, level-1 state device->host",
                 "resident": {"value": args.steps / resident_s, "h2d_bytes_per_step": 4,
-                             "d2h_bytes_per_step": 15 * 8 + 6 * 8}},
+                             "d2h_bytes_per_step": 15 * 8 + 9 * 8}},
         "gpu_launches": int(launches_per_cycle * args.steps),
         "roofline": {"kernel": "k_node_update<GATHER_CENTRAL> (level 1: central fluxes of the "
                                "incident edges computed in the node gather, fused with the RK "
@@ -316,6 +322,8 @@ def run_ours(args):
         line["time_to_1e-8"] = ttc
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if parity is not None:
+        line["parity"] = parity
     print(json.dumps(line), flush=True)
 
 
@@ -354,6 +362,49 @@ def time_to_converge(F, mesh, c, u0, max_cycles, options=None):
         out["CL_rel_diff"] = abs(b["CL"] - a["CL"]) / max(abs(a["CL"]), 1e-300)
         out["CD_rel_diff"] = abs(b["CD"] - a["CD"]) / max(abs(a["CD"]), 1e-300)
     return out
+
+
+def parity_check(F, mesh, c, u0, cycles, options=None):
+    """The bench workload itself, GPU against the CPU restatement: both
+    start from the seeded state u0 and run the same `cycles` growing-V
+    cycles (the restatement single-threaded, in the reference's edge order);
+    then every level's state is compared bit for bit, and the residual norms
+    and forces, which the GPU sums in another order, relatively."""
+    import torch
+    from flite3d_b200.solver import Backend, Solver
+    import flite3d_b200.build as b
+    b.build_oracle()
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
+    lib.oracle_set_threads(1)
+    g = F.Solver(c, mesh)
+    if options:
+        g.set_kernel_options(256, options[0], 1)
+        for lvl, lanes in options[1].items():
+            g.set_gather_lanes(lvl, lanes)
+    o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
+    t0 = time.perf_counter()
+    for s in (g, o):
+        s.set_state(u0)
+        s.start()
+        for cyc in range(1, cycles + 1):
+            s.cycle(cyc)
+    torch.cuda.synchronize()
+    levels = []
+    for level in range(1, g.nlevels + 1):
+        a, r = g.get_state(level), o.get_state(level)
+        levels.append({"level": level, "nodes": int(a.shape[1]), "bitwise": bool(np.array_equal(a, r)),
+                       "max_abs": float(np.abs(a - r).max())})
+    rg, ro = g.residuals()[0], o.residuals()[0]
+    fg, fo = g.forces(), o.forces()
+    g.close()
+    o.close()
+    return {"cycles": cycles, "bitwise": all(x["bitwise"] for x in levels),
+            "max_abs": max(x["max_abs"] for x in levels), "levels": levels,
+            "residual_max_rel": float(np.max(np.abs(rg - ro) / np.abs(ro))),
+            "CL_rel": float(abs(fg[0] - fo[0]) / abs(fo[0])), "CD_rel": float(abs(fg[1] - fo[1]) / abs(fo[1])),
+            "seconds": time.perf_counter() - t0,
+            "what": f"GPU vs the single-threaded CPU restatement from the same seeded state, {cycles} cycles of "
+                    "the bench workload; states compared with np.array_equal on every level"}
 
 
 def cpu_baseline(mesh, c, u0, cycles=2, sample_of="the same 2.1M-node workload"):
@@ -399,7 +450,7 @@ def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return
-    F, mesh, c, u0, _ = build_case()
+    F, mesh, c, u0, _ = build_case(host_only=True)
     import flite3d_b200.build as b
     from flite3d_b200.solver import Backend, Solver
     b.build_oracle()
@@ -425,6 +476,10 @@ def run_reference(args):
         "steps": steps, "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload(mesh.level(1).n_nodes, mesh.level(1).n_sides)},
+        "requested": {"steps": args.steps, "warmup": args.warmup,
+                      "why_fewer": "a bounded CPU sample: each cycle of the 2.1M-node workload takes about "
+                                   "a second on the host, so at most --cpu-cycles timed cycles after at most "
+                                   "3 warm-up cycles"},
         "cpu_baseline": {"value": v, "unit": "cycles/s", "cores": threads, "kind": "port",
                          "sample": f"{steps} cycles after {warm} warm-up cycles on {threads} threads; the "
                                    "Fortran reference cannot be compiled here (no Fortran "
@@ -719,8 +774,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the FLITE_MIXED cycle rate")
     ap.add_argument("--kernel-options", default=None,
                     help="NODE_BLOCK,UNROLL,LANES_L1,...: fixed launch options instead of tuning them")
-    ap.add_argument("--converge", action="store_true",
-                    help="also measure time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
+    ap.add_argument("--no-converge", action="store_true",
+                    help="skip the time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
+    ap.add_argument("--parity-cycles", type=int, default=2,
+                    help="cycles of the GPU-vs-CPU-restatement check on the bench mesh (0: none)")
     ap.add_argument("--converge-max", type=int, default=3000)
     ap.add_argument("--batch", action="store_true", help="the batched multi-condition workload instead")
     ap.add_argument("--rans", action="store_true", help="the RANS (Spalart-Allmaras, NACA0012) workload instead")

@@ -97,7 +97,8 @@ PREPRO_SYMBOLS = [
     "fp_bump_channel", "fp_naca0012", "fp_from_tets", "fp_free", "fp_num_levels", "fp_level_desc",
     "fp_node_perm", "fp_check", "fp_geometry", "fp_geometry_vjp", "fp_write_sol", "fp_read_sol", "fp_write_rst", "fp_read_rst",
     "fp_write_res", "fp_write_unk", "fp_read_unk", "fp_write_plotreg", "fp_makeplot", "fp_write_plt",
-    "fp_read_inp", "fp_parse_inp_text",
+    "fp_read_inp", "fp_parse_inp_text", "fp_rsd_line", "fp_append_rsd", "fp_cycle_line",
+    "fp_controls_default", "fp_controls_derive",
 ]
 
 _libs = {}

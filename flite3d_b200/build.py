@@ -56,12 +56,14 @@ def _sources(dirname, exts):
 
 
 def build_prepro(force=False, verbose=False):
-    src = [os.path.join(CSRC, "prepro", f) for f in ("prepro.cpp", "namelist.cpp")]
+    # the controls defaults are compiled in as fp_controls_default/derive
+    src = [os.path.join(CSRC, "prepro", f) for f in ("prepro.cpp", "namelist.cpp", "text_io.cpp")] + \
+        [os.path.join(CSRC, "solver", "controls.cpp")]
     deps = src + _sources(os.path.join(CSRC, "prepro"), {".hpp", ".h"}) + _sources(INC, {".h"})
     out = os.path.join(PKG, "libflite_prepro.so")
     if force or _stale(out, deps):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", f"-I{INC}", *src, "-o", out],
-             verbose)
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-DFLITE_CONTROLS_FP", f"-I{INC}",
+              *src, "-o", out], verbose)
     return out
 
 

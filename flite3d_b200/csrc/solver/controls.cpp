@@ -1,11 +1,21 @@
 // Controls defaults and derived values (readInputVariables,
 // SolverSource/mgnsg3d_def_par.F90:201-422).
+//
+// The same two functions are compiled into the host preprocessor library
+// under the fp_ prefix (FLITE_CONTROLS_FP defined), so a host-only program
+// can fill the controls without loading the CUDA library.
 #include <cmath>
 #include <cstring>
 
 #include "flite_gpu.h"
 
-extern "C" int flite_controls_default(flite_controls *c) {
+#ifdef FLITE_CONTROLS_FP
+#define FLITE_CONTROLS_FN(name) fp_##name
+#else
+#define FLITE_CONTROLS_FN(name) flite_##name
+#endif
+
+extern "C" int FLITE_CONTROLS_FN(controls_default)(flite_controls *c) {
     if (!c) return FLITE_EINVAL;
     std::memset(c, 0, sizeof *c);
     // def_par:217-378, in the order they appear there
@@ -92,7 +102,7 @@ extern "C" int flite_controls_default(flite_controls *c) {
     return FLITE_OK;
 }
 
-extern "C" int flite_controls_derive(flite_controls *c) {
+extern "C" int FLITE_CONTROLS_FN(controls_derive)(flite_controls *c) {
     if (!c) return FLITE_EINVAL;
     // def_par:387-415
     if (c->flowType == 0) c->maximumnumberofcycles = 1000000;

@@ -52,6 +52,8 @@ const char *unsupported_reason(const flite_controls &c) {
     if (c.flowType != 0 && c.flowType != 1) return "flowType must be 0 (steady) or 1 (unsteady, static mesh)";
     if (c.explicit_) return "explicit time stepping is not supported";
     if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return "unsteady runs need physicalTimeStep > 0";
+    if (c.forceCalcType != 1 && c.forceCalcType != 3)
+        return "forceCalcType must be 1 or 3 (2 is the spanwise load of gust runs)";
     if (c.SAS || c.GUSTMODEL || c.movingwall || c.patchInitialization || c.nspan != 0)
         return "SAS, gust, moving-wall, patch initialisation and spanwise loads are not supported";
     if (c.residualSmoothingFactor > 0 || c.prolongationSmoothingFactor > 0)
@@ -557,24 +559,47 @@ int flite_residuals(flite_ctx *ctx, double res[7], double maxres[7], int32_t max
     });
 }
 
-int flite_forces(flite_ctx *ctx, double out[6]) {
+int flite_forces(flite_ctx *ctx, double out[9]) {
     if (!ctx || !out) return FLITE_EINVAL;
     return guarded(ctx, [&] {
         flite_ctx &X = *ctx;
         DevLevel &D = X.lv[0];
         const double PI = 4.0 * std::atan(1.0);
-        if (D.wall.empty()) {
-            for (int k = 0; k < 6; ++k) out[k] = 0.0;
-            return FLITE_OK;
+        for (int k = 0; k < 9; ++k) out[k] = 0.0;
+        if (D.wall.empty()) return FLITE_OK;
+        const double aR = X.c.alpha * PI / 180., bR = X.c.beta * PI / 180.;
+        const bool calc3 = X.c.forceCalcType == 3;
+        // partials: calculateLiftAndDrag's 6 sums per block, then (type 3)
+        // calculateLiftAndDrag3's 7 sums per block
+        double *part1 = X.d_part, *part3 = X.d_part + 6 * kForceBlocks;
+        k_forces<<<kForceBlocks, 256, 0, X.s>>>(X.P, D.v, D.d_wall, (int)D.wall.size(), aR, bR, X.c.groundplane,
+                                               X.c.datum[0], X.c.datum[1], X.c.datum[2], part1);
+        k_forces_final<<<1, 32, 0, X.s>>>(part1, kForceBlocks, 6, X.d_out);
+        if (calc3) {
+            k_forces3<<<kForceBlocks, 256, 0, X.s>>>(X.P, D.v, D.d_wall, (int)D.wall.size(), aR, bR,
+                                                    X.c.groundplane, X.c.datum[0], X.c.datum[1], X.c.datum[2],
+                                                    part3);
+            k_forces_final<<<1, 32, 0, X.s>>>(part3, kForceBlocks, 7, X.d_out + 8);
         }
-        k_forces<<<kForceBlocks, 256, 0, X.s>>>(X.P, D.v, D.d_wall, (int)D.wall.size(), X.c.alpha * PI / 180.,
-                                               X.c.beta * PI / 180., X.c.groundplane, X.c.datum[0],
-                                               X.c.datum[1], X.c.datum[2], X.d_part);
-        k_forces_final<<<1, 32, 0, X.s>>>(X.d_part, kForceBlocks, X.d_out);
-        double h[6];
+        double h[15];
         CK(cudaMemcpyAsync(h, X.d_out, sizeof h, cudaMemcpyDeviceToHost, X.s));
         CK(cudaStreamSynchronize(X.s));
-        for (int k = 0; k < 6; ++k) out[k] = k < 4 ? h[k] / X.c.referenceArea : h[k];
+        const double A = X.c.referenceArea;
+        // lift, drag, latF, frictionDrag as coefficients; latM, longM as sums
+        for (int k = 0; k < 6; ++k) out[k] = k < 4 ? 2.0 * h[k] / A : h[k];
+        if (calc3) {
+            // writeResiduals (mg_par:1364-1366): type 3 replaces lift, drag,
+            // latF and latM and adds longMl, longMd and rollM; frictionDrag
+            // and longM stay calculateLiftAndDrag's
+            const double *g = h + 8;
+            out[0] = 2.0 * g[0] / A;
+            out[1] = 2.0 * g[1] / A;
+            out[2] = 2.0 * g[2] / A;
+            out[4] = 2.0 * g[3] / A;
+            out[6] = 2.0 * g[4] / A;
+            out[7] = 2.0 * g[5] / A;
+            out[8] = 2.0 * g[6] / A;
+        }
         return FLITE_OK;
     });
 }

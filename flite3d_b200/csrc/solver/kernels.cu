@@ -1673,11 +1673,70 @@ __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, doub
         for (int k = 0; k < 6; ++k) part[6 * blockIdx.x + k] = red[k][0];
 }
 
-__global__ void k_forces_final(const double *part, int nblk, double *out) {
-    if (threadIdx.x >= 6) return;
+// ---- forces of forceCalcType 3 (calculateLiftAndDrag3 def_par:15129-15313)
+// Per wall node (indicator register -20..-19) the face loads of its wall and
+// inviscid-wall faces (codes 1, 9) with a node above the ground plane, in
+// boundary-edge order as the reference's scatter adds them: 4 w_b (p - p_inf)
+// and, in viscous runs on code-1 faces, 4 tau_w |w_b|.  Then the seven sums
+// part[7*block + k] = (lift, drag, latF, latM, longMl, longMd, rollM).
+__global__ void k_forces3(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
+                          double ground, double d0, double d1, double d2, double *part) {
+    __shared__ double red[7][256];
+    double ft[3] = {cos(alphaR) * cos(betaR), sin(betaR), sin(alphaR)};
+    double fn1[3] = {-ft[2], 0.0, ft[0]}, fn2[3] = {-ft[1], ft[0], 0.0};
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const double pinf = 1. / (P.gamma * P.mach * P.mach);
+    const int N = L.N;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nwall; q += gridDim.x * blockDim.x) {
+        const int ip = wall[q];
+        double h0 = 0.0, h1 = 0.0, h2 = 0.0;
+        for (int k = L.binc_ptr[ip]; k < L.binc_ptr[ip + 1]; ++k) {
+            const int b = L.binc[k] >> 1;
+            const int code = L.bind[b];
+            if (!(code == 1 || code == 9)) continue;
+            const int2 nd = L.bedge[b];
+            if (!((L.cz[nd.x] > (ground + 0.01)) || (L.cz[nd.y] > (ground + 0.01)))) continue;
+            const double pp = L.p[ip] - pinf;
+            const double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
+            h0 = h0 + 4.0 * wx * pp;
+            h1 = h1 + 4.0 * wy * pp;
+            h2 = h2 + 4.0 * wz * pp;
+            if (P.viscous && code == 1) {
+                const double area = sqrt((wx * wx + wy * wy) + wz * wz);
+                h0 = h0 + 4.0 * L.wstress[ip] * area;
+                h1 = h1 + 4.0 * L.wstress[N + ip] * area;
+                h2 = h2 + 4.0 * L.wstress[2 * N + ip] * area;
+            }
+        }
+        const double xd = L.cx[ip] - d0, yd = L.cy[ip] - d1, zd = L.cz[ip] - d2;
+        const double hn1 = (h0 * fn1[0] + h1 * fn1[1]) + h2 * fn1[2];
+        const double hn2 = (h0 * fn2[0] + h1 * fn2[1]) + h2 * fn2[2];
+        const double ht = (h0 * ft[0] + h1 * ft[1]) + h2 * ft[2];
+        acc[0] += hn1;
+        acc[1] += ht;
+        acc[2] += hn2;
+        acc[3] += -xd * hn2 + yd * ht;
+        acc[4] += -xd * hn1;
+        acc[5] += zd * ht;
+        acc[6] += -yd * hn1 + zd * hn2;
+    }
+    for (int k = 0; k < 7; ++k) red[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 7; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 7; ++k) part[7 * blockIdx.x + k] = red[k][0];
+}
+
+// out[k] = sum over blocks of part[nval*block + k], in block order
+__global__ void k_forces_final(const double *part, int nblk, int nval, double *out) {
+    if (threadIdx.x >= nval) return;
     const int k = threadIdx.x;
     double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[6 * b + k];
-    out[k] = k < 4 ? 2.0 * s : s;
+    for (int b = 0; b < nblk; ++b) s += part[nval * b + k];
+    out[k] = s;
 }
 }  // namespace flite

@@ -61,7 +61,9 @@ __global__ void k_resid_partial(LevelView L, double *part, int nblk);
 __global__ void k_resid_final(const double *part, int nblk, double *out);
 __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
                          double ground, double d0, double d1, double d2, double *part);
-__global__ void k_forces_final(const double *part, int nblk, double *out);
+__global__ void k_forces3(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
+                          double ground, double d0, double d1, double d2, double *part);
+__global__ void k_forces_final(const double *part, int nblk, int nval, double *out);
 constexpr int kForceBlocks = 64;
 // transposed residual Jacobian at the state x (adjoint.cu)
 __global__ void k_vjp_farfield(Params P, LevelView L, const double *x, const double *rbar, double *bvjp);

@@ -13,12 +13,13 @@
 // The scratch array below is part of the library image: every GPU that loads
 // the library holds kScratchBytes of it until the process exits.  Its device
 // address is looked up once per device with cudaGetSymbolAddress, on the
-// first call made while that device is current.  That first call should come
-// before any CUDA stream capture.  All calls share the one array and it keeps
-// the last call's contents; each call re-initialises what must start at zero.
-// Calls that overlap on the GPU (different streams, or different host
-// threads on the same device) race on the scratch and must be serialised by
-// the caller.
+// first call made while that device is current.  A call copies its status
+// into host memory and synchronises the stream it is given, so no call may be
+// made while any stream is being captured into a CUDA graph.  All calls share
+// the one array and it keeps the last call's contents; each call
+// re-initialises what must start at zero.  Calls that overlap on the GPU
+// (different streams, or different host threads on the same device) race on
+// the scratch and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -61,21 +62,32 @@ __global__ void na_clear_flag(int *flag) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *flag = 0;
 }
 
-// 0-based copies of the caller's 1-based index arrays; an index outside
-// 1..N raises the error flag and its edge is dropped from every pass
+// Bits of the error flag: an index outside 1..N or a boundary code outside
+// 1..9 (FLITE_EINVAL), an engine face, codes 5..8 (FLITE_EUNSUPPORTED, as
+// flite_create refuses them for flite_residual_fwd).
+constexpr int kFlagInvalid = 1;
+constexpr int kFlagEngine = 2;
+
+// 0-based copies of the caller's 1-based index arrays; an edge that raises
+// the error flag is dropped from every pass
 __global__ void na_prepare(int N, int E, int B, const int32_t *side_idx, const int32_t *bnd_idx,
                            int2 *edge, int2 *bedge, int *bind, int *inc_ptr, int *binc_ptr, int *flag) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < E) {
         int a = side_idx[t] - 1, b = side_idx[E + t] - 1;
-        if (a < 0 || a >= N || b < 0 || b >= N || a == b) { atomicExch(flag, 1); a = -1; b = -1; }
+        if (a < 0 || a >= N || b < 0 || b >= N || a == b) { atomicOr(flag, kFlagInvalid); a = -1; b = -1; }
         edge[t] = make_int2(a, b);
     }
     if (t < B) {
         int a = bnd_idx[t] - 1, b = bnd_idx[B + t] - 1;
-        if (a < 0 || a >= N || b < 0 || b >= N) { atomicExch(flag, 1); a = -1; b = -1; }
+        const int code = bnd_idx[2 * B + t];
+        if (a < 0 || a >= N || b < 0 || b >= N || code < 1 || code > 9) {
+            atomicOr(flag, kFlagInvalid); a = -1; b = -1;
+        } else if (code >= 5 && code <= 8) {
+            atomicOr(flag, kFlagEngine); a = -1; b = -1;
+        }
         bedge[t] = make_int2(a, b);
-        bind[t] = bnd_idx[2 * B + t];
+        bind[t] = code;
     }
     if (t <= N) { inc_ptr[t] = 0; binc_ptr[t] = 0; }
 }
@@ -281,24 +293,29 @@ extern "C" int flite_residual_noalloc(const flite_controls *c, int32_t n_nodes, 
 
     const int T = 256;
     const int nmax = (int)std::max<int64_t>(std::max<int64_t>(E, B), N + 1);
+    const int ne = std::max(E, B);
+    // an error left pending by earlier, unrelated work is not this call's
+    (void)cudaGetLastError();
     na_clear_flag<<<1, 1, 0, s>>>(flag);
     na_prepare<<<(nmax + T - 1) / T, T, 0, s>>>(N, E, B, d_side_idx, d_bnd_idx, edge, bedge, bind, inc_ptr,
                                                binc_ptr, flag);
     na_zero<<<(2 * (N + 1) + T - 1) / T, T, 0, s>>>(cursor, 2 * (N + 1));
-    na_count<<<(std::max(E, B) + T - 1) / T, T, 0, s>>>(E, B, edge, bedge, inc_ptr, binc_ptr);
+    if (ne > 0) na_count<<<(ne + T - 1) / T, T, 0, s>>>(E, B, edge, bedge, inc_ptr, binc_ptr);
     na_scan<<<1, 1024, 0, s>>>(N, inc_ptr, binc_ptr);
-    na_place<<<(std::max(E, B) + T - 1) / T, T, 0, s>>>(E, B, edge, bedge, inc_ptr, binc_ptr, cursor, bcursor,
-                                                        inc, binc);
+    if (ne > 0)
+        na_place<<<(ne + T - 1) / T, T, 0, s>>>(E, B, edge, bedge, inc_ptr, binc_ptr, cursor, bcursor, inc, binc);
     na_sort<<<(N + T - 1) / T, T, 0, s>>>(N, inc_ptr, binc_ptr, inc, binc);
     na_pressure<<<(N + T - 1) / T, T, 0, s>>>(P, L);
     if (E > 0) na_edge<<<(E + T - 1) / T, T, 0, s>>>(P, L);
     if (B > 0) na_bnd<<<(B + T - 1) / T, T, 0, s>>>(P, L);
     na_gather<<<(N + T - 1) / T, T, 0, s>>>(L, d_rhs);
     if (cudaGetLastError() != cudaSuccess) return FLITE_ECUDA;
-    // the index check's verdict (a 4-byte copy into host memory; no
-    // allocation); this synchronises the caller's stream
+    // the checks' verdict (a 4-byte copy into host memory; no allocation);
+    // this synchronises the caller's stream
     int hflag = 0;
     if (cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FLITE_ECUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return FLITE_ECUDA;
-    return hflag ? FLITE_EINVAL : FLITE_OK;
+    if (hflag & kFlagInvalid) return FLITE_EINVAL;
+    if (hflag & kFlagEngine) return FLITE_EUNSUPPORTED;
+    return FLITE_OK;
 }

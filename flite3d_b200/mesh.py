@@ -227,6 +227,36 @@ def makeplot(plotreg, res_prefix, nvar, unk):
                "fp_makeplot")
 
 
+def rsd_line(iteration, res1, initial_res, forces, res, force_calc_type=1):
+    """One line of the .rsd residual history (writeResiduals format 504,
+    mg_par:1481-1514); forces as Solver.forces() returns them, res the norms
+    of Solver.residuals()."""
+    f = (ctypes.c_double * 9)(*[float(x) for x in forces[:9]])
+    r = (ctypes.c_double * 7)(*[float(x) for x in list(res)[:7]])
+    buf = ctypes.create_string_buffer(512)
+    _abi.check(_lib().fp_rsd_line(buf, len(buf), int(iteration), _c_double(res1), _c_double(initial_res), f, r,
+                                  len(res), int(force_calc_type)), "fp_rsd_line")
+    return buf.value.decode()
+
+
+def append_rsd(path, first, iteration, res1, initial_res, forces, res, force_calc_type=1):
+    """Write that line to path: a new file when first, else appended."""
+    f = (ctypes.c_double * 9)(*[float(x) for x in forces[:9]])
+    r = (ctypes.c_double * 7)(*[float(x) for x in list(res)[:7]])
+    _abi.check(_lib().fp_append_rsd(str(path).encode(), int(bool(first)), int(iteration), _c_double(res1),
+                                    _c_double(initial_res), f, r, len(res), int(force_calc_type)), "fp_append_rsd")
+
+
+def cycle_line(iteration, res, maxres, scale, lift, drag):
+    """The screen line of writeResiduals (format 501, mg_par:1451-1456)."""
+    r = (ctypes.c_double * 5)(*[float(x) for x in res[:5]])
+    m = (ctypes.c_double * 5)(*[float(x) for x in maxres[:5]])
+    buf = ctypes.create_string_buffer(512)
+    _abi.check(_lib().fp_cycle_line(buf, len(buf), int(iteration), r, m, _c_double(scale), _c_double(lift),
+                                    _c_double(drag)), "fp_cycle_line")
+    return buf.value.decode()
+
+
 def primitive_to_conserved(prim):
     """The restart conversion u(2:5) = rho*u(2:5) (def_par:3850-3856)."""
     prim = np.asarray(prim, dtype=np.float64)

@@ -40,6 +40,21 @@ def default_controls(**overrides):
     return c
 
 
+def host_controls(**overrides):
+    """default_controls computed by the host preprocessor library alone (the
+    same defaults and derivation compiled without CUDA), for programs that
+    must not load the GPU library."""
+    lib = _abi.prepro_lib()
+    c = _abi.Controls()
+    _abi.check(lib.fp_controls_default(ctypes.byref(c)), "fp_controls_default")
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise KeyError(f"unknown control {k}")
+        setattr(c, k, v)
+    _abi.check(lib.fp_controls_derive(ctypes.byref(c)), "fp_controls_derive")
+    return c
+
+
 def controls_from_inp(path_or_text, **overrides):
     """Defaults, then the &InputVariables deck, then overrides, then derive."""
     lib = _abi.gpu_lib()
@@ -165,7 +180,9 @@ class Solver:
         return np.array(res[:n]), np.array(mres[:n]), np.array(mind[:n])
 
     def forces(self):
-        out = (ctypes.c_double * 6)()
+        """lift, drag, latF, frictionDrag, latM, longM, longMl, longMd, rollM
+        (the last three with forceCalcType 3, else 0)."""
+        out = (ctypes.c_double * 9)()
         self._ck(self.be.forces(self._h, out), "forces")
         return np.array(out[:])
 
@@ -336,19 +353,28 @@ def initial_state(controls, mesh, perturb_seed=None, amplitude=0.01):
     return u
 
 
-def run_steady(solver, orders=8.0, max_cycles=1000, callback=None):
+def run_steady(solver, orders=8.0, max_cycles=1000, callback=None, rsd=None, screen=None):
     """Convergence loop of multiGridCycles (mg_par:789-816): cycles until
     log(res0)-log(res) >= orders*log(10) or max_cycles.  Returns the history
-    of (cycle, res1, lift, drag)."""
+    of (cycle, res1, lift, drag).  With rsd (a path) every cycle appends the
+    residual-history line of writeResiduals to that file, the first cycle
+    starting it afresh; with screen (a callable taking a string) every cycle
+    passes it the reference's screen line (mg_par:1449-1516)."""
+    from .mesh import append_rsd, cycle_line
     hist = []
     res0 = None
     for it in range(1, max_cycles + 1):
         solver.cycle(it)
-        res, _, _ = solver.residuals()
+        res, maxres, _ = solver.residuals()
         f = solver.forces()
         if res0 is None:
             res0 = res[0]
         hist.append((it, res[0], f[0], f[1]))
+        if rsd is not None:
+            append_rsd(rsd, it == 1, it, res[0], res0, f, res, solver.c.forceCalcType)
+        if screen is not None:
+            scale = 1.0 / float(solver.c.numberOfProcesses * solver.nodes[0])
+            screen(cycle_line(it, res[:5], maxres[:5], scale, f[0], f[1]))
         if callback:
             callback(it, res, f)
         if not (math.log(res0) - math.log(res[0]) < math.log(10.0) * orders):

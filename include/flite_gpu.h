@@ -7,7 +7,8 @@
  * for one; the reference routine it replaces is cited beside it.  All arrays
  * cross the boundary as plain host pointers in the reference's own layout
  * (Fortran column-major, 1-based node indices), so a Fortran host can bind them
- * with ISO_C_BINDING without copies or reshapes.
+ * with ISO_C_BINDING without copies or reshapes (the interface module
+ * include/flite_gpu_mod.f90 declares them for Fortran).
  *
  * Every function returns an int status (FLITE_OK on success).  The reference
  * STOPs on errors; this library returns a code and keeps a message that
@@ -198,9 +199,13 @@ int flite_cycle(flite_ctx *ctx, int cycle_no);
  * FLITE_ENAN when any res_k is not finite (the reference STOPs).          */
 int flite_residuals(flite_ctx *ctx, double res[7], double maxres[7],
                     int32_t maxind[7]);
-/* calculateLiftAndDrag (def_par:14710-14870): out = {lift, drag, latF,
- * frictionDrag, latM, longM} as coefficients.                              */
-int flite_forces(flite_ctx *ctx, double out[6]);
+/* the forces of writeResiduals (mg_par:1359-1367): calculateLiftAndDrag
+ * (def_par:14710-14870) gives out[0..5] = {lift, drag, latF, frictionDrag,
+ * latM, longM}, the first four as coefficients; with forceCalcType 3,
+ * calculateLiftAndDrag3 (def_par:15129-15313) replaces lift, drag, latF and
+ * latM and fills out[6..8] = {longMl, longMd, rollM} (else 0).  These are
+ * the force columns of the .rsd file (mg_par:1481-1507).                   */
+int flite_forces(flite_ctx *ctx, double out[9]);
 
 /* ---- one residual evaluation (adjoint primal / parity probe) ----------- */
 /* rhs = makeRHS(u) on a level (def_par:1525-2590) with the level's current
@@ -306,11 +311,14 @@ int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_bloc
  * [2][E] and bnd_idx [3][B] 1-based, side_w [3][E], bnd_w [3][B], u [5][N];
  * writes rhs [5][N].  Scratch lives in one static device array of the
  * library (24,380,160 bytes on every GPU that loads it); limits N <= 65536,
- * E <= 262144, B <= 65536, larger sizes return FLITE_EINVAL, as does an
- * index outside 1..N.  The first call on a device looks the scratch up for
- * that device and should come before any stream capture.  Calls share the
- * scratch: calls that overlap on the GPU race.  The call runs on `stream`
- * (a cudaStream_t, NULL for the default stream) and synchronises it.      */
+ * E <= 262144, B <= 65536, larger sizes return FLITE_EINVAL, as do an
+ * index outside 1..N and a boundary code outside 1..9; engine faces (codes
+ * 5..8) return FLITE_EUNSUPPORTED, as flite_create does.  The first call on
+ * a device looks the scratch up for that device.  The call runs on `stream`
+ * (a cudaStream_t, NULL for the default stream), copies its status to host
+ * memory and synchronises the stream, so it must not be made while any
+ * stream is being captured.  Calls share the scratch: calls that overlap on
+ * the GPU race.                                                            */
 int flite_residual_noalloc(const flite_controls *c, int32_t n_nodes, int32_t n_sides,
                            int32_t n_bsides, const int32_t *d_side_idx, const double *d_side_w,
                            const int32_t *d_bnd_idx, const double *d_bnd_w, const double *d_u,

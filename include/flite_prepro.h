@@ -86,6 +86,27 @@ int fp_makeplot(const char *plotreg, const char *res_prefix, int nvar, const cha
  * x(3,N); iface(5,nBF) with column 5 the surface (indicator) number.       */
 int fp_write_plt(const fp_mesh *m, const char *path);
 
+/* ---- residual history (writeResiduals, mg_par:1449-1516) ------------- */
+/* One .rsd line (format 504): iteration, log10(res1/initial_res) (-100/ln10
+ * below 1e-15), lift, drag (E14.5), then F13.6 columns: latF, frictionDrag,
+ * latM and longM with log10 res(2..nres), or with forceCalcType 3 longMl,
+ * longMd, rollM.  forces as flite_forces fills them; res[nres].            */
+int fp_rsd_line(char *buf, size_t len, int32_t iteration, double res1, double initial_res,
+                const double forces[9], const double *res, int32_t nres, int32_t force_calc_type);
+/* The same line written to path: a new file when first != 0, else appended
+ * (the reference reopens the file for every cycle, mg_par:1481-1488).       */
+int fp_append_rsd(const char *path, int32_t first, int32_t iteration, double res1, double initial_res,
+                  const double forces[9], const double *res, int32_t nres, int32_t force_calc_type);
+/* The screen line of a cycle (format 501): iteration, then res_k * scale
+ * with (max |u - uprev|) for k = 1..5, then lift and drag; the reference's
+ * scale is 1/(numberOfProcesses * N) (def_par:14258).                      */
+int fp_cycle_line(char *buf, size_t len, int32_t iteration, const double res[5], const double maxres[5],
+                  double scale, double lift, double drag);
+
+/* ---- controls (the defaults and derivation of flite_gpu.h, host only) -- */
+int fp_controls_default(flite_controls *c);
+int fp_controls_derive(flite_controls *c);
+
 /* ---- controls deck -------------------------------------------------- */
 /* Parse "&InputVariables ivd%key = value, ... /" onto c (which should hold
  * defaults).  Unknown keys are listed (comma separated) in unknown.         */

@@ -1847,6 +1847,59 @@ struct Oracle {
         out[3] = 2.0 * fric / c.referenceArea;
         out[4] = latM;
         out[5] = longM;
+        out[6] = out[7] = out[8] = 0.0;
+        if (c.forceCalcType == 3) {
+            // writeResiduals (mg_par:1364-1366): calculateLiftAndDrag3
+            // replaces lift, drag, latF, latM and adds longMl, longMd, rollM
+            double f3[7];
+            forces3(f3);
+            out[0] = f3[0]; out[1] = f3[1]; out[2] = f3[2]; out[4] = f3[3];
+            out[6] = f3[4]; out[7] = f3[5]; out[8] = f3[6];
+        }
+    }
+
+    // ---- calculateLiftAndDrag3 (def_par:15129-15313) ------------------------
+    // The face loads go through the shared nodeHelpArray(:, 1:3), as in the
+    // reference (its columns 1..3 are zeroed first and left holding them).
+    void forces3(double *out) {
+        Level &g = lv[0];
+        for (int k = 0; k < 3; ++k) std::fill(nh[k].begin(), nh[k].end(), 0.0);
+        const double pinf = 1. / (c.gamma * c.MachNumber * c.MachNumber);
+        for (int b = 0; b < g.B; ++b) {
+            const int i1 = g.b1[b], i2 = g.b2[b], ind = g.bind[b];
+            if (!(ind == 1 || ind == 9)) continue;
+            if (!((g.cz[i1] > (c.groundplane + 0.01)) || (g.cz[i2] > (c.groundplane + 0.01)))) continue;
+            const double p1 = g.p[i1] - pinf, p2 = g.p[i2] - pinf;
+            const double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
+            for (int k = 0; k < 3; ++k) nh[k][i1] = nh[k][i1] + 4.0 * w[k] * p1;
+            for (int k = 0; k < 3; ++k) nh[k][i2] = nh[k][i2] + 4.0 * w[k] * p2;
+            if (c.ReynoldsNumber > 0.0 && ind == 1) {
+                const double area = std::sqrt((w[0] * w[0] + w[1] * w[1]) + w[2] * w[2]);
+                for (int k = 0; k < 3; ++k) nh[k][i1] = nh[k][i1] + 4.0 * g.wallStress[k][i1] * area;
+                for (int k = 0; k < 3; ++k) nh[k][i2] = nh[k][i2] + 4.0 * g.wallStress[k][i2] * area;
+            }
+        }
+        const double PI = 4.0 * std::atan(1.0);
+        double aR = c.alpha * PI / 180., bR = c.beta * PI / 180.;
+        double ft[3] = {std::cos(aR) * std::cos(bR), std::sin(bR), std::sin(aR)};
+        double fn1[3] = {-ft[2], 0.0, ft[0]}, fn2[3] = {-ft[1], ft[0], 0.0};
+        double lift = 0, drag = 0, latF = 0, latM = 0, longMl = 0, longMd = 0, rollM = 0;
+        for_range(g, -20, -19, [&](int ip) {
+            double xd = g.cx[ip] - c.datum[0], yd = g.cy[ip] - c.datum[1], zd = g.cz[ip] - c.datum[2];
+            auto hd = [&](const double *a) { return (nh[0][ip] * a[0] + nh[1][ip] * a[1]) + nh[2][ip] * a[2]; };
+            lift = lift + hd(fn1);
+            drag = drag + hd(ft);
+            latF = latF + hd(fn2);
+            latM = latM - xd * hd(fn2);
+            latM = latM + yd * hd(ft);
+            rollM = rollM - yd * hd(fn1);
+            rollM = rollM + zd * hd(fn2);
+            longMl = longMl - xd * hd(fn1);
+            longMd = longMd + zd * hd(ft);
+        });
+        const double A = c.referenceArea;
+        out[0] = 2.0 * lift / A; out[1] = 2.0 * drag / A; out[2] = 2.0 * latF / A; out[3] = 2.0 * latM / A;
+        out[4] = 2.0 * longMl / A; out[5] = 2.0 * longMd / A; out[6] = 2.0 * rollM / A;
     }
 };
 
@@ -1860,6 +1913,7 @@ int check_controls(const flite_controls &c) {
     // Spalart-Allmaras (1) is on the path and needs a viscous run; k-omega
     // and SST (2, 3) are not
     if (c.turbulenceModel != 0 && c.turbulenceModel != 1) return FLITE_EUNSUPPORTED;
+    if (c.forceCalcType != 1 && c.forceCalcType != 3) return FLITE_EUNSUPPORTED;
     if (c.turbulenceModel == 1 && !(c.ReynoldsNumber > 0)) return FLITE_EUNSUPPORTED;
     if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return FLITE_EUNSUPPORTED;
     if (c.fluxType < 1 || c.fluxType > 4) return FLITE_EUNSUPPORTED;
@@ -2707,7 +2761,7 @@ int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[
     return FLITE_OK;
 }
 
-int oracle_forces(oracle_ctx *o, double out[6]) {
+int oracle_forces(oracle_ctx *o, double out[9]) {
     if (!o || !out) return FLITE_EINVAL;
     o->o.forces(out);
     return FLITE_OK;

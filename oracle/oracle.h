@@ -39,7 +39,7 @@ int oracle_cycle(oracle_ctx *o, int cycle_no);
 /* unsteady runs: close the physical time step, open the next one          */
 int oracle_next_physical_step(oracle_ctx *o);
 int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[7]);
-int oracle_forces(oracle_ctx *o, double out[6]);
+int oracle_forces(oracle_ctx *o, double out[9]);
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);
 /* the artificial dissipation (time steps, then the run's scheme) at the state u */
 int oracle_dissipation(oracle_ctx *o, int level, const double *u, double *diss);

@@ -48,3 +48,34 @@ def test_create_rejects_unsupported_controls():
         assert lib.flite_last_error(None, buf, len(buf)) == _abi.FLITE_OK
         assert buf.value, bad
     assert b"multigridScheme" in buf.value
+
+
+def test_fortran_interface_module_matches_the_c_abi():
+    # include/flite_gpu_mod.f90: its bind(C) names are exported symbols and
+    # its flite_controls type lists the C struct's fields in order and kind
+    text = open(os.path.join(ROOT, "include", "flite_gpu_mod.f90")).read()
+    code = "\n".join(ln.split("!")[0] for ln in text.splitlines())
+    code = code.replace("&\n", " ")
+    lib = _abi.gpu_lib()
+    names = re.findall(r'bind\(C,\s*name="(\w+)"\)', code)
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(lib, n), n
+    body = re.search(r"type, bind\(C\) :: flite_controls\n(.*?)end type flite_controls", code, re.S).group(1)
+    fields = []
+    for ln in body.splitlines():
+        m = re.match(r"\s*(real|integer)\(c_(\w+)\)\s*::\s*(.*)", ln)
+        if not m:
+            continue
+        for item in m.group(3).split(","):
+            item = item.strip()
+            if not item:
+                continue
+            nm = re.match(r"(\w+)(?:\((\d+)\))?", item)
+            fields.append((nm.group(1), m.group(2), int(nm.group(2) or 1)))
+    want = []
+    for name, typ in _abi.Controls._fields_:
+        n = getattr(typ, "_length_", 1)
+        base = typ._type_ if hasattr(typ, "_length_") else typ
+        want.append((name, "double" if base is ctypes.c_double else "int", n))
+    assert fields == want

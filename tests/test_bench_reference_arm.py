@@ -43,3 +43,15 @@ def test_product_arm_refuses_to_run_without_a_gpu():
                               "--warmup", "3", *extra], capture_output=True, text=True, timeout=600, cwd=ROOT)
         assert out.returncode != 0
         assert "no CPU fallback" in out.stderr + out.stdout
+
+
+def test_reference_arm_does_not_load_the_cuda_library():
+    # the CPU arm fills its controls from the host library: the product's
+    # CUDA library must not be mapped into its process
+    code = ("import sys, bench; sys.argv = ['bench.py', '--impl', 'reference', '--mesh', '8,4,4', '--steps', '1', "
+            "'--warmup', '3']; bench.main(); maps = open('/proc/self/maps').read(); "
+            "print('GPULIB' if 'libflite_gpu.so' in maps else 'NOGPULIB')")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT,
+                         env={**os.environ, "WORLD_SIZE": "1", "RANK": "0"})
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "NOGPULIB" in out.stdout

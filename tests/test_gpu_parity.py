@@ -53,6 +53,10 @@ CASES = {
                                       secondOrderDissipationFactor=0.6),
     "laminar_matrix_dissipation": dict(fluxType=1, useMatrixDissipation=1, ReynoldsNumber=5000.0,
                                        wallsAreIsentropic=1),
+    # forceCalcType 3 (calculateLiftAndDrag3): its face loads pass through
+    # the reference's shared help array, which the cycles after it must not see
+    "laminar_forces_type3": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=1, forceCalcType=3,
+                                 alpha=2.0, beta=1.0),
     # the upwind MUSCL / Van Albada extension and the five-stage scheme (no
     # reference counterpart): the GPU against the same extension on the CPU
     "roe_muscl_va_rk5": dict(fluxType=3, reconstruction=1, rungeKuttaStages=5,
