@@ -2792,6 +2792,27 @@ int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r) {
     return FLITE_OK;
 }
 
+// makeViscosityTerm (def_par:5198-5893) alone at the state u of a level:
+// pressure, |p|, then the term subtracted from a zeroed dissipation array;
+// diss [5][N] out (column 1 stays 0), with the laminar viscosity mu [N] and,
+// on level 1, the wall stress [3][N] it leaves behind
+int oracle_viscous_term(oracle_ctx *o, int level, const double *u, double *diss, double *mu,
+                        double *wall_stress) {
+    Level *g = lvl(o, level);
+    if (!g || !u || !diss || !mu || !wall_stress) return FLITE_EINVAL;
+    for (int k = 0; k < 5; ++k) std::memcpy(g->u[k].data(), u + (size_t)k * g->N, 8 * (size_t)g->N);
+    o->o.makePressureField(*g, g->u);
+    for (int i = 0; i < g->N; ++i) g->p[i] = std::fabs(g->p[i]);
+    for (int k = 0; k < 5; ++k) std::fill(g->diss[k].begin(), g->diss[k].end(), 0.0);
+    o->o.makeViscosityTerm(*g);
+    for (int k = 0; k < 5; ++k) std::memcpy(diss + (size_t)k * g->N, g->diss[k].data(), 8 * (size_t)g->N);
+    std::memcpy(mu, g->mu.data(), 8 * (size_t)g->N);
+    for (int k = 0; k < 3; ++k)
+        if (!g->wallStress[k].empty())
+            std::memcpy(wall_stress + (size_t)k * g->N, g->wallStress[k].data(), 8 * (size_t)g->N);
+    return FLITE_OK;
+}
+
 // one column of the shared help array (nodeHelpArray(:, col + 1)) after the
 // last evaluation, for tests of the dissipation schemes' intermediate sums
 int oracle_help_column(oracle_ctx *o, int col, double *out) {

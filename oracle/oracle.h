@@ -43,6 +43,10 @@ int oracle_forces(oracle_ctx *o, double out[9]);
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);
 /* the artificial dissipation (time steps, then the run's scheme) at the state u */
 int oracle_dissipation(oracle_ctx *o, int level, const double *u, double *diss);
+/* makeViscosityTerm alone at the state u: diss [5][N] (subtracted from
+ * zero), the laminar viscosity mu [N] and the wall stress [3][N] (level 1) */
+int oracle_viscous_term(oracle_ctx *o, int level, const double *u, double *diss, double *mu,
+                        double *wall_stress);
 /* nodeHelpArray(:, col + 1) of level 1 after the last evaluation */
 int oracle_help_column(oracle_ctx *o, int col, double *out);
 /* pinned exp (which 0) / log (which 1) of the SA source term            */
