@@ -119,6 +119,18 @@ def build_case(host_only=False):
     return F, mesh, c, u0, time.time() - t0
 
 
+def node_kernel_name(lanes, tiled, unroll):
+    """The instance of the level-1 node kernel the tuned launch options run."""
+    what = ("(level 1: central fluxes of the incident edges computed in the node gather, fused with the RK "
+            "stage update")
+    if lanes == 1 and tiled and unroll == 1:
+        return (f"k_node_update_tiled<{3 if tiled == 2 else 2}> {what}; node blocks and their halo staged in "
+                "shared memory)")
+    if lanes == 1 and unroll == 2:
+        return f"k_node_update<GATHER_CENTRAL2, 1> {what})"
+    return f"k_node_update<GATHER_CENTRAL, {lanes}> {what})"
+
+
 def node_kernel_bytes(mesh):
     """Algorithmic bytes of one launch of the dominant kernel on level 1: the
     node kernel that computes the central fluxes of every incident edge and
@@ -167,6 +179,8 @@ def run_ours(args):
         v = [int(x) for x in args.kernel_options.split(",")]
         best = (v[0], v[1])
         lanes = {lvl: v[1 + lvl] for lvl in range(1, solver.nlevels + 1)}
+        tm = [int(x) for x in args.tiled_modes.split(",")] if args.tiled_modes else []
+        tiled = {lvl: (tm[lvl - 1] if lvl - 1 < len(tm) else 1) for lvl in range(1, solver.nlevels + 1)}
     else:
         for nb in (128, 256):
             for unroll in (1, 2):
@@ -174,18 +188,25 @@ def run_ours(args):
                 tuning[(nb, unroll)] = solver.profile_level(1, reps=5)[1]
         best = min(tuning, key=tuning.get)
     solver.set_kernel_options(256, best[0], best[1])
-    # lanes per node of each level's gathers, by the device time of that
-    # level's kernels over one relaxation step
+    # lanes per node of each level's gathers (and, with a thread per node,
+    # whether the fused central gather stages node blocks in shared memory:
+    # mode 0 off, 1 or 2 on), by the device time of that level's kernels over
+    # one relaxation step
+    tuning_levels = {}
     if not args.kernel_options:
-        lanes = {}
+        lanes, tiled = {}, {}
         for lvl in range(1, solver.nlevels + 1):
             t = {}
             for g in ((1, 4, 8) if lvl == 1 else (1, 4, 8, 16, 32)):
                 solver.set_gather_lanes(lvl, g)
-                t[g] = sum(solver.profile_kernels(lvl, reps=5).values())
-            lanes[lvl] = min(t, key=t.get)
+                for mode in ((0, 1, 2) if g == 1 else (0,)):
+                    solver.set_tiled_gather(lvl, mode)
+                    t[(g, mode)] = sum(solver.profile_kernels(lvl, reps=5).values())
+            lanes[lvl], tiled[lvl] = min(t, key=t.get)
+            tuning_levels[lvl] = {f"lanes{g}_tiled{m}": v for (g, m), v in t.items()}
     for lvl in range(1, solver.nlevels + 1):
         solver.set_gather_lanes(lvl, lanes[lvl])
+        solver.set_tiled_gather(lvl, tiled[lvl] if lanes[lvl] == 1 else 0)
     solver.set_state(u0)
     solver.start()
     # warm-up (also captures the cycle graph)
@@ -253,6 +274,7 @@ def run_ours(args):
         solver_m.set_kernel_options(256, best[0], 1)
         for lvl, g in lanes.items():
             solver_m.set_gather_lanes(lvl, g)
+            solver_m.set_tiled_gather(lvl, tiled[lvl] if g == 1 else 0)
         solver_m.set_state(u0)
         solver_m.start()
         for i in range(1, args.warmup + 1):
@@ -266,14 +288,14 @@ def run_ours(args):
                  "node_kernel_ms": node_m_ms, "increment_records_ms": delta_ms}
     ttc = None
     if not args.no_converge:
-        ttc = time_to_converge(F, mesh, c, u0, args.converge_max, (best[0], lanes))
+        ttc = time_to_converge(F, mesh, c, u0, args.converge_max, (best[0], lanes, tiled))
 
     cpu = None
     parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mesh, c, u0, cycles=args.cpu_cycles)
     if rank == 0 and ws == 1 and args.parity_cycles > 0:
-        parity = parity_check(F, mesh, c, u0, args.parity_cycles, (best[0], lanes))
+        parity = parity_check(F, mesh, c, u0, args.parity_cycles, (best[0], lanes, tiled))
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -297,9 +319,7 @@ def run_ours(args):
                 "resident": {"value": args.steps / resident_s, "h2d_bytes_per_step": 4,
                              "d2h_bytes_per_step": 15 * 8 + 9 * 8}},
         "gpu_launches": int(launches_per_cycle * args.steps),
-        "roofline": {"kernel": "k_node_update<GATHER_CENTRAL> (level 1: central fluxes of the "
-                               "incident edges computed in the node gather, fused with the RK "
-                               "stage update)",
+        "roofline": {"kernel": node_kernel_name(lanes[1], tiled[1], best[1]),
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
                      "algorithmic_bytes": nbytes, "launch_ms": node_ms,
@@ -311,8 +331,9 @@ def run_ours(args):
         "level1_kernel_ms": kernels_l1,
         "coarse_kernel_ms": kernels_coarse,
         "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1],
-                                           "gather_lanes_per_level": lanes},
-                                "ms": {f"nb{k[0]}_unroll{k[1]}": v for k, v in tuning.items()}},
+                                           "gather_lanes_per_level": lanes, "tiled_mode_per_level": tiled},
+                                "ms": {f"nb{k[0]}_unroll{k[1]}": v for k, v in tuning.items()},
+                                "level_ms": tuning_levels},
         "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,
                     "what": "flite_residual_vjp vs flite_residual_fwd kernels on level 1, FP64"},
     }
@@ -339,6 +360,7 @@ def time_to_converge(F, mesh, c, u0, max_cycles, options=None):
             s.set_kernel_options(256, options[0], 1)
             for lvl, g in options[1].items():
                 s.set_gather_lanes(lvl, g)
+                s.set_tiled_gather(lvl, options[2][lvl] if g == 1 else 0)
         s.set_state(u0)
         s.start()
         torch.cuda.synchronize()
@@ -381,6 +403,7 @@ def parity_check(F, mesh, c, u0, cycles, options=None):
         g.set_kernel_options(256, options[0], 1)
         for lvl, lanes in options[1].items():
             g.set_gather_lanes(lvl, lanes)
+            g.set_tiled_gather(lvl, options[2][lvl] if lanes == 1 else 0)
     o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
     t0 = time.perf_counter()
     for s in (g, o):
@@ -774,6 +797,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the FLITE_MIXED cycle rate")
     ap.add_argument("--kernel-options", default=None,
                     help="NODE_BLOCK,UNROLL,LANES_L1,...: fixed launch options instead of tuning them")
+    ap.add_argument("--tiled-modes", default=None,
+                    help="with --kernel-options: TILED_L1,TILED_L2,... (0 off, 1 or 2 on; default 1)")
     ap.add_argument("--no-converge", action="store_true",
                     help="skip the time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
     ap.add_argument("--parity-cycles", type=int, default=2,

@@ -143,10 +143,10 @@ extern "C" int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, co
             CK(cudaMalloc(&X.adj_b, 10 * maxB * sizeof(double)));
             X.adj_n = n5;
         }
-        CK(cudaMemcpyAsync(L.u, u, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
-        CK(cudaMemcpyAsync(X.adj_rbar, rbar, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        X.put_nodes(level - 1, L.u, u, 5);
+        X.put_nodes(level - 1, X.adj_rbar, rbar, 5);
         X.vjp_kernels(level - 1);
-        CK(cudaMemcpyAsync(ubar, X.adj_ubar, n5 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        X.get_nodes(level - 1, ubar, X.adj_ubar, 5);
         CK(cudaStreamSynchronize(X.s));
         return FLITE_OK;
     } catch (const std::exception &e) {
@@ -172,7 +172,8 @@ extern "C" int flite_profile_adjoint(flite_ctx *ctx, int level, int reps, double
         if (!X.adj_rbar || X.adj_n < n5) {
             std::vector<double> zero(n5, 1.0);
             std::vector<double> u(n5);
-            CK(cudaMemcpy(u.data(), L.u, n5 * sizeof(double), cudaMemcpyDeviceToHost));
+            X.get_nodes(l, u.data(), L.u, 5);
+            CK(cudaStreamSynchronize(X.s));
             std::vector<double> out(n5);
             int rc = flite_residual_vjp(ctx, level, u.data(), zero.data(), out.data());
             if (rc != FLITE_OK) return rc;

@@ -99,6 +99,50 @@ struct flite_ctx {
     size_t adj_n = 0;
     void vjp_kernels(int l);
     flite::SteadyAdjoint *sadj = nullptr;
+    // node numbering of the device (renumber.h): perm[l][new] = the caller's
+    // number, iperm[l] its inverse; d_perm/d_iperm on the device (shared with
+    // contexts that share this mesh); a scratch array for the permutations
+    bool renumbered = false;
+    std::vector<std::vector<int>> perm, iperm;
+    std::vector<int *> d_perm, d_iperm;
+    double *d_io = nullptr;
+    size_t io_n = 0;
+    double *io_buffer(size_t n) {
+        if (io_n < n) {
+            if (d_io) CK(cudaFree(d_io));
+            d_io = nullptr;
+            io_n = 0;
+            CK(cudaMalloc(&d_io, n * sizeof(double)));
+            io_n = n;
+        }
+        return d_io;
+    }
+    // host [ncomp][N] in the caller's numbering -> device array in the
+    // device's numbering (stream-ordered on s)
+    void put_nodes(int l, double *dst, const double *host, int ncomp) {
+        const size_t n = (size_t)lv[l].v.N * ncomp;
+        if (!renumbered) {
+            CK(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, s));
+            return;
+        }
+        double *t = io_buffer(n);
+        CK(cudaMemcpyAsync(t, host, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        k_permute_nodes<<<blocks(n), kBlock, 0, s>>>(dst, t, d_perm[l], lv[l].v.N, ncomp);
+        CK(cudaGetLastError());
+    }
+    // device array -> host [ncomp][N] in the caller's numbering (the copy is
+    // stream-ordered on s: the caller synchronises before reading host)
+    void get_nodes(int l, double *host, const double *src, int ncomp) {
+        const size_t n = (size_t)lv[l].v.N * ncomp;
+        if (!renumbered) {
+            CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            return;
+        }
+        double *t = io_buffer(n);
+        k_permute_nodes<<<blocks(n), kBlock, 0, s>>>(t, src, d_iperm[l], lv[l].v.N, ncomp);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(host, t, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
     int adj_method = 1, adj_restart = 50;  // flite_set_adjoint_method (GMRES(50))
     std::string err;
 
@@ -121,6 +165,7 @@ struct flite_ctx {
         if (graph) cudaGraphExecDestroy(graph);
         if (adj_rbar) { cudaFree(adj_rbar); cudaFree(adj_ubar); cudaFree(adj_b); }
         if (sadj) flite::destroy_steady_adjoint(sadj);
+        if (d_io) cudaFree(d_io);
         for (void *p : allocs) cudaFree(p);
         if (h_cycle) cudaFreeHost(h_cycle);
         if (s) cudaStreamDestroy(s);
@@ -299,9 +344,26 @@ struct flite_ctx {
             default: launch_node_update_u<1>(l, mode, stage, anchor);
         }
     }
+    // levels whose fused central gather stages node blocks in shared memory
+    // (flite_set_tiled_gather; on by default where the staging data exist)
+    // (flite_set_tiled_gather: 0 off, 1 with two blocks of 256 threads per
+    // SM, 2 with three; 0 in tiled_mode means the default, 1)
+    int tiled_mode[kMaxLevels] = {0};
+    int tiled(int l) const {
+        if (!(fused() && !mixed() && unroll == 1 && lv[l].v.tile.ntiles > 0)) return 0;
+        const int m = l < kMaxLevels ? tiled_mode[l] : 0;
+        return m == 0 ? 1 : (m < 0 ? 0 : m);
+    }
     template <int U>
     void launch_node_update_u(int l, int mode, int stage, bool anchor) {
         const unsigned g = gblk(l, U);
+        if (U == 1 && tiled(l)) {
+            const TileView &T = V(l).tile;
+            const size_t sm = (size_t)T.stage_max * sizeof(NodeRec);
+            if (tiled(l) == 2) k_node_update_tiled<3><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
+            else k_node_update_tiled<2><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
+            return;
+        }
         if (mixed()) {
             if (anchor) k_node_update<GATHER_ANCHOR, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
             else k_node_update<GATHER_DELTA, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);

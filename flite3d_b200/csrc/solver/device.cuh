@@ -67,6 +67,25 @@ struct __align__(16) GradRec {
 
 // A level's mesh and state on the device.  Node-indexed arrays are SoA
 // ([component][node]), like the reference's column-major u(N,nvar).
+// Shared-memory staging of node blocks for the gathers with a thread per
+// node: block t of kTile consecutive nodes and its halo (the other nodes its
+// edges reach).  The incidences of the block are stored row by row: row k
+// holds incidence k (in edge order) of each of the block's nodes, with the
+// edge coefficients and the other node's staged slot (or, beyond the stage's
+// capacity, its node number with kTileGlobal set); kTileSecond marks the
+// node as the edge's second node.
+constexpr int kTile = 256;
+constexpr int kTileStageMax = 1024;  // records staged per block: 48 KB
+constexpr unsigned kTileSecond = 0x80000000u, kTileGlobal = 0x40000000u, kTileIndexMask = 0x3fffffffu;
+struct TileView {
+    int ntiles;                   // 0: no staging data for this level
+    int stage_max;                // staged records of the largest block (<= kTileStageMax)
+    const int *halo_ptr, *halo;   // [ntiles+1], halo nodes of each block in increasing order
+    const int *row;               // [ntiles+1] first incidence row of each block
+    const unsigned *meta;         // [rows*kTile]
+    const double *wx, *wy, *wz;   // [rows*kTile]
+};
+
 struct LevelView {
     int N, E, B, Nb, grid;
     int nvar;                    // 5, or 6 with the Spalart-Allmaras nu~
@@ -128,6 +147,10 @@ struct LevelView {
     // (uold2 on level 1 only)
     double *uold, *uold2;                  // [nvar][N]
     int *cyc;                              // cycle number of this level
+    // the caller's number of each node (renumber.h); NULL when the device
+    // numbering is the caller's
+    const int *perm;                       // [N]
+    TileView tile;                         // staging of node blocks (fluxType 1)
 };
 
 __device__ __forceinline__ EdgeW load_edgew(const EdgeW *w, int e) {

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "context.h"
+#include "renumber.h"
 
 namespace {
 
@@ -45,6 +46,66 @@ int guarded(flite_ctx *ctx, F &&f) {
     } catch (const std::exception &e) {
         return fail(ctx, FLITE_EINVAL, e.what());
     }
+}
+
+// The staging data of the tiled gathers of one level (TileView).
+struct TileHost {
+    int ntiles = 0, stage_max = 0;
+    std::vector<int> halo_ptr, halo, row;
+    std::vector<unsigned> meta;
+    std::vector<double> wx, wy, wz;
+};
+
+void build_tiles(int N, const std::vector<int> &ip, const std::vector<int2> &inc, const std::vector<double> &wx,
+                 const std::vector<double> &wy, const std::vector<double> &wz, TileHost &T) {
+    if (N <= 0 || N >= (int)kTileIndexMask) return;
+    T.ntiles = (N + kTile - 1) / kTile;
+    T.halo_ptr.assign(T.ntiles + 1, 0);
+    T.row.assign(T.ntiles + 1, 0);
+    for (int t = 0; t < T.ntiles; ++t) {
+        const int n0 = t * kTile, n1 = std::min(N, n0 + kTile);
+        int kmax = 0;
+        for (int i = n0; i < n1; ++i) kmax = std::max(kmax, ip[i + 1] - ip[i]);
+        T.row[t + 1] = T.row[t] + kmax;
+    }
+    const size_t cells = (size_t)T.row[T.ntiles] * kTile;
+    T.meta.assign(std::max<size_t>(cells, 1), 0u);
+    T.wx.assign(std::max<size_t>(cells, 1), 0.0);
+    T.wy.assign(std::max<size_t>(cells, 1), 0.0);
+    T.wz.assign(std::max<size_t>(cells, 1), 0.0);
+    T.stage_max = kTile;
+    std::vector<int> h;
+    for (int t = 0; t < T.ntiles; ++t) {
+        const int n0 = t * kTile, n1 = std::min(N, n0 + kTile);
+        h.clear();
+        for (int i = n0; i < n1; ++i)
+            for (int k = ip[i]; k < ip[i + 1]; ++k) {
+                const int j = inc[k].y;
+                if (j < n0 || j >= n1) h.push_back(j);
+            }
+        std::sort(h.begin(), h.end());
+        h.erase(std::unique(h.begin(), h.end()), h.end());
+        T.halo_ptr[t + 1] = T.halo_ptr[t] + (int)h.size();
+        T.halo.insert(T.halo.end(), h.begin(), h.end());
+        const int staged = std::min((int)h.size(), kTileStageMax - kTile);
+        T.stage_max = std::max(T.stage_max, kTile + staged);
+        for (int i = n0; i < n1; ++i)
+            for (int k = ip[i]; k < ip[i + 1]; ++k) {
+                const int es = inc[k].x, j = inc[k].y, e = es >= 0 ? es : ~es;
+                unsigned m;
+                if (j >= n0 && j < n1) {
+                    m = (unsigned)(j - n0);
+                } else {
+                    const int pos = (int)(std::lower_bound(h.begin(), h.end(), j) - h.begin());
+                    m = pos < staged ? (unsigned)(kTile + pos) : (kTileGlobal | (unsigned)j);
+                }
+                if (es < 0) m |= kTileSecond;
+                const size_t x = ((size_t)T.row[t] + (k - ip[i])) * kTile + (i - n0);
+                T.meta[x] = m;
+                T.wx[x] = wx[e]; T.wy[x] = wy[e]; T.wz[x] = wz[e];
+            }
+    }
+    if (T.halo.empty()) T.halo.push_back(0);
 }
 
 const char *unsupported_reason(const flite_controls &c) {
@@ -144,6 +205,25 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
 
         int G = nlevels;
         if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);  // mg_par:1212-1214
+        // the device numbering of the nodes (renumber.h); a context sharing
+        // a donor's mesh shares its numbering
+        Renumbered R;
+        if (donor) {
+            X.renumbered = donor->renumbered;
+            X.perm = donor->perm; X.iperm = donor->iperm;
+            X.d_perm = donor->d_perm; X.d_iperm = donor->d_iperm;
+        } else {
+            renumber_levels(G, levels, default_node_order(), R);
+            levels = R.desc.data();
+            X.renumbered = !R.identity;
+            X.perm = std::move(R.perm);
+            X.iperm = std::move(R.iperm);
+            if (X.renumbered)
+                for (int l = 0; l < G; ++l) {
+                    X.d_perm.push_back(X.upload(X.perm[l]));
+                    X.d_iperm.push_back(X.upload(X.iperm[l]));
+                }
+        }
         CK(cudaStreamCreateWithFlags(&X.s, cudaStreamNonBlocking));
         CK(cudaMallocHost(&X.h_cycle, sizeof(int)));
         X.d_cycle = X.alloc<int>(1);
@@ -269,6 +349,21 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L.ew = X.upload(ew);
             }
             L.inc32 = nullptr;
+            L.tile = TileView{};
+            if (c->fluxType == 1) {
+                // staging of node blocks for the fused central gather
+                TileHost T;
+                build_tiles(N, ip, inc, wx, wy, wz, T);
+                if (T.ntiles > 0) {
+                    L.tile.ntiles = T.ntiles;
+                    L.tile.stage_max = T.stage_max;
+                    L.tile.halo_ptr = X.upload(T.halo_ptr);
+                    L.tile.halo = X.upload(T.halo);
+                    L.tile.row = X.upload(T.row);
+                    L.tile.meta = X.upload(T.meta);
+                    L.tile.wx = X.upload(T.wx); L.tile.wy = X.upload(T.wy); L.tile.wz = X.upload(T.wz);
+                }
+            }
             L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
             L.V = X.upload(std::vector<double>(d.volume, d.volume + N));
             L.wdist = d.wall_dist ? X.upload(std::vector<double>(d.wall_dist, d.wall_dist + N))
@@ -292,14 +387,19 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     if (par[f] >= 0) cp[par[f] + 1]++;
                 }
                 for (int i = 0; i < N; ++i) cp[i + 1] += cp[i];
+                // children in the order of the caller's fine numbering, the
+                // order of mapFineToCoarse's loop (def_par:12572-12679)
                 std::vector<int> ch(std::max(cp[N], 1));
                 std::vector<int> fill(cp.begin(), cp.end() - 1);
-                for (int f = 0; f < nf; ++f)
+                for (int fo = 0; fo < nf; ++fo) {
+                    const int f = X.iperm[l - 1][fo];
                     if (par[f] >= 0) ch[fill[par[f]]++] = f;
+                }
                 L.parent = X.upload(par); L.rweight = X.upload(rw);
                 L.child_ptr = X.upload(cp); L.child = X.upload(ch);
             }
             if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
+            L.perm = X.renumbered ? X.d_perm[l] : nullptr;
             }  // mesh upload
             // state
             const size_t nv = (size_t)X.nvar();
@@ -398,8 +498,7 @@ static bool bad_level(flite_ctx *ctx, int level) { return !ctx || level < 1 || l
 int flite_set_state(flite_ctx *ctx, int level, const double *u) {
     if (bad_level(ctx, level) || !u) return FLITE_EINVAL;
     return guarded(ctx, [&] {
-        LevelView &L = ctx->V(level - 1);
-        CK(cudaMemcpyAsync(L.u, u, ctx->nvar() * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, ctx->s));
+        ctx->put_nodes(level - 1, ctx->V(level - 1).u, u, ctx->nvar());
         CK(cudaStreamSynchronize(ctx->s));
         return FLITE_OK;
     });
@@ -408,8 +507,7 @@ int flite_set_state(flite_ctx *ctx, int level, const double *u) {
 int flite_get_state(flite_ctx *ctx, int level, double *u) {
     if (bad_level(ctx, level) || !u) return FLITE_EINVAL;
     return guarded(ctx, [&] {
-        LevelView &L = ctx->V(level - 1);
-        CK(cudaMemcpyAsync(u, L.u, ctx->nvar() * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        ctx->get_nodes(level - 1, u, ctx->V(level - 1).u, ctx->nvar());
         CK(cudaStreamSynchronize(ctx->s));
         return FLITE_OK;
     });
@@ -418,8 +516,7 @@ int flite_get_state(flite_ctx *ctx, int level, double *u) {
 int flite_get_pressure(flite_ctx *ctx, int level, double *p) {
     if (bad_level(ctx, level) || !p) return FLITE_EINVAL;
     return guarded(ctx, [&] {
-        LevelView &L = ctx->V(level - 1);
-        CK(cudaMemcpyAsync(p, L.p, (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+        ctx->get_nodes(level - 1, p, ctx->V(level - 1).p, 1);
         CK(cudaStreamSynchronize(ctx->s));
         return FLITE_OK;
     });
@@ -616,11 +713,11 @@ int flite_residual_fwd(flite_ctx *ctx, int level, const double *u, double *r) {
             X.rhs_terms(l, true);
             X.node_update(l, MODE_RESID, 0, true);
         }
-        CK(cudaMemcpyAsync(L.u, u, 5 * (size_t)L.N * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        X.put_nodes(l, L.u, u, 5);
         X.pressure(l);
         X.rhs_terms(l, false);
         X.node_update(l, MODE_RESID, 0, false);
-        CK(cudaMemcpyAsync(r, L.rhs, 5 * (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        X.get_nodes(l, r, L.rhs, 5);
         CK(cudaStreamSynchronize(X.s));
         return FLITE_OK;
     });
@@ -703,6 +800,13 @@ int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_bl
     ctx->eb = edge_block;
     ctx->nb = node_block;
     ctx->unroll = gather_unroll;
+    return FLITE_OK;
+}
+
+int flite_set_tiled_gather(flite_ctx *ctx, int32_t level, int32_t on) {
+    if (bad_level(ctx, level) || on < 0 || on > 2 || level > kMaxLevels) return FLITE_EINVAL;
+    ctx->tiled_mode[level - 1] = on == 0 ? -1 : on;
+    ctx->drop_graph();
     return FLITE_OK;
 }
 

@@ -1217,42 +1217,13 @@ __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const do
     L.a32[4 * N + i] = (float)(u[4] + p);
 }
 
-// ---- the node part of one RK stage (def_par:1069-1178), fused -------------
-// mode STAGE:   u <- update of stage `stage`
-// mode RCOARSE: restrictGrid coarse one-step (def_par:12244-12263): src
-// mode RFINE:   restrictGrid fine increment (def_par:12356-12383): rhs
-// mode RESID:   rhs <- makeRHS only
-// PREC: GATHER_BUFFER (FP64 edge buffer of the upwind fluxes),
-// GATHER_CENTRAL (central fluxes computed in the gather), GATHER_ANCHOR (the
-// same, stored as the new mixed-precision anchor), GATHER_DELTA (anchor +
-// FP32 increments)
-template <int PREC, int U>
-__global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3 : 1))
-    k_node_update(Params P, LevelView L, int mode, int stage) {
-    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
-    const int i_raw = U > 1 ? tid() / U : tid();
-    if (U == 1 && i_raw >= L.N) return;
-    const bool active = i_raw < L.N;
-    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
+// the node part of a stage after the residual r of node i is summed:
+// time differences, dissipation, solveSystem, the increment conditions, the
+// clipped update and the solution and outer conditions, or the restrictGrid
+// one-step forms (modes as in k_node_update)
+__device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, int i, double *r, int mode,
+                                          int stage) {
     const int N = L.N;
-    double r[5];
-    if constexpr (PREC == GATHER_DELTA) {
-        gather_interior_delta<U>(L, i, r, active, gl);
-    } else if constexpr (PREC == GATHER_BUFFER) {
-        gather_interior<U>(L, i, r, active, gl);
-    } else if constexpr (PREC == GATHER_CENTRAL2) {
-        gather_interior_central2(L, i, r);
-    } else {
-        gather_interior_central<U>(L, i, r, active, gl);
-    }
-    double rint[5];
-    if constexpr (PREC == GATHER_ANCHOR)
-        for (int c = 0; c < 5; ++c) rint[c] = r[c];
-    gather_boundary<U>(L, i, r, active, gl);
-    // with a group per node every lane holds the same sums; one lane goes on
-    if constexpr (U > 1)
-        if (!active || gl) return;
-    if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, rint);
     if (mode == MODE_RESID) {
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
@@ -1303,6 +1274,112 @@ __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = un[c] - up[c];
     }
 }
+
+// ---- the node part of one RK stage (def_par:1069-1178), fused -------------
+// mode STAGE:   u <- update of stage `stage`
+// mode RCOARSE: restrictGrid coarse one-step (def_par:12244-12263): src
+// mode RFINE:   restrictGrid fine increment (def_par:12356-12383): rhs
+// mode RESID:   rhs <- makeRHS only
+// PREC: GATHER_BUFFER (FP64 edge buffer of the upwind fluxes),
+// GATHER_CENTRAL (central fluxes computed in the gather), GATHER_ANCHOR (the
+// same, stored as the new mixed-precision anchor), GATHER_DELTA (anchor +
+// FP32 increments)
+template <int PREC, int U>
+__global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3 : 1))
+    k_node_update(Params P, LevelView L, int mode, int stage) {
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
+    double r[5];
+    if constexpr (PREC == GATHER_DELTA) {
+        gather_interior_delta<U>(L, i, r, active, gl);
+    } else if constexpr (PREC == GATHER_BUFFER) {
+        gather_interior<U>(L, i, r, active, gl);
+    } else if constexpr (PREC == GATHER_CENTRAL2) {
+        gather_interior_central2(L, i, r);
+    } else {
+        gather_interior_central<U>(L, i, r, active, gl);
+    }
+    double rint[5];
+    if constexpr (PREC == GATHER_ANCHOR)
+        for (int c = 0; c < 5; ++c) rint[c] = r[c];
+    gather_boundary<U>(L, i, r, active, gl);
+    // with a group per node every lane holds the same sums; one lane goes on
+    if constexpr (U > 1)
+        if (!active || gl) return;
+    if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, rint);
+    node_tail(P, L, i, r, mode, stage);
+}
+// ---- the same node update with the central fluxes gathered from a
+// shared-memory stage of the node block (GATHER_CENTRAL, a thread per node).
+// Block t handles the kTile nodes t*kTile.. of the level; it first copies
+// their 48-byte records and those of the block's halo (the other nodes its
+// edges reach, in increasing node order) into shared memory with coalesced
+// or independent loads, then every thread walks its node's incidences in
+// edge order through the block's incidence rows (row k holds incidence k of
+// every node of the block: the coefficients and the staged slot of the
+// other node, read with coalesced loads).  A neighbour beyond the stage's
+// capacity is read from the global records.  The flux of each incidence and
+// the order of the additions are those of k_node_update, so the results are
+// identical bit for bit.
+__device__ __forceinline__ NodeRec load_node_shared(const NodeRec *rec, int slot) {
+    const float4 *p = reinterpret_cast<const float4 *>(rec + slot);
+    NodeRec o;
+    float4 *d = reinterpret_cast<float4 *>(&o);
+    d[0] = p[0]; d[1] = p[1]; d[2] = p[2];
+    return o;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kTile, MINB) k_node_update_tiled(Params P, LevelView L, int mode, int stage) {
+    extern __shared__ float4 stage_mem[];
+    NodeRec *rec = reinterpret_cast<NodeRec *>(stage_mem);
+    const TileView &T = L.tile;
+    const int t = blockIdx.x, n0 = t * kTile;
+    const int cnt = min(kTile, L.N - n0);
+    const int h0 = T.halo_ptr[t];
+    const int nh = min(T.halo_ptr[t + 1] - h0, kTileStageMax - kTile);
+    {
+        const float4 *q = reinterpret_cast<const float4 *>(L.q);
+        // 16-byte pieces: 3 per record, own records then the halo's
+        for (int s = threadIdx.x; s < 3 * (cnt + nh); s += blockDim.x) {
+            const int r = s / 3, part = s - 3 * r;
+            const int j = r < cnt ? n0 + r : T.halo[h0 + (r - cnt)];
+            const int slot = r < cnt ? r : kTile + (r - cnt);
+            stage_mem[3 * slot + part] = __ldg(q + 3 * (size_t)j + part);
+        }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x >= cnt) return;
+    const int i = n0 + threadIdx.x;
+    const NodeRec si = load_node_shared(rec, threadIdx.x);
+    const int deg = L.inc_ptr[i + 1] - L.inc_ptr[i];
+    const size_t base = (size_t)T.row[t] * kTile + threadIdx.x;
+    double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < deg; ++k) {
+        const size_t x = base + (size_t)k * kTile;
+        const unsigned m = __ldg(T.meta + x);
+        const double wx = __ldg(T.wx + x), wy = __ldg(T.wy + x), wz = __ldg(T.wz + x);
+        const int v = (int)(m & kTileIndexMask);
+        const NodeRec n = (m & kTileGlobal) ? load_node(L.q, v) : load_node_shared(rec, v);
+        double f[5];
+        if (!(m & kTileSecond)) {
+            central_flux_rec(si, n, wx, wy, wz, f);
+            r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
+        } else {
+            central_flux_rec(n, si, wx, wy, wz, f);
+            r[0] = r[0] + (-f[0]); r[1] = r[1] + (-f[1]); r[2] = r[2] + (-f[2]); r[3] = r[3] + (-f[3]);
+            r[4] = r[4] + (-f[4]);
+        }
+    }
+    gather_boundary<1>(L, i, r);
+    node_tail(P, L, i, r, mode, stage);
+}
+
+template __global__ void k_node_update_tiled<2>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<3>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 1>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 4>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 8>(Params, LevelView, int, int);
@@ -1568,11 +1645,13 @@ __global__ void k_resid_partial(LevelView L, double *part, int nblk) {
     double s[6] = {0, 0, 0, 0, 0, 0}, m[6] = {0, 0, 0, 0, 0, 0};
     int mi[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        // the first node in the caller's numbering wins a tie (mg_par:1387-1396)
+        const int oi = L.perm ? L.perm[i] : i;
         for (int k = 0; k < nv; ++k) {
             double d = L.u[k * N + i] - L.uprev[k * N + i];
             s[k] = s[k] + d * d;
             double a = fabs(d);
-            if (a > m[k]) { m[k] = a; mi[k] = i; }
+            if (a > m[k] || (a == m[k] && a > 0.0 && oi < mi[k])) { m[k] = a; mi[k] = oi; }
         }
     }
     for (int k = 0; k < 6; ++k) { ss[k][threadIdx.x] = s[k]; sm[k][threadIdx.x] = m[k]; si[k][threadIdx.x] = mi[k]; }
@@ -1671,6 +1750,13 @@ __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, doub
     }
     if (threadIdx.x == 0)
         for (int k = 0; k < 6; ++k) part[6 * blockIdx.x + k] = red[k][0];
+}
+
+__global__ void k_permute_nodes(double *dst, const double *src, const int *map, int N, int ncomp) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)N * ncomp) return;
+    const int c = (int)(t / N), i = (int)(t - (size_t)c * N);
+    dst[t] = src[(size_t)c * N + map[i]];
 }
 
 // ---- forces of forceCalcType 3 (calculateLiftAndDrag3 def_par:15129-15313)

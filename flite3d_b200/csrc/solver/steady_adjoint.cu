@@ -1457,7 +1457,7 @@ static void download_geometry(flite_ctx &X, SteadyAdjoint &A, double *swb, doubl
     if (swb) CK(cudaMemcpyAsync(swb, A.swbar, 3 * (size_t)L.E * sizeof(double), cudaMemcpyDeviceToHost, X.s));
     if (bwb && L.B > 0)
         CK(cudaMemcpyAsync(bwb, A.bwbar, 3 * (size_t)L.B * sizeof(double), cudaMemcpyDeviceToHost, X.s));
-    if (vb) CK(cudaMemcpyAsync(vb, A.Vbar, (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+    if (vb) X.get_nodes(0, vb, A.Vbar, 1);
 }
 
 // lam <- P (G_u^T lam + Ju) from lam = P Ju, `check` iterations per launch of
@@ -1648,12 +1648,12 @@ extern "C" int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double
         if (visc) {
             copy(X, L.mu, A.mu_keep, N);
             copy(X, L.wstress, A.ws_keep, 3 * N);
-            CK(cudaMemcpyAsync(A.mu0, mu, N * sizeof(double), cudaMemcpyHostToDevice, X.s));
-            if (lam_mu) CK(cudaMemcpyAsync(A.lam + n5, lam_mu, N * sizeof(double), cudaMemcpyHostToDevice, X.s));
+            X.put_nodes(0, A.mu0, mu, 1);
+            if (lam_mu) X.put_nodes(0, A.lam + n5, lam_mu, 1);
             else zero(X, A.lam + n5, N);
         }
-        CK(cudaMemcpyAsync(A.u0, u, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
-        CK(cudaMemcpyAsync(A.lam, lam, n5 * sizeof(double), cudaMemcpyHostToDevice, X.s));
+        X.put_nodes(0, A.u0, u, 5);
+        X.put_nodes(0, A.lam, lam, 5);
         record(X, A);
         zero(X, A.Vbar, N);
         zero(X, A.nbar, 3 * N);
@@ -1661,8 +1661,8 @@ extern "C" int flite_iteration_vjp(flite_ctx *ctx, const double *u, const double
         const bool geom = side_w_bar || bnd_w_bar || volume_bar;
         if (geom) geometry_sweep(X, A, A.lam);
         else reverse(X, A, A.lam, false);
-        CK(cudaMemcpyAsync(ubar, A.ubar, n5 * sizeof(double), cudaMemcpyDeviceToHost, X.s));
-        if (visc && mu_bar) CK(cudaMemcpyAsync(mu_bar, A.ubar + n5, N * sizeof(double), cudaMemcpyDeviceToHost, X.s));
+        X.get_nodes(0, ubar, A.ubar, 5);
+        if (visc && mu_bar) X.get_nodes(0, mu_bar, A.ubar + n5, 1);
         if (geom) download_geometry(X, A, side_w_bar, bnd_w_bar, volume_bar);
         if (visc) {
             copy(X, A.mu_keep, L.mu, N);

@@ -295,6 +295,12 @@ class Solver:
     def set_kernel_options(self, edge_block=256, node_block=256, gather_unroll=1):
         self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll), "set_kernel_options")
 
+    def set_tiled_gather(self, level, mode=1):
+        """0: the fused central gather reads neighbours from global memory;
+        1 (default) or 2: it stages node blocks in shared memory (compiled
+        for two or three blocks per SM).  No effect on any result."""
+        self._ck(self.be.set_tiled_gather(self._h, level, mode), "set_tiled_gather")
+
     def set_gather_lanes(self, level, lanes):
         """Lanes per node of a level's gathers: 1, 4, 8, 16, 32 (0: default)."""
         self._ck(self.be.set_gather_lanes(self._h, level, lanes), "set_gather_lanes")
@@ -331,6 +337,13 @@ class Solver:
         self._ck(self.be.profile_level(self._h, level, reps, ctypes.byref(a), ctypes.byref(b)),
                  "profile_level")
         return a.value, b.value
+
+
+def set_node_order(order):
+    """Node numbering of the contexts created afterwards: 1 (default) the
+    device's locality order, 0 the caller's.  No effect on any result; node
+    arrays always cross the ABI in the caller's numbering."""
+    _abi.check(_abi.gpu_lib().flite_set_node_order(int(order)), "flite_set_node_order")
 
 
 def initial_state(controls, mesh, perturb_seed=None, amplitude=0.01):

@@ -215,3 +215,49 @@ def test_gather_lanes_match(name, lanes):
         g.cycle(cyc)
         o.cycle(cyc)
     assert_same_state(g, o, f"{name} lanes {lanes}")
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("name", ["central_jst", "laminar_adiabatic", "fv_boundary_term"])
+def test_tiled_gather_modes_match(name, mode):
+    # the fused central gather with node blocks staged in shared memory
+    # (compiled for two or three blocks per SM) or reading every neighbour
+    # from global memory, on every level with a thread per node
+    mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+    c, g, o = make_pair(mesh, **CASES[name])
+    for level in (1, 2, 3):
+        g.set_gather_lanes(level, 1)
+        g.set_tiled_gather(level, mode)
+    for cyc in range(1, 4):
+        g.cycle(cyc)
+        o.cycle(cyc)
+    assert_same_state(g, o, f"{name} tiled mode {mode}")
+    assert np.array_equal(g.residual_fwd(g.get_state(1)), o.residual_fwd(o.get_state(1)))
+
+
+def test_node_order_changes_no_result():
+    # the device's locality numbering against the caller's: the same states,
+    # pressures, residual maxima and their (caller-numbered) nodes
+    from flite3d_b200.solver import set_node_order
+    mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+    c = default_controls(**{**BASE, "ReynoldsNumber": 5000.0, "wallsAreIsentropic": 1, "fluxType": 1})
+    u0 = initial_state(c, mesh, perturb_seed=20261203, amplitude=0.01)
+    runs = []
+    try:
+        for order in (0, 1):
+            set_node_order(order)
+            s = Solver(c, mesh)
+            s.set_state(u0)
+            s.start()
+            for cyc in range(1, 4):
+                s.cycle(cyc)
+            runs.append((s.get_state(1), s.get_state(2), s.get_state(3), s.get_pressure(1), s.residuals(),
+                         s.forces(), s.residual_fwd(u0)))
+    finally:
+        set_node_order(1)
+    a, b = runs
+    for k in (0, 1, 2, 3, 6):
+        assert np.array_equal(a[k], b[k]), k
+    np.testing.assert_allclose(a[4][0], b[4][0], rtol=1e-12)
+    assert np.array_equal(a[4][1], b[4][1]) and np.array_equal(a[4][2], b[4][2])
+    np.testing.assert_allclose(a[5], b[5], rtol=1e-12, atol=1e-15)
