@@ -123,9 +123,10 @@ def node_kernel_name(lanes, tiled, unroll):
     """The instance of the level-1 node kernel the tuned launch options run."""
     what = ("(level 1: central fluxes of the incident edges computed in the node gather, fused with the RK "
             "stage update")
-    if lanes == 1 and tiled and unroll == 1:
-        return (f"k_node_update_tiled<{3 if tiled == 2 else 2}> {what}; node blocks and their halo staged in "
-                "shared memory)")
+    if lanes == 1 and tiled:
+        minb, stage = (2, True) if tiled == 1 else (3, True) if tiled == 2 else (2, False) if tiled == 3 else (3, False)
+        return (f"k_node_update_tiled<{minb}, {str(stage).lower()}> {what}; incidences read through the incidence "
+                "rows of 256-node blocks" + (", blocks and halo staged in shared memory)" if stage else ")"))
     if lanes == 1 and unroll == 2:
         return f"k_node_update<GATHER_CENTRAL2, 1> {what})"
     return f"k_node_update<GATHER_CENTRAL, {lanes}> {what})"
@@ -167,6 +168,7 @@ def run_ours(args):
                                 timeout=__import__("datetime").timedelta(seconds=600))
     from flite3d_b200 import replicas
     F, mesh, c, u0, t_mesh = build_case()
+    F.solver.set_node_order(args.node_order)
     solver = F.Solver(c, mesh)
     solver.set_state(u0)
     solver.start()
@@ -190,8 +192,8 @@ def run_ours(args):
     solver.set_kernel_options(256, best[0], best[1])
     # lanes per node of each level's gathers (and, with a thread per node,
     # whether the fused central gather stages node blocks in shared memory:
-    # mode 0 off, 1 or 2 on), by the device time of that level's kernels over
-    # one relaxation step
+    # through the incidence rows of node blocks: modes 1..4, 0 off), by the
+    # device time of that level's kernels over one relaxation step
     tuning_levels = {}
     if not args.kernel_options:
         lanes, tiled = {}, {}
@@ -199,7 +201,7 @@ def run_ours(args):
             t = {}
             for g in ((1, 4, 8) if lvl == 1 else (1, 4, 8, 16, 32)):
                 solver.set_gather_lanes(lvl, g)
-                for mode in ((0, 1, 2) if g == 1 else (0,)):
+                for mode in ((0, 1, 2, 3, 4) if g == 1 else (0,)):
                     solver.set_tiled_gather(lvl, mode)
                     t[(g, mode)] = sum(solver.profile_kernels(lvl, reps=5).values())
             lanes[lvl], tiled[lvl] = min(t, key=t.get)
@@ -327,6 +329,7 @@ def run_ours(args):
                      "traffic_source": "ncu capture of one launch on the 192x64x64 mesh, "
                                        "scaled by the units processed"},
         "clocks": clk.summary(),
+        "node_order": args.node_order,
         "residual_after_warmup": float(res[0]),
         "level1_kernel_ms": kernels_l1,
         "coarse_kernel_ms": kernels_coarse,
@@ -528,6 +531,7 @@ def run_rans(args):
     c = F.default_controls(ReynoldsNumber=6.0e6, MachNumber=0.8, alpha=1.25, CFLNumber=1.0, fluxType=4,
                            HLLCFluxOrder=2, Automaticlipping=1, GradientMethod=1, multigridScheme=3,
                            numberOfGridsToUse=5, turbulenceModel=1, wallsAreIsentropic=1)
+    F.solver.set_node_order(args.node_order)
     s = F.Solver(c, mesh)
     s.init_freestream()
     s.start()
@@ -547,6 +551,7 @@ def run_rans(args):
                    "mesh_nodes": d.n_nodes, "mesh_edges": d.n_sides, "levels": mesh.nlevels,
                    "mesh_build_s": round(t_mesh, 2)},
         "residuals_after": [float(x) for x in res], "gpu_launches": s.cycle_launches() * args.steps,
+        "node_order": args.node_order,
     }), flush=True)
 
 
@@ -797,6 +802,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the FLITE_MIXED cycle rate")
     ap.add_argument("--kernel-options", default=None,
                     help="NODE_BLOCK,UNROLL,LANES_L1,...: fixed launch options instead of tuning them")
+    ap.add_argument("--node-order", type=int, default=0,
+                    help="device node numbering: 0 the mesh's own, 1 the locality (Morton) order")
     ap.add_argument("--tiled-modes", default=None,
                     help="with --kernel-options: TILED_L1,TILED_L2,... (0 off, 1 or 2 on; default 1)")
     ap.add_argument("--no-converge", action="store_true",

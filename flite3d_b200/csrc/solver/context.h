@@ -198,7 +198,33 @@ struct flite_ctx {
     }
     void timesteps(int l) {
         counted();
+        if (const int m = tiled_other(l)) {
+            const int K = !P.viscous ? 0 : (P.sa ? 3 : 2);
+            const unsigned g = V(l).tile.ntiles;
+            const size_t sm = tile_smem(l, m, K);
+            if (m <= 2) {
+                if (K == 0) k_timestep_tiled<0, true><<<g, kTile, sm, s>>>(P, V(l));
+                else if (K == 2) k_timestep_tiled<2, true><<<g, kTile, sm, s>>>(P, V(l));
+                else k_timestep_tiled<3, true><<<g, kTile, sm, s>>>(P, V(l));
+            } else {
+                if (K == 0) k_timestep_tiled<0, false><<<g, kTile, 0, s>>>(P, V(l));
+                else if (K == 2) k_timestep_tiled<2, false><<<g, kTile, 0, s>>>(P, V(l));
+                else k_timestep_tiled<3, false><<<g, kTile, 0, s>>>(P, V(l));
+            }
+            return;
+        }
         FLITE_GATHER(k_timestep, l, P, V(l));
+    }
+    // the incidence-row form of a level's other gathers (the mode of
+    // flite_set_tiled_gather: 1, 2 staged, 3, 4 not), where a thread serves
+    // a node and the rows exist; 0 otherwise
+    int tiled_other(int l) const {
+        if (lv[l].v.tile.ntiles <= 0 || lanes_of(l) != 1) return 0;
+        const int m = l < kMaxLevels ? tiled_mode[l] : 0;
+        return m < 0 ? 0 : m;
+    }
+    size_t tile_smem(int l, int m, int K) const {
+        return m <= 2 ? (size_t)lv[l].v.tile.stage_max * K * sizeof(double) : 0;
     }
     void zero_diss(int l) {
         counted();
@@ -212,11 +238,23 @@ struct flite_ctx {
             zero_diss(l);
             return;
         }
+        const int m = tiled_other(l);
+        const unsigned g = L.tile.ntiles;
         counted();
-        FLITE_GATHER(k_jst_lap, l, P, L);
+        if (m && !P.useDissW) {
+            if (m <= 2) k_jst_lap_tiled<true><<<g, kTile, tile_smem(l, m, 6), s>>>(P, L);
+            else k_jst_lap_tiled<false><<<g, kTile, 0, s>>>(P, L);
+        } else {
+            FLITE_GATHER(k_jst_lap, l, P, L);
+        }
         counted();
         if (P.matrixDiss) k_jst_flux_matrix<<<nblk(L.N), nb, 0, s>>>(P, L);
-        else FLITE_GATHER(k_jst_flux, l, P, L);
+        else if (m) {
+            if (m <= 2) k_jst_flux_tiled<true><<<g, kTile, tile_smem(l, m, 13), s>>>(P, L);
+            else k_jst_flux_tiled<false><<<g, kTile, 0, s>>>(P, L);
+        } else {
+            FLITE_GATHER(k_jst_flux, l, P, L);
+        }
     }
     void first_order_diss(int l) {
         counted();
@@ -245,8 +283,20 @@ struct flite_ctx {
         counted();
         visc_flux(l);
     }
-    void visc_grad(int l) { FLITE_GATHER(k_visc_grad, l, P, V(l)); }
+    void visc_grad(int l) {
+        if (const int m = tiled_other(l)) {
+            if (m <= 2) k_visc_grad_tiled<true><<<V(l).tile.ntiles, kTile, tile_smem(l, m, 4), s>>>(P, V(l));
+            else k_visc_grad_tiled<false><<<V(l).tile.ntiles, kTile, 0, s>>>(P, V(l));
+            return;
+        }
+        FLITE_GATHER(k_visc_grad, l, P, V(l));
+    }
     void visc_flux(int l) {
+        if (const int m = tiled_other(l)) {
+            if (m <= 2) k_visc_flux_tiled<true><<<V(l).tile.ntiles, kTile, tile_smem(l, m, 12), s>>>(P, V(l));
+            else k_visc_flux_tiled<false><<<V(l).tile.ntiles, kTile, 0, s>>>(P, V(l));
+            return;
+        }
         FLITE_GATHER(k_visc_flux, l, P, V(l));
     }
     // ---- Spalart-Allmaras ----------------------------------------------
@@ -346,13 +396,14 @@ struct flite_ctx {
     }
     // levels whose fused central gather stages node blocks in shared memory
     // (flite_set_tiled_gather; on by default where the staging data exist)
-    // (flite_set_tiled_gather: 0 off, 1 with two blocks of 256 threads per
-    // SM, 2 with three; 0 in tiled_mode means the default, 1)
+    // (flite_set_tiled_gather: 0 off; 1, 2 staged with two or three blocks
+    // of 256 threads per SM; 3, 4 the same incidence rows without staging;
+    // tiled_mode holds -1 for 0 and 0 for the default, off)
     int tiled_mode[kMaxLevels] = {0};
     int tiled(int l) const {
-        if (!(fused() && !mixed() && unroll == 1 && lv[l].v.tile.ntiles > 0)) return 0;
+        if (!(fused() && !mixed() && lv[l].v.tile.ntiles > 0)) return 0;
         const int m = l < kMaxLevels ? tiled_mode[l] : 0;
-        return m == 0 ? 1 : (m < 0 ? 0 : m);
+        return m < 0 ? 0 : m;
     }
     template <int U>
     void launch_node_update_u(int l, int mode, int stage, bool anchor) {
@@ -360,8 +411,12 @@ struct flite_ctx {
         if (U == 1 && tiled(l)) {
             const TileView &T = V(l).tile;
             const size_t sm = (size_t)T.stage_max * sizeof(NodeRec);
-            if (tiled(l) == 2) k_node_update_tiled<3><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
-            else k_node_update_tiled<2><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
+            switch (tiled(l)) {
+                case 2: k_node_update_tiled<3, true><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage); break;
+                case 3: k_node_update_tiled<2, false><<<T.ntiles, kTile, 0, s>>>(P, V(l), mode, stage); break;
+                case 4: k_node_update_tiled<3, false><<<T.ntiles, kTile, 0, s>>>(P, V(l), mode, stage); break;
+                default: k_node_update_tiled<2, true><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
+            }
             return;
         }
         if (mixed()) {

@@ -83,6 +83,7 @@ struct TileView {
     const int *halo_ptr, *halo;   // [ntiles+1], halo nodes of each block in increasing order
     const int *row;               // [ntiles+1] first incidence row of each block
     const unsigned *meta;         // [rows*kTile]
+    const unsigned *nmeta;        // [rows*kTile] the same with every other node as a node number
     const double *wx, *wy, *wz;   // [rows*kTile]
 };
 

@@ -52,7 +52,7 @@ int guarded(flite_ctx *ctx, F &&f) {
 struct TileHost {
     int ntiles = 0, stage_max = 0;
     std::vector<int> halo_ptr, halo, row;
-    std::vector<unsigned> meta;
+    std::vector<unsigned> meta, nmeta;
     std::vector<double> wx, wy, wz;
 };
 
@@ -70,6 +70,7 @@ void build_tiles(int N, const std::vector<int> &ip, const std::vector<int2> &inc
     }
     const size_t cells = (size_t)T.row[T.ntiles] * kTile;
     T.meta.assign(std::max<size_t>(cells, 1), 0u);
+    T.nmeta.assign(std::max<size_t>(cells, 1), 0u);
     T.wx.assign(std::max<size_t>(cells, 1), 0.0);
     T.wy.assign(std::max<size_t>(cells, 1), 0.0);
     T.wz.assign(std::max<size_t>(cells, 1), 0.0);
@@ -99,9 +100,10 @@ void build_tiles(int N, const std::vector<int> &ip, const std::vector<int2> &inc
                     const int pos = (int)(std::lower_bound(h.begin(), h.end(), j) - h.begin());
                     m = pos < staged ? (unsigned)(kTile + pos) : (kTileGlobal | (unsigned)j);
                 }
-                if (es < 0) m |= kTileSecond;
+                const unsigned second = es < 0 ? kTileSecond : 0u;
                 const size_t x = ((size_t)T.row[t] + (k - ip[i])) * kTile + (i - n0);
-                T.meta[x] = m;
+                T.meta[x] = m | second;
+                T.nmeta[x] = kTileGlobal | (unsigned)j | second;
                 T.wx[x] = wx[e]; T.wy[x] = wy[e]; T.wz[x] = wz[e];
             }
     }
@@ -225,6 +227,14 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 }
         }
         CK(cudaStreamCreateWithFlags(&X.s, cudaStreamNonBlocking));
+        // shared memory of the staged incidence-row gathers (above the
+        // default 48 KB for the wider node fields)
+        CK(cudaFuncSetAttribute(k_jst_flux_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                13 * 8 * kTileStageMax));
+        CK(cudaFuncSetAttribute(k_visc_flux_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                12 * 8 * kTileStageMax));
+        CK(cudaFuncSetAttribute(k_jst_lap_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                6 * 8 * kTileStageMax));
         CK(cudaMallocHost(&X.h_cycle, sizeof(int)));
         X.d_cycle = X.alloc<int>(1);
         X.d_cyc = X.alloc<int>(G);
@@ -361,6 +371,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     L.tile.halo = X.upload(T.halo);
                     L.tile.row = X.upload(T.row);
                     L.tile.meta = X.upload(T.meta);
+                    L.tile.nmeta = X.upload(T.nmeta);
                     L.tile.wx = X.upload(T.wx); L.tile.wy = X.upload(T.wy); L.tile.wz = X.upload(T.wz);
                 }
             }
@@ -804,7 +815,7 @@ int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_bl
 }
 
 int flite_set_tiled_gather(flite_ctx *ctx, int32_t level, int32_t on) {
-    if (bad_level(ctx, level) || on < 0 || on > 2 || level > kMaxLevels) return FLITE_EINVAL;
+    if (bad_level(ctx, level) || on < 0 || on > 4 || level > kMaxLevels) return FLITE_EINVAL;
     ctx->tiled_mode[level - 1] = on == 0 ? -1 : on;
     ctx->drop_graph();
     return FLITE_OK;

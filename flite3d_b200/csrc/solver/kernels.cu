@@ -524,66 +524,29 @@ __global__ void k_visc_prim(Params P, LevelView L) {
     L.prim[3 * N + i] = gOg * L.p[i] / r;
 }
 
-template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, LevelView L) {
-    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
-    const int i_raw = U > 1 ? tid() / U : tid();
-    if (U == 1 && i_raw >= L.N) return;
-    const bool active = i_raw < L.N;
-    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
+// the boundary-face terms of node i's Galerkin gradients of (u, v, w, T)
+// (def_par:5322-5409), added to g in boundary-edge order
+__device__ __forceinline__ void visc_grad_bterms(const LevelView &L, int k, double *d) {
+    const int N = L.N;
+    int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+    int2 nd = L.bedge[b];
+    const double q1[4] = {L.prim[nd.x], L.prim[N + nd.x], L.prim[2 * N + nd.x], L.prim[3 * N + nd.x]};
+    const double q2[4] = {L.prim[nd.y], L.prim[N + nd.y], L.prim[2 * N + nd.y], L.prim[3 * N + nd.y]};
+    const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 4; ++c) {
+            double sm = q1[c] + q2[c];
+            double own = side == 0 ? q1[c] : q2[c];
+            d[a * 4 + c] = (2. * own + sm) * w[a];
+        }
+}
+
+// from node i's summed gradients g: Sutherland's viscosity, the SA eddy
+// viscosity, vorticity and divergence, the stress tensor and heat flux, the
+// adiabatic-wall projection and the wall stress (def_par:5460-5640)
+__device__ __forceinline__ void visc_grad_finish(const Params &P, const LevelView &L, int i, const double *g) {
     const int N = L.N;
     const double gOg = P.gamma / (P.gamma - 1.0);
-    double g[12];
-    for (int c = 0; c < 12; ++c) g[c] = 0.0;
-    auto prim = [&](int j, double *q) {
-        q[0] = L.prim[j]; q[1] = L.prim[N + j]; q[2] = L.prim[2 * N + j]; q[3] = L.prim[3 * N + j];
-    };
-    double qi[4];
-    prim(i, qi);
-    auto iterms = [&](int k, double *d) {
-        int2 t = L.inc[k];
-        int e = t.x >= 0 ? t.x : ~t.x;
-        double qj[4];
-        prim(t.y, qj);
-        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
-        for (int a = 0; a < 3; ++a)
-            for (int c = 0; c < 4; ++c) {
-                double x = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
-                d[a * 4 + c] = t.x >= 0 ? x : -x;  // g - x is g + (-x)
-            }
-    };
-    auto bterms = [&](int k, double *d) {
-        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
-        int2 nd = L.bedge[b];
-        double q1[4], q2[4];
-        prim(nd.x, q1); prim(nd.y, q2);
-        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
-        for (int a = 0; a < 3; ++a)
-            for (int c = 0; c < 4; ++c) {
-                double sm = q1[c] + q2[c];
-                double own = side == 0 ? q1[c] : q2[c];
-                d[a * 4 + c] = (2. * own + sm) * w[a];
-            }
-    };
-    auto add = [&](const double *d) {
-        for (int c = 0; c < 12; ++c) g[c] = g[c] + d[c];
-    };
-    if constexpr (U > 1) {
-        group_gather<U, 12, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, iterms, add);
-        group_gather<U, 12, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, add);
-        if (!active || gl) return;
-    } else {
-        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-            double v[12];
-            iterms(k, v);
-            add(v);
-        }
-        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-            double v[12];
-            bterms(k, v);
-            add(v);
-        }
-    }
     const double vt = 1. / L.V[i];
     double dudx = g[0] * vt, dvdx = g[1] * vt, dwdx = g[2] * vt, dTdx = g[3] * vt;
     double dudy = g[4] * vt, dvdy = g[5] * vt, dwdy = g[6] * vt, dTdy = g[7] * vt;
@@ -633,6 +596,117 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, Lev
     for (int c = 0; c < 9; ++c) L.tau[c * N + i] = tau[c];
 }
 
+template <int U>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, LevelView L) {
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
+    const int N = L.N;
+    double g[12];
+    for (int c = 0; c < 12; ++c) g[c] = 0.0;
+    auto prim = [&](int j, double *q) {
+        q[0] = L.prim[j]; q[1] = L.prim[N + j]; q[2] = L.prim[2 * N + j]; q[3] = L.prim[3 * N + j];
+    };
+    double qi[4];
+    prim(i, qi);
+    auto iterms = [&](int k, double *d) {
+        int2 t = L.inc[k];
+        int e = t.x >= 0 ? t.x : ~t.x;
+        double qj[4];
+        prim(t.y, qj);
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 4; ++c) {
+                double x = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
+                d[a * 4 + c] = t.x >= 0 ? x : -x;  // g - x is g + (-x)
+            }
+    };
+    auto bterms = [&](int k, double *d) { visc_grad_bterms(L, k, d); };
+    auto add = [&](const double *d) {
+        for (int c = 0; c < 12; ++c) g[c] = g[c] + d[c];
+    };
+    if constexpr (U > 1) {
+        group_gather<U, 12, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, iterms, add);
+        group_gather<U, 12, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, add);
+        if (!active || gl) return;
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[12];
+            iterms(k, v);
+            add(v);
+        }
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[12];
+            bterms(k, v);
+            add(v);
+        }
+    }
+    visc_grad_finish(P, L, i, g);
+}
+
+// the viscous flux of an edge from the stress/heat-flux and velocity of its
+// first (a, ua) and second (b, ub) node (def_par:5688-5720)
+__device__ __forceinline__ void visc_edge_flux(const double *a, const double *b, const double *ua, const double *ub,
+                                               double wx, double wy, double wz, double *f) {
+    double dt[9];
+    for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
+    double dut1 = ((((ua[0] * a[0] + ub[0] * b[0]) + ua[1] * a[1]) + ub[1] * b[1]) + ua[2] * a[2]) + ub[2] * b[2];
+    double dut2 = ((((ua[0] * a[1] + ub[0] * b[1]) + ua[1] * a[3]) + ub[1] * b[3]) + ua[2] * a[4]) + ub[2] * b[4];
+    double dut3 = ((((ua[0] * a[2] + ub[0] * b[2]) + ua[1] * a[4]) + ub[1] * b[4]) + ua[2] * a[5]) + ub[2] * b[5];
+    f[0] = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+    f[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+    f[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+    f[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+}
+
+// the two terms of each component of boundary edge binc[k] for its node
+// (def_par:5730-5800); g[8] = 0 for symmetry and inviscid-wall faces,
+// which contribute nothing
+__device__ __forceinline__ void visc_flux_bterms(const LevelView &L, int k, double *g) {
+    const int N = L.N;
+    int bb = L.binc[k] >> 1, side = L.binc[k] & 1;
+    int ind = L.bind[bb];
+    g[8] = (ind == 2 || ind == 9) ? 0.0 : 1.0;
+    if (g[8] == 0.0) return;
+    int2 nd = L.bedge[bb];
+    double a[9], b[9], ua[3], ub[3];
+    for (int c = 0; c < 9; ++c) { a[c] = L.tau[c * N + nd.x]; b[c] = L.tau[c * N + nd.y]; }
+    ua[0] = L.prim[nd.x]; ua[1] = L.prim[N + nd.x]; ua[2] = L.prim[2 * N + nd.x];
+    ub[0] = L.prim[nd.y]; ub[1] = L.prim[N + nd.y]; ub[2] = L.prim[2 * N + nd.y];
+    const double wx = L.bwx[bb], wy = L.bwy[bb], wz = L.bwz[bb];
+    double dt[9];
+    for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
+    double d11 = (ua[0] * a[0] + ua[1] * a[1]) + ua[2] * a[2];
+    double d12 = (ub[0] * b[0] + ub[1] * b[1]) + ub[2] * b[2];
+    double d21 = (ua[0] * a[1] + ua[1] * a[3]) + ua[2] * a[4];
+    double d22 = (ub[0] * b[1] + ub[1] * b[3]) + ub[2] * b[4];
+    double d31 = (ua[0] * a[2] + ua[1] * a[4]) + ua[2] * a[5];
+    double d32 = (ub[0] * b[2] + ub[1] * b[4]) + ub[2] * b[5];
+    double dut1 = d11 + d12, dut2 = d21 + d22, dut3 = d31 + d32;
+    g[0] = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
+    g[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
+    g[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
+    g[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+    const double *o = side == 0 ? a : b;
+    double do1 = side == 0 ? d11 : d12, do2 = side == 0 ? d21 : d22, do3 = side == 0 ? d31 : d32;
+    g[4] = 2.0 * ((wx * o[0] + wy * o[1]) + wz * o[2]);
+    g[5] = 2.0 * ((wx * o[1] + wy * o[3]) + wz * o[4]);
+    g[6] = 2.0 * ((wx * o[2] + wy * o[4]) + wz * o[5]);
+    g[7] = 2.0 * ((wx * (o[6] + do1) + wy * (o[7] + do2)) + wz * (o[8] + do3));
+}
+
+// node i's boundary-edge terms added to acc in boundary-edge order
+__device__ __forceinline__ void visc_flux_boundary(const LevelView &L, int i, double *acc) {
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        double v[9];
+        visc_flux_bterms(L, k, v);
+        if (v[8] == 0.0) continue;
+        for (int c = 0; c < 4; ++c) acc[c] = (acc[c] + v[c]) + v[4 + c];
+    }
+}
+
 // pass 2: viscous edge fluxes gathered per node and subtracted from the
 // dissipation vector (def_par:5662-5892)
 template <int U>
@@ -655,56 +729,16 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, Lev
         for (int c = 0; c < 9; ++c) tj[c] = L.tau[c * N + j];
         uj[0] = L.prim[j]; uj[1] = L.prim[N + j]; uj[2] = L.prim[2 * N + j];
         const bool first = t.x >= 0;
-        const double *a = first ? ti : tj, *b = first ? tj : ti;
-        const double *ua = first ? ui : uj, *ub = first ? uj : ui;
-        const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
-        double dt[9];
-        for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
-        double dut1 = ((((ua[0] * a[0] + ub[0] * b[0]) + ua[1] * a[1]) + ub[1] * b[1]) + ua[2] * a[2]) + ub[2] * b[2];
-        double dut2 = ((((ua[0] * a[1] + ub[0] * b[1]) + ua[1] * a[3]) + ub[1] * b[3]) + ua[2] * a[4]) + ub[2] * b[4];
-        double dut3 = ((((ua[0] * a[2] + ub[0] * b[2]) + ua[1] * a[4]) + ub[1] * b[4]) + ua[2] * a[5]) + ub[2] * b[5];
         double f[4];
-        f[0] = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
-        f[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
-        f[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
-        f[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
+        visc_edge_flux(first ? ti : tj, first ? tj : ti, first ? ui : uj, first ? uj : ui, L.wx[e], L.wy[e], L.wz[e],
+                       f);
         for (int c = 0; c < 4; ++c) g[c] = first ? f[c] : -f[c];
     };
     auto iadd = [&](const double *g) {
         for (int c = 0; c < 4; ++c) acc[c] = acc[c] + g[c];
     };
     // boundary edge: the two terms of each component, g[8] = 1 if it counts
-    auto bterms = [&](int k, double *g) {
-        int bb = L.binc[k] >> 1, side = L.binc[k] & 1;
-        int ind = L.bind[bb];
-        g[8] = (ind == 2 || ind == 9) ? 0.0 : 1.0;
-        if (g[8] == 0.0) return;
-        int2 nd = L.bedge[bb];
-        double a[9], b[9], ua[3], ub[3];
-        for (int c = 0; c < 9; ++c) { a[c] = L.tau[c * N + nd.x]; b[c] = L.tau[c * N + nd.y]; }
-        ua[0] = L.prim[nd.x]; ua[1] = L.prim[N + nd.x]; ua[2] = L.prim[2 * N + nd.x];
-        ub[0] = L.prim[nd.y]; ub[1] = L.prim[N + nd.y]; ub[2] = L.prim[2 * N + nd.y];
-        const double wx = L.bwx[bb], wy = L.bwy[bb], wz = L.bwz[bb];
-        double dt[9];
-        for (int c = 0; c < 9; ++c) dt[c] = a[c] + b[c];
-        double d11 = (ua[0] * a[0] + ua[1] * a[1]) + ua[2] * a[2];
-        double d12 = (ub[0] * b[0] + ub[1] * b[1]) + ub[2] * b[2];
-        double d21 = (ua[0] * a[1] + ua[1] * a[3]) + ua[2] * a[4];
-        double d22 = (ub[0] * b[1] + ub[1] * b[3]) + ub[2] * b[4];
-        double d31 = (ua[0] * a[2] + ua[1] * a[4]) + ua[2] * a[5];
-        double d32 = (ub[0] * b[2] + ub[1] * b[4]) + ub[2] * b[5];
-        double dut1 = d11 + d12, dut2 = d21 + d22, dut3 = d31 + d32;
-        g[0] = (wx * dt[0] + wy * dt[1]) + wz * dt[2];
-        g[1] = (wx * dt[1] + wy * dt[3]) + wz * dt[4];
-        g[2] = (wx * dt[2] + wy * dt[4]) + wz * dt[5];
-        g[3] = (wx * (dt[6] + dut1) + wy * (dt[7] + dut2)) + wz * (dt[8] + dut3);
-        const double *o = side == 0 ? a : b;
-        double do1 = side == 0 ? d11 : d12, do2 = side == 0 ? d21 : d22, do3 = side == 0 ? d31 : d32;
-        g[4] = 2.0 * ((wx * o[0] + wy * o[1]) + wz * o[2]);
-        g[5] = 2.0 * ((wx * o[1] + wy * o[3]) + wz * o[4]);
-        g[6] = 2.0 * ((wx * o[2] + wy * o[4]) + wz * o[5]);
-        g[7] = 2.0 * ((wx * (o[6] + do1) + wy * (o[7] + do2)) + wz * (o[8] + do3));
-    };
+    auto bterms = [&](int k, double *g) { visc_flux_bterms(L, k, g); };
     auto badd = [&](const double *g) {
         if (g[8] == 0.0) return;
         for (int c = 0; c < 4; ++c) acc[c] = (acc[c] + g[c]) + g[4 + c];
@@ -1332,16 +1366,16 @@ __device__ __forceinline__ NodeRec load_node_shared(const NodeRec *rec, int slot
     return o;
 }
 
-template <int MINB>
+template <int MINB, bool STAGE>
 __global__ void __launch_bounds__(kTile, MINB) k_node_update_tiled(Params P, LevelView L, int mode, int stage) {
     extern __shared__ float4 stage_mem[];
     NodeRec *rec = reinterpret_cast<NodeRec *>(stage_mem);
     const TileView &T = L.tile;
     const int t = blockIdx.x, n0 = t * kTile;
     const int cnt = min(kTile, L.N - n0);
-    const int h0 = T.halo_ptr[t];
-    const int nh = min(T.halo_ptr[t + 1] - h0, kTileStageMax - kTile);
-    {
+    if (STAGE) {
+        const int h0 = T.halo_ptr[t];
+        const int nh = min(T.halo_ptr[t + 1] - h0, kTileStageMax - kTile);
         const float4 *q = reinterpret_cast<const float4 *>(L.q);
         // 16-byte pieces: 3 per record, own records then the halo's
         for (int s = threadIdx.x; s < 3 * (cnt + nh); s += blockDim.x) {
@@ -1350,36 +1384,333 @@ __global__ void __launch_bounds__(kTile, MINB) k_node_update_tiled(Params P, Lev
             const int slot = r < cnt ? r : kTile + (r - cnt);
             stage_mem[3 * slot + part] = __ldg(q + 3 * (size_t)j + part);
         }
+        __syncthreads();
     }
-    __syncthreads();
     if ((int)threadIdx.x >= cnt) return;
     const int i = n0 + threadIdx.x;
-    const NodeRec si = load_node_shared(rec, threadIdx.x);
+    const NodeRec si = STAGE ? load_node_shared(rec, threadIdx.x) : load_node(L.q, i);
     const int deg = L.inc_ptr[i + 1] - L.inc_ptr[i];
     const size_t base = (size_t)T.row[t] * kTile + threadIdx.x;
-    double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int k = 0; k < deg; ++k) {
-        const size_t x = base + (size_t)k * kTile;
-        const unsigned m = __ldg(T.meta + x);
-        const double wx = __ldg(T.wx + x), wy = __ldg(T.wy + x), wz = __ldg(T.wz + x);
+    const unsigned *meta = STAGE ? T.meta : T.nmeta;
+    auto fetch = [&](unsigned m) -> NodeRec {
         const int v = (int)(m & kTileIndexMask);
-        const NodeRec n = (m & kTileGlobal) ? load_node(L.q, v) : load_node_shared(rec, v);
+        if (!STAGE || (m & kTileGlobal)) return load_node(L.q, v);
+        return load_node_shared(rec, v);
+    };
+    double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // the loads of incidence k+1 are issued before incidence k is evaluated
+    unsigned m0 = 0;
+    double wx0 = 0, wy0 = 0, wz0 = 0;
+    NodeRec n0r{};
+    if (deg > 0) {
+        m0 = __ldg(meta + base);
+        wx0 = __ldg(T.wx + base); wy0 = __ldg(T.wy + base); wz0 = __ldg(T.wz + base);
+        n0r = fetch(m0);
+    }
+    for (int k = 0; k < deg; ++k) {
+        unsigned m1 = 0;
+        double wx1 = 0, wy1 = 0, wz1 = 0;
+        NodeRec n1r{};
+        if (k + 1 < deg) {
+            const size_t x = base + (size_t)(k + 1) * kTile;
+            m1 = __ldg(meta + x);
+            wx1 = __ldg(T.wx + x); wy1 = __ldg(T.wy + x); wz1 = __ldg(T.wz + x);
+            n1r = fetch(m1);
+        }
         double f[5];
-        if (!(m & kTileSecond)) {
-            central_flux_rec(si, n, wx, wy, wz, f);
+        if (!(m0 & kTileSecond)) {
+            central_flux_rec(si, n0r, wx0, wy0, wz0, f);
             r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
         } else {
-            central_flux_rec(n, si, wx, wy, wz, f);
+            central_flux_rec(n0r, si, wx0, wy0, wz0, f);
             r[0] = r[0] + (-f[0]); r[1] = r[1] + (-f[1]); r[2] = r[2] + (-f[2]); r[3] = r[3] + (-f[3]);
             r[4] = r[4] + (-f[4]);
         }
+        m0 = m1; wx0 = wx1; wy0 = wy1; wz0 = wz1; n0r = n1r;
     }
     gather_boundary<1>(L, i, r);
     node_tail(P, L, i, r, mode, stage);
 }
 
-template __global__ void k_node_update_tiled<2>(Params, LevelView, int, int);
-template __global__ void k_node_update_tiled<3>(Params, LevelView, int, int);
+// ---- the other gathers of a level through the incidence rows of node blocks
+// Each kernel walks its node's incidences in edge order through the block's
+// incidence rows (row k holds incidence k of each node of the block), with
+// the loads of incidence k+1 issued before incidence k is evaluated.  With
+// STAGE the K node fields (SoA arrays) it reads at the other node are first
+// copied for the block and its halo into shared memory as sm[slot*K + c];
+// without, they are read from the global arrays.  The per-incidence
+// arithmetic and the order of the additions are those of the kernels'
+// thread-per-node forms above, so the results are identical bit for bit.
+template <int K>
+__device__ __forceinline__ void stage_fields(double *sm, const TileView &T, const double *const *f, int n0, int cnt,
+                                             int h0, int nh) {
+#pragma unroll 1
+    for (int c = 0; c < K; ++c)
+        for (int s = threadIdx.x; s < cnt + nh; s += blockDim.x) {
+            const int j = s < cnt ? n0 + s : T.halo[h0 + (s - cnt)];
+            const int slot = s < cnt ? s : kTile + (s - cnt);
+            sm[slot * K + c] = __ldg(f[c] + j);
+        }
+}
+
+// the block of the calling thread and its halo (staged part), with the
+// fields staged when STAGE; returns the node, or -1 for the block's idle
+// threads
+template <int K, bool STAGE>
+__device__ __forceinline__ int tile_begin(double *sm, const LevelView &L, const double *const *f) {
+    const int n0 = blockIdx.x * kTile;
+    const int cnt = min(kTile, L.N - n0);
+    if (STAGE && K > 0) {
+        const int h0 = L.tile.halo_ptr[blockIdx.x];
+        const int nh = min(L.tile.halo_ptr[blockIdx.x + 1] - h0, kTileStageMax - kTile);
+        stage_fields<K>(sm, L.tile, f, n0, cnt, h0, nh);
+        __syncthreads();
+    }
+    return (int)threadIdx.x < cnt ? n0 + (int)threadIdx.x : -1;
+}
+
+// one incidence of the row walk: the other node's K fields, the flags and
+// (when W) the edge coefficients
+template <int K, bool STAGE, bool W>
+struct Inc {
+    unsigned m;
+    double w[3];
+    double v[K > 0 ? K : 1];
+    __device__ __forceinline__ void load(const LevelView &L, const double *sm, const double *const *f, size_t x) {
+        m = __ldg((STAGE ? L.tile.meta : L.tile.nmeta) + x);
+        if (W) { w[0] = __ldg(L.tile.wx + x); w[1] = __ldg(L.tile.wy + x); w[2] = __ldg(L.tile.wz + x); }
+        const int idx = (int)(m & kTileIndexMask);
+        if (!STAGE || (m & kTileGlobal)) {
+#pragma unroll
+            for (int c = 0; c < K; ++c) v[c] = __ldg(f[c] + idx);
+        } else {
+#pragma unroll
+            for (int c = 0; c < K; ++c) v[c] = sm[idx * K + c];
+        }
+    }
+    __device__ __forceinline__ bool first() const { return !(m & kTileSecond); }
+};
+
+// walk node i's incidence rows calling fn(inc) in edge order, one ahead
+template <int K, bool STAGE, bool W, class Fn>
+__device__ __forceinline__ void row_walk(const LevelView &L, const double *sm, const double *const *f, int i,
+                                         Fn &&fn) {
+    const int deg = L.inc_ptr[i + 1] - L.inc_ptr[i];
+    const size_t base = (size_t)L.tile.row[blockIdx.x] * kTile + threadIdx.x;
+    if (deg <= 0) return;
+    Inc<K, STAGE, W> a, b;
+    a.load(L, sm, f, base);
+    for (int k = 0; k < deg; ++k) {
+        if (k + 1 < deg) b.load(L, sm, f, base + (size_t)(k + 1) * kTile);
+        fn(a);
+        a = b;
+    }
+}
+
+// makeTimeSteps: K = 0 (inviscid: the other node is not read), 2 (mu, rho),
+// 3 (with the SA nu~)
+template <int K, bool STAGE>
+__global__ void __launch_bounds__(kTile, 3) k_timestep_tiled(Params P, LevelView L) {
+    extern __shared__ double sm[];
+    const int N = L.N;
+    const double *f[3] = {L.mu, L.u, L.u + 5 * (size_t)N};
+    const int i = tile_begin<K, STAGE>(sm, L, f);
+    if (i < 0) return;
+    const double c1 = P.gamma;
+    const double ri = L.u[i], ro = 1. / ri;
+    const double m1 = L.u[N + i], m2 = L.u[2 * N + i], m3 = L.u[3 * N + i];
+    const double cc = dmax(c1 * L.p[i] * ro, 0.001);
+    double acc = 0.0, h = 0.0;
+    row_walk<K, STAGE, true>(L, sm, f, i, [&](const Inc<K, STAGE, true> &t) {
+        const double wx = t.w[0], wy = t.w[1], wz = t.w[2];
+        double al = (wx * wx + wy * wy) + wz * wz;
+        double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
+        acc = (acc + fabs(vn)) + sqrt(cc * al);
+        if (K > 0) {
+            double vis = dmax(P.am, K == 3 ? t.v[0] + t.v[K == 3 ? 2 : 0] / P.Re : t.v[0]);
+            double dv = 2.0 * vis * al / t.v[K > 1 ? 1 : 0];
+            h = h + dv;
+        }
+    });
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        int2 nd = L.bedge[b];
+        double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
+        double al = (wx * wx + wy * wy) + wz * wz;
+        int j1 = nd.x, j2 = nd.y;
+        double ro1 = 1. / L.u[j1], ro2 = 1. / L.u[j2];
+        double cc1 = dmax(c1 * L.p[j1] * ro1, 0.001);
+        double cc2 = dmax(c1 * L.p[j2] * ro2, 0.001);
+        double vn1 = ((wx * L.u[N + j1] + wy * L.u[2 * N + j1]) + wz * L.u[3 * N + j1]) * ro1;
+        double vn2 = ((wx * L.u[N + j2] + wy * L.u[2 * N + j2]) + wz * L.u[3 * N + j2]) * ro2;
+        vn1 = fabs(vn1); vn2 = fabs(vn2);
+        cc1 = sqrt(cc1 * al); cc2 = sqrt(cc2 * al);
+        acc = (((acc + (side == 0 ? vn1 : vn2)) + (vn1 + vn2)) + (side == 0 ? cc1 : cc2)) + (cc1 + cc2);
+        if (P.viscous) {
+            double vis1 = dmax(P.am, P.sa ? L.mu[j1] + L.u[5 * N + j1] / P.Re : L.mu[j1]);
+            double vis2 = dmax(P.am, P.sa ? L.mu[j2] + L.u[5 * N + j2] / P.Re : L.mu[j2]);
+            double dv1 = 2.0 * vis1 * al / L.u[j1];
+            double dv2 = 2.0 * vis2 * al / L.u[j2];
+            h = (h + (side == 0 ? dv1 : dv2)) + (dv1 + dv2);
+        }
+    }
+    const double V = L.V[i];
+    const double dt = 0.5 / (acc / V + h / (V * V));
+    L.dt[i] = dt;
+    L.vdt[i] = V / dt;
+}
+
+// makeArtificialDissipation2 passes 1-2 (no dissipation weighting): the
+// other node's u and p
+template <bool STAGE>
+__global__ void __launch_bounds__(kTile, 3) k_jst_lap_tiled(Params P, LevelView L) {
+    extern __shared__ double sm[];
+    const int N = L.N;
+    const double *f[6] = {L.u, L.u + N, L.u + 2 * (size_t)N, L.u + 3 * (size_t)N, L.u + 4 * (size_t)N, L.p};
+    const int i = tile_begin<6, STAGE>(sm, L, f);
+    if (i < 0) return;
+    double l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, s7 = 0, s8 = 0;
+    const double ui0 = L.u[i], ui1 = L.u[N + i], ui2 = L.u[2 * N + i], ui3 = L.u[3 * N + i], ui4 = L.u[4 * N + i];
+    const double pi = L.p[i];
+    const double df = 1.0;
+    row_walk<6, STAGE, false>(L, sm, f, i, [&](const Inc<6, STAGE, false> &t) {
+        const double uj0 = t.v[0], uj1 = t.v[1], uj2 = t.v[2], uj3 = t.v[3], uj4 = t.v[4], pj = t.v[5];
+        if (t.first()) {
+            double d0 = ui0 - uj0, d1 = ui1 - uj1, d2 = ui2 - uj2, d3 = ui3 - uj3;
+            double d4 = ((ui4 - uj4) + pi) - pj;
+            l0 = l0 - d0 * df; l1 = l1 - d1 * df; l2 = l2 - d2 * df; l3 = l3 - d3 * df; l4 = l4 - d4 * df;
+            double dp = pi - pj, sp = pi + pj;
+            s7 = s7 - dp; s8 = s8 + sp;
+        } else {
+            double d0 = uj0 - ui0, d1 = uj1 - ui1, d2 = uj2 - ui2, d3 = uj3 - ui3;
+            double d4 = ((uj4 - ui4) + pj) - pi;
+            l0 = l0 + d0 * df; l1 = l1 + d1 * df; l2 = l2 + d2 * df; l3 = l3 + d3 * df; l4 = l4 + d4 * df;
+            double dp = pj - pi, sp = pj + pi;
+            s7 = s7 + dp; s8 = s8 + sp;
+        }
+    });
+    double fact = 1. / L.conn[i];
+    L.sens[i] = 12. * fabs(s7 / s8);
+    L.lap[i] = fact * l0;
+    L.lap[N + i] = fact * l1;
+    L.lap[2 * N + i] = fact * l2;
+    L.lap[3 * N + i] = fact * l3;
+    L.lap[4 * N + i] = fact * l4;
+}
+
+// makeArtificialDissipation2 pass 3, scalar: the other node's V/dt,
+// connectivity, sensor, Laplacian and u
+template <bool STAGE>
+__global__ void __launch_bounds__(kTile, 2) k_jst_flux_tiled(Params P, LevelView L) {
+    extern __shared__ double sm[];
+    const int N = L.N;
+    const double *f[13] = {L.vdt, L.conn, L.sens,
+                           L.lap, L.lap + N, L.lap + 2 * (size_t)N, L.lap + 3 * (size_t)N, L.lap + 4 * (size_t)N,
+                           L.u, L.u + N, L.u + 2 * (size_t)N, L.u + 3 * (size_t)N, L.u + 4 * (size_t)N};
+    const int i = tile_begin<13, STAGE>(sm, L, f);
+    if (i < 0) return;
+    const double k4 = L.grid == 1 ? P.k4 : P.cgdf;
+    double acc[5] = {0, 0, 0, 0, 0};
+    double Li[5], Ui[5];
+    for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
+    const double vdi = L.vdt[i], coni = L.conn[i], si = L.sens[i];
+    row_walk<13, STAGE, false>(L, sm, f, i, [&](const Inc<13, STAGE, false> &t) {
+        const bool first = t.first();
+        const double vdj = t.v[0], conj = t.v[1];
+        double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
+        d0 = d0 / (first ? (coni + conj) : (conj + coni));
+        const double sj = t.v[2];
+        double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
+        double d4 = d0 * k4;
+        d4 = d4 > d2 ? d4 - d2 : 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const double Lj = t.v[3 + c], Uj = t.v[8 + c];
+            if (first) {
+                double d4v = Li[c] - Lj, d2v = Ui[c] - Uj;
+                acc[c] = (acc[c] - d4v * d4) + d2v * d2;
+            } else {
+                double d4v = Lj - Li[c], d2v = Uj - Ui[c];
+                acc[c] = (acc[c] + d4v * d4) - d2v * d2;
+            }
+        }
+    });
+    for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
+}
+
+// makeViscosityTerm pass 1 (gradients, then the node's stress and heat
+// flux as in k_visc_grad): the other node's (u, v, w, T)
+template <bool STAGE>
+__global__ void __launch_bounds__(kTile, 3) k_visc_grad_tiled(Params P, LevelView L) {
+    extern __shared__ double sm[];
+    const int N = L.N;
+    const double *f[4] = {L.prim, L.prim + N, L.prim + 2 * (size_t)N, L.prim + 3 * (size_t)N};
+    const int i = tile_begin<4, STAGE>(sm, L, f);
+    if (i < 0) return;
+    double g[12];
+    for (int c = 0; c < 12; ++c) g[c] = 0.0;
+    const double qi[4] = {L.prim[i], L.prim[N + i], L.prim[2 * N + i], L.prim[3 * N + i]};
+    row_walk<4, STAGE, true>(L, sm, f, i, [&](const Inc<4, STAGE, true> &t) {
+        const bool first = t.first();
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                double v = (first ? qi[c] + t.v[c] : t.v[c] + qi[c]) * t.w[a];
+                g[a * 4 + c] = g[a * 4 + c] + (first ? v : -v);
+            }
+    });
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        double v[12];
+        visc_grad_bterms(L, k, v);
+        for (int c = 0; c < 12; ++c) g[c] = g[c] + v[c];
+    }
+    visc_grad_finish(P, L, i, g);
+}
+
+// makeViscosityTerm pass 2 (as k_visc_flux): the other node's stress, heat
+// flux and velocity
+template <bool STAGE>
+__global__ void __launch_bounds__(kTile, 2) k_visc_flux_tiled(Params P, LevelView L) {
+    extern __shared__ double sm[];
+    const int N = L.N;
+    const double *f[12] = {L.tau, L.tau + N, L.tau + 2 * (size_t)N, L.tau + 3 * (size_t)N, L.tau + 4 * (size_t)N,
+                           L.tau + 5 * (size_t)N, L.tau + 6 * (size_t)N, L.tau + 7 * (size_t)N,
+                           L.tau + 8 * (size_t)N, L.prim, L.prim + N, L.prim + 2 * (size_t)N};
+    const int i = tile_begin<12, STAGE>(sm, L, f);
+    if (i < 0) return;
+    double ti[9], ui[3];
+    for (int c = 0; c < 9; ++c) ti[c] = L.tau[c * N + i];
+    ui[0] = L.prim[i]; ui[1] = L.prim[N + i]; ui[2] = L.prim[2 * N + i];
+    double acc[4] = {0, 0, 0, 0};
+    row_walk<12, STAGE, true>(L, sm, f, i, [&](const Inc<12, STAGE, true> &t) {
+        const bool first = t.first();
+        const double *tj = t.v, *uj = t.v + 9;
+        double fl[4];
+        visc_edge_flux(first ? ti : tj, first ? tj : ti, first ? ui : uj, first ? uj : ui, t.w[0], t.w[1], t.w[2],
+                       fl);
+        for (int c = 0; c < 4; ++c) acc[c] = acc[c] + (first ? fl[c] : -fl[c]);
+    });
+    visc_flux_boundary(L, i, acc);
+    for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
+}
+
+#define FLITE_TILED_INST(STAGE)                                                     \
+    template __global__ void k_timestep_tiled<0, STAGE>(Params, LevelView);         \
+    template __global__ void k_timestep_tiled<2, STAGE>(Params, LevelView);         \
+    template __global__ void k_timestep_tiled<3, STAGE>(Params, LevelView);         \
+    template __global__ void k_jst_lap_tiled<STAGE>(Params, LevelView);            \
+    template __global__ void k_jst_flux_tiled<STAGE>(Params, LevelView);           \
+    template __global__ void k_visc_grad_tiled<STAGE>(Params, LevelView);          \
+    template __global__ void k_visc_flux_tiled<STAGE>(Params, LevelView);
+FLITE_TILED_INST(true)
+FLITE_TILED_INST(false)
+#undef FLITE_TILED_INST
+
+template __global__ void k_node_update_tiled<2, true>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<3, true>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<2, false>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<3, false>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 1>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 4>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 8>(Params, LevelView, int, int);

@@ -10,7 +10,7 @@
 namespace flite {
 namespace {
 
-std::atomic<int> g_default_order{1};
+std::atomic<int> g_default_order{0};
 
 // 21 bits of each coordinate interleaved into a 63-bit Morton key
 uint64_t spread3(uint64_t v) {

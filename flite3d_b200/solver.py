@@ -296,9 +296,10 @@ class Solver:
         self._ck(self.be.set_kernel_options(self._h, edge_block, node_block, gather_unroll), "set_kernel_options")
 
     def set_tiled_gather(self, level, mode=1):
-        """0: the fused central gather reads neighbours from global memory;
-        1 (default) or 2: it stages node blocks in shared memory (compiled
-        for two or three blocks per SM).  No effect on any result."""
+        """How the fused central gather of a level reads its incidences: 0
+        through the node's incidence list; 1..4 through the incidence rows of
+        256-node blocks, with the block and its halo staged in shared memory
+        (1, 2) or not (3, 4).  No effect on any result."""
         self._ck(self.be.set_tiled_gather(self._h, level, mode), "set_tiled_gather")
 
     def set_gather_lanes(self, level, lanes):
@@ -340,8 +341,8 @@ class Solver:
 
 
 def set_node_order(order):
-    """Node numbering of the contexts created afterwards: 1 (default) the
-    device's locality order, 0 the caller's.  No effect on any result; node
+    """Node numbering of the contexts created afterwards: 0 (default) the
+    caller's, 1 the device's locality order.  No effect on any result; node
     arrays always cross the ABI in the caller's numbering."""
     _abi.check(_abi.gpu_lib().flite_set_node_order(int(order)), "flite_set_node_order")
 

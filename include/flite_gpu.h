@@ -343,22 +343,25 @@ int flite_profile_level(flite_ctx *ctx, int level, int reps, double *edge_ms,
  * 2).  Drops the captured cycle graph.                                     */
 int flite_set_kernel_options(flite_ctx *ctx, int32_t edge_block, int32_t node_block, int32_t gather_unroll);
 /* Node numbering of the contexts created after this call (no effect on any
- * result; no reference counterpart): 1 (the default) renumbers the nodes of
- * every level for locality -- boundary nodes stay first, level 1 in Morton
- * order of the coordinates, coarse levels by their children -- and 0 keeps
- * the caller's numbering.  Node arrays always cross this ABI in the caller's
+ * result; no reference counterpart): 1 renumbers the nodes of every level
+ * for locality -- boundary nodes stay first, level 1 in Morton order of the
+ * coordinates, coarse levels by their children -- and 0 (the default) keeps
+ * the caller's numbering, which a structured mesh generated line by line
+ * already orders well.  Node arrays always cross this ABI in the caller's
  * numbering; edges keep their numbers.                                      */
 int flite_set_node_order(int32_t order);
 /* Lanes per node of the node gathers of a level (no effect on any result):
  * 1 (a thread per node), 4, 8, 16 or 32, or 0 for the default (32 below 8192
  * nodes, else 1).  Drops the captured cycle graph.                         */
 int flite_set_gather_lanes(flite_ctx *ctx, int32_t level, int32_t lanes);
-/* Whether a level's fused central gather with a thread per node (fluxType
- * 1, FP64) stages each block of 256 nodes and the other nodes its edges
- * reach in shared memory (1, the default: compiled for two blocks per SM;
- * 2: for three blocks per SM, fewer registers) or reads every neighbour
- * from global memory (0).  No effect on any result.  Drops the captured
- * cycle graph.                                                              */
+/* How a level's fused central gather with a thread per node (fluxType 1,
+ * FP64) reads its incidences: 0 (the default) through the node's incidence
+ * list; 1..4 through incidence rows of blocks of 256 nodes (row k holds
+ * incidence k of every node of the block with its edge coefficients, read
+ * with coalesced loads a step ahead), with the block's nodes and the other
+ * nodes its edges reach staged in shared memory (1: compiled for two blocks
+ * per SM, 2: three) or read from global memory (3: two, 4: three).  No
+ * effect on any result.  Drops the captured cycle graph.                   */
 int flite_set_tiled_gather(flite_ctx *ctx, int32_t level, int32_t on);
 /* Average device ms of the kernel groups of one relaxation step of a level,
  * in order: pressure, time steps, dissipation, viscous primitives, viscous

@@ -217,21 +217,29 @@ def test_gather_lanes_match(name, lanes):
     assert_same_state(g, o, f"{name} lanes {lanes}")
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
-@pytest.mark.parametrize("name", ["central_jst", "laminar_adiabatic", "fv_boundary_term"])
-def test_tiled_gather_modes_match(name, mode):
-    # the fused central gather with node blocks staged in shared memory
-    # (compiled for two or three blocks per SM) or reading every neighbour
-    # from global memory, on every level with a thread per node
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("name", ["central_jst", "laminar_adiabatic", "fv_boundary_term", "dissipation_weighting",
+                                  "matrix_dissipation"])
+def test_tiled_gather_modes_match(name, mode, order):
+    # the gathers of every level with a thread per node through the
+    # incidence rows of 256-node blocks, staged in shared memory (modes 1, 2)
+    # or not (3, 4), or through the incidence lists (0); in the caller's node
+    # numbering and in the locality numbering
+    from flite3d_b200.solver import set_node_order
     mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
-    c, g, o = make_pair(mesh, **CASES[name])
+    try:
+        set_node_order(order)
+        c, g, o = make_pair(mesh, **CASES[name])
+    finally:
+        set_node_order(0)
     for level in (1, 2, 3):
         g.set_gather_lanes(level, 1)
         g.set_tiled_gather(level, mode)
     for cyc in range(1, 4):
         g.cycle(cyc)
         o.cycle(cyc)
-    assert_same_state(g, o, f"{name} tiled mode {mode}")
+    assert_same_state(g, o, f"{name} tiled mode {mode} order {order}")
     assert np.array_equal(g.residual_fwd(g.get_state(1)), o.residual_fwd(o.get_state(1)))
 
 
@@ -254,7 +262,7 @@ def test_node_order_changes_no_result():
             runs.append((s.get_state(1), s.get_state(2), s.get_state(3), s.get_pressure(1), s.residuals(),
                          s.forces(), s.residual_fwd(u0)))
     finally:
-        set_node_order(1)
+        set_node_order(0)
     a, b = runs
     for k in (0, 1, 2, 3, 6):
         assert np.array_equal(a[k], b[k]), k
