@@ -284,6 +284,10 @@ struct flite_ctx {
         visc_flux(l);
     }
     void visc_grad(int l) {
+        if (c.viscosityScheme == 2) {  // makeViscosityTerm2 (def_par:5896-6807)
+            FLITE_GATHER(k_visc2_grad, l, P, V(l));
+            return;
+        }
         if (const int m = tiled_other(l)) {
             if (m <= 2) k_visc_grad_tiled<true><<<V(l).tile.ntiles, kTile, tile_smem(l, m, 4), s>>>(P, V(l));
             else k_visc_grad_tiled<false><<<V(l).tile.ntiles, kTile, 0, s>>>(P, V(l));
@@ -292,6 +296,10 @@ struct flite_ctx {
         FLITE_GATHER(k_visc_grad, l, P, V(l));
     }
     void visc_flux(int l) {
+        if (c.viscosityScheme == 2) {
+            FLITE_GATHER(k_visc2_flux, l, P, V(l));
+            return;
+        }
         if (const int m = tiled_other(l)) {
             if (m <= 2) k_visc_flux_tiled<true><<<V(l).tile.ntiles, kTile, tile_smem(l, m, 12), s>>>(P, V(l));
             else k_visc_flux_tiled<false><<<V(l).tile.ntiles, kTile, 0, s>>>(P, V(l));

@@ -125,7 +125,8 @@ const char *unsupported_reason(const flite_controls &c) {
         return "turbulenceModel 2 and 3 (k-omega, SST) are not supported";
     if (c.turbulenceModel == 1 && !(c.ReynoldsNumber > 0)) return "the Spalart-Allmaras model needs ReynoldsNumber > 0";
     if (c.turbulenceModel == 1 && c.precision != FLITE_FP64) return "the Spalart-Allmaras model runs in FP64";
-    if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return "viscosityScheme 2 is not supported";
+    if (c.ReynoldsNumber > 0 && c.viscosityScheme != 1 && c.viscosityScheme != 2)
+        return "viscosityScheme must be 1 or 2";
     if (c.fluxType < 1 || c.fluxType > 4) return "fluxType must be 1..4";
     if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && c.GradientMethod != 1 && c.numberOfGridsToUse != 1)
         return "least-squares gradients need numberOfGridsToUse = 1: the reference's LS gradient divides "
@@ -437,7 +438,9 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             const bool visc = c->ReynoldsNumber > 0.0;
             L.q = X.alloc<NodeRec>(N);
             CK(cudaMemset(L.q, 0, (size_t)N * sizeof(NodeRec)));
-            L.tau = visc ? X.alloc<double>(9 * (size_t)N) : nullptr;
+            // stress and heat flux (scheme 1), or the scaled gradients with mu
+            // and k (scheme 2)
+            L.tau = visc ? X.alloc<double>((c->viscosityScheme == 2 ? 14 : 9) * (size_t)N) : nullptr;
             L.prim = visc ? X.alloc<double>(4 * (size_t)N) : nullptr;
             L.lap = X.alloc<double>(5 * (size_t)N);
             L.sens = X.alloc<double>(N);

@@ -762,6 +762,252 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, Lev
     for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
 }
 
+// ---- makeViscosityTerm2, the compact stencil (def_par:5896-6807) ---------
+// pass 1: the Galerkin gradients of (u, v, w, T) as in k_visc_grad (with the
+// FV boundary form under boundaryTerm 2), then per node the viscosity and
+// the gradients scaled by mu (velocity) and k (temperature), stored with mu
+// and k as tau[14][N]; the adiabatic-wall projection and the wall stress of
+// the wall nodes on level 1; zero temperature gradients on every boundary
+// node of isentropic (adiabatic) walls
+__device__ __forceinline__ void visc2_grad_finish(const Params &P, const LevelView &L, int i, const double *g) {
+    const int N = L.N;
+    const double gOg = P.gamma / (P.gamma - 1.0);
+    const double vt = 1. / L.V[i];
+    double gs[12];
+    for (int c = 0; c < 12; ++c) gs[c] = g[c] * vt;
+    const double dudx = gs[0], dvdx = gs[1], dwdx = gs[2];
+    const double dudy = gs[4], dvdy = gs[5], dwdy = gs[6];
+    const double dudz = gs[8], dvdz = gs[9], dwdz = gs[10];
+    const double tempConv = (P.gamma - 1.0) * P.mach * P.mach;
+    double T = gOg * L.p[i] / L.u[i];
+    if (T <= 0.001) T = 0.001;
+    double a = tempConv * T;
+    double mu = (1. / P.Re) * ((a * sqrt(a)) * ((P.Tinf + 198.6) / (tempConv * P.Tinf * T + 198.6)));
+    double kc = (1. / P.Pr) * mu;
+    L.mu[i] = mu;
+    if (P.sa) {
+        const double a1 = dudy - dvdx, a2 = dvdz - dwdy, a3 = dwdx - dudz;
+        L.vort[i] = sqrt((a1 * a1 + a2 * a2) + a3 * a3);
+        L.divg[i] = (dudx + dvdy) + dwdz;
+        double tvc = (1. / P.Re) * L.u[i] * L.u[5 * N + i];
+        const double ksi3 = flite_pm::pm_cube(tvc / mu);
+        tvc = tvc * ksi3 / (ksi3 + 357.9);
+        mu = mu + tvc;
+        kc = kc + tvc * P.oPrt;
+    }
+#pragma unroll
+    for (int q = 0; q < 12; ++q) gs[q] = ((q & 3) == 3 ? kc : mu) * gs[q];
+    const unsigned char cls = L.bc[i];
+    if (L.grid == 1 && cls == BC_WALL) {
+        const double n0 = L.nx[i], n1 = L.ny[i], n2 = L.nz[i];
+        const double nt = (gs[3] * n0 + gs[7] * n1) + gs[11] * n2;
+        gs[3] = gs[3] - nt * n0;
+        gs[7] = gs[7] - nt * n1;
+        gs[11] = gs[11] - nt * n2;
+        const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+        const double c1 = fourThirds * gs[0] - twoThirds * (gs[5] + gs[10]), c2 = gs[4] + gs[1];
+        const double c3 = gs[8] + gs[2], c4 = fourThirds * gs[5] - twoThirds * (gs[0] + gs[10]);
+        const double c5 = gs[9] + gs[6], c6 = fourThirds * gs[10] - twoThirds * (gs[0] + gs[5]);
+        L.wstress[i] = (c1 * n0 + c2 * n1) + c3 * n2;
+        L.wstress[N + i] = (c2 * n0 + c4 * n1) + c5 * n2;
+        L.wstress[2 * N + i] = (c3 * n0 + c5 * n1) + c6 * n2;
+    }
+    if (P.isentropic && i < L.Nb) gs[3] = gs[7] = gs[11] = 0.0;
+    for (int q = 0; q < 12; ++q) L.tau[q * N + i] = gs[q];
+    L.tau[12 * N + i] = mu;
+    L.tau[13 * N + i] = kc;
+}
+
+template <int U>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc2_grad(Params P, LevelView L) {
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
+    const int N = L.N;
+    double g[12];
+    for (int c = 0; c < 12; ++c) g[c] = 0.0;
+    auto prim = [&](int j, double *q) {
+        q[0] = L.prim[j]; q[1] = L.prim[N + j]; q[2] = L.prim[2 * N + j]; q[3] = L.prim[3 * N + j];
+    };
+    double qi[4];
+    prim(i, qi);
+    auto iterms = [&](int k, double *d) {
+        int2 t = L.inc[k];
+        int e = t.x >= 0 ? t.x : ~t.x;
+        double qj[4];
+        prim(t.y, qj);
+        const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 4; ++c) {
+                double x = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
+                d[a * 4 + c] = t.x >= 0 ? x : -x;
+            }
+    };
+    auto bterms = [&](int k, double *d) {
+        if (P.boundaryTerm == 1) {
+            visc_grad_bterms(L, k, d);
+            return;
+        }
+        // boundaryTerm 2: 4 q w_b of the node itself (def_par:6113-6138)
+        const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+        const int2 nd = L.bedge[b];
+        const int j = side == 0 ? nd.x : nd.y;
+        double q[4];
+        prim(j, q);
+        const double w[3] = {L.bwx[b], L.bwy[b], L.bwz[b]};
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 4; ++c) d[a * 4 + c] = 4. * q[c] * w[a];
+    };
+    auto add = [&](const double *d) {
+        for (int c = 0; c < 12; ++c) g[c] = g[c] + d[c];
+    };
+    if constexpr (U > 1) {
+        group_gather<U, 12, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, iterms, add);
+        group_gather<U, 12, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, add);
+        if (!active || gl) return;
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[12];
+            iterms(k, v);
+            add(v);
+        }
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[12];
+            bterms(k, v);
+            add(v);
+        }
+    }
+    visc2_grad_finish(P, L, i, g);
+}
+
+// node j's data of the compact flux: scaled gradients (12), mu, k,
+// velocity and temperature (from 1/rho as the routine forms them) and
+// coordinates (zero on coarse levels)
+struct Visc2Node {
+    double G[12], mu, k, v[4], x[3];
+};
+__device__ __forceinline__ void load_visc2(const Params &P, const LevelView &L, int j, Visc2Node &o) {
+    const int N = L.N;
+    for (int q = 0; q < 12; ++q) o.G[q] = L.tau[q * N + j];
+    o.mu = L.tau[12 * N + j];
+    o.k = L.tau[13 * N + j];
+    const double ri = 1.0 / L.u[j];
+    o.v[0] = L.u[N + j] * ri; o.v[1] = L.u[2 * N + j] * ri; o.v[2] = L.u[3 * N + j] * ri;
+    o.v[3] = (P.gamma / (P.gamma - 1.0)) * L.p[j] * ri;
+    o.x[0] = L.cx[j]; o.x[1] = L.cy[j]; o.x[2] = L.cz[j];
+}
+
+// the compact flux of an edge from its first (a) and second (b) node
+// (def_par:6432-6556)
+__device__ __forceinline__ void visc2_edge_flux(const Visc2Node &a, const Visc2Node &b, double slen, double wx,
+                                                double wy, double wz, double *f) {
+    const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+    const double inv = 1.0 / slen;
+    const double r[3] = {(b.x[0] - a.x[0]) * inv, (b.x[1] - a.x[1]) * inv, (b.x[2] - a.x[2]) * inv};
+    double G[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) G[q][d] = a.G[d * 4 + q] + b.G[d * 4 + q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double dr = (G[q][0] * r[0] + G[q][1] * r[1]) + G[q][2] * r[2];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) G[q][d] = G[q][d] - dr * r[d];
+        const double cf = q < 3 ? a.mu + b.mu : a.k + b.k;
+        const double dq = cf * (b.v[q] - a.v[q]) * inv;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) G[q][d] = G[q][d] + dq * r[d];
+    }
+    const double dt1 = fourThirds * G[0][0] - twoThirds * (G[1][1] + G[2][2]), dt2 = G[0][1] + G[1][0];
+    const double dt3 = G[0][2] + G[2][0], dt4 = fourThirds * G[1][1] - twoThirds * (G[0][0] + G[2][2]);
+    const double dt5 = G[1][2] + G[2][1], dt6 = fourThirds * G[2][2] - twoThirds * (G[0][0] + G[1][1]);
+    const double dt7 = G[3][0], dt8 = G[3][1], dt9 = G[3][2];
+    const double au = 0.5 * (a.v[0] + b.v[0]), av = 0.5 * (a.v[1] + b.v[1]), aw = 0.5 * (a.v[2] + b.v[2]);
+    const double dut1 = (au * dt1 + av * dt2) + aw * dt3;
+    const double dut2 = (au * dt2 + av * dt4) + aw * dt5;
+    const double dut3 = (au * dt3 + av * dt5) + aw * dt6;
+    f[0] = (wx * dt1 + wy * dt2) + wz * dt3;
+    f[1] = (wx * dt2 + wy * dt4) + wz * dt5;
+    f[2] = (wx * dt3 + wy * dt5) + wz * dt6;
+    f[3] = (wx * (dt7 + dut1) + wy * (dt8 + dut2)) + wz * (dt9 + dut3);
+}
+
+// pass 2: the compact edge fluxes and the boundary faces' 4 w_b times each
+// node's own stress, gathered per node and subtracted from the dissipation
+template <int U>
+__global__ void __launch_bounds__(256, U == 1 ? 2 : 1) k_visc2_flux(Params P, LevelView L) {
+    const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
+    const int i_raw = U > 1 ? tid() / U : tid();
+    if (U == 1 && i_raw >= L.N) return;
+    const bool active = i_raw < L.N;
+    const int i = active ? i_raw : L.N - 1;  // idle groups read a valid node
+    const int N = L.N;
+    Visc2Node me;
+    load_visc2(P, L, i, me);
+    double acc[4] = {0, 0, 0, 0};
+    auto iterms = [&](int k, double *g) {
+        const int2 t = L.inc[k];
+        const int e = t.x >= 0 ? t.x : ~t.x;
+        Visc2Node nb;
+        load_visc2(P, L, t.y, nb);
+        double f[4];
+        if (t.x >= 0) visc2_edge_flux(me, nb, L.slen[e], L.wx[e], L.wy[e], L.wz[e], f);
+        else visc2_edge_flux(nb, me, L.slen[e], L.wx[e], L.wy[e], L.wz[e], f);
+        for (int c = 0; c < 4; ++c) g[c] = t.x >= 0 ? f[c] : -f[c];
+    };
+    // a boundary face of this node: g[4] = 1 when it counts (not symmetry or
+    // inviscid wall)
+    auto bterms = [&](int k, double *g) {
+        const int bb = L.binc[k] >> 1;
+        const int ind = L.bind[bb];
+        g[4] = (ind == 2 || ind == 9) ? 0.0 : 1.0;
+        if (g[4] == 0.0) return;
+        const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+        const double wx = L.bwx[bb], wy = L.bwy[bb], wz = L.bwz[bb];
+        const double *G = me.G;
+        const double t1 = fourThirds * G[0] - twoThirds * (G[5] + G[10]), t2 = G[4] + G[1], t3 = G[8] + G[2];
+        const double t4 = fourThirds * G[5] - twoThirds * (G[0] + G[10]), t5 = G[9] + G[6];
+        const double t6 = fourThirds * G[10] - twoThirds * (G[0] + G[5]);
+        double t7 = G[3], t8 = G[7], t9 = G[11];
+        if (P.isentropic) t7 = t8 = t9 = 0.0;
+        const double *v = me.v;
+        const double d1 = (v[0] * t1 + v[1] * t2) + v[2] * t3;
+        const double d2 = (v[0] * t2 + v[1] * t4) + v[2] * t5;
+        const double d3 = (v[0] * t3 + v[1] * t5) + v[2] * t6;
+        g[0] = 4.0 * ((wx * t1 + wy * t2) + wz * t3);
+        g[1] = 4.0 * ((wx * t2 + wy * t4) + wz * t5);
+        g[2] = 4.0 * ((wx * t3 + wy * t5) + wz * t6);
+        g[3] = 4.0 * ((wx * (t7 + d1) + wy * (t8 + d2)) + wz * (t9 + d3));
+    };
+    auto iadd = [&](const double *g) {
+        for (int c = 0; c < 4; ++c) acc[c] = acc[c] + g[c];
+    };
+    auto badd = [&](const double *g) {
+        if (g[4] == 0.0) return;
+        for (int c = 0; c < 4; ++c) acc[c] = acc[c] + g[c];
+    };
+    if constexpr (U > 1) {
+        group_gather<U, 4, double>(L.inc_ptr[i], L.inc_ptr[i + 1], active, gl, iterms, iadd);
+        group_gather<U, 5, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, badd);
+        if (!active || gl) return;
+    } else {
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+            double v[4];
+            iterms(k, v);
+            iadd(v);
+        }
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[5];
+            bterms(k, v);
+            badd(v);
+        }
+    }
+    for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
+}
+
 __global__ void k_fill(double *a, size_t n, double v) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = v;
@@ -1752,6 +1998,16 @@ template __global__ void k_visc_grad<4>(Params, LevelView);
 template __global__ void k_visc_grad<8>(Params, LevelView);
 template __global__ void k_visc_grad<16>(Params, LevelView);
 template __global__ void k_visc_grad<32>(Params, LevelView);
+template __global__ void k_visc2_grad<1>(Params, LevelView);
+template __global__ void k_visc2_grad<4>(Params, LevelView);
+template __global__ void k_visc2_grad<8>(Params, LevelView);
+template __global__ void k_visc2_grad<16>(Params, LevelView);
+template __global__ void k_visc2_grad<32>(Params, LevelView);
+template __global__ void k_visc2_flux<1>(Params, LevelView);
+template __global__ void k_visc2_flux<4>(Params, LevelView);
+template __global__ void k_visc2_flux<8>(Params, LevelView);
+template __global__ void k_visc2_flux<16>(Params, LevelView);
+template __global__ void k_visc2_flux<32>(Params, LevelView);
 template __global__ void k_visc_flux<1>(Params, LevelView);
 template __global__ void k_visc_flux<4>(Params, LevelView);
 template __global__ void k_visc_flux<8>(Params, LevelView);

@@ -20,6 +20,10 @@ template <int U>
 __global__ void k_visc_grad(Params P, LevelView L);
 template <int U>
 __global__ void k_visc_flux(Params P, LevelView L);
+template <int U>
+__global__ void k_visc2_grad(Params P, LevelView L);
+template <int U>
+__global__ void k_visc2_flux(Params P, LevelView L);
 __global__ void k_fill(double *a, size_t n, double v);
 __global__ void k_gradient(Params P, LevelView L);
 __global__ void k_jst_flux_matrix(Params P, LevelView L);

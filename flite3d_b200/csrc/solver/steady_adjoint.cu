@@ -1232,6 +1232,8 @@ static const char *steady_adjoint_unsupported(const flite_ctx &X) {
     if (c.dissipationScheme == 1 || c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";
     if (c.useDissipationWeighting) return "the steady adjoint takes unweighted dissipation";
     if (c.useMatrixDissipation) return "the steady adjoint takes the scalar JST dissipation";
+    if (c.ReynoldsNumber > 0 && c.viscosityScheme != 1)
+        return "the steady adjoint takes the viscous term of viscosityScheme 1";
     return nullptr;
 }
 

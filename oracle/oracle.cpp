@@ -612,6 +612,201 @@ struct Oracle {
         for_nodes(g.N, [&](int i) { for (int k = 0; k < 4; ++k) g.diss[1 + k][i] = g.diss[1 + k][i] - nh[9 + k][i]; });
     }
 
+    // the viscous routine of the run: makeViscosityTerm, or the compact
+    // makeViscosityTerm2 with viscosityScheme 2 (def_par:1038-1043)
+    void viscousTerm(Level &g) {
+        if (c.viscosityScheme == 2) makeViscosityTerm2(g);
+        else makeViscosityTerm(g);
+    }
+
+    // ---- makeViscosityTerm2, compact stencil (def_par:5896-6807) -----------
+    // Galerkin gradients of (u, v, w, T) as in makeViscosityTerm (with the FV
+    // boundary form under boundaryTerm 2), scaled per node by mu (velocity)
+    // and k (temperature); per edge the sum of both ends' scaled gradients
+    // with its component along the edge replaced by the compact difference
+    // (mu1 + mu2)(q2 - q1)/|dx| (coordinates of level 1; zero on coarse
+    // levels, where the correction vanishes); boundary faces take 4 w_b
+    // times each node's own stress.
+    void makeViscosityTerm2(Level &g) {
+        const double gOg = c.gamma / (c.gamma - 1.0);
+        const double tempConv = (c.gamma - 1.0) * c.MachNumber * c.MachNumber;
+        const double Tin = c.inflowTemperature;
+        for (int k = 0; k < 14; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        auto prim = [&](int i, double *q) {
+            double r = g.u[0][i];
+            q[0] = g.u[1][i] / r; q[1] = g.u[2][i] / r; q[2] = g.u[3][i] / r;
+            q[3] = gOg * g.p[i] / r;
+        };
+        for_edges(g, [&](int e) {
+            int i1 = g.s1[e], i2 = g.s2[e];
+            double w[3] = {g.wx[e], g.wy[e], g.wz[e]};
+            double q1[4], q2[4];
+            prim(i1, q1); prim(i2, q2);
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 4; ++k) {
+                    double d = (q1[k] + q2[k]) * w[a];
+                    nh[a * 4 + k][i1] = nh[a * 4 + k][i1] + d;
+                    nh[a * 4 + k][i2] = nh[a * 4 + k][i2] - d;
+                }
+        });
+        for_bedges(g, [&](int b) {
+            int i1 = g.b1[b], i2 = g.b2[b];
+            double w[3] = {g.bwx[b], g.bwy[b], g.bwz[b]};
+            double q1[4], q2[4];
+            prim(i1, q1); prim(i2, q2);
+            if (c.boundaryTerm == 1) {
+                for (int a = 0; a < 3; ++a)
+                    for (int k = 0; k < 4; ++k) nh[a * 4 + k][i1] = nh[a * 4 + k][i1] + (2. * q1[k] + (q1[k] + q2[k])) * w[a];
+                for (int a = 0; a < 3; ++a)
+                    for (int k = 0; k < 4; ++k) nh[a * 4 + k][i2] = nh[a * 4 + k][i2] + (2. * q2[k] + (q1[k] + q2[k])) * w[a];
+            } else {
+                for (int a = 0; a < 3; ++a)
+                    for (int k = 0; k < 4; ++k) nh[a * 4 + k][i1] = nh[a * 4 + k][i1] + 4. * q1[k] * w[a];
+                for (int a = 0; a < 3; ++a)
+                    for (int k = 0; k < 4; ++k) nh[a * 4 + k][i2] = nh[a * 4 + k][i2] + 4. * q2[k] * w[a];
+            }
+        });
+        const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+        const double oRe = 1. / c.ReynoldsNumber, oPr = 1. / c.PrandtlNumber;
+        for_nodes(g.N, [&](int i) {
+            const double vt = 1. / g.V[i];
+            for (int k = 0; k < 12; ++k) nh[k][i] = nh[k][i] * vt;
+            const double dudx = nh[0][i], dvdx = nh[1][i], dwdx = nh[2][i];
+            const double dudy = nh[4][i], dvdy = nh[5][i], dwdy = nh[6][i];
+            const double dudz = nh[8][i], dvdz = nh[9][i], dwdz = nh[10][i];
+            double T = gOg * g.p[i] / g.u[0][i];
+            if (T <= 0.001) T = 0.001;
+            double a = tempConv * T;
+            double mu = oRe * ((a * std::sqrt(a)) * ((Tin + 198.6) / (tempConv * Tin * T + 198.6)));
+            double k = oPr * mu;
+            g.mu[i] = mu;
+            {
+                const double a1 = dudy - dvdx, a2 = dvdz - dwdy, a3 = dwdx - dudz;
+                g.vort[i] = std::sqrt((a1 * a1 + a2 * a2) + a3 * a3);
+                g.divg[i] = (dudx + dvdy) + dwdz;
+            }
+            if (sa()) {  // def_par:6290-6300
+                double tvc = oRe * g.u[0][i] * g.u[5][i];
+                const double ksi3 = flite_pm::pm_cube(tvc / mu);
+                tvc = tvc * ksi3 / (ksi3 + 357.9);
+                mu = mu + tvc;
+                k = k + tvc * (1. / c.turbulentPrandtlNumber);
+            }
+            for (int q : {0, 1, 2, 4, 5, 6, 8, 9, 10}) nh[q][i] = mu * nh[q][i];
+            for (int q : {3, 7, 11}) nh[q][i] = k * nh[q][i];
+            nh[12][i] = mu;
+            nh[13][i] = k;
+        });
+        if (g.grid == 1) {
+            // setTemperatureForAdiabaticWall on the scaled temperature
+            // gradients (def_par:6346-6349), then the wall stress of the wall
+            // nodes (:6351-6393)
+            for_range(g, -20, -19, [&](int ip) {
+                double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+                double dT[3] = {nh[3][ip], nh[7][ip], nh[11][ip]};
+                double nt = (dT[0] * n[0] + dT[1] * n[1]) + dT[2] * n[2];
+                nh[3][ip] = dT[0] - nt * n[0];
+                nh[7][ip] = dT[1] - nt * n[1];
+                nh[11][ip] = dT[2] - nt * n[2];
+            });
+            for_range(g, -20, -19, [&](int ip) {
+                double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+                const double dudx = nh[0][ip], dvdx = nh[1][ip], dwdx = nh[2][ip];
+                const double dudy = nh[4][ip], dvdy = nh[5][ip], dwdy = nh[6][ip];
+                const double dudz = nh[8][ip], dvdz = nh[9][ip], dwdz = nh[10][ip];
+                const double c1 = fourThirds * dudx - twoThirds * (dvdy + dwdz), c2 = dudy + dvdx, c3 = dudz + dwdx;
+                const double c4 = fourThirds * dvdy - twoThirds * (dudx + dwdz), c5 = dvdz + dwdy;
+                const double c6 = fourThirds * dwdz - twoThirds * (dudx + dvdy);
+                g.wallStress[0][ip] = (c1 * n[0] + c2 * n[1]) + c3 * n[2];
+                g.wallStress[1][ip] = (c2 * n[0] + c4 * n[1]) + c5 * n[2];
+                g.wallStress[2][ip] = (c3 * n[0] + c5 * n[1]) + c6 * n[2];
+            });
+        }
+        if (c.wallsAreIsentropic)  // def_par:6399-6405
+            for (int i = 0; i < g.Nb; ++i) nh[3][i] = nh[7][i] = nh[11][i] = 0.0;
+        for (int k = 14; k < 18; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
+        auto vel = [&](int i, double *v) {
+            const double ri = 1.0 / g.u[0][i];
+            v[0] = g.u[1][i] * ri; v[1] = g.u[2][i] * ri; v[2] = g.u[3][i] * ri;
+            v[3] = gOg * g.p[i] * ri;
+        };
+        for_edges(g, [&](int e) {
+            const int i1 = g.s1[e], i2 = g.s2[e];
+            double f[4];
+            visc2_edge(g, e, i1, i2, vel, f);
+            for (int k = 0; k < 4; ++k) {
+                nh[14 + k][i1] = nh[14 + k][i1] + f[k];
+                nh[14 + k][i2] = nh[14 + k][i2] - f[k];
+            }
+        });
+        for (int bb = 0; bb < g.B; ++bb) {
+            const int ind = g.bind[bb];
+            if (ind == 2 || ind == 9) continue;
+            const int i1 = g.b1[bb], i2 = g.b2[bb];
+            const double wx = g.bwx[bb], wy = g.bwy[bb], wz = g.bwz[bb];
+            for (int side = 0; side < 2; ++side) {
+                const int ip = side == 0 ? i1 : i2;
+                double v[4];
+                vel(ip, v);
+                const double dudx = nh[0][ip], dvdx = nh[1][ip], dwdx = nh[2][ip], dTdx = nh[3][ip];
+                const double dudy = nh[4][ip], dvdy = nh[5][ip], dwdy = nh[6][ip], dTdy = nh[7][ip];
+                const double dudz = nh[8][ip], dvdz = nh[9][ip], dwdz = nh[10][ip], dTdz = nh[11][ip];
+                const double t1 = fourThirds * dudx - twoThirds * (dvdy + dwdz), t2 = dudy + dvdx, t3 = dudz + dwdx;
+                const double t4 = fourThirds * dvdy - twoThirds * (dudx + dwdz), t5 = dvdz + dwdy;
+                const double t6 = fourThirds * dwdz - twoThirds * (dudx + dvdy);
+                double t7 = dTdx, t8 = dTdy, t9 = dTdz;
+                if (c.wallsAreIsentropic) t7 = t8 = t9 = 0.0;
+                const double d1 = (v[0] * t1 + v[1] * t2) + v[2] * t3;
+                const double d2 = (v[0] * t2 + v[1] * t4) + v[2] * t5;
+                const double d3 = (v[0] * t3 + v[1] * t5) + v[2] * t6;
+                nh[14][ip] = nh[14][ip] + 4.0 * ((wx * t1 + wy * t2) + wz * t3);
+                nh[15][ip] = nh[15][ip] + 4.0 * ((wx * t2 + wy * t4) + wz * t5);
+                nh[16][ip] = nh[16][ip] + 4.0 * ((wx * t3 + wy * t5) + wz * t6);
+                nh[17][ip] = nh[17][ip] + 4.0 * ((wx * (t7 + d1) + wy * (t8 + d2)) + wz * (t9 + d3));
+            }
+        }
+        for_nodes(g.N, [&](int i) { for (int k = 0; k < 4; ++k) g.diss[1 + k][i] = g.diss[1 + k][i] - nh[14 + k][i]; });
+    }
+
+    // the compact viscous flux of edge e = (i1, i2) (def_par:6432-6556)
+    template <class Vel>
+    void visc2_edge(const Level &g, int e, int i1, int i2, Vel &&vel, double *f) {
+        const double twoThirds = 2. / 3., fourThirds = 4. / 3.;
+        const double inv = 1.0 / g.slen[e];
+        const double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
+        const double mmu1 = nh[12][i1], mmu2 = nh[12][i2], k1 = nh[13][i1], k2 = nh[13][i2];
+        double v1[4], v2[4];
+        vel(i1, v1);
+        vel(i2, v2);
+        const double r[3] = {(g.cx[i2] - g.cx[i1]) * inv, (g.cy[i2] - g.cy[i1]) * inv, (g.cz[i2] - g.cz[i1]) * inv};
+        // summed scaled gradients: G[q][a] = d q / d x_a, q = u, v, w, T
+        double G[4][3];
+        for (int q = 0; q < 4; ++q)
+            for (int a = 0; a < 3; ++a) G[q][a] = nh[a * 4 + q][i1] + nh[a * 4 + q][i2];
+        const double cf[4] = {mmu1 + mmu2, mmu1 + mmu2, mmu1 + mmu2, k1 + k2};
+        for (int q = 0; q < 4; ++q) {
+            const double dr = (G[q][0] * r[0] + G[q][1] * r[1]) + G[q][2] * r[2];
+            for (int a = 0; a < 3; ++a) G[q][a] = G[q][a] - dr * r[a];
+            const double dq = cf[q] * (v2[q] - v1[q]) * inv;
+            for (int a = 0; a < 3; ++a) G[q][a] = G[q][a] + dq * r[a];
+        }
+        const double dudx = G[0][0], dudy = G[0][1], dudz = G[0][2];
+        const double dvdx = G[1][0], dvdy = G[1][1], dvdz = G[1][2];
+        const double dwdx = G[2][0], dwdy = G[2][1], dwdz = G[2][2];
+        const double dt1 = fourThirds * dudx - twoThirds * (dvdy + dwdz), dt2 = dudy + dvdx, dt3 = dudz + dwdx;
+        const double dt4 = fourThirds * dvdy - twoThirds * (dudx + dwdz), dt5 = dvdz + dwdy;
+        const double dt6 = fourThirds * dwdz - twoThirds * (dudx + dvdy);
+        const double dt7 = G[3][0], dt8 = G[3][1], dt9 = G[3][2];
+        const double au = 0.5 * (v1[0] + v2[0]), av = 0.5 * (v1[1] + v2[1]), aw = 0.5 * (v1[2] + v2[2]);
+        const double dut1 = (au * dt1 + av * dt2) + aw * dt3;
+        const double dut2 = (au * dt2 + av * dt4) + aw * dt5;
+        const double dut3 = (au * dt3 + av * dt5) + aw * dt6;
+        f[0] = (wx * dt1 + wy * dt2) + wz * dt3;
+        f[1] = (wx * dt2 + wy * dt4) + wz * dt5;
+        f[2] = (wx * dt3 + wy * dt5) + wz * dt6;
+        f[3] = (wx * (dt7 + dut1) + wy * (dt8 + dut2)) + wz * (dt9 + dut3);
+    }
+
     // ---- computeGradient, Galerkin (def_par:2923-3245) --------------------
     void computeGradient(Level &g, vec *u) {
         for (int k = 0; k < 15; ++k) std::fill(nh[k].begin(), nh[k].begin() + g.N, 0.0);
@@ -1530,7 +1725,7 @@ struct Oracle {
             makeTimeSteps(g);
             dissipation_for(g, false);
             if (c.ReynoldsNumber > 0.0) {
-                makeViscosityTerm(g);
+                viscousTerm(g);
                 if (turb) {
                     makeTurbulentTimeSteps(g);
                     makeSADiffusion(g);
@@ -1620,7 +1815,7 @@ struct Oracle {
         makeTimeSteps(C);
         if (c.coarseGridDissipationScheme == 2) makeArtificialDissipation2(C);
         else if (c.coarseGridDissipationScheme == 3) makeArtificialDissipation3(C);
-        if (c.ReynoldsNumber > 0.0) makeViscosityTerm(C);
+        if (c.ReynoldsNumber > 0.0) viscousTerm(C);
         for (int k = 0; k < nv; ++k) std::fill(C.rhs[k].begin(), C.rhs[k].end(), 0.0);
         makeRHS(C);
         if (turb) {
@@ -1647,7 +1842,7 @@ struct Oracle {
         makePressureField(F, F.u);
         for (int i = 0; i < F.N; ++i) F.p[i] = std::fabs(F.p[i]);
         dissipation_for(F, true);
-        if (c.ReynoldsNumber > 0.0) makeViscosityTerm(F);
+        if (c.ReynoldsNumber > 0.0) viscousTerm(F);
         for (int k = 0; k < nv; ++k) std::fill(F.rhs[k].begin(), F.rhs[k].end(), 0.0);
         makeRHS(F);
         if (turb) {
@@ -1915,7 +2110,7 @@ int check_controls(const flite_controls &c) {
     if (c.turbulenceModel != 0 && c.turbulenceModel != 1) return FLITE_EUNSUPPORTED;
     if (c.forceCalcType != 1 && c.forceCalcType != 3) return FLITE_EUNSUPPORTED;
     if (c.turbulenceModel == 1 && !(c.ReynoldsNumber > 0)) return FLITE_EUNSUPPORTED;
-    if (c.ReynoldsNumber > 0 && c.viscosityScheme == 2) return FLITE_EUNSUPPORTED;
+    if (c.ReynoldsNumber > 0 && c.viscosityScheme != 1 && c.viscosityScheme != 2) return FLITE_EUNSUPPORTED;
     if (c.fluxType < 1 || c.fluxType > 4) return FLITE_EUNSUPPORTED;
     // least-squares gradients divide by |dx|^2 of coarse-level coordinates
     // the reference never fills (0*inf = NaN): single-grid runs only
@@ -2804,7 +2999,7 @@ int oracle_viscous_term(oracle_ctx *o, int level, const double *u, double *diss,
     o->o.makePressureField(*g, g->u);
     for (int i = 0; i < g->N; ++i) g->p[i] = std::fabs(g->p[i]);
     for (int k = 0; k < 5; ++k) std::fill(g->diss[k].begin(), g->diss[k].end(), 0.0);
-    o->o.makeViscosityTerm(*g);
+    o->o.viscousTerm(*g);
     for (int k = 0; k < 5; ++k) std::memcpy(diss + (size_t)k * g->N, g->diss[k].data(), 8 * (size_t)g->N);
     std::memcpy(mu, g->mu.data(), 8 * (size_t)g->N);
     for (int k = 0; k < 3; ++k)
@@ -2901,7 +3096,7 @@ int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const
     if (!o || !u || !du || !v || !dv) return FLITE_EINVAL;
     const flite_controls &c = o->o.c;
     if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 1 || c.dissipationScheme == 3 ||
-        c.useDissipationWeighting ||
+        c.useDissipationWeighting || (c.ReynoldsNumber > 0 && c.viscosityScheme != 1) ||
         c.useMatrixDissipation || c.flowType != 0 || c.rungeKuttaStages != 3)
         return FLITE_EUNSUPPORTED;
     const bool visc = c.ReynoldsNumber > 0;
@@ -2929,6 +3124,7 @@ int oracle_objective_jvp(oracle_ctx *o, int which, const double *u, const double
                          const double *dbw, const double *dvol, double *J, double *dJ) {
     if (!o || !u || !du || !J || !dJ || which < 0 || which > 1) return FLITE_EINVAL;
     if (o->o.c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
+    if (o->o.c.ReynoldsNumber > 0 && o->o.c.viscosityScheme != 1) return FLITE_EUNSUPPORTED;
     TanIteration T(o->o, dsw, dbw, dvol);
     const size_t N = T.N;
     std::vector<Dl> x[5];

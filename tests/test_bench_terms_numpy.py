@@ -410,3 +410,108 @@ def test_one_smoother_iteration_in_the_interior(re):
     assert deep.sum() > 50
     _close(u[:, deep], got[:, deep])
     assert np.abs(u[:, deep] - u0[:, deep]).max() > 1e-6
+
+
+def viscous_term_compact(c, g, u, p):
+    """makeViscosityTerm2 (def_par:5896-6807) from the Fortran: returns (the
+    term as added to the dissipation [5][N], mu, wall stress)."""
+    i1, i2, b1, b2 = g.i1, g.i2, g.b1, g.b2
+    gog = c.gamma / (c.gamma - 1.0)
+    q = np.vstack([u[1:4] / u[0], gog * p / u[0]])
+    grad = np.zeros((3, 4, g.N))
+    for a in range(3):
+        s = (q[:, i1] + q[:, i2]) * g.sw[a]
+        for k in range(4):
+            np.add.at(grad[a, k], i1, s[k])
+            np.add.at(grad[a, k], i2, -s[k])
+            if c.boundaryTerm == 1:
+                sb = q[:, b1] + q[:, b2]
+                np.add.at(grad[a, k], b1, (2.0 * q[k, b1] + sb[k]) * g.bw[a])
+                np.add.at(grad[a, k], b2, (2.0 * q[k, b2] + sb[k]) * g.bw[a])
+            else:
+                np.add.at(grad[a, k], b1, 4.0 * q[k, b1] * g.bw[a])
+                np.add.at(grad[a, k], b2, 4.0 * q[k, b2] * g.bw[a])
+    grad = grad / g.V
+    T = np.maximum(gog * p / u[0], 0.001)
+    tc = (c.gamma - 1.0) * c.MachNumber ** 2
+    tin = c.inflowTemperature
+    mu = (1.0 / c.ReynoldsNumber) * ((tc * T) ** 1.5 * ((tin + 198.6) / (tc * tin * T + 198.6)))
+    kk = mu / c.PrandtlNumber
+    G = grad.copy()                              # G[a, q] = scaled d q / d x_a
+    G[:, :3] *= mu
+    G[:, 3] *= kk
+    n = g.normal[:, g.wall]
+    dn = (G[:, 3, g.wall] * n).sum(0)
+    G[:, 3, g.wall] -= dn * n
+
+    def stress(Gn):
+        # Gn[a, q] at some nodes -> (t1..t6)
+        return np.array([4 / 3 * Gn[0, 0] - 2 / 3 * (Gn[1, 1] + Gn[2, 2]), Gn[1, 0] + Gn[0, 1],
+                         Gn[2, 0] + Gn[0, 2], 4 / 3 * Gn[1, 1] - 2 / 3 * (Gn[0, 0] + Gn[2, 2]),
+                         Gn[2, 1] + Gn[1, 2], 4 / 3 * Gn[2, 2] - 2 / 3 * (Gn[0, 0] + Gn[1, 1])])
+
+    ws = np.zeros((3, g.N))
+    t = stress(G[:, :, g.wall])
+    ws[0, g.wall] = t[0] * n[0] + t[1] * n[1] + t[2] * n[2]
+    ws[1, g.wall] = t[1] * n[0] + t[3] * n[1] + t[4] * n[2]
+    ws[2, g.wall] = t[2] * n[0] + t[4] * n[1] + t[5] * n[2]
+    if c.wallsAreIsentropic:
+        G[:, 3, :g.Nb] = 0.0
+    vel = np.vstack([u[1:4] * (1.0 / u[0]), gog * p * (1.0 / u[0])])
+    inv = 1.0 / g.slen
+    x = g.base.array(1, "coords")  # the coordinates the level descriptor carries
+    r = (x[:, i2] - x[:, i1]) * inv
+    S = G[:, :, i1] + G[:, :, i2]
+    cf = np.array([mu[i1] + mu[i2]] * 3 + [kk[i1] + kk[i2]])
+    for k in range(4):
+        dr = (S[:, k] * r).sum(0)
+        S[:, k] = S[:, k] - dr * r + cf[k] * (vel[k, i2] - vel[k, i1]) * inv * r
+    dt = stress(S)
+    av = 0.5 * (vel[:3, i1] + vel[:3, i2])
+    dut = np.array([av[0] * dt[0] + av[1] * dt[1] + av[2] * dt[2], av[0] * dt[1] + av[1] * dt[3] + av[2] * dt[4],
+                    av[0] * dt[2] + av[1] * dt[4] + av[2] * dt[5]])
+    w = g.sw
+    f = np.array([w[0] * dt[0] + w[1] * dt[1] + w[2] * dt[2], w[0] * dt[1] + w[1] * dt[3] + w[2] * dt[4],
+                  w[0] * dt[2] + w[1] * dt[4] + w[2] * dt[5],
+                  w[0] * (S[0, 3] + dut[0]) + w[1] * (S[1, 3] + dut[1]) + w[2] * (S[2, 3] + dut[2])])
+    acc = np.zeros((4, g.N))
+    for k in range(4):
+        np.add.at(acc[k], i1, f[k])
+        np.add.at(acc[k], i2, -f[k])
+    keep = (g.bind != 2) & (g.bind != 9)
+    for node, side in ((g.b1[keep], 0), (g.b2[keep], 1)):
+        bw = g.bw[:, keep]
+        tn = stress(G[:, :, node])
+        tT = G[:, 3, node] * (0.0 if c.wallsAreIsentropic else 1.0)
+        v = vel[:3, node]
+        d = np.array([v[0] * tn[0] + v[1] * tn[1] + v[2] * tn[2], v[0] * tn[1] + v[1] * tn[3] + v[2] * tn[4],
+                      v[0] * tn[2] + v[1] * tn[4] + v[2] * tn[5]])
+        fb = 4.0 * np.array([bw[0] * tn[0] + bw[1] * tn[1] + bw[2] * tn[2],
+                             bw[0] * tn[1] + bw[1] * tn[3] + bw[2] * tn[4],
+                             bw[0] * tn[2] + bw[1] * tn[4] + bw[2] * tn[5],
+                             bw[0] * (tT[0] + d[0]) + bw[1] * (tT[1] + d[1]) + bw[2] * (tT[2] + d[2])])
+        for k in range(4):
+            np.add.at(acc[k], node, fb[k])
+    term = np.zeros((5, g.N))
+    term[1:] = -acc
+    return term, mu, ws
+
+
+@pytest.mark.parametrize("isentropic,bterm", [(1, 1), (0, 1), (1, 2)], ids=["adiabatic", "isothermal", "fv_faces"])
+def test_compact_viscous_term(geo, isentropic, bterm):
+    # makeViscosityTerm2 (viscosityScheme 2): the compact stencil with the
+    # edge-direction difference, on the jittered mesh's level 1
+    c = default_controls(ReynoldsNumber=5000.0, fluxType=1, numberOfGridsToUse=1, wallsAreIsentropic=isentropic,
+                         viscosityScheme=2, boundaryTerm=bterm)
+    o = Solver(c, geo.mesh, backend=oracle_backend())
+    u = _state(c, geo, seed=12)
+    d_o, mu_o, ws_o = np.zeros((5, geo.N)), np.zeros(geo.N), np.zeros((3, geo.N))
+    assert o.be.viscous_term(o._h, 1, _ptr(u), _ptr(d_o), _ptr(mu_o), _ptr(ws_o)) == 0
+    term, mu, ws = viscous_term_compact(c, geo, u, np.abs(pressure(c, u)))
+    _close(mu, mu_o)
+    _close(term[1:], d_o[1:])
+    _close(ws[:, geo.wall], ws_o[:, geo.wall])
+    # the compact term differs from the wide one
+    wide = viscous_term(default_controls(ReynoldsNumber=5000.0, wallsAreIsentropic=isentropic), geo, u,
+                        np.abs(pressure(c, u)))[0]
+    assert np.abs(wide[1:] - term[1:]).max() > 1e-6 * np.abs(term[1:]).max()

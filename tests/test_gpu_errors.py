@@ -49,7 +49,8 @@ def test_out_of_range_indices_are_rejected(field, fn):
 @pytest.mark.parametrize("ctl,cpu_refuses", [
     (dict(turbulenceModel=2), True), (dict(flowType=2), True),
     (dict(flowType=1, physicalTimeStep=0.0), True),
-    (dict(viscosityScheme=2, ReynoldsNumber=100.0), True), (dict(coarseGridDissipationScheme=1), True),
+    (dict(viscosityScheme=3, ReynoldsNumber=100.0), True), (dict(coarseGridDissipationScheme=1), True),
+    (dict(forceCalcType=2), True),
     (dict(fluxType=4, HLLCFluxOrder=2, GradientMethod=2, numberOfGridsToUse=2), True),
     # the extension's reconstruction belongs to the Roe flux; 3 or 5 stages
     (dict(reconstruction=1, fluxType=1), True), (dict(reconstruction=1, fluxType=4), True),

@@ -53,6 +53,14 @@ CASES = {
                                       secondOrderDissipationFactor=0.6),
     "laminar_matrix_dissipation": dict(fluxType=1, useMatrixDissipation=1, ReynoldsNumber=5000.0,
                                        wallsAreIsentropic=1),
+    # viscosityScheme 2 (makeViscosityTerm2, the compact stencil)
+    "laminar_visc2_adiabatic": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=1, viscosityScheme=2),
+    "laminar_visc2_isothermal": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=0, CFLNumber=0.5,
+                                     viscosityScheme=2),
+    "laminar_visc2_fv": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=1, viscosityScheme=2,
+                             boundaryTerm=2),
+    "laminar_visc2_hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1, ReynoldsNumber=5000.0,
+                                wallsAreIsentropic=1, viscosityScheme=2),
     # forceCalcType 3 (calculateLiftAndDrag3): its face loads pass through
     # the reference's shared help array, which the cycles after it must not see
     "laminar_forces_type3": dict(fluxType=1, ReynoldsNumber=5000.0, wallsAreIsentropic=1, forceCalcType=3,
@@ -203,7 +211,7 @@ def test_launch_options_do_not_change_results(opts):
 
 @pytest.mark.parametrize("lanes", [1, 4, 8, 16, 32])
 @pytest.mark.parametrize("name", ["central_jst", "hllc2_autoclip", "laminar_adiabatic", "first_order_diss",
-                                  "roe_muscl_va_rk5"])
+                                  "roe_muscl_va_rk5", "laminar_visc2_isothermal"])
 def test_gather_lanes_match(name, lanes):
     # every gather shape (a thread, or a group of 4..32 lanes, per node) on
     # every level gives the reference's sums

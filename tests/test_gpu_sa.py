@@ -25,6 +25,7 @@ CASES = {
     "sa_scheme1": dict(multigridScheme=1),
     "sa_scheme0": dict(multigridScheme=0),
     "sa_fv_boundary": dict(boundaryTerm=2),
+    "sa_compact_viscous": dict(viscosityScheme=2),
 }
 
 
