@@ -203,7 +203,10 @@ def run_ours(args):
                 solver.set_gather_lanes(lvl, g)
                 for mode in ((0, 1, 2, 3, 4) if g == 1 else (0,)):
                     solver.set_tiled_gather(lvl, mode)
-                    t[(g, mode)] = sum(solver.profile_kernels(lvl, reps=5).values())
+                    groups = solver.profile_kernels(lvl, reps=5)
+                    t[(g, mode)] = sum(groups.values())
+                    if lvl <= 2 and g == 1:
+                        tuning_levels[f"{lvl}_groups_tiled{mode}"] = groups
             lanes[lvl], tiled[lvl] = min(t, key=t.get)
             tuning_levels[lvl] = {f"lanes{g}_tiled{m}": v for (g, m), v in t.items()}
     for lvl in range(1, solver.nlevels + 1):

@@ -63,6 +63,19 @@ using namespace flite_detail;
         }                                                                           \
     } while (0)
 
+// a row-gather kernel template (STAGE, AHEAD) launched for mode m (1: staged,
+// one ahead; 2: staged; 3: one ahead; 4: neither) over the level's blocks g,
+// staging K fields per node
+#define FLITE_ROWS(kern, K)                                                                    \
+    do {                                                                                       \
+        switch (m) {                                                                           \
+            case 1: kern<true, true><<<g, kTile, tile_smem(l, m, K), s>>>(P, V(l)); break;      \
+            case 2: kern<true, false><<<g, kTile, tile_smem(l, m, K), s>>>(P, V(l)); break;     \
+            case 3: kern<false, true><<<g, kTile, 0, s>>>(P, V(l)); break;                      \
+            default: kern<false, false><<<g, kTile, 0, s>>>(P, V(l));                           \
+        }                                                                                      \
+    } while (0)
+
 struct flite_ctx {
     flite_controls c{};
     Params P{};
@@ -202,15 +215,17 @@ struct flite_ctx {
             const int K = !P.viscous ? 0 : (P.sa ? 3 : 2);
             const unsigned g = V(l).tile.ntiles;
             const size_t sm = tile_smem(l, m, K);
-            if (m <= 2) {
-                if (K == 0) k_timestep_tiled<0, true><<<g, kTile, sm, s>>>(P, V(l));
-                else if (K == 2) k_timestep_tiled<2, true><<<g, kTile, sm, s>>>(P, V(l));
-                else k_timestep_tiled<3, true><<<g, kTile, sm, s>>>(P, V(l));
-            } else {
-                if (K == 0) k_timestep_tiled<0, false><<<g, kTile, 0, s>>>(P, V(l));
-                else if (K == 2) k_timestep_tiled<2, false><<<g, kTile, 0, s>>>(P, V(l));
-                else k_timestep_tiled<3, false><<<g, kTile, 0, s>>>(P, V(l));
-            }
+#define FLITE_TS(KK)                                                                                      \
+    switch (m) {                                                                                           \
+        case 1: k_timestep_tiled<KK, true, true><<<g, kTile, sm, s>>>(P, V(l)); break;                     \
+        case 2: k_timestep_tiled<KK, true, false><<<g, kTile, sm, s>>>(P, V(l)); break;                    \
+        case 3: k_timestep_tiled<KK, false, true><<<g, kTile, 0, s>>>(P, V(l)); break;                     \
+        default: k_timestep_tiled<KK, false, false><<<g, kTile, 0, s>>>(P, V(l));                          \
+    }
+            if (K == 0) { FLITE_TS(0) }
+            else if (K == 2) { FLITE_TS(2) }
+            else { FLITE_TS(3) }
+#undef FLITE_TS
             return;
         }
         FLITE_GATHER(k_timestep, l, P, V(l));
@@ -242,16 +257,14 @@ struct flite_ctx {
         const unsigned g = L.tile.ntiles;
         counted();
         if (m && !P.useDissW) {
-            if (m <= 2) k_jst_lap_tiled<true><<<g, kTile, tile_smem(l, m, 6), s>>>(P, L);
-            else k_jst_lap_tiled<false><<<g, kTile, 0, s>>>(P, L);
+            FLITE_ROWS(k_jst_lap_tiled, 6);
         } else {
             FLITE_GATHER(k_jst_lap, l, P, L);
         }
         counted();
         if (P.matrixDiss) k_jst_flux_matrix<<<nblk(L.N), nb, 0, s>>>(P, L);
         else if (m) {
-            if (m <= 2) k_jst_flux_tiled<true><<<g, kTile, tile_smem(l, m, 13), s>>>(P, L);
-            else k_jst_flux_tiled<false><<<g, kTile, 0, s>>>(P, L);
+            FLITE_ROWS(k_jst_flux_tiled, 13);
         } else {
             FLITE_GATHER(k_jst_flux, l, P, L);
         }
@@ -289,8 +302,8 @@ struct flite_ctx {
             return;
         }
         if (const int m = tiled_other(l)) {
-            if (m <= 2) k_visc_grad_tiled<true><<<V(l).tile.ntiles, kTile, tile_smem(l, m, 4), s>>>(P, V(l));
-            else k_visc_grad_tiled<false><<<V(l).tile.ntiles, kTile, 0, s>>>(P, V(l));
+            const unsigned g = V(l).tile.ntiles;
+            FLITE_ROWS(k_visc_grad_tiled, 4);
             return;
         }
         FLITE_GATHER(k_visc_grad, l, P, V(l));
@@ -301,8 +314,8 @@ struct flite_ctx {
             return;
         }
         if (const int m = tiled_other(l)) {
-            if (m <= 2) k_visc_flux_tiled<true><<<V(l).tile.ntiles, kTile, tile_smem(l, m, 12), s>>>(P, V(l));
-            else k_visc_flux_tiled<false><<<V(l).tile.ntiles, kTile, 0, s>>>(P, V(l));
+            const unsigned g = V(l).tile.ntiles;
+            FLITE_ROWS(k_visc_flux_tiled, 12);
             return;
         }
         FLITE_GATHER(k_visc_flux, l, P, V(l));
@@ -420,10 +433,10 @@ struct flite_ctx {
             const TileView &T = V(l).tile;
             const size_t sm = (size_t)T.stage_max * sizeof(NodeRec);
             switch (tiled(l)) {
-                case 2: k_node_update_tiled<3, true><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage); break;
-                case 3: k_node_update_tiled<2, false><<<T.ntiles, kTile, 0, s>>>(P, V(l), mode, stage); break;
-                case 4: k_node_update_tiled<3, false><<<T.ntiles, kTile, 0, s>>>(P, V(l), mode, stage); break;
-                default: k_node_update_tiled<2, true><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
+                case 2: k_node_update_tiled<true, false><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage); break;
+                case 3: k_node_update_tiled<false, true><<<T.ntiles, kTile, 0, s>>>(P, V(l), mode, stage); break;
+                case 4: k_node_update_tiled<false, false><<<T.ntiles, kTile, 0, s>>>(P, V(l), mode, stage); break;
+                default: k_node_update_tiled<true, true><<<T.ntiles, kTile, sm, s>>>(P, V(l), mode, stage);
             }
             return;
         }

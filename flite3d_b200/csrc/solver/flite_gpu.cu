@@ -230,12 +230,14 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         CK(cudaStreamCreateWithFlags(&X.s, cudaStreamNonBlocking));
         // shared memory of the staged incidence-row gathers (above the
         // default 48 KB for the wider node fields)
-        CK(cudaFuncSetAttribute(k_jst_flux_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                13 * 8 * kTileStageMax));
-        CK(cudaFuncSetAttribute(k_visc_flux_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                12 * 8 * kTileStageMax));
-        CK(cudaFuncSetAttribute(k_jst_lap_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                6 * 8 * kTileStageMax));
+        for (bool ahead : {true, false}) {
+            CK(cudaFuncSetAttribute(ahead ? k_jst_flux_tiled<true, true> : k_jst_flux_tiled<true, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 13 * 8 * kTileStageMax));
+            CK(cudaFuncSetAttribute(ahead ? k_visc_flux_tiled<true, true> : k_visc_flux_tiled<true, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * 8 * kTileStageMax));
+            CK(cudaFuncSetAttribute(ahead ? k_jst_lap_tiled<true, true> : k_jst_lap_tiled<true, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 6 * 8 * kTileStageMax));
+        }
         CK(cudaMallocHost(&X.h_cycle, sizeof(int)));
         X.d_cycle = X.alloc<int>(1);
         X.d_cyc = X.alloc<int>(G);

@@ -1612,8 +1612,9 @@ __device__ __forceinline__ NodeRec load_node_shared(const NodeRec *rec, int slot
     return o;
 }
 
-template <int MINB, bool STAGE>
-__global__ void __launch_bounds__(kTile, MINB) k_node_update_tiled(Params P, LevelView L, int mode, int stage) {
+template <bool STAGE, bool AHEAD>
+__global__ void __launch_bounds__(kTile, AHEAD ? 2 : 3) k_node_update_tiled(Params P, LevelView L, int mode,
+                                                                            int stage) {
     extern __shared__ float4 stage_mem[];
     NodeRec *rec = reinterpret_cast<NodeRec *>(stage_mem);
     const TileView &T = L.tile;
@@ -1644,6 +1645,26 @@ __global__ void __launch_bounds__(kTile, MINB) k_node_update_tiled(Params P, Lev
         return load_node_shared(rec, v);
     };
     double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!AHEAD) {
+        for (int k = 0; k < deg; ++k) {
+            const size_t x = base + (size_t)k * kTile;
+            const unsigned m = __ldg(meta + x);
+            const double wx = __ldg(T.wx + x), wy = __ldg(T.wy + x), wz = __ldg(T.wz + x);
+            const NodeRec n = fetch(m);
+            double f[5];
+            if (!(m & kTileSecond)) {
+                central_flux_rec(si, n, wx, wy, wz, f);
+                r[0] = r[0] + f[0]; r[1] = r[1] + f[1]; r[2] = r[2] + f[2]; r[3] = r[3] + f[3]; r[4] = r[4] + f[4];
+            } else {
+                central_flux_rec(n, si, wx, wy, wz, f);
+                r[0] = r[0] + (-f[0]); r[1] = r[1] + (-f[1]); r[2] = r[2] + (-f[2]); r[3] = r[3] + (-f[3]);
+                r[4] = r[4] + (-f[4]);
+            }
+        }
+        gather_boundary<1>(L, i, r);
+        node_tail(P, L, i, r, mode, stage);
+        return;
+    }
     // the loads of incidence k+1 are issued before incidence k is evaluated
     unsigned m0 = 0;
     double wx0 = 0, wy0 = 0, wz0 = 0;
@@ -1737,13 +1758,22 @@ struct Inc {
     __device__ __forceinline__ bool first() const { return !(m & kTileSecond); }
 };
 
-// walk node i's incidence rows calling fn(inc) in edge order, one ahead
-template <int K, bool STAGE, bool W, class Fn>
+// walk node i's incidence rows calling fn(inc) in edge order (AHEAD: the
+// loads of incidence k+1 issued before fn sees incidence k)
+template <int K, bool STAGE, bool W, bool AHEAD, class Fn>
 __device__ __forceinline__ void row_walk(const LevelView &L, const double *sm, const double *const *f, int i,
                                          Fn &&fn) {
     const int deg = L.inc_ptr[i + 1] - L.inc_ptr[i];
     const size_t base = (size_t)L.tile.row[blockIdx.x] * kTile + threadIdx.x;
     if (deg <= 0) return;
+    if (!AHEAD) {
+        for (int k = 0; k < deg; ++k) {
+            Inc<K, STAGE, W> a;
+            a.load(L, sm, f, base + (size_t)k * kTile);
+            fn(a);
+        }
+        return;
+    }
     Inc<K, STAGE, W> a, b;
     a.load(L, sm, f, base);
     for (int k = 0; k < deg; ++k) {
@@ -1755,7 +1785,7 @@ __device__ __forceinline__ void row_walk(const LevelView &L, const double *sm, c
 
 // makeTimeSteps: K = 0 (inviscid: the other node is not read), 2 (mu, rho),
 // 3 (with the SA nu~)
-template <int K, bool STAGE>
+template <int K, bool STAGE, bool AHEAD>
 __global__ void __launch_bounds__(kTile, 3) k_timestep_tiled(Params P, LevelView L) {
     extern __shared__ double sm[];
     const int N = L.N;
@@ -1767,7 +1797,7 @@ __global__ void __launch_bounds__(kTile, 3) k_timestep_tiled(Params P, LevelView
     const double m1 = L.u[N + i], m2 = L.u[2 * N + i], m3 = L.u[3 * N + i];
     const double cc = dmax(c1 * L.p[i] * ro, 0.001);
     double acc = 0.0, h = 0.0;
-    row_walk<K, STAGE, true>(L, sm, f, i, [&](const Inc<K, STAGE, true> &t) {
+    row_walk<K, STAGE, true, AHEAD>(L, sm, f, i, [&](const Inc<K, STAGE, true> &t) {
         const double wx = t.w[0], wy = t.w[1], wz = t.w[2];
         double al = (wx * wx + wy * wy) + wz * wz;
         double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
@@ -1808,7 +1838,7 @@ __global__ void __launch_bounds__(kTile, 3) k_timestep_tiled(Params P, LevelView
 
 // makeArtificialDissipation2 passes 1-2 (no dissipation weighting): the
 // other node's u and p
-template <bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void __launch_bounds__(kTile, 3) k_jst_lap_tiled(Params P, LevelView L) {
     extern __shared__ double sm[];
     const int N = L.N;
@@ -1819,7 +1849,7 @@ __global__ void __launch_bounds__(kTile, 3) k_jst_lap_tiled(Params P, LevelView 
     const double ui0 = L.u[i], ui1 = L.u[N + i], ui2 = L.u[2 * N + i], ui3 = L.u[3 * N + i], ui4 = L.u[4 * N + i];
     const double pi = L.p[i];
     const double df = 1.0;
-    row_walk<6, STAGE, false>(L, sm, f, i, [&](const Inc<6, STAGE, false> &t) {
+    row_walk<6, STAGE, false, AHEAD>(L, sm, f, i, [&](const Inc<6, STAGE, false> &t) {
         const double uj0 = t.v[0], uj1 = t.v[1], uj2 = t.v[2], uj3 = t.v[3], uj4 = t.v[4], pj = t.v[5];
         if (t.first()) {
             double d0 = ui0 - uj0, d1 = ui1 - uj1, d2 = ui2 - uj2, d3 = ui3 - uj3;
@@ -1846,8 +1876,8 @@ __global__ void __launch_bounds__(kTile, 3) k_jst_lap_tiled(Params P, LevelView 
 
 // makeArtificialDissipation2 pass 3, scalar: the other node's V/dt,
 // connectivity, sensor, Laplacian and u
-template <bool STAGE>
-__global__ void __launch_bounds__(kTile, 2) k_jst_flux_tiled(Params P, LevelView L) {
+template <bool STAGE, bool AHEAD>
+__global__ void __launch_bounds__(kTile, AHEAD ? 2 : 3) k_jst_flux_tiled(Params P, LevelView L) {
     extern __shared__ double sm[];
     const int N = L.N;
     const double *f[13] = {L.vdt, L.conn, L.sens,
@@ -1860,7 +1890,7 @@ __global__ void __launch_bounds__(kTile, 2) k_jst_flux_tiled(Params P, LevelView
     double Li[5], Ui[5];
     for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
     const double vdi = L.vdt[i], coni = L.conn[i], si = L.sens[i];
-    row_walk<13, STAGE, false>(L, sm, f, i, [&](const Inc<13, STAGE, false> &t) {
+    row_walk<13, STAGE, false, AHEAD>(L, sm, f, i, [&](const Inc<13, STAGE, false> &t) {
         const bool first = t.first();
         const double vdj = t.v[0], conj = t.v[1];
         double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
@@ -1886,7 +1916,7 @@ __global__ void __launch_bounds__(kTile, 2) k_jst_flux_tiled(Params P, LevelView
 
 // makeViscosityTerm pass 1 (gradients, then the node's stress and heat
 // flux as in k_visc_grad): the other node's (u, v, w, T)
-template <bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void __launch_bounds__(kTile, 3) k_visc_grad_tiled(Params P, LevelView L) {
     extern __shared__ double sm[];
     const int N = L.N;
@@ -1896,7 +1926,7 @@ __global__ void __launch_bounds__(kTile, 3) k_visc_grad_tiled(Params P, LevelVie
     double g[12];
     for (int c = 0; c < 12; ++c) g[c] = 0.0;
     const double qi[4] = {L.prim[i], L.prim[N + i], L.prim[2 * N + i], L.prim[3 * N + i]};
-    row_walk<4, STAGE, true>(L, sm, f, i, [&](const Inc<4, STAGE, true> &t) {
+    row_walk<4, STAGE, true, AHEAD>(L, sm, f, i, [&](const Inc<4, STAGE, true> &t) {
         const bool first = t.first();
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -1916,8 +1946,8 @@ __global__ void __launch_bounds__(kTile, 3) k_visc_grad_tiled(Params P, LevelVie
 
 // makeViscosityTerm pass 2 (as k_visc_flux): the other node's stress, heat
 // flux and velocity
-template <bool STAGE>
-__global__ void __launch_bounds__(kTile, 2) k_visc_flux_tiled(Params P, LevelView L) {
+template <bool STAGE, bool AHEAD>
+__global__ void __launch_bounds__(kTile, AHEAD ? 2 : 3) k_visc_flux_tiled(Params P, LevelView L) {
     extern __shared__ double sm[];
     const int N = L.N;
     const double *f[12] = {L.tau, L.tau + N, L.tau + 2 * (size_t)N, L.tau + 3 * (size_t)N, L.tau + 4 * (size_t)N,
@@ -1929,7 +1959,7 @@ __global__ void __launch_bounds__(kTile, 2) k_visc_flux_tiled(Params P, LevelVie
     for (int c = 0; c < 9; ++c) ti[c] = L.tau[c * N + i];
     ui[0] = L.prim[i]; ui[1] = L.prim[N + i]; ui[2] = L.prim[2 * N + i];
     double acc[4] = {0, 0, 0, 0};
-    row_walk<12, STAGE, true>(L, sm, f, i, [&](const Inc<12, STAGE, true> &t) {
+    row_walk<12, STAGE, true, AHEAD>(L, sm, f, i, [&](const Inc<12, STAGE, true> &t) {
         const bool first = t.first();
         const double *tj = t.v, *uj = t.v + 9;
         double fl[4];
@@ -1941,22 +1971,24 @@ __global__ void __launch_bounds__(kTile, 2) k_visc_flux_tiled(Params P, LevelVie
     for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
 }
 
-#define FLITE_TILED_INST(STAGE)                                                     \
-    template __global__ void k_timestep_tiled<0, STAGE>(Params, LevelView);         \
-    template __global__ void k_timestep_tiled<2, STAGE>(Params, LevelView);         \
-    template __global__ void k_timestep_tiled<3, STAGE>(Params, LevelView);         \
-    template __global__ void k_jst_lap_tiled<STAGE>(Params, LevelView);            \
-    template __global__ void k_jst_flux_tiled<STAGE>(Params, LevelView);           \
-    template __global__ void k_visc_grad_tiled<STAGE>(Params, LevelView);          \
-    template __global__ void k_visc_flux_tiled<STAGE>(Params, LevelView);
-FLITE_TILED_INST(true)
-FLITE_TILED_INST(false)
+#define FLITE_TILED_INST(STAGE, AHEAD)                                                     \
+    template __global__ void k_timestep_tiled<0, STAGE, AHEAD>(Params, LevelView);         \
+    template __global__ void k_timestep_tiled<2, STAGE, AHEAD>(Params, LevelView);         \
+    template __global__ void k_timestep_tiled<3, STAGE, AHEAD>(Params, LevelView);         \
+    template __global__ void k_jst_lap_tiled<STAGE, AHEAD>(Params, LevelView);            \
+    template __global__ void k_jst_flux_tiled<STAGE, AHEAD>(Params, LevelView);           \
+    template __global__ void k_visc_grad_tiled<STAGE, AHEAD>(Params, LevelView);          \
+    template __global__ void k_visc_flux_tiled<STAGE, AHEAD>(Params, LevelView);
+FLITE_TILED_INST(true, true)
+FLITE_TILED_INST(true, false)
+FLITE_TILED_INST(false, true)
+FLITE_TILED_INST(false, false)
 #undef FLITE_TILED_INST
 
-template __global__ void k_node_update_tiled<2, true>(Params, LevelView, int, int);
-template __global__ void k_node_update_tiled<3, true>(Params, LevelView, int, int);
-template __global__ void k_node_update_tiled<2, false>(Params, LevelView, int, int);
-template __global__ void k_node_update_tiled<3, false>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<true, true>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<true, false>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<false, true>(Params, LevelView, int, int);
+template __global__ void k_node_update_tiled<false, false>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 1>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 4>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 8>(Params, LevelView, int, int);

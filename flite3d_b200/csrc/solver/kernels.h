@@ -65,17 +65,17 @@ __global__ void k_resid_partial(LevelView L, double *part, int nblk);
 __global__ void k_resid_final(const double *part, int nblk, double *out);
 __global__ void k_forces(Params P, LevelView L, const int *wall, int nwall, double alphaR, double betaR,
                          double ground, double d0, double d1, double d2, double *part);
-template <int MINB, bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void k_node_update_tiled(Params P, LevelView L, int mode, int stage);
-template <int K, bool STAGE>
+template <int K, bool STAGE, bool AHEAD>
 __global__ void k_timestep_tiled(Params P, LevelView L);
-template <bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void k_jst_lap_tiled(Params P, LevelView L);
-template <bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void k_jst_flux_tiled(Params P, LevelView L);
-template <bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void k_visc_grad_tiled(Params P, LevelView L);
-template <bool STAGE>
+template <bool STAGE, bool AHEAD>
 __global__ void k_visc_flux_tiled(Params P, LevelView L);
 // dst[c*N + i] = src[c*N + map[i]] for c < ncomp (node arrays between the
 // caller's numbering and the device's)
