@@ -48,12 +48,6 @@ struct __align__(16) IncRec32 {  // the same in FP32 (16 B); j is ~j when this
 struct __align__(16) NodeRec {  // what the central flux reads of a node (48 B)
     double ru, rv, rw, rinv, p, rh;  // momentum, 1/rho, pressure, E + p
 };
-// NodeRec as stored: padded to 64 bytes and 32-byte aligned, so that a
-// neighbour is read with two 32-byte vector loads (two requests of one
-// sector per thread instead of three 16-byte ones)
-struct __align__(32) NodeRec64 {
-    double ru, rv, rw, rinv, p, rh, pad0, pad1;
-};
 struct __align__(16) DeltaRec {  // FP32 anchor primitives and increments (48 B)
     float ra, vax, vay, vaz, ha;  // anchor rho, velocity, E + p
     float dr, dmx, dmy, dmz, dE, dp, pad;  // u - ua and p - pa
@@ -130,7 +124,7 @@ struct LevelView {
     double *lpw;                           // [N]  edge-factor sums of dissipation scheme 1 (level 1)
     double *tau;                           // [9][N] stress tensor + heat flux
     double *prim;                          // [4][N] u, v, w, T of the viscous term
-    NodeRec64 *q;                          // [N] written with p by k_pressure (the level-1
+    NodeRec *q;                            // [N] written with p by k_pressure (48 B: the level-1
                                            // records of the bench mesh fit the 126 MB L2)
     // Spalart-Allmaras: nu~ is component 6 of u, uprev, rhs, src ([6][N])
     double *turbDiff, *dtT, *vort, *divg;  // [N] diffusion, turbulent dt, |curl u|, div u
@@ -160,16 +154,11 @@ struct LevelView {
     TileView tile;                         // staging of node blocks (fluxType 1)
 };
 
-// 32-byte vector load through the read-only path (p 32-byte aligned)
-__device__ __forceinline__ void ld_nc_v4(const double *p, double &a, double &b, double &c, double &d) {
-    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
-}
-__device__ __forceinline__ void st_v4(double *p, double a, double b, double c, double d) {
-    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
-}
 __device__ __forceinline__ EdgeW load_edgew(const EdgeW *w, int e) {
+    const double2 *p = reinterpret_cast<const double2 *>(w + e);
+    const double2 a = __ldg(p), b = __ldg(p + 1);
     EdgeW o;
-    ld_nc_v4(reinterpret_cast<const double *>(w + e), o.wx, o.wy, o.wz, o.pad);
+    o.wx = a.x; o.wy = a.y; o.wz = b.x; o.pad = b.y;
     return o;
 }
 __device__ __forceinline__ IncRec32 load_inc32(const IncRec32 *r, int k) {
@@ -198,22 +187,15 @@ __device__ __forceinline__ void store_rec(R *base, int j, const R &o) {
 #pragma unroll
     for (int k = 0; k < K; ++k) p[k] = d[k];
 }
-__device__ __forceinline__ NodeRec load_node(const NodeRec64 *q, int j) {
-    NodeRec o;
-    double pad0, pad1;
-    const double *p = reinterpret_cast<const double *>(q + j);
-    ld_nc_v4(p, o.ru, o.rv, o.rw, o.rinv);
-    ld_nc_v4(p + 4, o.p, o.rh, pad0, pad1);
-    return o;
-}
+__device__ __forceinline__ NodeRec load_node(const NodeRec *q, int j) { return load_rec<NodeRec, 3>(q, j); }
 __device__ __forceinline__ PrimRec load_prim(const PrimRec *q, int j) { return load_rec<PrimRec, 4>(q, j); }
 // 1/rho and E + p are the operations the central flux performs per edge
 // end, done once per node
-__device__ __forceinline__ void store_node(NodeRec64 *q, int j, double r, double ru, double rv, double rw, double E,
+__device__ __forceinline__ void store_node(NodeRec *q, int j, double r, double ru, double rv, double rw, double E,
                                            double p) {
-    double *d = reinterpret_cast<double *>(q + j);
-    st_v4(d, ru, rv, rw, 1. / r);
-    st_v4(d + 4, p, E + p, 0.0, 0.0);
+    NodeRec o;
+    o.ru = ru; o.rv = rv; o.rw = rw; o.rinv = 1. / r; o.p = p; o.rh = E + p;
+    store_rec<NodeRec, 3>(q, j, o);
 }
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }

@@ -438,8 +438,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             const bool hllc2 = c->fluxType == 4 && c->HLLCFluxOrder > 1 && l == 0;
             const bool muscl = c->reconstruction == FLITE_RECON_VAN_ALBADA && l == 0;
             const bool visc = c->ReynoldsNumber > 0.0;
-            L.q = X.alloc<NodeRec64>(N);
-            CK(cudaMemset(L.q, 0, (size_t)N * sizeof(NodeRec64)));
+            L.q = X.alloc<NodeRec>(N);
+            CK(cudaMemset(L.q, 0, (size_t)N * sizeof(NodeRec)));
             // stress and heat flux (scheme 1), or the scaled gradients with mu
             // and k (scheme 2)
             L.tau = visc ? X.alloc<double>((c->viscosityScheme == 2 ? 14 : 9) * (size_t)N) : nullptr;

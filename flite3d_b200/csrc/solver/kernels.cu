@@ -1624,13 +1624,12 @@ __global__ void __launch_bounds__(kTile, AHEAD ? 2 : 3) k_node_update_tiled(Para
         const int h0 = T.halo_ptr[t];
         const int nh = min(T.halo_ptr[t + 1] - h0, kTileStageMax - kTile);
         const float4 *q = reinterpret_cast<const float4 *>(L.q);
-        // 16-byte pieces: the 3 of a 48-byte record (of the 4 stored), own
-        // records then the halo's
+        // 16-byte pieces: 3 per record, own records then the halo's
         for (int s = threadIdx.x; s < 3 * (cnt + nh); s += blockDim.x) {
             const int r = s / 3, part = s - 3 * r;
             const int j = r < cnt ? n0 + r : T.halo[h0 + (r - cnt)];
             const int slot = r < cnt ? r : kTile + (r - cnt);
-            stage_mem[3 * slot + part] = __ldg(q + 4 * (size_t)j + part);
+            stage_mem[3 * slot + part] = __ldg(q + 3 * (size_t)j + part);
         }
         __syncthreads();
     }
