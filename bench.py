@@ -148,6 +148,56 @@ def node_kernel_bytes(mesh):
         + d.n_bnodes * 24
 
 
+def group_bytes(mesh, dissipation_weighting=False):
+    """Algorithmic bytes of each level-1 kernel group of one relaxation step
+    (the groups of flite_profile_kernels, laminar FP64 with the scalar JST and
+    a thread per node).  Every array is counted once per launch (a node's own
+    and its neighbours' reads of an array are one read), an incidence entry
+    is 8 bytes (two per interior edge), a boundary incidence 4 (two per
+    boundary edge), a CSR offset 4 per node and list:
+      pressure   u (40) in, p (8) and the 48-byte central-flux record out;
+      timestep   u0..3 (32), p, mu, volume (24), two offsets (8), dt and V/dt
+                 out (16); per edge two incidences and wx, wy, wz (24); per
+                 boundary edge its two incidences, node pair (8) and
+                 coefficients (24);
+      dissipation (k_jst_lap + k_jst_flux) u (40), p, connectivity, sensor
+                 out and in (8 each), the Laplacian out and in (40 each), V/dt
+                 (8), dissipation out (40), two offsets; per edge its two
+                 incidences twice (and the edge length twice with dissipation
+                 weighting);
+      visc_prim  u0..3 and p in (40), u, v, w, T out (32);
+      visc_grad  u, v, w, T (32), volume, p, rho (24), class (1), offsets (8),
+                 mu (8) and tau (72) out; per edge two incidences and its
+                 coefficients (40); per boundary edge as in timestep (40);
+                 per boundary node its normal (24) and wall stress out (24);
+      visc_flux  tau (72), u, v, w (24), dissipation 1..4 in and out (64),
+                 offsets (8); per edge 40; per boundary edge 40 and its code (4);
+      node_update as node_kernel_bytes."""
+    d = mesh.level(1)
+    N, E, B, Nb = d.n_nodes, d.n_sides, d.n_bsides, d.n_bnodes
+    return {
+        "pressure": N * (40 + 8 + 48),
+        "timestep": N * (32 + 8 + 8 + 8 + 8 + 16) + E * (16 + 24) + B * (8 + 8 + 24),
+        "dissipation": N * (40 + 8 + 8 + 8 + 8 + 40 + 40 + 8 + 40 + 8) + E * 32
+        + (E * 16 if dissipation_weighting else 0),
+        "visc_prim": N * (40 + 32),
+        "visc_grad": N * (32 + 24 + 1 + 8 + 8 + 72) + E * 40 + B * 40 + Nb * 48,
+        "visc_flux": N * (72 + 24 + 64 + 8) + E * 40 + B * 44,
+        "node_update": node_kernel_bytes(mesh),
+    }
+
+
+def group_roofline(ms, nbytes, hbm):
+    """{group: {ms, algorithmic_bytes, achieved GB/s, frac}} of the groups
+    that have a byte count."""
+    out = {}
+    for k, b in nbytes.items():
+        if k in ms and ms[k] > 0:
+            gbs = b / (ms[k] / 1e3) / 1e9
+            out[k] = {"ms": ms[k], "algorithmic_bytes": b, "achieved_gbs": gbs, "frac": gbs / hbm}
+    return out
+
+
 # DRAM traffic of the dominant kernel per algorithmic byte, from an ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 192x64x64 bump channel (462.0 MB measured against 448.8 MB algorithmic);
@@ -335,6 +385,7 @@ def run_ours(args):
         "node_order": args.node_order,
         "residual_after_warmup": float(res[0]),
         "level1_kernel_ms": kernels_l1,
+        "level1_roofline": group_roofline(kernels_l1, group_bytes(mesh), hbm),
         "coarse_kernel_ms": kernels_coarse,
         "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1],
                                            "gather_lanes_per_level": lanes, "tiled_mode_per_level": tiled},
