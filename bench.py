@@ -119,6 +119,18 @@ def build_case(host_only=False):
     return F, mesh, c, u0, time.time() - t0
 
 
+def apply_options(solver, options, unroll=1):
+    """Set the tuned launch options (node block, lanes, incidence-row mode
+    and shared walks per level) on a solver; none changes a result."""
+    if not options:
+        return
+    solver.set_kernel_options(256, options["node_block"], unroll)
+    for lvl, g in options["lanes"].items():
+        solver.set_gather_lanes(lvl, g)
+        solver.set_tiled_gather(lvl, options["tiled"][lvl] if g == 1 else 0)
+        solver.set_gather_fusion(lvl, options["fuse"][lvl])
+
+
 def node_kernel_name(lanes, tiled, unroll):
     """The instance of the level-1 node kernel the tuned launch options run."""
     what = ("(level 1: central fluxes of the incident edges computed in the node gather, fused with the RK "
@@ -172,7 +184,18 @@ def group_bytes(mesh, dissipation_weighting=False):
                  per boundary node its normal (24) and wall stress out (24);
       visc_flux  tau (72), u, v, w (24), dissipation 1..4 in and out (64),
                  offsets (8); per edge 40; per boundary edge 40 and its code (4);
-      node_update as node_kernel_bytes."""
+      node_update as node_kernel_bytes;
+      ts_lap     (the shared walk of timestep and the Laplacian) u (40), p, mu,
+                 volume, connectivity (32), offsets (8), dt and V/dt out (16),
+                 Laplacian and sensor out (48); per edge and boundary edge as
+                 in timestep;
+      jflux_vgrad (the shared walk of the JST flux and visc_grad) Laplacian,
+                 u (80), V/dt, connectivity, sensor (24), dissipation out
+                 (40), u, v, w, T (32), volume, p (16), class (1), offsets
+                 (8), mu and tau out (80); per edge, boundary edge and boundary
+                 node as in visc_grad.
+    With shared walks the timestep, dissipation and visc_grad groups launch
+    nothing (the viscous workload) and are left out of the fractions."""
     d = mesh.level(1)
     N, E, B, Nb = d.n_nodes, d.n_sides, d.n_bsides, d.n_bnodes
     return {
@@ -184,6 +207,12 @@ def group_bytes(mesh, dissipation_weighting=False):
         "visc_grad": N * (32 + 24 + 1 + 8 + 8 + 72) + E * 40 + B * 40 + Nb * 48,
         "visc_flux": N * (72 + 24 + 64 + 8) + E * 40 + B * 44,
         "node_update": node_kernel_bytes(mesh),
+        # the shared walks: the two groups' bytes less what the second walk
+        # would read again (incidences, offsets, edge coefficients and the
+        # arrays both read)
+        "ts_lap": N * (40 + 8 + 8 + 8 + 8 + 8 + 16 + 40 + 8) + E * (16 + 24) + B * (8 + 8 + 24),
+        "jflux_vgrad": N * (40 + 40 + 8 + 8 + 8 + 40 + 32 + 8 + 8 + 1 + 8 + 8 + 72) + E * (16 + 24) + B * 40
+        + Nb * 48,
     }
 
 
@@ -233,6 +262,8 @@ def run_ours(args):
         lanes = {lvl: v[1 + lvl] for lvl in range(1, solver.nlevels + 1)}
         tm = [int(x) for x in args.tiled_modes.split(",")] if args.tiled_modes else []
         tiled = {lvl: (tm[lvl - 1] if lvl - 1 < len(tm) else 1) for lvl in range(1, solver.nlevels + 1)}
+        fz = [int(x) for x in args.fusion.split(",")] if args.fusion else []
+        fuse = {lvl: (fz[lvl - 1] if lvl - 1 < len(fz) else 1) for lvl in range(1, solver.nlevels + 1)}
     else:
         for nb in (128, 256):
             for unroll in (1, 2):
@@ -244,24 +275,30 @@ def run_ours(args):
     # whether the fused central gather stages node blocks in shared memory:
     # through the incidence rows of node blocks: modes 1..4, 0 off), by the
     # device time of that level's kernels over one relaxation step
+    # (and, with the incidence lists, whether gathers that walk the same list
+    # share one walk), by the device time of that level's kernels over one
+    # relaxation step
     tuning_levels = {}
     if not args.kernel_options:
-        lanes, tiled = {}, {}
+        lanes, tiled, fuse = {}, {}, {}
         for lvl in range(1, solver.nlevels + 1):
             t = {}
             for g in ((1, 4, 8) if lvl == 1 else (1, 4, 8, 16, 32)):
                 solver.set_gather_lanes(lvl, g)
                 for mode in ((0, 1, 2, 3, 4) if g == 1 else (0,)):
                     solver.set_tiled_gather(lvl, mode)
-                    groups = solver.profile_kernels(lvl, reps=5)
-                    t[(g, mode)] = sum(groups.values())
-                    if lvl <= 2 and g == 1:
-                        tuning_levels[f"{lvl}_groups_tiled{mode}"] = groups
-            lanes[lvl], tiled[lvl] = min(t, key=t.get)
-            tuning_levels[lvl] = {f"lanes{g}_tiled{m}": v for (g, m), v in t.items()}
-    for lvl in range(1, solver.nlevels + 1):
-        solver.set_gather_lanes(lvl, lanes[lvl])
-        solver.set_tiled_gather(lvl, tiled[lvl] if lanes[lvl] == 1 else 0)
+                    for fz in ((1, 0) if g == 1 and mode == 0 else (1,)):
+                        solver.set_gather_fusion(lvl, fz)
+                        groups = solver.profile_kernels(lvl, reps=5)
+                        t[(g, mode, fz)] = sum(groups.values())
+                        if lvl <= 2 and g == 1:
+                            key = f"{lvl}_groups_tiled{mode}" + (("_shared" if fz else "_separate") if mode == 0 else "")
+                            tuning_levels[key] = groups
+            lanes[lvl], tiled[lvl], fuse[lvl] = min(t, key=t.get)
+            tuning_levels[lvl] = {f"lanes{g}_tiled{m}" + (f"_shared{f}" if g == 1 and m == 0 else ""): v
+                                  for (g, m, f), v in t.items()}
+    options = {"node_block": best[0], "lanes": lanes, "tiled": tiled, "fuse": fuse}
+    apply_options(solver, options, best[1])
     solver.set_state(u0)
     solver.start()
     # warm-up (also captures the cycle graph)
@@ -326,10 +363,7 @@ def run_ours(args):
     mixed = None
     if not args.no_mixed:
         solver_m = F.Solver(F.default_controls(**CONTROLS, precision=1), mesh)
-        solver_m.set_kernel_options(256, best[0], 1)
-        for lvl, g in lanes.items():
-            solver_m.set_gather_lanes(lvl, g)
-            solver_m.set_tiled_gather(lvl, tiled[lvl] if g == 1 else 0)
+        apply_options(solver_m, options)
         solver_m.set_state(u0)
         solver_m.start()
         for i in range(1, args.warmup + 1):
@@ -343,14 +377,14 @@ def run_ours(args):
                  "node_kernel_ms": node_m_ms, "increment_records_ms": delta_ms}
     ttc = None
     if not args.no_converge:
-        ttc = time_to_converge(F, mesh, c, u0, args.converge_max, (best[0], lanes, tiled))
+        ttc = time_to_converge(F, mesh, c, u0, args.converge_max, options)
 
     cpu = None
     parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mesh, c, u0, cycles=args.cpu_cycles)
     if rank == 0 and ws == 1 and args.parity_cycles > 0:
-        parity = parity_check(F, mesh, c, u0, args.parity_cycles, (best[0], lanes, tiled))
+        parity = parity_check(F, mesh, c, u0, args.parity_cycles, options)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -388,7 +422,8 @@ def run_ours(args):
         "level1_roofline": group_roofline(kernels_l1, group_bytes(mesh), hbm),
         "coarse_kernel_ms": kernels_coarse,
         "node_kernel_options": {"chosen": {"node_block": best[0], "gather_unroll": best[1],
-                                           "gather_lanes_per_level": lanes, "tiled_mode_per_level": tiled},
+                                           "gather_lanes_per_level": lanes, "tiled_mode_per_level": tiled,
+                                           "shared_walks_per_level": fuse},
                                 "ms": {f"nb{k[0]}_unroll{k[1]}": v for k, v in tuning.items()},
                                 "level_ms": tuning_levels},
         "adjoint": {"fwd_ms": fwd_ms, "vjp_ms": vjp_ms, "cost_ratio": vjp_ms / fwd_ms,
@@ -413,11 +448,7 @@ def time_to_converge(F, mesh, c, u0, max_cycles, options=None):
     for name, prec in (("fp64", 0), ("mixed", 1)):
         cc = F.default_controls(**CONTROLS, precision=prec)
         s = F.Solver(cc, mesh)
-        if options:
-            s.set_kernel_options(256, options[0], 1)
-            for lvl, g in options[1].items():
-                s.set_gather_lanes(lvl, g)
-                s.set_tiled_gather(lvl, options[2][lvl] if g == 1 else 0)
+        apply_options(s, options)
         s.set_state(u0)
         s.start()
         torch.cuda.synchronize()
@@ -456,11 +487,7 @@ def parity_check(F, mesh, c, u0, cycles, options=None):
     lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "liboracle.so"))
     lib.oracle_set_threads(1)
     g = F.Solver(c, mesh)
-    if options:
-        g.set_kernel_options(256, options[0], 1)
-        for lvl, lanes in options[1].items():
-            g.set_gather_lanes(lvl, lanes)
-            g.set_tiled_gather(lvl, options[2][lvl] if lanes == 1 else 0)
+    apply_options(g, options)
     o = Solver(c, mesh, backend=Backend(lib, "oracle_"))
     t0 = time.perf_counter()
     for s in (g, o):
@@ -860,6 +887,9 @@ def main():
                     help="device node numbering: 0 the mesh's own, 1 the locality (Morton) order")
     ap.add_argument("--tiled-modes", default=None,
                     help="with --kernel-options: TILED_L1,TILED_L2,... (0 off, 1 or 2 on; default 1)")
+    ap.add_argument("--fusion", default=None,
+                    help="with --kernel-options: per level 1 to share the walks of gathers over the same "
+                         "incidence list, 0 for separate kernels (default 1)")
     ap.add_argument("--no-converge", action="store_true",
                     help="skip the time to a 1e-8 residual reduction, FP64 and FLITE_MIXED")
     ap.add_argument("--parity-cycles", type=int, default=2,

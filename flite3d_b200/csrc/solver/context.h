@@ -204,6 +204,14 @@ struct flite_ctx {
         return lv[l].v.N < kSmallLevelNodes ? 32 : 1;
     }
     unsigned gblk(int l, int g) const { return (unsigned)((g * (size_t)lv[l].v.N + nb - 1) / nb); }
+    // levels whose gathers that walk the same incidence list share one walk
+    // (k_ts_lap, k_jflux_vgrad) where a thread serves a node
+    // (flite_set_gather_fusion: 1 on, the default; 0 off, held as -1)
+    int fuse_mode[kMaxLevels] = {0};
+    bool fuse_walks(int l) const {
+        if (lanes_of(l) != 1 || tiled_other(l)) return false;
+        return !(l < kMaxLevels && fuse_mode[l] < 0);
+    }
 
     void pressure(int l) {
         counted();
@@ -247,12 +255,20 @@ struct flite_ctx {
     }
     // makeArtificialDissipation2 (def_par:11484-11993), scalar form
     void jst(int l) {
-        const LevelView &L = V(l);
-        if ((c.fluxType == 4 && L.grid == 1) ||
-            (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0)) {
+        if (!jst_gathers(l)) {
             zero_diss(l);
             return;
         }
+        jst_lap(l);
+        jst_flux(l);
+    }
+    // the JST kernels run (not the zero dissipation of jst)
+    bool jst_gathers(int l) {
+        return !((c.fluxType == 4 && V(l).grid == 1) ||
+                 (c.fourthOrderDissipationFactor == 0 && c.secondOrderDissipationFactor == 0));
+    }
+    void jst_lap(int l) {
+        const LevelView &L = V(l);
         const int m = tiled_other(l);
         const unsigned g = L.tile.ntiles;
         counted();
@@ -261,12 +277,63 @@ struct flite_ctx {
         } else {
             FLITE_GATHER(k_jst_lap, l, P, L);
         }
+    }
+    void jst_flux(int l) {
+        const LevelView &L = V(l);
+        const int m = tiled_other(l);
+        const unsigned g = L.tile.ntiles;
         counted();
         if (P.matrixDiss) k_jst_flux_matrix<<<nblk(L.N), nb, 0, s>>>(P, L);
         else if (m) {
             FLITE_ROWS(k_jst_flux_tiled, 13);
         } else {
             FLITE_GATHER(k_jst_flux, l, P, L);
+        }
+    }
+    // the time step (ts), the JST dissipation (or its zero) and the viscous
+    // terms of a level, in the order of singleIteration and restrictGrid.
+    // Where a thread serves a node, the time step and the Laplacian share one
+    // walk of the incidence lists (k_ts_lap), and so do the JST flux and the
+    // viscous gradients (k_jflux_vgrad); the viscous primitives, which only
+    // these gradients read, go before the JST flux.
+    // the walks singleIteration's relaxation step shares on level l: 0 none;
+    // 1 k_ts_lap; 2 k_ts_lap and k_jflux_vgrad
+    int step_fusion(int l) {
+        if ((c.dissipationScheme == 1 && V(l).grid == 1) || c.dissipationScheme == 3) return 0;
+        if (!fuse_walks(l) || !jst_gathers(l)) return 0;
+        return (c.ReynoldsNumber > 0.0 && !P.matrixDiss && c.viscosityScheme == 1) ? 2 : 1;
+    }
+    void ts_jst_viscous(int l, bool ts) {
+        const bool visc = c.ReynoldsNumber > 0.0;
+        if (!fuse_walks(l) || !jst_gathers(l)) {
+            if (ts) timesteps(l);
+            jst(l);
+            viscous(l);
+            return;
+        }
+        if (ts) {
+            counted();
+            k_ts_lap<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        } else {
+            jst_lap(l);
+        }
+        if (visc) {
+            counted();
+            k_visc_prim<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        }
+        if (visc && !P.matrixDiss && c.viscosityScheme == 1) {
+            counted();
+            k_jflux_vgrad<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        } else {
+            jst_flux(l);
+            if (visc) {
+                counted();
+                visc_grad(l);
+            }
+        }
+        if (visc) {
+            counted();
+            visc_flux(l);
         }
     }
     void first_order_diss(int l) {
@@ -415,11 +482,10 @@ struct flite_ctx {
             default: launch_node_update_u<1>(l, mode, stage, anchor);
         }
     }
-    // levels whose fused central gather stages node blocks in shared memory
-    // (flite_set_tiled_gather; on by default where the staging data exist)
-    // (flite_set_tiled_gather: 0 off; 1, 2 staged with two or three blocks
-    // of 256 threads per SM; 3, 4 the same incidence rows without staging;
-    // tiled_mode holds -1 for 0 and 0 for the default, off)
+    // levels whose gathers read the incidences through the rows of node
+    // blocks (flite_set_tiled_gather: 0 off; 1, 2 staged in shared memory
+    // with two or three blocks of 256 threads per SM; 3, 4 the same rows
+    // without staging; tiled_mode holds -1 for 0 and 0 for the default, off)
     int tiled_mode[kMaxLevels] = {0};
     int tiled(int l) const {
         if (!(fused() && !mixed() && lv[l].v.tile.ntiles > 0)) return 0;
@@ -455,9 +521,13 @@ struct flite_ctx {
     void singleIteration(int l, bool calcDiss) {
         if (calcDiss) {
             pressure(l);  // p = |p| is the identity after the 0.1 floor
-            timesteps(l);
-            dissipation(l);
-            viscous(l);
+            if ((c.dissipationScheme == 1 && V(l).grid == 1) || c.dissipationScheme == 3) {
+                timesteps(l);
+                dissipation(l);
+                viscous(l);
+            } else {
+                ts_jst_viscous(l, true);
+            }
             if (turb()) {
                 sa_timesteps(l);
                 sa_diffusion(l);
@@ -465,8 +535,10 @@ struct flite_ctx {
         }
         for (int st = 1; st <= P.nstage; ++st) {
             // u == uprev at stage 1: the FP64 evaluation there is the anchor
-            // of the mixed-precision increments of the later stages
-            pressure(l);
+            // of the mixed-precision increments of the later stages.  The
+            // pressure and flux records of stage 1 are those of the step's
+            // own pressure pass when it ran (nothing has changed u since)
+            if (st > 1 || !calcDiss) pressure(l);
             rhs_terms(l, st == 1);
             sa_stage(l, MODE_STAGE, st);
             node_update(l, MODE_STAGE, st, st == 1);
@@ -487,10 +559,13 @@ struct flite_ctx {
         const int cl = fl + 1;
         counted();
         k_restrict_state<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
-        timesteps(cl);
-        if (c.coarseGridDissipationScheme == 2) jst(cl);
-        else if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
-        viscous(cl);
+        if (c.coarseGridDissipationScheme == 2) {
+            ts_jst_viscous(cl, true);
+        } else {
+            timesteps(cl);
+            if (c.coarseGridDissipationScheme == 3) first_order_diss(cl);
+            viscous(cl);
+        }
         rhs_terms(cl);
         if (turb()) {
             sa_timesteps(cl);
@@ -501,9 +576,12 @@ struct flite_ctx {
         pressure(fl);
         // the fine part uses scheme 1 on level 1 under dissipationScheme 1,
         // scheme 2 otherwise (def_par:12269-12273)
-        if (c.dissipationScheme == 1 && V(fl).grid == 1) lp_diss(fl);
-        else jst(fl);
-        viscous(fl);
+        if (c.dissipationScheme == 1 && V(fl).grid == 1) {
+            lp_diss(fl);
+            viscous(fl);
+        } else {
+            ts_jst_viscous(fl, false);
+        }
         rhs_terms(fl, false);
         if (turb()) sa_diffusion(fl);  // the fine level keeps its turbulent time steps
         sa_stage(fl, MODE_RFINE, 0);

@@ -826,6 +826,13 @@ int flite_set_tiled_gather(flite_ctx *ctx, int32_t level, int32_t on) {
     return FLITE_OK;
 }
 
+int flite_set_gather_fusion(flite_ctx *ctx, int32_t level, int32_t on) {
+    if (bad_level(ctx, level) || (on != 0 && on != 1) || level > kMaxLevels) return FLITE_EINVAL;
+    ctx->fuse_mode[level - 1] = on ? 1 : -1;
+    ctx->drop_graph();
+    return FLITE_OK;
+}
+
 int flite_set_gather_lanes(flite_ctx *ctx, int32_t level, int32_t lanes) {
     if (bad_level(ctx, level) || level > kMaxLevels) return FLITE_EINVAL;
     if (!(lanes == 0 || lanes == 1 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32)) return FLITE_EINVAL;
@@ -841,15 +848,25 @@ int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32
         const int l = level - 1;
         LevelView &L = X.V(l);
         // the kernels of one relaxation step of this level, in cycle order
+        // (with shared walks the time step and Laplacian are timed as
+        // ts_lap, the JST flux and viscous gradients as jflux_vgrad, and
+        // their separate groups hold what is left of them)
+        const int fz = X.step_fusion(l);
+        const bool visc = X.c.ReynoldsNumber > 0;
         std::vector<std::function<void()>> k;
         k.push_back([&] { X.pressure(l); });
-        k.push_back([&] { X.timesteps(l); });
-        k.push_back([&] { X.dissipation(l); });
-        k.push_back([&] { if (X.c.ReynoldsNumber > 0) k_visc_prim<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
-        k.push_back([&] { if (X.c.ReynoldsNumber > 0) X.visc_grad(l); });
-        k.push_back([&] { if (X.c.ReynoldsNumber > 0) X.visc_flux(l); });
+        k.push_back([&] { if (!fz) X.timesteps(l); });
+        k.push_back([&] {
+            if (!fz) X.dissipation(l);
+            else if (fz == 1) X.jst_flux(l);
+        });
+        k.push_back([&] { if (visc) k_visc_prim<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
+        k.push_back([&] { if (visc && fz != 2) X.visc_grad(l); });
+        k.push_back([&] { if (visc) X.visc_flux(l); });
         k.push_back([&] { X.rhs_terms(l, true); });
         k.push_back([&] { X.launch_node_update(l, MODE_RFINE, 0, true); });
+        k.push_back([&] { if (fz) k_ts_lap<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
+        k.push_back([&] { if (fz == 2) k_jflux_vgrad<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
         const int m = std::min<int>((int)k.size(), nmax);
         std::vector<cudaEvent_t> ev(m + 1);
         for (auto &e : ev) CK(cudaEventCreate(&e));

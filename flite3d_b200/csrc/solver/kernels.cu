@@ -66,6 +66,80 @@ __global__ void k_pressure(Params P, LevelView L) {
 }
 
 // ---- makeTimeSteps (def_par:13335-13610) as a node gather -----------------
+// The pieces of a thread-per-node gather, shared by the separate kernel, its
+// incidence-row form and the fused walks below.
+//
+// interior edge t of node i (momentum m, 1/rho ro, cc = max(gamma p/rho,
+// 0.001)): the convective and acoustic terms, and with viscosity the other
+// node's viscous term (def_par:13432-13433; with SA the viscosity is
+// mu + nu~/Re)
+__device__ __forceinline__ void ts_inc(const Params &P, const LevelView &L, int2 t, double m1, double m2, double m3,
+                                       double ro, double cc, double &acc, double &h) {
+    const int N = L.N;
+    const int e = t.x >= 0 ? t.x : ~t.x;
+    const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
+    const double al = (wx * wx + wy * wy) + wz * wz;
+    const double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
+    acc = (acc + fabs(vn)) + sqrt(cc * al);
+    if (P.viscous) {
+        const int j = t.y;
+        const double vis = dmax(P.am, P.sa ? L.mu[j] + L.u[5 * N + j] / P.Re : L.mu[j]);
+        const double dv = 2.0 * vis * al / L.u[j];
+        h = h + dv;
+    }
+}
+// boundary edge binc[k]: v[0..3] the convective and acoustic terms of the
+// node's side and of both, v[4..5] the viscous ones
+__device__ __forceinline__ void ts_bterms(const Params &P, const LevelView &L, int k, double *v) {
+    const int N = L.N;
+    const double c1 = P.gamma;
+    const int b = L.binc[k] >> 1, side = L.binc[k] & 1;
+    const int2 nd = L.bedge[b];
+    const double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
+    const double al = (wx * wx + wy * wy) + wz * wz;
+    const int j1 = nd.x, j2 = nd.y;
+    const double ro1 = 1. / L.u[j1], ro2 = 1. / L.u[j2];
+    double cc1 = dmax(c1 * L.p[j1] * ro1, 0.001);
+    double cc2 = dmax(c1 * L.p[j2] * ro2, 0.001);
+    double vn1 = ((wx * L.u[N + j1] + wy * L.u[2 * N + j1]) + wz * L.u[3 * N + j1]) * ro1;
+    double vn2 = ((wx * L.u[N + j2] + wy * L.u[2 * N + j2]) + wz * L.u[3 * N + j2]) * ro2;
+    vn1 = fabs(vn1); vn2 = fabs(vn2);
+    cc1 = sqrt(cc1 * al); cc2 = sqrt(cc2 * al);
+    v[0] = side == 0 ? vn1 : vn2;
+    v[1] = vn1 + vn2;
+    v[2] = side == 0 ? cc1 : cc2;
+    v[3] = cc1 + cc2;
+    if (P.viscous) {
+        const double vis1 = dmax(P.am, P.sa ? L.mu[j1] + L.u[5 * N + j1] / P.Re : L.mu[j1]);
+        const double vis2 = dmax(P.am, P.sa ? L.mu[j2] + L.u[5 * N + j2] / P.Re : L.mu[j2]);
+        const double dv1 = 2.0 * vis1 * al / L.u[j1];
+        const double dv2 = 2.0 * vis2 * al / L.u[j2];
+        v[4] = side == 0 ? dv1 : dv2;
+        v[5] = dv1 + dv2;
+    } else {
+        v[4] = v[5] = 0.0;
+    }
+}
+__device__ __forceinline__ void ts_badd(const Params &P, const double *x, double &acc, double &h) {
+    acc = (((acc + x[0]) + x[1]) + x[2]) + x[3];
+    if (P.viscous) h = (h + x[4]) + x[5];
+}
+__device__ __forceinline__ void ts_store(const LevelView &L, int i, double acc, double h) {
+    const double V = L.V[i];
+    const double dt = 0.5 / (acc / V + h / (V * V));
+    L.dt[i] = dt;
+    L.vdt[i] = V / dt;  // V/dt of the dissipation coefficient d0
+}
+// the boundary edges of node i in order, then dt and V/dt
+__device__ __forceinline__ void ts_finish(const Params &P, const LevelView &L, int i, double acc, double h) {
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        double v[6];
+        ts_bterms(P, L, k, v);
+        ts_badd(P, v, acc, h);
+    }
+    ts_store(L, i, acc, h);
+}
+
 template <int U>
 __global__ void k_timestep(Params P, LevelView L) {
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -102,71 +176,56 @@ __global__ void k_timestep(Params P, LevelView L) {
             if (P.viscous) h = h + x[2];
             });
     } else
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-        int2 t = L.inc[k];
-        int e = t.x >= 0 ? t.x : ~t.x;
-        double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
-        double al = (wx * wx + wy * wy) + wz * wz;
-        double vn = ((wx * m1 + wy * m2) + wz * m3) * ro;
-        acc = (acc + fabs(vn)) + sqrt(cc * al);
-        if (P.viscous) {
-            // the other node's viscous term (def_par:13432-13433); with SA
-            // the viscosity is mu + nu~/Re
-            int j = t.y;
-            double vis = dmax(P.am, P.sa ? L.mu[j] + L.u[5 * N + j] / P.Re : L.mu[j]);
-            double dv = 2.0 * vis * al / L.u[j];
-            h = h + dv;
-        }
-    }
-    auto bterms = [&](int k, double *v) {
-        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
-        int2 nd = L.bedge[b];
-        double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
-        double al = (wx * wx + wy * wy) + wz * wz;
-        int j1 = nd.x, j2 = nd.y;
-        double ro1 = 1. / L.u[j1], ro2 = 1. / L.u[j2];
-        double cc1 = dmax(c1 * L.p[j1] * ro1, 0.001);
-        double cc2 = dmax(c1 * L.p[j2] * ro2, 0.001);
-        double vn1 = ((wx * L.u[N + j1] + wy * L.u[2 * N + j1]) + wz * L.u[3 * N + j1]) * ro1;
-        double vn2 = ((wx * L.u[N + j2] + wy * L.u[2 * N + j2]) + wz * L.u[3 * N + j2]) * ro2;
-        vn1 = fabs(vn1); vn2 = fabs(vn2);
-        cc1 = sqrt(cc1 * al); cc2 = sqrt(cc2 * al);
-        v[0] = side == 0 ? vn1 : vn2;
-        v[1] = vn1 + vn2;
-        v[2] = side == 0 ? cc1 : cc2;
-        v[3] = cc1 + cc2;
-        if (P.viscous) {
-            double vis1 = dmax(P.am, P.sa ? L.mu[j1] + L.u[5 * N + j1] / P.Re : L.mu[j1]);
-            double vis2 = dmax(P.am, P.sa ? L.mu[j2] + L.u[5 * N + j2] / P.Re : L.mu[j2]);
-            double dv1 = 2.0 * vis1 * al / L.u[j1];
-            double dv2 = 2.0 * vis2 * al / L.u[j2];
-            v[4] = side == 0 ? dv1 : dv2;
-            v[5] = dv1 + dv2;
-        } else {
-            v[4] = v[5] = 0.0;
-        }
-    };
-    auto badd = [&](const double *x) {
-        acc = (((acc + x[0]) + x[1]) + x[2]) + x[3];
-        if (P.viscous) h = (h + x[4]) + x[5];
-    };
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) ts_inc(P, L, L.inc[k], m1, m2, m3, ro, cc, acc, h);
+    auto bterms = [&](int k, double *v) { ts_bterms(P, L, k, v); };
+    auto badd = [&](const double *x) { ts_badd(P, x, acc, h); };
     if constexpr (U > 1) {
         group_gather<U, 6, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, badd);
         if (!active || gl) return;
-    } else
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-        double v[6];
-        bterms(k, v);
-        badd(v);
+        ts_store(L, i, acc, h);
+    } else {
+        ts_finish(P, L, i, acc, h);
     }
-    const double V = L.V[i];
-    const double dt = 0.5 / (acc / V + h / (V * V));
-    L.dt[i] = dt;
-    L.vdt[i] = V / dt;  // V/dt of the dissipation coefficient d0
 }
 
 // ---- makeArtificialDissipation2, passes 1-2 and the node finish -----------
 // (def_par:11513-11780): undivided Laplacian with dE+dp, pressure sensor
+struct LapAcc {
+    double l[5], s7, s8;
+};
+// interior edge t of node i (state ui, pressure pi)
+__device__ __forceinline__ void lap_inc(const Params &P, const LevelView &L, int2 t, const double *ui, double pi,
+                                        LapAcc &a) {
+    const int N = L.N;
+    const int j = t.y;
+    double df = 1.0;
+    if (P.useDissW) df = 1. / L.slen[t.x >= 0 ? t.x : ~t.x];
+    const double uj[5] = {L.u[j], L.u[N + j], L.u[2 * N + j], L.u[3 * N + j], L.u[4 * N + j]};
+    const double pj = L.p[j];
+    if (t.x >= 0) {  // this node is i1: d = u(i) - u(j)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a.l[c] = a.l[c] - (ui[c] - uj[c]) * df;
+        const double d4 = ((ui[4] - uj[4]) + pi) - pj;
+        a.l[4] = a.l[4] - d4 * df;
+        const double dp = pi - pj, sp = pi + pj;
+        a.s7 = a.s7 - dp; a.s8 = a.s8 + sp;
+    } else {         // i2: d = u(j) - u(i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a.l[c] = a.l[c] + (uj[c] - ui[c]) * df;
+        const double d4 = ((uj[4] - ui[4]) + pj) - pi;
+        a.l[4] = a.l[4] + d4 * df;
+        const double dp = pj - pi, sp = pj + pi;
+        a.s7 = a.s7 + dp; a.s8 = a.s8 + sp;
+    }
+}
+__device__ __forceinline__ void lap_store(const LevelView &L, int i, const LapAcc &a) {
+    const int N = L.N;
+    const double fact = 1. / L.conn[i];
+    L.sens[i] = 12. * fabs(a.s7 / a.s8);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) L.lap[c * N + i] = fact * a.l[c];
+}
+
 template <int U>
 __global__ void k_jst_lap(Params P, LevelView L) {
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -206,38 +265,46 @@ __global__ void k_jst_lap(Params P, LevelView L) {
             s7 = s7 + x[5]; s8 = s8 + x[6];
             });
         if (!active || gl) return;
-    } else
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-        int2 t = L.inc[k];
-        int j = t.y;
-        double df = 1.0;
-        if (P.useDissW) df = 1. / L.slen[t.x >= 0 ? t.x : ~t.x];
-        double uj0 = L.u[j], uj1 = L.u[N + j], uj2 = L.u[2 * N + j], uj3 = L.u[3 * N + j], uj4 = L.u[4 * N + j];
-        double pj = L.p[j];
-        if (t.x >= 0) {  // this node is i1: d = u(i) - u(j)
-            double d0 = ui0 - uj0, d1 = ui1 - uj1, d2 = ui2 - uj2, d3 = ui3 - uj3;
-            double d4 = ((ui4 - uj4) + pi) - pj;
-            l0 = l0 - d0 * df; l1 = l1 - d1 * df; l2 = l2 - d2 * df; l3 = l3 - d3 * df; l4 = l4 - d4 * df;
-            double dp = pi - pj, sp = pi + pj;
-            s7 = s7 - dp; s8 = s8 + sp;
-        } else {          // i2: d = u(j) - u(i)
-            double d0 = uj0 - ui0, d1 = uj1 - ui1, d2 = uj2 - ui2, d3 = uj3 - ui3;
-            double d4 = ((uj4 - ui4) + pj) - pi;
-            l0 = l0 + d0 * df; l1 = l1 + d1 * df; l2 = l2 + d2 * df; l3 = l3 + d3 * df; l4 = l4 + d4 * df;
-            double dp = pj - pi, sp = pj + pi;
-            s7 = s7 + dp; s8 = s8 + sp;
-        }
+    } else {
+        LapAcc a = {{0, 0, 0, 0, 0}, 0, 0};
+        const double ui[5] = {ui0, ui1, ui2, ui3, ui4};
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) lap_inc(P, L, L.inc[k], ui, pi, a);
+        lap_store(L, i, a);
+        return;
     }
-    double fact = 1. / L.conn[i];
-    L.sens[i] = 12. * fabs(s7 / s8);
-    L.lap[i] = fact * l0;
-    L.lap[N + i] = fact * l1;
-    L.lap[2 * N + i] = fact * l2;
-    L.lap[3 * N + i] = fact * l3;
-    L.lap[4 * N + i] = fact * l4;
+    LapAcc a = {{l0, l1, l2, l3, l4}, s7, s8};
+    lap_store(L, i, a);
 }
 
 // ---- makeArtificialDissipation2, pass 3 (def_par:11770-11906), scalar -----
+// interior edge t of node i (Laplacian Li, state Ui, V/dt vdi, connectivity
+// coni, sensor si): the fourth- and second-order terms with the sign of
+// this node
+__device__ __forceinline__ void jflux_inc(const Params &P, const LevelView &L, int2 t, double k4, double vdi,
+                                          double coni, double si, const double *Li, const double *Ui, double *acc) {
+    const int N = L.N;
+    const int j = t.y;
+    const double vdj = L.vdt[j];
+    const bool first = t.x >= 0;
+    double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
+    d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
+    const double sj = L.sens[j];
+    const double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
+    double d4 = d0 * k4;
+    d4 = d4 > d2 ? d4 - d2 : 0.0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const double Lj = L.lap[c * N + j], Uj = L.u[c * N + j];
+        if (first) {
+            const double d4v = Li[c] - Lj, d2v = Ui[c] - Uj;
+            acc[c] = (acc[c] - d4v * d4) + d2v * d2;
+        } else {
+            const double d4v = Lj - Li[c], d2v = Uj - Ui[c];
+            acc[c] = (acc[c] + d4v * d4) - d2v * d2;
+        }
+    }
+}
+
 template <int U>
 __global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P, LevelView L) {
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -282,28 +349,7 @@ __global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P, Leve
             });
         if (!active || gl) return;
     } else
-    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-        int2 t = L.inc[k];
-        int j = t.y;
-        double vdj = L.vdt[j];
-        const bool first = t.x >= 0;
-        double d0 = first ? dmin(vdi, vdj) : dmin(vdj, vdi);
-        d0 = d0 / (first ? (coni + L.conn[j]) : (L.conn[j] + coni));
-        double sj = L.sens[j];
-        double d2 = d0 * P.k2 * (first ? dmax(si, sj) : dmax(sj, si));
-        double d4 = d0 * k4;
-        d4 = d4 > d2 ? d4 - d2 : 0.0;
-        for (int c = 0; c < 5; ++c) {
-            double Lj = L.lap[c * N + j], Uj = L.u[c * N + j];
-            if (first) {
-                double d4v = Li[c] - Lj, d2v = Ui[c] - Uj;
-                acc[c] = (acc[c] - d4v * d4) + d2v * d2;
-            } else {
-                double d4v = Lj - Li[c], d2v = Uj - Ui[c];
-                acc[c] = (acc[c] + d4v * d4) - d2v * d2;
-            }
-        }
-    }
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) jflux_inc(P, L, L.inc[k], k4, vdi, coni, si, Li, Ui, acc);
     for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
 }
 
@@ -596,6 +642,31 @@ __device__ __forceinline__ void visc_grad_finish(const Params &P, const LevelVie
     for (int c = 0; c < 9; ++c) L.tau[c * N + i] = tau[c];
 }
 
+// interior edge t of node i (u, v, w, T of the node qi): the edge's terms
+// of the 12 gradient sums, added with the sign of this node
+__device__ __forceinline__ void vgrad_inc(const LevelView &L, int2 t, const double *qi, double *g) {
+    const int N = L.N;
+    const int e = t.x >= 0 ? t.x : ~t.x, j = t.y;
+    const double qj[4] = {L.prim[j], L.prim[N + j], L.prim[2 * N + j], L.prim[3 * N + j]};
+    const double w[3] = {L.wx[e], L.wy[e], L.wz[e]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double x = (t.x >= 0 ? qi[c] + qj[c] : qj[c] + qi[c]) * w[a];
+            g[a * 4 + c] = t.x >= 0 ? g[a * 4 + c] + x : g[a * 4 + c] - x;
+        }
+}
+// the boundary edges of node i in order
+__device__ __forceinline__ void visc_grad_boundary(const LevelView &L, int i, double *g) {
+    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+        double v[12];
+        visc_grad_bterms(L, k, v);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) g[c] = g[c] + v[c];
+    }
+}
+
 template <int U>
 __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, LevelView L) {
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -632,16 +703,8 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, Lev
         group_gather<U, 12, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, bterms, add);
         if (!active || gl) return;
     } else {
-        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
-            double v[12];
-            iterms(k, v);
-            add(v);
-        }
-        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-            double v[12];
-            bterms(k, v);
-            add(v);
-        }
+        for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) vgrad_inc(L, L.inc[k], qi, g);
+        visc_grad_boundary(L, i, g);
     }
     visc_grad_finish(P, L, i, g);
 }
@@ -760,6 +823,61 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, Lev
         }
     }
     for (int c = 0; c < 4; ++c) L.diss[(1 + c) * N + i] = L.diss[(1 + c) * N + i] - acc[c];
+}
+
+// ---- fused walks of one incidence list (thread per node) -------------------
+// Gathers that read the same neighbours and write disjoint arrays share one
+// walk of the node's incidence list: the incidences, their edges and the
+// neighbours' state are read once for both.  Each sum keeps its own
+// accumulators and its own order, so the results are those of the separate
+// kernels bit for bit.
+//
+// makeTimeSteps with passes 1-2 of makeArtificialDissipation2: the time
+// step reads mu of the neighbours (the previous viscous pass) and writes dt
+// and V/dt; the Laplacian reads u and p and writes the Laplacian and sensor
+__global__ void __launch_bounds__(256, 3) k_ts_lap(Params P, LevelView L) {
+    const int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double ui[5] = {L.u[i], L.u[N + i], L.u[2 * N + i], L.u[3 * N + i], L.u[4 * N + i]};
+    const double pi = L.p[i];
+    const double ro = 1. / ui[0];
+    const double cc = dmax(P.gamma * pi * ro, 0.001);
+    double acc = 0.0, h = 0.0;
+    LapAcc a = {{0, 0, 0, 0, 0}, 0, 0};
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        ts_inc(P, L, t, ui[1], ui[2], ui[3], ro, cc, acc, h);
+        lap_inc(P, L, t, ui, pi, a);
+    }
+    lap_store(L, i, a);
+    ts_finish(P, L, i, acc, h);
+}
+
+// pass 3 of makeArtificialDissipation2 (scalar) with pass 1 of
+// makeViscosityTerm: the JST terms read the Laplacian, sensor, V/dt and u of
+// the neighbours and write the dissipation; the gradients read u, v, w, T
+// and write mu, the stress tensor and the wall stress
+__global__ void __launch_bounds__(256, 2) k_jflux_vgrad(Params P, LevelView L) {
+    const int i = tid();
+    if (i >= L.N) return;
+    const int N = L.N;
+    const double k4 = L.grid == 1 ? P.k4 : P.cgdf;
+    double acc[5] = {0, 0, 0, 0, 0};
+    double Li[5], Ui[5];
+    for (int c = 0; c < 5; ++c) { Li[c] = L.lap[c * N + i]; Ui[c] = L.u[c * N + i]; }
+    const double vdi = L.vdt[i], coni = L.conn[i], si = L.sens[i];
+    const double qi[4] = {L.prim[i], L.prim[N + i], L.prim[2 * N + i], L.prim[3 * N + i]};
+    double g[12];
+    for (int c = 0; c < 12; ++c) g[c] = 0.0;
+    for (int k = L.inc_ptr[i]; k < L.inc_ptr[i + 1]; ++k) {
+        const int2 t = L.inc[k];
+        jflux_inc(P, L, t, k4, vdi, coni, si, Li, Ui, acc);
+        vgrad_inc(L, t, qi, g);
+    }
+    for (int c = 0; c < 5; ++c) L.diss[c * N + i] = acc[c];
+    visc_grad_boundary(L, i, g);
+    visc_grad_finish(P, L, i, g);
 }
 
 // ---- makeViscosityTerm2, the compact stencil (def_par:5896-6807) ---------
@@ -1808,32 +1926,7 @@ __global__ void __launch_bounds__(kTile, 3) k_timestep_tiled(Params P, LevelView
             h = h + dv;
         }
     });
-    for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-        int b = L.binc[k] >> 1, side = L.binc[k] & 1;
-        int2 nd = L.bedge[b];
-        double wx = L.bwx[b], wy = L.bwy[b], wz = L.bwz[b];
-        double al = (wx * wx + wy * wy) + wz * wz;
-        int j1 = nd.x, j2 = nd.y;
-        double ro1 = 1. / L.u[j1], ro2 = 1. / L.u[j2];
-        double cc1 = dmax(c1 * L.p[j1] * ro1, 0.001);
-        double cc2 = dmax(c1 * L.p[j2] * ro2, 0.001);
-        double vn1 = ((wx * L.u[N + j1] + wy * L.u[2 * N + j1]) + wz * L.u[3 * N + j1]) * ro1;
-        double vn2 = ((wx * L.u[N + j2] + wy * L.u[2 * N + j2]) + wz * L.u[3 * N + j2]) * ro2;
-        vn1 = fabs(vn1); vn2 = fabs(vn2);
-        cc1 = sqrt(cc1 * al); cc2 = sqrt(cc2 * al);
-        acc = (((acc + (side == 0 ? vn1 : vn2)) + (vn1 + vn2)) + (side == 0 ? cc1 : cc2)) + (cc1 + cc2);
-        if (P.viscous) {
-            double vis1 = dmax(P.am, P.sa ? L.mu[j1] + L.u[5 * N + j1] / P.Re : L.mu[j1]);
-            double vis2 = dmax(P.am, P.sa ? L.mu[j2] + L.u[5 * N + j2] / P.Re : L.mu[j2]);
-            double dv1 = 2.0 * vis1 * al / L.u[j1];
-            double dv2 = 2.0 * vis2 * al / L.u[j2];
-            h = (h + (side == 0 ? dv1 : dv2)) + (dv1 + dv2);
-        }
-    }
-    const double V = L.V[i];
-    const double dt = 0.5 / (acc / V + h / (V * V));
-    L.dt[i] = dt;
-    L.vdt[i] = V / dt;
+    ts_finish(P, L, i, acc, h);
 }
 
 // makeArtificialDissipation2 passes 1-2 (no dissipation weighting): the

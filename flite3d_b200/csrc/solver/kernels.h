@@ -20,6 +20,8 @@ template <int U>
 __global__ void k_visc_grad(Params P, LevelView L);
 template <int U>
 __global__ void k_visc_flux(Params P, LevelView L);
+__global__ void k_ts_lap(Params P, LevelView L);
+__global__ void k_jflux_vgrad(Params P, LevelView L);
 template <int U>
 __global__ void k_visc2_grad(Params P, LevelView L);
 template <int U>

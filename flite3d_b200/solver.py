@@ -302,12 +302,19 @@ class Solver:
         (1, 2) or not (3, 4).  No effect on any result."""
         self._ck(self.be.set_tiled_gather(self._h, level, mode), "set_tiled_gather")
 
+    def set_gather_fusion(self, level, on=1):
+        """Whether a level's gathers that walk the same incidence list share
+        one walk (time step with Laplacian, JST flux with viscous gradients)
+        where a thread serves a node: 1 (default) or 0.  No effect on any
+        result."""
+        self._ck(self.be.set_gather_fusion(self._h, level, on), "set_gather_fusion")
+
     def set_gather_lanes(self, level, lanes):
         """Lanes per node of a level's gathers: 1, 4, 8, 16, 32 (0: default)."""
         self._ck(self.be.set_gather_lanes(self._h, level, lanes), "set_gather_lanes")
 
     KERNEL_GROUPS = ("pressure", "timestep", "dissipation", "visc_prim", "visc_grad", "visc_flux",
-                     "flux_terms", "node_update")
+                     "flux_terms", "node_update", "ts_lap", "jflux_vgrad")
 
     def profile_kernels(self, level=1, reps=10):
         """{kernel group: average device ms} over one relaxation step of a level."""

@@ -363,12 +363,20 @@ int flite_set_gather_lanes(flite_ctx *ctx, int32_t level, int32_t lanes);
  * per SM, 2: three) or read from global memory (3: two, 4: three).  No
  * effect on any result.  Drops the captured cycle graph.                   */
 int flite_set_tiled_gather(flite_ctx *ctx, int32_t level, int32_t on);
+/* Whether a level's node gathers that walk the same incidence list share one
+ * walk where a thread serves a node and the list form is used: the time step
+ * with the JST Laplacian, and the JST flux with the viscous gradients.  1 (the
+ * default) shares, 0 runs them as separate kernels.  No effect on any result.
+ * Drops the captured cycle graph.                                           */
+int flite_set_gather_fusion(flite_ctx *ctx, int32_t level, int32_t on);
 /* Average device ms of the kernel groups of one relaxation step of a level,
  * in order: pressure, time steps, dissipation, viscous primitives, viscous
  * gradients, viscous fluxes, flux terms (edge or boundary kernels), node
- * update (restrictGrid's fine-increment mode: the stage's read set); *n is
- * the number written (at most nmax).  The level's rhs and dissipation are
- * overwritten.                                                              */
+ * update (restrictGrid's fine-increment mode: the stage's read set), the
+ * shared walk of time step and Laplacian, the shared walk of JST flux and
+ * viscous gradients (where the walks are shared, the separate groups hold
+ * what is left of them); *n is the number written (at most nmax).  The
+ * level's rhs and dissipation are overwritten.                              */
 int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32_t nmax, int32_t *n);
 
 #ifdef __cplusplus

@@ -251,6 +251,26 @@ def test_tiled_gather_modes_match(name, mode, order):
     assert np.array_equal(g.residual_fwd(g.get_state(1)), o.residual_fwd(o.get_state(1)))
 
 
+@pytest.mark.parametrize("fuse", [0, 1])
+@pytest.mark.parametrize("name", ["central_jst", "laminar_adiabatic", "laminar_isothermal", "fv_boundary_term",
+                                  "dissipation_weighting", "matrix_dissipation", "laminar_matrix_dissipation",
+                                  "laminar_visc2_adiabatic", "first_order_diss", "relax_steps2"])
+def test_gather_fusion_matches(name, fuse):
+    # a thread per node on every level, the gathers that walk the same
+    # incidence list sharing one walk (k_ts_lap, k_jflux_vgrad) or not
+    mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+    c, g, o = make_pair(mesh, **CASES[name])
+    for level in (1, 2, 3):
+        g.set_gather_lanes(level, 1)
+        g.set_gather_fusion(level, fuse)
+    for cyc in range(1, 4):
+        g.cycle(cyc)
+        o.cycle(cyc)
+    assert_same_state(g, o, f"{name} fusion {fuse}")
+    groups = g.profile_kernels(1, reps=1)
+    assert set(groups) == set(Solver.KERNEL_GROUPS)
+
+
 def test_node_order_changes_no_result():
     # the device's locality numbering against the caller's: the same states,
     # pressures, residual maxima and their (caller-numbered) nodes
