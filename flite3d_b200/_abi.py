@@ -77,6 +77,7 @@ class LevelDesc(ctypes.Structure):
         ("side_idx", _P), ("side_w", _P), ("side_len", _P), ("bnd_idx", _P), ("bnd_w", _P),
         ("node_reg", _P), ("node_ind", _P), ("volume", _P), ("wall_dist", _P), ("coords", _P),
         ("coord_move", _P), ("parent", _P), ("rweight", _P),
+        ("side_gcl", _P), ("bnd_gcl", _P), ("volume_prev", _P), ("volume_prev2", _P),
     ]
 
 
@@ -90,7 +91,7 @@ GPU_SYMBOLS = [
     "flite_batch_cycle", "flite_batch_run", "flite_batch_time_cycles", "flite_batch_autotune", "flite_batch_set_blocks",
     "flite_residual_vjp", "flite_profile_adjoint", "flite_profile_kernels", "flite_set_kernel_options", "flite_set_gather_lanes",
     "flite_iteration_vjp", "flite_adjoint_solve", "flite_objective", "flite_set_adjoint_method",
-    "flite_next_physical_step", "flite_set_node_order", "flite_set_tiled_gather", "flite_set_gather_fusion",
+    "flite_next_physical_step", "flite_set_node_order", "flite_set_tiled_gather", "flite_set_gather_fusion", "flite_update_geometry",
 ]
 
 PREPRO_SYMBOLS = [
@@ -98,7 +99,7 @@ PREPRO_SYMBOLS = [
     "fp_node_perm", "fp_check", "fp_geometry", "fp_geometry_vjp", "fp_write_sol", "fp_read_sol", "fp_write_rst", "fp_read_rst",
     "fp_write_res", "fp_write_unk", "fp_read_unk", "fp_write_plotreg", "fp_makeplot", "fp_write_plt",
     "fp_read_inp", "fp_parse_inp_text", "fp_rsd_line", "fp_append_rsd", "fp_cycle_line",
-    "fp_controls_default", "fp_controls_derive",
+    "fp_controls_default", "fp_controls_derive", "fp_set_moving_geometry", "fp_coordinate_movement", "fp_gcl_check",
 ]
 
 _libs = {}

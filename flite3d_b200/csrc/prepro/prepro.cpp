@@ -62,6 +62,19 @@ struct LevelData {
     std::vector<int32_t> seed;    // [N] (coarse levels)
     std::vector<int32_t> parent;  // [N_finer] (coarse levels)
     std::vector<double> rweight;  // [N_finer]
+    // moving meshes (fp_set_moving_geometry): the GCL weights of the step and
+    // of the step before, the volumes at the two previous steps and the
+    // coordinate movement (level 1)
+    std::vector<double> gcl;         // [2][E]
+    std::vector<double> bgcl;        // [4][B] (GCL(1), GCL(2), GCLP(1), GCLP(2))
+    std::vector<double> volp, volp2;  // [N]
+    std::vector<double> cmove;       // [3][N]
+    std::vector<double> xyzp, xyzp2;  // [3][N] coordinates at the two previous steps
+    // coarse levels: the coarse side of each finer side (1-based, negative
+    // where the finer side runs the other way, 0 inside an aggregate) and
+    // the coarse boundary side of each finer one (negative where its two
+    // nodes swap)
+    std::vector<int32_t> side_of, bside_of;
 };
 
 }  // namespace
@@ -247,6 +260,110 @@ void tri_sides(const V3T<S> *x, TriSide<S> *out) {
     out[0] = {0, 1, scl(0.25, halfcross(xm - x1, xb1 - x1))};
     out[1] = {0, 2, scl(0.25, halfcross(xb3 - x1, xm - x1))};
     out[2] = {1, 2, scl(0.25, halfcross(xm - x2, xb2 - x2))};
+}
+
+// ---- moving meshes: three time levels (t = 0 the step, 1 and 2 the two
+// before), as makeCalcDataForTet and makeCalcDataForBoundary receive them
+// from crp, crpPrev and crpPrev2 ---------------------------------------------
+inline double dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+// the quarter cross product of the mixed time levels (Cyy of
+// registerSideGCL, gen3d_grid.f90:806-818)
+inline V3 qcross(V3 a, V3 b) {
+    return {0.25 * (a.y * b.z - a.z * b.y), 0.25 * (a.z * b.x - a.x * b.z), 0.25 * (a.x * b.y - a.y * b.x)};
+}
+// the displacement of a dual-face triangle's centroid between levels k and
+// k+1: ((p - p') + (q - q') + (r - r')) / 3 in the reference's order
+inline V3 sweep(const V3 *p, const V3 *q, const V3 *r, int k) {
+    return div3((((((p[k] - p[k + 1]) + q[k]) - q[k + 1]) + r[k]) - r[k + 1]));
+}
+
+// A tetrahedron side at three time levels (registerSideGCL, gen3d_grid.f90:
+// 786-855): half the side coefficient at t = 0, the nodal-volume share at
+// each level, and GCL(1) (levels 0-1) and GCL(2) (levels 1-2), the volumes
+// its two dual-face triangles sweep
+struct TetSideMoving { int a, b; V3 coef; double nv[3], gcl[2]; };
+void tet_sides_moving(const V3 (*x)[4], TetSideMoving *out) {
+    V3 xmm[3];
+    for (int t = 0; t < 3; ++t) xmm[t] = scl(0.25, x[t][0] + x[t][1] + x[t][2] + x[t][3]);
+    int n = 0;
+    // side a-b with the dual-face points xm (edge midpoint), P1 and P2 (face
+    // centroids): r1 = xmm - xm, r2 = P1 - xm, r3 = P2 - xm, r4 = xmm - xm
+    auto side = [&](int a, int b, const V3 *xm, const V3 *P1, const V3 *P2) {
+        V3 r1[3], r2[3], r3[3], r4[3], rv[3], c1[3], c2[3];
+        for (int t = 0; t < 3; ++t) {
+            r1[t] = xmm[t] - xm[t]; r2[t] = P1[t] - xm[t]; r3[t] = P2[t] - xm[t]; r4[t] = xmm[t] - xm[t];
+            rv[t] = xm[t] - x[t][a];
+            c1[t] = halfcross(r1[t], r2[t]);
+            c2[t] = halfcross(r3[t], r4[t]);
+        }
+        TetSideMoving &o = out[n++];
+        o.a = a; o.b = b;
+        for (int t = 0; t < 3; ++t) {
+            const V3 cxx = c1[t] + c2[t];
+            o.nv[t] = (rv[t].x * cxx.x + rv[t].y * cxx.y + rv[t].z * cxx.z) / 3.;
+            if (t == 0) o.coef = scl(0.5, cxx);
+        }
+        for (int k = 0; k < 2; ++k) {
+            const V3 vr1 = sweep(xm, xmm, P1, k), vr2 = sweep(xm, P2, xmm, k);
+            const V3 y1 = qcross(r1[k], r2[k + 1]) + qcross(r1[k + 1], r2[k]);
+            const V3 y2 = qcross(r3[k], r4[k + 1]) + qcross(r3[k + 1], r4[k]);
+            o.gcl[k] = (dot3((c1[k] + y1) + c1[k + 1], vr1) + dot3((c2[k] + y2) + c2[k + 1], vr2)) / 3.;
+        }
+    };
+    V3 xm1[3], xm2[3], xm3[3], xb1[3], xb2[3], xb3[3];
+    auto pts = [&](int i, int j, V3 *o) { for (int t = 0; t < 3; ++t) o[t] = scl(0.5, x[t][i] + x[t][j]); };
+    auto ctr = [&](int i, int j, int k, V3 *o) { for (int t = 0; t < 3; ++t) o[t] = div3(x[t][i] + x[t][j] + x[t][k]); };
+    // node 1
+    pts(0, 1, xm1); pts(0, 2, xm2); pts(0, 3, xm3);
+    ctr(0, 1, 2, xb1); ctr(0, 1, 3, xb2); ctr(0, 2, 3, xb3);
+    side(0, 1, xm1, xb2, xb1);
+    side(0, 2, xm2, xb1, xb3);
+    side(0, 3, xm3, xb3, xb2);
+    // node 2
+    pts(1, 2, xm1); pts(1, 3, xm2);
+    ctr(0, 1, 2, xb1); ctr(1, 2, 3, xb2); ctr(0, 1, 3, xb3);
+    side(1, 2, xm1, xb2, xb1);
+    side(1, 3, xm2, xb3, xb2);
+    // node 3
+    pts(2, 3, xm1);
+    ctr(0, 2, 3, xb1); ctr(1, 2, 3, xb2);
+    side(2, 3, xm1, xb2, xb1);
+}
+
+// A boundary triangle side at three time levels (registerBoundarySideGCL,
+// gen3d_boundary.f90:289-372, from makeCalcDataForBoundary :511-620): the
+// quarter coefficient at t = 0 and, for its first and second vertex,
+// GCL(1 or 2, 1) (levels 0-1) and GCL(1 or 2, 2) (levels 1-2)
+struct TriSideMoving { int a, b; V3 coef; double gcl[2][2]; };
+void tri_sides_moving(const V3 (*x)[3], TriSideMoving *out) {
+    V3 xm[3], xb[3][3];
+    for (int t = 0; t < 3; ++t) {
+        xm[t] = div3(x[t][0] + x[t][1] + x[t][2]);
+        xb[0][t] = scl(0.5, x[t][0] + x[t][1]);
+        xb[1][t] = scl(0.5, x[t][1] + x[t][2]);
+        xb[2][t] = scl(0.5, x[t][2] + x[t][0]);
+    }
+    // side a-b through the edge midpoint mid, r1 = A - x_a, r2 = B - x_a
+    auto side = [&](TriSideMoving &o, int a, int b, const V3 *A, const V3 *B, const V3 *mid) {
+        V3 r1[3], r2[3], cxx[3], xa[3], xbv[3];
+        for (int t = 0; t < 3; ++t) {
+            r1[t] = A[t] - x[t][a]; r2[t] = B[t] - x[t][a];
+            cxx[t] = halfcross(r1[t], r2[t]);
+            xa[t] = x[t][a]; xbv[t] = x[t][b];
+        }
+        o.a = a; o.b = b;
+        o.coef = scl(0.25, cxx[0]);
+        for (int k = 0; k < 2; ++k) {
+            const V3 vr1 = sweep(xa, xm, mid, k), vr2 = sweep(xbv, xm, mid, k);
+            const V3 y = qcross(r1[k], r2[k + 1]) + qcross(r1[k + 1], r2[k]);
+            const V3 s = (cxx[k] + y) + cxx[k + 1];
+            o.gcl[0][k] = dot3(s, vr1) / 3.;
+            o.gcl[1][k] = dot3(s, vr2) / 3.;
+        }
+    };
+    side(out[0], 0, 1, xm, xb[0], xb[0]);
+    side(out[1], 0, 2, xb[2], xm, xb[2]);
+    side(out[2], 1, 2, xm, xb[1], xb[1]);
 }
 
 // Indicator priority of setBoundIndForViscousMesh (gen3d_boundary.f90:
@@ -679,6 +796,7 @@ void agglomerate(const LevelData &F, LevelData &C) {
     // coarse edges (createSides)
     PairMap smap((size_t)E / 4 + 16);
     std::vector<int32_t> s1, s2; std::vector<V3> sc; std::vector<double> sl;
+    C.side_of.assign(E, 0);
     for (int32_t e = 0; e < E; ++e) {
         int32_t c1 = C.parent[F.side[e] - 1], c2 = C.parent[F.side[(size_t)E + e] - 1];
         if (c1 == c2) continue;
@@ -686,6 +804,8 @@ void agglomerate(const LevelData &F, LevelData &C) {
         int32_t i1 = std::min(c1, c2), i2 = c1 + c2 - i1;
         if (i1 != c1) w = scl(-1.0, w);
         int64_t slot = smap.find_or_insert(pkey(i1, i2), (int64_t)s1.size());
+        const int32_t id = slot < 0 ? (int32_t)s1.size() : (int32_t)slot;
+        C.side_of[e] = i1 != c1 ? -(id + 1) : id + 1;
         if (slot < 0) { s1.push_back(i1); s2.push_back(i2); sc.push_back(w); sl.push_back(F.slen[e]); }
         else sc[slot] = sc[slot] + w;
     }
@@ -698,11 +818,14 @@ void agglomerate(const LevelData &F, LevelData &C) {
     // coarse boundary edges (agglomerateBoundary): self-edges are kept
     PairMap bmap((size_t)F.B + 16);
     std::vector<int32_t> b1, b2, bi; std::vector<V3> bc;
+    C.bside_of.assign(F.B, 0);
     for (int32_t b = 0; b < F.B; ++b) {
         int32_t c1 = C.parent[F.bside[b] - 1], c2 = C.parent[F.bside[(size_t)F.B + b] - 1];
         int32_t i1 = std::min(c1, c2), i2 = std::max(c1, c2);
         V3 w = {F.bw[b], F.bw[(size_t)F.B + b], F.bw[2 * (size_t)F.B + b]};
         int64_t slot = bmap.find_or_insert(pkey(i1, i2), (int64_t)b1.size());
+        const int32_t id = slot < 0 ? (int32_t)b1.size() : (int32_t)slot;
+        C.bside_of[b] = c1 > c2 ? -(id + 1) : id + 1;
         if (slot < 0) { b1.push_back(i1); b2.push_back(i2); bi.push_back(F.bside[2 * (size_t)F.B + b]); bc.push_back(w); }
         else bc[slot] = bc[slot] + w;
     }
@@ -807,6 +930,64 @@ struct Geometry {
                 const int32_t b = bsides.find(std::min(p[ts[k].a], p[ts[k].b]), std::max(p[ts[k].a], p[ts[k].b]));
                 const V3 c = ts[k].coef;
                 bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
+            }
+        }
+    }
+    // The level-1 arrays of a moving mesh from the coordinates of the step
+    // and of the two before, x[0..2]: the coefficients at the step, the
+    // volumes at each level and the GCL weights of the step and of the one
+    // before, accumulated in the element order of eval with registerSideData's
+    // orientation rule (gen3d_struct.f90:381-396) and registerBoundarySideGCL's
+    // (gen3d_boundary.f90:316-362)
+    void eval_moving(const double *const x[3], double *sw, double *bw, double *vol, double *volp, double *volp2,
+                     double *gcl, double *bgcl) const {
+        const size_t E = L.E, B = L.B;
+        std::fill(sw, sw + 3 * E, 0.0);
+        std::fill(bw, bw + 3 * B, 0.0);
+        std::fill(gcl, gcl + 2 * E, 0.0);
+        std::fill(bgcl, bgcl + 4 * B, 0.0);
+        for (double *v : {vol, volp, volp2}) std::fill(v, v + L.N, 0.0);
+        for (int32_t t = 0; t < NT; ++t) {
+            int32_t p[4];
+            tet(t, p);
+            V3 xv[3][4];
+            for (int q = 0; q < 3; ++q)
+                for (int k = 0; k < 4; ++k) xv[q][k] = X(x[q], p[k]);
+            TetSideMoving ts[6];
+            tet_sides_moving(xv, ts);
+            for (int k = 0; k < 6; ++k) {
+                int32_t p1 = p[ts[k].a], p2 = p[ts[k].b];
+                vol[p1 - 1] += ts[k].nv[0]; vol[p2 - 1] += ts[k].nv[0];
+                volp[p1 - 1] += ts[k].nv[1]; volp[p2 - 1] += ts[k].nv[1];
+                volp2[p1 - 1] += ts[k].nv[2]; volp2[p2 - 1] += ts[k].nv[2];
+                V3 coef = ts[k].coef;
+                double g0 = 0.5 * ts[k].gcl[0], g1 = 0.5 * ts[k].gcl[1];
+                int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
+                if (i1 != p1) { coef = scl(-1.0, coef); g0 = -g0; g1 = -g1; }
+                const int32_t e = sides.find(i1, i2);
+                sw[e] = sw[e] + coef.x; sw[E + e] = sw[E + e] + coef.y; sw[2 * E + e] = sw[2 * E + e] + coef.z;
+                gcl[e] = gcl[e] + g0; gcl[E + e] = gcl[E + e] + g1;
+            }
+        }
+        for (int32_t f = 0; f < NF; ++f) {
+            int32_t p[3];
+            tri(f, p);
+            V3 xv[3][3];
+            for (int q = 0; q < 3; ++q)
+                for (int k = 0; k < 3; ++k) xv[q][k] = X(x[q], p[k]);
+            TriSideMoving ts[3];
+            tri_sides_moving(xv, ts);
+            for (int k = 0; k < 3; ++k) {
+                const int32_t pa = p[ts[k].a], pb = p[ts[k].b];
+                const int32_t b = bsides.find(std::min(pa, pb), std::max(pa, pb));
+                const V3 c = ts[k].coef;
+                bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
+                // the smaller node's weights first
+                const int s1 = pa < pb ? 0 : 1, s2 = 1 - s1;
+                bgcl[b] = bgcl[b] + 0.25 * ts[k].gcl[s1][0];
+                bgcl[B + b] = bgcl[B + b] + 0.25 * ts[k].gcl[s2][0];
+                bgcl[2 * B + b] = bgcl[2 * B + b] + 0.25 * ts[k].gcl[s1][1];
+                bgcl[3 * B + b] = bgcl[3 * B + b] + 0.25 * ts[k].gcl[s2][1];
             }
         }
     }
@@ -1101,7 +1282,11 @@ int fp_level_desc(const fp_mesh *m, int level, flite_level_desc *o) {
     o->node_reg = L.reg; o->node_ind = L.node_ind.data();
     o->volume = L.vol.data(); o->wall_dist = L.wdist.data();
     o->coords = L.xyz.empty() ? nullptr : L.xyz.data();
-    o->coord_move = nullptr;
+    o->coord_move = L.cmove.empty() ? nullptr : L.cmove.data();
+    o->side_gcl = L.gcl.empty() ? nullptr : L.gcl.data();
+    o->bnd_gcl = L.bgcl.empty() ? nullptr : L.bgcl.data();
+    o->volume_prev = L.volp.empty() || level > 1 ? nullptr : L.volp.data();
+    o->volume_prev2 = L.volp2.empty() || level > 1 ? nullptr : L.volp2.data();
     o->parent = L.parent.empty() ? nullptr : L.parent.data();
     o->rweight = L.rweight.empty() ? nullptr : L.rweight.data();
     return FLITE_OK;
@@ -1131,6 +1316,118 @@ int fp_geometry_vjp(const fp_mesh *m, const double *xyz, const double *side_w_ba
         G.vjp(xyz ? xyz : m->lv[0].xyz.data(), side_w_bar, bnd_w_bar, volume_bar, xyz_bar);
         return FLITE_OK;
     });
+}
+
+int fp_coordinate_movement(fp_mesh *m, int32_t time_scheme) {
+    if (!m || m->lv.empty() || (time_scheme != 1 && time_scheme != 2)) return FLITE_EINVAL;
+    LevelData &L = m->lv[0];
+    if (L.xyz.empty() || L.xyzp.size() != L.xyz.size() || L.xyzp2.size() != L.xyz.size()) return FLITE_EINVAL;
+    // readGridComputationData (def_par:13896-13900)
+    L.cmove.resize(L.xyz.size());
+    for (size_t k = 0; k < L.xyz.size(); ++k)
+        L.cmove[k] = time_scheme == 1 ? L.xyz[k] - L.xyzp[k]
+                                      : (1.5 * L.xyz[k] - 2.0 * L.xyzp[k]) + 0.5 * L.xyzp2[k];
+    return FLITE_OK;
+}
+
+int fp_set_moving_geometry(fp_mesh *m, const double *xyz, const double *xyz_prev, const double *xyz_prev2,
+                           int32_t time_scheme) {
+    if (!m || m->lv.empty() || m->tets.empty() || !xyz || !xyz_prev || !xyz_prev2 ||
+        (time_scheme != 1 && time_scheme != 2))
+        return FLITE_EINVAL;
+    return guarded([&] {
+        LevelData &L = m->lv[0];
+        const size_t N = L.N, E = L.E, B = L.B;
+        std::vector<double> sw(3 * E), bw(3 * B), vol(N), volp(N), volp2(N), gcl(2 * E), bgcl(4 * B);
+        {
+            Geometry G(*m);
+            const double *x[3] = {xyz, xyz_prev, xyz_prev2};
+            G.eval_moving(x, sw.data(), bw.data(), vol.data(), volp.data(), volp2.data(), gcl.data(), bgcl.data());
+        }
+        L.sw = std::move(sw); L.bw = std::move(bw); L.vol = std::move(vol);
+        L.volp = std::move(volp); L.volp2 = std::move(volp2); L.gcl = std::move(gcl); L.bgcl = std::move(bgcl);
+        L.xyz.assign(xyz, xyz + 3 * N);
+        L.xyzp.assign(xyz_prev, xyz_prev + 3 * N);
+        L.xyzp2.assign(xyz_prev2, xyz_prev2 + 3 * N);
+        // side lengths at the step's coordinates (registerSideGCL's
+        // sideLength; |x2 - x1| does not depend on the side's direction)
+        for (size_t e = 0; e < E; ++e) {
+            const int32_t a = L.side[e] - 1, b = L.side[E + e] - 1;
+            const double dx = L.xyz[b] - L.xyz[a], dy = L.xyz[N + b] - L.xyz[N + a];
+            const double dz = L.xyz[2 * N + b] - L.xyz[2 * N + a];
+            L.slen[e] = std::sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        int rc = fp_coordinate_movement(m, time_scheme);
+        if (rc != FLITE_OK) return rc;
+        // coarse levels: the finer level's arrays summed through the
+        // agglomeration, in the order agglomerate sums the static ones
+        for (size_t l = 1; l < m->lv.size(); ++l) {
+            const LevelData &F = m->lv[l - 1];
+            LevelData &C = m->lv[l];
+            const size_t Nf = F.N, Ef = F.E, Bf = F.B, Nc = C.N, Ec = C.E, Bc = C.B;
+            C.vol.assign(Nc, 0.0); C.volp.assign(Nc, 0.0); C.volp2.assign(Nc, 0.0);
+            for (size_t i = 0; i < Nf; ++i) {
+                const int32_t c = C.parent[i] - 1;
+                C.vol[c] += F.vol[i]; C.volp[c] += F.volp[i]; C.volp2[c] += F.volp2[i];
+            }
+            for (size_t i = 0; i < Nf; ++i) C.rweight[i] = F.vol[i] / C.vol[C.parent[i] - 1];
+            C.sw.assign(3 * Ec, 0.0); C.gcl.assign(2 * Ec, 0.0);
+            std::vector<char> seen(Ec, 0);
+            for (size_t e = 0; e < Ef; ++e) {
+                const int32_t so = C.side_of[e];
+                if (so == 0) continue;
+                const size_t id = (size_t)std::abs(so) - 1;
+                const double sg = so < 0 ? -1.0 : 1.0;
+                for (int k = 0; k < 3; ++k) C.sw[k * Ec + id] = C.sw[k * Ec + id] + sg * F.sw[k * Ef + e];
+                for (int k = 0; k < 2; ++k) C.gcl[k * Ec + id] = C.gcl[k * Ec + id] + sg * F.gcl[k * Ef + e];
+                if (!seen[id]) { seen[id] = 1; C.slen[id] = F.slen[e]; }
+            }
+            C.bw.assign(3 * Bc, 0.0); C.bgcl.assign(4 * Bc, 0.0);
+            for (size_t b = 0; b < Bf; ++b) {
+                const int32_t so = C.bside_of[b];
+                const size_t id = (size_t)std::abs(so) - 1;
+                for (int k = 0; k < 3; ++k) C.bw[k * Bc + id] = C.bw[k * Bc + id] + F.bw[k * Bf + b];
+                // the weights stay with their nodes when the coarse side's
+                // nodes come in the other order
+                const int sw1 = so < 0 ? 1 : 0;
+                const int from[4] = {sw1, 1 - sw1, 2 + sw1, 3 - sw1};
+                for (int k = 0; k < 4; ++k)
+                    C.bgcl[k * Bc + id] = C.bgcl[k * Bc + id] + F.bgcl[from[k] * Bf + b];
+            }
+        }
+        return FLITE_OK;
+    });
+}
+
+int fp_gcl_check(const fp_mesh *m, int level, int32_t time_scheme, double *err, double *scale) {
+    if (!m || level < 1 || level > (int)m->lv.size() || (time_scheme != 1 && time_scheme != 2) || !err || !scale)
+        return FLITE_EINVAL;
+    const LevelData &L = m->lv[level - 1];
+    if (L.gcl.empty() || L.volp.empty()) return FLITE_EINVAL;
+    const size_t N = L.N, E = L.E, B = L.B;
+    // the GCL weights as the solver's reader takes them (def_par:816-818,
+    // 13858-13860) and the sums of def_par:14590-14610
+    auto comb = [&](double g, double gp) { return time_scheme == 2 ? 1.5 * g - 0.5 * gp : g; };
+    std::vector<double> d(N, 0.0);
+    for (size_t e = 0; e < E; ++e) {
+        const double ww = comb(L.gcl[e], L.gcl[E + e]);
+        d[L.side[e] - 1] = d[L.side[e] - 1] + 2.0 * ww;
+        d[L.side[E + e] - 1] = d[L.side[E + e] - 1] - 2.0 * ww;
+    }
+    for (size_t b = 0; b < B; ++b) {
+        d[L.bside[b] - 1] = d[L.bside[b] - 1] + 4.0 * comb(L.bgcl[b], L.bgcl[2 * B + b]);
+        d[L.bside[B + b] - 1] = d[L.bside[B + b] - 1] + 4.0 * comb(L.bgcl[B + b], L.bgcl[3 * B + b]);
+    }
+    double e_max = 0, s_max = 0;
+    for (size_t i = 0; i < N; ++i) {
+        const double dv = time_scheme == 1 ? L.vol[i] - L.volp[i]
+                                           : (1.5 * L.vol[i] - 2.0 * L.volp[i]) + 0.5 * L.volp2[i];
+        e_max = std::max(e_max, std::fabs(d[i] - dv));
+        s_max = std::max(s_max, std::fabs(dv));
+    }
+    *err = e_max;
+    *scale = s_max;
+    return FLITE_OK;
 }
 
 int fp_check(const fp_mesh *m, int level, double *closure, double *volume) {
@@ -1179,7 +1476,12 @@ int fp_write_sol(const fp_mesh *m, const char *path) {
             for (int32_t b = 0; b < L.B; ++b) {
                 w.i4(L.bside[b]).i4(L.bside[(size_t)L.B + b]).i4(L.bside[2 * (size_t)L.B + b]);
                 w.r8(L.bw[b]).r8(L.bw[(size_t)L.B + b]).r8(L.bw[2 * (size_t)L.B + b]);
-                w.r8(0).r8(0).r8(0).r8(0).end();  // GCL(2), GCLprev(2): static mesh
+                if (L.bgcl.empty()) {
+                    w.r8(0).r8(0).r8(0).r8(0).end();  // GCL(2), GCLprev(2): static mesh
+                } else {
+                    for (int k = 0; k < 4; ++k) w.r8(L.bgcl[(size_t)k * L.B + b]);
+                    w.end();
+                }
             }
             const int32_t nn = (int32_t)L.node_ind.size();
             w.i4(L.Nb).i4(nn).end();
@@ -1193,15 +1495,22 @@ int fp_write_sol(const fp_mesh *m, const char *path) {
             for (int32_t e = 0; e < L.E; ++e) {
                 w.i4(L.side[e]).i4(L.side[(size_t)L.E + e]);
                 w.r8(L.sw[e]).r8(L.sw[(size_t)L.E + e]).r8(L.sw[2 * (size_t)L.E + e]);
-                w.r8(0).r8(0).r8(L.slen[e]).end();
+                if (L.gcl.empty()) w.r8(0).r8(0);
+                else w.r8(L.gcl[e]).r8(L.gcl[(size_t)L.E + e]);
+                w.r8(L.slen[e]).end();
             }
             // nodes
             w.i4(L.N).end();
             if (fine) {
                 for (int32_t i = 0; i < L.N; ++i) {
-                    double x = L.xyz[i], y = L.xyz[(size_t)L.N + i], z = L.xyz[2 * (size_t)L.N + i];
-                    w.i4(i + 1).r8(L.vol[i]).r8(L.vol[i]).r8(L.vol[i]).r8(L.wdist[i]).i4(L.wnode[i]);
-                    w.r8(x).r8(y).r8(z).r8(x).r8(y).r8(z).r8(x).r8(y).r8(z).end();
+                    // a static mesh's previous volumes and coordinates are its own
+                    const bool mv = !L.volp.empty() && !L.xyzp.empty();
+                    const std::vector<double> &xp = mv ? L.xyzp : L.xyz, &xp2 = mv ? L.xyzp2 : L.xyz;
+                    w.i4(i + 1).r8(L.vol[i]).r8(mv ? L.volp[i] : L.vol[i]).r8(mv ? L.volp2[i] : L.vol[i]);
+                    w.r8(L.wdist[i]).i4(L.wnode[i]);
+                    for (const std::vector<double> *x : {&L.xyz, &xp, &xp2})
+                        w.r8((*x)[i]).r8((*x)[(size_t)L.N + i]).r8((*x)[2 * (size_t)L.N + i]);
+                    w.end();
                 }
                 w.i4(0).end();  // trip nodes
                 w.i4(0).end();  // trip field nodes
@@ -1252,11 +1561,13 @@ int fp_read_sol(const char *path, fp_mesh **out) {
             const bool fine = l == 0;
             r.next(); L.B = r.i4();
             if (L.B < 0) throw fio::io_error("negative count");
-            L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B);
+            L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B); L.bgcl.assign(4 * (size_t)L.B, 0.0);
             for (int32_t b = 0; b < L.B; ++b) {
                 r.next();
                 for (int k = 0; k < 3; ++k) L.bside[(size_t)k * L.B + b] = r.i4();
                 for (int k = 0; k < 3; ++k) L.bw[(size_t)k * L.B + b] = r.r8();
+                if (r.remaining() >= 32)
+                    for (int k = 0; k < 4; ++k) L.bgcl[(size_t)k * L.B + b] = r.r8();
             }
             r.next(); L.Nb = r.i4(); int32_t nn = r.i4();
             for (int j = 0; j < 21; ++j) { r.next(); L.reg[j] = r.i4(); }
@@ -1270,26 +1581,28 @@ int fp_read_sol(const char *path, fp_mesh **out) {
             if (neis != 0) throw std::runtime_error("engine inlet sides are not supported");
             r.next(); L.E = r.i4();
             L.side.resize(2 * (size_t)L.E); L.sw.resize(3 * (size_t)L.E); L.slen.resize(L.E);
+            L.gcl.resize(2 * (size_t)L.E);
             for (int32_t e = 0; e < L.E; ++e) {
                 r.next();
                 L.side[e] = r.i4(); L.side[(size_t)L.E + e] = r.i4();
                 for (int k = 0; k < 3; ++k) L.sw[(size_t)k * L.E + e] = r.r8();
-                double g = r.r8(), gp = r.r8();
-                if (g != 0.0 || gp != 0.0) throw std::runtime_error("moving-mesh GCL weights are not supported");
+                L.gcl[e] = r.r8(); L.gcl[(size_t)L.E + e] = r.r8();
                 L.slen[e] = r.r8();
             }
             r.next(); L.N = r.i4();
             L.vol.resize(L.N); L.wdist.resize(L.N); L.wnode.resize(L.N);
             if (fine) {
-                L.xyz.resize(3 * (size_t)L.N);
+                L.xyz.resize(3 * (size_t)L.N); L.xyzp.resize(3 * (size_t)L.N); L.xyzp2.resize(3 * (size_t)L.N);
+                L.volp.resize(L.N); L.volp2.resize(L.N);
                 for (int32_t i = 0; i < L.N; ++i) {
                     r.next();
                     int32_t id = r.i4();
                     if (id < 1 || id > L.N) throw fio::io_error("node id out of range");
                     --id;
-                    L.vol[id] = r.r8(); r.r8(); r.r8();
+                    L.vol[id] = r.r8(); L.volp[id] = r.r8(); L.volp2[id] = r.r8();
                     L.wdist[id] = r.r8(); L.wnode[id] = r.i4();
-                    for (int k = 0; k < 3; ++k) L.xyz[(size_t)k * L.N + id] = r.r8();
+                    for (std::vector<double> *x : {&L.xyz, &L.xyzp, &L.xyzp2})
+                        for (int k = 0; k < 3; ++k) (*x)[(size_t)k * L.N + id] = r.r8();
                 }
                 r.next(); int32_t ntrip = r.i4();
                 for (int32_t i = 0; i < ntrip; ++i) r.next();

@@ -136,6 +136,7 @@ int flite_batch_create(int ncases, const flite_controls *controls, const int32_t
     for (int i = 0; i < ncases; ++i) {
         const int m = mesh_of_case[i];
         if (m < 0 || m >= nmeshes || !levels[m] || nlevels[m] < 1) return FLITE_EINVAL;
+        if (controls[i].flowType == 2) return FLITE_EUNSUPPORTED;  // moving meshes are not batched
         const flite_ctx *donor = owner[m] >= 0 ? B->cases[owner[m]] : nullptr;
         int rc = flite::create_context(&controls[i], nlevels[m], levels[m], donor, &B->cases[i]);
         if (rc != FLITE_OK) return rc;

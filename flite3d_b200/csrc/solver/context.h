@@ -116,6 +116,8 @@ struct flite_ctx {
     // number, iperm[l] its inverse; d_perm/d_iperm on the device (shared with
     // contexts that share this mesh); a scratch array for the permutations
     bool renumbered = false;
+    // the mesh arrays are another context's (a batch case on a shared mesh)
+    bool shares_mesh = false;
     std::vector<std::vector<int>> perm, iperm;
     std::vector<int *> d_perm, d_iperm;
     double *d_io = nullptr;
@@ -447,8 +449,9 @@ struct flite_ctx {
     }
     bool mixed() const { return c.precision == FLITE_MIXED; }
     // the central flux (and FLITE_MIXED, which only takes it) is computed
-    // inside the node gather; the upwind fluxes go through the edge buffer
-    bool fused() const { return c.fluxType == 1; }
+    // inside the node gather; the upwind fluxes, and every flux of a moving
+    // mesh (with its GCL term), go through the edge buffer
+    bool fused() const { return c.fluxType == 1 && c.flowType != 2; }
     // the flux kernel instance of this run's fluxType (and HLLC order; the
     // reconstruction only acts on level 1, where coordinates exist)
     void edge_flux_launch(const LevelView &L) {
@@ -759,4 +762,6 @@ struct flite_ctx {
 namespace flite {
 int create_context(const flite_controls *c, int nlevels, const flite_level_desc *levels, const flite_ctx *donor,
                    flite_ctx **out);
+// the geometry arrays of level l from its descriptor (allocated when create)
+void put_geometry(flite_ctx &X, int l, const flite_level_desc &d, bool create);
 }  // namespace flite

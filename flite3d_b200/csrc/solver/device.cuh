@@ -144,6 +144,14 @@ struct LevelView {
     DeltaRec *dq;                          // [N] anchor primitives and increments
     const IncRec32 *inc32;                 // [2E] incidences in FP32
     double *bflux;                         // [B][10] boundary-edge contributions
+    // moving meshes (flowType 2; NULL on a static mesh): per edge the GCL
+    // weight over physicalTimeStep (wgcl of makeRHS), per boundary edge its
+    // two nodes' (times 4 with boundaryTerm 2), the boundary edges' GCL
+    // terms, and the volumes of the two previous steps (level 1)
+    const double *gclw;                    // [E]
+    const double *bgclw;                   // [2][B]
+    double *bgterm;                        // [B][10]
+    const double *Vp, *Vp2;                // [N]
     // unsteady dual time: the solution of the previous physical time steps
     // (uold2 on level 1 only)
     double *uold, *uold2;                  // [nvar][N]
@@ -208,13 +216,16 @@ __device__ __forceinline__ double pressure(const Params &P, double r, double m1,
 }
 
 // addTimeDifferences (def_par:1184-1241) of component c at node i: the
-// second-order backward difference on level 1 with timeScheme 2, first order
-// elsewhere; static mesh (the previous volumes are the volumes)
+// second-order backward difference on level 1 with timeScheme 2 (with the
+// previous volumes of a moving mesh; a static mesh's are the volumes), first
+// order elsewhere
 __device__ __forceinline__ double time_difference(const Params &P, const LevelView &L, int i, int c) {
     const size_t k = (size_t)c * L.N + i;
     const double Vi = L.V[i];
-    if (L.grid == 1 && P.bdf2)
-        return (((1.5 * Vi) * L.u[k] - (2.0 * Vi) * L.uold[k]) + (0.5 * Vi) * L.uold2[k]) / P.dtp;
+    if (L.grid == 1 && P.bdf2) {
+        const double Vp = L.Vp ? L.Vp[i] : Vi, Vp2 = L.Vp2 ? L.Vp2[i] : Vi;
+        return (((1.5 * Vi) * L.u[k] - (2.0 * Vp) * L.uold[k]) + (0.5 * Vp2) * L.uold2[k]) / P.dtp;
+    }
     return Vi * (L.u[k] - L.uold[k]) / P.dtp;
 }
 

@@ -111,10 +111,13 @@ void build_tiles(int N, const std::vector<int> &ip, const std::vector<int2> &inc
 }
 
 const char *unsupported_reason(const flite_controls &c) {
-    if (c.flowType == 2) return "flowType 2 (moving meshes, ALE) is not supported";
-    if (c.flowType != 0 && c.flowType != 1) return "flowType must be 0 (steady) or 1 (unsteady, static mesh)";
+    if (c.flowType != 0 && c.flowType != 1 && c.flowType != 2)
+        return "flowType must be 0 (steady), 1 (unsteady, static mesh) or 2 (unsteady, moving mesh)";
     if (c.explicit_) return "explicit time stepping is not supported";
-    if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return "unsteady runs need physicalTimeStep > 0";
+    if (c.flowType != 0 && !(c.physicalTimeStep > 0)) return "unsteady runs need physicalTimeStep > 0";
+    if (c.flowType == 2 && c.precision != FLITE_FP64) return "moving meshes (flowType 2) run in FP64";
+    if (c.flowType == 2 && c.reconstruction != FLITE_RECON_NONE)
+        return "moving meshes (flowType 2) take the reference's fluxes (no reconstruction extension)";
     if (c.forceCalcType != 1 && c.forceCalcType != 3)
         return "forceCalcType must be 1 or 3 (2 is the spanwise load of gust runs)";
     if (c.SAS || c.GUSTMODEL || c.movingwall || c.patchInitialization || c.nspan != 0)
@@ -148,6 +151,95 @@ const char *unsupported_reason(const flite_controls &c) {
 }
 
 }  // namespace
+
+// The geometry arrays of level l (readGridComputationData and the set-up
+// it performs): coefficients, side lengths, volumes, wall distances, normals
+// (makeBoundaryNormals def_par:15394-15521), wall area (makeSurfaceArea
+// :15523-15634, level 1), coordinates and their movement, restriction
+// weights; on a moving mesh the GCL weights over physicalTimeStep (wgcl of
+// makeRHS, combined as 1.5 GCL - 0.5 GCLprev on level 1 with timeScheme 2,
+// def_par:816-818, 13858-13860) and the previous volumes.  Allocated and
+// uploaded at creation (create), copied over the existing arrays otherwise.
+void flite::put_geometry(flite_ctx &X, int l, const flite_level_desc &d, bool create) {
+    LevelView &L = X.lv[l].v;
+    const int N = L.N, E = L.E, B = L.B;
+    auto put = [&](auto &field, const auto &h) {
+        using T = typename std::decay_t<decltype(h)>::value_type;
+        if (create) field = X.upload(h);
+        else if (!h.empty())
+            CK(cudaMemcpy(const_cast<T *>(field), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    };
+    std::vector<double> wx(E), wy(E), wz(E), slen(E, 0.0);
+    std::vector<EdgeW> ew(std::max(E, 1));
+    for (int e = 0; e < E; ++e) {
+        wx[e] = d.side_w[e]; wy[e] = d.side_w[(size_t)E + e]; wz[e] = d.side_w[2 * (size_t)E + e];
+        if (d.side_len) slen[e] = d.side_len[e];
+        ew[e] = EdgeW{wx[e], wy[e], wz[e], 0.0};
+    }
+    std::vector<int2> bedge(B);
+    std::vector<double> bwx(B), bwy(B), bwz(B);
+    for (int b = 0; b < B; ++b) {
+        const int a = d.bnd_idx[b] - 1, q = d.bnd_idx[(size_t)B + b] - 1;
+        if (a < 0 || a >= N || q < 0 || q >= N) throw std::runtime_error("boundary edge index out of range");
+        bedge[b] = make_int2(a, q);
+        bwx[b] = d.bnd_w[b]; bwy[b] = d.bnd_w[(size_t)B + b]; bwz[b] = d.bnd_w[2 * (size_t)B + b];
+    }
+    std::vector<double> nx(N, 0.0), ny(N, 0.0), nz(N, 0.0), wa(N, 0.0);
+    for (int b = 0; b < B; ++b) {
+        const int a = bedge[b].x, q = bedge[b].y;
+        nx[a] = nx[a] - bwx[b]; ny[a] = ny[a] - bwy[b]; nz[a] = nz[a] - bwz[b];
+        nx[q] = nx[q] - bwx[b]; ny[q] = ny[q] - bwy[b]; nz[q] = nz[q] - bwz[b];
+    }
+    for (int i = 0; i < L.Nb; ++i) {
+        const double nrm = std::sqrt((nx[i] * nx[i] + ny[i] * ny[i]) + nz[i] * nz[i]);
+        if (nrm > 1.0e-10) { nx[i] = nx[i] / nrm; ny[i] = ny[i] / nrm; nz[i] = nz[i] / nrm; }
+        else { nx[i] = 0.0; ny[i] = 0.0; nz[i] = 0.0; }
+    }
+    if (l == 0)
+        for (int b = 0; b < B; ++b) {
+            const double ai = std::sqrt((bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b]);
+            wa[bedge[b].x] = wa[bedge[b].x] + 4.0 * ai;
+            wa[bedge[b].y] = wa[bedge[b].y] + 4.0 * ai;
+        }
+    std::vector<double> coords(3 * (size_t)N, 0.0), cm(3 * (size_t)N, 0.0);
+    if (l == 0 && d.coords) std::memcpy(coords.data(), d.coords, 3 * (size_t)N * sizeof(double));
+    if (l == 0 && d.coord_move) std::memcpy(cm.data(), d.coord_move, 3 * (size_t)N * sizeof(double));
+    put(L.wx, wx); put(L.wy, wy); put(L.wz, wz); put(L.slen, slen); put(L.ew, ew);
+    put(L.bwx, bwx); put(L.bwy, bwy); put(L.bwz, bwz);
+    put(L.V, std::vector<double>(d.volume, d.volume + N));
+    put(L.wdist, d.wall_dist ? std::vector<double>(d.wall_dist, d.wall_dist + N) : std::vector<double>(N, 0.0));
+    put(L.nx, nx); put(L.ny, ny); put(L.nz, nz); put(L.wallArea, wa);
+    put(L.cx, coords);
+    L.cy = L.cx + N; L.cz = L.cx + 2 * (size_t)N;
+    put(L.cmx, cm);
+    L.cmy = L.cmx + N; L.cmz = L.cmx + 2 * (size_t)N;
+    if (l > 0) {
+        if (!d.rweight) throw std::runtime_error("coarse level without transfer operators");
+        put(L.rweight, std::vector<double>(d.rweight, d.rweight + X.lv[l - 1].N));
+    }
+    if (X.c.flowType == 2) {
+        if (!d.side_gcl || !d.bnd_gcl || (l == 0 && (!d.volume_prev || !d.volume_prev2)))
+            throw std::invalid_argument("a moving mesh (flowType 2) needs side_gcl, bnd_gcl and, on level 1, "
+                                        "volume_prev and volume_prev2");
+        const bool comb = l == 0 && X.c.timeScheme == 2;
+        const double dtp = X.c.physicalTimeStep;
+        auto w = [&](double x, double xp) { return comb ? 1.5 * x - 0.5 * xp : x; };
+        std::vector<double> gw(std::max(E, 1)), bgw(2 * (size_t)std::max(B, 1));
+        for (int e = 0; e < E; ++e) gw[e] = w(d.side_gcl[e], d.side_gcl[(size_t)E + e]) / dtp;
+        for (int b = 0; b < B; ++b) {
+            const double g1 = w(d.bnd_gcl[b], d.bnd_gcl[2 * (size_t)B + b]);
+            const double g2 = w(d.bnd_gcl[(size_t)B + b], d.bnd_gcl[3 * (size_t)B + b]);
+            bgw[b] = X.c.boundaryTerm == 1 ? g1 / dtp : 4.0 * g1 / dtp;
+            bgw[(size_t)B + b] = X.c.boundaryTerm == 1 ? g2 / dtp : 4.0 * g2 / dtp;
+        }
+        put(L.gclw, gw);
+        put(L.bgclw, bgw);
+        if (l == 0) {
+            put(L.Vp, std::vector<double>(d.volume_prev, d.volume_prev + N));
+            put(L.Vp2, std::vector<double>(d.volume_prev2, d.volume_prev2 + N));
+        }
+    }
+}
 
 extern "C" {
 
@@ -211,6 +303,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         // the device numbering of the nodes (renumber.h); a context sharing
         // a donor's mesh shares its numbering
         Renumbered R;
+        X.shares_mesh = donor != nullptr;
         if (donor) {
             X.renumbered = donor->renumbered;
             X.perm = donor->perm; X.iperm = donor->iperm;
@@ -270,24 +363,19 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             } else {
             // edges
             std::vector<int2> edge(E);
-            std::vector<double> wx(E), wy(E), wz(E), slen(E, 0.0);
             for (int e = 0; e < E; ++e) {
                 int a = d.side_idx[e] - 1, b = d.side_idx[(size_t)E + e] - 1;
                 if (a < 0 || a >= N || b < 0 || b >= N || a == b) throw std::runtime_error("edge index out of range");
                 edge[e] = make_int2(a, b);
-                wx[e] = d.side_w[e]; wy[e] = d.side_w[(size_t)E + e]; wz[e] = d.side_w[2 * (size_t)E + e];
-                if (d.side_len) slen[e] = d.side_len[e];
             }
             std::vector<int2> bedge(B);
             std::vector<int> bind(B);
-            std::vector<double> bwx(B), bwy(B), bwz(B);
             for (int b = 0; b < B; ++b) {
                 int a = d.bnd_idx[b] - 1, q = d.bnd_idx[(size_t)B + b] - 1;
                 if (a < 0 || a >= N || q < 0 || q >= N) throw std::runtime_error("boundary edge index out of range");
                 bedge[b] = make_int2(a, q);
                 bind[b] = d.bnd_idx[2 * (size_t)B + b];
                 if (bind[b] >= 5 && bind[b] <= 8) return FLITE_EUNSUPPORTED;  // engine faces
-                bwx[b] = d.bnd_w[b]; bwy[b] = d.bnd_w[(size_t)B + b]; bwz[b] = d.bnd_w[2 * (size_t)B + b];
             }
             // node -> incident edges in edge order
             std::vector<int> ip(N + 1, 0);
@@ -312,25 +400,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     binc[fill[bedge[b].y]++] = 2 * b + 1;
                 }
             }
-            // geometry of readGridComputationData: normals (def_par:15394-
-            // 15521), wall area (:15523-15634, level 1), connectivity
-            std::vector<double> nx(N, 0.0), ny(N, 0.0), nz(N, 0.0), wa(N, 0.0), conn(N, 0.0);
-            for (int b = 0; b < B; ++b) {
-                int a = bedge[b].x, q = bedge[b].y;
-                nx[a] = nx[a] - bwx[b]; ny[a] = ny[a] - bwy[b]; nz[a] = nz[a] - bwz[b];
-                nx[q] = nx[q] - bwx[b]; ny[q] = ny[q] - bwy[b]; nz[q] = nz[q] - bwz[b];
-            }
-            for (int i = 0; i < Nb; ++i) {
-                double nrm = std::sqrt((nx[i] * nx[i] + ny[i] * ny[i]) + nz[i] * nz[i]);
-                if (nrm > 1.0e-10) { nx[i] = nx[i] / nrm; ny[i] = ny[i] / nrm; nz[i] = nz[i] / nrm; }
-                else { nx[i] = 0.0; ny[i] = 0.0; nz[i] = 0.0; }
-            }
-            if (l == 0)
-                for (int b = 0; b < B; ++b) {
-                    double ai = std::sqrt((bwx[b] * bwx[b] + bwy[b] * bwy[b]) + bwz[b] * bwz[b]);
-                    wa[bedge[b].x] = wa[bedge[b].x] + 4.0 * ai;
-                    wa[bedge[b].y] = wa[bedge[b].y] + 4.0 * ai;
-                }
+            // connectivity (def_par:14262-14275)
+            std::vector<double> conn(N, 0.0);
             for (int e = 0; e < E; ++e) { conn[edge[e].x] += 1.0; conn[edge[e].y] += 1.0; }
             // boundary classes from the indicator register
             std::vector<unsigned char> bc(N, BC_NONE);
@@ -347,24 +418,20 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     if (l == 0 && k == 1) D.wall.push_back(n);
                 }
             }
-            std::vector<double> coords(3 * (size_t)N, 0.0), cm(3 * (size_t)N, 0.0);
-            if (l == 0 && d.coords) std::memcpy(coords.data(), d.coords, 3 * (size_t)N * sizeof(double));
-            if (l == 0 && d.coord_move) std::memcpy(cm.data(), d.coord_move, 3 * (size_t)N * sizeof(double));
             // upload
             L.edge = X.upload(edge);
-            L.wx = X.upload(wx); L.wy = X.upload(wy); L.wz = X.upload(wz); L.slen = X.upload(slen);
             L.bedge = X.upload(bedge); L.bind = X.upload(bind);
-            L.bwx = X.upload(bwx); L.bwy = X.upload(bwy); L.bwz = X.upload(bwz);
             L.inc_ptr = X.upload(ip); L.inc = X.upload(inc);
-            {
-                std::vector<EdgeW> ew(std::max(E, 1));
-                for (int e = 0; e < E; ++e) ew[e] = EdgeW{wx[e], wy[e], wz[e], 0.0};
-                L.ew = X.upload(ew);
-            }
+            L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
+            L.conn = X.upload(conn);
+            L.bc = X.upload(bc);
+            put_geometry(X, l, d, true);
             L.inc32 = nullptr;
             L.tile = TileView{};
-            if (c->fluxType == 1) {
+            if (X.fused()) {
                 // staging of node blocks for the fused central gather
+                std::vector<double> wx(d.side_w, d.side_w + E), wy(d.side_w + E, d.side_w + 2 * (size_t)E),
+                    wz(d.side_w + 2 * (size_t)E, d.side_w + 3 * (size_t)E);
                 TileHost T;
                 build_tiles(N, ip, inc, wx, wy, wz, T);
                 if (T.ntiles > 0) {
@@ -378,22 +445,10 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     L.tile.wx = X.upload(T.wx); L.tile.wy = X.upload(T.wy); L.tile.wz = X.upload(T.wz);
                 }
             }
-            L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
-            L.V = X.upload(std::vector<double>(d.volume, d.volume + N));
-            L.wdist = d.wall_dist ? X.upload(std::vector<double>(d.wall_dist, d.wall_dist + N))
-                                  : X.upload(std::vector<double>(N, 0.0));
-            L.conn = X.upload(conn);
-            L.nx = X.upload(nx); L.ny = X.upload(ny); L.nz = X.upload(nz); L.wallArea = X.upload(wa);
-            double *dc = X.upload(coords);
-            L.cx = dc; L.cy = dc + N; L.cz = dc + 2 * (size_t)N;
-            double *dm = X.upload(cm);
-            L.cmx = dm; L.cmy = dm + N; L.cmz = dm + 2 * (size_t)N;
-            L.bc = X.upload(bc);
             if (l > 0) {
                 const int nf = X.lv[l - 1].N;
                 if (!d.parent || !d.rweight) throw std::runtime_error("coarse level without transfer operators");
                 std::vector<int> par(nf);
-                std::vector<double> rw(d.rweight, d.rweight + nf);
                 std::vector<int> cp(N + 1, 0);
                 for (int f = 0; f < nf; ++f) {
                     par[f] = d.parent[f] - 1;
@@ -409,7 +464,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     const int f = X.iperm[l - 1][fo];
                     if (par[f] >= 0) ch[fill[par[f]]++] = f;
                 }
-                L.parent = X.upload(par); L.rweight = X.upload(rw);
+                L.parent = X.upload(par);
                 L.child_ptr = X.upload(cp); L.child = X.upload(ch);
             }
             if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
@@ -456,7 +511,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             L.gq = muscl ? X.alloc<GradRec>(N) : nullptr;
             // the edge buffer carries the upwind fluxes; the central flux is
             // computed inside the node gather
-            L.flux = c->fluxType != 1 ? X.alloc<double>(5 * (size_t)std::max(E, 1)) : nullptr;
+            L.flux = !X.fused() ? X.alloc<double>(5 * (size_t)std::max(E, 1)) : nullptr;
             if (c->precision == FLITE_MIXED) {
                 L.ua = X.alloc<double>(5 * (size_t)N);
                 L.ra = X.alloc<double>(5 * (size_t)N);
@@ -480,6 +535,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L.dq = nullptr;
             }
             L.bflux = X.alloc<double>(10 * (size_t)std::max(B, 1));
+            L.bgterm = c->flowType == 2 ? X.alloc<double>(10 * (size_t)std::max(B, 1)) : nullptr;
             L.uold = c->flowType != 0 ? X.alloc<double>(nv * N) : nullptr;
             L.uold2 = c->flowType != 0 && l == 0 ? X.alloc<double>(nv * N) : nullptr;
             L.cyc = X.d_cyc + l;
@@ -587,6 +643,31 @@ int flite_next_physical_step(flite_ctx *ctx) {
         CK(cudaMemcpyAsync(X.V(0).uold2, X.V(0).uold, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
         CK(cudaMemcpyAsync(X.V(0).uold, X.V(0).u, n5 * sizeof(double), cudaMemcpyDeviceToDevice, X.s));
         // head of the next one
+        X.physical_step_start();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(X.s));
+        return FLITE_OK;
+    });
+}
+
+int flite_update_geometry(flite_ctx *ctx, int nlevels, const flite_level_desc *levels) {
+    if (!ctx || !levels || nlevels < (int)ctx->lv.size()) return FLITE_EINVAL;
+    if (ctx->c.flowType != 2) return fail(ctx, FLITE_EINVAL, "not a moving-mesh run (flowType 2)");
+    if (ctx->shares_mesh) return fail(ctx, FLITE_EUNSUPPORTED, "the mesh is shared with other cases of a batch");
+    return guarded(ctx, [&] {
+        flite_ctx &X = *ctx;
+        const int G = (int)X.lv.size();
+        for (int l = 0; l < G; ++l)
+            if (levels[l].n_nodes != X.lv[l].N || levels[l].n_sides != X.lv[l].E || levels[l].n_bsides != X.lv[l].B ||
+                !levels[l].side_w || !levels[l].bnd_w || !levels[l].bnd_idx || !levels[l].volume)
+                throw std::invalid_argument("the levels differ from those the context was created with");
+        // the device numbering of flite_create
+        Renumbered R;
+        renumber_as(G, levels, X.perm, X.iperm, !X.renumbered, R);
+        CK(cudaStreamSynchronize(X.s));
+        for (int l = 0; l < G; ++l) put_geometry(X, l, R.desc[l], false);
+        // the captured cycle holds no geometry value (only pointers), but the
+        // head of the step runs again with the new restriction weights
         X.physical_step_start();
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(X.s));
@@ -853,28 +934,32 @@ int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32
         // their separate groups hold what is left of them)
         const int fz = X.step_fusion(l);
         const bool visc = X.c.ReynoldsNumber > 0;
-        std::vector<std::function<void()>> k;
-        k.push_back([&] { X.pressure(l); });
-        k.push_back([&] { if (!fz) X.timesteps(l); });
+        // each group launches its kernels and tells whether it had any (a
+        // group without kernels reports 0 ms)
+        std::vector<std::function<bool()>> k;
+        k.push_back([&] { X.pressure(l); return true; });
+        k.push_back([&] { if (!fz) X.timesteps(l); return !fz; });
         k.push_back([&] {
             if (!fz) X.dissipation(l);
             else if (fz == 1) X.jst_flux(l);
+            return fz != 2;
         });
-        k.push_back([&] { if (visc) k_visc_prim<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
-        k.push_back([&] { if (visc && fz != 2) X.visc_grad(l); });
-        k.push_back([&] { if (visc) X.visc_flux(l); });
-        k.push_back([&] { X.rhs_terms(l, true); });
-        k.push_back([&] { X.launch_node_update(l, MODE_RFINE, 0, true); });
-        k.push_back([&] { if (fz) k_ts_lap<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
-        k.push_back([&] { if (fz == 2) k_jflux_vgrad<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); });
+        k.push_back([&] { if (visc) k_visc_prim<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); return visc; });
+        k.push_back([&] { if (visc && fz != 2) X.visc_grad(l); return visc && fz != 2; });
+        k.push_back([&] { if (visc) X.visc_flux(l); return visc; });
+        k.push_back([&] { X.rhs_terms(l, true); return true; });
+        k.push_back([&] { X.launch_node_update(l, MODE_RFINE, 0, true); return true; });
+        k.push_back([&] { if (fz) k_ts_lap<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); return fz != 0; });
+        k.push_back([&] { if (fz == 2) k_jflux_vgrad<<<X.nblk(L.N), X.nb, 0, X.s>>>(X.P, L); return fz == 2; });
         const int m = std::min<int>((int)k.size(), nmax);
         std::vector<cudaEvent_t> ev(m + 1);
         for (auto &e : ev) CK(cudaEventCreate(&e));
         std::vector<double> acc(m, 0.0);
+        std::vector<char> ran(m, 0);
         for (int r = 0; r < reps; ++r) {
             CK(cudaEventRecord(ev[0], X.s));
             for (int q = 0; q < m; ++q) {
-                k[q]();
+                ran[q] = k[q]() ? 1 : 0;
                 CK(cudaEventRecord(ev[q + 1], X.s));
             }
             CK(cudaEventSynchronize(ev[m]));
@@ -885,7 +970,7 @@ int flite_profile_kernels(flite_ctx *ctx, int level, int reps, double *ms, int32
             }
         }
         for (auto &e : ev) cudaEventDestroy(e);
-        for (int q = 0; q < m; ++q) ms[q] = acc[q] / reps;
+        for (int q = 0; q < m; ++q) ms[q] = ran[q] ? acc[q] / reps : 0.0;
         *n = m;
         return FLITE_OK;
     });

@@ -102,10 +102,20 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
     double E2 = b.E, rh2 = b.E + pr2;
     const double wx = L.wx[e], wy = L.wy[e], wz = L.wz[e];
     f[0] = f[1] = f[2] = f[3] = f[4] = 0.0;
+    // moving meshes: the GCL term -q wgcl (def_par:1662-1791)
+    const double wgcl = L.gclw ? L.gclw[e] : 0.0;
+    auto gcl_sum = [&]() {
+        if (!L.gclw) return;
+        f[0] = f[0] - (r1 + r2) * wgcl; f[1] = f[1] - (ru1 + ru2) * wgcl; f[2] = f[2] - (rv1 + rv2) * wgcl;
+        f[3] = f[3] - (rw1 + rw2) * wgcl; f[4] = f[4] - (E1 + E2) * wgcl;
+    };
     if constexpr (FT == 1 || FT == 4) {
         // central flux; HLLC starts from it too (def_par:1798)
         central_flux(a, b, wx, wy, wz, f);
-        if constexpr (FT == 1) return;
+        if constexpr (FT == 1) {
+            gcl_sum();
+            return;
+        }
     }
     if constexpr (FT == 2) {  // local Lax-Friedrichs (def_par:1670-1724)
         double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
@@ -125,6 +135,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
             f[2] = rnorm * (((pr1 * rny + rv1 * nv1) + (pr2 * rny + rv2 * nv2)) - lam * (rv1 - rv2));
             f[3] = rnorm * (((pr1 * rnz + rw1 * nv1) + (pr2 * rnz + rw2 * nv2)) - lam * (rw1 - rw2));
             f[4] = rnorm * ((rh1 * nv1 + rh2 * nv2) - lam * (E1 - E2));
+            gcl_sum();
         }
         return;
     }
@@ -165,6 +176,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
             f[2] = rnorm * ((f31 + f32) - ((l3 * du3 + cc1 * vi) + cc2 * rny));
             f[3] = rnorm * ((f41 + f42) - ((l3 * du4 + cc1 * wi) + cc2 * rnz));
             f[4] = rnorm * ((f51 + f52) - ((l3 * du5 + cc1 * hi) + cc2 * ucp));
+            gcl_sum();
         }
         return;
     }
@@ -236,6 +248,10 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
     double fact = roe2 * (sr - nv2) - roe1 * (sl - nv1);
     if (fact != 0.0) fact = 1.0 / fact;
     sm = fact * sm;
+    // the state of the GCL term: rho and E of the node with the
+    // (reconstructed) momentum outside the star region, the star state
+    // inside it (def_par:2046-2085)
+    double q[5] = {r1, ru1, rv1, rw1, E1};
     if (sl > 0.0) {
         f[0] = ((rnx * ru1 + rny * rv1) + rnz * rw1) * rnorm1;
         f[1] = ((rnx * (ru1 * u1 + pr1) + rny * (ru1 * v1)) + rnz * (ru1 * w1)) * rnorm1;
@@ -266,6 +282,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         f[2] = (fl2 + sl * (ls2 - rv1)) * rnorm1;
         f[3] = (fl3 + sl * (ls3 - rw1)) * rnorm1;
         f[4] = (fl4 + sl * (ls4 - re1)) * rnorm1;
+        q[0] = ls0; q[1] = ls1; q[2] = ls2; q[3] = ls3; q[4] = ls4;
     } else if (sm <= 0.0 && sr >= 0.0) {
         double fr0 = (rnx * ru2 + rny * rv2) + rnz * rw2;
         double fr1 = (rnx * (ru2 * u2 + pr2) + rny * (ru2 * v2)) + rnz * (ru2 * w2);
@@ -290,13 +307,17 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
         f[2] = (fr2 + sr * (rs2 - rv2)) * rnorm1;
         f[3] = (fr3 + sr * (rs3 - rw2)) * rnorm1;
         f[4] = (fr4 + sr * (rs4 - re2)) * rnorm1;
+        q[0] = rs0; q[1] = rs1; q[2] = rs2; q[3] = rs3; q[4] = rs4;
     } else if (sr < 0.0) {
         f[0] = ((rnx * ru2 + rny * rv2) + rnz * rw2) * rnorm1;
         f[1] = ((rnx * (ru2 * u2 + pr2) + rny * (ru2 * v2)) + rnz * (ru2 * w2)) * rnorm1;
         f[2] = ((rnx * (rv2 * u2) + rny * (rv2 * v2 + pr2)) + rnz * (rv2 * w2)) * rnorm1;
         f[3] = ((rnx * (rw2 * u2) + rny * (rw2 * v2)) + rnz * (rw2 * w2 + pr2)) * rnorm1;
         f[4] = ((rnx * (rh2 * u2) + rny * (rh2 * v2)) + rnz * (rh2 * w2)) * rnorm1;
+        q[0] = r2; q[1] = ru2; q[2] = rv2; q[3] = rw2; q[4] = E2;
     }
+    if (L.gclw)
+        for (int k = 0; k < 5; ++k) f[k] = f[k] - q[k] * wgcl;
     }
 }
 
@@ -352,8 +373,26 @@ __device__ __forceinline__ void farfield_flux(const Params &P, const NodeState &
     F[4] = 0.5 * (fr5 + fl5) - 0.5 * ((l3 * du5 + cc1 * hi) + cc2 * ucp);
 }
 
+// The GCL terms of boundary edge b of a moving mesh, subtracted from its
+// two nodes' residuals before the edge's flux (def_par:2124-2177)
+__device__ __forceinline__ void boundary_gcl(const Params &P, const LevelView &L, int b, double *t1, double *t2) {
+    const int2 nd = L.bedge[b];
+    const NodeState s1 = load_state(L, nd.x), s2 = load_state(L, nd.y);
+    const double q1[5] = {s1.r, s1.ru, s1.rv, s1.rw, s1.E}, q2[5] = {s2.r, s2.ru, s2.rv, s2.rw, s2.E};
+    const double w1 = L.bgclw[b], w2 = L.bgclw[L.B + b];
+    for (int k = 0; k < 5; ++k) {
+        if (P.boundaryTerm == 1) {
+            t1[k] = (3. * q1[k] + q2[k]) * w1;
+            t2[k] = (q1[k] + 3. * q2[k]) * w2;
+        } else {
+            t1[k] = q1[k] * w1;
+            t2[k] = q2[k] * w2;
+        }
+    }
+}
+
 // Contributions g1 (to node 1) and g2 (to node 2) of boundary edge b
-// (def_par:2182-2511, static mesh)
+// (def_par:2182-2511)
 __device__ __forceinline__ void boundary_flux(const Params &P, const LevelView &L, int b, double *g1, double *g2) {
     const int2 nd = L.bedge[b];
     const int ind = L.bind[b];

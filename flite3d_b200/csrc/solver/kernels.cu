@@ -1363,6 +1363,11 @@ __global__ void k_bnd_flux(Params P, LevelView L) {
     boundary_flux(P, L, b, g1, g2);
     double *o = L.bflux + (size_t)b * 10;
     for (int k = 0; k < 5; ++k) { o[k] = g1[k]; o[5 + k] = g2[k]; }
+    if (L.bgterm) {
+        boundary_gcl(P, L, b, g1, g2);
+        double *t = L.bgterm + (size_t)b * 10;
+        for (int k = 0; k < 5; ++k) { t[k] = g1[k]; t[5 + k] = g2[k]; }
+    }
 }
 
 // ---- mixed precision ------------------------------------------------------
@@ -1573,7 +1578,8 @@ __device__ __forceinline__ void gather_interior(const LevelView &L, int i, doubl
     }
 }
 
-// boundary edges of node i (FP64)
+// boundary edges of node i (FP64); on a moving mesh each edge's GCL term is
+// subtracted before its flux is added
 template <int U>
 __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, double *r, bool active = true,
                                          int gl = 0) {
@@ -1585,8 +1591,23 @@ __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, doubl
     auto add = [&](const double *g) {
         r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
     };
+    auto terms_gcl = [&](int k, double *g) {
+        const int v = L.binc[k];
+        const size_t o = (size_t)(v >> 1) * 10 + (v & 1) * 5;
+        for (int c = 0; c < 5; ++c) { g[c] = L.bgterm[o + c]; g[5 + c] = L.bflux[o + c]; }
+    };
+    auto add_gcl = [&](const double *g) {
+        for (int c = 0; c < 5; ++c) r[c] = (r[c] - g[c]) + g[5 + c];
+    };
     if constexpr (U > 1) {
-        group_gather<U, 5, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms, add);
+        if (L.bgterm) group_gather<U, 10, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms_gcl, add_gcl);
+        else group_gather<U, 5, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms, add);
+    } else if (L.bgterm) {
+        for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
+            double v[10];
+            terms_gcl(k, v);
+            add_gcl(v);
+        }
     } else {
         for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
             double v[5];

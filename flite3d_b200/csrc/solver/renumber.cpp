@@ -92,11 +92,27 @@ void renumber_levels(int nlevels, const flite_level_desc *lv, int mode, Renumber
         iperm.resize(N);
         for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
     }
+    permute_levels(nlevels, lv, out);
+}
+
+void renumber_as(int nlevels, const flite_level_desc *lv, const std::vector<std::vector<int>> &perm,
+                 const std::vector<std::vector<int>> &iperm, bool identity, Renumbered &out) {
+    out = Renumbered{};
+    out.desc.assign(lv, lv + nlevels);
+    out.perm = perm;
+    out.iperm = iperm;
+    out.identity = identity;
+    for (int l = 0; l < nlevels; ++l)
+        if ((int)perm.size() <= l || (int)perm[l].size() != lv[l].n_nodes) throw std::runtime_error("bad level sizes");
+    permute_levels(nlevels, lv, out);
+}
+
+void permute_levels(int nlevels, const flite_level_desc *lv, Renumbered &out) {
     if (out.identity) return;
     const size_t L = (size_t)nlevels;
     out.side_idx.resize(L); out.bnd_idx.resize(L); out.node_ind.resize(L); out.parent.resize(L);
     out.volume.resize(L); out.wall_dist.resize(L); out.coords.resize(L); out.coord_move.resize(L);
-    out.rweight.resize(L);
+    out.rweight.resize(L); out.volume_prev.resize(L); out.volume_prev2.resize(L);
     for (int l = 0; l < nlevels; ++l) {
         const flite_level_desc &d = lv[l];
         flite_level_desc &o = out.desc[l];
@@ -131,6 +147,8 @@ void renumber_levels(int nlevels, const flite_level_desc *lv, int mode, Renumber
         o.wall_dist = permute(d.wall_dist, 1, out.wall_dist[l]);
         o.coords = permute(d.coords, 3, out.coords[l]);
         o.coord_move = permute(d.coord_move, 3, out.coord_move[l]);
+        o.volume_prev = permute(d.volume_prev, 1, out.volume_prev[l]);
+        o.volume_prev2 = permute(d.volume_prev2, 1, out.volume_prev2[l]);
         if (l > 0) {
             // fine-indexed transfer arrays of this level: fine node in the
             // finer level's new numbering, parent in this level's

@@ -32,12 +32,18 @@ struct Renumbered {
     bool identity = true;
     // storage behind desc
     std::vector<std::vector<int32_t>> side_idx, bnd_idx, node_ind, parent;
-    std::vector<std::vector<double>> volume, wall_dist, coords, coord_move, rweight;
+    std::vector<std::vector<double>> volume, wall_dist, coords, coord_move, rweight, volume_prev, volume_prev2;
 };
 
 // mode 0: identity; 1: locality order.  Throws std::runtime_error on
 // inconsistent descriptors.
 void renumber_levels(int nlevels, const flite_level_desc *lv, int mode, Renumbered &out);
+// the same with a given numbering (perm, iperm per level; identity when the
+// device numbering is the caller's): the levels of a moving mesh's next step
+void renumber_as(int nlevels, const flite_level_desc *lv, const std::vector<std::vector<int>> &perm,
+                 const std::vector<std::vector<int>> &iperm, bool identity, Renumbered &out);
+// the descriptors of out in the numbering of out.perm / out.iperm
+void permute_levels(int nlevels, const flite_level_desc *lv, Renumbered &out);
 
 // process-wide default of flite_create (flite_set_node_order)
 int default_node_order();

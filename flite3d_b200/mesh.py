@@ -26,6 +26,9 @@ class Mesh:
         self._h = ctypes.c_void_p(handle) if not isinstance(handle, ctypes.c_void_p) else handle
         self.nlevels = _lib().fp_num_levels(self._h)
         self._descs = (_abi.LevelDesc * self.nlevels)()
+        self._refresh()
+
+    def _refresh(self):
         for level in range(self.nlevels):
             _abi.check(_lib().fp_level_desc(self._h, level + 1, ctypes.byref(self._descs[level])),
                        "fp_level_desc")
@@ -132,6 +135,23 @@ class Mesh:
                                           xb.ctypes.data_as(ctypes.c_void_p)), "fp_geometry_vjp")
         return xb
 
+    def set_moving(self, xyz, xyz_prev, xyz_prev2, time_scheme=2):
+        """Moving meshes (flowType 2): the geometry of every level for the
+        physical step with node coordinates xyz, the two steps before having
+        had xyz_prev and xyz_prev2 (each (3, N)); the descriptors then carry
+        the GCL weights, previous volumes and coordinate movement."""
+        xs = [np.ascontiguousarray(x, dtype=np.float64) for x in (xyz, xyz_prev, xyz_prev2)]
+        _abi.check(_lib().fp_set_moving_geometry(self._h, *[x.ctypes.data_as(ctypes.c_void_p) for x in xs],
+                                                 int(time_scheme)), "fp_set_moving_geometry")
+        self._refresh()
+
+    def gcl_check(self, level=1, time_scheme=2):
+        """(largest GCL defect, largest volume change) of a moving level."""
+        err, scale = _c_double(), _c_double()
+        _abi.check(_lib().fp_gcl_check(self._h, level, int(time_scheme), ctypes.byref(err), ctypes.byref(scale)),
+                   "fp_gcl_check")
+        return err.value, scale.value
+
     def with_level1_geometry(self, side_w, bnd_w, volume):
         """Level descriptors of this mesh with level 1's side_w, bnd_w and
         volume replaced (the arrays are kept alive by the returned object,
@@ -148,7 +168,9 @@ class Mesh:
             "bnd_w": (d.bnd_w, np.float64, (3, b)), "node_reg": (d.node_reg, np.int32, (21,)),
             "node_ind": (d.node_ind, np.int32, (d.n_normals,)),
             "volume": (d.volume, np.float64, (n,)), "wall_dist": (d.wall_dist, np.float64, (n,)),
-            "coords": (d.coords, np.float64, (3, n)),
+            "coords": (d.coords, np.float64, (3, n)), "coord_move": (d.coord_move, np.float64, (3, n)),
+            "side_gcl": (d.side_gcl, np.float64, (2, e)), "bnd_gcl": (d.bnd_gcl, np.float64, (4, b)),
+            "volume_prev": (d.volume_prev, np.float64, (n,)), "volume_prev2": (d.volume_prev2, np.float64, (n,)),
         }
         if level > 1:
             nf = self.level(level - 1).n_nodes

@@ -155,6 +155,11 @@ class Solver:
         u) and open the next one (viscosity reset, restrictions)."""
         self._ck(self.be.next_physical_step(self._h), "next_physical_step")
 
+    def update_geometry(self, mesh):
+        """Moving meshes (flowType 2): take the geometry the mesh now holds
+        (after Mesh.set_moving) for the physical step just opened."""
+        self._ck(self.be.update_geometry(self._h, mesh.nlevels, mesh.descs), "update_geometry")
+
     def do_time_iterations(self, level, nsteps=1, calc_diss=True, cycle=1, calc_turb=True):
         self._ck(self.be.do_time_iterations(self._h, level, nsteps, int(calc_diss), int(calc_turb), cycle),
                  "do_time_iterations")

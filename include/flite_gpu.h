@@ -134,6 +134,12 @@ typedef struct flite_level_desc {
     const double  *coord_move;  /* [3][N] coordinateMovement (NULL = zero)    */
     const int32_t *parent;      /* [N_finer] prolongationArray (levels >= 2)  */
     const double  *rweight;     /* [N_finer] restrictionArray  (levels >= 2)  */
+    /* moving meshes (flowType 2; NULL = static mesh): the records of the
+     * step's .sol (def_par:800-818, 13855-13899)                             */
+    const double  *side_gcl;    /* [2][E] GCLWeightsArray, the previous step's */
+    const double  *bnd_gcl;     /* [4][B] brp%GCLWeightsArray(B,1:2), previous */
+    const double  *volume_prev; /* [N]    nodeVolumeP  (level 1)              */
+    const double  *volume_prev2;/* [N]    nodeVolumeP2 (level 1)              */
 } flite_level_desc;
 
 typedef struct flite_ctx flite_ctx;
@@ -172,7 +178,8 @@ int flite_start(flite_ctx *ctx);
 
 /* ---- solver steps (one per replaced Fortran call) --------------------- */
 /* doTimeIterations (def_par:966-1000)                                     */
-/* Unsteady runs (flowType 1, dual time on a static mesh): between physical
+/* Unsteady runs (flowType 1 on a static mesh, 2 on a moving one; dual
+ * time): between physical
  * time steps of multiGridCycles (mg_par:483-890), uold2 = uold and uold = u
  * on level 1, then the head of the next step: laminar viscosity 1/Re on
  * every level, u and uold restricted to every coarse level (mg_par:586-602).
@@ -181,9 +188,27 @@ int flite_start(flite_ctx *ctx);
  * (def_par:1184-1241: second-order backward on level 1 with timeScheme 2,
  * first order elsewhere; for nu~ before its convection) and solveSystem
  * divides the local step by 1 + 1.5 dt / physicalTimeStep (def_par:
- * 1427-1442; solveTurbulenceSystem does not).  The mesh is static: the
+ * 1427-1442; solveTurbulenceSystem does not).  On a static mesh the
  * previous volumes are the volumes.                                         */
 int flite_next_physical_step(flite_ctx *ctx);
+/* Moving meshes (flowType 2, ALE): the geometry of the next physical step,
+ * read from that step's .sol (mg_par:525-545, readComputationData with the
+ * arrays already allocated).  Called after flite_next_physical_step; the
+ * levels must have the topology given to flite_create (sizes, side and
+ * boundary-side indices, indicators, transfer operators' parents); their
+ * coefficients, GCL weights, volumes (current and the two previous), wall
+ * distances, coordinates, coordinate movements and restriction weights are
+ * taken.  On level 1 with timeScheme 2 the GCL weights are combined as
+ * 1.5 GCL - 0.5 GCLprev (def_par:816-818, 13858-13860).  The head of the
+ * step (laminar viscosity, u and uold restricted to the coarse levels) is
+ * redone with the new restriction weights.  The GCL terms enter every
+ * interior-edge flux as -(q1 + q2) GCL/physicalTimeStep (the HLLC flux:
+ * -q* GCL/physicalTimeStep with the state of its wave region, def_par:
+ * 2046-2085) and every boundary edge as -(3 q1 + q2) GCL1/physicalTimeStep
+ * and -(q1 + 3 q2) GCL2/physicalTimeStep (boundaryTerm 2: -4 q GCL/
+ * physicalTimeStep; def_par:2124-2177), and the time differences use the
+ * current and previous volumes (def_par:1184-1241).                         */
+int flite_update_geometry(flite_ctx *ctx, int nlevels, const flite_level_desc *levels);
 int flite_do_time_iterations(flite_ctx *ctx, int level, int nsteps,
                              int calc_diss, int calc_turb, int cycle_no);
 /* restrictGrid (def_par:12141-12430)                                      */
@@ -217,7 +242,8 @@ int flite_residual_fwd(flite_ctx *ctx, int level, const double *u, double *r);
  * fluxType 1, FP64; wall, symmetry and far-field boundary fluxes), the
  * backward half of the forward/backward pair.  u, rbar, ubar are [5][N].
  * Like flite_residual_fwd it replaces the level's state by u.  No reference
- * counterpart: the reference has no adjoint.                               */
+ * counterpart: the reference has no adjoint.  Moving meshes (flowType 2):
+ * FLITE_EUNSUPPORTED.                                                      */
 int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, const double *rbar,
                        double *ubar);
 /* average device ms of one forward residual evaluation and of one adjoint

@@ -66,6 +66,8 @@ module flite_gpu
     integer(c_int32_t) :: n_nodes, n_sides, n_bsides, n_bnodes, n_normals
     type(c_ptr) :: side_idx, side_w, side_len, bnd_idx, bnd_w, node_reg, node_ind
     type(c_ptr) :: volume, wall_dist, coords, coord_move, parent, rweight
+    ! moving meshes (flowType 2): GCL weights and previous volumes
+    type(c_ptr) :: side_gcl, bnd_gcl, volume_prev, volume_prev2
   end type flite_level_desc
 
   interface
@@ -129,6 +131,15 @@ module flite_gpu
     integer(c_int) function flite_next_physical_step(ctx) bind(C, name="flite_next_physical_step")
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
+    end function
+
+    ! the geometry of the next physical step of a moving mesh (flowType 2),
+    ! in place of readComputationData(COMPINFILE, 1) (mg_par:525-545)
+    integer(c_int) function flite_update_geometry(ctx, nlevels, levels) bind(C, name="flite_update_geometry")
+      import :: c_int, c_ptr, flite_level_desc
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nlevels
+      type(flite_level_desc), intent(in) :: levels(*)
     end function
 
     ! doTimeIterations (def_par:966-1000)

@@ -64,6 +64,34 @@ int fp_geometry(const fp_mesh *m, const double *xyz, double *side_w, double *bnd
  * (d(side_w, bnd_w, volume)/d xyz)^T (side_w_bar, bnd_w_bar, volume_bar).   */
 int fp_geometry_vjp(const fp_mesh *m, const double *xyz, const double *side_w_bar, const double *bnd_w_bar,
                     const double *volume_bar, double *xyz_bar);
+/* Moving meshes (flowType 2): the arrays gen3d writes into a physical step's
+ * .sol, from the node coordinates of the step, xyz, and of the two steps
+ * before, xyz_prev and xyz_prev2 ([3][N], boundary-first numbering).  Level
+ * 1 takes the coefficients, volumes at the three steps and GCL weights of the
+ * mesh's own elements (makeCalcDataForTet / registerSideGCL gen3d_grid.f90:
+ * 786-855, 2092-2332; makeCalcDataForBoundary / registerBoundarySideGCL
+ * gen3d_boundary.f90:289-372, 511-766): per side the swept volume of its
+ * dual faces between the step and the one before (GCL) and between the two
+ * before (GCLprev), per boundary side those of each of its nodes; the side
+ * lengths and coordinates of the step and the coordinate movement of the
+ * solver's reader for time_scheme 1 or 2 (def_par:13896-13900).  Coarse
+ * levels sum them through the agglomeration (restriction weights from the
+ * new volumes).  The level descriptors then carry side_gcl, bnd_gcl,
+ * volume_prev, volume_prev2 and coord_move.  Three equal coordinate sets give
+ * the static arrays back bit for bit with zero GCL weights.                 */
+int fp_set_moving_geometry(fp_mesh *m, const double *xyz, const double *xyz_prev, const double *xyz_prev2,
+                           int32_t time_scheme);
+/* The level-1 coordinate movement of the solver's reader from the
+ * coordinates of the step and of the two before (a mesh read from a moving
+ * .sol holds all three).                                                    */
+int fp_coordinate_movement(fp_mesh *m, int32_t time_scheme);
+/* The discrete geometric conservation law of a moving level, as the solver
+ * checks it (def_par:14590-14703): per node the sum over its sides of
+ * +-2 GCL and over its boundary sides of 4 GCL (with time_scheme 2 the
+ * weights 1.5 GCL - 0.5 GCLprev) against V - Vprev (time_scheme 1) or
+ * 1.5 V - 2 Vprev + 0.5 Vprev2; *err is the largest difference, *scale the
+ * largest volume change.                                                    */
+int fp_gcl_check(const fp_mesh *m, int level, int32_t time_scheme, double *err, double *scale);
 
 /* ---- files (Fortran sequential unformatted, 4-byte record markers) ---- */
 int fp_write_sol(const fp_mesh *m, const char *path);

@@ -47,6 +47,10 @@ struct Level {
     int reg[21];
     std::vector<int> node_ind;  // 0-based node numbers
     vec V, wdist, cx, cy, cz, cmx, cmy, cmz;
+    // moving meshes (flowType 2): GCLWeightsArray of the sides and of the
+    // boundary sides' two nodes as the reader leaves them (combined for
+    // timeScheme 2 on level 1), and the previous volumes (level 1)
+    vec gcl, bgcl1, bgcl2, Vp, Vp2;
     std::vector<int> parent;  // [N_finer], 0-based coarse node or -1
     vec rweight;
     // state
@@ -1038,12 +1042,20 @@ struct Oracle {
             double E2 = g.u[4][i2], rh2 = g.u[4][i2] + pr2;
             double wx = g.wx[e], wy = g.wy[e], wz = g.wz[e];
             double f[5] = {0, 0, 0, 0, 0};
+            // the GCL term of a moving mesh, -q wgcl (def_par:1662-1791)
+            const bool ale = c.flowType == 2;
+            const double wgcl = ale ? g.gcl[e] / c.physicalTimeStep : 0.0;
+            auto gcl_sum = [&]() {
+                f[0] = f[0] - (r1 + r2) * wgcl; f[1] = f[1] - (ru1 + ru2) * wgcl; f[2] = f[2] - (rv1 + rv2) * wgcl;
+                f[3] = f[3] - (rw1 + rw2) * wgcl; f[4] = f[4] - (E1 + E2) * wgcl;
+            };
             if (c.fluxType == 1) {
                 f[0] = (wx * (ru1 + ru2) + wy * (rv1 + rv2)) + wz * (rw1 + rw2);
                 f[1] = (wx * (((ru1 * u1 + pr1) + ru2 * u2) + pr2) + wy * (ru1 * v1 + ru2 * v2)) + wz * (ru1 * w1 + ru2 * w2);
                 f[2] = (wx * (rv1 * u1 + rv2 * u2) + wy * (((rv1 * v1 + pr1) + rv2 * v2) + pr2)) + wz * (rv1 * w1 + rv2 * w2);
                 f[3] = (wx * (rw1 * u1 + rw2 * u2) + wy * (rw1 * v1 + rw2 * v2)) + wz * (((rw1 * w1 + pr1) + rw2 * w2) + pr2);
                 f[4] = (wx * (rh1 * u1 + rh2 * u2) + wy * (rh1 * v1 + rh2 * v2)) + wz * (rh1 * w1 + rh2 * w2);
+                if (ale) gcl_sum();
             } else if (c.fluxType == 2) {  // LLF (def_par:1670-1724)
                 double rnorm = std::sqrt((wx * wx + wy * wy) + wz * wz);
                 if (rnorm > 1.0e-10) {
@@ -1067,6 +1079,7 @@ struct Oracle {
                     f[2] = rnorm * ((f31 + f32) - lam * du[2]);
                     f[3] = rnorm * ((f41 + f42) - lam * du[3]);
                     f[4] = rnorm * ((f51 + f52) - lam * du[4]);
+                    if (ale) gcl_sum();
                 }
             } else if (c.fluxType == 3 && muscl) {
                 muscl_roe_flux(g, i1, i2, wx, wy, wz, f);
@@ -1108,6 +1121,7 @@ struct Oracle {
                     f[2] = rnorm * ((f31 + f32) - ((l3 * du3 + cc1 * vi) + cc2 * rny));
                     f[3] = rnorm * ((f41 + f42) - ((l3 * du4 + cc1 * wi) + cc2 * rnz));
                     f[4] = rnorm * ((f51 + f52) - ((l3 * du5 + cc1 * hi) + cc2 * ucp));
+                    if (ale) gcl_sum();
                 }
             } else {  // HLLC (def_par:1794-2085)
                 // central flux of the unreconstructed states (def_par:1798-
@@ -1215,25 +1229,50 @@ struct Oracle {
                     rs[0] = roe2; rs[1] = ru2; rs[2] = rv2; rs[3] = rw2; rs[4] = re2;
                 }
                 double L0[5] = {roe1, ru1, rv1, rw1, re1}, R0[5] = {roe2, ru2, rv2, rw2, re2};
+                // the state of the GCL term: r, E of the node and the
+                // (reconstructed) momentum outside the star region, the star
+                // state inside it (def_par:2046-2085)
+                double q[5] = {r1, ru1, rv1, rw1, E1};
                 if (sl > 0.0) {
                     for (int k = 0; k < 5; ++k) f[k] = fl[k] * rnorm1;
                 } else if (sl <= 0.0 && sm > 0.0) {
                     for (int k = 0; k < 5; ++k) f[k] = (fl[k] + sl * (ls[k] - L0[k])) * rnorm1;
+                    for (int k = 0; k < 5; ++k) q[k] = ls[k];
                 } else if (sm <= 0.0 && sr >= 0.0) {
                     for (int k = 0; k < 5; ++k) f[k] = (fr[k] + sr * (rs[k] - R0[k])) * rnorm1;
+                    for (int k = 0; k < 5; ++k) q[k] = rs[k];
                 } else if (sr < 0.0) {
                     for (int k = 0; k < 5; ++k) f[k] = fr[k] * rnorm1;
+                    q[0] = r2; q[1] = ru2; q[2] = rv2; q[3] = rw2; q[4] = E2;
                 }
+                if (ale)
+                    for (int k = 0; k < 5; ++k) f[k] = f[k] - q[k] * wgcl;
             }
             for (int k = 0; k < 5; ++k) {
                 g.rhs[k][i1] = g.rhs[k][i1] + f[k];
                 g.rhs[k][i2] = g.rhs[k][i2] - f[k];
             }
         });
-        // boundary faces (def_par:2116-2512); the GCL terms vanish for the
-        // static meshes this path accepts
+        // boundary faces (def_par:2116-2512), after the GCL terms of each
+        // boundary side (def_par:2124-2177; moving meshes)
+        const bool ale = c.flowType == 2;
         for_bedges(g, [&](int b) {
             const int i1 = g.b1[b], i2 = g.b2[b], ind = g.bind[b];
+            if (ale) {
+                const double q1[5] = {g.u[0][i1], g.u[1][i1], g.u[2][i1], g.u[3][i1], g.u[4][i1]};
+                const double q2[5] = {g.u[0][i2], g.u[1][i2], g.u[2][i2], g.u[3][i2], g.u[4][i2]};
+                if (c.boundaryTerm == 1) {
+                    double wgcl = g.bgcl1[b] / c.physicalTimeStep;
+                    for (int k = 0; k < 5; ++k) g.rhs[k][i1] = g.rhs[k][i1] - (3. * q1[k] + q2[k]) * wgcl;
+                    wgcl = g.bgcl2[b] / c.physicalTimeStep;
+                    for (int k = 0; k < 5; ++k) g.rhs[k][i2] = g.rhs[k][i2] - (q1[k] + 3. * q2[k]) * wgcl;
+                } else {
+                    double wgcl = 4.0 * g.bgcl1[b] / c.physicalTimeStep;
+                    for (int k = 0; k < 5; ++k) g.rhs[k][i1] = g.rhs[k][i1] - q1[k] * wgcl;
+                    wgcl = 4.0 * g.bgcl2[b] / c.physicalTimeStep;
+                    for (int k = 0; k < 5; ++k) g.rhs[k][i2] = g.rhs[k][i2] - q2[k] * wgcl;
+                }
+            }
             double g1[5], g2[5];
             boundary_flux(g, i1, i2, ind, g.bwx[b], g.bwy[b], g.bwz[b], g1, g2);
             for (int k = 0; k < 5; ++k) g.rhs[k][i1] = g.rhs[k][i1] + g1[k];
@@ -1699,16 +1738,17 @@ struct Oracle {
         else makeArtificialDissipation2(g);
     }
 
-    // ---- addTimeDifferences (def_par:1184-1241), static mesh: the previous
-    // volumes are the volumes -------------------------------------------------
+    // ---- addTimeDifferences (def_par:1184-1241): on a static mesh the
+    // previous volumes are the volumes ----------------------------------------
     void addTimeDifferences(Level &g) {
         if (c.flowType == 0) return;
         const double dtp = c.physicalTimeStep;
         if (g.grid == 1 && c.timeScheme == 2) {
+            const vec &Vp = c.flowType == 2 ? g.Vp : g.V, &Vp2 = c.flowType == 2 ? g.Vp2 : g.V;
             for (int i = 0; i < g.N; ++i)
                 for (int k = 0; k < nvar; ++k)
-                    g.rhs[k][i] = g.rhs[k][i] + (((1.5 * g.V[i]) * g.u[k][i] - (2.0 * g.V[i]) * g.uold[k][i]) +
-                                                 (0.5 * g.V[i]) * g.uold2[k][i]) / dtp;
+                    g.rhs[k][i] = g.rhs[k][i] + (((1.5 * g.V[i]) * g.u[k][i] - (2.0 * Vp[i]) * g.uold[k][i]) +
+                                                 (0.5 * Vp2[i]) * g.uold2[k][i]) / dtp;
         } else {
             for (int i = 0; i < g.N; ++i)
                 for (int k = 0; k < nvar; ++k)
@@ -2099,9 +2139,10 @@ struct Oracle {
 };
 
 int check_controls(const flite_controls &c) {
-    // flowType 1: dual time on a static mesh
-    if (c.flowType == 1 && !(c.physicalTimeStep > 0)) return FLITE_EUNSUPPORTED;
-    if ((c.flowType != 0 && c.flowType != 1) || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
+    // flowType 1: dual time on a static mesh; 2: on a moving mesh
+    if (c.flowType != 0 && !(c.physicalTimeStep > 0)) return FLITE_EUNSUPPORTED;
+    if (c.flowType == 2 && c.reconstruction != FLITE_RECON_NONE) return FLITE_EUNSUPPORTED;
+    if ((c.flowType != 0 && c.flowType != 1 && c.flowType != 2) || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
         c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
         c.prolongationSmoothingFactor > 0)
         return FLITE_EUNSUPPORTED;
@@ -2714,6 +2755,59 @@ struct oracle_ctx {
     Oracle o;
 };
 
+// The geometry of a level from its descriptor (readGridComputationData,
+// def_par:13812-14074): coefficients, side lengths, volumes, wall distances,
+// coordinates and their movement, restriction weights, the normals, wall
+// area and connectivity derived from them; for a moving mesh the GCL
+// weights, combined as 1.5 GCL - 0.5 GCLprev on level 1 with timeScheme 2
+// (def_par:816-818, 13858-13860), and the previous volumes.
+static int load_geometry(Oracle &o, Level &g, int l, const flite_level_desc &d) {
+    const size_t E = g.E, B = g.B, N = g.N;
+    g.wx.resize(E); g.wy.resize(E); g.wz.resize(E); g.slen.assign(E, 0.0);
+    for (size_t e = 0; e < E; ++e) {
+        g.wx[e] = d.side_w[e]; g.wy[e] = d.side_w[E + e]; g.wz[e] = d.side_w[2 * E + e];
+        if (d.side_len) g.slen[e] = d.side_len[e];
+    }
+    g.bwx.resize(B); g.bwy.resize(B); g.bwz.resize(B);
+    for (size_t b = 0; b < B; ++b) {
+        g.bwx[b] = d.bnd_w[b]; g.bwy[b] = d.bnd_w[B + b]; g.bwz[b] = d.bnd_w[2 * B + b];
+    }
+    g.V.assign(d.volume, d.volume + N);
+    g.wdist.assign(N, 0.0);
+    if (d.wall_dist) g.wdist.assign(d.wall_dist, d.wall_dist + N);
+    g.cx.assign(N, 0.0); g.cy.assign(N, 0.0); g.cz.assign(N, 0.0);
+    if (l == 0 && d.coords)
+        for (size_t i = 0; i < N; ++i) {
+            g.cx[i] = d.coords[i]; g.cy[i] = d.coords[N + i]; g.cz[i] = d.coords[2 * N + i];
+        }
+    g.cmx.assign(N, 0.0); g.cmy.assign(N, 0.0); g.cmz.assign(N, 0.0);
+    if (l == 0 && d.coord_move)
+        for (size_t i = 0; i < N; ++i) {
+            g.cmx[i] = d.coord_move[i]; g.cmy[i] = d.coord_move[N + i]; g.cmz[i] = d.coord_move[2 * N + i];
+        }
+    if (l > 0) {
+        if (!d.rweight) return FLITE_EINVAL;
+        g.rweight.assign(d.rweight, d.rweight + o.lv[l - 1].N);
+    }
+    if (o.c.flowType == 2) {
+        if (!d.side_gcl || !d.bnd_gcl || (l == 0 && (!d.volume_prev || !d.volume_prev2))) return FLITE_EINVAL;
+        const bool comb = l == 0 && o.c.timeScheme == 2;
+        auto w = [&](double x, double xp) { return comb ? 1.5 * x - 0.5 * xp : x; };
+        g.gcl.resize(E); g.bgcl1.resize(B); g.bgcl2.resize(B);
+        for (size_t e = 0; e < E; ++e) g.gcl[e] = w(d.side_gcl[e], d.side_gcl[E + e]);
+        for (size_t b = 0; b < B; ++b) {
+            g.bgcl1[b] = w(d.bnd_gcl[b], d.bnd_gcl[2 * B + b]);
+            g.bgcl2[b] = w(d.bnd_gcl[B + b], d.bnd_gcl[3 * B + b]);
+        }
+        if (l == 0) {
+            g.Vp.assign(d.volume_prev, d.volume_prev + N);
+            g.Vp2.assign(d.volume_prev2, d.volume_prev2 + N);
+        }
+    }
+    o.setup_level(g);
+    return FLITE_OK;
+}
+
 extern "C" {
 
 int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *lv, oracle_ctx **out) {
@@ -2734,46 +2828,27 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
         g.grid = l + 1;
         g.N = d.n_nodes; g.E = d.n_sides; g.B = d.n_bsides; g.Nb = d.n_bnodes; g.nnorm = d.n_normals;
         g.s1.resize(g.E); g.s2.resize(g.E);
-        g.wx.resize(g.E); g.wy.resize(g.E); g.wz.resize(g.E); g.slen.assign(g.E, 0.0);
         for (int e = 0; e < g.E; ++e) {
             g.s1[e] = d.side_idx[e] - 1; g.s2[e] = d.side_idx[(size_t)g.E + e] - 1;
-            g.wx[e] = d.side_w[e]; g.wy[e] = d.side_w[(size_t)g.E + e]; g.wz[e] = d.side_w[2 * (size_t)g.E + e];
-            if (d.side_len) g.slen[e] = d.side_len[e];
         }
         g.b1.resize(g.B); g.b2.resize(g.B); g.bind.resize(g.B);
-        g.bwx.resize(g.B); g.bwy.resize(g.B); g.bwz.resize(g.B);
         for (int b = 0; b < g.B; ++b) {
             g.b1[b] = d.bnd_idx[b] - 1; g.b2[b] = d.bnd_idx[(size_t)g.B + b] - 1;
             g.bind[b] = d.bnd_idx[2 * (size_t)g.B + b];
             if (g.bind[b] >= 5 && g.bind[b] <= 8) return FLITE_EUNSUPPORTED;
-            g.bwx[b] = d.bnd_w[b]; g.bwy[b] = d.bnd_w[(size_t)g.B + b]; g.bwz[b] = d.bnd_w[2 * (size_t)g.B + b];
         }
         std::memcpy(g.reg, d.node_reg, sizeof g.reg);
         for (int r = -12; r <= -5; r += 2)
             if (g.R(r + 1) >= g.R(r)) return FLITE_EUNSUPPORTED;  // engine nodes
         g.node_ind.resize(g.nnorm);
         for (int i = 0; i < g.nnorm; ++i) g.node_ind[i] = d.node_ind[i] - 1;
-        g.V.assign(d.volume, d.volume + g.N);
-        g.wdist.assign(g.N, 0.0);
-        if (d.wall_dist) g.wdist.assign(d.wall_dist, d.wall_dist + g.N);
-        g.cx.assign(g.N, 0.0); g.cy.assign(g.N, 0.0); g.cz.assign(g.N, 0.0);
-        if (l == 0 && d.coords) {
-            for (int i = 0; i < g.N; ++i) {
-                g.cx[i] = d.coords[i]; g.cy[i] = d.coords[(size_t)g.N + i]; g.cz[i] = d.coords[2 * (size_t)g.N + i];
-            }
-        }
-        g.cmx.assign(g.N, 0.0); g.cmy.assign(g.N, 0.0); g.cmz.assign(g.N, 0.0);
-        if (l == 0 && d.coord_move)
-            for (int i = 0; i < g.N; ++i) {
-                g.cmx[i] = d.coord_move[i]; g.cmy[i] = d.coord_move[(size_t)g.N + i];
-                g.cmz[i] = d.coord_move[2 * (size_t)g.N + i];
-            }
         if (l > 0) {
             int nf = o.lv[l - 1].N;
             if (!d.parent || !d.rweight) return FLITE_EINVAL;
-            g.parent.resize(nf); g.rweight.assign(d.rweight, d.rweight + nf);
+            g.parent.resize(nf);
             for (int i = 0; i < nf; ++i) g.parent[i] = d.parent[i] - 1;
         }
+        if (int rc = load_geometry(o, g, l, d)) return rc;
         for (int k = 0; k < 6; ++k) {
             g.u[k].assign(g.N, 0.0); g.uprev[k].assign(g.N, 0.0); g.rhs[k].assign(g.N, 0.0);
             g.src[k].assign(g.N, 0.0);
@@ -2784,7 +2859,6 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
         g.turbDiff.assign(g.N, 0.0); g.dtT.assign(g.N, 0.0); g.vort.assign(g.N, 0.0); g.divg.assign(g.N, 0.0);
         for (int k = 0; k < 3; ++k) g.wallStress[k].assign(g.N, 0.0);
         g.cycleNumber = l == 0 ? 1 : 0;
-        o.setup_level(g);
     }
     o.nh.assign(25, vec(o.lv[0].N, 0.0));
     *out = ctx.release();
@@ -2892,6 +2966,19 @@ int oracle_next_physical_step(oracle_ctx *o) {
     Level &g = O.lv[0];
     for (int k = 0; k < O.nvar; ++k) { g.uold2[k] = g.uold[k]; g.uold[k] = g.u[k]; }  // mg_par:889-890
     physical_step_head(O);
+    return FLITE_OK;
+}
+
+int oracle_update_geometry(oracle_ctx *o, int nlevels, const flite_level_desc *lv) {
+    if (!o || !lv || o->o.c.flowType != 2 || nlevels < (int)o->o.lv.size()) return FLITE_EINVAL;
+    Oracle &O = o->o;
+    for (size_t l = 0; l < O.lv.size(); ++l) {
+        Level &g = O.lv[l];
+        const flite_level_desc &d = lv[l];
+        if (d.n_nodes != g.N || d.n_sides != g.E || d.n_bsides != g.B) return FLITE_EINVAL;
+        if (int rc = load_geometry(O, g, (int)l, d)) return rc;
+    }
+    physical_step_head(O);  // again, with the new restriction weights
     return FLITE_OK;
 }
 

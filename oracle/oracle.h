@@ -38,6 +38,7 @@ int oracle_map_fine_to_coarse(oracle_ctx *o, int fine_level);
 int oracle_cycle(oracle_ctx *o, int cycle_no);
 /* unsteady runs: close the physical time step, open the next one          */
 int oracle_next_physical_step(oracle_ctx *o);
+int oracle_update_geometry(oracle_ctx *o, int nlevels, const flite_level_desc *levels);
 int oracle_residuals(oracle_ctx *o, double res[7], double maxres[7], int maxind[7]);
 int oracle_forces(oracle_ctx *o, double out[9]);
 int oracle_residual_fwd(oracle_ctx *o, int level, const double *u, double *r);

@@ -30,7 +30,7 @@ def test_prepro_library_exports_header():
 
 def test_struct_sizes_match_c():
     # sizeof(flite_controls) and sizeof(flite_level_desc) as compiled
-    assert ctypes.sizeof(_abi.LevelDesc) == 5 * 4 + 4 + 13 * 8
+    assert ctypes.sizeof(_abi.LevelDesc) == 5 * 4 + 4 + 17 * 8
 
 
 def test_create_rejects_unsupported_controls():
@@ -38,7 +38,8 @@ def test_create_rejects_unsupported_controls():
     m = Mesh.bump_channel(4, 2, 2, 0.05, nlevels=1)
     lib = _abi.gpu_lib()
     h = ctypes.c_void_p()
-    for bad in (dict(flowType=2), dict(turbulenceModel=2), dict(movingwall=1),
+    for bad in (dict(flowType=3), dict(flowType=2, physicalTimeStep=0.1, precision=1), dict(turbulenceModel=2),
+                dict(movingwall=1),
                 dict(ReynoldsNumber=0.0, multigridScheme=6)):
         c = default_controls(**bad)
         rc = lib.flite_create(ctypes.byref(c), m.nlevels, m.descs, ctypes.byref(h))

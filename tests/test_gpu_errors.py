@@ -47,7 +47,10 @@ def test_out_of_range_indices_are_rejected(field, fn):
 
 
 @pytest.mark.parametrize("ctl,cpu_refuses", [
-    (dict(turbulenceModel=2), True), (dict(flowType=2), True),
+    (dict(turbulenceModel=2), True), (dict(flowType=3), True), (dict(flowType=2, physicalTimeStep=0.0), True),
+    # moving meshes take the reference's fluxes, in FP64
+    (dict(flowType=2, physicalTimeStep=0.1, reconstruction=1, fluxType=3), True),
+    (dict(flowType=2, physicalTimeStep=0.1, precision=1), False),
     (dict(flowType=1, physicalTimeStep=0.0), True),
     (dict(viscosityScheme=3, ReynoldsNumber=100.0), True), (dict(coarseGridDissipationScheme=1), True),
     (dict(forceCalcType=2), True),
