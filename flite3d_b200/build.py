@@ -57,7 +57,7 @@ def _sources(dirname, exts):
 
 def build_prepro(force=False, verbose=False):
     # the controls defaults are compiled in as fp_controls_default/derive
-    src = [os.path.join(CSRC, "prepro", f) for f in ("prepro.cpp", "namelist.cpp", "text_io.cpp")] + \
+    src = [os.path.join(CSRC, "prepro", f) for f in ("prepro.cpp", "domains.cpp", "namelist.cpp", "text_io.cpp")] + \
         [os.path.join(CSRC, "solver", "controls.cpp")]
     deps = src + _sources(os.path.join(CSRC, "prepro"), {".hpp", ".h"}) + _sources(INC, {".h"})
     out = os.path.join(PKG, "libflite_prepro.so")

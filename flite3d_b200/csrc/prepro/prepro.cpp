@@ -5,7 +5,7 @@
 // What follows the reference step by step (file:line in PreProSource/):
 //   * median-dual edge coefficients and nodal volumes of a tetrahedron:
 //     makeCalcDataForTet gen3d_grid.f90:2092-2332 with registerSideGCL
-//     :786-855 (static mesh: the GCL terms vanish and are written as 0);
+//     :786-855 (a static mesh's GCL terms vanish and are written as 0);
 //   * edge registration with i1<i2 orientation and coefficient summation:
 //     registerSideData gen3d_struct.f90:366-464;
 //   * boundary-edge coefficients of a triangle: makeCalcDataForBoundary
@@ -19,7 +19,13 @@
 //     self-edges of one coarse node: agglomerateBoundary gen3d_boundary.f90:
 //     922-1023; coarse node indicators by the same priority :1101-1121;
 //   * coarse volumes as sums of fine volumes (mergeNodes gen3d_grid.f90:
-//     2822-2829) and restriction weights V_f/V_c.
+//     2822-2829) and restriction weights V_f/V_c; coarse wall distances as
+//     the children's volume-weighted mean (makeDistanceFieldsForCoarseMesh
+//     :5823-5846);
+//   * moving meshes: makeCalcDataForTet / registerSideGCL with three
+//     coordinate levels and makeCalcDataForBoundary / registerBoundarySideGCL
+//     (GCL weights of the step and of the step before), coarse levels by
+//     summation (fp_set_moving_geometry).
 // The seed selection of the agglomeration is this project's own greedy
 // scheme (largest available connectivity first, boundary nodes before
 // interior nodes, all free neighbours merged, single-node aggregates merged
@@ -43,49 +49,9 @@
 #include "flite_prepro.h"
 #include "fortran_io.hpp"
 
-namespace {
+#include "mesh_data.h"
 
-struct LevelData {
-    int32_t N = 0, E = 0, B = 0, Nb = 0;
-    std::vector<int32_t> side;   // [2][E] column-major, 1-based
-    std::vector<double> sw;      // [3][E]
-    std::vector<double> slen;    // [E]
-    std::vector<int32_t> bside;  // [3][B] (i1, i2, indicator)
-    std::vector<double> bw;      // [3][B]
-    int32_t reg[21] = {0};       // nodeIndicatorRegister(-20:0)
-    std::vector<int32_t> node_ind;
-    std::vector<double> bnormal;  // [3][n_normals]
-    std::vector<int32_t> bnd_indicator;  // [Nb] indicator per boundary node
-    std::vector<double> vol, wdist;
-    std::vector<int32_t> wnode;
-    std::vector<double> xyz;      // [3][N] (level 1 only)
-    std::vector<int32_t> seed;    // [N] (coarse levels)
-    std::vector<int32_t> parent;  // [N_finer] (coarse levels)
-    std::vector<double> rweight;  // [N_finer]
-    // moving meshes (fp_set_moving_geometry): the GCL weights of the step and
-    // of the step before, the volumes at the two previous steps and the
-    // coordinate movement (level 1)
-    std::vector<double> gcl;         // [2][E]
-    std::vector<double> bgcl;        // [4][B] (GCL(1), GCL(2), GCLP(1), GCLP(2))
-    std::vector<double> volp, volp2;  // [N]
-    std::vector<double> cmove;       // [3][N]
-    std::vector<double> xyzp, xyzp2;  // [3][N] coordinates at the two previous steps
-    // coarse levels: the coarse side of each finer side (1-based, negative
-    // where the finer side runs the other way, 0 inside an aggregate) and
-    // the coarse boundary side of each finer one (negative where its two
-    // nodes swap)
-    std::vector<int32_t> side_of, bside_of;
-};
-
-}  // namespace
-
-struct fp_mesh {
-    std::vector<LevelData> lv;
-    std::vector<int32_t> perm;    // new -> old, 1-based
-    std::vector<int32_t> tets;    // [4][ntet] new numbering
-    std::vector<int32_t> tris;    // [3][ntri]
-    std::vector<int32_t> tri_ind;
-};
+using fp_internal::LevelData;
 
 namespace {
 
@@ -382,42 +348,6 @@ inline int merge_indicator(int cur, int nw) {
 
 // Register and node list from per-boundary-node indicators (gen3d_grid.f90:
 // 4548-4580): counts at -21+2k, then running (start, end) pairs.
-void build_register(LevelData &L) {
-    int32_t r[21] = {0};
-    auto R = [&](int i) -> int32_t & { return r[i + 20]; };
-    for (int j = 0; j < L.Nb; ++j) {
-        int ind = L.bnd_indicator[j];
-        if (ind > 0) R(-21 + ind * 2) += 1;
-    }
-    R(-20) = 1;
-    for (int j = -18; j <= -2; j += 2) {
-        R(j + 1) = R(j + 1) + R(j - 1);
-        R(j) = R(j - 1) + 1;
-    }
-    std::memcpy(L.reg, r, sizeof r);
-    L.node_ind.clear();
-    std::vector<double> nrm;
-    for (int k = 1; k <= 9; ++k)
-        for (int j = 0; j < L.Nb; ++j)
-            if (L.bnd_indicator[j] == k) L.node_ind.push_back(j + 1);
-    // normals written beside each node (not read by the solver): -sum w_b
-    std::vector<double> acc(3 * (size_t)L.Nb, 0.0);
-    for (int b = 0; b < L.B; ++b) {
-        for (int s = 0; s < 2; ++s) {
-            int n = L.bside[(size_t)s * L.B + b] - 1;
-            for (int k = 0; k < 3; ++k) acc[3 * (size_t)n + k] -= L.bw[(size_t)k * L.B + b];
-        }
-    }
-    size_t nn = L.node_ind.size();
-    L.bnormal.assign(3 * nn, 0.0);
-    for (size_t i = 0; i < nn; ++i) {
-        int n = L.node_ind[i] - 1;
-        double a = acc[3 * n], b = acc[3 * n + 1], c = acc[3 * n + 2];
-        double s = std::sqrt(a * a + b * b + c * c);
-        if (s > 1e-20) { a /= s; b /= s; c /= s; } else { a = b = c = 0; }
-        L.bnormal[0 * nn + i] = a; L.bnormal[1 * nn + i] = b; L.bnormal[2 * nn + i] = c;
-    }
-}
 
 
 // k-d tree over a point subset for nearest-point queries
@@ -790,7 +720,15 @@ void agglomerate(const LevelData &F, LevelData &C) {
         if (!live[a] || seed_of[a] < 0) continue;
         int32_t c = newid[a], s = seed_of[a];
         int32_t lvl1 = F.seed.empty() ? s + 1 : F.seed[s];
-        C.seed[c] = lvl1; C.wdist[c] = F.wdist[s]; C.wnode[c] = F.wnode[s];
+        C.seed[c] = lvl1;
+    }
+    // wall distance: the children's volume-weighted mean, and the wall node:
+    // the parent of the first child's (makeDistanceFieldsForCoarseMesh
+    // gen3d_grid.f90:5823-5846)
+    for (int32_t i = 0; i < N; ++i) {
+        const int32_t c = C.parent[i] - 1;
+        C.wdist[c] = C.wdist[c] + F.vol[i] * F.wdist[i] / C.vol[c];
+        if (C.wnode[c] == 0 && F.wnode[i] >= 1) C.wnode[c] = C.parent[F.wnode[i] - 1];
     }
     // a merged single-node aggregate has no own coarse node: nothing to fix
     // coarse edges (createSides)
@@ -1058,6 +996,182 @@ int guarded(F &&f) {
 }
 
 }  // namespace
+
+// the indicator register (the layout of writeParallelComputationFiles
+// gen3d_grid.f90:4548-4580), the node list per indicator and the normals
+void fp_internal::build_register(LevelData &L) {
+    int32_t r[21] = {0};
+    auto R = [&](int i) -> int32_t & { return r[i + 20]; };
+    for (int j = 0; j < L.Nb; ++j) {
+        int ind = L.bnd_indicator[j];
+        if (ind > 0) R(-21 + ind * 2) += 1;
+    }
+    R(-20) = 1;
+    for (int j = -18; j <= -2; j += 2) {
+        R(j + 1) = R(j + 1) + R(j - 1);
+        R(j) = R(j - 1) + 1;
+    }
+    std::memcpy(L.reg, r, sizeof r);
+    L.node_ind.clear();
+    std::vector<double> nrm;
+    for (int k = 1; k <= 9; ++k)
+        for (int j = 0; j < L.Nb; ++j)
+            if (L.bnd_indicator[j] == k) L.node_ind.push_back(j + 1);
+    // normals written beside each node (not read by the solver): -sum w_b
+    std::vector<double> acc(3 * (size_t)L.Nb, 0.0);
+    for (int b = 0; b < L.B; ++b) {
+        for (int s = 0; s < 2; ++s) {
+            int n = L.bside[(size_t)s * L.B + b] - 1;
+            for (int k = 0; k < 3; ++k) acc[3 * (size_t)n + k] -= L.bw[(size_t)k * L.B + b];
+        }
+    }
+    size_t nn = L.node_ind.size();
+    L.bnormal.assign(3 * nn, 0.0);
+    for (size_t i = 0; i < nn; ++i) {
+        int n = L.node_ind[i] - 1;
+        double a = acc[3 * n], b = acc[3 * n + 1], c = acc[3 * n + 2];
+        double s = std::sqrt(a * a + b * b + c * c);
+        if (s > 1e-20) { a /= s; b /= s; c /= s; } else { a = b = c = 0; }
+        L.bnormal[0 * nn + i] = a; L.bnormal[1 * nn + i] = b; L.bnormal[2 * nn + i] = c;
+    }
+}
+
+// The canonical form of a mesh: level-1 nodes keep their numbers; every
+// level's sides run from the smaller to the larger node (a reversed side's
+// coefficients and GCL weights change sign) in node-pair order, and so do
+// the boundary sides (a reversed one's two nodes swap their GCL weights);
+// coarse nodes are numbered boundary nodes first, each class in the order
+// of their first (smallest) child; seeds become the smallest level-1
+// descendant and the wall-node numbers are dropped (the solver reads only
+// the distances).  Values are moved, never recomputed, so the canonical
+// forms of two orderings of one mesh are equal bit for bit.
+void fp_internal::canonicalize(fp_mesh &M) {
+    const size_t G = M.lv.size();
+    for (size_t l = 0; l < G; ++l) {
+        LevelData &L = M.lv[l];
+        const int32_t N = L.N, E = L.E, B = L.B;
+        std::vector<int32_t> newid(N);
+        for (int32_t j = 0; j < N; ++j) newid[j] = j;
+        if (l > 0) {
+            std::vector<int32_t> first(N, INT32_MAX);
+            const LevelData &F = M.lv[l - 1];
+            for (int32_t f = 0; f < F.N; ++f) {
+                const int32_t c = L.parent[f] - 1;
+                first[c] = std::min(first[c], f);
+            }
+            std::vector<int32_t> order(N);
+            for (int32_t j = 0; j < N; ++j) order[j] = j;
+            std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+                const int ca = a >= L.Nb, cb = b >= L.Nb;
+                return ca != cb ? ca < cb : first[a] < first[b];
+            });
+            for (int32_t k = 0; k < N; ++k) newid[order[k]] = k;
+            auto perm_d = [&](std::vector<double> &v, int ncomp) {
+                if (v.empty()) return;
+                std::vector<double> o(v.size());
+                for (int c = 0; c < ncomp; ++c)
+                    for (int32_t j = 0; j < N; ++j) o[(size_t)c * N + newid[j]] = v[(size_t)c * N + j];
+                v.swap(o);
+            };
+            perm_d(L.vol, 1); perm_d(L.wdist, 1); perm_d(L.volp, 1); perm_d(L.volp2, 1);
+            std::vector<int32_t> bi(L.bnd_indicator.size());
+            for (int32_t j = 0; j < L.Nb; ++j) bi[newid[j]] = L.bnd_indicator[j];
+            L.bnd_indicator.swap(bi);
+            for (auto &p : L.parent) p = newid[p - 1] + 1;
+            // seeds: the smallest level-1 descendant
+            L.seed.assign(N, INT32_MAX);
+            for (int32_t f = 0; f < F.N; ++f) {
+                const int32_t c = L.parent[f] - 1;
+                const int32_t s1 = l == 1 ? f + 1 : F.seed[f];
+                L.seed[c] = std::min(L.seed[c], s1);
+            }
+        }
+        if (!L.wnode.empty()) std::fill(L.wnode.begin(), L.wnode.end(), 0);
+        // the next level's arrays indexed by this level's nodes follow
+        if (l + 1 < G && l > 0) {
+            LevelData &C = M.lv[l + 1];
+            std::vector<int32_t> par(C.parent.size());
+            std::vector<double> rw(C.rweight.size());
+            for (int32_t f = 0; f < N; ++f) { par[newid[f]] = C.parent[f]; rw[newid[f]] = C.rweight[f]; }
+            C.parent.swap(par);
+            C.rweight.swap(rw);
+        }
+        // sides
+        {
+            std::vector<int32_t> a(E), b(E), ord(E);
+            std::vector<double> sg(E, 1.0);
+            for (int32_t e = 0; e < E; ++e) {
+                int32_t x = newid[L.side[e] - 1] + 1, y = newid[L.side[(size_t)E + e] - 1] + 1;
+                if (x > y) { std::swap(x, y); sg[e] = -1.0; }
+                a[e] = x; b[e] = y; ord[e] = e;
+            }
+            std::stable_sort(ord.begin(), ord.end(), [&](int32_t p, int32_t q) {
+                return a[p] != a[q] ? a[p] < a[q] : b[p] < b[q];
+            });
+            std::vector<int32_t> side(2 * (size_t)E);
+            std::vector<double> sw(3 * (size_t)E), slen(E), gcl(L.gcl.empty() ? 0 : 2 * (size_t)E);
+            for (int32_t k = 0; k < E; ++k) {
+                const int32_t e = ord[k];
+                side[k] = a[e]; side[(size_t)E + k] = b[e];
+                for (int c = 0; c < 3; ++c) sw[(size_t)c * E + k] = sg[e] * L.sw[(size_t)c * E + e];
+                slen[k] = L.slen[e];
+                if (!gcl.empty())
+                    for (int c = 0; c < 2; ++c) gcl[(size_t)c * E + k] = sg[e] * L.gcl[(size_t)c * E + e];
+            }
+            L.side.swap(side); L.sw.swap(sw); L.slen.swap(slen); L.gcl.swap(gcl);
+        }
+        // boundary sides
+        {
+            std::vector<int32_t> a(B), b(B), ord(B);
+            std::vector<char> sw(B, 0);
+            for (int32_t q = 0; q < B; ++q) {
+                int32_t x = newid[L.bside[q] - 1] + 1, y = newid[L.bside[(size_t)B + q] - 1] + 1;
+                if (x > y) { std::swap(x, y); sw[q] = 1; }
+                a[q] = x; b[q] = y; ord[q] = q;
+            }
+            std::stable_sort(ord.begin(), ord.end(), [&](int32_t p, int32_t q) {
+                return a[p] != a[q] ? a[p] < a[q] : b[p] < b[q];
+            });
+            std::vector<int32_t> bside(3 * (size_t)B);
+            std::vector<double> bw(3 * (size_t)B), bgcl(L.bgcl.empty() ? 0 : 4 * (size_t)B);
+            for (int32_t k = 0; k < B; ++k) {
+                const int32_t q = ord[k];
+                bside[k] = a[q]; bside[(size_t)B + k] = b[q]; bside[2 * (size_t)B + k] = L.bside[2 * (size_t)B + q];
+                for (int c = 0; c < 3; ++c) bw[(size_t)c * B + k] = L.bw[(size_t)c * B + q];
+                if (!bgcl.empty()) {
+                    const int from[4] = {sw[q] ? 1 : 0, sw[q] ? 0 : 1, sw[q] ? 3 : 2, sw[q] ? 2 : 3};
+                    for (int c = 0; c < 4; ++c) bgcl[(size_t)c * B + k] = L.bgcl[(size_t)from[c] * B + q];
+                }
+            }
+            L.bside.swap(bside); L.bw.swap(bw); L.bgcl.swap(bgcl);
+        }
+        build_register(L);
+    }
+    // the maps from finer to coarse sides of the canonical levels
+    for (size_t l = 1; l < G; ++l) {
+        const LevelData &F = M.lv[l - 1];
+        LevelData &C = M.lv[l];
+        std::map<std::pair<int32_t, int32_t>, int32_t> sid, bid;
+        for (int32_t e = 0; e < C.E; ++e) sid[{C.side[e], C.side[(size_t)C.E + e]}] = e;
+        for (int32_t q = 0; q < C.B; ++q) bid[{C.bside[q], C.bside[(size_t)C.B + q]}] = q;
+        C.side_of.assign(F.E, 0);
+        for (int32_t e = 0; e < F.E; ++e) {
+            const int32_t c1 = C.parent[F.side[e] - 1], c2 = C.parent[F.side[(size_t)F.E + e] - 1];
+            if (c1 == c2) continue;
+            auto it = sid.find({std::min(c1, c2), std::max(c1, c2)});
+            if (it == sid.end()) throw std::runtime_error("a side between two aggregates has no coarse side");
+            C.side_of[e] = c1 < c2 ? it->second + 1 : -(it->second + 1);
+        }
+        C.bside_of.assign(F.B, 0);
+        for (int32_t q = 0; q < F.B; ++q) {
+            const int32_t c1 = C.parent[F.bside[q] - 1], c2 = C.parent[F.bside[(size_t)F.B + q] - 1];
+            auto it = bid.find({std::min(c1, c2), std::max(c1, c2)});
+            if (it == bid.end()) throw std::runtime_error("a boundary side has no coarse boundary side");
+            C.bside_of[q] = c1 > c2 ? -(it->second + 1) : it->second + 1;
+        }
+    }
+}
+
 
 // ===========================================================================
 extern "C" {
@@ -1428,6 +1542,17 @@ int fp_gcl_check(const fp_mesh *m, int level, int32_t time_scheme, double *err, 
     *err = e_max;
     *scale = s_max;
     return FLITE_OK;
+}
+
+int fp_canonical(const fp_mesh *m, fp_mesh **out) {
+    if (!m || !out) return FLITE_EINVAL;
+    *out = nullptr;
+    return guarded([&] {
+        auto c = std::make_unique<fp_mesh>(*m);
+        fp_internal::canonicalize(*c);
+        *out = c.release();
+        return FLITE_OK;
+    });
 }
 
 int fp_check(const fp_mesh *m, int level, double *closure, double *volume) {

@@ -1578,8 +1578,11 @@ __device__ __forceinline__ void gather_interior(const LevelView &L, int i, doubl
     }
 }
 
-// boundary edges of node i (FP64); on a moving mesh each edge's GCL term is
-// subtracted before its flux is added
+// boundary edges of node i (FP64).  On a moving mesh each boundary edge
+// first subtracts its GCL terms from both its nodes, then adds its fluxes
+// (def_par:2124-2177): per node -t, +g; an edge with both ends at node i (a
+// coarse level's self-edge) gives -t1, -t2, +g1, +g2, its second end's
+// entry following its first in the node's list
 template <int U>
 __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, double *r, bool active = true,
                                          int gl = 0) {
@@ -1591,20 +1594,31 @@ __device__ __forceinline__ void gather_boundary(const LevelView &L, int i, doubl
     auto add = [&](const double *g) {
         r[0] = r[0] + g[0]; r[1] = r[1] + g[1]; r[2] = r[2] + g[2]; r[3] = r[3] + g[3]; r[4] = r[4] + g[4];
     };
+    // g[0..4] the GCL term, g[5..9] the flux, g[10] 0 (an edge between two
+    // nodes), 1 or 2 (first or second end of a self-edge)
     auto terms_gcl = [&](int k, double *g) {
         const int v = L.binc[k];
         const size_t o = (size_t)(v >> 1) * 10 + (v & 1) * 5;
         for (int c = 0; c < 5; ++c) { g[c] = L.bgterm[o + c]; g[5 + c] = L.bflux[o + c]; }
+        const int2 nd = L.bedge[v >> 1];
+        g[10] = nd.x == nd.y ? (double)(1 + (v & 1)) : 0.0;
     };
+    double pend[5];  // the flux of a self-edge's first end, added after its second GCL term
     auto add_gcl = [&](const double *g) {
-        for (int c = 0; c < 5; ++c) r[c] = (r[c] - g[c]) + g[5 + c];
+        if (g[10] == 1.0) {
+            for (int c = 0; c < 5; ++c) { r[c] = r[c] - g[c]; pend[c] = g[5 + c]; }
+        } else if (g[10] == 2.0) {
+            for (int c = 0; c < 5; ++c) r[c] = ((r[c] - g[c]) + pend[c]) + g[5 + c];
+        } else {
+            for (int c = 0; c < 5; ++c) r[c] = (r[c] - g[c]) + g[5 + c];
+        }
     };
     if constexpr (U > 1) {
-        if (L.bgterm) group_gather<U, 10, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms_gcl, add_gcl);
+        if (L.bgterm) group_gather<U, 11, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms_gcl, add_gcl);
         else group_gather<U, 5, double>(L.binc_ptr[i], L.binc_ptr[i + 1], active, gl, terms, add);
     } else if (L.bgterm) {
         for (int k = L.binc_ptr[i]; k < L.binc_ptr[i + 1]; ++k) {
-            double v[10];
+            double v[11];
             terms_gcl(k, v);
             add_gcl(v);
         }

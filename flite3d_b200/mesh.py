@@ -76,6 +76,38 @@ class Mesh:
     def write_sol(self, path):
         _abi.check(_lib().fp_write_sol(self._h, str(path).encode()), "fp_write_sol")
 
+    @classmethod
+    def read_sol_domains(cls, prefix, plotreg):
+        """The mesh of a parallel run's files prefix.sol_1.. with plotreg,
+        merged into one (canonical form)."""
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_read_sol_domains(str(prefix).encode(), str(plotreg).encode(), ctypes.byref(h)),
+                   "fp_read_sol_domains")
+        return cls(h)
+
+    def partition(self, ndomains):
+        """gen3d's greedy partition of level 1: the 1-based domain of every
+        node (N,)."""
+        col = np.zeros(self.level(1).n_nodes, dtype=np.int32)
+        n = ctypes.c_int32()
+        _abi.check(_lib().fp_partition(self._h, int(ndomains), col.ctypes.data_as(ctypes.c_void_p),
+                                       ctypes.byref(n)), "fp_partition")
+        return col
+
+    def write_sol_domains(self, prefix, plotreg, ndomains, color=None):
+        """The files of a parallel run over ndomains (or the given 1-based
+        level-1 domains): prefix.sol_1.. and plotreg."""
+        c = None if color is None else np.ascontiguousarray(color, dtype=np.int32)
+        _abi.check(_lib().fp_write_sol_domains(self._h, str(prefix).encode(), str(plotreg).encode(), int(ndomains),
+                                               None if c is None else c.ctypes.data_as(ctypes.c_void_p)),
+                   "fp_write_sol_domains")
+
+    def canonical(self):
+        """The canonical form of this mesh (a new Mesh)."""
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_canonical(self._h, ctypes.byref(h)), "fp_canonical")
+        return Mesh(h)
+
     def write_plt(self, path):
         _abi.check(_lib().fp_write_plt(self._h, str(path).encode()), "fp_write_plt")
 

@@ -93,6 +93,37 @@ int fp_coordinate_movement(fp_mesh *m, int32_t time_scheme);
  * largest volume change.                                                    */
 int fp_gcl_check(const fp_mesh *m, int level, int32_t time_scheme, double *err, double *scale);
 
+/* The canonical form of a mesh (a new mesh in *out): level-1 nodes keep
+ * their numbers; the sides of every level run from the smaller to the larger
+ * node (a reversed side's coefficients and GCL weights change sign) in
+ * node-pair order, the boundary sides likewise (a reversed one's nodes swap
+ * their GCL weights); coarse nodes are numbered boundary nodes first, each
+ * class in the order of its smallest child; seeds become the smallest
+ * level-1 descendant, wall-node numbers are dropped.  Values are moved, not
+ * recomputed: two orderings of one mesh have equal canonical forms.         */
+int fp_canonical(const fp_mesh *m, fp_mesh **out);
+
+/* ---- multi-domain files (parallel runs of the reference) ----------------- */
+/* gen3d's greedy partition of level 1 (greedyMeshPartition,
+ * gen3d_struct.f90:890-1055): color [N] in 1..*ndomains_out (the front may
+ * produce a different number of domains than asked for).                    */
+int fp_partition(const fp_mesh *m, int32_t ndomains, int32_t *color, int32_t *ndomains_out);
+/* The files of a parallel run: prefix.sol_1 .. prefix.sol_n, one per domain,
+ * with every level's local numbering, ghost nodes, domain-crossing sides and
+ * boundary sides, send/receive lists and the coarse levels' cross-domain
+ * transfer lists, and plotreg (the owned nodes' global numbers), as
+ * writeParallelComputationFiles writes them (gen3d_grid.f90:4082-5231).
+ * color [N] gives level 1's domains (1-based; NULL: fp_partition's for
+ * ndomains); coarse nodes go to the domain of most of their children
+ * (mergeNodes :2843-2864).                                                   */
+int fp_write_sol_domains(const fp_mesh *m, const char *prefix, const char *plotreg, int32_t ndomains,
+                         const int32_t *color);
+/* The mesh of a parallel run's files, merged into one: ghosts resolved
+ * through the matching send and receive lists (level 1's global numbers from
+ * plotreg, makeplot mgnsg3d_mg_par.F90:1599-1707), each side and node taken
+ * once, in the canonical form of fp_canonical.                              */
+int fp_read_sol_domains(const char *prefix, const char *plotreg, fp_mesh **out);
+
 /* ---- files (Fortran sequential unformatted, 4-byte record markers) ---- */
 int fp_write_sol(const fp_mesh *m, const char *path);
 int fp_read_sol(const char *path, fp_mesh **out);
