@@ -100,7 +100,7 @@ PREPRO_SYMBOLS = [
     "fp_write_res", "fp_write_unk", "fp_read_unk", "fp_write_plotreg", "fp_makeplot", "fp_write_plt",
     "fp_read_inp", "fp_parse_inp_text", "fp_rsd_line", "fp_append_rsd", "fp_cycle_line",
     "fp_controls_default", "fp_controls_derive", "fp_set_moving_geometry", "fp_coordinate_movement", "fp_gcl_check",
-    "fp_canonical", "fp_partition", "fp_write_sol_domains", "fp_read_sol_domains",
+    "fp_canonical", "fp_partition", "fp_write_sol_domains", "fp_read_sol_domains", "fp_from_elements",
 ]
 
 _libs = {}

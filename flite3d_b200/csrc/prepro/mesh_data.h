@@ -47,6 +47,13 @@ struct fp_mesh {
     std::vector<int32_t> tets;    // [4][ntet] new numbering
     std::vector<int32_t> tris;    // [3][ntri]
     std::vector<int32_t> tri_ind;
+    // the other elements and the quadrilateral boundary faces
+    std::vector<int32_t> hexes;     // [8][nhex]
+    std::vector<int32_t> prisms;    // [6][npri]
+    std::vector<int32_t> pyramids;  // [5][npyr]
+    std::vector<int32_t> quads;     // [4][nquad]
+    std::vector<int32_t> quad_ind;
+    bool hybrid() const { return !hexes.empty() || !prisms.empty() || !pyramids.empty() || !quads.empty(); }
 };
 
 

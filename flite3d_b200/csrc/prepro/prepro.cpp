@@ -248,52 +248,183 @@ inline V3 sweep(const V3 *p, const V3 *q, const V3 *r, int k) {
 // each level, and GCL(1) (levels 0-1) and GCL(2) (levels 1-2), the volumes
 // its two dual-face triangles sweep
 struct TetSideMoving { int a, b; V3 coef; double nv[3], gcl[2]; };
+// side a-b of an element with the centroid xmm and the dual-face points xm
+// (edge midpoint), P1 and P2 (face points) at the three levels: r1 = xmm -
+// xm, r2 = P1 - xm, r3 = P2 - xm, r4 = xmm - xm, rv = xm - x_a
+// (registerSideGCL gen3d_grid.f90:786-855 with the vectors every element
+// routine builds)
+void dual_side(int a, int b, const V3 *xa, const V3 *xmm, const V3 *xm, const V3 *P1, const V3 *P2,
+               TetSideMoving &o) {
+    V3 r1[3], r2[3], r3[3], r4[3], rv[3], c1[3], c2[3];
+    for (int t = 0; t < 3; ++t) {
+        r1[t] = xmm[t] - xm[t]; r2[t] = P1[t] - xm[t]; r3[t] = P2[t] - xm[t]; r4[t] = xmm[t] - xm[t];
+        rv[t] = xm[t] - xa[t];
+        c1[t] = halfcross(r1[t], r2[t]);
+        c2[t] = halfcross(r3[t], r4[t]);
+    }
+    o.a = a; o.b = b;
+    for (int t = 0; t < 3; ++t) {
+        const V3 cxx = c1[t] + c2[t];
+        o.nv[t] = (rv[t].x * cxx.x + rv[t].y * cxx.y + rv[t].z * cxx.z) / 3.;
+        if (t == 0) o.coef = scl(0.5, cxx);
+    }
+    for (int k = 0; k < 2; ++k) {
+        const V3 vr1 = sweep(xm, xmm, P1, k), vr2 = sweep(xm, P2, xmm, k);
+        const V3 y1 = qcross(r1[k], r2[k + 1]) + qcross(r1[k + 1], r2[k]);
+        const V3 y2 = qcross(r3[k], r4[k + 1]) + qcross(r3[k + 1], r4[k]);
+        o.gcl[k] = (dot3((c1[k] + y1) + c1[k + 1], vr1) + dot3((c2[k] + y2) + c2[k + 1], vr2)) / 3.;
+    }
+}
+
+// the element's points at the three levels: edge midpoints 0.5 (x_i + x_j),
+// face centroids (x_i + x_j + x_k) / 3, and the quarter sum 0.5 of four
+template <int NV>
+struct ElemPts {
+    const V3 (*x)[NV];
+    void H(int i, int j, V3 *o) const { for (int t = 0; t < 3; ++t) o[t] = scl(0.5, x[t][i] + x[t][j]); }
+    void T(int i, int j, int k, V3 *o) const {
+        for (int t = 0; t < 3; ++t) o[t] = div3(x[t][i] + x[t][j] + x[t][k]);
+    }
+    void Q(int i, int j, int k, int l, V3 *o) const {
+        for (int t = 0; t < 3; ++t) o[t] = scl(0.25, x[t][i] + x[t][j] + x[t][k] + x[t][l]);
+    }
+    // 0.5 (x_i + x_j) when q_c < q_d, else 0.5 (x_k + x_l): the diagonal of
+    // a quadrilateral face through its lower-numbered corner of c, d
+    void D(const int32_t *q, int c, int d, int i, int j, int k, int l, V3 *o) const {
+        if (q[c] < q[d]) H(i, j, o);
+        else H(k, l, o);
+    }
+    void vertex(int i, V3 *o) const { for (int t = 0; t < 3; ++t) o[t] = x[t][i]; }
+};
+
 void tet_sides_moving(const V3 (*x)[4], TetSideMoving *out) {
     V3 xmm[3];
     for (int t = 0; t < 3; ++t) xmm[t] = scl(0.25, x[t][0] + x[t][1] + x[t][2] + x[t][3]);
     int n = 0;
-    // side a-b with the dual-face points xm (edge midpoint), P1 and P2 (face
-    // centroids): r1 = xmm - xm, r2 = P1 - xm, r3 = P2 - xm, r4 = xmm - xm
     auto side = [&](int a, int b, const V3 *xm, const V3 *P1, const V3 *P2) {
-        V3 r1[3], r2[3], r3[3], r4[3], rv[3], c1[3], c2[3];
-        for (int t = 0; t < 3; ++t) {
-            r1[t] = xmm[t] - xm[t]; r2[t] = P1[t] - xm[t]; r3[t] = P2[t] - xm[t]; r4[t] = xmm[t] - xm[t];
-            rv[t] = xm[t] - x[t][a];
-            c1[t] = halfcross(r1[t], r2[t]);
-            c2[t] = halfcross(r3[t], r4[t]);
-        }
-        TetSideMoving &o = out[n++];
-        o.a = a; o.b = b;
-        for (int t = 0; t < 3; ++t) {
-            const V3 cxx = c1[t] + c2[t];
-            o.nv[t] = (rv[t].x * cxx.x + rv[t].y * cxx.y + rv[t].z * cxx.z) / 3.;
-            if (t == 0) o.coef = scl(0.5, cxx);
-        }
-        for (int k = 0; k < 2; ++k) {
-            const V3 vr1 = sweep(xm, xmm, P1, k), vr2 = sweep(xm, P2, xmm, k);
-            const V3 y1 = qcross(r1[k], r2[k + 1]) + qcross(r1[k + 1], r2[k]);
-            const V3 y2 = qcross(r3[k], r4[k + 1]) + qcross(r3[k + 1], r4[k]);
-            o.gcl[k] = (dot3((c1[k] + y1) + c1[k + 1], vr1) + dot3((c2[k] + y2) + c2[k + 1], vr2)) / 3.;
-        }
+        V3 xa[3];
+        for (int t = 0; t < 3; ++t) xa[t] = x[t][a];
+        dual_side(a, b, xa, xmm, xm, P1, P2, out[n++]);
     };
     V3 xm1[3], xm2[3], xm3[3], xb1[3], xb2[3], xb3[3];
-    auto pts = [&](int i, int j, V3 *o) { for (int t = 0; t < 3; ++t) o[t] = scl(0.5, x[t][i] + x[t][j]); };
-    auto ctr = [&](int i, int j, int k, V3 *o) { for (int t = 0; t < 3; ++t) o[t] = div3(x[t][i] + x[t][j] + x[t][k]); };
+    const ElemPts<4> e{x};
     // node 1
-    pts(0, 1, xm1); pts(0, 2, xm2); pts(0, 3, xm3);
-    ctr(0, 1, 2, xb1); ctr(0, 1, 3, xb2); ctr(0, 2, 3, xb3);
+    e.H(0, 1, xm1); e.H(0, 2, xm2); e.H(0, 3, xm3);
+    e.T(0, 1, 2, xb1); e.T(0, 1, 3, xb2); e.T(0, 2, 3, xb3);
     side(0, 1, xm1, xb2, xb1);
     side(0, 2, xm2, xb1, xb3);
     side(0, 3, xm3, xb3, xb2);
     // node 2
-    pts(1, 2, xm1); pts(1, 3, xm2);
-    ctr(0, 1, 2, xb1); ctr(1, 2, 3, xb2); ctr(0, 1, 3, xb3);
+    e.H(1, 2, xm1); e.H(1, 3, xm2);
+    e.T(0, 1, 2, xb1); e.T(1, 2, 3, xb2); e.T(0, 1, 3, xb3);
     side(1, 2, xm1, xb2, xb1);
     side(1, 3, xm2, xb3, xb2);
     // node 3
-    pts(2, 3, xm1);
-    ctr(0, 2, 3, xb1); ctr(1, 2, 3, xb2);
+    e.H(2, 3, xm1);
+    e.T(0, 2, 3, xb1); e.T(1, 2, 3, xb2);
     side(2, 3, xm1, xb2, xb1);
+}
+
+// The twelve sides of a hexahedron (vertices 1-4 one face, 5-8 the
+// opposite one, 1-5 an edge) from its four corners 1, 6, 3 and 8
+// (makeCalcDataForHex gen3d_grid.f90:902-1379): the centroid of the inner
+// tetrahedron 1-3-5-7 and, on each face, the diagonal through the corner
+// of the lower node number q.
+void hex_sides(const V3 (*x)[8], const int32_t *q, TetSideMoving *out) {
+    const ElemPts<8> e{x};
+    V3 xmm[3], xm1[3], xm2[3], xm3[3], xb1[3], xb2[3], xb3[3];
+    e.Q(0, 2, 4, 6, xmm);
+    int n = 0;
+    auto corner = [&](int c, int n1, int n2, int n3) {
+        V3 xa[3];
+        e.vertex(c, xa);
+        dual_side(c, n1, xa, xmm, xm1, xb2, xb1, out[n++]);
+        dual_side(c, n2, xa, xmm, xm2, xb1, xb3, out[n++]);
+        dual_side(c, n3, xa, xmm, xm3, xb3, xb2, out[n++]);
+    };
+    e.H(0, 1, xm1); e.H(0, 3, xm2); e.H(0, 4, xm3); e.H(0, 2, xb1);
+    e.D(q, 4, 5, 1, 4, 0, 5, xb2); e.D(q, 4, 7, 3, 4, 0, 7, xb3);
+    corner(0, 1, 3, 4);
+    e.H(5, 4, xm1); e.H(5, 6, xm2); e.H(5, 1, xm3); e.H(4, 6, xb1);
+    e.D(q, 4, 5, 1, 4, 0, 5, xb2); e.D(q, 5, 6, 5, 2, 1, 6, xb3);
+    corner(5, 4, 6, 1);
+    e.H(2, 3, xm1); e.H(1, 2, xm2); e.H(2, 6, xm3); e.H(0, 2, xb1);
+    e.D(q, 6, 7, 6, 3, 2, 7, xb2); e.D(q, 5, 6, 5, 2, 1, 6, xb3);
+    corner(2, 3, 1, 6);
+    e.H(7, 6, xm1); e.H(7, 4, xm2); e.H(7, 3, xm3); e.H(4, 6, xb1);
+    e.D(q, 6, 7, 6, 3, 2, 7, xb2); e.D(q, 4, 7, 4, 3, 0, 7, xb3);
+    corner(7, 6, 4, 3);
+}
+
+// The nine sides of a prism (triangles 1-2-3 and 4-5-6, 1-4 an edge)
+// (makeCalcDataForPri gen3d_grid.f90:1381-1777): the centroid of the three
+// quadrilateral faces' diagonal midpoints, each diagonal through the corner
+// of the lower node number q.
+void pri_sides(const V3 (*x)[6], const int32_t *q, TetSideMoving *out) {
+    const ElemPts<6> e{x};
+    V3 xmm[3], xm1[3], xm2[3], xm3[3], xb1[3], xb2[3], xb3[3], xa[3];
+    e.D(q, 3, 4, 3, 1, 0, 4, xb1); e.D(q, 3, 5, 3, 2, 0, 5, xb2); e.D(q, 4, 5, 4, 2, 1, 5, xb3);
+    for (int t = 0; t < 3; ++t) xmm[t] = div3(xb1[t] + xb2[t] + xb3[t]);
+    int n = 0;
+    // node 1
+    e.H(0, 1, xm1); e.H(0, 2, xm2); e.H(0, 3, xm3); e.T(0, 1, 2, xb1);
+    e.D(q, 3, 4, 3, 1, 0, 4, xb2); e.D(q, 3, 5, 3, 2, 0, 5, xb3);
+    e.vertex(0, xa);
+    dual_side(0, 1, xa, xmm, xm1, xb2, xb1, out[n++]);
+    dual_side(0, 2, xa, xmm, xm2, xb1, xb3, out[n++]);
+    dual_side(0, 3, xa, xmm, xm3, xb3, xb2, out[n++]);
+    // node 6
+    e.H(5, 4, xm1); e.H(5, 3, xm2); e.H(5, 2, xm3); e.T(3, 4, 5, xb1);
+    e.D(q, 4, 5, 4, 2, 1, 5, xb2); e.D(q, 3, 5, 3, 2, 0, 5, xb3);
+    e.vertex(5, xa);
+    dual_side(5, 4, xa, xmm, xm1, xb2, xb1, out[n++]);
+    dual_side(5, 3, xa, xmm, xm2, xb1, xb3, out[n++]);
+    dual_side(5, 2, xa, xmm, xm3, xb3, xb2, out[n++]);
+    // node 2
+    e.H(1, 4, xm1); e.H(1, 2, xm2); e.T(0, 1, 2, xb3);
+    e.D(q, 4, 5, 4, 2, 1, 5, xb1); e.D(q, 3, 4, 3, 1, 0, 4, xb2);
+    e.vertex(1, xa);
+    dual_side(1, 2, xa, xmm, xm2, xb1, xb3, out[n++]);
+    dual_side(1, 4, xa, xmm, xm1, xb2, xb1, out[n++]);
+    // node 4
+    e.H(3, 4, xm1); e.T(3, 4, 5, xb1);
+    e.D(q, 3, 4, 3, 1, 0, 4, xb2);
+    e.vertex(3, xa);
+    dual_side(3, 4, xa, xmm, xm1, xb1, xb2, out[n++]);
+}
+
+// The eight sides of a pyramid (base 1-2-3-4, apex 5) (makeCalcDataForPyr
+// gen3d_grid.f90:1779-2090): the point (2 (x1 + x3) + x5) / 5 and the base
+// diagonal 1-3.
+void pyr_sides(const V3 (*x)[5], TetSideMoving *out) {
+    const ElemPts<5> e{x};
+    V3 xmm[3], xm1[3], xm2[3], xm3[3], xb1[3], xb2[3], xb3[3], xa[3];
+    for (int t = 0; t < 3; ++t) {
+        const V3 s = x[t][0] + x[t][2];
+        const V3 u = {2.0 * s.x + x[t][4].x, 2.0 * s.y + x[t][4].y, 2.0 * s.z + x[t][4].z};
+        xmm[t] = {u.x / 5., u.y / 5., u.z / 5.};
+    }
+    int n = 0;
+    // node 1
+    e.H(0, 1, xm1); e.H(0, 3, xm2); e.H(0, 4, xm3); e.H(0, 2, xb1); e.T(0, 1, 4, xb2); e.T(0, 3, 4, xb3);
+    e.vertex(0, xa);
+    dual_side(0, 1, xa, xmm, xm1, xb2, xb1, out[n++]);
+    dual_side(0, 3, xa, xmm, xm2, xb1, xb3, out[n++]);
+    dual_side(0, 4, xa, xmm, xm3, xb3, xb2, out[n++]);
+    // node 3
+    e.H(1, 2, xm1); e.H(2, 3, xm2); e.H(2, 4, xm3); e.H(0, 2, xb1); e.T(1, 2, 4, xb2); e.T(2, 3, 4, xb3);
+    e.vertex(2, xa);
+    dual_side(2, 1, xa, xmm, xm1, xb1, xb2, out[n++]);
+    dual_side(2, 3, xa, xmm, xm2, xb3, xb1, out[n++]);
+    dual_side(2, 4, xa, xmm, xm3, xb2, xb3, out[n++]);
+    // node 2
+    e.H(1, 4, xm3); e.T(1, 2, 4, xb2); e.T(0, 1, 4, xb3);
+    e.vertex(1, xa);
+    dual_side(1, 4, xa, xmm, xm3, xb3, xb2, out[n++]);
+    // node 4
+    e.H(3, 4, xm3); e.T(0, 3, 4, xb2); e.T(2, 3, 4, xb3);
+    e.vertex(3, xa);
+    dual_side(3, 4, xa, xmm, xm3, xb3, xb2, out[n++]);
 }
 
 // A boundary triangle side at three time levels (registerBoundarySideGCL,
@@ -301,35 +432,57 @@ void tet_sides_moving(const V3 (*x)[4], TetSideMoving *out) {
 // quarter coefficient at t = 0 and, for its first and second vertex,
 // GCL(1 or 2, 1) (levels 0-1) and GCL(1 or 2, 2) (levels 1-2)
 struct TriSideMoving { int a, b; V3 coef; double gcl[2][2]; };
+// boundary side a-b of a face with the centre ctr (sweeps) through the edge
+// midpoint mid: r1 = A - x_a, r2 = B - x_a
+void bnd_side(int a, int b, const V3 *xa, const V3 *xb, const V3 *A, const V3 *B, const V3 *mid, const V3 *ctr,
+              TriSideMoving &o) {
+    V3 r1[3], r2[3], cxx[3];
+    for (int t = 0; t < 3; ++t) {
+        r1[t] = A[t] - xa[t]; r2[t] = B[t] - xa[t];
+        cxx[t] = halfcross(r1[t], r2[t]);
+    }
+    o.a = a; o.b = b;
+    o.coef = scl(0.25, cxx[0]);
+    for (int k = 0; k < 2; ++k) {
+        const V3 vr1 = sweep(xa, ctr, mid, k), vr2 = sweep(xb, ctr, mid, k);
+        const V3 y = qcross(r1[k], r2[k + 1]) + qcross(r1[k + 1], r2[k]);
+        const V3 s = (cxx[k] + y) + cxx[k + 1];
+        o.gcl[0][k] = dot3(s, vr1) / 3.;
+        o.gcl[1][k] = dot3(s, vr2) / 3.;
+    }
+}
+
 void tri_sides_moving(const V3 (*x)[3], TriSideMoving *out) {
-    V3 xm[3], xb[3][3];
+    V3 xm[3], xb[3][3], v[3][3];
     for (int t = 0; t < 3; ++t) {
         xm[t] = div3(x[t][0] + x[t][1] + x[t][2]);
         xb[0][t] = scl(0.5, x[t][0] + x[t][1]);
         xb[1][t] = scl(0.5, x[t][1] + x[t][2]);
         xb[2][t] = scl(0.5, x[t][2] + x[t][0]);
+        for (int k = 0; k < 3; ++k) v[k][t] = x[t][k];
     }
-    // side a-b through the edge midpoint mid, r1 = A - x_a, r2 = B - x_a
-    auto side = [&](TriSideMoving &o, int a, int b, const V3 *A, const V3 *B, const V3 *mid) {
-        V3 r1[3], r2[3], cxx[3], xa[3], xbv[3];
-        for (int t = 0; t < 3; ++t) {
-            r1[t] = A[t] - x[t][a]; r2[t] = B[t] - x[t][a];
-            cxx[t] = halfcross(r1[t], r2[t]);
-            xa[t] = x[t][a]; xbv[t] = x[t][b];
-        }
-        o.a = a; o.b = b;
-        o.coef = scl(0.25, cxx[0]);
-        for (int k = 0; k < 2; ++k) {
-            const V3 vr1 = sweep(xa, xm, mid, k), vr2 = sweep(xbv, xm, mid, k);
-            const V3 y = qcross(r1[k], r2[k + 1]) + qcross(r1[k + 1], r2[k]);
-            const V3 s = (cxx[k] + y) + cxx[k + 1];
-            o.gcl[0][k] = dot3(s, vr1) / 3.;
-            o.gcl[1][k] = dot3(s, vr2) / 3.;
-        }
-    };
-    side(out[0], 0, 1, xm, xb[0], xb[0]);
-    side(out[1], 0, 2, xb[2], xm, xb[2]);
-    side(out[2], 1, 2, xm, xb[1], xb[1]);
+    bnd_side(0, 1, v[0], v[1], xm, xb[0], xb[0], xm, out[0]);
+    bnd_side(0, 2, v[0], v[2], xb[2], xm, xb[2], xm, out[1]);
+    bnd_side(1, 2, v[1], v[2], xm, xb[1], xb[1], xm, out[2]);
+}
+
+// The four sides of a quadrilateral boundary face (makeCalcDataForBoundary
+// gen3d_boundary.f90:627-766): the centre is the midpoint of the diagonal
+// 1-3
+void quad_sides_moving(const V3 (*x)[4], TriSideMoving *out) {
+    V3 xm[3], xb[4][3], v[4][3];
+    for (int t = 0; t < 3; ++t) {
+        xm[t] = scl(0.5, x[t][0] + x[t][2]);
+        xb[0][t] = scl(0.5, x[t][0] + x[t][1]);
+        xb[1][t] = scl(0.5, x[t][1] + x[t][2]);
+        xb[2][t] = scl(0.5, x[t][2] + x[t][3]);
+        xb[3][t] = scl(0.5, x[t][0] + x[t][3]);
+        for (int k = 0; k < 4; ++k) v[k][t] = x[t][k];
+    }
+    bnd_side(0, 1, v[0], v[1], xm, xb[0], xb[0], xm, out[0]);
+    bnd_side(0, 3, v[0], v[3], xb[3], xm, xb[3], xm, out[1]);
+    bnd_side(2, 1, v[2], v[1], xb[1], xm, xb[1], xm, out[2]);
+    bnd_side(2, 3, v[2], v[3], xm, xb[2], xb[2], xm, out[3]);
 }
 
 // Indicator priority of setBoundIndForViscousMesh (gen3d_boundary.f90:
@@ -408,16 +561,26 @@ class KdTree {
 };
 
 // ---- level 1 from tetrahedra --------------------------------------------
+// the elements other than tetrahedra and the quadrilateral boundary faces,
+// [k][n] column-major, 1-based
+struct Hybrid {
+    std::vector<int32_t> hex, pri, pyr, quad, quad_ind;
+};
+
 void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
                 std::vector<int32_t> tets_old, std::vector<int32_t> tris_old,
-                const std::vector<int32_t> &tri_ind) {
+                const std::vector<int32_t> &tri_ind, Hybrid hy = Hybrid{}) {
     const int32_t NT = (int32_t)(tets_old.size() / 4);
     const int32_t NF = (int32_t)(tris_old.size() / 3);
+    const int32_t NH = (int32_t)(hy.hex.size() / 8), NP = (int32_t)(hy.pri.size() / 6);
+    const int32_t NY = (int32_t)(hy.pyr.size() / 5), NQ = (int32_t)(hy.quad.size() / 4);
     // boundary-first numbering (gen3d_grid.f90:127-383): boundary nodes keep
     // their relative order and take 1..Nb, interior nodes follow
     std::vector<char> isb(N, 0);
     for (int32_t f = 0; f < NF; ++f)
         for (int k = 0; k < 3; ++k) isb[tris_old[(size_t)k * NF + f] - 1] = 1;
+    for (int32_t f = 0; f < NQ; ++f)
+        for (int k = 0; k < 4; ++k) isb[hy.quad[(size_t)k * NQ + f] - 1] = 1;
     std::vector<int32_t> o2n(N), n2o(N);
     int32_t nb = 0;
     for (int32_t i = 0; i < N; ++i) if (isb[i]) { o2n[i] = nb; n2o[nb] = i; ++nb; }
@@ -436,6 +599,8 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
     };
     for (auto &t : tets_old) t = o2n[t - 1] + 1;
     for (auto &t : tris_old) t = o2n[t - 1] + 1;
+    for (std::vector<int32_t> *v : {&hy.hex, &hy.pri, &hy.pyr, &hy.quad})
+        for (auto &t : *v) t = o2n[t - 1] + 1;
 
     // edges of every tetrahedron (makeCalcDataForTet, gen3d_grid.f90:2092-2332)
     auto *tm_edges = new SectionTimer("tet edges");
@@ -484,6 +649,39 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         }
         return nv;
     };
+    // hexahedra, prisms and pyramids (makeCalculationData gen3d_grid.f90:
+    // 699-785 takes them in this order before the tetrahedra); a negative
+    // element volume is an error (gen3d warns)
+    auto hybrid = [&](const std::vector<int32_t> &el, int nv, int ns, auto &&sides_of) {
+        const int32_t ne = (int32_t)(el.size() / nv);
+        for (int32_t t = 0; t < ne; ++t) {
+            int32_t p[8];
+            V3 xv[3][8];
+            for (int k = 0; k < nv; ++k) {
+                p[k] = el[(size_t)k * ne + t];
+                xv[0][k] = xv[1][k] = xv[2][k] = X(p[k]);
+            }
+            TetSideMoving ts[12];
+            sides_of(xv, p, ts);
+            double ev = 0;
+            for (int k = 0; k < ns; ++k) {
+                TetSide<double> s1{ts[k].a, ts[k].b, ts[k].coef, ts[k].nv[0]};
+                ev += 2. * register_side(p[ts[k].a], p[ts[k].b], s1);
+            }
+            if (ev <= 0) ++nneg;
+        }
+    };
+    hybrid(hy.hex, 8, 12, [](const V3 (*x)[8], const int32_t *q, TetSideMoving *o) { hex_sides(x, q, o); });
+    hybrid(hy.pri, 6, 9, [](const V3 (*x)[8], const int32_t *q, TetSideMoving *o) {
+        V3 y[3][6];
+        for (int t = 0; t < 3; ++t) for (int k = 0; k < 6; ++k) y[t][k] = x[t][k];
+        pri_sides(y, q, o);
+    });
+    hybrid(hy.pyr, 5, 8, [](const V3 (*x)[8], const int32_t *, TetSideMoving *o) {
+        V3 y[3][5];
+        for (int t = 0; t < 3; ++t) for (int k = 0; k < 5; ++k) y[t][k] = x[t][k];
+        pyr_sides(y, o);
+    });
     for (int32_t t = 0; t < NT; ++t) {
         int32_t p[4] = {tets_old[t], tets_old[(size_t)NT + t], tets_old[2 * (size_t)NT + t],
                         tets_old[3 * (size_t)NT + t]};
@@ -526,9 +724,17 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         // 21 bits per index would overflow for big meshes; combine two keys
         return std::make_pair(pkey(s[0], s[1]), (uint64_t)s[2]);
     };
-    // face -> opposite vertex: store in a map keyed by (min,mid) with a
+    // face -> a point inside its element (a tetrahedron's opposite vertex,
+    // another element's vertex mean): a map keyed by (min,mid) with a
     // per-face list; faces sharing (min,mid) are few, resolved linearly
     std::vector<int32_t> fopp(NF, 0);
+    std::vector<V3> fint(NF);
+    std::vector<char> fhas(NF, 0);
+    auto centroid = [&](const int32_t *p, int nv) {
+        V3 c = {0, 0, 0};
+        for (int k = 0; k < nv; ++k) c = c + X(p[k]);
+        return scl(1.0 / nv, c);
+    };
     {
         std::vector<std::vector<std::pair<int32_t, int32_t>>> buckets;  // (max, face)
         buckets.reserve(NF);
@@ -549,9 +755,59 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
                 int64_t slot = fmap.find(k.first);
                 if (slot < 0) continue;
                 for (auto &pr : buckets[slot])
-                    if (pr.first == (int32_t)k.second) fopp[pr.second] = p[o];
+                    if (pr.first == (int32_t)k.second) { fopp[pr.second] = p[o]; fint[pr.second] = X(p[o]); fhas[pr.second] = 1; }
             }
         }
+        // triangular faces of prisms (the two caps) and pyramids (the sides)
+        auto tri_faces = [&](const std::vector<int32_t> &el, int nv, const int (*fc)[3], int nf) {
+            const int32_t ne = (int32_t)(el.size() / nv);
+            for (int32_t t = 0; t < ne; ++t) {
+                int32_t p[8];
+                for (int k = 0; k < nv; ++k) p[k] = el[(size_t)k * ne + t];
+                for (int o = 0; o < nf; ++o) {
+                    auto k = fkey(p[fc[o][0]], p[fc[o][1]], p[fc[o][2]]);
+                    int64_t slot = fmap.find(k.first);
+                    if (slot < 0) continue;
+                    for (auto &pr : buckets[slot])
+                        if (pr.first == (int32_t)k.second) { fint[pr.second] = centroid(p, nv); fhas[pr.second] = 1; }
+                }
+            }
+        };
+        const int pri_tri[2][3] = {{0, 1, 2}, {3, 4, 5}};
+        const int pyr_tri[4][3] = {{0, 1, 4}, {1, 2, 4}, {2, 3, 4}, {3, 0, 4}};
+        tri_faces(hy.pri, 6, pri_tri, 2);
+        tri_faces(hy.pyr, 5, pyr_tri, 4);
+    }
+    // quadrilateral faces -> the vertex mean of their element (hexahedra,
+    // prism sides, pyramid bases)
+    std::vector<V3> qint(NQ);
+    std::vector<char> qhas(NQ, 0);
+    {
+        auto qkey = [&](int32_t a, int32_t b, int32_t c, int32_t d) {
+            int32_t q4[4] = {a, b, c, d};
+            std::sort(q4, q4 + 4);
+            return std::make_pair(pkey(q4[0], q4[1]), pkey(q4[2], q4[3]));
+        };
+        std::map<std::pair<uint64_t, uint64_t>, int32_t> qmap;
+        for (int32_t f = 0; f < NQ; ++f)
+            qmap[qkey(hy.quad[f], hy.quad[(size_t)NQ + f], hy.quad[2 * (size_t)NQ + f], hy.quad[3 * (size_t)NQ + f])] = f;
+        auto quad_faces = [&](const std::vector<int32_t> &el, int nv, const int (*fc)[4], int nf) {
+            const int32_t ne = (int32_t)(el.size() / nv);
+            for (int32_t t = 0; t < ne; ++t) {
+                int32_t p[8];
+                for (int k = 0; k < nv; ++k) p[k] = el[(size_t)k * ne + t];
+                for (int o = 0; o < nf; ++o) {
+                    auto it = qmap.find(qkey(p[fc[o][0]], p[fc[o][1]], p[fc[o][2]], p[fc[o][3]]));
+                    if (it != qmap.end()) { qint[it->second] = centroid(p, nv); qhas[it->second] = 1; }
+                }
+            }
+        };
+        const int hex_q[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}};
+        const int pri_q[3][4] = {{0, 1, 4, 3}, {1, 2, 5, 4}, {2, 0, 3, 5}};
+        const int pyr_q[1][4] = {{0, 1, 2, 3}};
+        quad_faces(hy.hex, 8, hex_q, 6);
+        quad_faces(hy.pri, 6, pri_q, 3);
+        quad_faces(hy.pyr, 5, pyr_q, 1);
     }
     PairMap bmap((size_t)NF * 2 + 16);
     std::vector<int32_t> b1, b2, bi;
@@ -568,8 +824,8 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
     std::vector<int32_t> tris_new(3 * (size_t)NF);
     for (int32_t f = 0; f < NF; ++f) {
         int32_t p1 = tris_old[f], p2 = tris_old[(size_t)NF + f], p3 = tris_old[2 * (size_t)NF + f];
-        if (fopp[f] == 0) throw std::runtime_error("boundary triangle without a tetrahedron");
-        V3 a = X(p2) - X(p1), b = X(p3) - X(p1), d = X(fopp[f]) - X(p1);
+        if (!fhas[f]) throw std::runtime_error("boundary triangle without an element");
+        V3 a = X(p2) - X(p1), b = X(p3) - X(p1), d = fint[f] - X(p1);
         V3 n = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
         if (n.x * d.x + n.y * d.y + n.z * d.z < 0) std::swap(p2, p3);
         tris_new[f] = p1; tris_new[(size_t)NF + f] = p2; tris_new[2 * (size_t)NF + f] = p3;
@@ -579,6 +835,24 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         TriSide<double> ts[3];
         tri_sides(xv, ts);
         for (int k = 0; k < 3; ++k) register_bside(pv[ts[k].a], pv[ts[k].b], ts[k].coef, ind);
+    }
+    // quadrilateral faces after the triangles (makeCalcDataForBoundary
+    // gen3d_boundary.f90:627-766), oriented like them
+    std::vector<int32_t> quads_new(4 * (size_t)NQ);
+    for (int32_t f = 0; f < NQ; ++f) {
+        int32_t p[4] = {hy.quad[f], hy.quad[(size_t)NQ + f], hy.quad[2 * (size_t)NQ + f], hy.quad[3 * (size_t)NQ + f]};
+        if (!qhas[f]) throw std::runtime_error("boundary quadrilateral without an element");
+        V3 a = X(p[2]) - X(p[0]), b = X(p[3]) - X(p[1]), d = qint[f] - X(p[0]);
+        V3 n = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+        if (n.x * d.x + n.y * d.y + n.z * d.z < 0) std::swap(p[1], p[3]);
+        V3 xv[3][4];
+        for (int k = 0; k < 4; ++k) {
+            quads_new[(size_t)k * NQ + f] = p[k];
+            xv[0][k] = xv[1][k] = xv[2][k] = X(p[k]);
+        }
+        TriSideMoving ts[4];
+        quad_sides_moving(xv, ts);
+        for (int k = 0; k < 4; ++k) register_bside(p[ts[k].a], p[ts[k].b], ts[k].coef, hy.quad_ind[f]);
     }
     L.B = (int32_t)b1.size();
     L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B);
@@ -592,6 +866,11 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         for (int k = 0; k < 3; ++k) {
             int32_t n = tris_new[(size_t)k * NF + f] - 1;
             L.bnd_indicator[n] = merge_indicator(L.bnd_indicator[n], tri_ind[f]);
+        }
+    for (int32_t f = 0; f < NQ; ++f)
+        for (int k = 0; k < 4; ++k) {
+            int32_t n = quads_new[(size_t)k * NQ + f] - 1;
+            L.bnd_indicator[n] = merge_indicator(L.bnd_indicator[n], hy.quad_ind[f]);
         }
     build_register(L);
 
@@ -620,6 +899,8 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
     M.tets = std::move(tets_old);
     M.tris = std::move(tris_new);
     M.tri_ind = tri_ind;
+    M.hexes = std::move(hy.hex); M.prisms = std::move(hy.pri); M.pyramids = std::move(hy.pyr);
+    M.quads = std::move(quads_new); M.quad_ind = std::move(hy.quad_ind);
     M.lv.clear();
     M.lv.push_back(std::move(L));
 }
@@ -836,11 +1117,67 @@ struct Geometry {
     void tri(int32_t f, int32_t *p) const {
         for (int k = 0; k < 3; ++k) p[k] = M.tris[(size_t)k * NF + f];
     }
+    // the sides of the hexahedra, prisms and pyramids (in this order) at the
+    // three coordinate levels x[0..2], each passed to f(p1, p2, side)
+    template <class F>
+    void hybrid_sides(const double *const x[3], F &&f) const {
+        auto run = [&](const std::vector<int32_t> &el, int nv, int ns, auto &&sides_of) {
+            const int32_t ne = (int32_t)(el.size() / nv);
+            for (int32_t t = 0; t < ne; ++t) {
+                int32_t p[8];
+                V3 xv[3][8];
+                for (int k = 0; k < nv; ++k) {
+                    p[k] = el[(size_t)k * ne + t];
+                    for (int q = 0; q < 3; ++q) xv[q][k] = X(x[q], p[k]);
+                }
+                TetSideMoving ts[12];
+                sides_of(xv, p, ts);
+                for (int k = 0; k < ns; ++k) f(p[ts[k].a], p[ts[k].b], ts[k]);
+            }
+        };
+        run(M.hexes, 8, 12, [](const V3 (*xv)[8], const int32_t *q, TetSideMoving *o) { hex_sides(xv, q, o); });
+        run(M.prisms, 6, 9, [](const V3 (*xv)[8], const int32_t *q, TetSideMoving *o) {
+            V3 y[3][6];
+            for (int t = 0; t < 3; ++t) for (int k = 0; k < 6; ++k) y[t][k] = xv[t][k];
+            pri_sides(y, q, o);
+        });
+        run(M.pyramids, 5, 8, [](const V3 (*xv)[8], const int32_t *, TetSideMoving *o) {
+            V3 y[3][5];
+            for (int t = 0; t < 3; ++t) for (int k = 0; k < 5; ++k) y[t][k] = xv[t][k];
+            pyr_sides(y, o);
+        });
+    }
+    // the quadrilateral boundary faces' sides, each passed to f(pa, pb, side)
+    template <class F>
+    void quad_sides(const double *const x[3], F &&f) const {
+        const int32_t NQ = (int32_t)(M.quads.size() / 4);
+        for (int32_t q4 = 0; q4 < NQ; ++q4) {
+            int32_t p[4];
+            V3 xv[3][4];
+            for (int k = 0; k < 4; ++k) {
+                p[k] = M.quads[(size_t)k * NQ + q4];
+                for (int q = 0; q < 3; ++q) xv[q][k] = X(x[q], p[k]);
+            }
+            TriSideMoving ts[4];
+            quad_sides_moving(xv, ts);
+            for (int k = 0; k < 4; ++k) f(p[ts[k].a], p[ts[k].b], ts[k]);
+        }
+    }
     void eval(const double *xyz, double *sw, double *bw, double *vol) const {
         const size_t E = L.E, B = L.B;
         std::fill(sw, sw + 3 * E, 0.0);
         std::fill(bw, bw + 3 * B, 0.0);
         std::fill(vol, vol + L.N, 0.0);
+        const double *x3[3] = {xyz, xyz, xyz};
+        hybrid_sides(x3, [&](int32_t p1, int32_t p2, const TetSideMoving &ts) {
+            vol[p1 - 1] += ts.nv[0];
+            vol[p2 - 1] += ts.nv[0];
+            V3 coef = ts.coef;
+            int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
+            if (i1 != p1) coef = scl(-1.0, coef);
+            const int32_t e = sides.find(i1, i2);
+            sw[e] = sw[e] + coef.x; sw[E + e] = sw[E + e] + coef.y; sw[2 * E + e] = sw[2 * E + e] + coef.z;
+        });
         for (int32_t t = 0; t < NT; ++t) {
             int32_t p[4];
             tet(t, p);
@@ -870,6 +1207,11 @@ struct Geometry {
                 bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
             }
         }
+        quad_sides(x3, [&](int32_t pa, int32_t pb, const TriSideMoving &ts) {
+            const int32_t b = bsides.find(std::min(pa, pb), std::max(pa, pb));
+            const V3 c = ts.coef;
+            bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
+        });
     }
     // The level-1 arrays of a moving mesh from the coordinates of the step
     // and of the two before, x[0..2]: the coefficients at the step, the
@@ -885,6 +1227,19 @@ struct Geometry {
         std::fill(gcl, gcl + 2 * E, 0.0);
         std::fill(bgcl, bgcl + 4 * B, 0.0);
         for (double *v : {vol, volp, volp2}) std::fill(v, v + L.N, 0.0);
+        auto add_side = [&](int32_t p1, int32_t p2, const TetSideMoving &ts) {
+            vol[p1 - 1] += ts.nv[0]; vol[p2 - 1] += ts.nv[0];
+            volp[p1 - 1] += ts.nv[1]; volp[p2 - 1] += ts.nv[1];
+            volp2[p1 - 1] += ts.nv[2]; volp2[p2 - 1] += ts.nv[2];
+            V3 coef = ts.coef;
+            double g0 = 0.5 * ts.gcl[0], g1 = 0.5 * ts.gcl[1];
+            int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
+            if (i1 != p1) { coef = scl(-1.0, coef); g0 = -g0; g1 = -g1; }
+            const int32_t e = sides.find(i1, i2);
+            sw[e] = sw[e] + coef.x; sw[E + e] = sw[E + e] + coef.y; sw[2 * E + e] = sw[2 * E + e] + coef.z;
+            gcl[e] = gcl[e] + g0; gcl[E + e] = gcl[E + e] + g1;
+        };
+        hybrid_sides(x, add_side);
         for (int32_t t = 0; t < NT; ++t) {
             int32_t p[4];
             tet(t, p);
@@ -893,20 +1248,19 @@ struct Geometry {
                 for (int k = 0; k < 4; ++k) xv[q][k] = X(x[q], p[k]);
             TetSideMoving ts[6];
             tet_sides_moving(xv, ts);
-            for (int k = 0; k < 6; ++k) {
-                int32_t p1 = p[ts[k].a], p2 = p[ts[k].b];
-                vol[p1 - 1] += ts[k].nv[0]; vol[p2 - 1] += ts[k].nv[0];
-                volp[p1 - 1] += ts[k].nv[1]; volp[p2 - 1] += ts[k].nv[1];
-                volp2[p1 - 1] += ts[k].nv[2]; volp2[p2 - 1] += ts[k].nv[2];
-                V3 coef = ts[k].coef;
-                double g0 = 0.5 * ts[k].gcl[0], g1 = 0.5 * ts[k].gcl[1];
-                int32_t i1 = std::min(p1, p2), i2 = p1 + p2 - i1;
-                if (i1 != p1) { coef = scl(-1.0, coef); g0 = -g0; g1 = -g1; }
-                const int32_t e = sides.find(i1, i2);
-                sw[e] = sw[e] + coef.x; sw[E + e] = sw[E + e] + coef.y; sw[2 * E + e] = sw[2 * E + e] + coef.z;
-                gcl[e] = gcl[e] + g0; gcl[E + e] = gcl[E + e] + g1;
-            }
+            for (int k = 0; k < 6; ++k) add_side(p[ts[k].a], p[ts[k].b], ts[k]);
         }
+        auto add_bside = [&](int32_t pa, int32_t pb, const TriSideMoving &ts) {
+            const int32_t b = bsides.find(std::min(pa, pb), std::max(pa, pb));
+            const V3 c = ts.coef;
+            bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
+            // the smaller node's weights first
+            const int s1 = pa < pb ? 0 : 1, s2 = 1 - s1;
+            bgcl[b] = bgcl[b] + 0.25 * ts.gcl[s1][0];
+            bgcl[B + b] = bgcl[B + b] + 0.25 * ts.gcl[s2][0];
+            bgcl[2 * B + b] = bgcl[2 * B + b] + 0.25 * ts.gcl[s1][1];
+            bgcl[3 * B + b] = bgcl[3 * B + b] + 0.25 * ts.gcl[s2][1];
+        };
         for (int32_t f = 0; f < NF; ++f) {
             int32_t p[3];
             tri(f, p);
@@ -915,22 +1269,13 @@ struct Geometry {
                 for (int k = 0; k < 3; ++k) xv[q][k] = X(x[q], p[k]);
             TriSideMoving ts[3];
             tri_sides_moving(xv, ts);
-            for (int k = 0; k < 3; ++k) {
-                const int32_t pa = p[ts[k].a], pb = p[ts[k].b];
-                const int32_t b = bsides.find(std::min(pa, pb), std::max(pa, pb));
-                const V3 c = ts[k].coef;
-                bw[b] = bw[b] + c.x; bw[B + b] = bw[B + b] + c.y; bw[2 * B + b] = bw[2 * B + b] + c.z;
-                // the smaller node's weights first
-                const int s1 = pa < pb ? 0 : 1, s2 = 1 - s1;
-                bgcl[b] = bgcl[b] + 0.25 * ts[k].gcl[s1][0];
-                bgcl[B + b] = bgcl[B + b] + 0.25 * ts[k].gcl[s2][0];
-                bgcl[2 * B + b] = bgcl[2 * B + b] + 0.25 * ts[k].gcl[s1][1];
-                bgcl[3 * B + b] = bgcl[3 * B + b] + 0.25 * ts[k].gcl[s2][1];
-            }
+            for (int k = 0; k < 3; ++k) add_bside(p[ts[k].a], p[ts[k].b], ts[k]);
         }
+        quad_sides(x, add_bside);
     }
     // xyz_bar = (d(sw, bw, vol)/d xyz)^T (sw_bar, bw_bar, vol_bar)
     void vjp(const double *xyz, const double *swb, const double *bwb, const double *volb, double *xb) const {
+        if (M.hybrid()) throw std::invalid_argument("the geometry derivative covers tetrahedral meshes");
         const size_t E = L.E, B = L.B, N = L.N;
         std::fill(xb, xb + 3 * N, 0.0);
         for (int32_t t = 0; t < NT; ++t) {
@@ -1195,6 +1540,44 @@ int fp_from_tets(int32_t nnodes, const double *xyz, int32_t ntet, const int32_t 
     });
 }
 
+int fp_from_elements(int32_t nnodes, const double *xyz, int32_t ntet, const int32_t *tets, int32_t npyr,
+                     const int32_t *pyrs, int32_t npri, const int32_t *pris, int32_t nhex, const int32_t *hexes,
+                     int32_t ntri, const int32_t *tris, const int32_t *tri_ind, int32_t nquad, const int32_t *quads,
+                     const int32_t *quad_ind, int nlevels, fp_mesh **out) {
+    return guarded([&] {
+        if (!out || !xyz || nnodes <= 0 || nlevels < 1 || ntet < 0 || npyr < 0 || npri < 0 || nhex < 0 || ntri < 0 ||
+            nquad < 0 || ntet + npyr + npri + nhex == 0 || ntri + nquad == 0)
+            return FLITE_EINVAL;
+        auto take = [&](const int32_t *a, int32_t n, int nv, const char *what) {
+            if (n > 0 && !a) throw std::invalid_argument(std::string("missing ") + what);
+            std::vector<int32_t> v(a ? a : nullptr, a ? a + (size_t)nv * n : nullptr);
+            for (auto x : v)
+                if (x < 1 || x > nnodes) throw std::runtime_error(std::string(what) + " index out of range");
+            return v;
+        };
+        auto inds = [&](const int32_t *a, int32_t n) {
+            if (n > 0 && !a) throw std::invalid_argument("missing boundary indicators");
+            std::vector<int32_t> v(a ? a : nullptr, a ? a + n : nullptr);
+            for (auto x : v)
+                if (x < 1 || x > 9) throw std::runtime_error("boundary indicator out of range");
+            return v;
+        };
+        auto M = std::make_unique<fp_mesh>();
+        std::vector<double> x(xyz, xyz + 3 * (size_t)nnodes);
+        Hybrid hy;
+        hy.hex = take(hexes, nhex, 8, "hexahedron");
+        hy.pri = take(pris, npri, 6, "prism");
+        hy.pyr = take(pyrs, npyr, 5, "pyramid");
+        hy.quad = take(quads, nquad, 4, "quadrilateral");
+        hy.quad_ind = inds(quad_ind, nquad);
+        build_fine(*M, nnodes, x, take(tets, ntet, 4, "tetrahedron"), take(tris, ntri, 3, "triangle"),
+                   inds(tri_ind, ntri), std::move(hy));
+        build_levels(*M, nlevels);
+        *out = M.release();
+        return FLITE_OK;
+    });
+}
+
 int fp_bump_channel(int nx, int ny, int nz, double bump_h, int nlevels, fp_mesh **out) {
     return guarded([&] {
         if (nx < 1 || ny < 1 || nz < 1) return FLITE_EINVAL;
@@ -1413,7 +1796,7 @@ int fp_node_perm(const fp_mesh *m, int32_t *perm) {
 }
 
 int fp_geometry(const fp_mesh *m, const double *xyz, double *side_w, double *bnd_w, double *volume) {
-    if (!m || m->lv.empty() || m->tets.empty() || !side_w || !bnd_w || !volume) return FLITE_EINVAL;
+    if (!m || m->lv.empty() || (m->tets.empty() && !m->hybrid()) || !side_w || !bnd_w || !volume) return FLITE_EINVAL;
     return guarded([&] {
         Geometry G(*m);
         G.eval(xyz ? xyz : m->lv[0].xyz.data(), side_w, bnd_w, volume);
@@ -1446,7 +1829,7 @@ int fp_coordinate_movement(fp_mesh *m, int32_t time_scheme) {
 
 int fp_set_moving_geometry(fp_mesh *m, const double *xyz, const double *xyz_prev, const double *xyz_prev2,
                            int32_t time_scheme) {
-    if (!m || m->lv.empty() || m->tets.empty() || !xyz || !xyz_prev || !xyz_prev2 ||
+    if (!m || m->lv.empty() || (m->tets.empty() && !m->hybrid()) || !xyz || !xyz_prev || !xyz_prev2 ||
         (time_scheme != 1 && time_scheme != 2))
         return FLITE_EINVAL;
     return guarded([&] {

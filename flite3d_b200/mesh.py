@@ -68,6 +68,40 @@ class Mesh:
         return cls(h)
 
     @classmethod
+    def from_elements(cls, xyz, tets=None, pyramids=None, prisms=None, hexes=None, tris=None, tri_indicator=None,
+                      quads=None, quad_indicator=None, nlevels=3):
+        """A mesh of hybrid elements: xyz (N, 3); tets (n, 4), pyramids
+        (n, 5), prisms (n, 6), hexes (n, 8); boundary tris (n, 3) and quads
+        (n, 4) with indicators; 1-based node numbers."""
+        xyz = np.asfortranarray(np.asarray(xyz, dtype=np.float64))
+        keep = []
+
+        def arr(a, k):
+            if a is None or len(a) == 0:
+                return 0, None
+            v = np.asfortranarray(np.asarray(a, dtype=np.int32).reshape(-1, k))
+            keep.append(v)
+            return v.shape[0], v.ctypes.data_as(ctypes.c_void_p)
+
+        def ind(a):
+            if a is None or len(a) == 0:
+                return None
+            v = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+            keep.append(v)
+            return v.ctypes.data_as(ctypes.c_void_p)
+        nt, pt = arr(tets, 4)
+        ny, py = arr(pyramids, 5)
+        npr, pp = arr(prisms, 6)
+        nh, ph = arr(hexes, 8)
+        nf, pf = arr(tris, 3)
+        nq, pq = arr(quads, 4)
+        h = ctypes.c_void_p()
+        _abi.check(_lib().fp_from_elements(xyz.shape[0], xyz.ctypes.data_as(ctypes.c_void_p), nt, pt, ny, py, npr, pp,
+                                           nh, ph, nf, pf, ind(tri_indicator), nq, pq, ind(quad_indicator),
+                                           int(nlevels), ctypes.byref(h)), "fp_from_elements")
+        return cls(h)
+
+    @classmethod
     def read_sol(cls, path):
         h = ctypes.c_void_p()
         _abi.check(_lib().fp_read_sol(str(path).encode(), ctypes.byref(h)), "fp_read_sol")

@@ -35,6 +35,21 @@ int fp_bump_channel(int nx, int ny, int nz, double bump_h, int nlevels,
 int fp_from_tets(int32_t nnodes, const double *xyz, int32_t ntet,
                  const int32_t *tets, int32_t ntri, const int32_t *tris,
                  const int32_t *tri_ind, int nlevels, fp_mesh **out);
+/* The same from hybrid elements (gen3d's element types): tetrahedra
+ * [4][ntet], pyramids [5][npyr] (base 1-2-3-4, apex 5), prisms [6][npri]
+ * (triangles 1-2-3 and 4-5-6, edge 1-4), hexahedra [8][nhex] (faces 1-2-3-4
+ * and 5-6-7-8, edge 1-5), boundary triangles [3][ntri] and quadrilaterals
+ * [4][nquad] with their indicators; any count may be 0 (the pointer then
+ * NULL).  Median-dual coefficients and volumes per element type as
+ * makeCalcDataForHex / Pri / Pyr / Tet (gen3d_grid.f90:902-2332, in that
+ * order) and makeCalcDataForBoundary (gen3d_boundary.f90:511-766); the face
+ * diagonals of hexahedra and prisms follow the lower boundary-first node
+ * number.  Elements must be positively oriented (FLITE_EINVAL otherwise);
+ * boundary faces are oriented here.                                          */
+int fp_from_elements(int32_t nnodes, const double *xyz, int32_t ntet, const int32_t *tets, int32_t npyr,
+                     const int32_t *pyrs, int32_t npri, const int32_t *pris, int32_t nhex, const int32_t *hexes,
+                     int32_t ntri, const int32_t *tris, const int32_t *tri_ind, int32_t nquad, const int32_t *quads,
+                     const int32_t *quad_ind, int nlevels, fp_mesh **out);
 /* Extruded NACA0012 O-grid: ni points around the section, nj cells from the
  * wall (nlayer cells from first_cell growing by `growth`, then stretched to a
  * circular far field of radius `farfield` chords), nk cells over `span`.

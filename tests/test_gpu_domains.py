@@ -1,7 +1,8 @@
-"""A parallel run's multi-domain .sol files ingested into one mesh and solved
-on the GPU: bit for bit against the CPU restatement on the ingested mesh, and
-bit for bit against the canonical form of the mesh the files were written
-from (the two are the same mesh).
+"""Meshes from other sources on the GPU: a parallel run's multi-domain .sol
+files ingested into one mesh, bit for bit against the CPU restatement on the
+ingested mesh and against the canonical form of the mesh the files were
+written from (the two are the same mesh); meshes of hexahedra, prisms and
+pyramids, bit for bit against the CPU restatement.
 """
 import numpy as np
 import pytest
@@ -35,3 +36,24 @@ def test_ingested_domains_solve_like_the_canonical_mesh(tmp_path, nd):
         s.close()
     for m in (merged, canon, mesh):
         m.close()
+
+
+@pytest.mark.parametrize("kind", ["hex", "prism", "pyramid", "mixed"])
+def test_hybrid_element_meshes_match(kind):
+    # meshes of gen3d's other element types run the same device path
+    from hybrid_meshes import box
+    mesh = box(8, 4, 4, kind=kind, nlevels=2)
+    c = default_controls(ReynoldsNumber=2000.0, wallsAreIsentropic=1, fluxType=1, CFLNumber=2.0,
+                         numberOfGridsToUse=2)
+    u0 = initial_state(c, mesh, perturb_seed=9, amplitude=0.02)
+    g, o = Solver(c, mesh), Solver(c, mesh, backend=oracle_backend())
+    for s in (g, o):
+        s.set_state(u0)
+        s.start()
+        for cyc in range(1, 4):
+            s.cycle(cyc)
+    for level in (1, 2):
+        assert np.array_equal(g.get_state(level), o.get_state(level)), (kind, level)
+    g.close()
+    o.close()
+    mesh.close()

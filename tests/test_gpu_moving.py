@@ -34,10 +34,10 @@ CASES = {
     "central": dict(),
     "central_bdf1": dict(timeScheme=1),
     "fv_boundary": dict(boundaryTerm=2),
-    "llf": dict(fluxType=2),
-    "roe": dict(fluxType=3),
-    "hllc1": dict(fluxType=4, HLLCFluxOrder=1),
-    "hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1),
+    "llf": dict(fluxType=2, CFLNumber=0.5),
+    "roe": dict(fluxType=3, CFLNumber=1.0),
+    "hllc1": dict(fluxType=4, HLLCFluxOrder=1, CFLNumber=1.0),
+    "hllc2": dict(fluxType=4, HLLCFluxOrder=2, Automaticlipping=1, CFLNumber=1.0),
     "laminar": dict(ReynoldsNumber=500.0, CFLNumber=1.0, wallsAreIsentropic=1),
     "laminar_isothermal": dict(ReynoldsNumber=500.0, CFLNumber=1.0, wallsAreIsentropic=0),
     "sa": dict(ReynoldsNumber=1.0e5, CFLNumber=1.0, turbulenceModel=1, wallsAreIsentropic=1),
@@ -77,6 +77,7 @@ def test_moving_mesh_steps_match(name, lanes):
             o.cycle(it)
         for level in range(1, 4):
             a, b = g.get_state(level), o.get_state(level)
+            assert np.all(np.isfinite(b)), (name, step, level)
             assert np.array_equal(a, b), (name, step, level, np.abs(a - b).max())
         assert np.allclose(g.residuals()[0], o.residuals()[0], rtol=1e-12, atol=0)
         assert np.allclose(g.forces(), o.forces(), rtol=1e-12, atol=1e-300)
