@@ -51,6 +51,8 @@ _CONTROL_FIELDS = [
     ("patchInitialization", _i), ("nspan", _i), ("timeScheme", _i), ("numberOfRSSteps", _i),
     ("numberOfPSSteps", _i), ("residualSmoothingFactor", _d),
     ("prolongationSmoothingFactor", _d), ("physicalTimeStep", _d), ("engineBCRelaxation", _d),
+    ("engineFlowType", _i), ("numberOfEORelaxationSteps", _i), ("enginesFrontMassFlow", _d * 2),
+    ("enginesRearParameters", _d * 14),
     ("inflowField", _d * 12),
     ("precision", _i), ("reconstruction", _i), ("rungeKuttaStages", _i),
 ]
@@ -78,6 +80,7 @@ class LevelDesc(ctypes.Structure):
         ("node_reg", _P), ("node_ind", _P), ("volume", _P), ("wall_dist", _P), ("coords", _P),
         ("coord_move", _P), ("parent", _P), ("rweight", _P),
         ("side_gcl", _P), ("bnd_gcl", _P), ("volume_prev", _P), ("volume_prev2", _P),
+        ("n_engine_sides", ctypes.c_int32), ("engine_idx", _P), ("engine_w", _P),
     ]
 
 

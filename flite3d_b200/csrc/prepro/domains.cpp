@@ -249,7 +249,21 @@ void write_domain_level(fio::Writer &w, const LevelData &L, const std::vector<in
         for (int32_t j = 0; j < Nb; ++j)
             if (o2n[j] > 0 && L.bnd_indicator[j] == ind)
                 w.i4(o2n[j]).r8(nrm[3 * (size_t)j]).r8(nrm[3 * (size_t)j + 1]).r8(nrm[3 * (size_t)j + 2]).end();
-    w.i4(0).end();  // engine inlet sides
+    // engine inlet sides, each in the lower domain of its two nodes
+    // (gen3d_grid.f90:4599-4630)
+    {
+        const int32_t n = L.nes();
+        int32_t cnt = 0;
+        for (int32_t s = 0; s < n; ++s)
+            if (lower(L.eside[s] - 1, L.eside[(size_t)n + s] - 1) == d) cnt++;
+        w.i4(cnt).end();
+        for (int32_t s = 0; s < n; ++s) {
+            const int32_t a = L.eside[s] - 1, b = L.eside[(size_t)n + s] - 1;
+            if (lower(a, b) != d) continue;
+            w.i4(o2n[a]).i4(o2n[b]).i4(L.eside[2 * (size_t)n + s]);
+            w.r8(L.ew[s]).r8(L.ew[(size_t)n + s]).r8(L.ew[2 * (size_t)n + s]).end();
+        }
+    }
     // sides
     int32_t ns = 0, ncs = 0;
     for (int32_t e = 0; e < E; ++e)
@@ -392,6 +406,8 @@ struct DomLevel {
     int32_t N = 0, nbnd = 0;
     int32_t reg[21] = {0};
     std::vector<int32_t> bs1, bs2, bind, s1, s2, node_ind;  // local, 1-based
+    std::vector<int32_t> es1, es2, ein;                     // engine inlet sides, local
+    std::vector<double> ew;                                 // [n][3]
     std::vector<double> bw, bgcl, sw, gcl, slen;           // [B][3], [B][4], [E][3], [E][2], [E]
     std::vector<double> vol, volp, volp2, wdist, xyz, xyzp, xyzp2;  // by local node (0-based)
     std::vector<int32_t> wnode, seed;
@@ -415,7 +431,13 @@ DomLevel read_domain_level(fio::Reader &r, bool fine, int nd) {
     r.next(); D.nbnd = r.i4(); const int32_t nn = r.i4();
     for (int j = 0; j < 21; ++j) { r.next(); D.reg[j] = r.i4(); }
     for (int32_t i = 0; i < nn; ++i) { r.next(); D.node_ind.push_back(r.i4()); }
-    r.next(); if (r.i4() != 0) throw std::runtime_error("engine inlet sides are not supported");
+    r.next(); const int32_t neis = r.i4();
+    if (neis < 0) throw fio::io_error("negative count");
+    for (int32_t s = 0; s < neis; ++s) {
+        r.next();
+        D.es1.push_back(r.i4()); D.es2.push_back(r.i4()); D.ein.push_back(r.i4());
+        for (int k = 0; k < 3; ++k) D.ew.push_back(r.r8());
+    }
     r.next(); const int32_t E = r.i4();
     if (E < 0) throw fio::io_error("negative count");
     for (int32_t e = 0; e < E; ++e) {
@@ -670,16 +692,27 @@ int fp_read_sol_domains(const char *prefix, const char *plotreg, fp_mesh **out) 
             // sides and boundary sides, each once (in its lower domain)
             for (int d = 1; d <= nd; ++d) {
                 const DomLevel &D = dom[d][l];
+                auto gid = [&](int32_t loc) {  // global 1-based number of a local node
+                    if (loc < 1 || loc > D.N) throw fio::io_error("side record node out of range");
+                    return glob[d][loc - 1] + 1;
+                };
                 for (size_t e = 0; e < D.s1.size(); ++e) {
-                    L.side.push_back(glob[d][D.s1[e] - 1] + 1);
-                    L.side.push_back(glob[d][D.s2[e] - 1] + 1);
+                    L.side.push_back(gid(D.s1[e]));
+                    L.side.push_back(gid(D.s2[e]));
                     for (int k = 0; k < 3; ++k) L.sw.push_back(D.sw[3 * e + k]);
                     L.gcl.push_back(D.gcl[2 * e]); L.gcl.push_back(D.gcl[2 * e + 1]);
                     L.slen.push_back(D.slen[e]);
                 }
+                for (size_t s = 0; s < D.es1.size(); ++s) {
+                    if (D.ein[s] < 1 || D.ein[s] > 2) throw fio::io_error("bad engine inlet number");
+                    L.eside.push_back(gid(D.es1[s]));
+                    L.eside.push_back(gid(D.es2[s]));
+                    L.eside.push_back(D.ein[s]);
+                    for (int k = 0; k < 3; ++k) L.ew.push_back(D.ew[3 * s + k]);
+                }
                 for (size_t b = 0; b < D.bs1.size(); ++b) {
-                    L.bside.push_back(glob[d][D.bs1[b] - 1] + 1);
-                    L.bside.push_back(glob[d][D.bs2[b] - 1] + 1);
+                    L.bside.push_back(gid(D.bs1[b]));
+                    L.bside.push_back(gid(D.bs2[b]));
                     L.bside.push_back(D.bind[b]);
                     for (int k = 0; k < 3; ++k) L.bw.push_back(D.bw[3 * b + k]);
                     for (int k = 0; k < 4; ++k) L.bgcl.push_back(D.bgcl[4 * b + k]);
@@ -702,6 +735,7 @@ int fp_read_sol_domains(const char *prefix, const char *plotreg, fp_mesh **out) 
             L.B = (int32_t)(L.bw.size() / 3);
             transpose_i(L.side, L.E, 2); transpose(L.sw, L.E, 3); transpose(L.gcl, L.E, 2);
             transpose_i(L.bside, L.B, 3); transpose(L.bw, L.B, 3); transpose(L.bgcl, L.B, 4);
+            transpose_i(L.eside, L.ew.size() / 3, 3); transpose(L.ew, L.ew.size() / 3, 3);
             // coarse levels: parents and restriction weights of the finer
             // level's nodes
             if (l > 0) {

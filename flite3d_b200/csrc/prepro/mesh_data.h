@@ -37,6 +37,12 @@ struct LevelData {
     // the coarse boundary side of each finer one (negative where its two
     // nodes swap)
     std::vector<int32_t> side_of, bside_of;
+    // engine inlet sides (makeEngineInflowData, gen3d_boundary.f90:768-920;
+    // coarse levels agglomerateBoundary :1061-1099): (i1 <= i2, inlet 1|2)
+    // and the coefficient vector of each, [3][n] column-major, 1-based
+    std::vector<int32_t> eside;
+    std::vector<double> ew;
+    int32_t nes() const { return (int32_t)(eside.size() / 3); }
 };
 
 }  // namespace fp_internal

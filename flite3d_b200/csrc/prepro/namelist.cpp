@@ -5,7 +5,8 @@
 // (def_par:213, 384; SolverExampleInput/C13_1.inp:1-84).  This reader accepts
 // that form: items separated by commas or blanks, '!' comments, logicals as
 // .true./.false./T/F, reals with E or D exponents, quoted strings, and the
-// array elements datum(i) and inflowField(i,j).  Keys are matched without
+// array elements datum(i), inflowField(i,j), enginesFrontMassFlow(i) and
+// enginesRearParameters(i,j).  Keys are matched without
 // regard to case, as Fortran does.  Keys the hot path does not use are listed
 // back to the caller and otherwise ignored.
 #include <cctype>
@@ -53,7 +54,8 @@ const Field kFields[] = {
     {"explicit", LOG, offsetof(flite_controls, explicit_)}, F_L(SAS), F_L(GUSTMODEL),
     F_L(movingwall), F_L(patchInitialization), F_I(nspan), F_I(timeScheme), F_I(numberOfRSSteps),
     F_I(numberOfPSSteps), F_D(residualSmoothingFactor), F_D(prolongationSmoothingFactor),
-    F_D(physicalTimeStep), F_D(engineBCRelaxation),
+    F_D(physicalTimeStep), F_D(engineBCRelaxation), F_I(engineFlowType),
+    F_I(numberOfEORelaxationSteps),
 };
 
 bool ieq(const std::string &a, const char *b) {
@@ -163,13 +165,20 @@ extern "C" int fp_parse_inp_text(const char *text, flite_controls *c, char *unkn
                 done = true;
                 break;
             }
-        } else if (ieq(base, "datum") || ieq(base, "inflowField")) {
+        } else if (ieq(base, "datum") || ieq(base, "inflowField") || ieq(base, "enginesFrontMassFlow") ||
+                   ieq(base, "enginesRearParameters")) {
             int i = 0, j = 1;
             if (std::sscanf(idx.c_str(), "(%d,%d)", &i, &j) < 1) return FLITE_EIO;
             double d; if (!parse_real(val, &d)) return FLITE_EIO;
             if (ieq(base, "datum") && i >= 1 && i <= 3) { c->datum[i - 1] = d; done = true; }
             if (ieq(base, "inflowField") && i >= 1 && i <= 6 && j >= 1 && j <= 2) {
                 c->inflowField[(j - 1) * 6 + (i - 1)] = d; done = true;
+            }
+            if (ieq(base, "enginesFrontMassFlow") && i >= 1 && i <= 2) {
+                c->enginesFrontMassFlow[i - 1] = d; done = true;
+            }
+            if (ieq(base, "enginesRearParameters") && i >= 1 && i <= 7 && j >= 1 && j <= 2) {
+                c->enginesRearParameters[(j - 1) * 7 + (i - 1)] = d; done = true;
             }
         }
         if (!done) {

@@ -567,6 +567,54 @@ struct Hybrid {
     std::vector<int32_t> hex, pri, pyr, quad, quad_ind;
 };
 
+// The engine inlet sides of a level under construction: a side is found by
+// its node pair and its coefficients are summed; a new one is appended with
+// its inlet number (registerEngineInletSide, gen3d_boundary.f90:431-485, and
+// its coarse-level form in agglomerateBoundary :1061-1099).
+struct EngineSideSet {
+    std::map<std::pair<int32_t, int32_t>, int32_t> at;
+    std::vector<int32_t> a, b, inlet;
+    std::vector<V3> w;
+    void add(int32_t p1, int32_t p2, V3 c, int32_t in) {
+        const std::pair<int32_t, int32_t> key{std::min(p1, p2), std::max(p1, p2)};
+        auto it = at.find(key);
+        if (it != at.end()) { w[it->second] = w[it->second] + c; return; }
+        at.emplace(key, (int32_t)a.size());
+        a.push_back(key.first); b.push_back(key.second); inlet.push_back(in); w.push_back(c);
+    }
+    void store(LevelData &L) const {
+        const size_t n = a.size();
+        L.eside.resize(3 * n); L.ew.resize(3 * n);
+        for (size_t s = 0; s < n; ++s) {
+            L.eside[s] = a[s]; L.eside[n + s] = b[s]; L.eside[2 * n + s] = inlet[s];
+            L.ew[s] = w[s].x; L.ew[n + s] = w[s].y; L.ew[2 * n + s] = w[s].z;
+        }
+    }
+};
+
+// The engine inlet sides of one boundary face of indicator 5 (inlet 1) or 6
+// (inlet 2), from the face's median-dual pieces (makeEngineInflowData,
+// triangles gen3d_boundary.f90:790-843, quadrilaterals :846-916).  The faces
+// are taken in the orientation the preprocessor gives them (right-hand normal
+// into the domain), so the coefficients point out of the domain and the mass
+// flow into an engine is positive.
+void engine_tri_sides(const int32_t p[3], const V3 x[3], int32_t inlet, EngineSideSet &es) {
+    const V3 xm = div3((x[0] + x[1]) + x[2]);
+    const V3 xb1 = scl(0.5, x[0] + x[1]), xb2 = scl(0.5, x[1] + x[2]), xb3 = scl(0.5, x[2] + x[0]);
+    es.add(p[0], p[1], halfcross(xm - x[0], xb1 - x[0]), inlet);
+    es.add(p[0], p[2], halfcross(xb3 - x[0], xm - x[0]), inlet);
+    es.add(p[1], p[2], halfcross(xm - x[1], xb2 - x[1]), inlet);
+}
+void engine_quad_sides(const int32_t p[4], const V3 x[4], int32_t inlet, EngineSideSet &es) {
+    const V3 xm = scl(0.25, ((x[0] + x[1]) + x[2]) + x[3]);
+    const V3 xb1 = scl(0.5, x[0] + x[1]), xb2 = scl(0.5, x[1] + x[2]), xb3 = scl(0.5, x[2] + x[3]),
+             xb4 = scl(0.5, x[0] + x[3]);
+    es.add(p[0], p[1], halfcross(xm - x[0], xb1 - x[0]), inlet);
+    es.add(p[0], p[3], halfcross(xb4 - x[0], xm - x[0]), inlet);
+    es.add(p[2], p[1], halfcross(xb2 - x[2], xm - x[2]), inlet);
+    es.add(p[2], p[3], halfcross(xm - x[2], xb3 - x[2]), inlet);
+}
+
 void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
                 std::vector<int32_t> tets_old, std::vector<int32_t> tris_old,
                 const std::vector<int32_t> &tri_ind, Hybrid hy = Hybrid{}) {
@@ -821,6 +869,7 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
             b1.push_back(i1); b2.push_back(i2); bi.push_back(ind); bc.push_back(coef);
         }
     };
+    EngineSideSet esides;
     std::vector<int32_t> tris_new(3 * (size_t)NF);
     for (int32_t f = 0; f < NF; ++f) {
         int32_t p1 = tris_old[f], p2 = tris_old[(size_t)NF + f], p3 = tris_old[2 * (size_t)NF + f];
@@ -835,6 +884,7 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         TriSide<double> ts[3];
         tri_sides(xv, ts);
         for (int k = 0; k < 3; ++k) register_bside(pv[ts[k].a], pv[ts[k].b], ts[k].coef, ind);
+        if (ind == 5 || ind == 6) engine_tri_sides(pv, xv, ind - 4, esides);
     }
     // quadrilateral faces after the triangles (makeCalcDataForBoundary
     // gen3d_boundary.f90:627-766), oriented like them
@@ -853,7 +903,9 @@ void build_fine(fp_mesh &M, int32_t N, const std::vector<double> &xyz_old,
         TriSideMoving ts[4];
         quad_sides_moving(xv, ts);
         for (int k = 0; k < 4; ++k) register_bside(p[ts[k].a], p[ts[k].b], ts[k].coef, hy.quad_ind[f]);
+        if (hy.quad_ind[f] == 5 || hy.quad_ind[f] == 6) engine_quad_sides(p, xv[0], hy.quad_ind[f] - 4, esides);
     }
+    esides.store(L);
     L.B = (int32_t)b1.size();
     L.bside.resize(3 * (size_t)L.B); L.bw.resize(3 * (size_t)L.B);
     for (int32_t b = 0; b < L.B; ++b) {
@@ -1053,6 +1105,17 @@ void agglomerate(const LevelData &F, LevelData &C) {
     for (int32_t b = 0; b < C.B; ++b) {
         C.bside[b] = b1[b]; C.bside[(size_t)C.B + b] = b2[b]; C.bside[2 * (size_t)C.B + b] = bi[b];
         C.bw[b] = bc[b].x; C.bw[(size_t)C.B + b] = bc[b].y; C.bw[2 * (size_t)C.B + b] = bc[b].z;
+    }
+    // coarse engine inlet sides: a side whose two nodes fall in one aggregate
+    // is kept (agglomerateBoundary, gen3d_boundary.f90:1061-1099)
+    {
+        EngineSideSet es;
+        const int32_t n = F.nes();
+        for (int32_t s = 0; s < n; ++s) {
+            const int32_t c1 = C.parent[F.eside[s] - 1], c2 = C.parent[F.eside[(size_t)n + s] - 1];
+            es.add(c1, c2, {F.ew[s], F.ew[(size_t)n + s], F.ew[2 * (size_t)n + s]}, F.eside[2 * (size_t)n + s]);
+        }
+        es.store(C);
     }
     C.bnd_indicator.assign(ncb, 0);
     for (int32_t i = 0; i < F.Nb; ++i) {
@@ -1490,6 +1553,26 @@ void fp_internal::canonicalize(fp_mesh &M) {
             }
             L.bside.swap(bside); L.bw.swap(bw); L.bgcl.swap(bgcl);
         }
+        // engine inlet sides, in node-pair order
+        {
+            const int32_t n = L.nes();
+            std::vector<int32_t> a(n), b(n), ord(n);
+            for (int32_t s = 0; s < n; ++s) {
+                int32_t x = newid[L.eside[s] - 1] + 1, y = newid[L.eside[(size_t)n + s] - 1] + 1;
+                a[s] = std::min(x, y); b[s] = std::max(x, y); ord[s] = s;
+            }
+            std::stable_sort(ord.begin(), ord.end(), [&](int32_t p, int32_t q) {
+                return a[p] != a[q] ? a[p] < a[q] : b[p] < b[q];
+            });
+            std::vector<int32_t> es(3 * (size_t)n);
+            std::vector<double> ew(3 * (size_t)n);
+            for (int32_t k = 0; k < n; ++k) {
+                const int32_t s = ord[k];
+                es[k] = a[s]; es[(size_t)n + k] = b[s]; es[2 * (size_t)n + k] = L.eside[2 * (size_t)n + s];
+                for (int c = 0; c < 3; ++c) ew[(size_t)c * n + k] = L.ew[(size_t)c * n + s];
+            }
+            L.eside.swap(es); L.ew.swap(ew);
+        }
         build_register(L);
     }
     // the maps from finer to coarse sides of the canonical levels
@@ -1786,6 +1869,9 @@ int fp_level_desc(const fp_mesh *m, int level, flite_level_desc *o) {
     o->volume_prev2 = L.volp2.empty() || level > 1 ? nullptr : L.volp2.data();
     o->parent = L.parent.empty() ? nullptr : L.parent.data();
     o->rweight = L.rweight.empty() ? nullptr : L.rweight.data();
+    o->n_engine_sides = L.nes();
+    o->engine_idx = L.eside.empty() ? nullptr : L.eside.data();
+    o->engine_w = L.ew.empty() ? nullptr : L.ew.data();
     return FLITE_OK;
 }
 
@@ -1997,7 +2083,12 @@ int fp_write_sol(const fp_mesh *m, const char *path) {
             for (int32_t i = 0; i < nn; ++i)
                 w.i4(L.node_ind[i]).r8(L.bnormal[i]).r8(L.bnormal[(size_t)nn + i])
                     .r8(L.bnormal[2 * (size_t)nn + i]).end();
-            w.i4(0).end();  // engine inlet sides
+            // engine inlet sides (def_par:852-864)
+            const int32_t ne = L.nes();
+            w.i4(ne).end();
+            for (int32_t s = 0; s < ne; ++s)
+                w.i4(L.eside[s]).i4(L.eside[(size_t)ne + s]).i4(L.eside[2 * (size_t)ne + s])
+                    .r8(L.ew[s]).r8(L.ew[(size_t)ne + s]).r8(L.ew[2 * (size_t)ne + s]).end();
             // sides
             w.i4(L.E).end();
             for (int32_t e = 0; e < L.E; ++e) {
@@ -2085,8 +2176,14 @@ int fp_read_sol(const char *path, fp_mesh **out) {
                 if (r.remaining() >= 24)
                     for (int k = 0; k < 3; ++k) L.bnormal[(size_t)k * nn + i] = r.r8();
             }
-            r.next(); int32_t neis = r.i4();
-            if (neis != 0) throw std::runtime_error("engine inlet sides are not supported");
+            r.next(); const int32_t neis = r.i4();
+            if (neis < 0) throw std::runtime_error("negative engine inlet side count");
+            L.eside.resize(3 * (size_t)neis); L.ew.resize(3 * (size_t)neis);
+            for (int32_t s = 0; s < neis; ++s) {
+                r.next();
+                for (int k = 0; k < 3; ++k) L.eside[(size_t)k * neis + s] = r.i4();
+                for (int k = 0; k < 3; ++k) L.ew[(size_t)k * neis + s] = r.r8();
+            }
             r.next(); L.E = r.i4();
             L.side.resize(2 * (size_t)L.E); L.sw.resize(3 * (size_t)L.E); L.slen.resize(L.E);
             L.gcl.resize(2 * (size_t)L.E);
@@ -2098,6 +2195,11 @@ int fp_read_sol(const char *path, fp_mesh **out) {
                 L.slen[e] = r.r8();
             }
             r.next(); L.N = r.i4();
+            for (int32_t s = 0; s < neis; ++s) {
+                const int32_t a = L.eside[s], b = L.eside[(size_t)neis + s], in = L.eside[2 * (size_t)neis + s];
+                if (a < 1 || a > L.N || b < 1 || b > L.N || in < 1 || in > 2)
+                    throw fio::io_error("bad engine inlet side record");
+            }
             L.vol.resize(L.N); L.wdist.resize(L.N); L.wnode.resize(L.N);
             if (fine) {
                 L.xyz.resize(3 * (size_t)L.N); L.xyzp.resize(3 * (size_t)L.N); L.xyzp2.resize(3 * (size_t)L.N);

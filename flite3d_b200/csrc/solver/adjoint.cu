@@ -128,7 +128,8 @@ __global__ void k_vjp_node(Params P, LevelView L, const double *x, const double 
 extern "C" int flite_residual_vjp(flite_ctx *ctx, int level, const double *u, const double *rbar, double *ubar) {
     if (!ctx || level < 1 || level > (int)ctx->lv.size() || !u || !rbar || !ubar) return FLITE_EINVAL;
     // the transpose of the static-mesh residual (no GCL terms)
-    if (ctx->c.fluxType != 1 || ctx->c.precision != FLITE_FP64 || ctx->c.flowType == 2) return FLITE_EUNSUPPORTED;
+    if (ctx->c.fluxType != 1 || ctx->c.precision != FLITE_FP64 || ctx->c.flowType == 2 || ctx->P.engines)
+        return FLITE_EUNSUPPORTED;  // the products of the engine-free residual
     try {
         flite_ctx &X = *ctx;
         LevelView &L = X.V(level - 1);

@@ -476,6 +476,19 @@ struct flite_ctx {
         counted();
         launch_node_update(l, mode, stage, anchor);
     }
+    // the level-1 engine inlet terms after a node pass of `mode` (engine.cu)
+    void engine_pass(int l, int mode) {
+        const LevelView &L = V(l);
+        if (l != 0 || !L.eng.f) return;
+        counted();
+        k_engine_sums<<<1, kEngineLanes, 0, s>>>(P, L, mode);
+        const bool all = P.eftype == 2;
+        const int n = all ? L.N : L.eng.nnode;
+        if (n > 0) {
+            counted();
+            k_engine_finish<<<nblk(n), nb, 0, s>>>(P, L, mode, all ? 1 : 0);
+        }
+    }
     void launch_node_update(int l, int mode, int stage, bool anchor) {
         switch (lanes_of(l)) {
             case 4: launch_node_update_u<4>(l, mode, stage, anchor); break;
@@ -545,6 +558,7 @@ struct flite_ctx {
             rhs_terms(l, st == 1);
             sa_stage(l, MODE_STAGE, st);
             node_update(l, MODE_STAGE, st, st == 1);
+            engine_pass(l, MODE_STAGE);
         }
     }
     // ---- doTimeIterations (def_par:966-1000) -----------------------------
@@ -589,6 +603,7 @@ struct flite_ctx {
         if (turb()) sa_diffusion(fl);  // the fine level keeps its turbulent time steps
         sa_stage(fl, MODE_RFINE, 0);
         node_update(fl, MODE_RFINE, 0, false);
+        engine_pass(fl, MODE_RFINE);
         counted();
         k_restrict_incr<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
     }
@@ -599,6 +614,7 @@ struct flite_ctx {
         k_prolong_coarse<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
         counted();
         k_prolong_fine<<<nblk(V(fl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        engine_pass(fl, MODE_PROLONG);
     }
     // the head of a physical time step (mg_par:586-602): laminar viscosity
     // 1/Re on every level, u (and in unsteady runs uold) restricted to every

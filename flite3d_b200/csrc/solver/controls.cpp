@@ -41,6 +41,8 @@ extern "C" int FLITE_CONTROLS_FN(controls_default)(flite_controls *c) {
     c->movingwall = 0;
     c->wallTemperature = 528.0;
     c->patchInitialization = 0;
+    c->engineFlowType = 1;  // enginesFrontMassFlow, enginesRearParameters = 0
+    c->numberOfEORelaxationSteps = 0;
     c->engineBCRelaxation = 1.0;
     c->dissipationScheme = 2;
     c->coarseGridDissipationScheme = 2;

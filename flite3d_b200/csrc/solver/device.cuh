@@ -9,8 +9,15 @@
 namespace flite {
 
 // Node boundary classes, from the indicator ranges of nodeIndicatorRegister
-// (def_par:4033-4042): 1 wall, 2 symmetry, 3/4 far field, 9 inviscid wall.
-enum : unsigned char { BC_NONE = 0, BC_WALL = 1, BC_SYM = 2, BC_FAR3 = 3, BC_FAR4 = 4, BC_IWALL = 9 };
+// (def_par:4033-4042): 1 wall, 2 symmetry, 3/4 far field, 5/6 engine inlets
+// 1 and 2, 7/8 engine exhausts 1 and 2, 9 inviscid wall.
+enum : unsigned char {
+    BC_NONE = 0, BC_WALL = 1, BC_SYM = 2, BC_FAR3 = 3, BC_FAR4 = 4,
+    BC_EIN1 = 5, BC_EIN2 = 6, BC_EOUT1 = 7, BC_EOUT2 = 8, BC_IWALL = 9
+};
+__device__ __forceinline__ bool is_engine(unsigned char c) { return c >= BC_EIN1 && c <= BC_EOUT2; }
+__device__ __forceinline__ bool is_inlet(unsigned char c) { return c == BC_EIN1 || c == BC_EIN2; }
+__device__ __forceinline__ bool is_exhaust(unsigned char c) { return c == BC_EOUT1 || c == BC_EOUT2; }
 
 struct Params {
     double gamma, gm1, CFL, maxInc, minRho, Re, am, k2, k4, cgdf, pts, Tinf, mach;
@@ -32,6 +39,33 @@ struct Params {
     // Spalart-Allmaras (turbulenceModel 1)
     int sa, nTurbGrids;
     double turbCFL, turbK, maxTurb, turbProlRelax, oPrt;
+    // engine boundary conditions (def_par:4488-4918, 5084-5125): engines
+    // set when the mesh has engine faces or nodes; the inlet mass flow kind
+    // (engineFlowType), the cycles of the exhaust ramp, the increment
+    // relaxation of the inlets, the mass flow targets and the exhaust states
+    // (enginesRearParameters(7,2), column-major)
+    int engines, eftype, eoSteps;
+    double engRelax;
+    double front[2];
+    double rear[14];
+};
+
+// The level-1 engine inlet terms: the sides with their nodes, inlet (0|1)
+// and coefficients; the engine nodes; the exhaust pressure each node pass
+// leaves in pbc; and the factors and the go-ahead of the inlet scaling
+// (scale = 0 where engineFlowType 2 jumps past it, def_par:4784-4801).
+struct EngineFactors {
+    double fac[2];
+    int scale;
+};
+struct EngineView {
+    int nside, nnode;
+    const int2 *side;            // [nside]
+    const int *inlet;            // [nside]
+    const double *wx, *wy, *wz;  // [nside]
+    const int *node;             // [nnode] the level's engine nodes
+    double *pbc;                 // [N]
+    EngineFactors *f;
 };
 
 // Records gathered by node kernels from a node's incident edges and from its
@@ -160,6 +194,7 @@ struct LevelView {
     // numbering is the caller's
     const int *perm;                       // [N]
     TileView tile;                         // staging of node blocks (fluxType 1)
+    EngineView eng;                        // level 1 of a mesh with engines; zero otherwise
 };
 
 __device__ __forceinline__ EdgeW load_edgew(const EdgeW *w, int e) {
@@ -251,6 +286,10 @@ __device__ __forceinline__ void bc_increment(const Params &P, unsigned char cls,
         }
     } else if (cls == BC_IWALL || cls == BC_SYM) {
         remove_normal(r, n0, n1, n2, 1.0);
+    } else if (is_inlet(cls)) {  // engine inlets relaxed (def_par:5084-5099)
+        for (int c = 0; c < 5; ++c) r[c] = P.engRelax * r[c];
+    } else if (is_exhaust(cls)) {  // engine exhausts held (def_par:5100-5125)
+        for (int c = 0; c < 5; ++c) r[c] = 0.0;
     }
 }
 
@@ -301,6 +340,27 @@ __device__ __forceinline__ double relax_param(const Params &P, int cycle) {
         return dmin(r, 1.0);
     }
     return 1.0;
+}
+
+// ramp of the engine exhaust state (def_par:4490-4495)
+__device__ __forceinline__ double eo_relax(const Params &P, int cycle) {
+    if (P.eoSteps > 0) {
+        double r = (double)(cycle - 1) / (double)P.eoSteps;
+        return dmin(r, 1.0);
+    }
+    return 1.0;
+}
+
+// the state of an engine exhaust node (def_par:4497-4540); returns the
+// exhaust pressure, which the reference stores into grp%p
+__device__ __forceinline__ double bc_exhaust(const Params &P, unsigned char cls, double rp, double *u) {
+    const double *rear = &P.rear[cls == BC_EOUT1 ? 0 : 7];
+    for (int c = 0; c < 5; ++c) u[c] = (1.0 - rp) * P.inf[c] + rp * rear[c];
+    return (1.0 - rp) * P.inf[5] + rp * rear[5];
+}
+// the exhaust nu~ (def_par:4507-4509, 4528-4530)
+__device__ __forceinline__ double sa_exhaust(const Params &P, unsigned char cls, double rp) {
+    return rp * P.rear[cls == BC_EOUT1 ? 6 : 13];
 }
 
 // density update with the increment clip (def_par:1343-1366)

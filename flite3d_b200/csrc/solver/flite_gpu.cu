@@ -297,6 +297,11 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         P.turbCFL = c->turbulentCFLNumber; P.turbK = c->turbK; P.maxTurb = c->maxTurbulenceValue;
         P.turbProlRelax = c->turbProlongationRelaxation;
         P.oPrt = c->turbulentPrandtlNumber > 0 ? 1. / c->turbulentPrandtlNumber : 0.0;
+        P.engines = 0;  // set from level 1 below
+        P.eftype = c->engineFlowType; P.eoSteps = c->numberOfEORelaxationSteps;
+        P.engRelax = c->engineBCRelaxation;
+        for (int k = 0; k < 2; ++k) P.front[k] = c->enginesFrontMassFlow[k];
+        for (int k = 0; k < 14; ++k) P.rear[k] = c->enginesRearParameters[k];
 
         int G = nlevels;
         if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);  // mg_par:1212-1214
@@ -360,6 +365,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 L = donor->lv[l].v;  // mesh arrays shared; state set below
                 D.wall = donor->lv[l].wall;
                 D.d_wall = donor->lv[l].d_wall;
+                if (l == 0) P.engines = donor->P.engines;
             } else {
             // edges
             std::vector<int2> edge(E);
@@ -375,7 +381,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                 if (a < 0 || a >= N || q < 0 || q >= N) throw std::runtime_error("boundary edge index out of range");
                 bedge[b] = make_int2(a, q);
                 bind[b] = d.bnd_idx[2 * (size_t)B + b];
-                if (bind[b] >= 5 && bind[b] <= 8) return FLITE_EUNSUPPORTED;  // engine faces
+                if (l == 0 && bind[b] >= 5 && bind[b] <= 8) P.engines = 1;  // engine faces
             }
             // node -> incident edges in edge order
             std::vector<int> ip(N + 1, 0);
@@ -413,7 +419,6 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
                     if (ib < 1 || ib > d.n_normals) throw std::runtime_error("indicator register out of range");
                     int n = d.node_ind[ib - 1] - 1;
                     if (n < 0 || n >= N) throw std::runtime_error("indicator node out of range");
-                    if (k >= 5 && k <= 8) return FLITE_EUNSUPPORTED;  // engine nodes
                     bc[n] = (unsigned char)cls_of[k];
                     if (l == 0 && k == 1) D.wall.push_back(n);
                 }
@@ -425,6 +430,38 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             L.binc_ptr = X.upload(bp); L.binc = X.upload(binc);
             L.conn = X.upload(conn);
             L.bc = X.upload(bc);
+            L.eng = EngineView{};
+            if (l == 0) {
+                // engine inlet sides and engine nodes (level 1)
+                const int ns = d.n_engine_sides;
+                if (ns < 0 || (ns > 0 && (!d.engine_idx || !d.engine_w)))
+                    throw std::runtime_error("bad engine inlet sides");
+                std::vector<int2> es(ns);
+                std::vector<int> ein(ns);
+                for (int s = 0; s < ns; ++s) {
+                    const int a = d.engine_idx[s] - 1, q = d.engine_idx[(size_t)ns + s] - 1;
+                    const int in = d.engine_idx[2 * (size_t)ns + s];
+                    if (a < 0 || a >= N || q < 0 || q >= N || in < 1 || in > 2)
+                        throw std::runtime_error("engine inlet side out of range");
+                    es[s] = make_int2(a, q);
+                    ein[s] = in - 1;
+                }
+                std::vector<int> en;
+                for (int i = 0; i < N; ++i)
+                    if (bc[i] >= BC_EIN1 && bc[i] <= BC_EOUT2) en.push_back(i);
+                if (ns > 0 || !en.empty()) P.engines = 1;
+                if (P.engines) {
+                    EngineView &G = L.eng;
+                    G.nside = ns;
+                    G.nnode = (int)en.size();
+                    G.side = X.upload(es);
+                    G.inlet = X.upload(ein);
+                    G.wx = X.upload(std::vector<double>(d.engine_w, d.engine_w + ns));
+                    G.wy = X.upload(std::vector<double>(d.engine_w + ns, d.engine_w + 2 * (size_t)ns));
+                    G.wz = X.upload(std::vector<double>(d.engine_w + 2 * (size_t)ns, d.engine_w + 3 * (size_t)ns));
+                    G.node = X.upload(en);
+                }
+            }
             put_geometry(X, l, d, true);
             L.inc32 = nullptr;
             L.tile = TileView{};
@@ -470,6 +507,18 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
             L.perm = X.renumbered ? X.d_perm[l] : nullptr;
             }  // mesh upload
+            if (l > 0) L.eng = EngineView{};
+            if (l == 0 && P.engines) {
+                if (c->flowType == 2) {
+                    X.err = "engine conditions on a moving mesh (flowType 2) are not supported";
+                    return FLITE_EUNSUPPORTED;
+                }
+                // the engine pass's scratch belongs to this context
+                L.eng.pbc = X.alloc<double>(N);
+                CK(cudaMemset(L.eng.pbc, 0, (size_t)N * sizeof(double)));
+                L.eng.f = X.alloc<EngineFactors>(1);
+                CK(cudaMemset(L.eng.f, 0, sizeof(EngineFactors)));
+            }
             // state
             const size_t nv = (size_t)X.nvar();
             L.u = X.alloc<double>(nv * N); L.uprev = X.alloc<double>(nv * N);
@@ -620,6 +669,7 @@ int flite_start(flite_ctx *ctx) {
         X.set_cycle(1);
         k_set_int<<<1, 1, 0, X.s>>>(X.V(0).cyc, X.d_cycle);
         k_bc_solution<<<flite_ctx::blocks(X.V(0).N), kBlock, 0, X.s>>>(X.P, X.V(0));
+        X.engine_pass(0, MODE_START);
         // an unsteady run starts with uold = uold2 = u (def_par:3594-3596)
         if (X.P.unsteady) {
             const size_t n5 = X.nvar() * (size_t)X.V(0).N;

@@ -373,6 +373,19 @@ __device__ __forceinline__ void farfield_flux(const Params &P, const NodeState &
     F[4] = 0.5 * (fr5 + fl5) - 0.5 * ((l3 * du5 + cc1 * hi) + cc2 * ucp);
 }
 
+// The flux of a node state through an engine face's coefficients
+// (def_par:2448-2491)
+__device__ __forceinline__ void engine_flux(const NodeState &s, double wx, double wy, double wz, double *F) {
+    const double pr = s.p, r = s.r, rinv = 1. / s.r;
+    const double uu = rinv * s.ru, vv = rinv * s.rv, ww = rinv * s.rw;
+    const double pu = pr * rinv * s.ru, pv = pr * rinv * s.rv, pw = pr * rinv * s.rw;
+    F[0] = (wx * r * uu + wy * r * vv) + wz * r * ww;
+    F[1] = (wx * (s.ru * uu + pr) + wy * s.ru * vv) + wz * s.ru * ww;
+    F[2] = (wx * s.rv * uu + wy * (s.rv * vv + pr)) + wz * s.rv * ww;
+    F[3] = (wx * s.rw * uu + wy * s.rw * vv) + wz * (s.rw * ww + pr);
+    F[4] = (wx * (s.E * uu + pu) + wy * (s.E * vv + pv)) + wz * (s.E * ww + pw);
+}
+
 // The GCL terms of boundary edge b of a moving mesh, subtracted from its
 // two nodes' residuals before the edge's flux (def_par:2124-2177)
 __device__ __forceinline__ void boundary_gcl(const Params &P, const LevelView &L, int b, double *t1, double *t2) {
@@ -414,8 +427,15 @@ __device__ __forceinline__ void boundary_flux(const Params &P, const LevelView &
         const double *inf = &P.inf[(ind - 3) * 6];
         farfield_flux(P, s1, rnx, rny, rnz, inf, F1);
         farfield_flux(P, s2, rnx, rny, rnz, inf, F2);
-    } else {
-        return;  // engine faces are rejected at context creation
+    } else {  // engine faces: the two fluxes' sum plus twice the node's own (def_par:2493-2505)
+        engine_flux(s1, wx, wy, wz, F1);
+        engine_flux(s2, wx, wy, wz, F2);
+        for (int k = 0; k < 5; ++k) {
+            const double fs = F1[k] + F2[k];
+            g1[k] = fs + 2.0 * F1[k];
+            g2[k] = fs + 2.0 * F2[k];
+        }
+        return;
     }
     const double rnorm = sqrt((wx * wx + wy * wy) + wz * wz);
     for (int k = 0; k < 5; ++k) {

@@ -1673,8 +1673,8 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
     if (cls != BC_NONE) { n0 = L.nx[i]; n1 = L.ny[i]; n2 = L.nz[i]; }
     bc_increment(P, cls, n0, n1, n2, r);
     // nullifyOuterBoundary (coarse levels): zeroes the far-field (indicator
-    // 3) increments for the SA model and is a no-op otherwise
-    if (P.sa && L.grid > 1 && cls == BC_FAR3) r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
+    // 3) and engine increments for the SA model and is a no-op otherwise
+    if (P.sa && L.grid > 1 && (cls == BC_FAR3 || is_engine(cls))) r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     const double dtJ = stage > 0 ? P.CFL * P.RK[stage - 1] : P.CFL;
     double d[5], up[5], un[5];
     for (int c = 0; c < 5; ++c) { d[c] = dtJ * r[c]; up[c] = L.uprev[c * N + i]; }
@@ -1689,6 +1689,20 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
     double cm0 = 0, cm1 = 0, cm2 = 0;
     if (cls == BC_WALL && P.viscous) { cm0 = L.cmx[i]; cm1 = L.cmy[i]; cm2 = L.cmz[i]; }
     bc_solution(P, cls, n0, n1, n2, cm0, cm1, cm2, relax_param(P, *L.cyc), un);
+    if (is_exhaust(cls)) {
+        // the exhaust pressure matters on level 1 only: coarse pressures are
+        // recomputed before anything reads them
+        const double pex = bc_exhaust(P, cls, eo_relax(P, *L.cyc), un);
+        if (L.eng.f) L.eng.pbc[i] = pex;
+    }
+    if (L.eng.f && mode != MODE_RCOARSE && (P.eftype == 2 || is_engine(cls))) {
+        // level 1: the engine inlet terms need every node's state first;
+        // k_engine_finish completes the node (the candidate state of
+        // restrictGrid's fine step goes to rhs)
+        double *T = mode == MODE_RFINE ? L.rhs : L.u;
+        for (int c = 0; c < 5; ++c) T[c * N + i] = un[c];
+        return;
+    }
     if (mode == MODE_STAGE) {
         if (L.grid > 1) {
             const double a = P.RK[stage - 1];
@@ -2213,11 +2227,19 @@ __global__ void k_restrict_arr(LevelView C, LevelView F, const double *fsrc, dou
 }
 
 // the nu~ solution conditions: zero on walls (def_par:4416-4418, 4446-4448,
-// 4469-4471), 0.1 on the far field (def_par:4076-4140)
-__device__ __forceinline__ double sa_bc_solution(unsigned char cls, double v) {
+// 4469-4471), the ramped exhaust value on engine exhausts (:4507-4530), 0.1
+// on the far field (def_par:4076-4140); rp is the exhaust ramp
+__device__ __forceinline__ double sa_bc_solution(const Params &P, unsigned char cls, double rp, double v) {
     if (cls == BC_WALL || cls == BC_IWALL) return 0.0;
+    if (is_exhaust(cls)) return sa_exhaust(P, cls, rp);
     if (cls == BC_FAR3 || cls == BC_FAR4) return 0.1;
     return v;
+}
+// the nu~ increment conditions (def_par:4978-5125)
+__device__ __forceinline__ double sa_bc_increment(const Params &P, unsigned char cls, double r) {
+    if (cls == BC_WALL || cls == BC_IWALL || is_exhaust(cls)) return 0.0;
+    if (is_inlet(cls)) return P.engRelax * r;
+    return r;
 }
 
 // restrictGrid head (def_par:12159-12185): C.u = R(F.u), C.mu = R(F.mu),
@@ -2235,12 +2257,14 @@ __global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
     double n0 = 0, n1 = 0, n2 = 0;
     if (cls != BC_NONE) { n0 = C.nx[c]; n1 = C.ny[c]; n2 = C.nz[c]; }
     bc_solution(P, cls, n0, n1, n2, 0.0, 0.0, 0.0, relax_param(P, *C.cyc), v);
+    const double rp = eo_relax(P, *C.cyc);
+    if (is_exhaust(cls)) bc_exhaust(P, cls, rp, v);
     bc_outer(P, cls, n0, n1, n2, p0, v);
     for (int k = 0; k < 5; ++k) { C.u[k * N + c] = v[k]; C.uprev[k * N + c] = v[k]; }
     if (P.sa) {
         double t;
         restrict_gather(C, F.u + 5 * (size_t)F.N, F.N, c, 1, &t);
-        t = sa_bc_solution(cls, t);
+        t = sa_bc_solution(P, cls, rp, t);
         C.u[5 * N + c] = t;
         C.uprev[5 * N + c] = t;
     }
@@ -2268,7 +2292,7 @@ __global__ void k_restrict_incr(Params P, LevelView C, LevelView F) {
     if (P.sa) {
         double t;
         restrict_gather(C, F.rhs + 5 * (size_t)F.N, F.N, c, 1, &t);
-        if (cls == BC_WALL || cls == BC_IWALL) t = 0.0;
+        t = sa_bc_increment(P, cls, t);
         C.rhs[5 * N + c] = t;
         C.src[5 * N + c] = C.src[5 * N + c] - t;
         C.u[5 * N + c] = C.u[5 * N + c] + t;
@@ -2287,6 +2311,8 @@ __global__ void k_prolong_coarse(Params P, LevelView C, LevelView F) {
     double n0 = 0, n1 = 0, n2 = 0;
     if (cls != BC_NONE) { n0 = C.nx[c]; n1 = C.ny[c]; n2 = C.nz[c]; }
     bc_solution(P, cls, n0, n1, n2, 0.0, 0.0, 0.0, relax_param(P, *C.cyc), v);
+    const double rp = eo_relax(P, *C.cyc);
+    if (is_exhaust(cls)) bc_exhaust(P, cls, rp, v);
     bc_outer(P, cls, n0, n1, n2, C.p[c], v);
     double r[5];
     for (int k = 0; k < 5; ++k) {
@@ -2297,12 +2323,12 @@ __global__ void k_prolong_coarse(Params P, LevelView C, LevelView F) {
     if (P.sa) {
         double t;
         restrict_gather(C, F.u + 5 * (size_t)F.N, F.N, c, 1, &t);
-        t = sa_bc_solution(cls, t);
+        t = sa_bc_solution(P, cls, rp, t);
         C.uprev[5 * N + c] = t;
         r6 = C.u[5 * N + c] - t;
         // nullifyOuterBoundary, then the increment conditions
-        if (cls == BC_FAR3) { r[0] = r[1] = r[2] = r[3] = r[4] = 0.0; r6 = 0.0; }
-        if (cls == BC_WALL || cls == BC_IWALL) r6 = 0.0;
+        if (cls == BC_FAR3 || is_engine(cls)) { r[0] = r[1] = r[2] = r[3] = r[4] = 0.0; r6 = 0.0; }
+        r6 = sa_bc_increment(P, cls, r6);
     }
     bc_increment(P, cls, n0, n1, n2, r);
     for (int k = 0; k < 5; ++k) C.rhs[k * N + c] = r[k];
@@ -2318,7 +2344,7 @@ __global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
     int pc = C.parent[i];
     const unsigned char cls = F.bc[i];
     // nullifyOuterBoundary of the injected correction (SA runs only)
-    const bool nul = P.sa && cls == BC_FAR3;
+    const bool nul = P.sa && (cls == BC_FAR3 || is_engine(cls));
     double un[5];
     for (int k = 0; k < 5; ++k) un[k] = F.u[k * N + i];
     for (int k = 0; k < 5; ++k) {
@@ -2339,7 +2365,7 @@ __global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
         // the nu~ correction reaches the levels finer than
         // numberOfTurbulenceGrids (def_par:12540-12552)
         if (F.grid < P.nTurbGrids) un6 = un6 + r;
-        un6 = sa_bc_solution(cls, un6);
+        un6 = sa_bc_solution(P, cls, eo_relax(P, *F.cyc), un6);
         un6 = dmax(un6, 0.0);
         F.u[5 * N + i] = un6;
     }
@@ -2348,6 +2374,14 @@ __global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
     double cm0 = 0, cm1 = 0, cm2 = 0;
     if (cls == BC_WALL && P.viscous && F.grid == 1) { cm0 = F.cmx[i]; cm1 = F.cmy[i]; cm2 = F.cmz[i]; }
     bc_solution(P, cls, n0, n1, n2, cm0, cm1, cm2, relax_param(P, *F.cyc), un);
+    if (is_exhaust(cls)) {
+        const double pex = bc_exhaust(P, cls, eo_relax(P, *F.cyc), un);
+        if (F.eng.f) F.eng.pbc[i] = pex;
+    }
+    if (F.eng.f && (P.eftype == 2 || is_engine(cls))) {  // completed by k_engine_finish
+        for (int k = 0; k < 5; ++k) F.u[k * N + i] = un[k];
+        return;
+    }
     bc_outer(P, cls, n0, n1, n2, F.p[i], un);
     un[0] = dmax(un[0], P.minRho);
     for (int k = 0; k < 5; ++k) F.u[k * N + i] = un[k];
@@ -2374,6 +2408,12 @@ __global__ void k_bc_solution(Params P, LevelView L) {
     double cm0 = 0, cm1 = 0, cm2 = 0;
     if (cls == BC_WALL && P.viscous) { cm0 = L.cmx[i]; cm1 = L.cmy[i]; cm2 = L.cmz[i]; }
     bc_solution(P, cls, L.nx[i], L.ny[i], L.nz[i], cm0, cm1, cm2, relax_param(P, *L.cyc), un);
+    if (is_exhaust(cls)) {
+        const double rp = eo_relax(P, *L.cyc);
+        const double pex = bc_exhaust(P, cls, rp, un);
+        if (L.eng.f) L.eng.pbc[i] = pex;
+        if (P.sa) L.u[5 * N + i] = sa_exhaust(P, cls, rp);
+    }
     for (int k = 0; k < 5; ++k) L.u[k * N + i] = un[k];
     if (P.sa && (cls == BC_WALL || cls == BC_IWALL)) L.u[5 * N + i] = 0.0;
 }

@@ -4,7 +4,10 @@
 
 namespace flite {
 
-enum { MODE_STAGE = 0, MODE_RCOARSE = 1, MODE_RFINE = 2, MODE_RESID = 3 };
+// node passes: an RK stage, restrictGrid's coarse and fine one-step updates,
+// makeRHS alone; MODE_PROLONG and MODE_START name prolongateGrid's fine part
+// and the start-up conditions for the engine pass that follows them
+enum { MODE_STAGE = 0, MODE_RCOARSE = 1, MODE_RFINE = 2, MODE_RESID = 3, MODE_PROLONG = 4, MODE_START = 5 };
 
 __global__ void k_pressure(Params P, LevelView L);
 template <int U>
@@ -62,6 +65,10 @@ __global__ void k_prolong_coarse(Params P, LevelView C, LevelView F);
 __global__ void k_prolong_fine(Params P, LevelView C, LevelView F);
 __global__ void k_inject_u(LevelView C, LevelView F);
 __global__ void k_bc_solution(Params P, LevelView L);
+// level-1 engine inlet terms after a node pass (engine.cu)
+constexpr int kEngineLanes = 256;
+__global__ void __launch_bounds__(kEngineLanes) k_engine_sums(Params P, LevelView L, int mode);
+__global__ void k_engine_finish(Params P, LevelView L, int mode, int all);
 __global__ void k_set_int(int *dst, const int *src);
 __global__ void k_resid_partial(LevelView L, double *part, int nblk);
 __global__ void k_resid_final(const double *part, int nblk, double *out);

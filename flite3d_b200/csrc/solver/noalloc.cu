@@ -62,11 +62,9 @@ __global__ void na_clear_flag(int *flag) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *flag = 0;
 }
 
-// Bits of the error flag: an index outside 1..N or a boundary code outside
-// 1..9 (FLITE_EINVAL), an engine face, codes 5..8 (FLITE_EUNSUPPORTED, as
-// flite_create refuses them for flite_residual_fwd).
+// The error flag: an index outside 1..N or a boundary code outside 1..9
+// (FLITE_EINVAL).
 constexpr int kFlagInvalid = 1;
-constexpr int kFlagEngine = 2;
 
 // 0-based copies of the caller's 1-based index arrays; an edge that raises
 // the error flag is dropped from every pass
@@ -83,8 +81,6 @@ __global__ void na_prepare(int N, int E, int B, const int32_t *side_idx, const i
         const int code = bnd_idx[2 * B + t];
         if (a < 0 || a >= N || b < 0 || b >= N || code < 1 || code > 9) {
             atomicOr(flag, kFlagInvalid); a = -1; b = -1;
-        } else if (code >= 5 && code <= 8) {
-            atomicOr(flag, kFlagEngine); a = -1; b = -1;
         }
         bedge[t] = make_int2(a, b);
         bind[t] = code;
@@ -316,6 +312,5 @@ extern "C" int flite_residual_noalloc(const flite_controls *c, int32_t n_nodes, 
     if (cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FLITE_ECUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return FLITE_ECUDA;
     if (hflag & kFlagInvalid) return FLITE_EINVAL;
-    if (hflag & kFlagEngine) return FLITE_EUNSUPPORTED;
     return FLITE_OK;
 }

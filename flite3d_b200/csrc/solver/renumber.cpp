@@ -111,6 +111,7 @@ void permute_levels(int nlevels, const flite_level_desc *lv, Renumbered &out) {
     if (out.identity) return;
     const size_t L = (size_t)nlevels;
     out.side_idx.resize(L); out.bnd_idx.resize(L); out.node_ind.resize(L); out.parent.resize(L);
+    out.engine_idx.resize(L);
     out.volume.resize(L); out.wall_dist.resize(L); out.coords.resize(L); out.coord_move.resize(L);
     out.rweight.resize(L); out.volume_prev.resize(L); out.volume_prev2.resize(L);
     for (int l = 0; l < nlevels; ++l) {
@@ -129,6 +130,13 @@ void permute_levels(int nlevels, const flite_level_desc *lv, Renumbered &out) {
             v.assign(d.bnd_idx, d.bnd_idx + 3 * (size_t)B);
             for (size_t k = 0; k < 2 * (size_t)B; ++k) v[k] = remap(d.bnd_idx[k], iperm);
             o.bnd_idx = v.data();
+        }
+        if (d.engine_idx && d.n_engine_sides > 0) {
+            const size_t ns = (size_t)d.n_engine_sides;
+            auto &v = out.engine_idx[l];
+            v.assign(d.engine_idx, d.engine_idx + 3 * ns);
+            for (size_t k = 0; k < 2 * ns; ++k) v[k] = remap(d.engine_idx[k], iperm);
+            o.engine_idx = v.data();
         }
         if (d.node_ind && d.n_normals > 0) {
             auto &v = out.node_ind[l];

@@ -31,7 +31,7 @@ struct Renumbered {
     std::vector<flite_level_desc> desc;
     bool identity = true;
     // storage behind desc
-    std::vector<std::vector<int32_t>> side_idx, bnd_idx, node_ind, parent;
+    std::vector<std::vector<int32_t>> side_idx, bnd_idx, node_ind, parent, engine_idx;
     std::vector<std::vector<double>> volume, wall_dist, coords, coord_move, rweight, volume_prev, volume_prev2;
 };
 

@@ -30,6 +30,9 @@ namespace {
 __device__ __forceinline__ int tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ bool sa_wall(unsigned char cls) { return cls == BC_WALL || cls == BC_IWALL; }
 __device__ __forceinline__ bool sa_far(unsigned char cls) { return cls == BC_FAR3 || cls == BC_FAR4; }
+__device__ __forceinline__ double rp_exhaust(const Params &P, const LevelView &L, unsigned char cls) {
+    return sa_exhaust(P, cls, eo_relax(P, *L.cyc));
+}
 }  // namespace
 
 __global__ void k_sa_timestep(Params P, LevelView L) {
@@ -250,12 +253,16 @@ __global__ void k_sa_stage(Params P, LevelView L, int mode, int stage, int turb)
     // the turbulence is recomputed (def_par:12238-12240, 12315-12317)
     if (turb || mode != MODE_STAGE) r = r + L.turbDiff[i];
     r = L.dtT[i] * r / L.V[i];
-    if (sa_wall(cls)) r = 0.0;
-    if (L.grid > 1 && cls == BC_FAR3) r = 0.0;  // nullifyOuterBoundary
+    if (sa_wall(cls) || is_exhaust(cls)) r = 0.0;
+    if (is_inlet(cls)) r = P.engRelax * r;  // the engine inlets' relaxation (def_par:5084-5099)
+    if (L.grid > 1 && (cls == BC_FAR3 || is_engine(cls))) r = 0.0;  // nullifyOuterBoundary
     const double dtJ = stage > 0 ? P.turbCFL * P.RK[stage - 1] : P.turbCFL;
     double un = L.uprev[o6] - dtJ * r;
     un = dmax(un, 0.0);
     if (sa_wall(cls)) un = 0.0;
+    // the exhausts' nu~; an inlet's is zeroed on level 1 by k_engine_finish
+    // when its momenta are scaled
+    if (is_exhaust(cls)) un = rp_exhaust(P, L, cls);
     if (mode == MODE_STAGE) {
         if (L.grid > 1 && turb) un = un - P.RK[stage - 1] * L.src[o6];
         if (turb) {  // limitTurbulence

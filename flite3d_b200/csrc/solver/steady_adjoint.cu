@@ -1227,6 +1227,7 @@ static const char *steady_adjoint_unsupported(const flite_ctx &X) {
     const flite_controls &c = X.c;
     if (c.fluxType != 1) return "the steady adjoint takes the central flux (fluxType 1)";
     if (c.flowType != 0) return "the steady adjoint takes steady runs (flowType 0)";
+    if (X.P.engines) return "the steady adjoint covers meshes without engine boundary conditions";
     if (c.rungeKuttaStages != 3) return "the steady adjoint takes the reference's three stages";
     if (c.turbulenceModel != 0) return "the steady adjoint covers inviscid and laminar runs (no turbulence model)";
     if (c.dissipationScheme == 1 || c.dissipationScheme == 3) return "the steady adjoint takes the scalar JST dissipation (scheme 2)";

@@ -237,6 +237,8 @@ class Mesh:
             "coords": (d.coords, np.float64, (3, n)), "coord_move": (d.coord_move, np.float64, (3, n)),
             "side_gcl": (d.side_gcl, np.float64, (2, e)), "bnd_gcl": (d.bnd_gcl, np.float64, (4, b)),
             "volume_prev": (d.volume_prev, np.float64, (n,)), "volume_prev2": (d.volume_prev2, np.float64, (n,)),
+            "engine_idx": (d.engine_idx, np.int32, (3, d.n_engine_sides)),
+            "engine_w": (d.engine_w, np.float64, (3, d.n_engine_sides)),
         }
         if level > 1:
             nf = self.level(level - 1).n_nodes

@@ -32,12 +32,25 @@ def default_controls(**overrides):
     lib = _abi.gpu_lib()
     c = _abi.Controls()
     _abi.check(lib.flite_controls_default(ctypes.byref(c)), "flite_controls_default")
+    _override(c, overrides)
+    _abi.check(lib.flite_controls_derive(ctypes.byref(c)), "flite_controls_derive")
+    return c
+
+
+def _override(c, overrides):
+    """Set controls by name; an array control takes a sequence of its length."""
     for k, v in overrides.items():
         if not hasattr(c, k):
             raise KeyError(f"unknown control {k}")
-        setattr(c, k, v)
-    _abi.check(lib.flite_controls_derive(ctypes.byref(c)), "flite_controls_derive")
-    return c
+        cur = getattr(c, k)
+        if hasattr(cur, "__len__"):
+            v = list(v)
+            if len(v) != len(cur):
+                raise ValueError(f"control {k} takes {len(cur)} values")
+            for i, x in enumerate(v):
+                cur[i] = x
+        else:
+            setattr(c, k, v)
 
 
 def host_controls(**overrides):
@@ -47,10 +60,7 @@ def host_controls(**overrides):
     lib = _abi.prepro_lib()
     c = _abi.Controls()
     _abi.check(lib.fp_controls_default(ctypes.byref(c)), "fp_controls_default")
-    for k, v in overrides.items():
-        if not hasattr(c, k):
-            raise KeyError(f"unknown control {k}")
-        setattr(c, k, v)
+    _override(c, overrides)
     _abi.check(lib.fp_controls_derive(ctypes.byref(c)), "fp_controls_derive")
     return c
 
@@ -68,8 +78,7 @@ def controls_from_inp(path_or_text, **overrides):
     else:
         rc = pre.fp_read_inp(text.encode(), ctypes.byref(c), unk, len(unk))
     _abi.check(rc, "namelist read")
-    for k, v in overrides.items():
-        setattr(c, k, v)
+    _override(c, overrides)
     _abi.check(lib.flite_controls_derive(ctypes.byref(c)), "flite_controls_derive")
     return c, [u for u in unk.value.decode().split(",") if u]
 

@@ -84,6 +84,15 @@ typedef struct flite_controls {
     int    timeScheme, numberOfRSSteps, numberOfPSSteps;
     double residualSmoothingFactor, prolongationSmoothingFactor, physicalTimeStep;
     double engineBCRelaxation;
+    /* engine boundary conditions (def_par:114-117, 182): the inlet mass flow
+     * target of engines 1 and 2, the exhaust state (rho, rho u, rho v, rho w,
+     * rho E, p, nu~) of each engine as enginesRearParameters(7,2) stored
+     * column-major, and the cycles over which the exhaust state is ramped in
+     * from the freestream                                                    */
+    int    engineFlowType;      /* 1 mass flow, 2 mass flow function          */
+    int    numberOfEORelaxationSteps;
+    double enginesFrontMassFlow[2];
+    double enginesRearParameters[14];
     /* derived: inflowField(1:6, 1:2) stored column-major as in def_par:88 */
     double inflowField[12];
     /* extension controls (no reference counterpart) */
@@ -140,6 +149,12 @@ typedef struct flite_level_desc {
     const double  *bnd_gcl;     /* [4][B] brp%GCLWeightsArray(B,1:2), previous */
     const double  *volume_prev; /* [N]    nodeVolumeP  (level 1)              */
     const double  *volume_prev2;/* [N]    nodeVolumeP2 (level 1)              */
+    /* engine inlet sides (def_par:852-864; 0 = none): per side its two nodes
+     * and inlet number 1|2 as engineInletSideIndexes(n,3), its coefficient
+     * vector as engineInletSideCoefficients(n,3)                              */
+    int32_t n_engine_sides;
+    const int32_t *engine_idx;  /* [3][n_engine_sides]                        */
+    const double  *engine_w;    /* [3][n_engine_sides]                        */
 } flite_level_desc;
 
 typedef struct flite_ctx flite_ctx;
@@ -338,8 +353,8 @@ int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_bloc
  * writes rhs [5][N].  Scratch lives in one static device array of the
  * library (24,380,160 bytes on every GPU that loads it); limits N <= 65536,
  * E <= 262144, B <= 65536, larger sizes return FLITE_EINVAL, as do an
- * index outside 1..N and a boundary code outside 1..9; engine faces (codes
- * 5..8) return FLITE_EUNSUPPORTED, as flite_create does.  The first call on
+ * index outside 1..N and a boundary code outside 1..9 (engine faces, codes
+ * 5..8, take their flux as in flite_residual_fwd).  The first call on
  * a device looks the scratch up for that device.  The call runs on `stream`
  * (a cudaStream_t, NULL for the default stream), copies its status to host
  * memory and synchronises the stream, so it must not be made while any

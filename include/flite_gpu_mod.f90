@@ -55,6 +55,9 @@ module flite_gpu
     integer(c_int) :: timeScheme, numberOfRSSteps, numberOfPSSteps
     real(c_double) :: residualSmoothingFactor, prolongationSmoothingFactor, physicalTimeStep
     real(c_double) :: engineBCRelaxation
+    integer(c_int) :: engineFlowType, numberOfEORelaxationSteps
+    real(c_double) :: enginesFrontMassFlow(2)
+    real(c_double) :: enginesRearParameters(14)  ! enginesRearParameters(7,2), column-major
     real(c_double) :: inflowField(12)          ! inflowField(1:6,1:2), column-major
     integer(c_int) :: precision                ! extension: FLITE_FP64 | FLITE_MIXED
     integer(c_int) :: reconstruction           ! extension: FLITE_RECON_*
@@ -68,6 +71,9 @@ module flite_gpu
     type(c_ptr) :: volume, wall_dist, coords, coord_move, parent, rweight
     ! moving meshes (flowType 2): GCL weights and previous volumes
     type(c_ptr) :: side_gcl, bnd_gcl, volume_prev, volume_prev2
+    ! engine inlet sides: engineInletSideIndexes(n,3), engineInletSideCoefficients(n,3)
+    integer(c_int32_t) :: n_engine_sides
+    type(c_ptr) :: engine_idx, engine_w
   end type flite_level_desc
 
   interface

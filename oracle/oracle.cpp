@@ -22,6 +22,10 @@
 //  * the cycle number of a coarse level before its first relaxation is 0.
 //  * the LED limiter's (1+t^nsig)^(1/nsig) (def_par:1861) is evaluated as
 //    sqrt(sqrt(1+(t*t)*(t*t))) for nsig=4 and sqrt(1+t*t) for nsig=2.
+//  * the engine mass-flow factor of an inlet whose flow sum is not positive
+//    is an uninitialised local (def_par:4593-4598, 4779-4806): pinned to 1.
+//    The sums over the engine inlet sides follow the device's fixed order
+//    (engine_sums) in place of the reference's side order.
 #include "oracle.h"
 #include "pinned_math.h"
 
@@ -53,6 +57,9 @@ struct Level {
     vec gcl, bgcl1, bgcl2, Vp, Vp2;
     std::vector<int> parent;  // [N_finer], 0-based coarse node or -1
     vec rweight;
+    // engine inlet sides: 0-based nodes, inlet 0|1, coefficients
+    std::vector<int> e1, e2, ein;
+    vec ewx, ewy, ewz;
     // state
     vec u[6], uprev[6], rhs[6], src[6], diss[5];
     vec uold[6], uold2[6];  // unsteady runs: previous physical time steps
@@ -166,6 +173,7 @@ struct Oracle {
     flite_controls c;
     std::vector<Level> lv;
     int nvar = 5;
+    bool engines = false;  // the mesh has engine faces or nodes (indicators 5..8)
     std::vector<vec> nh;  // nodeHelpArray(:,1:25), sized for level 1
     double RK[5] = {0.6, 0.6, 1.0, 0.0, 0.0};  // def_par:14240-14244
     int nstage = 3;
@@ -1643,6 +1651,15 @@ struct Oracle {
             if (t) rhs[5][ip] = 0.0;
         });
         for_range(g, -18, -17, [&](int ip) { remove_normal(g, rhs, ip, 1.0); });
+        // engine inlets relaxed, engine exhausts held (def_par:5084-5125)
+        for (int r : {-12, -10})
+            for_range(g, r, r + 1, [&](int ip) {
+                for (int k = 0; k < nvar; ++k) rhs[k][ip] = c.engineBCRelaxation * rhs[k][ip];
+            });
+        for (int r : {-8, -6})
+            for_range(g, r, r + 1, [&](int ip) {
+                for (int k = 0; k < nvar; ++k) rhs[k][ip] = 0.0;
+            });
     }
 
     // ---- updateSolutionVector (def_par:1292-1405); u may alias delu -------
@@ -1698,6 +1715,113 @@ struct Oracle {
             if (sa()) u[5][ip] = 0.0;
         });
         for_range(g, -18, -17, [&](int ip) { remove_normal(g, u, ip, 1.0); });
+        if (engines) engine_conditions(g, u);
+    }
+
+    // ---- engine conditions of setBCsOnSolutionField (def_par:4488-4918) ----
+    // The exhausts take the ramped exhaust state, and its pressure into grp%p;
+    // on level 1 the inlets' momenta are scaled to the target mass flow
+    // (engineFlowType 1) or mass flow function (2) with the internal energy
+    // of grp%u kept, and an inflow through an inlet is turned out.  u is the
+    // array the conditions act on (grp%u, or the candidate state of
+    // restrictGrid's fine step); grp%u and grp%p are the level's.
+    double eo_relax(const Level &g) const {  // def_par:4490-4495
+        if (c.numberOfEORelaxationSteps > 0) {
+            double r = (double)(g.cycleNumber - 1) / (double)c.numberOfEORelaxationSteps;
+            return std::min(r, 1.0);
+        }
+        return 1.0;
+    }
+    static double ke(const vec *u, int i) { return (u[1][i] * u[1][i] + u[2][i] * u[2][i]) + u[3][i] * u[3][i]; }
+
+    // Sums over the engine inlet sides in the device's fixed order: side s
+    // goes to partial kEngineLanes-strided sums (s mod kEngineLanes), in side
+    // order, and the partials meet in a pairwise tree.  The reference sums in
+    // side order on each domain and then over the domains.
+    static constexpr int kEngineLanes = 256;
+    template <class Term>
+    void engine_sums(const Level &g, int nq, Term term, double (*out)[2]) {
+        std::vector<double> part((size_t)nq * 2 * kEngineLanes, 0.0);
+        const int n = (int)g.e1.size();
+        for (int s = 0; s < n; ++s) {
+            double q[3];
+            term(s, q);
+            const size_t base = ((size_t)g.ein[s] * nq) * kEngineLanes + s % kEngineLanes;
+            for (int k = 0; k < nq; ++k) part[base + (size_t)k * kEngineLanes] += q[k];
+        }
+        for (int e = 0; e < 2; ++e)
+            for (int k = 0; k < nq; ++k) {
+                double *a = &part[((size_t)e * nq + k) * kEngineLanes];
+                for (int w = kEngineLanes / 2; w >= 1; w /= 2)
+                    for (int t = 0; t < w; ++t) a[t] = a[t] + a[t + w];
+                out[k][e] = a[0];
+            }
+    }
+
+    void engine_conditions(Level &g, vec *u) {
+        const double rp = eo_relax(g);
+        for (int e = 0; e < 2; ++e) {  // exhausts (def_par:4497-4540)
+            const double *rear = &c.enginesRearParameters[7 * e];
+            for_range(g, e == 0 ? -8 : -6, e == 0 ? -7 : -5, [&](int ip) {
+                for (int k = 0; k < 5; ++k) u[k][ip] = (1.0 - rp) * c.inflowField[k] + rp * rear[k];
+                g.p[ip] = (1.0 - rp) * c.inflowField[5] + rp * rear[5];
+                if (sa()) u[5][ip] = rp * rear[6];
+            });
+        }
+        if (g.grid != 1) return;  // the inlet terms act on level 1 only
+        double fac[2] = {1.0, 1.0};  // the reference's is uninitialised where the flow is not positive
+        bool scale = true;
+        if (c.engineFlowType == 1) {  // def_par:4541-4599
+            double s[1][2];
+            engine_sums(g, 1, [&](int q, double *t) {
+                const int a = g.e1[q], b = g.e2[q];
+                const double w[3] = {g.ewx[q], g.ewy[q], g.ewz[q]};
+                const double s1 = (u[1][a] * w[0] + u[2][a] * w[1]) + u[3][a] * w[2];
+                const double s2 = (u[1][b] * w[0] + u[2][b] * w[1]) + u[3][b] * w[2];
+                t[0] = s1 + s2;
+            }, s);
+            for (int e = 0; e < 2; ++e)
+                if (s[0][e] > 0.0) fac[e] = c.enginesFrontMassFlow[e] / s[0][e];
+        } else if (c.engineFlowType == 2) {  // def_par:4689-4806
+            double s[3][2];
+            engine_sums(g, 3, [&](int q, double *t) {
+                const int a = g.e1[q], b = g.e2[q];
+                const double w[3] = {g.ewx[q], g.ewy[q], g.ewz[q]};
+                const double s1 = (u[1][a] * w[0] + u[2][a] * w[1]) + u[3][a] * w[2];
+                const double s2 = (u[1][b] * w[0] + u[2][b] * w[1]) + u[3][b] * w[2];
+                const double press = 0.5 * ((g.p[a] + 0.5 * ke(u, a) / u[0][a]) + (g.p[b] + 0.5 * ke(u, b) / u[0][b]));
+                const double temp1 = (c.gamma / u[0][a]) * (u[4][a] - (0.5 * ke(u, a)) / u[0][a]);
+                const double temp2 = (c.gamma / u[0][b]) * (u[4][b] - (0.5 * ke(u, b)) / u[0][b]);
+                const double temp = 0.5 * (temp1 + temp2);
+                const double wn = std::sqrt((w[0] * w[0] + w[1] * w[1]) + w[2] * w[2]);
+                t[0] = s1 + s2;
+                t[1] = (std::sqrt(temp) / press) * 2.0 * wn;
+                t[2] = 2.0 * wn;
+            }, s);
+            for (int e = 0; e < 2 && scale; ++e) {
+                if (!(s[0][e] > 0.0)) continue;
+                const double mff = s[0][e] * (s[1][e] / s[2][e]);
+                fac[e] = c.enginesFrontMassFlow[e] / mff;
+                if (fac[e] > 99999999999.) scale = false;  // the goto 9999 past the scaling
+            }
+        }
+        if (scale) {  // def_par:4615-4649, 4827-4860
+            for (int e = 0; e < 2; ++e)
+                for_range(g, e == 0 ? -12 : -10, e == 0 ? -11 : -9, [&](int ip) {
+                    const double intE = g.u[4][ip] - 0.5 * ke(g.u, ip) / g.u[0][ip];
+                    for (int k = 1; k < 4; ++k) u[k][ip] = u[k][ip] * fac[e];
+                    u[4][ip] = intE + 0.5 * ke(u, ip) / u[0][ip];
+                    if (sa()) u[5][ip] = 0.0;
+                });
+            if (c.engineFlowType == 2) makePressureField(g, g.u);  // def_par:4864
+        }
+        for (int e = 0; e < 2; ++e)  // no inflow through an inlet (def_par:4653-4686)
+            for_range(g, e == 0 ? -12 : -10, e == 0 ? -11 : -9, [&](int ip) {
+                const double n[3] = {g.nx[ip], g.ny[ip], g.nz[ip]};
+                const double nv = (((-n[0]) * u[1][ip] + (-n[1]) * u[2][ip]) + (-n[2]) * u[3][ip]) / u[0][ip];
+                if (nv < 0.00)
+                    for (int k = 0; k < 3; ++k) u[1 + k][ip] = u[1 + k][ip] + u[0][ip] * (nv - 0.01) * n[k];
+            });
     }
 
     // ---- setOuterBoundaryConditions (def_par:4018-4251) -------------------
@@ -2835,11 +2959,26 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
         for (int b = 0; b < g.B; ++b) {
             g.b1[b] = d.bnd_idx[b] - 1; g.b2[b] = d.bnd_idx[(size_t)g.B + b] - 1;
             g.bind[b] = d.bnd_idx[2 * (size_t)g.B + b];
-            if (g.bind[b] >= 5 && g.bind[b] <= 8) return FLITE_EUNSUPPORTED;
+            if (g.bind[b] >= 5 && g.bind[b] <= 8) o.engines = true;
         }
         std::memcpy(g.reg, d.node_reg, sizeof g.reg);
         for (int r = -12; r <= -5; r += 2)
-            if (g.R(r + 1) >= g.R(r)) return FLITE_EUNSUPPORTED;  // engine nodes
+            if (g.R(r + 1) >= g.R(r)) o.engines = true;  // engine nodes
+        const int ne = d.n_engine_sides;
+        if (ne < 0 || (ne > 0 && (!d.engine_idx || !d.engine_w))) return FLITE_EINVAL;
+        g.e1.resize(ne); g.e2.resize(ne); g.ein.resize(ne);
+        g.ewx.resize(ne); g.ewy.resize(ne); g.ewz.resize(ne);
+        for (int s = 0; s < ne; ++s) {
+            g.e1[s] = d.engine_idx[s] - 1; g.e2[s] = d.engine_idx[(size_t)ne + s] - 1;
+            g.ein[s] = d.engine_idx[2 * (size_t)ne + s] - 1;
+            if (g.e1[s] < 0 || g.e1[s] >= g.N || g.e2[s] < 0 || g.e2[s] >= g.N || g.ein[s] < 0 || g.ein[s] > 1)
+                return FLITE_EINVAL;
+            g.ewx[s] = d.engine_w[s]; g.ewy[s] = d.engine_w[(size_t)ne + s]; g.ewz[s] = d.engine_w[2 * (size_t)ne + s];
+        }
+        if (ne > 0) o.engines = true;
+        // engine conditions on a moving mesh would need the engine sides of
+        // every step
+        if (o.engines && c->flowType == 2) return FLITE_EUNSUPPORTED;
         g.node_ind.resize(g.nnorm);
         for (int i = 0; i < g.nnorm; ++i) g.node_ind[i] = d.node_ind[i] - 1;
         if (l > 0) {
@@ -3125,7 +3264,7 @@ int oracle_residual_jvp(oracle_ctx *o, int level, const double *u, const double 
     Level *g = lvl(o, level);
     if (!g || !u || !du || !jv) return FLITE_EINVAL;
     const flite_controls &c = o->o.c;
-    if (c.fluxType != 1) return FLITE_EUNSUPPORTED;
+    if (c.fluxType != 1 || o->o.engines) return FLITE_EUNSUPPORTED;  // tangents of the engine-free path
     const size_t N = g->N;
     std::vector<Dl> acc(5 * N);
     auto state = [&](int i, Dl *q) { for (int k = 0; k < 5; ++k) q[k] = Dl(u[k * N + i], du[k * N + i]); };
@@ -3184,7 +3323,7 @@ int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const
     const flite_controls &c = o->o.c;
     if (c.fluxType != 1 || c.turbulenceModel != 0 || c.dissipationScheme == 1 || c.dissipationScheme == 3 ||
         c.useDissipationWeighting || (c.ReynoldsNumber > 0 && c.viscosityScheme != 1) ||
-        c.useMatrixDissipation || c.flowType != 0 || c.rungeKuttaStages != 3)
+        c.useMatrixDissipation || c.flowType != 0 || c.rungeKuttaStages != 3 || o->o.engines)
         return FLITE_EUNSUPPORTED;
     const bool visc = c.ReynoldsNumber > 0;
     if (visc && (!mu || !mu_out || !dmu_out)) return FLITE_EINVAL;
@@ -3210,7 +3349,7 @@ int oracle_iteration_jvp(oracle_ctx *o, const double *u, const double *du, const
 int oracle_objective_jvp(oracle_ctx *o, int which, const double *u, const double *du, const double *dsw,
                          const double *dbw, const double *dvol, double *J, double *dJ) {
     if (!o || !u || !du || !J || !dJ || which < 0 || which > 1) return FLITE_EINVAL;
-    if (o->o.c.turbulenceModel != 0) return FLITE_EUNSUPPORTED;
+    if (o->o.c.turbulenceModel != 0 || o->o.engines) return FLITE_EUNSUPPORTED;
     if (o->o.c.ReynoldsNumber > 0 && o->o.c.viscosityScheme != 1) return FLITE_EUNSUPPORTED;
     TanIteration T(o->o, dsw, dbw, dvol);
     const size_t N = T.N;

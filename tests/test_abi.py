@@ -30,7 +30,8 @@ def test_prepro_library_exports_header():
 
 def test_struct_sizes_match_c():
     # sizeof(flite_controls) and sizeof(flite_level_desc) as compiled
-    assert ctypes.sizeof(_abi.LevelDesc) == 5 * 4 + 4 + 17 * 8
+    # five counts (+4 padding), 17 arrays, the engine side count (+4) and its two arrays
+    assert ctypes.sizeof(_abi.LevelDesc) == 5 * 4 + 4 + 17 * 8 + 4 + 4 + 2 * 8
 
 
 def test_create_rejects_unsupported_controls():

@@ -66,3 +66,29 @@ def test_deck_leaves_the_extension_controls_alone():
     # a reference deck cannot name them: they keep their defaults
     c, unknown = controls_from_inp(DECK)
     assert c.reconstruction == 0 and c.rungeKuttaStages == 3 and c.precision == 0
+
+
+ENGINE_DECK = """&inputVariables
+ ivd%engineFlowType = 2,
+ ivd%enginesFrontMassFlow(1) = 0.3,
+ ivd%enginesFrontMassFlow(2) = 0.25,
+ ivd%enginesRearParameters(1,1) = 0.5, ivd%enginesRearParameters(2,1) = 0.9,
+ ivd%enginesRearParameters(6,1) = 0.35, ivd%enginesRearParameters(7,2) = 0.1,
+ ivd%engineBCRelaxation = 0.8,
+ ivd%numberOfEORelaxationSteps = 20
+/
+"""
+
+
+def test_engine_controls():
+    # defaults (def_par:256-260) and the deck's array elements, stored
+    # column-major as enginesRearParameters(7,2)
+    c = default_controls()
+    assert c.engineFlowType == 1 and c.numberOfEORelaxationSteps == 0 and c.engineBCRelaxation == 1.0
+    assert list(c.enginesFrontMassFlow) == [0.0, 0.0] and not any(c.enginesRearParameters)
+    c, unknown = controls_from_inp(ENGINE_DECK)
+    assert not unknown
+    assert c.engineFlowType == 2 and c.numberOfEORelaxationSteps == 20 and c.engineBCRelaxation == 0.8
+    assert list(c.enginesFrontMassFlow) == [0.3, 0.25]
+    r = list(c.enginesRearParameters)
+    assert r[0] == 0.5 and r[1] == 0.9 and r[5] == 0.35 and r[7 + 6] == 0.1

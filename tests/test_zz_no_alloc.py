@@ -128,12 +128,15 @@ def test_noalloc_refuses_bad_indices_and_codes_as_create_does(gpu):
         b2 = bidx.copy()
         b2[2, 3] = bad
         assert _call(lib, c, n, e, b, dev(sidx), side_w, dev(b2), bnd_w, u, rhs) == _abi.FLITE_EINVAL
-    # an engine face (codes 5..8): refused as flite_create refuses it
+    # an engine face (codes 5..8) takes the engine flux, as in residual_fwd
     b5 = bidx.copy()
     b5[2, 3] = 5
-    assert _call(lib, c, n, e, b, dev(sidx), side_w, dev(b5), bnd_w, u, rhs) == _abi.FLITE_EUNSUPPORTED
-    with pytest.raises(RuntimeError, match=f"status {_abi.FLITE_EUNSUPPORTED}"):
-        Solver(c, _BoundaryCodesView(mesh, b5))
+    b5[2, 9] = 8
+    assert _call(lib, c, n, e, b, dev(sidx), side_w, dev(b5), bnd_w, u, rhs) == _abi.FLITE_OK
+    torch.cuda.synchronize()
+    engine_view = Solver(c, _BoundaryCodesView(mesh, b5))
+    assert np.array_equal(rhs.cpu().numpy(), engine_view.residual_fwd(u.cpu().numpy()))
+    engine_view.close()
     # the entry point still works after the refusals
     good = torch.full((5, n), np.nan, dtype=torch.float64, device="cuda")
     assert _call(lib, c, n, e, b, dev(sidx), side_w, dev(bidx), bnd_w, u, good) == _abi.FLITE_OK
