@@ -827,7 +827,10 @@ def run_batch(args):
     264x88x88 hexes x 16 flow conditions each (angle of attack uniform in
     [-4, 8] degrees, Mach uniform in [0.3, 0.8], SplitMix64 seed 5), inviscid,
     FLITE_MIXED.  One JSON line: case-cycles per second of one graph launch
-    per batch cycle against the cases' graphs launched one after another."""
+    per batch cycle (the cases on one mesh as a case group: every kernel of
+    the cycle launched once for all of them), against the same graph with a
+    branch per case and against the cases' graphs launched one after
+    another."""
     import torch
     import flite3d_b200 as F
     from flite3d_b200.mesh import splitmix64
@@ -851,12 +854,18 @@ def run_batch(args):
         s.set_state(F.initial_state(c, m))
         s.start()
     e, nb, best = batch.autotune(reps=2)
+    lanes, best_lanes = batch.autotune_lanes(reps=2)
     for (c, m), s in zip(cases, batch.cases):
         s.set_state(F.initial_state(c, m))
         s.start()
     batch.time_cycles(args.warmup)
     ms_g, launches = batch.time_cycles(args.steps, cycle_no=args.warmup + 1, sequential=False)
-    ms_s, _ = batch.time_cycles(args.steps, cycle_no=args.warmup + args.steps + 1, sequential=True)
+    groups = batch.groups()
+    # the same batch graph with each case's cycle as its own branch, and the
+    # cases' graphs one after another
+    batch.set_grouping(False)
+    ms_c, launches_c = batch.time_cycles(args.steps, cycle_no=args.warmup + args.steps + 1, sequential=False)
+    ms_s, _ = batch.time_cycles(args.steps, cycle_no=args.warmup + 2 * args.steps + 1, sequential=True)
     n = len(cases)
     print(json.dumps({
         "metric": "batched MG case-cycles/s", "value": n * args.steps / (ms_g / 1e3), "unit": "case-cycles/s",
@@ -865,9 +874,15 @@ def run_batch(args):
         "config": {"workload": f"{len(meshes)} bump-channel meshes {sizes} x {args.batch_conditions} "
                                "conditions (alpha U[-4,8] deg, M U[0.3,0.8]), inviscid, FLITE_MIXED",
                    "cases": n, "mesh_nodes": [m.level(1).n_nodes for m in meshes]},
+        "case_groups": groups,
+        "case_graphs": {"value": n * args.steps / (ms_c / 1e3), "ms_per_step": ms_c / args.steps,
+                        "kernel_launches_per_batch_cycle": launches_c,
+                        "what": "the batch graph with every case's cycle graph as its own branch"},
         "sequential": {"value": n * args.steps / (ms_s / 1e3), "ms_per_step": ms_s / args.steps},
-        "graph_vs_sequential": ms_s / ms_g, "kernel_launches_per_batch_cycle": launches,
-        "autotune": {"edge_block": e, "node_block": nb, "best_ms": best},
+        "graph_vs_sequential": ms_s / ms_g, "groups_vs_case_graphs": ms_c / ms_g,
+        "kernel_launches_per_batch_cycle": launches,
+        "autotune": {"edge_block": e, "node_block": nb, "best_ms": best, "lanes_per_level": lanes,
+                     "best_ms_lanes": best_lanes},
     }), flush=True)
 
 

@@ -3,15 +3,22 @@
 // A batch holds one context per case (mesh x flow condition).  Cases on the
 // same mesh share that mesh's device copy (edges, coefficients, incidence
 // lists, transfer operators, geometry); each case has its own solution state
-// and controls.  One batch cycle is ONE launch of a CUDA graph whose
-// independent branches are the cases' own cycle graphs, so small meshes and
-// coarse levels of different cases run concurrently instead of one launch
-// after another.  All cases read the cycle number from one device word.
+// and controls.  One batch cycle is ONE launch of a CUDA graph.  The cases on
+// one mesh form a case group: every kernel of the cycle runs once for the
+// whole group, its grid's y index naming the case (the kernels' group form,
+// which reads the case's level view and parameters from tables), so a group
+// of G cases costs the launches of one case, and the coarse levels of all G
+// fill the GPU together.  The groups (and cases whose controls take a path
+// without a group form, each as its own cycle graph) are independent
+// branches of the batch graph and run concurrently.  All cases read the
+// cycle number from one device word.
 //
 // The autotuner times batch cycles for a set of edge-kernel and node-kernel
 // block sizes and keeps the fastest pair (the caller stores the choice).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <memory>
 #include <vector>
 
@@ -29,9 +36,13 @@ struct flite_batch {
     cudaGraphExec_t graph = nullptr;
     int64_t launches = 0;
     std::string err;
+    bool grouping = true;          // cases on one mesh advance as a case group
+    std::vector<void *> tables;    // device tables of the graph's case groups
+    int ngroups = 0;               // case groups in the graph
 
     ~flite_batch() {
         if (graph) cudaGraphExecDestroy(graph);
+        free_tables();
         // cases that borrow a mesh go first, mesh owners last
         for (size_t i = cases.size(); i-- > 0;)
             if (donor[i] != (int)i && cases[i]) { flite_destroy(cases[i]); cases[i] = nullptr; }
@@ -51,6 +62,69 @@ struct flite_batch {
             if (graph && turb[i] != (char)cases[i]->calcTurb) drop_graph();
         }
     }
+    void free_tables() {
+        for (void *p : tables) cudaFree(p);
+        tables.clear();
+    }
+    template <class T>
+    T *put_table(const std::vector<T> &h) {
+        void *d = nullptr;
+        CK(cudaMalloc(&d, h.size() * sizeof(T)));
+        tables.push_back(d);
+        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return static_cast<T *>(d);
+    }
+    // cases whose cycles take the same launches (the controls that choose
+    // kernels and grids agree; the freestream, CFL numbers and the other
+    // values the kernels read may differ) and whose path has a group form
+    static bool same_path(const flite_ctx &a, const flite_ctx &b) {
+        const flite_controls &x = a.c, &y = b.c;
+        return x.fluxType == y.fluxType && x.precision == y.precision &&
+               (x.ReynoldsNumber > 0) == (y.ReynoldsNumber > 0) && x.viscosityScheme == y.viscosityScheme &&
+               x.dissipationScheme == y.dissipationScheme &&
+               x.coarseGridDissipationScheme == y.coarseGridDissipationScheme &&
+               x.useMatrixDissipation == y.useMatrixDissipation &&
+               x.useDissipationWeighting == y.useDissipationWeighting &&
+               (x.secondOrderDissipationFactor == 0 && x.fourthOrderDissipationFactor == 0) ==
+                   (y.secondOrderDissipationFactor == 0 && y.fourthOrderDissipationFactor == 0) &&
+               x.multigridScheme == y.multigridScheme && x.numberOfRelaxationSteps == y.numberOfRelaxationSteps &&
+               x.rungeKuttaStages == y.rungeKuttaStages && x.turbulenceModel == y.turbulenceModel &&
+               x.flowType == y.flowType && x.reconstruction == y.reconstruction &&
+               x.HLLCFluxOrder == y.HLLCFluxOrder && x.GradientMethod == y.GradientMethod &&
+               x.Automaticlipping == y.Automaticlipping && a.lv.size() == b.lv.size() &&
+               a.P.engines == b.P.engines;
+    }
+    // the cycle graph of a case group led by its first case, or nullptr
+    // when the group's path has no group form
+    cudaGraph_t capture_group(const std::vector<int> &m) {
+        flite_ctx *lead = cases[m[0]];
+        for (int k : m)
+            if (!same_path(*lead, *cases[k])) return nullptr;
+        const size_t G = m.size(), nl = lead->lv.size();
+        std::vector<Params> pt(G);
+        for (size_t k = 0; k < G; ++k) pt[k] = cases[m[k]]->P;
+        const Params *d_pt = put_table(pt);
+        std::vector<const LevelView *> d_v(nl);
+        for (size_t l = 0; l < nl; ++l) {
+            std::vector<LevelView> vt(G);
+            for (size_t k = 0; k < G; ++k) {
+                vt[k] = cases[m[k]]->lv[l].v;
+                vt[k].btab = nullptr;
+                vt[k].ptab = nullptr;
+            }
+            d_v[l] = put_table(vt);
+        }
+        for (size_t l = 0; l < nl; ++l) { lead->lv[l].v.btab = d_v[l]; lead->lv[l].v.ptab = d_pt; }
+        lead->group = (int)G;
+        cudaGraph_t g = nullptr;
+        try {
+            lead->capture_cycle(&g);
+        } catch (const flite_ctx::no_group_error &) {  // a path without a group form
+            g = nullptr;
+        }
+        lead->group = 0;
+        return g;
+    }
     void build_graph() {
         if (graph) return;
         turb.resize(cases.size());
@@ -58,17 +132,34 @@ struct flite_batch {
         cudaGraph_t parent = nullptr;
         CK(cudaGraphCreate(&parent, 0));
         launches = 0;
+        ngroups = 0;
+        auto add = [&](cudaGraph_t g) {
+            cudaGraphNode_t node;
+            cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, g);
+            cudaGraphDestroy(g);
+            CK(e);
+        };
         try {
+            std::vector<char> done(cases.size(), 0);
             for (size_t i = 0; i < cases.size(); ++i) {
-                if (!active[i]) continue;
+                if (!active[i] || done[i]) continue;
+                // the active cases on case i's mesh
+                std::vector<int> m;
+                for (size_t j = i; j < cases.size(); ++j)
+                    if (active[j] && !done[j] && donor[j] == donor[i]) m.push_back((int)j);
+                cudaGraph_t g = grouping && m.size() > 1 ? capture_group(m) : nullptr;
+                if (g) {
+                    launches += cases[m[0]]->launches;
+                    ++ngroups;
+                    add(g);
+                    for (int k : m) done[k] = 1;
+                    continue;
+                }
                 flite_ctx *c = cases[i];
-                cudaGraph_t g = nullptr;
                 c->capture_cycle(&g);
                 launches += c->launches;
-                cudaGraphNode_t node;
-                cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, g);
-                cudaGraphDestroy(g);
-                CK(e);
+                add(g);
+                done[i] = 1;
             }
             CK(cudaGraphInstantiate(&graph, parent, 0));
         } catch (...) {
@@ -80,6 +171,7 @@ struct flite_batch {
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
+        free_tables();
         for (flite_ctx *c : cases) c->drop_graph();
     }
     void set_cycle(int cyc) {
@@ -219,9 +311,10 @@ int flite_batch_run(flite_batch *b, int first_cycle, int max_cycles, double orde
                 }
             }
             if (changed) {
-                // converged cases leave the batch graph
+                // converged cases leave the batch graph (and their groups)
                 if (b->graph) cudaGraphExecDestroy(b->graph);
                 b->graph = nullptr;
+                b->free_tables();
             }
         }
         for (size_t i = 0; i < n; ++i)
@@ -260,7 +353,10 @@ int flite_batch_time_cycles(flite_batch *b, int cycle_no, int ncycles, int seque
         *ms = t;
         if (launches_per_cycle) {
             int64_t n = 0;
-            for (flite_ctx *c : b->cases) n += c->launches;
+            if (sequential)
+                for (flite_ctx *c : b->cases) n += c->launches;
+            else
+                n = b->launches;
             *launches_per_cycle = n;
         }
         return FLITE_OK;
@@ -301,6 +397,76 @@ int flite_batch_autotune(flite_batch *b, int cycle_no, int reps, int32_t *edge_b
         if (best_ms) *best_ms = best;
         return FLITE_OK;
     });
+}
+
+// The lanes per node of each level's gathers (the gather tile: a thread, or
+// 4..32 lanes of a warp per node), chosen level by level, coarsest first,
+// by timing batch cycles; the other levels keep their choice meanwhile.
+// lanes[l] receives level l+1's choice for l < nlevels (0 past the deepest
+// level of any case).
+int flite_batch_autotune_lanes(flite_batch *b, int cycle_no, int reps, int32_t nlevels, int32_t *lanes,
+                               double *best_ms) {
+    if (!b || reps < 1 || nlevels < 1 || !lanes) return FLITE_EINVAL;
+    return bguard(b, [&] {
+        static const int cand[5] = {1, 4, 8, 16, 32};
+        int deep = 0;
+        for (flite_ctx *c : b->cases) deep = std::max(deep, (int)c->lv.size());
+        deep = std::min(deep, std::min((int)nlevels, kMaxLevels));
+        auto time = [&]() {
+            b->drop_graph();
+            b->build_graph();
+            b->set_cycle(cycle_no);
+            CK(cudaGraphLaunch(b->graph, b->s));  // warm
+            cudaEvent_t e0, e1;
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            CK(cudaEventRecord(e0, b->s));
+            for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(b->graph, b->s));
+            CK(cudaEventRecord(e1, b->s));
+            CK(cudaEventSynchronize(e1));
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, e0, e1));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return (double)t / reps;
+        };
+        double best = 1e300;
+        for (int l = deep - 1; l >= 0; --l) {
+            int keep = 1;
+            double bl = 1e300;
+            for (int u : cand) {
+                for (flite_ctx *c : b->cases)
+                    if (l < (int)c->lv.size()) c->lanes[l] = u;
+                const double t = time();
+                if (t < bl) { bl = t; keep = u; }
+            }
+            for (flite_ctx *c : b->cases)
+                if (l < (int)c->lv.size()) c->lanes[l] = keep;
+            best = bl;
+        }
+        b->drop_graph();
+        for (int l = 0; l < nlevels; ++l) {
+            int v = 0;
+            for (flite_ctx *c : b->cases)
+                if (l < (int)c->lv.size() && l < kMaxLevels) v = c->lanes[l];
+            lanes[l] = v;
+        }
+        if (best_ms) *best_ms = best;
+        return FLITE_OK;
+    });
+}
+
+int flite_batch_set_grouping(flite_batch *b, int on) {
+    if (!b) return FLITE_EINVAL;
+    b->drop_graph();
+    b->grouping = on != 0;
+    return FLITE_OK;
+}
+
+int flite_batch_groups(const flite_batch *b, int32_t *ngroups) {
+    if (!b || !ngroups) return FLITE_EINVAL;
+    *ngroups = b->ngroups;
+    return FLITE_OK;
 }
 
 int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_block) {

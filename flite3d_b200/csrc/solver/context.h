@@ -51,16 +51,27 @@ struct DevLevel {
 
 using namespace flite_detail;
 
+#define FLITE_UNPAREN(...) __VA_ARGS__
+// a launch of kernel template `kern` (its other template arguments `targs`,
+// parenthesised with a trailing comma, or ()) for this context, or in group
+// form for every case of its group: the same grid for each case, the case
+// in blockIdx.y
+#define FLITE_LAUNCH(kern, targs, grid, block, smem, ...)                                                   \
+    do {                                                                                                     \
+        if (group) kern<FLITE_UNPAREN targs true><<<dim3((grid), group), (block), (smem), s>>>(__VA_ARGS__); \
+        else kern<FLITE_UNPAREN targs false><<<(grid), (block), (smem), s>>>(__VA_ARGS__);                   \
+    } while (0)
+
 // a gather kernel template launched with the lanes per node of level l
-#define FLITE_GATHER(kern, l, ...)                                                  \
-    do {                                                                            \
-        switch (lanes_of(l)) {                                                      \
-            case 4: kern<4><<<gblk(l, 4), nb, 0, s>>>(__VA_ARGS__); break;          \
-            case 8: kern<8><<<gblk(l, 8), nb, 0, s>>>(__VA_ARGS__); break;          \
-            case 16: kern<16><<<gblk(l, 16), nb, 0, s>>>(__VA_ARGS__); break;       \
-            case 32: kern<32><<<gblk(l, 32), nb, 0, s>>>(__VA_ARGS__); break;       \
-            default: kern<1><<<gblk(l, 1), nb, 0, s>>>(__VA_ARGS__);                \
-        }                                                                           \
+#define FLITE_GATHER(kern, l, ...)                                                       \
+    do {                                                                                 \
+        switch (lanes_of(l)) {                                                           \
+            case 4: FLITE_LAUNCH(kern, (4,), gblk(l, 4), nb, 0, __VA_ARGS__); break;     \
+            case 8: FLITE_LAUNCH(kern, (8,), gblk(l, 8), nb, 0, __VA_ARGS__); break;     \
+            case 16: FLITE_LAUNCH(kern, (16,), gblk(l, 16), nb, 0, __VA_ARGS__); break;  \
+            case 32: FLITE_LAUNCH(kern, (32,), gblk(l, 32), nb, 0, __VA_ARGS__); break;  \
+            default: FLITE_LAUNCH(kern, (1,), gblk(l, 1), nb, 0, __VA_ARGS__);           \
+        }                                                                                \
     } while (0)
 
 // a row-gather kernel template (STAGE, AHEAD) launched for mode m (1: staged,
@@ -89,6 +100,17 @@ struct flite_ctx {
     cudaGraphExec_t graph = nullptr;
     int64_t launches = 0;
     bool counting = false;
+    // a case group (batch cases on one mesh, advanced together): while
+    // `group` > 0 the cycle's launches run in group form for that many
+    // cases, whose level views and parameters the views of this context
+    // carry (btab, ptab).  Paths without a group form refuse it.
+    int group = 0;
+    struct no_group_error : std::runtime_error {
+        using std::runtime_error::runtime_error;
+    };
+    void no_group(const char *what) const {
+        if (group) throw no_group_error(std::string(what) + " has no case-group form");
+    }
     // threads per block of the edge kernels and of the node kernels (the
     // batch autotuner may change them; kernels with launch bounds take <= 256)
     int eb = kBlock, nb = kBlock;
@@ -217,7 +239,7 @@ struct flite_ctx {
 
     void pressure(int l) {
         counted();
-        k_pressure<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        FLITE_LAUNCH(k_pressure, (), nblk(V(l).N), nb, 0, P, V(l));
     }
     void timesteps(int l) {
         counted();
@@ -244,7 +266,7 @@ struct flite_ctx {
     // flite_set_tiled_gather: 1, 2 staged, 3, 4 not), where a thread serves
     // a node and the rows exist; 0 otherwise
     int tiled_other(int l) const {
-        if (lv[l].v.tile.ntiles <= 0 || lanes_of(l) != 1) return 0;
+        if (group || lv[l].v.tile.ntiles <= 0 || lanes_of(l) != 1) return 0;
         const int m = l < kMaxLevels ? tiled_mode[l] : 0;
         return m < 0 ? 0 : m;
     }
@@ -253,7 +275,7 @@ struct flite_ctx {
     }
     void zero_diss(int l) {
         counted();
-        k_fill<<<nblk(5 * (size_t)V(l).N), nb, 0, s>>>(V(l).diss, 5 * (size_t)V(l).N, 0.0);
+        FLITE_LAUNCH(k_case_zero, (), nblk(5 * (size_t)V(l).N), nb, 0, V(l), 0, 5 * (size_t)V(l).N);
     }
     // makeArtificialDissipation2 (def_par:11484-11993), scalar form
     void jst(int l) {
@@ -285,7 +307,10 @@ struct flite_ctx {
         const int m = tiled_other(l);
         const unsigned g = L.tile.ntiles;
         counted();
-        if (P.matrixDiss) k_jst_flux_matrix<<<nblk(L.N), nb, 0, s>>>(P, L);
+        if (P.matrixDiss) {
+            no_group("the matrix dissipation");
+            k_jst_flux_matrix<<<nblk(L.N), nb, 0, s>>>(P, L);
+        }
         else if (m) {
             FLITE_ROWS(k_jst_flux_tiled, 13);
         } else {
@@ -315,17 +340,17 @@ struct flite_ctx {
         }
         if (ts) {
             counted();
-            k_ts_lap<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+            FLITE_LAUNCH(k_ts_lap, (), nblk(V(l).N), nb, 0, P, V(l));
         } else {
             jst_lap(l);
         }
         if (visc) {
             counted();
-            k_visc_prim<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+            FLITE_LAUNCH(k_visc_prim, (), nblk(V(l).N), nb, 0, P, V(l));
         }
         if (visc && !P.matrixDiss && c.viscosityScheme == 1) {
             counted();
-            k_jflux_vgrad<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+            FLITE_LAUNCH(k_jflux_vgrad, (), nblk(V(l).N), nb, 0, P, V(l));
         } else {
             jst_flux(l);
             if (visc) {
@@ -339,6 +364,7 @@ struct flite_ctx {
         }
     }
     void first_order_diss(int l) {
+        no_group("dissipation scheme 3");
         counted();
         k_first_order_diss<1><<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
@@ -350,6 +376,7 @@ struct flite_ctx {
     }
     // makeArtificialDissipation1 (def_par:10706-11482), level 1 only
     void lp_diss(int l) {
+        no_group("dissipation scheme 1");
         counted();
         k_lp_sums<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
         counted();
@@ -359,7 +386,7 @@ struct flite_ctx {
     void viscous(int l) {
         if (!(c.ReynoldsNumber > 0.0)) return;
         counted();
-        k_visc_prim<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
+        FLITE_LAUNCH(k_visc_prim, (), nblk(V(l).N), nb, 0, P, V(l));
         counted();
         visc_grad(l);
         counted();
@@ -391,10 +418,12 @@ struct flite_ctx {
     }
     // ---- Spalart-Allmaras ----------------------------------------------
     void sa_timesteps(int l) {
+        no_group("the Spalart-Allmaras model");
         counted();
         k_sa_timestep<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
     }
     void sa_diffusion(int l) {
+        no_group("the Spalart-Allmaras model");
         counted();
         k_sa_grad<<<nblk(V(l).N), nb, 0, s>>>(P, V(l));
         counted();
@@ -404,6 +433,7 @@ struct flite_ctx {
     // update, which overwrites the density the source term reads
     void sa_stage(int l, int mode, int stage) {
         if (!sa()) return;
+        no_group("the Spalart-Allmaras model");
         if (turb()) {
             counted();
             k_sa_conv<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), P.unsteady && mode == MODE_STAGE ? 1 : 0);
@@ -419,11 +449,13 @@ struct flite_ctx {
         if (c.reconstruction == FLITE_RECON_VAN_ALBADA && L.grid == 1) {
             // the extension reconstructs from the Galerkin gradients, through
             // the primitive and gradient records
+            no_group("the reconstruction extension");
             counted();
             k_prim_rec<<<nblk(L.N), nb, 0, s>>>(L);
             counted();
             k_gradient_rec<<<nblk(L.N), nb, 0, s>>>(L);
         } else if (c.fluxType == 4 && c.HLLCFluxOrder > 1 && L.grid == 1) {
+            no_group("the HLLC order-2 gradients");
             counted();
             if (c.GradientMethod == 1) k_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
             else k_ls_gradient<<<nblk(L.N), nb, 0, s>>>(P, L);
@@ -436,15 +468,16 @@ struct flite_ctx {
             if (mixed() && !anchor) {
                 // FP32 records of the increments over the anchor
                 counted();
-                k_delta_state<<<nblk(L.N), nb, 0, s>>>(L);
+                FLITE_LAUNCH(k_delta_state, (), nblk(L.N), nb, 0, L);
             } else if (!fused()) {
+                no_group("the upwind fluxes");
                 counted();
                 edge_flux_launch(L);
             }
         }
         if (L.B > 0) {
             counted();
-            k_bnd_flux<<<eblk(L.B), eb, 0, s>>>(P, L);
+            FLITE_LAUNCH(k_bnd_flux, (), eblk(L.B), eb, 0, P, L);
         }
     }
     bool mixed() const { return c.precision == FLITE_MIXED; }
@@ -480,6 +513,7 @@ struct flite_ctx {
     void engine_pass(int l, int mode) {
         const LevelView &L = V(l);
         if (l != 0 || !L.eng.f) return;
+        no_group("the engine conditions");
         counted();
         k_engine_sums<<<1, kEngineLanes, 0, s>>>(P, L, mode);
         const bool all = P.eftype == 2;
@@ -504,7 +538,7 @@ struct flite_ctx {
     // without staging; tiled_mode holds -1 for 0 and 0 for the default, off)
     int tiled_mode[kMaxLevels] = {0};
     int tiled(int l) const {
-        if (!(fused() && !mixed() && lv[l].v.tile.ntiles > 0)) return 0;
+        if (group || !(fused() && !mixed() && lv[l].v.tile.ntiles > 0)) return 0;
         const int m = l < kMaxLevels ? tiled_mode[l] : 0;
         return m < 0 ? 0 : m;
     }
@@ -523,13 +557,13 @@ struct flite_ctx {
             return;
         }
         if (mixed()) {
-            if (anchor) k_node_update<GATHER_ANCHOR, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
-            else k_node_update<GATHER_DELTA, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            if (anchor) FLITE_LAUNCH(k_node_update, (GATHER_ANCHOR, U,), g, nb, 0, P, V(l), mode, stage);
+            else FLITE_LAUNCH(k_node_update, (GATHER_DELTA, U,), g, nb, 0, P, V(l), mode, stage);
         } else if (fused()) {
-            if (unroll == 2 && U == 1) k_node_update<GATHER_CENTRAL2, 1><<<g, nb, 0, s>>>(P, V(l), mode, stage);
-            else k_node_update<GATHER_CENTRAL, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            if (unroll == 2 && U == 1) FLITE_LAUNCH(k_node_update, (GATHER_CENTRAL2, 1,), g, nb, 0, P, V(l), mode, stage);
+            else FLITE_LAUNCH(k_node_update, (GATHER_CENTRAL, U,), g, nb, 0, P, V(l), mode, stage);
         } else {
-            k_node_update<GATHER_BUFFER, U><<<g, nb, 0, s>>>(P, V(l), mode, stage);
+            FLITE_LAUNCH(k_node_update, (GATHER_BUFFER, U,), g, nb, 0, P, V(l), mode, stage);
         }
     }
 
@@ -564,10 +598,10 @@ struct flite_ctx {
     // ---- doTimeIterations (def_par:966-1000) -----------------------------
     void doTimeIterations(int l, int nsteps, bool calcDiss) {
         counted();
-        k_set_int<<<1, 1, 0, s>>>(V(l).cyc, d_cycle);
+        FLITE_LAUNCH(k_case_cycle, (), 1, 1, 0, V(l), d_cycle);
         for (int i = 0; i < nsteps; ++i) {
             counted();
-            k_copy<<<nblk(nvar() * (size_t)V(l).N), nb, 0, s>>>(V(l).u, V(l).uprev, nvar() * (size_t)V(l).N);
+            FLITE_LAUNCH(k_case_save_u, (), nblk(nvar() * (size_t)V(l).N), nb, 0, V(l), nvar() * (size_t)V(l).N);
             singleIteration(l, calcDiss);
         }
     }
@@ -575,7 +609,7 @@ struct flite_ctx {
     void restrictGrid(int fl) {
         const int cl = fl + 1;
         counted();
-        k_restrict_state<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        FLITE_LAUNCH(k_restrict_state, (), nblk(V(cl).N), nb, 0, P, V(cl), V(fl));
         if (c.coarseGridDissipationScheme == 2) {
             ts_jst_viscous(cl, true);
         } else {
@@ -605,15 +639,15 @@ struct flite_ctx {
         node_update(fl, MODE_RFINE, 0, false);
         engine_pass(fl, MODE_RFINE);
         counted();
-        k_restrict_incr<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        FLITE_LAUNCH(k_restrict_incr, (), nblk(V(cl).N), nb, 0, P, V(cl), V(fl));
     }
     // ---- prolongateGrid (def_par:12432-12570) ----------------------------
     void prolongateGrid(int cl) {
         const int fl = cl - 1;
         counted();
-        k_prolong_coarse<<<nblk(V(cl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        FLITE_LAUNCH(k_prolong_coarse, (), nblk(V(cl).N), nb, 0, P, V(cl), V(fl));
         counted();
-        k_prolong_fine<<<nblk(V(fl).N), nb, 0, s>>>(P, V(cl), V(fl));
+        FLITE_LAUNCH(k_prolong_fine, (), nblk(V(fl).N), nb, 0, P, V(cl), V(fl));
         engine_pass(fl, MODE_PROLONG);
     }
     // the head of a physical time step (mg_par:586-602): laminar viscosity
@@ -632,7 +666,7 @@ struct flite_ctx {
     }
     void mapFineToCoarse(int fl) {
         counted();
-        k_restrict_u<<<nblk(V(fl + 1).N), nb, 0, s>>>(V(fl + 1), V(fl));
+        FLITE_LAUNCH(k_restrict_u, (), nblk(V(fl + 1).N), nb, 0, V(fl + 1), V(fl));
     }
     // ---- oneCycle (mg_par:907-1196) --------------------------------------
     void oneCycle() {
@@ -643,16 +677,17 @@ struct flite_ctx {
         if (sch <= 0) {
             for (int i = 1; i <= G - 1; ++i) {
                 counted();
-                k_copy<<<nblk(nvar() * (size_t)V(i - 1).N), nb, 0, s>>>(V(i - 1).u, V(i - 1).uprev,
-                                                                            nvar() * (size_t)V(i - 1).N);
+                FLITE_LAUNCH(k_case_save_u, (), nblk(nvar() * (size_t)V(i - 1).N), nb, 0, V(i - 1),
+                             nvar() * (size_t)V(i - 1).N);
                 mapFineToCoarse(i - 1);
             }
             counted();
-            k_fill<<<nblk(nvar() * (size_t)V(G - 1).N), nb, 0, s>>>(V(G - 1).src, nvar() * (size_t)V(G - 1).N, 0.0);
+            FLITE_LAUNCH(k_case_zero, (), nblk(nvar() * (size_t)V(G - 1).N), nb, 0, V(G - 1), 1,
+                         nvar() * (size_t)V(G - 1).N);
             relax(G, nr, true);
             for (int i = G; i >= 2; --i) {
                 counted();
-                k_inject_u<<<nblk(V(i - 2).N), nb, 0, s>>>(V(i - 1), V(i - 2));
+                FLITE_LAUNCH(k_inject_u, (), nblk(V(i - 2).N), nb, 0, V(i - 1), V(i - 2));
             }
         } else if (sch == 1) {
             for (int i = 1; i <= G - 1; ++i) {

@@ -55,7 +55,10 @@ __device__ __forceinline__ void group_gather(int beg, int end, bool active, int 
 }
 
 // ---- makePressureField (def_par:13612-13630) ------------------------------
-__global__ void k_pressure(Params P, LevelView L) {
+template <bool B>
+__global__ void k_pressure(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -140,8 +143,10 @@ __device__ __forceinline__ void ts_finish(const Params &P, const LevelView &L, i
     ts_store(L, i, acc, h);
 }
 
-template <int U>
-__global__ void k_timestep(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void k_timestep(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -226,8 +231,10 @@ __device__ __forceinline__ void lap_store(const LevelView &L, int i, const LapAc
     for (int c = 0; c < 5; ++c) L.lap[c * N + i] = fact * a.l[c];
 }
 
-template <int U>
-__global__ void k_jst_lap(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void k_jst_lap(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -305,8 +312,10 @@ __device__ __forceinline__ void jflux_inc(const Params &P, const LevelView &L, i
     }
 }
 
-template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -558,7 +567,10 @@ __global__ void k_first_order_diss(Params P, LevelView L) {
 // flux, the adiabatic-wall projection and the wall stress (level 1)
 // per node (u, v, w, T) of the viscous routine (def_par:5260-5270): each
 // edge of the reference divides again; the quotients are the same numbers
-__global__ void k_visc_prim(Params P, LevelView L) {
+template <bool B>
+__global__ void k_visc_prim(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -667,8 +679,10 @@ __device__ __forceinline__ void visc_grad_boundary(const LevelView &L, int i, do
     }
 }
 
-template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -772,8 +786,10 @@ __device__ __forceinline__ void visc_flux_boundary(const LevelView &L, int i, do
 
 // pass 2: viscous edge fluxes gathered per node and subtracted from the
 // dissipation vector (def_par:5662-5892)
-template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -835,7 +851,10 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P, Lev
 // makeTimeSteps with passes 1-2 of makeArtificialDissipation2: the time
 // step reads mu of the neighbours (the previous viscous pass) and writes dt
 // and V/dt; the Laplacian reads u and p and writes the Laplacian and sensor
-__global__ void __launch_bounds__(256, 3) k_ts_lap(Params P, LevelView L) {
+template <bool B>
+__global__ void __launch_bounds__(256, 3) k_ts_lap(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -858,7 +877,10 @@ __global__ void __launch_bounds__(256, 3) k_ts_lap(Params P, LevelView L) {
 // makeViscosityTerm: the JST terms read the Laplacian, sensor, V/dt and u of
 // the neighbours and write the dissipation; the gradients read u, v, w, T
 // and write mu, the stress tensor and the wall stress
-__global__ void __launch_bounds__(256, 2) k_jflux_vgrad(Params P, LevelView L) {
+template <bool B>
+__global__ void __launch_bounds__(256, 2) k_jflux_vgrad(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -936,8 +958,10 @@ __device__ __forceinline__ void visc2_grad_finish(const Params &P, const LevelVi
     L.tau[13 * N + i] = kc;
 }
 
-template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc2_grad(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc2_grad(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -1055,8 +1079,10 @@ __device__ __forceinline__ void visc2_edge_flux(const Visc2Node &a, const Visc2N
 
 // pass 2: the compact edge fluxes and the boundary faces' 4 w_b times each
 // node's own stress, gathered per node and subtracted from the dissipation
-template <int U>
-__global__ void __launch_bounds__(256, U == 1 ? 2 : 1) k_visc2_flux(Params P, LevelView L) {
+template <int U, bool B>
+__global__ void __launch_bounds__(256, U == 1 ? 2 : 1) k_visc2_flux(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -1356,7 +1382,10 @@ __global__ void __launch_bounds__(256) k_edge_flux_muscl(Params P, LevelView L) 
 }
 
 // ---- boundary-edge contributions ------------------------------------------
-__global__ void k_bnd_flux(Params P, LevelView L) {
+template <bool B>
+__global__ void k_bnd_flux(Params P_, LevelView L_) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     int b = tid();
     if (b >= L.B) return;
     double g1[5], g2[5];
@@ -1388,7 +1417,9 @@ __global__ void k_bnd_flux(Params P, LevelView L) {
 
 // the node's record for the increments: anchor primitives and u - ua (FP64
 // difference, rounded once), p - pa
-__global__ void k_delta_state(LevelView L) {
+template <bool B>
+__global__ void k_delta_state(LevelView L_) {
+    FLITE_CASE_L(B, L);
     int i = tid();
     if (i >= L.N) return;
     const int N = L.N;
@@ -1731,9 +1762,11 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
 // GATHER_CENTRAL (central fluxes computed in the gather), GATHER_ANCHOR (the
 // same, stored as the new mixed-precision anchor), GATHER_DELTA (anchor +
 // FP32 increments)
-template <int PREC, int U>
+template <int PREC, int U, bool B>
 __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3 : 1))
-    k_node_update(Params P, LevelView L, int mode, int stage) {
+    k_node_update(Params P_, LevelView L_, int mode, int stage) {
+    FLITE_CASE_P(B, P, L);
+    FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
     const int i_raw = U > 1 ? tid() / U : tid();
     if (U == 1 && i_raw >= L.N) return;
@@ -2131,63 +2164,143 @@ template __global__ void k_node_update_tiled<true, true>(Params, LevelView, int,
 template __global__ void k_node_update_tiled<true, false>(Params, LevelView, int, int);
 template __global__ void k_node_update_tiled<false, true>(Params, LevelView, int, int);
 template __global__ void k_node_update_tiled<false, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 1>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 4>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 8>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 16>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 32>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 1>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 4>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 8>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 16>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 32>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 1>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 4>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 8>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 16>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 32>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 1>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 4>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 8>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 16>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 32>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL2, 1>(Params, LevelView, int, int);
-template __global__ void k_timestep<1>(Params, LevelView);
-template __global__ void k_timestep<4>(Params, LevelView);
-template __global__ void k_timestep<8>(Params, LevelView);
-template __global__ void k_timestep<16>(Params, LevelView);
-template __global__ void k_timestep<32>(Params, LevelView);
-template __global__ void k_jst_lap<1>(Params, LevelView);
-template __global__ void k_jst_lap<4>(Params, LevelView);
-template __global__ void k_jst_lap<8>(Params, LevelView);
-template __global__ void k_jst_lap<16>(Params, LevelView);
-template __global__ void k_jst_lap<32>(Params, LevelView);
-template __global__ void k_jst_flux<1>(Params, LevelView);
-template __global__ void k_jst_flux<4>(Params, LevelView);
-template __global__ void k_jst_flux<8>(Params, LevelView);
-template __global__ void k_jst_flux<16>(Params, LevelView);
-template __global__ void k_jst_flux<32>(Params, LevelView);
-template __global__ void k_visc_grad<1>(Params, LevelView);
-template __global__ void k_visc_grad<4>(Params, LevelView);
-template __global__ void k_visc_grad<8>(Params, LevelView);
-template __global__ void k_visc_grad<16>(Params, LevelView);
-template __global__ void k_visc_grad<32>(Params, LevelView);
-template __global__ void k_visc2_grad<1>(Params, LevelView);
-template __global__ void k_visc2_grad<4>(Params, LevelView);
-template __global__ void k_visc2_grad<8>(Params, LevelView);
-template __global__ void k_visc2_grad<16>(Params, LevelView);
-template __global__ void k_visc2_grad<32>(Params, LevelView);
-template __global__ void k_visc2_flux<1>(Params, LevelView);
-template __global__ void k_visc2_flux<4>(Params, LevelView);
-template __global__ void k_visc2_flux<8>(Params, LevelView);
-template __global__ void k_visc2_flux<16>(Params, LevelView);
-template __global__ void k_visc2_flux<32>(Params, LevelView);
-template __global__ void k_visc_flux<1>(Params, LevelView);
-template __global__ void k_visc_flux<4>(Params, LevelView);
-template __global__ void k_visc_flux<8>(Params, LevelView);
-template __global__ void k_visc_flux<16>(Params, LevelView);
-template __global__ void k_visc_flux<32>(Params, LevelView);
+template __global__ void k_node_update<GATHER_BUFFER, 1, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 4, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 8, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 16, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 32, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 1, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 4, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 8, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 16, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 32, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 1, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 4, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 8, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 16, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 32, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 1, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 4, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 8, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 16, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 32, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2, 1, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2, 1, true>(Params, LevelView, int, int);
+template __global__ void k_timestep<1, false>(Params, LevelView);
+template __global__ void k_timestep<1, true>(Params, LevelView);
+template __global__ void k_timestep<4, false>(Params, LevelView);
+template __global__ void k_timestep<4, true>(Params, LevelView);
+template __global__ void k_timestep<8, false>(Params, LevelView);
+template __global__ void k_timestep<8, true>(Params, LevelView);
+template __global__ void k_timestep<16, false>(Params, LevelView);
+template __global__ void k_timestep<16, true>(Params, LevelView);
+template __global__ void k_timestep<32, false>(Params, LevelView);
+template __global__ void k_timestep<32, true>(Params, LevelView);
+template __global__ void k_jst_lap<1, false>(Params, LevelView);
+template __global__ void k_jst_lap<1, true>(Params, LevelView);
+template __global__ void k_jst_lap<4, false>(Params, LevelView);
+template __global__ void k_jst_lap<4, true>(Params, LevelView);
+template __global__ void k_jst_lap<8, false>(Params, LevelView);
+template __global__ void k_jst_lap<8, true>(Params, LevelView);
+template __global__ void k_jst_lap<16, false>(Params, LevelView);
+template __global__ void k_jst_lap<16, true>(Params, LevelView);
+template __global__ void k_jst_lap<32, false>(Params, LevelView);
+template __global__ void k_jst_lap<32, true>(Params, LevelView);
+template __global__ void k_jst_flux<1, false>(Params, LevelView);
+template __global__ void k_jst_flux<1, true>(Params, LevelView);
+template __global__ void k_jst_flux<4, false>(Params, LevelView);
+template __global__ void k_jst_flux<4, true>(Params, LevelView);
+template __global__ void k_jst_flux<8, false>(Params, LevelView);
+template __global__ void k_jst_flux<8, true>(Params, LevelView);
+template __global__ void k_jst_flux<16, false>(Params, LevelView);
+template __global__ void k_jst_flux<16, true>(Params, LevelView);
+template __global__ void k_jst_flux<32, false>(Params, LevelView);
+template __global__ void k_jst_flux<32, true>(Params, LevelView);
+template __global__ void k_visc_grad<1, false>(Params, LevelView);
+template __global__ void k_visc_grad<1, true>(Params, LevelView);
+template __global__ void k_visc_grad<4, false>(Params, LevelView);
+template __global__ void k_visc_grad<4, true>(Params, LevelView);
+template __global__ void k_visc_grad<8, false>(Params, LevelView);
+template __global__ void k_visc_grad<8, true>(Params, LevelView);
+template __global__ void k_visc_grad<16, false>(Params, LevelView);
+template __global__ void k_visc_grad<16, true>(Params, LevelView);
+template __global__ void k_visc_grad<32, false>(Params, LevelView);
+template __global__ void k_visc_grad<32, true>(Params, LevelView);
+template __global__ void k_visc2_grad<1, false>(Params, LevelView);
+template __global__ void k_visc2_grad<1, true>(Params, LevelView);
+template __global__ void k_visc2_grad<4, false>(Params, LevelView);
+template __global__ void k_visc2_grad<4, true>(Params, LevelView);
+template __global__ void k_visc2_grad<8, false>(Params, LevelView);
+template __global__ void k_visc2_grad<8, true>(Params, LevelView);
+template __global__ void k_visc2_grad<16, false>(Params, LevelView);
+template __global__ void k_visc2_grad<16, true>(Params, LevelView);
+template __global__ void k_visc2_grad<32, false>(Params, LevelView);
+template __global__ void k_visc2_grad<32, true>(Params, LevelView);
+template __global__ void k_visc2_flux<1, false>(Params, LevelView);
+template __global__ void k_visc2_flux<1, true>(Params, LevelView);
+template __global__ void k_visc2_flux<4, false>(Params, LevelView);
+template __global__ void k_visc2_flux<4, true>(Params, LevelView);
+template __global__ void k_visc2_flux<8, false>(Params, LevelView);
+template __global__ void k_visc2_flux<8, true>(Params, LevelView);
+template __global__ void k_visc2_flux<16, false>(Params, LevelView);
+template __global__ void k_visc2_flux<16, true>(Params, LevelView);
+template __global__ void k_visc2_flux<32, false>(Params, LevelView);
+template __global__ void k_visc2_flux<32, true>(Params, LevelView);
+template __global__ void k_visc_flux<1, false>(Params, LevelView);
+template __global__ void k_visc_flux<1, true>(Params, LevelView);
+template __global__ void k_visc_flux<4, false>(Params, LevelView);
+template __global__ void k_visc_flux<4, true>(Params, LevelView);
+template __global__ void k_visc_flux<8, false>(Params, LevelView);
+template __global__ void k_visc_flux<8, true>(Params, LevelView);
+template __global__ void k_visc_flux<16, false>(Params, LevelView);
+template __global__ void k_visc_flux<16, true>(Params, LevelView);
+template __global__ void k_visc_flux<32, false>(Params, LevelView);
+template __global__ void k_visc_flux<32, true>(Params, LevelView);
 template __global__ void k_first_order_diss<1>(Params, LevelView);
+template __global__ void k_pressure<false>(Params, LevelView);
+template __global__ void k_pressure<true>(Params, LevelView);
+template __global__ void k_visc_prim<false>(Params, LevelView);
+template __global__ void k_visc_prim<true>(Params, LevelView);
+template __global__ void k_ts_lap<false>(Params, LevelView);
+template __global__ void k_ts_lap<true>(Params, LevelView);
+template __global__ void k_jflux_vgrad<false>(Params, LevelView);
+template __global__ void k_jflux_vgrad<true>(Params, LevelView);
+template __global__ void k_bnd_flux<false>(Params, LevelView);
+template __global__ void k_bnd_flux<true>(Params, LevelView);
+template __global__ void k_delta_state<false>(LevelView);
+template __global__ void k_delta_state<true>(LevelView);
+template __global__ void k_restrict_u<false>(LevelView, LevelView);
+template __global__ void k_restrict_u<true>(LevelView, LevelView);
+template __global__ void k_restrict_state<false>(Params, LevelView, LevelView);
+template __global__ void k_restrict_state<true>(Params, LevelView, LevelView);
+template __global__ void k_restrict_incr<false>(Params, LevelView, LevelView);
+template __global__ void k_restrict_incr<true>(Params, LevelView, LevelView);
+template __global__ void k_prolong_coarse<false>(Params, LevelView, LevelView);
+template __global__ void k_prolong_coarse<true>(Params, LevelView, LevelView);
+template __global__ void k_prolong_fine<false>(Params, LevelView, LevelView);
+template __global__ void k_prolong_fine<true>(Params, LevelView, LevelView);
+template __global__ void k_inject_u<false>(LevelView, LevelView);
+template __global__ void k_inject_u<true>(LevelView, LevelView);
 
 // ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
 __global__ void k_copy(const double *a, double *b, size_t n) {
@@ -2209,7 +2322,10 @@ __device__ __forceinline__ void restrict_gather(const LevelView &C, const double
 }
 
 // C.u = R(F.u) (plain mapFineToCoarse of the solution)
-__global__ void k_restrict_u(LevelView C, LevelView F) {
+template <bool B>
+__global__ void k_restrict_u(LevelView C_, LevelView F_) {
+    FLITE_CASE_L(B, C);
+    FLITE_CASE_L(B, F);
     int c = tid();
     if (c >= C.N) return;
     double v[6];
@@ -2244,7 +2360,11 @@ __device__ __forceinline__ double sa_bc_increment(const Params &P, unsigned char
 
 // restrictGrid head (def_par:12159-12185): C.u = R(F.u), C.mu = R(F.mu),
 // pressure, boundary conditions, uprev = u, pressure again
-__global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
+template <bool B>
+__global__ void k_restrict_state(Params P_, LevelView C_, LevelView F_) {
+    FLITE_CASE_P(B, P, C);
+    FLITE_CASE_L(B, C);
+    FLITE_CASE_L(B, F);
     int c = tid();
     if (c >= C.N) return;
     const int N = C.N;
@@ -2274,7 +2394,11 @@ __global__ void k_restrict_state(Params P, LevelView C, LevelView F) {
 
 // restrictGrid tail (def_par:12385-12427): C.rhs = R(F.rhs), increment
 // conditions, src -= rhs, u += rhs
-__global__ void k_restrict_incr(Params P, LevelView C, LevelView F) {
+template <bool B>
+__global__ void k_restrict_incr(Params P_, LevelView C_, LevelView F_) {
+    FLITE_CASE_P(B, P, C);
+    FLITE_CASE_L(B, C);
+    FLITE_CASE_L(B, F);
     int c = tid();
     if (c >= C.N) return;
     const int N = C.N;
@@ -2301,7 +2425,11 @@ __global__ void k_restrict_incr(Params P, LevelView C, LevelView F) {
 
 // prolongateGrid coarse part (def_par:12445-12468): uprev = R(F.u) with the
 // solution conditions, rhs = u - uprev with the increment conditions
-__global__ void k_prolong_coarse(Params P, LevelView C, LevelView F) {
+template <bool B>
+__global__ void k_prolong_coarse(Params P_, LevelView C_, LevelView F_) {
+    FLITE_CASE_P(B, P, C);
+    FLITE_CASE_L(B, C);
+    FLITE_CASE_L(B, F);
     int c = tid();
     if (c >= C.N) return;
     const int N = C.N;
@@ -2337,7 +2465,11 @@ __global__ void k_prolong_coarse(Params P, LevelView C, LevelView F) {
 
 // prolongateGrid fine part (def_par:12470-12567): injection, relaxation,
 // u += correction, boundary conditions, floors
-__global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
+template <bool B>
+__global__ void k_prolong_fine(Params P_, LevelView C_, LevelView F_) {
+    FLITE_CASE_P(B, P, C);
+    FLITE_CASE_L(B, C);
+    FLITE_CASE_L(B, F);
     int i = tid();
     if (i >= F.N) return;
     const int N = F.N;
@@ -2388,7 +2520,10 @@ __global__ void k_prolong_fine(Params P, LevelView C, LevelView F) {
 }
 
 // mapCoarseToFine of the solution (injection, def_par:12694-12700)
-__global__ void k_inject_u(LevelView C, LevelView F) {
+template <bool B>
+__global__ void k_inject_u(LevelView C_, LevelView F_) {
+    FLITE_CASE_L(B, C);
+    FLITE_CASE_L(B, F);
     int i = tid();
     if (i >= F.N) return;
     int pc = C.parent[i];
@@ -2421,6 +2556,34 @@ __global__ void k_bc_solution(Params P, LevelView L) {
 __global__ void k_set_int(int *dst, const int *src) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *src;
 }
+
+// The same steps of the multigrid cycle on a level's view, so that a case
+// group runs them for every case in one launch: the level's cycle number
+// (doTimeIterations), uprev = u over n = nvar N values, and the zeroed
+// dissipation (which 0) or FAS source (which 1) over n values.
+template <bool B>
+__global__ void k_case_cycle(LevelView L_, const int *src) {
+    FLITE_CASE_L(B, L);
+    if (threadIdx.x == 0 && blockIdx.x == 0) *L.cyc = *src;
+}
+template <bool B>
+__global__ void k_case_save_u(LevelView L_, size_t n) {
+    FLITE_CASE_L(B, L);
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) L.uprev[i] = L.u[i];
+}
+template <bool B>
+__global__ void k_case_zero(LevelView L_, int which, size_t n) {
+    FLITE_CASE_L(B, L);
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) (which ? L.src : L.diss)[i] = 0.0;
+}
+template __global__ void k_case_cycle<false>(LevelView, const int *);
+template __global__ void k_case_cycle<true>(LevelView, const int *);
+template __global__ void k_case_save_u<false>(LevelView, size_t);
+template __global__ void k_case_save_u<true>(LevelView, size_t);
+template __global__ void k_case_zero<false>(LevelView, int, size_t);
+template __global__ void k_case_zero<true>(LevelView, int, size_t);
 
 // ---- residual norms (writeResiduals mg_par:1299-1443) ---------------------
 // per block: sum (u-uprev)^2 and max |u-uprev| with its first index

@@ -438,7 +438,9 @@ def run_unsteady(solver, steps, cycles_per_step, callback=None):
 
 class Batch:
     """Many solves (mesh x flow condition) advanced together: one CUDA-graph
-    launch per batch cycle; cases on one mesh share the mesh's device copy."""
+    launch per batch cycle; cases on one mesh share the mesh's device copy
+    and, where their controls take the same kernels, every launch of the
+    cycle (a case group)."""
 
     def __init__(self, cases):
         """cases: list of (controls, mesh) pairs."""
@@ -507,6 +509,27 @@ class Batch:
     def set_blocks(self, edge_block, node_block):
         _abi.check(self._lib.flite_batch_set_blocks(self._h, edge_block, node_block),
                    "flite_batch_set_blocks")
+
+    def autotune_lanes(self, reps=2, cycle_no=1, nlevels=8):
+        """Lanes per node of each level's gathers, timed level by level
+        (coarsest first) and set on every case; returns the choice per level
+        and the best batch-cycle time in ms."""
+        lanes = (ctypes.c_int32 * nlevels)()
+        ms = ctypes.c_double()
+        _abi.check(self._lib.flite_batch_autotune_lanes(self._h, cycle_no, reps, nlevels, lanes, ctypes.byref(ms)),
+                   "flite_batch_autotune_lanes")
+        return [v for v in lanes[:] if v], ms.value
+
+    def set_grouping(self, on):
+        """Case groups on (the default) or off: with them every kernel of the
+        cycle runs once for all the cases on one mesh."""
+        _abi.check(self._lib.flite_batch_set_grouping(self._h, int(bool(on))), "flite_batch_set_grouping")
+
+    def groups(self):
+        """The case groups of the last batch graph."""
+        n = ctypes.c_int32()
+        _abi.check(self._lib.flite_batch_groups(self._h, ctypes.byref(n)), "flite_batch_groups")
+        return n.value
 
     def close(self):
         if self._h:

@@ -341,6 +341,18 @@ int flite_batch_time_cycles(flite_batch *b, int cycle_no, int ncycles, int seque
  * keep the fastest pair (advances every case by 9*(reps+1) cycles)       */
 int flite_batch_autotune(flite_batch *b, int cycle_no, int reps, int32_t *edge_block,
                          int32_t *node_block, double *best_ms);
+/* Case groups (on by default): the cases on one mesh whose controls take
+ * the same kernels advance together, every kernel of the cycle launched once
+ * for the group with the case in its grid's y index; 0 turns them off (each
+ * case its own cycle graph inside the batch graph).  Results are the same
+ * either way.  flite_batch_groups gives the groups of the last batch graph. */
+int flite_batch_set_grouping(flite_batch *b, int on);
+/* The gather tile of each level (lanes per node: 1, 4, 8, 16 or 32) picked
+ * by timing batch cycles, coarsest level first, and set on every case;
+ * lanes[l] receives level l+1's choice.  Results do not depend on it.     */
+int flite_batch_autotune_lanes(flite_batch *b, int cycle_no, int reps, int32_t nlevels, int32_t *lanes,
+                               double *best_ms);
+int flite_batch_groups(const flite_batch *b, int32_t *ngroups);
 int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_block);
 
 /* ---- residual evaluation that allocates nothing ------------------------

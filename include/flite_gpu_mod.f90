@@ -262,5 +262,11 @@ module flite_gpu
       integer(c_int32_t), intent(out) :: cycles(*)
       real(c_double), intent(out) :: log10_reduction(*)
     end function
+    ! case groups of the batch: 1 (default) on, 0 off
+    integer(c_int) function flite_batch_set_grouping(batch, on) bind(C, name="flite_batch_set_grouping")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: batch
+      integer(c_int), value :: on
+    end function
   end interface
 end module flite_gpu
