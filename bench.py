@@ -822,6 +822,37 @@ def run_adjoint(args):
     }), flush=True)
 
 
+def small_batch(args, ncases=64, size=(48, 16, 16)):
+    """Many small solves, where launches dominate: the c1 mesh (bump
+    48x16x16, 3 levels) x 64 conditions, inviscid FP64, with case groups and
+    with a graph per case."""
+    import flite3d_b200 as F
+    from flite3d_b200.mesh import splitmix64
+    from flite3d_b200.solver import Batch
+    m = F.Mesh.bump_channel(*size, 0.05, 3)
+    bits = splitmix64(9, 2 * ncases) >> np.uint64(11)
+    uni = bits.astype(np.float64) / float(1 << 53)
+    cases = [(F.default_controls(ReynoldsNumber=0.0, MachNumber=0.3 + 0.5 * uni[2 * k + 1],
+                                 alpha=-4.0 + 12.0 * uni[2 * k], CFLNumber=2.0, fluxType=1, multigridScheme=3,
+                                 numberOfGridsToUse=3), m) for k in range(ncases)]
+    out = {"workload": f"bump {size} x {ncases} conditions, inviscid, FP64, 3 levels", "nodes": m.level(1).n_nodes}
+    for on in (True, False):
+        batch = Batch(cases)
+        batch.set_grouping(on)
+        for (c, mm), s in zip(cases, batch.cases):
+            s.set_state(F.initial_state(c, mm))
+            s.start()
+        batch.time_cycles(args.warmup)
+        ms, launches = batch.time_cycles(args.steps, cycle_no=args.warmup + 1, sequential=False)
+        out["case_groups" if on else "graph_per_case"] = {
+            "value": ncases * args.steps / (ms / 1e3), "unit": "case-cycles/s", "ms_per_step": ms / args.steps,
+            "kernel_launches_per_batch_cycle": launches}
+        batch.close()
+    m.close()
+    out["groups_vs_graph_per_case"] = out["case_groups"]["value"] / out["graph_per_case"]["value"]
+    return out
+
+
 def run_batch(args):
     """Batched solves: the bump channel at 120x40x40, 192x64x64 and
     264x88x88 hexes x 16 flow conditions each (angle of attack uniform in
@@ -855,17 +886,19 @@ def run_batch(args):
         s.start()
     e, nb, best = batch.autotune(reps=2)
     lanes, best_lanes = batch.autotune_lanes(reps=2)
+    grouped = batch.grouping()
     for (c, m), s in zip(cases, batch.cases):
         s.set_state(F.initial_state(c, m))
         s.start()
     batch.time_cycles(args.warmup)
     ms_g, launches = batch.time_cycles(args.steps, cycle_no=args.warmup + 1, sequential=False)
     groups = batch.groups()
-    # the same batch graph with each case's cycle as its own branch, and the
-    # cases' graphs one after another
-    batch.set_grouping(False)
-    ms_c, launches_c = batch.time_cycles(args.steps, cycle_no=args.warmup + args.steps + 1, sequential=False)
+    # the other grouping mode, and the cases' graphs one after another
+    batch.set_grouping(not grouped)
+    ms_o, launches_o = batch.time_cycles(args.steps, cycle_no=args.warmup + args.steps + 1, sequential=False)
     ms_s, _ = batch.time_cycles(args.steps, cycle_no=args.warmup + 2 * args.steps + 1, sequential=True)
+    batch.close()
+    small = small_batch(args)
     n = len(cases)
     print(json.dumps({
         "metric": "batched MG case-cycles/s", "value": n * args.steps / (ms_g / 1e3), "unit": "case-cycles/s",
@@ -875,12 +908,12 @@ def run_batch(args):
                                "conditions (alpha U[-4,8] deg, M U[0.3,0.8]), inviscid, FLITE_MIXED",
                    "cases": n, "mesh_nodes": [m.level(1).n_nodes for m in meshes]},
         "case_groups": groups,
-        "case_graphs": {"value": n * args.steps / (ms_c / 1e3), "ms_per_step": ms_c / args.steps,
-                        "kernel_launches_per_batch_cycle": launches_c,
-                        "what": "the batch graph with every case's cycle graph as its own branch"},
+        "grouping": {"chosen": "case groups" if grouped else "a graph per case",
+                     "other": {"value": n * args.steps / (ms_o / 1e3), "ms_per_step": ms_o / args.steps,
+                               "kernel_launches_per_batch_cycle": launches_o}},
         "sequential": {"value": n * args.steps / (ms_s / 1e3), "ms_per_step": ms_s / args.steps},
-        "graph_vs_sequential": ms_s / ms_g, "groups_vs_case_graphs": ms_c / ms_g,
-        "kernel_launches_per_batch_cycle": launches,
+        "graph_vs_sequential": ms_s / ms_g, "kernel_launches_per_batch_cycle": launches,
+        "small_meshes": small,
         "autotune": {"edge_block": e, "node_block": nb, "best_ms": best, "lanes_per_level": lanes,
                      "best_ms_lanes": best_lanes},
     }), flush=True)

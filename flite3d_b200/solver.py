@@ -525,6 +525,12 @@ class Batch:
         cycle runs once for all the cases on one mesh."""
         _abi.check(self._lib.flite_batch_set_grouping(self._h, int(bool(on))), "flite_batch_set_grouping")
 
+    def grouping(self):
+        """Whether case groups are on (the autotuner keeps the faster mode)."""
+        n = ctypes.c_int32()
+        _abi.check(self._lib.flite_batch_grouping(self._h, ctypes.byref(n)), "flite_batch_grouping")
+        return bool(n.value)
+
     def groups(self):
         """The case groups of the last batch graph."""
         n = ctypes.c_int32()

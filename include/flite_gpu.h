@@ -345,7 +345,8 @@ int flite_batch_autotune(flite_batch *b, int cycle_no, int reps, int32_t *edge_b
  * the same kernels advance together, every kernel of the cycle launched once
  * for the group with the case in its grid's y index; 0 turns them off (each
  * case its own cycle graph inside the batch graph).  Results are the same
- * either way.  flite_batch_groups gives the groups of the last batch graph. */
+ * either way.  flite_batch_groups gives the groups of the last batch graph;
+ * flite_batch_autotune keeps groups on or off, whichever it times faster.  */
 int flite_batch_set_grouping(flite_batch *b, int on);
 /* The gather tile of each level (lanes per node: 1, 4, 8, 16 or 32) picked
  * by timing batch cycles, coarsest level first, and set on every case;
@@ -353,6 +354,7 @@ int flite_batch_set_grouping(flite_batch *b, int on);
 int flite_batch_autotune_lanes(flite_batch *b, int cycle_no, int reps, int32_t nlevels, int32_t *lanes,
                                double *best_ms);
 int flite_batch_groups(const flite_batch *b, int32_t *ngroups);
+int flite_batch_grouping(const flite_batch *b, int32_t *on);
 int flite_batch_set_blocks(flite_batch *b, int32_t edge_block, int32_t node_block);
 
 /* ---- residual evaluation that allocates nothing ------------------------
