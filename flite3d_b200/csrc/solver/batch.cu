@@ -4,9 +4,9 @@
 // same mesh share that mesh's device copy (edges, coefficients, incidence
 // lists, transfer operators, geometry); each case has its own solution state
 // and controls.  One batch cycle is ONE launch of a CUDA graph.  The cases on
-// one mesh form a case group: every kernel of the cycle runs once for the
-// whole group, its grid's y index naming the case (the kernels' group form,
-// which reads the case's level view and parameters from tables), so a group
+// one mesh form case groups: every kernel of the cycle runs once for a whole
+// group, its grid's y index naming the case (the kernels' group form, which
+// takes every case's level view and parameters as its arguments), so a group
 // of G cases costs the launches of one case, and the coarse levels of all G
 // fill the GPU together.  The groups (and cases whose controls take a path
 // without a group form, each as its own cycle graph) are independent
@@ -37,12 +37,10 @@ struct flite_batch {
     int64_t launches = 0;
     std::string err;
     bool grouping = true;          // cases on one mesh advance as a case group
-    std::vector<void *> tables;    // device tables of the graph's case groups
     int ngroups = 0;               // case groups in the graph
 
     ~flite_batch() {
         if (graph) cudaGraphExecDestroy(graph);
-        free_tables();
         // cases that borrow a mesh go first, mesh owners last
         for (size_t i = cases.size(); i-- > 0;)
             if (donor[i] != (int)i && cases[i]) { flite_destroy(cases[i]); cases[i] = nullptr; }
@@ -61,18 +59,6 @@ struct flite_batch {
             cases[i]->select_cycle(cyc);
             if (graph && turb[i] != (char)cases[i]->calcTurb) drop_graph();
         }
-    }
-    void free_tables() {
-        for (void *p : tables) cudaFree(p);
-        tables.clear();
-    }
-    template <class T>
-    T *put_table(const std::vector<T> &h) {
-        void *d = nullptr;
-        CK(cudaMalloc(&d, h.size() * sizeof(T)));
-        tables.push_back(d);
-        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-        return static_cast<T *>(d);
     }
     // cases whose cycles take the same launches (the controls that choose
     // kernels and grids agree; the freestream, CFL numbers and the other
@@ -101,20 +87,11 @@ struct flite_batch {
         for (int k : m)
             if (!same_path(*lead, *cases[k])) return nullptr;
         const size_t G = m.size(), nl = lead->lv.size();
-        std::vector<Params> pt(G);
-        for (size_t k = 0; k < G; ++k) pt[k] = cases[m[k]]->P;
-        const Params *d_pt = put_table(pt);
-        std::vector<const LevelView *> d_v(nl);
-        for (size_t l = 0; l < nl; ++l) {
-            std::vector<LevelView> vt(G);
-            for (size_t k = 0; k < G; ++k) {
-                vt[k] = cases[m[k]]->lv[l].v;
-                vt[k].btab = nullptr;
-                vt[k].ptab = nullptr;
-            }
-            d_v[l] = put_table(vt);
+        lead->gV.assign(nl, CaseTab<LevelView>{});
+        for (size_t k = 0; k < G; ++k) {
+            lead->gP.v[k] = cases[m[k]]->P;
+            for (size_t l = 0; l < nl; ++l) lead->gV[l].v[k] = cases[m[k]]->lv[l].v;
         }
-        for (size_t l = 0; l < nl; ++l) { lead->lv[l].v.btab = d_v[l]; lead->lv[l].v.ptab = d_pt; }
         lead->group = (int)G;
         cudaGraph_t g = nullptr;
         try {
@@ -147,6 +124,10 @@ struct flite_batch {
                 std::vector<int> m;
                 for (size_t j = i; j < cases.size(); ++j)
                     if (active[j] && !done[j] && donor[j] == donor[i]) m.push_back((int)j);
+                // at most kGroupMax cases a group (the parameter bank), in
+                // groups of even size
+                const size_t nchunk = (m.size() + kGroupMax - 1) / kGroupMax;
+                m.resize((m.size() + nchunk - 1) / nchunk);
                 cudaGraph_t g = grouping && m.size() > 1 ? capture_group(m) : nullptr;
                 if (g) {
                     launches += cases[m[0]]->launches;
@@ -171,7 +152,6 @@ struct flite_batch {
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        free_tables();
         for (flite_ctx *c : cases) c->drop_graph();
     }
     void set_cycle(int cyc) {
@@ -314,7 +294,6 @@ int flite_batch_run(flite_batch *b, int first_cycle, int max_cycles, double orde
                 // converged cases leave the batch graph (and their groups)
                 if (b->graph) cudaGraphExecDestroy(b->graph);
                 b->graph = nullptr;
-                b->free_tables();
             }
         }
         for (size_t i = 0; i < n; ++i)

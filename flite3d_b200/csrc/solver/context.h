@@ -56,10 +56,10 @@ using namespace flite_detail;
 // parenthesised with a trailing comma, or ()) for this context, or in group
 // form for every case of its group: the same grid for each case, the case
 // in blockIdx.y
-#define FLITE_LAUNCH(kern, targs, grid, block, smem, ...)                                                   \
-    do {                                                                                                     \
-        if (group) kern<FLITE_UNPAREN targs true><<<dim3((grid), group), (block), (smem), s>>>(__VA_ARGS__); \
-        else kern<FLITE_UNPAREN targs false><<<(grid), (block), (smem), s>>>(__VA_ARGS__);                   \
+#define FLITE_LAUNCH(kern, targs, grid, block, smem, ...)                                                     \
+    do {                                                                                                       \
+        if (group) launch_group(kern<FLITE_UNPAREN targs true>, dim3((grid), group), (block), (smem), __VA_ARGS__); \
+        else kern<FLITE_UNPAREN targs false><<<(grid), (block), (smem), s>>>(__VA_ARGS__);                     \
     } while (0)
 
 // a gather kernel template launched with the lanes per node of level l
@@ -102,9 +102,23 @@ struct flite_ctx {
     bool counting = false;
     // a case group (batch cases on one mesh, advanced together): while
     // `group` > 0 the cycle's launches run in group form for that many
-    // cases, whose level views and parameters the views of this context
-    // carry (btab, ptab).  Paths without a group form refuse it.
+    // cases, with every case's parameters and level views (gP, gV) in the
+    // kernel's parameter bank.  Paths without a group form refuse it.
     int group = 0;
+    CaseTab<Params> gP{};
+    std::vector<CaseTab<LevelView>> gV;
+    const CaseTab<Params> &to_group(const Params &) const { return gP; }
+    const CaseTab<LevelView> &to_group(const LevelView &v) const {
+        for (size_t l = 0; l < lv.size(); ++l)
+            if (&lv[l].v == &v) return gV[l];
+        throw std::runtime_error("a group launch argument is not one of the context's level views");
+    }
+    template <class T>
+    const T &to_group(const T &x) const { return x; }
+    template <class... KP, class... A>
+    void launch_group(void (*k)(KP...), dim3 g, unsigned b, size_t sm, const A &...a) {
+        k<<<g, b, sm, s>>>(to_group(a)...);
+    }
     struct no_group_error : std::runtime_error {
         using std::runtime_error::runtime_error;
     };

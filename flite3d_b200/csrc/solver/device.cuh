@@ -195,24 +195,37 @@ struct LevelView {
     const int *perm;                       // [N]
     TileView tile;                         // staging of node blocks (fluxType 1)
     EngineView eng;                        // level 1 of a mesh with engines; zero otherwise
-    // a case group (cases of one batch on one mesh, advanced by the same
-    // launches): every case's view of this level and every case's
-    // parameters, indexed by blockIdx.y in the group form of a kernel
-    const LevelView *btab;
-    const Params *ptab;
 };
 
 // The view and parameters a kernel works on: its own arguments, or in the
-// group form (B) those of case blockIdx.y of the group, whose every case
-// has the same mesh and so the same grid.  The kernels name their arguments
-// P_ and L_ (C_, F_) and take P and L (C, F) from these.
+// group form (B) those of case blockIdx.y of its group, whose every case has
+// the same mesh and so the same grid.  The group form takes every case's
+// arguments in its parameter bank (CaseTab; kernel parameters of up to
+// 32,764 bytes: kGroupMax cases of a kernel with two level views), read
+// with the case's index like the single form's own.  The kernels name their
+// arguments P_ and L_ (C_, F_) and take P and L (C, F) from these.
+constexpr int kGroupMax = 14;
+template <class T>
+struct CaseTab {
+    T v[kGroupMax];
+};
 template <bool B, class T>
-__device__ __forceinline__ const T &case_of(const T &own, const T *tab) {
-    if constexpr (B) return tab[blockIdx.y];
-    else return own;
+struct CaseArgT {
+    using type = T;
+};
+template <class T>
+struct CaseArgT<true, T> {
+    using type = CaseTab<T>;
+};
+template <bool B, class T>
+using CaseArg = typename CaseArgT<B, T>::type;
+template <bool B, class T>
+__device__ __forceinline__ const T &case_of(const CaseArg<B, T> &a) {
+    if constexpr (B) return a.v[blockIdx.y];
+    else return a;
 }
-#define FLITE_CASE_P(B, P, V) const Params &P = case_of<B>(P##_, V##_.ptab)
-#define FLITE_CASE_L(B, V) const LevelView &V = case_of<B>(V##_, V##_.btab)
+#define FLITE_CASE_P(B, P, V) const Params &P = case_of<B, Params>(P##_)
+#define FLITE_CASE_L(B, V) const LevelView &V = case_of<B, LevelView>(V##_)
 
 __device__ __forceinline__ EdgeW load_edgew(const EdgeW *w, int e) {
     const double2 *p = reinterpret_cast<const double2 *>(w + e);

@@ -56,7 +56,7 @@ __device__ __forceinline__ void group_gather(int beg, int end, bool active, int 
 
 // ---- makePressureField (def_par:13612-13630) ------------------------------
 template <bool B>
-__global__ void k_pressure(Params P_, LevelView L_) {
+__global__ void k_pressure(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     int i = tid();
@@ -144,7 +144,7 @@ __device__ __forceinline__ void ts_finish(const Params &P, const LevelView &L, i
 }
 
 template <int U, bool B>
-__global__ void k_timestep(Params P_, LevelView L_) {
+__global__ void k_timestep(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -232,7 +232,7 @@ __device__ __forceinline__ void lap_store(const LevelView &L, int i, const LapAc
 }
 
 template <int U, bool B>
-__global__ void k_jst_lap(Params P_, LevelView L_) {
+__global__ void k_jst_lap(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -313,7 +313,7 @@ __device__ __forceinline__ void jflux_inc(const Params &P, const LevelView &L, i
 }
 
 template <int U, bool B>
-__global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, U == 1 ? 4 : 1) k_jst_flux(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -568,7 +568,7 @@ __global__ void k_first_order_diss(Params P, LevelView L) {
 // per node (u, v, w, T) of the viscous routine (def_par:5260-5270): each
 // edge of the reference divides again; the quotients are the same numbers
 template <bool B>
-__global__ void k_visc_prim(Params P_, LevelView L_) {
+__global__ void k_visc_prim(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     int i = tid();
@@ -680,7 +680,7 @@ __device__ __forceinline__ void visc_grad_boundary(const LevelView &L, int i, do
 }
 
 template <int U, bool B>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_grad(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -787,7 +787,7 @@ __device__ __forceinline__ void visc_flux_boundary(const LevelView &L, int i, do
 // pass 2: viscous edge fluxes gathered per node and subtracted from the
 // dissipation vector (def_par:5662-5892)
 template <int U, bool B>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -852,7 +852,7 @@ __global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc_flux(Params P_, Le
 // step reads mu of the neighbours (the previous viscous pass) and writes dt
 // and V/dt; the Laplacian reads u and p and writes the Laplacian and sensor
 template <bool B>
-__global__ void __launch_bounds__(256, 3) k_ts_lap(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, 3) k_ts_lap(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int i = tid();
@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(256, 3) k_ts_lap(Params P_, LevelView L_) {
 // the neighbours and write the dissipation; the gradients read u, v, w, T
 // and write mu, the stress tensor and the wall stress
 template <bool B>
-__global__ void __launch_bounds__(256, 2) k_jflux_vgrad(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, 2) k_jflux_vgrad(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int i = tid();
@@ -959,7 +959,7 @@ __device__ __forceinline__ void visc2_grad_finish(const Params &P, const LevelVi
 }
 
 template <int U, bool B>
-__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc2_grad(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, U == 1 ? 3 : 1) k_visc2_grad(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -1080,7 +1080,7 @@ __device__ __forceinline__ void visc2_edge_flux(const Visc2Node &a, const Visc2N
 // pass 2: the compact edge fluxes and the boundary faces' 4 w_b times each
 // node's own stress, gathered per node and subtracted from the dissipation
 template <int U, bool B>
-__global__ void __launch_bounds__(256, U == 1 ? 2 : 1) k_visc2_flux(Params P_, LevelView L_) {
+__global__ void __launch_bounds__(256, U == 1 ? 2 : 1) k_visc2_flux(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -1383,7 +1383,7 @@ __global__ void __launch_bounds__(256) k_edge_flux_muscl(Params P, LevelView L) 
 
 // ---- boundary-edge contributions ------------------------------------------
 template <bool B>
-__global__ void k_bnd_flux(Params P_, LevelView L_) {
+__global__ void k_bnd_flux(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     int b = tid();
@@ -1418,7 +1418,7 @@ __global__ void k_bnd_flux(Params P_, LevelView L_) {
 // the node's record for the increments: anchor primitives and u - ua (FP64
 // difference, rounded once), p - pa
 template <bool B>
-__global__ void k_delta_state(LevelView L_) {
+__global__ void k_delta_state(CaseArg<B, LevelView> L_) {
     FLITE_CASE_L(B, L);
     int i = tid();
     if (i >= L.N) return;
@@ -1764,7 +1764,7 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
 // FP32 increments)
 template <int PREC, int U, bool B>
 __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3 : 1))
-    k_node_update(Params P_, LevelView L_, int mode, int stage) {
+    k_node_update(CaseArg<B, Params> P_, CaseArg<B, LevelView> L_, int mode, int stage) {
     FLITE_CASE_P(B, P, L);
     FLITE_CASE_L(B, L);
     const int gl = U > 1 ? (int)(threadIdx.x % U) : 0;  // lane in the node's group
@@ -2165,142 +2165,142 @@ template __global__ void k_node_update_tiled<true, false>(Params, LevelView, int
 template __global__ void k_node_update_tiled<false, true>(Params, LevelView, int, int);
 template __global__ void k_node_update_tiled<false, false>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 1, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 4, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 4, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 8, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 8, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 16, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 16, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 32, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_BUFFER, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_BUFFER, 32, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 1, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 4, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 4, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 8, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 8, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 16, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 16, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 32, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL, 32, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 1, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 4, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 4, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 8, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 8, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 16, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 16, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_ANCHOR, 32, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_ANCHOR, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_ANCHOR, 32, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 1, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 4, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 4, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 4, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 8, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 8, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 8, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 16, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 16, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 16, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_DELTA, 32, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_DELTA, 32, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_DELTA, 32, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL2, 1, false>(Params, LevelView, int, int);
-template __global__ void k_node_update<GATHER_CENTRAL2, 1, true>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_CENTRAL2, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_timestep<1, false>(Params, LevelView);
-template __global__ void k_timestep<1, true>(Params, LevelView);
+template __global__ void k_timestep<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_timestep<4, false>(Params, LevelView);
-template __global__ void k_timestep<4, true>(Params, LevelView);
+template __global__ void k_timestep<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_timestep<8, false>(Params, LevelView);
-template __global__ void k_timestep<8, true>(Params, LevelView);
+template __global__ void k_timestep<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_timestep<16, false>(Params, LevelView);
-template __global__ void k_timestep<16, true>(Params, LevelView);
+template __global__ void k_timestep<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_timestep<32, false>(Params, LevelView);
-template __global__ void k_timestep<32, true>(Params, LevelView);
+template __global__ void k_timestep<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_lap<1, false>(Params, LevelView);
-template __global__ void k_jst_lap<1, true>(Params, LevelView);
+template __global__ void k_jst_lap<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_lap<4, false>(Params, LevelView);
-template __global__ void k_jst_lap<4, true>(Params, LevelView);
+template __global__ void k_jst_lap<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_lap<8, false>(Params, LevelView);
-template __global__ void k_jst_lap<8, true>(Params, LevelView);
+template __global__ void k_jst_lap<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_lap<16, false>(Params, LevelView);
-template __global__ void k_jst_lap<16, true>(Params, LevelView);
+template __global__ void k_jst_lap<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_lap<32, false>(Params, LevelView);
-template __global__ void k_jst_lap<32, true>(Params, LevelView);
+template __global__ void k_jst_lap<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_flux<1, false>(Params, LevelView);
-template __global__ void k_jst_flux<1, true>(Params, LevelView);
+template __global__ void k_jst_flux<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_flux<4, false>(Params, LevelView);
-template __global__ void k_jst_flux<4, true>(Params, LevelView);
+template __global__ void k_jst_flux<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_flux<8, false>(Params, LevelView);
-template __global__ void k_jst_flux<8, true>(Params, LevelView);
+template __global__ void k_jst_flux<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_flux<16, false>(Params, LevelView);
-template __global__ void k_jst_flux<16, true>(Params, LevelView);
+template __global__ void k_jst_flux<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jst_flux<32, false>(Params, LevelView);
-template __global__ void k_jst_flux<32, true>(Params, LevelView);
+template __global__ void k_jst_flux<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_grad<1, false>(Params, LevelView);
-template __global__ void k_visc_grad<1, true>(Params, LevelView);
+template __global__ void k_visc_grad<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_grad<4, false>(Params, LevelView);
-template __global__ void k_visc_grad<4, true>(Params, LevelView);
+template __global__ void k_visc_grad<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_grad<8, false>(Params, LevelView);
-template __global__ void k_visc_grad<8, true>(Params, LevelView);
+template __global__ void k_visc_grad<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_grad<16, false>(Params, LevelView);
-template __global__ void k_visc_grad<16, true>(Params, LevelView);
+template __global__ void k_visc_grad<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_grad<32, false>(Params, LevelView);
-template __global__ void k_visc_grad<32, true>(Params, LevelView);
+template __global__ void k_visc_grad<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_grad<1, false>(Params, LevelView);
-template __global__ void k_visc2_grad<1, true>(Params, LevelView);
+template __global__ void k_visc2_grad<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_grad<4, false>(Params, LevelView);
-template __global__ void k_visc2_grad<4, true>(Params, LevelView);
+template __global__ void k_visc2_grad<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_grad<8, false>(Params, LevelView);
-template __global__ void k_visc2_grad<8, true>(Params, LevelView);
+template __global__ void k_visc2_grad<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_grad<16, false>(Params, LevelView);
-template __global__ void k_visc2_grad<16, true>(Params, LevelView);
+template __global__ void k_visc2_grad<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_grad<32, false>(Params, LevelView);
-template __global__ void k_visc2_grad<32, true>(Params, LevelView);
+template __global__ void k_visc2_grad<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_flux<1, false>(Params, LevelView);
-template __global__ void k_visc2_flux<1, true>(Params, LevelView);
+template __global__ void k_visc2_flux<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_flux<4, false>(Params, LevelView);
-template __global__ void k_visc2_flux<4, true>(Params, LevelView);
+template __global__ void k_visc2_flux<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_flux<8, false>(Params, LevelView);
-template __global__ void k_visc2_flux<8, true>(Params, LevelView);
+template __global__ void k_visc2_flux<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_flux<16, false>(Params, LevelView);
-template __global__ void k_visc2_flux<16, true>(Params, LevelView);
+template __global__ void k_visc2_flux<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc2_flux<32, false>(Params, LevelView);
-template __global__ void k_visc2_flux<32, true>(Params, LevelView);
+template __global__ void k_visc2_flux<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_flux<1, false>(Params, LevelView);
-template __global__ void k_visc_flux<1, true>(Params, LevelView);
+template __global__ void k_visc_flux<1, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_flux<4, false>(Params, LevelView);
-template __global__ void k_visc_flux<4, true>(Params, LevelView);
+template __global__ void k_visc_flux<4, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_flux<8, false>(Params, LevelView);
-template __global__ void k_visc_flux<8, true>(Params, LevelView);
+template __global__ void k_visc_flux<8, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_flux<16, false>(Params, LevelView);
-template __global__ void k_visc_flux<16, true>(Params, LevelView);
+template __global__ void k_visc_flux<16, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_flux<32, false>(Params, LevelView);
-template __global__ void k_visc_flux<32, true>(Params, LevelView);
+template __global__ void k_visc_flux<32, true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_first_order_diss<1>(Params, LevelView);
 template __global__ void k_pressure<false>(Params, LevelView);
-template __global__ void k_pressure<true>(Params, LevelView);
+template __global__ void k_pressure<true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_visc_prim<false>(Params, LevelView);
-template __global__ void k_visc_prim<true>(Params, LevelView);
+template __global__ void k_visc_prim<true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_ts_lap<false>(Params, LevelView);
-template __global__ void k_ts_lap<true>(Params, LevelView);
+template __global__ void k_ts_lap<true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_jflux_vgrad<false>(Params, LevelView);
-template __global__ void k_jflux_vgrad<true>(Params, LevelView);
+template __global__ void k_jflux_vgrad<true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_bnd_flux<false>(Params, LevelView);
-template __global__ void k_bnd_flux<true>(Params, LevelView);
+template __global__ void k_bnd_flux<true>(CaseTab<Params>, CaseTab<LevelView>);
 template __global__ void k_delta_state<false>(LevelView);
-template __global__ void k_delta_state<true>(LevelView);
+template __global__ void k_delta_state<true>(CaseTab<LevelView>);
 template __global__ void k_restrict_u<false>(LevelView, LevelView);
-template __global__ void k_restrict_u<true>(LevelView, LevelView);
+template __global__ void k_restrict_u<true>(CaseTab<LevelView>, CaseTab<LevelView>);
 template __global__ void k_restrict_state<false>(Params, LevelView, LevelView);
-template __global__ void k_restrict_state<true>(Params, LevelView, LevelView);
+template __global__ void k_restrict_state<true>(CaseTab<Params>, CaseTab<LevelView>, CaseTab<LevelView>);
 template __global__ void k_restrict_incr<false>(Params, LevelView, LevelView);
-template __global__ void k_restrict_incr<true>(Params, LevelView, LevelView);
+template __global__ void k_restrict_incr<true>(CaseTab<Params>, CaseTab<LevelView>, CaseTab<LevelView>);
 template __global__ void k_prolong_coarse<false>(Params, LevelView, LevelView);
-template __global__ void k_prolong_coarse<true>(Params, LevelView, LevelView);
+template __global__ void k_prolong_coarse<true>(CaseTab<Params>, CaseTab<LevelView>, CaseTab<LevelView>);
 template __global__ void k_prolong_fine<false>(Params, LevelView, LevelView);
-template __global__ void k_prolong_fine<true>(Params, LevelView, LevelView);
+template __global__ void k_prolong_fine<true>(CaseTab<Params>, CaseTab<LevelView>, CaseTab<LevelView>);
 template __global__ void k_inject_u<false>(LevelView, LevelView);
-template __global__ void k_inject_u<true>(LevelView, LevelView);
+template __global__ void k_inject_u<true>(CaseTab<LevelView>, CaseTab<LevelView>);
 
 // ---- copy u -> uprev (doTimeIterations def_par:983-987) -------------------
 __global__ void k_copy(const double *a, double *b, size_t n) {
@@ -2323,7 +2323,7 @@ __device__ __forceinline__ void restrict_gather(const LevelView &C, const double
 
 // C.u = R(F.u) (plain mapFineToCoarse of the solution)
 template <bool B>
-__global__ void k_restrict_u(LevelView C_, LevelView F_) {
+__global__ void k_restrict_u(CaseArg<B, LevelView> C_, CaseArg<B, LevelView> F_) {
     FLITE_CASE_L(B, C);
     FLITE_CASE_L(B, F);
     int c = tid();
@@ -2361,7 +2361,7 @@ __device__ __forceinline__ double sa_bc_increment(const Params &P, unsigned char
 // restrictGrid head (def_par:12159-12185): C.u = R(F.u), C.mu = R(F.mu),
 // pressure, boundary conditions, uprev = u, pressure again
 template <bool B>
-__global__ void k_restrict_state(Params P_, LevelView C_, LevelView F_) {
+__global__ void k_restrict_state(CaseArg<B, Params> P_, CaseArg<B, LevelView> C_, CaseArg<B, LevelView> F_) {
     FLITE_CASE_P(B, P, C);
     FLITE_CASE_L(B, C);
     FLITE_CASE_L(B, F);
@@ -2395,7 +2395,7 @@ __global__ void k_restrict_state(Params P_, LevelView C_, LevelView F_) {
 // restrictGrid tail (def_par:12385-12427): C.rhs = R(F.rhs), increment
 // conditions, src -= rhs, u += rhs
 template <bool B>
-__global__ void k_restrict_incr(Params P_, LevelView C_, LevelView F_) {
+__global__ void k_restrict_incr(CaseArg<B, Params> P_, CaseArg<B, LevelView> C_, CaseArg<B, LevelView> F_) {
     FLITE_CASE_P(B, P, C);
     FLITE_CASE_L(B, C);
     FLITE_CASE_L(B, F);
@@ -2426,7 +2426,7 @@ __global__ void k_restrict_incr(Params P_, LevelView C_, LevelView F_) {
 // prolongateGrid coarse part (def_par:12445-12468): uprev = R(F.u) with the
 // solution conditions, rhs = u - uprev with the increment conditions
 template <bool B>
-__global__ void k_prolong_coarse(Params P_, LevelView C_, LevelView F_) {
+__global__ void k_prolong_coarse(CaseArg<B, Params> P_, CaseArg<B, LevelView> C_, CaseArg<B, LevelView> F_) {
     FLITE_CASE_P(B, P, C);
     FLITE_CASE_L(B, C);
     FLITE_CASE_L(B, F);
@@ -2466,7 +2466,7 @@ __global__ void k_prolong_coarse(Params P_, LevelView C_, LevelView F_) {
 // prolongateGrid fine part (def_par:12470-12567): injection, relaxation,
 // u += correction, boundary conditions, floors
 template <bool B>
-__global__ void k_prolong_fine(Params P_, LevelView C_, LevelView F_) {
+__global__ void k_prolong_fine(CaseArg<B, Params> P_, CaseArg<B, LevelView> C_, CaseArg<B, LevelView> F_) {
     FLITE_CASE_P(B, P, C);
     FLITE_CASE_L(B, C);
     FLITE_CASE_L(B, F);
@@ -2521,7 +2521,7 @@ __global__ void k_prolong_fine(Params P_, LevelView C_, LevelView F_) {
 
 // mapCoarseToFine of the solution (injection, def_par:12694-12700)
 template <bool B>
-__global__ void k_inject_u(LevelView C_, LevelView F_) {
+__global__ void k_inject_u(CaseArg<B, LevelView> C_, CaseArg<B, LevelView> F_) {
     FLITE_CASE_L(B, C);
     FLITE_CASE_L(B, F);
     int i = tid();
@@ -2562,28 +2562,28 @@ __global__ void k_set_int(int *dst, const int *src) {
 // (doTimeIterations), uprev = u over n = nvar N values, and the zeroed
 // dissipation (which 0) or FAS source (which 1) over n values.
 template <bool B>
-__global__ void k_case_cycle(LevelView L_, const int *src) {
+__global__ void k_case_cycle(CaseArg<B, LevelView> L_, const int *src) {
     FLITE_CASE_L(B, L);
     if (threadIdx.x == 0 && blockIdx.x == 0) *L.cyc = *src;
 }
 template <bool B>
-__global__ void k_case_save_u(LevelView L_, size_t n) {
+__global__ void k_case_save_u(CaseArg<B, LevelView> L_, size_t n) {
     FLITE_CASE_L(B, L);
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) L.uprev[i] = L.u[i];
 }
 template <bool B>
-__global__ void k_case_zero(LevelView L_, int which, size_t n) {
+__global__ void k_case_zero(CaseArg<B, LevelView> L_, int which, size_t n) {
     FLITE_CASE_L(B, L);
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) (which ? L.src : L.diss)[i] = 0.0;
 }
 template __global__ void k_case_cycle<false>(LevelView, const int *);
-template __global__ void k_case_cycle<true>(LevelView, const int *);
+template __global__ void k_case_cycle<true>(CaseTab<LevelView>, const int *);
 template __global__ void k_case_save_u<false>(LevelView, size_t);
-template __global__ void k_case_save_u<true>(LevelView, size_t);
+template __global__ void k_case_save_u<true>(CaseTab<LevelView>, size_t);
 template __global__ void k_case_zero<false>(LevelView, int, size_t);
-template __global__ void k_case_zero<true>(LevelView, int, size_t);
+template __global__ void k_case_zero<true>(CaseTab<LevelView>, int, size_t);
 
 // ---- residual norms (writeResiduals mg_par:1299-1443) ---------------------
 // per block: sum (u-uprev)^2 and max |u-uprev| with its first index
