@@ -16,7 +16,11 @@
 //    dissipation, multiply by dt/V, boundary conditions on the increment,
 //    the clipped update, boundary conditions on the solution, the FAS
 //    source, the density floor, the far-field conditions) is fused into the
-//    node kernel that gathers the residual.
+//    node kernel that gathers the residual;
+//  * the kernels of the multigrid cycle also have a group form (template
+//    flag B): one launch serves every case of a batch's case group, the
+//    case in blockIdx.y and its parameters and level views among the
+//    arguments (FLITE_CASE_P / FLITE_CASE_L).
 #include <cuda_runtime.h>
 
 #include "flux.cuh"
