@@ -139,3 +139,97 @@ def test_engine_refusals():
         s.close()
     finally:
         mesh.close()
+
+
+@pytest.mark.parametrize("ftype", [1, 2])
+def test_engines_in_the_device_node_order(ftype):
+    # the locality renumbering at the ABI maps the engine sides' nodes too
+    from flite3d_b200.solver import set_node_order
+    mesh = box(8, 4, 4, kind="tet", nlevels=3, engines=2)
+    c = default_controls(**{**BASE, "engineFlowType": ftype,
+                            "enginesFrontMassFlow": [0.09, 0.07] if ftype == 2 else [0.06, 0.05]})
+    set_node_order(1)
+    try:
+        g = Solver(c, mesh)
+    finally:
+        set_node_order(0)
+    o = Solver(c, mesh, backend=oracle_backend())
+    try:
+        u0 = initial_state(c, mesh, perturb_seed=11, amplitude=0.02)
+        for s in (g, o):
+            s.set_state(u0)
+            s.start()
+        for cyc in range(1, 4):
+            g.cycle(cyc)
+            o.cycle(cyc)
+            assert_same(g, o, 3, (ftype, cyc))
+    finally:
+        g.close()
+        o.close()
+        mesh.close()
+
+
+def test_engines_from_domain_files(tmp_path):
+    # a parallel run's files with engine inlet sides, ingested, on the GPU
+    from flite3d_b200 import Mesh
+    mesh = box(8, 4, 4, kind="hex", nlevels=3, engines=2)
+    mesh.write_sol_domains(tmp_path / "e", tmp_path / "plotreg.reg", 3)
+    merged = Mesh.read_sol_domains(tmp_path / "e", tmp_path / "plotreg.reg")
+    c = default_controls(**BASE)
+    g, o = run_pair(c, merged)
+    try:
+        for cyc in range(1, 4):
+            g.cycle(cyc)
+            o.cycle(cyc)
+            assert_same(g, o, 3, cyc)
+    finally:
+        g.close()
+        o.close()
+        merged.close()
+        mesh.close()
+
+
+def test_engine_cases_in_a_batch_keep_their_own_graphs():
+    # the engine conditions have no case-group form: such cases run as their
+    # own branches of the batch graph, each as its solve alone
+    from flite3d_b200.solver import Batch
+    mesh = box(8, 4, 4, kind="tet", nlevels=3, engines=2)
+    cases = [(default_controls(**{**BASE, "alpha": a}), mesh) for a in (0.0, 2.0)]
+    batch = Batch(cases)
+    try:
+        singles = [Solver(c, m) for c, m in cases]
+        for (c, m), bs, ss in zip(cases, batch.cases, singles):
+            u0 = initial_state(c, m, perturb_seed=5, amplitude=0.02)
+            for s in (bs, ss):
+                s.set_state(u0)
+                s.start()
+        for cyc in range(1, 3):
+            batch.cycle(cyc)
+            for s in singles:
+                s.cycle(cyc)
+        assert batch.groups() == 0
+        for bs, ss in zip(batch.cases, singles):
+            assert np.array_equal(bs.get_state(1), ss.get_state(1))
+        for s in singles:
+            s.close()
+    finally:
+        batch.close()
+        mesh.close()
+
+
+def test_engines_with_mixed_precision_run():
+    # FLITE_MIXED takes the engine conditions in FP64 like every node step
+    mesh = box(8, 4, 4, kind="tet", nlevels=3, engines=2)
+    c = default_controls(**{**BASE, "precision": 1})
+    s = Solver(c, mesh)
+    try:
+        s.set_state(initial_state(c, mesh, perturb_seed=11, amplitude=0.02))
+        s.start()
+        res = []
+        for cyc in range(1, 11):
+            s.cycle(cyc)
+            res.append(s.residuals()[0][0])
+        assert np.all(np.isfinite(s.get_state(1))) and res[-1] < res[0]
+    finally:
+        s.close()
+        mesh.close()
