@@ -1918,6 +1918,9 @@ int fp_set_moving_geometry(fp_mesh *m, const double *xyz, const double *xyz_prev
     if (!m || m->lv.empty() || (m->tets.empty() && !m->hybrid()) || !xyz || !xyz_prev || !xyz_prev2 ||
         (time_scheme != 1 && time_scheme != 2))
         return FLITE_EINVAL;
+    // the engine inlet sides would need the step's coordinates too; the
+    // solver takes no engine conditions on a moving mesh
+    if (m->lv[0].nes() > 0) return FLITE_EUNSUPPORTED;
     return guarded([&] {
         LevelData &L = m->lv[0];
         const size_t N = L.N, E = L.E, B = L.B;

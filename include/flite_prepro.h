@@ -93,7 +93,9 @@ int fp_geometry_vjp(const fp_mesh *m, const double *xyz, const double *side_w_ba
  * levels sum them through the agglomeration (restriction weights from the
  * new volumes).  The level descriptors then carry side_gcl, bnd_gcl,
  * volume_prev, volume_prev2 and coord_move.  Three equal coordinate sets give
- * the static arrays back bit for bit with zero GCL weights.                 */
+ * the static arrays back bit for bit with zero GCL weights.  A mesh with
+ * engine inlet sides returns FLITE_EUNSUPPORTED (the solver takes no engine
+ * conditions on a moving mesh).                                            */
 int fp_set_moving_geometry(fp_mesh *m, const double *xyz, const double *xyz_prev, const double *xyz_prev2,
                            int32_t time_scheme);
 /* The level-1 coordinate movement of the solver's reader from the

@@ -187,6 +187,9 @@ def test_refusals():
         c = engine_controls(numberOfGridsToUse=1, flowType=2, physicalTimeStep=0.1)
         with pytest.raises(RuntimeError):
             Solver(c, m, backend=oracle_backend())
+        x0 = m.array(1, "coords")
+        with pytest.raises(RuntimeError):
+            m.set_moving(x0, x0, x0, 2)
         # the tangent products are of the engine-free residual
         c = engine_controls(numberOfGridsToUse=1)
         o = Solver(c, m, backend=oracle_backend())
