@@ -31,11 +31,12 @@ def _lowest_first(q):
     return q[k:] + q[:k]
 
 
-def box(nx=6, ny=3, nz=3, kind="hex", nlevels=2, engines=False):
+def box(nx=6, ny=3, nz=3, kind="hex", nlevels=2, engines=False, far_only=False):
     """kind: "hex", "prism", "pyramid", "mixed" (columns of hexahedra and
-    prisms, whose face diagonals follow the node numbers alike) or "tet"."""
+    prisms, whose face diagonals follow the node numbers alike) or "tet";
+    far_only (tetrahedra): every face that is not an engine face is far field."""
     if kind == "tet":
-        return _tet_box(nx, ny, nz, nlevels, engines)
+        return _tet_box(nx, ny, nz, nlevels, engines, far_only)
     xyz = _grid(nx, ny, nz)
 
     def nid(i, j, k):
@@ -97,7 +98,7 @@ def _x_face_indicator(outflow, j, k, ny, nz, engines):
     return 3
 
 
-def _tet_box(nx, ny, nz, nlevels, engines):
+def _tet_box(nx, ny, nz, nlevels, engines, far_only=False):
     xyz = _grid(nx, ny, nz)
 
     def nid(i, j, k):
@@ -113,6 +114,8 @@ def _tet_box(nx, ny, nz, nlevels, engines):
                     tets.append([h[t[0]], h[t[1]], h[t[2]], h[t[3]]])
 
     def quad(q, indicator):  # split along q0-q2, the diagonal of the tetrahedra
+        if far_only and indicator in (1, 2):
+            indicator = 3
         tris.extend([[q[0], q[1], q[2]], [q[0], q[2], q[3]]])
         ind.extend([indicator, indicator])
 
