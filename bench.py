@@ -884,8 +884,12 @@ def run_batch(args):
     for (c, m), s in zip(cases, batch.cases):
         s.set_state(F.initial_state(c, m))
         s.start()
-    e, nb, best = batch.autotune(reps=2)
-    lanes, best_lanes = batch.autotune_lanes(reps=2)
+    e, nb, best, lanes, best_lanes = 256, 256, None, None, None
+    if not args.batch_no_autotune:
+        e, nb, best = batch.autotune(reps=2)
+        lanes, best_lanes = batch.autotune_lanes(reps=2)
+    if args.batch_grouping != "auto":  # the mode asked for in place of the tuner's
+        batch.set_grouping(args.batch_grouping == "on")
     grouped = batch.grouping()
     for (c, m), s in zip(cases, batch.cases):
         s.set_state(F.initial_state(c, m))
@@ -898,7 +902,7 @@ def run_batch(args):
     ms_o, launches_o = batch.time_cycles(args.steps, cycle_no=args.warmup + args.steps + 1, sequential=False)
     ms_s, _ = batch.time_cycles(args.steps, cycle_no=args.warmup + 2 * args.steps + 1, sequential=True)
     batch.close()
-    small = small_batch(args)
+    small = None if args.no_small_batch else small_batch(args)
     n = len(cases)
     print(json.dumps({
         "metric": "batched MG case-cycles/s", "value": n * args.steps / (ms_g / 1e3), "unit": "case-cycles/s",
@@ -962,6 +966,10 @@ def main():
     ap.add_argument("--upwind-mesh", default="48,16,16", help="NX,NY,NZ hexes of the upwind workload")
     ap.add_argument("--batch-meshes", type=int, default=3)
     ap.add_argument("--batch-conditions", type=int, default=16)
+    ap.add_argument("--batch-grouping", default="auto", choices=["auto", "on", "off"],
+                    help="case groups on or off, or the autotuner's choice")
+    ap.add_argument("--no-small-batch", action="store_true", help="skip the batch of small meshes")
+    ap.add_argument("--batch-no-autotune", action="store_true", help="default block sizes and gather tiles")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -105,6 +105,9 @@ def _run_batch(cases, cycles, grouping, lanes=0, seed=7):
     dict(ReynoldsNumber=800.0, wallsAreIsentropic=1),
     dict(ReynoldsNumber=800.0, wallsAreIsentropic=0, viscosityScheme=2, CFLNumber=1.0),
     dict(ReynoldsNumber=0.0, multigridScheme=1, rungeKuttaStages=5),
+    dict(ReynoldsNumber=0.0, multigridScheme=2, numberOfRelaxationSteps=2),
+    dict(ReynoldsNumber=0.0, multigridScheme=0),
+    dict(ReynoldsNumber=0.0, flowType=1, physicalTimeStep=0.2, timeScheme=2),
 ])
 @pytest.mark.parametrize("lanes", [0, 4])
 def test_case_groups_match_separate_case_graphs(gpu, config, lanes):
