@@ -92,7 +92,7 @@ GPU_SYMBOLS = [
     "flite_forces", "flite_residual_fwd", "flite_time_cycles", "flite_cycle_launches",
     "flite_profile_level", "flite_batch_create", "flite_batch_destroy", "flite_batch_context",
     "flite_batch_cycle", "flite_batch_run", "flite_batch_time_cycles", "flite_batch_autotune", "flite_batch_set_blocks", "flite_batch_set_grouping", "flite_batch_groups", "flite_batch_grouping",
-    "flite_batch_autotune_lanes",
+    "flite_batch_autotune_lanes", "flite_explicit_time_step",
     "flite_residual_vjp", "flite_profile_adjoint", "flite_profile_kernels", "flite_set_kernel_options", "flite_set_gather_lanes",
     "flite_iteration_vjp", "flite_adjoint_solve", "flite_objective", "flite_set_adjoint_method",
     "flite_next_physical_step", "flite_set_node_order", "flite_set_tiled_gather", "flite_set_gather_fusion", "flite_update_geometry",

@@ -96,6 +96,7 @@ struct flite_ctx {
     int *d_cycle = nullptr;
     int *d_cyc = nullptr;  // per-level cycle numbers
     double *d_part = nullptr, *d_out = nullptr;
+    double *d_ptsg = nullptr;  // ivd%physicalTimeStep (explicit time stepping)
     int *h_cycle = nullptr;  // pinned
     cudaGraphExec_t graph = nullptr;
     int64_t launches = 0;
@@ -255,7 +256,21 @@ struct flite_ctx {
         counted();
         FLITE_LAUNCH(k_pressure, (), nblk(V(l).N), nb, 0, P, V(l));
     }
+    // makeTimeSteps's ivd%physicalTimeStep under explicit time stepping
+    // (unsteady runs read it; steady ones never do)
+    void explicit_step(int l) {
+        if (!(P.explicit_ && P.unsteady)) return;
+        no_group("explicit time stepping");
+        counted();
+        k_min_dt_init<<<1, 1, 0, s>>>(V(l));
+        counted();
+        k_min_dt<<<(unsigned)std::min<size_t>((V(l).N + 255) / 256, kResidBlocks), 256, 0, s>>>(V(l));
+    }
     void timesteps(int l) {
+        timestep_kernels(l);
+        explicit_step(l);
+    }
+    void timestep_kernels(int l) {
         counted();
         if (const int m = tiled_other(l)) {
             const int K = !P.viscous ? 0 : (P.sa ? 3 : 2);
@@ -355,6 +370,7 @@ struct flite_ctx {
         if (ts) {
             counted();
             FLITE_LAUNCH(k_ts_lap, (), nblk(V(l).N), nb, 0, P, V(l));
+            explicit_step(l);
         } else {
             jst_lap(l);
         }
@@ -450,7 +466,7 @@ struct flite_ctx {
         no_group("the Spalart-Allmaras model");
         if (turb()) {
             counted();
-            k_sa_conv<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), P.unsteady && mode == MODE_STAGE ? 1 : 0);
+            k_sa_conv<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), P.addts && mode == MODE_STAGE ? 1 : 0);
         }
         counted();
         k_sa_stage<<<nblk(V(l).N), nb, 0, s>>>(P, V(l), mode, stage, turb() ? 1 : 0);

@@ -33,8 +33,11 @@ struct Params {
     double harten;
     int fluxType, hllcOrder, autoClip, nsig, isentropic, viscous, boundaryTerm, useDissW, ncfl;
     // unsteady dual time (flowType 1): the physical time step and the
-    // second-order backward difference on level 1 (timeScheme 2)
-    int unsteady, bdf2;
+    // second-order backward difference on level 1 (timeScheme 2); addts
+    // whether the time differences are added (addTimeStep: unsteady and not
+    // explicit, def_par:386-394); explicit time stepping, whose solve takes
+    // one step for every node (LevelView::ptsg)
+    int unsteady, bdf2, addts, explicit_;
     double dtp;
     // Spalart-Allmaras (turbulenceModel 1)
     int sa, nTurbGrids;
@@ -195,6 +198,9 @@ struct LevelView {
     const int *perm;                       // [N]
     TileView tile;                         // staging of node blocks (fluxType 1)
     EngineView eng;                        // level 1 of a mesh with engines; zero otherwise
+    // ivd%physicalTimeStep under explicit time stepping: the smallest local
+    // time step of the last makeTimeSteps on any level (one per context)
+    double *ptsg;
 };
 
 // The view and parameters a kernel works on: its own arguments, or in the

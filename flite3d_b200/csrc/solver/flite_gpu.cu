@@ -113,7 +113,6 @@ void build_tiles(int N, const std::vector<int> &ip, const std::vector<int2> &inc
 const char *unsupported_reason(const flite_controls &c) {
     if (c.flowType != 0 && c.flowType != 1 && c.flowType != 2)
         return "flowType must be 0 (steady), 1 (unsteady, static mesh) or 2 (unsteady, moving mesh)";
-    if (c.explicit_) return "explicit time stepping is not supported";
     if (c.flowType != 0 && !(c.physicalTimeStep > 0)) return "unsteady runs need physicalTimeStep > 0";
     if (c.flowType == 2 && c.precision != FLITE_FP64) return "moving meshes (flowType 2) run in FP64";
     if (c.flowType == 2 && c.reconstruction != FLITE_RECON_NONE)
@@ -293,6 +292,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         P.isentropic = c->wallsAreIsentropic; P.viscous = c->ReynoldsNumber > 0.0;
         P.boundaryTerm = c->boundaryTerm; P.useDissW = c->useDissipationWeighting; P.ncfl = c->numberOfCFLIncrements;
         P.unsteady = c->flowType != 0; P.bdf2 = c->timeScheme == 2; P.dtp = c->physicalTimeStep;
+        P.explicit_ = c->explicit_ != 0;
+        P.addts = P.unsteady && !P.explicit_;
         P.sa = c->turbulenceModel == 1; P.nTurbGrids = c->numberOfTurbulenceGrids;
         P.turbCFL = c->turbulentCFLNumber; P.turbK = c->turbK; P.maxTurb = c->maxTurbulenceValue;
         P.turbProlRelax = c->turbProlongationRelaxation;
@@ -346,6 +347,9 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         }
         X.d_part = X.alloc<double>(kResidBlocks * 18);
         X.d_out = X.alloc<double>(32);
+        // ivd%physicalTimeStep, which explicit time stepping overwrites
+        X.d_ptsg = X.alloc<double>(1);
+        CK(cudaMemcpy(X.d_ptsg, &c->physicalTimeStep, sizeof(double), cudaMemcpyHostToDevice));
         X.lv.resize(G);
         for (int l = 0; l < G; ++l) {
             const flite_level_desc &d = levels[l];
@@ -507,6 +511,7 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
             if (!D.wall.empty()) D.d_wall = X.upload(D.wall);
             L.perm = X.renumbered ? X.d_perm[l] : nullptr;
             }  // mesh upload
+            L.ptsg = X.d_ptsg;
             if (l > 0) L.eng = EngineView{};
             if (l == 0 && P.engines) {
                 if (c->flowType == 2) {
@@ -679,6 +684,15 @@ int flite_start(flite_ctx *ctx) {
         X.physical_step_start();
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(X.s));
+        return FLITE_OK;
+    });
+}
+
+int flite_explicit_time_step(flite_ctx *ctx, double *dt) {
+    if (!ctx || !dt) return FLITE_EINVAL;
+    return guarded(ctx, [&] {
+        CK(cudaStreamSynchronize(ctx->s));
+        CK(cudaMemcpy(dt, ctx->d_ptsg, sizeof(double), cudaMemcpyDeviceToHost));
         return FLITE_OK;
     });
 }

@@ -1696,12 +1696,13 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
         for (int c = 0; c < 5; ++c) L.rhs[c * N + i] = r[c];
         return;
     }
-    if (P.unsteady && mode == MODE_STAGE)  // addTimeDifferences (def_par:1184-1241)
+    if (P.addts && mode == MODE_STAGE)  // addTimeDifferences (def_par:1184-1241)
         for (int c = 0; c < 5; ++c) r[c] = r[c] + time_difference(P, L, i, c);
     for (int c = 0; c < 5; ++c) r[c] = r[c] + L.diss[c * N + i];
     double dt = L.dt[i];
     const double V = L.V[i];
-    if (P.unsteady) dt = dt / (1.0 + 1.5 * dt / P.dtp);  // solveSystem's dual-time step (def_par:1427-1442)
+    // solveSystem's dual-time step, or the explicit global step (def_par:1427-1442)
+    if (P.unsteady) dt = P.explicit_ ? *L.ptsg : dt / (1.0 + 1.5 * dt / P.dtp);
     for (int c = 0; c < 5; ++c) r[c] = dt * r[c] / V;  // solveSystem
     const unsigned char cls = L.bc[i];
     double n0 = 0, n1 = 0, n2 = 0;
@@ -2559,6 +2560,30 @@ __global__ void k_bc_solution(Params P, LevelView L) {
 
 __global__ void k_set_int(int *dst, const int *src) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *src;
+}
+
+// ivd%physicalTimeStep = the smallest local time step of the level
+// (makeTimeSteps under explicit time stepping, def_par:13598-13607): the
+// minimum of positive doubles as the minimum of their bit patterns, which
+// integer atomics take in any order to the same value.  k_min_dt_init
+// starts it at the reference's 9999999.9.
+__global__ void k_min_dt_init(LevelView L) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *L.ptsg = 9999999.9;
+}
+__global__ void k_min_dt(LevelView L) {
+    __shared__ unsigned long long m[256];
+    unsigned long long v = __double_as_longlong(9999999.9);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.N; i += gridDim.x * blockDim.x) {
+        const double d = L.dt[i];
+        if (d < __longlong_as_double((long long)v)) v = (unsigned long long)__double_as_longlong(d);
+    }
+    m[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w && m[threadIdx.x + w] < m[threadIdx.x]) m[threadIdx.x] = m[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicMin(reinterpret_cast<unsigned long long *>(L.ptsg), m[0]);
 }
 
 // The same steps of the multigrid cycle on a level's view, so that a case

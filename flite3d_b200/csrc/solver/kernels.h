@@ -82,6 +82,9 @@ constexpr int kEngineLanes = 256;
 __global__ void __launch_bounds__(kEngineLanes) k_engine_sums(Params P, LevelView L, int mode);
 __global__ void k_engine_finish(Params P, LevelView L, int mode, int all);
 __global__ void k_set_int(int *dst, const int *src);
+// the explicit time step: the level's smallest local time step (256 threads a block)
+__global__ void k_min_dt_init(LevelView L);
+__global__ void k_min_dt(LevelView L);
 // steps of the cycle on a level view (group form: every case of a group)
 template <bool B = false>
 __global__ void k_case_cycle(CaseArg<B, LevelView> L, const int *src);

@@ -247,12 +247,13 @@ __global__ void k_sa_stage(Params P, LevelView L, int mode, int stage, int turb)
     const unsigned char cls = L.bc[i];
     // convection from k_sa_conv (after the time difference of an unsteady
     // stage, which is all of it when the turbulence is not recomputed)
-    double r = turb ? L.rhs[o6] : (P.unsteady && mode == MODE_STAGE ? time_difference(P, L, i, 5) : 0.0);
+    double r = turb ? L.rhs[o6] : (P.addts && mode == MODE_STAGE ? time_difference(P, L, i, 5) : 0.0);
     if (turb) r = sa_source(P, L, i, r);
     // restrictGrid adds the (last computed) diffusion term whether or not
     // the turbulence is recomputed (def_par:12238-12240, 12315-12317)
     if (turb || mode != MODE_STAGE) r = r + L.turbDiff[i];
-    r = L.dtT[i] * r / L.V[i];
+    // solveTurbulenceSystem: the local step, or the explicit global one
+    r = ((P.unsteady && P.explicit_) ? *L.ptsg : L.dtT[i]) * r / L.V[i];
     if (sa_wall(cls) || is_exhaust(cls)) r = 0.0;
     if (is_inlet(cls)) r = P.engRelax * r;  // the engine inlets' relaxation (def_par:5084-5099)
     if (L.grid > 1 && (cls == BC_FAR3 || is_engine(cls))) r = 0.0;  // nullifyOuterBoundary

@@ -155,6 +155,13 @@ class Solver:
     def init_freestream(self):
         self._ck(self.be.init_freestream(self._h), "init_freestream")
 
+    def explicit_time_step(self):
+        """ivd%physicalTimeStep after the last cycle of an explicit run (the
+        smallest local time step of the last makeTimeSteps)."""
+        v = ctypes.c_double()
+        self._ck(self.be.explicit_time_step(self._h, ctypes.byref(v)), "explicit_time_step")
+        return v.value
+
     def start(self):
         self._ck(self.be.start(self._h), "start")
 

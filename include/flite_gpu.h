@@ -205,6 +205,12 @@ int flite_start(flite_ctx *ctx);
  * divides the local step by 1 + 1.5 dt / physicalTimeStep (def_par:
  * 1427-1442; solveTurbulenceSystem does not).  On a static mesh the
  * previous volumes are the volumes.                                         */
+/* Explicit time stepping (explicit = 1 with flowType 1 or 2, def_par:386-394,
+ * 1427-1517, 13598-13607): no time differences, and every node's solve takes
+ * ivd%physicalTimeStep, which each makeTimeSteps sets to the smallest local
+ * time step of its level.  The value after the last cycle (the step the host
+ * adds to its current time, mg_par:711-713):                               */
+int flite_explicit_time_step(flite_ctx *ctx, double *dt);
 int flite_next_physical_step(flite_ctx *ctx);
 /* Moving meshes (flowType 2, ALE): the geometry of the next physical step,
  * read from that step's .sol (mg_par:525-545, readComputationData with the

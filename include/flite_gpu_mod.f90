@@ -138,6 +138,12 @@ module flite_gpu
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    ! explicit time stepping: ivd%physicalTimeStep after the last cycle
+    integer(c_int) function flite_explicit_time_step(ctx, dt) bind(C, name="flite_explicit_time_step")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: dt
+    end function
 
     ! the geometry of the next physical step of a moving mesh (flowType 2),
     ! in place of readComputationData(COMPINFILE, 1) (mg_par:525-545)

@@ -173,7 +173,11 @@ struct Oracle {
     flite_controls c;
     std::vector<Level> lv;
     int nvar = 5;
-    bool engines = false;  // the mesh has engine faces or nodes (indicators 5..8)
+    bool engines = false;
+    // ivd%physicalTimeStep: the control's value, and under explicit time
+    // stepping the smallest local time step of the last makeTimeSteps
+    // (def_par:13598-13607), whichever level it ran on
+    double pts_global = 0.0;  // the mesh has engine faces or nodes (indicators 5..8)
     std::vector<vec> nh;  // nodeHelpArray(:,1:25), sized for level 1
     double RK[5] = {0.6, 0.6, 1.0, 0.0, 0.0};  // def_par:14240-14244
     int nstage = 3;
@@ -250,6 +254,12 @@ struct Oracle {
             }
         });
         for_nodes(g.N, [&](int i) { g.dt[i] = 0.5 / (g.dt[i] / g.V[i] + h1[i] / (g.V[i] * g.V[i])); });
+        if (c.explicit_) {
+            double minVal = 9999999.9;
+            for (int i = 0; i < g.N; ++i)
+                if (g.dt[i] < minVal) minVal = g.dt[i];
+            pts_global = minVal;
+        }
     }
 
     // ---- makeArtificialDissipation2, scalar form (def_par:11484-11993) ----
@@ -1601,15 +1611,18 @@ struct Oracle {
     // ---- solveSystem (def_par:1407-1479) + solveTurbulenceSystem
     // (def_par:1481-1522) -------------------------------------------------
     void solveSystem(Level &g, vec *rhs) {
-        // flowType != 0: the dual-time step dt / (1 + 1.5 dt / physicalTimeStep)
-        // (def_par:1427-1442)
+        // flowType != 0: the dual-time step dt / (1 + 1.5 dt / physicalTimeStep),
+        // or under explicit time stepping ivd%physicalTimeStep for every node
+        // (def_par:1427-1442; solveTurbulenceSystem :1505-1517)
         const bool unsteady = c.flowType != 0;
+        const bool glob = unsteady && c.explicit_;
         for_nodes(g.N, [&](int i) {
             double dt = g.dt[i];
-            if (unsteady) dt = dt / (1.0 + 1.5 * dt / c.physicalTimeStep);
+            if (glob) dt = pts_global;
+            else if (unsteady) dt = dt / (1.0 + 1.5 * dt / c.physicalTimeStep);
             for (int k = 0; k < 5; ++k) rhs[k][i] = dt * rhs[k][i] / g.V[i];
         });
-        if (sa()) for_nodes(g.N, [&](int i) { rhs[5][i] = g.dtT[i] * rhs[5][i] / g.V[i]; });
+        if (sa()) for_nodes(g.N, [&](int i) { rhs[5][i] = (glob ? pts_global : g.dtT[i]) * rhs[5][i] / g.V[i]; });
     }
 
     double relaxation_param(const Level &g) const {
@@ -1865,7 +1878,7 @@ struct Oracle {
     // ---- addTimeDifferences (def_par:1184-1241): on a static mesh the
     // previous volumes are the volumes ----------------------------------------
     void addTimeDifferences(Level &g) {
-        if (c.flowType == 0) return;
+        if (c.flowType == 0 || c.explicit_) return;  // addTimeStep (def_par:386-394, 1195)
         const double dtp = c.physicalTimeStep;
         if (g.grid == 1 && c.timeScheme == 2) {
             const vec &Vp = c.flowType == 2 ? g.Vp : g.V, &Vp2 = c.flowType == 2 ? g.Vp2 : g.V;
@@ -2266,7 +2279,7 @@ int check_controls(const flite_controls &c) {
     // flowType 1: dual time on a static mesh; 2: on a moving mesh
     if (c.flowType != 0 && !(c.physicalTimeStep > 0)) return FLITE_EUNSUPPORTED;
     if (c.flowType == 2 && c.reconstruction != FLITE_RECON_NONE) return FLITE_EUNSUPPORTED;
-    if ((c.flowType != 0 && c.flowType != 1 && c.flowType != 2) || c.explicit_ || c.SAS || c.GUSTMODEL || c.movingwall ||
+    if ((c.flowType != 0 && c.flowType != 1 && c.flowType != 2) || c.SAS || c.GUSTMODEL || c.movingwall ||
         c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
         c.prolongationSmoothingFactor > 0)
         return FLITE_EUNSUPPORTED;
@@ -2942,6 +2955,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
     Oracle &o = ctx->o;
     o.c = *c;
     o.set_stages(c->rungeKuttaStages);
+    o.pts_global = c->physicalTimeStep;
     o.nvar = c->turbulenceModel == 1 ? 6 : 5;
     int G = nlevels;
     if (c->numberOfGridsToUse > 0) G = std::min(G, c->numberOfGridsToUse);
@@ -3097,6 +3111,12 @@ static void physical_step_head(Oracle &O) {
             if (O.c.flowType != 0) O.mapFineToCoarse(O.lv[l - 1], O.lv[l], O.lv[l - 1].uold, O.lv[l].uold, O.nvar);
         }
     }
+}
+
+int oracle_explicit_time_step(oracle_ctx *o, double *dt) {
+    if (!o || !dt) return FLITE_EINVAL;
+    *dt = o->o.pts_global;
+    return FLITE_OK;
 }
 
 int oracle_next_physical_step(oracle_ctx *o) {

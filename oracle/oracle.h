@@ -24,6 +24,7 @@ int oracle_create(const flite_controls *c, int nlevels, const flite_level_desc *
 int oracle_destroy(oracle_ctx *o);
 int oracle_set_state(oracle_ctx *o, int level, const double *u);
 int oracle_get_state(oracle_ctx *o, int level, double *u);
+int oracle_explicit_time_step(oracle_ctx *o, double *dt);
 int oracle_get_pressure(oracle_ctx *o, int level, double *p);
 /* named per-level arrays: "dt", "diss", "rhs", "uprev", "src", "normal",
  * "wallArea", "conn", "mu", "grad" (15 columns of nodeHelpArray)          */

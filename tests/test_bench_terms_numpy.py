@@ -515,3 +515,44 @@ def test_compact_viscous_term(geo, isentropic, bterm):
     wide = viscous_term(default_controls(ReynoldsNumber=5000.0, wallsAreIsentropic=isentropic), geo, u,
                         np.abs(pressure(c, u)))[0]
     assert np.abs(wide[1:] - term[1:]).max() > 1e-6 * np.abs(term[1:]).max()
+
+
+@pytest.mark.parametrize("re", [0.0, 5000.0], ids=["inviscid", "laminar"])
+def test_one_explicit_iteration_in_the_interior(re):
+    # explicit time stepping (explicit with flowType 1, def_par:386-394,
+    # 1427-1442, 13598-13607): no time differences, and every node's solve
+    # takes the smallest local time step of the level
+    g = Geo(16, 8, 8, seed=5)
+    c = default_controls(ReynoldsNumber=re, fluxType=1, numberOfGridsToUse=1, CFLNumber=1.0,
+                         wallsAreIsentropic=1, maxIncrementFactor=0.02, flowType=1, physicalTimeStep=0.2,
+                         explicit_=1)
+    o = Solver(c, g.mesh, backend=oracle_backend())
+    u0 = _state(c, g, seed=8)
+    o.set_state(u0)
+    o.start()
+    u0 = o.get_state(1)
+    mu = np.zeros(g.N)
+    assert o.be.get_array(o._h, 1, b"mu", _ptr(mu)) == 0
+    assert o.explicit_time_step() == 0.2  # the control's value until a time step is made
+    o.do_time_iterations(1, 1, True, 1)
+    got = o.get_state(1)
+
+    p = np.abs(pressure(c, u0))
+    dt = time_steps(c, g, u0, p, mu)
+    dtg = dt.min()
+    np.testing.assert_allclose(o.explicit_time_step(), dtg, rtol=TOL)
+    diss = jst_scalar(c, g, u0, p, dt)
+    if re > 0:
+        diss = diss + viscous_term(c, g, u0, p)[0]
+    u = u0.copy()
+    for alpha in (0.6, 0.6, 1.0):
+        rhs = central_rhs(c, g, u, pressure(c, u)) + diss
+        delu = c.CFLNumber * alpha * (dtg * rhs / g.V)
+        new = u0 - delu
+        big = np.abs(delu[0] / u0[0]) >= c.maxIncrementFactor
+        new[0] = np.where(big, u0[0] - np.sign(delu[0]) * c.maxIncrementFactor * u0[0], new[0])
+        new[0] = np.maximum(new[0], c.minimumDensity)
+        u = new
+    deep = _hops_from_boundary(g) >= 3
+    _close(u[:, deep], got[:, deep])
+    assert np.abs(u[:, deep] - u0[:, deep]).max() > 1e-8

@@ -61,3 +61,36 @@ def test_unsteady_spalart_allmaras_steps_match(ctl):
             assert a.shape[0] == 6 and np.array_equal(a, b), (step, level)
         g.next_physical_step()
         o.next_physical_step()
+
+
+@pytest.mark.parametrize("ctl", [dict(numberOfGridsToUse=1), dict(), dict(ReynoldsNumber=500.0, CFLNumber=0.5),
+                                 dict(ReynoldsNumber=1.0e5, turbulenceModel=1, wallsAreIsentropic=1, CFLNumber=0.5)])
+def test_explicit_time_stepping_matches(ctl):
+    # explicit time stepping: no time differences, the smallest local time
+    # step of the last makeTimeSteps for every node (on any level, the
+    # reference's global ivd%physicalTimeStep), advancing the current time
+    mesh = Mesh.bump_channel(24, 8, 8, 0.05, nlevels=3)
+    base = dict(ReynoldsNumber=0.0, fluxType=1, CFLNumber=1.0, numberOfGridsToUse=3, flowType=1,
+                physicalTimeStep=0.2, explicit_=1)
+    c = default_controls(**{**base, **ctl})
+    g, o = Solver(c, mesh), Solver(c, mesh, backend=oracle_backend())
+    u0 = initial_state(c, mesh, perturb_seed=5, amplitude=0.02)
+    for s in (g, o):
+        s.set_state(u0)
+        s.start()
+    t = 0.0
+    for it in range(1, 7):
+        g.cycle(it)
+        o.cycle(it)
+        dt = g.explicit_time_step()
+        assert dt == o.explicit_time_step() and 0.0 < dt < 1.0
+        t += dt
+        for level in range(1, c.numberOfGridsToUse + 1):
+            a, b = g.get_state(level), o.get_state(level)
+            assert np.all(np.isfinite(b)), (it, level)
+            assert np.array_equal(a, b), (it, level, np.abs(a - b).max())
+        assert np.allclose(g.forces(), o.forces(), rtol=1e-12, atol=1e-300)
+    assert t > 0.0
+    g.close()
+    o.close()
+    mesh.close()
