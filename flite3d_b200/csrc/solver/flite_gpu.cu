@@ -119,8 +119,12 @@ const char *unsupported_reason(const flite_controls &c) {
         return "moving meshes (flowType 2) take the reference's fluxes (no reconstruction extension)";
     if (c.forceCalcType != 1 && c.forceCalcType != 3)
         return "forceCalcType must be 1 or 3 (2 is the spanwise load of gust runs)";
-    if (c.SAS || c.GUSTMODEL || c.movingwall || c.patchInitialization || c.nspan != 0)
-        return "SAS, gust, moving-wall, patch initialisation and spanwise loads are not supported";
+    // SAS acts only on the SST model (turbulenceModel 3, def_par:1053-1056, 9002)
+    // and patchInitialization only in the interactive start-up of
+    // communicateSeq (setUpInitialField, def_par:3620-3675; mg_par:1579): both
+    // are read and have no effect on this path, as in the reference's solver
+    if (c.GUSTMODEL || c.movingwall || c.nspan != 0)
+        return "gust, moving-wall and spanwise loads are not supported";
     if (c.residualSmoothingFactor > 0 || c.prolongationSmoothingFactor > 0)
         return "residual and prolongation smoothing are not supported";
     if (c.turbulenceModel != 0 && c.turbulenceModel != 1)

@@ -79,7 +79,9 @@ typedef struct flite_controls {
     double maxTurbulenceValue, turbulentPrandtlNumber;
     double referenceArea, datum[3], groundplane;
     int    forceCalcType, restartNumber, numberOfProcesses;
-    /* controls the path rejects unless they hold their steady default */
+    /* controls the path rejects unless they hold their steady default (SAS
+     * and patchInitialization change nothing on this path, as in the
+     * reference's solver; flowType and explicit_ are taken)                 */
     int    flowType, explicit_, SAS, GUSTMODEL, movingwall, patchInitialization, nspan;
     int    timeScheme, numberOfRSSteps, numberOfPSSteps;
     double residualSmoothingFactor, prolongationSmoothingFactor, physicalTimeStep;

@@ -2279,8 +2279,10 @@ int check_controls(const flite_controls &c) {
     // flowType 1: dual time on a static mesh; 2: on a moving mesh
     if (c.flowType != 0 && !(c.physicalTimeStep > 0)) return FLITE_EUNSUPPORTED;
     if (c.flowType == 2 && c.reconstruction != FLITE_RECON_NONE) return FLITE_EUNSUPPORTED;
-    if ((c.flowType != 0 && c.flowType != 1 && c.flowType != 2) || c.SAS || c.GUSTMODEL || c.movingwall ||
-        c.patchInitialization || c.nspan != 0 || c.residualSmoothingFactor > 0 ||
+    // SAS (SST only) and patchInitialization (communicateSeq's start-up only)
+    // have no effect on this path
+    if ((c.flowType != 0 && c.flowType != 1 && c.flowType != 2) || c.GUSTMODEL || c.movingwall ||
+        c.nspan != 0 || c.residualSmoothingFactor > 0 ||
         c.prolongationSmoothingFactor > 0)
         return FLITE_EUNSUPPORTED;
     // Spalart-Allmaras (1) is on the path and needs a viscous run; k-omega

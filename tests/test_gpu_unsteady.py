@@ -89,7 +89,10 @@ def test_explicit_time_stepping_matches(ctl):
             a, b = g.get_state(level), o.get_state(level)
             assert np.all(np.isfinite(b)), (it, level)
             assert np.array_equal(a, b), (it, level, np.abs(a - b).max())
-        assert np.allclose(g.forces(), o.forces(), rtol=1e-12, atol=1e-300)
+        # the force sums run in another order on the device: a component
+        # that cancels (the lateral force) is close to the scale of the others
+        fg, fo = g.forces(), o.forces()
+        np.testing.assert_allclose(fg, fo, rtol=1e-12, atol=1e-12 * np.abs(fo).max())
     assert t > 0.0
     g.close()
     o.close()
