@@ -78,7 +78,7 @@ struct flite_batch {
                x.flowType == y.flowType && x.reconstruction == y.reconstruction &&
                x.HLLCFluxOrder == y.HLLCFluxOrder && x.GradientMethod == y.GradientMethod &&
                x.Automaticlipping == y.Automaticlipping && a.lv.size() == b.lv.size() &&
-               a.P.engines == b.P.engines;
+               a.P.engines == b.P.engines && x.explicit_ == y.explicit_;
     }
     // the cycle graph of a case group led by its first case, or nullptr
     // when the group's path has no group form

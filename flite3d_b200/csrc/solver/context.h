@@ -591,6 +591,8 @@ struct flite_ctx {
             else FLITE_LAUNCH(k_node_update, (GATHER_DELTA, U,), g, nb, 0, P, V(l), mode, stage);
         } else if (fused()) {
             if (unroll == 2 && U == 1) FLITE_LAUNCH(k_node_update, (GATHER_CENTRAL2, 1,), g, nb, 0, P, V(l), mode, stage);
+            else if (U == 1 && !P.engines && !(P.unsteady && P.explicit_))
+                FLITE_LAUNCH(k_node_update, (GATHER_LEAN, 1,), g, nb, 0, P, V(l), mode, stage);
             else FLITE_LAUNCH(k_node_update, (GATHER_CENTRAL, U,), g, nb, 0, P, V(l), mode, stage);
         } else {
             FLITE_LAUNCH(k_node_update, (GATHER_BUFFER, U,), g, nb, 0, P, V(l), mode, stage);

@@ -22,6 +22,9 @@ __device__ __forceinline__ bool is_exhaust(unsigned char c) { return c == BC_EOU
 struct Params {
     double gamma, gm1, CFL, maxInc, minRho, Re, am, k2, k4, cgdf, pts, Tinf, mach;
     double mgBCRelax, prolRelax, clip, Pr;
+    // the HLLC wave-speed factor sqrt((gamma-1)/(2 gamma)) (def_par:1826, 1953),
+    // correctly rounded on the host like the per-edge expression it replaces
+    double hllcBeta0;
     double inf[12];
     // stage coefficients: the reference's three (def_par:14240-14244) or the
     // five of the extension; recon selects the MUSCL reconstruction of the
@@ -310,7 +313,9 @@ __device__ __forceinline__ void remove_normal(double *x, double n0, double n1, d
     x[3] = x[3] - s * n2;
 }
 
-// setBCsOnIncrementField (def_par:4978-5140)
+// setBCsOnIncrementField (def_par:4978-5140); ENG = false leaves out the
+// engine classes (for a level without engine nodes)
+template <bool ENG = true>
 __device__ __forceinline__ void bc_increment(const Params &P, unsigned char cls, double n0, double n1, double n2,
                                              double *r) {
     if (cls == BC_WALL) {
@@ -322,9 +327,9 @@ __device__ __forceinline__ void bc_increment(const Params &P, unsigned char cls,
         }
     } else if (cls == BC_IWALL || cls == BC_SYM) {
         remove_normal(r, n0, n1, n2, 1.0);
-    } else if (is_inlet(cls)) {  // engine inlets relaxed (def_par:5084-5099)
+    } else if (ENG && is_inlet(cls)) {  // engine inlets relaxed (def_par:5084-5099)
         for (int c = 0; c < 5; ++c) r[c] = P.engRelax * r[c];
-    } else if (is_exhaust(cls)) {  // engine exhausts held (def_par:5100-5125)
+    } else if (ENG && is_exhaust(cls)) {  // engine exhausts held (def_par:5100-5125)
         for (int c = 0; c < 5; ++c) r[c] = 0.0;
     }
 }
@@ -390,13 +395,16 @@ __device__ __forceinline__ double eo_relax(const Params &P, int cycle) {
 // the state of an engine exhaust node (def_par:4497-4540); returns the
 // exhaust pressure, which the reference stores into grp%p
 __device__ __forceinline__ double bc_exhaust(const Params &P, unsigned char cls, double rp, double *u) {
-    const double *rear = &P.rear[cls == BC_EOUT1 ? 0 : 7];
-    for (int c = 0; c < 5; ++c) u[c] = (1.0 - rp) * P.inf[c] + rp * rear[c];
-    return (1.0 - rp) * P.inf[5] + rp * rear[5];
+    // the exhaust's column selected per component: constant offsets into
+    // the parameters, which keeps them out of local memory
+    const bool one = cls == BC_EOUT1;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) u[c] = (1.0 - rp) * P.inf[c] + rp * (one ? P.rear[c] : P.rear[7 + c]);
+    return (1.0 - rp) * P.inf[5] + rp * (one ? P.rear[5] : P.rear[12]);
 }
 // the exhaust nu~ (def_par:4507-4509, 4528-4530)
 __device__ __forceinline__ double sa_exhaust(const Params &P, unsigned char cls, double rp) {
-    return rp * P.rear[cls == BC_EOUT1 ? 6 : 13];
+    return rp * (cls == BC_EOUT1 ? P.rear[6] : P.rear[13]);
 }
 
 // density update with the increment clip (def_par:1343-1366)

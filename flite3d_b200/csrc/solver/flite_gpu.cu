@@ -274,7 +274,8 @@ int flite::create_context(const flite_controls *c, int nlevels, const flite_leve
         flite_ctx &X = *ctx;
         X.c = *c;
         Params &P = X.P;
-        P.gamma = c->gamma; P.gm1 = c->gamma - 1.0; P.CFL = c->CFLNumber; P.maxInc = c->maxIncrementFactor;
+        P.gamma = c->gamma; P.gm1 = c->gamma - 1.0; P.hllcBeta0 = std::sqrt(P.gm1 / (2 * P.gamma));
+        P.CFL = c->CFLNumber; P.maxInc = c->maxIncrementFactor;
         P.minRho = c->minimumDensity; P.Re = c->ReynoldsNumber; P.am = c->ReynoldsNumber > 0 ? 1.0 / c->ReynoldsNumber : 0.0;
         P.k2 = c->secondOrderDissipationFactor; P.k4 = c->fourthOrderDissipationFactor;
         P.cgdf = c->coarseGridDissipationFactor; P.pts = c->physicalTimeStep; P.Tinf = c->inflowTemperature;

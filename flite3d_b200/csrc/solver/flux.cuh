@@ -229,7 +229,7 @@ __device__ __forceinline__ void edge_flux(const Params &P, const LevelView &L, i
     }
     double nv1 = (u1 * rnx + v1 * rny) + w1 * rnz;
     double nv2 = (u2 * rnx + v2 * rny) + w2 * rnz;
-    double beta0 = sqrt(gam1 / (2 * gam));
+    const double beta0 = P.hllcBeta0;
     double rroe = sqrt(roe2 / roe1);
     double ut = (u1 + u2 * rroe) / (1 + rroe), vt = (v1 + v2 * rroe) / (1 + rroe);
     double wt = (w1 + w2 * rroe) / (1 + rroe);

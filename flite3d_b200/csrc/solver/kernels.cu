@@ -1689,6 +1689,9 @@ __device__ __forceinline__ void store_anchor(const LevelView &L, int i, const do
 // time differences, dissipation, solveSystem, the increment conditions, the
 // clipped update and the solution and outer conditions, or the restrictGrid
 // one-step forms (modes as in k_node_update)
+// LEAN: a run without engine conditions and without explicit time stepping
+// (the branches for those are left out of the code)
+template <bool LEAN = false>
 __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, int i, double *r, int mode,
                                           int stage) {
     const int N = L.N;
@@ -1702,15 +1705,15 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
     double dt = L.dt[i];
     const double V = L.V[i];
     // solveSystem's dual-time step, or the explicit global step (def_par:1427-1442)
-    if (P.unsteady) dt = P.explicit_ ? *L.ptsg : dt / (1.0 + 1.5 * dt / P.dtp);
+    if (P.unsteady) dt = (!LEAN && P.explicit_) ? *L.ptsg : dt / (1.0 + 1.5 * dt / P.dtp);
     for (int c = 0; c < 5; ++c) r[c] = dt * r[c] / V;  // solveSystem
     const unsigned char cls = L.bc[i];
     double n0 = 0, n1 = 0, n2 = 0;
     if (cls != BC_NONE) { n0 = L.nx[i]; n1 = L.ny[i]; n2 = L.nz[i]; }
-    bc_increment(P, cls, n0, n1, n2, r);
+    bc_increment<!LEAN>(P, cls, n0, n1, n2, r);
     // nullifyOuterBoundary (coarse levels): zeroes the far-field (indicator
     // 3) and engine increments for the SA model and is a no-op otherwise
-    if (P.sa && L.grid > 1 && (cls == BC_FAR3 || is_engine(cls))) r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
+    if (P.sa && L.grid > 1 && (cls == BC_FAR3 || (!LEAN && is_engine(cls)))) r[0] = r[1] = r[2] = r[3] = r[4] = 0.0;
     const double dtJ = stage > 0 ? P.CFL * P.RK[stage - 1] : P.CFL;
     double d[5], up[5], un[5];
     for (int c = 0; c < 5; ++c) { d[c] = dtJ * r[c]; up[c] = L.uprev[c * N + i]; }
@@ -1725,13 +1728,13 @@ __device__ __forceinline__ void node_tail(const Params &P, const LevelView &L, i
     double cm0 = 0, cm1 = 0, cm2 = 0;
     if (cls == BC_WALL && P.viscous) { cm0 = L.cmx[i]; cm1 = L.cmy[i]; cm2 = L.cmz[i]; }
     bc_solution(P, cls, n0, n1, n2, cm0, cm1, cm2, relax_param(P, *L.cyc), un);
-    if (is_exhaust(cls)) {
+    if (!LEAN && is_exhaust(cls)) {
         // the exhaust pressure matters on level 1 only: coarse pressures are
         // recomputed before anything reads them
         const double pex = bc_exhaust(P, cls, eo_relax(P, *L.cyc), un);
         if (L.eng.f) L.eng.pbc[i] = pex;
     }
-    if (L.eng.f && mode != MODE_RCOARSE && (P.eftype == 2 || is_engine(cls))) {
+    if (!LEAN && L.eng.f && mode != MODE_RCOARSE && (P.eftype == 2 || is_engine(cls))) {
         // level 1: the engine inlet terms need every node's state first;
         // k_engine_finish completes the node (the candidate state of
         // restrictGrid's fine step goes to rhs)
@@ -1795,7 +1798,7 @@ __global__ void __launch_bounds__(256, PREC == GATHER_CENTRAL2 ? 2 : (U == 1 ? 3
     if constexpr (U > 1)
         if (!active || gl) return;
     if constexpr (PREC == GATHER_ANCHOR) store_anchor(L, i, rint);
-    node_tail(P, L, i, r, mode, stage);
+    node_tail<PREC == GATHER_LEAN>(P, L, i, r, mode, stage);
 }
 // ---- the same node update with the central fluxes gathered from a
 // shared-memory stage of the node block (GATHER_CENTRAL, a thread per node).
@@ -2179,6 +2182,8 @@ template __global__ void k_node_update<GATHER_BUFFER, 16, false>(Params, LevelVi
 template __global__ void k_node_update<GATHER_BUFFER, 16, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 32, false>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_BUFFER, 32, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
+template __global__ void k_node_update<GATHER_LEAN, 1, false>(Params, LevelView, int, int);
+template __global__ void k_node_update<GATHER_LEAN, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 1, false>(Params, LevelView, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 1, true>(CaseTab<Params>, CaseTab<LevelView>, int, int);
 template __global__ void k_node_update<GATHER_CENTRAL, 4, false>(Params, LevelView, int, int);

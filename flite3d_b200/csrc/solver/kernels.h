@@ -47,7 +47,10 @@ template <int FT, bool O2>
 __global__ void k_edge_flux(Params P, LevelView L);
 template <bool B = false>
 __global__ void k_bnd_flux(CaseArg<B, Params> P, CaseArg<B, LevelView> L);
-enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3, GATHER_CENTRAL2 = 4 };
+// GATHER_LEAN: GATHER_CENTRAL for runs without engine conditions and
+// without explicit time stepping, whose node tail leaves those branches out
+// (they cost the thread-per-node form its last free registers)
+enum { GATHER_BUFFER = 0, GATHER_CENTRAL = 1, GATHER_ANCHOR = 2, GATHER_DELTA = 3, GATHER_CENTRAL2 = 4, GATHER_LEAN = 5 };
 template <int PREC, int U, bool B = false>
 __global__ void k_node_update(CaseArg<B, Params> P, CaseArg<B, LevelView> L, int mode, int stage);
 // gathers: U lanes per node (1 = a thread per node); by default levels
